@@ -1,0 +1,576 @@
+// ctx.cu -- context, mask set-up and the C-ABI entry points (include/getm_b200.h).
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "common.cuh"
+#include "launch.h"
+
+struct getm_ctx {
+  getm_domain dom;
+  gb::Dev dev;
+  cudaStream_t stream = nullptr;
+  int device = 0;
+  uint8_t* planes = nullptr;   // 8 byte masks of init_advection, n2d each (see MaskPlane)
+  int32_t* zmask = nullptr;    // copies of az, au, av (n2d each)
+  bool adv_ready = false;
+  void* scr[3] = {nullptr, nullptr, nullptr};  // 3D scratch: tracer ping-pong, hi, adv
+  size_t scr_bytes = 0;
+  double* red = nullptr;                // reduction partials (2*RED_BLOCKS) + result (2)
+  unsigned long long* cnt = nullptr;    // [0] warnings, [1] range-check count
+  std::string err;
+  // per-stage device timers (the counterpart of getm_timers' tic/toc, getm_timers.F90:275-357)
+  bool timing = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending[GETM_NTIMERS];
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pool;
+  double total_ms[GETM_NTIMERS] = {};
+  long long launches[GETM_NTIMERS] = {};
+};
+
+namespace {
+// Records a CUDA event pair around one launch when timing is enabled.
+struct TimerScope {
+  getm_ctx* c;
+  int slot;
+  std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
+  TimerScope(getm_ctx* c_, int slot_) : c(c_), slot(slot_) {
+    if (!c || !c->timing) return;
+    if (!c->pool.empty()) {
+      ev = c->pool.back();
+      c->pool.pop_back();
+    } else {
+      cudaEventCreate(&ev.first);
+      cudaEventCreate(&ev.second);
+    }
+    cudaEventRecord(ev.first, c->stream);
+  }
+  ~TimerScope() {
+    if (!ev.first) return;
+    cudaEventRecord(ev.second, c->stream);
+    c->pending[slot].push_back(ev);
+  }
+};
+}  // namespace
+
+namespace gb {
+
+enum MaskPlane { P_UPDATEH = 0, P_UFLUX, P_VFLUX, P_XFLUX, P_UUPDATEU, P_VUPDATEV, P_UFLUX_U, P_VFLUX_V, NPLANES };
+
+static long long n2d(const Dev& d) { return d.sj * (long long)d.nj(); }
+static long long n3d(const Dev& d) { return d.sk * (long long)(d.kmax + 1); }
+
+// init_advection (advection.F90:263-318) from az/au/av/ax.
+__global__ void k_build_masks(Dev d, const int32_t* __restrict__ az, const int32_t* __restrict__ au,
+                              const int32_t* __restrict__ av, const int32_t* __restrict__ ax, uint8_t* planes) {
+  const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+  const int jj = blockIdx.y * blockDim.y + threadIdx.y;
+  const int ni = d.ni(), nj = d.nj();
+  if (ii >= ni || jj >= nj) return;
+  const long long c = (long long)ii + (long long)jj * d.sj;
+  const long long n = d.sj * (long long)nj;
+  const bool last_i = (ii == ni - 1), last_j = (jj == nj - 1);
+  planes[P_UPDATEH * n + c] = az[c] == 1;
+  planes[P_UFLUX * n + c] = (au[c] == 1 || au[c] == 2) && !last_i;
+  planes[P_VFLUX * n + c] = (av[c] == 1 || av[c] == 2) && !last_j;
+  planes[P_XFLUX * n + c] = ax[c] == 1 && !last_i && !last_j;
+  planes[P_UUPDATEU * n + c] = au[c] == 1;
+  planes[P_VUPDATEV * n + c] = av[c] == 1;
+  // U grid u-flux = mask_updateH(i+1,j); V grid v-flux = mask_updateH(i,j+1)
+  planes[P_UFLUX_U * n + c] = !last_i && az[c + 1] == 1;
+  planes[P_VFLUX_V * n + c] = !last_j && az[c + d.sj] == 1;
+}
+
+int run_build_masks(const Dev& d, cudaStream_t s, const int32_t* az, const int32_t* au, const int32_t* av,
+                    const int32_t* ax, uint8_t* planes) {
+  dim3 blk(64, 4, 1);
+  dim3 grd((d.ni() + 63) / 64, (d.nj() + 3) / 4, 1);
+  k_build_masks<<<grd, blk, 0, s>>>(d, az, au, av, ax, planes);
+  return (int)cudaGetLastError();
+}
+
+}  // namespace gb
+
+using namespace gb;
+
+static int fail(getm_ctx* c, int code, const char* what) {
+  if (c) c->err = what;
+  return code;
+}
+
+static int cuda_fail(getm_ctx* c, int e, const char* where) {
+  if (e == 0) return GETM_OK;
+  if (c) c->err = std::string(where) + ": " + cudaGetErrorString((cudaError_t)e);
+  return GETM_ERR_CUDA;
+}
+
+#define GB_TRY(expr, where)                                   \
+  do {                                                        \
+    int _e = (int)(expr);                                     \
+    if (_e != 0) return cuda_fail(ctx, _e, where);            \
+  } while (0)
+
+#define GB_TIMED(slot, expr, where)                           \
+  do {                                                        \
+    TimerScope _ts(ctx, slot);                                \
+    int _e = (int)(expr);                                     \
+    if (_e != 0) return cuda_fail(ctx, _e, where);            \
+  } while (0)
+
+static int ensure_scratch(getm_ctx* ctx, size_t bytes) {
+  if (ctx->scr_bytes >= bytes) return GETM_OK;
+  for (auto& p : ctx->scr) {
+    if (p) cudaFree(p);
+    p = nullptr;
+  }
+  ctx->scr_bytes = 0;
+  for (auto& p : ctx->scr)
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(ctx, GETM_ERR_NOMEM, "scratch allocation failed");
+    }
+  ctx->scr_bytes = bytes;
+  return GETM_OK;
+}
+
+static bool grid_for_tag(const getm_ctx* ctx, int tag, getm_adv_grid* g) {
+  const long long n = n2d(ctx->dev);
+  const uint8_t* P = ctx->planes;
+  const int32_t* az = ctx->zmask;
+  const int32_t* au = ctx->zmask + n;
+  const int32_t* av = ctx->zmask + 2 * n;
+  switch (tag) {
+    case GETM_H_TAG:
+    case GETM_D_TAG:
+    case GETM_W_TAG:
+      *g = {P + P_UFLUX * n, P + P_VFLUX * n, P + P_UPDATEH * n, P + P_UPDATEH * n, P + P_UPDATEH * n, az};
+      return true;
+    case GETM_U_TAG:
+      *g = {P + P_UFLUX_U * n, P + P_XFLUX * n, P + P_UUPDATEU * n, P + P_UFLUX * n, P + P_UFLUX * n, au};
+      return true;
+    case GETM_V_TAG:
+      *g = {P + P_XFLUX * n, P + P_VFLUX_V * n, P + P_VFLUX * n, P + P_VUPDATEV * n, P + P_VFLUX * n, av};
+      return true;
+    default:
+      return false;
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// do_advection_3d (advection_3d.F90:279-566) on device pointers (level-0 origin).
+template <class R>
+static int do_adv3d(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, const R* hu,
+                    const R* hv, const R* ho, const R* hn, int split, int hs, int vs, R AH, int tag, R* hires,
+                    R* advres, int iters) {
+  (void)hn;
+  if (!ctx) return GETM_ERR_ARG;
+  if (!ctx->adv_ready) return fail(ctx, GETM_ERR_STATE, "getm_init_advection has not been called");
+  getm_adv_grid g;
+  if (!grid_for_tag(ctx, tag, &g)) return fail(ctx, GETM_ERR_ARG, "do_advection_3d: tag is invalid");
+  if (!f || !ho) return fail(ctx, GETM_ERR_ARG, "do_advection_3d: null field");
+  if (hs != NOADV && !is_split_scheme(hs)) {
+    if (hs == UPSTREAM_2DH || hs == 7 || hs == 8 || hs == 9)
+      return fail(ctx, GETM_ERR_UNSUPPORTED, "do_advection_3d: 2DH schemes are not provided");
+    return fail(ctx, GETM_ERR_ARG, "do_advection_3d: hscheme is invalid");
+  }
+  if (vs != NOADV && !is_split_scheme(vs)) return fail(ctx, GETM_ERR_ARG, "do_advection_3d: vscheme is invalid");
+  if (iters < 1) iters = 1;
+  if (iters > 1 && ctx->dom.kmax > 128)
+    return fail(ctx, GETM_ERR_UNSUPPORTED, "adv_ver_iterations > 1 needs kmax <= 128");
+  const Dev& d = ctx->dev;
+  cudaStream_t s = ctx->stream;
+  const int kmax = d.kmax;
+  const long long sk = d.sk;
+  const long long n3 = n3d(d);
+  const size_t bytes3 = (size_t)n3 * sizeof(R);
+  const int kshift = (tag == GETM_W_TAG) ? 1 : 0;
+  int rc = ensure_scratch(ctx, bytes3);
+  if (rc) return rc;
+  R* S = (R*)ctx->scr[0];
+  R* H = hires ? hires : (R*)ctx->scr[1];
+  const bool needs_adv = (hs != NOADV && vs != NOADV && (split == GETM_NOSPLIT || split == GETM_HVSPLIT)) ||
+                         (hs != NOADV && vs == NOADV && split == GETM_NOSPLIT);
+  R* A = advres ? advres : (needs_adv ? (R*)ctx->scr[2] : nullptr);
+  if (A) GB_TRY(cudaMemsetAsync(A, 0, bytes3, s), "memset adv");
+  auto L = [&](auto* p, int k) { return p + (long long)k * sk; };
+  const R half = R(0.5), one = R(1);
+  unsigned long long* warn = ctx->cnt;
+
+  if (hs == NOADV || vs == NOADV || kmax < 1) {
+    // p_hi = ho over the whole array
+    GB_TIMED(GETM_TIM_COPY, cudaMemcpyAsync(H, ho, bytes3, cudaMemcpyDeviceToDevice, s), "copy ho");
+  } else {
+    // level 0 of p_hi (the sweeps below write levels 1..kmax from ho)
+    GB_TRY(cudaMemcpyAsync(H, ho, (size_t)sk * sizeof(R), cudaMemcpyDeviceToDevice, s), "copy ho(0)");
+  }
+  if (hs == NOADV && vs == NOADV) return GETM_OK;
+  if (hs == NOADV) {
+    if (kmax > 1) GB_TIMED(GETM_TIM_ADV_W, run_sweep_w<R>(d, s, dt, one, vs, kshift, iters, f, f, f, H, A, ww, g.az, warn), "w");
+    return GETM_OK;
+  }
+  const int nk = kmax;
+  if (vs == NOADV) {
+    // per-level 2D do_advection (advection.F90:469-666) on levels 1..kmax
+    if (split == GETM_NOSPLIT) {
+      GB_TIMED(GETM_TIM_COPY, cudaMemcpyAsync(S, f, bytes3, cudaMemcpyDeviceToDevice, s), "copy f");
+      GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<R, 0>(d, s, nk, dt, one, hs, AH, L(f, 1), L(S, 1), L(S, 1), L(H, 1), L(H, 1), L(A, 1),
+                                L(uu, 1), L(hu, 1), g.mask_uflux, g.mask_uupdate)), "u");
+      GB_TIMED(GETM_TIM_ADV_V, (run_sweep_h<R, 1>(d, s, nk, dt, one, hs, AH, L(f, 1), L(S, 1), L(S, 1), L(H, 1), L(H, 1), L(A, 1),
+                                L(vv, 1), L(hv, 1), g.mask_vflux, g.mask_vupdate)), "v");
+      GB_TIMED(GETM_TIM_ADV_FINALISE, run_finalise<R>(d, s, dt, f, ho, A, H, g.mask_finalise), "finalise");
+    } else if (split == GETM_FULLSPLIT) {
+      GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<R, 0>(d, s, nk, dt, one, hs, AH, L(f, 1), L(f, 1), L(S, 1), L(ho, 1), L(H, 1),
+                                A ? L(A, 1) : nullptr, L(uu, 1), L(hu, 1), g.mask_uflux, g.mask_uupdate)), "u");
+      GB_TIMED(GETM_TIM_ADV_V, (run_sweep_h<R, 1>(d, s, nk, dt, one, hs, AH, L(S, 1), L(S, 1), L(f, 1), L(H, 1), L(H, 1),
+                                A ? L(A, 1) : nullptr, L(vv, 1), L(hv, 1), g.mask_vflux, g.mask_vupdate)), "v");
+    } else if (split == GETM_HALFSPLIT) {
+      GB_TIMED(GETM_TIM_COPY, cudaMemcpyAsync(S, f, bytes3, cudaMemcpyDeviceToDevice, s), "copy f");
+      GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<R, 0>(d, s, nk, dt, half, hs, AH, L(S, 1), L(S, 1), L(f, 1), L(ho, 1), L(H, 1),
+                                A ? L(A, 1) : nullptr, L(uu, 1), L(hu, 1), g.mask_uflux, g.mask_uupdate)), "u");
+      GB_TIMED(GETM_TIM_ADV_V, (run_sweep_h<R, 1>(d, s, nk, dt, one, hs, AH, L(f, 1), L(f, 1), L(S, 1), L(H, 1), L(H, 1),
+                                A ? L(A, 1) : nullptr, L(vv, 1), L(hv, 1), g.mask_vflux, g.mask_vupdate)), "v");
+      GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<R, 0>(d, s, nk, dt, half, hs, AH, L(S, 1), L(S, 1), L(f, 1), L(H, 1), L(H, 1),
+                                A ? L(A, 1) : nullptr, L(uu, 1), L(hu, 1), g.mask_uflux, g.mask_uupdate)), "u");
+    } else {
+      return fail(ctx, GETM_ERR_ARG, "do_advection: split is invalid");
+    }
+    return GETM_OK;
+  }
+  R* Al = A ? L(A, 1) : nullptr;
+  switch (split) {
+    case GETM_NOSPLIT:
+      GB_TIMED(GETM_TIM_COPY, cudaMemcpyAsync(S, f, bytes3, cudaMemcpyDeviceToDevice, s), "copy f");
+      GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<R, 0>(d, s, nk, dt, one, hs, AH, L(f, 1), L(S, 1), L(S, 1), L(ho, 1), L(H, 1), Al,
+                                L(uu, 1), L(hu, 1), g.mask_uflux, g.mask_uupdate)), "u");
+      GB_TIMED(GETM_TIM_ADV_V, (run_sweep_h<R, 1>(d, s, nk, dt, one, hs, AH, L(f, 1), L(S, 1), L(S, 1), L(H, 1), L(H, 1), Al,
+                                L(vv, 1), L(hv, 1), g.mask_vflux, g.mask_vupdate)), "v");
+      if (kmax > 1) GB_TIMED(GETM_TIM_ADV_W, run_sweep_w<R>(d, s, dt, one, vs, kshift, 1, f, S, S, H, A, ww, g.az, warn), "w");
+      GB_TIMED(GETM_TIM_ADV_FINALISE, run_finalise<R>(d, s, dt, f, ho, A, H, g.mask_finalise), "finalise");
+      break;
+    case GETM_FULLSPLIT:
+      GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<R, 0>(d, s, nk, dt, one, hs, AH, L(f, 1), L(f, 1), L(S, 1), L(ho, 1), L(H, 1), Al,
+                                L(uu, 1), L(hu, 1), g.mask_uflux, g.mask_uupdate)), "u");
+      GB_TIMED(GETM_TIM_ADV_V, (run_sweep_h<R, 1>(d, s, nk, dt, one, hs, AH, L(S, 1), L(S, 1), L(f, 1), L(H, 1), L(H, 1), Al,
+                                L(vv, 1), L(hv, 1), g.mask_vflux, g.mask_vupdate)), "v");
+      if (kmax > 1) GB_TIMED(GETM_TIM_ADV_W, run_sweep_w<R>(d, s, dt, one, vs, kshift, iters, f, f, f, H, A, ww, g.az, warn), "w");
+      break;
+    case GETM_HALFSPLIT:
+      GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<R, 0>(d, s, nk, dt, half, hs, AH, L(f, 1), L(f, 1), L(S, 1), L(ho, 1), L(H, 1), Al,
+                                L(uu, 1), L(hu, 1), g.mask_uflux, g.mask_uupdate)), "u1");
+      GB_TIMED(GETM_TIM_ADV_V, (run_sweep_h<R, 1>(d, s, nk, dt, half, hs, AH, L(S, 1), L(S, 1), L(f, 1), L(H, 1), L(H, 1), Al,
+                                L(vv, 1), L(hv, 1), g.mask_vflux, g.mask_vupdate)), "v1");
+      if (kmax > 1) GB_TIMED(GETM_TIM_ADV_W, run_sweep_w<R>(d, s, dt, one, vs, kshift, iters, f, f, f, H, A, ww, g.az, warn), "w");
+      GB_TIMED(GETM_TIM_ADV_V, (run_sweep_h<R, 1>(d, s, nk, dt, half, hs, AH, L(f, 1), L(f, 1), L(S, 1), L(H, 1), L(H, 1), Al,
+                                L(vv, 1), L(hv, 1), g.mask_vflux, g.mask_vupdate)), "v2");
+      GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<R, 0>(d, s, nk, dt, half, hs, AH, L(S, 1), L(S, 1), L(f, 1), L(H, 1), L(H, 1), Al,
+                                L(uu, 1), L(hu, 1), g.mask_uflux, g.mask_uupdate)), "u2");
+      break;
+    case GETM_HVSPLIT:
+      GB_TIMED(GETM_TIM_COPY, cudaMemcpyAsync(S, f, bytes3, cudaMemcpyDeviceToDevice, s), "copy f");
+      GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<R, 0>(d, s, nk, dt, one, hs, AH, L(f, 1), L(S, 1), L(S, 1), L(ho, 1), L(H, 1), Al,
+                                L(uu, 1), L(hu, 1), g.mask_uflux, g.mask_uupdate)), "u");
+      GB_TIMED(GETM_TIM_ADV_V, (run_sweep_h<R, 1>(d, s, nk, dt, one, hs, AH, L(f, 1), L(S, 1), L(S, 1), L(H, 1), L(H, 1), Al,
+                                L(vv, 1), L(hv, 1), g.mask_vflux, g.mask_vupdate)), "v");
+      GB_TIMED(GETM_TIM_ADV_FINALISE, run_finalise<R>(d, s, dt, f, ho, A, H, g.mask_finalise), "finalise");
+      if (kmax > 1) GB_TIMED(GETM_TIM_ADV_W, run_sweep_w<R>(d, s, dt, one, vs, kshift, iters, f, f, f, H, A, ww, g.az, warn), "w");
+      break;
+    default:
+      return fail(ctx, GETM_ERR_ARG, "do_advection_3d: split is invalid");
+  }
+  return GETM_OK;
+}
+
+template <class R>
+static int sweep_h_api(getm_ctx* ctx, int dir, int nk, R dt, const R* f, R* fi, R* Di, R* adv, const R* U,
+                       const R* DU, R splitfac, int scheme, R AH, const uint8_t* mflux, const uint8_t* mupd) {
+  if (!ctx || !f || !fi || !Di || !U || !DU || !mflux || !mupd || nk < 1)
+    return fail(ctx, GETM_ERR_ARG, "adv_split: bad argument");
+  if (!is_split_scheme(scheme)) return fail(ctx, GETM_ERR_ARG, "adv_split: scheme is invalid");
+  const Dev& d = ctx->dev;
+  const R* src = f;
+  if (f == fi) {
+    // in-place call: fluxes must see the pre-sweep field (the reference's separate flux phase)
+    const size_t bytes = (size_t)(d.sk * (long long)(nk - 1) + n2d(d)) * sizeof(R);
+    int rc = ensure_scratch(ctx, (size_t)n3d(d) * sizeof(R) > bytes ? (size_t)n3d(d) * sizeof(R) : bytes);
+    if (rc) return rc;
+    GB_TRY(cudaMemcpyAsync(ctx->scr[0], f, bytes, cudaMemcpyDeviceToDevice, ctx->stream), "copy f");
+    src = (const R*)ctx->scr[0];
+  }
+  int e = dir == 0 ? run_sweep_h<R, 0>(d, ctx->stream, nk, dt, splitfac, scheme, AH, src, fi, fi, Di, Di, adv, U,
+                                       DU, mflux, mupd)
+                   : run_sweep_h<R, 1>(d, ctx->stream, nk, dt, splitfac, scheme, AH, src, fi, fi, Di, Di, adv, U,
+                                       DU, mflux, mupd);
+  return cuda_fail(ctx, e, "adv_split");
+}
+
+template <class R>
+static int vdiff_api(getm_ctx* ctx, R dt, R cnpar, R avmol, R* S, const R* hn, const R* nuh, const int32_t* az,
+                     const R* src) {
+  if (!ctx || !S || !hn || !nuh || !az) return fail(ctx, GETM_ERR_ARG, "tracer_vdiff: bad argument");
+  if ((size_t)2 * (ctx->dom.kmax + 1) * 64 * sizeof(R) > 200 * 1024)
+    return fail(ctx, GETM_ERR_UNSUPPORTED, "tracer_vdiff: kmax too large");
+  GB_TIMED(GETM_TIM_VDIFF, run_vdiff<R>(ctx->dev, ctx->stream, dt, cnpar, avmol, S, hn, nuh, az, src), "tracer_vdiff");
+  return GETM_OK;
+}
+
+template <class R>
+static int tracer_step(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, const R* hu, const R* hv,
+                       const R* ho, const R* hn, const R* nuh, int split, int hs, int vs, R AH, R cnpar, R avmol,
+                       int iters) {
+  int rc = do_adv3d<R>(ctx, dt, f, uu, vv, ww, hu, hv, ho, hn, split, hs, vs, AH, GETM_H_TAG, nullptr, nullptr,
+                       iters);
+  if (rc) return rc;
+  return vdiff_api<R>(ctx, dt, cnpar, avmol, f, hn, nuh, ctx->zmask, nullptr);
+}
+
+template <class R>
+static int content_api(getm_ctx* ctx, const R* f, const R* h, const int32_t* az, double* out) {
+  if (!ctx || !f || !h || !az || !out) return fail(ctx, GETM_ERR_ARG, "tracer_content: bad argument");
+  GB_TRY(run_content<R>(ctx->dev, ctx->stream, f, h, az, ctx->red, ctx->red + 2 * RED_BLOCKS), "content");
+  double r[2];
+  GB_TRY(cudaMemcpyAsync(r, ctx->red + 2 * RED_BLOCKS, sizeof(r), cudaMemcpyDeviceToHost, ctx->stream), "read");
+  GB_TRY(cudaStreamSynchronize(ctx->stream), "sync");
+  *out = r[0];
+  return GETM_OK;
+}
+
+extern "C" {
+
+const char* getm_version(void) { return "getm-b200 0.1 (sm_100a)"; }
+
+int getm_ctx_create(const getm_domain* dom, void* stream, getm_ctx** out) {
+  if (!dom || !out) return GETM_ERR_ARG;
+  *out = nullptr;
+  if (dom->imax < dom->imin || dom->jmax < dom->jmin || dom->kmax < 0) return GETM_ERR_ARG;
+  const long long ni = dom->imax - dom->imin + 1 + 2 * HALO;
+  const long long nj = dom->jmax - dom->jmin + 1 + 2 * HALO;
+  if (dom->sj < ni || dom->sk < dom->sj * nj) return GETM_ERR_ARG;
+  if (!(dom->dx > 0) || !(dom->dy > 0) || !(dom->ard1 > 0)) return GETM_ERR_ARG;
+  getm_ctx* ctx = new getm_ctx();
+  ctx->dom = *dom;
+  ctx->dev = to_dev(*dom);
+  ctx->stream = (cudaStream_t)stream;
+  cudaGetDevice(&ctx->device);
+  const long long n = n2d(ctx->dev);
+  if (cudaMalloc(&ctx->planes, (size_t)n * NPLANES) != cudaSuccess ||
+      cudaMalloc(&ctx->zmask, (size_t)n * 3 * sizeof(int32_t)) != cudaSuccess ||
+      cudaMalloc(&ctx->red, (2 * RED_BLOCKS + 2) * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&ctx->cnt, 2 * sizeof(unsigned long long)) != cudaSuccess) {
+    cudaGetLastError();
+    getm_ctx_destroy(ctx);
+    return GETM_ERR_NOMEM;
+  }
+  if (cudaMemsetAsync(ctx->cnt, 0, 2 * sizeof(unsigned long long), ctx->stream) != cudaSuccess) {
+    getm_ctx_destroy(ctx);
+    return GETM_ERR_CUDA;
+  }
+  *out = ctx;
+  return GETM_OK;
+}
+
+int getm_ctx_destroy(getm_ctx* ctx) {
+  if (!ctx) return GETM_OK;
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream); else cudaDeviceSynchronize();
+  cudaFree(ctx->planes);
+  cudaFree(ctx->zmask);
+  cudaFree(ctx->red);
+  cudaFree(ctx->cnt);
+  for (auto p : ctx->scr) cudaFree(p);
+  for (int t = 0; t < GETM_NTIMERS; ++t)
+    for (auto& ev : ctx->pending[t]) ctx->pool.push_back(ev);
+  for (auto& ev : ctx->pool) {
+    cudaEventDestroy(ev.first);
+    cudaEventDestroy(ev.second);
+  }
+  delete ctx;
+  return GETM_OK;
+}
+
+int getm_ctx_set_stream(getm_ctx* ctx, void* stream) {
+  if (!ctx) return GETM_ERR_ARG;
+  ctx->stream = (cudaStream_t)stream;
+  return GETM_OK;
+}
+
+int getm_ctx_take_warnings(getm_ctx* ctx, int64_t* n_warnings) {
+  if (!ctx || !n_warnings) return GETM_ERR_ARG;
+  unsigned long long h = 0;
+  GB_TRY(cudaMemcpyAsync(&h, ctx->cnt, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream), "read warnings");
+  GB_TRY(cudaMemsetAsync(ctx->cnt, 0, sizeof(h), ctx->stream), "reset warnings");
+  GB_TRY(cudaStreamSynchronize(ctx->stream), "sync");
+  *n_warnings = (int64_t)h;
+  return GETM_OK;
+}
+
+const char* getm_ctx_last_error(const getm_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+static const char* kTimerNames[GETM_NTIMERS] = {"adv_split_u", "adv_split_v", "adv_split_w", "adv_finalise",
+                                                 "tracer_vdiff", "copy", "tracer_fused_uv",
+                                                 "tracer_fused_wvu", "reserved8", "reserved9", "reserved10",
+                                                 "reserved11", "reserved12", "reserved13", "reserved14",
+                                                 "reserved15"};
+
+const char* getm_timer_name(int slot) {
+  return (slot >= 0 && slot < GETM_NTIMERS) ? kTimerNames[slot] : "";
+}
+
+static void drain_timers(getm_ctx* ctx) {
+  for (int t = 0; t < GETM_NTIMERS; ++t) {
+    for (auto& ev : ctx->pending[t]) {
+      float ms = 0.f;
+      cudaEventSynchronize(ev.second);
+      cudaEventElapsedTime(&ms, ev.first, ev.second);
+      ctx->total_ms[t] += ms;
+      ctx->launches[t] += 1;
+      ctx->pool.push_back(ev);
+    }
+    ctx->pending[t].clear();
+  }
+}
+
+int getm_timers_enable(getm_ctx* ctx, int on) {
+  if (!ctx) return GETM_ERR_ARG;
+  ctx->timing = on != 0;
+  return GETM_OK;
+}
+
+int getm_timers_reset(getm_ctx* ctx) {
+  if (!ctx) return GETM_ERR_ARG;
+  drain_timers(ctx);
+  for (int t = 0; t < GETM_NTIMERS; ++t) {
+    ctx->total_ms[t] = 0.0;
+    ctx->launches[t] = 0;
+  }
+  return GETM_OK;
+}
+
+int getm_timers_read(getm_ctx* ctx, int slot, double* total_ms, int64_t* launches) {
+  if (!ctx || slot < 0 || slot >= GETM_NTIMERS || !total_ms || !launches) return GETM_ERR_ARG;
+  drain_timers(ctx);
+  *total_ms = ctx->total_ms[slot];
+  *launches = ctx->launches[slot];
+  return GETM_OK;
+}
+
+int getm_init_advection(getm_ctx* ctx, const int32_t* az, const int32_t* au, const int32_t* av,
+                        const int32_t* ax) {
+  if (!ctx || !az || !au || !av || !ax) return fail(ctx, GETM_ERR_ARG, "init_advection: null mask");
+  const long long n = n2d(ctx->dev);
+  GB_TRY(run_build_masks(ctx->dev, ctx->stream, az, au, av, ax, ctx->planes), "build masks");
+  GB_TRY(cudaMemcpyAsync(ctx->zmask, az, n * sizeof(int32_t), cudaMemcpyDeviceToDevice, ctx->stream), "az");
+  GB_TRY(cudaMemcpyAsync(ctx->zmask + n, au, n * sizeof(int32_t), cudaMemcpyDeviceToDevice, ctx->stream), "au");
+  GB_TRY(cudaMemcpyAsync(ctx->zmask + 2 * n, av, n * sizeof(int32_t), cudaMemcpyDeviceToDevice, ctx->stream),
+         "av");
+  ctx->adv_ready = true;
+  return GETM_OK;
+}
+
+int getm_adv_grid_for_tag(const getm_ctx* ctx, int tag, getm_adv_grid* out) {
+  if (!ctx || !out) return GETM_ERR_ARG;
+  if (!ctx->adv_ready) return GETM_ERR_STATE;
+  return grid_for_tag(ctx, tag, out) ? GETM_OK : GETM_ERR_ARG;
+}
+
+int getm_adv_split_u(getm_ctx* ctx, int nk, double dt, const double* f, double* fi, double* Di, double* adv,
+                     const double* U, const double* DU, double splitfac, int scheme, double AH,
+                     const uint8_t* mask_flux, const uint8_t* mask_update) {
+  return sweep_h_api<double>(ctx, 0, nk, dt, f, fi, Di, adv, U, DU, splitfac, scheme, AH, mask_flux, mask_update);
+}
+
+int getm_adv_split_v(getm_ctx* ctx, int nk, double dt, const double* f, double* fi, double* Di, double* adv,
+                     const double* V, const double* DV, double splitfac, int scheme, double AH,
+                     const uint8_t* mask_flux, const uint8_t* mask_update) {
+  return sweep_h_api<double>(ctx, 1, nk, dt, f, fi, Di, adv, V, DV, splitfac, scheme, AH, mask_flux, mask_update);
+}
+
+int getm_adv_split_w(getm_ctx* ctx, double dt, const double* f, double* fi, double* hi, double* adv,
+                     const double* ww, double splitfac, int scheme, int tag, const int32_t* az, int itersmax) {
+  if (!ctx || !f || !fi || !hi || !ww || !az) return fail(ctx, GETM_ERR_ARG, "adv_split_w: bad argument");
+  if (scheme == NOADV) return GETM_OK;
+  if (!is_split_scheme(scheme)) return fail(ctx, GETM_ERR_ARG, "adv_split_w: scheme is invalid");
+  if (itersmax > 1 && ctx->dom.kmax > 128)
+    return fail(ctx, GETM_ERR_UNSUPPORTED, "adv_split_w: itersmax > 1 needs kmax <= 128");
+  const int kshift = (tag == GETM_W_TAG) ? 1 : 0;
+  return cuda_fail(ctx,
+                   run_sweep_w<double>(ctx->dev, ctx->stream, dt, splitfac, scheme, kshift, itersmax < 1 ? 1 : itersmax,
+                                       f, fi, fi, hi, adv, ww, az, ctx->cnt),
+                   "adv_split_w");
+}
+
+int getm_do_advection_3d(getm_ctx* ctx, double dt, double* f, const double* uu, const double* vv,
+                         const double* ww, const double* hu, const double* hv, const double* ho,
+                         const double* hn, int split, int hscheme, int vscheme, double AH, int tag,
+                         double* hires, double* advres, int adv_ver_iterations) {
+  return do_adv3d<double>(ctx, dt, f, uu, vv, ww, hu, hv, ho, hn, split, hscheme, vscheme, AH, tag, hires,
+                          advres, adv_ver_iterations);
+}
+
+int getm_do_advection_3d_f32(getm_ctx* ctx, float dt, float* f, const float* uu, const float* vv,
+                             const float* ww, const float* hu, const float* hv, const float* ho, const float* hn,
+                             int split, int hscheme, int vscheme, float AH, int tag, float* hires,
+                             float* advres, int adv_ver_iterations) {
+  return do_adv3d<float>(ctx, dt, f, uu, vv, ww, hu, hv, ho, hn, split, hscheme, vscheme, AH, tag, hires, advres,
+                         adv_ver_iterations);
+}
+
+int getm_tridiagonal_columns(getm_ctx* ctx, int ncol, int kmax, int fi, int lt, const double* au,
+                             const double* bu, const double* cu, const double* du, double* value) {
+  if (!ctx || ncol < 0 || kmax < 1 || fi < 0 || lt > kmax || fi >= lt || !au || !bu || !cu || !du || !value)
+    return fail(ctx, GETM_ERR_ARG, "tridiagonal: bad argument");
+  if (ncol == 0) return GETM_OK;
+  if ((size_t)2 * (kmax + 1) * 64 * sizeof(double) > 200 * 1024)
+    return fail(ctx, GETM_ERR_UNSUPPORTED, "tridiagonal: kmax too large");
+  return cuda_fail(ctx, run_tridiag<double>(ctx->stream, ncol, kmax, fi, lt, au, bu, cu, du, value), "tridiagonal");
+}
+
+
+int getm_tracer_vdiff(getm_ctx* ctx, double dt, double cnpar, double avmol, double* S, const double* hn,
+                      const double* nuh, const int32_t* az, const double* src) {
+  return vdiff_api<double>(ctx, dt, cnpar, avmol, S, hn, nuh, az, src);
+}
+
+int getm_tracer_vdiff_f32(getm_ctx* ctx, float dt, float cnpar, float avmol, float* S, const float* hn,
+                          const float* nuh, const int32_t* az, const float* src) {
+  return vdiff_api<float>(ctx, dt, cnpar, avmol, S, hn, nuh, az, src);
+}
+
+
+int getm_tracer_step(getm_ctx* ctx, double dt, double* f, const double* uu, const double* vv, const double* ww,
+                     const double* hu, const double* hv, const double* ho, const double* hn, const double* nuh,
+                     int split, int hscheme, int vscheme, double AH, double cnpar, double avmol,
+                     int adv_ver_iterations) {
+  return tracer_step<double>(ctx, dt, f, uu, vv, ww, hu, hv, ho, hn, nuh, split, hscheme, vscheme, AH, cnpar, avmol,
+                             adv_ver_iterations);
+}
+
+int getm_tracer_step_f32(getm_ctx* ctx, float dt, float* f, const float* uu, const float* vv, const float* ww,
+                         const float* hu, const float* hv, const float* ho, const float* hn, const float* nuh,
+                         int split, int hscheme, int vscheme, float AH, float cnpar, float avmol,
+                         int adv_ver_iterations) {
+  return tracer_step<float>(ctx, dt, f, uu, vv, ww, hu, hv, ho, hn, nuh, split, hscheme, vscheme, AH, cnpar, avmol,
+                            adv_ver_iterations);
+}
+
+
+int getm_tracer_content(getm_ctx* ctx, const double* f, const double* h, const int32_t* az, double* out) {
+  return content_api<double>(ctx, f, h, az, out);
+}
+
+int getm_tracer_content_f32(getm_ctx* ctx, const float* f, const float* h, const int32_t* az, double* out) {
+  return content_api<float>(ctx, f, h, az, out);
+}
+
+int getm_check_3d_fields(getm_ctx* ctx, const double* f, const int32_t* az, double minval, double maxval,
+                         int64_t* status) {
+  if (!ctx || !f || !az || !status) return fail(ctx, GETM_ERR_ARG, "check_3d_fields: bad argument");
+  GB_TRY(cudaMemsetAsync(ctx->cnt + 1, 0, sizeof(unsigned long long), ctx->stream), "reset");
+  GB_TRY(run_check_range<double>(ctx->dev, ctx->stream, f, az, minval, maxval, ctx->cnt + 1), "check");
+  unsigned long long h = 0;
+  GB_TRY(cudaMemcpyAsync(&h, ctx->cnt + 1, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream), "read");
+  GB_TRY(cudaStreamSynchronize(ctx->stream), "sync");
+  *status = (int64_t)h;
+  return GETM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,473 @@
+// kernels.cuh -- CUDA kernels of the hot path, templated on the arithmetic type R.
+// Instantiated for double in kernels_f64.cu (built without FMA contraction so that every
+// expression rounds exactly as the reference's) and for float in kernels_f32.cu.
+#pragma once
+#include "common.cuh"
+#include "launch.h"
+
+namespace gb {
+
+// ---------------------------------------------------------------------------------------------
+// Horizontal split sweeps (adv_split_u.F90:205-285, adv_split_v.F90:63-135).
+//
+// One thread per cell of the haloed plane and level. A cell in the update range with
+// mask_update computes the fluxes of both of its faces (each face is evaluated identically by
+// its two neighbours, so the result equals the reference's flux array) from the read-only
+// stencil source f, then writes fi_dst / Di_dst; every other cell copies fi_src / Di_src through
+// when source and destination differ. f must not alias fi_dst (callers ping-pong); fi_src may
+// alias fi_dst and Di_src may alias Di_dst (a cell reads and writes only itself).
+// Flux through the face between cell q and its +DIR neighbour (reference phase 1). p is the
+// 3D offset of the face's cell, c its 2D offset, st the element stride along the sweep
+// direction (1 for u, sj for v).
+template <class R>
+__device__ __forceinline__ R face_flux(const R* __restrict__ f, const R* __restrict__ U,
+                                       const R* __restrict__ DU, const uint8_t* __restrict__ mflux,
+                                       long long p, long long c, long long st, int scheme, R dti, R AH,
+                                       bool use_AH, R dxf) {
+  if (!mflux[c]) return R(0);
+  const R Uf = U[p];
+  R fu, cfl = R(0), fuu = R(0), fd = R(0);
+  bool lim = false;
+  if (Uf > R(0)) {
+    fu = f[p];
+    if (scheme != UPSTREAM) lim = mflux[c - st] != 0;
+    if (lim) {
+      cfl = Uf / DU[p] * dti / dxf;
+      fuu = f[p - st];
+      fd = f[p + st];
+    }
+  } else {
+    fu = f[p + st];
+    if (scheme != UPSTREAM) lim = mflux[c + st] != 0;
+    if (lim) {
+      cfl = -Uf / DU[p] * dti / dxf;
+      fuu = f[p + 2 * st];
+      fd = f[p];
+    }
+  }
+  if (lim) fu = recon<R>(scheme, cfl, fuu, fu, fd);
+  R fl = Uf * fu;
+  if (use_AH) fl = fl - AH * DU[p] * (f[p + st] - f[p]) / dxf;
+  return fl;
+}
+
+// DIR 0 = u (adv_split_u), 1 = v (adv_split_v)
+template <class R, int DIR>
+__global__ void __launch_bounds__(256) k_sweep_h(Dev d, R dt, R splitfac, int scheme, R AH,
+                                                 const R* __restrict__ f, const R* fi_src, R* fi_dst,
+                                                 const R* Di_src, R* Di_dst, R* adv,
+                                                 const R* __restrict__ U, const R* __restrict__ DU,
+                                                 const uint8_t* __restrict__ mflux,
+                                                 const uint8_t* __restrict__ mupd) {
+  const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+  const int jj = blockIdx.y * blockDim.y + threadIdx.y;
+  if (ii >= d.ni() || jj >= d.nj()) return;
+  const long long c = (long long)ii + (long long)jj * d.sj;
+  const long long p = c + (long long)blockIdx.z * d.sk;
+  const int sub = (scheme == UPSTREAM) ? 0 : 1;
+  // index along the sweep direction, in reference numbering
+  const int q = (DIR == 0) ? ii + d.imin - HALO : jj + d.jmin - HALO;
+  const int qmin = (DIR == 0) ? d.imin : d.jmin;
+  const int qmax = (DIR == 0) ? d.imax : d.jmax;
+  const bool in_range = (q >= qmin - HALO + 1 + sub) && (q <= qmax + HALO - 1 - sub);
+  if (in_range && mupd[c]) {
+    const long long st = (DIR == 0) ? 1 : d.sj;
+    const R dti = splitfac * dt;
+    const bool use_AH = AH > R(0);
+    const R dxf = (DIR == 0) ? R(d.dx) : R(d.dy);  // DXU / DYV
+    const R dyf = (DIR == 0) ? R(d.dy) : R(d.dx);  // DYU / DXV
+    const R ard1 = R(d.ard1);
+    const R fe = face_flux<R>(f, U, DU, mflux, p, c, st, scheme, dti, AH, use_AH, dxf);
+    const R fw = face_flux<R>(f, U, DU, mflux, p - st, c - st, st, scheme, dti, AH, use_AH, dxf);
+    const R Dio = Di_src[p];
+    const R Dn = Dio - dti * (U[p] * dyf - U[p - st] * dyf) * ard1;
+    const R advn = splitfac * (fe * dyf - fw * dyf) * ard1;
+    const R fio = fi_src[p];
+    Di_dst[p] = Dn;
+    fi_dst[p] = (Dio * fio - dt * advn) / Dn;
+    if (adv) adv[p] = adv[p] + advn;
+  } else {
+    if (fi_dst != fi_src) fi_dst[p] = fi_src[p];
+    if (Di_dst != Di_src) Di_dst[p] = Di_src[p];
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Vertical split sweep (adv_split_w.F90:158-307) without sub-iterations (itersmax = 1):
+// one thread per water column, k-sequential, streaming with a register window so that every
+// level of f and hi is read before it is overwritten -- f, fi and hi may therefore alias.
+template <class R>
+__device__ __forceinline__ R wface(int k, int kshift, int kmax, int scheme, R dti, R w, R fkm1, R fk,
+                                   R fkp1, R fkp2, R hk, R hkp1) {
+  R fu, fuu = R(0), fd = R(0);
+  bool lim = false;
+  if (w > R(0)) {
+    fu = fk;
+    if (scheme != UPSTREAM) lim = (k > 1 - kshift);
+    if (lim) { fuu = fkm1; fd = fkp1; }
+  } else {
+    fu = fkp1;
+    if (scheme != UPSTREAM) lim = (k < kmax - 1);
+    if (lim) { fuu = fkp2; fd = fk; }
+  }
+  if (lim) {
+    const R cfl = fabs(w) * dti / (R(0.5) * (hk + hkp1));
+    fu = recon<R>(scheme, cfl, fuu, fu, fd);
+  }
+  return w * fu;
+}
+
+template <class R>
+__global__ void __launch_bounds__(128) k_sweep_w(Dev d, R dt, R splitfac, int scheme, int kshift,
+                                                 const R* f, const R* fi_src, R* fi_dst, R* hi, R* adv,
+                                                 const R* __restrict__ ww,
+                                                 const int32_t* __restrict__ az) {
+  const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+  const int jj = blockIdx.y * blockDim.y + threadIdx.y;
+  // columns i = imin-2..imax+1, j = jmin-2..jmax+1 (adv_split_w.F90:160-162)
+  if (ii >= d.ni() - 1 || jj >= d.nj() - 1) return;
+  const long long c = (long long)ii + (long long)jj * d.sj;
+  if (az[c] != 1) return;
+  const int kmax = d.kmax;
+  const long long sk = d.sk;
+  const R dti = splitfac * dt;
+  auto F = [&](int k) -> R { return (k >= 0 && k <= kmax) ? f[c + k * sk] : R(0); };
+  auto H = [&](int k) -> R { return (k >= 0 && k <= kmax) ? hi[c + k * sk] : R(0); };
+  R wprev = R(0);  // wflux(k-1); wflux(0) = 0 unless W_TAG computes face 0
+  if (kshift == 1) wprev = wface<R>(0, 1, kmax, scheme, dti, ww[c], R(0), F(0), F(1), F(2), H(0), H(1));
+  // register window for face k = 1: f(0..3), hi(1..2)
+  R a = F(0), b = F(1), e = F(2), g = F(3);
+  R hA = H(1), hB = H(2);
+  R wkm1 = ww[c];
+  for (int k = 1; k <= kmax - kshift; ++k) {
+    const R wk = ww[c + k * sk];
+    R wfl = R(0);
+    if (k <= kmax - 1) wfl = wface<R>(k, kshift, kmax, scheme, dti, wk, a, b, e, g, hA, hB);
+    const R hio = hA;
+    const R hin = hio - dti * (wk - wkm1);
+    const R advn = splitfac * (wfl - wprev);
+    const R fio = fi_src[c + k * sk];
+    // read the next window entries before this level is overwritten (f/hi may alias fi/hi)
+    const R gn = F(k + 3);
+    const R hn2 = H(k + 2);
+    fi_dst[c + k * sk] = (hio * fio - dt * advn) / hin;
+    hi[c + k * sk] = hin;
+    if (adv) adv[c + k * sk] = adv[c + k * sk] + advn;
+    a = b; b = e; e = g; g = gn;
+    hA = hB; hB = hn2;
+    wkm1 = wk;
+    wprev = wfl;
+  }
+}
+
+// adv_split_w with sub-iterations (itersmax > 1, adv_split_w.F90:193-299): the column is held in
+// thread-local arrays (kmax <= GB_KMAX_ITER). Counts columns whose estimate exceeded itersmax.
+#ifndef GB_KMAX_ITER
+#define GB_KMAX_ITER 128
+#endif
+template <class R>
+__global__ void __launch_bounds__(64) k_sweep_w_iter(Dev d, R dt, R splitfac, int scheme, int kshift,
+                                                     int itersmax, const R* f, const R* fi_src,
+                                                     R* fi_dst, R* hi, R* adv,
+                                                     const R* __restrict__ ww,
+                                                     const int32_t* __restrict__ az,
+                                                     unsigned long long* warn) {
+  const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+  const int jj = blockIdx.y * blockDim.y + threadIdx.y;
+  if (ii >= d.ni() - 1 || jj >= d.nj() - 1) return;
+  const long long c = (long long)ii + (long long)jj * d.sj;
+  if (az[c] != 1) return;
+  const int kmax = d.kmax;
+  const long long sk = d.sk;
+  const R dti = splitfac * dt;
+  R fo[GB_KMAX_ITER + 1], fia[GB_KMAX_ITER + 1], hia[GB_KMAX_ITER + 1], ada[GB_KMAX_ITER + 1],
+      wfl[GB_KMAX_ITER + 1], cfl0[GB_KMAX_ITER + 1], cfls[GB_KMAX_ITER + 1];
+  for (int k = 0; k <= kmax; ++k) {
+    fo[k] = f[c + k * sk];
+    cfl0[k] = R(0);
+  }
+  for (int k = 1 - kshift; k <= kmax - 1; ++k)
+    cfl0[k] = fabs(ww[c + k * sk]) * dti / (R(0.5) * (hi[c + k * sk] + hi[c + (k + 1) * sk]));
+  wfl[0] = R(0);
+  wfl[kmax] = R(0);
+  int iters = 1;
+  R itersm1 = R(1), dtik = dti, splitfack = splitfac;
+  const R* faux = fo;
+  int it = 1;
+  while (it <= iters) {
+    if (it == 1) {
+      for (int k = 0; k <= kmax; ++k) {
+        fia[k] = fi_src[c + k * sk];
+        hia[k] = hi[c + k * sk];
+        ada[k] = adv ? adv[c + k * sk] : R(0);
+      }
+      faux = fo;
+      for (int k = 0; k <= kmax; ++k) cfls[k] = cfl0[k];
+    } else if (scheme != UPSTREAM || iters < itersmax) {
+      for (int k = 1 - kshift; k <= kmax - 1; ++k)
+        cfls[k] = fabs(ww[c + k * sk]) * dti / (R(0.5) * (hia[k] + hia[k + 1]));
+    }
+    if (iters < itersmax) {
+      int iters_new = 1;
+      for (int k = 1 - kshift; k <= kmax - 1; ++k) {
+        const int cn = (int)ceil(cfls[k]);
+        iters_new = iters_new > cn ? iters_new : cn;
+      }
+      if (iters_new > iters) {
+        if (iters_new > itersmax) {
+          atomicAdd(warn, 1ull);
+          iters = itersmax;
+        } else {
+          iters = iters_new;
+        }
+        itersm1 = R(1) / R(iters);
+        dtik = dti * itersm1;
+        splitfack = splitfac * itersm1;
+        if (it > 1) {
+          it = 1;
+          continue;
+        }
+      }
+    }
+    for (int k = 1 - kshift; k <= kmax - 1; ++k) {
+      const R w = ww[c + k * sk];
+      R fu, fuu = R(0), fd = R(0);
+      bool lim = false;
+      if (w > R(0)) {
+        fu = faux[k];
+        if (scheme != UPSTREAM) lim = (k > 1 - kshift);
+        if (lim) { fuu = faux[k - 1]; fd = faux[k + 1]; }
+      } else {
+        fu = faux[k + 1];
+        if (scheme != UPSTREAM) lim = (k < kmax - 1);
+        if (lim) { fuu = faux[k + 2]; fd = faux[k]; }
+      }
+      if (lim) fu = recon<R>(scheme, cfls[k] * itersm1, fuu, fu, fd);
+      wfl[k] = w * fu;
+    }
+    for (int k = 1; k <= kmax - kshift; ++k) {
+      const R hio = hia[k];
+      hia[k] = hio - dtik * (ww[c + k * sk] - ww[c + (k - 1) * sk]);
+      const R advn = splitfack * (wfl[k] - wfl[k - 1]);
+      fia[k] = (hio * fia[k] - dt * advn) / hia[k];
+      ada[k] = ada[k] + advn;
+    }
+    faux = fia;
+    ++it;
+  }
+  for (int k = 1; k <= kmax - kshift; ++k) {
+    fi_dst[c + k * sk] = fia[k];
+    hi[c + k * sk] = hia[k];
+    if (adv) adv[c + k * sk] = ada[k];
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Thomas solve of one column (tridiagonal.F90:35-48); ru/qu live in shared memory [k][tid].
+template <class R>
+struct ThomasSmem {
+  R* ru;
+  R* qu;
+  int nt;
+  __device__ R& RU(int k) { return ru[k * nt + threadIdx.x]; }
+  __device__ R& QU(int k) { return qu[k * nt + threadIdx.x]; }
+};
+
+// Implicit vertical diffusion (salinity.F90:348-389; temperature form with src). One thread per
+// interior column; the matrix rows are built top-down as the elimination proceeds.
+template <class R>
+__global__ void __launch_bounds__(64) k_vdiff(Dev d, R dt, R cnpar, R avmol, R* S,
+                                              const R* __restrict__ hn, const R* __restrict__ nuh,
+                                              const int32_t* __restrict__ az, const R* __restrict__ src) {
+  extern __shared__ unsigned char smem_raw[];
+  const int kmax = d.kmax;
+  ThomasSmem<R> sm{reinterpret_cast<R*>(smem_raw), reinterpret_cast<R*>(smem_raw) + (kmax + 1) * blockDim.x,
+                   (int)blockDim.x};
+  const int i = d.imin + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = d.jmin + blockIdx.y;
+  if (i > d.imax || j > d.jmax) return;
+  const long long c = d.ix(i, j);
+  if (az[c] != 1 || kmax <= 1) return;
+  const long long sk = d.sk;
+  auto L = [&](const R* a, int k) -> R { return a[c + k * sk]; };
+  const R co = R(2) * (R(1) - cnpar) * dt;
+  const R cn = R(2) * cnpar * dt;
+  auto auxo = [&](int k) -> R { return co * (L(nuh, k) + avmol) / (L(hn, k + 1) + L(hn, k)); };
+  auto auxn = [&](int k) -> R { return cn * (L(nuh, k) + avmol) / (L(hn, k + 1) + L(hn, k)); };
+  // surface row k = kmax: au = a1, bu = a2, du = a4
+  int k = kmax;
+  R ao_km1 = auxo(k - 1), an_km1 = auxn(k - 1);
+  R Sk = L(S, k), Skm1 = L(S, k - 1);
+  {
+    const R a1 = -an_km1;
+    const R a2 = L(hn, k) + an_km1;
+    R a4 = Sk * (L(hn, k) - ao_km1) + Skm1 * ao_km1;
+    if (src) a4 = a4 + L(src, k);
+    sm.RU(k) = a1 / a2;
+    sm.QU(k) = a4 / a2;
+  }
+  // inner rows k = kmax-1 .. 2
+  for (k = kmax - 1; k >= 2; --k) {
+    const R ao_k = ao_km1, an_k = an_km1;  // aux at interface k (computed as k-1 of row k+1)
+    ao_km1 = auxo(k - 1);
+    an_km1 = auxn(k - 1);
+    const R Skp1 = Sk;
+    Sk = Skm1;
+    Skm1 = L(S, k - 1);
+    const R a3 = -an_k;
+    const R a1 = -an_km1;
+    const R a2 = L(hn, k) + an_k + an_km1;
+    R a4 = Skp1 * ao_k + Sk * (L(hn, k) - ao_k - ao_km1) + Skm1 * ao_km1;
+    if (src) a4 = a4 + L(src, k);
+    const R den = a2 - a3 * sm.RU(k + 1);
+    sm.RU(k) = a1 / den;
+    sm.QU(k) = (a4 - a3 * sm.QU(k + 1)) / den;
+  }
+  // bottom row k = 1 (fi): only qu
+  {
+    k = 1;
+    const R ao_k = ao_km1, an_k = an_km1;
+    const R Skp1 = Sk;  // S(2)
+    const R S1 = Skm1;  // S(1)
+    const R a3 = -an_k;
+    const R a2 = L(hn, 1) + an_k;
+    R a4 = Skp1 * ao_k + S1 * (L(hn, 1) - ao_k);
+    if (src) a4 = a4 + L(src, 1);
+    sm.QU(1) = (a4 - a3 * sm.QU(2)) / (a2 - a3 * sm.RU(2));
+  }
+  R v = sm.QU(1);
+  S[c + 1 * sk] = v;
+  for (k = 2; k <= kmax; ++k) {
+    v = sm.QU(k) - sm.RU(k) * v;
+    S[c + k * sk] = v;
+  }
+}
+
+// getm_tridiagonal on ncol independent columns, coefficients laid out [k][col].
+template <class R>
+__global__ void __launch_bounds__(64) k_tridiag(int ncol, int kmax, int fi, int lt, const R* __restrict__ au,
+                                                const R* __restrict__ bu, const R* __restrict__ cu,
+                                                const R* __restrict__ du, R* value) {
+  extern __shared__ unsigned char smem_raw[];
+  ThomasSmem<R> sm{reinterpret_cast<R*>(smem_raw), reinterpret_cast<R*>(smem_raw) + (kmax + 1) * blockDim.x,
+                   (int)blockDim.x};
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= ncol) return;
+  auto A = [&](const R* a, int k) -> R { return a[(long long)k * ncol + col]; };
+  sm.RU(lt) = A(au, lt) / A(bu, lt);
+  sm.QU(lt) = A(du, lt) / A(bu, lt);
+  for (int i = lt - 1; i >= fi + 1; --i) {
+    const R den = A(bu, i) - A(cu, i) * sm.RU(i + 1);
+    sm.RU(i) = A(au, i) / den;
+    sm.QU(i) = (A(du, i) - A(cu, i) * sm.QU(i + 1)) / den;
+  }
+  sm.QU(fi) = (A(du, fi) - A(cu, fi) * sm.QU(fi + 1)) / (A(bu, fi) - A(cu, fi) * sm.RU(fi + 1));
+  R v = sm.QU(fi);
+  value[(long long)fi * ncol + col] = v;
+  for (int i = fi + 1; i <= lt; ++i) {
+    v = sm.QU(i) - sm.RU(i) * v;
+    value[(long long)i * ncol + col] = v;
+  }
+}
+
+// NOSPLIT finaliser (advection_3d.F90:416-423): f = (ho*f - dt*adv)/hi on mask_finalise columns,
+// levels 1..kmax.
+template <class R>
+__global__ void k_finalise(Dev d, R dt, R* f, const R* __restrict__ ho, const R* __restrict__ adv,
+                           const R* __restrict__ hi, const uint8_t* __restrict__ mfin) {
+  const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+  const int jj = blockIdx.y * blockDim.y + threadIdx.y;
+  if (ii >= d.ni() || jj >= d.nj()) return;
+  const long long c = (long long)ii + (long long)jj * d.sj;
+  if (!mfin[c]) return;
+  const long long p = c + (long long)(blockIdx.z + 1) * d.sk;
+  f[p] = (ho[p] * f[p] - dt * adv[p]) / hi[p];
+}
+
+// ---------------------------------------------------------------------------------------------
+// Deterministic compensated reduction of f*h/ard1 (Neumaier pairs combined in a fixed order).
+struct Neu {
+  double s, c;
+};
+__device__ __forceinline__ void neu_add(Neu& a, double x) {
+  const double t = a.s + x;
+  if (fabs(a.s) >= fabs(x)) a.c += (a.s - t) + x; else a.c += (x - t) + a.s;
+  a.s = t;
+}
+__device__ __forceinline__ void neu_merge(Neu& a, const Neu& b) {
+  neu_add(a, b.s);
+  a.c += b.c;
+}
+
+
+template <class R>
+__global__ void __launch_bounds__(RED_THREADS) k_content_partial(Dev d, const R* __restrict__ f,
+                                                                 const R* __restrict__ h,
+                                                                 const int32_t* __restrict__ az,
+                                                                 double* partial) {
+  __shared__ Neu sh[RED_THREADS];
+  const int nx = d.imax - d.imin + 1, ny = d.jmax - d.jmin + 1;
+  const long long ncell = (long long)nx * ny * d.kmax;
+  const double area = 1.0 / d.ard1;
+  Neu acc{0.0, 0.0};
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < ncell;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % nx);
+    const long long r = q / nx;
+    const int j = (int)(r % ny);
+    const int k = 1 + (int)(r / ny);
+    const long long c = d.ix(d.imin + i, d.jmin + j);
+    if (az[c] < 1) continue;
+    const long long p = c + (long long)k * d.sk;
+    neu_add(acc, (double)f[p] * (double)h[p] * area);
+  }
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = RED_THREADS / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) neu_merge(sh[threadIdx.x], sh[threadIdx.x + s]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    partial[2 * blockIdx.x] = sh[0].s;
+    partial[2 * blockIdx.x + 1] = sh[0].c;
+  }
+}
+
+static __global__ void __launch_bounds__(RED_THREADS) k_content_final(const double* partial, int nb,
+                                                                        double* out) {
+  __shared__ Neu sh[RED_THREADS];
+  Neu acc{0.0, 0.0};
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+    neu_add(acc, partial[2 * b]);
+    acc.c += partial[2 * b + 1];
+  }
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = RED_THREADS / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) neu_merge(sh[threadIdx.x], sh[threadIdx.x + s]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[0] = sh[0].s + sh[0].c;
+    out[1] = sh[0].c;
+  }
+}
+
+template <class R>
+__global__ void k_check_range(Dev d, const R* __restrict__ f, const int32_t* __restrict__ az, R lo, R hi,
+                              unsigned long long* count) {
+  const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+  const int jj = blockIdx.y * blockDim.y + threadIdx.y;
+  const int nx = d.imax - d.imin + 1, ny = d.jmax - d.jmin + 1;
+  if (ii >= nx || jj >= ny) return;
+  const long long c = d.ix(d.imin + ii, d.jmin + jj);
+  if (az[c] <= 0) return;
+  unsigned long long n = 0;
+  for (int k = 0; k <= d.kmax; ++k) {
+    const R v = f[c + (long long)k * d.sk];
+    if (v < lo || v > hi) ++n;
+  }
+  if (n) atomicAdd(count, n);
+}
+
+}  // namespace gb

@@ -1,0 +1,116 @@
+// kernels_inst.cuh -- launcher definitions; included once per precision by kernels_f64.cu and
+// kernels_f32.cu with GB_REAL defined to the arithmetic type.
+#pragma once
+#include "kernels.cuh"
+
+namespace gb {
+
+template <class R, int DIR>
+int run_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int scheme, R AH, const R* f,
+                const R* fi_src, R* fi_dst, const R* Di_src, R* Di_dst, R* adv, const R* U, const R* DU,
+                const uint8_t* mflux, const uint8_t* mupd) {
+  if (nk <= 0) return 0;
+  dim3 blk(64, 4, 1);
+  dim3 grd((d.ni() + blk.x - 1) / blk.x, (d.nj() + blk.y - 1) / blk.y, nk);
+  k_sweep_h<R, DIR><<<grd, blk, 0, s>>>(d, dt, splitfac, scheme, AH, f, fi_src, fi_dst, Di_src, Di_dst, adv,
+                                        U, DU, mflux, mupd);
+  return (int)cudaGetLastError();
+}
+
+template <class R>
+int run_sweep_w(const Dev& d, cudaStream_t s, R dt, R splitfac, int scheme, int kshift, int itersmax,
+                const R* f, const R* fi_src, R* fi_dst, R* hi, R* adv, const R* ww, const int32_t* az,
+                unsigned long long* warn) {
+  if (itersmax > 1) {
+    dim3 blk(32, 2, 1);
+    dim3 grd((d.ni() - 1 + blk.x - 1) / blk.x, (d.nj() - 1 + blk.y - 1) / blk.y, 1);
+    k_sweep_w_iter<R><<<grd, blk, 0, s>>>(d, dt, splitfac, scheme, kshift, itersmax, f, fi_src, fi_dst, hi,
+                                          adv, ww, az, warn);
+  } else {
+    dim3 blk(64, 2, 1);
+    dim3 grd((d.ni() - 1 + blk.x - 1) / blk.x, (d.nj() - 1 + blk.y - 1) / blk.y, 1);
+    k_sweep_w<R><<<grd, blk, 0, s>>>(d, dt, splitfac, scheme, kshift, f, fi_src, fi_dst, hi, adv, ww, az);
+  }
+  return (int)cudaGetLastError();
+}
+
+template <class R>
+int run_finalise(const Dev& d, cudaStream_t s, R dt, R* f, const R* ho, const R* adv, const R* hi,
+                 const uint8_t* mfin) {
+  dim3 blk(64, 4, 1);
+  dim3 grd((d.ni() + blk.x - 1) / blk.x, (d.nj() + blk.y - 1) / blk.y, d.kmax);
+  k_finalise<R><<<grd, blk, 0, s>>>(d, dt, f, ho, adv, hi, mfin);
+  return (int)cudaGetLastError();
+}
+
+template <class R>
+int run_vdiff(const Dev& d, cudaStream_t s, R dt, R cnpar, R avmol, R* S, const R* hn, const R* nuh,
+              const int32_t* az, const R* src) {
+  if (d.kmax <= 1) return 0;
+  const int nt = 64;
+  const size_t smem = 2 * (size_t)(d.kmax + 1) * nt * sizeof(R);
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(k_vdiff<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_set = true;
+  }
+  const int nx = d.imax - d.imin + 1, ny = d.jmax - d.jmin + 1;
+  dim3 grd((nx + nt - 1) / nt, ny, 1);
+  k_vdiff<R><<<grd, nt, smem, s>>>(d, dt, cnpar, avmol, S, hn, nuh, az, src);
+  return (int)cudaGetLastError();
+}
+
+template <class R>
+int run_tridiag(cudaStream_t s, int ncol, int kmax, int fi, int lt, const R* au, const R* bu, const R* cu,
+                const R* du, R* value) {
+  const int nt = 64;
+  const size_t smem = 2 * (size_t)(kmax + 1) * nt * sizeof(R);
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(k_tridiag<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_set = true;
+  }
+  k_tridiag<R><<<(ncol + nt - 1) / nt, nt, smem, s>>>(ncol, kmax, fi, lt, au, bu, cu, du, value);
+  return (int)cudaGetLastError();
+}
+
+template <class R>
+int run_content(const Dev& d, cudaStream_t s, const R* f, const R* h, const int32_t* az, double* partial,
+                double* out) {
+  k_content_partial<R><<<RED_BLOCKS, RED_THREADS, 0, s>>>(d, f, h, az, partial);
+  k_content_final<<<1, RED_THREADS, 0, s>>>(partial, RED_BLOCKS, out);
+  return (int)cudaGetLastError();
+}
+
+template <class R>
+int run_check_range(const Dev& d, cudaStream_t s, const R* f, const int32_t* az, R lo, R hi,
+                    unsigned long long* count) {
+  dim3 blk(64, 4, 1);
+  const int nx = d.imax - d.imin + 1, ny = d.jmax - d.jmin + 1;
+  dim3 grd((nx + blk.x - 1) / blk.x, (ny + blk.y - 1) / blk.y, 1);
+  k_check_range<R><<<grd, blk, 0, s>>>(d, f, az, lo, hi, count);
+  return (int)cudaGetLastError();
+}
+
+// explicit instantiations for GB_REAL
+template int run_sweep_h<GB_REAL, 0>(const Dev&, cudaStream_t, int, GB_REAL, GB_REAL, int, GB_REAL,
+                                     const GB_REAL*, const GB_REAL*, GB_REAL*, const GB_REAL*, GB_REAL*,
+                                     GB_REAL*, const GB_REAL*, const GB_REAL*, const uint8_t*, const uint8_t*);
+template int run_sweep_h<GB_REAL, 1>(const Dev&, cudaStream_t, int, GB_REAL, GB_REAL, int, GB_REAL,
+                                     const GB_REAL*, const GB_REAL*, GB_REAL*, const GB_REAL*, GB_REAL*,
+                                     GB_REAL*, const GB_REAL*, const GB_REAL*, const uint8_t*, const uint8_t*);
+template int run_sweep_w<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL, int, int, int, const GB_REAL*,
+                                  const GB_REAL*, GB_REAL*, GB_REAL*, GB_REAL*, const GB_REAL*, const int32_t*,
+                                  unsigned long long*);
+template int run_finalise<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL*, const GB_REAL*, const GB_REAL*,
+                                   const GB_REAL*, const uint8_t*);
+template int run_vdiff<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL, GB_REAL, GB_REAL*, const GB_REAL*,
+                                const GB_REAL*, const int32_t*, const GB_REAL*);
+template int run_tridiag<GB_REAL>(cudaStream_t, int, int, int, int, const GB_REAL*, const GB_REAL*,
+                                  const GB_REAL*, const GB_REAL*, GB_REAL*);
+template int run_content<GB_REAL>(const Dev&, cudaStream_t, const GB_REAL*, const GB_REAL*, const int32_t*,
+                                  double*, double*);
+template int run_check_range<GB_REAL>(const Dev&, cudaStream_t, const GB_REAL*, const int32_t*, GB_REAL,
+                                      GB_REAL, unsigned long long*);
+
+}  // namespace gb

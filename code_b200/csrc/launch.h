@@ -1,0 +1,50 @@
+// launch.h -- host-side launchers of the templated kernels (instantiated per precision in
+// kernels_f64.cu / kernels_f32.cu). Each returns a cudaError_t as int (0 = success).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace gb {
+
+struct Dev;
+
+constexpr int RED_BLOCKS = 1184;  // 8 x 148 SMs
+constexpr int RED_THREADS = 256;
+
+// Horizontal sweep over nk levels starting at the given level pointers. DIR 0 = u, 1 = v.
+template <class R, int DIR>
+int run_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int scheme, R AH, const R* f,
+                const R* fi_src, R* fi_dst, const R* Di_src, R* Di_dst, R* adv, const R* U, const R* DU,
+                const uint8_t* mflux, const uint8_t* mupd);
+
+// Vertical sweep on full 3D fields (level-0 pointers).
+template <class R>
+int run_sweep_w(const Dev& d, cudaStream_t s, R dt, R splitfac, int scheme, int kshift, int itersmax,
+                const R* f, const R* fi_src, R* fi_dst, R* hi, R* adv, const R* ww, const int32_t* az,
+                unsigned long long* warn);
+
+template <class R>
+int run_finalise(const Dev& d, cudaStream_t s, R dt, R* f, const R* ho, const R* adv, const R* hi,
+                 const uint8_t* mfin);
+
+template <class R>
+int run_vdiff(const Dev& d, cudaStream_t s, R dt, R cnpar, R avmol, R* S, const R* hn, const R* nuh,
+              const int32_t* az, const R* src);
+
+template <class R>
+int run_tridiag(cudaStream_t s, int ncol, int kmax, int fi, int lt, const R* au, const R* bu, const R* cu,
+                const R* du, R* value);
+
+// Two-stage deterministic content reduction; partial must hold 2*RED_BLOCKS doubles.
+template <class R>
+int run_content(const Dev& d, cudaStream_t s, const R* f, const R* h, const int32_t* az, double* partial,
+                double* out);
+
+template <class R>
+int run_check_range(const Dev& d, cudaStream_t s, const R* f, const int32_t* az, R lo, R hi,
+                    unsigned long long* count);
+
+int run_build_masks(const Dev& d, cudaStream_t s, const int32_t* az, const int32_t* au, const int32_t* av,
+                    const int32_t* ax, uint8_t* planes);
+
+}  // namespace gb

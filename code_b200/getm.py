@@ -1,0 +1,263 @@
+"""Host-side mirror of GETM's hot-path routines over the CUDA library's C ABI.
+
+Each method keeps the reference subroutine's name, argument order and argument meaning
+(``do_advection_3d(dt,f,uu,vv,ww,hu,hv,ho,hn,split,hscheme,vscheme,AH,tag,hires,advres)``,
+advection_3d.F90:120-122, and so on) and operates on CUDA tensors laid out like the reference's
+arrays (see :mod:`code_b200.grid`). torch supplies device memory and the stream only; all
+arithmetic runs in the library's kernels. There is no CPU fallback: without the compiled library
+or a CUDA device every call raises.
+
+Errors: where the reference stops (``stop 'do_advection_3d: tag is invalid'``) the library
+returns a status code and this layer raises :class:`GetmError` with the library's message.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+from .grid import Grid
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libgetm_b200.so")
+
+# scheme / split / tag ids (advection.F90:55-62, halo_zones.F90:25-27, advection_3d.F90:42)
+NOSPLIT, FULLSPLIT, HALFSPLIT, HVSPLIT = 0, 1, 2, 3
+NOADV, UPSTREAM, UPSTREAM_2DH, P2, SUPERBEE, MUSCL, P2_PDM, J7, FCT, P2_2DH = range(10)
+H_TAG, D_TAG, U_TAG, V_TAG, W_TAG = 10, 20, 31, 32, 33
+
+ERRORS = {-1: "GETM_ERR_ARG", -2: "GETM_ERR_CUDA", -3: "GETM_ERR_UNSUPPORTED", -4: "GETM_ERR_CHECK",
+          -5: "GETM_ERR_TIMEOUT", -6: "GETM_ERR_NOMEM", -7: "GETM_ERR_STATE"}
+
+
+class GetmError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+_lock = threading.Lock()
+P = C.c_void_p
+I = C.c_int
+D = C.c_double
+F = C.c_float
+
+
+class AdvGrid(C.Structure):
+    _fields_ = [("mask_uflux", P), ("mask_vflux", P), ("mask_uupdate", P), ("mask_vupdate", P),
+                ("mask_finalise", P), ("az", P)]
+
+
+# name -> argtypes (restype int unless listed in _RESTYPES)
+_PROTOS = {
+    "getm_ctx_create": [P, P, P],
+    "getm_ctx_destroy": [P],
+    "getm_ctx_set_stream": [P, P],
+    "getm_ctx_take_warnings": [P, P],
+    "getm_ctx_last_error": [P],
+    "getm_version": [],
+    "getm_init_advection": [P, P, P, P, P],
+    "getm_adv_grid_for_tag": [P, I, P],
+    "getm_adv_split_u": [P, I, D, P, P, P, P, P, P, D, I, D, P, P],
+    "getm_adv_split_v": [P, I, D, P, P, P, P, P, P, D, I, D, P, P],
+    "getm_adv_split_w": [P, D, P, P, P, P, P, D, I, I, P, I],
+    "getm_do_advection_3d": [P, D, P, P, P, P, P, P, P, P, I, I, I, D, I, P, P, I],
+    "getm_do_advection_3d_f32": [P, F, P, P, P, P, P, P, P, P, I, I, I, F, I, P, P, I],
+    "getm_tridiagonal_columns": [P, I, I, I, I, P, P, P, P, P],
+    "getm_tracer_vdiff": [P, D, D, D, P, P, P, P, P],
+    "getm_tracer_vdiff_f32": [P, F, F, F, P, P, P, P, P],
+    "getm_tracer_step": [P, D, P, P, P, P, P, P, P, P, P, I, I, I, D, D, D, I],
+    "getm_tracer_step_f32": [P, F, P, P, P, P, P, P, P, P, P, I, I, I, F, F, F, I],
+    "getm_tracer_content": [P, P, P, P, P],
+    "getm_tracer_content_f32": [P, P, P, P, P],
+    "getm_check_3d_fields": [P, P, P, D, D, P],
+    "getm_timers_enable": [P, I],
+    "getm_timers_reset": [P],
+    "getm_timers_read": [P, I, P, P],
+    "getm_timer_name": [I],
+}
+_RESTYPES = {"getm_ctx_last_error": C.c_char_p, "getm_version": C.c_char_p, "getm_timer_name": C.c_char_p}
+NTIMERS = 16
+
+
+def lib():
+    """Load the compiled library (raises if it has not been built)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(f"CUDA library not built: {LIB_PATH} is missing "
+                                   "(run __graft_entry__.build() or python code_b200/build.py)")
+            L = C.CDLL(LIB_PATH)
+            for name, args in _PROTOS.items():
+                fn = getattr(L, name)
+                fn.argtypes = args
+                fn.restype = _RESTYPES.get(name, C.c_int)
+            _lib = L
+    return _lib
+
+
+def exported_symbols():
+    return list(_PROTOS)
+
+
+def _ptr(t):
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise ValueError("expected a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError("expected a contiguous tensor")
+    return t.data_ptr()
+
+
+def _same_dtype(ref, *ts):
+    for t in ts:
+        if t is not None and t.dtype != ref.dtype:
+            raise TypeError(f"dtype mismatch: {t.dtype} vs {ref.dtype}")
+
+
+class Context:
+    """One device context (getm_ctx): grid, stream, advection masks and scratch."""
+
+    def __init__(self, grid: Grid, stream=None):
+        import torch
+
+        if not torch.cuda.is_available():
+            raise RuntimeError("a CUDA device is required (no CPU fallback)")
+        self.grid = grid
+        self.L = lib()
+        self._dom = grid.domain()
+        if stream is None:
+            stream = torch.cuda.current_stream()
+        self.stream = stream
+        h = P()
+        self._check(self.L.getm_ctx_create(C.byref(self._dom), P(stream.cuda_stream), C.byref(h)), None)
+        self.h = h
+
+    # ------------------------------------------------------------------------------------------
+    def _check(self, rc: int, h=0):
+        if rc != 0:
+            hh = self.h if h == 0 else h
+            msg = self.L.getm_ctx_last_error(hh).decode() if hh else "context creation failed"
+            raise GetmError(rc, msg)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.getm_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream):
+        self.stream = stream
+        self._check(self.L.getm_ctx_set_stream(self.h, P(stream.cuda_stream)))
+
+    def take_warnings(self) -> int:
+        n = C.c_int64()
+        self._check(self.L.getm_ctx_take_warnings(self.h, C.byref(n)))
+        return n.value
+
+    # ------------------------------------------------------------------------------------------
+    def timers(self, enable: bool | None = None, reset: bool = False) -> dict:
+        """Per-stage device timers (tic/toc of getm_timers): {name: (total_ms, launches)}."""
+        if enable is not None:
+            self._check(self.L.getm_timers_enable(self.h, 1 if enable else 0))
+        out = {}
+        for t in range(NTIMERS):
+            ms, n = C.c_double(), C.c_int64()
+            self._check(self.L.getm_timers_read(self.h, t, C.byref(ms), C.byref(n)))
+            if n.value:
+                out[self.L.getm_timer_name(t).decode()] = (ms.value, n.value)
+        if reset:
+            self._check(self.L.getm_timers_reset(self.h))
+        return out
+
+    def init_advection(self, az, au, av, ax):
+        """init_advection (advection.F90:204-354) from int32 device masks."""
+        self._masks = (az, au, av, ax)  # keep alive
+        self._check(self.L.getm_init_advection(self.h, _ptr(az), _ptr(au), _ptr(av), _ptr(ax)))
+
+    def adv_grid(self, tag: int) -> AdvGrid:
+        g = AdvGrid()
+        self._check(self.L.getm_adv_grid_for_tag(self.h, tag, C.byref(g)))
+        return g
+
+    def adv_split_u(self, dt, f, fi, Di, adv, U, DU, splitfac, scheme, AH, mask_flux, mask_update, nk=None):
+        _same_dtype(f, fi, Di, adv, U, DU)
+        nk = nk if nk is not None else (f.shape[0] if f.dim() == 3 else 1)
+        self._check(self.L.getm_adv_split_u(self.h, nk, dt, _ptr(f), _ptr(fi), _ptr(Di), _ptr(adv), _ptr(U), _ptr(DU),
+                                            splitfac, scheme, AH, _mask(mask_flux), _mask(mask_update)))
+
+    def adv_split_v(self, dt, f, fi, Di, adv, V, DV, splitfac, scheme, AH, mask_flux, mask_update, nk=None):
+        _same_dtype(f, fi, Di, adv, V, DV)
+        nk = nk if nk is not None else (f.shape[0] if f.dim() == 3 else 1)
+        self._check(self.L.getm_adv_split_v(self.h, nk, dt, _ptr(f), _ptr(fi), _ptr(Di), _ptr(adv), _ptr(V), _ptr(DV),
+                                            splitfac, scheme, AH, _mask(mask_flux), _mask(mask_update)))
+
+    def adv_split_w(self, dt, f, fi, hi, adv, ww, splitfac, scheme, tag, az, itersmax=1):
+        _same_dtype(f, fi, hi, adv, ww)
+        self._check(self.L.getm_adv_split_w(self.h, dt, _ptr(f), _ptr(fi), _ptr(hi), _ptr(adv), _ptr(ww), splitfac,
+                                            scheme, tag, _ptr(az), itersmax))
+
+    def do_advection_3d(self, dt, f, uu, vv, ww, hu, hv, ho, hn, split, hscheme, vscheme, AH, tag,
+                        hires=None, advres=None, adv_ver_iterations=1):
+        """do_advection_3d (advection_3d.F90:120-598); f is advanced in place."""
+        _same_dtype(f, uu, vv, ww, hu, hv, ho, hn, hires, advres)
+        fn = self.L.getm_do_advection_3d if _is64(f) else self.L.getm_do_advection_3d_f32
+        self._check(fn(self.h, dt, _ptr(f), _ptr(uu), _ptr(vv), _ptr(ww), _ptr(hu), _ptr(hv), _ptr(ho), _ptr(hn),
+                       split, hscheme, vscheme, AH, tag, _ptr(hires), _ptr(advres), adv_ver_iterations))
+
+    def tridiagonal(self, kmax, fi, lt, au, bu, cu, du, value):
+        """getm_tridiagonal (tridiagonal.F90:8-51) on the columns of [k][col] tensors."""
+        ncol = au.shape[1]
+        self._check(self.L.getm_tridiagonal_columns(self.h, ncol, kmax, fi, lt, _ptr(au), _ptr(bu), _ptr(cu),
+                                                    _ptr(du), _ptr(value)))
+
+    def tracer_vdiff(self, dt, cnpar, avmol, S, hn, nuh, az, src=None):
+        """Vertical-diffusion solve of do_salinity / do_temperature (salinity.F90:348-389)."""
+        _same_dtype(S, hn, nuh, src)
+        fn = self.L.getm_tracer_vdiff if _is64(S) else self.L.getm_tracer_vdiff_f32
+        self._check(fn(self.h, dt, cnpar, avmol, _ptr(S), _ptr(hn), _ptr(nuh), _ptr(az), _ptr(src)))
+
+    def tracer_step(self, dt, f, uu, vv, ww, hu, hv, ho, hn, nuh, split, hscheme, vscheme, AH, cnpar, avmol,
+                    adv_ver_iterations=1):
+        """Advection + vertical diffusion of one tracer (the body of do_salinity)."""
+        _same_dtype(f, uu, vv, ww, hu, hv, ho, hn, nuh)
+        fn = self.L.getm_tracer_step if _is64(f) else self.L.getm_tracer_step_f32
+        self._check(fn(self.h, dt, _ptr(f), _ptr(uu), _ptr(vv), _ptr(ww), _ptr(hu), _ptr(hv), _ptr(ho), _ptr(hn),
+                       _ptr(nuh), split, hscheme, vscheme, AH, cnpar, avmol, adv_ver_iterations))
+
+    def tracer_content(self, f, h, az) -> float:
+        out = C.c_double()
+        fn = self.L.getm_tracer_content if _is64(f) else self.L.getm_tracer_content_f32
+        self._check(fn(self.h, _ptr(f), _ptr(h), _ptr(az), C.byref(out)))
+        return out.value
+
+    def check_3d_fields(self, f, az, minval, maxval) -> int:
+        st = C.c_int64()
+        self._check(self.L.getm_check_3d_fields(self.h, _ptr(f), _ptr(az), minval, maxval, C.byref(st)))
+        return st.value
+
+
+def _is64(t) -> bool:
+    import torch
+
+    if t.dtype == torch.float64:
+        return True
+    if t.dtype == torch.float32:
+        return False
+    raise TypeError(f"unsupported dtype {t.dtype}")
+
+
+def _mask(m):
+    if m is None:
+        return None
+    if isinstance(m, int):
+        return m
+    return _ptr(m)

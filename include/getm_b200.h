@@ -1,0 +1,195 @@
+/* getm_b200.h -- C ABI of the B200 implementation of GETM's per-timestep 3D hot path.
+ *
+ * Every entry point is a drop-in for one GETM 2.5 subroutine (getm-model/code, cited per
+ * function as path:line) or for a fused group of them. Arrays are DEVICE pointers in the
+ * reference's own layout: a 3D field covers the haloed index space
+ * (imin-2:imax+2, jmin-2:jmax+2, 0:kmax), i fastest, element (i,j,k) at
+ *     base + (i-(imin-2)) + (j-(jmin-2))*sj + k*sk
+ * (Fortran column-major when sj = imax-imin+5 and sk = sj*(jmax-jmin+5); padded pitches are
+ * allowed). 2D fields use the same (i,j) addressing with no k term. Masks az/au/av/ax are int32
+ * like the reference's integer masks.
+ *
+ * Calling convention: one host thread per context; every call is stream-ordered on the context's
+ * stream and returns a status (0 = OK, < 0 = error, see GETM_ERR_*). No call exits the process:
+ * where the reference calls stop / getm_error, the entry point returns an error code and the
+ * Fortran-side wrapper turns it into getm_error (INTEGRATION.md shows that wrapper).
+ *
+ * Suffixes: no suffix = FP64 (the reference's REALTYPE, cppdefs.h:130-131),
+ *           _f32      = FP32 arithmetic for the same routine (the mixed-precision variant).
+ */
+#ifndef GETM_B200_H
+#define GETM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------------------------- */
+#define GETM_OK 0
+#define GETM_ERR_ARG (-1)         /* invalid argument (reference: stop '... is invalid') */
+#define GETM_ERR_CUDA (-2)        /* a CUDA runtime call or kernel launch failed */
+#define GETM_ERR_UNSUPPORTED (-3) /* valid in the reference but not provided here */
+#define GETM_ERR_CHECK (-4)       /* a device-side check failed (range / NaN / iteration cap) */
+#define GETM_ERR_TIMEOUT (-5)     /* a bounded device wait ran out */
+#define GETM_ERR_NOMEM (-6)       /* device allocation failed */
+#define GETM_ERR_STATE (-7)       /* call order violated (e.g. masks not initialised) */
+
+/* ---- scheme / split / tag identifiers (values as in the reference) --------------------- */
+/* advection.F90:55,60-62 ; advection_3d.F90:42 */
+#define GETM_NOSPLIT 0
+#define GETM_FULLSPLIT 1
+#define GETM_HALFSPLIT 2
+#define GETM_HVSPLIT 3
+#define GETM_NOADV 0
+#define GETM_UPSTREAM 1
+#define GETM_UPSTREAM_2DH 2
+#define GETM_P2 3
+#define GETM_SUPERBEE 4
+#define GETM_MUSCL 5
+#define GETM_P2_PDM 6
+#define GETM_J7 7
+#define GETM_FCT 8
+#define GETM_P2_2DH 9
+/* halo_zones.F90:25-27 ; advection_3d.F90:42 */
+#define GETM_H_TAG 10
+#define GETM_D_TAG 20
+#define GETM_U_TAG 31
+#define GETM_V_TAG 32
+#define GETM_W_TAG 33
+
+/* ---- domain and context ---------------------------------------------------------------- */
+/* The index space and Cartesian metrics of domain.F90 (imin..kmax, dx, dy, ard1=1/(dx*dy),
+ * domain.F90:596). */
+typedef struct getm_domain {
+  int32_t imin, imax, jmin, jmax, kmax;
+  int64_t sj, sk; /* element strides of j and k (the i stride is 1) */
+  double dx, dy, ard1;
+} getm_domain;
+
+typedef struct getm_ctx getm_ctx;
+
+/* Device pointers of one t_adv_grid (advection.F90:43-51): byte masks, 1 = .true. */
+typedef struct getm_adv_grid {
+  const uint8_t *mask_uflux, *mask_vflux, *mask_uupdate, *mask_vupdate, *mask_finalise;
+  const int32_t *az;
+} getm_adv_grid;
+
+/* Creates a context on the current CUDA device; `stream` is a cudaStream_t (NULL = legacy
+ * default stream). Replaces the allocation part of init_3d / init_advection (m3d.F90:88,
+ * advection.F90:204). */
+int getm_ctx_create(const getm_domain *dom, void *stream, getm_ctx **out);
+int getm_ctx_destroy(getm_ctx *ctx);
+int getm_ctx_set_stream(getm_ctx *ctx, void *stream);
+/* Accumulated device-side warnings since the last call, e.g. the number of water columns whose
+ * vertical-advection iteration estimate exceeded adv_ver_iterations (adv_split_w.F90:223-228
+ * prints these). Synchronises the context's stream. */
+int getm_ctx_take_warnings(getm_ctx *ctx, int64_t *n_warnings);
+/* Per-stage device timers: the counterpart of the reference's tic/toc subsystem timers
+ * (src/futils/getm_timers.F90:275-357). When enabled, every kernel launch of a stage is
+ * bracketed by CUDA events on the context's stream; read accumulates (synchronising) the elapsed
+ * device time and the launch count of a slot. */
+#define GETM_TIM_ADV_U 0
+#define GETM_TIM_ADV_V 1
+#define GETM_TIM_ADV_W 2
+#define GETM_TIM_ADV_FINALISE 3
+#define GETM_TIM_VDIFF 4
+#define GETM_TIM_COPY 5
+#define GETM_TIM_TRACER_UV 6
+#define GETM_TIM_TRACER_WVU 7
+#define GETM_NTIMERS 16
+int getm_timers_enable(getm_ctx *ctx, int on);
+int getm_timers_reset(getm_ctx *ctx);
+int getm_timers_read(getm_ctx *ctx, int slot, double *total_ms, int64_t *launches);
+const char *getm_timer_name(int slot);
+/* Human-readable text of the last error on this context (never NULL). */
+const char *getm_ctx_last_error(const getm_ctx *ctx);
+const char *getm_version(void);
+
+/* init_advection (advection.F90:204-354): builds the flux/update/finalise masks of the H, U and
+ * V advection grids from the device masks az, au, av, ax (int32, E2DFIELD). Must precede any
+ * advection call. The context keeps its own copies. */
+int getm_init_advection(getm_ctx *ctx, const int32_t *az, const int32_t *au, const int32_t *av,
+                        const int32_t *ax);
+/* The mask set that do_advection_3d selects for `tag` (advection_3d.F90:262-277). */
+int getm_adv_grid_for_tag(const getm_ctx *ctx, int tag, getm_adv_grid *out);
+
+/* ---- split advection sweeps ------------------------------------------------------------ */
+/* adv_split_u (src/2d/adv_split_u.F90:8-295) applied to `nk` consecutive k-levels (pointers
+ * point at the first level, levels are sk apart; nk = 1 is the reference's 2D call). f and fi
+ * may alias (the reference's in-place call, advection_3d.F90:446). adv may be NULL when the
+ * caller does not need the advective increments. */
+int getm_adv_split_u(getm_ctx *ctx, int nk, double dt, const double *f, double *fi, double *Di,
+                     double *adv, const double *U, const double *DU, double splitfac, int scheme,
+                     double AH, const uint8_t *mask_flux, const uint8_t *mask_update);
+/* adv_split_v (src/2d/adv_split_v.F90:8-145), same conventions. */
+int getm_adv_split_v(getm_ctx *ctx, int nk, double dt, const double *f, double *fi, double *Di,
+                     double *adv, const double *V, const double *DV, double splitfac, int scheme,
+                     double AH, const uint8_t *mask_flux, const uint8_t *mask_update);
+/* adv_split_w (src/3d/adv_split_w.F90:7-360), full 3D fields; f and fi may alias. */
+int getm_adv_split_w(getm_ctx *ctx, double dt, const double *f, double *fi, double *hi, double *adv,
+                     const double *ww, double splitfac, int scheme, int tag, const int32_t *az,
+                     int itersmax);
+
+/* do_advection_3d (src/3d/advection_3d.F90:120-598): NOSPLIT / FULLSPLIT / HALFSPLIT / HVSPLIT
+ * with the split schemes UPSTREAM, P2, SUPERBEE, MUSCL, P2_PDM (the 2DH schemes are not
+ * provided: GETM_ERR_UNSUPPORTED). hires and advres are the optional outputs (NULL = absent).
+ * adv_ver_iterations is the module variable of advection_3d.F90:41. */
+int getm_do_advection_3d(getm_ctx *ctx, double dt, double *f, const double *uu, const double *vv,
+                         const double *ww, const double *hu, const double *hv, const double *ho,
+                         const double *hn, int split, int hscheme, int vscheme, double AH, int tag,
+                         double *hires, double *advres, int adv_ver_iterations);
+int getm_do_advection_3d_f32(getm_ctx *ctx, float dt, float *f, const float *uu, const float *vv,
+                             const float *ww, const float *hu, const float *hv, const float *ho,
+                             const float *hn, int split, int hscheme, int vscheme, float AH,
+                             int tag, float *hires, float *advres, int adv_ver_iterations);
+
+/* ---- vertical columns ------------------------------------------------------------------ */
+/* getm_tridiagonal (src/futils/tridiagonal.F90:8-51) on ncol independent systems of size
+ * 0:kmax. Coefficient arrays are laid out [k][col] (column fastest): au[k*ncol+c]. Levels fi..lt
+ * are solved; value is written on fi..lt only. */
+int getm_tridiagonal_columns(getm_ctx *ctx, int ncol, int kmax, int fi, int lt, const double *au,
+                             const double *bu, const double *cu, const double *du, double *value);
+
+/* Implicit vertical diffusion of a tracer on all wet interior columns (az==1, imin..imax x
+ * jmin..jmax): the matrix assembly and solve of do_salinity (src/3d/salinity.F90:348-389) when
+ * src == NULL, or of do_temperature (src/3d/temperature.F90:471-550) with src holding per layer
+ * the radiation / surface-flux increment dry_z*dt*(rad1d(k)[+shf*rho_0_cpi]-rad1d(k-1)). */
+int getm_tracer_vdiff(getm_ctx *ctx, double dt, double cnpar, double avmol, double *S,
+                      const double *hn, const double *nuh, const int32_t *az, const double *src);
+int getm_tracer_vdiff_f32(getm_ctx *ctx, float dt, float cnpar, float avmol, float *S,
+                          const float *hn, const float *nuh, const int32_t *az, const float *src);
+
+/* Fused tracer step = do_advection_3d(H_TAG) followed by the vertical-diffusion solve, i.e. the
+ * body of do_salinity (salinity.F90:301-389) for fwf_int = 0 and no numerical-mixing analysis. */
+int getm_tracer_step(getm_ctx *ctx, double dt, double *f, const double *uu, const double *vv,
+                     const double *ww, const double *hu, const double *hv, const double *ho,
+                     const double *hn, const double *nuh, int split, int hscheme, int vscheme,
+                     double AH, double cnpar, double avmol, int adv_ver_iterations);
+int getm_tracer_step_f32(getm_ctx *ctx, float dt, float *f, const float *uu, const float *vv,
+                         const float *ww, const float *hu, const float *hv, const float *ho,
+                         const float *hn, const float *nuh, int split, int hscheme, int vscheme,
+                         float AH, float cnpar, float avmol, int adv_ver_iterations);
+
+/* ---- diagnostics ----------------------------------------------------------------------- */
+/* Compensated (Neumaier) FP64 sum of f*h/ard1 over wet interior cells (az>=1, k=1..kmax):
+ * the global tracer content. Deterministic (fixed reduction order). Result written to the HOST
+ * double *out (the call synchronises the stream). No counterpart routine in the reference; it
+ * backs the tracer-conservation checks. */
+int getm_tracer_content(getm_ctx *ctx, const double *f, const double *h, const int32_t *az,
+                        double *out);
+int getm_tracer_content_f32(getm_ctx *ctx, const float *f, const float *h, const int32_t *az,
+                            double *out);
+/* check_3d_fields (src/futils/check_3d_fields.F90:8-59): counts cells of the interior with az>0
+ * and k>=kmin (kmin = 0, the sigma-coordinate value) whose value is below minval or above
+ * maxval (a NaN compares false both ways and is not counted, as in the reference). Count written
+ * to the HOST int64 *status. */
+int getm_check_3d_fields(getm_ctx *ctx, const double *f, const int32_t *az, double minval,
+                         double maxval, int64_t *status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GETM_B200_H */
