@@ -1,0 +1,235 @@
+"""Module state of the mode-split step (variables_2d / variables_3d / domain of the reference)
+as one table of fields, plus seeded synthetic baroclinic cases.
+
+The order of the name lists is part of the C ABI (getm_bc_state in include/getm_b200.h; the
+oracle keeps the same order): F2_NAMES are the 2D fields (always FP64), F3_NAMES the 3D fields
+(FP64, or FP32 in the mixed-precision variant), PD/PI the real and integer parameters.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .cases import derive_uvx
+from .grid import HALO, Grid
+
+F2_NAMES = ["z", "zo", "U", "V", "D", "DU", "DV", "UEx", "VEx", "fU", "fV", "ru", "rv", "ruu", "rvv", "Uint", "Vint",
+            "Uinto", "Vinto", "SlUx", "SlVx", "Slru", "Slrv", "zub", "zvb", "zub0", "zvb0", "fwf", "H", "HU", "HV",
+            "dry_z", "dry_u", "dry_v", "coru", "corv", "tausx", "tausy", "airp", "sseo", "ssen", "ssuo", "ssun",
+            "ssvo", "ssvn", "Dn", "Dun", "Dvn", "rru", "rrv", "taubx", "tauby", "taub", "taus"]
+F3_NAMES = ["uu", "vv", "ww", "ho", "hn", "huo", "hun", "hvo", "hvn", "uuEx", "vvEx", "idpdx", "idpdy", "T", "S",
+            "rho", "buoy", "num", "nuh"]
+PD_NAMES = ["dtm", "dt", "cnpar", "min_depth", "crit_depth", "g", "rho_0", "kappa", "avmmol", "avmolt", "avmols", "T0",
+            "S0", "dtr0", "dsr0", "ip_fac", "temp_AH", "salt_AH"]
+PI_NAMES = ["M", "MM", "runtype", "vel2d_adv_split", "vel2d_adv_hor", "vel3d_adv_split", "vel3d_adv_hor",
+            "vel3d_adv_ver", "temp_adv_split", "temp_adv_hor", "temp_adv_ver", "salt_adv_split", "salt_adv_hor",
+            "salt_adv_ver", "adv_ver_iterations", "ufirst2d", "ufirst3d", "calc_temp", "calc_salt"]
+
+F32 = lambda x: float(np.float32(x))  # noqa: E731  -- a Fortran default-kind real literal widened to double
+
+# parameters.F90:21-27 and eqstate.F90:27 literals are single precision in the reference
+DEFAULT_PD = dict(g=F32(9.81), rho_0=1025.0, kappa=F32(0.4), avmmol=F32(1.8e-6), avmolt=F32(1.4e-7),
+                  avmols=F32(1.1e-9), T0=10.0, S0=33.75, dtr0=F32(-0.17), dsr0=F32(0.78), ip_fac=1.0, temp_AH=-1.0,
+                  salt_AH=-1.0, cnpar=F32(0.9), min_depth=0.5, crit_depth=2.0)
+P2_PDM, HALFSPLIT = 6, 2
+
+
+class BcCase:
+    """A full model state (numpy arrays in the reference layout) with parameters."""
+
+    def __init__(self, grid: Grid, dtype3=np.float64):
+        self.grid = grid
+        self.dtype3 = np.dtype(dtype3)
+        self.f2 = {n: np.zeros(grid.shape2()) for n in F2_NAMES}
+        self.f3 = {n: np.zeros(grid.shape3(), dtype=self.dtype3) for n in F3_NAMES}
+        self.az = self.au = self.av = self.ax = None
+        self.pd = {n: 0.0 for n in PD_NAMES}
+        self.pi = {n: 0 for n in PI_NAMES}
+
+    def copy(self, dtype3=None):
+        c = BcCase(self.grid, dtype3 or self.dtype3)
+        c.f2 = {k: v.copy() for k, v in self.f2.items()}
+        c.f3 = {k: v.astype(c.dtype3) for k, v in self.f3.items()}
+        c.az, c.au, c.av, c.ax = self.az.copy(), self.au.copy(), self.av.copy(), self.ax.copy()
+        c.pd, c.pi = dict(self.pd), dict(self.pi)
+        return c
+
+    def masks(self):
+        return self.az, self.au, self.av, self.ax
+
+
+def _eqstate(c: BcCase):
+    p = c.pd
+    T, S = c.f3["T"].astype(np.float64), c.f3["S"].astype(np.float64)
+    rho = p["rho_0"] + p["dtr0"] * (T - p["T0"]) + p["dsr0"] * (S - p["S0"])
+    rho[0] = 0.0
+    buoy = (-p["g"] / p["rho_0"]) * (rho - p["rho_0"])
+    buoy[0] = 0.0
+    c.f3["rho"][...] = rho
+    c.f3["buoy"][...] = buoy
+
+
+def baroclinic_case(nx=32, ny=24, kmax=8, recipe="shelf", dx=1000.0, M=20, dt3=60.0, seed=2, dtype3=np.float64,
+                    land=0.0, hmin=5.0, hmax=150.0, nu_max=1e-2, latitude=54.0) -> BcCase:
+    """Seeded initial state of the mode-split step, closed basin.
+
+    recipe 'shelf': H = 10 + 190*0.5*(1+tanh((x-x0)/L)), L = 20 cells, x0 = nx/2.
+    recipe 'flat':  H = 20 m.
+    recipe 'islands': H = hmin + (hmax-hmin)*(field-p)/(max-p) on wet cells of a Gaussian-smoothed
+      noise field (sigma = 40 cells, scaled with the grid), land where field < its `land` quantile.
+    Stratification: T from 20 C (surface) to 8 C (bottom) linear in depth plus N(0, 0.1) noise,
+    S from 30 to 35 psu; linear EOS. Viscosity / diffusivity: static parabolic 4*nu_max*s*(1-s)
+    (+1e-6) over the sigma levels. Coriolis on an f-plane at `latitude` (domain.F90:364-369 with the
+    reference's single-precision omega = 2*pi/86164).
+    """
+    g = Grid(nx, ny, kmax, dx, dx)
+    rng = np.random.default_rng(seed)
+    c = BcCase(g, dtype3)
+    i = np.arange(g.imin - HALO, g.imax + HALO + 1)
+    xT = (i - g.imin + 0.5) * dx
+    az = np.zeros(g.shape2(), np.int32)
+    if recipe == "shelf":
+        L = 20 * dx
+        x0 = nx / 2 * dx
+        H = np.broadcast_to(10.0 + 190.0 * 0.5 * (1.0 + np.tanh((xT - x0) / L)), g.shape2()).copy()
+        az[g.interior()] = 1
+    elif recipe == "flat":
+        H = np.full(g.shape2(), 20.0)
+        az[g.interior()] = 1
+    elif recipe == "islands":
+        field = rng.normal(size=(ny, nx))
+        sig = max(1.0, 40.0 * nx / 2048.0)
+        k1 = np.fft.fftfreq(nx)[None, :]
+        k2 = np.fft.fftfreq(ny)[:, None]
+        field = np.real(np.fft.ifft2(np.fft.fft2(field) * np.exp(-2 * (math.pi * sig) ** 2 * (k1 ** 2 + k2 ** 2))))
+        field = (field - field.mean()) / field.std()
+        p = np.quantile(field, land) if land > 0 else field.min() - 1e-9
+        wet = field >= p
+        Hi = np.where(wet, hmin + (hmax - hmin) * (field - p) / (field.max() - p), 0.0)
+        H = np.zeros(g.shape2())
+        H[g.interior()] = Hi
+        az[g.interior()] = wet.astype(np.int32)
+        # halo depths mirror the first interior line (update_2d_halo with mirror, halo_zones.F90:110-118)
+        H[:, 1] = H[:, 2]; H[:, -2] = H[:, -3]; H[1, :] = H[2, :]; H[-2, :] = H[-3, :]  # noqa: E702
+    else:
+        raise ValueError(recipe)
+    if recipe != "islands":
+        H[:, 1] = H[:, 2]; H[:, -2] = H[:, -3]; H[1, :] = H[2, :]; H[-2, :] = H[-3, :]  # noqa: E702
+        H[:, 0] = H[:, 1]; H[:, -1] = H[:, -2]; H[0, :] = H[1, :]; H[-1, :] = H[-2, :]  # noqa: E702
+    au, av, ax = derive_uvx(az)
+    c.az, c.au, c.av, c.ax = az, au, av, ax
+    f2 = c.f2
+    f2["H"][...] = H
+    # uv_depths vel_depth_method = 0 (uv_depths.F90: HU = 0.5*(H(i)+H(i+1)))
+    f2["HU"][:, :-1] = 0.5 * (H[:, :-1] + H[:, 1:])
+    f2["HV"][:-1, :] = 0.5 * (H[:-1, :] + H[1:, :])
+    p = c.pd
+    p.update(DEFAULT_PD)
+    dtm = dt3 / M
+    p.update(dtm=dtm, dt=dt3)
+    c.pi.update(M=M, MM=1, runtype=4, vel2d_adv_split=HALFSPLIT, vel2d_adv_hor=P2_PDM, vel3d_adv_split=HALFSPLIT,
+                vel3d_adv_hor=P2_PDM, vel3d_adv_ver=P2_PDM, temp_adv_split=HALFSPLIT, temp_adv_hor=P2_PDM,
+                temp_adv_ver=P2_PDM, salt_adv_split=HALFSPLIT, salt_adv_hor=P2_PDM, salt_adv_ver=P2_PDM,
+                adv_ver_iterations=1, ufirst2d=0, ufirst3d=1, calc_temp=1, calc_salt=1)
+    pi_ = F32(3.141592654)
+    omega = 2.0 * pi_ / F32(86164.0)
+    cori = 2.0 * omega * math.sin(pi_ / 180.0 * latitude)
+    f2["coru"][...] = cori * (au > 0)
+    f2["corv"][...] = cori * (av > 0)
+    f2["zub0"][...] = 0.01
+    f2["zvb0"][...] = 0.01
+    f2["zub"][...] = 0.01
+    f2["zvb"][...] = 0.01
+    # elevation: small seeded perturbation on wet points; depths from depth_update
+    z = np.zeros(g.shape2())
+    wet = az >= 1
+    z[wet] = 0.05 * rng.normal(size=int(wet.sum()))
+    f2["z"][...] = z
+    f2["zo"][...] = z
+    zo = z
+    D = z + H
+    f2["D"][...] = D
+    xu = np.maximum(0.25 * (zo[:, :-1] + zo[:, 1:] + z[:, :-1] + z[:, 1:]), -f2["HU"][:, :-1] + p["min_depth"])
+    f2["DU"][:, :-1] = xu + f2["HU"][:, :-1]
+    xv = np.maximum(0.25 * (zo[:-1, :] + zo[1:, :] + z[:-1, :] + z[1:, :]), -f2["HV"][:-1, :] + p["min_depth"])
+    f2["DV"][:-1, :] = xv + f2["HV"][:-1, :]
+    d1 = 2 * p["min_depth"]
+    d2i = 1.0 / (p["crit_depth"] - 2 * p["min_depth"])
+    f2["dry_z"][...] = np.where(az > 0, np.clip((D - 0.5 * d1) * d2i, 0, 1), 0.0)
+    f2["dry_u"][...] = np.where(au > 0, np.clip((f2["DU"] - d1) * d2i, 0, 1), 0.0)
+    f2["dry_v"][...] = np.where(av > 0, np.clip((f2["DV"] - d1) * d2i, 0, 1), 0.0)
+    # macro-step elevations: old = new = z (start-up)
+    for a, b in (("sseo", "z"), ("ssen", "z")):
+        f2[a][...] = f2[b]
+    ssu = np.zeros(g.shape2())
+    ssu[:, :-1] = np.maximum(0.5 * (z[:, :-1] + z[:, 1:]), -f2["HU"][:, :-1] + p["min_depth"])
+    ssv = np.zeros(g.shape2())
+    ssv[:-1, :] = np.maximum(0.5 * (z[:-1, :] + z[1:, :]), -f2["HV"][:-1, :] + p["min_depth"])
+    f2["ssuo"][...] = ssu
+    f2["ssun"][...] = ssu
+    f2["ssvo"][...] = ssv
+    f2["ssvn"][...] = ssv
+    f2["Dn"][...] = f2["ssen"] + H
+    f2["Dun"][...] = f2["ssun"] + f2["HU"]
+    f2["Dvn"][...] = f2["ssvn"] + f2["HV"]
+    # layer heights (sigma_coordinates, all levels)
+    f3 = c.f3
+    f3["ho"][...] = ((f2["sseo"] + H) / kmax)[None]
+    f3["hn"][...] = ((f2["ssen"] + H) / kmax)[None]
+    f3["huo"][...] = ((f2["ssuo"] + f2["HU"]) / kmax)[None]
+    f3["hun"][...] = ((f2["ssun"] + f2["HU"]) / kmax)[None]
+    f3["hvo"][...] = ((f2["ssvo"] + f2["HV"]) / kmax)[None]
+    f3["hvn"][...] = ((f2["ssvn"] + f2["HV"]) / kmax)[None]
+    # stratification on sigma levels: depth of layer centre
+    sig = (np.arange(kmax + 1) - 0.5) / kmax  # centre of layer k as fraction of depth from bottom
+    depth_frac = (1.0 - sig)[:, None, None]  # 0 at surface, 1 at bottom
+    T = 20.0 - 12.0 * depth_frac + 0.1 * rng.normal(size=g.shape3())
+    S = 30.0 + 5.0 * depth_frac + np.zeros(g.shape3())
+    T[0] = 0.0
+    S[0] = 0.0
+    wet3 = (az >= 1)[None]
+    f3["T"][...] = np.where(wet3, T, 0.0)
+    f3["S"][...] = np.where(wet3, S, 0.0)
+    # viscosity / diffusivity at interfaces k (between layers k and k+1): sigma_k = k/kmax
+    s = np.arange(kmax + 1) / kmax
+    nu = 4 * nu_max * s * (1 - s) + 1e-6
+    f3["num"][...] = nu[:, None, None]
+    f3["nuh"][...] = nu[:, None, None]
+    _eqstate(c)
+    return c
+
+
+# -------------------------------------------------------------------------------------------------
+def oracle_struct(c: BcCase):
+    """ctypes struct (or_bc) of numpy pointers for the oracle; keeps references alive."""
+    import ctypes as C
+
+    from .grid import HALO as _  # noqa: F401
+
+    n2, n3, npd, npi = len(F2_NAMES), len(F3_NAMES), len(PD_NAMES), len(PI_NAMES)
+
+    class OrBc(C.Structure):
+        _fields_ = [("f2", C.c_void_p * n2), ("f3", C.c_void_p * n3), ("az", C.c_void_p), ("au", C.c_void_p),
+                    ("av", C.c_void_p), ("ax", C.c_void_p), ("par", C.c_double * npd), ("ipar", C.c_int * npi)]
+
+    s = OrBc()
+    for q, nm in enumerate(F2_NAMES):
+        a = c.f2[nm]
+        assert a.flags.c_contiguous and a.dtype == np.float64
+        s.f2[q] = a.ctypes.data
+    for q, nm in enumerate(F3_NAMES):
+        a = c.f3[nm]
+        assert a.flags.c_contiguous and a.dtype == c.dtype3
+        s.f3[q] = a.ctypes.data
+    s.az, s.au, s.av, s.ax = (m.ctypes.data for m in c.masks())
+    for q, nm in enumerate(PD_NAMES):
+        s.par[q] = c.pd[nm]
+    for q, nm in enumerate(PI_NAMES):
+        s.ipar[q] = int(c.pi[nm])
+    return s
+
+
+def read_back_ipar(c: BcCase, s):
+    for q, nm in enumerate(PI_NAMES):
+        c.pi[nm] = int(s.ipar[q])

@@ -78,6 +78,55 @@ def _declare(L):
         rc.restype = C.c_int
     L.or_derive_uvx.argtypes = [P, P, P, P, P]
     L.or_build_masks.argtypes = [P, P, P, P, P, P]
+    for suf in ("d", "f"):
+        fn = getattr(L, f"or_bc_steps_{suf}")
+        fn.argtypes = [P, P, C.c_int, C.c_int]
+        fn.restype = C.c_longlong
+        fn = getattr(L, f"or_bc_call_{suf}")
+        fn.argtypes = [P, P, C.c_int, C.c_int]
+        fn.restype = C.c_int
+    L.or_bc_sizes.argtypes = [P]
+
+
+# routine ids of or_bc_call (oracle_capi.cpp)
+BC_ROUTINES = ["bottom_friction", "uv_advect_2d", "umomentum", "vmomentum", "sealevel", "depth_update",
+               "start_macro", "bottom_friction_3d", "internal_pressure", "uu_momentum_3d", "vv_momentum_3d",
+               "sigma_coordinates", "ww_momentum_3d", "uv_advect_3d", "stresses_3d", "do_eqstate",
+               "slow_bottom_friction", "slow_terms", "integrate_2d", "integrate_3d"]
+
+
+def bc_sizes():
+    out = (C.c_int * 4)()
+    lib().or_bc_sizes(out)
+    return tuple(out)
+
+
+def bc_steps(case, n0: int, count: int):
+    """time_loop over micro steps n0..n0+count-1 on a code_b200.state.BcCase (in place)."""
+    from code_b200.state import oracle_struct, read_back_ipar
+
+    s = oracle_struct(case)
+    dom = OrDom(case.grid.imin, case.grid.imax, case.grid.jmin, case.grid.jmax, case.grid.kmax, case.grid.ni,
+                case.grid.ni * case.grid.nj, case.grid.dx, case.grid.dy, case.grid.ard1)
+    fn = lib().or_bc_steps_d if case.dtype3 == np.float64 else lib().or_bc_steps_f
+    r = fn(C.addressof(dom), C.addressof(s), n0, count)
+    read_back_ipar(case, s)
+    if r < 0:
+        raise ValueError("bc_steps failed")
+
+
+def bc_call(case, routine: str, arg: int = 0):
+    """One routine of the mode-split step on a BcCase (in place)."""
+    from code_b200.state import oracle_struct, read_back_ipar
+
+    s = oracle_struct(case)
+    dom = OrDom(case.grid.imin, case.grid.imax, case.grid.jmin, case.grid.jmax, case.grid.kmax, case.grid.ni,
+                case.grid.ni * case.grid.nj, case.grid.dx, case.grid.dy, case.grid.ard1)
+    fn = lib().or_bc_call_d if case.dtype3 == np.float64 else lib().or_bc_call_f
+    r = fn(C.addressof(dom), C.addressof(s), BC_ROUTINES.index(routine), arg)
+    read_back_ipar(case, s)
+    if r != 0:
+        raise ValueError(f"{routine} failed ({r})")
 
 
 def _p(a):

@@ -1,0 +1,858 @@
+// getm_baroclinic.hpp -- TEST INFRASTRUCTURE ONLY.
+//
+// CPU restatement of GETM 2.5's mode-split time step (the barotropic micro step integrate_2d and
+// the baroclinic macro step integrate_3d) for the closed-boundary, sigma-coordinate, prescribed
+// viscosity configuration, used as the parity oracle of the CUDA baroclinic path. Each routine
+// follows the reference file:line given beside it, with the same loop bounds and expression order
+// (no contraction: build with -ffp-contract=off). Fields of the module state (variables_2d,
+// variables_3d, domain) are passed as one table of pointers (BcState); 3D fields may be FP64 or
+// FP32 (template R3), 2D fields are always FP64.
+//
+// Scope: runtype 4 (prognostic T and S); no open boundaries (update_2d_bdy, mirror_bdy_2d/3d
+// are no-ops); vert_cord = 1 with equidistant sigma; eqstate_method = 1 (linear); ip_method = 1
+// (Blumberg-Mellor); num/nuh prescribed (gotm() leaves them unchanged); no numerical-mixing
+// analysis; no rivers; An_method = 0 and Am = 0 (no horizontal momentum diffusion).
+#pragma once
+#include <cmath>
+#include <cstdint>
+#include <vector>
+
+#include "getm_oracle.hpp"
+
+namespace gor {
+
+// Field tables: ORDER MATTERS (mirrored by code_b200/state.py and include/getm_b200.h).
+enum F2 {
+  Z, ZO, U_, V_, D_, DU, DV, UEX, VEX, FU, FV, RU, RV, RUU, RVV, UINT, VINT, UINTO, VINTO, SLUX, SLVX, SLRU, SLRV,
+  ZUB, ZVB, ZUB0, ZVB0, FWF, HH, HU, HV, DRY_Z, DRY_U, DRY_V, CORU, CORV, TAUSX, TAUSY, AIRP, SSEO, SSEN, SSUO,
+  SSUN, SSVO, SSVN, DN, DUN, DVN, RRU, RRV, TAUBX, TAUBY, TAUB, TAUS, NF2
+};
+enum F3 { UU, VV, WW, HO, HN, HUO, HUN, HVO, HVN, UUEX, VVEX, IDPDX, IDPDY, TT, SS, RHO, BUOY, NUM, NUH, NF3 };
+enum PD {
+  P_DTM, P_DT, P_CNPAR, P_MIN_DEPTH, P_CRIT_DEPTH, P_G, P_RHO_0, P_KAPPA, P_AVMMOL, P_AVMOLT, P_AVMOLS, P_T0, P_S0,
+  P_DTR0, P_DSR0, P_IP_FAC, P_TEMP_AH, P_SALT_AH, NPD
+};
+enum PI {
+  I_M, I_MM, I_RUNTYPE, I_VEL2D_SPLIT, I_VEL2D_HOR, I_VEL3D_SPLIT, I_VEL3D_HOR, I_VEL3D_VER, I_TEMP_SPLIT, I_TEMP_HOR,
+  I_TEMP_VER, I_SALT_SPLIT, I_SALT_HOR, I_SALT_VER, I_ADV_VER_ITERS, I_UFIRST2D, I_UFIRST3D, I_CALC_TEMP,
+  I_CALC_SALT, NPI
+};
+
+template <class R3>
+struct BcState {
+  double* f2[NF2];
+  R3* f3[NF3];
+  const int32_t *az, *au, *av, *ax;
+  double par[NPD];
+  int ipar[NPI];
+};
+
+// ---------------------------------------------------------------------------------------------
+// 2D helpers
+struct A2 {
+  const Dom& d;
+  double* p;
+  double& operator()(int i, int j) const { return p[d.ix(i, j)]; }
+};
+struct M2 {
+  const Dom& d;
+  const int32_t* p;
+  int operator()(int i, int j) const { return p[d.ix(i, j)]; }
+};
+template <class R>
+struct A3 {
+  const Dom& d;
+  R* p;
+  R& operator()(int i, int j, int k) const { return p[d.ix3(i, j, k)]; }
+};
+
+// bottom_friction.F90:48-150 (runtype>1 branch uses the stored ruu/rvv).
+inline void bottom_friction(const Dom& d, BcState<double>* /*unused*/, double** f2, const int32_t* aup,
+                            const int32_t* avp, const double* par, int runtype) {
+  A2 U{d, f2[U_]}, V{d, f2[V_]}, DU_{d, f2[DU]}, DV_{d, f2[DV]}, ruu{d, f2[RUU]}, rvv{d, f2[RVV]}, ru{d, f2[RU]},
+      rv{d, f2[RV]}, zub{d, f2[ZUB]}, zvb{d, f2[ZVB]}, zub0{d, f2[ZUB0]}, zvb0{d, f2[ZVB0]};
+  M2 au{d, aup}, av{d, avp};
+  const double kappa = par[P_KAPPA], avmmol = par[P_AVMMOL], min_depth = par[P_MIN_DEPTH];
+  const long n = d.n2d();
+  std::vector<double> uloc_(n, 0.0), vloc_(n, 0.0), HH_(n, 0.0), fricvel_(n, 0.0);
+  A2 uloc{d, uloc_.data()}, vloc{d, vloc_.data()}, HH{d, HH_.data()}, fricvel{d, fricvel_.data()};
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i) {
+      if (au(i, j) > 0)
+        vloc(i, j) = 0.25 * (V(i, j) / DV_(i, j) + V(i + 1, j) / DV_(i + 1, j) + V(i, j - 1) / DV_(i, j - 1) +
+                             V(i + 1, j - 1) / DV_(i + 1, j - 1));
+      else
+        vloc(i, j) = 0.0;
+    }
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO - 1; ++i)
+      if (au(i, j) > 0) {
+        uloc(i, j) = U(i, j) / DU_(i, j);
+        HH(i, j) = std::max(min_depth, DU_(i, j));
+        double x = kappa / std::log((zub(i, j) + 0.5 * HH(i, j)) / zub(i, j));
+        ruu(i, j) = x * x;
+      }
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO - 1; ++i)
+      if (au(i, j) > 0) {
+        if (runtype == 1) {
+          fricvel(i, j) = std::sqrt(ruu(i, j) * (uloc(i, j) * uloc(i, j) + vloc(i, j) * vloc(i, j)));
+          zub(i, j) = std::min(HH(i, j), zub0(i, j) + 0.1 * avmmol / std::max(avmmol, fricvel(i, j)));
+          ruu(i, j) = (zub(i, j) + 0.5 * HH(i, j)) / zub(i, j);
+          double x = kappa / std::log(ruu(i, j));
+          ruu(i, j) = x * x;
+        }
+        ru(i, j) = ruu(i, j) * std::sqrt(uloc(i, j) * uloc(i, j) + vloc(i, j) * vloc(i, j));
+      }
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i) {
+      if (av(i, j) > 0)
+        uloc(i, j) = 0.25 * (U(i, j) / DU_(i, j) + U(i - 1, j) / DU_(i - 1, j) + U(i, j + 1) / DU_(i, j + 1) +
+                             U(i - 1, j + 1) / DU_(i - 1, j + 1));
+      else
+        uloc(i, j) = 0.0;
+    }
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO - 1; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO; ++i)
+      if (av(i, j) > 0) {
+        vloc(i, j) = V(i, j) / DV_(i, j);
+        HH(i, j) = std::max(min_depth, DV_(i, j));
+        double x = kappa / std::log((zvb(i, j) + 0.5 * HH(i, j)) / zvb(i, j));
+        rvv(i, j) = x * x;
+      }
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO - 1; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO; ++i)
+      if (av(i, j) > 0) {
+        if (runtype == 1) {
+          fricvel(i, j) = std::sqrt(rvv(i, j) * (uloc(i, j) * uloc(i, j) + vloc(i, j) * vloc(i, j)));
+          zvb(i, j) = std::min(HH(i, j), zvb0(i, j) + 0.1 * avmmol / std::max(avmmol, fricvel(i, j)));
+          rvv(i, j) = (zvb(i, j) + 0.5 * HH(i, j)) / zvb(i, j);
+          double x = kappa / std::log(rvv(i, j));
+          rvv(i, j) = x * x;
+        }
+        rv(i, j) = rvv(i, j) * std::sqrt(uloc(i, j) * uloc(i, j) + vloc(i, j) * vloc(i, j));
+      }
+}
+
+// uv_advect.F90:94-300 (split schemes only, vel2d_adv_hor != J7): 2D momentum advection on the
+// U and V grids via do_advection with advres = UEx / VEx.
+inline int uv_advect_2d(const Dom& d, const AdvMasks& m, const int32_t* az, const int32_t* au, const int32_t* av,
+                        double dtm, const double* Up, const double* Vp, const double* DUp, const double* DVp,
+                        int split, int hor, double* UEx, double* VEx) {
+  const long n = d.n2d();
+  if (hor == NOADV) {
+    std::fill(UEx, UEx + n, 0.0);
+    std::fill(VEx, VEx + n, 0.0);
+    return 0;
+  }
+  A2 U{d, const_cast<double*>(Up)}, V{d, const_cast<double*>(Vp)}, DU_{d, const_cast<double*>(DUp)},
+      DV_{d, const_cast<double*>(DVp)};
+  // automatic arrays of the reference: undefined outside the loops; zero here
+  std::vector<double> fadv_(n, 0.0), Uadv_(n, 0.0), Vadv_(n, 0.0), DUadv_(n, 0.0), DVadv_(n, 0.0);
+  A2 fadv{d, fadv_.data()}, Uadv{d, Uadv_.data()}, Vadv{d, Vadv_.data()}, DUadv{d, DUadv_.data()},
+      DVadv{d, DVadv_.data()};
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO - 1; ++i) {
+      fadv(i, j) = U(i, j) / DU_(i, j);
+      Uadv(i, j) = 0.5 * (U(i, j) + U(i + 1, j));
+      Vadv(i, j) = 0.5 * (V(i, j) + V(i + 1, j));
+      DUadv(i, j) = 0.5 * (DU_(i, j) + DU_(i + 1, j));
+      DVadv(i, j) = 0.5 * (DV_(i, j) + DV_(i + 1, j));
+    }
+  AdvGrid gu = adv_grid(m, U_TAG, az, au, av);
+  if (do_advection<double>(d, gu, dtm, fadv_.data(), Uadv_.data(), Vadv_.data(), DUadv_.data(), DVadv_.data(), DUp,
+                           DUp, split, hor, 0.0, nullptr, UEx) != 0)
+    return -1;
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO - 1; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO; ++i) {
+      fadv(i, j) = V(i, j) / DV_(i, j);
+      Uadv(i, j) = 0.5 * (U(i, j) + U(i, j + 1));
+      Vadv(i, j) = 0.5 * (V(i, j) + V(i, j + 1));
+      DUadv(i, j) = 0.5 * (DU_(i, j) + DU_(i, j + 1));
+      DVadv(i, j) = 0.5 * (DV_(i, j) + DV_(i, j + 1));
+    }
+  AdvGrid gv = adv_grid(m, V_TAG, az, au, av);
+  if (do_advection<double>(d, gv, dtm, fadv_.data(), Uadv_.data(), Vadv_.data(), DUadv_.data(), DVadv_.data(), DVp,
+                           DVp, split, hor, 0.0, nullptr, VEx) != 0)
+    return -1;
+  return 0;
+}
+
+// momentum.F90:69-223 umomentum, :232-386 vmomentum (CARTESIAN, no NEW_CORI).
+inline void umomentum(const Dom& d, double** f2, const int32_t* aup, const int32_t* avp, const double* par) {
+  A2 U{d, f2[U_]}, DU_{d, f2[DU]}, z{d, f2[Z]}, H{d, f2[HH]}, D{d, f2[D_]}, airp{d, f2[AIRP]}, tausx{d, f2[TAUSX]},
+      Slru{d, f2[SLRU]}, dry_u{d, f2[DRY_U]}, fV{d, f2[FV]}, UEx{d, f2[UEX]}, SlUx{d, f2[SLUX]}, ru{d, f2[RU]},
+      fU{d, f2[FU]}, corv{d, f2[CORV]};
+  M2 au{d, aup}, av{d, avp};
+  const double g = par[P_G], rho_0 = par[P_RHO_0], dtm = par[P_DTM], min_depth = par[P_MIN_DEPTH];
+  const double gamma = rho_0 * g;
+  const double gammai = 1.0 / gamma;
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i)
+      if (au(i, j) == 1 || au(i, j) == 2) {
+        double zp = std::max(z(i + 1, j), -H(i, j) + std::min(min_depth, D(i + 1, j)));
+        double zm = std::max(z(i, j), -H(i + 1, j) + std::min(min_depth, D(i, j)));
+        double zx = (zp - zm + (airp(i + 1, j) - airp(i, j)) * gammai) / d.dx;
+        double tausu = 0.5 * (tausx(i, j) + tausx(i + 1, j));
+        double Slr = U(i, j) > 0.0 ? std::max(Slru(i, j), 0.0) : std::min(Slru(i, j), 0.0);
+        U(i, j) = (U(i, j) - dtm * (g * DU_(i, j) * zx +
+                                    dry_u(i, j) * (-tausu / rho_0 - fV(i, j) + UEx(i, j) + SlUx(i, j) + Slr))) /
+                  (1.0 + dtm * ru(i, j) / DU_(i, j));
+      }
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i) {
+      if (av(i, j) >= 1) {
+        double Uloc = 0.25 * (U(i - 1, j) + U(i, j) + U(i - 1, j + 1) + U(i, j + 1));
+        fU(i, j) = corv(i, j) * Uloc;
+      } else {
+        fU(i, j) = 0.0;
+      }
+    }
+}
+
+inline void vmomentum(const Dom& d, double** f2, const int32_t* aup, const int32_t* avp, const double* par) {
+  A2 V{d, f2[V_]}, DV_{d, f2[DV]}, z{d, f2[Z]}, H{d, f2[HH]}, D{d, f2[D_]}, airp{d, f2[AIRP]}, tausy{d, f2[TAUSY]},
+      Slrv{d, f2[SLRV]}, dry_v{d, f2[DRY_V]}, fU{d, f2[FU]}, VEx{d, f2[VEX]}, SlVx{d, f2[SLVX]}, rv{d, f2[RV]},
+      fV{d, f2[FV]}, coru{d, f2[CORU]};
+  M2 au{d, aup}, av{d, avp};
+  const double g = par[P_G], rho_0 = par[P_RHO_0], dtm = par[P_DTM], min_depth = par[P_MIN_DEPTH];
+  const double gamma = rho_0 * g;
+  const double gammai = 1.0 / gamma;
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i)
+      if (av(i, j) == 1 || av(i, j) == 2) {
+        double zp = std::max(z(i, j + 1), -H(i, j) + std::min(min_depth, D(i, j + 1)));
+        double zm = std::max(z(i, j), -H(i, j + 1) + std::min(min_depth, D(i, j)));
+        double zy = (zp - zm + (airp(i, j + 1) - airp(i, j)) * gammai) / d.dy;
+        double tausv = 0.5 * (tausy(i, j) + tausy(i, j + 1));
+        double Slr = V(i, j) > 0.0 ? std::max(Slrv(i, j), 0.0) : std::min(Slrv(i, j), 0.0);
+        V(i, j) = (V(i, j) - dtm * (g * DV_(i, j) * zy +
+                                    dry_v(i, j) * (-tausv / rho_0 + fU(i, j) + VEx(i, j) + SlVx(i, j) + Slr))) /
+                  (1.0 + dtm * rv(i, j) / DV_(i, j));
+      }
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i) {
+      if (au(i, j) >= 1) {
+        double Vloc = 0.25 * (V(i, j - 1) + V(i + 1, j - 1) + V(i, j) + V(i + 1, j));
+        fV(i, j) = coru(i, j) * Vloc;
+      } else {
+        fV(i, j) = 0.0;
+      }
+    }
+}
+
+// sealevel.F90:65-112
+inline void sealevel(const Dom& d, double** f2, const int32_t* azp, const double* par) {
+  A2 z{d, f2[Z]}, zo{d, f2[ZO]}, U{d, f2[U_]}, V{d, f2[V_]}, fwf{d, f2[FWF]};
+  M2 az{d, azp};
+  const double dtm = par[P_DTM];
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO; ++i) zo(i, j) = z(i, j);
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i)
+      if (az(i, j) == 1)
+        z(i, j) = z(i, j) - dtm * ((U(i, j) * d.dy - U(i - 1, j) * d.dy) + (V(i, j) * d.dx - V(i, j - 1) * d.dx)) * d.ard1 +
+                  dtm * fwf(i, j);
+}
+
+// depth_update.F90:55-110
+inline void depth_update(const Dom& d, double** f2, const int32_t* azp, const int32_t* aup, const int32_t* avp,
+                         const double* par) {
+  A2 D{d, f2[D_]}, z{d, f2[Z]}, zo{d, f2[ZO]}, H{d, f2[HH]}, HU_{d, f2[HU]}, HV_{d, f2[HV]}, DU_{d, f2[DU]},
+      DV_{d, f2[DV]}, dry_z{d, f2[DRY_Z]}, dry_u{d, f2[DRY_U]}, dry_v{d, f2[DRY_V]};
+  M2 az{d, azp}, au{d, aup}, av{d, avp};
+  const double min_depth = par[P_MIN_DEPTH], crit_depth = par[P_CRIT_DEPTH];
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO; ++i) D(i, j) = z(i, j) + H(i, j);
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO - 1; ++i) {
+      double x = std::max(0.25 * (zo(i, j) + zo(i + 1, j) + z(i, j) + z(i + 1, j)), -HU_(i, j) + min_depth);
+      DU_(i, j) = x + HU_(i, j);
+    }
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO - 1; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO; ++i) {
+      double x = std::max(0.25 * (zo(i, j) + zo(i, j + 1) + z(i, j) + z(i, j + 1)), -HV_(i, j) + min_depth);
+      DV_(i, j) = x + HV_(i, j);
+    }
+  const double d1 = 2 * min_depth;
+  const double d2i = 1.0 / (crit_depth - 2 * min_depth);
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO; ++i) {
+      if (az(i, j) > 0) dry_z(i, j) = std::max(0.0, std::min(1.0, (D(i, j) - 0.5 * d1) * d2i));
+      if (au(i, j) > 0) dry_u(i, j) = std::max(0.0, std::min(1.0, (DU_(i, j) - d1) * d2i));
+      if (av(i, j) > 0) dry_v(i, j) = std::max(0.0, std::min(1.0, (DV_(i, j) - d1) * d2i));
+    }
+}
+
+// m2d.F90:412-490 integrate_2d (closed boundaries, no residual, no uv_diffusion).
+template <class R3>
+int integrate_2d(const Dom& d, const AdvMasks& m, BcState<R3>& st, int loop) {
+  double** f2 = st.f2;
+  const double* par = st.par;
+  int* ip = st.ipar;
+  if ((loop - 1) % ip[I_MM] == 0) bottom_friction(d, nullptr, f2, st.au, st.av, par, ip[I_RUNTYPE]);
+  if (uv_advect_2d(d, m, st.az, st.au, st.av, par[P_DTM], f2[U_], f2[V_], f2[DU], f2[DV], ip[I_VEL2D_SPLIT],
+                   ip[I_VEL2D_HOR], f2[UEX], f2[VEX]) != 0)
+    return -1;
+  // momentum.F90:44-52: SAVEd toggle ufirst (initially .false.)
+  if (ip[I_UFIRST2D]) {
+    umomentum(d, f2, st.au, st.av, par);
+    vmomentum(d, f2, st.au, st.av, par);
+    ip[I_UFIRST2D] = 0;
+  } else {
+    vmomentum(d, f2, st.au, st.av, par);
+    umomentum(d, f2, st.au, st.av, par);
+    ip[I_UFIRST2D] = 1;
+  }
+  if (ip[I_RUNTYPE] > 1) {
+    const long n = d.n2d();
+    for (long q = 0; q < n; ++q) {
+      f2[UINT][q] = f2[UINT][q] + f2[U_][q];
+      f2[VINT][q] = f2[VINT][q] + f2[V_][q];
+    }
+  }
+  sealevel(d, f2, st.az, par);
+  depth_update(d, f2, st.az, st.au, st.av, par);
+  return 0;
+}
+
+// ---------------------------------------------------------------------------------------------
+// start_macro.F90:54-86
+inline void start_macro(const Dom& d, double** f2, const double* par, int M) {
+  A2 sseo{d, f2[SSEO]}, ssen{d, f2[SSEN]}, z{d, f2[Z]}, Dn{d, f2[DN]}, H{d, f2[HH]}, ssuo{d, f2[SSUO]},
+      ssun{d, f2[SSUN]}, HU_{d, f2[HU]}, Dun{d, f2[DUN]}, ssvo{d, f2[SSVO]}, ssvn{d, f2[SSVN]}, HV_{d, f2[HV]},
+      Dvn{d, f2[DVN]};
+  const double min_depth = par[P_MIN_DEPTH];
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO; ++i) {
+      sseo(i, j) = ssen(i, j);
+      ssen(i, j) = z(i, j);
+      Dn(i, j) = ssen(i, j) + H(i, j);
+    }
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO - 1; ++i) {
+      ssuo(i, j) = ssun(i, j);
+      ssun(i, j) = 0.25 * (sseo(i, j) + sseo(i + 1, j) + ssen(i, j) + ssen(i + 1, j));
+      ssun(i, j) = std::max(ssun(i, j), -HU_(i, j) + min_depth);
+      Dun(i, j) = ssun(i, j) + HU_(i, j);
+    }
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO - 1; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO; ++i) {
+      ssvo(i, j) = ssvn(i, j);
+      ssvn(i, j) = 0.25 * (sseo(i, j) + sseo(i, j + 1) + ssen(i, j) + ssen(i, j + 1));
+      ssvn(i, j) = std::max(ssvn(i, j), -HV_(i, j) + min_depth);
+      Dvn(i, j) = ssvn(i, j) + HV_(i, j);
+    }
+  const double split = 1.0 / (double)(float)M;
+  const long n = d.n2d();
+  for (long q = 0; q < n; ++q) {
+    f2[UINT][q] = split * f2[UINT][q];
+    f2[VINT][q] = split * f2[VINT][q];
+  }
+}
+
+// bottom_friction_3d.F90:50-130 (kumin = kvmin = 1)
+template <class R3>
+void bottom_friction_3d(const Dom& d, BcState<R3>& st) {
+  double** f2 = st.f2;
+  A2 zub{d, f2[ZUB]}, zvb{d, f2[ZVB]}, rru{d, f2[RRU]}, rrv{d, f2[RRV]};
+  A3<R3> uu{d, st.f3[UU]}, vv{d, st.f3[VV]}, huo{d, st.f3[HUO]}, hvo{d, st.f3[HVO]}, hun{d, st.f3[HUN]},
+      hvn{d, st.f3[HVN]};
+  M2 au{d, st.au}, av{d, st.av};
+  const double kappa = st.par[P_KAPPA], min_depth = st.par[P_MIN_DEPTH];
+  const long n = d.n2d();
+  std::vector<double> a_(n, 0.0), b_(n, 0.0), c_(n, 0.0), e_(n, 0.0);
+  A2 uuloc{d, a_.data()}, uvloc{d, b_.data()}, vuloc{d, c_.data()}, vvloc{d, e_.data()};
+  const int kk = 1;
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i) {
+      if (au(i, j) >= 1) {
+        uuloc(i, j) = (double)uu(i, j, kk) / ((double)huo(i, j, kk));
+        uvloc(i, j) = 0.25 * ((double)vv(i, j, kk) / (double)hvo(i, j, kk) + (double)vv(i + 1, j, kk) / (double)hvo(i + 1, j, kk) +
+                              (double)vv(i, j - 1, kk) / (double)hvo(i, j - 1, kk) +
+                              (double)vv(i + 1, j - 1, kk) / (double)hvo(i + 1, j - 1, kk));
+      } else {
+        uuloc(i, j) = 0.0;
+        uvloc(i, j) = 0.0;
+      }
+    }
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i) {
+      if (av(i, j) >= 1) {
+        vuloc(i, j) = 0.25 * ((double)uu(i, j, kk) / (double)huo(i, j, kk) + (double)uu(i - 1, j, kk) / (double)huo(i - 1, j, kk) +
+                              (double)uu(i, j + 1, kk) / (double)huo(i, j + 1, kk) +
+                              (double)uu(i - 1, j + 1, kk) / (double)huo(i - 1, j + 1, kk));
+        vvloc(i, j) = (double)vv(i, j, kk) / ((double)hvo(i, j, kk));
+      } else {
+        vuloc(i, j) = 0.0;
+        vvloc(i, j) = 0.0;
+      }
+    }
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i)
+      if (au(i, j) >= 1) {
+        double hh = std::max(min_depth / d.kmax, (double)hun(i, j, kk));
+        double r = (zub(i, j) + 0.5 * hh) / zub(i, j);
+        r = kappa / std::log(r);
+        r = r * r;
+        rru(i, j) = r * std::sqrt(uuloc(i, j) * uuloc(i, j) + uvloc(i, j) * uvloc(i, j));
+      }
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i)
+      if (av(i, j) >= 1) {
+        double hh = std::max(min_depth / d.kmax, (double)hvn(i, j, kk));
+        double r = (zvb(i, j) + 0.5 * hh) / zvb(i, j);
+        r = kappa / std::log(r);
+        r = r * r;
+        rrv(i, j) = r * std::sqrt(vuloc(i, j) * vuloc(i, j) + vvloc(i, j) * vvloc(i, j));
+      }
+}
+
+// ip_blumberg_mellor.F90:71-148
+template <class R3>
+void ip_blumberg_mellor(const Dom& d, BcState<R3>& st) {
+  A3<R3> hn{d, st.f3[HN]}, hun{d, st.f3[HUN]}, hvn{d, st.f3[HVN]}, buoy{d, st.f3[BUOY]}, idpdx{d, st.f3[IDPDX]},
+      idpdy{d, st.f3[IDPDY]};
+  A2 H{d, st.f2[HH]};
+  M2 az{d, st.az}, au{d, st.au}, av{d, st.av};
+  const int kmax = d.kmax;
+  const R3 dxm1 = R3(1.0 / d.dx), dym1 = R3(1.0 / d.dy);
+  std::vector<R3> zz_(d.n3d(), R3(0));
+  A3<R3> zz{d, zz_.data()};
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO; ++i) {
+      idpdx(i, j, 0) = R3(0);
+      idpdy(i, j, 0) = R3(0);
+    }
+  for (int j = d.jmin; j <= d.jmax + 1; ++j)
+    for (int i = d.imin; i <= d.imax + 1; ++i)
+      if (az(i, j) >= 1) {
+        zz(i, j, 1) = R3(-H(i, j)) + hn(i, j, 1);
+        for (int k = 2; k <= kmax; ++k) zz(i, j, k) = zz(i, j, k - 1) + hn(i, j, k);
+      }
+  const R3 half = R3(0.5);
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i)
+      if (au(i, j) >= 1) {
+        R3 grdl = (buoy(i + 1, j, kmax) - buoy(i, j, kmax)) * dxm1;
+        R3 buoyl = half * (buoy(i + 1, j, kmax) + buoy(i, j, kmax));
+        R3 prgr = grdl * half * hun(i, j, kmax);
+        idpdx(i, j, kmax) = hun(i, j, kmax) * prgr;
+        for (int k = kmax - 1; k >= 1; --k) {
+          R3 grdu = grdl;
+          grdl = (buoy(i + 1, j, k) - buoy(i, j, k)) * dxm1;
+          R3 buoyu = buoyl;
+          buoyl = half * (buoy(i + 1, j, k) + buoy(i, j, k));
+          R3 dxz = (zz(i + 1, j, k) - zz(i, j, k)) * dxm1;
+          prgr = prgr + half * (grdu + grdl) * half * (hun(i, j, k) + hun(i, j, k + 1)) - dxz * (buoyu - buoyl);
+          idpdx(i, j, k) = hun(i, j, k) * prgr;
+        }
+      }
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i)
+      if (av(i, j) >= 1) {
+        R3 grdl = (buoy(i, j + 1, kmax) - buoy(i, j, kmax)) * dym1;
+        R3 buoyl = half * (buoy(i, j + 1, kmax) + buoy(i, j, kmax));
+        R3 prgr = grdl * half * hvn(i, j, kmax);
+        idpdy(i, j, kmax) = hvn(i, j, kmax) * prgr;
+        for (int k = kmax - 1; k >= 1; --k) {
+          R3 grdu = grdl;
+          grdl = (buoy(i, j + 1, k) - buoy(i, j, k)) * dym1;
+          R3 buoyu = buoyl;
+          buoyl = half * (buoy(i, j + 1, k) + buoy(i, j, k));
+          R3 dyz = (zz(i, j + 1, k) - zz(i, j, k)) * dym1;
+          prgr = prgr + half * (grdu + grdl) * half * (hvn(i, j, k) + hvn(i, j, k + 1)) - dyz * (buoyu - buoyl);
+          idpdy(i, j, k) = hvn(i, j, k) * prgr;
+        }
+      }
+}
+
+// uu_momentum_3d.F90:169-337 / vv_momentum_3d.F90:174-340 (kumin = kvmin = 1). dir 0 = uu.
+template <class R3>
+void uv_momentum_3d(const Dom& d, BcState<R3>& st, int dir) {
+  double** f2 = st.f2;
+  const double* par = st.par;
+  const int kmax = d.kmax;
+  A3<R3> uu{d, st.f3[dir == 0 ? UU : VV]}, vv{d, st.f3[dir == 0 ? VV : UU]};
+  A3<R3> ho_{d, st.f3[dir == 0 ? HUO : HVO]}, hn_{d, st.f3[dir == 0 ? HUN : HVN]};
+  A3<R3> Ex{d, st.f3[dir == 0 ? UUEX : VVEX]}, idp{d, st.f3[dir == 0 ? IDPDX : IDPDY]}, num{d, st.f3[NUM]};
+  A2 dry{d, f2[dir == 0 ? DRY_U : DRY_V]}, cor{d, f2[dir == 0 ? CORU : CORV]}, taus{d, f2[dir == 0 ? TAUSX : TAUSY]},
+      sseo{d, f2[SSEO]}, H{d, f2[HH]}, D{d, f2[D_]}, airp{d, f2[AIRP]}, rr{d, f2[dir == 0 ? RRU : RRV]},
+      Uint{d, f2[dir == 0 ? UINT : VINT]}, sso{d, f2[dir == 0 ? SSUO : SSVO]}, HX{d, f2[dir == 0 ? HU : HV]};
+  M2 mask{d, dir == 0 ? st.au : st.av};
+  const double g = par[P_G], rho_0 = par[P_RHO_0], dt = par[P_DT], cnpar = par[P_CNPAR], avmmol = par[P_AVMMOL],
+               min_depth = par[P_MIN_DEPTH], ip_fac = par[P_IP_FAC];
+  const double gamma = g * rho_0;
+  const double gammai = 1.0 / gamma, rho_0i = 1.0 / rho_0;
+  const int di = dir == 0 ? 1 : 0, dj = dir == 0 ? 0 : 1;
+  const double dxy = dir == 0 ? d.dx : d.dy;
+  std::vector<double> dif(kmax + 1), auxn(kmax + 1), auxo(kmax + 1), a1(kmax + 1), a2(kmax + 1), a3(kmax + 1),
+      a4(kmax + 1), Res(kmax + 1), ex(kmax + 1);
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i) {
+      if (!(mask(i, j) == 1 || mask(i, j) == 2)) continue;
+      const int kmn = 1;
+      if (kmax > kmn) {
+        for (int k = kmn; k <= kmax; ++k) {
+          double loc, e;
+          if (dir == 0) {
+            loc = 0.25 * ((double)vv(i, j, k) + (double)vv(i + 1, j, k) + (double)vv(i, j - 1, k) + (double)vv(i + 1, j - 1, k));
+            e = cor(i, j) * loc;
+          } else {
+            loc = 0.25 * ((double)vv(i, j, k) + (double)vv(i - 1, j, k) + (double)vv(i, j + 1, k) + (double)vv(i - 1, j + 1, k));
+            e = -cor(i, j) * loc;
+          }
+          ex[k] = dry(i, j) * (e - (double)Ex(i, j, k) + ip_fac * (double)idp(i, j, k));
+        }
+        ex[kmax] = ex[kmax] + dry(i, j) * 0.5 * (taus(i, j) + taus(i + di, j + dj)) * rho_0i;
+        for (int k = kmn; k <= kmax - 1; ++k) dif[k] = 0.5 * ((double)num(i, j, k) + (double)num(i + di, j + dj, k)) + avmmol;
+        for (int k = kmn; k <= kmax - 1; ++k) {
+          auxo[k] = 2.0 * (1.0 - cnpar) * dt * dif[k] / ((double)ho_(i, j, k + 1) + (double)ho_(i, j, k));
+          auxn[k] = 2.0 * cnpar * dt * dif[k] / ((double)hn_(i, j, k + 1) + (double)hn_(i, j, k));
+        }
+        double zp = std::max(sseo(i + di, j + dj), -H(i, j) + std::min(min_depth, D(i + di, j + dj)));
+        double zm = std::max(sseo(i, j), -H(i + di, j + dj) + std::min(min_depth, D(i, j)));
+        double zx;
+        if (dir == 0)
+          zx = (zp - zm + (airp(i + 1, j) - airp(i, j)) * gammai) / dxy;
+        else
+          zx = (zp - zm + (airp(i, j + 1) - airp(i, j)) / gamma) / dxy;
+        auto HOd = [&](int k) { return (double)ho_(i, j, k); };
+        auto HNd = [&](int k) { return (double)hn_(i, j, k); };
+        auto UUd = [&](int k) { return (double)uu(i, j, k); };
+        int k = kmax;
+        a1[k] = -auxn[k - 1] / HNd(k - 1);
+        a2[k] = 1. + auxn[k - 1] / HNd(k);
+        a4[k] = UUd(k) * (1 - auxo[k - 1] / HOd(k)) + UUd(k - 1) * auxo[k - 1] / HOd(k - 1) + dt * ex[k] -
+                dt * 0.5 * (HOd(k) + HNd(k)) * g * zx;
+        for (k = kmn + 1; k <= kmax - 1; ++k) {
+          a3[k] = -auxn[k] / HNd(k + 1);
+          a1[k] = -auxn[k - 1] / HNd(k - 1);
+          a2[k] = 1.0 + (auxn[k] + auxn[k - 1]) / HNd(k);
+          a4[k] = UUd(k + 1) * auxo[k] / HOd(k + 1) + UUd(k) * (1 - (auxo[k] + auxo[k - 1]) / HOd(k)) +
+                  UUd(k - 1) * auxo[k - 1] / HOd(k - 1) + dt * ex[k] - dt * 0.5 * (HOd(k) + HNd(k)) * g * zx;
+        }
+        k = kmn;
+        a3[k] = -auxn[k] / HNd(k + 1);
+        a2[k] = 1.0 + auxn[k] / HNd(k) + dt * rr(i, j) / (0.5 * (HNd(k) + HOd(k)));
+        a4[k] = UUd(k + 1) * auxo[k] / HOd(k + 1) + UUd(k) * (1 - auxo[k] / HOd(k)) + dt * ex[k] -
+                dt * 0.5 * (HOd(k) + HNd(k)) * g * zx;
+        getm_tridiagonal<double>(kmax, kmn, kmax, a1.data(), a2.data(), a3.data(), a4.data(), Res.data());
+        double ResInt = 0.0;
+        for (k = kmn; k <= kmax; ++k) ResInt = ResInt + Res[k];
+        double Diff = (Uint(i, j) - ResInt) / (sso(i, j) + HX(i, j));
+        for (k = kmn; k <= kmax; ++k) uu(i, j, k) = R3(Res[k] + HNd(k) * Diff);
+      } else {
+        uu(i, j, kmax) = R3(Uint(i, j));
+      }
+    }
+}
+
+// sigma_coordinates.F90:85-113 (equidistant), all levels 0..kmax
+template <class R3>
+void sigma_coordinates(const Dom& d, BcState<R3>& st) {
+  double** f2 = st.f2;
+  A2 sseo{d, f2[SSEO]}, ssen{d, f2[SSEN]}, H{d, f2[HH]}, ssuo{d, f2[SSUO]}, ssun{d, f2[SSUN]}, HU_{d, f2[HU]},
+      ssvo{d, f2[SSVO]}, ssvn{d, f2[SSVN]}, HV_{d, f2[HV]};
+  A3<R3> ho{d, st.f3[HO]}, hn{d, st.f3[HN]}, huo{d, st.f3[HUO]}, hun{d, st.f3[HUN]}, hvo{d, st.f3[HVO]},
+      hvn{d, st.f3[HVN]};
+  const double kmaxm1 = 1.0 / (double)(float)d.kmax;
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO; ++i) {
+      const R3 a = R3((sseo(i, j) + H(i, j)) * kmaxm1), b = R3((ssen(i, j) + H(i, j)) * kmaxm1);
+      for (int k = 0; k <= d.kmax; ++k) {
+        ho(i, j, k) = a;
+        hn(i, j, k) = b;
+      }
+    }
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO - 1; ++i) {
+      const R3 a = R3((ssuo(i, j) + HU_(i, j)) * kmaxm1), b = R3((ssun(i, j) + HU_(i, j)) * kmaxm1);
+      for (int k = 0; k <= d.kmax; ++k) {
+        huo(i, j, k) = a;
+        hun(i, j, k) = b;
+      }
+    }
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO - 1; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO; ++i) {
+      const R3 a = R3((ssvo(i, j) + HV_(i, j)) * kmaxm1), b = R3((ssvn(i, j) + HV_(i, j)) * kmaxm1);
+      for (int k = 0; k <= d.kmax; ++k) {
+        hvo(i, j, k) = a;
+        hvn(i, j, k) = b;
+      }
+    }
+}
+
+// ww_momentum_3d.F90:74-106 (kmin = 1)
+template <class R3>
+void ww_momentum_3d(const Dom& d, BcState<R3>& st) {
+  A3<R3> ww{d, st.f3[WW]}, hn{d, st.f3[HN]}, ho{d, st.f3[HO]}, uu{d, st.f3[UU]}, vv{d, st.f3[VV]};
+  M2 az{d, st.az};
+  const R3 dtm1 = R3(1.0 / st.par[P_DT]);
+  const R3 dx = R3(d.dx), dy = R3(d.dy), ard1 = R3(d.ard1);
+  for (int k = 1; k <= d.kmax - 1; ++k)
+    for (int j = d.jmin; j <= d.jmax; ++j)
+      for (int i = d.imin; i <= d.imax; ++i)
+        if (az(i, j) == 1)
+          ww(i, j, k) = ww(i, j, k - 1) - (hn(i, j, k) - ho(i, j, k)) * dtm1 -
+                        (uu(i, j, k) * dy - uu(i - 1, j, k) * dy + vv(i, j, k) * dx - vv(i, j - 1, k) * dx) * ard1;
+}
+
+// uv_advect_3d.F90:62-460 (split schemes, no J7, no numerical analyses)
+template <class R3>
+int uv_advect_3d(const Dom& d, const AdvMasks& m, BcState<R3>& st) {
+  const int* ip = st.ipar;
+  const int split = ip[I_VEL3D_SPLIT], hor = ip[I_VEL3D_HOR], ver = ip[I_VEL3D_VER];
+  if (hor == NOADV && ver == NOADV) return 0;
+  const long n3 = d.n3d();
+  std::vector<R3> f_(n3, R3(0)), ua_(n3, R3(0)), va_(n3, R3(0)), wa_(n3, R3(0)), hua_(n3, R3(0)), hva_(n3, R3(0));
+  A3<R3> fadv{d, f_.data()}, uuadv{d, ua_.data()}, vvadv{d, va_.data()}, wwadv{d, wa_.data()}, huadv{d, hua_.data()},
+      hvadv{d, hva_.data()};
+  A3<R3> uu{d, st.f3[UU]}, vv{d, st.f3[VV]}, ww{d, st.f3[WW]}, ho{d, st.f3[HO]}, hn{d, st.f3[HN]}, hun{d, st.f3[HUN]},
+      hvn{d, st.f3[HVN]};
+  const R3 half = R3(0.5);
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO; ++i) wwadv(i, j, 0) = R3(0);
+  for (int k = 1; k <= d.kmax; ++k)
+    for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
+      for (int i = d.imin - HALO; i <= d.imax + HALO - 1; ++i) {
+        fadv(i, j, k) = uu(i, j, k) / hun(i, j, k);
+        uuadv(i, j, k) = half * (uu(i, j, k) + uu(i + 1, j, k));
+        vvadv(i, j, k) = half * (vv(i, j, k) + vv(i + 1, j, k));
+        wwadv(i, j, k) = half * (ww(i, j, k) + ww(i + 1, j, k));
+        huadv(i, j, k) = half * (ho(i + 1, j, k) + hn(i + 1, j, k));
+        hvadv(i, j, k) = half * (hvn(i, j, k) + hvn(i + 1, j, k));
+      }
+  AdvGrid gu = adv_grid(m, U_TAG, st.az, st.au, st.av);
+  if (do_advection_3d<R3>(d, gu, R3(st.par[P_DT]), f_.data(), ua_.data(), va_.data(), wa_.data(), hua_.data(),
+                          hva_.data(), st.f3[HUN], st.f3[HUN], split, hor, ver, R3(0), U_TAG, nullptr, st.f3[UUEX],
+                          ip[I_ADV_VER_ITERS]) < 0)
+    return -1;
+  for (int k = 1; k <= d.kmax; ++k)
+    for (int j = d.jmin - HALO; j <= d.jmax + HALO - 1; ++j)
+      for (int i = d.imin - HALO; i <= d.imax + HALO; ++i) {
+        fadv(i, j, k) = vv(i, j, k) / hvn(i, j, k);
+        uuadv(i, j, k) = half * (uu(i, j, k) + uu(i, j + 1, k));
+        vvadv(i, j, k) = half * (vv(i, j, k) + vv(i, j + 1, k));
+        wwadv(i, j, k) = half * (ww(i, j, k) + ww(i, j + 1, k));
+        huadv(i, j, k) = half * (hun(i, j, k) + hun(i, j + 1, k));
+        hvadv(i, j, k) = half * (ho(i, j + 1, k) + hn(i, j + 1, k));
+      }
+  AdvGrid gv = adv_grid(m, V_TAG, st.az, st.au, st.av);
+  if (do_advection_3d<R3>(d, gv, R3(st.par[P_DT]), f_.data(), ua_.data(), va_.data(), wa_.data(), hua_.data(),
+                          hva_.data(), st.f3[HVN], st.f3[HVN], split, hor, ver, R3(0), V_TAG, nullptr, st.f3[VVEX],
+                          ip[I_ADV_VER_ITERS]) < 0)
+    return -1;
+  return 0;
+}
+
+// stresses_3d.F90:50-104 (taub/taus feed the turbulence closure only)
+template <class R3>
+void stresses_3d(const Dom& d, BcState<R3>& st) {
+  double** f2 = st.f2;
+  A2 rru{d, f2[RRU]}, rrv{d, f2[RRV]}, taubx{d, f2[TAUBX]}, tauby{d, f2[TAUBY]}, taub{d, f2[TAUB]}, taus{d, f2[TAUS]},
+      tausx{d, f2[TAUSX]}, tausy{d, f2[TAUSY]};
+  A3<R3> uu{d, st.f3[UU]}, vv{d, st.f3[VV]}, hun{d, st.f3[HUN]}, hvn{d, st.f3[HVN]};
+  const double rho_0i = 1.0 / st.par[P_RHO_0];
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin - 1; i <= d.imax; ++i) taubx(i, j) = -(double)uu(i, j, 1) / (double)hun(i, j, 1) * rru(i, j);
+  for (int j = d.jmin - 1; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i) tauby(i, j) = -(double)vv(i, j, 1) / (double)hvn(i, j, 1) * rrv(i, j);
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i) {
+      double a = (double)uu(i - 1, j, 1) / (double)hun(i - 1, j, 1) * rru(i - 1, j);
+      double b = (double)uu(i, j, 1) / (double)hun(i, j, 1) * rru(i, j);
+      double c = (double)vv(i, j - 1, 1) / (double)hvn(i, j - 1, 1) * rrv(i, j - 1);
+      double e = (double)vv(i, j, 1) / (double)hvn(i, j, 1) * rrv(i, j);
+      taub(i, j) = std::sqrt(0.5 * (a * a + b * b + c * c + e * e));
+      taus(i, j) = rho_0i * std::sqrt(tausx(i, j) * tausx(i, j) + tausy(i, j) * tausy(i, j));
+    }
+}
+
+// eqstate.F90:127-137 (linear) and :252-261 (buoyancy)
+template <class R3>
+void do_eqstate(const Dom& d, BcState<R3>& st) {
+  A3<R3> rho{d, st.f3[RHO]}, buoy{d, st.f3[BUOY]}, T{d, st.f3[TT]}, S{d, st.f3[SS]};
+  const double* par = st.par;
+  const R3 rho_0 = R3(par[P_RHO_0]), dtr0 = R3(par[P_DTR0]), dsr0 = R3(par[P_DSR0]), T0 = R3(par[P_T0]),
+           S0 = R3(par[P_S0]);
+  for (int k = 1; k <= d.kmax; ++k)
+    for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
+      for (int i = d.imin - HALO; i <= d.imax + HALO; ++i)
+        rho(i, j, k) = rho_0 + dtr0 * (T(i, j, k) - T0) + dsr0 * (S(i, j, k) - S0);
+  const R3 x = R3(-par[P_G] / par[P_RHO_0]);
+  for (int k = 1; k <= d.kmax; ++k)
+    for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
+      for (int i = d.imin - HALO; i <= d.imax + HALO; ++i) buoy(i, j, k) = x * (rho(i, j, k) - rho_0);
+}
+
+// slow_bottom_friction.F90:53-170
+template <class R3>
+void slow_bottom_friction(const Dom& d, BcState<R3>& st) {
+  double** f2 = st.f2;
+  A2 Uinto{d, f2[UINTO]}, Vinto{d, f2[VINTO]}, ssuo{d, f2[SSUO]}, ssun{d, f2[SSUN]}, ssvo{d, f2[SSVO]},
+      ssvn{d, f2[SSVN]}, HU_{d, f2[HU]}, HV_{d, f2[HV]}, zub{d, f2[ZUB]}, zvb{d, f2[ZVB]}, ru{d, f2[RU]},
+      rv{d, f2[RV]};
+  M2 au{d, st.au}, av{d, st.av};
+  const double kappa = st.par[P_KAPPA], min_depth = st.par[P_MIN_DEPTH];
+  const long n = d.n2d();
+  std::vector<double> Ui_(n, 0.0), Vi_(n, 0.0), ruu_(n, 0.0), rvv_(n, 0.0);
+  A2 Ui{d, Ui_.data()}, Vi{d, Vi_.data()}, ruu{d, ruu_.data()}, rvv{d, rvv_.data()};
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i)
+      Ui(i, j) = au(i, j) >= 1 ? Uinto(i, j) / (ssuo(i, j) + HU_(i, j)) : 0.0;
+  for (int i = d.imin - HALO; i <= d.imax + HALO; ++i)
+    Ui(i, d.jmax + 1) = Uinto(i, d.jmax + 1) / (ssuo(i, d.jmax + 1) + HU_(i, d.jmax + 1));
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
+    Ui(d.imin - 1, j) = Uinto(d.imin - 1, j) / (ssuo(d.imin - 1, j) + HU_(d.imin - 1, j));
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i)
+      Vi(i, j) = av(i, j) >= 1 ? Vinto(i, j) / (ssvo(i, j) + HV_(i, j)) : 0.0;
+  for (int i = d.imin - HALO; i <= d.imax + HALO; ++i)
+    Vi(i, d.jmin - 1) = Vinto(i, d.jmin - 1) / (ssvo(i, d.jmin - 1) + HV_(i, d.jmin - 1));
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
+    Vi(d.imax + 1, j) = Vinto(d.imax + 1, j) / (ssvo(d.imax + 1, j) + HV_(d.imax + 1, j));
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i)
+      if (au(i, j) >= 1) {
+        double HHl = std::max(min_depth, ssun(i, j) + HU_(i, j));
+        ruu(i, j) = (zub(i, j) + 0.5 * HHl) / zub(i, j);
+        double x = kappa / std::log(ruu(i, j));
+        ruu(i, j) = x * x;
+      }
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i)
+      if (av(i, j) >= 1) {
+        double HHl = std::max(min_depth, ssvn(i, j) + HV_(i, j));
+        rvv(i, j) = (zvb(i, j) + 0.5 * HHl) / zvb(i, j);
+        double x = kappa / std::log(rvv(i, j));
+        rvv(i, j) = x * x;
+      }
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i) {
+      if (au(i, j) >= 1) {
+        double uloc = Ui(i, j);
+        double vloc = 0.25 * (Vi(i, j) + Vi(i + 1, j) + Vi(i, j - 1) + Vi(i + 1, j - 1));
+        ru(i, j) = ruu(i, j) * std::sqrt(uloc * uloc + vloc * vloc);
+      } else {
+        ru(i, j) = 0.0;
+      }
+    }
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i) {
+      if (av(i, j) >= 1) {
+        double uloc = 0.25 * (Ui(i, j) + Ui(i - 1, j) + Ui(i, j + 1) + Ui(i - 1, j + 1));
+        double vloc = Vi(i, j);
+        rv(i, j) = rvv(i, j) * std::sqrt(uloc * uloc + vloc * vloc);
+      } else {
+        rv(i, j) = 0.0;
+      }
+    }
+}
+
+// slow_terms.F90:57-181 (kmax > 1, kumin = kvmin = 1)
+template <class R3>
+void slow_terms(const Dom& d, BcState<R3>& st) {
+  double** f2 = st.f2;
+  A2 UEx{d, f2[UEX]}, VEx{d, f2[VEX]}, SlUx{d, f2[SLUX]}, SlVx{d, f2[SLVX]}, Slru{d, f2[SLRU]}, Slrv{d, f2[SLRV]},
+      Uint{d, f2[UINT]}, Vint{d, f2[VINT]}, ssuo{d, f2[SSUO]}, ssun{d, f2[SSUN]}, ssvo{d, f2[SSVO]}, ssvn{d, f2[SSVN]},
+      HU_{d, f2[HU]}, HV_{d, f2[HV]}, ru{d, f2[RU]}, rv{d, f2[RV]}, rru{d, f2[RRU]}, rrv{d, f2[RRV]};
+  A3<R3> uuEx{d, st.f3[UUEX]}, vvEx{d, st.f3[VVEX]}, idpdx{d, st.f3[IDPDX]}, idpdy{d, st.f3[IDPDY]}, uu{d, st.f3[UU]},
+      vv{d, st.f3[VV]}, huo{d, st.f3[HUO]}, hun{d, st.f3[HUN]}, hvo{d, st.f3[HVO]}, hvn{d, st.f3[HVN]};
+  M2 au{d, st.au}, av{d, st.av};
+  const double ip_fac = st.par[P_IP_FAC];
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i)
+      if (au(i, j) >= 1) {
+        double vs = -UEx(i, j);
+        for (int k = 1; k <= d.kmax; ++k) vs = vs + (double)uuEx(i, j, k) - ip_fac * (double)idpdx(i, j, k);
+        SlUx(i, j) = vs;
+      }
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i)
+      if (av(i, j) >= 1) {
+        double vs = -VEx(i, j);
+        for (int k = 1; k <= d.kmax; ++k) vs = vs + (double)vvEx(i, j, k) - ip_fac * (double)idpdy(i, j, k);
+        SlVx(i, j) = vs;
+      }
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i)
+      if (au(i, j) >= 1)
+        Slru(i, j) = -Uint(i, j) / (0.5 * (ssuo(i, j) + ssun(i, j)) + HU_(i, j)) * ru(i, j) +
+                     (double)uu(i, j, 1) / (0.5 * ((double)huo(i, j, 1) + (double)hun(i, j, 1))) * rru(i, j);
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i)
+      if (av(i, j) >= 1)
+        Slrv(i, j) = -Vint(i, j) / (0.5 * (ssvo(i, j) + ssvn(i, j)) + HV_(i, j)) * rv(i, j) +
+                     (double)vv(i, j, 1) / (0.5 * ((double)hvo(i, j, 1) + (double)hvn(i, j, 1))) * rrv(i, j);
+}
+
+// m3d.F90:422-636 integrate_3d for runtype 4 (see header for the configuration covered)
+template <class R3>
+int integrate_3d(const Dom& d, const AdvMasks& m, BcState<R3>& st, int n) {
+  (void)n;
+  double** f2 = st.f2;
+  int* ip = st.ipar;
+  const double* par = st.par;
+  const long n3 = d.n3d();
+  const long n2 = d.n2d();
+  start_macro(d, f2, par, ip[I_M]);
+  if (d.kmax > 1) bottom_friction_3d(d, st);
+  if (ip[I_RUNTYPE] == 4) ip_blumberg_mellor(d, st);
+  for (long q = 0; q < n3; ++q) {
+    st.f3[HUO][q] = st.f3[HUN][q];
+    st.f3[HVO][q] = st.f3[HVN][q];
+  }
+  if (ip[I_UFIRST3D]) {
+    uv_momentum_3d(d, st, 0);
+    uv_momentum_3d(d, st, 1);
+    ip[I_UFIRST3D] = 0;
+  } else {
+    uv_momentum_3d(d, st, 1);
+    uv_momentum_3d(d, st, 0);
+    ip[I_UFIRST3D] = 1;
+  }
+  sigma_coordinates(d, st);
+  if (d.kmax > 1) {
+    ww_momentum_3d(d, st);
+    if (uv_advect_3d(d, m, st) != 0) return -1;
+    stresses_3d(d, st);
+  }
+  if (ip[I_RUNTYPE] == 4) {
+    const R3 dt = R3(par[P_DT]);
+    if (ip[I_CALC_TEMP]) {
+      AdvGrid g = adv_grid(m, H_TAG, st.az, st.au, st.av);
+      if (do_advection_3d<R3>(d, g, dt, st.f3[TT], st.f3[UU], st.f3[VV], st.f3[WW], st.f3[HUN], st.f3[HVN],
+                              st.f3[HO], st.f3[HN], ip[I_TEMP_SPLIT], ip[I_TEMP_HOR], ip[I_TEMP_VER],
+                              R3(par[P_TEMP_AH]), H_TAG, nullptr, nullptr, ip[I_ADV_VER_ITERS]) < 0)
+        return -1;
+      tracer_vdiff<R3>(d, dt, R3(par[P_CNPAR]), R3(par[P_AVMOLT]), st.f3[TT], st.f3[HN], st.f3[NUH], st.az, nullptr);
+    }
+    if (ip[I_CALC_SALT]) {
+      AdvGrid g = adv_grid(m, H_TAG, st.az, st.au, st.av);
+      if (do_advection_3d<R3>(d, g, dt, st.f3[SS], st.f3[UU], st.f3[VV], st.f3[WW], st.f3[HUN], st.f3[HVN],
+                              st.f3[HO], st.f3[HN], ip[I_SALT_SPLIT], ip[I_SALT_HOR], ip[I_SALT_VER],
+                              R3(par[P_SALT_AH]), H_TAG, nullptr, nullptr, ip[I_ADV_VER_ITERS]) < 0)
+        return -1;
+      tracer_vdiff<R3>(d, dt, R3(par[P_CNPAR]), R3(par[P_AVMOLS]), st.f3[SS], st.f3[HN], st.f3[NUH], st.az, nullptr);
+    }
+    do_eqstate(d, st);
+  }
+  if (d.kmax > 1) {
+    slow_bottom_friction(d, st);
+    if (uv_advect_2d(d, m, st.az, st.au, st.av, par[P_DTM], f2[UINT], f2[VINT], f2[DUN], f2[DVN], ip[I_VEL2D_SPLIT],
+                     ip[I_VEL2D_HOR], f2[UEX], f2[VEX]) != 0)
+      return -1;
+  }
+  slow_terms(d, st);
+  // stop_macro.F90:36-39
+  for (long q = 0; q < n2; ++q) {
+    f2[UINTO][q] = f2[UINT][q];
+    f2[UINT][q] = 0.0;
+    f2[VINTO][q] = f2[VINT][q];
+    f2[VINT][q] = 0.0;
+  }
+  return 0;
+}
+
+}  // namespace gor

@@ -2,6 +2,7 @@
 // (getm_oracle.hpp) for the Python test harness (oracle/__init__.py, via ctypes).
 // Suffix _d = FP64 (the reference's REALTYPE), _f = FP32.
 #include "getm_oracle.hpp"
+#include "getm_baroclinic.hpp"
 
 extern "C" {
 
@@ -113,5 +114,108 @@ void or_build_masks(const or_dom* o, const int32_t* az, const int32_t* au, const
 
 OR_DEFINE(d, double)
 OR_DEFINE(f, float)
+
+// ---- mode-split time loop (getm_baroclinic.hpp) -------------------------------------------------
+typedef struct {
+  double* f2[gor::NF2];
+  void* f3[gor::NF3];
+  const int32_t *az, *au, *av, *ax;
+  double par[gor::NPD];
+  int ipar[gor::NPI];
+} or_bc;
+
+int or_bc_sizes(int* out) {
+  out[0] = gor::NF2;
+  out[1] = gor::NF3;
+  out[2] = gor::NPD;
+  out[3] = gor::NPI;
+  return 0;
+}
+
+extern "C++" {
+template <class R3>
+static gor::BcState<R3> to_state(or_bc* s) {
+  gor::BcState<R3> st;
+  for (int q = 0; q < gor::NF2; ++q) st.f2[q] = s->f2[q];
+  for (int q = 0; q < gor::NF3; ++q) st.f3[q] = (R3*)s->f3[q];
+  st.az = s->az; st.au = s->au; st.av = s->av; st.ax = s->ax;
+  for (int q = 0; q < gor::NPD; ++q) st.par[q] = s->par[q];
+  for (int q = 0; q < gor::NPI; ++q) st.ipar[q] = s->ipar[q];
+  return st;
+}
+}  // extern "C++"
+
+// time_loop (integration.F90:98-172): micro steps n = n0 .. n0+count-1, integrate_2d every step and
+// integrate_3d when mod(n, M) == 0. The SAVEd momentum toggles are carried in ipar.
+extern "C++" {
+template <class R3>
+static long long bc_steps(const or_dom* o, or_bc* s, int n0, int count) {
+  gor::Dom d = mk(o);
+  gor::AdvMasks m;
+  gor::build_adv_masks(d, s->az, s->au, s->av, s->ax, m);
+  gor::BcState<R3> st = to_state<R3>(s);
+  for (int n = n0; n < n0 + count; ++n) {
+    if (gor::integrate_2d(d, m, st, n) != 0) return -1;
+    if (n % st.ipar[gor::I_M] == 0)
+      if (gor::integrate_3d(d, m, st, n) != 0) return -1;
+  }
+  for (int q = 0; q < gor::NPI; ++q) s->ipar[q] = st.ipar[q];
+  return 0;
+}
+}  // extern "C++"
+
+long long or_bc_steps_d(const or_dom* o, or_bc* s, int n0, int count) { return bc_steps<double>(o, s, n0, count); }
+long long or_bc_steps_f(const or_dom* o, or_bc* s, int n0, int count) { return bc_steps<float>(o, s, n0, count); }
+
+// single routines of the step (for routine-level parity tests)
+enum {
+  BC_BOTTOM_FRICTION = 0, BC_UV_ADVECT_2D, BC_UMOMENTUM, BC_VMOMENTUM, BC_SEALEVEL, BC_DEPTH_UPDATE,
+  BC_START_MACRO, BC_BOTTOM_FRICTION_3D, BC_IP, BC_UU_MOMENTUM_3D, BC_VV_MOMENTUM_3D, BC_SIGMA, BC_WW,
+  BC_UV_ADVECT_3D, BC_STRESSES_3D, BC_EQSTATE, BC_SLOW_BOTTOM_FRICTION, BC_SLOW_TERMS, BC_INTEGRATE_2D,
+  BC_INTEGRATE_3D
+};
+
+extern "C++" {
+template <class R3>
+static int bc_call(const or_dom* o, or_bc* s, int which, int arg) {
+  gor::Dom d = mk(o);
+  gor::AdvMasks m;
+  gor::build_adv_masks(d, s->az, s->au, s->av, s->ax, m);
+  gor::BcState<R3> st = to_state<R3>(s);
+  int rc = 0;
+  switch (which) {
+    case BC_BOTTOM_FRICTION: gor::bottom_friction(d, nullptr, st.f2, st.au, st.av, st.par, st.ipar[gor::I_RUNTYPE]); break;
+    case BC_UV_ADVECT_2D:
+      rc = gor::uv_advect_2d(d, m, st.az, st.au, st.av, st.par[gor::P_DTM], st.f2[gor::U_], st.f2[gor::V_],
+                             st.f2[gor::DU], st.f2[gor::DV], st.ipar[gor::I_VEL2D_SPLIT], st.ipar[gor::I_VEL2D_HOR],
+                             st.f2[gor::UEX], st.f2[gor::VEX]);
+      break;
+    case BC_UMOMENTUM: gor::umomentum(d, st.f2, st.au, st.av, st.par); break;
+    case BC_VMOMENTUM: gor::vmomentum(d, st.f2, st.au, st.av, st.par); break;
+    case BC_SEALEVEL: gor::sealevel(d, st.f2, st.az, st.par); break;
+    case BC_DEPTH_UPDATE: gor::depth_update(d, st.f2, st.az, st.au, st.av, st.par); break;
+    case BC_START_MACRO: gor::start_macro(d, st.f2, st.par, st.ipar[gor::I_M]); break;
+    case BC_BOTTOM_FRICTION_3D: gor::bottom_friction_3d(d, st); break;
+    case BC_IP: gor::ip_blumberg_mellor(d, st); break;
+    case BC_UU_MOMENTUM_3D: gor::uv_momentum_3d(d, st, 0); break;
+    case BC_VV_MOMENTUM_3D: gor::uv_momentum_3d(d, st, 1); break;
+    case BC_SIGMA: gor::sigma_coordinates(d, st); break;
+    case BC_WW: gor::ww_momentum_3d(d, st); break;
+    case BC_UV_ADVECT_3D: rc = gor::uv_advect_3d(d, m, st); break;
+    case BC_STRESSES_3D: gor::stresses_3d(d, st); break;
+    case BC_EQSTATE: gor::do_eqstate(d, st); break;
+    case BC_SLOW_BOTTOM_FRICTION: gor::slow_bottom_friction(d, st); break;
+    case BC_SLOW_TERMS: gor::slow_terms(d, st); break;
+    case BC_INTEGRATE_2D: rc = gor::integrate_2d(d, m, st, arg); break;
+    case BC_INTEGRATE_3D: rc = gor::integrate_3d(d, m, st, arg); break;
+    default: return -2;
+  }
+  for (int q = 0; q < gor::NPI; ++q) s->ipar[q] = st.ipar[q];
+  return rc;
+}
+}  // extern "C++"
+
+int or_bc_call_d(const or_dom* o, or_bc* s, int which, int arg) { return bc_call<double>(o, s, which, arg); }
+int or_bc_call_f(const or_dom* o, or_bc* s, int which, int arg) { return bc_call<float>(o, s, which, arg); }
 
 }  // extern "C"

@@ -339,8 +339,17 @@ INTRINSICS = {
     "abs": "_abs", "min": "_fmin", "max": "_fmax", "ceiling": "_ceiling", "floor": "_floor", "maxval": "_maxval",
     "minval": "_minval", "sum": "_sum", "real": "_real", "dble": "_real", "int": "_int", "mod": "_mod",
     "sign": "_sign", "exp": "_exp", "sqrt": "_sqrt", "present": "_present", "tanh": "np.tanh", "sin": "np.sin",
-    "cos": "np.cos", "log": "np.log", "selected_real_kind": "_srk",
+    "cos": "np.cos", "log": "np.log", "selected_real_kind": "_srk", "allocated": "_allocated", "float": "_real",
+    "huge": "_huge",
 }
+
+
+def _allocated(x):
+    return x is not None
+
+
+def _huge(x):
+    return np.finfo(np.float64).max
 
 
 def _srk(*a):
@@ -849,9 +858,24 @@ def _parse_use(low: str):
 class Gen:
     def __init__(self, unit: Unit, module_arrays=(), module_derived=(), funcs=(), modvars=()):
         self.u = unit
-        self.modvars = set(modvars) - set(unit.decls) - set(unit.args)
+        self.modvars = set(modvars) - set(unit.decls) - set(unit.args) - {unit.name, unit.result}
         arrays = set(module_arrays)
         derived = set(module_derived)
+        # names that the body allocates or assigns element-wise are arrays even when their
+        # declaration lives in a module this translator has only as a namespace
+        for s in unit.body:
+            low = s.lower()
+            m = re.match(r"^allocate\s*\((.*)\)$", low)
+            if m:
+                for item in _split_top(m.group(1), ","):
+                    item = item.strip()
+                    if "(" in item and "%" not in item.split("(")[0]:
+                        arrays.add(item[:item.index("(")].strip())
+                continue
+            m = re.match(r"^(\w+)\s*\(", low)
+            if m and m.group(1) not in ("if", "call", "do", "select", "case", "allocate", "deallocate", "write",
+                                        "print", "where", "elseif") and _top_assign(low) is not None:
+                arrays.add(m.group(1))
         for d in unit.decls.values():
             if d.is_array:
                 arrays.add(d.name)
@@ -861,8 +885,14 @@ class Gen:
         self.lines = []
         self.ind = 1
         self.sel = 0
+        self.saved = []
 
     def emit(self, s):
+        if self.lines and self.lines[-1].rstrip().endswith(":"):
+            prev = self.lines[-1]
+            prev_ind = len(prev) - len(prev.lstrip(" "))
+            if 4 * self.ind <= prev_ind:  # empty block (e.g. 'case (2) ! z-level')
+                self.lines.append(" " * (prev_ind + 4) + "pass")
         self.lines.append("    " * self.ind + s)
 
     def gen(self) -> str:
@@ -895,19 +925,36 @@ class Gen:
             if d.kind == "derived":
                 self.emit(f"{pyname(name)} = None")
                 continue
+            saved = "save" in d.attrs or d.init is not None  # explicit SAVE or implicit (initialiser)
+            if saved:
+                self.saved.append(name)
             if d.is_array:
                 b = dim_bounds(d.dims, self.scope)
                 if b is None or "allocatable" in d.attrs or "pointer" in d.attrs:
-                    self.emit(f"{pyname(name)} = None")
+                    init = "None"
                 else:
-                    self.emit(f"{pyname(name)} = _alloc({b}, {kind!r})")
+                    init = f"_alloc({b}, {kind!r})"
             else:
                 init = tr_expr(d.init, self.scope) if d.init else {"real": "np.float64(0)", "integer": "0",
                                                                    "logical": "False"}.get(kind, "None")
+            if saved:
+                self.emit(f"{pyname(name)} = _SV[{name!r}] if {name!r} in _SV else {init}")
+            else:
                 self.emit(f"{pyname(name)} = {init}")
+        if self.saved:
+            # SAVEd locals persist across calls (written back on every exit)
+            self.emit("try:")
+            self.ind += 1
         for s in u.body:
             self.stmt(s)
         self.emit("return _result")
+        if self.saved:
+            self.ind -= 1
+            self.emit("finally:")
+            self.ind += 1
+            for name in self.saved:
+                self.emit(f"_SV[{name!r}] = {pyname(name)}")
+            self.ind -= 1
         return "\n".join(self.lines)
 
     def stmt(self, s: str):
@@ -1170,6 +1217,46 @@ class Program:
         self.procs = {}       # external procedures
         self.sources = {}
 
+    def visible(self, mname, _seen=None):
+        """Names a `use mname` makes visible: the module's own entities and, transitively, those of
+        the modules it uses (use-association re-exports them unless private)."""
+        seen = _seen if _seen is not None else set()
+        if mname in seen:
+            return {}
+        seen.add(mname)
+        out = {}
+        mu = self.mod_units.get(mname)
+        if mu is not None:
+            for sub, only in mu.uses:
+                for k, v in self.visible(sub, set(seen)).items():
+                    if only is None or k in only:
+                        out[k] = v
+        mns = self.modules.get(mname)
+        if mns is not None:
+            out.update(vars(mns))
+        return out
+
+    def visible_owner(self, mname, _seen=None):
+        """Like visible(), mapping each name to the module whose namespace holds it."""
+        seen = _seen if _seen is not None else set()
+        if mname in seen:
+            return {}
+        seen.add(mname)
+        out = {}
+        mu = self.mod_units.get(mname)
+        if mu is not None:
+            for sub, only in mu.uses:
+                for k, o in self.visible_owner(sub, set(seen)).items():
+                    if only is None or k in only:
+                        out[k] = o
+            for k in mu.decls:
+                out[k] = mname
+        mns = self.modules.get(mname)
+        if mns is not None:
+            for k in vars(mns):
+                out[k] = mname
+        return out
+
     def add_module_namespace(self, name, **values):
         ns = self.modules.setdefault(name, types.SimpleNamespace())
         for k, v in values.items():
@@ -1213,15 +1300,14 @@ class Program:
             mu = self.mod_units.get(mname)
             if mu is not None:
                 sources.append((mu, only))
-            ns = self.modules.get(mname)
-            if ns is not None:
-                for k, v in vars(ns).items():
-                    if only is None or k in only:
-                        if isinstance(v, FArr) or (v is None and mu is not None and mu.decls.get(k) and
-                                                   mu.decls[k].is_array):
-                            arrays.add(k)
-                        if isinstance(v, types.SimpleNamespace):
-                            derived.add(k)
+            for k, v in self.visible(mname).items():
+                if only is None or k in only:
+                    declared_array = any(m.decls.get(k) is not None and m.decls[k].is_array
+                                         for m in self.mod_units.values())
+                    if isinstance(v, FArr) or (v is None and declared_array):
+                        arrays.add(k)
+                    if isinstance(v, types.SimpleNamespace):
+                        derived.add(k)
         for mu, only in sources:
             for k, d in mu.decls.items():
                 if only is None or k in only:
@@ -1236,52 +1322,43 @@ class Program:
         return g
 
     def _compile(self, unit: Unit, mod: Unit | None, ns):
-        arrays, derived = self._module_arrays(unit, mod)
-        owner = {}
-        uses = ([(mod.name, None)] + list(mod.uses) if mod else []) + list(unit.uses)
-        for mname, only in uses:
-            mns = self.modules.get(mname)
-            mu = self.mod_units.get(mname)
-            names = set(vars(mns)) if mns is not None else set()
-            if mu is not None:
-                names |= set(mu.decls)
-            for k in names:
-                if only is None or k in only:
-                    owner.setdefault(k, mname)
-        # names declared locally shadow module arrays
-        for k, d in unit.decls.items():
-            if not d.is_array and k in arrays:
-                arrays.discard(k)
-        gen = Gen(unit, arrays, derived, modvars=owner.keys())
-        try:
-            src = gen.gen()
-        except SyntaxError as ex:
-            # routines outside the supported subset (namelist / netCDF I/O, ...) fail only if called
-            msg = f"{unit.name}: not translatable ({ex})"
-
-            def unsupported(*a, **k):
-                raise NotImplementedError(msg)
-
-            unsupported.__name__ = unit.name
-            if mod is not None:
-                setattr(ns, unit.name, unsupported)
-            self.procs.setdefault(unit.name, unsupported)
-            return
-        self.sources[unit.name] = src
-        modname = mod.name if mod else None
         prog = self
+        modname = mod.name if mod else None
+        saved_store = {}  # SAVEd locals of this procedure
+        cache = {}
+
+        def translate():
+            # translated on first call, once every file of the program is loaded
+            arrays, derived = prog._module_arrays(unit, mod)
+            owner = {}
+            uses = ([(mod.name, None)] + list(mod.uses) if mod else []) + list(unit.uses)
+            for mname, only in uses:
+                for k, o in prog.visible_owner(mname).items():
+                    if only is None or k in only:
+                        owner.setdefault(k, o)
+            for k, d in unit.decls.items():  # names declared locally shadow module arrays
+                if not d.is_array and k in arrays:
+                    arrays.discard(k)
+            gen = Gen(unit, arrays, derived, modvars=owner.keys())
+            try:
+                src = gen.gen()
+            except SyntaxError as ex:
+                # routines outside the supported subset (namelist / netCDF I/O, ...) fail only if called
+                raise NotImplementedError(f"{unit.name}: not translatable ({ex})")
+            prog.sources[unit.name] = src
+            cache.update(src=src, gen=gen, owner=owner, code=compile(src, f"<{unit.name}>", "exec"))
 
         def runner(*args, **kw):
+            if not cache:
+                translate()
+            gen, owner = cache["gen"], cache["owner"]
             g = prog._globals(unit, ns)
             # resolve module names at call time (use-association)
             uses = list(unit.uses)
             if mod is not None:
                 uses = [(mod.name, None)] + list(mod.uses) + uses
             for mname, only in uses:
-                mns = prog.modules.get(mname)
-                if mns is None:
-                    continue
-                for k, v in vars(mns).items():
+                for k, v in prog.visible(mname).items():
                     if only is None or k in only:
                         g[k] = v
             for k, v in prog.procs.items():
@@ -1289,11 +1366,10 @@ class Program:
             if modname:
                 for k, v in vars(prog.modules[modname]).items():
                     g.setdefault(k, v)
-            code = compile(src, f"<{unit.name}>", "exec")
+            g["_SV"] = saved_store
             loc = {}
-            exec(code, g, loc)
+            exec(cache["code"], g, loc)
             fn = loc[unit.name]
-            fn.__globals__.update(g)
             try:
                 return fn(*args, **kw)
             finally:

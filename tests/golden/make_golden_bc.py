@@ -1,0 +1,204 @@
+"""Generates tests/golden/reference_mode_split.npz: the reference's own integrate_2d / integrate_3d
+(the mode-split time loop, integration.F90:98-172) executed from source (fortran_subset.py) on a
+small closed basin, together with the inputs. The oracle and the CUDA path are compared with it
+bit for bit (tests/test_golden_bc_cpu.py, tests/test_gpu_golden_bc.py).
+
+    python tests/golden/make_golden_bc.py
+
+Configuration: runtype 4 (prognostic T and S), sigma coordinates (equidistant), linear equation of
+state, Blumberg-Mellor internal pressure, P2_PDM / HALFSPLIT advection of momentum (2D and 3D) and
+tracers, closed boundaries, num/nuh prescribed (the turbulence closure -- the un-vendored GOTM -- is
+replaced by a routine that leaves them unchanged; ss_nn, whose outputs only feed it, likewise),
+no wind, air pressure, freshwater or short-wave forcing.
+"""
+from __future__ import annotations
+
+import os
+import sys
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, HERE)
+sys.path.insert(0, ROOT)
+
+import fortran_subset as fs  # noqa: E402
+from code_b200 import state as S  # noqa: E402
+
+FILES = [
+    "src/futils/tridiagonal.F90", "src/2d/advection.F90", "src/2d/adv_split_u.F90", "src/2d/adv_split_v.F90",
+    "src/3d/advection_3d.F90", "src/3d/adv_split_w.F90",
+    "src/2d/bottom_friction.F90", "src/2d/uv_advect.F90", "src/2d/uv_diffusion.F90", "src/2d/momentum.F90",
+    "src/2d/sealevel.F90", "src/2d/depth_update.F90", "src/domain/mirror_bdy_2d.F90", "src/domain/mirror_bdy_3d.F90",
+    "src/3d/start_macro.F90", "src/3d/stop_macro.F90", "src/3d/bottom_friction_3d.F90",
+    "src/3d/internal_pressure.F90", "src/3d/ip_blumberg_mellor.F90", "src/3d/uu_momentum_3d.F90",
+    "src/3d/vv_momentum_3d.F90", "src/3d/coordinates.F90", "src/3d/sigma_coordinates.F90",
+    "src/3d/ww_momentum_3d.F90", "src/3d/uv_advect_3d.F90", "src/3d/uv_diffusion_3d.F90", "src/3d/stresses_3d.F90",
+    "src/3d/temperature.F90", "src/3d/salinity.F90", "src/3d/eqstate.F90", "src/3d/slow_bottom_friction.F90",
+    "src/3d/slow_terms.F90", "src/2d/m2d.F90", "src/3d/m3d.F90",
+]
+
+
+class RefBc:
+    def __init__(self, c: S.BcCase):
+        self.c = c
+        g = self.g = c.grid
+        P = self.P = fs.Program()
+        F2, F3 = self.F2, self.F3
+        f2 = {k.lower(): F2(v) for k, v in c.f2.items()}
+        f3 = {k.lower(): F3(v) for k, v in c.f3.items()}
+        self.f2, self.f3 = f2, f3
+        zero2 = lambda: F2(np.zeros(g.shape2()))  # noqa: E731
+        zero3 = lambda: F3(np.zeros(g.shape3()))  # noqa: E731
+        pd, pi = c.pd, c.pi
+        P.add_module_namespace("parameters", g=pd["g"], rho_0=pd["rho_0"], cp=fs._real_literal and np.float64(np.float32(3985.)),
+                               kappa=pd["kappa"], avmmol=pd["avmmol"], avmolt=pd["avmolt"], avmols=pd["avmols"])
+        P.add_module_namespace(
+            "domain", imin=g.imin, imax=g.imax, jmin=g.jmin, jmax=g.jmax, kmax=g.kmax, ioff=0, joff=0, dx=g.dx,
+            dy=g.dy, ard1=g.ard1, az=F2(c.az), au=F2(c.au), av=F2(c.av), ax=F2(c.ax), h=f2["h"], hu=f2["hu"],
+            hv=f2["hv"], min_depth=pd["min_depth"], crit_depth=pd["crit_depth"], dry_z=f2["dry_z"],
+            dry_u=f2["dry_u"], dry_v=f2["dry_v"], cori=zero2(), coru=f2["coru"], corv=f2["corv"],
+            ga=None, ddu=np.float64(0.0), ddl=np.float64(0.0), vert_cord=1, openbdy=False, have_boundaries=False,
+            nwb=0, nnb=0, neb=0, nsb=0, maxdepth=np.float64(0.0), z0_method=0, z0_const=np.float64(0.01), z0=zero2(),
+            ill=g.imin, ihl=g.imax, jll=g.jmin, jhl=g.jmax, ilg=g.imin, ihg=g.imax, jlg=g.jmin, jhg=g.jmax)
+        v2 = {k: f2[k] for k in ("z", "zo", "u", "v", "d", "du", "dv", "uex", "vex", "fu", "fv", "ru", "rv", "ruu",
+                                 "rvv", "uint", "vint", "uinto", "vinto", "slux", "slvx", "slru", "slrv", "zub",
+                                 "zvb", "zub0", "zvb0", "fwf")}
+        v2["fwf_int"] = zero2()
+        P.add_module_namespace("variables_2d", **v2)
+        v3 = {k: f3[k] for k in ("uu", "vv", "ww", "ho", "hn", "huo", "hun", "hvo", "hvn", "uuex", "vvex", "idpdx",
+                                 "idpdy", "t", "s", "rho", "buoy", "num", "nuh")}
+        v3["s"] = f3["s"]
+        for k in ("sseo", "ssen", "ssuo", "ssun", "ssvo", "ssvn", "dn", "dun", "dvn", "rru", "rrv", "taubx", "tauby",
+                  "taub", "taus"):
+            v3[k] = f2[k]
+        ones2 = F2(np.ones(g.shape2()))
+        v3.update(dt=np.float64(pd["dt"]), cnpar=np.float64(pd["cnpar"]), kmin=F2(np.ones(g.shape2())),
+                  kumin=F2(np.ones(g.shape2())), kvmin=F2(np.ones(g.shape2())), ss=zero3(), nn=zero3(), zc=zero3(),
+                  rad=zero3(), a=ones2, g1=ones2, g2=ones2, alpha=zero3(), beta=zero3(), rk=None,
+                  do_numerical_analyses=False, nummix3d_s=None, nummix2d_s=None, phymix3d_s=None,
+                  phymix2d_s=None, nummix3d_t=None, nummix2d_t=None, phymix3d_t=None, phymix2d_t=None,
+                  numdis3d=None, numdis2d=None, light=None, tke=zero3(), eps=zero3())
+        for k in ("kmin", "kumin", "kvmin"):
+            v3[k].a = v3[k].a.astype(np.int64)
+        for v in (v2, v3):  # variables_2d/3d re-export the domain's index bounds (use domain)
+            v.update(imin=g.imin, imax=g.imax, jmin=g.jmin, jmax=g.jmax, kmax=g.kmax)
+        P.add_module_namespace("variables_2d", **v2)
+        P.add_module_namespace("variables_3d", **v3)
+        P.add_module_namespace("meteo", tausx=f2["tausx"], tausy=f2["tausy"], airp=f2["airp"], swr=zero2(),
+                               shf=zero2(), albedo=zero2())
+        P.add_module_namespace("halo_zones", h_tag=10, hu_tag=11, hv_tag=12, d_tag=20, du_tag=21, dv_tag=22,
+                               z_tag=30, u_tag=31, v_tag=32, update_2d_halo=lambda *a, **k: None,
+                               update_3d_halo=lambda *a, **k: None, wait_halo=lambda *a, **k: None)
+        timers = {f"tim_{n}": q for q, n in enumerate(
+            "adv advh adv3d adv3dh salt temp mixanalysis bottfrict integr2d uvadv uvadvh uvdiff momentum momentumh "
+            "sealevel sealevelh dpthupdate startmcr stopmcr bottfrict3d intpress uumomentum uumomentumh vvmomentum "
+            "vvmomentumh coords wwmomentum wwmomentumh uvadv3d uvadv3dh uvdiff3d stresses3d stresses3dh tempH saltH "
+            "eqstate slowbfrict slowterms integr3d check3df temph salth".split())}
+        P.add_module_namespace("getm_timers", tic=lambda *a: None, toc=lambda *a: None, **timers)
+        P.add_module_namespace("bdy_3d", do_bdy_3d=lambda *a, **k: None, init_bdy_3d=lambda *a, **k: None,
+                               bdy3d_tmrlx=False, bdy3d_tmrlx_ucut=0.0, bdy3d_tmrlx_max=0.0, bdy3d_tmrlx_min=0.0)
+        P.add_module_namespace("exceptions", getm_error=self._error)
+        P.add_module_namespace("time", julianday=0, secondsofday=0, month=1, yearday=1)
+        for f in FILES:
+            P.load(f)
+        # prescribed viscosity: the turbulence interface and its shear/stratification inputs are inert
+        P.procs["gotm"] = lambda *a, **k: None
+        P.procs["ss_nn"] = lambda *a, **k: None
+        P.procs["tke_eps_advect_3d"] = lambda *a, **k: None
+        P.procs["do_residual"] = lambda *a, **k: None
+        P.procs["update_2d_bdy"] = lambda *a, **k: None
+        P.procs["check_3d_fields"] = lambda *a, **k: None
+        m2 = P.modules["m2d"]
+        m2.dtm = np.float64(pd["dtm"])
+        m2.mm = pi["MM"]
+        m2.vel2d_adv_split, m2.vel2d_adv_hor = pi["vel2d_adv_split"], pi["vel2d_adv_hor"]
+        m2.am, m2.an_method, m2.residual, m2.sealevel_check, m2.bdy2d_ramp = np.float64(-1.0), 0, -1, 0, -1
+        m3 = P.modules["m3d"]
+        m3.m = pi["M"]
+        m3.vel3d_adv_split, m3.vel3d_adv_hor, m3.vel3d_adv_ver = (pi["vel3d_adv_split"], pi["vel3d_adv_hor"],
+                                                                  pi["vel3d_adv_ver"])
+        m3.calc_temp, m3.calc_salt, m3.bdy3d, m3.advect_turbulence = True, True, False, False
+        m3.ip_fac, m3.ip_ramp, m3.vel_check = np.float64(pd["ip_fac"]), -1, 0
+        m3.vert_cord = 1
+        tm = P.modules["temperature"]
+        tm.temp_adv_split, tm.temp_adv_hor, tm.temp_adv_ver = (pi["temp_adv_split"], pi["temp_adv_hor"],
+                                                               pi["temp_adv_ver"])
+        tm.temp_ah, tm.temp_check, tm.ncid = np.float64(pd["temp_AH"]), 0, -1
+        sm = P.modules["salinity"]
+        sm.salt_adv_split, sm.salt_adv_hor, sm.salt_adv_ver = (pi["salt_adv_split"], pi["salt_adv_hor"],
+                                                               pi["salt_adv_ver"])
+        sm.salt_ah, sm.salt_check = np.float64(pd["salt_AH"]), 0
+        eq = P.modules["eqstate"]
+        eq.eqstate_method = 1
+        eq.t0, eq.s0, eq.dtr0, eq.dsr0 = (np.float64(pd["T0"]), np.float64(pd["S0"]), np.float64(pd["dtr0"]),
+                                          np.float64(pd["dsr0"]))
+        ipm = P.modules["internal_pressure"]
+        ipm.ip_method = 1
+        ipm.zz = zero3()
+        P.modules["advection"].init_advection()
+        # sigma coordinates' first call sets the SAVEd equidistant switch and ga (coordinates.F90)
+        P.procs["sigma_coordinates"](True)
+
+    def _error(self, where, msg):
+        raise fs.FortranStop(f"{where}: {msg}")
+
+    def F2(self, a):
+        g = self.g
+        return fs.FArr(np.asfortranarray(np.asarray(a).T.copy()), [g.imin - 2, g.jmin - 2])
+
+    def F3(self, a):
+        g = self.g
+        return fs.FArr(np.asfortranarray(np.transpose(np.asarray(a, np.float64), (2, 1, 0)).copy()),
+                       [g.imin - 2, g.jmin - 2, 0])
+
+    @staticmethod
+    def N(fa):
+        a = fa.a
+        return np.ascontiguousarray(a.T if a.ndim == 2 else np.transpose(a, (2, 1, 0)))
+
+    def time_loop(self, n0, count, runtype=4):
+        tz = self.f2
+        m2 = self.P.modules["m2d"]
+        m3 = self.P.modules["m3d"]
+        zeros = self.F2(np.zeros(self.g.shape2()))
+        for n in range(n0, n0 + count):
+            m2.integrate_2d(runtype, n, self.f2["tausx"], self.f2["tausy"], self.f2["airp"])
+            if n % m3.m == 0:
+                m3.integrate_3d(runtype, n)
+        del tz, zeros
+
+    def state(self):
+        out = {}
+        for k in S.F2_NAMES:
+            out["f2_" + k] = self.N(self.f2[k.lower()])
+        for k in S.F3_NAMES:
+            out["f3_" + k] = self.N(self.f3[k.lower()])
+        return out
+
+
+def main():
+    c = S.baroclinic_case(nx=12, ny=10, kmax=4, recipe="shelf", M=4, dt3=60.0, seed=3)
+    out = {"meta": np.array([c.grid.nx, c.grid.ny, c.grid.kmax, c.grid.dx, c.grid.dy])}
+    for k, v in c.f2.items():
+        out["in_f2_" + k] = v
+    for k, v in c.f3.items():
+        out["in_f3_" + k] = v
+    for k, v in zip(("az", "au", "av", "ax"), c.masks()):
+        out["in_" + k] = v
+    out["in_pd"] = np.array([c.pd[n] for n in S.PD_NAMES])
+    out["in_pi"] = np.array([c.pi[n] for n in S.PI_NAMES])
+    r = RefBc(c)
+    # two macro steps (M = 4 micro steps each)
+    r.time_loop(1, 8)
+    for k, v in r.state().items():
+        out["out_" + k] = v
+    path = os.path.join(HERE, "reference_mode_split.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path} ({os.path.getsize(path) / 1024:.0f} KiB)")
+
+
+if __name__ == "__main__":
+    main()
