@@ -26,6 +26,7 @@ UNITS = {
     "kernels_f64.cu": ["--fmad=false"],
     "kernels_f32.cu": ["--fmad=true"],
     "ctx.cu": [],
+    "bc.cu": ["--fmad=false"],
 }
 
 

@@ -1,0 +1,617 @@
+// bc.cu -- the mode-split time step on the device: 2D (barotropic) kernels, the drivers of
+// integrate_2d / integrate_3d / the micro-step loop, and their C-ABI entry points.
+// Built with --fmad=false: the FP64 arithmetic rounds exactly as written (as in the reference).
+#include "bc_common.cuh"
+#include "ctx_internal.h"
+
+namespace gb {
+
+#define GB_IJ2                                                          \
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + d.imin - HALO; \
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + d.jmin - HALO; \
+  if (i > d.imax + HALO || j > d.jmax + HALO) return;
+
+struct W2 {
+  const Dev& d;
+  double* p;
+  __device__ double& operator()(int i, int j) const { return p[d.ix(i, j)]; }
+};
+struct M2 {
+  const Dev& d;
+  const int32_t* p;
+  __device__ int operator()(int i, int j) const { return p[d.ix(i, j)]; }
+};
+__device__ __forceinline__ bool interior(const Dev& d, int i, int j) {
+  return i >= d.imin && i <= d.imax && j >= d.jmin && j <= d.jmax;
+}
+
+// bottom_friction.F90:48-150: ru/rv from the depth-averaged velocities (log-law drag).
+__global__ void k_bottom_friction(Dev d, Bc2 s, int runtype) {
+  GB_IJ2
+  W2 U{d, s.f2[U_]}, V{d, s.f2[V_]}, DU_{d, s.f2[DU]}, DV_{d, s.f2[DV]}, ruu{d, s.f2[RUU]}, rvv{d, s.f2[RVV]},
+      ru{d, s.f2[RU]}, rv{d, s.f2[RV]}, zub{d, s.f2[ZUB]}, zvb{d, s.f2[ZVB]}, zub0{d, s.f2[ZUB0]}, zvb0{d, s.f2[ZVB0]};
+  M2 au{d, s.au}, av{d, s.av};
+  const double kappa = s.par[P_KAPPA], avmmol = s.par[P_AVMMOL], min_depth = s.par[P_MIN_DEPTH];
+  const bool in = interior(d, i, j);
+  if (i <= d.imax + HALO - 1 && au(i, j) > 0) {
+    // vloc: 4-point average on interior U points (0 elsewhere, as the reference's work array holds)
+    const double vloc = in ? 0.25 * (V(i, j) / DV_(i, j) + V(i + 1, j) / DV_(i + 1, j) + V(i, j - 1) / DV_(i, j - 1) +
+                                     V(i + 1, j - 1) / DV_(i + 1, j - 1))
+                           : 0.0;
+    const double uloc = U(i, j) / DU_(i, j);
+    const double HHl = fmax(min_depth, DU_(i, j));
+    double x = kappa / log((zub(i, j) + 0.5 * HHl) / zub(i, j));
+    double r = x * x;
+    if (runtype == 1) {
+      const double fricvel = sqrt(r * (uloc * uloc + vloc * vloc));
+      zub(i, j) = fmin(HHl, zub0(i, j) + 0.1 * avmmol / fmax(avmmol, fricvel));
+      r = (zub(i, j) + 0.5 * HHl) / zub(i, j);
+      x = kappa / log(r);
+      r = x * x;
+    }
+    ruu(i, j) = r;
+    ru(i, j) = r * sqrt(uloc * uloc + vloc * vloc);
+  }
+  if (j <= d.jmax + HALO - 1 && av(i, j) > 0) {
+    // uloc: 4-point average on interior V points; elsewhere the U-point quotient where au > 0
+    double uloc;
+    if (in)
+      uloc = 0.25 * (U(i, j) / DU_(i, j) + U(i - 1, j) / DU_(i - 1, j) + U(i, j + 1) / DU_(i, j + 1) +
+                     U(i - 1, j + 1) / DU_(i - 1, j + 1));
+    else
+      uloc = (i <= d.imax + HALO - 1 && au(i, j) > 0) ? U(i, j) / DU_(i, j) : 0.0;
+    const double vloc = V(i, j) / DV_(i, j);
+    const double HHl = fmax(min_depth, DV_(i, j));
+    double x = kappa / log((zvb(i, j) + 0.5 * HHl) / zvb(i, j));
+    double r = x * x;
+    if (runtype == 1) {
+      const double fricvel = sqrt(r * (uloc * uloc + vloc * vloc));
+      zvb(i, j) = fmin(HHl, zvb0(i, j) + 0.1 * avmmol / fmax(avmmol, fricvel));
+      r = (zvb(i, j) + 0.5 * HHl) / zvb(i, j);
+      x = kappa / log(r);
+      r = x * x;
+    }
+    rvv(i, j) = r;
+    rv(i, j) = r * sqrt(uloc * uloc + vloc * vloc);
+  }
+}
+
+// uv_advect.F90:94-110 (U grid) / :204-220 (V grid): quantities of the 2D momentum volumes.
+template <int DIR>
+__global__ void k_uvadv2d_prep(Dev d, const double* Up, const double* Vp, const double* DUp, const double* DVp,
+                               double* fadvp, double* Uadvp, double* Vadvp, double* DUadvp, double* DVadvp) {
+  GB_IJ2
+  W2 U{d, const_cast<double*>(Up)}, V{d, const_cast<double*>(Vp)}, DU_{d, const_cast<double*>(DUp)},
+      DV_{d, const_cast<double*>(DVp)}, fadv{d, fadvp}, Uadv{d, Uadvp}, Vadv{d, Vadvp}, DUadv{d, DUadvp},
+      DVadv{d, DVadvp};
+  if (DIR == 0) {
+    if (i > d.imax + HALO - 1) return;
+    fadv(i, j) = U(i, j) / DU_(i, j);
+    Uadv(i, j) = 0.5 * (U(i, j) + U(i + 1, j));
+    Vadv(i, j) = 0.5 * (V(i, j) + V(i + 1, j));
+    DUadv(i, j) = 0.5 * (DU_(i, j) + DU_(i + 1, j));
+    DVadv(i, j) = 0.5 * (DV_(i, j) + DV_(i + 1, j));
+  } else {
+    if (j > d.jmax + HALO - 1) return;
+    fadv(i, j) = V(i, j) / DV_(i, j);
+    Uadv(i, j) = 0.5 * (U(i, j) + U(i, j + 1));
+    Vadv(i, j) = 0.5 * (V(i, j) + V(i, j + 1));
+    DUadv(i, j) = 0.5 * (DU_(i, j) + DU_(i, j + 1));
+    DVadv(i, j) = 0.5 * (DV_(i, j) + DV_(i, j + 1));
+  }
+}
+
+// NOSPLIT finaliser of the 2D driver (advection.F90:500-507)
+__global__ void k_finalise2d(Dev d, double dt, double* f, const double* Do, const double* adv, const double* Di,
+                             const uint8_t* mfin) {
+  GB_IJ2
+  const long long c = d.ix(i, j);
+  if (mfin[c]) f[c] = (Do[c] * f[c] - dt * adv[c]) / Di[c];
+}
+
+// momentum.F90:157-174 (umomentum, DIR 0) / :319-336 (vmomentum, DIR 1): depth-integrated
+// transport update on U (V) points of the interior.
+template <int DIR>
+__global__ void k_momentum(Dev d, Bc2 s) {
+  GB_IJ2
+  if (!interior(d, i, j)) return;
+  M2 mask{d, DIR == 0 ? s.au : s.av};
+  if (!(mask(i, j) == 1 || mask(i, j) == 2)) return;
+  W2 X{d, s.f2[DIR == 0 ? U_ : V_]}, DX{d, s.f2[DIR == 0 ? DU : DV]}, z{d, s.f2[Z]}, H{d, s.f2[HH]}, D{d, s.f2[D_]},
+      airp{d, s.f2[AIRP]}, taus{d, s.f2[DIR == 0 ? TAUSX : TAUSY]}, Slr_{d, s.f2[DIR == 0 ? SLRU : SLRV]},
+      dry{d, s.f2[DIR == 0 ? DRY_U : DRY_V]}, fC{d, s.f2[DIR == 0 ? FV : FU]}, Ex{d, s.f2[DIR == 0 ? UEX : VEX]},
+      Slx{d, s.f2[DIR == 0 ? SLUX : SLVX]}, r{d, s.f2[DIR == 0 ? RU : RV]};
+  const double g = s.par[P_G], rho_0 = s.par[P_RHO_0], dtm = s.par[P_DTM], min_depth = s.par[P_MIN_DEPTH];
+  const double gamma = rho_0 * g;
+  const double gammai = 1.0 / gamma;
+  const int di = DIR == 0 ? 1 : 0, dj = DIR == 0 ? 0 : 1;
+  const double zp = fmax(z(i + di, j + dj), -H(i, j) + fmin(min_depth, D(i + di, j + dj)));
+  const double zm = fmax(z(i, j), -H(i + di, j + dj) + fmin(min_depth, D(i, j)));
+  const double zx = (zp - zm + (airp(i + di, j + dj) - airp(i, j)) * gammai) / (DIR == 0 ? d.dx : d.dy);
+  const double tau = 0.5 * (taus(i, j) + taus(i + di, j + dj));
+  const double Slr = X(i, j) > 0.0 ? fmax(Slr_(i, j), 0.0) : fmin(Slr_(i, j), 0.0);
+  if (DIR == 0)
+    X(i, j) = (X(i, j) - dtm * (g * DX(i, j) * zx + dry(i, j) * (-tau / rho_0 - fC(i, j) + Ex(i, j) + Slx(i, j) + Slr))) /
+              (1.0 + dtm * r(i, j) / DX(i, j));
+  else
+    X(i, j) = (X(i, j) - dtm * (g * DX(i, j) * zx + dry(i, j) * (-tau / rho_0 + fC(i, j) + Ex(i, j) + Slx(i, j) + Slr))) /
+              (1.0 + dtm * r(i, j) / DX(i, j));
+}
+
+// momentum.F90:193-216 / :356-379: Coriolis terms fU (after the U update) and fV (after V).
+template <int DIR>
+__global__ void k_coriolis(Dev d, Bc2 s) {
+  GB_IJ2
+  if (!interior(d, i, j)) return;
+  if (DIR == 0) {  // fU on V points from the new U
+    W2 U{d, s.f2[U_]}, fU{d, s.f2[FU]}, corv{d, s.f2[CORV]};
+    M2 av{d, s.av};
+    if (av(i, j) >= 1) {
+      const double Uloc = 0.25 * (U(i - 1, j) + U(i, j) + U(i - 1, j + 1) + U(i, j + 1));
+      fU(i, j) = corv(i, j) * Uloc;
+    } else {
+      fU(i, j) = 0.0;
+    }
+  } else {  // fV on U points from the new V
+    W2 V{d, s.f2[V_]}, fV{d, s.f2[FV]}, coru{d, s.f2[CORU]};
+    M2 au{d, s.au};
+    if (au(i, j) >= 1) {
+      const double Vloc = 0.25 * (V(i, j - 1) + V(i + 1, j - 1) + V(i, j) + V(i + 1, j));
+      fV(i, j) = coru(i, j) * Vloc;
+    } else {
+      fV(i, j) = 0.0;
+    }
+  }
+}
+
+// m2d.F90:471-472 (Uint, Vint accumulation, FP64) + sealevel.F90:89-112 (zo = z; z update).
+__global__ void k_accum_sealevel(Dev d, Bc2 s, int accumulate) {
+  GB_IJ2
+  W2 z{d, s.f2[Z]}, zo{d, s.f2[ZO]}, U{d, s.f2[U_]}, V{d, s.f2[V_]}, fwf{d, s.f2[FWF]}, Uint{d, s.f2[UINT]},
+      Vint{d, s.f2[VINT]};
+  M2 az{d, s.az};
+  const double dtm = s.par[P_DTM];
+  if (accumulate) {
+    Uint(i, j) = Uint(i, j) + U(i, j);
+    Vint(i, j) = Vint(i, j) + V(i, j);
+  }
+  const double zold = z(i, j);
+  zo(i, j) = zold;
+  if (interior(d, i, j) && az(i, j) == 1)
+    z(i, j) = zold - dtm * ((U(i, j) * d.dy - U(i - 1, j) * d.dy) + (V(i, j) * d.dx - V(i, j - 1) * d.dx)) * d.ard1 +
+              dtm * fwf(i, j);
+}
+
+// depth_update.F90:55-110
+__global__ void k_depth_update(Dev d, Bc2 s) {
+  GB_IJ2
+  W2 D{d, s.f2[D_]}, z{d, s.f2[Z]}, zo{d, s.f2[ZO]}, H{d, s.f2[HH]}, HU_{d, s.f2[HU]}, HV_{d, s.f2[HV]},
+      DU_{d, s.f2[DU]}, DV_{d, s.f2[DV]}, dry_z{d, s.f2[DRY_Z]}, dry_u{d, s.f2[DRY_U]}, dry_v{d, s.f2[DRY_V]};
+  M2 az{d, s.az}, au{d, s.au}, av{d, s.av};
+  const double min_depth = s.par[P_MIN_DEPTH], crit_depth = s.par[P_CRIT_DEPTH];
+  D(i, j) = z(i, j) + H(i, j);
+  if (i <= d.imax + HALO - 1) {
+    const double x = fmax(0.25 * (zo(i, j) + zo(i + 1, j) + z(i, j) + z(i + 1, j)), -HU_(i, j) + min_depth);
+    DU_(i, j) = x + HU_(i, j);
+  }
+  if (j <= d.jmax + HALO - 1) {
+    const double x = fmax(0.25 * (zo(i, j) + zo(i, j + 1) + z(i, j) + z(i, j + 1)), -HV_(i, j) + min_depth);
+    DV_(i, j) = x + HV_(i, j);
+  }
+  const double d1 = 2 * min_depth;
+  const double d2i = 1.0 / (crit_depth - 2 * min_depth);
+  if (az(i, j) > 0) dry_z(i, j) = fmax(0.0, fmin(1.0, (D(i, j) - 0.5 * d1) * d2i));
+  if (au(i, j) > 0) dry_u(i, j) = fmax(0.0, fmin(1.0, (DU_(i, j) - d1) * d2i));
+  if (av(i, j) > 0) dry_v(i, j) = fmax(0.0, fmin(1.0, (DV_(i, j) - d1) * d2i));
+}
+
+// start_macro.F90:54-86, first loop (T points) ...
+__global__ void k_start_macro_t(Dev d, Bc2 s) {
+  GB_IJ2
+  W2 sseo{d, s.f2[SSEO]}, ssen{d, s.f2[SSEN]}, z{d, s.f2[Z]}, Dn{d, s.f2[DN]}, H{d, s.f2[HH]};
+  sseo(i, j) = ssen(i, j);
+  ssen(i, j) = z(i, j);
+  Dn(i, j) = ssen(i, j) + H(i, j);
+}
+// ... then U and V points and Uint/M, Vint/M
+__global__ void k_start_macro_uv(Dev d, Bc2 s, double split) {
+  GB_IJ2
+  W2 sseo{d, s.f2[SSEO]}, ssen{d, s.f2[SSEN]}, ssuo{d, s.f2[SSUO]}, ssun{d, s.f2[SSUN]}, HU_{d, s.f2[HU]},
+      Dun{d, s.f2[DUN]}, ssvo{d, s.f2[SSVO]}, ssvn{d, s.f2[SSVN]}, HV_{d, s.f2[HV]}, Dvn{d, s.f2[DVN]},
+      Uint{d, s.f2[UINT]}, Vint{d, s.f2[VINT]};
+  const double min_depth = s.par[P_MIN_DEPTH];
+  if (i <= d.imax + HALO - 1) {
+    ssuo(i, j) = ssun(i, j);
+    double v = 0.25 * (sseo(i, j) + sseo(i + 1, j) + ssen(i, j) + ssen(i + 1, j));
+    v = fmax(v, -HU_(i, j) + min_depth);
+    ssun(i, j) = v;
+    Dun(i, j) = v + HU_(i, j);
+  }
+  if (j <= d.jmax + HALO - 1) {
+    ssvo(i, j) = ssvn(i, j);
+    double v = 0.25 * (sseo(i, j) + sseo(i, j + 1) + ssen(i, j) + ssen(i, j + 1));
+    v = fmax(v, -HV_(i, j) + min_depth);
+    ssvn(i, j) = v;
+    Dvn(i, j) = v + HV_(i, j);
+  }
+  Uint(i, j) = split * Uint(i, j);
+  Vint(i, j) = split * Vint(i, j);
+}
+
+// slow_bottom_friction.F90:53-93: depth-averaged velocities of the last macro step (scratch Ui/Vi)
+__global__ void k_sbf_uv(Dev d, Bc2 s, double* Uip, double* Vip) {
+  GB_IJ2
+  W2 Uinto{d, s.f2[UINTO]}, Vinto{d, s.f2[VINTO]}, ssuo{d, s.f2[SSUO]}, ssvo{d, s.f2[SSVO]}, HU_{d, s.f2[HU]},
+      HV_{d, s.f2[HV]}, Ui{d, Uip}, Vi{d, Vip};
+  M2 au{d, s.au}, av{d, s.av};
+  const bool in = interior(d, i, j);
+  if (in)
+    Ui(i, j) = au(i, j) >= 1 ? Uinto(i, j) / (ssuo(i, j) + HU_(i, j)) : 0.0;
+  else
+    Ui(i, j) = (j == d.jmax + 1 || i == d.imin - 1) ? Uinto(i, j) / (ssuo(i, j) + HU_(i, j)) : 0.0;
+  if (in)
+    Vi(i, j) = av(i, j) >= 1 ? Vinto(i, j) / (ssvo(i, j) + HV_(i, j)) : 0.0;
+  else
+    Vi(i, j) = (j == d.jmin - 1 || i == d.imax + 1) ? Vinto(i, j) / (ssvo(i, j) + HV_(i, j)) : 0.0;
+}
+
+// slow_bottom_friction.F90:95-170: ru, rv of the slow (macro) friction. Counts non-positive log
+// arguments (the reference stops with 'Bottom friction coefficient infinite').
+__global__ void k_sbf_r(Dev d, Bc2 s, const double* Uip, const double* Vip, unsigned long long* bad) {
+  GB_IJ2
+  if (!interior(d, i, j)) return;
+  W2 ssun{d, s.f2[SSUN]}, ssvn{d, s.f2[SSVN]}, HU_{d, s.f2[HU]}, HV_{d, s.f2[HV]}, zub{d, s.f2[ZUB]},
+      zvb{d, s.f2[ZVB]}, ru{d, s.f2[RU]}, rv{d, s.f2[RV]}, Ui{d, const_cast<double*>(Uip)},
+      Vi{d, const_cast<double*>(Vip)};
+  M2 au{d, s.au}, av{d, s.av};
+  const double kappa = s.par[P_KAPPA], min_depth = s.par[P_MIN_DEPTH];
+  if (au(i, j) >= 1) {
+    const double HHl = fmax(min_depth, ssun(i, j) + HU_(i, j));
+    double r = (zub(i, j) + 0.5 * HHl) / zub(i, j);
+    if (!(r > 1.0)) atomicAdd(bad, 1ull);
+    const double x = kappa / log(r);
+    r = x * x;
+    const double uloc = Ui(i, j);
+    const double vloc = 0.25 * (Vi(i, j) + Vi(i + 1, j) + Vi(i, j - 1) + Vi(i + 1, j - 1));
+    ru(i, j) = r * sqrt(uloc * uloc + vloc * vloc);
+  } else {
+    ru(i, j) = 0.0;
+  }
+  if (av(i, j) >= 1) {
+    const double HHl = fmax(min_depth, ssvn(i, j) + HV_(i, j));
+    double r = (zvb(i, j) + 0.5 * HHl) / zvb(i, j);
+    if (!(r > 1.0)) atomicAdd(bad, 1ull);
+    const double x = kappa / log(r);
+    r = x * x;
+    const double uloc = 0.25 * (Ui(i, j) + Ui(i - 1, j) + Ui(i, j + 1) + Ui(i - 1, j + 1));
+    const double vloc = Vi(i, j);
+    rv(i, j) = r * sqrt(uloc * uloc + vloc * vloc);
+  } else {
+    rv(i, j) = 0.0;
+  }
+}
+
+// stop_macro.F90:36-39
+__global__ void k_stop_macro(Dev d, Bc2 s) {
+  GB_IJ2
+  W2 Uint{d, s.f2[UINT]}, Vint{d, s.f2[VINT]}, Uinto{d, s.f2[UINTO]}, Vinto{d, s.f2[VINTO]};
+  Uinto(i, j) = Uint(i, j);
+  Uint(i, j) = 0.0;
+  Vinto(i, j) = Vint(i, j);
+  Vint(i, j) = 0.0;
+}
+
+}  // namespace gb
+
+// =============================================================================================
+// host side
+namespace {
+
+using namespace gb;
+
+const dim3 kBlk2(32, 4, 1);
+dim3 grid2(const Dev& d) { return dim3((d.ni() + 31) / 32, (d.nj() + 3) / 4, 1); }
+
+Bc2 to_bc2(const getm_bc_state* st) {
+  Bc2 s;
+  for (int q = 0; q < NF2; ++q) s.f2[q] = st->f2[q];
+  s.az = st->az; s.au = st->au; s.av = st->av; s.ax = st->ax;
+  for (int q = 0; q < NPD; ++q) s.par[q] = st->par[q];
+  return s;
+}
+
+template <class R3>
+Bc3<R3> to_bc3(const getm_bc_state* st) {
+  Bc3<R3> s;
+  for (int q = 0; q < NF2; ++q) s.f2[q] = st->f2[q];
+  for (int q = 0; q < NF3; ++q) s.f3[q] = (R3*)st->f3[q];
+  s.az = st->az; s.au = st->au; s.av = st->av; s.ax = st->ax;
+  for (int q = 0; q < NPD; ++q) s.par[q] = st->par[q];
+  return s;
+}
+
+int check_state(getm_ctx* ctx, const getm_bc_state* st) {
+  if (!ctx || !st) return GETM_ERR_ARG;
+  if (!ctx->adv_ready) return fail(ctx, GETM_ERR_STATE, "getm_init_advection has not been called");
+  if (st->prec3d != 8 && st->prec3d != 4) return fail(ctx, GETM_ERR_ARG, "getm_bc_state.prec3d must be 8 or 4");
+  for (int q = 0; q < NF2; ++q)
+    if (!st->f2[q]) return fail(ctx, GETM_ERR_ARG, "getm_bc_state: null 2D field");
+  for (int q = 0; q < NF3; ++q)
+    if (!st->f3[q]) return fail(ctx, GETM_ERR_ARG, "getm_bc_state: null 3D field");
+  if (!st->az || !st->au || !st->av || !st->ax) return fail(ctx, GETM_ERR_ARG, "getm_bc_state: null mask");
+  if (st->ipar[I_RUNTYPE] != 4 && st->ipar[I_RUNTYPE] != 2 && st->ipar[I_RUNTYPE] != 1 && st->ipar[I_RUNTYPE] != 3)
+    return fail(ctx, GETM_ERR_ARG, "runtype must be 1..4");
+  if (st->ipar[I_M] < 1 || st->ipar[I_MM] < 1) return fail(ctx, GETM_ERR_ARG, "M and MM must be >= 1");
+  if ((size_t)2 * (ctx->dom.kmax + 1) * 64 * sizeof(double) > 200 * 1024)
+    return fail(ctx, GETM_ERR_UNSUPPORTED, "kmax too large for the column solvers");
+  return GETM_OK;
+}
+
+int ensure_bc_scratch(getm_ctx* ctx, size_t elem3) {
+  const long long n3 = n3d(ctx->dev), n2 = n2d(ctx->dev);
+  const size_t b3 = (size_t)NB3 * n3 * elem3;
+  if (ctx->bc_scr3_bytes < b3) {
+    if (ctx->bc_scr3) cudaFree(ctx->bc_scr3);
+    ctx->bc_scr3 = nullptr;
+    ctx->bc_scr3_bytes = 0;
+    if (cudaMalloc(&ctx->bc_scr3, b3) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(ctx, GETM_ERR_NOMEM, "mode-split 3D scratch allocation failed");
+    }
+    cudaMemsetAsync(ctx->bc_scr3, 0, b3, ctx->stream);
+    ctx->bc_scr3_bytes = b3;
+  }
+  if (!ctx->bc_scr2) {
+    if (cudaMalloc(&ctx->bc_scr2, (size_t)NB2 * n2 * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(ctx, GETM_ERR_NOMEM, "mode-split 2D scratch allocation failed");
+    }
+    cudaMemsetAsync(ctx->bc_scr2, 0, (size_t)NB2 * n2 * sizeof(double), ctx->stream);
+  }
+  return GETM_OK;
+}
+
+// do_advection (advection.F90:362-702) on 2D FP64 fields, split schemes. Di and adv come from the
+// 2D scratch when the caller passes none.
+int do_adv2d(getm_ctx* ctx, double dt, double* f, const double* U, const double* V, const double* DUa,
+             const double* DVa, const double* Do, int split, int scheme, int tag, double* advres) {
+  const Dev& d = ctx->dev;
+  cudaStream_t s = ctx->stream;
+  const long long n2 = n2d(d);
+  const size_t b2 = (size_t)n2 * sizeof(double);
+  double* Di = ctx->bc_scr2 + 5 * n2;
+  double* A = advres ? advres : ctx->bc_scr2 + 6 * n2;
+  double* S = ctx->bc_scr2 + 7 * n2;
+  getm_adv_grid g;
+  if (!grid_for_tag(ctx, tag, &g)) return fail(ctx, GETM_ERR_ARG, "do_advection: tag is invalid");
+  GB_TRY(cudaMemcpyAsync(Di, Do, b2, cudaMemcpyDeviceToDevice, s), "copy Do");
+  GB_TRY(cudaMemsetAsync(A, 0, b2, s), "zero adv");
+  if (scheme == NOADV) return GETM_OK;
+  if (!is_split_scheme(scheme)) return fail(ctx, GETM_ERR_UNSUPPORTED, "do_advection: 2DH schemes not provided");
+  const double one = 1.0, half = 0.5;
+  switch (split) {
+    case GETM_NOSPLIT:
+      GB_TRY(cudaMemcpyAsync(S, f, b2, cudaMemcpyDeviceToDevice, s), "copy f");
+      GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<double, 0>(d, s, 1, dt, one, scheme, 0.0, f, S, S, Di, Di, A, U, DUa,
+                                                        g.mask_uflux, g.mask_uupdate)), "u");
+      GB_TIMED(GETM_TIM_ADV_V, (run_sweep_h<double, 1>(d, s, 1, dt, one, scheme, 0.0, f, S, S, Di, Di, A, V, DVa,
+                                                        g.mask_vflux, g.mask_vupdate)), "v");
+      k_finalise2d<<<grid2(d), kBlk2, 0, s>>>(d, dt, f, Do, A, Di, g.mask_finalise);
+      GB_TRY(cudaGetLastError(), "finalise2d");
+      break;
+    case GETM_FULLSPLIT:
+      GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<double, 0>(d, s, 1, dt, one, scheme, 0.0, f, f, S, Di, Di, A, U, DUa,
+                                                        g.mask_uflux, g.mask_uupdate)), "u");
+      GB_TIMED(GETM_TIM_ADV_V, (run_sweep_h<double, 1>(d, s, 1, dt, one, scheme, 0.0, S, S, f, Di, Di, A, V, DVa,
+                                                        g.mask_vflux, g.mask_vupdate)), "v");
+      break;
+    case GETM_HALFSPLIT:
+      GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<double, 0>(d, s, 1, dt, half, scheme, 0.0, f, f, S, Di, Di, A, U, DUa,
+                                                        g.mask_uflux, g.mask_uupdate)), "u");
+      GB_TIMED(GETM_TIM_ADV_V, (run_sweep_h<double, 1>(d, s, 1, dt, one, scheme, 0.0, S, S, f, Di, Di, A, V, DVa,
+                                                        g.mask_vflux, g.mask_vupdate)), "v");
+      GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<double, 0>(d, s, 1, dt, half, scheme, 0.0, f, f, S, Di, Di, A, U, DUa,
+                                                        g.mask_uflux, g.mask_uupdate)), "u");
+      GB_TRY(cudaMemcpyAsync(f, S, b2, cudaMemcpyDeviceToDevice, s), "copy back");
+      break;
+    default:
+      return fail(ctx, GETM_ERR_ARG, "do_advection: split is invalid");
+  }
+  return GETM_OK;
+}
+
+// uv_advect.F90:94-300 on (U, V, DU, DV) -> UEx, VEx (split schemes).
+int uv_advect_2d(getm_ctx* ctx, const getm_bc_state* st, const double* U, const double* V, const double* DU_,
+                 const double* DV_) {
+  const Dev& d = ctx->dev;
+  cudaStream_t s = ctx->stream;
+  const long long n2 = n2d(d);
+  const int split = st->ipar[I_VEL2D_SPLIT], hor = st->ipar[I_VEL2D_HOR];
+  double* UEx = st->f2[UEX];
+  double* VEx = st->f2[VEX];
+  if (hor == NOADV) {
+    GB_TRY(cudaMemsetAsync(UEx, 0, n2 * sizeof(double), s), "UEx=0");
+    GB_TRY(cudaMemsetAsync(VEx, 0, n2 * sizeof(double), s), "VEx=0");
+    return GETM_OK;
+  }
+  double* w = ctx->bc_scr2;
+  double *fadv = w, *Uadv = w + n2, *Vadv = w + 2 * n2, *DUadv = w + 3 * n2, *DVadv = w + 4 * n2;
+  {
+    TimerScope ts(ctx, GETM_TIM_BC2D);
+    k_uvadv2d_prep<0><<<grid2(d), kBlk2, 0, s>>>(d, U, V, DU_, DV_, fadv, Uadv, Vadv, DUadv, DVadv);
+    GB_TRY(cudaGetLastError(), "uv_advect prep U");
+  }
+  int rc = do_adv2d(ctx, st->par[P_DTM], fadv, Uadv, Vadv, DUadv, DVadv, DU_, split, hor, GETM_U_TAG, UEx);
+  if (rc) return rc;
+  {
+    TimerScope ts(ctx, GETM_TIM_BC2D);
+    k_uvadv2d_prep<1><<<grid2(d), kBlk2, 0, s>>>(d, U, V, DU_, DV_, fadv, Uadv, Vadv, DUadv, DVadv);
+    GB_TRY(cudaGetLastError(), "uv_advect prep V");
+  }
+  return do_adv2d(ctx, st->par[P_DTM], fadv, Uadv, Vadv, DUadv, DVadv, DV_, split, hor, GETM_V_TAG, VEx);
+}
+
+#define GB_K2(kernel, ...)                                         \
+  do {                                                             \
+    TimerScope _ts(ctx, GETM_TIM_BC2D);                            \
+    kernel<<<grid2(d), kBlk2, 0, ctx->stream>>>(__VA_ARGS__);      \
+    GB_TRY(cudaGetLastError(), #kernel);                           \
+  } while (0)
+
+// m2d.F90:412-490 integrate_2d (closed boundaries; no residual; Am <= 0, An_method = 0)
+int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop) {
+  const Dev& d = ctx->dev;
+  const Bc2 s = to_bc2(st);
+  int* ip = st->ipar;
+  if ((loop - 1) % ip[I_MM] == 0) GB_K2(k_bottom_friction, d, s, ip[I_RUNTYPE]);
+  int rc = uv_advect_2d(ctx, st, st->f2[U_], st->f2[V_], st->f2[DU], st->f2[DV]);
+  if (rc) return rc;
+  if (ip[I_UFIRST2D]) {
+    GB_K2(k_momentum<0>, d, s);
+    GB_K2(k_coriolis<0>, d, s);
+    GB_K2(k_momentum<1>, d, s);
+    GB_K2(k_coriolis<1>, d, s);
+    ip[I_UFIRST2D] = 0;
+  } else {
+    GB_K2(k_momentum<1>, d, s);
+    GB_K2(k_coriolis<1>, d, s);
+    GB_K2(k_momentum<0>, d, s);
+    GB_K2(k_coriolis<0>, d, s);
+    ip[I_UFIRST2D] = 1;
+  }
+  GB_K2(k_accum_sealevel, d, s, ip[I_RUNTYPE] > 1 ? 1 : 0);
+  GB_K2(k_depth_update, d, s);
+  return GETM_OK;
+}
+
+template <class R3>
+int bc3(getm_ctx* ctx, const getm_bc_state* st, int which, int slot) {
+  const Bc3<R3> s = to_bc3<R3>(st);
+  const long long n3 = n3d(ctx->dev);
+  R3* base = (R3*)ctx->bc_scr3;
+  R3* scr[NB3];
+  for (int q = 0; q < NB3; ++q) scr[q] = base + q * n3;
+  GB_TIMED(slot, (run_bc3<R3>(which, ctx->dev, ctx->stream, s, scr)), "macro-step kernel");
+  return GETM_OK;
+}
+
+// m3d.F90:422-636 integrate_3d for runtype 4 (closed boundaries, sigma coordinates, linear EOS,
+// Blumberg-Mellor internal pressure, prescribed viscosity)
+template <class R3>
+int integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
+  (void)n;
+  const Dev& d = ctx->dev;
+  cudaStream_t s = ctx->stream;
+  const Bc2 s2 = to_bc2(st);
+  int* ip = st->ipar;
+  const long long n3 = n3d(d);
+  const size_t b3 = (size_t)n3 * sizeof(R3);
+  R3** f3 = (R3**)st->f3;
+  int rc;
+  // start_macro
+  GB_K2(k_start_macro_t, d, s2);
+  GB_K2(k_start_macro_uv, d, s2, 1.0 / (double)(float)ip[I_M]);
+  if (d.kmax > 1 && (rc = bc3<R3>(ctx, st, BC3_BF3D, GETM_TIM_BC3D))) return rc;
+  if (ip[I_RUNTYPE] == 4) {
+    if ((rc = bc3<R3>(ctx, st, BC3_ZZ, GETM_TIM_IP))) return rc;
+    if ((rc = bc3<R3>(ctx, st, BC3_IP, GETM_TIM_IP))) return rc;
+  }
+  {
+    TimerScope ts(ctx, GETM_TIM_COPY);
+    GB_TRY(cudaMemcpyAsync(f3[HUO], f3[HUN], b3, cudaMemcpyDeviceToDevice, s), "huo=hun");
+    GB_TRY(cudaMemcpyAsync(f3[HVO], f3[HVN], b3, cudaMemcpyDeviceToDevice, s), "hvo=hvn");
+  }
+  if (ip[I_UFIRST3D]) {
+    if ((rc = bc3<R3>(ctx, st, BC3_UUMOM, GETM_TIM_MOM3D))) return rc;
+    if ((rc = bc3<R3>(ctx, st, BC3_VVMOM, GETM_TIM_MOM3D))) return rc;
+    ip[I_UFIRST3D] = 0;
+  } else {
+    if ((rc = bc3<R3>(ctx, st, BC3_VVMOM, GETM_TIM_MOM3D))) return rc;
+    if ((rc = bc3<R3>(ctx, st, BC3_UUMOM, GETM_TIM_MOM3D))) return rc;
+    ip[I_UFIRST3D] = 1;
+  }
+  if ((rc = bc3<R3>(ctx, st, BC3_SIGMA, GETM_TIM_BC3D))) return rc;
+  if (d.kmax > 1) {
+    if ((rc = bc3<R3>(ctx, st, BC3_WW, GETM_TIM_BC3D))) return rc;
+    // uv_advect_3d (uv_advect_3d.F90:62-460)
+    const int split = ip[I_VEL3D_SPLIT], hor = ip[I_VEL3D_HOR], ver = ip[I_VEL3D_VER];
+    if (hor != NOADV || ver != NOADV) {
+      R3* w = (R3*)ctx->bc_scr3;
+      R3 *fadv = w, *ua = w + n3, *va = w + 2 * n3, *wa = w + 3 * n3, *hua = w + 4 * n3, *hva = w + 5 * n3;
+      if ((rc = bc3<R3>(ctx, st, BC3_UVADV_PREP_U, GETM_TIM_BC3D))) return rc;
+      if ((rc = do_adv3d<R3>(ctx, R3(st->par[P_DT]), fadv, ua, va, wa, hua, hva, f3[HUN], f3[HUN], split, hor, ver,
+                             R3(0), GETM_U_TAG, nullptr, f3[UUEX], ip[I_ADV_VER_ITERS])))
+        return rc;
+      if ((rc = bc3<R3>(ctx, st, BC3_UVADV_PREP_V, GETM_TIM_BC3D))) return rc;
+      if ((rc = do_adv3d<R3>(ctx, R3(st->par[P_DT]), fadv, ua, va, wa, hua, hva, f3[HVN], f3[HVN], split, hor, ver,
+                             R3(0), GETM_V_TAG, nullptr, f3[VVEX], ip[I_ADV_VER_ITERS])))
+        return rc;
+    }
+    if ((rc = bc3<R3>(ctx, st, BC3_STRESSES, GETM_TIM_BC3D))) return rc;
+  }
+  if (ip[I_RUNTYPE] == 4) {
+    const R3 dt = R3(st->par[P_DT]);
+    if (ip[I_CALC_TEMP]) {
+      if ((rc = do_adv3d<R3>(ctx, dt, f3[TT], f3[UU], f3[VV], f3[WW], f3[HUN], f3[HVN], f3[HO], f3[HN],
+                             ip[I_TEMP_SPLIT], ip[I_TEMP_HOR], ip[I_TEMP_VER], R3(st->par[P_TEMP_AH]), GETM_H_TAG,
+                             nullptr, nullptr, ip[I_ADV_VER_ITERS])))
+        return rc;
+      GB_TIMED(GETM_TIM_VDIFF, run_vdiff<R3>(d, s, dt, R3(st->par[P_CNPAR]), R3(st->par[P_AVMOLT]), f3[TT], f3[HN],
+                                             f3[NUH], st->az, (const R3*)nullptr), "vdiff T");
+    }
+    if (ip[I_CALC_SALT]) {
+      if ((rc = do_adv3d<R3>(ctx, dt, f3[SS], f3[UU], f3[VV], f3[WW], f3[HUN], f3[HVN], f3[HO], f3[HN],
+                             ip[I_SALT_SPLIT], ip[I_SALT_HOR], ip[I_SALT_VER], R3(st->par[P_SALT_AH]), GETM_H_TAG,
+                             nullptr, nullptr, ip[I_ADV_VER_ITERS])))
+        return rc;
+      GB_TIMED(GETM_TIM_VDIFF, run_vdiff<R3>(d, s, dt, R3(st->par[P_CNPAR]), R3(st->par[P_AVMOLS]), f3[SS], f3[HN],
+                                             f3[NUH], st->az, (const R3*)nullptr), "vdiff S");
+    }
+    if ((rc = bc3<R3>(ctx, st, BC3_EQSTATE, GETM_TIM_BC3D))) return rc;
+  }
+  if (d.kmax > 1) {
+    const long long n2 = n2d(d);
+    double* Ui = ctx->bc_scr2 + 8 * n2;
+    double* Vi = ctx->bc_scr2 + 9 * n2;
+    GB_K2(k_sbf_uv, d, s2, Ui, Vi);
+    GB_K2(k_sbf_r, d, s2, Ui, Vi, ctx->cnt + 2);
+    if ((rc = uv_advect_2d(ctx, st, st->f2[UINT], st->f2[VINT], st->f2[DUN], st->f2[DVN]))) return rc;
+  }
+  if ((rc = bc3<R3>(ctx, st, BC3_SLOW_TERMS, GETM_TIM_BC3D))) return rc;
+  GB_K2(k_stop_macro, d, s2);
+  return GETM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int getm_integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop) {
+  int rc = check_state(ctx, st);
+  if (rc) return rc;
+  if ((rc = ensure_bc_scratch(ctx, (size_t)st->prec3d))) return rc;
+  return integrate_2d(ctx, st, loop);
+}
+
+int getm_integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
+  int rc = check_state(ctx, st);
+  if (rc) return rc;
+  if ((rc = ensure_bc_scratch(ctx, (size_t)st->prec3d))) return rc;
+  return st->prec3d == 8 ? integrate_3d<double>(ctx, st, n) : integrate_3d<float>(ctx, st, n);
+}
+
+int getm_time_loop(getm_ctx* ctx, getm_bc_state* st, int n0, int count) {
+  int rc = check_state(ctx, st);
+  if (rc) return rc;
+  if ((rc = ensure_bc_scratch(ctx, (size_t)st->prec3d))) return rc;
+  for (int n = n0; n < n0 + count; ++n) {
+    if ((rc = integrate_2d(ctx, st, n))) return rc;
+    if (n % st->ipar[I_M] == 0) {
+      rc = st->prec3d == 8 ? integrate_3d<double>(ctx, st, n) : integrate_3d<float>(ctx, st, n);
+      if (rc) return rc;
+    }
+  }
+  return GETM_OK;
+}
+
+}  // extern "C"

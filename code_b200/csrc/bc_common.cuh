@@ -1,0 +1,43 @@
+// bc_common.cuh -- the state table of the mode-split step as the kernels see it.
+// Field order is part of the C ABI (getm_bc_state, include/getm_b200.h).
+#pragma once
+#include "common.cuh"
+
+namespace gb {
+
+enum F2 {
+  Z, ZO, U_, V_, D_, DU, DV, UEX, VEX, FU, FV, RU, RV, RUU, RVV, UINT, VINT, UINTO, VINTO, SLUX, SLVX, SLRU, SLRV,
+  ZUB, ZVB, ZUB0, ZVB0, FWF, HH, HU, HV, DRY_Z, DRY_U, DRY_V, CORU, CORV, TAUSX, TAUSY, AIRP, SSEO, SSEN, SSUO,
+  SSUN, SSVO, SSVN, DN, DUN, DVN, RRU, RRV, TAUBX, TAUBY, TAUB, TAUS, NF2
+};
+enum F3 { UU, VV, WW, HO, HN, HUO, HUN, HVO, HVN, UUEX, VVEX, IDPDX, IDPDY, TT, SS, RHO, BUOY, NUM, NUH, NF3 };
+enum PD {
+  P_DTM, P_DT, P_CNPAR, P_MIN_DEPTH, P_CRIT_DEPTH, P_G, P_RHO_0, P_KAPPA, P_AVMMOL, P_AVMOLT, P_AVMOLS, P_T0, P_S0,
+  P_DTR0, P_DSR0, P_IP_FAC, P_TEMP_AH, P_SALT_AH, NPD
+};
+enum PI {
+  I_M, I_MM, I_RUNTYPE, I_VEL2D_SPLIT, I_VEL2D_HOR, I_VEL3D_SPLIT, I_VEL3D_HOR, I_VEL3D_VER, I_TEMP_SPLIT, I_TEMP_HOR,
+  I_TEMP_VER, I_SALT_SPLIT, I_SALT_HOR, I_SALT_VER, I_ADV_VER_ITERS, I_UFIRST2D, I_UFIRST3D, I_CALC_TEMP,
+  I_CALC_SALT, NPI
+};
+
+// 2D part (all FP64) -- passed to kernels by value
+struct Bc2 {
+  double* f2[NF2];
+  const int32_t *az, *au, *av, *ax;
+  double par[NPD];
+};
+
+template <class R3>
+struct Bc3 {
+  double* f2[NF2];
+  R3* f3[NF3];
+  const int32_t *az, *au, *av, *ax;
+  double par[NPD];
+};
+
+// number of 3D / 2D scratch arrays of the mode-split step
+constexpr int NB3 = 7;   // fadv, uuadv, vvadv, wwadv, huadv, hvadv, zz
+constexpr int NB2 = 10;  // fadv, Uadv, Vadv, DUadv, DVadv, Di, adv, S, Ui, Vi
+
+}  // namespace gb

@@ -1,0 +1,426 @@
+// bc_kernels.cuh -- 3D kernels of the mode-split macro step (integrate_3d), templated on the type
+// R3 of the 3D fields (double: the plain FP64 step, bit for bit with the oracle; float: the
+// mixed-precision step). 2D fields are always FP64. Included by kernels_inst.cuh.
+#pragma once
+#include "bc_common.cuh"
+#include "common.cuh"
+
+namespace gb {
+
+template <class R3>
+struct V3 {
+  const Dev& d;
+  R3* p;
+  __device__ R3& operator()(int i, int j, int k) const { return p[d.ix(i, j) + (long long)k * d.sk]; }
+};
+struct V2 {
+  const Dev& d;
+  double* p;
+  __device__ double& operator()(int i, int j) const { return p[d.ix(i, j)]; }
+};
+struct I2 {
+  const Dev& d;
+  const int32_t* p;
+  __device__ int operator()(int i, int j) const { return p[d.ix(i, j)]; }
+};
+
+// thread -> reference index over the haloed plane
+#define GB_IJ_HALO                                          \
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + d.imin - HALO; \
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + d.jmin - HALO; \
+  if (i > d.imax + HALO || j > d.jmax + HALO) return;
+
+// ---------------------------------------------------------------------------------------------
+// bottom_friction_3d.F90:50-130 (kumin = kvmin = 1); 2D output rru, rrv. Bottom-layer quotients
+// in FP64.
+template <class R3>
+__global__ void k_bf3d(Dev d, Bc3<R3> s) {
+  GB_IJ_HALO
+  if (i < d.imin || i > d.imax || j < d.jmin || j > d.jmax) return;
+  V3<R3> uu{d, s.f3[UU]}, vv{d, s.f3[VV]}, huo{d, s.f3[HUO]}, hvo{d, s.f3[HVO]}, hun{d, s.f3[HUN]}, hvn{d, s.f3[HVN]};
+  V2 zub{d, s.f2[ZUB]}, zvb{d, s.f2[ZVB]}, rru{d, s.f2[RRU]}, rrv{d, s.f2[RRV]};
+  I2 au{d, s.au}, av{d, s.av};
+  const double kappa = s.par[P_KAPPA], min_depth = s.par[P_MIN_DEPTH];
+  auto q = [](R3 a, R3 b) { return (double)a / (double)b; };
+  if (au(i, j) >= 1) {
+    const double uuloc = q(uu(i, j, 1), huo(i, j, 1));
+    const double uvloc = 0.25 * (q(vv(i, j, 1), hvo(i, j, 1)) + q(vv(i + 1, j, 1), hvo(i + 1, j, 1)) +
+                                 q(vv(i, j - 1, 1), hvo(i, j - 1, 1)) + q(vv(i + 1, j - 1, 1), hvo(i + 1, j - 1, 1)));
+    const double hh = fmax(min_depth / d.kmax, (double)hun(i, j, 1)) ;
+    double r = (zub(i, j) + 0.5 * hh) / zub(i, j);
+    r = kappa / log(r);
+    r = r * r;
+    rru(i, j) = r * sqrt(uuloc * uuloc + uvloc * uvloc);
+  }
+  if (av(i, j) >= 1) {
+    const double vuloc = 0.25 * (q(uu(i, j, 1), huo(i, j, 1)) + q(uu(i - 1, j, 1), huo(i - 1, j, 1)) +
+                                 q(uu(i, j + 1, 1), huo(i, j + 1, 1)) + q(uu(i - 1, j + 1, 1), huo(i - 1, j + 1, 1)));
+    const double vvloc = q(vv(i, j, 1), hvo(i, j, 1));
+    const double hh = fmax(min_depth / d.kmax, (double)hvn(i, j, 1));
+    double r = (zvb(i, j) + 0.5 * hh) / zvb(i, j);
+    r = kappa / log(r);
+    r = r * r;
+    rrv(i, j) = r * sqrt(vuloc * vuloc + vvloc * vvloc);
+  }
+}
+
+// ip_blumberg_mellor.F90:83-92: interface heights zz of every wet T column (j <= jmax+1,
+// i <= imax+1); zz is a scratch 3D array.
+template <class R3>
+__global__ void k_zz(Dev d, Bc3<R3> s, R3* zzp) {
+  GB_IJ_HALO
+  if (i < d.imin || i > d.imax + 1 || j < d.jmin || j > d.jmax + 1) return;
+  I2 az{d, s.az};
+  if (az(i, j) < 1) return;
+  V3<R3> hn{d, s.f3[HN]}, zz{d, zzp};
+  V2 H{d, s.f2[HH]};
+  R3 z = R3(-H(i, j)) + hn(i, j, 1);
+  zz(i, j, 1) = z;
+  for (int k = 2; k <= d.kmax; ++k) {
+    z = z + hn(i, j, k);
+    zz(i, j, k) = z;
+  }
+}
+
+// ip_blumberg_mellor.F90:94-148: downward integral of the buoyancy gradient per U and V column.
+template <class R3>
+__global__ void k_ip(Dev d, Bc3<R3> s, const R3* zzp) {
+  GB_IJ_HALO
+  V3<R3> hun{d, s.f3[HUN]}, hvn{d, s.f3[HVN]}, buoy{d, s.f3[BUOY]}, idpdx{d, s.f3[IDPDX]}, idpdy{d, s.f3[IDPDY]},
+      zz{d, const_cast<R3*>(zzp)};
+  idpdx(i, j, 0) = R3(0);
+  idpdy(i, j, 0) = R3(0);
+  if (i < d.imin || i > d.imax || j < d.jmin || j > d.jmax) return;
+  I2 au{d, s.au}, av{d, s.av};
+  const int kmax = d.kmax;
+  const R3 half = R3(0.5);
+  if (au(i, j) >= 1) {
+    const R3 dxm1 = R3(1.0 / d.dx);
+    R3 grdl = (buoy(i + 1, j, kmax) - buoy(i, j, kmax)) * dxm1;
+    R3 buoyl = half * (buoy(i + 1, j, kmax) + buoy(i, j, kmax));
+    R3 prgr = grdl * half * hun(i, j, kmax);
+    idpdx(i, j, kmax) = hun(i, j, kmax) * prgr;
+    for (int k = kmax - 1; k >= 1; --k) {
+      const R3 grdu = grdl;
+      grdl = (buoy(i + 1, j, k) - buoy(i, j, k)) * dxm1;
+      const R3 buoyu = buoyl;
+      buoyl = half * (buoy(i + 1, j, k) + buoy(i, j, k));
+      const R3 dxz = (zz(i + 1, j, k) - zz(i, j, k)) * dxm1;
+      prgr = prgr + half * (grdu + grdl) * half * (hun(i, j, k) + hun(i, j, k + 1)) - dxz * (buoyu - buoyl);
+      idpdx(i, j, k) = hun(i, j, k) * prgr;
+    }
+  }
+  if (av(i, j) >= 1) {
+    const R3 dym1 = R3(1.0 / d.dy);
+    R3 grdl = (buoy(i, j + 1, kmax) - buoy(i, j, kmax)) * dym1;
+    R3 buoyl = half * (buoy(i, j + 1, kmax) + buoy(i, j, kmax));
+    R3 prgr = grdl * half * hvn(i, j, kmax);
+    idpdy(i, j, kmax) = hvn(i, j, kmax) * prgr;
+    for (int k = kmax - 1; k >= 1; --k) {
+      const R3 grdu = grdl;
+      grdl = (buoy(i, j + 1, k) - buoy(i, j, k)) * dym1;
+      const R3 buoyu = buoyl;
+      buoyl = half * (buoy(i, j + 1, k) + buoy(i, j, k));
+      const R3 dyz = (zz(i, j + 1, k) - zz(i, j, k)) * dym1;
+      prgr = prgr + half * (grdu + grdl) * half * (hvn(i, j, k) + hvn(i, j, k + 1)) - dyz * (buoyu - buoyl);
+      idpdy(i, j, k) = hvn(i, j, k) * prgr;
+    }
+  }
+}
+
+// uu_momentum_3d.F90:169-304 (DIR 0) / vv_momentum_3d.F90:174-315 (DIR 1), kumin = 1: explicit
+// terms, implicit vertical viscosity (Thomas solve with ru/qu in shared memory, column per thread)
+// and the transport correction to the depth-integrated transport Uint. Arithmetic in FP64.
+template <class R3, int DIR>
+__global__ void __launch_bounds__(64) k_uvmom3d(Dev d, Bc3<R3> s) {
+  extern __shared__ double smem_d[];
+  const int kmax = d.kmax;
+  const int nt = blockDim.x * blockDim.y;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  double* RU = smem_d;                    // [k][tid]
+  double* QU = smem_d + (kmax + 1) * nt;  // [k][tid]
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + d.imin;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + d.jmin;
+  if (i > d.imax || j > d.jmax) return;
+  I2 mask{d, DIR == 0 ? s.au : s.av};
+  if (!(mask(i, j) == 1 || mask(i, j) == 2)) return;
+  V3<R3> uu{d, s.f3[DIR == 0 ? UU : VV]}, vv{d, s.f3[DIR == 0 ? VV : UU]}, ho{d, s.f3[DIR == 0 ? HUO : HVO]},
+      hn{d, s.f3[DIR == 0 ? HUN : HVN]}, Ex{d, s.f3[DIR == 0 ? UUEX : VVEX]}, idp{d, s.f3[DIR == 0 ? IDPDX : IDPDY]},
+      num{d, s.f3[NUM]};
+  V2 dry{d, s.f2[DIR == 0 ? DRY_U : DRY_V]}, cor{d, s.f2[DIR == 0 ? CORU : CORV]},
+      taus{d, s.f2[DIR == 0 ? TAUSX : TAUSY]}, sseo{d, s.f2[SSEO]}, H{d, s.f2[HH]}, D{d, s.f2[D_]},
+      airp{d, s.f2[AIRP]}, rr{d, s.f2[DIR == 0 ? RRU : RRV]}, Uint{d, s.f2[DIR == 0 ? UINT : VINT]},
+      sso{d, s.f2[DIR == 0 ? SSUO : SSVO]}, HX{d, s.f2[DIR == 0 ? HU : HV]};
+  const double g = s.par[P_G], rho_0 = s.par[P_RHO_0], dt = s.par[P_DT], cnpar = s.par[P_CNPAR],
+               avmmol = s.par[P_AVMMOL], min_depth = s.par[P_MIN_DEPTH], ip_fac = s.par[P_IP_FAC];
+  const int di = DIR == 0 ? 1 : 0, dj = DIR == 0 ? 0 : 1;
+  if (kmax <= 1) {
+    uu(i, j, kmax) = R3(Uint(i, j));
+    return;
+  }
+  const double gamma = g * rho_0;
+  const double gammai = 1.0 / gamma, rho_0i = 1.0 / rho_0;
+  auto HO = [&](int k) { return (double)ho(i, j, k); };
+  auto HN = [&](int k) { return (double)hn(i, j, k); };
+  auto UU_ = [&](int k) { return (double)uu(i, j, k); };
+  auto exk = [&](int k) {
+    double loc, e;
+    if (DIR == 0) {
+      loc = 0.25 * ((double)vv(i, j, k) + (double)vv(i + 1, j, k) + (double)vv(i, j - 1, k) + (double)vv(i + 1, j - 1, k));
+      e = cor(i, j) * loc;
+    } else {
+      loc = 0.25 * ((double)vv(i, j, k) + (double)vv(i - 1, j, k) + (double)vv(i, j + 1, k) + (double)vv(i - 1, j + 1, k));
+      e = -cor(i, j) * loc;
+    }
+    double x = dry(i, j) * (e - (double)Ex(i, j, k) + ip_fac * (double)idp(i, j, k));
+    if (k == kmax) x = x + dry(i, j) * 0.5 * (taus(i, j) + taus(i + di, j + dj)) * rho_0i;
+    return x;
+  };
+  auto dif = [&](int k) { return 0.5 * ((double)num(i, j, k) + (double)num(i + di, j + dj, k)) + avmmol; };
+  auto auxo = [&](int k) { return 2.0 * (1.0 - cnpar) * dt * dif(k) / (HO(k + 1) + HO(k)); };
+  auto auxn = [&](int k) { return 2.0 * cnpar * dt * dif(k) / (HN(k + 1) + HN(k)); };
+  const double zp = fmax(sseo(i + di, j + dj), -H(i, j) + fmin(min_depth, D(i + di, j + dj)));
+  const double zm = fmax(sseo(i, j), -H(i + di, j + dj) + fmin(min_depth, D(i, j)));
+  double zx;
+  if (DIR == 0)
+    zx = (zp - zm + (airp(i + 1, j) - airp(i, j)) * gammai) / d.dx;
+  else
+    zx = (zp - zm + (airp(i, j + 1) - airp(i, j)) / gamma) / d.dy;
+  // surface row (lt = kmax)
+  int k = kmax;
+  double ao_km1 = auxo(k - 1), an_km1 = auxn(k - 1);
+  {
+    const double a1 = -an_km1 / HN(k - 1);
+    const double a2 = 1. + an_km1 / HN(k);
+    const double a4 = UU_(k) * (1 - ao_km1 / HO(k)) + UU_(k - 1) * ao_km1 / HO(k - 1) + dt * exk(k) -
+                      dt * 0.5 * (HO(k) + HN(k)) * g * zx;
+    RU[k * nt + tid] = a1 / a2;
+    QU[k * nt + tid] = a4 / a2;
+  }
+  for (k = kmax - 1; k >= 2; --k) {
+    const double ao_k = ao_km1, an_k = an_km1;
+    ao_km1 = auxo(k - 1);
+    an_km1 = auxn(k - 1);
+    const double a3 = -an_k / HN(k + 1);
+    const double a1 = -an_km1 / HN(k - 1);
+    const double a2 = 1.0 + (an_k + an_km1) / HN(k);
+    const double a4 = UU_(k + 1) * ao_k / HO(k + 1) + UU_(k) * (1 - (ao_k + ao_km1) / HO(k)) +
+                      UU_(k - 1) * ao_km1 / HO(k - 1) + dt * exk(k) - dt * 0.5 * (HO(k) + HN(k)) * g * zx;
+    const double den = a2 - a3 * RU[(k + 1) * nt + tid];
+    RU[k * nt + tid] = a1 / den;
+    QU[k * nt + tid] = (a4 - a3 * QU[(k + 1) * nt + tid]) / den;
+  }
+  {
+    k = 1;
+    const double ao_k = ao_km1, an_k = an_km1;
+    const double a3 = -an_k / HN(k + 1);
+    const double a2 = 1.0 + an_k / HN(k) + dt * rr(i, j) / (0.5 * (HN(k) + HO(k)));
+    const double a4 = UU_(k + 1) * ao_k / HO(k + 1) + UU_(k) * (1 - ao_k / HO(k)) + dt * exk(k) -
+                      dt * 0.5 * (HO(k) + HN(k)) * g * zx;
+    QU[1 * nt + tid] = (a4 - a3 * QU[2 * nt + tid]) / (a2 - a3 * RU[2 * nt + tid]);
+  }
+  // back substitution; Res(k) kept in QU, its sum in ascending k
+  double v = QU[1 * nt + tid];
+  double ResInt = 0.0;
+  ResInt = ResInt + v;
+  for (k = 2; k <= kmax; ++k) {
+    v = QU[k * nt + tid] - RU[k * nt + tid] * v;
+    QU[k * nt + tid] = v;
+    ResInt = ResInt + v;
+  }
+  const double Diff = (Uint(i, j) - ResInt) / (sso(i, j) + HX(i, j));
+  for (k = 1; k <= kmax; ++k) uu(i, j, k) = R3(QU[k * nt + tid] + HN(k) * Diff);
+}
+
+// sigma_coordinates.F90:85-113 (equidistant sigma): layer heights of all levels 0..kmax.
+template <class R3>
+__global__ void k_sigma(Dev d, Bc3<R3> s) {
+  GB_IJ_HALO
+  V2 sseo{d, s.f2[SSEO]}, ssen{d, s.f2[SSEN]}, H{d, s.f2[HH]}, ssuo{d, s.f2[SSUO]}, ssun{d, s.f2[SSUN]},
+      HU_{d, s.f2[HU]}, ssvo{d, s.f2[SSVO]}, ssvn{d, s.f2[SSVN]}, HV_{d, s.f2[HV]};
+  V3<R3> ho{d, s.f3[HO]}, hn{d, s.f3[HN]}, huo{d, s.f3[HUO]}, hun{d, s.f3[HUN]}, hvo{d, s.f3[HVO]}, hvn{d, s.f3[HVN]};
+  const double kmaxm1 = 1.0 / (double)(float)d.kmax;
+  {
+    const R3 a = R3((sseo(i, j) + H(i, j)) * kmaxm1), b = R3((ssen(i, j) + H(i, j)) * kmaxm1);
+    for (int k = 0; k <= d.kmax; ++k) {
+      ho(i, j, k) = a;
+      hn(i, j, k) = b;
+    }
+  }
+  if (i <= d.imax + HALO - 1) {
+    const R3 a = R3((ssuo(i, j) + HU_(i, j)) * kmaxm1), b = R3((ssun(i, j) + HU_(i, j)) * kmaxm1);
+    for (int k = 0; k <= d.kmax; ++k) {
+      huo(i, j, k) = a;
+      hun(i, j, k) = b;
+    }
+  }
+  if (j <= d.jmax + HALO - 1) {
+    const R3 a = R3((ssvo(i, j) + HV_(i, j)) * kmaxm1), b = R3((ssvn(i, j) + HV_(i, j)) * kmaxm1);
+    for (int k = 0; k <= d.kmax; ++k) {
+      hvo(i, j, k) = a;
+      hvn(i, j, k) = b;
+    }
+  }
+}
+
+// ww_momentum_3d.F90:74-106 (kmin = 1): upward continuity integral per wet interior column.
+template <class R3>
+__global__ void k_ww(Dev d, Bc3<R3> s) {
+  GB_IJ_HALO
+  if (i < d.imin || i > d.imax || j < d.jmin || j > d.jmax) return;
+  I2 az{d, s.az};
+  if (az(i, j) != 1) return;
+  V3<R3> ww{d, s.f3[WW]}, hn{d, s.f3[HN]}, ho{d, s.f3[HO]}, uu{d, s.f3[UU]}, vv{d, s.f3[VV]};
+  const R3 dtm1 = R3(1.0 / s.par[P_DT]);
+  const R3 dx = R3(d.dx), dy = R3(d.dy), ard1 = R3(d.ard1);
+  R3 w = ww(i, j, 0);
+  for (int k = 1; k <= d.kmax - 1; ++k) {
+    w = w - (hn(i, j, k) - ho(i, j, k)) * dtm1 -
+        (uu(i, j, k) * dy - uu(i - 1, j, k) * dy + vv(i, j, k) * dx - vv(i, j - 1, k) * dx) * ard1;
+    ww(i, j, k) = w;
+  }
+}
+
+// uv_advect_3d.F90:76-98 (DIR 0, U grid) / :267-289 (DIR 1, V grid): the velocity, transports and
+// heights of the momentum control volumes. One thread per (i,j), levels 1..kmax; wwadv(:,:,0) = 0.
+template <class R3, int DIR>
+__global__ void k_uvadv3d_prep(Dev d, Bc3<R3> s, R3* fadvp, R3* uuadvp, R3* vvadvp, R3* wwadvp, R3* huadvp,
+                               R3* hvadvp) {
+  GB_IJ_HALO
+  V3<R3> uu{d, s.f3[UU]}, vv{d, s.f3[VV]}, ww{d, s.f3[WW]}, ho{d, s.f3[HO]}, hn{d, s.f3[HN]}, hun{d, s.f3[HUN]},
+      hvn{d, s.f3[HVN]};
+  V3<R3> fadv{d, fadvp}, uuadv{d, uuadvp}, vvadv{d, vvadvp}, wwadv{d, wwadvp}, huadv{d, huadvp}, hvadv{d, hvadvp};
+  const R3 half = R3(0.5);
+  if (DIR == 0) {
+    wwadv(i, j, 0) = R3(0);
+    if (i > d.imax + HALO - 1) return;
+    for (int k = 1; k <= d.kmax; ++k) {
+      fadv(i, j, k) = uu(i, j, k) / hun(i, j, k);
+      uuadv(i, j, k) = half * (uu(i, j, k) + uu(i + 1, j, k));
+      vvadv(i, j, k) = half * (vv(i, j, k) + vv(i + 1, j, k));
+      wwadv(i, j, k) = half * (ww(i, j, k) + ww(i + 1, j, k));
+      huadv(i, j, k) = half * (ho(i + 1, j, k) + hn(i + 1, j, k));
+      hvadv(i, j, k) = half * (hvn(i, j, k) + hvn(i + 1, j, k));
+    }
+  } else {
+    if (j > d.jmax + HALO - 1) return;
+    for (int k = 1; k <= d.kmax; ++k) {
+      fadv(i, j, k) = vv(i, j, k) / hvn(i, j, k);
+      uuadv(i, j, k) = half * (uu(i, j, k) + uu(i, j + 1, k));
+      vvadv(i, j, k) = half * (vv(i, j, k) + vv(i, j + 1, k));
+      wwadv(i, j, k) = half * (ww(i, j, k) + ww(i, j + 1, k));
+      huadv(i, j, k) = half * (hun(i, j, k) + hun(i, j + 1, k));
+      hvadv(i, j, k) = half * (ho(i, j + 1, k) + hn(i, j + 1, k));
+    }
+  }
+}
+
+// stresses_3d.F90:50-104 (bottom and surface stresses; FP64 from the bottom layer)
+template <class R3>
+__global__ void k_stresses(Dev d, Bc3<R3> s) {
+  GB_IJ_HALO
+  V3<R3> uu{d, s.f3[UU]}, vv{d, s.f3[VV]}, hun{d, s.f3[HUN]}, hvn{d, s.f3[HVN]};
+  V2 rru{d, s.f2[RRU]}, rrv{d, s.f2[RRV]}, taubx{d, s.f2[TAUBX]}, tauby{d, s.f2[TAUBY]}, taub{d, s.f2[TAUB]},
+      taus{d, s.f2[TAUS]}, tausx{d, s.f2[TAUSX]}, tausy{d, s.f2[TAUSY]};
+  const double rho_0i = 1.0 / s.par[P_RHO_0];
+  if (j >= d.jmin && j <= d.jmax && i >= d.imin - 1 && i <= d.imax)
+    taubx(i, j) = -(double)uu(i, j, 1) / (double)hun(i, j, 1) * rru(i, j);
+  if (j >= d.jmin - 1 && j <= d.jmax && i >= d.imin && i <= d.imax)
+    tauby(i, j) = -(double)vv(i, j, 1) / (double)hvn(i, j, 1) * rrv(i, j);
+  if (j >= d.jmin && j <= d.jmax && i >= d.imin && i <= d.imax) {
+    const double a = (double)uu(i - 1, j, 1) / (double)hun(i - 1, j, 1) * rru(i - 1, j);
+    const double b = (double)uu(i, j, 1) / (double)hun(i, j, 1) * rru(i, j);
+    const double c = (double)vv(i, j - 1, 1) / (double)hvn(i, j - 1, 1) * rrv(i, j - 1);
+    const double e = (double)vv(i, j, 1) / (double)hvn(i, j, 1) * rrv(i, j);
+    taub(i, j) = sqrt(0.5 * (a * a + b * b + c * c + e * e));
+    taus(i, j) = rho_0i * sqrt(tausx(i, j) * tausx(i, j) + tausy(i, j) * tausy(i, j));
+  }
+}
+
+// eqstate.F90:127-137 (linear) + :252-261 (buoyancy), levels 1..kmax over the haloed plane
+template <class R3>
+__global__ void k_eqstate(Dev d, Bc3<R3> s) {
+  GB_IJ_HALO
+  const int k = blockIdx.z + 1;
+  V3<R3> rho{d, s.f3[RHO]}, buoy{d, s.f3[BUOY]}, T{d, s.f3[TT]}, S{d, s.f3[SS]};
+  const R3 rho_0 = R3(s.par[P_RHO_0]), dtr0 = R3(s.par[P_DTR0]), dsr0 = R3(s.par[P_DSR0]), T0 = R3(s.par[P_T0]),
+           S0 = R3(s.par[P_S0]);
+  const R3 x = R3(-s.par[P_G] / s.par[P_RHO_0]);
+  const R3 r = rho_0 + dtr0 * (T(i, j, k) - T0) + dsr0 * (S(i, j, k) - S0);
+  rho(i, j, k) = r;
+  buoy(i, j, k) = x * (r - rho_0);
+}
+
+// slow_terms.F90:57-181 (kmax > 1, kumin = kvmin = 1): vertical sums in FP64
+template <class R3>
+__global__ void k_slow_terms(Dev d, Bc3<R3> s) {
+  GB_IJ_HALO
+  if (i < d.imin || i > d.imax || j < d.jmin || j > d.jmax) return;
+  V2 UEx{d, s.f2[UEX]}, VEx{d, s.f2[VEX]}, SlUx{d, s.f2[SLUX]}, SlVx{d, s.f2[SLVX]}, Slru{d, s.f2[SLRU]},
+      Slrv{d, s.f2[SLRV]}, Uint{d, s.f2[UINT]}, Vint{d, s.f2[VINT]}, ssuo{d, s.f2[SSUO]}, ssun{d, s.f2[SSUN]},
+      ssvo{d, s.f2[SSVO]}, ssvn{d, s.f2[SSVN]}, HU_{d, s.f2[HU]}, HV_{d, s.f2[HV]}, ru{d, s.f2[RU]}, rv{d, s.f2[RV]},
+      rru{d, s.f2[RRU]}, rrv{d, s.f2[RRV]};
+  V3<R3> uuEx{d, s.f3[UUEX]}, vvEx{d, s.f3[VVEX]}, idpdx{d, s.f3[IDPDX]}, idpdy{d, s.f3[IDPDY]}, uu{d, s.f3[UU]},
+      vv{d, s.f3[VV]}, huo{d, s.f3[HUO]}, hun{d, s.f3[HUN]}, hvo{d, s.f3[HVO]}, hvn{d, s.f3[HVN]};
+  I2 au{d, s.au}, av{d, s.av};
+  const double ip_fac = s.par[P_IP_FAC];
+  if (au(i, j) >= 1) {
+    double vs = -UEx(i, j);
+    for (int k = 1; k <= d.kmax; ++k) vs = vs + (double)uuEx(i, j, k) - ip_fac * (double)idpdx(i, j, k);
+    SlUx(i, j) = vs;
+    Slru(i, j) = -Uint(i, j) / (0.5 * (ssuo(i, j) + ssun(i, j)) + HU_(i, j)) * ru(i, j) +
+                 (double)uu(i, j, 1) / (0.5 * ((double)huo(i, j, 1) + (double)hun(i, j, 1))) * rru(i, j);
+  }
+  if (av(i, j) >= 1) {
+    double vs = -VEx(i, j);
+    for (int k = 1; k <= d.kmax; ++k) vs = vs + (double)vvEx(i, j, k) - ip_fac * (double)idpdy(i, j, k);
+    SlVx(i, j) = vs;
+    Slrv(i, j) = -Vint(i, j) / (0.5 * (ssvo(i, j) + ssvn(i, j)) + HV_(i, j)) * rv(i, j) +
+                 (double)vv(i, j, 1) / (0.5 * ((double)hvo(i, j, 1) + (double)hvn(i, j, 1))) * rrv(i, j);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// launchers
+inline dim3 plane_grid(const Dev& d, dim3 blk, int nz = 1) {
+  return dim3((d.ni() + blk.x - 1) / blk.x, (d.nj() + blk.y - 1) / blk.y, nz);
+}
+
+template <class R3>
+int run_bc3(int which, const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* const* scr) {
+  const dim3 blk(32, 4, 1);
+  switch (which) {
+    case BC3_BF3D: k_bf3d<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s); break;
+    case BC3_ZZ: k_zz<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6]); break;
+    case BC3_IP: k_ip<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6]); break;
+    case BC3_UUMOM:
+    case BC3_VVMOM: {
+      const dim3 b2(32, 2, 1);
+      const size_t smem = 2 * (size_t)(d.kmax + 1) * 64 * sizeof(double);
+      dim3 g2((d.imax - d.imin + 1 + 31) / 32, (d.jmax - d.jmin + 1 + 1) / 2, 1);
+      if (which == BC3_UUMOM) {
+        cudaFuncSetAttribute(k_uvmom3d<R3, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        k_uvmom3d<R3, 0><<<g2, b2, smem, st>>>(d, s);
+      } else {
+        cudaFuncSetAttribute(k_uvmom3d<R3, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        k_uvmom3d<R3, 1><<<g2, b2, smem, st>>>(d, s);
+      }
+      break;
+    }
+    case BC3_SIGMA: k_sigma<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s); break;
+    case BC3_WW: k_ww<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s); break;
+    case BC3_UVADV_PREP_U:
+      k_uvadv3d_prep<R3, 0><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[0], scr[1], scr[2], scr[3], scr[4], scr[5]);
+      break;
+    case BC3_UVADV_PREP_V:
+      k_uvadv3d_prep<R3, 1><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[0], scr[1], scr[2], scr[3], scr[4], scr[5]);
+      break;
+    case BC3_STRESSES: k_stresses<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s); break;
+    case BC3_EQSTATE: k_eqstate<R3><<<plane_grid(d, blk, d.kmax), blk, 0, st>>>(d, s); break;
+    case BC3_SLOW_TERMS: k_slow_terms<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s); break;
+    default: return (int)cudaErrorInvalidValue;
+  }
+  return (int)cudaGetLastError();
+}
+
+}  // namespace gb

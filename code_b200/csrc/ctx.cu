@@ -8,58 +8,11 @@
 #include "common.cuh"
 #include "launch.h"
 
-struct getm_ctx {
-  getm_domain dom;
-  gb::Dev dev;
-  cudaStream_t stream = nullptr;
-  int device = 0;
-  uint8_t* planes = nullptr;   // 8 byte masks of init_advection, n2d each (see MaskPlane)
-  int32_t* zmask = nullptr;    // copies of az, au, av (n2d each)
-  bool adv_ready = false;
-  void* scr[3] = {nullptr, nullptr, nullptr};  // 3D scratch: tracer ping-pong, hi, adv
-  size_t scr_bytes = 0;
-  double* red = nullptr;                // reduction partials (2*RED_BLOCKS) + result (2)
-  unsigned long long* cnt = nullptr;    // [0] warnings, [1] range-check count
-  std::string err;
-  // per-stage device timers (the counterpart of getm_timers' tic/toc, getm_timers.F90:275-357)
-  bool timing = false;
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending[GETM_NTIMERS];
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pool;
-  double total_ms[GETM_NTIMERS] = {};
-  long long launches[GETM_NTIMERS] = {};
-};
-
-namespace {
-// Records a CUDA event pair around one launch when timing is enabled.
-struct TimerScope {
-  getm_ctx* c;
-  int slot;
-  std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
-  TimerScope(getm_ctx* c_, int slot_) : c(c_), slot(slot_) {
-    if (!c || !c->timing) return;
-    if (!c->pool.empty()) {
-      ev = c->pool.back();
-      c->pool.pop_back();
-    } else {
-      cudaEventCreate(&ev.first);
-      cudaEventCreate(&ev.second);
-    }
-    cudaEventRecord(ev.first, c->stream);
-  }
-  ~TimerScope() {
-    if (!ev.first) return;
-    cudaEventRecord(ev.second, c->stream);
-    c->pending[slot].push_back(ev);
-  }
-};
-}  // namespace
+#include "ctx_internal.h"
 
 namespace gb {
 
-enum MaskPlane { P_UPDATEH = 0, P_UFLUX, P_VFLUX, P_XFLUX, P_UUPDATEU, P_VUPDATEV, P_UFLUX_U, P_VFLUX_V, NPLANES };
 
-static long long n2d(const Dev& d) { return d.sj * (long long)d.nj(); }
-static long long n3d(const Dev& d) { return d.sk * (long long)(d.kmax + 1); }
 
 // init_advection (advection.F90:263-318) from az/au/av/ax.
 __global__ void k_build_masks(Dev d, const int32_t* __restrict__ az, const int32_t* __restrict__ au,
@@ -94,73 +47,10 @@ int run_build_masks(const Dev& d, cudaStream_t s, const int32_t* az, const int32
 
 using namespace gb;
 
-static int fail(getm_ctx* c, int code, const char* what) {
-  if (c) c->err = what;
-  return code;
-}
-
-static int cuda_fail(getm_ctx* c, int e, const char* where) {
-  if (e == 0) return GETM_OK;
-  if (c) c->err = std::string(where) + ": " + cudaGetErrorString((cudaError_t)e);
-  return GETM_ERR_CUDA;
-}
-
-#define GB_TRY(expr, where)                                   \
-  do {                                                        \
-    int _e = (int)(expr);                                     \
-    if (_e != 0) return cuda_fail(ctx, _e, where);            \
-  } while (0)
-
-#define GB_TIMED(slot, expr, where)                           \
-  do {                                                        \
-    TimerScope _ts(ctx, slot);                                \
-    int _e = (int)(expr);                                     \
-    if (_e != 0) return cuda_fail(ctx, _e, where);            \
-  } while (0)
-
-static int ensure_scratch(getm_ctx* ctx, size_t bytes) {
-  if (ctx->scr_bytes >= bytes) return GETM_OK;
-  for (auto& p : ctx->scr) {
-    if (p) cudaFree(p);
-    p = nullptr;
-  }
-  ctx->scr_bytes = 0;
-  for (auto& p : ctx->scr)
-    if (cudaMalloc(&p, bytes) != cudaSuccess) {
-      cudaGetLastError();
-      return fail(ctx, GETM_ERR_NOMEM, "scratch allocation failed");
-    }
-  ctx->scr_bytes = bytes;
-  return GETM_OK;
-}
-
-static bool grid_for_tag(const getm_ctx* ctx, int tag, getm_adv_grid* g) {
-  const long long n = n2d(ctx->dev);
-  const uint8_t* P = ctx->planes;
-  const int32_t* az = ctx->zmask;
-  const int32_t* au = ctx->zmask + n;
-  const int32_t* av = ctx->zmask + 2 * n;
-  switch (tag) {
-    case GETM_H_TAG:
-    case GETM_D_TAG:
-    case GETM_W_TAG:
-      *g = {P + P_UFLUX * n, P + P_VFLUX * n, P + P_UPDATEH * n, P + P_UPDATEH * n, P + P_UPDATEH * n, az};
-      return true;
-    case GETM_U_TAG:
-      *g = {P + P_UFLUX_U * n, P + P_XFLUX * n, P + P_UUPDATEU * n, P + P_UFLUX * n, P + P_UFLUX * n, au};
-      return true;
-    case GETM_V_TAG:
-      *g = {P + P_XFLUX * n, P + P_VFLUX_V * n, P + P_VFLUX * n, P + P_VUPDATEV * n, P + P_VFLUX * n, av};
-      return true;
-    default:
-      return false;
-  }
-}
-
 // ---------------------------------------------------------------------------------------------
 // do_advection_3d (advection_3d.F90:279-566) on device pointers (level-0 origin).
 template <class R>
-static int do_adv3d(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, const R* hu,
+int do_adv3d(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, const R* hu,
                     const R* hv, const R* ho, const R* hn, int split, int hs, int vs, R AH, int tag, R* hires,
                     R* advres, int iters) {
   (void)hn;
@@ -281,6 +171,13 @@ static int do_adv3d(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R
   return GETM_OK;
 }
 
+template int do_adv3d<double>(getm_ctx*, double, double*, const double*, const double*, const double*,
+                               const double*, const double*, const double*, const double*, int, int, int, double,
+                               int, double*, double*, int);
+template int do_adv3d<float>(getm_ctx*, float, float*, const float*, const float*, const float*, const float*,
+                             const float*, const float*, const float*, int, int, int, float, int, float*, float*,
+                             int);
+
 template <class R>
 static int sweep_h_api(getm_ctx* ctx, int dir, int nk, R dt, const R* f, R* fi, R* Di, R* adv, const R* U,
                        const R* DU, R splitfac, int scheme, R AH, const uint8_t* mflux, const uint8_t* mupd) {
@@ -356,12 +253,12 @@ int getm_ctx_create(const getm_domain* dom, void* stream, getm_ctx** out) {
   if (cudaMalloc(&ctx->planes, (size_t)n * NPLANES) != cudaSuccess ||
       cudaMalloc(&ctx->zmask, (size_t)n * 3 * sizeof(int32_t)) != cudaSuccess ||
       cudaMalloc(&ctx->red, (2 * RED_BLOCKS + 2) * sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&ctx->cnt, 2 * sizeof(unsigned long long)) != cudaSuccess) {
+      cudaMalloc(&ctx->cnt, 4 * sizeof(unsigned long long)) != cudaSuccess) {
     cudaGetLastError();
     getm_ctx_destroy(ctx);
     return GETM_ERR_NOMEM;
   }
-  if (cudaMemsetAsync(ctx->cnt, 0, 2 * sizeof(unsigned long long), ctx->stream) != cudaSuccess) {
+  if (cudaMemsetAsync(ctx->cnt, 0, 4 * sizeof(unsigned long long), ctx->stream) != cudaSuccess) {
     getm_ctx_destroy(ctx);
     return GETM_ERR_CUDA;
   }
@@ -377,6 +274,8 @@ int getm_ctx_destroy(getm_ctx* ctx) {
   cudaFree(ctx->red);
   cudaFree(ctx->cnt);
   for (auto p : ctx->scr) cudaFree(p);
+  cudaFree(ctx->bc_scr3);
+  cudaFree(ctx->bc_scr2);
   for (int t = 0; t < GETM_NTIMERS; ++t)
     for (auto& ev : ctx->pending[t]) ctx->pool.push_back(ev);
   for (auto& ev : ctx->pool) {
@@ -407,8 +306,8 @@ const char* getm_ctx_last_error(const getm_ctx* ctx) { return ctx ? ctx->err.c_s
 
 static const char* kTimerNames[GETM_NTIMERS] = {"adv_split_u", "adv_split_v", "adv_split_w", "adv_finalise",
                                                  "tracer_vdiff", "copy", "tracer_fused_uv",
-                                                 "tracer_fused_wvu", "reserved8", "reserved9", "reserved10",
-                                                 "reserved11", "reserved12", "reserved13", "reserved14",
+                                                 "tracer_fused_wvu", "mode_split_2d", "macro_3d_other", "internal_pressure",
+                                                 "uv_momentum_3d", "reserved12", "reserved13", "reserved14",
                                                  "reserved15"};
 
 const char* getm_timer_name(int slot) {

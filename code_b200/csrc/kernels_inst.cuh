@@ -114,3 +114,9 @@ template int run_check_range<GB_REAL>(const Dev&, cudaStream_t, const GB_REAL*, 
                                       GB_REAL, unsigned long long*);
 
 }  // namespace gb
+
+// ---- mode-split macro step (3D kernels) ----
+#include "bc_kernels.cuh"
+namespace gb {
+template int run_bc3<GB_REAL>(int, const Dev&, cudaStream_t, const Bc3<GB_REAL>&, GB_REAL* const*);
+}  // namespace gb

@@ -47,4 +47,14 @@ int run_check_range(const Dev& d, cudaStream_t s, const R* f, const int32_t* az,
 int run_build_masks(const Dev& d, cudaStream_t s, const int32_t* az, const int32_t* au, const int32_t* av,
                     const int32_t* ax, uint8_t* planes);
 
+// 3D kernels of the macro step (bc_kernels.cuh); scr = the NB3 scratch arrays
+enum {
+  BC3_BF3D = 0, BC3_ZZ, BC3_IP, BC3_UUMOM, BC3_VVMOM, BC3_SIGMA, BC3_WW, BC3_UVADV_PREP_U, BC3_UVADV_PREP_V,
+  BC3_STRESSES, BC3_EQSTATE, BC3_SLOW_TERMS
+};
+template <class R3>
+struct Bc3;
+template <class R3>
+int run_bc3(int which, const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* const* scr);
+
 }  // namespace gb

@@ -76,6 +76,9 @@ _PROTOS = {
     "getm_timers_reset": [P],
     "getm_timers_read": [P, I, P, P],
     "getm_timer_name": [I],
+    "getm_integrate_2d": [P, P, I],
+    "getm_integrate_3d": [P, P, I],
+    "getm_time_loop": [P, P, I, I],
 }
 _RESTYPES = {"getm_ctx_last_error": C.c_char_p, "getm_version": C.c_char_p, "getm_timer_name": C.c_char_p}
 NTIMERS = 16
@@ -239,6 +242,19 @@ class Context:
         self._check(fn(self.h, _ptr(f), _ptr(h), _ptr(az), C.byref(out)))
         return out.value
 
+    # ---- mode-split step ----------------------------------------------------------------------
+    def integrate_2d(self, st: "BcDevice", loop: int):
+        """integrate_2d (m2d.F90:412-490) on a device state."""
+        self._check(self.L.getm_integrate_2d(self.h, C.byref(st.c), loop))
+
+    def integrate_3d(self, st: "BcDevice", n: int):
+        """integrate_3d (m3d.F90:422-636) on a device state."""
+        self._check(self.L.getm_integrate_3d(self.h, C.byref(st.c), n))
+
+    def time_loop(self, st: "BcDevice", n0: int, count: int):
+        """Micro steps n0..n0+count-1 of time_loop (integration.F90:98-172)."""
+        self._check(self.L.getm_time_loop(self.h, C.byref(st.c), n0, count))
+
     def check_3d_fields(self, f, az, minval, maxval) -> int:
         st = C.c_int64()
         self._check(self.L.getm_check_3d_fields(self.h, _ptr(f), _ptr(az), minval, maxval, C.byref(st)))
@@ -261,3 +277,67 @@ def _mask(m):
     if isinstance(m, int):
         return m
     return _ptr(m)
+
+
+class BcState(C.Structure):
+    """Mirror of getm_bc_state (include/getm_b200.h)."""
+
+    _fields_ = [("f2", P * 54), ("f3", P * 19), ("az", P), ("au", P), ("av", P), ("ax", P), ("par", D * 18),
+                ("ipar", C.c_int32 * 19), ("prec3d", C.c_int32)]
+
+
+class BcDevice:
+    """Device copy of a mode-split state (code_b200.state.BcCase) plus its C table."""
+
+    def __init__(self, case=None, dtype3=None, tensors=None, pd=None, pi=None):
+        import torch
+
+        from . import state as S
+
+        if tensors is None:
+            dt3 = dtype3 or (torch.float64 if case.dtype3 == "float64" else torch.float32)
+            t = {}
+            for n in S.F2_NAMES:
+                t["f2_" + n] = torch.from_numpy(case.f2[n]).cuda()
+            for n in S.F3_NAMES:
+                t["f3_" + n] = torch.from_numpy(case.f3[n]).to(dt3).cuda()
+            for n, m in zip(("az", "au", "av", "ax"), case.masks()):
+                t[n] = torch.from_numpy(m).cuda()
+            pd, pi = dict(case.pd), dict(case.pi)
+        self.t = tensors if tensors is not None else t
+        self.pd, self.pi = pd, pi
+        f3dt = self.t["f3_uu"].dtype
+        self.prec = 8 if f3dt == torch.float64 else 4
+        c = BcState()
+        for q, n in enumerate(S.F2_NAMES):
+            c.f2[q] = _ptr(self.t["f2_" + n])
+        for q, n in enumerate(S.F3_NAMES):
+            assert self.t["f3_" + n].dtype == f3dt
+            c.f3[q] = _ptr(self.t["f3_" + n])
+        c.az, c.au, c.av, c.ax = (_ptr(self.t[n]) for n in ("az", "au", "av", "ax"))
+        for q, n in enumerate(S.PD_NAMES):
+            c.par[q] = float(pd[n])
+        for q, n in enumerate(S.PI_NAMES):
+            c.ipar[q] = int(pi[n])
+        c.prec3d = self.prec
+        self.c = c
+
+    def masks(self):
+        return tuple(self.t[n] for n in ("az", "au", "av", "ax"))
+
+    def ipar(self) -> dict:
+        from . import state as S
+
+        return {n: int(self.c.ipar[q]) for q, n in enumerate(S.PI_NAMES)}
+
+    def to_host(self, case):
+        """Copy the device fields back into a BcCase (3D fields cast to the case's dtype)."""
+        from . import state as S
+
+        for n in S.F2_NAMES:
+            case.f2[n][...] = self.t["f2_" + n].cpu().numpy()
+        for n in S.F3_NAMES:
+            case.f3[n][...] = self.t["f3_" + n].cpu().numpy().astype(case.dtype3)
+        for q, n in enumerate(S.PI_NAMES):
+            case.pi[n] = int(self.c.ipar[q])
+        return case

@@ -99,6 +99,10 @@ int getm_ctx_take_warnings(getm_ctx *ctx, int64_t *n_warnings);
 #define GETM_TIM_COPY 5
 #define GETM_TIM_TRACER_UV 6
 #define GETM_TIM_TRACER_WVU 7
+#define GETM_TIM_BC2D 8  /* 2D kernels of the mode-split step */
+#define GETM_TIM_BC3D 9  /* other 3D kernels of the macro step */
+#define GETM_TIM_IP 10   /* internal pressure */
+#define GETM_TIM_MOM3D 11 /* uu/vv_momentum_3d */
 #define GETM_NTIMERS 16
 int getm_timers_enable(getm_ctx *ctx, int on);
 int getm_timers_reset(getm_ctx *ctx);
@@ -172,6 +176,51 @@ int getm_tracer_step_f32(getm_ctx *ctx, float dt, float *f, const float *uu, con
                          const float *ww, const float *hu, const float *hv, const float *ho,
                          const float *hn, const float *nuh, int split, int hscheme, int vscheme,
                          float AH, float cnpar, float avmol, int adv_ver_iterations);
+
+/* ---- the mode-split time step ----------------------------------------------------------- */
+/* The module state that integrate_2d / integrate_3d read and write (variables_2d, variables_3d,
+ * domain and the m2d/m3d/temperature/salinity/eqstate settings of the reference) as one table of
+ * DEVICE pointers. 2D fields are FP64 (E2DFIELD); 3D fields (I3DFIELD) are FP64 when prec3d = 8
+ * (the plain FP64 step) or FP32 when prec3d = 4 (the mixed-precision step, whose 2D substeps,
+ * transport accumulation Uint/Vint and all vertical sums stay FP64). The table order is:
+ *  f2:  z zo U V D DU DV UEx VEx fU fV ru rv ruu rvv Uint Vint Uinto Vinto SlUx SlVx Slru Slrv
+ *       zub zvb zub0 zvb0 fwf H HU HV dry_z dry_u dry_v coru corv tausx tausy airp sseo ssen
+ *       ssuo ssun ssvo ssvn Dn Dun Dvn rru rrv taubx tauby taub taus
+ *  f3:  uu vv ww ho hn huo hun hvo hvn uuEx vvEx idpdx idpdy T S rho buoy num nuh
+ *  par: dtm dt cnpar min_depth crit_depth g rho_0 kappa avmmol avmolt avmols T0 S0 dtr0 dsr0
+ *       ip_fac temp_AH salt_AH
+ *  ipar: M MM runtype vel2d_adv_split vel2d_adv_hor vel3d_adv_split vel3d_adv_hor
+ *       vel3d_adv_ver temp_adv_split temp_adv_hor temp_adv_ver salt_adv_split salt_adv_hor
+ *       salt_adv_ver adv_ver_iterations ufirst2d ufirst3d calc_temp calc_salt
+ * ufirst2d / ufirst3d are the SAVEd alternation switches of momentum.F90:33 (initially 0) and
+ * m3d.F90:504 (initially 1); the calls update them in the host-side struct. */
+#define GETM_NF2 54
+#define GETM_NF3 19
+#define GETM_NPD 18
+#define GETM_NPI 19
+typedef struct getm_bc_state {
+  double *f2[GETM_NF2];
+  void *f3[GETM_NF3];
+  const int32_t *az, *au, *av, *ax;
+  double par[GETM_NPD];
+  int32_t ipar[GETM_NPI];
+  int32_t prec3d; /* bytes per 3D element: 8 or 4 */
+} getm_bc_state;
+
+/* integrate_2d (src/2d/m2d.F90:412-490): one barotropic micro step -- bottom_friction (every MM
+ * steps), uv_advect, momentum (alternating u/v order), Uint/Vint accumulation, sealevel and
+ * depth_update. Closed boundaries (no update_2d_bdy), Am <= 0, An_method = 0, no residual. */
+int getm_integrate_2d(getm_ctx *ctx, getm_bc_state *st, int loop);
+/* integrate_3d (src/3d/m3d.F90:422-636): one baroclinic macro step for runtype 4 with sigma
+ * coordinates, linear equation of state, Blumberg-Mellor internal pressure and prescribed
+ * num/nuh: start_macro, bottom_friction_3d, internal pressure, uu/vv_momentum_3d, coordinates,
+ * ww_momentum_3d, uv_advect_3d, stresses_3d, do_temperature / do_salinity (advection + implicit
+ * vertical diffusion, no radiation / surface fluxes), do_eqstate, slow_bottom_friction,
+ * uv_advect of Uint/Vint, slow_terms and stop_macro. */
+int getm_integrate_3d(getm_ctx *ctx, getm_bc_state *st, int n);
+/* The micro-step loop of time_loop (src/getm/integration.F90:98-172) for n = n0..n0+count-1:
+ * integrate_2d every step, integrate_3d when mod(n, M) == 0. */
+int getm_time_loop(getm_ctx *ctx, getm_bc_state *st, int n0, int count);
 
 /* ---- diagnostics ----------------------------------------------------------------------- */
 /* Compensated (Neumaier) FP64 sum of f*h/ard1 over wet interior cells (az>=1, k=1..kmax):

@@ -1,0 +1,106 @@
+"""The CUDA mode-split step (getm_time_loop / getm_integrate_2d / getm_integrate_3d) against the
+reference's own integrate_2d / integrate_3d (golden fixture) and against the oracle.
+
+Tolerance (FP64): every field within 1e-12 of the reference, relative to the field's largest
+magnitude. All arithmetic is evaluated in the reference's order without contraction; the one
+source of difference is the natural logarithm of the log-law drag (bottom_friction.F90,
+bottom_friction_3d.F90, slow_bottom_friction.F90), where the device's log and the host's libm
+may differ in the last bit.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from code_b200 import state as S
+from code_b200.getm import BcDevice
+from helpers import make_ctx
+from test_golden_bc_cpu import GOLD, load_case
+
+pytestmark = pytest.mark.gpu
+
+
+def field_err(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    scale = max(float(np.nanmax(np.abs(b))), 1e-300)
+    return float(np.nanmax(np.abs(a - b))) / scale
+
+
+def compare(case_gpu, ref_f2, ref_f3, tol):
+    worst = {}
+    for k in S.F2_NAMES:
+        worst[k] = field_err(case_gpu.f2[k], ref_f2[k])
+    for k in S.F3_NAMES:
+        worst[k] = field_err(case_gpu.f3[k], ref_f3[k])
+    bad = {k: v for k, v in worst.items() if not v <= tol}
+    return bad, worst
+
+
+def run_gpu(c, n0, count, dtype3=None):
+    import torch
+
+    ctx, _ = make_ctx(c)
+    st = BcDevice(c, dtype3=dtype3)
+    ctx.time_loop(st, n0, count)
+    torch.cuda.synchronize()
+    out = c.copy()
+    st.to_host(out)
+    return out, ctx
+
+
+def test_time_loop_vs_reference_fixture():
+    gold = dict(np.load(GOLD))
+    c = load_case(gold)
+    out, _ = run_gpu(c, 1, 8)
+    bad, worst = compare(out, {k: gold["out_f2_" + k] for k in S.F2_NAMES},
+                         {k: gold["out_f3_" + k] for k in S.F3_NAMES}, 1e-12)
+    assert not bad, bad
+
+
+@pytest.mark.parametrize("recipe,nx,ny,kmax", [("shelf", 40, 28, 10), ("islands", 48, 40, 8), ("flat", 33, 21, 6)])
+def test_time_loop_vs_oracle(recipe, nx, ny, kmax):
+    c = S.baroclinic_case(nx=nx, ny=ny, kmax=kmax, recipe=recipe, M=5, dt3=60.0, seed=11, land=0.3)
+    ref = c.copy()
+    oracle.bc_steps(ref, 1, 15)
+    out, ctx = run_gpu(c, 1, 15)
+    assert out.pi["ufirst2d"] == ref.pi["ufirst2d"] and out.pi["ufirst3d"] == ref.pi["ufirst3d"]
+    bad, worst = compare(out, ref.f2, ref.f3, 1e-12)
+    assert not bad, bad
+    assert ctx.take_warnings() == 0
+
+
+def test_integrate_entry_points_match_time_loop():
+    """getm_integrate_2d + getm_integrate_3d called one by one equal getm_time_loop."""
+    import torch
+
+    c = S.baroclinic_case(nx=24, ny=20, kmax=6, recipe="shelf", M=3, seed=5)
+    a, _ = run_gpu(c, 1, 6)
+    ctx, _ = make_ctx(c)
+    st = BcDevice(c)
+    for n in range(1, 7):
+        ctx.integrate_2d(st, n)
+        if n % 3 == 0:
+            ctx.integrate_3d(st, n)
+    torch.cuda.synchronize()
+    b = st.to_host(c.copy())
+    for k in S.F2_NAMES:
+        assert np.array_equal(a.f2[k], b.f2[k], equal_nan=True), k
+    for k in S.F3_NAMES:
+        assert np.array_equal(a.f3[k], b.f3[k], equal_nan=True), k
+
+
+def test_mixed_precision_error_vs_fp64():
+    """The mixed variant (3D fields FP32; 2D, Uint/Vint and vertical sums FP64) against the FP64
+    oracle after 10 macro steps: per-field error relative to the field's scale (stated bounds)."""
+    import torch
+
+    c = S.baroclinic_case(nx=48, ny=40, kmax=10, recipe="shelf", M=10, seed=3)
+    ref = c.copy()
+    oracle.bc_steps(ref, 1, 100)
+    out, _ = run_gpu(c.copy(dtype3=np.float32), 1, 100, dtype3=torch.float32)
+    errs = {k: field_err(out.f2[k], ref.f2[k]) for k in ("z", "U", "V")}
+    errs.update({k: field_err(out.f3[k], ref.f3[k]) for k in ("uu", "vv", "T", "S")})
+    for k in ("T", "S"):
+        assert errs[k] < 1e-5, errs
+    for k in ("z", "U", "V", "uu", "vv"):
+        assert errs[k] < 1e-3, errs
