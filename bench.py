@@ -1,17 +1,21 @@
 #!/usr/bin/env python
-"""Benchmark of the B200 hot path: cell-steps/s of the tracer step, mixed FP32/FP64 vs plain FP64.
+"""Benchmark of the B200 mode-split step: cell-steps/s of the mixed FP32/FP64 baroclinic step
+against the plain FP64 step, on the 2048 x 2048 x 50 irregular domain.
 
-One step = one tracer advection-diffusion step, i.e. do_advection_3d (HALFSPLIT, SUPERBEE in
-u, v and w) followed by the implicit vertical-diffusion solve (the body of do_salinity,
-salinity.F90:301-389), on the rotation recipe (closed flat basin, solid-body rotation, Gaussian
-blob + seeded noise) at 2048 x 2048 x 50. A cell-step is one interior cell advanced by one step.
+Workload (the reference's large irregular-domain configuration): 2048 x 2048 x 50 sigma layers,
+dx = dy = 1 km, seeded land mask of about 30 % (Gaussian-smoothed noise, sigma = 40 cells,
+islands kept), depth 5-150 m, stratified T/S with linear EOS, Blumberg-Mellor internal pressure,
+P2_PDM / HALFSPLIT advection of momentum and tracers, prescribed parabolic viscosity, closed
+boundaries, mode-split ratio M = 20 (dt = 60 s, dtm = 3 s). One STEP = one macro step = 20 micro
+steps (integrate_2d) + one integrate_3d. A cell-step is one of the 2048*2048*50 cells (land
+included) advanced by one step.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
-Prints one JSON line (rank 0). The default arm runs the CUDA library; `--impl reference` times
-the CPU restatement of the reference routines (the oracle, OpenMP over all host cores) on a
-bounded sample of the same workload. Multi-GPU runs (torchrun) are weak-scaled replicas: every
-rank advances its own 2048 x 2048 x 50 basin; the tracer step of a closed basin has no exchange.
+Prints one JSON line (rank 0). `--impl reference` times the CPU restatement of the reference's
+routines (the oracle, OpenMP over the host cores) on a bounded sample of the same workload.
+Multi-GPU runs (torchrun) are weak-scaled replicas: every rank advances its own domain; the
+closed-basin step as configured has no inter-rank exchange.
 """
 from __future__ import annotations
 
@@ -27,21 +31,26 @@ sys.path.insert(0, ROOT)
 
 METRIC = "cell-steps/s mixed-prec vs plain FP64 on 1 B200 at stated err; adjoint/fwd ratio"
 UNIT = "cell-steps/s"
-# algorithmic words per interior cell per launch of each stage (read + write, each field once)
-STAGE_WORDS = {"adv_split_u": 6, "adv_split_v": 6, "adv_split_w": 5, "tracer_vdiff": 4, "adv_finalise": 4,
-               "tracer_fused_uv": 8, "tracer_fused_wvu": 9}
+WORKLOAD = ("mode-split baroclinic step (20 x integrate_2d + integrate_3d: 2D momentum/sealevel, internal "
+            "pressure, 3D momentum with implicit viscosity, P2_PDM advection of u, v, T, S, implicit diffusion), "
+            "2048x2048x50 irregular domain, 30% land, depth 5-150 m")
+# algorithmic words per interior cell per launch of a stage (each field read/written once)
+STAGE_WORDS = {"adv_split_u": 6, "adv_split_v": 6, "adv_split_w": 5, "tracer_vdiff": 4, "uv_momentum_3d": 8,
+               "internal_pressure": 6}
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--nx", type=int, default=2048)
     ap.add_argument("--ny", type=int, default=2048)
     ap.add_argument("--kmax", type=int, default=50)
+    ap.add_argument("--M", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--variants", default="fp64,mixed")
     return ap.parse_args()
 
 
@@ -64,6 +73,7 @@ class ClockSampler:
     def __init__(self, index: int):
         self.index = index
         self.p = None
+        self.out = ""
 
     def __enter__(self):
         try:
@@ -75,7 +85,6 @@ class ClockSampler:
         return self
 
     def __exit__(self, *a):
-        self.out = ""
         if self.p:
             self.p.terminate()
             try:
@@ -86,14 +95,21 @@ class ClockSampler:
 
     def summary(self):
         rows = []
-        for line in (getattr(self, "out", "") or "").strip().splitlines():
+        for line in (self.out or "").strip().splitlines():
             parts = [x.strip() for x in line.split(",")]
             if len(parts) >= 9:
                 rows.append(parts)
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
-        sm = sorted(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
-        mx = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = sorted(v for v in (num(r[1]) for r in rows) if v is not None)
+        mx = max((v for v in (num(r[2]) for r in rows) if v is not None), default=None)
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[q] for r in rows for q in range(4) if r[5 + q].lower() == "active"})
         return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
@@ -101,32 +117,33 @@ class ClockSampler:
 
 
 def dist_setup():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+    return int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def oracle_sample(nx, ny, kmax, M):
+    from code_b200 import state as S
+
+    return S.baroclinic_case(nx=nx, ny=ny, kmax=kmax, recipe="islands", land=0.3, M=M, dt3=60.0, seed=6)
 
 
 def run_reference(args, world, rank):
     """CPU restatement (oracle) on a bounded sample of the workload, all host threads."""
     if rank != 0:
         return
-    import numpy as np
-
     import oracle
-    from code_b200 import cases
 
-    snx, sny = min(args.nx, 1024), min(args.ny, 1024)
-    c = cases.tracer_rotation(nx=snx, ny=sny, kmax=args.kmax, depth=50.0, dx=1000.0, dt=60.0, sigma_cells=32.0)
-    p = c.par
-    o = oracle.Oracle(c.grid)
-    names = ("uu", "vv", "ww", "hun", "hvn", "ho", "hn", "nuh")
-    f = c["f"].copy()
-    arr = [c[n] for n in names]
-    run = lambda n: o.tracer_steps(c.masks(), n, p["dt"], f, *arr, 2, 4, 4, 0.0, 1.0, 0.0)  # noqa: E731
-    run(max(args.warmup, 0))
+    snx = min(args.nx, 256)
+    sny = min(args.ny, 256)
+    c = oracle_sample(snx, sny, args.kmax, args.M)
+    M = args.M
+    n = 1
+    for _ in range(args.warmup):
+        oracle.bc_steps(c, n, M)
+        n += M
     t0 = time.perf_counter()
-    run(args.steps)
+    for _ in range(args.steps):
+        oracle.bc_steps(c, n, M)
+        n += M
     el = time.perf_counter() - t0
     cells = snx * sny * args.kmax
     v = cells * args.steps / el
@@ -135,37 +152,33 @@ def run_reference(args, world, rank):
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "tracer step (do_advection_3d HALFSPLIT SUPERBEE + implicit vertical diffusion), "
-                               "rotation recipe, closed flat basin", "nx": args.nx, "ny": args.ny,
-                   "kmax": args.kmax, "sample": f"{snx}x{sny}x{args.kmax} per step"},
+        "config": {"workload": WORKLOAD, "nx": args.nx, "ny": args.ny, "kmax": args.kmax, "M": M,
+                   "sample": f"{snx}x{sny}x{args.kmax} islands domain per step"},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{snx}x{sny}x{args.kmax}, {args.steps} steps after {args.warmup} warm-up"},
+                         "sample": f"oracle FP64 mode-split step on {snx}x{sny}x{args.kmax}, {args.steps} macro steps "
+                                   f"after {args.warmup} warm-up"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
 
 def cpu_baseline_sample(args):
     import oracle
-    from code_b200 import cases
 
-    snx, sny = min(args.nx, 1024), min(args.ny, 512)
-    c = cases.tracer_rotation(nx=snx, ny=sny, kmax=args.kmax, depth=50.0, dx=1000.0, dt=60.0, sigma_cells=32.0)
-    p = c.par
-    o = oracle.Oracle(c.grid)
-    names = ("uu", "vv", "ww", "hun", "hvn", "ho", "hn", "nuh")
-    f = c["f"].copy()
-    arr = [c[n] for n in names]
-    o.tracer_steps(c.masks(), 1, p["dt"], f, *arr, 2, 4, 4, 0.0, 1.0, 0.0)
-    n, t0 = 0, time.perf_counter()
+    snx, sny = min(args.nx, 256), min(args.ny, 256)
+    c = oracle_sample(snx, sny, args.kmax, args.M)
+    oracle.bc_steps(c, 1, args.M)
+    n, steps, t0 = 1 + args.M, 0, time.perf_counter()
     while True:
-        o.tracer_steps(c.masks(), 1, p["dt"], f, *arr, 2, 4, 4, 0.0, 1.0, 0.0)
-        n += 1
+        oracle.bc_steps(c, n, args.M)
+        n += args.M
+        steps += 1
         el = time.perf_counter() - t0
-        if el > 10.0 or n >= 50:
+        if el > 10.0 or steps >= 20:
             break
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return {"value": snx * sny * args.kmax * n / el, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"oracle FP64 tracer step on {snx}x{sny}x{args.kmax}, {n} steps ({el:.1f} s)"}
+    return {"value": snx * sny * args.kmax * steps / el, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"oracle FP64 mode-split step on {snx}x{sny}x{args.kmax} (islands), {steps} macro steps "
+                      f"({el:.1f} s)"}
 
 
 def main():
@@ -177,7 +190,7 @@ def main():
     import torch
     import torch.distributed as dist
 
-    from code_b200 import cases
+    from code_b200 import state as S
     from code_b200.getm import Context
 
     torch.cuda.set_device(local)
@@ -199,77 +212,88 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    names = ("uu", "vv", "ww", "hun", "hvn", "ho", "hn", "nuh")
-    res = {}
-    variants = {}
-    for key, dt_ in (("fp64", torch.float64), ("mixed", torch.float32)):
-        g, fld, par = cases.tracer_rotation_device(args.nx, args.ny, args.kmax, dtype=dt_, seed=1 + rank)
-        ctx = Context(g, stream)
-        ctx.init_advection(fld["az"], fld["au"], fld["av"], fld["ax"])
-        variants[key] = (g, fld, par, ctx)
-    steps_done = {}
-
-    def step(key):
-        g, fld, par, ctx = variants[key]
-        cast = float
-        ctx.tracer_step(cast(par["dt"]), fld["f"], *[fld[n] for n in names], 2, 4, 4, 0.0, 1.0, 0.0)
-        steps_done[key] = steps_done.get(key, 0) + 1
-
+    M = args.M
     cells = args.nx * args.ny * args.kmax
+    variants = {}
+    wanted = args.variants.split(",")
+    for key, dt3 in (("fp64", torch.float64), ("mixed", torch.float32)):
+        if key not in wanted:
+            continue
+        g, st = S.baroclinic_case_device(args.nx, args.ny, args.kmax, recipe="islands", land=0.3, M=M, dt3=60.0,
+                                         seed=6 + rank, dtype3=dt3)
+        ctx = Context(g, stream)
+        ctx.init_advection(*st.masks())
+        variants[key] = dict(g=g, st=st, ctx=ctx, n=1)
+
+    def macro_step(key):
+        v = variants[key]
+        v["ctx"].time_loop(v["st"], v["n"], M)
+        v["n"] += M
+
+    res = {}
     clocks = None
-    for key in ("fp64", "mixed"):
+    for key in variants:
         for _ in range(args.warmup):
-            step(key)
+            macro_step(key)
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with ClockSampler(local) as cs:
             e0.record(stream)
             for _ in range(args.steps):
-                step(key)
+                macro_step(key)
             e1.record(stream)
             barrier()
         ms = max_over_ranks(e0.elapsed_time(e1))
         res[key] = {"ms": ms, "value": world * cells * args.steps / (ms / 1e3)}
-        if key == "mixed":
+        if key == "mixed" or clocks is None:
             clocks = cs.summary()
-    # stated error of the mixed variant against FP64 after the same number of steps
-    f64 = variants["fp64"][1]["f"]
-    f32 = variants["mixed"][1]["f"]
+    # stated error of the mixed variant against the FP64 run after the same number of steps
     err = None
-    if steps_done["fp64"] == steps_done["mixed"]:
-        d = (f32.double() - f64).abs()
-        err = {"field": "tracer", "max_abs": float(d.max()), "rms": float(d.pow(2).mean().sqrt()),
-               "amplitude": float(f64.abs().max()), "steps": steps_done["fp64"]}
-    # per-stage timers over K more steps of the mixed variant (dominant kernel roofline)
-    ctx = variants["mixed"][3]
-    ctx.timers(enable=True, reset=True)
+    if "fp64" in variants and "mixed" in variants and variants["fp64"]["n"] == variants["mixed"]["n"]:
+        err = {"steps": (variants["fp64"]["n"] - 1) // M, "relative_to": "max |field| of the FP64 run"}
+        for name in ("f3_T", "f3_S", "f3_uu", "f3_vv", "f2_z", "f2_U", "f2_V"):
+            a = variants["fp64"]["st"].t[name]
+            b = variants["mixed"]["st"].t[name].double()
+            scale = float(a.abs().max())
+            d = (a - b).abs()
+            err[name[3:]] = {"max": float(d.max()) / max(scale, 1e-300),
+                             "rms": float(d.pow(2).mean().sqrt()) / max(scale, 1e-300)}
+    head = "mixed" if "mixed" in variants else "fp64"
+    v = variants[head]
+    # per-stage device timers over K more steps of the headline variant (dominant kernel roofline)
+    v["ctx"].timers(enable=True, reset=True)
     for _ in range(args.steps):
-        step("mixed")
+        macro_step(head)
     torch.cuda.synchronize()
-    tim = ctx.timers(enable=False, reset=True)
+    tim = v["ctx"].timers(enable=False, reset=True)
     launches = sum(n for _, n in tim.values())
-    top = max(tim.items(), key=lambda kv: kv[1][0])
-    top_name, (top_ms, top_n) = top
-    wb = 4
-    alg_bytes = STAGE_WORDS.get(top_name, 0) * cells * wb
+    timed = {k: t for k, t in tim.items() if k in STAGE_WORDS}
+    top_name, (top_ms, top_n) = max(timed.items(), key=lambda kv: kv[1][0])
+    wb = 4 if head == "mixed" else 8
+    alg_bytes = STAGE_WORDS[top_name] * cells * wb
     peak, peak_kind = load_peaks()
     achieved = alg_bytes / (top_ms / top_n / 1e3) / 1e9
-    # end-to-end through the C ABI with host buffers: per step H2D of the tracer, step, D2H
-    g, fld, par, ctx = variants["mixed"]
-    hbuf = torch.empty_like(fld["f"], device="cpu").pin_memory()
-    hbuf.copy_(fld["f"])
+    # whole-step algorithmic bytes (3D: read+write uu, vv, T, S; 2D: 17 FP64 words per column per micro step)
+    step_bytes = (8 * wb) * cells + 17 * 8 * args.nx * args.ny * M
+    # end to end through the C ABI with host buffers: per step the 2D forcing (tausx, tausy, airp) is
+    # uploaded from pinned host memory and the new elevation z read back
+    st = v["st"]
+    hf = {n: torch.empty_like(st.t["f2_" + n], device="cpu").pin_memory() for n in ("tausx", "tausy", "airp", "z")}
+    for n in ("tausx", "tausy", "airp"):
+        hf[n].copy_(st.t["f2_" + n])
     barrier()
-    k2 = max(3, args.steps // 4)
+    k2 = max(3, args.steps // 2)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(k2):
-        fld["f"].copy_(hbuf, non_blocking=True)
-        step("mixed")
-        hbuf.copy_(fld["f"], non_blocking=True)
+        for n in ("tausx", "tausy", "airp"):
+            st.t["f2_" + n].copy_(hf[n], non_blocking=True)
+        macro_step(head)
+        hf["z"].copy_(st.t["f2_z"], non_blocking=True)
     e1.record(stream)
     barrier()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1))
-    nbytes = fld["f"].numel() * fld["f"].element_size()
+    n2b = st.t["f2_z"].numel() * 8
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -278,30 +302,32 @@ def main():
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {ex}"}
     if rank == 0:
         out = {
-            "metric": METRIC, "value": res["mixed"]["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": res["mixed"]["ms"] / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-            "config": {"workload": "tracer step (do_advection_3d HALFSPLIT SUPERBEE + implicit vertical diffusion), "
-                                   "rotation recipe, closed flat basin", "nx": args.nx, "ny": args.ny,
-                       "kmax": args.kmax, "l2": "inputs larger than L2 (FP32 field 0.84 GB, FP64 1.7 GB)",
-                       "parallelism": f"replicas x{world}"},
-            "plain_fp64": {"value": res["fp64"]["value"], "ms_per_step": res["fp64"]["ms"] / args.steps},
-            "mixed_over_fp64": res["mixed"]["value"] / res["fp64"]["value"],
+            "metric": METRIC, "value": res[head]["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": res[head]["ms"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if head == "mixed" else "f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "nx": args.nx, "ny": args.ny, "kmax": args.kmax, "M": M,
+                       "l2": "inputs larger than L2 (one FP32 3D field 0.86 GB)", "parallelism": f"replicas x{world}"},
+            "plain_fp64": ({"value": res["fp64"]["value"], "ms_per_step": res["fp64"]["ms"] / args.steps}
+                           if "fp64" in res else None),
+            "mixed_over_fp64": (res["mixed"]["value"] / res["fp64"]["value"]) if len(res) == 2 else None,
             "err_vs_fp64": err,
             "adjoint_fwd_ratio": None,
             "gpu_launches": launches,
-            "stage_ms_per_step": {k: v[0] / args.steps for k, v in tim.items()},
+            "stage_ms_per_step": {k: t[0] / args.steps for k, t in tim.items()},
             "roofline": {"bound": "hbm", "kernel": top_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
-                         "alg_bytes_per_launch": alg_bytes},
-            "e2e": {"value": world * cells * k2 / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
-                    "d2h_bytes_per_step": nbytes},
+                         "alg_bytes_per_launch": alg_bytes,
+                         "step_alg_bytes": step_bytes,
+                         "step_frac": step_bytes / (res[head]["ms"] / args.steps / 1e3) / 1e9 / peak},
+            "e2e": {"value": world * cells * k2 / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": 3 * n2b,
+                    "d2h_bytes_per_step": n2b},
             "clocks": clocks,
             "cpu_baseline": cpu,
         }
         print(json.dumps(out), flush=True)
     for key in variants:
-        variants[key][3].close()
+        variants[key]["ctx"].close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -392,25 +392,25 @@ int do_adv2d(getm_ctx* ctx, double dt, double* f, const double* U, const double*
   switch (split) {
     case GETM_NOSPLIT:
       GB_TRY(cudaMemcpyAsync(S, f, b2, cudaMemcpyDeviceToDevice, s), "copy f");
-      GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<double, 0>(d, s, 1, dt, one, scheme, 0.0, f, S, S, Di, Di, A, U, DUa,
+      GB_TIMED(GETM_TIM_BC2D, (run_sweep_h<double, 0>(d, s, 1, dt, one, scheme, 0.0, f, S, S, Di, Di, A, U, DUa,
                                                         g.mask_uflux, g.mask_uupdate)), "u");
-      GB_TIMED(GETM_TIM_ADV_V, (run_sweep_h<double, 1>(d, s, 1, dt, one, scheme, 0.0, f, S, S, Di, Di, A, V, DVa,
+      GB_TIMED(GETM_TIM_BC2D, (run_sweep_h<double, 1>(d, s, 1, dt, one, scheme, 0.0, f, S, S, Di, Di, A, V, DVa,
                                                         g.mask_vflux, g.mask_vupdate)), "v");
       k_finalise2d<<<grid2(d), kBlk2, 0, s>>>(d, dt, f, Do, A, Di, g.mask_finalise);
       GB_TRY(cudaGetLastError(), "finalise2d");
       break;
     case GETM_FULLSPLIT:
-      GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<double, 0>(d, s, 1, dt, one, scheme, 0.0, f, f, S, Di, Di, A, U, DUa,
+      GB_TIMED(GETM_TIM_BC2D, (run_sweep_h<double, 0>(d, s, 1, dt, one, scheme, 0.0, f, f, S, Di, Di, A, U, DUa,
                                                         g.mask_uflux, g.mask_uupdate)), "u");
-      GB_TIMED(GETM_TIM_ADV_V, (run_sweep_h<double, 1>(d, s, 1, dt, one, scheme, 0.0, S, S, f, Di, Di, A, V, DVa,
+      GB_TIMED(GETM_TIM_BC2D, (run_sweep_h<double, 1>(d, s, 1, dt, one, scheme, 0.0, S, S, f, Di, Di, A, V, DVa,
                                                         g.mask_vflux, g.mask_vupdate)), "v");
       break;
     case GETM_HALFSPLIT:
-      GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<double, 0>(d, s, 1, dt, half, scheme, 0.0, f, f, S, Di, Di, A, U, DUa,
+      GB_TIMED(GETM_TIM_BC2D, (run_sweep_h<double, 0>(d, s, 1, dt, half, scheme, 0.0, f, f, S, Di, Di, A, U, DUa,
                                                         g.mask_uflux, g.mask_uupdate)), "u");
-      GB_TIMED(GETM_TIM_ADV_V, (run_sweep_h<double, 1>(d, s, 1, dt, one, scheme, 0.0, S, S, f, Di, Di, A, V, DVa,
+      GB_TIMED(GETM_TIM_BC2D, (run_sweep_h<double, 1>(d, s, 1, dt, one, scheme, 0.0, S, S, f, Di, Di, A, V, DVa,
                                                         g.mask_vflux, g.mask_vupdate)), "v");
-      GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<double, 0>(d, s, 1, dt, half, scheme, 0.0, f, f, S, Di, Di, A, U, DUa,
+      GB_TIMED(GETM_TIM_BC2D, (run_sweep_h<double, 0>(d, s, 1, dt, half, scheme, 0.0, f, f, S, Di, Di, A, U, DUa,
                                                         g.mask_uflux, g.mask_uupdate)), "u");
       GB_TRY(cudaMemcpyAsync(f, S, b2, cudaMemcpyDeviceToDevice, s), "copy back");
       break;
@@ -513,7 +513,7 @@ int integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
   GB_K2(k_start_macro_uv, d, s2, 1.0 / (double)(float)ip[I_M]);
   if (d.kmax > 1 && (rc = bc3<R3>(ctx, st, BC3_BF3D, GETM_TIM_BC3D))) return rc;
   if (ip[I_RUNTYPE] == 4) {
-    if ((rc = bc3<R3>(ctx, st, BC3_ZZ, GETM_TIM_IP))) return rc;
+    if ((rc = bc3<R3>(ctx, st, BC3_ZZ, GETM_TIM_BC3D))) return rc;
     if ((rc = bc3<R3>(ctx, st, BC3_IP, GETM_TIM_IP))) return rc;
   }
   {

@@ -318,10 +318,15 @@ __global__ void __launch_bounds__(64) k_vdiff(Dev d, R dt, R cnpar, R avmol, R* 
   int k = kmax;
   R ao_km1 = auxo(k - 1), an_km1 = auxn(k - 1);
   R Sk = L(S, k), Skm1 = L(S, k - 1);
+  // FP64 solves the reference's system for the new value. FP32 solves the same matrix for the
+  // increment dS = S_new - S_old, whose right-hand side is the flux divergence at the old level,
+  // (ao+an)(k)*(S(k+1)-S(k)) - (ao+an)(k-1)*(S(k)-S(k-1)) [+ src]; the rounding then acts on the
+  // small increment rather than on h*S (bias-free over hundreds of steps).
+  constexpr bool incr = sizeof(R) == 4;
   {
     const R a1 = -an_km1;
     const R a2 = L(hn, k) + an_km1;
-    R a4 = Sk * (L(hn, k) - ao_km1) + Skm1 * ao_km1;
+    R a4 = incr ? -(ao_km1 + an_km1) * (Sk - Skm1) : Sk * (L(hn, k) - ao_km1) + Skm1 * ao_km1;
     if (src) a4 = a4 + L(src, k);
     sm.RU(k) = a1 / a2;
     sm.QU(k) = a4 / a2;
@@ -337,7 +342,8 @@ __global__ void __launch_bounds__(64) k_vdiff(Dev d, R dt, R cnpar, R avmol, R* 
     const R a3 = -an_k;
     const R a1 = -an_km1;
     const R a2 = L(hn, k) + an_k + an_km1;
-    R a4 = Skp1 * ao_k + Sk * (L(hn, k) - ao_k - ao_km1) + Skm1 * ao_km1;
+    R a4 = incr ? (ao_k + an_k) * (Skp1 - Sk) - (ao_km1 + an_km1) * (Sk - Skm1)
+                : Skp1 * ao_k + Sk * (L(hn, k) - ao_k - ao_km1) + Skm1 * ao_km1;
     if (src) a4 = a4 + L(src, k);
     const R den = a2 - a3 * sm.RU(k + 1);
     sm.RU(k) = a1 / den;
@@ -351,15 +357,15 @@ __global__ void __launch_bounds__(64) k_vdiff(Dev d, R dt, R cnpar, R avmol, R* 
     const R S1 = Skm1;  // S(1)
     const R a3 = -an_k;
     const R a2 = L(hn, 1) + an_k;
-    R a4 = Skp1 * ao_k + S1 * (L(hn, 1) - ao_k);
+    R a4 = incr ? (ao_k + an_k) * (Skp1 - S1) : Skp1 * ao_k + S1 * (L(hn, 1) - ao_k);
     if (src) a4 = a4 + L(src, 1);
     sm.QU(1) = (a4 - a3 * sm.QU(2)) / (a2 - a3 * sm.RU(2));
   }
   R v = sm.QU(1);
-  S[c + 1 * sk] = v;
+  S[c + 1 * sk] = incr ? L(S, 1) + v : v;
   for (k = 2; k <= kmax; ++k) {
     v = sm.QU(k) - sm.RU(k) * v;
-    S[c + k * sk] = v;
+    S[c + k * sk] = incr ? L(S, k) + v : v;
   }
 }
 

@@ -38,11 +38,11 @@ P2_PDM, HALFSPLIT = 6, 2
 class BcCase:
     """A full model state (numpy arrays in the reference layout) with parameters."""
 
-    def __init__(self, grid: Grid, dtype3=np.float64):
+    def __init__(self, grid: Grid, dtype3=np.float64, alloc3=True):
         self.grid = grid
         self.dtype3 = np.dtype(dtype3)
         self.f2 = {n: np.zeros(grid.shape2()) for n in F2_NAMES}
-        self.f3 = {n: np.zeros(grid.shape3(), dtype=self.dtype3) for n in F3_NAMES}
+        self.f3 = {n: np.zeros(grid.shape3(), dtype=self.dtype3) for n in F3_NAMES} if alloc3 else {}
         self.az = self.au = self.av = self.ax = None
         self.pd = {n: 0.0 for n in PD_NAMES}
         self.pi = {n: 0 for n in PI_NAMES}
@@ -83,9 +83,16 @@ def baroclinic_case(nx=32, ny=24, kmax=8, recipe="shelf", dx=1000.0, M=20, dt3=6
     (+1e-6) over the sigma levels. Coriolis on an f-plane at `latitude` (domain.F90:364-369 with the
     reference's single-precision omega = 2*pi/86164).
     """
+    c, rng = _baroclinic_2d(nx, ny, kmax, recipe, dx, M, dt3, seed, dtype3, land, hmin, hmax, latitude, True)
+    _baroclinic_3d_numpy(c, rng, nu_max)
+    return c
+
+
+def _baroclinic_2d(nx, ny, kmax, recipe, dx, M, dt3, seed, dtype3, land, hmin, hmax, latitude, alloc3):
+    """The 2D part of :func:`baroclinic_case` (masks, depths, elevations, parameters)."""
     g = Grid(nx, ny, kmax, dx, dx)
     rng = np.random.default_rng(seed)
-    c = BcCase(g, dtype3)
+    c = BcCase(g, dtype3, alloc3=alloc3)
     i = np.arange(g.imin - HALO, g.imax + HALO + 1)
     xT = (i - g.imin + 0.5) * dx
     az = np.zeros(g.shape2(), np.int32)
@@ -173,6 +180,25 @@ def baroclinic_case(nx=32, ny=24, kmax=8, recipe="shelf", dx=1000.0, M=20, dt3=6
     f2["Dn"][...] = f2["ssen"] + H
     f2["Dun"][...] = f2["ssun"] + f2["HU"]
     f2["Dvn"][...] = f2["ssvn"] + f2["HV"]
+    return c, rng
+
+
+def _profiles(kmax, nu_max):
+    """1D vertical profiles: depth fraction of layer centres (0 at the surface, 1 at the bottom)
+    and the parabolic viscosity at the interfaces."""
+    sig = (np.arange(kmax + 1) - 0.5) / kmax
+    depth_frac = 1.0 - sig
+    s = np.arange(kmax + 1) / kmax
+    nu = 4 * nu_max * s * (1 - s) + 1e-6
+    return depth_frac, nu
+
+
+def _baroclinic_3d_numpy(c: BcCase, rng, nu_max):
+    g = c.grid
+    kmax = g.kmax
+    f2 = c.f2
+    H = f2["H"]
+    az = c.az
     # layer heights (sigma_coordinates, all levels)
     f3 = c.f3
     f3["ho"][...] = ((f2["sseo"] + H) / kmax)[None]
@@ -182,8 +208,8 @@ def baroclinic_case(nx=32, ny=24, kmax=8, recipe="shelf", dx=1000.0, M=20, dt3=6
     f3["hvo"][...] = ((f2["ssvo"] + f2["HV"]) / kmax)[None]
     f3["hvn"][...] = ((f2["ssvn"] + f2["HV"]) / kmax)[None]
     # stratification on sigma levels: depth of layer centre
-    sig = (np.arange(kmax + 1) - 0.5) / kmax  # centre of layer k as fraction of depth from bottom
-    depth_frac = (1.0 - sig)[:, None, None]  # 0 at surface, 1 at bottom
+    depth_frac, nu = _profiles(kmax, nu_max)
+    depth_frac = depth_frac[:, None, None]
     T = 20.0 - 12.0 * depth_frac + 0.1 * rng.normal(size=g.shape3())
     S = 30.0 + 5.0 * depth_frac + np.zeros(g.shape3())
     T[0] = 0.0
@@ -192,12 +218,65 @@ def baroclinic_case(nx=32, ny=24, kmax=8, recipe="shelf", dx=1000.0, M=20, dt3=6
     f3["T"][...] = np.where(wet3, T, 0.0)
     f3["S"][...] = np.where(wet3, S, 0.0)
     # viscosity / diffusivity at interfaces k (between layers k and k+1): sigma_k = k/kmax
-    s = np.arange(kmax + 1) / kmax
-    nu = 4 * nu_max * s * (1 - s) + 1e-6
     f3["num"][...] = nu[:, None, None]
     f3["nuh"][...] = nu[:, None, None]
     _eqstate(c)
-    return c
+
+
+def baroclinic_case_device(nx=2048, ny=2048, kmax=50, recipe="islands", dx=1000.0, M=20, dt3=60.0, seed=6,
+                           dtype3=None, land=0.3, hmin=5.0, hmax=150.0, nu_max=1e-2, latitude=54.0, device="cuda"):
+    """:func:`baroclinic_case` with the 3D fields built on the device (for the 2048 x 2048 x 50
+    domain, whose 19 FP64 3D fields would take ~33 GB of host memory). 2D fields and parameters
+    are computed in numpy exactly as in baroclinic_case; the temperature noise comes from a seeded
+    device generator. Returns a code_b200.getm.BcDevice."""
+    import torch
+
+    from .getm import BcDevice
+
+    dtype3 = dtype3 or torch.float64
+    c, _ = _baroclinic_2d(nx, ny, kmax, recipe, dx, M, dt3, seed, np.float64, land, hmin, hmax, latitude, False)
+    g = c.grid
+    kmax = g.kmax
+    t = {}
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)  # noqa: E731
+    for n in F2_NAMES:
+        t["f2_" + n] = dev(c.f2[n])
+    for n, m in zip(("az", "au", "av", "ax"), c.masks()):
+        t[n] = dev(m)
+    f2 = c.f2
+    shp = g.shape3()
+    ones = torch.ones((kmax + 1, 1, 1), dtype=torch.float64, device=device)
+
+    def level_const(a2):
+        return (ones * dev(a2)[None]).to(dtype3).contiguous()
+
+    t["f3_ho"] = level_const((f2["sseo"] + f2["H"]) / kmax)
+    t["f3_hn"] = level_const((f2["ssen"] + f2["H"]) / kmax)
+    t["f3_huo"] = level_const((f2["ssuo"] + f2["HU"]) / kmax)
+    t["f3_hun"] = level_const((f2["ssun"] + f2["HU"]) / kmax)
+    t["f3_hvo"] = level_const((f2["ssvo"] + f2["HV"]) / kmax)
+    t["f3_hvn"] = level_const((f2["ssvn"] + f2["HV"]) / kmax)
+    depth_frac, nu = _profiles(kmax, nu_max)
+    dfr = dev(depth_frac)[:, None, None]
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    wet = dev((c.az >= 1).astype(np.float64))[None]
+    T = (20.0 - 12.0 * dfr + 0.1 * torch.randn(shp, generator=gen, device=device, dtype=torch.float64)) * wet
+    S = (30.0 + 5.0 * dfr + torch.zeros(shp, dtype=torch.float64, device=device)) * wet
+    T[0] = 0.0
+    S[0] = 0.0
+    p = c.pd
+    rho = p["rho_0"] + p["dtr0"] * (T - p["T0"]) + p["dsr0"] * (S - p["S0"])
+    rho[0] = 0.0
+    buoy = (-p["g"] / p["rho_0"]) * (rho - p["rho_0"])
+    buoy[0] = 0.0
+    t["f3_T"], t["f3_S"], t["f3_rho"], t["f3_buoy"] = (x.to(dtype3).contiguous() for x in (T, S, rho, buoy))
+    nuv = dev(nu)[:, None, None] * torch.ones(shp, dtype=torch.float64, device=device)
+    t["f3_num"] = nuv.to(dtype3).contiguous()
+    t["f3_nuh"] = nuv.to(dtype3).contiguous()
+    for n in ("uu", "vv", "ww", "uuEx", "vvEx", "idpdx", "idpdy"):
+        t["f3_" + n] = torch.zeros(shp, dtype=dtype3, device=device)
+    return g, BcDevice(tensors=t, pd=dict(c.pd), pi=dict(c.pi))
 
 
 # -------------------------------------------------------------------------------------------------

@@ -431,6 +431,7 @@ void ip_blumberg_mellor(const Dom& d, BcState<R3>& st) {
         for (int k = 2; k <= kmax; ++k) zz(i, j, k) = zz(i, j, k - 1) + hn(i, j, k);
       }
   const R3 half = R3(0.5);
+#pragma omp parallel for schedule(static)
   for (int j = d.jmin; j <= d.jmax; ++j)
     for (int i = d.imin; i <= d.imax; ++i)
       if (au(i, j) >= 1) {
@@ -448,6 +449,7 @@ void ip_blumberg_mellor(const Dom& d, BcState<R3>& st) {
           idpdx(i, j, k) = hun(i, j, k) * prgr;
         }
       }
+#pragma omp parallel for schedule(static)
   for (int j = d.jmin; j <= d.jmax; ++j)
     for (int i = d.imin; i <= d.imax; ++i)
       if (av(i, j) >= 1) {
@@ -486,9 +488,10 @@ void uv_momentum_3d(const Dom& d, BcState<R3>& st, int dir) {
   const double gammai = 1.0 / gamma, rho_0i = 1.0 / rho_0;
   const int di = dir == 0 ? 1 : 0, dj = dir == 0 ? 0 : 1;
   const double dxy = dir == 0 ? d.dx : d.dy;
-  std::vector<double> dif(kmax + 1), auxn(kmax + 1), auxo(kmax + 1), a1(kmax + 1), a2(kmax + 1), a3(kmax + 1),
-      a4(kmax + 1), Res(kmax + 1), ex(kmax + 1);
-  for (int j = d.jmin; j <= d.jmax; ++j)
+#pragma omp parallel for schedule(static)
+  for (int j = d.jmin; j <= d.jmax; ++j) {
+    std::vector<double> dif(kmax + 1), auxn(kmax + 1), auxo(kmax + 1), a1(kmax + 1), a2(kmax + 1),
+        a3(kmax + 1), a4(kmax + 1), Res(kmax + 1), ex(kmax + 1);
     for (int i = d.imin; i <= d.imax; ++i) {
       if (!(mask(i, j) == 1 || mask(i, j) == 2)) continue;
       const int kmn = 1;
@@ -546,6 +549,7 @@ void uv_momentum_3d(const Dom& d, BcState<R3>& st, int dir) {
         uu(i, j, kmax) = R3(Uint(i, j));
       }
     }
+  }
 }
 
 // sigma_coordinates.F90:85-113 (equidistant), all levels 0..kmax
@@ -557,6 +561,7 @@ void sigma_coordinates(const Dom& d, BcState<R3>& st) {
   A3<R3> ho{d, st.f3[HO]}, hn{d, st.f3[HN]}, huo{d, st.f3[HUO]}, hun{d, st.f3[HUN]}, hvo{d, st.f3[HVO]},
       hvn{d, st.f3[HVN]};
   const double kmaxm1 = 1.0 / (double)(float)d.kmax;
+#pragma omp parallel for schedule(static)
   for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
     for (int i = d.imin - HALO; i <= d.imax + HALO; ++i) {
       const R3 a = R3((sseo(i, j) + H(i, j)) * kmaxm1), b = R3((ssen(i, j) + H(i, j)) * kmaxm1);
@@ -591,6 +596,7 @@ void ww_momentum_3d(const Dom& d, BcState<R3>& st) {
   const R3 dtm1 = R3(1.0 / st.par[P_DT]);
   const R3 dx = R3(d.dx), dy = R3(d.dy), ard1 = R3(d.ard1);
   for (int k = 1; k <= d.kmax - 1; ++k)
+#pragma omp parallel for schedule(static)
     for (int j = d.jmin; j <= d.jmax; ++j)
       for (int i = d.imin; i <= d.imax; ++i)
         if (az(i, j) == 1)
@@ -613,6 +619,7 @@ int uv_advect_3d(const Dom& d, const AdvMasks& m, BcState<R3>& st) {
   const R3 half = R3(0.5);
   for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
     for (int i = d.imin - HALO; i <= d.imax + HALO; ++i) wwadv(i, j, 0) = R3(0);
+#pragma omp parallel for schedule(static)
   for (int k = 1; k <= d.kmax; ++k)
     for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
       for (int i = d.imin - HALO; i <= d.imax + HALO - 1; ++i) {
@@ -628,6 +635,7 @@ int uv_advect_3d(const Dom& d, const AdvMasks& m, BcState<R3>& st) {
                           hva_.data(), st.f3[HUN], st.f3[HUN], split, hor, ver, R3(0), U_TAG, nullptr, st.f3[UUEX],
                           ip[I_ADV_VER_ITERS]) < 0)
     return -1;
+#pragma omp parallel for schedule(static)
   for (int k = 1; k <= d.kmax; ++k)
     for (int j = d.jmin - HALO; j <= d.jmax + HALO - 1; ++j)
       for (int i = d.imin - HALO; i <= d.imax + HALO; ++i) {
@@ -676,11 +684,13 @@ void do_eqstate(const Dom& d, BcState<R3>& st) {
   const double* par = st.par;
   const R3 rho_0 = R3(par[P_RHO_0]), dtr0 = R3(par[P_DTR0]), dsr0 = R3(par[P_DSR0]), T0 = R3(par[P_T0]),
            S0 = R3(par[P_S0]);
+#pragma omp parallel for schedule(static)
   for (int k = 1; k <= d.kmax; ++k)
     for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
       for (int i = d.imin - HALO; i <= d.imax + HALO; ++i)
         rho(i, j, k) = rho_0 + dtr0 * (T(i, j, k) - T0) + dsr0 * (S(i, j, k) - S0);
   const R3 x = R3(-par[P_G] / par[P_RHO_0]);
+#pragma omp parallel for schedule(static)
   for (int k = 1; k <= d.kmax; ++k)
     for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
       for (int i = d.imin - HALO; i <= d.imax + HALO; ++i) buoy(i, j, k) = x * (rho(i, j, k) - rho_0);
