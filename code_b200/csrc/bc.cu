@@ -76,34 +76,44 @@ __global__ void k_bottom_friction(Dev d, Bc2 s, int runtype) {
   }
 }
 
-// uv_advect.F90:94-110 (U grid) / :204-220 (V grid): quantities of the 2D momentum volumes.
-template <int DIR>
+// uv_advect.F90:94-110 (U grid) / :204-220 (V grid): quantities of the 2D momentum volumes, in
+// the working type T of the 2D advection (FP64 in the plain step, FP32 in the mixed step), plus
+// the control-volume depth Do (= DU or DV) in T.
+template <int DIR, class T>
 __global__ void k_uvadv2d_prep(Dev d, const double* Up, const double* Vp, const double* DUp, const double* DVp,
-                               double* fadvp, double* Uadvp, double* Vadvp, double* DUadvp, double* DVadvp) {
+                               T* fadv, T* Uadv, T* Vadv, T* DUadv, T* DVadv, T* Do) {
   GB_IJ2
   W2 U{d, const_cast<double*>(Up)}, V{d, const_cast<double*>(Vp)}, DU_{d, const_cast<double*>(DUp)},
-      DV_{d, const_cast<double*>(DVp)}, fadv{d, fadvp}, Uadv{d, Uadvp}, Vadv{d, Vadvp}, DUadv{d, DUadvp},
-      DVadv{d, DVadvp};
+      DV_{d, const_cast<double*>(DVp)};
+  const long long c = d.ix(i, j);
+  if (Do) Do[c] = T(DIR == 0 ? DU_(i, j) : DV_(i, j));
   if (DIR == 0) {
     if (i > d.imax + HALO - 1) return;
-    fadv(i, j) = U(i, j) / DU_(i, j);
-    Uadv(i, j) = 0.5 * (U(i, j) + U(i + 1, j));
-    Vadv(i, j) = 0.5 * (V(i, j) + V(i + 1, j));
-    DUadv(i, j) = 0.5 * (DU_(i, j) + DU_(i + 1, j));
-    DVadv(i, j) = 0.5 * (DV_(i, j) + DV_(i + 1, j));
+    fadv[c] = T(U(i, j) / DU_(i, j));
+    Uadv[c] = T(0.5 * (U(i, j) + U(i + 1, j)));
+    Vadv[c] = T(0.5 * (V(i, j) + V(i + 1, j)));
+    DUadv[c] = T(0.5 * (DU_(i, j) + DU_(i + 1, j)));
+    DVadv[c] = T(0.5 * (DV_(i, j) + DV_(i + 1, j)));
   } else {
     if (j > d.jmax + HALO - 1) return;
-    fadv(i, j) = V(i, j) / DV_(i, j);
-    Uadv(i, j) = 0.5 * (U(i, j) + U(i, j + 1));
-    Vadv(i, j) = 0.5 * (V(i, j) + V(i, j + 1));
-    DUadv(i, j) = 0.5 * (DU_(i, j) + DU_(i, j + 1));
-    DVadv(i, j) = 0.5 * (DV_(i, j) + DV_(i, j + 1));
+    fadv[c] = T(V(i, j) / DV_(i, j));
+    Uadv[c] = T(0.5 * (U(i, j) + U(i, j + 1)));
+    Vadv[c] = T(0.5 * (V(i, j) + V(i, j + 1)));
+    DUadv[c] = T(0.5 * (DU_(i, j) + DU_(i, j + 1)));
+    DVadv[c] = T(0.5 * (DV_(i, j) + DV_(i, j + 1)));
   }
 }
 
+// FP32 advective increments of the mixed step widened into the FP64 UEx / VEx
+__global__ void k_widen2d(Dev d, const float* a, double* out) {
+  GB_IJ2
+  const long long c = d.ix(i, j);
+  out[c] = (double)a[c];
+}
+
 // NOSPLIT finaliser of the 2D driver (advection.F90:500-507)
-__global__ void k_finalise2d(Dev d, double dt, double* f, const double* Do, const double* adv, const double* Di,
-                             const uint8_t* mfin) {
+template <class T>
+__global__ void k_finalise2d(Dev d, T dt, T* f, const T* Do, const T* adv, const T* Di, const uint8_t* mfin) {
   GB_IJ2
   const long long c = d.ix(i, j);
   if (mfin[c]) f[c] = (Do[c] * f[c] - dt * adv[c]) / Di[c];
@@ -371,48 +381,48 @@ int ensure_bc_scratch(getm_ctx* ctx, size_t elem3) {
   return GETM_OK;
 }
 
-// do_advection (advection.F90:362-702) on 2D FP64 fields, split schemes. Di and adv come from the
-// 2D scratch when the caller passes none.
-int do_adv2d(getm_ctx* ctx, double dt, double* f, const double* U, const double* V, const double* DUa,
-             const double* DVa, const double* Do, int split, int scheme, int tag, double* advres) {
+// do_advection (advection.F90:362-702) on 2D fields of type T, split schemes, with advres:
+// p_Di starts as Do (read by the first sweep), p_adv = 0. f is a work field of the caller: when
+// need_f is false its final value is not produced (uv_advect only keeps the increments).
+template <class T>
+int do_adv2d(getm_ctx* ctx, T dt, T* f, const T* U, const T* V, const T* DUa, const T* DVa, const T* Do, int split,
+             int scheme, int tag, T* A, T* Di, T* S, bool need_f) {
   const Dev& d = ctx->dev;
   cudaStream_t s = ctx->stream;
   const long long n2 = n2d(d);
-  const size_t b2 = (size_t)n2 * sizeof(double);
-  double* Di = ctx->bc_scr2 + 5 * n2;
-  double* A = advres ? advres : ctx->bc_scr2 + 6 * n2;
-  double* S = ctx->bc_scr2 + 7 * n2;
+  const size_t b2 = (size_t)n2 * sizeof(T);
   getm_adv_grid g;
   if (!grid_for_tag(ctx, tag, &g)) return fail(ctx, GETM_ERR_ARG, "do_advection: tag is invalid");
-  GB_TRY(cudaMemcpyAsync(Di, Do, b2, cudaMemcpyDeviceToDevice, s), "copy Do");
   GB_TRY(cudaMemsetAsync(A, 0, b2, s), "zero adv");
   if (scheme == NOADV) return GETM_OK;
   if (!is_split_scheme(scheme)) return fail(ctx, GETM_ERR_UNSUPPORTED, "do_advection: 2DH schemes not provided");
-  const double one = 1.0, half = 0.5;
+  const T one = T(1), half = T(0.5), zero = T(0);
   switch (split) {
     case GETM_NOSPLIT:
       GB_TRY(cudaMemcpyAsync(S, f, b2, cudaMemcpyDeviceToDevice, s), "copy f");
-      GB_TIMED(GETM_TIM_BC2D, (run_sweep_h<double, 0>(d, s, 1, dt, one, scheme, 0.0, f, S, S, Di, Di, A, U, DUa,
-                                                        g.mask_uflux, g.mask_uupdate)), "u");
-      GB_TIMED(GETM_TIM_BC2D, (run_sweep_h<double, 1>(d, s, 1, dt, one, scheme, 0.0, f, S, S, Di, Di, A, V, DVa,
-                                                        g.mask_vflux, g.mask_vupdate)), "v");
-      k_finalise2d<<<grid2(d), kBlk2, 0, s>>>(d, dt, f, Do, A, Di, g.mask_finalise);
-      GB_TRY(cudaGetLastError(), "finalise2d");
+      GB_TIMED(GETM_TIM_BC2D, (run_sweep_h<T, 0>(d, s, 1, dt, one, scheme, zero, f, S, S, Do, Di, A, U, DUa,
+                                                  g.mask_uflux, g.mask_uupdate)), "u");
+      GB_TIMED(GETM_TIM_BC2D, (run_sweep_h<T, 1>(d, s, 1, dt, one, scheme, zero, f, S, S, Di, Di, A, V, DVa,
+                                                  g.mask_vflux, g.mask_vupdate)), "v");
+      if (need_f) {
+        k_finalise2d<T><<<grid2(d), kBlk2, 0, s>>>(d, dt, f, Do, A, Di, g.mask_finalise);
+        GB_TRY(cudaGetLastError(), "finalise2d");
+      }
       break;
     case GETM_FULLSPLIT:
-      GB_TIMED(GETM_TIM_BC2D, (run_sweep_h<double, 0>(d, s, 1, dt, one, scheme, 0.0, f, f, S, Di, Di, A, U, DUa,
-                                                        g.mask_uflux, g.mask_uupdate)), "u");
-      GB_TIMED(GETM_TIM_BC2D, (run_sweep_h<double, 1>(d, s, 1, dt, one, scheme, 0.0, S, S, f, Di, Di, A, V, DVa,
-                                                        g.mask_vflux, g.mask_vupdate)), "v");
+      GB_TIMED(GETM_TIM_BC2D, (run_sweep_h<T, 0>(d, s, 1, dt, one, scheme, zero, f, f, S, Do, Di, A, U, DUa,
+                                                  g.mask_uflux, g.mask_uupdate)), "u");
+      GB_TIMED(GETM_TIM_BC2D, (run_sweep_h<T, 1>(d, s, 1, dt, one, scheme, zero, S, S, f, Di, Di, A, V, DVa,
+                                                  g.mask_vflux, g.mask_vupdate)), "v");
       break;
     case GETM_HALFSPLIT:
-      GB_TIMED(GETM_TIM_BC2D, (run_sweep_h<double, 0>(d, s, 1, dt, half, scheme, 0.0, f, f, S, Di, Di, A, U, DUa,
-                                                        g.mask_uflux, g.mask_uupdate)), "u");
-      GB_TIMED(GETM_TIM_BC2D, (run_sweep_h<double, 1>(d, s, 1, dt, one, scheme, 0.0, S, S, f, Di, Di, A, V, DVa,
-                                                        g.mask_vflux, g.mask_vupdate)), "v");
-      GB_TIMED(GETM_TIM_BC2D, (run_sweep_h<double, 0>(d, s, 1, dt, half, scheme, 0.0, f, f, S, Di, Di, A, U, DUa,
-                                                        g.mask_uflux, g.mask_uupdate)), "u");
-      GB_TRY(cudaMemcpyAsync(f, S, b2, cudaMemcpyDeviceToDevice, s), "copy back");
+      GB_TIMED(GETM_TIM_BC2D, (run_sweep_h<T, 0>(d, s, 1, dt, half, scheme, zero, f, f, S, Do, Di, A, U, DUa,
+                                                  g.mask_uflux, g.mask_uupdate)), "u");
+      GB_TIMED(GETM_TIM_BC2D, (run_sweep_h<T, 1>(d, s, 1, dt, one, scheme, zero, S, S, f, Di, Di, A, V, DVa,
+                                                  g.mask_vflux, g.mask_vupdate)), "v");
+      GB_TIMED(GETM_TIM_BC2D, (run_sweep_h<T, 0>(d, s, 1, dt, half, scheme, zero, f, f, S, Di, Di, A, U, DUa,
+                                                  g.mask_uflux, g.mask_uupdate)), "u");
+      if (need_f) GB_TRY(cudaMemcpyAsync(f, S, b2, cudaMemcpyDeviceToDevice, s), "copy back");
       break;
     default:
       return fail(ctx, GETM_ERR_ARG, "do_advection: split is invalid");
@@ -420,35 +430,56 @@ int do_adv2d(getm_ctx* ctx, double dt, double* f, const double* U, const double*
   return GETM_OK;
 }
 
-// uv_advect.F90:94-300 on (U, V, DU, DV) -> UEx, VEx (split schemes).
-int uv_advect_2d(getm_ctx* ctx, const getm_bc_state* st, const double* U, const double* V, const double* DU_,
-                 const double* DV_) {
+// uv_advect.F90:94-300 on (U, V, DU, DV) -> UEx, VEx (split schemes). The plain step works in
+// FP64 (bit for bit with the reference); the mixed step advects the depth-averaged momentum in
+// FP32 and widens the increments into the FP64 UEx / VEx.
+template <class T>
+int uv_advect_2d_t(getm_ctx* ctx, const getm_bc_state* st, const double* U, const double* V, const double* DU_,
+                   const double* DV_) {
   const Dev& d = ctx->dev;
   cudaStream_t s = ctx->stream;
   const long long n2 = n2d(d);
   const int split = st->ipar[I_VEL2D_SPLIT], hor = st->ipar[I_VEL2D_HOR];
-  double* UEx = st->f2[UEX];
-  double* VEx = st->f2[VEX];
+  double* Ex[2] = {st->f2[UEX], st->f2[VEX]};
   if (hor == NOADV) {
-    GB_TRY(cudaMemsetAsync(UEx, 0, n2 * sizeof(double), s), "UEx=0");
-    GB_TRY(cudaMemsetAsync(VEx, 0, n2 * sizeof(double), s), "VEx=0");
+    GB_TRY(cudaMemsetAsync(Ex[0], 0, n2 * sizeof(double), s), "UEx=0");
+    GB_TRY(cudaMemsetAsync(Ex[1], 0, n2 * sizeof(double), s), "VEx=0");
     return GETM_OK;
   }
-  double* w = ctx->bc_scr2;
-  double *fadv = w, *Uadv = w + n2, *Vadv = w + 2 * n2, *DUadv = w + 3 * n2, *DVadv = w + 4 * n2;
-  {
-    TimerScope ts(ctx, GETM_TIM_BC2D);
-    k_uvadv2d_prep<0><<<grid2(d), kBlk2, 0, s>>>(d, U, V, DU_, DV_, fadv, Uadv, Vadv, DUadv, DVadv);
-    GB_TRY(cudaGetLastError(), "uv_advect prep U");
+  // 2D scratch (NB2 FP64-sized arrays) viewed as T
+  T* w = (T*)ctx->bc_scr2;
+  T *fadv = w, *Uadv = w + n2, *Vadv = w + 2 * n2, *DUadv = w + 3 * n2, *DVadv = w + 4 * n2, *Di = w + 5 * n2,
+    *S = w + 6 * n2, *Do = w + 7 * n2;
+  constexpr bool is64 = sizeof(T) == 8;
+  for (int dir = 0; dir < 2; ++dir) {
+    T* A = is64 ? (T*)Ex[dir] : w + 8 * n2;
+    {
+      TimerScope ts(ctx, GETM_TIM_BC2D);
+      if (dir == 0)
+        k_uvadv2d_prep<0, T><<<grid2(d), kBlk2, 0, s>>>(d, U, V, DU_, DV_, fadv, Uadv, Vadv, DUadv, DVadv,
+                                                         is64 ? nullptr : Do);
+      else
+        k_uvadv2d_prep<1, T><<<grid2(d), kBlk2, 0, s>>>(d, U, V, DU_, DV_, fadv, Uadv, Vadv, DUadv, DVadv,
+                                                         is64 ? nullptr : Do);
+      GB_TRY(cudaGetLastError(), "uv_advect prep");
+    }
+    const T* Dsrc = is64 ? (const T*)(dir == 0 ? DU_ : DV_) : Do;
+    int rc = do_adv2d<T>(ctx, T(st->par[P_DTM]), fadv, Uadv, Vadv, DUadv, DVadv, Dsrc, split, hor,
+                         dir == 0 ? GETM_U_TAG : GETM_V_TAG, A, Di, S, false);
+    if (rc) return rc;
+    if (!is64) {
+      TimerScope ts(ctx, GETM_TIM_BC2D);
+      k_widen2d<<<grid2(d), kBlk2, 0, s>>>(d, (const float*)A, Ex[dir]);
+      GB_TRY(cudaGetLastError(), "widen");
+    }
   }
-  int rc = do_adv2d(ctx, st->par[P_DTM], fadv, Uadv, Vadv, DUadv, DVadv, DU_, split, hor, GETM_U_TAG, UEx);
-  if (rc) return rc;
-  {
-    TimerScope ts(ctx, GETM_TIM_BC2D);
-    k_uvadv2d_prep<1><<<grid2(d), kBlk2, 0, s>>>(d, U, V, DU_, DV_, fadv, Uadv, Vadv, DUadv, DVadv);
-    GB_TRY(cudaGetLastError(), "uv_advect prep V");
-  }
-  return do_adv2d(ctx, st->par[P_DTM], fadv, Uadv, Vadv, DUadv, DVadv, DV_, split, hor, GETM_V_TAG, VEx);
+  return GETM_OK;
+}
+
+int uv_advect_2d(getm_ctx* ctx, const getm_bc_state* st, const double* U, const double* V, const double* DU_,
+                 const double* DV_) {
+  return st->prec3d == 8 ? uv_advect_2d_t<double>(ctx, st, U, V, DU_, DV_)
+                         : uv_advect_2d_t<float>(ctx, st, U, V, DU_, DV_);
 }
 
 #define GB_K2(kernel, ...)                                         \
@@ -557,7 +588,8 @@ int integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
                              nullptr, nullptr, ip[I_ADV_VER_ITERS])))
         return rc;
       GB_TIMED(GETM_TIM_VDIFF, run_vdiff<R3>(d, s, dt, R3(st->par[P_CNPAR]), R3(st->par[P_AVMOLT]), f3[TT], f3[HN],
-                                             f3[NUH], st->az, (const R3*)nullptr), "vdiff T");
+                                             f3[NUH], st->az, (const R3*)nullptr, (R3*)ctx->scr[0], (R3*)ctx->scr[1]),
+               "vdiff T");
     }
     if (ip[I_CALC_SALT]) {
       if ((rc = do_adv3d<R3>(ctx, dt, f3[SS], f3[UU], f3[VV], f3[WW], f3[HUN], f3[HVN], f3[HO], f3[HN],
@@ -565,7 +597,8 @@ int integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
                              nullptr, nullptr, ip[I_ADV_VER_ITERS])))
         return rc;
       GB_TIMED(GETM_TIM_VDIFF, run_vdiff<R3>(d, s, dt, R3(st->par[P_CNPAR]), R3(st->par[P_AVMOLS]), f3[SS], f3[HN],
-                                             f3[NUH], st->az, (const R3*)nullptr), "vdiff S");
+                                             f3[NUH], st->az, (const R3*)nullptr, (R3*)ctx->scr[0], (R3*)ctx->scr[1]),
+               "vdiff S");
     }
     if ((rc = bc3<R3>(ctx, st, BC3_EQSTATE, GETM_TIM_BC3D))) return rc;
   }

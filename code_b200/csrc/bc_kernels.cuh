@@ -129,16 +129,14 @@ __global__ void k_ip(Dev d, Bc3<R3> s, const R3* zzp) {
 }
 
 // uu_momentum_3d.F90:169-304 (DIR 0) / vv_momentum_3d.F90:174-315 (DIR 1), kumin = 1: explicit
-// terms, implicit vertical viscosity (Thomas solve with ru/qu in shared memory, column per thread)
-// and the transport correction to the depth-integrated transport Uint. Arithmetic in FP64.
+// terms, implicit vertical viscosity and the transport correction to the depth-integrated
+// transport Uint. One thread per column, arithmetic in FP64. The elimination carries ru(k+1),
+// qu(k+1) in registers and stores ru(k), qu(k) in two scratch 3D arrays (RUs, QUs, type R3: exact
+// for FP64) so that occupancy is not limited by shared memory; the back substitution overwrites
+// QUs with Res(k) and the last pass writes uu = Res + hn*Diff.
 template <class R3, int DIR>
-__global__ void __launch_bounds__(64) k_uvmom3d(Dev d, Bc3<R3> s) {
-  extern __shared__ double smem_d[];
+__global__ void __launch_bounds__(128) k_uvmom3d(Dev d, Bc3<R3> s, R3* RUs, R3* QUs) {
   const int kmax = d.kmax;
-  const int nt = blockDim.x * blockDim.y;
-  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-  double* RU = smem_d;                    // [k][tid]
-  double* QU = smem_d + (kmax + 1) * nt;  // [k][tid]
   const int i = blockIdx.x * blockDim.x + threadIdx.x + d.imin;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + d.jmin;
   if (i > d.imax || j > d.jmax) return;
@@ -146,7 +144,7 @@ __global__ void __launch_bounds__(64) k_uvmom3d(Dev d, Bc3<R3> s) {
   if (!(mask(i, j) == 1 || mask(i, j) == 2)) return;
   V3<R3> uu{d, s.f3[DIR == 0 ? UU : VV]}, vv{d, s.f3[DIR == 0 ? VV : UU]}, ho{d, s.f3[DIR == 0 ? HUO : HVO]},
       hn{d, s.f3[DIR == 0 ? HUN : HVN]}, Ex{d, s.f3[DIR == 0 ? UUEX : VVEX]}, idp{d, s.f3[DIR == 0 ? IDPDX : IDPDY]},
-      num{d, s.f3[NUM]};
+      num{d, s.f3[NUM]}, RU{d, RUs}, QU{d, QUs};
   V2 dry{d, s.f2[DIR == 0 ? DRY_U : DRY_V]}, cor{d, s.f2[DIR == 0 ? CORU : CORV]},
       taus{d, s.f2[DIR == 0 ? TAUSX : TAUSY]}, sseo{d, s.f2[SSEO]}, H{d, s.f2[HH]}, D{d, s.f2[D_]},
       airp{d, s.f2[AIRP]}, rr{d, s.f2[DIR == 0 ? RRU : RRV]}, Uint{d, s.f2[DIR == 0 ? UINT : VINT]},
@@ -160,6 +158,7 @@ __global__ void __launch_bounds__(64) k_uvmom3d(Dev d, Bc3<R3> s) {
   }
   const double gamma = g * rho_0;
   const double gammai = 1.0 / gamma, rho_0i = 1.0 / rho_0;
+  const double dryij = dry(i, j), corij = cor(i, j);
   auto HO = [&](int k) { return (double)ho(i, j, k); };
   auto HN = [&](int k) { return (double)hn(i, j, k); };
   auto UU_ = [&](int k) { return (double)uu(i, j, k); };
@@ -167,18 +166,17 @@ __global__ void __launch_bounds__(64) k_uvmom3d(Dev d, Bc3<R3> s) {
     double loc, e;
     if (DIR == 0) {
       loc = 0.25 * ((double)vv(i, j, k) + (double)vv(i + 1, j, k) + (double)vv(i, j - 1, k) + (double)vv(i + 1, j - 1, k));
-      e = cor(i, j) * loc;
+      e = corij * loc;
     } else {
       loc = 0.25 * ((double)vv(i, j, k) + (double)vv(i - 1, j, k) + (double)vv(i, j + 1, k) + (double)vv(i - 1, j + 1, k));
-      e = -cor(i, j) * loc;
+      e = -corij * loc;
     }
-    double x = dry(i, j) * (e - (double)Ex(i, j, k) + ip_fac * (double)idp(i, j, k));
-    if (k == kmax) x = x + dry(i, j) * 0.5 * (taus(i, j) + taus(i + di, j + dj)) * rho_0i;
+    double x = dryij * (e - (double)Ex(i, j, k) + ip_fac * (double)idp(i, j, k));
+    if (k == kmax) x = x + dryij * 0.5 * (taus(i, j) + taus(i + di, j + dj)) * rho_0i;
     return x;
   };
   auto dif = [&](int k) { return 0.5 * ((double)num(i, j, k) + (double)num(i + di, j + dj, k)) + avmmol; };
-  auto auxo = [&](int k) { return 2.0 * (1.0 - cnpar) * dt * dif(k) / (HO(k + 1) + HO(k)); };
-  auto auxn = [&](int k) { return 2.0 * cnpar * dt * dif(k) / (HN(k + 1) + HN(k)); };
+  const double c_o = 2.0 * (1.0 - cnpar) * dt, c_n = 2.0 * cnpar * dt;
   const double zp = fmax(sseo(i + di, j + dj), -H(i, j) + fmin(min_depth, D(i + di, j + dj)));
   const double zm = fmax(sseo(i, j), -H(i + di, j + dj) + fmin(min_depth, D(i, j)));
   double zx;
@@ -186,50 +184,63 @@ __global__ void __launch_bounds__(64) k_uvmom3d(Dev d, Bc3<R3> s) {
     zx = (zp - zm + (airp(i + 1, j) - airp(i, j)) * gammai) / d.dx;
   else
     zx = (zp - zm + (airp(i, j + 1) - airp(i, j)) / gamma) / d.dy;
-  // surface row (lt = kmax)
+  // column window: heights and velocity at k-1, k, k+1
   int k = kmax;
-  double ao_km1 = auxo(k - 1), an_km1 = auxn(k - 1);
+  double hok = HO(k), hnk = HN(k), hokm1 = HO(k - 1), hnkm1 = HN(k - 1);
+  double uk = UU_(k), ukm1 = UU_(k - 1), ukp1 = 0.0, hokp1 = 0.0, hnkp1 = 0.0;
+  double difk = dif(k - 1);
+  double ao_km1 = c_o * difk / (hok + hokm1), an_km1 = c_n * difk / (hnk + hnkm1);
+  double ru, qu;
   {
-    const double a1 = -an_km1 / HN(k - 1);
-    const double a2 = 1. + an_km1 / HN(k);
-    const double a4 = UU_(k) * (1 - ao_km1 / HO(k)) + UU_(k - 1) * ao_km1 / HO(k - 1) + dt * exk(k) -
-                      dt * 0.5 * (HO(k) + HN(k)) * g * zx;
-    RU[k * nt + tid] = a1 / a2;
-    QU[k * nt + tid] = a4 / a2;
+    const double a1 = -an_km1 / hnkm1;
+    const double a2 = 1. + an_km1 / hnk;
+    const double a4 = uk * (1 - ao_km1 / hok) + ukm1 * ao_km1 / hokm1 + dt * exk(k) - dt * 0.5 * (hok + hnk) * g * zx;
+    ru = a1 / a2;
+    qu = a4 / a2;
+    RU(i, j, k) = R3(ru);
+    QU(i, j, k) = R3(qu);
   }
   for (k = kmax - 1; k >= 2; --k) {
     const double ao_k = ao_km1, an_k = an_km1;
-    ao_km1 = auxo(k - 1);
-    an_km1 = auxn(k - 1);
-    const double a3 = -an_k / HN(k + 1);
-    const double a1 = -an_km1 / HN(k - 1);
-    const double a2 = 1.0 + (an_k + an_km1) / HN(k);
-    const double a4 = UU_(k + 1) * ao_k / HO(k + 1) + UU_(k) * (1 - (ao_k + ao_km1) / HO(k)) +
-                      UU_(k - 1) * ao_km1 / HO(k - 1) + dt * exk(k) - dt * 0.5 * (HO(k) + HN(k)) * g * zx;
-    const double den = a2 - a3 * RU[(k + 1) * nt + tid];
-    RU[k * nt + tid] = a1 / den;
-    QU[k * nt + tid] = (a4 - a3 * QU[(k + 1) * nt + tid]) / den;
+    hokp1 = hok; hnkp1 = hnk; ukp1 = uk;
+    hok = hokm1; hnk = hnkm1; uk = ukm1;
+    hokm1 = HO(k - 1); hnkm1 = HN(k - 1); ukm1 = UU_(k - 1);
+    difk = dif(k - 1);
+    ao_km1 = c_o * difk / (hok + hokm1);
+    an_km1 = c_n * difk / (hnk + hnkm1);
+    const double a3 = -an_k / hnkp1;
+    const double a1 = -an_km1 / hnkm1;
+    const double a2 = 1.0 + (an_k + an_km1) / hnk;
+    const double a4 = ukp1 * ao_k / hokp1 + uk * (1 - (ao_k + ao_km1) / hok) + ukm1 * ao_km1 / hokm1 + dt * exk(k) -
+                      dt * 0.5 * (hok + hnk) * g * zx;
+    const double den = a2 - a3 * ru;
+    ru = a1 / den;
+    qu = (a4 - a3 * qu) / den;
+    RU(i, j, k) = R3(ru);
+    QU(i, j, k) = R3(qu);
   }
+  double v;
   {
     k = 1;
     const double ao_k = ao_km1, an_k = an_km1;
-    const double a3 = -an_k / HN(k + 1);
-    const double a2 = 1.0 + an_k / HN(k) + dt * rr(i, j) / (0.5 * (HN(k) + HO(k)));
-    const double a4 = UU_(k + 1) * ao_k / HO(k + 1) + UU_(k) * (1 - ao_k / HO(k)) + dt * exk(k) -
-                      dt * 0.5 * (HO(k) + HN(k)) * g * zx;
-    QU[1 * nt + tid] = (a4 - a3 * QU[2 * nt + tid]) / (a2 - a3 * RU[2 * nt + tid]);
+    hokp1 = hok; hnkp1 = hnk; ukp1 = uk;
+    hok = hokm1; hnk = hnkm1; uk = ukm1;
+    const double a3 = -an_k / hnkp1;
+    const double a2 = 1.0 + an_k / hnk + dt * rr(i, j) / (0.5 * (hnk + hok));
+    const double a4 = ukp1 * ao_k / hokp1 + uk * (1 - ao_k / hok) + dt * exk(k) - dt * 0.5 * (hok + hnk) * g * zx;
+    v = (a4 - a3 * qu) / (a2 - a3 * ru);
   }
-  // back substitution; Res(k) kept in QU, its sum in ascending k
-  double v = QU[1 * nt + tid];
+  // back substitution (Res in QU) and its sum in ascending k
   double ResInt = 0.0;
   ResInt = ResInt + v;
+  QU(i, j, 1) = R3(v);
   for (k = 2; k <= kmax; ++k) {
-    v = QU[k * nt + tid] - RU[k * nt + tid] * v;
-    QU[k * nt + tid] = v;
+    v = (double)QU(i, j, k) - (double)RU(i, j, k) * v;
+    QU(i, j, k) = R3(v);
     ResInt = ResInt + v;
   }
   const double Diff = (Uint(i, j) - ResInt) / (sso(i, j) + HX(i, j));
-  for (k = 1; k <= kmax; ++k) uu(i, j, k) = R3(QU[k * nt + tid] + HN(k) * Diff);
+  for (k = 1; k <= kmax; ++k) uu(i, j, k) = R3((double)QU(i, j, k) + HN(k) * Diff);
 }
 
 // sigma_coordinates.F90:85-113 (equidistant sigma): layer heights of all levels 0..kmax.
@@ -395,16 +406,12 @@ int run_bc3(int which, const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* cons
     case BC3_IP: k_ip<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6]); break;
     case BC3_UUMOM:
     case BC3_VVMOM: {
-      const dim3 b2(32, 2, 1);
-      const size_t smem = 2 * (size_t)(d.kmax + 1) * 64 * sizeof(double);
-      dim3 g2((d.imax - d.imin + 1 + 31) / 32, (d.jmax - d.jmin + 1 + 1) / 2, 1);
-      if (which == BC3_UUMOM) {
-        cudaFuncSetAttribute(k_uvmom3d<R3, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        k_uvmom3d<R3, 0><<<g2, b2, smem, st>>>(d, s);
-      } else {
-        cudaFuncSetAttribute(k_uvmom3d<R3, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        k_uvmom3d<R3, 1><<<g2, b2, smem, st>>>(d, s);
-      }
+      const dim3 b2(32, 4, 1);
+      dim3 g2((d.imax - d.imin + 1 + 31) / 32, (d.jmax - d.jmin + 1 + 3) / 4, 1);
+      if (which == BC3_UUMOM)
+        k_uvmom3d<R3, 0><<<g2, b2, 0, st>>>(d, s, scr[0], scr[1]);
+      else
+        k_uvmom3d<R3, 1><<<g2, b2, 0, st>>>(d, s, scr[0], scr[1]);
       break;
     }
     case BC3_SIGMA: k_sigma<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s); break;

@@ -205,9 +205,11 @@ template <class R>
 static int vdiff_api(getm_ctx* ctx, R dt, R cnpar, R avmol, R* S, const R* hn, const R* nuh, const int32_t* az,
                      const R* src) {
   if (!ctx || !S || !hn || !nuh || !az) return fail(ctx, GETM_ERR_ARG, "tracer_vdiff: bad argument");
-  if ((size_t)2 * (ctx->dom.kmax + 1) * 64 * sizeof(R) > 200 * 1024)
-    return fail(ctx, GETM_ERR_UNSUPPORTED, "tracer_vdiff: kmax too large");
-  GB_TIMED(GETM_TIM_VDIFF, run_vdiff<R>(ctx->dev, ctx->stream, dt, cnpar, avmol, S, hn, nuh, az, src), "tracer_vdiff");
+  int rc = ensure_scratch(ctx, (size_t)n3d(ctx->dev) * sizeof(R));
+  if (rc) return rc;
+  GB_TIMED(GETM_TIM_VDIFF,
+           run_vdiff<R>(ctx->dev, ctx->stream, dt, cnpar, avmol, S, hn, nuh, az, src, (R*)ctx->scr[0], (R*)ctx->scr[1]),
+           "tracer_vdiff");
   return GETM_OK;
 }
 

@@ -111,6 +111,181 @@ __global__ void __launch_bounds__(256) k_sweep_h(Dev d, R dt, R splitfac, int sc
 }
 
 // ---------------------------------------------------------------------------------------------
+// Tiled horizontal sweeps: every face flux is computed once. A block stages the stencil source f,
+// the face transports/heights and the flux masks of its tile in shared memory, computes the fluxes
+// of the tile's faces into shared memory and then updates its cells -- the same arithmetic, in the
+// same order, as face_flux / k_sweep_h (bit-identical results), with each input read once.
+//
+// Face flux from staged values: f at q-1..q+2, flux masks at q-1..q+1 (face q between cells q, q+1).
+template <class R>
+__device__ __forceinline__ R face_flux_v(R Uf, R DUf, R fm1, R f0, R f1, R f2, bool mm1, bool m0, bool mp1,
+                                         int scheme, R dti, R AH, bool use_AH, R dxf) {
+  if (!m0) return R(0);
+  R fu, cfl = R(0), fuu = R(0), fd = R(0);
+  bool lim = false;
+  if (Uf > R(0)) {
+    fu = f0;
+    if (scheme != UPSTREAM) lim = mm1;
+    if (lim) {
+      cfl = Uf / DUf * dti / dxf;
+      fuu = fm1;
+      fd = f1;
+    }
+  } else {
+    fu = f1;
+    if (scheme != UPSTREAM) lim = mp1;
+    if (lim) {
+      cfl = -Uf / DUf * dti / dxf;
+      fuu = f2;
+      fd = f0;
+    }
+  }
+  if (lim) fu = recon<R>(scheme, cfl, fuu, fu, fd);
+  R fl = Uf * fu;
+  if (use_AH) fl = fl - AH * DUf * (f1 - f0) / dxf;
+  return fl;
+}
+
+constexpr int TU = 128;             // u sweep: cells per block along i
+constexpr int TVX = 32, TVY = 8;    // v sweep: tile of 32 (i) x 8 (j) cells
+
+// u sweep (adv_split_u.F90:222-285) over one (j, k) row segment of TU cells.
+template <class R>
+__global__ void __launch_bounds__(TU) k_sweep_u_tile(Dev d, R dt, R splitfac, int scheme, R AH,
+                                                     const R* __restrict__ f, const R* fi_src, R* fi_dst,
+                                                     const R* Di_src, R* Di_dst, R* adv,
+                                                     const R* __restrict__ U, const R* __restrict__ DU,
+                                                     const uint8_t* __restrict__ mflux,
+                                                     const uint8_t* __restrict__ mupd) {
+  __shared__ R sf[TU + 4];      // f(i0-2 .. i0+TU+1)
+  __shared__ R sU[TU + 1];      // U(i0-1 .. i0+TU-1)
+  __shared__ R sDU[TU + 1];
+  __shared__ uint8_t sm[TU + 4];  // mflux(i0-2 .. i0+TU+1)
+  __shared__ R sfl[TU + 1];     // flux of faces i0-1 .. i0+TU-1
+  const int t = threadIdx.x;
+  const int ni = d.ni();
+  const int ii0 = blockIdx.x * TU;  // array index of the tile's first cell
+  const int jj = blockIdx.y;
+  const long long row = (long long)jj * d.sj + (long long)blockIdx.z * d.sk;
+  const long long crow = (long long)jj * d.sj;
+  // stage inputs (array indices outside 0..ni-1 are never used by a valid face)
+  for (int q = t; q < TU + 4; q += TU) {
+    const int ii = ii0 - 2 + q;
+    const bool ok = ii >= 0 && ii < ni;
+    sf[q] = ok ? f[row + ii] : R(0);
+    sm[q] = ok ? mflux[crow + ii] : 0;
+  }
+  for (int q = t; q < TU + 1; q += TU) {
+    const int ii = ii0 - 1 + q;
+    const bool ok = ii >= 0 && ii < ni;
+    sU[q] = ok ? U[row + ii] : R(0);
+    sDU[q] = ok ? DU[row + ii] : R(0);
+  }
+  __syncthreads();
+  const int sub = (scheme == UPSTREAM) ? 0 : 1;
+  const R dti = splitfac * dt;
+  const bool use_AH = AH > R(0);
+  const R dxf = R(d.dx), dyf = R(d.dy), ard1 = R(d.ard1);
+  // faces: face index in array coordinates fi_ = ii0-1+q; valid if fi_ in [sub, ni-2-sub]
+  for (int q = t; q < TU + 1; q += TU) {
+    const int fa = ii0 - 1 + q;
+    R fl = R(0);
+    if (fa >= sub && fa <= ni - 2 - sub)
+      fl = face_flux_v<R>(sU[q], sDU[q], sf[q], sf[q + 1], sf[q + 2], sf[q + 3], sm[q] != 0, sm[q + 1] != 0,
+                          sm[q + 2] != 0, scheme, dti, AH, use_AH, dxf);
+    sfl[q] = fl;
+  }
+  __syncthreads();
+  const int ii = ii0 + t;
+  if (ii >= ni) return;
+  const long long p = row + ii;
+  const long long c = crow + ii;
+  const bool in_range = (ii >= 1 + sub) && (ii <= ni - 2 - sub);
+  if (in_range && mupd[c]) {
+    const R fe = sfl[t + 1], fw = sfl[t];
+    const R Dio = Di_src[p];
+    const R dD = dti * (sU[t + 1] * dyf - sU[t] * dyf) * ard1;
+    const R Dn = Dio - dD;
+    const R advn = splitfac * (fe * dyf - fw * dyf) * ard1;
+    const R fio = (fi_src == f) ? sf[t + 2] : fi_src[p];
+    Di_dst[p] = Dn;
+    fi_dst[p] = fv_update<R>(Dio, dD, Dn, fio, dt, advn);
+    if (adv) adv[p] = adv[p] + advn;
+  } else {
+    if (fi_dst != fi_src) fi_dst[p] = (fi_src == f) ? sf[t + 2] : fi_src[p];
+    if (Di_dst != Di_src) Di_dst[p] = Di_src[p];
+  }
+}
+
+// v sweep (adv_split_v.F90:79-135) over a tile of TVX x TVY cells of one level.
+template <class R>
+__global__ void __launch_bounds__(TVX * TVY) k_sweep_v_tile(Dev d, R dt, R splitfac, int scheme, R AH,
+                                                            const R* __restrict__ f, const R* fi_src, R* fi_dst,
+                                                            const R* Di_src, R* Di_dst, R* adv,
+                                                            const R* __restrict__ V, const R* __restrict__ DV,
+                                                            const uint8_t* __restrict__ mflux,
+                                                            const uint8_t* __restrict__ mupd) {
+  __shared__ R sf[TVY + 4][TVX];       // f(j0-2 .. j0+TVY+1)
+  __shared__ R sV[TVY + 1][TVX];       // V(j0-1 .. j0+TVY-1)
+  __shared__ R sDV[TVY + 1][TVX];
+  __shared__ uint8_t sm[TVY + 4][TVX];  // mflux(j0-2 .. j0+TVY+1)
+  __shared__ R sfl[TVY + 1][TVX];      // flux of faces j0-1 .. j0+TVY-1
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int ni = d.ni(), nj = d.nj();
+  const int ii = blockIdx.x * TVX + tx;
+  const int jj0 = blockIdx.y * TVY;
+  const long long lev = (long long)blockIdx.z * d.sk;
+  const bool iok = ii < ni;
+  for (int q = ty; q < TVY + 4; q += TVY) {
+    const int jj = jj0 - 2 + q;
+    const bool ok = iok && jj >= 0 && jj < nj;
+    const long long c = (long long)jj * d.sj + ii;
+    sf[q][tx] = ok ? f[lev + c] : R(0);
+    sm[q][tx] = ok ? mflux[c] : 0;
+  }
+  for (int q = ty; q < TVY + 1; q += TVY) {
+    const int jj = jj0 - 1 + q;
+    const bool ok = iok && jj >= 0 && jj < nj;
+    const long long c = (long long)jj * d.sj + ii;
+    sV[q][tx] = ok ? V[lev + c] : R(0);
+    sDV[q][tx] = ok ? DV[lev + c] : R(0);
+  }
+  __syncthreads();
+  const int sub = (scheme == UPSTREAM) ? 0 : 1;
+  const R dti = splitfac * dt;
+  const bool use_AH = AH > R(0);
+  const R dxf = R(d.dy), dyf = R(d.dx), ard1 = R(d.ard1);  // DYV, DXV
+  for (int q = ty; q < TVY + 1; q += TVY) {
+    const int fa = jj0 - 1 + q;
+    R fl = R(0);
+    if (iok && fa >= sub && fa <= nj - 2 - sub)
+      fl = face_flux_v<R>(sV[q][tx], sDV[q][tx], sf[q][tx], sf[q + 1][tx], sf[q + 2][tx], sf[q + 3][tx],
+                          sm[q][tx] != 0, sm[q + 1][tx] != 0, sm[q + 2][tx] != 0, scheme, dti, AH, use_AH, dxf);
+    sfl[q][tx] = fl;
+  }
+  __syncthreads();
+  const int jj = jj0 + ty;
+  if (!iok || jj >= nj) return;
+  const long long c = (long long)jj * d.sj + ii;
+  const long long p = lev + c;
+  const bool in_range = (jj >= 1 + sub) && (jj <= nj - 2 - sub);
+  if (in_range && mupd[c]) {
+    const R fe = sfl[ty + 1][tx], fw = sfl[ty][tx];
+    const R Dio = Di_src[p];
+    const R dD = dti * (sV[ty + 1][tx] * dyf - sV[ty][tx] * dyf) * ard1;
+    const R Dn = Dio - dD;
+    const R advn = splitfac * (fe * dyf - fw * dyf) * ard1;
+    const R fio = (fi_src == f) ? sf[ty + 2][tx] : fi_src[p];
+    Di_dst[p] = Dn;
+    fi_dst[p] = fv_update<R>(Dio, dD, Dn, fio, dt, advn);
+    if (adv) adv[p] = adv[p] + advn;
+  } else {
+    if (fi_dst != fi_src) fi_dst[p] = (fi_src == f) ? sf[ty + 2][tx] : fi_src[p];
+    if (Di_dst != Di_src) Di_dst[p] = Di_src[p];
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
 // Vertical split sweep (adv_split_w.F90:158-307) without sub-iterations (itersmax = 1):
 // one thread per water column, k-sequential, streaming with a register window so that every
 // level of f and hi is read before it is overwritten -- f, fi and hi may therefore alias.
@@ -294,17 +469,16 @@ struct ThomasSmem {
 };
 
 // Implicit vertical diffusion (salinity.F90:348-389; temperature form with src). One thread per
-// interior column; the matrix rows are built top-down as the elimination proceeds.
+// interior column; the matrix rows are built top-down as the elimination proceeds, ru(k+1)/qu(k+1)
+// carried in registers and ru(k)/qu(k) stored in two scratch 3D arrays (full occupancy, no shared
+// memory) for the back substitution.
 template <class R>
-__global__ void __launch_bounds__(64) k_vdiff(Dev d, R dt, R cnpar, R avmol, R* S,
-                                              const R* __restrict__ hn, const R* __restrict__ nuh,
-                                              const int32_t* __restrict__ az, const R* __restrict__ src) {
-  extern __shared__ unsigned char smem_raw[];
+__global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, R* S, const R* __restrict__ hn,
+                                               const R* __restrict__ nuh, const int32_t* __restrict__ az,
+                                               const R* __restrict__ src, R* RUs, R* QUs) {
   const int kmax = d.kmax;
-  ThomasSmem<R> sm{reinterpret_cast<R*>(smem_raw), reinterpret_cast<R*>(smem_raw) + (kmax + 1) * blockDim.x,
-                   (int)blockDim.x};
   const int i = d.imin + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = d.jmin + blockIdx.y;
+  const int j = d.jmin + blockIdx.y * blockDim.y + threadIdx.y;
   if (i > d.imax || j > d.jmax) return;
   const long long c = d.ix(i, j);
   if (az[c] != 1 || kmax <= 1) return;
@@ -312,59 +486,67 @@ __global__ void __launch_bounds__(64) k_vdiff(Dev d, R dt, R cnpar, R avmol, R* 
   auto L = [&](const R* a, int k) -> R { return a[c + k * sk]; };
   const R co = R(2) * (R(1) - cnpar) * dt;
   const R cn = R(2) * cnpar * dt;
-  auto auxo = [&](int k) -> R { return co * (L(nuh, k) + avmol) / (L(hn, k + 1) + L(hn, k)); };
-  auto auxn = [&](int k) -> R { return cn * (L(nuh, k) + avmol) / (L(hn, k + 1) + L(hn, k)); };
-  // surface row k = kmax: au = a1, bu = a2, du = a4
-  int k = kmax;
-  R ao_km1 = auxo(k - 1), an_km1 = auxn(k - 1);
-  R Sk = L(S, k), Skm1 = L(S, k - 1);
   // FP64 solves the reference's system for the new value. FP32 solves the same matrix for the
   // increment dS = S_new - S_old, whose right-hand side is the flux divergence at the old level,
   // (ao+an)(k)*(S(k+1)-S(k)) - (ao+an)(k-1)*(S(k)-S(k-1)) [+ src]; the rounding then acts on the
   // small increment rather than on h*S (bias-free over hundreds of steps).
   constexpr bool incr = sizeof(R) == 4;
+  // surface row k = kmax: au = a1, bu = a2, du = a4
+  int k = kmax;
+  R hnk = L(hn, k), hnkm1 = L(hn, k - 1);
+  R nu = L(nuh, k - 1) + avmol;
+  R ao_km1 = co * nu / (hnk + hnkm1), an_km1 = cn * nu / (hnk + hnkm1);
+  R Sk = L(S, k), Skm1 = L(S, k - 1);
+  R ru, qu;
   {
     const R a1 = -an_km1;
-    const R a2 = L(hn, k) + an_km1;
-    R a4 = incr ? -(ao_km1 + an_km1) * (Sk - Skm1) : Sk * (L(hn, k) - ao_km1) + Skm1 * ao_km1;
+    const R a2 = hnk + an_km1;
+    R a4 = incr ? -(ao_km1 + an_km1) * (Sk - Skm1) : Sk * (hnk - ao_km1) + Skm1 * ao_km1;
     if (src) a4 = a4 + L(src, k);
-    sm.RU(k) = a1 / a2;
-    sm.QU(k) = a4 / a2;
+    ru = a1 / a2;
+    qu = a4 / a2;
+    RUs[c + k * sk] = ru;
+    QUs[c + k * sk] = qu;
   }
   // inner rows k = kmax-1 .. 2
   for (k = kmax - 1; k >= 2; --k) {
     const R ao_k = ao_km1, an_k = an_km1;  // aux at interface k (computed as k-1 of row k+1)
-    ao_km1 = auxo(k - 1);
-    an_km1 = auxn(k - 1);
+    hnk = hnkm1;
+    hnkm1 = L(hn, k - 1);
+    nu = L(nuh, k - 1) + avmol;
+    ao_km1 = co * nu / (hnk + hnkm1);
+    an_km1 = cn * nu / (hnk + hnkm1);
     const R Skp1 = Sk;
     Sk = Skm1;
     Skm1 = L(S, k - 1);
     const R a3 = -an_k;
     const R a1 = -an_km1;
-    const R a2 = L(hn, k) + an_k + an_km1;
+    const R a2 = hnk + an_k + an_km1;
     R a4 = incr ? (ao_k + an_k) * (Skp1 - Sk) - (ao_km1 + an_km1) * (Sk - Skm1)
-                : Skp1 * ao_k + Sk * (L(hn, k) - ao_k - ao_km1) + Skm1 * ao_km1;
+                : Skp1 * ao_k + Sk * (hnk - ao_k - ao_km1) + Skm1 * ao_km1;
     if (src) a4 = a4 + L(src, k);
-    const R den = a2 - a3 * sm.RU(k + 1);
-    sm.RU(k) = a1 / den;
-    sm.QU(k) = (a4 - a3 * sm.QU(k + 1)) / den;
+    const R den = a2 - a3 * ru;
+    ru = a1 / den;
+    qu = (a4 - a3 * qu) / den;
+    RUs[c + k * sk] = ru;
+    QUs[c + k * sk] = qu;
   }
   // bottom row k = 1 (fi): only qu
+  R v;
   {
-    k = 1;
     const R ao_k = ao_km1, an_k = an_km1;
     const R Skp1 = Sk;  // S(2)
     const R S1 = Skm1;  // S(1)
+    const R h1 = hnkm1;
     const R a3 = -an_k;
-    const R a2 = L(hn, 1) + an_k;
-    R a4 = incr ? (ao_k + an_k) * (Skp1 - S1) : Skp1 * ao_k + S1 * (L(hn, 1) - ao_k);
+    const R a2 = h1 + an_k;
+    R a4 = incr ? (ao_k + an_k) * (Skp1 - S1) : Skp1 * ao_k + S1 * (h1 - ao_k);
     if (src) a4 = a4 + L(src, 1);
-    sm.QU(1) = (a4 - a3 * sm.QU(2)) / (a2 - a3 * sm.RU(2));
+    v = (a4 - a3 * qu) / (a2 - a3 * ru);
+    S[c + 1 * sk] = incr ? S1 + v : v;
   }
-  R v = sm.QU(1);
-  S[c + 1 * sk] = incr ? L(S, 1) + v : v;
   for (k = 2; k <= kmax; ++k) {
-    v = sm.QU(k) - sm.RU(k) * v;
+    v = QUs[c + k * sk] - RUs[c + k * sk] * v;
     S[c + k * sk] = incr ? L(S, k) + v : v;
   }
 }

@@ -10,10 +10,16 @@ int run_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int sche
                 const R* fi_src, R* fi_dst, const R* Di_src, R* Di_dst, R* adv, const R* U, const R* DU,
                 const uint8_t* mflux, const uint8_t* mupd) {
   if (nk <= 0) return 0;
-  dim3 blk(64, 4, 1);
-  dim3 grd((d.ni() + blk.x - 1) / blk.x, (d.nj() + blk.y - 1) / blk.y, nk);
-  k_sweep_h<R, DIR><<<grd, blk, 0, s>>>(d, dt, splitfac, scheme, AH, f, fi_src, fi_dst, Di_src, Di_dst, adv,
-                                        U, DU, mflux, mupd);
+  if (DIR == 0) {
+    dim3 grd((d.ni() + TU - 1) / TU, d.nj(), nk);
+    k_sweep_u_tile<R><<<grd, TU, 0, s>>>(d, dt, splitfac, scheme, AH, f, fi_src, fi_dst, Di_src, Di_dst, adv, U, DU,
+                                         mflux, mupd);
+  } else {
+    dim3 blk(TVX, TVY, 1);
+    dim3 grd((d.ni() + TVX - 1) / TVX, (d.nj() + TVY - 1) / TVY, nk);
+    k_sweep_v_tile<R><<<grd, blk, 0, s>>>(d, dt, splitfac, scheme, AH, f, fi_src, fi_dst, Di_src, Di_dst, adv, U,
+                                          DU, mflux, mupd);
+  }
   return (int)cudaGetLastError();
 }
 
@@ -45,18 +51,12 @@ int run_finalise(const Dev& d, cudaStream_t s, R dt, R* f, const R* ho, const R*
 
 template <class R>
 int run_vdiff(const Dev& d, cudaStream_t s, R dt, R cnpar, R avmol, R* S, const R* hn, const R* nuh,
-              const int32_t* az, const R* src) {
+              const int32_t* az, const R* src, R* rus, R* qus) {
   if (d.kmax <= 1) return 0;
-  const int nt = 64;
-  const size_t smem = 2 * (size_t)(d.kmax + 1) * nt * sizeof(R);
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(k_vdiff<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_set = true;
-  }
   const int nx = d.imax - d.imin + 1, ny = d.jmax - d.jmin + 1;
-  dim3 grd((nx + nt - 1) / nt, ny, 1);
-  k_vdiff<R><<<grd, nt, smem, s>>>(d, dt, cnpar, avmol, S, hn, nuh, az, src);
+  dim3 blk(32, 4, 1);
+  dim3 grd((nx + 31) / 32, (ny + 3) / 4, 1);
+  k_vdiff<R><<<grd, blk, 0, s>>>(d, dt, cnpar, avmol, S, hn, nuh, az, src, rus, qus);
   return (int)cudaGetLastError();
 }
 
@@ -105,7 +105,7 @@ template int run_sweep_w<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL, in
 template int run_finalise<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL*, const GB_REAL*, const GB_REAL*,
                                    const GB_REAL*, const uint8_t*);
 template int run_vdiff<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL, GB_REAL, GB_REAL*, const GB_REAL*,
-                                const GB_REAL*, const int32_t*, const GB_REAL*);
+                                const GB_REAL*, const int32_t*, const GB_REAL*, GB_REAL*, GB_REAL*);
 template int run_tridiag<GB_REAL>(cudaStream_t, int, int, int, int, const GB_REAL*, const GB_REAL*,
                                   const GB_REAL*, const GB_REAL*, GB_REAL*);
 template int run_content<GB_REAL>(const Dev&, cudaStream_t, const GB_REAL*, const GB_REAL*, const int32_t*,

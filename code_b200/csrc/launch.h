@@ -27,9 +27,10 @@ template <class R>
 int run_finalise(const Dev& d, cudaStream_t s, R dt, R* f, const R* ho, const R* adv, const R* hi,
                  const uint8_t* mfin);
 
+// rus/qus: two scratch 3D arrays (Thomas coefficients)
 template <class R>
 int run_vdiff(const Dev& d, cudaStream_t s, R dt, R cnpar, R avmol, R* S, const R* hn, const R* nuh,
-              const int32_t* az, const R* src);
+              const int32_t* az, const R* src, R* rus, R* qus);
 
 template <class R>
 int run_tridiag(cudaStream_t s, int ncol, int kmax, int fi, int lt, const R* au, const R* bu, const R* cu,
