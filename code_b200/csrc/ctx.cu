@@ -296,11 +296,14 @@ int getm_ctx_set_stream(getm_ctx* ctx, void* stream) {
 
 int getm_ctx_take_warnings(getm_ctx* ctx, int64_t* n_warnings) {
   if (!ctx || !n_warnings) return GETM_ERR_ARG;
-  unsigned long long h = 0;
-  GB_TRY(cudaMemcpyAsync(&h, ctx->cnt, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream), "read warnings");
-  GB_TRY(cudaMemsetAsync(ctx->cnt, 0, sizeof(h), ctx->stream), "reset warnings");
+  // counters [0] (iteration cap of adv_split_w) and [2] (log-law arguments <= 1 of the slow
+  // bottom friction); [1] belongs to check_3d_fields
+  unsigned long long h[3] = {0, 0, 0};
+  GB_TRY(cudaMemcpyAsync(h, ctx->cnt, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream), "read warnings");
+  GB_TRY(cudaMemsetAsync(ctx->cnt, 0, sizeof(unsigned long long), ctx->stream), "reset warnings");
+  GB_TRY(cudaMemsetAsync(ctx->cnt + 2, 0, sizeof(unsigned long long), ctx->stream), "reset warnings");
   GB_TRY(cudaStreamSynchronize(ctx->stream), "sync");
-  *n_warnings = (int64_t)h;
+  *n_warnings = (int64_t)(h[0] + h[2]);
   return GETM_OK;
 }
 
