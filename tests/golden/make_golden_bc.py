@@ -1,7 +1,7 @@
 """Generates tests/golden/reference_mode_split.npz: the reference's own integrate_2d / integrate_3d
 (the mode-split time loop, integration.F90:98-172) executed from source (fortran_subset.py) on a
 small closed basin, together with the inputs. The oracle and the CUDA path are compared with it
-bit for bit (tests/test_golden_bc_cpu.py, tests/test_gpu_golden_bc.py).
+bit for bit (tests/test_golden_bc_cpu.py) and the CUDA path within 1e-12 (tests/test_gpu_baroclinic.py).
 
     python tests/golden/make_golden_bc.py
 
