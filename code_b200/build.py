@@ -27,6 +27,7 @@ UNITS = {
     "kernels_f32.cu": ["--fmad=true"],
     "ctx.cu": [],
     "bc.cu": ["--fmad=false"],
+    "noalloc.cu": ["--fmad=false"],
 }
 
 

@@ -67,6 +67,7 @@ _PROTOS = {
     "getm_tridiagonal_columns": [P, I, I, I, I, P, P, P, P, P],
     "getm_tracer_vdiff": [P, D, D, D, P, P, P, P, P],
     "getm_tracer_vdiff_f32": [P, F, F, F, P, P, P, P, P],
+    "getm_tracer_vdiff_noalloc": [P, P, D, D, D, P, P, P, P, P],
     "getm_tracer_step": [P, D, P, P, P, P, P, P, P, P, P, I, I, I, D, D, D, I],
     "getm_tracer_step_f32": [P, F, P, P, P, P, P, P, P, P, P, I, I, I, F, F, F, I],
     "getm_tracer_content": [P, P, P, P, P],

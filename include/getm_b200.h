@@ -36,6 +36,7 @@ extern "C" {
 #define GETM_ERR_TIMEOUT (-5)     /* a bounded device wait ran out */
 #define GETM_ERR_NOMEM (-6)       /* device allocation failed */
 #define GETM_ERR_STATE (-7)       /* call order violated (e.g. masks not initialised) */
+#define GETM_ERR_TOO_LARGE (-8)   /* the domain exceeds a fixed size limit of the entry point */
 
 /* ---- scheme / split / tag identifiers (values as in the reference) --------------------- */
 /* advection.F90:55,60-62 ; advection_3d.F90:42 */
@@ -237,6 +238,29 @@ int getm_tracer_content_f32(getm_ctx *ctx, const float *f, const float *h, const
  * to the HOST int64 *status. */
 int getm_check_3d_fields(getm_ctx *ctx, const double *f, const int32_t *az, double minval,
                          double maxval, int64_t *status);
+
+/* ---- context-free, allocation-free variant ------------------------------------------- */
+/* getm_tracer_vdiff without a context and without any device allocation. No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory while they step (they keep
+ * no context, their device memory is fully committed, or they cannot afford the device-wide wait
+ * of cudaFree). Same kernel, arguments and results as getm_tracer_vdiff (FP64).
+ *
+ * Scratch: one array with static storage in the library, sized for domains whose padded 3D index
+ * space sk*(kmax+1) holds at most GETM_VDIFF_NOALLOC_MAX_CELLS elements (two FP64 coefficients
+ * per element: 64 MiB of device memory, which the CUDA runtime reserves when it loads the module
+ * holding it: at start-up, or at the first call where modules load lazily). A larger domain
+ * returns GETM_ERR_TOO_LARGE and nothing runs. Nothing in the scratch has to start at zero.
+ * Device and stream: the caller makes the device that owns the arrays current and passes a
+ * stream of that device (NULL = legacy default stream). The first call on each device looks up
+ * the scratch address there (a one-time set-up, no allocation); make that first call before any
+ * stream capture begins.
+ * Concurrency: all calls on one device share the one scratch array. Calls whose work overlaps in
+ * time (on different streams, or from several host threads without ordering) race on it and give
+ * wrong results; calls on one stream are ordered and safe. */
+#define GETM_VDIFF_NOALLOC_MAX_CELLS 4194304LL
+int getm_tracer_vdiff_noalloc(const getm_domain *dom, void *stream, double dt, double cnpar,
+                              double avmol, double *S, const double *hn, const double *nuh,
+                              const int32_t *az, const double *src);
 
 #ifdef __cplusplus
 }
