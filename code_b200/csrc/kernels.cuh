@@ -10,45 +10,47 @@ namespace gb {
 // ---------------------------------------------------------------------------------------------
 // Horizontal split sweeps (adv_split_u.F90:205-285, adv_split_v.F90:63-135).
 //
-// One thread per cell of the haloed plane and level. A cell in the update range with
-// mask_update computes the fluxes of both of its faces (each face is evaluated identically by
-// its two neighbours, so the result equals the reference's flux array) from the read-only
-// stencil source f, then writes fi_dst / Di_dst; every other cell copies fi_src / Di_src through
-// when source and destination differ. f must not alias fi_dst (callers ping-pong); fi_src may
-// alias fi_dst and Di_src may alias Di_dst (a cell reads and writes only itself).
-// Flux through the face between cell q and its +DIR neighbour (reference phase 1). p is the
-// 3D offset of the face's cell, c its 2D offset, st the element stride along the sweep
-// direction (1 for u, sj for v).
+// The limiter scheme S is a template parameter. FP64 evaluates the reference's expressions in the
+// reference's order (bit-identical results, IEEE division). FP32 -- the mixed-precision variant --
+// evaluates the same interface values with fewer instructions: the ratio-based limiters are
+// rewritten without the ratio (L(r)*deltaf from the magnitudes |deltafu|, |deltaf|, which equals
+// the reference's value in exact arithmetic) and the remaining divisions by face quantities use
+// the fast reciprocal (__fdividef, <= 2 ulp).
+
 template <class R>
-__device__ __forceinline__ R face_flux(const R* __restrict__ f, const R* __restrict__ U,
-                                       const R* __restrict__ DU, const uint8_t* __restrict__ mflux,
-                                       long long p, long long c, long long st, int scheme, R dti, R AH,
-                                       bool use_AH, R dxf) {
-  if (!mflux[c]) return R(0);
-  const R Uf = U[p];
-  R fu, cfl = R(0), fuu = R(0), fd = R(0);
-  bool lim = false;
-  if (Uf > R(0)) {
-    fu = f[p];
-    if (scheme != UPSTREAM) lim = mflux[c - st] != 0;
-    if (lim) {
-      cfl = Uf / DU[p] * dti / dxf;
-      fuu = f[p - st];
-      fd = f[p + st];
-    }
+__device__ __forceinline__ R qdiv(R a, R b) {
+  if constexpr (sizeof(R) == 4) return __fdividef(a, b);
+  else return a / b;
+}
+
+// Interface value from (fuu, fu, fd) at Courant number cfl (advection.F90:785-879).
+template <class R, int S>
+__device__ __forceinline__ R recon_s(R cfl, R fuu, R fu, R fd) {
+  if constexpr (sizeof(R) == 8) {
+    return recon<R>(S, cfl, fuu, fu, fd);
   } else {
-    fu = f[p + st];
-    if (scheme != UPSTREAM) lim = mflux[c + st] != 0;
-    if (lim) {
-      cfl = -Uf / DU[p] * dti / dxf;
-      fuu = f[p + 2 * st];
-      fd = f[p];
+    const float df = fd - fu, du = fu - fuu;
+    if constexpr (S == P2) {
+      const float x = (1.f / 6.f) * (1.f - 2.f * cfl);
+      return fu + 0.5f * (1.f - cfl) * ((0.5f + x) * df + (0.5f - x) * du);
+    } else if constexpr (S == SUPERBEE || S == MUSCL || S == P2_PDM) {
+      if (!(df * du > 0.f)) return fu;
+      const float a = fabsf(du), b = fabsf(df);  // L(r)*|deltaf| with r = a/b
+      float Lb;
+      if constexpr (S == SUPERBEE) {
+        Lb = fmaxf(fminf(2.f * a, b), fminf(a, 2.f * b));
+      } else if constexpr (S == MUSCL) {
+        Lb = fminf(fminf(2.f * a, 0.5f * (b + a)), 2.f * b);
+      } else {
+        const float x = (1.f / 6.f) * (1.f - 2.f * cfl);
+        Lb = fminf(fminf(__fdividef(2.f * a, cfl + 1.e-10f), (0.5f + x) * b + (0.5f - x) * a),
+                   __fdividef(2.f * b, 1.f - cfl));
+      }
+      return fu + 0.5f * (1.f - cfl) * copysignf(Lb, df);
+    } else {
+      return fu;
     }
   }
-  if (lim) fu = recon<R>(scheme, cfl, fuu, fu, fd);
-  R fl = Uf * fu;
-  if (use_AH) fl = fl - AH * DU[p] * (f[p + st] - f[p]) / dxf;
-  return fl;
 }
 
 // Finite-volume update of one cell after a split step: hin = hio - dh is the new layer height and
@@ -64,94 +66,46 @@ __device__ __forceinline__ R fv_update(R hio, R dh, R hin, R fio, R dt, R advn) 
     return (hio * fio - dt * advn) / hin;
   } else {
     (void)hio;
-    return fio + (fio * dh - dt * advn) / hin;
+    return fio + __fdividef(fio * dh - dt * advn, hin);
   }
 }
 
-// DIR 0 = u (adv_split_u), 1 = v (adv_split_v)
-template <class R, int DIR>
-__global__ void __launch_bounds__(256) k_sweep_h(Dev d, R dt, R splitfac, int scheme, R AH,
-                                                 const R* __restrict__ f, const R* fi_src, R* fi_dst,
-                                                 const R* Di_src, R* Di_dst, R* adv,
-                                                 const R* __restrict__ U, const R* __restrict__ DU,
-                                                 const uint8_t* __restrict__ mflux,
-                                                 const uint8_t* __restrict__ mupd) {
-  const int ii = blockIdx.x * blockDim.x + threadIdx.x;
-  const int jj = blockIdx.y * blockDim.y + threadIdx.y;
-  if (ii >= d.ni() || jj >= d.nj()) return;
-  const long long c = (long long)ii + (long long)jj * d.sj;
-  const long long p = c + (long long)blockIdx.z * d.sk;
-  const int sub = (scheme == UPSTREAM) ? 0 : 1;
-  // index along the sweep direction, in reference numbering
-  const int q = (DIR == 0) ? ii + d.imin - HALO : jj + d.jmin - HALO;
-  const int qmin = (DIR == 0) ? d.imin : d.jmin;
-  const int qmax = (DIR == 0) ? d.imax : d.jmax;
-  const bool in_range = (q >= qmin - HALO + 1 + sub) && (q <= qmax + HALO - 1 - sub);
-  if (in_range && mupd[c]) {
-    const long long st = (DIR == 0) ? 1 : d.sj;
-    const R dti = splitfac * dt;
-    const bool use_AH = AH > R(0);
-    const R dxf = (DIR == 0) ? R(d.dx) : R(d.dy);  // DXU / DYV
-    const R dyf = (DIR == 0) ? R(d.dy) : R(d.dx);  // DYU / DXV
-    const R ard1 = R(d.ard1);
-    const R fe = face_flux<R>(f, U, DU, mflux, p, c, st, scheme, dti, AH, use_AH, dxf);
-    const R fw = face_flux<R>(f, U, DU, mflux, p - st, c - st, st, scheme, dti, AH, use_AH, dxf);
-    const R Dio = Di_src[p];
-    const R dD = dti * (U[p] * dyf - U[p - st] * dyf) * ard1;
-    const R Dn = Dio - dD;
-    const R advn = splitfac * (fe * dyf - fw * dyf) * ard1;
-    const R fio = fi_src[p];
-    Di_dst[p] = Dn;
-    fi_dst[p] = fv_update<R>(Dio, dD, Dn, fio, dt, advn);
-    if (adv) adv[p] = adv[p] + advn;
-  } else {
-    if (fi_dst != fi_src) fi_dst[p] = fi_src[p];
-    if (Di_dst != Di_src) Di_dst[p] = Di_src[p];
-  }
-}
-
-// ---------------------------------------------------------------------------------------------
-// Tiled horizontal sweeps: every face flux is computed once. A block stages the stencil source f,
-// the face transports/heights and the flux masks of its tile in shared memory, computes the fluxes
-// of the tile's faces into shared memory and then updates its cells -- the same arithmetic, in the
-// same order, as face_flux / k_sweep_h (bit-identical results), with each input read once.
-//
-// Face flux from staged values: f at q-1..q+2, flux masks at q-1..q+1 (face q between cells q, q+1).
-template <class R>
-__device__ __forceinline__ R face_flux_v(R Uf, R DUf, R fm1, R f0, R f1, R f2, bool mm1, bool m0, bool mp1,
-                                         int scheme, R dti, R AH, bool use_AH, R dxf) {
+// Flux through face q (between cells q and q+1) from staged values: f at q-1..q+2, flux masks at
+// q-1..q+1. cdx = dti/dx (used by FP32 only).
+template <class R, int S>
+__device__ __forceinline__ R face_flux_s(R Uf, R DUf, R fm1, R f0, R f1, R f2, bool mm1, bool m0, bool mp1,
+                                         R dti, R cdx, R AH, bool use_AH, R dxf) {
   if (!m0) return R(0);
-  R fu, cfl = R(0), fuu = R(0), fd = R(0);
-  bool lim = false;
-  if (Uf > R(0)) {
-    fu = f0;
-    if (scheme != UPSTREAM) lim = mm1;
-    if (lim) {
-      cfl = Uf / DUf * dti / dxf;
-      fuu = fm1;
-      fd = f1;
+  const bool pos = Uf > R(0);
+  R fu = pos ? f0 : f1;
+  if (S != UPSTREAM && (pos ? mm1 : mp1)) {
+    const R fuu = pos ? fm1 : f2;
+    const R fd = pos ? f1 : f0;
+    R cfl;
+    if constexpr (sizeof(R) == 8) {
+      (void)cdx;
+      cfl = pos ? Uf / DUf * dti / dxf : -Uf / DUf * dti / dxf;
+    } else {
+      cfl = __fdividef(fabsf(Uf) * cdx, DUf);
     }
-  } else {
-    fu = f1;
-    if (scheme != UPSTREAM) lim = mp1;
-    if (lim) {
-      cfl = -Uf / DUf * dti / dxf;
-      fuu = f2;
-      fd = f0;
-    }
+    fu = recon_s<R, S>(cfl, fuu, fu, fd);
   }
-  if (lim) fu = recon<R>(scheme, cfl, fuu, fu, fd);
   R fl = Uf * fu;
   if (use_AH) fl = fl - AH * DUf * (f1 - f0) / dxf;
   return fl;
 }
 
+// Tiled sweeps: a block stages the stencil source f, the face transports/heights and the flux
+// masks of its tile in shared memory, computes each face flux of the tile once into shared memory
+// and then updates its cells. A cell in the update range with mask_update takes fi/Di from the
+// sources, every other cell copies them through when source and destination differ. f must not
+// alias fi_dst (callers ping-pong); fi_src may be f or alias fi_dst, Di_src may alias Di_dst.
 constexpr int TU = 128;             // u sweep: cells per block along i
 constexpr int TVX = 32, TVY = 8;    // v sweep: tile of 32 (i) x 8 (j) cells
 
 // u sweep (adv_split_u.F90:222-285) over one (j, k) row segment of TU cells.
-template <class R>
-__global__ void __launch_bounds__(TU) k_sweep_u_tile(Dev d, R dt, R splitfac, int scheme, R AH,
+template <class R, int S>
+__global__ void __launch_bounds__(TU) k_sweep_u_tile(Dev d, R dt, R splitfac, R AH,
                                                      const R* __restrict__ f, const R* fi_src, R* fi_dst,
                                                      const R* Di_src, R* Di_dst, R* adv,
                                                      const R* __restrict__ U, const R* __restrict__ DU,
@@ -166,8 +120,8 @@ __global__ void __launch_bounds__(TU) k_sweep_u_tile(Dev d, R dt, R splitfac, in
   const int ni = d.ni();
   const int ii0 = blockIdx.x * TU;  // array index of the tile's first cell
   const int jj = blockIdx.y;
-  const long long row = (long long)jj * d.sj + (long long)blockIdx.z * d.sk;
   const long long crow = (long long)jj * d.sj;
+  const long long row = crow + (long long)blockIdx.z * d.sk;
   // stage inputs (array indices outside 0..ni-1 are never used by a valid face)
   for (int q = t; q < TU + 4; q += TU) {
     const int ii = ii0 - 2 + q;
@@ -182,17 +136,18 @@ __global__ void __launch_bounds__(TU) k_sweep_u_tile(Dev d, R dt, R splitfac, in
     sDU[q] = ok ? DU[row + ii] : R(0);
   }
   __syncthreads();
-  const int sub = (scheme == UPSTREAM) ? 0 : 1;
+  constexpr int sub = (S == UPSTREAM) ? 0 : 1;
   const R dti = splitfac * dt;
   const bool use_AH = AH > R(0);
   const R dxf = R(d.dx), dyf = R(d.dy), ard1 = R(d.ard1);
-  // faces: face index in array coordinates fi_ = ii0-1+q; valid if fi_ in [sub, ni-2-sub]
+  const R cdx = dti / dxf;
+  // faces: face index in array coordinates fa = ii0-1+q; valid if fa in [sub, ni-2-sub]
   for (int q = t; q < TU + 1; q += TU) {
     const int fa = ii0 - 1 + q;
     R fl = R(0);
     if (fa >= sub && fa <= ni - 2 - sub)
-      fl = face_flux_v<R>(sU[q], sDU[q], sf[q], sf[q + 1], sf[q + 2], sf[q + 3], sm[q] != 0, sm[q + 1] != 0,
-                          sm[q + 2] != 0, scheme, dti, AH, use_AH, dxf);
+      fl = face_flux_s<R, S>(sU[q], sDU[q], sf[q], sf[q + 1], sf[q + 2], sf[q + 3], sm[q] != 0, sm[q + 1] != 0,
+                             sm[q + 2] != 0, dti, cdx, AH, use_AH, dxf);
     sfl[q] = fl;
   }
   __syncthreads();
@@ -201,25 +156,25 @@ __global__ void __launch_bounds__(TU) k_sweep_u_tile(Dev d, R dt, R splitfac, in
   const long long p = row + ii;
   const long long c = crow + ii;
   const bool in_range = (ii >= 1 + sub) && (ii <= ni - 2 - sub);
+  const R fio = (fi_src == f) ? sf[t + 2] : fi_src[p];
   if (in_range && mupd[c]) {
     const R fe = sfl[t + 1], fw = sfl[t];
     const R Dio = Di_src[p];
     const R dD = dti * (sU[t + 1] * dyf - sU[t] * dyf) * ard1;
     const R Dn = Dio - dD;
     const R advn = splitfac * (fe * dyf - fw * dyf) * ard1;
-    const R fio = (fi_src == f) ? sf[t + 2] : fi_src[p];
     Di_dst[p] = Dn;
     fi_dst[p] = fv_update<R>(Dio, dD, Dn, fio, dt, advn);
     if (adv) adv[p] = adv[p] + advn;
   } else {
-    if (fi_dst != fi_src) fi_dst[p] = (fi_src == f) ? sf[t + 2] : fi_src[p];
+    if (fi_dst != fi_src) fi_dst[p] = fio;
     if (Di_dst != Di_src) Di_dst[p] = Di_src[p];
   }
 }
 
 // v sweep (adv_split_v.F90:79-135) over a tile of TVX x TVY cells of one level.
-template <class R>
-__global__ void __launch_bounds__(TVX * TVY) k_sweep_v_tile(Dev d, R dt, R splitfac, int scheme, R AH,
+template <class R, int S>
+__global__ void __launch_bounds__(TVX * TVY) k_sweep_v_tile(Dev d, R dt, R splitfac, R AH,
                                                             const R* __restrict__ f, const R* fi_src, R* fi_dst,
                                                             const R* Di_src, R* Di_dst, R* adv,
                                                             const R* __restrict__ V, const R* __restrict__ DV,
@@ -251,16 +206,17 @@ __global__ void __launch_bounds__(TVX * TVY) k_sweep_v_tile(Dev d, R dt, R split
     sDV[q][tx] = ok ? DV[lev + c] : R(0);
   }
   __syncthreads();
-  const int sub = (scheme == UPSTREAM) ? 0 : 1;
+  constexpr int sub = (S == UPSTREAM) ? 0 : 1;
   const R dti = splitfac * dt;
   const bool use_AH = AH > R(0);
   const R dxf = R(d.dy), dyf = R(d.dx), ard1 = R(d.ard1);  // DYV, DXV
+  const R cdx = dti / dxf;
   for (int q = ty; q < TVY + 1; q += TVY) {
     const int fa = jj0 - 1 + q;
     R fl = R(0);
     if (iok && fa >= sub && fa <= nj - 2 - sub)
-      fl = face_flux_v<R>(sV[q][tx], sDV[q][tx], sf[q][tx], sf[q + 1][tx], sf[q + 2][tx], sf[q + 3][tx],
-                          sm[q][tx] != 0, sm[q + 1][tx] != 0, sm[q + 2][tx] != 0, scheme, dti, AH, use_AH, dxf);
+      fl = face_flux_s<R, S>(sV[q][tx], sDV[q][tx], sf[q][tx], sf[q + 1][tx], sf[q + 2][tx], sf[q + 3][tx],
+                             sm[q][tx] != 0, sm[q + 1][tx] != 0, sm[q + 2][tx] != 0, dti, cdx, AH, use_AH, dxf);
     sfl[q][tx] = fl;
   }
   __syncthreads();
@@ -269,18 +225,18 @@ __global__ void __launch_bounds__(TVX * TVY) k_sweep_v_tile(Dev d, R dt, R split
   const long long c = (long long)jj * d.sj + ii;
   const long long p = lev + c;
   const bool in_range = (jj >= 1 + sub) && (jj <= nj - 2 - sub);
+  const R fio = (fi_src == f) ? sf[ty + 2][tx] : fi_src[p];
   if (in_range && mupd[c]) {
     const R fe = sfl[ty + 1][tx], fw = sfl[ty][tx];
     const R Dio = Di_src[p];
     const R dD = dti * (sV[ty + 1][tx] * dyf - sV[ty][tx] * dyf) * ard1;
     const R Dn = Dio - dD;
     const R advn = splitfac * (fe * dyf - fw * dyf) * ard1;
-    const R fio = (fi_src == f) ? sf[ty + 2][tx] : fi_src[p];
     Di_dst[p] = Dn;
     fi_dst[p] = fv_update<R>(Dio, dD, Dn, fio, dt, advn);
     if (adv) adv[p] = adv[p] + advn;
   } else {
-    if (fi_dst != fi_src) fi_dst[p] = (fi_src == f) ? sf[ty + 2][tx] : fi_src[p];
+    if (fi_dst != fi_src) fi_dst[p] = fio;
     if (Di_dst != Di_src) Di_dst[p] = Di_src[p];
   }
 }
@@ -288,30 +244,27 @@ __global__ void __launch_bounds__(TVX * TVY) k_sweep_v_tile(Dev d, R dt, R split
 // ---------------------------------------------------------------------------------------------
 // Vertical split sweep (adv_split_w.F90:158-307) without sub-iterations (itersmax = 1):
 // one thread per water column, k-sequential, streaming with a register window so that every
-// level of f and hi is read before it is overwritten -- f, fi and hi may therefore alias.
-template <class R>
-__device__ __forceinline__ R wface(int k, int kshift, int kmax, int scheme, R dti, R w, R fkm1, R fk,
-                                   R fkp1, R fkp2, R hk, R hkp1) {
-  R fu, fuu = R(0), fd = R(0);
-  bool lim = false;
-  if (w > R(0)) {
-    fu = fk;
-    if (scheme != UPSTREAM) lim = (k > 1 - kshift);
-    if (lim) { fuu = fkm1; fd = fkp1; }
-  } else {
-    fu = fkp1;
-    if (scheme != UPSTREAM) lim = (k < kmax - 1);
-    if (lim) { fuu = fkp2; fd = fk; }
-  }
-  if (lim) {
-    const R cfl = fabs(w) * dti / (R(0.5) * (hk + hkp1));
-    fu = recon<R>(scheme, cfl, fuu, fu, fd);
+// level of f and hi is read before it is overwritten -- f, fi and hi may therefore alias. The
+// window reaches two levels ahead of the face being computed so that several loads per thread
+// are in flight.
+template <class R, int S>
+__device__ __forceinline__ R wface_s(int k, int kshift, int kmax, R dti, R w, R fkm1, R fk, R fkp1, R fkp2,
+                                     R hk, R hkp1) {
+  const bool pos = w > R(0);
+  R fu = pos ? fk : fkp1;
+  if (S != UPSTREAM && (pos ? (k > 1 - kshift) : (k < kmax - 1))) {
+    const R fuu = pos ? fkm1 : fkp2;
+    const R fd = pos ? fkp1 : fk;
+    R cfl;
+    if constexpr (sizeof(R) == 8) cfl = fabs(w) * dti / (R(0.5) * (hk + hkp1));
+    else cfl = __fdividef(2.f * fabsf(w) * dti, hk + hkp1);
+    fu = recon_s<R, S>(cfl, fuu, fu, fd);
   }
   return w * fu;
 }
 
-template <class R>
-__global__ void __launch_bounds__(128) k_sweep_w(Dev d, R dt, R splitfac, int scheme, int kshift,
+template <class R, int S>
+__global__ void __launch_bounds__(128) k_sweep_w(Dev d, R dt, R splitfac, int kshift,
                                                  const R* f, const R* fi_src, R* fi_dst, R* hi, R* adv,
                                                  const R* __restrict__ ww,
                                                  const int32_t* __restrict__ az) {
@@ -324,32 +277,35 @@ __global__ void __launch_bounds__(128) k_sweep_w(Dev d, R dt, R splitfac, int sc
   const int kmax = d.kmax;
   const long long sk = d.sk;
   const R dti = splitfac * dt;
+  const bool fi_is_f = (fi_src == f);
   auto F = [&](int k) -> R { return (k >= 0 && k <= kmax) ? f[c + k * sk] : R(0); };
   auto H = [&](int k) -> R { return (k >= 0 && k <= kmax) ? hi[c + k * sk] : R(0); };
+  auto W = [&](int k) -> R { return (k <= kmax) ? ww[c + k * sk] : R(0); };
   R wprev = R(0);  // wflux(k-1); wflux(0) = 0 unless W_TAG computes face 0
-  if (kshift == 1) wprev = wface<R>(0, 1, kmax, scheme, dti, ww[c], R(0), F(0), F(1), F(2), H(0), H(1));
-  // register window for face k = 1: f(0..3), hi(1..2)
-  R a = F(0), b = F(1), e = F(2), g = F(3);
-  R hA = H(1), hB = H(2);
-  R wkm1 = ww[c];
+  if (kshift == 1) wprev = wface_s<R, S>(0, 1, kmax, dti, ww[c], R(0), F(0), F(1), F(2), H(0), H(1));
+  // window for face k = 1: f(0..4), hi(1..3), ww(0..2)
+  R a = F(0), b = F(1), e = F(2), g = F(3), g2 = F(4);
+  R hA = H(1), hB = H(2), hC = H(3);
+  R wkm1 = W(0), wk = W(1), wk1 = W(2);
   for (int k = 1; k <= kmax - kshift; ++k) {
-    const R wk = ww[c + k * sk];
+    // loads two levels ahead, issued before this level's stores (f/hi may alias fi/hi)
+    const R gn = F(k + 4);
+    const R hn3 = H(k + 3);
+    const R wn = W(k + 2);
+    const R fio = fi_is_f ? b : fi_src[c + k * sk];
+    const R advo = adv ? adv[c + k * sk] : R(0);
     R wfl = R(0);
-    if (k <= kmax - 1) wfl = wface<R>(k, kshift, kmax, scheme, dti, wk, a, b, e, g, hA, hB);
+    if (k <= kmax - 1) wfl = wface_s<R, S>(k, kshift, kmax, dti, wk, a, b, e, g, hA, hB);
     const R hio = hA;
     const R dh = dti * (wk - wkm1);
     const R hin = hio - dh;
     const R advn = splitfac * (wfl - wprev);
-    const R fio = fi_src[c + k * sk];
-    // read the next window entries before this level is overwritten (f/hi may alias fi/hi)
-    const R gn = F(k + 3);
-    const R hn2 = H(k + 2);
     fi_dst[c + k * sk] = fv_update<R>(hio, dh, hin, fio, dt, advn);
     hi[c + k * sk] = hin;
-    if (adv) adv[c + k * sk] = adv[c + k * sk] + advn;
-    a = b; b = e; e = g; g = gn;
-    hA = hB; hB = hn2;
-    wkm1 = wk;
+    if (adv) adv[c + k * sk] = advo + advn;
+    a = b; b = e; e = g; g = g2; g2 = gn;
+    hA = hB; hB = hC; hC = hn3;
+    wkm1 = wk; wk = wk1; wk1 = wn;
     wprev = wfl;
   }
 }

@@ -1,26 +1,45 @@
 // kernels_inst.cuh -- launcher definitions; included once per precision by kernels_f64.cu and
 // kernels_f32.cu with GB_REAL defined to the arithmetic type.
 #pragma once
+#include <type_traits>
+
 #include "kernels.cuh"
 
 namespace gb {
+
+// Calls F.template operator()<S>() with the scheme id as a compile-time constant; returns
+// cudaErrorInvalidValue for an id that is not a split scheme.
+template <class Fn>
+static int dispatch_scheme(int scheme, Fn&& fn) {
+  switch (scheme) {
+    case UPSTREAM: return fn(std::integral_constant<int, UPSTREAM>());
+    case P2: return fn(std::integral_constant<int, P2>());
+    case SUPERBEE: return fn(std::integral_constant<int, SUPERBEE>());
+    case MUSCL: return fn(std::integral_constant<int, MUSCL>());
+    case P2_PDM: return fn(std::integral_constant<int, P2_PDM>());
+    default: return (int)cudaErrorInvalidValue;
+  }
+}
 
 template <class R, int DIR>
 int run_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int scheme, R AH, const R* f,
                 const R* fi_src, R* fi_dst, const R* Di_src, R* Di_dst, R* adv, const R* U, const R* DU,
                 const uint8_t* mflux, const uint8_t* mupd) {
   if (nk <= 0) return 0;
-  if (DIR == 0) {
-    dim3 grd((d.ni() + TU - 1) / TU, d.nj(), nk);
-    k_sweep_u_tile<R><<<grd, TU, 0, s>>>(d, dt, splitfac, scheme, AH, f, fi_src, fi_dst, Di_src, Di_dst, adv, U, DU,
-                                         mflux, mupd);
-  } else {
-    dim3 blk(TVX, TVY, 1);
-    dim3 grd((d.ni() + TVX - 1) / TVX, (d.nj() + TVY - 1) / TVY, nk);
-    k_sweep_v_tile<R><<<grd, blk, 0, s>>>(d, dt, splitfac, scheme, AH, f, fi_src, fi_dst, Di_src, Di_dst, adv, U,
-                                          DU, mflux, mupd);
-  }
-  return (int)cudaGetLastError();
+  return dispatch_scheme(scheme, [&](auto sc) {
+    constexpr int S = decltype(sc)::value;
+    if (DIR == 0) {
+      dim3 grd((d.ni() + TU - 1) / TU, d.nj(), nk);
+      k_sweep_u_tile<R, S><<<grd, TU, 0, s>>>(d, dt, splitfac, AH, f, fi_src, fi_dst, Di_src, Di_dst, adv, U, DU,
+                                              mflux, mupd);
+    } else {
+      dim3 blk(TVX, TVY, 1);
+      dim3 grd((d.ni() + TVX - 1) / TVX, (d.nj() + TVY - 1) / TVY, nk);
+      k_sweep_v_tile<R, S><<<grd, blk, 0, s>>>(d, dt, splitfac, AH, f, fi_src, fi_dst, Di_src, Di_dst, adv, U,
+                                               DU, mflux, mupd);
+    }
+    return (int)cudaGetLastError();
+  });
 }
 
 template <class R>
@@ -32,12 +51,15 @@ int run_sweep_w(const Dev& d, cudaStream_t s, R dt, R splitfac, int scheme, int 
     dim3 grd((d.ni() - 1 + blk.x - 1) / blk.x, (d.nj() - 1 + blk.y - 1) / blk.y, 1);
     k_sweep_w_iter<R><<<grd, blk, 0, s>>>(d, dt, splitfac, scheme, kshift, itersmax, f, fi_src, fi_dst, hi,
                                           adv, ww, az, warn);
-  } else {
+    return (int)cudaGetLastError();
+  }
+  return dispatch_scheme(scheme, [&](auto sc) {
+    constexpr int S = decltype(sc)::value;
     dim3 blk(64, 2, 1);
     dim3 grd((d.ni() - 1 + blk.x - 1) / blk.x, (d.nj() - 1 + blk.y - 1) / blk.y, 1);
-    k_sweep_w<R><<<grd, blk, 0, s>>>(d, dt, splitfac, scheme, kshift, f, fi_src, fi_dst, hi, adv, ww, az);
-  }
-  return (int)cudaGetLastError();
+    k_sweep_w<R, S><<<grd, blk, 0, s>>>(d, dt, splitfac, kshift, f, fi_src, fi_dst, hi, adv, ww, az);
+    return (int)cudaGetLastError();
+  });
 }
 
 template <class R>
