@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--M", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variants", default="fp64,mixed")
+    ap.add_argument("--adj-steps", type=int, default=20, help="tracer steps of the adjoint measurement (0 = skip)")
+    ap.add_argument("--adj-every", type=int, default=10, help="checkpoint interval of the adjoint")
     return ap.parse_args()
 
 
@@ -267,6 +269,15 @@ def main():
     torch.cuda.synchronize()
     tim = v["ctx"].timers(enable=False, reset=True)
     launches = sum(n for _, n in tim.values())
+    # the same per-stage breakdown of the plain FP64 step, for the comparison
+    tim64 = None
+    if head == "mixed" and "fp64" in variants:
+        c64 = variants["fp64"]["ctx"]
+        c64.timers(enable=True, reset=True)
+        for _ in range(args.steps):
+            macro_step("fp64")
+        torch.cuda.synchronize()
+        tim64 = c64.timers(enable=False, reset=True)
     timed = {k: t for k, t in tim.items() if k in STAGE_WORDS}
     top_name, (top_ms, top_n) = max(timed.items(), key=lambda kv: kv[1][0])
     wb = 4 if head == "mixed" else 8
@@ -294,6 +305,36 @@ def main():
     barrier()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1))
     n2b = st.t["f2_z"].numel() * 8
+    # adjoint of the tracer subsystem on the headline state: gradient of the salinity content of a
+    # central 512 x 512 column block after adj_steps tracer steps (advection + implicit diffusion,
+    # velocities, layer heights and nuh of the current state), checkpointed every adj_every steps;
+    # ratio = device time of the reverse pass (recomputation included) / forward pass
+    adj = None
+    if args.adj_steps > 0:
+        t3, pd, pi = st.t, st.pd, st.pi
+        fs = t3["f3_S"].clone()
+        wgt = torch.zeros_like(fs)
+        g = v["g"]
+        b = min(512, args.nx, args.ny)
+        j0, i0 = 2 + (args.ny - b) // 2, 2 + (args.nx - b) // 2
+        wgt[1:, j0:j0 + b, i0:i0 + b] = t3["f3_hn"][1:, j0:j0 + b, i0:i0 + b] / g.ard1
+        wgt *= (t3["az"] == 1).to(wgt.dtype)[None]
+        nubar = torch.zeros_like(fs)
+        args3 = [t3["f3_" + n] for n in ("uu", "vv", "ww", "hun", "hvn", "ho", "hn", "nuh")]
+        adj_ms = []
+        for rep in range(2):  # the first call allocates the checkpoints and tapes
+            f = fs.clone()
+            fbar = wgt.clone()
+            nubar.zero_()
+            barrier()
+            ms_f, ms_r = v["ctx"].tracer_gradient(args.adj_steps, args.adj_every, pd["dt"], f, *args3,
+                                                  pi["salt_adv_split"], pi["salt_adv_hor"], pi["salt_adv_ver"],
+                                                  pd["salt_AH"], pd["cnpar"], pd["avmols"], fbar, nubar)
+            adj_ms.append((max_over_ranks(ms_f), max_over_ranks(ms_r)))
+        ms_f, ms_r = adj_ms[-1]
+        adj = {"steps": args.adj_steps, "checkpoint_every": args.adj_every, "field": "S",
+               "dtype": "f32" if fs.dtype == torch.float32 else "f64", "ms_forward": ms_f, "ms_reverse": ms_r,
+               "objective": f"salinity content of the central {b}x{b} column block"}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -312,9 +353,11 @@ def main():
                            if "fp64" in res else None),
             "mixed_over_fp64": (res["mixed"]["value"] / res["fp64"]["value"]) if len(res) == 2 else None,
             "err_vs_fp64": err,
-            "adjoint_fwd_ratio": None,
+            "adjoint_fwd_ratio": (adj["ms_reverse"] / adj["ms_forward"]) if adj else None,
+            "adjoint": adj,
             "gpu_launches": launches,
             "stage_ms_per_step": {k: t[0] / args.steps for k, t in tim.items()},
+            "stage_ms_per_step_fp64": ({k: t[0] / args.steps for k, t in tim64.items()} if tim64 else None),
             "roofline": {"bound": "hbm", "kernel": top_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
                          "alg_bytes_per_launch": alg_bytes,

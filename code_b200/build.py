@@ -28,6 +28,7 @@ UNITS = {
     "ctx.cu": [],
     "bc.cu": ["--fmad=false"],
     "noalloc.cu": ["--fmad=false"],
+    "adjoint.cu": [],
 }
 
 

@@ -152,6 +152,83 @@ def tracer_rotation_device(nx=2048, ny=2048, kmax=50, depth=50.0, dx=1000.0, dt=
     return g, out, par
 
 
+def streamfunction_flow(nx=256, ny=256, kmax=30, depth=30.0, dx=500.0, dt=300.0, umax=0.5, modes=8,
+                        sigma_cells=16.0, noise=1e-3, nuh=1e-4, seed=4, vertical=0.0, slope=0.0, shear=0.0,
+                        dtype=np.float64) -> Case:
+    """Tracer advection-diffusion in a closed flat basin driven by a random divergence-free flow
+    (the tracer-adjoint configuration).
+
+    Streamfunction at X-points psi = sum over `modes` seeded (m, n) in 1..8 of
+    a_mn sin(m pi x/Lx) sin(n pi y/Ly), a_mn ~ N(0,1), scaled so that max |u|, |v| = umax; the
+    transports are its discrete curl (divergence-free, zero normal flux at the walls), ww = 0; with
+    shear > 0 layer k carries the flow times 1 + shear*((k-1/2)/kmax - 1/2) (still divergence-free
+    in every layer).
+    Tracer: a centred Gaussian (sigma = sigma_cells), times 1 + vertical*cos(pi*(k-1/2)/kmax) on
+    layer k, plus slope*(x/Lx + y/Ly) and uniform noise. SUPERBEE, HALFSPLIT, implicit diffusion
+    with constant nuh.
+    """
+    g = Grid(nx, ny, kmax, dx, dx)
+    rng = np.random.default_rng(seed)
+    az = closed_basin(g)
+    au, av, ax = derive_uvx(az)
+    h = depth / kmax
+    i = np.arange(g.imin - HALO, g.imax + HALO + 1)
+    j = np.arange(g.jmin - HALO, g.jmax + HALO + 1)
+    Lx, Ly = nx * dx, ny * dx
+    xX = np.clip((i - g.imin + 1) * dx, 0.0, Lx)
+    yX = np.clip((j - g.jmin + 1) * dx, 0.0, Ly)
+    psi = np.zeros(g.shape2())
+    mn = rng.integers(1, 9, size=(modes, 2))
+    amp = rng.normal(size=modes)
+    for (m, n), a in zip(mn, amp):
+        psi += a * np.sin(m * np.pi * xX[None, :] / Lx) * np.sin(n * np.pi * yX[:, None] / Ly)
+    u = np.zeros(g.shape2())
+    v = np.zeros(g.shape2())
+    u[1:, :] = -(psi[1:, :] - psi[:-1, :]) / dx
+    v[:, 1:] = (psi[:, 1:] - psi[:, :-1]) / dx
+    u *= (au == 1)
+    v *= (av == 1)
+    scale = umax / max(np.abs(u).max(), np.abs(v).max(), 1e-300)
+    u *= scale
+    v *= scale
+    shp = g.shape3()
+    hh = np.full(shp, h)
+    hh[0] = 0.0
+    uu = np.zeros(shp)
+    vv = np.zeros(shp)
+    lay = 1.0 + shear * ((np.arange(1, kmax + 1) - 0.5) / kmax - 0.5)
+    uu[1:] = u[None] * h * lay[:, None, None]
+    vv[1:] = v[None] * h * lay[:, None, None]
+    xT = (i - g.imin + 0.5) * dx
+    yT = (j - g.jmin + 0.5) * dx
+    s = sigma_cells * dx
+    blob = np.exp(-((xT[None, :] - Lx / 2) ** 2 + (yT[:, None] - Ly / 2) ** 2) / (2 * s * s))
+    f = np.zeros(shp)
+    prof = 1.0 + vertical * np.cos(np.pi * (np.arange(1, kmax + 1) - 0.5) / kmax)
+    f[1:] = blob[None] * prof[:, None, None]
+    f[1:] += slope * (xT[None, None, :] / Lx + yT[None, :, None] / Ly)
+    f[1:] += rng.uniform(-noise, noise, size=(kmax, g.nj, g.ni))
+    f *= (az >= 1)[None]
+    c = Case(g, az=az, au=au, av=av, ax=ax, f=f.astype(dtype), uu=uu.astype(dtype), vv=vv.astype(dtype),
+             ww=np.zeros(shp, dtype), ho=hh.astype(dtype), hn=hh.copy().astype(dtype),
+             hun=hh.copy().astype(dtype), hvn=hh.copy().astype(dtype), nuh=np.full(shp, nuh, dtype=dtype))
+    c.par.update(dt=dt, split=2, hscheme=4, vscheme=4, AH=0.0, cnpar=1.0, avmol=0.0, adv_ver_iterations=1)
+    return c
+
+
+def box_weights(case: Case, box=32):
+    """dJ/df for J = tracer content of a centred box x box column block, all levels:
+    J = sum f * hn / ard1 over its wet cells (k = 1..kmax)."""
+    g = case.grid
+    w = np.zeros(g.shape3())
+    j0 = HALO + (g.ny - box) // 2
+    i0 = HALO + (g.nx - box) // 2
+    sl = (slice(1, None), slice(j0, j0 + box), slice(i0, i0 + box))
+    w[sl] = case["hn"][sl] / g.ard1
+    w *= (case["az"] == 1)[None]
+    return w
+
+
 def random_case(nx=24, ny=20, kmax=7, seed=0, dtype=np.float64, land=0.2, open_bdy=True, dx=400.0, dy=300.0,
                 dt=30.0, cfl=0.8, wscale=0.5) -> Case:
     """Random fields over a random mask for routine-level parity tests.

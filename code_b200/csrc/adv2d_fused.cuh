@@ -1,0 +1,206 @@
+// adv2d_fused.cuh -- the depth-averaged momentum advection of one micro step (uv_advect.F90:94-300
+// with split = HALFSPLIT) as ONE kernel per momentum component. Included by kernels_inst.cuh.
+//
+// uv_advect builds the advected quantity and the face transports of the U (or V) control volumes
+// from U, V, DU, DV (uv_advect.F90:94-110 / :204-220) and runs do_advection (advection.F90:
+// 362-702) on them: u/2, v, u/2 split sweeps whose flux divergences sum to UEx (VEx). Done as
+// separate launches that is six passes over the 2D state per component. Here a block owns an
+// FX x FY tile, stages U, V, DU, DV over the tile plus the halo the three sweeps need (4 cells in
+// x for two u/2 sweeps, 2 in y for the v sweep) in shared memory, runs u/2 on the tile+halo, v on
+// the tile widened in x, u/2 on the tile, and writes UEx once. Every flux and update is the
+// expression of the split-sweep kernels (face_flux_s, fv_update) in the same order, so FP64
+// results equal the three-sweep sequence bit for bit.
+#pragma once
+#include "kernels.cuh"
+
+namespace gb {
+
+constexpr int FX = 32, FY = 16;             // own tile
+constexpr int RW = FX + 8, RH = FY + 4;     // staged region: i in [-4, FX+3], j in [-2, FY+1]
+constexpr int FT = 256;                     // threads per block
+
+template <class T>
+struct Adv2dSmem {
+  T F0[RH][RW];   // advected quantity; reused for the field after the v sweep
+  T F1[RH][RW];   // after the first u/2 sweep
+  T Di[RH][RW];   // control-volume depth, updated in place by each sweep
+  T Ua[RH][RW], DUa[RH][RW], Va[RH][RW], DVa[RH][RW];  // face transports / depths
+  T FL[RH][RW];   // face fluxes of the current sweep
+  T A[FY][FX];    // flux divergence of the own cells, summed over the sweeps (adv = 0 + u/2 + v + u/2)
+  uint8_t mfu[RH][RW], mfv[RH][RW], mpu[RH][RW], mpv[RH][RW];
+};
+
+// DIR 0: UEx on the U grid (fadv = U/DU, faces between U points); DIR 1: VEx on the V grid.
+template <class T, int S, int DIR>
+__global__ void __launch_bounds__(FT) k_uvadv2d_fused(Dev d, T dt, const double* __restrict__ U,
+                                                      const double* __restrict__ V, const double* __restrict__ DU,
+                                                      const double* __restrict__ DV,
+                                                      const uint8_t* __restrict__ mflux_u,
+                                                      const uint8_t* __restrict__ mflux_v,
+                                                      const uint8_t* __restrict__ mupd_u,
+                                                      const uint8_t* __restrict__ mupd_v, double* __restrict__ Ex) {
+  extern __shared__ unsigned char smem_raw[];
+  Adv2dSmem<T>& sm = *reinterpret_cast<Adv2dSmem<T>*>(smem_raw);
+  const int ni = d.ni(), nj = d.nj();
+  const long long sj = d.sj;
+  const int ii0 = blockIdx.x * FX, jj0 = blockIdx.y * FY;
+  constexpr int sub = (S == UPSTREAM) ? 0 : 1;
+  const T half = T(0.5), one = T(1), zero = T(0);
+  const T dxu = T(d.dx), dyu = T(d.dy), ard1 = T(d.ard1);
+  // ---- stage: region cell (r, q) <-> array (jj0-2+r, ii0-4+q)
+  for (int e = threadIdx.x; e < RH * RW; e += FT) {
+    const int r = e / RW, q = e % RW;
+    const int jj = jj0 - 2 + r, ii = ii0 - 4 + q;
+    T f0 = zero, ua = zero, dua = zero, va = zero, dva = zero, dio = zero;
+    uint8_t a = 0, b = 0, c2 = 0, e2 = 0;
+    if (ii >= 0 && ii < ni && jj >= 0 && jj < nj) {
+      const long long c = (long long)jj * sj + ii;
+      a = mflux_u[c];
+      b = mflux_v[c];
+      c2 = mupd_u[c];
+      e2 = mupd_v[c];
+      dio = T(DIR == 0 ? DU[c] : DV[c]);
+      const long long cn = DIR == 0 ? c + 1 : c + sj;  // the next U (V) point
+      const bool ok = DIR == 0 ? (ii <= ni - 2) : (jj <= nj - 2);
+      if (ok) {
+        f0 = T(DIR == 0 ? U[c] / DU[c] : V[c] / DV[c]);
+        ua = T(0.5 * (U[c] + U[cn]));
+        va = T(0.5 * (V[c] + V[cn]));
+        dua = T(0.5 * (DU[c] + DU[cn]));
+        dva = T(0.5 * (DV[c] + DV[cn]));
+      }
+    }
+    sm.F0[r][q] = f0;
+    sm.Ua[r][q] = ua;
+    sm.DUa[r][q] = dua;
+    sm.Va[r][q] = va;
+    sm.DVa[r][q] = dva;
+    sm.Di[r][q] = dio;
+    sm.mfu[r][q] = a;
+    sm.mfv[r][q] = b;
+    sm.mpu[r][q] = c2;
+    sm.mpv[r][q] = e2;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < FX * FY; e += FT) sm.A[e / FX][e % FX] = zero;
+  // region (r, q) -> own cell, for the flux-divergence sum
+  auto own = [&](int r, int q) { return r >= 2 && r < FY + 2 && q >= 4 && q < FX + 4; };
+  __syncthreads();
+
+  // ---- sweep 1: u/2 on rows r in [0, RH), cells q in [2, RW-2), faces q in [1, RW-3]
+  {
+    const T dti = half * dt, cdx = dti / dxu;
+    for (int e = threadIdx.x; e < RH * (RW - 3); e += FT) {
+      const int r = e / (RW - 3), q = 1 + e % (RW - 3);  // face between q and q+1
+      const int fa = ii0 - 4 + q;
+      T fl = zero;
+      if (fa >= sub && fa <= ni - 2 - sub)
+        fl = face_flux_s<T, S>(sm.Ua[r][q], sm.DUa[r][q], sm.F0[r][q - 1], sm.F0[r][q], sm.F0[r][q + 1],
+                               sm.F0[r][q + 2], sm.mfu[r][q - 1] != 0, sm.mfu[r][q] != 0, sm.mfu[r][q + 1] != 0,
+                               dti, cdx, zero, false, dxu);
+      sm.FL[r][q] = fl;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < RH * (RW - 4); e += FT) {
+      const int r = e / (RW - 4), q = 2 + e % (RW - 4);
+      const int ii = ii0 - 4 + q;
+      const T fio = sm.F0[r][q];
+      T fnew = fio;
+      if (ii >= 1 + sub && ii <= ni - 2 - sub && sm.mpu[r][q]) {
+        const T Dio = sm.Di[r][q];
+        const T dD = dti * (sm.Ua[r][q] * dyu - sm.Ua[r][q - 1] * dyu) * ard1;
+        const T Dn = Dio - dD;
+        const T advn = half * (sm.FL[r][q] * dyu - sm.FL[r][q - 1] * dyu) * ard1;
+        sm.Di[r][q] = Dn;
+        fnew = fv_update<T>(Dio, dD, Dn, fio, dt, advn);
+        if (own(r, q)) sm.A[r - 2][q - 4] = sm.A[r - 2][q - 4] + advn;
+      }
+      sm.F1[r][q] = fnew;
+    }
+    __syncthreads();
+  }
+  // ---- sweep 2: v on columns q in [2, RW-2), cells r in [2, RH-2), faces r in [1, RH-3]
+  {
+    const T dti = one * dt, cdy = dti / dyu;
+    for (int e = threadIdx.x; e < (RH - 3) * (RW - 4); e += FT) {
+      const int r = 1 + e / (RW - 4), q = 2 + e % (RW - 4);  // face between r and r+1
+      const int fa = jj0 - 2 + r;
+      T fl = zero;
+      if (fa >= sub && fa <= nj - 2 - sub)
+        fl = face_flux_s<T, S>(sm.Va[r][q], sm.DVa[r][q], sm.F1[r - 1][q], sm.F1[r][q], sm.F1[r + 1][q],
+                               sm.F1[r + 2][q], sm.mfv[r - 1][q] != 0, sm.mfv[r][q] != 0, sm.mfv[r + 1][q] != 0,
+                               dti, cdy, zero, false, dyu);
+      sm.FL[r][q] = fl;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < (RH - 4) * (RW - 4); e += FT) {
+      const int r = 2 + e / (RW - 4), q = 2 + e % (RW - 4);
+      const int jj = jj0 - 2 + r;
+      const T fio = sm.F1[r][q];
+      T fnew = fio;
+      if (jj >= 1 + sub && jj <= nj - 2 - sub && sm.mpv[r][q]) {
+        const T Dio = sm.Di[r][q];
+        const T dD = dti * (sm.Va[r][q] * dxu - sm.Va[r - 1][q] * dxu) * ard1;
+        const T Dn = Dio - dD;
+        const T advn = one * (sm.FL[r][q] * dxu - sm.FL[r - 1][q] * dxu) * ard1;
+        sm.Di[r][q] = Dn;
+        fnew = fv_update<T>(Dio, dD, Dn, fio, dt, advn);
+        if (own(r, q)) sm.A[r - 2][q - 4] = sm.A[r - 2][q - 4] + advn;
+      }
+      sm.F0[r][q] = fnew;  // the field after v (F0 is no longer needed)
+    }
+    __syncthreads();
+  }
+  // ---- sweep 3: u/2 on the own rows r in [2, RH-2), own cells q in [4, RW-4), faces q in [3, RW-5]
+  {
+    const T dti = half * dt, cdx = dti / dxu;
+    for (int e = threadIdx.x; e < (RH - 4) * (RW - 7); e += FT) {
+      const int r = 2 + e / (RW - 7), q = 3 + e % (RW - 7);
+      const int fa = ii0 - 4 + q;
+      T fl = zero;
+      if (fa >= sub && fa <= ni - 2 - sub)
+        fl = face_flux_s<T, S>(sm.Ua[r][q], sm.DUa[r][q], sm.F0[r][q - 1], sm.F0[r][q], sm.F0[r][q + 1],
+                               sm.F0[r][q + 2], sm.mfu[r][q - 1] != 0, sm.mfu[r][q] != 0, sm.mfu[r][q + 1] != 0,
+                               dti, cdx, zero, false, dxu);
+      sm.FL[r][q] = fl;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < FX * FY; e += FT) {
+      const int r = 2 + e / FX, q = 4 + e % FX;
+      const int ii = ii0 - 4 + q, jj = jj0 - 2 + r;
+      T a = sm.A[r - 2][q - 4];
+      if (ii >= 1 + sub && ii <= ni - 2 - sub && jj < nj && sm.mpu[r][q]) {
+        const T advn = half * (sm.FL[r][q] * dyu - sm.FL[r][q - 1] * dyu) * ard1;
+        a = a + advn;
+      }
+      if (ii < ni && jj < nj) Ex[(long long)jj * sj + ii] = (double)a;
+    }
+  }
+}
+
+template <class T, int S, int DIR>
+int launch_uvadv2d_fused(const Dev& d, cudaStream_t s, T dt, const double* U, const double* V, const double* DU,
+                         const double* DV, const uint8_t* mflux_u, const uint8_t* mflux_v, const uint8_t* mupd_u,
+                         const uint8_t* mupd_v, double* Ex) {
+  const size_t smem = sizeof(Adv2dSmem<T>);
+  // opt-in above 48 KB of shared memory (a host-side setting of the current device's function)
+  const cudaError_t e = cudaFuncSetAttribute(k_uvadv2d_fused<T, S, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+  if (e != cudaSuccess) return (int)e;
+  dim3 grd((d.ni() + FX - 1) / FX, (d.nj() + FY - 1) / FY, 1);
+  k_uvadv2d_fused<T, S, DIR><<<grd, FT, smem, s>>>(d, dt, U, V, DU, DV, mflux_u, mflux_v, mupd_u, mupd_v, Ex);
+  return (int)cudaGetLastError();
+}
+
+template <class T>
+int run_uvadv2d_fused(const Dev& d, cudaStream_t s, int dir, T dt, int scheme, const double* U, const double* V,
+                      const double* DU, const double* DV, const uint8_t* mflux_u, const uint8_t* mflux_v,
+                      const uint8_t* mupd_u, const uint8_t* mupd_v, double* Ex) {
+  return dispatch_scheme(scheme, [&](auto sc) {
+    constexpr int S = decltype(sc)::value;
+    return dir == 0 ? launch_uvadv2d_fused<T, S, 0>(d, s, dt, U, V, DU, DV, mflux_u, mflux_v, mupd_u, mupd_v, Ex)
+                    : launch_uvadv2d_fused<T, S, 1>(d, s, dt, U, V, DU, DV, mflux_u, mflux_v, mupd_u, mupd_v, Ex);
+  });
+}
+
+}  // namespace gb

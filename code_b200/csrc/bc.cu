@@ -446,6 +446,17 @@ int uv_advect_2d_t(getm_ctx* ctx, const getm_bc_state* st, const double* U, cons
     GB_TRY(cudaMemsetAsync(Ex[1], 0, n2 * sizeof(double), s), "VEx=0");
     return GETM_OK;
   }
+  if (split == GETM_HALFSPLIT && is_split_scheme(hor)) {
+    // all three sweeps of each component in one launch (adv2d_fused.cuh)
+    for (int dir = 0; dir < 2; ++dir) {
+      getm_adv_grid g;
+      grid_for_tag(ctx, dir == 0 ? GETM_U_TAG : GETM_V_TAG, &g);
+      GB_TIMED(GETM_TIM_BC2D, run_uvadv2d_fused<T>(d, s, dir, T(st->par[P_DTM]), hor, U, V, DU_, DV_, g.mask_uflux,
+                                                   g.mask_vflux, g.mask_uupdate, g.mask_vupdate, Ex[dir]),
+               "uv_advect");
+    }
+    return GETM_OK;
+  }
   // 2D scratch (NB2 FP64-sized arrays) viewed as T
   T* w = (T*)ctx->bc_scr2;
   T *fadv = w, *Uadv = w + n2, *Vadv = w + 2 * n2, *DUadv = w + 3 * n2, *DVadv = w + 4 * n2, *Di = w + 5 * n2,

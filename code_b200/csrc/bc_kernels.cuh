@@ -130,12 +130,15 @@ __global__ void k_ip(Dev d, Bc3<R3> s, const R3* zzp) {
 
 // uu_momentum_3d.F90:169-304 (DIR 0) / vv_momentum_3d.F90:174-315 (DIR 1), kumin = 1: explicit
 // terms, implicit vertical viscosity and the transport correction to the depth-integrated
-// transport Uint. One thread per column, arithmetic in FP64. The elimination carries ru(k+1),
-// qu(k+1) in registers and stores ru(k), qu(k) in two scratch 3D arrays (RUs, QUs, type R3: exact
-// for FP64) so that occupancy is not limited by shared memory; the back substitution overwrites
-// QUs with Res(k) and the last pass writes uu = Res + hn*Diff.
+// transport Uint. One thread per column. The column arithmetic type T is FP64 for the FP64 step
+// (the reference's expressions in the reference's order) and FP32 for the mixed step (divisions by
+// the fast reciprocal); the depth integral of the solution and the transport correction are FP64
+// in both. The elimination carries ru(k+1), qu(k+1) in registers and stores ru(k), qu(k) in two
+// scratch 3D arrays (RUs, QUs) so that occupancy is not limited by shared memory; the back
+// substitution overwrites QUs with Res(k) and the last pass writes uu = Res + hn*Diff.
 template <class R3, int DIR>
 __global__ void __launch_bounds__(128) k_uvmom3d(Dev d, Bc3<R3> s, R3* RUs, R3* QUs) {
+  using T = R3;
   const int kmax = d.kmax;
   const int i = blockIdx.x * blockDim.x + threadIdx.x + d.imin;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + d.jmin;
@@ -158,25 +161,30 @@ __global__ void __launch_bounds__(128) k_uvmom3d(Dev d, Bc3<R3> s, R3* RUs, R3* 
   }
   const double gamma = g * rho_0;
   const double gammai = 1.0 / gamma, rho_0i = 1.0 / rho_0;
-  const double dryij = dry(i, j), corij = cor(i, j);
-  auto HO = [&](int k) { return (double)ho(i, j, k); };
-  auto HN = [&](int k) { return (double)hn(i, j, k); };
-  auto UU_ = [&](int k) { return (double)uu(i, j, k); };
+  const T dryij = T(dry(i, j)), corij = T(cor(i, j));
+  const T ip_t = T(ip_fac), avm_t = T(avmmol), dt_t = T(dt), g_t = T(g);
+  const T taus_top = T(dry(i, j) * 0.5 * (taus(i, j) + taus(i + di, j + dj)) * rho_0i);
+  auto HO = [&](int k) { return T(ho(i, j, k)); };
+  auto HN = [&](int k) { return T(hn(i, j, k)); };
+  auto UU_ = [&](int k) { return T(uu(i, j, k)); };
   auto exk = [&](int k) {
-    double loc, e;
+    T loc, e;
     if (DIR == 0) {
-      loc = 0.25 * ((double)vv(i, j, k) + (double)vv(i + 1, j, k) + (double)vv(i, j - 1, k) + (double)vv(i + 1, j - 1, k));
+      loc = T(0.25) * (T(vv(i, j, k)) + T(vv(i + 1, j, k)) + T(vv(i, j - 1, k)) + T(vv(i + 1, j - 1, k)));
       e = corij * loc;
     } else {
-      loc = 0.25 * ((double)vv(i, j, k) + (double)vv(i - 1, j, k) + (double)vv(i, j + 1, k) + (double)vv(i - 1, j + 1, k));
+      loc = T(0.25) * (T(vv(i, j, k)) + T(vv(i - 1, j, k)) + T(vv(i, j + 1, k)) + T(vv(i - 1, j + 1, k)));
       e = -corij * loc;
     }
-    double x = dryij * (e - (double)Ex(i, j, k) + ip_fac * (double)idp(i, j, k));
-    if (k == kmax) x = x + dryij * 0.5 * (taus(i, j) + taus(i + di, j + dj)) * rho_0i;
+    T x = dryij * (e - T(Ex(i, j, k)) + ip_t * T(idp(i, j, k)));
+    if (k == kmax) {
+      if constexpr (sizeof(T) == 8) x = x + dryij * 0.5 * (taus(i, j) + taus(i + di, j + dj)) * rho_0i;
+      else x = x + taus_top;
+    }
     return x;
   };
-  auto dif = [&](int k) { return 0.5 * ((double)num(i, j, k) + (double)num(i + di, j + dj, k)) + avmmol; };
-  const double c_o = 2.0 * (1.0 - cnpar) * dt, c_n = 2.0 * cnpar * dt;
+  auto dif = [&](int k) { return T(0.5) * (T(num(i, j, k)) + T(num(i + di, j + dj, k))) + avm_t; };
+  const T c_o = T(2.0 * (1.0 - cnpar) * dt), c_n = T(2.0 * cnpar * dt);
   const double zp = fmax(sseo(i + di, j + dj), -H(i, j) + fmin(min_depth, D(i + di, j + dj)));
   const double zm = fmax(sseo(i, j), -H(i + di, j + dj) + fmin(min_depth, D(i, j)));
   double zx;
@@ -184,63 +192,66 @@ __global__ void __launch_bounds__(128) k_uvmom3d(Dev d, Bc3<R3> s, R3* RUs, R3* 
     zx = (zp - zm + (airp(i + 1, j) - airp(i, j)) * gammai) / d.dx;
   else
     zx = (zp - zm + (airp(i, j + 1) - airp(i, j)) / gamma) / d.dy;
+  const T zx_t = T(zx);
   // column window: heights and velocity at k-1, k, k+1
   int k = kmax;
-  double hok = HO(k), hnk = HN(k), hokm1 = HO(k - 1), hnkm1 = HN(k - 1);
-  double uk = UU_(k), ukm1 = UU_(k - 1), ukp1 = 0.0, hokp1 = 0.0, hnkp1 = 0.0;
-  double difk = dif(k - 1);
-  double ao_km1 = c_o * difk / (hok + hokm1), an_km1 = c_n * difk / (hnk + hnkm1);
-  double ru, qu;
+  T hok = HO(k), hnk = HN(k), hokm1 = HO(k - 1), hnkm1 = HN(k - 1);
+  T uk = UU_(k), ukm1 = UU_(k - 1), ukp1 = T(0), hokp1 = T(0), hnkp1 = T(0);
+  T difk = dif(k - 1);
+  T ao_km1 = qdiv(c_o * difk, hok + hokm1), an_km1 = qdiv(c_n * difk, hnk + hnkm1);
+  T ru, qu;
   {
-    const double a1 = -an_km1 / hnkm1;
-    const double a2 = 1. + an_km1 / hnk;
-    const double a4 = uk * (1 - ao_km1 / hok) + ukm1 * ao_km1 / hokm1 + dt * exk(k) - dt * 0.5 * (hok + hnk) * g * zx;
-    ru = a1 / a2;
-    qu = a4 / a2;
+    const T a1 = qdiv(-an_km1, hnkm1);
+    const T a2 = T(1) + qdiv(an_km1, hnk);
+    const T a4 = uk * (1 - qdiv(ao_km1, hok)) + qdiv(ukm1 * ao_km1, hokm1) + dt_t * exk(k) -
+                 dt_t * T(0.5) * (hok + hnk) * g_t * zx_t;
+    ru = qdiv(a1, a2);
+    qu = qdiv(a4, a2);
     RU(i, j, k) = R3(ru);
     QU(i, j, k) = R3(qu);
   }
   for (k = kmax - 1; k >= 2; --k) {
-    const double ao_k = ao_km1, an_k = an_km1;
+    const T ao_k = ao_km1, an_k = an_km1;
     hokp1 = hok; hnkp1 = hnk; ukp1 = uk;
     hok = hokm1; hnk = hnkm1; uk = ukm1;
     hokm1 = HO(k - 1); hnkm1 = HN(k - 1); ukm1 = UU_(k - 1);
     difk = dif(k - 1);
-    ao_km1 = c_o * difk / (hok + hokm1);
-    an_km1 = c_n * difk / (hnk + hnkm1);
-    const double a3 = -an_k / hnkp1;
-    const double a1 = -an_km1 / hnkm1;
-    const double a2 = 1.0 + (an_k + an_km1) / hnk;
-    const double a4 = ukp1 * ao_k / hokp1 + uk * (1 - (ao_k + ao_km1) / hok) + ukm1 * ao_km1 / hokm1 + dt * exk(k) -
-                      dt * 0.5 * (hok + hnk) * g * zx;
-    const double den = a2 - a3 * ru;
-    ru = a1 / den;
-    qu = (a4 - a3 * qu) / den;
+    ao_km1 = qdiv(c_o * difk, hok + hokm1);
+    an_km1 = qdiv(c_n * difk, hnk + hnkm1);
+    const T a3 = qdiv(-an_k, hnkp1);
+    const T a1 = qdiv(-an_km1, hnkm1);
+    const T a2 = T(1) + qdiv(an_k + an_km1, hnk);
+    const T a4 = qdiv(ukp1 * ao_k, hokp1) + uk * (1 - qdiv(ao_k + ao_km1, hok)) + qdiv(ukm1 * ao_km1, hokm1) +
+                 dt_t * exk(k) - dt_t * T(0.5) * (hok + hnk) * g_t * zx_t;
+    const T den = a2 - a3 * ru;
+    ru = qdiv(a1, den);
+    qu = qdiv(a4 - a3 * qu, den);
     RU(i, j, k) = R3(ru);
     QU(i, j, k) = R3(qu);
   }
-  double v;
+  T v;
   {
     k = 1;
-    const double ao_k = ao_km1, an_k = an_km1;
+    const T ao_k = ao_km1, an_k = an_km1;
     hokp1 = hok; hnkp1 = hnk; ukp1 = uk;
     hok = hokm1; hnk = hnkm1; uk = ukm1;
-    const double a3 = -an_k / hnkp1;
-    const double a2 = 1.0 + an_k / hnk + dt * rr(i, j) / (0.5 * (hnk + hok));
-    const double a4 = ukp1 * ao_k / hokp1 + uk * (1 - ao_k / hok) + dt * exk(k) - dt * 0.5 * (hok + hnk) * g * zx;
-    v = (a4 - a3 * qu) / (a2 - a3 * ru);
+    const T a3 = qdiv(-an_k, hnkp1);
+    const T a2 = T(1) + qdiv(an_k, hnk) + qdiv(dt_t * T(rr(i, j)), T(0.5) * (hnk + hok));
+    const T a4 = qdiv(ukp1 * ao_k, hokp1) + uk * (1 - qdiv(ao_k, hok)) + dt_t * exk(k) -
+                 dt_t * T(0.5) * (hok + hnk) * g_t * zx_t;
+    v = qdiv(a4 - a3 * qu, a2 - a3 * ru);
   }
-  // back substitution (Res in QU) and its sum in ascending k
+  // back substitution (Res in QU) and its FP64 sum in ascending k
   double ResInt = 0.0;
-  ResInt = ResInt + v;
+  ResInt = ResInt + (double)v;
   QU(i, j, 1) = R3(v);
   for (k = 2; k <= kmax; ++k) {
-    v = (double)QU(i, j, k) - (double)RU(i, j, k) * v;
+    v = T(QU(i, j, k)) - T(RU(i, j, k)) * v;
     QU(i, j, k) = R3(v);
-    ResInt = ResInt + v;
+    ResInt = ResInt + (double)v;
   }
   const double Diff = (Uint(i, j) - ResInt) / (sso(i, j) + HX(i, j));
-  for (k = 1; k <= kmax; ++k) uu(i, j, k) = R3((double)QU(i, j, k) + HN(k) * Diff);
+  for (k = 1; k <= kmax; ++k) uu(i, j, k) = R3((double)QU(i, j, k) + (double)hn(i, j, k) * Diff);
 }
 
 // sigma_coordinates.F90:85-113 (equidistant sigma): layer heights of all levels 0..kmax.

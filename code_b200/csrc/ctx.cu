@@ -214,14 +214,20 @@ static int vdiff_api(getm_ctx* ctx, R dt, R cnpar, R avmol, R* S, const R* hn, c
 }
 
 template <class R>
-static int tracer_step(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, const R* hu, const R* hv,
-                       const R* ho, const R* hn, const R* nuh, int split, int hs, int vs, R AH, R cnpar, R avmol,
-                       int iters) {
+int tracer_step_impl(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, const R* hu, const R* hv,
+                     const R* ho, const R* hn, const R* nuh, int split, int hs, int vs, R AH, R cnpar, R avmol,
+                     int iters) {
   int rc = do_adv3d<R>(ctx, dt, f, uu, vv, ww, hu, hv, ho, hn, split, hs, vs, AH, GETM_H_TAG, nullptr, nullptr,
                        iters);
   if (rc) return rc;
   return vdiff_api<R>(ctx, dt, cnpar, avmol, f, hn, nuh, ctx->zmask, nullptr);
 }
+template int tracer_step_impl<double>(getm_ctx*, double, double*, const double*, const double*, const double*,
+                                      const double*, const double*, const double*, const double*, const double*, int,
+                                      int, int, double, double, double, int);
+template int tracer_step_impl<float>(getm_ctx*, float, float*, const float*, const float*, const float*,
+                                     const float*, const float*, const float*, const float*, const float*, int, int,
+                                     int, float, float, float, int);
 
 template <class R>
 static int content_api(getm_ctx* ctx, const R* f, const R* h, const int32_t* az, double* out) {
@@ -278,6 +284,8 @@ int getm_ctx_destroy(getm_ctx* ctx) {
   for (auto p : ctx->scr) cudaFree(p);
   cudaFree(ctx->bc_scr3);
   cudaFree(ctx->bc_scr2);
+  cudaFree(ctx->adj_scr);
+  cudaFree(ctx->adj_store);
   for (int t = 0; t < GETM_NTIMERS; ++t)
     for (auto& ev : ctx->pending[t]) ctx->pool.push_back(ev);
   for (auto& ev : ctx->pool) {
@@ -312,7 +320,7 @@ const char* getm_ctx_last_error(const getm_ctx* ctx) { return ctx ? ctx->err.c_s
 static const char* kTimerNames[GETM_NTIMERS] = {"adv_split_u", "adv_split_v", "adv_split_w", "adv_finalise",
                                                  "tracer_vdiff", "copy", "tracer_fused_uv",
                                                  "tracer_fused_wvu", "mode_split_2d", "macro_3d_other", "internal_pressure",
-                                                 "uv_momentum_3d", "reserved12", "reserved13", "reserved14",
+                                                 "uv_momentum_3d", "tracer_record", "tracer_adjoint", "reserved14",
                                                  "reserved15"};
 
 const char* getm_timer_name(int slot) {
@@ -444,7 +452,7 @@ int getm_tracer_step(getm_ctx* ctx, double dt, double* f, const double* uu, cons
                      const double* hu, const double* hv, const double* ho, const double* hn, const double* nuh,
                      int split, int hscheme, int vscheme, double AH, double cnpar, double avmol,
                      int adv_ver_iterations) {
-  return tracer_step<double>(ctx, dt, f, uu, vv, ww, hu, hv, ho, hn, nuh, split, hscheme, vscheme, AH, cnpar, avmol,
+  return tracer_step_impl<double>(ctx, dt, f, uu, vv, ww, hu, hv, ho, hn, nuh, split, hscheme, vscheme, AH, cnpar, avmol,
                              adv_ver_iterations);
 }
 
@@ -452,7 +460,7 @@ int getm_tracer_step_f32(getm_ctx* ctx, float dt, float* f, const float* uu, con
                          const float* hu, const float* hv, const float* ho, const float* hn, const float* nuh,
                          int split, int hscheme, int vscheme, float AH, float cnpar, float avmol,
                          int adv_ver_iterations) {
-  return tracer_step<float>(ctx, dt, f, uu, vv, ww, hu, hv, ho, hn, nuh, split, hscheme, vscheme, AH, cnpar, avmol,
+  return tracer_step_impl<float>(ctx, dt, f, uu, vv, ww, hu, hv, ho, hn, nuh, split, hscheme, vscheme, AH, cnpar, avmol,
                             adv_ver_iterations);
 }
 

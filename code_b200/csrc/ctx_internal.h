@@ -40,6 +40,12 @@ struct getm_ctx {
   void* bc_scr3 = nullptr;
   size_t bc_scr3_bytes = 0;
   double* bc_scr2 = nullptr;
+  // scratch of the tracer adjoint: ADJ_NSCR 3D arrays (adjoint.cu) and the checkpoints and tapes
+  // of the checkpointed gradient
+  void* adj_scr = nullptr;
+  size_t adj_scr_bytes = 0;
+  void* adj_store = nullptr;
+  size_t adj_store_bytes = 0;
 };
 
 namespace {
@@ -138,3 +144,8 @@ static inline bool grid_for_tag(const getm_ctx* ctx, int tag, getm_adv_grid* g) 
 template <class R>
 int do_adv3d(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, const R* hu, const R* hv,
              const R* ho, const R* hn, int split, int hs, int vs, R AH, int tag, R* hires, R* advres, int iters);
+// Tracer step: do_advection_3d(H_TAG) then the implicit vertical diffusion (ctx.cu).
+template <class R>
+int tracer_step_impl(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, const R* hu, const R* hv,
+                     const R* ho, const R* hn, const R* nuh, int split, int hs, int vs, R AH, R cnpar, R avmol,
+                     int iters);

@@ -53,6 +53,90 @@ __device__ __forceinline__ R recon_s(R cfl, R fuu, R fu, R fd) {
   }
 }
 
+// Limiter branch taken by recon_s for one face, for the adjoint (0 = first-order value fu).
+//   SUPERBEE: 1 L=2r, 2 L=1, 3 L=r, 4 L=2;  MUSCL: 1 L=2r, 2 L=(1+r)/2, 3 L=2;
+//   P2_PDM: 1 L=2r/(cfl+1e-10), 2 L=(1/2+x)+(1/2-x)r, 3 L=2/(1-cfl);  P2: 1.
+// The comparisons are those of recon_s (the reference's MIN/MAX order in FP64, the magnitude form
+// in FP32), so the code names the branch whose value the forward sweep used.
+template <class R, int S>
+__device__ __forceinline__ uint8_t recon_code(R cfl, R fuu, R fu, R fd) {
+  if constexpr (S == P2) {
+    return 1;
+  } else if constexpr (S == SUPERBEE || S == MUSCL || S == P2_PDM) {
+    const R df = fd - fu, du = fu - fuu;
+    if (!(df * du > R(0))) return 0;
+    R t1, t2, t3, t4;
+    if constexpr (sizeof(R) == 8) {
+      const R ratio = du / df;
+      if constexpr (S == SUPERBEE) {
+        t1 = R(2) * ratio; t2 = R(1); t3 = ratio; t4 = R(2);
+      } else if constexpr (S == MUSCL) {
+        t1 = R(2) * ratio; t2 = R(0.5) * (R(1) + ratio); t3 = R(2); t4 = R(0);
+      } else {
+        const R x = (R(1) / R(6)) * (R(1) - R(2) * cfl);
+        t2 = (R(0.5) + x) + (R(0.5) - x) * ratio;
+        t1 = R(2) * ratio / (cfl + R(1.e-10));
+        t3 = R(2) / (R(1) - cfl); t4 = R(0);
+      }
+    } else {
+      const float a = fabsf(du), b = fabsf(df);
+      if constexpr (S == SUPERBEE) {
+        t1 = 2.f * a; t2 = b; t3 = a; t4 = 2.f * b;
+      } else if constexpr (S == MUSCL) {
+        t1 = 2.f * a; t2 = 0.5f * (b + a); t3 = 2.f * b; t4 = 0.f;
+      } else {
+        const float x = (1.f / 6.f) * (1.f - 2.f * cfl);
+        t1 = __fdividef(2.f * a, cfl + 1.e-10f);
+        t2 = (0.5f + x) * b + (0.5f - x) * a;
+        t3 = __fdividef(2.f * b, 1.f - cfl); t4 = 0.f;
+      }
+    }
+    if constexpr (S == SUPERBEE) {
+      const R m1 = (t2 < t1) ? t2 : t1, m2 = (t4 < t3) ? t4 : t3;
+      const uint8_t c1 = (t2 < t1) ? 2 : 1, c2 = (t4 < t3) ? 4 : 3;
+      return (m2 > m1) ? c2 : c1;
+    } else {
+      (void)t4;
+      const R m = (t2 < t1) ? t2 : t1;
+      const uint8_t c = (t2 < t1) ? 2 : 1;
+      return (t3 < m) ? 3 : c;
+    }
+  } else {
+    (void)cfl; (void)fuu; (void)fu; (void)fd;
+    return 0;
+  }
+}
+
+// Derivative of the interface value fu + A*(fu-fuu) + B*(fd-fu) for limiter branch `code`
+// (the frozen-branch linearisation of recon_s).
+template <class R, int S>
+__device__ __forceinline__ void recon_coef(uint8_t code, R cfl, R& A, R& B) {
+  A = R(0);
+  B = R(0);
+  if (code == 0) return;
+  const R omc = R(1) - cfl;
+  if constexpr (S == SUPERBEE) {
+    if (code == 1) A = omc;
+    else if (code == 2) B = R(0.5) * omc;
+    else if (code == 3) A = R(0.5) * omc;
+    else B = omc;
+  } else if constexpr (S == MUSCL) {
+    if (code == 1) A = omc;
+    else if (code == 2) A = B = R(0.25) * omc;
+    else B = omc;
+  } else if constexpr (S == P2_PDM || S == P2) {
+    if (S == P2 || code == 2) {
+      const R x = (R(1) / R(6)) * (R(1) - R(2) * cfl);
+      A = R(0.5) * omc * (R(0.5) - x);
+      B = R(0.5) * omc * (R(0.5) + x);
+    } else if (code == 1) {
+      A = omc / (cfl + R(1.e-10));
+    } else {
+      B = R(1);
+    }
+  }
+}
+
 // Finite-volume update of one cell after a split step: hin = hio - dh is the new layer height and
 // advn the flux divergence (adv_split_u.F90:274-279, adv_split_w.F90:289-292).
 // FP64 keeps the reference's form (hio*fio - dt*advn)/hin, bit for bit. FP32 evaluates the same
@@ -72,22 +156,31 @@ __device__ __forceinline__ R fv_update(R hio, R dh, R hin, R fio, R dt, R advn) 
 
 // Flux through face q (between cells q and q+1) from staged values: f at q-1..q+2, flux masks at
 // q-1..q+1. cdx = dti/dx (used by FP32 only).
-template <class R, int S>
+// Courant number of a horizontal face (adv_split_u.F90:229-246); cdx = dti/dx is used by FP32.
+template <class R>
+__device__ __forceinline__ R face_cfl(bool pos, R Uf, R DUf, R dti, R cdx, R dxf) {
+  if constexpr (sizeof(R) == 8) {
+    (void)cdx;
+    return pos ? Uf / DUf * dti / dxf : -Uf / DUf * dti / dxf;
+  } else {
+    (void)dti; (void)dxf;
+    return __fdividef(fabsf(Uf) * cdx, DUf);
+  }
+}
+
+// With REC the limiter branch is written to *code (0 when the face is not limited).
+template <class R, int S, bool REC = false>
 __device__ __forceinline__ R face_flux_s(R Uf, R DUf, R fm1, R f0, R f1, R f2, bool mm1, bool m0, bool mp1,
-                                         R dti, R cdx, R AH, bool use_AH, R dxf) {
+                                         R dti, R cdx, R AH, bool use_AH, R dxf, uint8_t* code = nullptr) {
+  if (REC) *code = 0;
   if (!m0) return R(0);
   const bool pos = Uf > R(0);
   R fu = pos ? f0 : f1;
   if (S != UPSTREAM && (pos ? mm1 : mp1)) {
     const R fuu = pos ? fm1 : f2;
     const R fd = pos ? f1 : f0;
-    R cfl;
-    if constexpr (sizeof(R) == 8) {
-      (void)cdx;
-      cfl = pos ? Uf / DUf * dti / dxf : -Uf / DUf * dti / dxf;
-    } else {
-      cfl = __fdividef(fabsf(Uf) * cdx, DUf);
-    }
+    const R cfl = face_cfl<R>(pos, Uf, DUf, dti, cdx, dxf);
+    if (REC) *code = recon_code<R, S>(cfl, fuu, fu, fd);
     fu = recon_s<R, S>(cfl, fuu, fu, fd);
   }
   R fl = Uf * fu;
@@ -102,15 +195,37 @@ __device__ __forceinline__ R face_flux_s(R Uf, R DUf, R fm1, R f0, R f1, R f2, b
 // alias fi_dst (callers ping-pong); fi_src may be f or alias fi_dst, Di_src may alias Di_dst.
 constexpr int TU = 128;             // u sweep: cells per block along i
 constexpr int TVX = 32, TVY = 8;    // v sweep: tile of 32 (i) x 8 (j) cells
+constexpr int NKB = 8;              // levels per block (the 2D masks are staged once for them)
 
-// u sweep (adv_split_u.F90:222-285) over one (j, k) row segment of TU cells.
-template <class R, int S>
-__global__ void __launch_bounds__(TU) k_sweep_u_tile(Dev d, R dt, R splitfac, R AH,
-                                                     const R* __restrict__ f, const R* fi_src, R* fi_dst,
-                                                     const R* Di_src, R* Di_dst, R* adv,
+// Constants of one sweep, computed on the host in R (the same IEEE operations the reference
+// performs per cell, so FP64 results are unchanged): dti = splitfac*dt, dxf = the face spacing
+// along the sweep (DXU / DYV), dyf = the face width (DYU / DXV), cdx = dti/dxf.
+template <class R>
+struct SweepC {
+  R dt, splitfac, AH, dti, dxf, dyf, ard1, cdx;
+};
+
+template <class R>
+inline SweepC<R> sweep_consts(const Dev& d, int dir, R dt, R splitfac, R AH) {
+  SweepC<R> c;
+  c.dt = dt;
+  c.splitfac = splitfac;
+  c.AH = AH;
+  c.dti = splitfac * dt;
+  c.dxf = dir == 0 ? R(d.dx) : R(d.dy);
+  c.dyf = dir == 0 ? R(d.dy) : R(d.dx);
+  c.ard1 = R(d.ard1);
+  c.cdx = c.dti / c.dxf;
+  return c;
+}
+
+// u sweep (adv_split_u.F90:222-285) over one row segment of TU cells, for up to NKB levels.
+template <class R, int S, bool REC>
+__global__ void __launch_bounds__(TU) k_sweep_u_tile(Dev d, SweepC<R> C, int nk, const R* __restrict__ f,
+                                                     const R* fi_src, R* fi_dst, const R* Di_src, R* Di_dst, R* adv,
                                                      const R* __restrict__ U, const R* __restrict__ DU,
                                                      const uint8_t* __restrict__ mflux,
-                                                     const uint8_t* __restrict__ mupd) {
+                                                     const uint8_t* __restrict__ mupd, uint8_t* code) {
   __shared__ R sf[TU + 4];      // f(i0-2 .. i0+TU+1)
   __shared__ R sU[TU + 1];      // U(i0-1 .. i0+TU-1)
   __shared__ R sDU[TU + 1];
@@ -118,68 +233,77 @@ __global__ void __launch_bounds__(TU) k_sweep_u_tile(Dev d, R dt, R splitfac, R 
   __shared__ R sfl[TU + 1];     // flux of faces i0-1 .. i0+TU-1
   const int t = threadIdx.x;
   const int ni = d.ni();
-  const int ii0 = blockIdx.x * TU;  // array index of the tile's first cell
-  const int jj = blockIdx.y;
-  const long long crow = (long long)jj * d.sj;
-  const long long row = crow + (long long)blockIdx.z * d.sk;
-  // stage inputs (array indices outside 0..ni-1 are never used by a valid face)
+  const int ii0 = blockIdx.x * TU;
+  const long long crow = (long long)blockIdx.y * d.sj;
+  const int k0 = blockIdx.z * NKB;
+  const int k1 = min(k0 + NKB, nk);
+  constexpr int sub = (S == UPSTREAM) ? 0 : 1;
+  const bool use_AH = C.AH > R(0);
+  // masks of the row (levels share them)
   for (int q = t; q < TU + 4; q += TU) {
     const int ii = ii0 - 2 + q;
-    const bool ok = ii >= 0 && ii < ni;
-    sf[q] = ok ? f[row + ii] : R(0);
-    sm[q] = ok ? mflux[crow + ii] : 0;
+    sm[q] = (ii >= 0 && ii < ni) ? mflux[crow + ii] : 0;
   }
-  for (int q = t; q < TU + 1; q += TU) {
-    const int ii = ii0 - 1 + q;
-    const bool ok = ii >= 0 && ii < ni;
-    sU[q] = ok ? U[row + ii] : R(0);
-    sDU[q] = ok ? DU[row + ii] : R(0);
-  }
-  __syncthreads();
-  constexpr int sub = (S == UPSTREAM) ? 0 : 1;
-  const R dti = splitfac * dt;
-  const bool use_AH = AH > R(0);
-  const R dxf = R(d.dx), dyf = R(d.dy), ard1 = R(d.ard1);
-  const R cdx = dti / dxf;
-  // faces: face index in array coordinates fa = ii0-1+q; valid if fa in [sub, ni-2-sub]
-  for (int q = t; q < TU + 1; q += TU) {
-    const int fa = ii0 - 1 + q;
-    R fl = R(0);
-    if (fa >= sub && fa <= ni - 2 - sub)
-      fl = face_flux_s<R, S>(sU[q], sDU[q], sf[q], sf[q + 1], sf[q + 2], sf[q + 3], sm[q] != 0, sm[q + 1] != 0,
-                             sm[q + 2] != 0, dti, cdx, AH, use_AH, dxf);
-    sfl[q] = fl;
-  }
-  __syncthreads();
   const int ii = ii0 + t;
-  if (ii >= ni) return;
-  const long long p = row + ii;
-  const long long c = crow + ii;
-  const bool in_range = (ii >= 1 + sub) && (ii <= ni - 2 - sub);
-  const R fio = (fi_src == f) ? sf[t + 2] : fi_src[p];
-  if (in_range && mupd[c]) {
-    const R fe = sfl[t + 1], fw = sfl[t];
-    const R Dio = Di_src[p];
-    const R dD = dti * (sU[t + 1] * dyf - sU[t] * dyf) * ard1;
-    const R Dn = Dio - dD;
-    const R advn = splitfac * (fe * dyf - fw * dyf) * ard1;
-    Di_dst[p] = Dn;
-    fi_dst[p] = fv_update<R>(Dio, dD, Dn, fio, dt, advn);
-    if (adv) adv[p] = adv[p] + advn;
-  } else {
-    if (fi_dst != fi_src) fi_dst[p] = fio;
-    if (Di_dst != Di_src) Di_dst[p] = Di_src[p];
+  const bool own = ii < ni;
+  const bool upd = own && (ii >= 1 + sub) && (ii <= ni - 2 - sub) && mupd[crow + ii];
+  const bool fi_is_f = (fi_src == f);
+  for (int k = k0; k < k1; ++k) {
+    const long long row = crow + (long long)k * d.sk;
+    const R* fr = f + row;
+    for (int q = t; q < TU + 4; q += TU) {
+      const int i2 = ii0 - 2 + q;
+      sf[q] = (i2 >= 0 && i2 < ni) ? fr[i2] : R(0);
+    }
+    for (int q = t; q < TU + 1; q += TU) {
+      const int i2 = ii0 - 1 + q;
+      const bool ok = i2 >= 0 && i2 < ni;
+      sU[q] = ok ? U[row + i2] : R(0);
+      sDU[q] = ok ? DU[row + i2] : R(0);
+    }
+    // own-cell inputs, in flight during the face phase
+    const R Dio = own ? Di_src[row + ii] : R(0);
+    const R fio_g = (own && !fi_is_f) ? fi_src[row + ii] : R(0);
+    __syncthreads();
+    for (int q = t; q < TU + 1; q += TU) {
+      const int fa = ii0 - 1 + q;
+      R fl = R(0);
+      uint8_t cd = 0;
+      if (fa >= sub && fa <= ni - 2 - sub)
+        fl = face_flux_s<R, S, REC>(sU[q], sDU[q], sf[q], sf[q + 1], sf[q + 2], sf[q + 3], sm[q] != 0,
+                                    sm[q + 1] != 0, sm[q + 2] != 0, C.dti, C.cdx, C.AH, use_AH, C.dxf, &cd);
+      sfl[q] = fl;
+      if (REC && q >= 1 && fa < ni) code[row + fa] = cd;  // face fa is stored at its left cell
+    }
+    __syncthreads();
+    if (own) {
+      const long long p = row + ii;
+      const R fio = fi_is_f ? sf[t + 2] : fio_g;
+      if (upd) {
+        const R fe = sfl[t + 1], fw = sfl[t];
+        const R dD = C.dti * (sU[t + 1] * C.dyf - sU[t] * C.dyf) * C.ard1;
+        const R Dn = Dio - dD;
+        const R advn = C.splitfac * (fe * C.dyf - fw * C.dyf) * C.ard1;
+        Di_dst[p] = Dn;
+        fi_dst[p] = fv_update<R>(Dio, dD, Dn, fio, C.dt, advn);
+        if (adv) adv[p] = adv[p] + advn;
+      } else {
+        if (fi_dst != fi_src) fi_dst[p] = fio;
+        if (Di_dst != Di_src) Di_dst[p] = Dio;
+      }
+    }
+    __syncthreads();  // sf/sU/sfl are restaged for the next level
   }
 }
 
-// v sweep (adv_split_v.F90:79-135) over a tile of TVX x TVY cells of one level.
-template <class R, int S>
-__global__ void __launch_bounds__(TVX * TVY) k_sweep_v_tile(Dev d, R dt, R splitfac, R AH,
-                                                            const R* __restrict__ f, const R* fi_src, R* fi_dst,
-                                                            const R* Di_src, R* Di_dst, R* adv,
-                                                            const R* __restrict__ V, const R* __restrict__ DV,
+// v sweep (adv_split_v.F90:79-135) over a tile of TVX x TVY cells, for up to NKB levels.
+template <class R, int S, bool REC>
+__global__ void __launch_bounds__(TVX * TVY) k_sweep_v_tile(Dev d, SweepC<R> C, int nk, const R* __restrict__ f,
+                                                            const R* fi_src, R* fi_dst, const R* Di_src, R* Di_dst,
+                                                            R* adv, const R* __restrict__ V,
+                                                            const R* __restrict__ DV,
                                                             const uint8_t* __restrict__ mflux,
-                                                            const uint8_t* __restrict__ mupd) {
+                                                            const uint8_t* __restrict__ mupd, uint8_t* code) {
   __shared__ R sf[TVY + 4][TVX];       // f(j0-2 .. j0+TVY+1)
   __shared__ R sV[TVY + 1][TVX];       // V(j0-1 .. j0+TVY-1)
   __shared__ R sDV[TVY + 1][TVX];
@@ -189,55 +313,66 @@ __global__ void __launch_bounds__(TVX * TVY) k_sweep_v_tile(Dev d, R dt, R split
   const int ni = d.ni(), nj = d.nj();
   const int ii = blockIdx.x * TVX + tx;
   const int jj0 = blockIdx.y * TVY;
-  const long long lev = (long long)blockIdx.z * d.sk;
+  const int k0 = blockIdx.z * NKB;
+  const int k1 = min(k0 + NKB, nk);
   const bool iok = ii < ni;
+  const long long sj = d.sj;
+  constexpr int sub = (S == UPSTREAM) ? 0 : 1;
+  const bool use_AH = C.AH > R(0);
   for (int q = ty; q < TVY + 4; q += TVY) {
     const int jj = jj0 - 2 + q;
-    const bool ok = iok && jj >= 0 && jj < nj;
-    const long long c = (long long)jj * d.sj + ii;
-    sf[q][tx] = ok ? f[lev + c] : R(0);
-    sm[q][tx] = ok ? mflux[c] : 0;
+    sm[q][tx] = (iok && jj >= 0 && jj < nj) ? mflux[(long long)jj * sj + ii] : 0;
   }
-  for (int q = ty; q < TVY + 1; q += TVY) {
-    const int jj = jj0 - 1 + q;
-    const bool ok = iok && jj >= 0 && jj < nj;
-    const long long c = (long long)jj * d.sj + ii;
-    sV[q][tx] = ok ? V[lev + c] : R(0);
-    sDV[q][tx] = ok ? DV[lev + c] : R(0);
-  }
-  __syncthreads();
-  constexpr int sub = (S == UPSTREAM) ? 0 : 1;
-  const R dti = splitfac * dt;
-  const bool use_AH = AH > R(0);
-  const R dxf = R(d.dy), dyf = R(d.dx), ard1 = R(d.ard1);  // DYV, DXV
-  const R cdx = dti / dxf;
-  for (int q = ty; q < TVY + 1; q += TVY) {
-    const int fa = jj0 - 1 + q;
-    R fl = R(0);
-    if (iok && fa >= sub && fa <= nj - 2 - sub)
-      fl = face_flux_s<R, S>(sV[q][tx], sDV[q][tx], sf[q][tx], sf[q + 1][tx], sf[q + 2][tx], sf[q + 3][tx],
-                             sm[q][tx] != 0, sm[q + 1][tx] != 0, sm[q + 2][tx] != 0, dti, cdx, AH, use_AH, dxf);
-    sfl[q][tx] = fl;
-  }
-  __syncthreads();
   const int jj = jj0 + ty;
-  if (!iok || jj >= nj) return;
-  const long long c = (long long)jj * d.sj + ii;
-  const long long p = lev + c;
-  const bool in_range = (jj >= 1 + sub) && (jj <= nj - 2 - sub);
-  const R fio = (fi_src == f) ? sf[ty + 2][tx] : fi_src[p];
-  if (in_range && mupd[c]) {
-    const R fe = sfl[ty + 1][tx], fw = sfl[ty][tx];
-    const R Dio = Di_src[p];
-    const R dD = dti * (sV[ty + 1][tx] * dyf - sV[ty][tx] * dyf) * ard1;
-    const R Dn = Dio - dD;
-    const R advn = splitfac * (fe * dyf - fw * dyf) * ard1;
-    Di_dst[p] = Dn;
-    fi_dst[p] = fv_update<R>(Dio, dD, Dn, fio, dt, advn);
-    if (adv) adv[p] = adv[p] + advn;
-  } else {
-    if (fi_dst != fi_src) fi_dst[p] = fio;
-    if (Di_dst != Di_src) Di_dst[p] = Di_src[p];
+  const bool own = iok && jj < nj;
+  const long long c = (long long)jj * sj + ii;
+  const bool upd = own && (jj >= 1 + sub) && (jj <= nj - 2 - sub) && mupd[c];
+  const bool fi_is_f = (fi_src == f);
+  for (int k = k0; k < k1; ++k) {
+    const long long lev = (long long)k * d.sk;
+    for (int q = ty; q < TVY + 4; q += TVY) {
+      const int j2 = jj0 - 2 + q;
+      sf[q][tx] = (iok && j2 >= 0 && j2 < nj) ? f[lev + (long long)j2 * sj + ii] : R(0);
+    }
+    for (int q = ty; q < TVY + 1; q += TVY) {
+      const int j2 = jj0 - 1 + q;
+      const bool ok = iok && j2 >= 0 && j2 < nj;
+      const long long c2 = lev + (long long)j2 * sj + ii;
+      sV[q][tx] = ok ? V[c2] : R(0);
+      sDV[q][tx] = ok ? DV[c2] : R(0);
+    }
+    const R Dio = own ? Di_src[lev + c] : R(0);
+    const R fio_g = (own && !fi_is_f) ? fi_src[lev + c] : R(0);
+    __syncthreads();
+    for (int q = ty; q < TVY + 1; q += TVY) {
+      const int fa = jj0 - 1 + q;
+      R fl = R(0);
+      uint8_t cd = 0;
+      if (iok && fa >= sub && fa <= nj - 2 - sub)
+        fl = face_flux_s<R, S, REC>(sV[q][tx], sDV[q][tx], sf[q][tx], sf[q + 1][tx], sf[q + 2][tx],
+                                    sf[q + 3][tx], sm[q][tx] != 0, sm[q + 1][tx] != 0, sm[q + 2][tx] != 0, C.dti,
+                                    C.cdx, C.AH, use_AH, C.dxf, &cd);
+      sfl[q][tx] = fl;
+      if (REC && q >= 1 && iok && fa < nj) code[lev + (long long)fa * sj + ii] = cd;
+    }
+    __syncthreads();
+    if (own) {
+      const long long p = lev + c;
+      const R fio = fi_is_f ? sf[ty + 2][tx] : fio_g;
+      if (upd) {
+        const R fe = sfl[ty + 1][tx], fw = sfl[ty][tx];
+        const R dD = C.dti * (sV[ty + 1][tx] * C.dyf - sV[ty][tx] * C.dyf) * C.ard1;
+        const R Dn = Dio - dD;
+        const R advn = C.splitfac * (fe * C.dyf - fw * C.dyf) * C.ard1;
+        Di_dst[p] = Dn;
+        fi_dst[p] = fv_update<R>(Dio, dD, Dn, fio, C.dt, advn);
+        if (adv) adv[p] = adv[p] + advn;
+      } else {
+        if (fi_dst != fi_src) fi_dst[p] = fio;
+        if (Di_dst != Di_src) Di_dst[p] = Dio;
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -247,27 +382,34 @@ __global__ void __launch_bounds__(TVX * TVY) k_sweep_v_tile(Dev d, R dt, R split
 // level of f and hi is read before it is overwritten -- f, fi and hi may therefore alias. The
 // window reaches two levels ahead of the face being computed so that several loads per thread
 // are in flight.
-template <class R, int S>
+// Courant number of vertical face k (adv_split_w.F90:167-169) from the layer heights around it.
+template <class R>
+__device__ __forceinline__ R wface_cfl(R w, R dti, R hk, R hkp1) {
+  if constexpr (sizeof(R) == 8) return fabs(w) * dti / (R(0.5) * (hk + hkp1));
+  else return __fdividef(2.f * fabsf(w) * dti, hk + hkp1);
+}
+
+template <class R, int S, bool REC = false>
 __device__ __forceinline__ R wface_s(int k, int kshift, int kmax, R dti, R w, R fkm1, R fk, R fkp1, R fkp2,
-                                     R hk, R hkp1) {
+                                     R hk, R hkp1, uint8_t* code = nullptr) {
   const bool pos = w > R(0);
   R fu = pos ? fk : fkp1;
+  if (REC) *code = 0;
   if (S != UPSTREAM && (pos ? (k > 1 - kshift) : (k < kmax - 1))) {
     const R fuu = pos ? fkm1 : fkp2;
     const R fd = pos ? fkp1 : fk;
-    R cfl;
-    if constexpr (sizeof(R) == 8) cfl = fabs(w) * dti / (R(0.5) * (hk + hkp1));
-    else cfl = __fdividef(2.f * fabsf(w) * dti, hk + hkp1);
+    const R cfl = wface_cfl<R>(w, dti, hk, hkp1);
+    if (REC) *code = recon_code<R, S>(cfl, fuu, fu, fd);
     fu = recon_s<R, S>(cfl, fuu, fu, fd);
   }
   return w * fu;
 }
 
-template <class R, int S>
+template <class R, int S, bool REC>
 __global__ void __launch_bounds__(128) k_sweep_w(Dev d, R dt, R splitfac, int kshift,
                                                  const R* f, const R* fi_src, R* fi_dst, R* hi, R* adv,
                                                  const R* __restrict__ ww,
-                                                 const int32_t* __restrict__ az) {
+                                                 const int32_t* __restrict__ az, uint8_t* code) {
   const int ii = blockIdx.x * blockDim.x + threadIdx.x;
   const int jj = blockIdx.y * blockDim.y + threadIdx.y;
   // columns i = imin-2..imax+1, j = jmin-2..jmax+1 (adv_split_w.F90:160-162)
@@ -282,7 +424,11 @@ __global__ void __launch_bounds__(128) k_sweep_w(Dev d, R dt, R splitfac, int ks
   auto H = [&](int k) -> R { return (k >= 0 && k <= kmax) ? hi[c + k * sk] : R(0); };
   auto W = [&](int k) -> R { return (k <= kmax) ? ww[c + k * sk] : R(0); };
   R wprev = R(0);  // wflux(k-1); wflux(0) = 0 unless W_TAG computes face 0
-  if (kshift == 1) wprev = wface_s<R, S>(0, 1, kmax, dti, ww[c], R(0), F(0), F(1), F(2), H(0), H(1));
+  if (kshift == 1) {
+    uint8_t cd = 0;
+    wprev = wface_s<R, S, REC>(0, 1, kmax, dti, ww[c], R(0), F(0), F(1), F(2), H(0), H(1), &cd);
+    if (REC) code[c] = cd;
+  }
   // window for face k = 1: f(0..4), hi(1..3), ww(0..2)
   R a = F(0), b = F(1), e = F(2), g = F(3), g2 = F(4);
   R hA = H(1), hB = H(2), hC = H(3);
@@ -295,7 +441,11 @@ __global__ void __launch_bounds__(128) k_sweep_w(Dev d, R dt, R splitfac, int ks
     const R fio = fi_is_f ? b : fi_src[c + k * sk];
     const R advo = adv ? adv[c + k * sk] : R(0);
     R wfl = R(0);
-    if (k <= kmax - 1) wfl = wface_s<R, S>(k, kshift, kmax, dti, wk, a, b, e, g, hA, hB);
+    if (k <= kmax - 1) {
+      uint8_t cd = 0;
+      wfl = wface_s<R, S, REC>(k, kshift, kmax, dti, wk, a, b, e, g, hA, hB, &cd);
+      if (REC) code[c + k * sk] = cd;
+    }
     const R hio = hA;
     const R dh = dti * (wk - wkm1);
     const R hin = hio - dh;

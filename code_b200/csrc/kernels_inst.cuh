@@ -24,19 +24,29 @@ static int dispatch_scheme(int scheme, Fn&& fn) {
 template <class R, int DIR>
 int run_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int scheme, R AH, const R* f,
                 const R* fi_src, R* fi_dst, const R* Di_src, R* Di_dst, R* adv, const R* U, const R* DU,
-                const uint8_t* mflux, const uint8_t* mupd) {
+                const uint8_t* mflux, const uint8_t* mupd, uint8_t* code) {
   if (nk <= 0) return 0;
+  const SweepC<R> C = sweep_consts<R>(d, DIR, dt, splitfac, AH);
+  const int nz = (nk + NKB - 1) / NKB;
   return dispatch_scheme(scheme, [&](auto sc) {
     constexpr int S = decltype(sc)::value;
     if (DIR == 0) {
-      dim3 grd((d.ni() + TU - 1) / TU, d.nj(), nk);
-      k_sweep_u_tile<R, S><<<grd, TU, 0, s>>>(d, dt, splitfac, AH, f, fi_src, fi_dst, Di_src, Di_dst, adv, U, DU,
-                                              mflux, mupd);
+      dim3 grd((d.ni() + TU - 1) / TU, d.nj(), nz);
+      if (code)
+        k_sweep_u_tile<R, S, true><<<grd, TU, 0, s>>>(d, C, nk, f, fi_src, fi_dst, Di_src, Di_dst, adv, U, DU,
+                                                      mflux, mupd, code);
+      else
+        k_sweep_u_tile<R, S, false><<<grd, TU, 0, s>>>(d, C, nk, f, fi_src, fi_dst, Di_src, Di_dst, adv, U, DU,
+                                                       mflux, mupd, nullptr);
     } else {
       dim3 blk(TVX, TVY, 1);
-      dim3 grd((d.ni() + TVX - 1) / TVX, (d.nj() + TVY - 1) / TVY, nk);
-      k_sweep_v_tile<R, S><<<grd, blk, 0, s>>>(d, dt, splitfac, AH, f, fi_src, fi_dst, Di_src, Di_dst, adv, U,
-                                               DU, mflux, mupd);
+      dim3 grd((d.ni() + TVX - 1) / TVX, (d.nj() + TVY - 1) / TVY, nz);
+      if (code)
+        k_sweep_v_tile<R, S, true><<<grd, blk, 0, s>>>(d, C, nk, f, fi_src, fi_dst, Di_src, Di_dst, adv, U, DU,
+                                                       mflux, mupd, code);
+      else
+        k_sweep_v_tile<R, S, false><<<grd, blk, 0, s>>>(d, C, nk, f, fi_src, fi_dst, Di_src, Di_dst, adv, U, DU,
+                                                        mflux, mupd, nullptr);
     }
     return (int)cudaGetLastError();
   });
@@ -45,8 +55,9 @@ int run_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int sche
 template <class R>
 int run_sweep_w(const Dev& d, cudaStream_t s, R dt, R splitfac, int scheme, int kshift, int itersmax,
                 const R* f, const R* fi_src, R* fi_dst, R* hi, R* adv, const R* ww, const int32_t* az,
-                unsigned long long* warn) {
+                unsigned long long* warn, uint8_t* code) {
   if (itersmax > 1) {
+    if (code) return (int)cudaErrorInvalidValue;
     dim3 blk(32, 2, 1);
     dim3 grd((d.ni() - 1 + blk.x - 1) / blk.x, (d.nj() - 1 + blk.y - 1) / blk.y, 1);
     k_sweep_w_iter<R><<<grd, blk, 0, s>>>(d, dt, splitfac, scheme, kshift, itersmax, f, fi_src, fi_dst, hi,
@@ -57,7 +68,11 @@ int run_sweep_w(const Dev& d, cudaStream_t s, R dt, R splitfac, int scheme, int 
     constexpr int S = decltype(sc)::value;
     dim3 blk(64, 2, 1);
     dim3 grd((d.ni() - 1 + blk.x - 1) / blk.x, (d.nj() - 1 + blk.y - 1) / blk.y, 1);
-    k_sweep_w<R, S><<<grd, blk, 0, s>>>(d, dt, splitfac, kshift, f, fi_src, fi_dst, hi, adv, ww, az);
+    if (code)
+      k_sweep_w<R, S, true><<<grd, blk, 0, s>>>(d, dt, splitfac, kshift, f, fi_src, fi_dst, hi, adv, ww, az, code);
+    else
+      k_sweep_w<R, S, false><<<grd, blk, 0, s>>>(d, dt, splitfac, kshift, f, fi_src, fi_dst, hi, adv, ww, az,
+                                                 nullptr);
     return (int)cudaGetLastError();
   });
 }
@@ -117,13 +132,15 @@ int run_check_range(const Dev& d, cudaStream_t s, const R* f, const int32_t* az,
 // explicit instantiations for GB_REAL
 template int run_sweep_h<GB_REAL, 0>(const Dev&, cudaStream_t, int, GB_REAL, GB_REAL, int, GB_REAL,
                                      const GB_REAL*, const GB_REAL*, GB_REAL*, const GB_REAL*, GB_REAL*,
-                                     GB_REAL*, const GB_REAL*, const GB_REAL*, const uint8_t*, const uint8_t*);
+                                     GB_REAL*, const GB_REAL*, const GB_REAL*, const uint8_t*, const uint8_t*,
+                                     uint8_t*);
 template int run_sweep_h<GB_REAL, 1>(const Dev&, cudaStream_t, int, GB_REAL, GB_REAL, int, GB_REAL,
                                      const GB_REAL*, const GB_REAL*, GB_REAL*, const GB_REAL*, GB_REAL*,
-                                     GB_REAL*, const GB_REAL*, const GB_REAL*, const uint8_t*, const uint8_t*);
+                                     GB_REAL*, const GB_REAL*, const GB_REAL*, const uint8_t*, const uint8_t*,
+                                     uint8_t*);
 template int run_sweep_w<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL, int, int, int, const GB_REAL*,
                                   const GB_REAL*, GB_REAL*, GB_REAL*, GB_REAL*, const GB_REAL*, const int32_t*,
-                                  unsigned long long*);
+                                  unsigned long long*, uint8_t*);
 template int run_finalise<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL*, const GB_REAL*, const GB_REAL*,
                                    const GB_REAL*, const uint8_t*);
 template int run_vdiff<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL, GB_REAL, GB_REAL*, const GB_REAL*,
@@ -135,6 +152,33 @@ template int run_content<GB_REAL>(const Dev&, cudaStream_t, const GB_REAL*, cons
 template int run_check_range<GB_REAL>(const Dev&, cudaStream_t, const GB_REAL*, const int32_t*, GB_REAL,
                                       GB_REAL, unsigned long long*);
 
+}  // namespace gb
+
+// ---- fused 2D momentum advection ----
+#include "adv2d_fused.cuh"
+namespace gb {
+template int run_uvadv2d_fused<GB_REAL>(const Dev&, cudaStream_t, int, GB_REAL, int, const double*, const double*,
+                                        const double*, const double*, const uint8_t*, const uint8_t*,
+                                        const uint8_t*, const uint8_t*, double*);
+}  // namespace gb
+
+// ---- adjoint of the tracer step ----
+#include "adjoint.cuh"
+namespace gb {
+template int run_adj_heights<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, int, bool, const GB_REAL*, const GB_REAL*,
+                                      const GB_REAL*, const GB_REAL*, const uint8_t*, const uint8_t*,
+                                      const int32_t*, GB_REAL*, GB_REAL*, GB_REAL*, GB_REAL*);
+template int run_adj_sweep_h<GB_REAL, 0>(const Dev&, cudaStream_t, int, GB_REAL, GB_REAL, int, GB_REAL,
+                                         const GB_REAL*, GB_REAL*, const GB_REAL*, const GB_REAL*, const GB_REAL*,
+                                         const uint8_t*, const uint8_t*, const uint8_t*);
+template int run_adj_sweep_h<GB_REAL, 1>(const Dev&, cudaStream_t, int, GB_REAL, GB_REAL, int, GB_REAL,
+                                         const GB_REAL*, GB_REAL*, const GB_REAL*, const GB_REAL*, const GB_REAL*,
+                                         const uint8_t*, const uint8_t*, const uint8_t*);
+template int run_adj_sweep_w<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL, int, int, const GB_REAL*,
+                                      GB_REAL*, const GB_REAL*, const GB_REAL*, const int32_t*, const uint8_t*);
+template int run_adj_vdiff<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL, GB_REAL, const GB_REAL*, GB_REAL*,
+                                    GB_REAL*, const GB_REAL*, const GB_REAL*, const GB_REAL*, const GB_REAL*,
+                                    const int32_t*, GB_REAL*, GB_REAL*);
 }  // namespace gb
 
 // ---- mode-split macro step (3D kernels) ----

@@ -12,16 +12,50 @@ constexpr int RED_BLOCKS = 1184;  // 8 x 148 SMs
 constexpr int RED_THREADS = 256;
 
 // Horizontal sweep over nk levels starting at the given level pointers. DIR 0 = u, 1 = v.
+// code != nullptr also writes the limiter branch of every face (one byte per face, stored at the
+// face's left / lower cell, same level pointer origin as f).
 template <class R, int DIR>
 int run_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int scheme, R AH, const R* f,
                 const R* fi_src, R* fi_dst, const R* Di_src, R* Di_dst, R* adv, const R* U, const R* DU,
-                const uint8_t* mflux, const uint8_t* mupd);
+                const uint8_t* mflux, const uint8_t* mupd, uint8_t* code = nullptr);
 
-// Vertical sweep on full 3D fields (level-0 pointers).
+// Vertical sweep on full 3D fields (level-0 pointers); code as above (face k stored at level k;
+// only without sub-iterations).
 template <class R>
 int run_sweep_w(const Dev& d, cudaStream_t s, R dt, R splitfac, int scheme, int kshift, int itersmax,
                 const R* f, const R* fi_src, R* fi_dst, R* hi, R* adv, const R* ww, const int32_t* az,
-                unsigned long long* warn);
+                unsigned long long* warn, uint8_t* code = nullptr);
+
+// Depth-averaged momentum advection of one micro step with HALFSPLIT (adv2d_fused.cuh): UEx
+// (dir 0, U-grid masks) or VEx (dir 1, V-grid masks) from U, V, DU, DV in one launch, arithmetic
+// in T; Ex is FP64.
+template <class T>
+int run_uvadv2d_fused(const Dev& d, cudaStream_t s, int dir, T dt, int scheme, const double* U, const double* V,
+                      const double* DU, const double* DV, const uint8_t* mflux_u, const uint8_t* mflux_v,
+                      const uint8_t* mupd_u, const uint8_t* mupd_v, double* Ex);
+
+// ---- adjoint of the tracer step (adjoint.cuh) ----
+// Layer heights before sweeps 2..5 of the HALFSPLIT sequence u/2 v/2 w v/2 u/2, from ho (levels
+// 1..kmax): H1 after u/2, H2 after v/2, H3 after w, H4 after v/2.
+template <class R>
+int run_adj_heights(const Dev& d, cudaStream_t s, R dt, int sub, bool has_w, const R* ho, const R* uu,
+                    const R* vv, const R* ww, const uint8_t* mupd_u, const uint8_t* mupd_v,
+                    const int32_t* az, R* H1, R* H2, R* H3, R* H4);
+// Adjoint of one horizontal sweep over nk levels (level pointers): gbar (cotangent of the sweep's
+// output) -> fbar (cotangent of its input). Dio = heights before the sweep.
+template <class R, int DIR>
+int run_adj_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int scheme, R AH, const R* gbar,
+                    R* fbar, const R* Dio, const R* U, const R* DU, const uint8_t* mflux, const uint8_t* mupd,
+                    const uint8_t* code);
+// Adjoint of the vertical sweep (full 3D fields); hi = heights before the sweep.
+template <class R>
+int run_adj_sweep_w(const Dev& d, cudaStream_t s, R dt, R splitfac, int scheme, int kshift, const R* gbar,
+                    R* fbar, const R* hi, const R* ww, const int32_t* az, const uint8_t* code);
+// Adjoint of the implicit vertical diffusion: fbar (cotangent of the new tracer) -> gbar
+// (cotangent of the old one); nubar += cotangent of nuh. g = old tracer, Sn = new tracer.
+template <class R>
+int run_adj_vdiff(const Dev& d, cudaStream_t s, R dt, R cnpar, R avmol, const R* fbar, R* gbar, R* nubar,
+                  const R* g, const R* Sn, const R* hn, const R* nuh, const int32_t* az, R* rus, R* qus);
 
 template <class R>
 int run_finalise(const Dev& d, cudaStream_t s, R dt, R* f, const R* ho, const R* adv, const R* hi,

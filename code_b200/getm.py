@@ -27,7 +27,8 @@ NOADV, UPSTREAM, UPSTREAM_2DH, P2, SUPERBEE, MUSCL, P2_PDM, J7, FCT, P2_2DH = ra
 H_TAG, D_TAG, U_TAG, V_TAG, W_TAG = 10, 20, 31, 32, 33
 
 ERRORS = {-1: "GETM_ERR_ARG", -2: "GETM_ERR_CUDA", -3: "GETM_ERR_UNSUPPORTED", -4: "GETM_ERR_CHECK",
-          -5: "GETM_ERR_TIMEOUT", -6: "GETM_ERR_NOMEM", -7: "GETM_ERR_STATE"}
+          -5: "GETM_ERR_TIMEOUT", -6: "GETM_ERR_NOMEM", -7: "GETM_ERR_STATE",
+          -8: "GETM_ERR_TOO_LARGE"}
 
 
 class GetmError(RuntimeError):
@@ -68,6 +69,12 @@ _PROTOS = {
     "getm_tracer_vdiff": [P, D, D, D, P, P, P, P, P],
     "getm_tracer_vdiff_f32": [P, F, F, F, P, P, P, P, P],
     "getm_tracer_vdiff_noalloc": [P, P, D, D, D, P, P, P, P, P],
+    "getm_tracer_step_record": [P, D, P, P, P, P, P, P, P, P, P, I, I, I, D, D, D, P, P],
+    "getm_tracer_step_record_f32": [P, F, P, P, P, P, P, P, P, P, P, I, I, I, F, F, F, P, P],
+    "getm_tracer_step_adjoint": [P, D, P, P, P, P, P, P, P, P, P, P, I, I, I, D, D, D, P, P],
+    "getm_tracer_step_adjoint_f32": [P, F, P, P, P, P, P, P, P, P, P, P, I, I, I, F, F, F, P, P],
+    "getm_tracer_gradient": [P, I, I, D, P, P, P, P, P, P, P, P, P, I, I, I, D, D, D, P, P, P, P],
+    "getm_tracer_gradient_f32": [P, I, I, F, P, P, P, P, P, P, P, P, P, I, I, I, F, F, F, P, P, P, P],
     "getm_tracer_step": [P, D, P, P, P, P, P, P, P, P, P, I, I, I, D, D, D, I],
     "getm_tracer_step_f32": [P, F, P, P, P, P, P, P, P, P, P, I, I, I, F, F, F, I],
     "getm_tracer_content": [P, P, P, P, P],
@@ -236,6 +243,43 @@ class Context:
         fn = self.L.getm_tracer_step if _is64(f) else self.L.getm_tracer_step_f32
         self._check(fn(self.h, dt, _ptr(f), _ptr(uu), _ptr(vv), _ptr(ww), _ptr(hu), _ptr(hv), _ptr(ho), _ptr(hn),
                        _ptr(nuh), split, hscheme, vscheme, AH, cnpar, avmol, adv_ver_iterations))
+
+    # ---- adjoint of the tracer step --------------------------------------------------------
+    def tape(self, dtype):
+        """Allocates the tape of one step: (codes uint8[5*n3], g of the field's dtype)."""
+        import torch
+
+        n3 = self.grid.ni * self.grid.nj * (self.grid.kmax + 1)
+        return (torch.empty(5 * n3, dtype=torch.uint8, device="cuda"),
+                torch.empty(self.grid.shape3(), dtype=dtype, device="cuda"))
+
+    def tracer_step_record(self, dt, f, uu, vv, ww, hu, hv, ho, hn, nuh, split, hscheme, vscheme, AH, cnpar,
+                           avmol, tape):
+        """getm_tracer_step that also writes the adjoint tape (see Context.tape)."""
+        _same_dtype(f, uu, vv, ww, hu, hv, ho, hn, nuh, tape[1])
+        fn = self.L.getm_tracer_step_record if _is64(f) else self.L.getm_tracer_step_record_f32
+        self._check(fn(self.h, dt, _ptr(f), _ptr(uu), _ptr(vv), _ptr(ww), _ptr(hu), _ptr(hv), _ptr(ho), _ptr(hn),
+                       _ptr(nuh), split, hscheme, vscheme, AH, cnpar, avmol, _ptr(tape[0]), _ptr(tape[1])))
+
+    def tracer_step_adjoint(self, dt, fbar, nubar, uu, vv, ww, hu, hv, ho, hn, nuh, split, hscheme, vscheme, AH,
+                            cnpar, avmol, tape):
+        """Adjoint of one recorded tracer step: fbar in place, nubar accumulated."""
+        _same_dtype(fbar, nubar, uu, vv, ww, hu, hv, ho, hn, nuh, tape[1])
+        fn = self.L.getm_tracer_step_adjoint if _is64(fbar) else self.L.getm_tracer_step_adjoint_f32
+        self._check(fn(self.h, dt, _ptr(fbar), _ptr(nubar), _ptr(uu), _ptr(vv), _ptr(ww), _ptr(hu), _ptr(hv),
+                       _ptr(ho), _ptr(hn), _ptr(nuh), split, hscheme, vscheme, AH, cnpar, avmol, _ptr(tape[0]),
+                       _ptr(tape[1])))
+
+    def tracer_gradient(self, nsteps, every, dt, f, uu, vv, ww, hu, hv, ho, hn, nuh, split, hscheme, vscheme, AH,
+                        cnpar, avmol, fbar, nubar):
+        """Checkpointed gradient over nsteps steps; returns (ms_forward, ms_reverse)."""
+        _same_dtype(f, uu, vv, ww, hu, hv, ho, hn, nuh, fbar, nubar)
+        fn = self.L.getm_tracer_gradient if _is64(f) else self.L.getm_tracer_gradient_f32
+        a, r = C.c_float(), C.c_float()
+        self._check(fn(self.h, nsteps, every, dt, _ptr(f), _ptr(uu), _ptr(vv), _ptr(ww), _ptr(hu), _ptr(hv),
+                       _ptr(ho), _ptr(hn), _ptr(nuh), split, hscheme, vscheme, AH, cnpar, avmol, _ptr(fbar),
+                       _ptr(nubar), C.byref(a), C.byref(r)))
+        return a.value, r.value
 
     def tracer_content(self, f, h, az) -> float:
         out = C.c_double()

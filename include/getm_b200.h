@@ -104,6 +104,8 @@ int getm_ctx_take_warnings(getm_ctx *ctx, int64_t *n_warnings);
 #define GETM_TIM_BC3D 9  /* other 3D kernels of the macro step */
 #define GETM_TIM_IP 10   /* internal pressure */
 #define GETM_TIM_MOM3D 11 /* uu/vv_momentum_3d */
+#define GETM_TIM_ADJ_RECORD 12 /* forward tracer steps that write the adjoint tape */
+#define GETM_TIM_ADJ 13        /* adjoint tracer steps */
 #define GETM_NTIMERS 16
 int getm_timers_enable(getm_ctx *ctx, int on);
 int getm_timers_reset(getm_ctx *ctx);
@@ -222,6 +224,58 @@ int getm_integrate_3d(getm_ctx *ctx, getm_bc_state *st, int n);
 /* The micro-step loop of time_loop (src/getm/integration.F90:98-172) for n = n0..n0+count-1:
  * integrate_2d every step, integrate_3d when mod(n, M) == 0. */
 int getm_time_loop(getm_ctx *ctx, getm_bc_state *st, int n0, int count);
+
+/* ---- adjoint of the tracer step ---------------------------------------------------------- */
+/* No counterpart in the reference. The tracer step of getm_tracer_step (HALFSPLIT advection,
+ * split schemes, adv_ver_iterations = 1, then implicit vertical diffusion) is differentiated in
+ * reverse mode with the limiter branch of every face frozen at the forward pass's choice (the
+ * step is then linear in the tracer, and the adjoint is its exact transpose).
+ *
+ * Tape of one step, written by getm_tracer_step_record: tape_codes = 5 planes of n3 bytes
+ * (n3 = sk*(kmax+1); the branch of every face of the sweeps u/2, v/2, w, v/2, u/2) and tape_g =
+ * the tracer after advection (one 3D field). getm_tracer_step_record advances f exactly as
+ * getm_tracer_step does.
+ * getm_tracer_step_adjoint turns fbar (cotangent of the step's output tracer) into the cotangent
+ * of its input, in place, and ADDS the cotangent of nuh to nubar (zero it before the first step).
+ * Velocities, layer heights and nuh are the step's (constant within the step). Other splits,
+ * schemes or iteration counts return GETM_ERR_UNSUPPORTED. */
+int getm_tracer_step_record(getm_ctx *ctx, double dt, double *f, const double *uu, const double *vv,
+                            const double *ww, const double *hu, const double *hv, const double *ho,
+                            const double *hn, const double *nuh, int split, int hscheme, int vscheme,
+                            double AH, double cnpar, double avmol, uint8_t *tape_codes,
+                            double *tape_g);
+int getm_tracer_step_record_f32(getm_ctx *ctx, float dt, float *f, const float *uu, const float *vv,
+                                const float *ww, const float *hu, const float *hv, const float *ho,
+                                const float *hn, const float *nuh, int split, int hscheme,
+                                int vscheme, float AH, float cnpar, float avmol,
+                                uint8_t *tape_codes, float *tape_g);
+int getm_tracer_step_adjoint(getm_ctx *ctx, double dt, double *fbar, double *nubar, const double *uu,
+                             const double *vv, const double *ww, const double *hu, const double *hv,
+                             const double *ho, const double *hn, const double *nuh, int split,
+                             int hscheme, int vscheme, double AH, double cnpar, double avmol,
+                             const uint8_t *tape_codes, const double *tape_g);
+int getm_tracer_step_adjoint_f32(getm_ctx *ctx, float dt, float *fbar, float *nubar, const float *uu,
+                                 const float *vv, const float *ww, const float *hu, const float *hv,
+                                 const float *ho, const float *hn, const float *nuh, int split,
+                                 int hscheme, int vscheme, float AH, float cnpar, float avmol,
+                                 const uint8_t *tape_codes, const float *tape_g);
+/* Gradient over nsteps steps with fixed velocities, heights and nuh, checkpointed: the forward
+ * pass keeps f every `every` steps (f leaves holding the final tracer); the reverse pass recomputes
+ * each block of steps from its checkpoint with the tape recorded and runs the adjoint steps
+ * backwards. fbar: in = dJ/d(final tracer), out = dJ/d(initial tracer); nubar += dJ/d(nuh).
+ * ms_forward / ms_reverse (may be NULL) receive the device time of the two passes. Device memory
+ * used: ceil(nsteps/every) checkpoints + `every` tapes, plus 8 3D work arrays. */
+int getm_tracer_gradient(getm_ctx *ctx, int nsteps, int every, double dt, double *f,
+                         const double *uu, const double *vv, const double *ww, const double *hu,
+                         const double *hv, const double *ho, const double *hn, const double *nuh,
+                         int split, int hscheme, int vscheme, double AH, double cnpar, double avmol,
+                         double *fbar, double *nubar, float *ms_forward, float *ms_reverse);
+int getm_tracer_gradient_f32(getm_ctx *ctx, int nsteps, int every, float dt, float *f,
+                             const float *uu, const float *vv, const float *ww, const float *hu,
+                             const float *hv, const float *ho, const float *hn, const float *nuh,
+                             int split, int hscheme, int vscheme, float AH, float cnpar,
+                             float avmol, float *fbar, float *nubar, float *ms_forward,
+                             float *ms_reverse);
 
 /* ---- diagnostics ----------------------------------------------------------------------- */
 /* Compensated (Neumaier) FP64 sum of f*h/ard1 over wet interior cells (az>=1, k=1..kmax):

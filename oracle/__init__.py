@@ -76,6 +76,9 @@ def _declare(L):
         rc = getattr(L, f"or_recon_{suf}")
         rc.argtypes = [C.c_int, P, P, P, P, P, C.c_longlong]
         rc.restype = C.c_int
+    L.or_tracer_steps_tl.argtypes = [P, P, P, P, P, C.c_int, C.c_double, P, P, P, P, P, P, P, P, P, P, P,
+                                     C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]
+    L.or_tracer_steps_tl.restype = C.c_longlong
     L.or_derive_uvx.argtypes = [P, P, P, P, P]
     L.or_build_masks.argtypes = [P, P, P, P, P, P]
     for suf in ("d", "f"):
@@ -258,4 +261,17 @@ class Oracle:
             _p(ho), _p(hn), _p(nuh), split, hscheme, vscheme, AH, cnpar, avmol, adv_ver_iterations)
         if r < 0:
             raise ValueError("tracer_steps: invalid split/scheme")
+        return r
+
+    def tracer_steps_tl(self, masks, nsteps, dt, f, df, uu, vv, ww, hu, hv, ho, hn, nuh, dnuh, split, hscheme,
+                        vscheme, AH, cnpar, avmol):
+        """Tangent-linear FP64 tracer steps (dual numbers, getm_tangent.hpp): f and df advance in
+        place; df is the derivative of the state in the direction (df, dnuh) of (initial tracer, nuh)."""
+        az, au, av, ax = masks
+        r = self.L.or_tracer_steps_tl(
+            self._pd, _p(az), _p(au), _p(av), _p(ax), nsteps, dt, _p(f), _p(df), _p(uu), _p(vv), _p(ww), _p(hu),
+            _p(hv), _p(ho), _p(hn), _p(nuh), None if dnuh is None else _p(dnuh), split, hscheme, vscheme, AH, cnpar,
+            avmol)
+        if r < 0:
+            raise ValueError("tracer_steps_tl: invalid split/scheme")
         return r

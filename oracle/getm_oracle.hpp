@@ -27,6 +27,19 @@ namespace gor {
 
 constexpr int HALO = 2;
 
+// |x| and ceil(x) found by argument-dependent lookup, so that the templates also accept the
+// dual-number type of getm_tangent.hpp; for float/double they are std::fabs / std::ceil.
+template <class R>
+inline R absval(R x) {
+  using std::fabs;
+  return fabs(x);
+}
+template <class R>
+inline int ceil_int(R x) {
+  using std::ceil;
+  return (int)ceil(x);
+}
+
 // advection.F90:55-62, advection_3d.F90:42
 enum { NOSPLIT = 0, FULLSPLIT = 1, HALFSPLIT = 2, HVSPLIT = 3 };
 enum { NOADV = 0, UPSTREAM = 1, UPSTREAM_2DH = 2, P2 = 3, SUPERBEE = 4, MUSCL = 5, P2_PDM = 6 };
@@ -240,7 +253,7 @@ long adv_split_w(const Dom& d, R dt, const R* f, R* fi, R* hi, R* adv, const R* 
       if (az[c] != 1) continue;
       if (scheme != UPSTREAM || iterate)
         for (int k = 1 - kshift; k <= kmax - 1; ++k)
-          cfl0[k] = std::fabs(ww[c + k * d.sk]) * dti /
+          cfl0[k] = absval(ww[c + k * d.sk]) * dti /
                     (R(0.5) * (hi[c + k * d.sk] + hi[c + (k + 1) * d.sk]));
       R* cfls = iterate ? cflsv.data() : cfl0.data();
       int iters = 1;
@@ -262,12 +275,12 @@ long adv_split_w(const Dom& d, R dt, const R* f, R* fi, R* hi, R* adv, const R* 
             for (int k = 0; k <= kmax; ++k) cflsv[k] = cfl0[k];
           } else if (scheme != UPSTREAM || iters < itersmax) {
             for (int k = 1 - kshift; k <= kmax - 1; ++k)
-              cflsv[k] = std::fabs(ww[c + k * d.sk]) * dti / (R(0.5) * (hiaux[k] + hiaux[k + 1]));
+              cflsv[k] = absval(ww[c + k * d.sk]) * dti / (R(0.5) * (hiaux[k] + hiaux[k + 1]));
           }
           if (iters < itersmax) {
             int iters_new = 1;
             for (int k = 1 - kshift; k <= kmax - 1; ++k)
-              iters_new = std::max(iters_new, (int)std::ceil(cflsv[k]));
+              iters_new = std::max(iters_new, ceil_int(cflsv[k]));
             if (iters_new > iters) {
               if (iters_new > itersmax) {
                 ++too_many;

@@ -3,6 +3,7 @@
 // Suffix _d = FP64 (the reference's REALTYPE), _f = FP32.
 #include "getm_oracle.hpp"
 #include "getm_baroclinic.hpp"
+#include "getm_tangent.hpp"
 
 extern "C" {
 
@@ -114,6 +115,47 @@ void or_build_masks(const or_dom* o, const int32_t* az, const int32_t* au, const
 
 OR_DEFINE(d, double)
 OR_DEFINE(f, float)
+
+// Tangent-linear tracer steps (getm_tangent.hpp): nsteps of the FP64 tracer step carrying the
+// derivative in the direction (df, dnuh); f and df are advanced in place.
+long long or_tracer_steps_tl(const or_dom* o, const int32_t* az, const int32_t* au, const int32_t* av,
+                             const int32_t* ax, int nsteps, double dt, double* f, double* df, const double* uu,
+                             const double* vv, const double* ww, const double* hu, const double* hv,
+                             const double* ho, const double* hn, const double* nuh, const double* dnuh, int split,
+                             int hscheme, int vscheme, double AH, double cnpar, double avmol) {
+  using gor::Dual;
+  gor::Dom d = mk(o);
+  gor::AdvMasks m;
+  gor::build_adv_masks(d, az, au, av, ax, m);
+  gor::AdvGrid g = gor::adv_grid(m, gor::H_TAG, az, au, av);
+  const long n3 = d.n3d();
+  auto cst = [&](const double* a) {
+    std::vector<Dual> v(n3);
+    for (long q = 0; q < n3; ++q) v[q] = Dual(a[q]);
+    return v;
+  };
+  std::vector<Dual> F(n3), NU(n3);
+  for (long q = 0; q < n3; ++q) {
+    F[q] = Dual(f[q], df[q]);
+    NU[q] = Dual(nuh[q], dnuh ? dnuh[q] : 0.0);
+  }
+  std::vector<Dual> UU = cst(uu), VV = cst(vv), WW = cst(ww), HU = cst(hu), HV = cst(hv), HO = cst(ho),
+                    HN = cst(hn);
+  long long warn = 0;
+  for (int s = 0; s < nsteps; ++s) {
+    long r = gor::do_advection_3d<Dual>(d, g, Dual(dt), F.data(), UU.data(), VV.data(), WW.data(), HU.data(),
+                                        HV.data(), HO.data(), HN.data(), split, hscheme, vscheme, Dual(AH), gor::H_TAG,
+                                        nullptr, nullptr, 1);
+    if (r < 0) return -1;
+    warn += r;
+    gor::tracer_vdiff<Dual>(d, Dual(dt), Dual(cnpar), Dual(avmol), F.data(), HN.data(), NU.data(), az, nullptr);
+  }
+  for (long q = 0; q < n3; ++q) {
+    f[q] = F[q].v;
+    df[q] = F[q].d;
+  }
+  return warn;
+}
 
 // ---- mode-split time loop (getm_baroclinic.hpp) -------------------------------------------------
 typedef struct {

@@ -1,0 +1,279 @@
+"""Adjoint of the tracer step on the GPU, through the C ABI.
+
+Checks (FP64 unless stated):
+  * the recording forward step advances the tracer exactly like getm_tracer_step;
+  * one adjoint step against the oracle's tangent-linear step (dual numbers):
+    <fbar0, df> + <nubar, dnuh> = <w, tangent(df, dnuh)> for every split scheme, to 1e-10;
+  * the checkpointed multi-step gradient against the tangent-linear oracle (1e-9) and against the
+    step-by-step adjoint (bit for bit);
+  * the gradient against central finite differences of the GPU forward run (1e-4): dJ/df0 and
+    dJ/dnuh with the linear P2 scheme, and dJ/df0 on 64 directions in the tracer-adjoint
+    configuration (256 x 256 x 30, SUPERBEE, 50 steps);
+  * the FP32 gradient against the FP64 tangent (1e-4 with P2; 1e-3 with SUPERBEE, see the test).
+"""
+import numpy as np
+import pytest
+
+import oracle
+from code_b200 import cases
+from helpers import dev, host, make_ctx
+
+pytestmark = pytest.mark.gpu
+
+NAMES = ("uu", "vv", "ww", "hun", "hvn", "ho", "hn")
+SCHEMES = {"UPSTREAM": 1, "P2": 3, "SUPERBEE": 4, "MUSCL": 5, "P2_PDM": 6}
+
+
+def _dev_fields(c, dtype=None):
+    import torch
+
+    t = {n: dev(c[n]) for n in NAMES + ("nuh",)}
+    if dtype is not None:
+        t = {n: v.to(dtype) for n, v in t.items()}
+    return t
+
+
+def _steps(ctx, c, t, f, nsteps, hs, vs):
+    p = c.par
+    for _ in range(nsteps):
+        ctx.tracer_step(p["dt"], f, *[t[n] for n in NAMES], t["nuh"], 2, hs, vs, p["AH"], p["cnpar"], p["avmol"])
+
+
+def test_record_step_equals_plain_step():
+    import torch
+
+    c = cases.random_case(nx=37, ny=29, kmax=9, seed=3)
+    c.par.update(AH=0.0, cnpar=0.9, avmol=1e-6)
+    ctx, m = make_ctx(c)
+    for dtype in (torch.float64, torch.float32):
+        t = _dev_fields(c, dtype)
+        f1 = dev(c["f"]).to(dtype)
+        f2 = f1.clone()
+        tape = ctx.tape(dtype)
+        _steps(ctx, c, t, f1, 1, 6, 6)
+        ctx.tracer_step_record(c.par["dt"], f2, *[t[n] for n in NAMES], t["nuh"], 2, 6, 6, 0.0, 0.9, 1e-6, tape)
+        torch.cuda.synchronize()
+        if dtype == torch.float64:
+            assert torch.equal(f1, f2)
+        else:
+            assert torch.allclose(f1, f2, rtol=1e-6, atol=1e-6)
+
+
+@pytest.mark.parametrize("scheme", list(SCHEMES))
+@pytest.mark.parametrize("AH", [0.0, 5.0])
+def test_adjoint_step_vs_tangent(scheme, AH):
+    import torch
+
+    hs = SCHEMES[scheme]
+    c = cases.random_case(nx=33, ny=27, kmax=8, seed=11)
+    p = c.par
+    p.update(AH=AH, cnpar=0.9, avmol=1e-6, split=2, hscheme=hs, vscheme=hs)
+    o = oracle.Oracle(c.grid)
+    ctx, m = make_ctx(c)
+    t = _dev_fields(c)
+    rng = np.random.default_rng(7)
+    w = rng.normal(size=c["f"].shape)
+    df = rng.normal(size=c["f"].shape)
+    dnuh = rng.normal(size=c["f"].shape) * 1e-3
+    # tangent on the CPU
+    fo, dfo = c["f"].copy(), df.copy()
+    o.tracer_steps_tl(c.masks(), 1, p["dt"], fo, dfo, *[c[n] for n in NAMES], c["nuh"], dnuh, 2, hs, hs, AH,
+                      p["cnpar"], p["avmol"])
+    tl = float(np.sum(w * dfo))
+    # adjoint on the GPU
+    f = dev(c["f"])
+    tape = ctx.tape(torch.float64)
+    ctx.tracer_step_record(p["dt"], f, *[t[n] for n in NAMES], t["nuh"], 2, hs, hs, AH, p["cnpar"], p["avmol"],
+                           tape)
+    assert np.array_equal(host(f), fo)  # the tangent's values are the plain FP64 step
+    fbar = dev(w)
+    nubar = torch.zeros_like(fbar)
+    ctx.tracer_step_adjoint(p["dt"], fbar, nubar, *[t[n] for n in NAMES], t["nuh"], 2, hs, hs, AH, p["cnpar"],
+                            p["avmol"], tape)
+    ad = float(np.sum(host(fbar) * df) + np.sum(host(nubar) * dnuh))
+    assert abs(ad - tl) <= 1e-10 * (abs(tl) + 1e-300), (ad, tl)
+
+
+def _flow(nx=48, ny=40, kmax=8):
+    c = cases.streamfunction_flow(nx=nx, ny=ny, kmax=kmax, dt=300.0, seed=4)
+    c.par.update(cnpar=0.9, avmol=1e-6)
+    return c
+
+
+def _gradient(ctx, c, t, nsteps, every, w, dtype=None):
+    import torch
+
+    p = c.par
+    f = dev(c["f"]) if dtype is None else dev(c["f"]).to(dtype)
+    fbar = dev(w) if dtype is None else dev(w).to(dtype)
+    nubar = torch.zeros_like(fbar)
+    ms = ctx.tracer_gradient(nsteps, every, p["dt"], f, *[t[n] for n in NAMES], t["nuh"], 2, p["hscheme"],
+                             p["vscheme"], p["AH"], p["cnpar"], p["avmol"], fbar, nubar)
+    return f, fbar, nubar, ms
+
+
+def test_gradient_vs_tangent_and_stepwise():
+    import torch
+
+    c = _flow()
+    p = c.par
+    o = oracle.Oracle(c.grid)
+    ctx, m = make_ctx(c)
+    t = _dev_fields(c)
+    w = cases.box_weights(c, box=16)
+    nsteps, every = 12, 5
+    f, fbar, nubar, _ = _gradient(ctx, c, t, nsteps, every, w)
+    # final state = plain forward
+    fp = dev(c["f"])
+    _steps(ctx, c, t, fp, nsteps, p["hscheme"], p["vscheme"])
+    assert torch.equal(f, fp)
+    # step-by-step adjoint with every tape kept
+    fs = dev(c["f"])
+    tapes = []
+    for _ in range(nsteps):
+        tp = ctx.tape(torch.float64)
+        ctx.tracer_step_record(p["dt"], fs, *[t[n] for n in NAMES], t["nuh"], 2, p["hscheme"], p["vscheme"],
+                               p["AH"], p["cnpar"], p["avmol"], tp)
+        tapes.append(tp)
+    gb = dev(w)
+    nb = torch.zeros_like(gb)
+    for tp in reversed(tapes):
+        ctx.tracer_step_adjoint(p["dt"], gb, nb, *[t[n] for n in NAMES], t["nuh"], 2, p["hscheme"], p["vscheme"],
+                                p["AH"], p["cnpar"], p["avmol"], tp)
+    assert torch.equal(gb, fbar) and torch.equal(nb, nubar)
+    # tangent-linear oracle on four directions
+    rng = np.random.default_rng(5)
+    G, NB = host(fbar), host(nubar)
+    for q in range(4):
+        df = rng.normal(size=c["f"].shape) * (c["az"] >= 1)[None]
+        dnuh = rng.normal(size=c["f"].shape) * 1e-5 if q % 2 else None
+        fo, dfo = c["f"].copy(), df.copy()
+        o.tracer_steps_tl(c.masks(), nsteps, p["dt"], fo, dfo, *[c[n] for n in NAMES], c["nuh"], dnuh, 2,
+                          p["hscheme"], p["vscheme"], p["AH"], p["cnpar"], p["avmol"])
+        tl = float(np.sum(w * dfo))
+        ad = float(np.sum(G * df) + (np.sum(NB * dnuh) if dnuh is not None else 0.0))
+        assert abs(ad - tl) <= 1e-9 * abs(tl), (q, ad, tl)
+
+
+def _fd_check(c, nsteps, every, box, dirs, eps_f, eps_nu, tol):
+    """Directional derivatives of the checkpointed gradient against central differences of the GPU
+    forward run; dirs = sequence of "f" / "nuh". The difference J(+) - J(-) is taken as
+    sum(w * (f+ - f-)) so that the two large sums do not cancel. The +/- runs record their limiter
+    branches: a direction whose secant crosses a limiter kink (a branch differs from the base
+    run's) measures a different piecewise-linear map and is reported, not compared. Returns
+    (worst relative error over the compared directions, number of directions with a kink)."""
+    import torch
+
+    p = c.par
+    ctx, m = make_ctx(c)
+    t = _dev_fields(c)
+    w = cases.box_weights(c, box=box)
+    wt = dev(w)
+    _, fbar, nubar, _ = _gradient(ctx, c, t, nsteps, every, w)
+    rng = np.random.default_rng(5)
+    wet = torch.from_numpy((c["az"] >= 1)[None].astype(np.float64)).cuda()
+    tape = ctx.tape(torch.float64)
+
+    def run(f0, nuh, base=None):
+        """nsteps recorded steps; returns (f, codes of every step, or the count of codes that
+        differ from `base`)."""
+        f = f0.clone()
+        codes, flips = [], 0
+        for q in range(nsteps):
+            ctx.tracer_step_record(p["dt"], f, *[t[n] for n in NAMES], nuh, 2, p["hscheme"], p["vscheme"],
+                                   p["AH"], p["cnpar"], p["avmol"], tape)
+            if base is None:
+                codes.append(tape[0].clone())
+            else:
+                flips += int((tape[0] != base[q]).sum())
+        return f, (codes if base is None else flips)
+
+    f0 = dev(c["f"])
+    _, base = run(f0, t["nuh"])
+    worst, kinked = 0.0, 0
+    for q, which in enumerate(dirs):
+        d = torch.from_numpy(rng.normal(size=c["f"].shape)).cuda() * wet
+        if which == "f":
+            (fp, np_), (fm, nm) = run(f0 + eps_f * d, t["nuh"], base), run(f0 - eps_f * d, t["nuh"], base)
+            eps, ad = eps_f, float(torch.sum(fbar * d))
+        else:
+            d = d * t["nuh"]  # relative perturbation of the diffusivity
+            (fp, np_), (fm, nm) = run(f0, t["nuh"] + eps_nu * d, base), run(f0, t["nuh"] - eps_nu * d, base)
+            eps, ad = eps_nu, float(torch.sum(nubar * d))
+        fd = float(torch.sum(wt * (fp - fm))) / (2 * eps)
+        err = abs(ad - fd) / abs(fd)
+        if np_ or nm:
+            kinked += 1
+            continue
+        worst = max(worst, err)
+        assert err <= tol, (q, which, ad, fd)
+    return worst, kinked
+
+
+def test_gradient_vs_finite_differences_p2():
+    """P2 (the unlimited, linear scheme), vertically sheared flow, stratified tracer: both dJ/df0
+    and dJ/dnuh agree with central differences to 1e-4 (about 1e-7 obtained)."""
+    c = cases.streamfunction_flow(nx=64, ny=64, kmax=10, dt=300.0, seed=4, vertical=0.5, shear=1.0)
+    c.par.update(cnpar=0.9, avmol=1e-6, hscheme=3, vscheme=3)
+    worst, kinked = _fd_check(c, 20, 10, 32, ["f", "nuh"] * 4, eps_f=1e-6, eps_nu=1e-3, tol=1e-4)
+    assert kinked == 0 and worst <= 1e-4
+
+
+def test_gradient_tracer_adjoint_configuration_fd():
+    """The tracer-adjoint configuration: 256 x 256 x 30, flat 30 m, dx = 500 m, random
+    divergence-free flow (8 modes, max 0.5 m/s), SUPERBEE + implicit diffusion (nuh = 1e-4),
+    50 steps checkpointed every 10, J = tracer content of the central 32 x 32 box. dJ/df0 against
+    central differences on 64 seeded random directions, 1e-4 on every direction whose secant
+    stays on one branch of every limiter (at most 8 of 64 may cross a kink). (Directions in nuh
+    are checked against the tangent-linear model instead: a perturbation of nuh moves the limiter
+    ratio of every face, and the secant then crosses SUPERBEE's kinks.)"""
+    c = cases.streamfunction_flow(nx=256, ny=256, kmax=30, dt=300.0, seed=4)
+    c.par.update(cnpar=1.0, avmol=0.0)
+    worst, kinked = _fd_check(c, 50, 10, 32, ["f"] * 64, eps_f=1e-9, eps_nu=None, tol=1e-4)
+    print(f"64 directions: {64 - kinked} compared, worst relative error {worst:.2e}; {kinked} crossed a kink")
+    assert kinked <= 8
+
+
+@pytest.mark.parametrize("scheme,tol", [(3, 1e-4), (4, 1e-3)])
+def test_gradient_fp32_vs_fp64_tangent(scheme, tol):
+    """FP32 checkpointed gradient against the FP64 tangent-linear oracle. With the linear P2 scheme
+    only FP32 rounding separates them (1e-4). With SUPERBEE the FP32 trajectory takes the other
+    limiter branch at faces whose limiter ratio sits at a kink within FP32 rounding, so the FP32
+    gradient is that of a slightly different piecewise-linear map (1e-3)."""
+    import torch
+
+    c = cases.streamfunction_flow(nx=48, ny=40, kmax=8, dt=300.0, seed=4, vertical=0.5, shear=1.0)
+    c.par.update(cnpar=0.9, avmol=1e-6, hscheme=scheme, vscheme=scheme)
+    p = c.par
+    o = oracle.Oracle(c.grid)
+    ctx, m = make_ctx(c)
+    t32 = _dev_fields(c, torch.float32)
+    w = cases.box_weights(c, box=16)
+    nsteps, every = 12, 5
+    _, fbar, nubar, _ = _gradient(ctx, c, t32, nsteps, every, w, dtype=torch.float32)
+    G, NB = host(fbar).astype(np.float64), host(nubar).astype(np.float64)
+    rng = np.random.default_rng(6)
+    for q in range(4):
+        df = rng.normal(size=c["f"].shape) * (c["az"] >= 1)[None]
+        dnuh = (rng.normal(size=c["f"].shape) * c["nuh"]) if q % 2 else None
+        if dnuh is not None:
+            df = np.zeros_like(df)
+        fo, dfo = c["f"].copy(), df.copy()
+        o.tracer_steps_tl(c.masks(), nsteps, p["dt"], fo, dfo, *[c[n] for n in NAMES], c["nuh"], dnuh, 2,
+                          p["hscheme"], p["vscheme"], p["AH"], p["cnpar"], p["avmol"])
+        tl = float(np.sum(w * dfo))
+        ad = float(np.sum(G * df) + (np.sum(NB * dnuh) if dnuh is not None else 0.0))
+        assert abs(ad - tl) <= tol * abs(tl), (q, ad, tl)
+
+
+def test_adjoint_rejects_other_splits():
+    from code_b200.getm import GetmError
+    import torch
+
+    c = cases.random_case(nx=20, ny=16, kmax=5, seed=1)
+    ctx, m = make_ctx(c)
+    t = _dev_fields(c)
+    f = dev(c["f"])
+    with pytest.raises(GetmError):
+        ctx.tracer_step_record(30.0, f, *[t[n] for n in NAMES], t["nuh"], 1, 4, 4, 0.0, 0.9, 0.0,
+                               ctx.tape(torch.float64))
