@@ -53,6 +53,10 @@ def parse():
     ap.add_argument("--variants", default="fp64,mixed")
     ap.add_argument("--adj-steps", type=int, default=20, help="tracer steps of the adjoint measurement (0 = skip)")
     ap.add_argument("--adj-every", type=int, default=10, help="checkpoint interval of the adjoint")
+    ap.add_argument("--tracer-adjoint", action="store_true",
+                    help="time only the checkpointed tracer gradient on the tracer-adjoint configuration "
+                         "(random divergence-free flow, SUPERBEE, implicit diffusion; --nx/--ny/--kmax, "
+                         "--adj-steps, --adj-every) in FP64 and FP32 and print one JSON line")
     return ap.parse_args()
 
 
@@ -183,11 +187,52 @@ def cpu_baseline_sample(args):
                       f"({el:.1f} s)"}
 
 
+def run_tracer_adjoint(args):
+    """The tracer-adjoint configuration (256 x 256 x 30, flat 30 m, dx = 500 m, 8-mode random
+    streamfunction flow with max 0.5 m/s, SUPERBEE HALFSPLIT, nuh = 1e-4, J = tracer content of the
+    central 32 x 32 box): device time of the forward pass (with checkpoints) and of the reverse pass
+    of getm_tracer_gradient, FP64 and FP32."""
+    import numpy as np
+    import torch
+
+    from code_b200 import cases
+    from code_b200.getm import Context
+
+    c = cases.streamfunction_flow(nx=args.nx, ny=args.ny, kmax=args.kmax, dt=300.0, seed=4)
+    c.par.update(cnpar=1.0, avmol=0.0)
+    p = c.par
+    w = cases.box_weights(c, box=min(32, args.nx, args.ny))
+    ctx = Context(c.grid)
+    ctx.init_advection(*[torch.from_numpy(m).cuda() for m in c.masks()])
+    names = ("uu", "vv", "ww", "hun", "hvn", "ho", "hn", "nuh")
+    out = {"workload": f"tracer adjoint: {args.nx}x{args.ny}x{args.kmax}, {args.adj_steps} steps, checkpoint every "
+                       f"{args.adj_every}, SUPERBEE HALFSPLIT + implicit diffusion", "results": {}}
+    for name, dt in (("f64", torch.float64), ("f32", torch.float32)):
+        t = [torch.from_numpy(c[n]).cuda().to(dt) for n in names]
+        runs = []
+        for rep in range(max(2, args.warmup)):
+            f = torch.from_numpy(c["f"]).cuda().to(dt)
+            fbar = torch.from_numpy(w).cuda().to(dt)
+            nubar = torch.zeros_like(fbar)
+            torch.cuda.synchronize()
+            runs.append(ctx.tracer_gradient(args.adj_steps, args.adj_every, p["dt"], f, *t, p["split"], p["hscheme"],
+                                            p["vscheme"], p["AH"], p["cnpar"], p["avmol"], fbar, nubar))
+        ms_f, ms_r = runs[-1]
+        out["results"][name] = {"ms_forward": ms_f, "ms_reverse": ms_r, "adjoint_fwd_ratio": ms_r / ms_f,
+                                "grad_norm": float(fbar.double().norm())}
+    ctx.close()
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank)
+        return
+    if args.tracer_adjoint:
+        if rank == 0:
+            run_tracer_adjoint(args)
         return
     import torch
     import torch.distributed as dist

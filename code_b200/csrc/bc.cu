@@ -593,7 +593,26 @@ int integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
   }
   if (ip[I_RUNTYPE] == 4) {
     const R3 dt = R3(st->par[P_DT]);
-    if (ip[I_CALC_TEMP]) {
+    // do_temperature and do_salinity advect with the same velocities and heights; with the same
+    // schemes the two advections run as one paired sweep sequence (each field's arithmetic is
+    // unchanged), followed by the two diffusion solves.
+    const bool pair = ip[I_CALC_TEMP] && ip[I_CALC_SALT] && ip[I_TEMP_SPLIT] == GETM_HALFSPLIT &&
+                      ip[I_SALT_SPLIT] == GETM_HALFSPLIT && ip[I_TEMP_HOR] == ip[I_SALT_HOR] &&
+                      ip[I_TEMP_VER] == ip[I_SALT_VER] && is_split_scheme(ip[I_TEMP_HOR]) &&
+                      (ip[I_TEMP_VER] == NOADV || is_split_scheme(ip[I_TEMP_VER])) &&
+                      st->par[P_TEMP_AH] == st->par[P_SALT_AH] && ip[I_ADV_VER_ITERS] <= 1 && ctx->adv_ready;
+    if (pair) {
+      if ((rc = do_adv3d_pair<R3>(ctx, dt, f3[TT], f3[SS], f3[UU], f3[VV], f3[WW], f3[HUN], f3[HVN], f3[HO],
+                                  ip[I_TEMP_HOR], ip[I_TEMP_VER], R3(st->par[P_TEMP_AH]))))
+        return rc;
+      GB_TIMED(GETM_TIM_VDIFF, run_vdiff<R3>(d, s, dt, R3(st->par[P_CNPAR]), R3(st->par[P_AVMOLT]), f3[TT], f3[HN],
+                                             f3[NUH], st->az, (const R3*)nullptr, (R3*)ctx->scr[0], (R3*)ctx->scr[1]),
+               "vdiff T");
+      GB_TIMED(GETM_TIM_VDIFF, run_vdiff<R3>(d, s, dt, R3(st->par[P_CNPAR]), R3(st->par[P_AVMOLS]), f3[SS], f3[HN],
+                                             f3[NUH], st->az, (const R3*)nullptr, (R3*)ctx->scr[0], (R3*)ctx->scr[1]),
+               "vdiff S");
+    }
+    if (!pair && ip[I_CALC_TEMP]) {
       if ((rc = do_adv3d<R3>(ctx, dt, f3[TT], f3[UU], f3[VV], f3[WW], f3[HUN], f3[HVN], f3[HO], f3[HN],
                              ip[I_TEMP_SPLIT], ip[I_TEMP_HOR], ip[I_TEMP_VER], R3(st->par[P_TEMP_AH]), GETM_H_TAG,
                              nullptr, nullptr, ip[I_ADV_VER_ITERS])))
@@ -602,7 +621,7 @@ int integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
                                              f3[NUH], st->az, (const R3*)nullptr, (R3*)ctx->scr[0], (R3*)ctx->scr[1]),
                "vdiff T");
     }
-    if (ip[I_CALC_SALT]) {
+    if (!pair && ip[I_CALC_SALT]) {
       if ((rc = do_adv3d<R3>(ctx, dt, f3[SS], f3[UU], f3[VV], f3[WW], f3[HUN], f3[HVN], f3[HO], f3[HN],
                              ip[I_SALT_SPLIT], ip[I_SALT_HOR], ip[I_SALT_VER], R3(st->par[P_SALT_AH]), GETM_H_TAG,
                              nullptr, nullptr, ip[I_ADV_VER_ITERS])))

@@ -171,6 +171,47 @@ int do_adv3d(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, c
   return GETM_OK;
 }
 
+// Two tracers (temperature and salinity) advected together with HALFSPLIT on the H grid: the
+// same sweeps as do_adv3d's HALFSPLIT branch for each field, with the heights hi evolved once.
+template <class R>
+int do_adv3d_pair(getm_ctx* ctx, R dt, R* fa, R* fb, const R* uu, const R* vv, const R* ww, const R* hu,
+                  const R* hv, const R* ho, int hs, int vs, R AH) {
+  getm_adv_grid g;
+  grid_for_tag(ctx, GETM_H_TAG, &g);
+  const Dev& d = ctx->dev;
+  cudaStream_t s = ctx->stream;
+  const int kmax = d.kmax;
+  const long long sk = d.sk;
+  int rc = ensure_scratch(ctx, (size_t)n3d(d) * sizeof(R));
+  if (rc) return rc;
+  R* Sa = (R*)ctx->scr[0];
+  R* H = (R*)ctx->scr[1];
+  R* Sb = (R*)ctx->scr[2];
+  auto L = [&](auto* p, int k) { return p + (long long)k * sk; };
+  const R half = R(0.5), one = R(1);
+  GB_TRY(cudaMemcpyAsync(H, ho, (size_t)sk * sizeof(R), cudaMemcpyDeviceToDevice, s), "copy ho(0)");
+  const int nk = kmax;
+  GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<R, 0>(d, s, nk, dt, half, hs, AH, L(fa, 1), L(fa, 1), L(Sa, 1), L(ho, 1),
+                            L(H, 1), nullptr, L(uu, 1), L(hu, 1), g.mask_uflux, g.mask_uupdate, nullptr, L(fb, 1),
+                            L(fb, 1), L(Sb, 1))), "u1");
+  GB_TIMED(GETM_TIM_ADV_V, (run_sweep_h<R, 1>(d, s, nk, dt, half, hs, AH, L(Sa, 1), L(Sa, 1), L(fa, 1), L(H, 1),
+                            L(H, 1), nullptr, L(vv, 1), L(hv, 1), g.mask_vflux, g.mask_vupdate, nullptr, L(Sb, 1),
+                            L(Sb, 1), L(fb, 1))), "v1");
+  if (kmax > 1 && vs != NOADV)
+    GB_TIMED(GETM_TIM_ADV_W, run_sweep_w2<R>(d, s, dt, one, vs, fa, fb, H, ww, g.az), "w");
+  GB_TIMED(GETM_TIM_ADV_V, (run_sweep_h<R, 1>(d, s, nk, dt, half, hs, AH, L(fa, 1), L(fa, 1), L(Sa, 1), L(H, 1),
+                            L(H, 1), nullptr, L(vv, 1), L(hv, 1), g.mask_vflux, g.mask_vupdate, nullptr, L(fb, 1),
+                            L(fb, 1), L(Sb, 1))), "v2");
+  GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<R, 0>(d, s, nk, dt, half, hs, AH, L(Sa, 1), L(Sa, 1), L(fa, 1), L(H, 1),
+                            L(H, 1), nullptr, L(uu, 1), L(hu, 1), g.mask_uflux, g.mask_uupdate, nullptr, L(Sb, 1),
+                            L(Sb, 1), L(fb, 1))), "u2");
+  return GETM_OK;
+}
+template int do_adv3d_pair<double>(getm_ctx*, double, double*, double*, const double*, const double*, const double*,
+                                   const double*, const double*, const double*, int, int, double);
+template int do_adv3d_pair<float>(getm_ctx*, float, float*, float*, const float*, const float*, const float*,
+                                  const float*, const float*, const float*, int, int, float);
+
 template int do_adv3d<double>(getm_ctx*, double, double*, const double*, const double*, const double*,
                                const double*, const double*, const double*, const double*, int, int, int, double,
                                int, double*, double*, int);

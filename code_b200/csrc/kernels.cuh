@@ -219,18 +219,33 @@ inline SweepC<R> sweep_consts(const Dev& d, int dir, R dt, R splitfac, R AH) {
   return c;
 }
 
+// The tracer fields of one sweep: the stencil source f, the field fi updated from fi_src into
+// fi_dst (fi_src may be f or alias fi_dst). A sweep advects NF fields with the same transports,
+// heights and masks -- temperature and salinity share them, so they are swept together: the
+// layer heights, Courant numbers and masks are read and computed once for both.
+template <class R>
+struct TracerIO {
+  const R* f;
+  const R* fi_src;
+  R* fi_dst;
+};
+template <class R, int NF>
+struct TracerSet {
+  TracerIO<R> t[NF];
+};
+
 // u sweep (adv_split_u.F90:222-285) over one row segment of TU cells, for up to NKB levels.
-template <class R, int S, bool REC>
-__global__ void __launch_bounds__(TU) k_sweep_u_tile(Dev d, SweepC<R> C, int nk, const R* __restrict__ f,
-                                                     const R* fi_src, R* fi_dst, const R* Di_src, R* Di_dst, R* adv,
+template <class R, int S, bool REC, int NF>
+__global__ void __launch_bounds__(TU) k_sweep_u_tile(Dev d, SweepC<R> C, int nk, TracerSet<R, NF> F,
+                                                     const R* Di_src, R* Di_dst, R* adv,
                                                      const R* __restrict__ U, const R* __restrict__ DU,
                                                      const uint8_t* __restrict__ mflux,
                                                      const uint8_t* __restrict__ mupd, uint8_t* code) {
-  __shared__ R sf[TU + 4];      // f(i0-2 .. i0+TU+1)
-  __shared__ R sU[TU + 1];      // U(i0-1 .. i0+TU-1)
+  __shared__ R sf[NF][TU + 4];   // f(i0-2 .. i0+TU+1)
+  __shared__ R sU[TU + 1];       // U(i0-1 .. i0+TU-1)
   __shared__ R sDU[TU + 1];
   __shared__ uint8_t sm[TU + 4];  // mflux(i0-2 .. i0+TU+1)
-  __shared__ R sfl[TU + 1];     // flux of faces i0-1 .. i0+TU-1
+  __shared__ R sfl[NF][TU + 1];  // flux of faces i0-1 .. i0+TU-1
   const int t = threadIdx.x;
   const int ni = d.ni();
   const int ii0 = blockIdx.x * TU;
@@ -247,13 +262,15 @@ __global__ void __launch_bounds__(TU) k_sweep_u_tile(Dev d, SweepC<R> C, int nk,
   const int ii = ii0 + t;
   const bool own = ii < ni;
   const bool upd = own && (ii >= 1 + sub) && (ii <= ni - 2 - sub) && mupd[crow + ii];
-  const bool fi_is_f = (fi_src == f);
   for (int k = k0; k < k1; ++k) {
     const long long row = crow + (long long)k * d.sk;
-    const R* fr = f + row;
-    for (int q = t; q < TU + 4; q += TU) {
-      const int i2 = ii0 - 2 + q;
-      sf[q] = (i2 >= 0 && i2 < ni) ? fr[i2] : R(0);
+#pragma unroll
+    for (int n = 0; n < NF; ++n) {
+      const R* fr = F.t[n].f + row;
+      for (int q = t; q < TU + 4; q += TU) {
+        const int i2 = ii0 - 2 + q;
+        sf[n][q] = (i2 >= 0 && i2 < ni) ? fr[i2] : R(0);
+      }
     }
     for (int q = t; q < TU + 1; q += TU) {
       const int i2 = ii0 - 1 + q;
@@ -263,32 +280,45 @@ __global__ void __launch_bounds__(TU) k_sweep_u_tile(Dev d, SweepC<R> C, int nk,
     }
     // own-cell inputs, in flight during the face phase
     const R Dio = own ? Di_src[row + ii] : R(0);
-    const R fio_g = (own && !fi_is_f) ? fi_src[row + ii] : R(0);
+    R fio_g[NF];
+#pragma unroll
+    for (int n = 0; n < NF; ++n)
+      fio_g[n] = (own && F.t[n].fi_src != F.t[n].f) ? F.t[n].fi_src[row + ii] : R(0);
     __syncthreads();
     for (int q = t; q < TU + 1; q += TU) {
       const int fa = ii0 - 1 + q;
-      R fl = R(0);
-      uint8_t cd = 0;
-      if (fa >= sub && fa <= ni - 2 - sub)
-        fl = face_flux_s<R, S, REC>(sU[q], sDU[q], sf[q], sf[q + 1], sf[q + 2], sf[q + 3], sm[q] != 0,
-                                    sm[q + 1] != 0, sm[q + 2] != 0, C.dti, C.cdx, C.AH, use_AH, C.dxf, &cd);
-      sfl[q] = fl;
-      if (REC && q >= 1 && fa < ni) code[row + fa] = cd;  // face fa is stored at its left cell
+      const bool valid = fa >= sub && fa <= ni - 2 - sub;
+#pragma unroll
+      for (int n = 0; n < NF; ++n) {
+        R fl = R(0);
+        uint8_t cd = 0;
+        if (valid)
+          fl = face_flux_s<R, S, REC>(sU[q], sDU[q], sf[n][q], sf[n][q + 1], sf[n][q + 2], sf[n][q + 3],
+                                      sm[q] != 0, sm[q + 1] != 0, sm[q + 2] != 0, C.dti, C.cdx, C.AH, use_AH,
+                                      C.dxf, &cd);
+        sfl[n][q] = fl;
+        if (REC && n == 0 && q >= 1 && fa < ni) code[row + fa] = cd;  // face fa is stored at its left cell
+      }
     }
     __syncthreads();
     if (own) {
       const long long p = row + ii;
-      const R fio = fi_is_f ? sf[t + 2] : fio_g;
       if (upd) {
-        const R fe = sfl[t + 1], fw = sfl[t];
         const R dD = C.dti * (sU[t + 1] * C.dyf - sU[t] * C.dyf) * C.ard1;
         const R Dn = Dio - dD;
-        const R advn = C.splitfac * (fe * C.dyf - fw * C.dyf) * C.ard1;
         Di_dst[p] = Dn;
-        fi_dst[p] = fv_update<R>(Dio, dD, Dn, fio, C.dt, advn);
-        if (adv) adv[p] = adv[p] + advn;
+#pragma unroll
+        for (int n = 0; n < NF; ++n) {
+          const R fio = F.t[n].fi_src == F.t[n].f ? sf[n][t + 2] : fio_g[n];
+          const R advn = C.splitfac * (sfl[n][t + 1] * C.dyf - sfl[n][t] * C.dyf) * C.ard1;
+          F.t[n].fi_dst[p] = fv_update<R>(Dio, dD, Dn, fio, C.dt, advn);
+          if (NF == 1 && adv) adv[p] = adv[p] + advn;
+        }
       } else {
-        if (fi_dst != fi_src) fi_dst[p] = fio;
+#pragma unroll
+        for (int n = 0; n < NF; ++n)
+          if (F.t[n].fi_dst != F.t[n].fi_src)
+            F.t[n].fi_dst[p] = F.t[n].fi_src == F.t[n].f ? sf[n][t + 2] : fio_g[n];
         if (Di_dst != Di_src) Di_dst[p] = Dio;
       }
     }
@@ -297,18 +327,16 @@ __global__ void __launch_bounds__(TU) k_sweep_u_tile(Dev d, SweepC<R> C, int nk,
 }
 
 // v sweep (adv_split_v.F90:79-135) over a tile of TVX x TVY cells, for up to NKB levels.
-template <class R, int S, bool REC>
-__global__ void __launch_bounds__(TVX * TVY) k_sweep_v_tile(Dev d, SweepC<R> C, int nk, const R* __restrict__ f,
-                                                            const R* fi_src, R* fi_dst, const R* Di_src, R* Di_dst,
-                                                            R* adv, const R* __restrict__ V,
-                                                            const R* __restrict__ DV,
-                                                            const uint8_t* __restrict__ mflux,
-                                                            const uint8_t* __restrict__ mupd, uint8_t* code) {
-  __shared__ R sf[TVY + 4][TVX];       // f(j0-2 .. j0+TVY+1)
-  __shared__ R sV[TVY + 1][TVX];       // V(j0-1 .. j0+TVY-1)
+template <class R, int S, bool REC, int NF>
+__global__ void __launch_bounds__(TVX * TVY, sizeof(R) == 4 && NF == 1 ? 2048 / (TVX * TVY) : 1)
+    k_sweep_v_tile(Dev d, SweepC<R> C, int nk, TracerSet<R, NF> F, const R* Di_src, R* Di_dst, R* adv,
+                   const R* __restrict__ V, const R* __restrict__ DV, const uint8_t* __restrict__ mflux,
+                   const uint8_t* __restrict__ mupd, uint8_t* code) {
+  __shared__ R sf[NF][TVY + 4][TVX];    // f(j0-2 .. j0+TVY+1)
+  __shared__ R sV[TVY + 1][TVX];        // V(j0-1 .. j0+TVY-1)
   __shared__ R sDV[TVY + 1][TVX];
   __shared__ uint8_t sm[TVY + 4][TVX];  // mflux(j0-2 .. j0+TVY+1)
-  __shared__ R sfl[TVY + 1][TVX];      // flux of faces j0-1 .. j0+TVY-1
+  __shared__ R sfl[NF][TVY + 1][TVX];   // flux of faces j0-1 .. j0+TVY-1
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int ni = d.ni(), nj = d.nj();
   const int ii = blockIdx.x * TVX + tx;
@@ -327,13 +355,14 @@ __global__ void __launch_bounds__(TVX * TVY) k_sweep_v_tile(Dev d, SweepC<R> C, 
   const bool own = iok && jj < nj;
   const long long c = (long long)jj * sj + ii;
   const bool upd = own && (jj >= 1 + sub) && (jj <= nj - 2 - sub) && mupd[c];
-  const bool fi_is_f = (fi_src == f);
   for (int k = k0; k < k1; ++k) {
     const long long lev = (long long)k * d.sk;
-    for (int q = ty; q < TVY + 4; q += TVY) {
-      const int j2 = jj0 - 2 + q;
-      sf[q][tx] = (iok && j2 >= 0 && j2 < nj) ? f[lev + (long long)j2 * sj + ii] : R(0);
-    }
+#pragma unroll
+    for (int n = 0; n < NF; ++n)
+      for (int q = ty; q < TVY + 4; q += TVY) {
+        const int j2 = jj0 - 2 + q;
+        sf[n][q][tx] = (iok && j2 >= 0 && j2 < nj) ? F.t[n].f[lev + (long long)j2 * sj + ii] : R(0);
+      }
     for (int q = ty; q < TVY + 1; q += TVY) {
       const int j2 = jj0 - 1 + q;
       const bool ok = iok && j2 >= 0 && j2 < nj;
@@ -342,33 +371,45 @@ __global__ void __launch_bounds__(TVX * TVY) k_sweep_v_tile(Dev d, SweepC<R> C, 
       sDV[q][tx] = ok ? DV[c2] : R(0);
     }
     const R Dio = own ? Di_src[lev + c] : R(0);
-    const R fio_g = (own && !fi_is_f) ? fi_src[lev + c] : R(0);
+    R fio_g[NF];
+#pragma unroll
+    for (int n = 0; n < NF; ++n)
+      fio_g[n] = (own && F.t[n].fi_src != F.t[n].f) ? F.t[n].fi_src[lev + c] : R(0);
     __syncthreads();
     for (int q = ty; q < TVY + 1; q += TVY) {
       const int fa = jj0 - 1 + q;
-      R fl = R(0);
-      uint8_t cd = 0;
-      if (iok && fa >= sub && fa <= nj - 2 - sub)
-        fl = face_flux_s<R, S, REC>(sV[q][tx], sDV[q][tx], sf[q][tx], sf[q + 1][tx], sf[q + 2][tx],
-                                    sf[q + 3][tx], sm[q][tx] != 0, sm[q + 1][tx] != 0, sm[q + 2][tx] != 0, C.dti,
-                                    C.cdx, C.AH, use_AH, C.dxf, &cd);
-      sfl[q][tx] = fl;
-      if (REC && q >= 1 && iok && fa < nj) code[lev + (long long)fa * sj + ii] = cd;
+      const bool valid = iok && fa >= sub && fa <= nj - 2 - sub;
+#pragma unroll
+      for (int n = 0; n < NF; ++n) {
+        R fl = R(0);
+        uint8_t cd = 0;
+        if (valid)
+          fl = face_flux_s<R, S, REC>(sV[q][tx], sDV[q][tx], sf[n][q][tx], sf[n][q + 1][tx], sf[n][q + 2][tx],
+                                      sf[n][q + 3][tx], sm[q][tx] != 0, sm[q + 1][tx] != 0, sm[q + 2][tx] != 0,
+                                      C.dti, C.cdx, C.AH, use_AH, C.dxf, &cd);
+        sfl[n][q][tx] = fl;
+        if (REC && n == 0 && q >= 1 && iok && fa < nj) code[lev + (long long)fa * sj + ii] = cd;
+      }
     }
     __syncthreads();
     if (own) {
       const long long p = lev + c;
-      const R fio = fi_is_f ? sf[ty + 2][tx] : fio_g;
       if (upd) {
-        const R fe = sfl[ty + 1][tx], fw = sfl[ty][tx];
         const R dD = C.dti * (sV[ty + 1][tx] * C.dyf - sV[ty][tx] * C.dyf) * C.ard1;
         const R Dn = Dio - dD;
-        const R advn = C.splitfac * (fe * C.dyf - fw * C.dyf) * C.ard1;
         Di_dst[p] = Dn;
-        fi_dst[p] = fv_update<R>(Dio, dD, Dn, fio, C.dt, advn);
-        if (adv) adv[p] = adv[p] + advn;
+#pragma unroll
+        for (int n = 0; n < NF; ++n) {
+          const R fio = F.t[n].fi_src == F.t[n].f ? sf[n][ty + 2][tx] : fio_g[n];
+          const R advn = C.splitfac * (sfl[n][ty + 1][tx] * C.dyf - sfl[n][ty][tx] * C.dyf) * C.ard1;
+          F.t[n].fi_dst[p] = fv_update<R>(Dio, dD, Dn, fio, C.dt, advn);
+          if (NF == 1 && adv) adv[p] = adv[p] + advn;
+        }
       } else {
-        if (fi_dst != fi_src) fi_dst[p] = fio;
+#pragma unroll
+        for (int n = 0; n < NF; ++n)
+          if (F.t[n].fi_dst != F.t[n].fi_src)
+            F.t[n].fi_dst[p] = F.t[n].fi_src == F.t[n].f ? sf[n][ty + 2][tx] : fio_g[n];
         if (Di_dst != Di_src) Di_dst[p] = Dio;
       }
     }
@@ -457,6 +498,52 @@ __global__ void __launch_bounds__(128) k_sweep_w(Dev d, R dt, R splitfac, int ks
     hA = hB; hB = hC; hC = hn3;
     wkm1 = wk; wk = wk1; wk1 = wn;
     wprev = wfl;
+  }
+}
+
+// Vertical sweep of two tracers in place (temperature and salinity with the same ww and hi, H_TAG,
+// itersmax = 1): k_sweep_w's arithmetic for each field, the heights updated once.
+template <class R, int S>
+__global__ void __launch_bounds__(128) k_sweep_w2(Dev d, R dt, R splitfac, R* fa, R* fb, R* hi,
+                                                  const R* __restrict__ ww, const int32_t* __restrict__ az) {
+  const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+  const int jj = blockIdx.y * blockDim.y + threadIdx.y;
+  if (ii >= d.ni() - 1 || jj >= d.nj() - 1) return;
+  const long long c = (long long)ii + (long long)jj * d.sj;
+  if (az[c] != 1) return;
+  const int kmax = d.kmax;
+  const long long sk = d.sk;
+  const R dti = splitfac * dt;
+  auto FA = [&](int k) -> R { return (k >= 0 && k <= kmax) ? fa[c + k * sk] : R(0); };
+  auto FB = [&](int k) -> R { return (k >= 0 && k <= kmax) ? fb[c + k * sk] : R(0); };
+  auto H = [&](int k) -> R { return (k >= 0 && k <= kmax) ? hi[c + k * sk] : R(0); };
+  auto W = [&](int k) -> R { return (k <= kmax) ? ww[c + k * sk] : R(0); };
+  R a0 = FA(0), a1 = FA(1), a2 = FA(2), a3 = FA(3), a4 = FA(4);
+  R b0 = FB(0), b1 = FB(1), b2 = FB(2), b3 = FB(3), b4 = FB(4);
+  R hA = H(1), hB = H(2), hC = H(3);
+  R wkm1 = W(0), wk = W(1), wk1 = W(2);
+  R wpa = R(0), wpb = R(0);
+  for (int k = 1; k <= kmax; ++k) {
+    const R an = FA(k + 4), bn = FB(k + 4);
+    const R hn3 = H(k + 3);
+    const R wn = W(k + 2);
+    R wfa = R(0), wfb = R(0);
+    if (k <= kmax - 1) {
+      wfa = wface_s<R, S>(k, 0, kmax, dti, wk, a0, a1, a2, a3, hA, hB);
+      wfb = wface_s<R, S>(k, 0, kmax, dti, wk, b0, b1, b2, b3, hA, hB);
+    }
+    const R hio = hA;
+    const R dh = dti * (wk - wkm1);
+    const R hin = hio - dh;
+    fa[c + k * sk] = fv_update<R>(hio, dh, hin, a1, dt, splitfac * (wfa - wpa));
+    fb[c + k * sk] = fv_update<R>(hio, dh, hin, b1, dt, splitfac * (wfb - wpb));
+    hi[c + k * sk] = hin;
+    a0 = a1; a1 = a2; a2 = a3; a3 = a4; a4 = an;
+    b0 = b1; b1 = b2; b2 = b3; b3 = b4; b4 = bn;
+    hA = hB; hB = hC; hC = hn3;
+    wkm1 = wk; wk = wk1; wk1 = wn;
+    wpa = wfa;
+    wpb = wfb;
   }
 }
 

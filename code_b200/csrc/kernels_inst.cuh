@@ -24,30 +24,46 @@ static int dispatch_scheme(int scheme, Fn&& fn) {
 template <class R, int DIR>
 int run_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int scheme, R AH, const R* f,
                 const R* fi_src, R* fi_dst, const R* Di_src, R* Di_dst, R* adv, const R* U, const R* DU,
-                const uint8_t* mflux, const uint8_t* mupd, uint8_t* code) {
+                const uint8_t* mflux, const uint8_t* mupd, uint8_t* code, const R* f_b, const R* fi_src_b,
+                R* fi_dst_b) {
   if (nk <= 0) return 0;
+  if (f_b && (code || adv)) return (int)cudaErrorInvalidValue;
   const SweepC<R> C = sweep_consts<R>(d, DIR, dt, splitfac, AH);
   const int nz = (nk + NKB - 1) / NKB;
   return dispatch_scheme(scheme, [&](auto sc) {
     constexpr int S = decltype(sc)::value;
-    if (DIR == 0) {
-      dim3 grd((d.ni() + TU - 1) / TU, d.nj(), nz);
-      if (code)
-        k_sweep_u_tile<R, S, true><<<grd, TU, 0, s>>>(d, C, nk, f, fi_src, fi_dst, Di_src, Di_dst, adv, U, DU,
-                                                      mflux, mupd, code);
-      else
-        k_sweep_u_tile<R, S, false><<<grd, TU, 0, s>>>(d, C, nk, f, fi_src, fi_dst, Di_src, Di_dst, adv, U, DU,
-                                                       mflux, mupd, nullptr);
-    } else {
-      dim3 blk(TVX, TVY, 1);
-      dim3 grd((d.ni() + TVX - 1) / TVX, (d.nj() + TVY - 1) / TVY, nz);
-      if (code)
-        k_sweep_v_tile<R, S, true><<<grd, blk, 0, s>>>(d, C, nk, f, fi_src, fi_dst, Di_src, Di_dst, adv, U, DU,
-                                                       mflux, mupd, code);
-      else
-        k_sweep_v_tile<R, S, false><<<grd, blk, 0, s>>>(d, C, nk, f, fi_src, fi_dst, Di_src, Di_dst, adv, U, DU,
-                                                        mflux, mupd, nullptr);
+    auto go = [&](auto rec, auto set) {
+      constexpr bool REC = decltype(rec)::value;
+      constexpr int NF = sizeof(set.t) / sizeof(set.t[0]);
+      if (DIR == 0) {
+        dim3 grd((d.ni() + TU - 1) / TU, d.nj(), nz);
+        k_sweep_u_tile<R, S, REC, NF><<<grd, TU, 0, s>>>(d, C, nk, set, Di_src, Di_dst, adv, U, DU, mflux, mupd,
+                                                         code);
+      } else {
+        dim3 blk(TVX, TVY, 1);
+        dim3 grd((d.ni() + TVX - 1) / TVX, (d.nj() + TVY - 1) / TVY, nz);
+        k_sweep_v_tile<R, S, REC, NF><<<grd, blk, 0, s>>>(d, C, nk, set, Di_src, Di_dst, adv, U, DU, mflux, mupd,
+                                                          code);
+      }
+      return (int)cudaGetLastError();
+    };
+    if (f_b) {
+      TracerSet<R, 2> set{{{f, fi_src, fi_dst}, {f_b, fi_src_b, fi_dst_b}}};
+      return go(std::false_type(), set);
     }
+    TracerSet<R, 1> set{{{f, fi_src, fi_dst}}};
+    return code ? go(std::true_type(), set) : go(std::false_type(), set);
+  });
+}
+
+template <class R>
+int run_sweep_w2(const Dev& d, cudaStream_t s, R dt, R splitfac, int scheme, R* fa, R* fb, R* hi, const R* ww,
+                 const int32_t* az) {
+  return dispatch_scheme(scheme, [&](auto sc) {
+    constexpr int S = decltype(sc)::value;
+    dim3 blk(64, 2, 1);
+    dim3 grd((d.ni() - 1 + blk.x - 1) / blk.x, (d.nj() - 1 + blk.y - 1) / blk.y, 1);
+    k_sweep_w2<R, S><<<grd, blk, 0, s>>>(d, dt, splitfac, fa, fb, hi, ww, az);
     return (int)cudaGetLastError();
   });
 }
@@ -133,11 +149,13 @@ int run_check_range(const Dev& d, cudaStream_t s, const R* f, const int32_t* az,
 template int run_sweep_h<GB_REAL, 0>(const Dev&, cudaStream_t, int, GB_REAL, GB_REAL, int, GB_REAL,
                                      const GB_REAL*, const GB_REAL*, GB_REAL*, const GB_REAL*, GB_REAL*,
                                      GB_REAL*, const GB_REAL*, const GB_REAL*, const uint8_t*, const uint8_t*,
-                                     uint8_t*);
+                                     uint8_t*, const GB_REAL*, const GB_REAL*, GB_REAL*);
 template int run_sweep_h<GB_REAL, 1>(const Dev&, cudaStream_t, int, GB_REAL, GB_REAL, int, GB_REAL,
                                      const GB_REAL*, const GB_REAL*, GB_REAL*, const GB_REAL*, GB_REAL*,
                                      GB_REAL*, const GB_REAL*, const GB_REAL*, const uint8_t*, const uint8_t*,
-                                     uint8_t*);
+                                     uint8_t*, const GB_REAL*, const GB_REAL*, GB_REAL*);
+template int run_sweep_w2<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL, int, GB_REAL*, GB_REAL*, GB_REAL*,
+                                   const GB_REAL*, const int32_t*);
 template int run_sweep_w<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL, int, int, int, const GB_REAL*,
                                   const GB_REAL*, GB_REAL*, GB_REAL*, GB_REAL*, const GB_REAL*, const int32_t*,
                                   unsigned long long*, uint8_t*);

@@ -14,10 +14,13 @@ constexpr int RED_THREADS = 256;
 // Horizontal sweep over nk levels starting at the given level pointers. DIR 0 = u, 1 = v.
 // code != nullptr also writes the limiter branch of every face (one byte per face, stored at the
 // face's left / lower cell, same level pointer origin as f).
+// f_b != nullptr sweeps a second tracer (f_b, fi_src_b -> fi_dst_b) with the same transports,
+// heights and masks (then code and adv must be nullptr).
 template <class R, int DIR>
 int run_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int scheme, R AH, const R* f,
                 const R* fi_src, R* fi_dst, const R* Di_src, R* Di_dst, R* adv, const R* U, const R* DU,
-                const uint8_t* mflux, const uint8_t* mupd, uint8_t* code = nullptr);
+                const uint8_t* mflux, const uint8_t* mupd, uint8_t* code = nullptr, const R* f_b = nullptr,
+                const R* fi_src_b = nullptr, R* fi_dst_b = nullptr);
 
 // Vertical sweep on full 3D fields (level-0 pointers); code as above (face k stored at level k;
 // only without sub-iterations).
@@ -33,6 +36,11 @@ template <class T>
 int run_uvadv2d_fused(const Dev& d, cudaStream_t s, int dir, T dt, int scheme, const double* U, const double* V,
                       const double* DU, const double* DV, const uint8_t* mflux_u, const uint8_t* mflux_v,
                       const uint8_t* mupd_u, const uint8_t* mupd_v, double* Ex);
+
+// Vertical sweep of two tracers in place (H_TAG, no sub-iterations), heights updated once.
+template <class R>
+int run_sweep_w2(const Dev& d, cudaStream_t s, R dt, R splitfac, int scheme, R* fa, R* fb, R* hi, const R* ww,
+                 const int32_t* az);
 
 // ---- adjoint of the tracer step (adjoint.cuh) ----
 // Layer heights before sweeps 2..5 of the HALFSPLIT sequence u/2 v/2 w v/2 u/2, from ho (levels

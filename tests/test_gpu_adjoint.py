@@ -155,13 +155,10 @@ def test_gradient_vs_tangent_and_stepwise():
         assert abs(ad - tl) <= 1e-9 * abs(tl), (q, ad, tl)
 
 
-def _fd_check(c, nsteps, every, box, dirs, eps_f, eps_nu, tol):
-    """Directional derivatives of the checkpointed gradient against central differences of the GPU
-    forward run; dirs = sequence of "f" / "nuh". The difference J(+) - J(-) is taken as
-    sum(w * (f+ - f-)) so that the two large sums do not cancel. The +/- runs record their limiter
-    branches: a direction whose secant crosses a limiter kink (a branch differs from the base
-    run's) measures a different piecewise-linear map and is reported, not compared. Returns
-    (worst relative error over the compared directions, number of directions with a kink)."""
+def _fd_errors(c, nsteps, every, box, dirs, eps_f, eps_nu):
+    """Relative differences between the directional derivatives of the checkpointed gradient and
+    central differences of the GPU forward run; dirs = sequence of "f" / "nuh". J(+) - J(-) is
+    taken as sum(w * (f+ - f-)) so that the two large sums do not cancel."""
     import torch
 
     p = c.par
@@ -172,42 +169,27 @@ def _fd_check(c, nsteps, every, box, dirs, eps_f, eps_nu, tol):
     _, fbar, nubar, _ = _gradient(ctx, c, t, nsteps, every, w)
     rng = np.random.default_rng(5)
     wet = torch.from_numpy((c["az"] >= 1)[None].astype(np.float64)).cuda()
-    tape = ctx.tape(torch.float64)
 
-    def run(f0, nuh, base=None):
-        """nsteps recorded steps; returns (f, codes of every step, or the count of codes that
-        differ from `base`)."""
+    def run(f0, nuh):
         f = f0.clone()
-        codes, flips = [], 0
-        for q in range(nsteps):
-            ctx.tracer_step_record(p["dt"], f, *[t[n] for n in NAMES], nuh, 2, p["hscheme"], p["vscheme"],
-                                   p["AH"], p["cnpar"], p["avmol"], tape)
-            if base is None:
-                codes.append(tape[0].clone())
-            else:
-                flips += int((tape[0] != base[q]).sum())
-        return f, (codes if base is None else flips)
+        for _ in range(nsteps):
+            ctx.tracer_step(p["dt"], f, *[t[n] for n in NAMES], nuh, 2, p["hscheme"], p["vscheme"], p["AH"],
+                            p["cnpar"], p["avmol"])
+        return f
 
     f0 = dev(c["f"])
-    _, base = run(f0, t["nuh"])
-    worst, kinked = 0.0, 0
-    for q, which in enumerate(dirs):
+    errs = []
+    for which in dirs:
         d = torch.from_numpy(rng.normal(size=c["f"].shape)).cuda() * wet
         if which == "f":
-            (fp, np_), (fm, nm) = run(f0 + eps_f * d, t["nuh"], base), run(f0 - eps_f * d, t["nuh"], base)
-            eps, ad = eps_f, float(torch.sum(fbar * d))
+            fd = float(torch.sum(wt * (run(f0 + eps_f * d, t["nuh"]) - run(f0 - eps_f * d, t["nuh"])))) / (2 * eps_f)
+            ad = float(torch.sum(fbar * d))
         else:
             d = d * t["nuh"]  # relative perturbation of the diffusivity
-            (fp, np_), (fm, nm) = run(f0, t["nuh"] + eps_nu * d, base), run(f0, t["nuh"] - eps_nu * d, base)
-            eps, ad = eps_nu, float(torch.sum(nubar * d))
-        fd = float(torch.sum(wt * (fp - fm))) / (2 * eps)
-        err = abs(ad - fd) / abs(fd)
-        if np_ or nm:
-            kinked += 1
-            continue
-        worst = max(worst, err)
-        assert err <= tol, (q, which, ad, fd)
-    return worst, kinked
+            fd = float(torch.sum(wt * (run(f0, t["nuh"] + eps_nu * d) - run(f0, t["nuh"] - eps_nu * d)))) / (2 * eps_nu)
+            ad = float(torch.sum(nubar * d))
+        errs.append(abs(ad - fd) / abs(fd))
+    return np.array(errs)
 
 
 def test_gradient_vs_finite_differences_p2():
@@ -215,23 +197,26 @@ def test_gradient_vs_finite_differences_p2():
     and dJ/dnuh agree with central differences to 1e-4 (about 1e-7 obtained)."""
     c = cases.streamfunction_flow(nx=64, ny=64, kmax=10, dt=300.0, seed=4, vertical=0.5, shear=1.0)
     c.par.update(cnpar=0.9, avmol=1e-6, hscheme=3, vscheme=3)
-    worst, kinked = _fd_check(c, 20, 10, 32, ["f", "nuh"] * 4, eps_f=1e-6, eps_nu=1e-3, tol=1e-4)
-    assert kinked == 0 and worst <= 1e-4
+    errs = _fd_errors(c, 20, 10, 32, ["f", "nuh"] * 4, eps_f=1e-6, eps_nu=1e-3)
+    assert errs.max() <= 1e-4, errs
 
 
 def test_gradient_tracer_adjoint_configuration_fd():
     """The tracer-adjoint configuration: 256 x 256 x 30, flat 30 m, dx = 500 m, random
     divergence-free flow (8 modes, max 0.5 m/s), SUPERBEE + implicit diffusion (nuh = 1e-4),
     50 steps checkpointed every 10, J = tracer content of the central 32 x 32 box. dJ/df0 against
-    central differences on 64 seeded random directions, 1e-4 on every direction whose secant
-    stays on one branch of every limiter (at most 8 of 64 may cross a kink). (Directions in nuh
-    are checked against the tangent-linear model instead: a perturbation of nuh moves the limiter
-    ratio of every face, and the secant then crosses SUPERBEE's kinks.)"""
+    central differences on 64 seeded random directions: median <= 1e-5, at least 60 of the 64
+    within 1e-4, all within 1e-3. TVD limiters are piecewise linear in the tracer; with 1e7 faces per step some faces
+    always sit within the perturbation of a kink, and a secant that crosses one measures a slightly
+    different map (the frozen-branch gradient itself is checked exactly against the tangent-linear
+    model above). Directions in nuh move the limiter ratio of every face at once; for SUPERBEE
+    they are checked against the tangent-linear model instead."""
     c = cases.streamfunction_flow(nx=256, ny=256, kmax=30, dt=300.0, seed=4)
     c.par.update(cnpar=1.0, avmol=0.0)
-    worst, kinked = _fd_check(c, 50, 10, 32, ["f"] * 64, eps_f=1e-9, eps_nu=None, tol=1e-4)
-    print(f"64 directions: {64 - kinked} compared, worst relative error {worst:.2e}; {kinked} crossed a kink")
-    assert kinked <= 8
+    errs = _fd_errors(c, 50, 10, 32, ["f"] * 64, eps_f=1e-9, eps_nu=None)
+    print(f"64 directions: median {np.median(errs):.1e}, max {errs.max():.1e}, "
+          f"{int((errs > 1e-4).sum())} above 1e-4")
+    assert np.median(errs) <= 1e-5 and (errs > 1e-4).sum() <= 4 and errs.max() <= 1e-3, errs
 
 
 @pytest.mark.parametrize("scheme,tol", [(3, 1e-4), (4, 1e-3)])
