@@ -95,11 +95,14 @@ int step_record(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww
 }
 
 // Adjoint of one tracer step: fbar (cotangent of the step's output) becomes the cotangent of its
-// input; nubar accumulates the cotangent of nuh.
+// input; nubar accumulates the cotangent of nuh. Sn_in = the step's output (the diffusion's
+// result) when the caller kept it, else it is re-solved from g; heights_ready = the heights before
+// sweeps 2..5 are already in the adjoint scratch (the velocities and layer heights are those of
+// the previous call).
 template <class R>
 int step_adjoint(getm_ctx* ctx, R dt, R* fbar, R* nubar, const R* uu, const R* vv, const R* ww, const R* hu,
                  const R* hv, const R* ho, const R* hn, const R* nuh, int hs, int vs, R AH, R cnpar, R avmol,
-                 const uint8_t* codes, const R* g) {
+                 const uint8_t* codes, const R* g, const R* Sn_in = nullptr, bool heights_ready = false) {
   const Dev& d = ctx->dev;
   cudaStream_t s = ctx->stream;
   const long long n3 = n3d(d);
@@ -119,13 +122,18 @@ int step_adjoint(getm_ctx* ctx, R dt, R* fbar, R* nubar, const R* uu, const R* v
   const R half = R(0.5), one = R(1);
   const bool has_w = vs != NOADV && kmax > 1;
   const size_t b0 = (size_t)sk * sizeof(R);  // level 0 (untouched by the horizontal sweeps)
-  // the diffusion's output, recomputed from its input on the tape
-  GB_TIMED(GETM_TIM_ADJ, cudaMemcpyAsync(Sn, g, (size_t)n3 * sizeof(R), cudaMemcpyDeviceToDevice, s), "copy g");
-  GB_TIMED(GETM_TIM_ADJ, run_vdiff<R>(d, s, dt, cnpar, avmol, Sn, hn, nuh, ctx->zmask, nullptr, RU, QU), "vdiff");
-  GB_TIMED(GETM_TIM_ADJ, run_adj_vdiff<R>(d, s, dt, cnpar, avmol, fbar, tmp, nubar, g, Sn, hn, nuh, ctx->zmask, RU,
-                                          QU), "adjoint vdiff");
-  GB_TIMED(GETM_TIM_ADJ, run_adj_heights<R>(d, s, dt, hs == UPSTREAM ? 0 : 1, has_w, ho, uu, vv, ww,
-                                            gr.mask_uupdate, gr.mask_vupdate, gr.az, H1, H2, H3, H4), "heights");
+  // the diffusion's output: kept by the caller, or re-solved from its input on the tape
+  const R* Sout = Sn_in;
+  if (!Sout) {
+    GB_TIMED(GETM_TIM_ADJ, cudaMemcpyAsync(Sn, g, (size_t)n3 * sizeof(R), cudaMemcpyDeviceToDevice, s), "copy g");
+    GB_TIMED(GETM_TIM_ADJ, run_vdiff<R>(d, s, dt, cnpar, avmol, Sn, hn, nuh, ctx->zmask, nullptr, RU, QU), "vdiff");
+    Sout = Sn;
+  }
+  GB_TIMED(GETM_TIM_ADJ, run_adj_vdiff<R>(d, s, dt, cnpar, avmol, fbar, tmp, nubar, g, Sout, hn, nuh, ctx->zmask,
+                                          RU, QU), "adjoint vdiff");
+  if (!heights_ready)
+    GB_TIMED(GETM_TIM_ADJ, run_adj_heights<R>(d, s, dt, hs == UPSTREAM ? 0 : 1, has_w, ho, uu, vv, ww,
+                                              gr.mask_uupdate, gr.mask_vupdate, gr.az, H1, H2, H3, H4), "heights");
   // u/2 (sweep 5): tmp -> fbar
   GB_TRY(cudaMemcpyAsync(fbar, tmp, b0, cudaMemcpyDeviceToDevice, s), "level 0");
   GB_TIMED(GETM_TIM_ADJ, (run_adj_sweep_h<R, 0>(d, s, kmax, dt, half, hs, AH, L(tmp, 1), L(fbar, 1), L(H4, 1),
@@ -194,7 +202,7 @@ int gradient_api(getm_ctx* ctx, int nsteps, int every, R dt, R* f, const R* uu, 
   const size_t fb = (size_t)n3 * sizeof(R);
   const int nblk = (nsteps + every - 1) / every;
   const int blk = nsteps < every ? nsteps : every;
-  const size_t tape1 = 5 * (size_t)n3 + fb;  // codes + g of one step
+  const size_t tape1 = 5 * (size_t)n3 + 2 * fb;  // codes + g + the step's output of one step
   const size_t need = (size_t)nblk * fb + (size_t)blk * tape1 + 256;
   if (ctx->adj_store_bytes < need) {
     cudaFree(ctx->adj_store);
@@ -212,7 +220,8 @@ int gradient_api(getm_ctx* ctx, int nsteps, int every, R dt, R* f, const R* uu, 
   // multiple of the element size, so the g parts are placed after all code planes instead
   uint8_t* codes0 = tape;
   R* g0 = (R*)(tape + (size_t)blk * 5 * n3 + (256 - ((size_t)blk * 5 * n3) % 256) % 256);
-  if ((uint8_t*)(g0 + (size_t)blk * n3) > (uint8_t*)ctx->adj_store + need)
+  R* sn0 = g0 + (size_t)blk * n3;  // the output of each step of the block (the diffusion's result)
+  if ((uint8_t*)(sn0 + (size_t)blk * n3) > (uint8_t*)ctx->adj_store + need)
     return fail(ctx, GETM_ERR_NOMEM, "tracer_gradient: tape layout");
   cudaEvent_t ev[3];
   for (auto& e : ev) GB_TRY(cudaEventCreate(&e), "event");
@@ -228,6 +237,7 @@ int gradient_api(getm_ctx* ctx, int nsteps, int every, R dt, R* f, const R* uu, 
     if (rc) return rc;
   }
   GB_TRY(cudaEventRecord(ev[1], s), "event");
+  bool heights_done = false;
   // reverse: blocks from the last; the forward state of a block is rebuilt in scr-independent
   // storage (the checkpoint slot itself: its value is not needed again)
   for (int b = nblk - 1; b >= 0; --b) {
@@ -238,11 +248,16 @@ int gradient_api(getm_ctx* ctx, int nsteps, int every, R dt, R* f, const R* uu, 
       rc = step_record<R>(ctx, dt, fw, uu, vv, ww, hu, hv, ho, hn, nuh, hs, vs, AH, cnpar, avmol,
                           codes0 + (size_t)q * 5 * n3, g0 + (size_t)q * n3);
       if (rc) return rc;
+      GB_TIMED(GETM_TIM_ADJ_RECORD,
+               cudaMemcpyAsync(sn0 + (size_t)q * n3, fw, fb, cudaMemcpyDeviceToDevice, s), "tape output");
     }
     for (int q = cnt - 1; q >= 0; --q) {
+      // velocities, heights and nuh are the same in every step: the heights before each sweep are
+      // computed by the first adjoint step and reused
       rc = step_adjoint<R>(ctx, dt, fbar, nubar, uu, vv, ww, hu, hv, ho, hn, nuh, hs, vs, AH, cnpar, avmol,
-                           codes0 + (size_t)q * 5 * n3, g0 + (size_t)q * n3);
+                           codes0 + (size_t)q * 5 * n3, g0 + (size_t)q * n3, sn0 + (size_t)q * n3, heights_done);
       if (rc) return rc;
+      heights_done = true;
     }
   }
   GB_TRY(cudaEventRecord(ev[2], s), "event");

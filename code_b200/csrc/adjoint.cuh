@@ -50,99 +50,110 @@ __global__ void k_adj_heights(Dev d, R dt, int sub, int has_w, const R* __restri
 }
 
 // ---------------------------------------------------------------------------------------------
-// Adjoint of the u sweep over a row segment of TU cells. Staged: U, DU, flux masks at cells
-// i0-3 .. i0+TU+1, cotangents and heights at cells i0-2 .. i0+TU+1, branch codes of faces
-// i0-2 .. i0+TU.
+// Adjoint of the u sweep over a row segment of TU cells, for up to NKB levels (the 2D masks are
+// staged once). Staged per level: U, DU at cells i0-3 .. i0+TU+1, cotangents and heights at cells
+// i0-2 .. i0+TU+1, branch codes of faces i0-2 .. i0+TU.
 template <class R, int S>
-__global__ void __launch_bounds__(TU) k_adj_sweep_u(Dev d, R dt, R splitfac, R AH, const R* __restrict__ gbar,
-                                                    R* __restrict__ fbar, const R* __restrict__ Dio,
-                                                    const R* __restrict__ U, const R* __restrict__ DU,
-                                                    const uint8_t* __restrict__ mflux,
+__global__ void __launch_bounds__(TU) k_adj_sweep_u(Dev d, R dt, R splitfac, R AH, int nk,
+                                                    const R* __restrict__ gbar, R* __restrict__ fbar,
+                                                    const R* __restrict__ Dio, const R* __restrict__ U,
+                                                    const R* __restrict__ DU, const uint8_t* __restrict__ mflux,
                                                     const uint8_t* __restrict__ mupd,
                                                     const uint8_t* __restrict__ code) {
   __shared__ R sU[TU + 5], sDU[TU + 5];
-  __shared__ uint8_t sm[TU + 5];
+  __shared__ uint8_t sm[TU + 5], su[TU + 4];
   __shared__ R sg[TU + 4], skc[TU + 4], spc[TU + 4];
   __shared__ R sw[4][TU + 3];
   const int t = threadIdx.x;
   const int ni = d.ni();
   const int ii0 = blockIdx.x * TU;
   const long long crow = (long long)blockIdx.y * d.sj;
-  const long long row = crow + (long long)blockIdx.z * d.sk;
+  const int k0 = blockIdx.z * NKB;
+  const int k1 = min(k0 + NKB, nk);
   constexpr int sub = (S == UPSTREAM) ? 0 : 1;
   const R dti = splitfac * dt;
   const R dxf = R(d.dx), dyf = R(d.dy), ard1 = R(d.ard1);
   const R cdx = dti / dxf;
   const bool use_AH = AH > R(0);
+  const R kfac = dt * splitfac * dyf * ard1;
   for (int q = t; q < TU + 5; q += TU) {
     const int ii = ii0 - 3 + q;
-    const bool ok = ii >= 0 && ii < ni;
-    sU[q] = ok ? U[row + ii] : R(0);
-    sDU[q] = ok ? DU[row + ii] : R(0);
-    sm[q] = ok ? mflux[crow + ii] : 0;
+    sm[q] = (ii >= 0 && ii < ni) ? mflux[crow + ii] : 0;
   }
-  __syncthreads();
-  // cells q <-> ii = ii0-2+q; U of its east face = sU[q+1], of its west face = sU[q]
-  const R kfac = dt * splitfac * dyf * ard1;
   for (int q = t; q < TU + 4; q += TU) {
     const int ii = ii0 - 2 + q;
-    R g = R(0), kc = R(0), pc = R(1);
-    if (ii >= 0 && ii < ni) {
-      g = gbar[row + ii];
-      if ((ii >= 1 + sub) && (ii <= ni - 2 - sub) && mupd[crow + ii]) {
-        const R hio = Dio[row + ii];
-        const R dD = dti * (sU[q + 1] * dyf - sU[q] * dyf) * ard1;
-        const R hin = hio - dD;
-        kc = kfac / hin;
-        pc = hio / hin;
-      }
-    }
-    sg[q] = g;
-    skc[q] = kc;
-    spc[q] = pc;
+    su[q] = (ii >= 0 && ii < ni && ii >= 1 + sub && ii <= ni - 2 - sub) ? mupd[crow + ii] : 0;
   }
-  __syncthreads();
-  // faces r <-> fa = ii0-2+r (between cells fa and fa+1); U index r+1, cells r and r+1
-  for (int r = t; r < TU + 3; r += TU) {
-    const int fa = ii0 - 2 + r;
-    R wm1 = R(0), w0 = R(0), w1 = R(0), w2 = R(0);
-    if (fa >= sub && fa <= ni - 2 - sub && sm[r + 1]) {
-      const R Fb = -sg[r] * skc[r] + sg[r + 1] * skc[r + 1];
-      const R Uf = sU[r + 1], DUf = sDU[r + 1];
-      const bool pos = Uf > R(0);
-      R A = R(0), B = R(0);
-      if (S != UPSTREAM && (pos ? sm[r] : sm[r + 2])) {
-        const R cfl = face_cfl<R>(pos, Uf, DUf, dti, cdx, dxf);
-        recon_coef<R, S>(code[row + fa], cfl, A, B);
-      }
-      const R FU = Fb * Uf;
-      const R cu = FU * (R(1) + A - B), cuu = -FU * A, cd = FU * B;
-      if (pos) {
-        wm1 = cuu; w0 = cu; w1 = cd;
-      } else {
-        w0 = cd; w1 = cu; w2 = cuu;
-      }
-      if (use_AH) {
-        const R ka = Fb * AH * DUf / dxf;
-        w0 = w0 + ka;
-        w1 = w1 - ka;
-      }
+  for (int k = k0; k < k1; ++k) {
+    const long long row = crow + (long long)k * d.sk;
+    for (int q = t; q < TU + 5; q += TU) {
+      const int ii = ii0 - 3 + q;
+      const bool ok = ii >= 0 && ii < ni;
+      sU[q] = ok ? U[row + ii] : R(0);
+      sDU[q] = ok ? DU[row + ii] : R(0);
     }
-    sw[0][r] = wm1;
-    sw[1][r] = w0;
-    sw[2][r] = w1;
-    sw[3][r] = w2;
+    __syncthreads();
+    // cells q <-> ii = ii0-2+q; U of its east face = sU[q+1], of its west face = sU[q]
+    for (int q = t; q < TU + 4; q += TU) {
+      const int ii = ii0 - 2 + q;
+      R g = R(0), kc = R(0), pc = R(1);
+      if (ii >= 0 && ii < ni) {
+        g = gbar[row + ii];
+        if (su[q]) {
+          const R hio = Dio[row + ii];
+          const R dD = dti * (sU[q + 1] * dyf - sU[q] * dyf) * ard1;
+          const R hin = hio - dD;
+          kc = kfac / hin;
+          pc = hio / hin;
+        }
+      }
+      sg[q] = g;
+      skc[q] = kc;
+      spc[q] = pc;
+    }
+    __syncthreads();
+    // faces r <-> fa = ii0-2+r (between cells fa and fa+1); U index r+1, cells r and r+1
+    for (int r = t; r < TU + 3; r += TU) {
+      const int fa = ii0 - 2 + r;
+      R wm1 = R(0), w0 = R(0), w1 = R(0), w2 = R(0);
+      if (fa >= sub && fa <= ni - 2 - sub && sm[r + 1]) {
+        const R Fb = -sg[r] * skc[r] + sg[r + 1] * skc[r + 1];
+        const R Uf = sU[r + 1], DUf = sDU[r + 1];
+        const bool pos = Uf > R(0);
+        R A = R(0), B = R(0);
+        if (S != UPSTREAM && (pos ? sm[r] : sm[r + 2])) {
+          const R cfl = face_cfl<R>(pos, Uf, DUf, dti, cdx, dxf);
+          recon_coef<R, S>(code[row + fa], cfl, A, B);
+        }
+        const R FU = Fb * Uf;
+        const R cu = FU * (R(1) + A - B), cuu = -FU * A, cd = FU * B;
+        if (pos) {
+          wm1 = cuu; w0 = cu; w1 = cd;
+        } else {
+          w0 = cd; w1 = cu; w2 = cuu;
+        }
+        if (use_AH) {
+          const R ka = Fb * AH * DUf / dxf;
+          w0 = w0 + ka;
+          w1 = w1 - ka;
+        }
+      }
+      sw[0][r] = wm1;
+      sw[1][r] = w0;
+      sw[2][r] = w1;
+      sw[3][r] = w2;
+    }
+    __syncthreads();
+    const int ii = ii0 + t;
+    // cell ii: q = t+2; faces ii+1, ii, ii-1, ii-2 <-> r = t+3, t+2, t+1, t
+    if (ii < ni) fbar[row + ii] = sg[t + 2] * spc[t + 2] + sw[0][t + 3] + sw[1][t + 2] + sw[2][t + 1] + sw[3][t];
+    __syncthreads();
   }
-  __syncthreads();
-  const int ii = ii0 + t;
-  if (ii >= ni) return;
-  // cell ii: q = t+2; faces ii+1, ii, ii-1, ii-2 <-> r = t+3, t+2, t+1, t
-  fbar[row + ii] = sg[t + 2] * spc[t + 2] + sw[0][t + 3] + sw[1][t + 2] + sw[2][t + 1] + sw[3][t];
 }
 
-// Adjoint of the v sweep over a tile of TVX x TVY cells (same scheme along j).
+// Adjoint of the v sweep over a tile of TVX x TVY cells, for up to NKB levels.
 template <class R, int S>
-__global__ void __launch_bounds__(TVX * TVY) k_adj_sweep_v(Dev d, R dt, R splitfac, R AH,
+__global__ void __launch_bounds__(TVX * TVY) k_adj_sweep_v(Dev d, R dt, R splitfac, R AH, int nk,
                                                            const R* __restrict__ gbar, R* __restrict__ fbar,
                                                            const R* __restrict__ Dio, const R* __restrict__ V,
                                                            const R* __restrict__ DV,
@@ -150,84 +161,98 @@ __global__ void __launch_bounds__(TVX * TVY) k_adj_sweep_v(Dev d, R dt, R splitf
                                                            const uint8_t* __restrict__ mupd,
                                                            const uint8_t* __restrict__ code) {
   __shared__ R sV[TVY + 5][TVX], sDV[TVY + 5][TVX];
-  __shared__ uint8_t sm[TVY + 5][TVX];
+  __shared__ uint8_t sm[TVY + 5][TVX], su[TVY + 4][TVX];
   __shared__ R sg[TVY + 4][TVX], skc[TVY + 4][TVX], spc[TVY + 4][TVX];
   __shared__ R sw[4][TVY + 3][TVX];
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int ni = d.ni(), nj = d.nj();
   const int ii = blockIdx.x * TVX + tx;
   const int jj0 = blockIdx.y * TVY;
-  const long long lev = (long long)blockIdx.z * d.sk;
+  const int k0 = blockIdx.z * NKB;
+  const int k1 = min(k0 + NKB, nk);
   const bool iok = ii < ni;
+  const long long sj = d.sj;
   constexpr int sub = (S == UPSTREAM) ? 0 : 1;
   const R dti = splitfac * dt;
   const R dxf = R(d.dy), dyf = R(d.dx), ard1 = R(d.ard1);  // DYV, DXV
   const R cdx = dti / dxf;
   const bool use_AH = AH > R(0);
+  const R kfac = dt * splitfac * dyf * ard1;
   for (int q = ty; q < TVY + 5; q += TVY) {
     const int jj = jj0 - 3 + q;
-    const bool ok = iok && jj >= 0 && jj < nj;
-    const long long c = (long long)jj * d.sj + ii;
-    sV[q][tx] = ok ? V[lev + c] : R(0);
-    sDV[q][tx] = ok ? DV[lev + c] : R(0);
-    sm[q][tx] = ok ? mflux[c] : 0;
+    sm[q][tx] = (iok && jj >= 0 && jj < nj) ? mflux[(long long)jj * sj + ii] : 0;
   }
-  __syncthreads();
-  const R kfac = dt * splitfac * dyf * ard1;
   for (int q = ty; q < TVY + 4; q += TVY) {
     const int jj = jj0 - 2 + q;
-    R g = R(0), kc = R(0), pc = R(1);
-    if (iok && jj >= 0 && jj < nj) {
-      const long long c = (long long)jj * d.sj + ii;
-      g = gbar[lev + c];
-      if ((jj >= 1 + sub) && (jj <= nj - 2 - sub) && mupd[c]) {
-        const R hio = Dio[lev + c];
-        const R dD = dti * (sV[q + 1][tx] * dyf - sV[q][tx] * dyf) * ard1;
-        const R hin = hio - dD;
-        kc = kfac / hin;
-        pc = hio / hin;
-      }
-    }
-    sg[q][tx] = g;
-    skc[q][tx] = kc;
-    spc[q][tx] = pc;
+    su[q][tx] = (iok && jj >= 0 && jj < nj && jj >= 1 + sub && jj <= nj - 2 - sub) ? mupd[(long long)jj * sj + ii]
+                                                                                   : 0;
   }
-  __syncthreads();
-  for (int r = ty; r < TVY + 3; r += TVY) {
-    const int fa = jj0 - 2 + r;
-    R wm1 = R(0), w0 = R(0), w1 = R(0), w2 = R(0);
-    if (iok && fa >= sub && fa <= nj - 2 - sub && sm[r + 1][tx]) {
-      const R Fb = -sg[r][tx] * skc[r][tx] + sg[r + 1][tx] * skc[r + 1][tx];
-      const R Vf = sV[r + 1][tx], DVf = sDV[r + 1][tx];
-      const bool pos = Vf > R(0);
-      R A = R(0), B = R(0);
-      if (S != UPSTREAM && (pos ? sm[r][tx] : sm[r + 2][tx])) {
-        const R cfl = face_cfl<R>(pos, Vf, DVf, dti, cdx, dxf);
-        recon_coef<R, S>(code[lev + (long long)fa * d.sj + ii], cfl, A, B);
-      }
-      const R FV = Fb * Vf;
-      const R cu = FV * (R(1) + A - B), cuu = -FV * A, cd = FV * B;
-      if (pos) {
-        wm1 = cuu; w0 = cu; w1 = cd;
-      } else {
-        w0 = cd; w1 = cu; w2 = cuu;
-      }
-      if (use_AH) {
-        const R ka = Fb * AH * DVf / dxf;
-        w0 = w0 + ka;
-        w1 = w1 - ka;
-      }
+  for (int k = k0; k < k1; ++k) {
+    const long long lev = (long long)k * d.sk;
+    for (int q = ty; q < TVY + 5; q += TVY) {
+      const int jj = jj0 - 3 + q;
+      const bool ok = iok && jj >= 0 && jj < nj;
+      const long long c = lev + (long long)jj * sj + ii;
+      sV[q][tx] = ok ? V[c] : R(0);
+      sDV[q][tx] = ok ? DV[c] : R(0);
     }
-    sw[0][r][tx] = wm1;
-    sw[1][r][tx] = w0;
-    sw[2][r][tx] = w1;
-    sw[3][r][tx] = w2;
+    __syncthreads();
+    for (int q = ty; q < TVY + 4; q += TVY) {
+      const int jj = jj0 - 2 + q;
+      R g = R(0), kc = R(0), pc = R(1);
+      if (iok && jj >= 0 && jj < nj) {
+        const long long c = lev + (long long)jj * sj + ii;
+        g = gbar[c];
+        if (su[q][tx]) {
+          const R hio = Dio[c];
+          const R dD = dti * (sV[q + 1][tx] * dyf - sV[q][tx] * dyf) * ard1;
+          const R hin = hio - dD;
+          kc = kfac / hin;
+          pc = hio / hin;
+        }
+      }
+      sg[q][tx] = g;
+      skc[q][tx] = kc;
+      spc[q][tx] = pc;
+    }
+    __syncthreads();
+    for (int r = ty; r < TVY + 3; r += TVY) {
+      const int fa = jj0 - 2 + r;
+      R wm1 = R(0), w0 = R(0), w1 = R(0), w2 = R(0);
+      if (iok && fa >= sub && fa <= nj - 2 - sub && sm[r + 1][tx]) {
+        const R Fb = -sg[r][tx] * skc[r][tx] + sg[r + 1][tx] * skc[r + 1][tx];
+        const R Vf = sV[r + 1][tx], DVf = sDV[r + 1][tx];
+        const bool pos = Vf > R(0);
+        R A = R(0), B = R(0);
+        if (S != UPSTREAM && (pos ? sm[r][tx] : sm[r + 2][tx])) {
+          const R cfl = face_cfl<R>(pos, Vf, DVf, dti, cdx, dxf);
+          recon_coef<R, S>(code[lev + (long long)fa * sj + ii], cfl, A, B);
+        }
+        const R FV = Fb * Vf;
+        const R cu = FV * (R(1) + A - B), cuu = -FV * A, cd = FV * B;
+        if (pos) {
+          wm1 = cuu; w0 = cu; w1 = cd;
+        } else {
+          w0 = cd; w1 = cu; w2 = cuu;
+        }
+        if (use_AH) {
+          const R ka = Fb * AH * DVf / dxf;
+          w0 = w0 + ka;
+          w1 = w1 - ka;
+        }
+      }
+      sw[0][r][tx] = wm1;
+      sw[1][r][tx] = w0;
+      sw[2][r][tx] = w1;
+      sw[3][r][tx] = w2;
+    }
+    __syncthreads();
+    const int jj = jj0 + ty;
+    if (iok && jj < nj)
+      fbar[lev + (long long)jj * sj + ii] = sg[ty + 2][tx] * spc[ty + 2][tx] + sw[0][ty + 3][tx] +
+                                            sw[1][ty + 2][tx] + sw[2][ty + 1][tx] + sw[3][ty][tx];
+    __syncthreads();
   }
-  __syncthreads();
-  const int jj = jj0 + ty;
-  if (!iok || jj >= nj) return;
-  fbar[lev + (long long)jj * d.sj + ii] = sg[ty + 2][tx] * spc[ty + 2][tx] + sw[0][ty + 3][tx] +
-                                          sw[1][ty + 2][tx] + sw[2][ty + 1][tx] + sw[3][ty][tx];
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -357,40 +382,40 @@ __global__ void __launch_bounds__(128) k_adj_vdiff(Dev d, R dt, R cnpar, R avmol
     RUs[c + k * sk] = ru;
     QUs[c + k * sk] = qu;
   }
-  R lam;
+  R lam1;
   {
     const R an_k = an_km1;
     const R a3 = -an_k, a2 = hnkm1 + an_k;
-    lam = (L(fbar, 1) - a3 * qu) / (a2 - a3 * ru);
-    QUs[c + sk] = lam;
+    lam1 = (L(fbar, 1) - a3 * qu) / (a2 - a3 * ru);
   }
-  for (k = 2; k <= kmax; ++k) {
-    lam = QUs[c + k * sk] - RUs[c + k * sk] * lam;
-    QUs[c + k * sk] = lam;
-  }
-  // gbar = B lambda and the nuh cotangent, bottom-up with lambda(k-1), lambda(k), lambda(k+1)
+  // back substitution upwards, lambda(k) = qu(k) - ru(k) lambda(k-1), fused with the output pass:
+  // once lambda(k) is known, level k-1 is complete --
+  //   gbar(k-1) = h(k-1) l(k-1) + ao(k-1) (l(k) - l(k-1)) - ao(k-2) (l(k-1) - l(k-2)),
+  //   nubar(k-1) += (l(k-1) - l(k)) (co (g(k) - g(k-1)) + cn (Sn(k) - Sn(k-1))) / (h(k-1) + h(k)).
   gbar[c] = L(fbar, 0);
-  R lm = R(0), l0 = QUs[c + sk];
-  R ao_m = R(0);  // ao of the interface below level k
-  R hk = L(hn, 1);
-  for (k = 1; k <= kmax; ++k) {
-    const R l1 = (k < kmax) ? QUs[c + (k + 1) * sk] : R(0);
-    R ao_k = R(0);
-    R hk1 = R(0);
-    if (k < kmax) {
-      hk1 = L(hn, k + 1);
+  R lm = R(0), l0 = lam1;     // lambda(k-2), lambda(k-1)
+  R ao_m = R(0);              // ao of the interface below level k-1
+  R hk = L(hn, 1), gk = L(g, 1), sk0 = L(Sn, 1);  // h, g, Sn at level k-1
+  for (k = 2; k <= kmax + 1; ++k) {
+    R l1 = R(0), ao_k = R(0), hk1 = R(0), gk1 = R(0), sk1 = R(0);
+    if (k <= kmax) {
+      l1 = QUs[c + k * sk] - RUs[c + k * sk] * l0;
+      hk1 = L(hn, k);
+      gk1 = L(g, k);
+      sk1 = L(Sn, k);
       const R hs = hk + hk1;
-      const R nu = L(nuh, k) + avmol;
+      const R nu = L(nuh, k - 1) + avmol;
       ao_k = co * nu / hs;
       const R dl = l0 - l1;
-      nubar[c + k * sk] = nubar[c + k * sk] +
-                          dl * (co * (L(g, k + 1) - L(g, k)) + cn * (L(Sn, k + 1) - L(Sn, k))) / hs;
+      nubar[c + (k - 1) * sk] = nubar[c + (k - 1) * sk] + dl * (co * (gk1 - gk) + cn * (sk1 - sk0)) / hs;
     }
-    gbar[c + k * sk] = hk * l0 + ao_k * (l1 - l0) - ao_m * (l0 - lm);
+    gbar[c + (k - 1) * sk] = hk * l0 + ao_k * (l1 - l0) - ao_m * (l0 - lm);
     lm = l0;
     l0 = l1;
     ao_m = ao_k;
     hk = hk1;
+    gk = gk1;
+    sk0 = sk1;
   }
 }
 
@@ -416,13 +441,14 @@ int run_adj_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int 
   if (nk <= 0) return 0;
   return dispatch_scheme(scheme, [&](auto sc) {
     constexpr int S = decltype(sc)::value;
+    const int nz = (nk + NKB - 1) / NKB;
     if (DIR == 0) {
-      dim3 grd((d.ni() + TU - 1) / TU, d.nj(), nk);
-      k_adj_sweep_u<R, S><<<grd, TU, 0, s>>>(d, dt, splitfac, AH, gbar, fbar, Dio, U, DU, mflux, mupd, code);
+      dim3 grd((d.ni() + TU - 1) / TU, d.nj(), nz);
+      k_adj_sweep_u<R, S><<<grd, TU, 0, s>>>(d, dt, splitfac, AH, nk, gbar, fbar, Dio, U, DU, mflux, mupd, code);
     } else {
       dim3 blk(TVX, TVY, 1);
-      dim3 grd((d.ni() + TVX - 1) / TVX, (d.nj() + TVY - 1) / TVY, nk);
-      k_adj_sweep_v<R, S><<<grd, blk, 0, s>>>(d, dt, splitfac, AH, gbar, fbar, Dio, U, DU, mflux, mupd, code);
+      dim3 grd((d.ni() + TVX - 1) / TVX, (d.nj() + TVY - 1) / TVY, nz);
+      k_adj_sweep_v<R, S><<<grd, blk, 0, s>>>(d, dt, splitfac, AH, nk, gbar, fbar, Dio, U, DU, mflux, mupd, code);
     }
     return (int)cudaGetLastError();
   });

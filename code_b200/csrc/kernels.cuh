@@ -236,7 +236,7 @@ struct TracerSet {
 
 // u sweep (adv_split_u.F90:222-285) over one row segment of TU cells, for up to NKB levels.
 template <class R, int S, bool REC, int NF>
-__global__ void __launch_bounds__(TU) k_sweep_u_tile(Dev d, SweepC<R> C, int nk, TracerSet<R, NF> F,
+__global__ void __launch_bounds__(TU, sizeof(R) == 4 ? 16 : 8) k_sweep_u_tile(Dev d, SweepC<R> C, int nk, TracerSet<R, NF> F,
                                                      const R* Di_src, R* Di_dst, R* adv,
                                                      const R* __restrict__ U, const R* __restrict__ DU,
                                                      const uint8_t* __restrict__ mflux,
@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(TU) k_sweep_u_tile(Dev d, SweepC<R> C, int nk,
 
 // v sweep (adv_split_v.F90:79-135) over a tile of TVX x TVY cells, for up to NKB levels.
 template <class R, int S, bool REC, int NF>
-__global__ void __launch_bounds__(TVX * TVY, sizeof(R) == 4 && NF == 1 ? 2048 / (TVX * TVY) : 1)
+__global__ void __launch_bounds__(TVX * TVY, sizeof(R) == 4 ? (NF == 1 ? 8 : 4) : (NF == 1 ? 4 : 3))
     k_sweep_v_tile(Dev d, SweepC<R> C, int nk, TracerSet<R, NF> F, const R* Di_src, R* Di_dst, R* adv,
                    const R* __restrict__ V, const R* __restrict__ DV, const uint8_t* __restrict__ mflux,
                    const uint8_t* __restrict__ mupd, uint8_t* code) {
@@ -684,18 +684,24 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, R*
   // (ao+an)(k)*(S(k+1)-S(k)) - (ao+an)(k-1)*(S(k)-S(k-1)) [+ src]; the rounding then acts on the
   // small increment rather than on h*S (bias-free over hundreds of steps).
   constexpr bool incr = sizeof(R) == 4;
+  // The loads of level k-2 are issued one iteration ahead of their use (the elimination is a
+  // serial chain per column; this keeps two levels of loads in flight per thread).
   // surface row k = kmax: au = a1, bu = a2, du = a4
   int k = kmax;
   R hnk = L(hn, k), hnkm1 = L(hn, k - 1);
   R nu = L(nuh, k - 1) + avmol;
-  R ao_km1 = co * nu / (hnk + hnkm1), an_km1 = cn * nu / (hnk + hnkm1);
   R Sk = L(S, k), Skm1 = L(S, k - 1);
+  R srck = src ? L(src, k) : R(0);
+  // next window entries (level kmax-2 and the interface below it)
+  R hn_n = kmax >= 2 ? L(hn, kmax - 2) : R(0), nuh_n = kmax >= 2 ? L(nuh, kmax - 2) : R(0);
+  R S_n = kmax >= 2 ? L(S, kmax - 2) : R(0), src_n = (src && kmax >= 2) ? L(src, kmax - 1) : R(0);
+  R ao_km1 = co * nu / (hnk + hnkm1), an_km1 = cn * nu / (hnk + hnkm1);
   R ru, qu;
   {
     const R a1 = -an_km1;
     const R a2 = hnk + an_km1;
     R a4 = incr ? -(ao_km1 + an_km1) * (Sk - Skm1) : Sk * (hnk - ao_km1) + Skm1 * ao_km1;
-    if (src) a4 = a4 + L(src, k);
+    if (src) a4 = a4 + srck;
     ru = a1 / a2;
     qu = a4 / a2;
     RUs[c + k * sk] = ru;
@@ -705,19 +711,26 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, R*
   for (k = kmax - 1; k >= 2; --k) {
     const R ao_k = ao_km1, an_k = an_km1;  // aux at interface k (computed as k-1 of row k+1)
     hnk = hnkm1;
-    hnkm1 = L(hn, k - 1);
-    nu = L(nuh, k - 1) + avmol;
-    ao_km1 = co * nu / (hnk + hnkm1);
-    an_km1 = cn * nu / (hnk + hnkm1);
+    hnkm1 = hn_n;
+    nu = nuh_n + avmol;
     const R Skp1 = Sk;
     Sk = Skm1;
-    Skm1 = L(S, k - 1);
+    Skm1 = S_n;
+    const R srcv = src_n;
+    if (k >= 3) {
+      hn_n = L(hn, k - 2);
+      nuh_n = L(nuh, k - 2);
+      S_n = L(S, k - 2);
+    }
+    if (src) src_n = L(src, k - 1);
+    ao_km1 = co * nu / (hnk + hnkm1);
+    an_km1 = cn * nu / (hnk + hnkm1);
     const R a3 = -an_k;
     const R a1 = -an_km1;
     const R a2 = hnk + an_k + an_km1;
     R a4 = incr ? (ao_k + an_k) * (Skp1 - Sk) - (ao_km1 + an_km1) * (Sk - Skm1)
                 : Skp1 * ao_k + Sk * (hnk - ao_k - ao_km1) + Skm1 * ao_km1;
-    if (src) a4 = a4 + L(src, k);
+    if (src) a4 = a4 + srcv;
     const R den = a2 - a3 * ru;
     ru = a1 / den;
     qu = (a4 - a3 * qu) / den;
@@ -738,9 +751,18 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, R*
     v = (a4 - a3 * qu) / (a2 - a3 * ru);
     S[c + 1 * sk] = incr ? S1 + v : v;
   }
+  // back substitution upwards, with the next level's coefficients loaded one step ahead
+  R qn = kmax >= 2 ? QUs[c + 2 * sk] : R(0), rn = kmax >= 2 ? RUs[c + 2 * sk] : R(0);
+  R sn = (incr && kmax >= 2) ? L(S, 2) : R(0);
   for (k = 2; k <= kmax; ++k) {
-    v = QUs[c + k * sk] - RUs[c + k * sk] * v;
-    S[c + k * sk] = incr ? L(S, k) + v : v;
+    const R q = qn, r = rn, so = sn;
+    if (k < kmax) {
+      qn = QUs[c + (k + 1) * sk];
+      rn = RUs[c + (k + 1) * sk];
+      if (incr) sn = L(S, k + 1);
+    }
+    v = q - r * v;
+    S[c + k * sk] = incr ? so + v : v;
   }
 }
 
