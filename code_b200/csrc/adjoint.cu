@@ -121,7 +121,6 @@ int step_adjoint(getm_ctx* ctx, R dt, R* fbar, R* nubar, const R* uu, const R* v
   auto plane = [&](int q) { return codes + (long long)q * n3; };
   const R half = R(0.5), one = R(1);
   const bool has_w = vs != NOADV && kmax > 1;
-  const size_t b0 = (size_t)sk * sizeof(R);  // level 0 (untouched by the horizontal sweeps)
   // the diffusion's output: kept by the caller, or re-solved from its input on the tape
   const R* Sout = Sn_in;
   if (!Sout) {
@@ -135,15 +134,13 @@ int step_adjoint(getm_ctx* ctx, R dt, R* fbar, R* nubar, const R* uu, const R* v
     GB_TIMED(GETM_TIM_ADJ, run_adj_heights<R>(d, s, dt, hs == UPSTREAM ? 0 : 1, has_w, ho, uu, vv, ww,
                                               gr.mask_uupdate, gr.mask_vupdate, gr.az, H1, H2, H3, H4), "heights");
   // u/2 (sweep 5): tmp -> fbar
-  GB_TRY(cudaMemcpyAsync(fbar, tmp, b0, cudaMemcpyDeviceToDevice, s), "level 0");
   GB_TIMED(GETM_TIM_ADJ, (run_adj_sweep_h<R, 0>(d, s, kmax, dt, half, hs, AH, L(tmp, 1), L(fbar, 1), L(H4, 1),
                                                 L(uu, 1), L(hu, 1), gr.mask_uflux, gr.mask_uupdate,
-                                                L(plane(4), 1))), "adjoint u2");
+                                                L(plane(4), 1), true)), "adjoint u2");
   // v/2 (sweep 4): fbar -> tmp
-  GB_TRY(cudaMemcpyAsync(tmp, fbar, b0, cudaMemcpyDeviceToDevice, s), "level 0");
   GB_TIMED(GETM_TIM_ADJ, (run_adj_sweep_h<R, 1>(d, s, kmax, dt, half, hs, AH, L(fbar, 1), L(tmp, 1), L(H3, 1),
                                                 L(vv, 1), L(hv, 1), gr.mask_vflux, gr.mask_vupdate,
-                                                L(plane(3), 1))), "adjoint v2");
+                                                L(plane(3), 1), true)), "adjoint v2");
   // w (sweep 3): tmp -> fbar
   if (has_w) {
     GB_TIMED(GETM_TIM_ADJ, run_adj_sweep_w<R>(d, s, dt, one, vs, 0, tmp, fbar, H2, ww, gr.az, plane(2)),
@@ -152,15 +149,13 @@ int step_adjoint(getm_ctx* ctx, R dt, R* fbar, R* nubar, const R* uu, const R* v
     GB_TRY(cudaMemcpyAsync(fbar, tmp, (size_t)n3 * sizeof(R), cudaMemcpyDeviceToDevice, s), "copy");
   }
   // v/2 (sweep 2): fbar -> tmp
-  GB_TRY(cudaMemcpyAsync(tmp, fbar, b0, cudaMemcpyDeviceToDevice, s), "level 0");
   GB_TIMED(GETM_TIM_ADJ, (run_adj_sweep_h<R, 1>(d, s, kmax, dt, half, hs, AH, L(fbar, 1), L(tmp, 1), L(H1, 1),
                                                 L(vv, 1), L(hv, 1), gr.mask_vflux, gr.mask_vupdate,
-                                                L(plane(1), 1))), "adjoint v1");
+                                                L(plane(1), 1), true)), "adjoint v1");
   // u/2 (sweep 1): tmp -> fbar
-  GB_TRY(cudaMemcpyAsync(fbar, tmp, b0, cudaMemcpyDeviceToDevice, s), "level 0");
   GB_TIMED(GETM_TIM_ADJ, (run_adj_sweep_h<R, 0>(d, s, kmax, dt, half, hs, AH, L(tmp, 1), L(fbar, 1), L(ho, 1),
                                                 L(uu, 1), L(hu, 1), gr.mask_uflux, gr.mask_uupdate,
-                                                L(plane(0), 1))), "adjoint u1");
+                                                L(plane(0), 1), true)), "adjoint u1");
   return GETM_OK;
 }
 

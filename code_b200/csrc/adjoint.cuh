@@ -54,7 +54,7 @@ __global__ void k_adj_heights(Dev d, R dt, int sub, int has_w, const R* __restri
 // staged once). Staged per level: U, DU at cells i0-3 .. i0+TU+1, cotangents and heights at cells
 // i0-2 .. i0+TU+1, branch codes of faces i0-2 .. i0+TU.
 template <class R, int S>
-__global__ void __launch_bounds__(TU) k_adj_sweep_u(Dev d, R dt, R splitfac, R AH, int nk,
+__global__ void __launch_bounds__(TU) k_adj_sweep_u(Dev d, R dt, R splitfac, R AH, int nk, bool copy0,
                                                     const R* __restrict__ gbar, R* __restrict__ fbar,
                                                     const R* __restrict__ Dio, const R* __restrict__ U,
                                                     const R* __restrict__ DU, const uint8_t* __restrict__ mflux,
@@ -84,6 +84,8 @@ __global__ void __launch_bounds__(TU) k_adj_sweep_u(Dev d, R dt, R splitfac, R A
     const int ii = ii0 - 2 + q;
     su[q] = (ii >= 0 && ii < ni && ii >= 1 + sub && ii <= ni - 2 - sub) ? mupd[crow + ii] : 0;
   }
+  // level 0 (below the level pointers' origin) is not touched by the sweep: its cotangent passes
+  if (copy0 && blockIdx.z == 0 && ii0 + t < ni) fbar[crow - d.sk + ii0 + t] = gbar[crow - d.sk + ii0 + t];
   for (int k = k0; k < k1; ++k) {
     const long long row = crow + (long long)k * d.sk;
     for (int q = t; q < TU + 5; q += TU) {
@@ -153,7 +155,7 @@ __global__ void __launch_bounds__(TU) k_adj_sweep_u(Dev d, R dt, R splitfac, R A
 
 // Adjoint of the v sweep over a tile of TVX x TVY cells, for up to NKB levels.
 template <class R, int S>
-__global__ void __launch_bounds__(TVX * TVY) k_adj_sweep_v(Dev d, R dt, R splitfac, R AH, int nk,
+__global__ void __launch_bounds__(TVX * TVY) k_adj_sweep_v(Dev d, R dt, R splitfac, R AH, int nk, bool copy0,
                                                            const R* __restrict__ gbar, R* __restrict__ fbar,
                                                            const R* __restrict__ Dio, const R* __restrict__ V,
                                                            const R* __restrict__ DV,
@@ -186,6 +188,11 @@ __global__ void __launch_bounds__(TVX * TVY) k_adj_sweep_v(Dev d, R dt, R splitf
     const int jj = jj0 - 2 + q;
     su[q][tx] = (iok && jj >= 0 && jj < nj && jj >= 1 + sub && jj <= nj - 2 - sub) ? mupd[(long long)jj * sj + ii]
                                                                                    : 0;
+  }
+  // level 0 (below the level pointers' origin) is not touched by the sweep: its cotangent passes
+  if (copy0 && blockIdx.z == 0 && iok && jj0 + ty < nj) {
+    const long long c0 = (long long)(jj0 + ty) * sj + ii - d.sk;
+    fbar[c0] = gbar[c0];
   }
   for (int k = k0; k < k1; ++k) {
     const long long lev = (long long)k * d.sk;
@@ -437,18 +444,20 @@ int run_adj_heights(const Dev& d, cudaStream_t s, R dt, int sub, bool has_w, con
 template <class R, int DIR>
 int run_adj_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int scheme, R AH, const R* gbar,
                     R* fbar, const R* Dio, const R* U, const R* DU, const uint8_t* mflux, const uint8_t* mupd,
-                    const uint8_t* code) {
+                    const uint8_t* code, bool copy0) {
   if (nk <= 0) return 0;
   return dispatch_scheme(scheme, [&](auto sc) {
     constexpr int S = decltype(sc)::value;
     const int nz = (nk + NKB - 1) / NKB;
     if (DIR == 0) {
       dim3 grd((d.ni() + TU - 1) / TU, d.nj(), nz);
-      k_adj_sweep_u<R, S><<<grd, TU, 0, s>>>(d, dt, splitfac, AH, nk, gbar, fbar, Dio, U, DU, mflux, mupd, code);
+      k_adj_sweep_u<R, S><<<grd, TU, 0, s>>>(d, dt, splitfac, AH, nk, copy0, gbar, fbar, Dio, U, DU, mflux, mupd,
+                                             code);
     } else {
       dim3 blk(TVX, TVY, 1);
       dim3 grd((d.ni() + TVX - 1) / TVX, (d.nj() + TVY - 1) / TVY, nz);
-      k_adj_sweep_v<R, S><<<grd, blk, 0, s>>>(d, dt, splitfac, AH, nk, gbar, fbar, Dio, U, DU, mflux, mupd, code);
+      k_adj_sweep_v<R, S><<<grd, blk, 0, s>>>(d, dt, splitfac, AH, nk, copy0, gbar, fbar, Dio, U, DU, mflux, mupd,
+                                              code);
     }
     return (int)cudaGetLastError();
   });

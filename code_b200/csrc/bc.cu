@@ -301,6 +301,79 @@ __global__ void k_sbf_r(Dev d, Bc2 s, const double* Uip, const double* Vip, unsi
   }
 }
 
+// update_2d_bdy.F90:74-178: elevations of the open-boundary points [p0, p1) of one side (sides are
+// launched in the reference's order W, N, E, S). Harmonic data: amp*sin(2*pi*loop*dtm/period+phase).
+__global__ void k_bdy2d(Dev d, Bc2 s, const int4* __restrict__ pts, int p0, int p1, const double* data,
+                        const double* data_u, const double* data_v, const double* amp, const double* phase,
+                        double period, double fac, int loop) {
+  const int p = p0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= p1) return;
+  W2 z{d, s.f2[Z]}, D{d, s.f2[D_]}, U{d, s.f2[U_]}, DU_{d, s.f2[DU]}, V{d, s.f2[V_]}, DV_{d, s.f2[DV]},
+      H{d, s.f2[HH]};
+  const int4 q = pts[p];
+  const int i = q.x, j = q.y, type = q.z, side = q.w;
+  const double dtm = s.par[P_DTM], min_depth = s.par[P_MIN_DEPTH];
+  const double g = (double)9.81f;  // the single-precision literal of update_2d_bdy.F90:92,96
+  double bd;
+  if (amp) {
+    const double pi2 = 2.0 * 3.14159265358979323846;
+    bd = amp[p] * sin(pi2 * (loop * dtm) / period + phase[p]);
+  } else {
+    bd = data[p];
+  }
+  const double bu = data_u ? data_u[p] : 0.0, bv = data_v ? data_v[p] : 0.0;
+  double zn = z(i, j);
+  switch (side) {
+    case 0:  // western
+      if (type == 1) zn = z(i + 1, j);
+      else if (type == 2) zn = z(i, j) + dtm / d.dx * sqrt(g * D(i, j)) * (z(i + 1, j) - z(i, j));
+      else if (type == 3) zn = fmax(fac * bd, -H(i, j) + min_depth);
+      else {
+        const double a = sqrt(DU_(i, j) / g) * (U(i, j) / DU_(i, j) - bu);
+        zn = fmax(fac * (bd - a), -H(i, j) + min_depth);
+      }
+      break;
+    case 1:  // northern
+      if (type == 1) zn = z(i, j - 1);
+      else if (type == 2) zn = z(i, j) - dtm / d.dy * sqrt(g * D(i, j)) * (z(i, j) - z(i, j - 1));
+      else if (type == 3) zn = fmax(fac * bd, -H(i, j) + min_depth);
+      else {
+        const double a = sqrt(DV_(i, j) / g) * (V(i, j - 1) / DV_(i, j - 1) - bv);
+        zn = fmax(fac * (bd + a), -H(i, j) + min_depth);
+      }
+      break;
+    case 2:  // eastern
+      if (type == 1) zn = z(i - 1, j);
+      else if (type == 2) zn = z(i, j) - dtm / d.dx * sqrt(g * D(i, j)) * (z(i, j) - z(i - 1, j));
+      else if (type == 3) zn = fmax(fac * bd, -H(i, j) + min_depth);
+      else {
+        const double a = sqrt(DU_(i, j) / g) * (U(i - 1, j) / DU_(i - 1, j) - bu);
+        zn = fmax(fac * (bd + a), -H(i, j) + min_depth);
+      }
+      break;
+    default:  // southern
+      if (type == 1) zn = z(i, j + 1);
+      else if (type == 2) zn = z(i, j) + dtm / d.dy * sqrt(g * D(i, j)) * (z(i, j + 1) - z(i, j));
+      else if (type == 3) zn = fmax(fac * bd, -H(i, j) + min_depth);
+      else {
+        const double a = sqrt(DV_(i, j) / g) * (V(i, j) / DV_(i, j) - bv);
+        zn = fmax(fac * (bd - a), -H(i, j) + min_depth);
+      }
+      break;
+  }
+  z(i, j) = zn;
+}
+
+// mirror_bdy_2d.F90 / mirror_bdy_3d.F90: f(dst) = f(src) for the (dst, src) 2D offsets of one side,
+// on nl levels with stride sk.
+template <class T>
+__global__ void k_mirror(T* f, const long long* __restrict__ pairs, int n, int nl, long long sk) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const long long dst = pairs[2 * p], src = pairs[2 * p + 1];
+  for (int k = 0; k < nl; ++k) f[dst + k * sk] = f[src + k * sk];
+}
+
 // stop_macro.F90:36-39
 __global__ void k_stop_macro(Dev d, Bc2 s) {
   GB_IJ2
@@ -354,6 +427,41 @@ int check_state(getm_ctx* ctx, const getm_bc_state* st) {
   if (st->ipar[I_M] < 1 || st->ipar[I_MM] < 1) return fail(ctx, GETM_ERR_ARG, "M and MM must be >= 1");
   if ((size_t)2 * (ctx->dom.kmax + 1) * 64 * sizeof(double) > 200 * 1024)
     return fail(ctx, GETM_ERR_UNSUPPORTED, "kmax too large for the column solvers");
+  return GETM_OK;
+}
+
+// mirror_bdy copies of one tag (0 U, 1 V, 2 H/D) on a 2D (nl = 1) or 3D (nl = kmax+1) field, side
+// by side in the reference's order.
+template <class T>
+int mirror_bdy(getm_ctx* ctx, T* f, int tag, int nl) {
+  if (!ctx->has_bdy) return GETM_OK;
+  const auto& b = ctx->bdy;
+  for (int side = 0; side < 4; ++side) {
+    const int p0 = b.pair_first[tag][side], p1 = b.pair_first[tag][side + 1];
+    if (p1 <= p0) continue;
+    TimerScope ts(ctx, nl > 1 ? GETM_TIM_BC3D : GETM_TIM_BC2D);
+    k_mirror<T><<<(p1 - p0 + 127) / 128, 128, 0, ctx->stream>>>(f, b.pairs + 2 * (long long)p0, p1 - p0, nl,
+                                                                ctx->dev.sk);
+    GB_TRY(cudaGetLastError(), "mirror_bdy");
+  }
+  return GETM_OK;
+}
+
+// update_2d_bdy (m2d.F90:475)
+int bdy_2d(getm_ctx* ctx, const Bc2& s, int loop) {
+  if (!ctx->has_bdy) return GETM_OK;
+  const auto& b = ctx->bdy;
+  double fac = 1.0;
+  if (b.ramp > 1) fac = fmin(1.0, 4.0 * loop / (double)(float)b.ramp);
+  for (int side = 0; side < 4; ++side) {
+    const int p0 = b.side_first[side], p1 = b.side_first[side + 1];
+    if (p1 <= p0) continue;
+    TimerScope ts(ctx, GETM_TIM_BC2D);
+    k_bdy2d<<<(p1 - p0 + 127) / 128, 128, 0, ctx->stream>>>(ctx->dev, s, b.pts, p0, p1, b.data, b.data_u, b.data_v,
+                                                            b.harmonic ? b.amp : nullptr, b.phase, b.period, fac,
+                                                            loop);
+    GB_TRY(cudaGetLastError(), "update_2d_bdy");
+  }
   return GETM_OK;
 }
 
@@ -508,19 +616,31 @@ int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop) {
   if ((loop - 1) % ip[I_MM] == 0) GB_K2(k_bottom_friction, d, s, ip[I_RUNTYPE]);
   int rc = uv_advect_2d(ctx, st, st->f2[U_], st->f2[V_], st->f2[DU], st->f2[DV]);
   if (rc) return rc;
-  if (ip[I_UFIRST2D]) {
+  // umomentum / vmomentum: transport update, mirror_bdy_2d (momentum.F90:190,353), Coriolis term
+  auto umom = [&]() -> int {
     GB_K2(k_momentum<0>, d, s);
+    int r = mirror_bdy<double>(ctx, st->f2[U_], 0, 1);
+    if (r) return r;
     GB_K2(k_coriolis<0>, d, s);
+    return GETM_OK;
+  };
+  auto vmom = [&]() -> int {
     GB_K2(k_momentum<1>, d, s);
+    int r = mirror_bdy<double>(ctx, st->f2[V_], 1, 1);
+    if (r) return r;
     GB_K2(k_coriolis<1>, d, s);
+    return GETM_OK;
+  };
+  if (ip[I_UFIRST2D]) {
+    if ((rc = umom()) || (rc = vmom())) return rc;
     ip[I_UFIRST2D] = 0;
   } else {
-    GB_K2(k_momentum<1>, d, s);
-    GB_K2(k_coriolis<1>, d, s);
-    GB_K2(k_momentum<0>, d, s);
-    GB_K2(k_coriolis<0>, d, s);
+    if ((rc = vmom()) || (rc = umom())) return rc;
     ip[I_UFIRST2D] = 1;
   }
+  // update_2d_bdy sets the boundary elevations after the Uint accumulation and before sealevel
+  // (m2d.F90:467-476); the accumulation does not touch z, so it runs inside the sealevel kernel
+  if ((rc = bdy_2d(ctx, s, loop))) return rc;
   GB_K2(k_accum_sealevel, d, s, ip[I_RUNTYPE] > 1 ? 1 : 0);
   GB_K2(k_depth_update, d, s);
   return GETM_OK;
@@ -563,13 +683,20 @@ int integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
     GB_TRY(cudaMemcpyAsync(f3[HUO], f3[HUN], b3, cudaMemcpyDeviceToDevice, s), "huo=hun");
     GB_TRY(cudaMemcpyAsync(f3[HVO], f3[HVN], b3, cudaMemcpyDeviceToDevice, s), "hvo=hvn");
   }
+  // uu/vv_momentum_3d, each followed by its mirror_bdy_3d (uu_momentum_3d.F90:389, vv_momentum_3d.F90:400)
+  auto uum = [&]() -> int {
+    int r = bc3<R3>(ctx, st, BC3_UUMOM, GETM_TIM_MOM3D);
+    return r ? r : mirror_bdy<R3>(ctx, f3[UU], 0, d.kmax + 1);
+  };
+  auto vvm = [&]() -> int {
+    int r = bc3<R3>(ctx, st, BC3_VVMOM, GETM_TIM_MOM3D);
+    return r ? r : mirror_bdy<R3>(ctx, f3[VV], 1, d.kmax + 1);
+  };
   if (ip[I_UFIRST3D]) {
-    if ((rc = bc3<R3>(ctx, st, BC3_UUMOM, GETM_TIM_MOM3D))) return rc;
-    if ((rc = bc3<R3>(ctx, st, BC3_VVMOM, GETM_TIM_MOM3D))) return rc;
+    if ((rc = uum()) || (rc = vvm())) return rc;
     ip[I_UFIRST3D] = 0;
   } else {
-    if ((rc = bc3<R3>(ctx, st, BC3_VVMOM, GETM_TIM_MOM3D))) return rc;
-    if ((rc = bc3<R3>(ctx, st, BC3_UUMOM, GETM_TIM_MOM3D))) return rc;
+    if ((rc = vvm()) || (rc = uum())) return rc;
     ip[I_UFIRST3D] = 1;
   }
   if ((rc = bc3<R3>(ctx, st, BC3_SIGMA, GETM_TIM_BC3D))) return rc;
@@ -630,6 +757,9 @@ int integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
                                              f3[NUH], st->az, (const R3*)nullptr, (R3*)ctx->scr[0], (R3*)ctx->scr[1]),
                "vdiff S");
     }
+    // m3d.F90:595,602
+    if (ip[I_CALC_TEMP] && (rc = mirror_bdy<R3>(ctx, f3[TT], 2, d.kmax + 1))) return rc;
+    if (ip[I_CALC_SALT] && (rc = mirror_bdy<R3>(ctx, f3[SS], 2, d.kmax + 1))) return rc;
     if ((rc = bc3<R3>(ctx, st, BC3_EQSTATE, GETM_TIM_BC3D))) return rc;
   }
   if (d.kmax > 1) {
@@ -648,6 +778,139 @@ int integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
 }  // namespace
 
 extern "C" {
+
+int getm_set_open_boundaries(getm_ctx* ctx, const getm_bdy* b) {
+  if (!ctx || !b) return GETM_ERR_ARG;
+  if (!ctx->adv_ready) return fail(ctx, GETM_ERR_STATE, "getm_init_advection has not been called");
+  const Dev& d = ctx->dev;
+  const int cnt[4] = {b->nwb, b->nnb, b->neb, b->nsb};
+  const int nseg = cnt[0] + cnt[1] + cnt[2] + cnt[3];
+  if (cnt[0] < 0 || cnt[1] < 0 || cnt[2] < 0 || cnt[3] < 0 || (nseg > 0 && (!b->seg || !b->type2d)))
+    return fail(ctx, GETM_ERR_ARG, "open boundaries: bad segment description");
+  // masks on the host (they select the mirrored points)
+  const long long n2 = n2d(d);
+  std::vector<int32_t> az(n2), au(n2), av(n2);
+  GB_TRY(cudaMemcpyAsync(az.data(), ctx->zmask, n2 * 4, cudaMemcpyDeviceToHost, ctx->stream), "masks");
+  GB_TRY(cudaMemcpyAsync(au.data(), ctx->zmask + n2, n2 * 4, cudaMemcpyDeviceToHost, ctx->stream), "masks");
+  GB_TRY(cudaMemcpyAsync(av.data(), ctx->zmask + 2 * n2, n2 * 4, cudaMemcpyDeviceToHost, ctx->stream), "masks");
+  GB_TRY(cudaStreamSynchronize(ctx->stream), "masks");
+  auto ix = [&](int i, int j) { return (long long)(i - (d.imin - HALO)) + (long long)(j - (d.jmin - HALO)) * d.sj; };
+  auto inside = [&](int i, int j) { return i >= d.imin && i <= d.imax && j >= d.jmin && j <= d.jmax; };
+  // boundary points in segment order (bdy_map), side by side
+  std::vector<int4> pts;
+  auto& B = ctx->bdy;
+  int l = 0;
+  for (int side = 0; side < 4; ++side) {
+    B.side_first[side] = (int)pts.size();
+    for (int n = 0; n < cnt[side]; ++n, ++l) {
+      const int pos = b->seg[3 * l], f = b->seg[3 * l + 1], e = b->seg[3 * l + 2], t = b->type2d[l];
+      if (t < 1 || t > 4) return fail(ctx, GETM_ERR_ARG, "open boundaries: illegal 2D boundary type");
+      for (int q = f; q <= e; ++q) {
+        const int i = (side == 0 || side == 2) ? pos : q, j = (side == 0 || side == 2) ? q : pos;
+        if (!inside(i, j)) return fail(ctx, GETM_ERR_ARG, "open boundaries: point outside the domain");
+        pts.push_back(make_int4(i, j, t, side));
+      }
+    }
+  }
+  B.side_first[4] = (int)pts.size();
+  const int np = (int)pts.size();
+  if (b->npoints != np) return fail(ctx, GETM_ERR_ARG, "open boundaries: npoints does not match the segments");
+  // mirror copies (mirror_bdy_2d.F90 / mirror_bdy_3d.F90), per tag and side
+  std::vector<long long> pairs;
+  auto seg = [&](int side, int n, int q) {
+    int first = 0;
+    for (int s2 = 0; s2 < side; ++s2) first += cnt[s2];
+    return b->seg[3 * (first + n) + q];
+  };
+  auto in_array = [&](int i, int j) {
+    return i >= d.imin - HALO && i <= d.imax + HALO && j >= d.jmin - HALO && j <= d.jmax + HALO;
+  };
+  for (int tag = 0; tag < 3; ++tag)
+    for (int side = 0; side < 4; ++side) {
+      B.pair_first[tag][side] = (int)(pairs.size() / 2);
+      for (int n = 0; n < cnt[side]; ++n) {
+        const int pos = seg(side, n, 0), f = seg(side, n, 1) - HALO, e = seg(side, n, 2) + HALO;
+        for (int q = f; q <= e; ++q) {
+          const int i = (side == 0 || side == 2) ? pos : q, j = (side == 0 || side == 2) ? q : pos;
+          if (!in_array(i, j)) continue;
+          int di = 0, dj = 0, si = 0, sj = 0;
+          bool use = false;
+          if (tag == 0 && (side == 1 || side == 3)) {  // U points, au == 3
+            use = au[ix(i, j)] == 3;
+            di = i; dj = j; si = i; sj = side == 1 ? j - 1 : j + 1;
+          } else if (tag == 1 && (side == 0 || side == 2)) {  // V points, av == 3
+            use = av[ix(i, j)] == 3;
+            di = i; dj = j; si = side == 0 ? i + 1 : i - 1; sj = j;
+          } else if (tag == 2) {  // boundary value into the point outside
+            use = az[ix(i, j)] > 1;
+            si = i; sj = j;
+            di = side == 0 ? i - 1 : side == 2 ? i + 1 : i;
+            dj = side == 1 ? j + 1 : side == 3 ? j - 1 : j;
+          }
+          if (use && in_array(di, dj) && in_array(si, sj)) {
+            pairs.push_back(ix(di, dj));
+            pairs.push_back(ix(si, sj));
+          }
+        }
+      }
+      B.pair_first[tag][side + 1] = (int)(pairs.size() / 2);
+    }
+  // device copies
+  auto up = [&](auto*& dst, const auto* src, size_t count) -> int {
+    cudaFree(dst);
+    dst = nullptr;
+    if (!src || count == 0) return GETM_OK;
+    using E = std::remove_pointer_t<std::remove_reference_t<decltype(dst)>>;
+    if (cudaMalloc((void**)&dst, count * sizeof(E)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(ctx, GETM_ERR_NOMEM, "open boundaries: allocation failed");
+    }
+    return cudaMemcpy(dst, src, count * sizeof(E), cudaMemcpyHostToDevice) == cudaSuccess
+               ? GETM_OK
+               : fail(ctx, GETM_ERR_CUDA, "open boundaries: copy failed");
+  };
+  int rc;
+  if ((rc = up(B.pts, pts.data(), pts.size())) || (rc = up(B.pairs, pairs.data(), pairs.size())) ||
+      (rc = up(B.data, b->data, np)) || (rc = up(B.data_u, b->data_u, np)) || (rc = up(B.data_v, b->data_v, np)) ||
+      (rc = up(B.amp, b->amp, np)) || (rc = up(B.phase, b->phase, np)))
+    return rc;
+  if (b->amp && !b->phase) return fail(ctx, GETM_ERR_ARG, "open boundaries: harmonic data needs phase");
+  if (!b->amp && !b->data && np > 0) return fail(ctx, GETM_ERR_ARG, "open boundaries: no elevation data");
+  B.npoints = np;
+  B.harmonic = b->amp != nullptr;
+  B.period = b->period;
+  B.ramp = b->ramp;
+  if (B.harmonic && !(b->period > 0)) return fail(ctx, GETM_ERR_ARG, "open boundaries: period must be > 0");
+  ctx->has_bdy = nseg > 0;
+  return GETM_OK;
+}
+
+int getm_set_bdy_data(getm_ctx* ctx, const double* data, const double* data_u, const double* data_v) {
+  if (!ctx || !data) return GETM_ERR_ARG;
+  if (!ctx->has_bdy) return fail(ctx, GETM_ERR_STATE, "getm_set_open_boundaries has not been called");
+  auto& B = ctx->bdy;
+  const size_t nb = (size_t)B.npoints * sizeof(double);
+  auto put = [&](double*& dst, const double* src) -> int {
+    if (!src) {
+      cudaFree(dst);
+      dst = nullptr;
+      return GETM_OK;
+    }
+    if (!dst && cudaMalloc((void**)&dst, nb) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(ctx, GETM_ERR_NOMEM, "boundary data: allocation failed");
+    }
+    return cudaMemcpyAsync(dst, src, nb, cudaMemcpyHostToDevice, ctx->stream) == cudaSuccess
+               ? GETM_OK
+               : fail(ctx, GETM_ERR_CUDA, "boundary data: copy failed");
+  };
+  int rc;
+  if ((rc = put(B.data, data)) || (rc = put(B.data_u, data_u)) || (rc = put(B.data_v, data_v))) return rc;
+  // the host arrays may be reused by the caller right after the call
+  GB_TRY(cudaStreamSynchronize(ctx->stream), "boundary data");
+  B.harmonic = false;
+  return GETM_OK;
+}
 
 int getm_integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop) {
   int rc = check_state(ctx, st);

@@ -327,6 +327,9 @@ int getm_ctx_destroy(getm_ctx* ctx) {
   cudaFree(ctx->bc_scr2);
   cudaFree(ctx->adj_scr);
   cudaFree(ctx->adj_store);
+  for (void* p : {(void*)ctx->bdy.pts, (void*)ctx->bdy.data, (void*)ctx->bdy.data_u, (void*)ctx->bdy.data_v,
+                  (void*)ctx->bdy.amp, (void*)ctx->bdy.phase, (void*)ctx->bdy.pairs})
+    cudaFree(p);
   for (int t = 0; t < GETM_NTIMERS; ++t)
     for (auto& ev : ctx->pending[t]) ctx->pool.push_back(ev);
   for (auto& ev : ctx->pool) {

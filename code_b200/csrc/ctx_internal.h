@@ -46,6 +46,20 @@ struct getm_ctx {
   size_t adj_scr_bytes = 0;
   void* adj_store = nullptr;
   size_t adj_store_bytes = 0;
+  // open boundaries (getm_set_open_boundaries): boundary points and mirror copies, device arrays
+  struct Bdy {
+    int npoints = 0;
+    int side_first[5] = {0, 0, 0, 0, 0};  // points of side s: [side_first[s], side_first[s+1])
+    int4* pts = nullptr;                   // (i, j, type, side) per point, reference indices
+    double *data = nullptr, *data_u = nullptr, *data_v = nullptr, *amp = nullptr, *phase = nullptr;
+    bool harmonic = false;
+    double period = 0.0;
+    int ramp = -1;
+    // mirror copies (dst, src 2D offsets) per tag (0 U, 1 V, 2 H/D) and side
+    long long* pairs = nullptr;
+    int pair_first[3][5] = {};
+  } bdy;
+  bool has_bdy = false;
 };
 
 namespace {

@@ -188,10 +188,10 @@ template int run_adj_heights<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, int, bo
                                       const int32_t*, GB_REAL*, GB_REAL*, GB_REAL*, GB_REAL*);
 template int run_adj_sweep_h<GB_REAL, 0>(const Dev&, cudaStream_t, int, GB_REAL, GB_REAL, int, GB_REAL,
                                          const GB_REAL*, GB_REAL*, const GB_REAL*, const GB_REAL*, const GB_REAL*,
-                                         const uint8_t*, const uint8_t*, const uint8_t*);
+                                         const uint8_t*, const uint8_t*, const uint8_t*, bool);
 template int run_adj_sweep_h<GB_REAL, 1>(const Dev&, cudaStream_t, int, GB_REAL, GB_REAL, int, GB_REAL,
                                          const GB_REAL*, GB_REAL*, const GB_REAL*, const GB_REAL*, const GB_REAL*,
-                                         const uint8_t*, const uint8_t*, const uint8_t*);
+                                         const uint8_t*, const uint8_t*, const uint8_t*, bool);
 template int run_adj_sweep_w<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL, int, int, const GB_REAL*,
                                       GB_REAL*, const GB_REAL*, const GB_REAL*, const int32_t*, const uint8_t*);
 template int run_adj_vdiff<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL, GB_REAL, const GB_REAL*, GB_REAL*,

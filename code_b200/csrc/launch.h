@@ -50,11 +50,12 @@ int run_adj_heights(const Dev& d, cudaStream_t s, R dt, int sub, bool has_w, con
                     const R* vv, const R* ww, const uint8_t* mupd_u, const uint8_t* mupd_v,
                     const int32_t* az, R* H1, R* H2, R* H3, R* H4);
 // Adjoint of one horizontal sweep over nk levels (level pointers): gbar (cotangent of the sweep's
-// output) -> fbar (cotangent of its input). Dio = heights before the sweep.
+// output) -> fbar (cotangent of its input). Dio = heights before the sweep. copy0: also pass the
+// level below the pointers' origin (level 0 of the 3D field) through.
 template <class R, int DIR>
 int run_adj_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int scheme, R AH, const R* gbar,
                     R* fbar, const R* Dio, const R* U, const R* DU, const uint8_t* mflux, const uint8_t* mupd,
-                    const uint8_t* code);
+                    const uint8_t* code, bool copy0 = false);
 // Adjoint of the vertical sweep (full 3D fields); hi = heights before the sweep.
 template <class R>
 int run_adj_sweep_w(const Dev& d, cudaStream_t s, R dt, R splitfac, int scheme, int kshift, const R* gbar,

@@ -69,6 +69,8 @@ _PROTOS = {
     "getm_tracer_vdiff": [P, D, D, D, P, P, P, P, P],
     "getm_tracer_vdiff_f32": [P, F, F, F, P, P, P, P, P],
     "getm_tracer_vdiff_noalloc": [P, P, D, D, D, P, P, P, P, P],
+    "getm_set_open_boundaries": [P, P],
+    "getm_set_bdy_data": [P, P, P, P],
     "getm_tracer_step_record": [P, D, P, P, P, P, P, P, P, P, P, I, I, I, D, D, D, P, P],
     "getm_tracer_step_record_f32": [P, F, P, P, P, P, P, P, P, P, P, I, I, I, F, F, F, P, P],
     "getm_tracer_step_adjoint": [P, D, P, P, P, P, P, P, P, P, P, P, I, I, I, D, D, D, P, P],
@@ -243,6 +245,23 @@ class Context:
         fn = self.L.getm_tracer_step if _is64(f) else self.L.getm_tracer_step_f32
         self._check(fn(self.h, dt, _ptr(f), _ptr(uu), _ptr(vv), _ptr(ww), _ptr(hu), _ptr(hv), _ptr(ho), _ptr(hn),
                        _ptr(nuh), split, hscheme, vscheme, AH, cnpar, avmol, adv_ver_iterations))
+
+    # ---- open boundaries ---------------------------------------------------------------------
+    def set_open_boundaries(self, bdy):
+        """Open-boundary segments and elevation data (a code_b200.state.OpenBoundaries), used by
+        integrate_2d / integrate_3d / time_loop from now on (None: closed domain)."""
+        from .state import OpenBoundaries
+
+        b = bdy if bdy is not None else OpenBoundaries()
+        st = b.struct()
+        self._check(self.L.getm_set_open_boundaries(self.h, C.byref(st)))
+
+    def set_bdy_data(self, data, data_u=None, data_v=None):
+        """New boundary elevations (and Flather velocities) per boundary point, numpy FP64."""
+        import numpy as np
+
+        arrs = [None if a is None else np.ascontiguousarray(a, np.float64) for a in (data, data_u, data_v)]
+        self._check(self.L.getm_set_bdy_data(self.h, *[None if a is None else a.ctypes.data for a in arrs]))
 
     # ---- adjoint of the tracer step --------------------------------------------------------
     def tape(self, dtype):

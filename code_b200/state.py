@@ -35,6 +35,74 @@ DEFAULT_PD = dict(g=F32(9.81), rho_0=1025.0, kappa=F32(0.4), avmmol=F32(1.8e-6),
 P2_PDM, HALFSPLIT = 6, 2
 
 
+# 2D open-boundary types (cppdefs.h:65-68)
+ZERO_GRADIENT, SOMMERFELD, CLAMPED, FLATHER_ELEV = 1, 2, 3, 4
+
+
+class OpenBoundaries:
+    """Open-boundary segments of a domain (bdy_spec.F90) and their elevation data.
+
+    Each side is a list of (pos, first, last, type2d): western (wi, wfj, wlj), northern
+    (nj, nfi, nli), eastern (ei, efj, elj), southern (sj, sfi, sli), reference indices. The
+    boundary points are numbered in segment order W, N, E, S (bdy_map). Elevation data: either a
+    fixed `data` array per point (plus `data_u` / `data_v` for FLATHER_ELEV), or harmonic,
+    amp*sin(2*pi*loop*dtm/period + phase) per point at micro step `loop`.
+    """
+
+    def __init__(self, west=(), north=(), east=(), south=(), ramp=-1, amp=None, phase=None, period=0.0,
+                 data=None, data_u=None, data_v=None):
+        self.sides = [list(west), list(north), list(east), list(south)]
+        self.ramp = int(ramp)
+        n = self.npoints()
+        self.amp = None if amp is None else np.broadcast_to(np.asarray(amp, np.float64), (n,)).copy()
+        self.phase = (None if amp is None else
+                      np.broadcast_to(np.asarray(0.0 if phase is None else phase, np.float64), (n,)).copy())
+        self.period = float(period)
+        self.data = None if data is None else np.asarray(data, np.float64).copy()
+        self.data_u = None if data_u is None else np.asarray(data_u, np.float64).copy()
+        self.data_v = None if data_v is None else np.asarray(data_v, np.float64).copy()
+
+    def segments(self):
+        return [seg for side in self.sides for seg in side]
+
+    def npoints(self):
+        return sum(last - first + 1 for (_, first, last, _) in self.segments())
+
+    def struct(self):
+        """ctypes struct of the C layout getm_bdy (include/getm_b200.h); keeps its arrays alive."""
+        import ctypes as C
+
+        segs = self.segments()
+        self._seg = np.array([[p, f, l] for (p, f, l, _) in segs], np.int32).reshape(-1)
+        self._typ = np.array([t for (_, _, _, t) in segs], np.int32)
+        b = GetmBdy()
+        b.nwb, b.nnb, b.neb, b.nsb = (len(x) for x in self.sides)
+        b.seg = self._seg.ctypes.data if len(segs) else None
+        b.type2d = self._typ.ctypes.data if len(segs) else None
+        b.ramp = self.ramp
+        b.npoints = self.npoints()
+        for name in ("data", "data_u", "data_v", "amp", "phase"):
+            a = getattr(self, name)
+            setattr(b, name, None if a is None else a.ctypes.data)
+        b.period = self.period
+        return b
+
+
+def _bdy_struct_type():
+    import ctypes as C
+
+    class _GetmBdy(C.Structure):
+        _fields_ = [("nwb", C.c_int32), ("nnb", C.c_int32), ("neb", C.c_int32), ("nsb", C.c_int32),
+                    ("seg", C.c_void_p), ("type2d", C.c_void_p), ("ramp", C.c_int32), ("npoints", C.c_int32),
+                    ("data", C.c_void_p), ("data_u", C.c_void_p), ("data_v", C.c_void_p), ("amp", C.c_void_p),
+                    ("phase", C.c_void_p), ("period", C.c_double)]
+
+    return _GetmBdy
+
+
+GetmBdy = _bdy_struct_type()
+
+
 class BcCase:
     """A full model state (numpy arrays in the reference layout) with parameters."""
 
@@ -46,6 +114,7 @@ class BcCase:
         self.az = self.au = self.av = self.ax = None
         self.pd = {n: 0.0 for n in PD_NAMES}
         self.pi = {n: 0 for n in PI_NAMES}
+        self.bdy = None  # OpenBoundaries, or None for a closed domain
 
     def copy(self, dtype3=None):
         c = BcCase(self.grid, dtype3 or self.dtype3)
@@ -53,6 +122,7 @@ class BcCase:
         c.f3 = {k: v.astype(c.dtype3) for k, v in self.f3.items()}
         c.az, c.au, c.av, c.ax = self.az.copy(), self.au.copy(), self.av.copy(), self.ax.copy()
         c.pd, c.pi = dict(self.pd), dict(self.pi)
+        c.bdy = self.bdy
         return c
 
     def masks(self):
@@ -71,7 +141,7 @@ def _eqstate(c: BcCase):
 
 
 def baroclinic_case(nx=32, ny=24, kmax=8, recipe="shelf", dx=1000.0, M=20, dt3=60.0, seed=2, dtype3=np.float64,
-                    land=0.0, hmin=5.0, hmax=150.0, nu_max=1e-2, latitude=54.0) -> BcCase:
+                    land=0.0, hmin=5.0, hmax=150.0, nu_max=1e-2, latitude=54.0, bdy=None) -> BcCase:
     """Seeded initial state of the mode-split step, closed basin.
 
     recipe 'shelf': H = 10 + 190*0.5*(1+tanh((x-x0)/L)), L = 20 cells, x0 = nx/2.
@@ -82,13 +152,14 @@ def baroclinic_case(nx=32, ny=24, kmax=8, recipe="shelf", dx=1000.0, M=20, dt3=6
     S from 30 to 35 psu; linear EOS. Viscosity / diffusivity: static parabolic 4*nu_max*s*(1-s)
     (+1e-6) over the sigma levels. Coriolis on an f-plane at `latitude` (domain.F90:364-369 with the
     reference's single-precision omega = 2*pi/86164).
+    bdy: OpenBoundaries; its segment points become boundary points (az = 2, domain.F90:263-280).
     """
-    c, rng = _baroclinic_2d(nx, ny, kmax, recipe, dx, M, dt3, seed, dtype3, land, hmin, hmax, latitude, True)
+    c, rng = _baroclinic_2d(nx, ny, kmax, recipe, dx, M, dt3, seed, dtype3, land, hmin, hmax, latitude, True, bdy)
     _baroclinic_3d_numpy(c, rng, nu_max)
     return c
 
 
-def _baroclinic_2d(nx, ny, kmax, recipe, dx, M, dt3, seed, dtype3, land, hmin, hmax, latitude, alloc3):
+def _baroclinic_2d(nx, ny, kmax, recipe, dx, M, dt3, seed, dtype3, land, hmin, hmax, latitude, alloc3, bdy=None):
     """The 2D part of :func:`baroclinic_case` (masks, depths, elevations, parameters)."""
     g = Grid(nx, ny, kmax, dx, dx)
     rng = np.random.default_rng(seed)
@@ -124,6 +195,14 @@ def _baroclinic_2d(nx, ny, kmax, recipe, dx, M, dt3, seed, dtype3, land, hmin, h
     if recipe != "islands":
         H[:, 1] = H[:, 2]; H[:, -2] = H[:, -3]; H[1, :] = H[2, :]; H[-2, :] = H[-3, :]  # noqa: E702
         H[:, 0] = H[:, 1]; H[:, -1] = H[:, -2]; H[0, :] = H[1, :]; H[-1, :] = H[-2, :]  # noqa: E702
+    if bdy is not None:
+        def ix(i, j):
+            return j - (g.jmin - HALO), i - (g.imin - HALO)
+        for side, segs in enumerate(bdy.sides):
+            for (pos, first, last, _) in segs:
+                for q in range(first, last + 1):
+                    az[ix(pos, q) if side in (0, 2) else ix(q, pos)] = 2
+        c.bdy = bdy
     au, av, ax = derive_uvx(az)
     c.az, c.au, c.av, c.ax = az, au, av, ax
     f2 = c.f2
@@ -290,7 +369,8 @@ def oracle_struct(c: BcCase):
 
     class OrBc(C.Structure):
         _fields_ = [("f2", C.c_void_p * n2), ("f3", C.c_void_p * n3), ("az", C.c_void_p), ("au", C.c_void_p),
-                    ("av", C.c_void_p), ("ax", C.c_void_p), ("par", C.c_double * npd), ("ipar", C.c_int * npi)]
+                    ("av", C.c_void_p), ("ax", C.c_void_p), ("par", C.c_double * npd), ("ipar", C.c_int * npi),
+                    ("bdy", C.c_void_p)]
 
     s = OrBc()
     for q, nm in enumerate(F2_NAMES):
@@ -306,6 +386,9 @@ def oracle_struct(c: BcCase):
         s.par[q] = c.pd[nm]
     for q, nm in enumerate(PI_NAMES):
         s.ipar[q] = int(c.pi[nm])
+    if c.bdy is not None:
+        s._bdy = c.bdy.struct()
+        s.bdy = C.addressof(s._bdy)
     return s
 
 

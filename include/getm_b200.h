@@ -225,6 +225,33 @@ int getm_integrate_3d(getm_ctx *ctx, getm_bc_state *st, int n);
  * integrate_2d every step, integrate_3d when mod(n, M) == 0. */
 int getm_time_loop(getm_ctx *ctx, getm_bc_state *st, int n0, int count);
 
+/* ---- open boundaries ------------------------------------------------------------------ */
+/* The open-boundary description of bdy_spec.F90 (domain.F90:263-280 marks the points az = 2):
+ * segments per side, in the order western (wi, wfj, wlj), northern (nj, nfi, nli), eastern
+ * (ei, efj, elj), southern (sj, sfi, sli) -- seg holds 3 ints per segment, reference indices --
+ * with a 2D type each (ZERO_GRADIENT 1, SOMMERFELD 2, CLAMPED 3, FLATHER_ELEV 4, cppdefs.h:65-68).
+ * The nsbv = npoints boundary points are numbered in segment order (bdy_map). Elevation data
+ * (bdy_data): `data` per point, or harmonic amp[p]*sin(2*pi*loop*dtm/period + phase[p]) at micro
+ * step `loop` when amp != NULL; data_u / data_v = bdy_data_u / bdy_data_v of FLATHER_ELEV (NULL =
+ * zero). All pointers are HOST arrays, copied by getm_set_open_boundaries. With boundaries set,
+ * getm_integrate_2d / getm_integrate_3d / getm_time_loop apply update_2d_bdy (m2d.F90:475) and
+ * the mirror_bdy_2d / mirror_bdy_3d copies of momentum.F90:190,353, uu_momentum_3d.F90:389,
+ * vv_momentum_3d.F90:400 and m3d.F90:595,602. Call after getm_init_advection (the masks select
+ * the mirrored points). */
+typedef struct {
+  int32_t nwb, nnb, neb, nsb;
+  const int32_t *seg;
+  const int32_t *type2d;
+  int32_t ramp;    /* bdy2d_ramp (<= 1: no ramp) */
+  int32_t npoints; /* nsbv */
+  const double *data, *data_u, *data_v, *amp, *phase;
+  double period;
+} getm_bdy;
+int getm_set_open_boundaries(getm_ctx *ctx, const getm_bdy *bdy);
+/* New boundary data for the following steps (get_2d_bdy's job in the reference): HOST arrays of
+ * npoints values each (data_u / data_v may be NULL); switches off harmonic data. */
+int getm_set_bdy_data(getm_ctx *ctx, const double *data, const double *data_u, const double *data_v);
+
 /* ---- adjoint of the tracer step ---------------------------------------------------------- */
 /* No counterpart in the reference. The tracer step of getm_tracer_step (HALFSPLIT advection,
  * split schemes, adv_ver_iterations = 1, then implicit vertical diffusion) is differentiated in

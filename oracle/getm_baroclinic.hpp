@@ -38,6 +38,24 @@ enum PI {
   I_CALC_SALT, NPI
 };
 
+// Open boundaries (domain.F90:263-280, bdy_spec.F90:225-290): segments per side -- western
+// (wi, wfj..wlj), northern (nj, nfi..nli), eastern (ei, efj..elj), southern (sj, sfi..sli) -- with
+// a 2D type each (cppdefs.h:65-69), and the elevation data of the boundary points in segment
+// order (bdy_data; bdy_data_u/v for FLATHER_ELEV). With harmonic data the elevation of point p at
+// micro step `loop` is amp[p]*sin(2*pi*loop*dtm/period + phase[p]) (the configurations' tide;
+// the reference reads its boundary data from files).
+enum { ZERO_GRADIENT = 1, SOMMERFELD = 2, CLAMPED = 3, FLATHER_ELEV = 4 };
+struct Bdy {
+  int nwb = 0, nnb = 0, neb = 0, nsb = 0;
+  std::vector<int> seg;     // 3 ints per segment, sides in the order W, N, E, S
+  std::vector<int> type2d;  // per segment
+  int ramp = -1;            // bdy2d_ramp
+  std::vector<double> data, data_u, data_v;  // per boundary point (used when amp is empty)
+  std::vector<double> amp, phase;            // harmonic elevation per boundary point
+  double period = 0.0;
+  int nseg() const { return nwb + nnb + neb + nsb; }
+};
+
 template <class R3>
 struct BcState {
   double* f2[NF2];
@@ -45,6 +63,7 @@ struct BcState {
   const int32_t *az, *au, *av, *ax;
   double par[NPD];
   int ipar[NPI];
+  const Bdy* bdy = nullptr;  // open boundaries (nullptr: closed domain)
 };
 
 // ---------------------------------------------------------------------------------------------
@@ -178,8 +197,138 @@ inline int uv_advect_2d(const Dom& d, const AdvMasks& m, const int32_t* az, cons
   return 0;
 }
 
+// update_2d_bdy.F90:74-178 -- elevations of the open-boundary points (after the Uint accumulation,
+// before sealevel, m2d.F90:475).
+inline void update_2d_bdy(const Dom& d, const Bdy& b, double** f2, const double* par, int loop) {
+  A2 z{d, f2[Z]}, D{d, f2[D_]}, U{d, f2[U_]}, DU_{d, f2[DU]}, V{d, f2[V_]}, DV_{d, f2[DV]}, H{d, f2[HH]};
+  const double dtm = par[P_DTM], min_depth = par[P_MIN_DEPTH];
+  const double g = (double)9.81f;  // the single-precision literal of update_2d_bdy.F90:92,96
+  double fac = 1.0;
+  if (b.ramp > 1) fac = std::min(1.0, 4.0 * loop / (double)(float)b.ramp);
+  auto data = [&](int k, int which) -> double {  // k: 1-based point index
+    if (which == 0) {
+      if (!b.amp.empty()) {
+        const double pi2 = 2.0 * 3.14159265358979323846;
+        return b.amp[k - 1] * std::sin(pi2 * (loop * dtm) / b.period + b.phase[k - 1]);
+      }
+      return b.data[k - 1];
+    }
+    const std::vector<double>& v = which == 1 ? b.data_u : b.data_v;
+    return v.empty() ? 0.0 : v[k - 1];
+  };
+  int l = 0, k = 1;
+  for (int n = 0; n < b.nwb; ++n, ++l) {
+    const int i = b.seg[3 * l], jf = b.seg[3 * l + 1], jl = b.seg[3 * l + 2];
+    for (int j = jf; j <= jl; ++j, ++k) switch (b.type2d[l]) {
+        case ZERO_GRADIENT: z(i, j) = z(i + 1, j); break;
+        case SOMMERFELD: z(i, j) = z(i, j) + dtm / d.dx * std::sqrt(g * D(i, j)) * (z(i + 1, j) - z(i, j)); break;
+        case CLAMPED: z(i, j) = std::max(fac * data(k, 0), -H(i, j) + min_depth); break;
+        case FLATHER_ELEV: {
+          const double a = std::sqrt(DU_(i, j) / g) * (U(i, j) / DU_(i, j) - data(k, 1));
+          z(i, j) = std::max(fac * (data(k, 0) - a), -H(i, j) + min_depth);
+        } break;
+      }
+  }
+  for (int n = 0; n < b.nnb; ++n, ++l) {
+    const int j = b.seg[3 * l], if_ = b.seg[3 * l + 1], il = b.seg[3 * l + 2];
+    for (int i = if_; i <= il; ++i, ++k) switch (b.type2d[l]) {
+        case ZERO_GRADIENT: z(i, j) = z(i, j - 1); break;
+        case SOMMERFELD: z(i, j) = z(i, j) - dtm / d.dy * std::sqrt(g * D(i, j)) * (z(i, j) - z(i, j - 1)); break;
+        case CLAMPED: z(i, j) = std::max(fac * data(k, 0), -H(i, j) + min_depth); break;
+        case FLATHER_ELEV: {
+          const double a = std::sqrt(DV_(i, j) / g) * (V(i, j - 1) / DV_(i, j - 1) - data(k, 2));
+          z(i, j) = std::max(fac * (data(k, 0) + a), -H(i, j) + min_depth);
+        } break;
+      }
+  }
+  for (int n = 0; n < b.neb; ++n, ++l) {
+    const int i = b.seg[3 * l], jf = b.seg[3 * l + 1], jl = b.seg[3 * l + 2];
+    for (int j = jf; j <= jl; ++j, ++k) switch (b.type2d[l]) {
+        case ZERO_GRADIENT: z(i, j) = z(i - 1, j); break;
+        case SOMMERFELD: z(i, j) = z(i, j) - dtm / d.dx * std::sqrt(g * D(i, j)) * (z(i, j) - z(i - 1, j)); break;
+        case CLAMPED: z(i, j) = std::max(fac * data(k, 0), -H(i, j) + min_depth); break;
+        case FLATHER_ELEV: {
+          const double a = std::sqrt(DU_(i, j) / g) * (U(i - 1, j) / DU_(i - 1, j) - data(k, 1));
+          z(i, j) = std::max(fac * (data(k, 0) + a), -H(i, j) + min_depth);
+        } break;
+      }
+  }
+  for (int n = 0; n < b.nsb; ++n, ++l) {
+    const int j = b.seg[3 * l], if_ = b.seg[3 * l + 1], il = b.seg[3 * l + 2];
+    for (int i = if_; i <= il; ++i, ++k) switch (b.type2d[l]) {
+        case ZERO_GRADIENT: z(i, j) = z(i, j + 1); break;
+        case SOMMERFELD: z(i, j) = z(i, j) + dtm / d.dy * std::sqrt(g * D(i, j)) * (z(i, j + 1) - z(i, j)); break;
+        case CLAMPED: z(i, j) = std::max(fac * data(k, 0), -H(i, j) + min_depth); break;
+        case FLATHER_ELEV: {
+          const double a = std::sqrt(DV_(i, j) / g) * (V(i, j) / DV_(i, j) - data(k, 2));
+          z(i, j) = std::max(fac * (data(k, 0) - a), -H(i, j) + min_depth);
+        } break;
+      }
+  }
+}
+
+// mirror_bdy_2d.F90 / mirror_bdy_3d.F90: copies across the open boundaries. tag 0 = U_TAG (U points
+// with au == 3 on northern/southern boundaries), 1 = V_TAG (av == 3 on western/eastern ones),
+// 2 = H/D_TAG (the value of a boundary point, az > 1, into the point outside). nl levels of a
+// field with level stride sk (nl = 1 for 2D fields).
+template <class R>
+inline void mirror_bdy(const Dom& d, const Bdy& b, const int32_t* azp, const int32_t* aup, const int32_t* avp,
+                       R* f, int tag, int nl, long sk) {
+  M2 az{d, azp}, au{d, aup}, av{d, avp};
+  auto cp = [&](int id, int jd, int is, int js) {
+    for (int k = 0; k < nl; ++k) f[d.ix(id, jd) + k * sk] = f[d.ix(is, js) + k * sk];
+  };
+  const int W = 0, N = b.nwb, E = N + b.nnb, S = E + b.neb;
+  auto sg = [&](int l, int q) { return b.seg[3 * l + q]; };
+  if (tag == 0) {
+    for (int n = 0; n < b.nnb; ++n) {
+      const int j = sg(N + n, 0);
+      for (int i = sg(N + n, 1) - HALO; i <= sg(N + n, 2) + HALO; ++i)
+        if (au(i, j) == 3) cp(i, j, i, j - 1);
+    }
+    for (int n = 0; n < b.nsb; ++n) {
+      const int j = sg(S + n, 0);
+      for (int i = sg(S + n, 1) - HALO; i <= sg(S + n, 2) + HALO; ++i)
+        if (au(i, j) == 3) cp(i, j, i, j + 1);
+    }
+  } else if (tag == 1) {
+    for (int n = 0; n < b.nwb; ++n) {
+      const int i = sg(W + n, 0);
+      for (int j = sg(W + n, 1) - HALO; j <= sg(W + n, 2) + HALO; ++j)
+        if (av(i, j) == 3) cp(i, j, i + 1, j);
+    }
+    for (int n = 0; n < b.neb; ++n) {
+      const int i = sg(E + n, 0);
+      for (int j = sg(E + n, 1) - HALO; j <= sg(E + n, 2) + HALO; ++j)
+        if (av(i, j) == 3) cp(i, j, i - 1, j);
+    }
+  } else {
+    for (int n = 0; n < b.nwb; ++n) {
+      const int i = sg(W + n, 0);
+      for (int j = sg(W + n, 1) - HALO; j <= sg(W + n, 2) + HALO; ++j)
+        if (az(i, j) > 1) cp(i - 1, j, i, j);
+    }
+    for (int n = 0; n < b.nnb; ++n) {
+      const int j = sg(N + n, 0);
+      for (int i = sg(N + n, 1) - HALO; i <= sg(N + n, 2) + HALO; ++i)
+        if (az(i, j) > 1) cp(i, j + 1, i, j);
+    }
+    for (int n = 0; n < b.neb; ++n) {
+      const int i = sg(E + n, 0);
+      for (int j = sg(E + n, 1) - HALO; j <= sg(E + n, 2) + HALO; ++j)
+        if (az(i, j) > 1) cp(i + 1, j, i, j);
+    }
+    for (int n = 0; n < b.nsb; ++n) {
+      const int j = sg(S + n, 0);
+      for (int i = sg(S + n, 1) - HALO; i <= sg(S + n, 2) + HALO; ++i)
+        if (az(i, j) > 1) cp(i, j - 1, i, j);
+    }
+  }
+}
+
 // momentum.F90:69-223 umomentum, :232-386 vmomentum (CARTESIAN, no NEW_CORI).
-inline void umomentum(const Dom& d, double** f2, const int32_t* aup, const int32_t* avp, const double* par) {
+inline void umomentum(const Dom& d, double** f2, const int32_t* aup, const int32_t* avp, const double* par,
+                      const Bdy* bdy = nullptr, const int32_t* azp = nullptr) {
   A2 U{d, f2[U_]}, DU_{d, f2[DU]}, z{d, f2[Z]}, H{d, f2[HH]}, D{d, f2[D_]}, airp{d, f2[AIRP]}, tausx{d, f2[TAUSX]},
       Slru{d, f2[SLRU]}, dry_u{d, f2[DRY_U]}, fV{d, f2[FV]}, UEx{d, f2[UEX]}, SlUx{d, f2[SLUX]}, ru{d, f2[RU]},
       fU{d, f2[FU]}, corv{d, f2[CORV]};
@@ -199,6 +348,7 @@ inline void umomentum(const Dom& d, double** f2, const int32_t* aup, const int32
                                     dry_u(i, j) * (-tausu / rho_0 - fV(i, j) + UEx(i, j) + SlUx(i, j) + Slr))) /
                   (1.0 + dtm * ru(i, j) / DU_(i, j));
       }
+  if (bdy) mirror_bdy<double>(d, *bdy, azp, aup, avp, f2[U_], 0, 1, 0);  // momentum.F90:190
   for (int j = d.jmin; j <= d.jmax; ++j)
     for (int i = d.imin; i <= d.imax; ++i) {
       if (av(i, j) >= 1) {
@@ -210,7 +360,8 @@ inline void umomentum(const Dom& d, double** f2, const int32_t* aup, const int32
     }
 }
 
-inline void vmomentum(const Dom& d, double** f2, const int32_t* aup, const int32_t* avp, const double* par) {
+inline void vmomentum(const Dom& d, double** f2, const int32_t* aup, const int32_t* avp, const double* par,
+                      const Bdy* bdy = nullptr, const int32_t* azp = nullptr) {
   A2 V{d, f2[V_]}, DV_{d, f2[DV]}, z{d, f2[Z]}, H{d, f2[HH]}, D{d, f2[D_]}, airp{d, f2[AIRP]}, tausy{d, f2[TAUSY]},
       Slrv{d, f2[SLRV]}, dry_v{d, f2[DRY_V]}, fU{d, f2[FU]}, VEx{d, f2[VEX]}, SlVx{d, f2[SLVX]}, rv{d, f2[RV]},
       fV{d, f2[FV]}, coru{d, f2[CORU]};
@@ -230,6 +381,7 @@ inline void vmomentum(const Dom& d, double** f2, const int32_t* aup, const int32
                                     dry_v(i, j) * (-tausv / rho_0 + fU(i, j) + VEx(i, j) + SlVx(i, j) + Slr))) /
                   (1.0 + dtm * rv(i, j) / DV_(i, j));
       }
+  if (bdy) mirror_bdy<double>(d, *bdy, azp, aup, avp, f2[V_], 1, 1, 0);  // momentum.F90:353
   for (int j = d.jmin; j <= d.jmax; ++j)
     for (int i = d.imin; i <= d.imax; ++i) {
       if (au(i, j) >= 1) {
@@ -296,12 +448,12 @@ int integrate_2d(const Dom& d, const AdvMasks& m, BcState<R3>& st, int loop) {
     return -1;
   // momentum.F90:44-52: SAVEd toggle ufirst (initially .false.)
   if (ip[I_UFIRST2D]) {
-    umomentum(d, f2, st.au, st.av, par);
-    vmomentum(d, f2, st.au, st.av, par);
+    umomentum(d, f2, st.au, st.av, par, st.bdy, st.az);
+    vmomentum(d, f2, st.au, st.av, par, st.bdy, st.az);
     ip[I_UFIRST2D] = 0;
   } else {
-    vmomentum(d, f2, st.au, st.av, par);
-    umomentum(d, f2, st.au, st.av, par);
+    vmomentum(d, f2, st.au, st.av, par, st.bdy, st.az);
+    umomentum(d, f2, st.au, st.av, par, st.bdy, st.az);
     ip[I_UFIRST2D] = 1;
   }
   if (ip[I_RUNTYPE] > 1) {
@@ -311,6 +463,7 @@ int integrate_2d(const Dom& d, const AdvMasks& m, BcState<R3>& st, int loop) {
       f2[VINT][q] = f2[VINT][q] + f2[V_][q];
     }
   }
+  if (st.bdy && st.bdy->nseg() > 0) update_2d_bdy(d, *st.bdy, f2, par, loop);  // m2d.F90:475
   sealevel(d, f2, st.az, par);
   depth_update(d, f2, st.az, st.au, st.av, par);
   return 0;
@@ -550,6 +703,8 @@ void uv_momentum_3d(const Dom& d, BcState<R3>& st, int dir) {
       }
     }
   }
+  // uu_momentum_3d.F90:389 / vv_momentum_3d.F90:400
+  if (st.bdy) mirror_bdy<R3>(d, *st.bdy, st.az, st.au, st.av, st.f3[dir == 0 ? UU : VV], dir, kmax + 1, d.sk);
 }
 
 // sigma_coordinates.F90:85-113 (equidistant), all levels 0..kmax
@@ -845,6 +1000,10 @@ int integrate_3d(const Dom& d, const AdvMasks& m, BcState<R3>& st, int n) {
                               R3(par[P_SALT_AH]), H_TAG, nullptr, nullptr, ip[I_ADV_VER_ITERS]) < 0)
         return -1;
       tracer_vdiff<R3>(d, dt, R3(par[P_CNPAR]), R3(par[P_AVMOLS]), st.f3[SS], st.f3[HN], st.f3[NUH], st.az, nullptr);
+    }
+    if (st.bdy) {  // m3d.F90:595,602
+      if (ip[I_CALC_TEMP]) mirror_bdy<R3>(d, *st.bdy, st.az, st.au, st.av, st.f3[TT], 2, d.kmax + 1, d.sk);
+      if (ip[I_CALC_SALT]) mirror_bdy<R3>(d, *st.bdy, st.az, st.au, st.av, st.f3[SS], 2, d.kmax + 1, d.sk);
     }
     do_eqstate(d, st);
   }

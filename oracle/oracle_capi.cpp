@@ -158,12 +158,23 @@ long long or_tracer_steps_tl(const or_dom* o, const int32_t* az, const int32_t* 
 }
 
 // ---- mode-split time loop (getm_baroclinic.hpp) -------------------------------------------------
+// Open boundaries: the layout of getm_bdy in include/getm_b200.h.
+typedef struct {
+  int32_t nwb, nnb, neb, nsb;
+  const int32_t* seg;
+  const int32_t* type2d;
+  int32_t ramp, npoints;
+  const double *data, *data_u, *data_v, *amp, *phase;
+  double period;
+} or_bdy;
+
 typedef struct {
   double* f2[gor::NF2];
   void* f3[gor::NF3];
   const int32_t *az, *au, *av, *ax;
   double par[gor::NPD];
   int ipar[gor::NPI];
+  const or_bdy* bdy;  // NULL: closed domain
 } or_bc;
 
 int or_bc_sizes(int* out) {
@@ -175,9 +186,26 @@ int or_bc_sizes(int* out) {
 }
 
 extern "C++" {
+static gor::Bdy to_bdy(const or_bdy* b) {
+  gor::Bdy o;
+  o.nwb = b->nwb; o.nnb = b->nnb; o.neb = b->neb; o.nsb = b->nsb;
+  const int ns = o.nseg(), np = b->npoints;
+  o.seg.assign(b->seg, b->seg + 3 * ns);
+  o.type2d.assign(b->type2d, b->type2d + ns);
+  o.ramp = b->ramp;
+  auto cp = [&](const double* p, std::vector<double>& v) { if (p) v.assign(p, p + np); };
+  cp(b->data, o.data); cp(b->data_u, o.data_u); cp(b->data_v, o.data_v); cp(b->amp, o.amp); cp(b->phase, o.phase);
+  o.period = b->period;
+  return o;
+}
+
 template <class R3>
-static gor::BcState<R3> to_state(or_bc* s) {
+static gor::BcState<R3> to_state(or_bc* s, gor::Bdy* bdy) {
   gor::BcState<R3> st;
+  if (s->bdy) {
+    *bdy = to_bdy(s->bdy);
+    st.bdy = bdy;
+  }
   for (int q = 0; q < gor::NF2; ++q) st.f2[q] = s->f2[q];
   for (int q = 0; q < gor::NF3; ++q) st.f3[q] = (R3*)s->f3[q];
   st.az = s->az; st.au = s->au; st.av = s->av; st.ax = s->ax;
@@ -195,7 +223,8 @@ static long long bc_steps(const or_dom* o, or_bc* s, int n0, int count) {
   gor::Dom d = mk(o);
   gor::AdvMasks m;
   gor::build_adv_masks(d, s->az, s->au, s->av, s->ax, m);
-  gor::BcState<R3> st = to_state<R3>(s);
+  gor::Bdy bdy;
+  gor::BcState<R3> st = to_state<R3>(s, &bdy);
   for (int n = n0; n < n0 + count; ++n) {
     if (gor::integrate_2d(d, m, st, n) != 0) return -1;
     if (n % st.ipar[gor::I_M] == 0)
@@ -223,7 +252,8 @@ static int bc_call(const or_dom* o, or_bc* s, int which, int arg) {
   gor::Dom d = mk(o);
   gor::AdvMasks m;
   gor::build_adv_masks(d, s->az, s->au, s->av, s->ax, m);
-  gor::BcState<R3> st = to_state<R3>(s);
+  gor::Bdy bdy;
+  gor::BcState<R3> st = to_state<R3>(s, &bdy);
   int rc = 0;
   switch (which) {
     case BC_BOTTOM_FRICTION: gor::bottom_friction(d, nullptr, st.f2, st.au, st.av, st.par, st.ipar[gor::I_RUNTYPE]); break;

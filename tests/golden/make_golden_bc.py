@@ -3,13 +3,15 @@
 small closed basin, together with the inputs. The oracle and the CUDA path are compared with it
 bit for bit (tests/test_golden_bc_cpu.py) and the CUDA path within 1e-12 (tests/test_gpu_baroclinic.py).
 
-    python tests/golden/make_golden_bc.py
+    python tests/golden/make_golden_bc.py [closed] [bdy]
 
 Configuration: runtype 4 (prognostic T and S), sigma coordinates (equidistant), linear equation of
 state, Blumberg-Mellor internal pressure, P2_PDM / HALFSPLIT advection of momentum (2D and 3D) and
 tracers, closed boundaries, num/nuh prescribed (the turbulence closure -- the un-vendored GOTM -- is
 replaced by a routine that leaves them unchanged; ss_nn, whose outputs only feed it, likewise),
-no wind, air pressure, freshwater or short-wave forcing.
+no wind, air pressure, freshwater or short-wave forcing. The second fixture,
+reference_mode_split_bdy.npz, adds open boundaries of all four 2D types (update_2d_bdy.F90,
+mirror_bdy_2d.F90, mirror_bdy_3d.F90); see bdy_case().
 """
 from __future__ import annotations
 
@@ -37,7 +39,7 @@ FILES = [
     "src/3d/vv_momentum_3d.F90", "src/3d/coordinates.F90", "src/3d/sigma_coordinates.F90",
     "src/3d/ww_momentum_3d.F90", "src/3d/uv_advect_3d.F90", "src/3d/uv_diffusion_3d.F90", "src/3d/stresses_3d.F90",
     "src/3d/temperature.F90", "src/3d/salinity.F90", "src/3d/eqstate.F90", "src/3d/slow_bottom_friction.F90",
-    "src/3d/slow_terms.F90", "src/2d/m2d.F90", "src/3d/m3d.F90",
+    "src/3d/slow_terms.F90", "src/2d/m2d.F90", "src/3d/m3d.F90", "src/2d/update_2d_bdy.F90",
 ]
 
 
@@ -60,9 +62,9 @@ class RefBc:
             dy=g.dy, ard1=g.ard1, az=F2(c.az), au=F2(c.au), av=F2(c.av), ax=F2(c.ax), h=f2["h"], hu=f2["hu"],
             hv=f2["hv"], min_depth=pd["min_depth"], crit_depth=pd["crit_depth"], dry_z=f2["dry_z"],
             dry_u=f2["dry_u"], dry_v=f2["dry_v"], cori=zero2(), coru=f2["coru"], corv=f2["corv"],
-            ga=None, ddu=np.float64(0.0), ddl=np.float64(0.0), vert_cord=1, openbdy=False, have_boundaries=False,
-            nwb=0, nnb=0, neb=0, nsb=0, maxdepth=np.float64(0.0), z0_method=0, z0_const=np.float64(0.01), z0=zero2(),
-            ill=g.imin, ihl=g.imax, jll=g.jmin, jhl=g.jmax, ilg=g.imin, ihg=g.imax, jlg=g.jmin, jhg=g.jmax)
+            ga=None, ddu=np.float64(0.0), ddl=np.float64(0.0), vert_cord=1, maxdepth=np.float64(0.0), z0_method=0,
+            z0_const=np.float64(0.01), z0=zero2(), ill=g.imin, ihl=g.imax, jll=g.jmin, jhl=g.jmax, ilg=g.imin,
+            ihg=g.imax, jlg=g.jmin, jhg=g.jmax, **self._bdy_domain(c.bdy))
         v2 = {k: f2[k] for k in ("z", "zo", "u", "v", "d", "du", "dv", "uex", "vex", "fu", "fv", "ru", "rv", "ruu",
                                  "rvv", "uint", "vint", "uinto", "vinto", "slux", "slvx", "slru", "slrv", "zub",
                                  "zvb", "zub0", "zvb0", "fwf")}
@@ -109,13 +111,21 @@ class RefBc:
         P.procs["ss_nn"] = lambda *a, **k: None
         P.procs["tke_eps_advect_3d"] = lambda *a, **k: None
         P.procs["do_residual"] = lambda *a, **k: None
-        P.procs["update_2d_bdy"] = lambda *a, **k: None
+        if c.bdy is None:
+            P.procs["update_2d_bdy"] = lambda *a, **k: None
         P.procs["check_3d_fields"] = lambda *a, **k: None
         m2 = P.modules["m2d"]
         m2.dtm = np.float64(pd["dtm"])
         m2.mm = pi["MM"]
         m2.vel2d_adv_split, m2.vel2d_adv_hor = pi["vel2d_adv_split"], pi["vel2d_adv_hor"]
         m2.am, m2.an_method, m2.residual, m2.sealevel_check, m2.bdy2d_ramp = np.float64(-1.0), 0, -1, 0, -1
+        if c.bdy is not None:
+            b, n = c.bdy, c.bdy.npoints()
+            m2.bdy2d_ramp = b.ramp
+            m2.bdyfmt_2d = 2  # NETCDF (cppdefs.h:88): data placed in bdy_data before each micro step
+            m2.bdy_data = fs.FArr(np.zeros(n), [1])
+            m2.bdy_data_u = fs.FArr(np.zeros(n) if b.data_u is None else b.data_u.copy(), [1])
+            m2.bdy_data_v = fs.FArr(np.zeros(n) if b.data_v is None else b.data_v.copy(), [1])
         m3 = P.modules["m3d"]
         m3.m = pi["M"]
         m3.vel3d_adv_split, m3.vel3d_adv_hor, m3.vel3d_adv_ver = (pi["vel3d_adv_split"], pi["vel3d_adv_hor"],
@@ -142,6 +152,28 @@ class RefBc:
         # sigma coordinates' first call sets the SAVEd equidistant switch and ga (coordinates.F90)
         P.procs["sigma_coordinates"](True)
 
+    @staticmethod
+    def _bdy_domain(b):
+        """The domain module's boundary description (bdy_spec.F90:225-290) for an OpenBoundaries."""
+        if b is None:
+            return dict(openbdy=False, have_boundaries=False, nwb=0, nnb=0, neb=0, nsb=0)
+        out = dict(openbdy=True, have_boundaries=True, nsbv=b.npoints())
+        names = (("nwb", "wi", "wfj", "wlj"), ("nnb", "nj", "nfi", "nli"), ("neb", "ei", "efj", "elj"),
+                 ("nsb", "sj", "sfi", "sli"))
+        index, types, k = [], [], 1
+        for side, (cnt, a, f, l) in zip(b.sides, names):
+            out[cnt] = len(side)
+            out[a] = fs.FArr(np.array([x[0] for x in side] or [0], np.int64), [1])
+            out[f] = fs.FArr(np.array([x[1] for x in side] or [0], np.int64), [1])
+            out[l] = fs.FArr(np.array([x[2] for x in side] or [0], np.int64), [1])
+            for (_, first, last, typ) in side:
+                index.append(k)
+                types.append(typ)
+                k += last - first + 1
+        out["bdy_index"] = fs.FArr(np.array(index, np.int64), [1])
+        out["bdy_2d_type"] = fs.FArr(np.array(types, np.int64), [1])
+        return out
+
     def _error(self, where, msg):
         raise fs.FortranStop(f"{where}: {msg}")
 
@@ -164,7 +196,13 @@ class RefBc:
         m2 = self.P.modules["m2d"]
         m3 = self.P.modules["m3d"]
         zeros = self.F2(np.zeros(self.g.shape2()))
+        b = self.c.bdy
         for n in range(n0, n0 + count):
+            if b is not None:  # the harness's boundary data of micro step n (the reference reads files)
+                if b.amp is not None:
+                    m2.bdy_data.a[:] = b.amp * np.sin(2.0 * np.pi * (n * m2.dtm) / b.period + b.phase)
+                else:
+                    m2.bdy_data.a[:] = b.data
             m2.integrate_2d(runtype, n, self.f2["tausx"], self.f2["tausy"], self.f2["airp"])
             if n % m3.m == 0:
                 m3.integrate_3d(runtype, n)
@@ -179,8 +217,22 @@ class RefBc:
         return out
 
 
-def main():
-    c = S.baroclinic_case(nx=12, ny=10, kmax=4, recipe="shelf", M=4, dt3=60.0, seed=3)
+def bdy_case():
+    """12 x 10 x 4 shelf with a segment of each 2D boundary type on each side: CLAMPED (west),
+    ZERO_GRADIENT (north), SOMMERFELD (east), FLATHER_ELEV (south); harmonic elevations (amplitude
+    0.3 m, period 120 s = 8 micro steps, phase varying along the boundary), a ramp over 16 micro
+    steps, and a constant bdy_data_v for the Flather segment."""
+    g = S.Grid(12, 10, 4, 1000.0, 1000.0)
+    b = S.OpenBoundaries(west=[(g.imin, g.jmin + 2, g.jmax - 2, S.CLAMPED)],
+                         north=[(g.jmax, g.imin + 3, g.imax - 3, S.ZERO_GRADIENT)],
+                         east=[(g.imax, g.jmin + 2, g.jmax - 2, S.SOMMERFELD)],
+                         south=[(g.jmin, g.imin + 3, g.imax - 3, S.FLATHER_ELEV)], ramp=16, amp=0.3, period=120.0)
+    b.phase = 0.1 * np.arange(b.npoints())
+    b.data_v = np.full(b.npoints(), 0.02)
+    return S.baroclinic_case(nx=12, ny=10, kmax=4, recipe="shelf", M=4, dt3=60.0, seed=3, bdy=b)
+
+
+def write(c, name):
     out = {"meta": np.array([c.grid.nx, c.grid.ny, c.grid.kmax, c.grid.dx, c.grid.dy])}
     for k, v in c.f2.items():
         out["in_f2_" + k] = v
@@ -190,14 +242,30 @@ def main():
         out["in_" + k] = v
     out["in_pd"] = np.array([c.pd[n] for n in S.PD_NAMES])
     out["in_pi"] = np.array([c.pi[n] for n in S.PI_NAMES])
+    if c.bdy is not None:
+        b = c.bdy
+        out["bdy_counts"] = np.array([len(x) for x in b.sides])
+        out["bdy_seg"] = np.array([[p_, f, l, t] for (p_, f, l, t) in b.segments()])
+        out["bdy_ramp"] = np.array(b.ramp)
+        out["bdy_amp"], out["bdy_phase"], out["bdy_period"] = b.amp, b.phase, np.array(b.period)
+        out["bdy_data_v"] = b.data_v
     r = RefBc(c)
     # two macro steps (M = 4 micro steps each)
     r.time_loop(1, 8)
     for k, v in r.state().items():
         out["out_" + k] = v
-    path = os.path.join(HERE, "reference_mode_split.npz")
+    path = os.path.join(HERE, name)
     np.savez_compressed(path, **out)
     print(f"wrote {path} ({os.path.getsize(path) / 1024:.0f} KiB)")
+
+
+def main():
+    which = sys.argv[1:] or ["closed", "bdy"]
+    if "closed" in which:
+        write(S.baroclinic_case(nx=12, ny=10, kmax=4, recipe="shelf", M=4, dt3=60.0, seed=3),
+              "reference_mode_split.npz")
+    if "bdy" in which:
+        write(bdy_case(), "reference_mode_split_bdy.npz")
 
 
 if __name__ == "__main__":

@@ -1,7 +1,8 @@
 """The oracle's mode-split time loop against the reference's own integrate_2d / integrate_3d
 (tests/golden/reference_mode_split.npz, made by tests/golden/make_golden_bc.py from the
 reference's Fortran source): every 2D and 3D field of the state, bit for bit, after two macro
-steps of four micro steps."""
+steps of four micro steps -- a closed basin, and (reference_mode_split_bdy.npz) a basin with open
+boundaries of all four 2D types (update_2d_bdy, mirror_bdy_2d/3d)."""
 import os
 
 import numpy as np
@@ -12,6 +13,7 @@ from code_b200 import state as S
 from code_b200.grid import Grid
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_mode_split.npz")
+GOLD_BDY = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_mode_split_bdy.npz")
 
 
 def load_case(gold, dtype3=np.float64):
@@ -24,12 +26,20 @@ def load_case(gold, dtype3=np.float64):
     c.az, c.au, c.av, c.ax = (gold["in_" + k].copy() for k in ("az", "au", "av", "ax"))
     c.pd = dict(zip(S.PD_NAMES, (float(x) for x in gold["in_pd"])))
     c.pi = dict(zip(S.PI_NAMES, (int(x) for x in gold["in_pi"])))
+    if "bdy_counts" in gold:
+        sides, q = [], 0
+        for n in gold["bdy_counts"]:
+            sides.append([tuple(int(x) for x in row) for row in gold["bdy_seg"][q:q + int(n)]])
+            q += int(n)
+        b = S.OpenBoundaries(*sides, ramp=int(gold["bdy_ramp"]), amp=gold["bdy_amp"], phase=gold["bdy_phase"],
+                             period=float(gold["bdy_period"]), data_v=gold["bdy_data_v"])
+        c.bdy = b
     return c
 
 
-@pytest.fixture(scope="module")
-def gold():
-    return dict(np.load(GOLD))
+@pytest.fixture(scope="module", params=["closed", "open boundaries"])
+def gold(request):
+    return dict(np.load(GOLD if request.param == "closed" else GOLD_BDY))
 
 
 # fields the configuration never writes or reads (kept for the layout) are still compared

@@ -14,7 +14,7 @@ import oracle
 from code_b200 import state as S
 from code_b200.getm import BcDevice
 from helpers import make_ctx
-from test_golden_bc_cpu import GOLD, load_case
+from test_golden_bc_cpu import GOLD, GOLD_BDY, load_case
 
 pytestmark = pytest.mark.gpu
 
@@ -40,6 +40,8 @@ def run_gpu(c, n0, count, dtype3=None):
     import torch
 
     ctx, _ = make_ctx(c)
+    if c.bdy is not None:
+        ctx.set_open_boundaries(c.bdy)
     st = BcDevice(c, dtype3=dtype3)
     ctx.time_loop(st, n0, count)
     torch.cuda.synchronize()
@@ -48,8 +50,9 @@ def run_gpu(c, n0, count, dtype3=None):
     return out, ctx
 
 
-def test_time_loop_vs_reference_fixture():
-    gold = dict(np.load(GOLD))
+@pytest.mark.parametrize("path", [GOLD, GOLD_BDY], ids=["closed", "open boundaries"])
+def test_time_loop_vs_reference_fixture(path):
+    gold = dict(np.load(path))
     c = load_case(gold)
     out, _ = run_gpu(c, 1, 8)
     bad, worst = compare(out, {k: gold["out_f2_" + k] for k in S.F2_NAMES},
@@ -67,6 +70,44 @@ def test_time_loop_vs_oracle(recipe, nx, ny, kmax):
     bad, worst = compare(out, ref.f2, ref.f3, 1e-12)
     assert not bad, bad
     assert ctx.take_warnings() == 0
+
+
+def tidal_shelf(nx=40, ny=28, kmax=10, M=5, period=900.0, seed=11):
+    """The shelf configuration with its western side open and clamped to a tide (1 m amplitude;
+    the period is shortened from M2 so that the test sees a full cycle), ramped over 40 micro
+    steps."""
+    g = S.Grid(nx, ny, kmax, 1000.0, 1000.0)
+    b = S.OpenBoundaries(west=[(g.imin, g.jmin, g.jmax, S.CLAMPED)], ramp=40, amp=1.0, period=period)
+    return S.baroclinic_case(nx=nx, ny=ny, kmax=kmax, recipe="shelf", M=M, dt3=60.0, seed=seed, bdy=b)
+
+
+def test_open_boundary_tide_vs_oracle():
+    c = tidal_shelf()
+    ref = c.copy()
+    oracle.bc_steps(ref, 1, 30)
+    out, ctx = run_gpu(c, 1, 30)
+    bad, worst = compare(out, ref.f2, ref.f3, 1e-12)
+    assert not bad, bad
+    # the boundary moved the sea surface
+    assert np.abs(out.f2["z"][:, 2]).max() > 0.1
+
+
+def test_open_boundary_data_from_host():
+    """getm_set_bdy_data (fixed data, all four types) equals the oracle run with the same data."""
+    g = S.Grid(30, 24, 6, 1000.0, 1000.0)
+    b = S.OpenBoundaries(west=[(g.imin, g.jmin + 2, g.jmax - 2, S.CLAMPED)],
+                         north=[(g.jmax, g.imin + 3, g.imax - 3, S.ZERO_GRADIENT)],
+                         east=[(g.imax, g.jmin + 2, g.jmax - 2, S.SOMMERFELD)],
+                         south=[(g.jmin, g.imin + 3, g.imax - 3, S.FLATHER_ELEV)], ramp=8)
+    n = b.npoints()
+    b.data = np.linspace(-0.2, 0.3, n)
+    b.data_v = np.full(n, 0.01)
+    c = S.baroclinic_case(nx=30, ny=24, kmax=6, recipe="shelf", M=4, seed=2, bdy=b)
+    ref = c.copy()
+    oracle.bc_steps(ref, 1, 12)
+    out, _ = run_gpu(c, 1, 12)
+    bad, worst = compare(out, ref.f2, ref.f3, 1e-12)
+    assert not bad, bad
 
 
 def test_integrate_entry_points_match_time_loop():
@@ -91,10 +132,11 @@ def test_integrate_entry_points_match_time_loop():
 
 def test_mixed_precision_error_vs_fp64():
     """The mixed variant (3D fields FP32; 2D, Uint/Vint and vertical sums FP64) against the FP64
-    oracle after 10 macro steps: per-field error relative to the field's scale (stated bounds)."""
+    oracle after 10 macro steps of the tidally forced shelf: per-field error relative to the
+    field's scale (stated bounds)."""
     import torch
 
-    c = S.baroclinic_case(nx=48, ny=40, kmax=10, recipe="shelf", M=10, seed=3)
+    c = tidal_shelf(nx=48, ny=40, kmax=10, M=10, period=3000.0, seed=3)
     ref = c.copy()
     oracle.bc_steps(ref, 1, 100)
     out, _ = run_gpu(c.copy(dtype3=np.float32), 1, 100, dtype3=torch.float32)
