@@ -56,7 +56,7 @@ int ensure_adj_scratch(getm_ctx* ctx, size_t bytes) {
 template <class R>
 int step_record(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, const R* hu, const R* hv,
                 const R* ho, const R* hn, const R* nuh, int hs, int vs, R AH, R cnpar, R avmol, uint8_t* codes,
-                R* g) {
+                R* g, R* sn = nullptr) {
   const Dev& d = ctx->dev;
   cudaStream_t s = ctx->stream;
   const long long n3 = n3d(d);
@@ -71,7 +71,7 @@ int step_record(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww
   auto L = [&](auto* p, int k) { return p + (long long)k * sk; };
   auto plane = [&](int q) { return codes + (long long)q * n3; };
   const R half = R(0.5), one = R(1);
-  GB_TRY(cudaMemcpyAsync(H, ho, (size_t)sk * sizeof(R), cudaMemcpyDeviceToDevice, s), "copy ho(0)");
+  // (level 0 of the heights is not read by the H-grid sweeps)
   const int nk = kmax;
   GB_TIMED(GETM_TIM_ADJ_RECORD, (run_sweep_h<R, 0>(d, s, nk, dt, half, hs, AH, L(f, 1), L(f, 1), L(S, 1), L(ho, 1),
                                  L(H, 1), nullptr, L(uu, 1), L(hu, 1), gr.mask_uflux, gr.mask_uupdate,
@@ -89,8 +89,10 @@ int step_record(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww
                                  L(H, 1), nullptr, L(uu, 1), L(hu, 1), gr.mask_uflux, gr.mask_uupdate,
                                  L(plane(4), 1))), "u2");
   GB_TIMED(GETM_TIM_ADJ_RECORD, cudaMemcpyAsync(g, f, (size_t)n3 * sizeof(R), cudaMemcpyDeviceToDevice, s), "tape g");
+  // the diffusion's result also goes to sn when the caller keeps the step outputs (only the solved
+  // columns are written there -- the only ones the adjoint diffusion reads)
   GB_TIMED(GETM_TIM_ADJ_RECORD, run_vdiff<R>(d, s, dt, cnpar, avmol, f, hn, nuh, ctx->zmask, nullptr, (R*)ctx->scr[0],
-                                             (R*)ctx->scr[1]), "vdiff");
+                                             (R*)ctx->scr[1], nullptr, sn), "vdiff");
   return GETM_OK;
 }
 
@@ -241,10 +243,8 @@ int gradient_api(getm_ctx* ctx, int nsteps, int every, R dt, R* f, const R* uu, 
     R* fw = ckpt + (size_t)b * n3;
     for (int q = 0; q < cnt; ++q) {
       rc = step_record<R>(ctx, dt, fw, uu, vv, ww, hu, hv, ho, hn, nuh, hs, vs, AH, cnpar, avmol,
-                          codes0 + (size_t)q * 5 * n3, g0 + (size_t)q * n3);
+                          codes0 + (size_t)q * 5 * n3, g0 + (size_t)q * n3, sn0 + (size_t)q * n3);
       if (rc) return rc;
-      GB_TIMED(GETM_TIM_ADJ_RECORD,
-               cudaMemcpyAsync(sn0 + (size_t)q * n3, fw, fb, cudaMemcpyDeviceToDevice, s), "tape output");
     }
     for (int q = cnt - 1; q >= 0; --q) {
       // velocities, heights and nuh are the same in every step: the heights before each sweep are

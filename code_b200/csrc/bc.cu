@@ -25,27 +25,34 @@ __device__ __forceinline__ bool interior(const Dev& d, int i, int j) {
   return i >= d.imin && i <= d.imax && j >= d.jmin && j <= d.jmax;
 }
 
-// bottom_friction.F90:48-150: ru/rv from the depth-averaged velocities (log-law drag).
+// bottom_friction.F90:48-150: ru/rv from the depth-averaged velocities (log-law drag). Arithmetic
+// type T: FP64 in the plain step (the reference's expressions and order), FP32 in the mixed step
+// (inputs and outputs stay FP64 arrays).
+template <class T>
 __global__ void k_bottom_friction(Dev d, Bc2 s, int runtype) {
   GB_IJ2
   W2 U{d, s.f2[U_]}, V{d, s.f2[V_]}, DU_{d, s.f2[DU]}, DV_{d, s.f2[DV]}, ruu{d, s.f2[RUU]}, rvv{d, s.f2[RVV]},
       ru{d, s.f2[RU]}, rv{d, s.f2[RV]}, zub{d, s.f2[ZUB]}, zvb{d, s.f2[ZVB]}, zub0{d, s.f2[ZUB0]}, zvb0{d, s.f2[ZVB0]};
   M2 au{d, s.au}, av{d, s.av};
-  const double kappa = s.par[P_KAPPA], avmmol = s.par[P_AVMMOL], min_depth = s.par[P_MIN_DEPTH];
+  const T kappa = T(s.par[P_KAPPA]), avmmol = T(s.par[P_AVMMOL]), min_depth = T(s.par[P_MIN_DEPTH]);
+  const T q = T(0.25), h = T(0.5);
+  auto qt = [](double a, double b) { return T(a) / T(b); };
   const bool in = interior(d, i, j);
   if (i <= d.imax + HALO - 1 && au(i, j) > 0) {
     // vloc: 4-point average on interior U points (0 elsewhere, as the reference's work array holds)
-    const double vloc = in ? 0.25 * (V(i, j) / DV_(i, j) + V(i + 1, j) / DV_(i + 1, j) + V(i, j - 1) / DV_(i, j - 1) +
-                                     V(i + 1, j - 1) / DV_(i + 1, j - 1))
-                           : 0.0;
-    const double uloc = U(i, j) / DU_(i, j);
-    const double HHl = fmax(min_depth, DU_(i, j));
-    double x = kappa / log((zub(i, j) + 0.5 * HHl) / zub(i, j));
-    double r = x * x;
+    const T vloc = in ? q * (qt(V(i, j), DV_(i, j)) + qt(V(i + 1, j), DV_(i + 1, j)) + qt(V(i, j - 1), DV_(i, j - 1)) +
+                             qt(V(i + 1, j - 1), DV_(i + 1, j - 1)))
+                      : T(0);
+    const T uloc = qt(U(i, j), DU_(i, j));
+    const T HHl = fmax(min_depth, T(DU_(i, j)));
+    const T zb = T(zub(i, j));
+    T x = kappa / log((zb + h * HHl) / zb);
+    T r = x * x;
     if (runtype == 1) {
-      const double fricvel = sqrt(r * (uloc * uloc + vloc * vloc));
-      zub(i, j) = fmin(HHl, zub0(i, j) + 0.1 * avmmol / fmax(avmmol, fricvel));
-      r = (zub(i, j) + 0.5 * HHl) / zub(i, j);
+      const T fricvel = sqrt(r * (uloc * uloc + vloc * vloc));
+      const T zn = fmin(HHl, T(zub0(i, j)) + T(0.1) * avmmol / fmax(avmmol, fricvel));
+      zub(i, j) = zn;
+      r = (zn + h * HHl) / zn;
       x = kappa / log(r);
       r = x * x;
     }
@@ -54,20 +61,22 @@ __global__ void k_bottom_friction(Dev d, Bc2 s, int runtype) {
   }
   if (j <= d.jmax + HALO - 1 && av(i, j) > 0) {
     // uloc: 4-point average on interior V points; elsewhere the U-point quotient where au > 0
-    double uloc;
+    T uloc;
     if (in)
-      uloc = 0.25 * (U(i, j) / DU_(i, j) + U(i - 1, j) / DU_(i - 1, j) + U(i, j + 1) / DU_(i, j + 1) +
-                     U(i - 1, j + 1) / DU_(i - 1, j + 1));
+      uloc = q * (qt(U(i, j), DU_(i, j)) + qt(U(i - 1, j), DU_(i - 1, j)) + qt(U(i, j + 1), DU_(i, j + 1)) +
+                  qt(U(i - 1, j + 1), DU_(i - 1, j + 1)));
     else
-      uloc = (i <= d.imax + HALO - 1 && au(i, j) > 0) ? U(i, j) / DU_(i, j) : 0.0;
-    const double vloc = V(i, j) / DV_(i, j);
-    const double HHl = fmax(min_depth, DV_(i, j));
-    double x = kappa / log((zvb(i, j) + 0.5 * HHl) / zvb(i, j));
-    double r = x * x;
+      uloc = (i <= d.imax + HALO - 1 && au(i, j) > 0) ? qt(U(i, j), DU_(i, j)) : T(0);
+    const T vloc = qt(V(i, j), DV_(i, j));
+    const T HHl = fmax(min_depth, T(DV_(i, j)));
+    const T zb = T(zvb(i, j));
+    T x = kappa / log((zb + h * HHl) / zb);
+    T r = x * x;
     if (runtype == 1) {
-      const double fricvel = sqrt(r * (uloc * uloc + vloc * vloc));
-      zvb(i, j) = fmin(HHl, zvb0(i, j) + 0.1 * avmmol / fmax(avmmol, fricvel));
-      r = (zvb(i, j) + 0.5 * HHl) / zvb(i, j);
+      const T fricvel = sqrt(r * (uloc * uloc + vloc * vloc));
+      const T zn = fmin(HHl, T(zvb0(i, j)) + T(0.1) * avmmol / fmax(avmmol, fricvel));
+      zvb(i, j) = zn;
+      r = (zn + h * HHl) / zn;
       x = kappa / log(r);
       r = x * x;
     }
@@ -613,7 +622,10 @@ int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop) {
   const Dev& d = ctx->dev;
   const Bc2 s = to_bc2(st);
   int* ip = st->ipar;
-  if ((loop - 1) % ip[I_MM] == 0) GB_K2(k_bottom_friction, d, s, ip[I_RUNTYPE]);
+  if ((loop - 1) % ip[I_MM] == 0) {
+    if (st->prec3d == 8) GB_K2(k_bottom_friction<double>, d, s, ip[I_RUNTYPE]);
+    else GB_K2(k_bottom_friction<float>, d, s, ip[I_RUNTYPE]);
+  }
   int rc = uv_advect_2d(ctx, st, st->f2[U_], st->f2[V_], st->f2[DU], st->f2[DV]);
   if (rc) return rc;
   // umomentum / vmomentum: transport update, mirror_bdy_2d (momentum.F90:190,353), Coriolis term

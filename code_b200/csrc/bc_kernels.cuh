@@ -254,34 +254,26 @@ __global__ void __launch_bounds__(128) k_uvmom3d(Dev d, Bc3<R3> s, R3* RUs, R3* 
   for (k = 1; k <= kmax; ++k) uu(i, j, k) = R3((double)QU(i, j, k) + (double)hn(i, j, k) * Diff);
 }
 
-// sigma_coordinates.F90:85-113 (equidistant sigma): layer heights of all levels 0..kmax.
+// sigma_coordinates.F90:85-113 (equidistant sigma): layer heights of all levels 0..kmax. One thread
+// per cell and level (grid z = level): the six stores of a thread are independent, so many are in
+// flight; the 2D inputs of a column are re-read per level from L1/L2.
 template <class R3>
 __global__ void k_sigma(Dev d, Bc3<R3> s) {
   GB_IJ_HALO
+  const int k = blockIdx.z;
   V2 sseo{d, s.f2[SSEO]}, ssen{d, s.f2[SSEN]}, H{d, s.f2[HH]}, ssuo{d, s.f2[SSUO]}, ssun{d, s.f2[SSUN]},
       HU_{d, s.f2[HU]}, ssvo{d, s.f2[SSVO]}, ssvn{d, s.f2[SSVN]}, HV_{d, s.f2[HV]};
   V3<R3> ho{d, s.f3[HO]}, hn{d, s.f3[HN]}, huo{d, s.f3[HUO]}, hun{d, s.f3[HUN]}, hvo{d, s.f3[HVO]}, hvn{d, s.f3[HVN]};
   const double kmaxm1 = 1.0 / (double)(float)d.kmax;
-  {
-    const R3 a = R3((sseo(i, j) + H(i, j)) * kmaxm1), b = R3((ssen(i, j) + H(i, j)) * kmaxm1);
-    for (int k = 0; k <= d.kmax; ++k) {
-      ho(i, j, k) = a;
-      hn(i, j, k) = b;
-    }
-  }
+  ho(i, j, k) = R3((sseo(i, j) + H(i, j)) * kmaxm1);
+  hn(i, j, k) = R3((ssen(i, j) + H(i, j)) * kmaxm1);
   if (i <= d.imax + HALO - 1) {
-    const R3 a = R3((ssuo(i, j) + HU_(i, j)) * kmaxm1), b = R3((ssun(i, j) + HU_(i, j)) * kmaxm1);
-    for (int k = 0; k <= d.kmax; ++k) {
-      huo(i, j, k) = a;
-      hun(i, j, k) = b;
-    }
+    huo(i, j, k) = R3((ssuo(i, j) + HU_(i, j)) * kmaxm1);
+    hun(i, j, k) = R3((ssun(i, j) + HU_(i, j)) * kmaxm1);
   }
   if (j <= d.jmax + HALO - 1) {
-    const R3 a = R3((ssvo(i, j) + HV_(i, j)) * kmaxm1), b = R3((ssvn(i, j) + HV_(i, j)) * kmaxm1);
-    for (int k = 0; k <= d.kmax; ++k) {
-      hvo(i, j, k) = a;
-      hvn(i, j, k) = b;
-    }
+    hvo(i, j, k) = R3((ssvo(i, j) + HV_(i, j)) * kmaxm1);
+    hvn(i, j, k) = R3((ssvn(i, j) + HV_(i, j)) * kmaxm1);
   }
 }
 
@@ -304,36 +296,36 @@ __global__ void k_ww(Dev d, Bc3<R3> s) {
 }
 
 // uv_advect_3d.F90:76-98 (DIR 0, U grid) / :267-289 (DIR 1, V grid): the velocity, transports and
-// heights of the momentum control volumes. One thread per (i,j), levels 1..kmax; wwadv(:,:,0) = 0.
+// heights of the momentum control volumes on levels 1..kmax; wwadv(:,:,0) = 0 (U grid).
 template <class R3, int DIR>
 __global__ void k_uvadv3d_prep(Dev d, Bc3<R3> s, R3* fadvp, R3* uuadvp, R3* vvadvp, R3* wwadvp, R3* huadvp,
                                R3* hvadvp) {
   GB_IJ_HALO
+  const int k = blockIdx.z;  // one thread per cell and level 0..kmax (independent loads in flight)
   V3<R3> uu{d, s.f3[UU]}, vv{d, s.f3[VV]}, ww{d, s.f3[WW]}, ho{d, s.f3[HO]}, hn{d, s.f3[HN]}, hun{d, s.f3[HUN]},
       hvn{d, s.f3[HVN]};
   V3<R3> fadv{d, fadvp}, uuadv{d, uuadvp}, vvadv{d, vvadvp}, wwadv{d, wwadvp}, huadv{d, huadvp}, hvadv{d, hvadvp};
   const R3 half = R3(0.5);
   if (DIR == 0) {
-    wwadv(i, j, 0) = R3(0);
+    if (k == 0) {
+      wwadv(i, j, 0) = R3(0);
+      return;
+    }
     if (i > d.imax + HALO - 1) return;
-    for (int k = 1; k <= d.kmax; ++k) {
-      fadv(i, j, k) = uu(i, j, k) / hun(i, j, k);
-      uuadv(i, j, k) = half * (uu(i, j, k) + uu(i + 1, j, k));
-      vvadv(i, j, k) = half * (vv(i, j, k) + vv(i + 1, j, k));
-      wwadv(i, j, k) = half * (ww(i, j, k) + ww(i + 1, j, k));
-      huadv(i, j, k) = half * (ho(i + 1, j, k) + hn(i + 1, j, k));
-      hvadv(i, j, k) = half * (hvn(i, j, k) + hvn(i + 1, j, k));
-    }
+    fadv(i, j, k) = uu(i, j, k) / hun(i, j, k);
+    uuadv(i, j, k) = half * (uu(i, j, k) + uu(i + 1, j, k));
+    vvadv(i, j, k) = half * (vv(i, j, k) + vv(i + 1, j, k));
+    wwadv(i, j, k) = half * (ww(i, j, k) + ww(i + 1, j, k));
+    huadv(i, j, k) = half * (ho(i + 1, j, k) + hn(i + 1, j, k));
+    hvadv(i, j, k) = half * (hvn(i, j, k) + hvn(i + 1, j, k));
   } else {
-    if (j > d.jmax + HALO - 1) return;
-    for (int k = 1; k <= d.kmax; ++k) {
-      fadv(i, j, k) = vv(i, j, k) / hvn(i, j, k);
-      uuadv(i, j, k) = half * (uu(i, j, k) + uu(i, j + 1, k));
-      vvadv(i, j, k) = half * (vv(i, j, k) + vv(i, j + 1, k));
-      wwadv(i, j, k) = half * (ww(i, j, k) + ww(i, j + 1, k));
-      huadv(i, j, k) = half * (hun(i, j, k) + hun(i, j + 1, k));
-      hvadv(i, j, k) = half * (ho(i, j + 1, k) + hn(i, j + 1, k));
-    }
+    if (k == 0 || j > d.jmax + HALO - 1) return;
+    fadv(i, j, k) = vv(i, j, k) / hvn(i, j, k);
+    uuadv(i, j, k) = half * (uu(i, j, k) + uu(i, j + 1, k));
+    vvadv(i, j, k) = half * (vv(i, j, k) + vv(i, j + 1, k));
+    wwadv(i, j, k) = half * (ww(i, j, k) + ww(i, j + 1, k));
+    huadv(i, j, k) = half * (hun(i, j, k) + hun(i, j + 1, k));
+    hvadv(i, j, k) = half * (ho(i, j + 1, k) + hn(i, j + 1, k));
   }
 }
 
@@ -425,13 +417,15 @@ int run_bc3(int which, const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* cons
         k_uvmom3d<R3, 1><<<g2, b2, 0, st>>>(d, s, scr[0], scr[1]);
       break;
     }
-    case BC3_SIGMA: k_sigma<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s); break;
+    case BC3_SIGMA: k_sigma<R3><<<plane_grid(d, blk, d.kmax + 1), blk, 0, st>>>(d, s); break;
     case BC3_WW: k_ww<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s); break;
     case BC3_UVADV_PREP_U:
-      k_uvadv3d_prep<R3, 0><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[0], scr[1], scr[2], scr[3], scr[4], scr[5]);
+      k_uvadv3d_prep<R3, 0><<<plane_grid(d, blk, d.kmax + 1), blk, 0, st>>>(d, s, scr[0], scr[1], scr[2], scr[3],
+                                                                            scr[4], scr[5]);
       break;
     case BC3_UVADV_PREP_V:
-      k_uvadv3d_prep<R3, 1><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[0], scr[1], scr[2], scr[3], scr[4], scr[5]);
+      k_uvadv3d_prep<R3, 1><<<plane_grid(d, blk, d.kmax + 1), blk, 0, st>>>(d, s, scr[0], scr[1], scr[2], scr[3],
+                                                                            scr[4], scr[5]);
       break;
     case BC3_STRESSES: k_stresses<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s); break;
     case BC3_EQSTATE: k_eqstate<R3><<<plane_grid(d, blk, d.kmax), blk, 0, st>>>(d, s); break;

@@ -90,8 +90,9 @@ int do_adv3d(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, c
   if (hs == NOADV || vs == NOADV || kmax < 1) {
     // p_hi = ho over the whole array
     GB_TIMED(GETM_TIM_COPY, cudaMemcpyAsync(H, ho, bytes3, cudaMemcpyDeviceToDevice, s), "copy ho");
-  } else {
-    // level 0 of p_hi (the sweeps below write levels 1..kmax from ho)
+  } else if (hires || kshift == 1) {
+    // level 0 of p_hi (the sweeps below write levels 1..kmax from ho); read only by the W-grid
+    // vertical sweep (face 0) and returned in hires
     GB_TRY(cudaMemcpyAsync(H, ho, (size_t)sk * sizeof(R), cudaMemcpyDeviceToDevice, s), "copy ho(0)");
   }
   if (hs == NOADV && vs == NOADV) return GETM_OK;
@@ -189,7 +190,6 @@ int do_adv3d_pair(getm_ctx* ctx, R dt, R* fa, R* fb, const R* uu, const R* vv, c
   R* Sb = (R*)ctx->scr[2];
   auto L = [&](auto* p, int k) { return p + (long long)k * sk; };
   const R half = R(0.5), one = R(1);
-  GB_TRY(cudaMemcpyAsync(H, ho, (size_t)sk * sizeof(R), cudaMemcpyDeviceToDevice, s), "copy ho(0)");
   const int nk = kmax;
   GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<R, 0>(d, s, nk, dt, half, hs, AH, L(fa, 1), L(fa, 1), L(Sa, 1), L(ho, 1),
                             L(H, 1), nullptr, L(uu, 1), L(hu, 1), g.mask_uflux, g.mask_uupdate, nullptr, L(fb, 1),

@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(TU, sizeof(R) == 4 ? 16 : 8) k_sweep_u_tile(De
 
 // v sweep (adv_split_v.F90:79-135) over a tile of TVX x TVY cells, for up to NKB levels.
 template <class R, int S, bool REC, int NF>
-__global__ void __launch_bounds__(TVX * TVY, sizeof(R) == 4 ? (NF == 1 ? 8 : 4) : (NF == 1 ? 4 : 3))
+__global__ void __launch_bounds__(TVX * TVY, sizeof(R) == 4 ? (NF == 1 ? 8 : 6) : (NF == 1 ? 4 : 3))
     k_sweep_v_tile(Dev d, SweepC<R> C, int nk, TracerSet<R, NF> F, const R* Di_src, R* Di_dst, R* adv,
                    const R* __restrict__ V, const R* __restrict__ DV, const uint8_t* __restrict__ mflux,
                    const uint8_t* __restrict__ mupd, uint8_t* code) {
@@ -666,9 +666,10 @@ struct ThomasSmem {
 // carried in registers and ru(k)/qu(k) stored in two scratch 3D arrays (full occupancy, no shared
 // memory) for the back substitution.
 template <class R>
-__global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, R* S, const R* __restrict__ hn,
-                                               const R* __restrict__ nuh, const int32_t* __restrict__ az,
-                                               const R* __restrict__ src, R* RUs, R* QUs) {
+__global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, const R* Sin, R* S,
+                                               const R* __restrict__ hn, const R* __restrict__ nuh,
+                                               const int32_t* __restrict__ az, const R* __restrict__ src, R* RUs,
+                                               R* QUs, R* S2) {
   const int kmax = d.kmax;
   const int i = d.imin + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = d.jmin + blockIdx.y * blockDim.y + threadIdx.y;
@@ -677,6 +678,12 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, R*
   if (az[c] != 1 || kmax <= 1) return;
   const long long sk = d.sk;
   auto L = [&](const R* a, int k) -> R { return a[c + k * sk]; };
+  // the old tracer is read from Sin and the new one written to S (they may alias) and, when S2 is
+  // given, also to S2
+  auto put = [&](int k, R v) {
+    S[c + k * sk] = v;
+    if (S2) S2[c + k * sk] = v;
+  };
   const R co = R(2) * (R(1) - cnpar) * dt;
   const R cn = R(2) * cnpar * dt;
   // FP64 solves the reference's system for the new value. FP32 solves the same matrix for the
@@ -690,11 +697,11 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, R*
   int k = kmax;
   R hnk = L(hn, k), hnkm1 = L(hn, k - 1);
   R nu = L(nuh, k - 1) + avmol;
-  R Sk = L(S, k), Skm1 = L(S, k - 1);
+  R Sk = L(Sin, k), Skm1 = L(Sin, k - 1);
   R srck = src ? L(src, k) : R(0);
   // next window entries (level kmax-2 and the interface below it)
   R hn_n = kmax >= 2 ? L(hn, kmax - 2) : R(0), nuh_n = kmax >= 2 ? L(nuh, kmax - 2) : R(0);
-  R S_n = kmax >= 2 ? L(S, kmax - 2) : R(0), src_n = (src && kmax >= 2) ? L(src, kmax - 1) : R(0);
+  R S_n = kmax >= 2 ? L(Sin, kmax - 2) : R(0), src_n = (src && kmax >= 2) ? L(src, kmax - 1) : R(0);
   R ao_km1 = co * nu / (hnk + hnkm1), an_km1 = cn * nu / (hnk + hnkm1);
   R ru, qu;
   {
@@ -720,7 +727,7 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, R*
     if (k >= 3) {
       hn_n = L(hn, k - 2);
       nuh_n = L(nuh, k - 2);
-      S_n = L(S, k - 2);
+      S_n = L(Sin, k - 2);
     }
     if (src) src_n = L(src, k - 1);
     ao_km1 = co * nu / (hnk + hnkm1);
@@ -749,20 +756,20 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, R*
     R a4 = incr ? (ao_k + an_k) * (Skp1 - S1) : Skp1 * ao_k + S1 * (h1 - ao_k);
     if (src) a4 = a4 + L(src, 1);
     v = (a4 - a3 * qu) / (a2 - a3 * ru);
-    S[c + 1 * sk] = incr ? S1 + v : v;
+    put(1, incr ? S1 + v : v);
   }
   // back substitution upwards, with the next level's coefficients loaded one step ahead
   R qn = kmax >= 2 ? QUs[c + 2 * sk] : R(0), rn = kmax >= 2 ? RUs[c + 2 * sk] : R(0);
-  R sn = (incr && kmax >= 2) ? L(S, 2) : R(0);
+  R sn = (incr && kmax >= 2) ? L(Sin, 2) : R(0);
   for (k = 2; k <= kmax; ++k) {
     const R q = qn, r = rn, so = sn;
     if (k < kmax) {
       qn = QUs[c + (k + 1) * sk];
       rn = RUs[c + (k + 1) * sk];
-      if (incr) sn = L(S, k + 1);
+      if (incr) sn = L(Sin, k + 1);
     }
     v = q - r * v;
-    S[c + k * sk] = incr ? so + v : v;
+    put(k, incr ? so + v : v);
   }
 }
 

@@ -104,12 +104,12 @@ int run_finalise(const Dev& d, cudaStream_t s, R dt, R* f, const R* ho, const R*
 
 template <class R>
 int run_vdiff(const Dev& d, cudaStream_t s, R dt, R cnpar, R avmol, R* S, const R* hn, const R* nuh,
-              const int32_t* az, const R* src, R* rus, R* qus) {
+              const int32_t* az, const R* src, R* rus, R* qus, const R* Sin, R* S2) {
   if (d.kmax <= 1) return 0;
   const int nx = d.imax - d.imin + 1, ny = d.jmax - d.jmin + 1;
   dim3 blk(32, 4, 1);
   dim3 grd((nx + 31) / 32, (ny + 3) / 4, 1);
-  k_vdiff<R><<<grd, blk, 0, s>>>(d, dt, cnpar, avmol, S, hn, nuh, az, src, rus, qus);
+  k_vdiff<R><<<grd, blk, 0, s>>>(d, dt, cnpar, avmol, Sin ? Sin : S, S, hn, nuh, az, src, rus, qus, S2);
   return (int)cudaGetLastError();
 }
 
@@ -162,7 +162,8 @@ template int run_sweep_w<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL, in
 template int run_finalise<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL*, const GB_REAL*, const GB_REAL*,
                                    const GB_REAL*, const uint8_t*);
 template int run_vdiff<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL, GB_REAL, GB_REAL*, const GB_REAL*,
-                                const GB_REAL*, const int32_t*, const GB_REAL*, GB_REAL*, GB_REAL*);
+                                const GB_REAL*, const int32_t*, const GB_REAL*, GB_REAL*, GB_REAL*, const GB_REAL*,
+                                GB_REAL*);
 template int run_tridiag<GB_REAL>(cudaStream_t, int, int, int, int, const GB_REAL*, const GB_REAL*,
                                   const GB_REAL*, const GB_REAL*, GB_REAL*);
 template int run_content<GB_REAL>(const Dev&, cudaStream_t, const GB_REAL*, const GB_REAL*, const int32_t*,

@@ -70,10 +70,12 @@ template <class R>
 int run_finalise(const Dev& d, cudaStream_t s, R dt, R* f, const R* ho, const R* adv, const R* hi,
                  const uint8_t* mfin);
 
-// rus/qus: two scratch 3D arrays (Thomas coefficients)
+// rus/qus: two scratch 3D arrays (Thomas coefficients). The old tracer is read from Sin (default:
+// S itself) and the new one written to S and, when given, to S2 as well; only the solved columns
+// (interior, az == 1) are written.
 template <class R>
 int run_vdiff(const Dev& d, cudaStream_t s, R dt, R cnpar, R avmol, R* S, const R* hn, const R* nuh,
-              const int32_t* az, const R* src, R* rus, R* qus);
+              const int32_t* az, const R* src, R* rus, R* qus, const R* Sin = nullptr, R* S2 = nullptr);
 
 template <class R>
 int run_tridiag(cudaStream_t s, int ncol, int kmax, int fi, int lt, const R* au, const R* bu, const R* cu,
