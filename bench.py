@@ -53,6 +53,12 @@ def parse():
     ap.add_argument("--variants", default="fp64,mixed")
     ap.add_argument("--adj-steps", type=int, default=20, help="tracer steps of the adjoint measurement (0 = skip)")
     ap.add_argument("--adj-every", type=int, default=10, help="checkpoint interval of the adjoint")
+    ap.add_argument("--accuracy", type=int, default=0, metavar="STEPS",
+                    help="run the mixed-precision accuracy configuration (the 'rotation' recipe: flat 20 m, "
+                         "dx = 500 m, closed, solid-body rotation and a temperature anomaly; --nx/--ny/--kmax) for "
+                         "STEPS macro steps in FP64 and in the mixed variant and print the per-field errors")
+    ap.add_argument("--tile-sweeps", action="store_true",
+                    help="use the shared-memory tile kernels for every horizontal sweep (comparison)")
     ap.add_argument("--tracer-adjoint", action="store_true",
                     help="time only the checkpointed tracer gradient on the tracer-adjoint configuration "
                          "(random divergence-free flow, SUPERBEE, implicit diffusion; --nx/--ny/--kmax, "
@@ -224,15 +230,61 @@ def run_tracer_adjoint(args):
     print(json.dumps(out), flush=True)
 
 
+def run_accuracy(args):
+    """Mixed variant against the FP64 variant after args.accuracy macro steps: per field, the largest
+    and the RMS difference relative to the largest magnitude of the FP64 field."""
+    import numpy as np
+    import torch
+
+    from code_b200 import state as S
+    from code_b200.getm import BcDevice, Context
+
+    c = S.baroclinic_case(nx=args.nx, ny=args.ny, kmax=args.kmax, recipe="rotation", dx=500.0, M=args.M, dt3=60.0,
+                          seed=3)
+    res = {}
+    t0 = time.time()
+    for key, dt in (("fp64", torch.float64), ("mixed", torch.float32)):
+        ctx = Context(c.grid)
+        ctx.init_advection(*[torch.from_numpy(m).cuda() for m in c.masks()])
+        st = BcDevice(c, dtype3=dt)
+        ctx.time_loop(st, 1, args.M * args.accuracy)
+        torch.cuda.synchronize()
+        res[key] = {n: st.t[n].double() for n in ("f2_z", "f2_U", "f2_V", "f3_uu", "f3_vv", "f3_T", "f3_S")}
+        ctx.close()
+        del st
+    err = {}
+    for n in res["fp64"]:
+        a, b = res["fp64"][n], res["mixed"][n]
+        scale = float(a.abs().max())
+        d = (a - b).abs()
+        at = np.unravel_index(int(d.argmax()), tuple(d.shape))
+        dn = d.flatten().cpu().numpy()
+        err[n[3:]] = {"max": float(d.max()) / scale, "rms": float(d.pow(2).mean().sqrt()) / scale,
+                      "p99_9": float(np.percentile(dn, 99.9)) / scale, "argmax": [int(x) for x in at],
+                      "shape": list(d.shape)}
+    print(json.dumps({"workload": f"mixed-precision accuracy: rotation recipe {args.nx}x{args.ny}x{args.kmax}, "
+                                  f"M = {args.M}, {args.accuracy} macro steps",
+                      "relative_to": "max |field| of the FP64 run", "errors": err,
+                      "wall_s": time.time() - t0}), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup()
+    if args.tile_sweeps and args.impl != "reference":
+        from code_b200 import getm as G
+
+        G.set_vector_sweeps(False)
     if args.impl == "reference":
         run_reference(args, world, rank)
         return
     if args.tracer_adjoint:
         if rank == 0:
             run_tracer_adjoint(args)
+        return
+    if args.accuracy > 0:
+        if rank == 0:
+            run_accuracy(args)
         return
     import torch
     import torch.distributed as dist

@@ -227,7 +227,17 @@ int gradient_api(getm_ctx* ctx, int nsteps, int every, R dt, R* f, const R* uu, 
     ~EvFree() { for (int i = 0; i < 3; ++i) cudaEventDestroy(e[i]); }
   } evfree{ev};
   GB_TRY(cudaEventRecord(ev[0], s), "event");
+  // the steps of the last block are taped while they run forward: the reverse starts with that
+  // block, so it needs no checkpoint and is not recomputed
+  const int last0 = (nblk - 1) * every;
   for (int n = 0; n < nsteps; ++n) {
+    if (n >= last0) {
+      const int q = n - last0;
+      rc = step_record<R>(ctx, dt, f, uu, vv, ww, hu, hv, ho, hn, nuh, hs, vs, AH, cnpar, avmol,
+                          codes0 + (size_t)q * 5 * n3, g0 + (size_t)q * n3, sn0 + (size_t)q * n3);
+      if (rc) return rc;
+      continue;
+    }
     if (n % every == 0)
       GB_TRY(cudaMemcpyAsync(ckpt + (size_t)(n / every) * n3, f, fb, cudaMemcpyDeviceToDevice, s), "checkpoint");
     rc = tracer_step_impl<R>(ctx, dt, f, uu, vv, ww, hu, hv, ho, hn, nuh, split, hs, vs, AH, cnpar, avmol, 1);
@@ -241,7 +251,7 @@ int gradient_api(getm_ctx* ctx, int nsteps, int every, R dt, R* f, const R* uu, 
     const int n0 = b * every;
     const int cnt = (n0 + every <= nsteps) ? every : nsteps - n0;
     R* fw = ckpt + (size_t)b * n3;
-    for (int q = 0; q < cnt; ++q) {
+    for (int q = 0; q < cnt && b != nblk - 1; ++q) {
       rc = step_record<R>(ctx, dt, fw, uu, vv, ww, hu, hv, ho, hn, nuh, hs, vs, AH, cnpar, avmol,
                           codes0 + (size_t)q * 5 * n3, g0 + (size_t)q * n3, sn0 + (size_t)q * n3);
       if (rc) return rc;

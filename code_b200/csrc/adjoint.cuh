@@ -377,15 +377,23 @@ __global__ void __launch_bounds__(128) k_adj_vdiff(Dev d, R dt, R cnpar, R avmol
     RUs[c + k * sk] = ru;
     QUs[c + k * sk] = qu;
   }
+  // the next level's loads are issued one iteration ahead (the elimination is a serial chain)
+  R hn_n = L(hn, kmax - 2), nu_n = L(nuh, kmax - 2), fb_n = L(fbar, kmax - 1);
   for (k = kmax - 1; k >= 2; --k) {
     const R an_k = an_km1;
     hnk = hnkm1;
-    hnkm1 = L(hn, k - 1);
-    an_km1 = cn * (L(nuh, k - 1) + avmol) / (hnk + hnkm1);
+    hnkm1 = hn_n;
+    const R nuv = nu_n, fbk = fb_n;
+    if (k >= 3) {
+      hn_n = L(hn, k - 2);
+      nu_n = L(nuh, k - 2);
+    }
+    fb_n = L(fbar, k - 1);
+    an_km1 = cn * (nuv + avmol) / (hnk + hnkm1);
     const R a3 = -an_k, a1 = -an_km1, a2 = hnk + an_k + an_km1;
     const R den = a2 - a3 * ru;
     ru = a1 / den;
-    qu = (L(fbar, k) - a3 * qu) / den;
+    qu = (fbk - a3 * qu) / den;
     RUs[c + k * sk] = ru;
     QUs[c + k * sk] = qu;
   }
@@ -403,15 +411,26 @@ __global__ void __launch_bounds__(128) k_adj_vdiff(Dev d, R dt, R cnpar, R avmol
   R lm = R(0), l0 = lam1;     // lambda(k-2), lambda(k-1)
   R ao_m = R(0);              // ao of the interface below level k-1
   R hk = L(hn, 1), gk = L(g, 1), sk0 = L(Sn, 1);  // h, g, Sn at level k-1
+  // level k's inputs, loaded one iteration ahead
+  R q_n = QUs[c + 2 * sk], r_n = RUs[c + 2 * sk], h_n = L(hn, 2), g_n = L(g, 2), s_n = L(Sn, 2), v_n = L(nuh, 1);
   for (k = 2; k <= kmax + 1; ++k) {
     R l1 = R(0), ao_k = R(0), hk1 = R(0), gk1 = R(0), sk1 = R(0);
     if (k <= kmax) {
-      l1 = QUs[c + k * sk] - RUs[c + k * sk] * l0;
-      hk1 = L(hn, k);
-      gk1 = L(g, k);
-      sk1 = L(Sn, k);
+      const R qk = q_n, rk = r_n, nuk = v_n;
+      hk1 = h_n;
+      gk1 = g_n;
+      sk1 = s_n;
+      if (k < kmax) {
+        q_n = QUs[c + (k + 1) * sk];
+        r_n = RUs[c + (k + 1) * sk];
+        h_n = L(hn, k + 1);
+        g_n = L(g, k + 1);
+        s_n = L(Sn, k + 1);
+        v_n = L(nuh, k);
+      }
+      l1 = qk - rk * l0;
       const R hs = hk + hk1;
-      const R nu = L(nuh, k - 1) + avmol;
+      const R nu = nuk + avmol;
       ao_k = co * nu / hs;
       const R dl = l0 - l1;
       nubar[c + (k - 1) * sk] = nubar[c + (k - 1) * sk] + dl * (co * (gk1 - gk) + cn * (sk1 - sk0)) / hs;

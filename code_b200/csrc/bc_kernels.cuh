@@ -254,26 +254,38 @@ __global__ void __launch_bounds__(128) k_uvmom3d(Dev d, Bc3<R3> s, R3* RUs, R3* 
   for (k = 1; k <= kmax; ++k) uu(i, j, k) = R3((double)QU(i, j, k) + (double)hn(i, j, k) * Diff);
 }
 
-// sigma_coordinates.F90:85-113 (equidistant sigma): layer heights of all levels 0..kmax. One thread
-// per cell and level (grid z = level): the six stores of a thread are independent, so many are in
-// flight; the 2D inputs of a column are re-read per level from L1/L2.
+// sigma_coordinates.F90:85-113 (equidistant sigma): layer heights of all levels 0..kmax. A thread
+// covers LVC levels of one column (grid z = level chunk): the column's 2D inputs are read once per
+// chunk, and its stores (six per level) are independent.
+constexpr int LVC = 8;
 template <class R3>
 __global__ void k_sigma(Dev d, Bc3<R3> s) {
   GB_IJ_HALO
-  const int k = blockIdx.z;
+  const int k0 = blockIdx.z * LVC, k1 = min(k0 + LVC, d.kmax + 1);
   V2 sseo{d, s.f2[SSEO]}, ssen{d, s.f2[SSEN]}, H{d, s.f2[HH]}, ssuo{d, s.f2[SSUO]}, ssun{d, s.f2[SSUN]},
       HU_{d, s.f2[HU]}, ssvo{d, s.f2[SSVO]}, ssvn{d, s.f2[SSVN]}, HV_{d, s.f2[HV]};
   V3<R3> ho{d, s.f3[HO]}, hn{d, s.f3[HN]}, huo{d, s.f3[HUO]}, hun{d, s.f3[HUN]}, hvo{d, s.f3[HVO]}, hvn{d, s.f3[HVN]};
   const double kmaxm1 = 1.0 / (double)(float)d.kmax;
-  ho(i, j, k) = R3((sseo(i, j) + H(i, j)) * kmaxm1);
-  hn(i, j, k) = R3((ssen(i, j) + H(i, j)) * kmaxm1);
+  {
+    const R3 a = R3((sseo(i, j) + H(i, j)) * kmaxm1), b = R3((ssen(i, j) + H(i, j)) * kmaxm1);
+    for (int k = k0; k < k1; ++k) {
+      ho(i, j, k) = a;
+      hn(i, j, k) = b;
+    }
+  }
   if (i <= d.imax + HALO - 1) {
-    huo(i, j, k) = R3((ssuo(i, j) + HU_(i, j)) * kmaxm1);
-    hun(i, j, k) = R3((ssun(i, j) + HU_(i, j)) * kmaxm1);
+    const R3 a = R3((ssuo(i, j) + HU_(i, j)) * kmaxm1), b = R3((ssun(i, j) + HU_(i, j)) * kmaxm1);
+    for (int k = k0; k < k1; ++k) {
+      huo(i, j, k) = a;
+      hun(i, j, k) = b;
+    }
   }
   if (j <= d.jmax + HALO - 1) {
-    hvo(i, j, k) = R3((ssvo(i, j) + HV_(i, j)) * kmaxm1);
-    hvn(i, j, k) = R3((ssvn(i, j) + HV_(i, j)) * kmaxm1);
+    const R3 a = R3((ssvo(i, j) + HV_(i, j)) * kmaxm1), b = R3((ssvn(i, j) + HV_(i, j)) * kmaxm1);
+    for (int k = k0; k < k1; ++k) {
+      hvo(i, j, k) = a;
+      hvn(i, j, k) = b;
+    }
   }
 }
 
@@ -417,7 +429,7 @@ int run_bc3(int which, const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* cons
         k_uvmom3d<R3, 1><<<g2, b2, 0, st>>>(d, s, scr[0], scr[1]);
       break;
     }
-    case BC3_SIGMA: k_sigma<R3><<<plane_grid(d, blk, d.kmax + 1), blk, 0, st>>>(d, s); break;
+    case BC3_SIGMA: k_sigma<R3><<<plane_grid(d, blk, (d.kmax + LVC) / LVC), blk, 0, st>>>(d, s); break;
     case BC3_WW: k_ww<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s); break;
     case BC3_UVADV_PREP_U:
       k_uvadv3d_prep<R3, 0><<<plane_grid(d, blk, d.kmax + 1), blk, 0, st>>>(d, s, scr[0], scr[1], scr[2], scr[3],

@@ -1,4 +1,5 @@
 // ctx.cu -- context, mask set-up and the C-ABI entry points (include/getm_b200.h).
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -11,6 +12,9 @@
 #include "ctx_internal.h"
 
 namespace gb {
+
+std::atomic<int> g_vector_sweeps{1};
+bool vector_sweeps_enabled() { return g_vector_sweeps.load(std::memory_order_relaxed) != 0; }
 
 
 
@@ -383,6 +387,10 @@ static void drain_timers(getm_ctx* ctx) {
     }
     ctx->pending[t].clear();
   }
+}
+
+int getm_set_vector_sweeps(int on) {
+  return gb::g_vector_sweeps.exchange(on != 0 ? 1 : 0);
 }
 
 int getm_timers_enable(getm_ctx* ctx, int on) {

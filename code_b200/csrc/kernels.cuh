@@ -23,6 +23,25 @@ __device__ __forceinline__ R qdiv(R a, R b) {
   else return a / b;
 }
 
+// FP32 P2_PDM limiter in scaled form. With w = (1-cfl)/2 > 0 (Courant numbers below 1, the
+// stability limit of the split schemes) the reference's candidates 2r/(cfl+1e-10),
+// (1/2+x)+(1/2-x)r and 2/(1-cfl) (r = a/b, x = (1-2cfl)/6), multiplied by w*|deltaf| = w*b, are
+// v1 = a(1-cfl)/(cfl+1e-10), v2 = w((1/2+x)b + (1/2-x)a) and b itself: the interface value is
+// fu + sign(deltaf)*min(v1, v2, b) with one division instead of two (the third branch gives the
+// downwind value). Every operation is an explicitly rounded intrinsic, so the branch comparisons
+// of recon_code round exactly like the value of recon_s wherever they are inlined.
+struct Pdm32 {
+  float v1, v2;
+};
+__device__ __forceinline__ Pdm32 pdm32(float cfl, float a, float b) {
+  const float omc = __fsub_rn(1.f, cfl);
+  const float x = __fmul_rn(1.f / 6.f, __fsub_rn(1.f, __fmul_rn(2.f, cfl)));
+  Pdm32 p;
+  p.v1 = __fdividef(__fmul_rn(a, omc), __fadd_rn(cfl, 1.e-10f));
+  p.v2 = __fmul_rn(__fmul_rn(0.5f, omc), __fmaf_rn(__fadd_rn(0.5f, x), b, __fmul_rn(__fsub_rn(0.5f, x), a)));
+  return p;
+}
+
 // Interface value from (fuu, fu, fd) at Courant number cfl (advection.F90:785-879).
 template <class R, int S>
 __device__ __forceinline__ R recon_s(R cfl, R fuu, R fu, R fd) {
@@ -31,22 +50,21 @@ __device__ __forceinline__ R recon_s(R cfl, R fuu, R fu, R fd) {
   } else {
     const float df = fd - fu, du = fu - fuu;
     if constexpr (S == P2) {
-      const float x = (1.f / 6.f) * (1.f - 2.f * cfl);
-      return fu + 0.5f * (1.f - cfl) * ((0.5f + x) * df + (0.5f - x) * du);
+      const float x = __fmul_rn(1.f / 6.f, __fsub_rn(1.f, __fmul_rn(2.f, cfl)));
+      return __fadd_rn(fu, __fmul_rn(__fmul_rn(0.5f, __fsub_rn(1.f, cfl)),
+                                     __fadd_rn(__fmul_rn(__fadd_rn(0.5f, x), df), __fmul_rn(__fsub_rn(0.5f, x), du))));
     } else if constexpr (S == SUPERBEE || S == MUSCL || S == P2_PDM) {
       if (!(df * du > 0.f)) return fu;
       const float a = fabsf(du), b = fabsf(df);  // L(r)*|deltaf| with r = a/b
-      float Lb;
-      if constexpr (S == SUPERBEE) {
-        Lb = fmaxf(fminf(2.f * a, b), fminf(a, 2.f * b));
-      } else if constexpr (S == MUSCL) {
-        Lb = fminf(fminf(2.f * a, 0.5f * (b + a)), 2.f * b);
+      if constexpr (S == P2_PDM) {
+        const Pdm32 p = pdm32(cfl, a, b);
+        return fu + copysignf(fminf(fminf(p.v1, p.v2), b), df);
       } else {
-        const float x = (1.f / 6.f) * (1.f - 2.f * cfl);
-        Lb = fminf(fminf(__fdividef(2.f * a, cfl + 1.e-10f), (0.5f + x) * b + (0.5f - x) * a),
-                   __fdividef(2.f * b, 1.f - cfl));
+        float Lb;
+        if constexpr (S == SUPERBEE) Lb = fmaxf(fminf(2.f * a, b), fminf(a, 2.f * b));
+        else Lb = fminf(fminf(2.f * a, 0.5f * (b + a)), 2.f * b);
+        return __fadd_rn(fu, __fmul_rn(__fmul_rn(0.5f, __fsub_rn(1.f, cfl)), copysignf(Lb, df)));
       }
-      return fu + 0.5f * (1.f - cfl) * copysignf(Lb, df);
     } else {
       return fu;
     }
@@ -84,11 +102,9 @@ __device__ __forceinline__ uint8_t recon_code(R cfl, R fuu, R fu, R fd) {
         t1 = 2.f * a; t2 = b; t3 = a; t4 = 2.f * b;
       } else if constexpr (S == MUSCL) {
         t1 = 2.f * a; t2 = 0.5f * (b + a); t3 = 2.f * b; t4 = 0.f;
-      } else {
-        const float x = (1.f / 6.f) * (1.f - 2.f * cfl);
-        t1 = __fdividef(2.f * a, cfl + 1.e-10f);
-        t2 = (0.5f + x) * b + (0.5f - x) * a;
-        t3 = __fdividef(2.f * b, 1.f - cfl); t4 = 0.f;
+      } else {  // the scaled candidates of recon_s (pdm32): the same order as t1, t2, t3
+        const Pdm32 p = pdm32(cfl, a, b);
+        t1 = p.v1; t2 = p.v2; t3 = b; t4 = 0.f;
       }
     }
     if constexpr (S == SUPERBEE) {
@@ -150,7 +166,7 @@ __device__ __forceinline__ R fv_update(R hio, R dh, R hin, R fio, R dt, R advn) 
     return (hio * fio - dt * advn) / hin;
   } else {
     (void)hio;
-    return fio + __fdividef(fio * dh - dt * advn, hin);
+    return __fadd_rn(fio, __fdividef(__fmaf_rn(fio, dh, -__fmul_rn(dt, advn)), hin));
   }
 }
 
@@ -193,7 +209,8 @@ __device__ __forceinline__ R face_flux_s(R Uf, R DUf, R fm1, R f0, R f1, R f2, b
 // and then updates its cells. A cell in the update range with mask_update takes fi/Di from the
 // sources, every other cell copies them through when source and destination differ. f must not
 // alias fi_dst (callers ping-pong); fi_src may be f or alias fi_dst, Di_src may alias Di_dst.
-constexpr int TU = 128;             // u sweep: cells per block along i
+constexpr int TU = 128;             // u sweep: threads (faces) per block along i
+constexpr int OWU = TU - 1;         // u sweep: cells updated per block
 constexpr int TVX = 32, TVY = 8;    // v sweep: tile of 32 (i) x 8 (j) cells
 constexpr int NKB = 8;              // levels per block (the 2D masks are staged once for them)
 
@@ -203,6 +220,7 @@ constexpr int NKB = 8;              // levels per block (the 2D masks are staged
 template <class R>
 struct SweepC {
   R dt, splitfac, AH, dti, dxf, dyf, ard1, cdx;
+  R cdy, cadv;  // FP32 cell update: dti*dyf*ard1 and splitfac*dyf*ard1
 };
 
 template <class R>
@@ -216,7 +234,24 @@ inline SweepC<R> sweep_consts(const Dev& d, int dir, R dt, R splitfac, R AH) {
   c.dyf = dir == 0 ? R(d.dy) : R(d.dx);
   c.ard1 = R(d.ard1);
   c.cdx = c.dti / c.dxf;
+  c.cdy = c.dti * c.dyf * c.ard1;
+  c.cadv = splitfac * c.dyf * c.ard1;
   return c;
+}
+
+// Height decrement and flux divergence of a cell between its faces lo and hi
+// (adv_split_u.F90:274-276). FP64: the reference's expressions. FP32: one difference times a
+// host constant, with explicitly rounded operations, so every sweep kernel that calls these
+// rounds identically (no compiler-chosen contraction).
+template <class R>
+__device__ __forceinline__ R cell_dD(const SweepC<R>& C, R Uhi, R Ulo) {
+  if constexpr (sizeof(R) == 8) return C.dti * (Uhi * C.dyf - Ulo * C.dyf) * C.ard1;
+  else return __fmul_rn(__fsub_rn(Uhi, Ulo), C.cdy);
+}
+template <class R>
+__device__ __forceinline__ R cell_advn(const SweepC<R>& C, R flhi, R fllo) {
+  if constexpr (sizeof(R) == 8) return C.splitfac * (flhi * C.dyf - fllo * C.dyf) * C.ard1;
+  else return __fmul_rn(__fsub_rn(flhi, fllo), C.cadv);
 }
 
 // The tracer fields of one sweep: the stencil source f, the field fi updated from fi_src into
@@ -234,58 +269,111 @@ struct TracerSet {
   TracerIO<R> t[NF];
 };
 
-// u sweep (adv_split_u.F90:222-285) over one row segment of TU cells, for up to NKB levels.
+// Asynchronous global -> shared copies (cp.async, 4 or 8 bytes): the tile sweeps stage level k+1
+// while they compute level k, so the loads of the next level are in flight during the face and
+// update phases instead of stalling every warp at the start of each level.
+template <class R>
+__device__ __forceinline__ void cp_async(R* smem, const R* gmem) {
+  static_assert(sizeof(R) == 4 || sizeof(R) == 8, "cp_async: 4 or 8 bytes");
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem), "n"(sizeof(R)) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// u sweep (adv_split_u.F90:222-285) over one row segment, for up to NKB levels. The TU threads
+// compute the TU faces i0-1 .. i0+TU-2 (one each) and update the OWU = TU-1 cells between them,
+// so no warp computes a second face. Levels are double-buffered in shared memory: the copies of
+// level k+1 (stencil source, transports, heights, own-cell inputs) are issued before level k is
+// computed.
 template <class R, int S, bool REC, int NF>
 __global__ void __launch_bounds__(TU, sizeof(R) == 4 ? 16 : 8) k_sweep_u_tile(Dev d, SweepC<R> C, int nk, TracerSet<R, NF> F,
                                                      const R* Di_src, R* Di_dst, R* adv,
                                                      const R* __restrict__ U, const R* __restrict__ DU,
                                                      const uint8_t* __restrict__ mflux,
                                                      const uint8_t* __restrict__ mupd, uint8_t* code) {
-  __shared__ R sf[NF][TU + 4];   // f(i0-2 .. i0+TU+1)
-  __shared__ R sU[TU + 1];       // U(i0-1 .. i0+TU-1)
-  __shared__ R sDU[TU + 1];
-  __shared__ uint8_t sm[TU + 4];  // mflux(i0-2 .. i0+TU+1)
-  __shared__ R sfl[NF][TU + 1];  // flux of faces i0-1 .. i0+TU-1
+  __shared__ R sf[2][NF][TU + 3];   // f(i0-2 .. i0+TU)
+  __shared__ R sU[2][TU];           // U(i0-1 .. i0+TU-2)
+  __shared__ R sDU[2][TU];
+  __shared__ R sD[2][TU];           // Di_src of the own cells
+  __shared__ R sfi[2][NF][TU];      // fi_src of the own cells (when it is not f)
+  __shared__ R sA[2][TU];           // adv of the own cells (momentum sweeps)
+  __shared__ uint8_t sm[TU + 3];    // mflux(i0-2 .. i0+TU)
+  __shared__ R sfl[NF][TU];         // flux of faces i0-1 .. i0+TU-2
   const int t = threadIdx.x;
   const int ni = d.ni();
-  const int ii0 = blockIdx.x * TU;
+  const int ii0 = blockIdx.x * OWU;
   const long long crow = (long long)blockIdx.y * d.sj;
   const int k0 = blockIdx.z * NKB;
   const int k1 = min(k0 + NKB, nk);
   constexpr int sub = (S == UPSTREAM) ? 0 : 1;
   const bool use_AH = C.AH > R(0);
   // masks of the row (levels share them)
-  for (int q = t; q < TU + 4; q += TU) {
+  for (int q = t; q < TU + 3; q += TU) {
     const int ii = ii0 - 2 + q;
     sm[q] = (ii >= 0 && ii < ni) ? mflux[crow + ii] : 0;
   }
   const int ii = ii0 + t;
-  const bool own = ii < ni;
+  const bool own = t < OWU && ii < ni;
   const bool upd = own && (ii >= 1 + sub) && (ii <= ni - 2 - sub) && mupd[crow + ii];
-  for (int k = k0; k < k1; ++k) {
+  // tiles away from the ends of the row stage without bounds checks
+  const bool inner = ii0 >= 2 && ii0 + TU + 1 <= ni;
+  auto stage = [&](int k, int b) {
     const long long row = crow + (long long)k * d.sk;
+    const R* Ur = U + row;
+    const R* DUr = DU + row;
+    if (inner) {
 #pragma unroll
-    for (int n = 0; n < NF; ++n) {
-      const R* fr = F.t[n].f + row;
-      for (int q = t; q < TU + 4; q += TU) {
-        const int i2 = ii0 - 2 + q;
-        sf[n][q] = (i2 >= 0 && i2 < ni) ? fr[i2] : R(0);
+      for (int n = 0; n < NF; ++n) {
+        const R* fr = F.t[n].f + row + (ii0 - 2);
+        cp_async(&sf[b][n][t], fr + t);
+        if (t < 3) cp_async(&sf[b][n][TU + t], fr + TU + t);
+      }
+      cp_async(&sU[b][t], Ur + ii0 - 1 + t);
+      cp_async(&sDU[b][t], DUr + ii0 - 1 + t);
+    } else {
+#pragma unroll
+      for (int n = 0; n < NF; ++n) {
+        const R* fr = F.t[n].f + row;
+        for (int q = t; q < TU + 3; q += TU) {
+          const int i2 = ii0 - 2 + q;
+          if (i2 >= 0 && i2 < ni) cp_async(&sf[b][n][q], fr + i2);
+          else sf[b][n][q] = R(0);
+        }
+      }
+      const int i2 = ii0 - 1 + t;
+      if (i2 >= 0 && i2 < ni) {
+        cp_async(&sU[b][t], Ur + i2);
+        cp_async(&sDU[b][t], DUr + i2);
+      } else {
+        sU[b][t] = R(0);
+        sDU[b][t] = R(0);
       }
     }
-    for (int q = t; q < TU + 1; q += TU) {
-      const int i2 = ii0 - 1 + q;
-      const bool ok = i2 >= 0 && i2 < ni;
-      sU[q] = ok ? U[row + i2] : R(0);
-      sDU[q] = ok ? DU[row + i2] : R(0);
-    }
-    // own-cell inputs, in flight during the face phase
-    const R Dio = own ? Di_src[row + ii] : R(0);
-    R fio_g[NF];
+    if (own) {
+      cp_async(&sD[b][t], Di_src + row + ii);
 #pragma unroll
-    for (int n = 0; n < NF; ++n)
-      fio_g[n] = (own && F.t[n].fi_src != F.t[n].f) ? F.t[n].fi_src[row + ii] : R(0);
+      for (int n = 0; n < NF; ++n)
+        if (F.t[n].fi_src != F.t[n].f) cp_async(&sfi[b][n][t], F.t[n].fi_src + row + ii);
+      if (NF == 1 && adv && upd) cp_async(&sA[b][t], adv + row + ii);
+    }
+    cp_async_commit();
+  };
+  if (k0 < k1) stage(k0, 0);
+  for (int k = k0, b = 0; k < k1; ++k, b ^= 1) {
+    const long long row = crow + (long long)k * d.sk;
+    if (k + 1 < k1) {
+      stage(k + 1, b ^ 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
     __syncthreads();
-    for (int q = t; q < TU + 1; q += TU) {
+    {
+      const int q = t;
       const int fa = ii0 - 1 + q;
       const bool valid = fa >= sub && fa <= ni - 2 - sub;
 #pragma unroll
@@ -293,9 +381,9 @@ __global__ void __launch_bounds__(TU, sizeof(R) == 4 ? 16 : 8) k_sweep_u_tile(De
         R fl = R(0);
         uint8_t cd = 0;
         if (valid)
-          fl = face_flux_s<R, S, REC>(sU[q], sDU[q], sf[n][q], sf[n][q + 1], sf[n][q + 2], sf[n][q + 3],
-                                      sm[q] != 0, sm[q + 1] != 0, sm[q + 2] != 0, C.dti, C.cdx, C.AH, use_AH,
-                                      C.dxf, &cd);
+          fl = face_flux_s<R, S, REC>(sU[b][q], sDU[b][q], sf[b][n][q], sf[b][n][q + 1], sf[b][n][q + 2],
+                                      sf[b][n][q + 3], sm[q] != 0, sm[q + 1] != 0, sm[q + 2] != 0, C.dti, C.cdx,
+                                      C.AH, use_AH, C.dxf, &cd);
         sfl[n][q] = fl;
         if (REC && n == 0 && q >= 1 && fa < ni) code[row + fa] = cd;  // face fa is stored at its left cell
       }
@@ -303,40 +391,45 @@ __global__ void __launch_bounds__(TU, sizeof(R) == 4 ? 16 : 8) k_sweep_u_tile(De
     __syncthreads();
     if (own) {
       const long long p = row + ii;
+      const R Dio = sD[b][t];
       if (upd) {
-        const R dD = C.dti * (sU[t + 1] * C.dyf - sU[t] * C.dyf) * C.ard1;
+        const R dD = cell_dD<R>(C, sU[b][t + 1], sU[b][t]);
         const R Dn = Dio - dD;
         Di_dst[p] = Dn;
 #pragma unroll
         for (int n = 0; n < NF; ++n) {
-          const R fio = F.t[n].fi_src == F.t[n].f ? sf[n][t + 2] : fio_g[n];
-          const R advn = C.splitfac * (sfl[n][t + 1] * C.dyf - sfl[n][t] * C.dyf) * C.ard1;
+          const R fio = F.t[n].fi_src == F.t[n].f ? sf[b][n][t + 2] : sfi[b][n][t];
+          const R advn = cell_advn<R>(C, sfl[n][t + 1], sfl[n][t]);
           F.t[n].fi_dst[p] = fv_update<R>(Dio, dD, Dn, fio, C.dt, advn);
-          if (NF == 1 && adv) adv[p] = adv[p] + advn;
+          if (NF == 1 && adv) adv[p] = sA[b][t] + advn;
         }
       } else {
 #pragma unroll
         for (int n = 0; n < NF; ++n)
           if (F.t[n].fi_dst != F.t[n].fi_src)
-            F.t[n].fi_dst[p] = F.t[n].fi_src == F.t[n].f ? sf[n][t + 2] : fio_g[n];
+            F.t[n].fi_dst[p] = F.t[n].fi_src == F.t[n].f ? sf[b][n][t + 2] : sfi[b][n][t];
         if (Di_dst != Di_src) Di_dst[p] = Dio;
       }
     }
-    __syncthreads();  // sf/sU/sfl are restaged for the next level
+    __syncthreads();  // buffer b and sfl are restaged / rewritten for level k+2 / k+1
   }
 }
 
-// v sweep (adv_split_v.F90:79-135) over a tile of TVX x TVY cells, for up to NKB levels.
+// v sweep (adv_split_v.F90:79-135) over a tile of TVX x TVY cells, for up to NKB levels, with the
+// levels double-buffered in shared memory like the u sweep.
 template <class R, int S, bool REC, int NF>
 __global__ void __launch_bounds__(TVX * TVY, sizeof(R) == 4 ? (NF == 1 ? 8 : 6) : (NF == 1 ? 4 : 3))
     k_sweep_v_tile(Dev d, SweepC<R> C, int nk, TracerSet<R, NF> F, const R* Di_src, R* Di_dst, R* adv,
                    const R* __restrict__ V, const R* __restrict__ DV, const uint8_t* __restrict__ mflux,
                    const uint8_t* __restrict__ mupd, uint8_t* code) {
-  __shared__ R sf[NF][TVY + 4][TVX];    // f(j0-2 .. j0+TVY+1)
-  __shared__ R sV[TVY + 1][TVX];        // V(j0-1 .. j0+TVY-1)
-  __shared__ R sDV[TVY + 1][TVX];
-  __shared__ uint8_t sm[TVY + 4][TVX];  // mflux(j0-2 .. j0+TVY+1)
-  __shared__ R sfl[NF][TVY + 1][TVX];   // flux of faces j0-1 .. j0+TVY-1
+  __shared__ R sf[2][NF][TVY + 4][TVX];  // f(j0-2 .. j0+TVY+1)
+  __shared__ R sV[2][TVY + 1][TVX];      // V(j0-1 .. j0+TVY-1)
+  __shared__ R sDV[2][TVY + 1][TVX];
+  __shared__ R sD[2][TVY][TVX];          // Di_src of the own cells
+  __shared__ R sfi[2][NF][TVY][TVX];     // fi_src of the own cells (when it is not f)
+  __shared__ R sA[2][TVY][TVX];          // adv of the own cells (momentum sweeps)
+  __shared__ uint8_t sm[TVY + 4][TVX];   // mflux(j0-2 .. j0+TVY+1)
+  __shared__ R sfl[NF][TVY + 1][TVX];    // flux of faces j0-1 .. j0+TVY-1
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int ni = d.ni(), nj = d.nj();
   const int ii = blockIdx.x * TVX + tx;
@@ -355,26 +448,64 @@ __global__ void __launch_bounds__(TVX * TVY, sizeof(R) == 4 ? (NF == 1 ? 8 : 6) 
   const bool own = iok && jj < nj;
   const long long c = (long long)jj * sj + ii;
   const bool upd = own && (jj >= 1 + sub) && (jj <= nj - 2 - sub) && mupd[c];
-  for (int k = k0; k < k1; ++k) {
+  // tiles away from the ends of the columns stage without bounds checks
+  const bool inner = iok && jj0 >= 2 && jj0 + TVY + 2 <= nj;
+  auto stage = [&](int k, int b) {
     const long long lev = (long long)k * d.sk;
+    if (inner) {
+      const long long b0 = lev + (long long)(jj0 - 2) * sj + ii;  // row jj0-2 of this column
 #pragma unroll
-    for (int n = 0; n < NF; ++n)
-      for (int q = ty; q < TVY + 4; q += TVY) {
-        const int j2 = jj0 - 2 + q;
-        sf[n][q][tx] = (iok && j2 >= 0 && j2 < nj) ? F.t[n].f[lev + (long long)j2 * sj + ii] : R(0);
+      for (int n = 0; n < NF; ++n) {
+        const R* fc = F.t[n].f + b0;
+        cp_async(&sf[b][n][ty][tx], fc + (long long)ty * sj);
+        if (ty < 4) cp_async(&sf[b][n][TVY + ty][tx], fc + (long long)(TVY + ty) * sj);
       }
-    for (int q = ty; q < TVY + 1; q += TVY) {
-      const int j2 = jj0 - 1 + q;
-      const bool ok = iok && j2 >= 0 && j2 < nj;
-      const long long c2 = lev + (long long)j2 * sj + ii;
-      sV[q][tx] = ok ? V[c2] : R(0);
-      sDV[q][tx] = ok ? DV[c2] : R(0);
-    }
-    const R Dio = own ? Di_src[lev + c] : R(0);
-    R fio_g[NF];
+      const R* Vc = V + b0 + sj;  // row jj0-1
+      const R* DVc = DV + b0 + sj;
+      cp_async(&sV[b][ty][tx], Vc + (long long)ty * sj);
+      cp_async(&sDV[b][ty][tx], DVc + (long long)ty * sj);
+      if (ty == 0) {
+        cp_async(&sV[b][TVY][tx], Vc + (long long)TVY * sj);
+        cp_async(&sDV[b][TVY][tx], DVc + (long long)TVY * sj);
+      }
+    } else {
 #pragma unroll
-    for (int n = 0; n < NF; ++n)
-      fio_g[n] = (own && F.t[n].fi_src != F.t[n].f) ? F.t[n].fi_src[lev + c] : R(0);
+      for (int n = 0; n < NF; ++n)
+        for (int q = ty; q < TVY + 4; q += TVY) {
+          const int j2 = jj0 - 2 + q;
+          if (iok && j2 >= 0 && j2 < nj) cp_async(&sf[b][n][q][tx], F.t[n].f + lev + (long long)j2 * sj + ii);
+          else sf[b][n][q][tx] = R(0);
+        }
+      for (int q = ty; q < TVY + 1; q += TVY) {
+        const int j2 = jj0 - 1 + q;
+        if (iok && j2 >= 0 && j2 < nj) {
+          const long long c2 = lev + (long long)j2 * sj + ii;
+          cp_async(&sV[b][q][tx], V + c2);
+          cp_async(&sDV[b][q][tx], DV + c2);
+        } else {
+          sV[b][q][tx] = R(0);
+          sDV[b][q][tx] = R(0);
+        }
+      }
+    }
+    if (own) {
+      cp_async(&sD[b][ty][tx], Di_src + lev + c);
+#pragma unroll
+      for (int n = 0; n < NF; ++n)
+        if (F.t[n].fi_src != F.t[n].f) cp_async(&sfi[b][n][ty][tx], F.t[n].fi_src + lev + c);
+      if (NF == 1 && adv && upd) cp_async(&sA[b][ty][tx], adv + lev + c);
+    }
+    cp_async_commit();
+  };
+  if (k0 < k1) stage(k0, 0);
+  for (int k = k0, b = 0; k < k1; ++k, b ^= 1) {
+    const long long lev = (long long)k * d.sk;
+    if (k + 1 < k1) {
+      stage(k + 1, b ^ 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
     __syncthreads();
     for (int q = ty; q < TVY + 1; q += TVY) {
       const int fa = jj0 - 1 + q;
@@ -384,9 +515,9 @@ __global__ void __launch_bounds__(TVX * TVY, sizeof(R) == 4 ? (NF == 1 ? 8 : 6) 
         R fl = R(0);
         uint8_t cd = 0;
         if (valid)
-          fl = face_flux_s<R, S, REC>(sV[q][tx], sDV[q][tx], sf[n][q][tx], sf[n][q + 1][tx], sf[n][q + 2][tx],
-                                      sf[n][q + 3][tx], sm[q][tx] != 0, sm[q + 1][tx] != 0, sm[q + 2][tx] != 0,
-                                      C.dti, C.cdx, C.AH, use_AH, C.dxf, &cd);
+          fl = face_flux_s<R, S, REC>(sV[b][q][tx], sDV[b][q][tx], sf[b][n][q][tx], sf[b][n][q + 1][tx],
+                                      sf[b][n][q + 2][tx], sf[b][n][q + 3][tx], sm[q][tx] != 0, sm[q + 1][tx] != 0,
+                                      sm[q + 2][tx] != 0, C.dti, C.cdx, C.AH, use_AH, C.dxf, &cd);
         sfl[n][q][tx] = fl;
         if (REC && n == 0 && q >= 1 && iok && fa < nj) code[lev + (long long)fa * sj + ii] = cd;
       }
@@ -394,26 +525,27 @@ __global__ void __launch_bounds__(TVX * TVY, sizeof(R) == 4 ? (NF == 1 ? 8 : 6) 
     __syncthreads();
     if (own) {
       const long long p = lev + c;
+      const R Dio = sD[b][ty][tx];
       if (upd) {
-        const R dD = C.dti * (sV[ty + 1][tx] * C.dyf - sV[ty][tx] * C.dyf) * C.ard1;
+        const R dD = cell_dD<R>(C, sV[b][ty + 1][tx], sV[b][ty][tx]);
         const R Dn = Dio - dD;
         Di_dst[p] = Dn;
 #pragma unroll
         for (int n = 0; n < NF; ++n) {
-          const R fio = F.t[n].fi_src == F.t[n].f ? sf[n][ty + 2][tx] : fio_g[n];
-          const R advn = C.splitfac * (sfl[n][ty + 1][tx] * C.dyf - sfl[n][ty][tx] * C.dyf) * C.ard1;
+          const R fio = F.t[n].fi_src == F.t[n].f ? sf[b][n][ty + 2][tx] : sfi[b][n][ty][tx];
+          const R advn = cell_advn<R>(C, sfl[n][ty + 1][tx], sfl[n][ty][tx]);
           F.t[n].fi_dst[p] = fv_update<R>(Dio, dD, Dn, fio, C.dt, advn);
-          if (NF == 1 && adv) adv[p] = adv[p] + advn;
+          if (NF == 1 && adv) adv[p] = sA[b][ty][tx] + advn;
         }
       } else {
 #pragma unroll
         for (int n = 0; n < NF; ++n)
           if (F.t[n].fi_dst != F.t[n].fi_src)
-            F.t[n].fi_dst[p] = F.t[n].fi_src == F.t[n].f ? sf[n][ty + 2][tx] : fio_g[n];
+            F.t[n].fi_dst[p] = F.t[n].fi_src == F.t[n].f ? sf[b][n][ty + 2][tx] : sfi[b][n][ty][tx];
         if (Di_dst != Di_src) Di_dst[p] = Dio;
       }
     }
-    __syncthreads();
+    __syncthreads();  // buffer b and sfl are restaged / rewritten for level k+2 / k+1
   }
 }
 

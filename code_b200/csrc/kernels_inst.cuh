@@ -1,11 +1,30 @@
 // kernels_inst.cuh -- launcher definitions; included once per precision by kernels_f64.cu and
 // kernels_f32.cu with GB_REAL defined to the arithmetic type.
 #pragma once
+#include <cstdint>
+#include <initializer_list>
 #include <type_traits>
 
 #include "kernels.cuh"
+#include "sweeps_vec.cuh"
 
 namespace gb {
+
+// The vectorised sweeps of sweeps_vec.cuh apply when every row and level of the fields starts on
+// a 16-byte boundary; the tile kernels serve every other layout (and all layouts when the
+// vectorised sweeps are switched off, for comparison).
+template <class R>
+static bool vec_layout(const Dev& d, int nk, std::initializer_list<const void*> ptrs,
+                       std::initializer_list<const void*> bytes) {
+  constexpr long long N = 16 / sizeof(R);
+  if (!vector_sweeps_enabled()) return false;
+  if (d.sj % N != 0 || (nk > 1 && d.sk % N != 0)) return false;
+  for (const void* p : ptrs)
+    if (p && (reinterpret_cast<uintptr_t>(p) % 16) != 0) return false;
+  for (const void* p : bytes)
+    if (p && (reinterpret_cast<uintptr_t>(p) % N) != 0) return false;
+  return true;
+}
 
 // Calls F.template operator()<S>() with the scheme id as a compile-time constant; returns
 // cudaErrorInvalidValue for an id that is not a split scheme.
@@ -35,8 +54,39 @@ int run_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int sche
     auto go = [&](auto rec, auto set) {
       constexpr bool REC = decltype(rec)::value;
       constexpr int NF = sizeof(set.t) / sizeof(set.t[0]);
+      // FP64 sweeps measure faster in the tile kernels (division-bound faces), FP32 in the
+      // vectorised ones
+      const bool vec = sizeof(R) == 4 &&
+                       vec_layout<R>(d, nk,
+                                     {set.t[0].f, set.t[0].fi_src, set.t[0].fi_dst, set.t[NF - 1].f,
+                                      set.t[NF - 1].fi_src, set.t[NF - 1].fi_dst, Di_src, Di_dst, adv, U, DU},
+                                     {mflux, mupd, code});
+      if constexpr (sizeof(R) == 4) {
+        constexpr int N = 16 / sizeof(R);
+        if (vec && DIR == 0) {
+          const int nseg = (d.ni() + UOWN * N - 1) / (UOWN * N);
+          dim3 blk(32, UWB, 1);
+          dim3 grd((nseg + UWB - 1) / UWB, d.nj(), nz);
+          k_sweep_u_vec<R, S, REC, NF><<<grd, blk, 0, s>>>(d, C, nk, set, Di_src, Di_dst, adv, U, DU, mflux,
+                                                           mupd, code);
+          return (int)cudaGetLastError();
+        }
+        if (vec) {
+          // rows per thread: VJS, halved while the grid would give fewer than ~24 warps per SM
+          const long long nx = (d.ni() + 32 * N - 1) / (32 * N), nz = (nk + VKW - 1) / VKW;
+          int rows = VJS;
+          while (rows > 8 && nx * ((d.nj() + rows - 1) / rows) * nz * VKW < 148LL * 24) rows /= 2;
+          dim3 blk(32, VKW, 1);
+          dim3 grd((unsigned)nx, (d.nj() + rows - 1) / rows, (unsigned)nz);
+          k_sweep_v_vec<R, S, REC, NF><<<grd, blk, 0, s>>>(d, C, nk, rows, set, Di_src, Di_dst, adv, U, DU, mflux,
+                                                           mupd, code);
+          return (int)cudaGetLastError();
+        }
+      } else {
+        (void)vec;
+      }
       if (DIR == 0) {
-        dim3 grd((d.ni() + TU - 1) / TU, d.nj(), nz);
+        dim3 grd((d.ni() + OWU - 1) / OWU, d.nj(), nz);
         k_sweep_u_tile<R, S, REC, NF><<<grd, TU, 0, s>>>(d, C, nk, set, Di_src, Di_dst, adv, U, DU, mflux, mupd,
                                                          code);
       } else {

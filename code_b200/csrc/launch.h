@@ -8,6 +8,9 @@ namespace gb {
 
 struct Dev;
 
+// Process-wide switch of the vectorised horizontal sweeps (getm_set_vector_sweeps; on by default).
+bool vector_sweeps_enabled();
+
 constexpr int RED_BLOCKS = 1184;  // 8 x 148 SMs
 constexpr int RED_THREADS = 256;
 

@@ -82,6 +82,7 @@ _PROTOS = {
     "getm_tracer_content": [P, P, P, P, P],
     "getm_tracer_content_f32": [P, P, P, P, P],
     "getm_check_3d_fields": [P, P, P, D, D, P],
+    "getm_set_vector_sweeps": [I],
     "getm_timers_enable": [P, I],
     "getm_timers_reset": [P],
     "getm_timers_read": [P, I, P, P],
@@ -109,6 +110,12 @@ def lib():
                 fn.restype = _RESTYPES.get(name, C.c_int)
             _lib = L
     return _lib
+
+
+def set_vector_sweeps(on: bool) -> bool:
+    """Process-wide choice of the horizontal sweep kernels (vectorised where the layout allows, or
+    the shared-memory tile sweeps everywhere); returns the previous setting."""
+    return bool(lib().getm_set_vector_sweeps(1 if on else 0))
 
 
 def exported_symbols():

@@ -146,6 +146,7 @@ def baroclinic_case(nx=32, ny=24, kmax=8, recipe="shelf", dx=1000.0, M=20, dt3=6
 
     recipe 'shelf': H = 10 + 190*0.5*(1+tanh((x-x0)/L)), L = 20 cells, x0 = nx/2.
     recipe 'flat':  H = 20 m.
+    recipe 'rotation': H = 20 m, solid-body rotation and a temperature anomaly (see _rotation_start).
     recipe 'islands': H = hmin + (hmax-hmin)*(field-p)/(max-p) on wet cells of a Gaussian-smoothed
       noise field (sigma = 40 cells, scaled with the grid), land where field < its `land` quantile.
     Stratification: T from 20 C (surface) to 8 C (bottom) linear in depth plus N(0, 0.1) noise,
@@ -156,7 +157,51 @@ def baroclinic_case(nx=32, ny=24, kmax=8, recipe="shelf", dx=1000.0, M=20, dt3=6
     """
     c, rng = _baroclinic_2d(nx, ny, kmax, recipe, dx, M, dt3, seed, dtype3, land, hmin, hmax, latitude, True, bdy)
     _baroclinic_3d_numpy(c, rng, nu_max)
+    if recipe == "rotation":
+        _rotation_start(c)
     return c
+
+
+def _rotation_start(c: BcCase, umax=0.5, sigma_cells=8.0):
+    """recipe 'rotation' (flat 20 m): solid-body rotation of the whole water column (the discrete
+    curl of psi = 0.5*omega*min(r,R)^2 at X points, R = nx/2 cells, omega = umax/R; depth-uniform
+    velocity, so uu = u*hun, U = sum of uu) and a temperature anomaly of 1 C (Gaussian, sigma =
+    sigma_cells) on 15 C at (0.3 nx, 0.5 ny); S = 35."""
+    g = c.grid
+    f2, f3 = c.f2, c.f3
+    dx = g.dx
+    i = np.arange(g.imin - HALO, g.imax + HALO + 1)
+    j = np.arange(g.jmin - HALO, g.jmax + HALO + 1)
+    xX, yX = (i - g.imin + 1) * dx, (j - g.jmin + 1) * dx
+    xc, yc, R = g.nx * dx / 2, g.ny * dx / 2, (g.nx / 2) * dx
+    om = umax / R
+    r = np.sqrt((xX[None, :] - xc) ** 2 + (yX[:, None] - yc) ** 2)
+    psi = 0.5 * om * np.minimum(r, R) ** 2
+    u = np.zeros(g.shape2())
+    v = np.zeros(g.shape2())
+    u[1:, :] = -(psi[1:, :] - psi[:-1, :]) / dx
+    v[:, 1:] = (psi[:, 1:] - psi[:, :-1]) / dx
+    u *= (c.au == 1)
+    v *= (c.av == 1)
+    uu = u[None] * f3["hun"].astype(np.float64)
+    vv = v[None] * f3["hvn"].astype(np.float64)
+    uu[0] = 0.0
+    vv[0] = 0.0
+    f3["uu"][...] = uu
+    f3["vv"][...] = vv
+    f2["U"][...] = uu[1:].sum(axis=0)
+    f2["V"][...] = vv[1:].sum(axis=0)
+    xT, yT = (i - g.imin + 0.5) * dx, (j - g.jmin + 0.5) * dx
+    s = sigma_cells * dx
+    blob = np.exp(-((xT[None, :] - 0.3 * g.nx * dx) ** 2 + (yT[:, None] - 0.5 * g.ny * dx) ** 2) / (2 * s * s))
+    wet3 = (c.az >= 1)[None]
+    T = 15.0 + blob[None] + np.zeros(g.shape3())
+    S = np.full(g.shape3(), 35.0)
+    T[0] = 0.0
+    S[0] = 0.0
+    f3["T"][...] = np.where(wet3, T, 0.0)
+    f3["S"][...] = np.where(wet3, S, 0.0)
+    _eqstate(c)
 
 
 def _baroclinic_2d(nx, ny, kmax, recipe, dx, M, dt3, seed, dtype3, land, hmin, hmax, latitude, alloc3, bdy=None):
@@ -172,7 +217,7 @@ def _baroclinic_2d(nx, ny, kmax, recipe, dx, M, dt3, seed, dtype3, land, hmin, h
         x0 = nx / 2 * dx
         H = np.broadcast_to(10.0 + 190.0 * 0.5 * (1.0 + np.tanh((xT - x0) / L)), g.shape2()).copy()
         az[g.interior()] = 1
-    elif recipe == "flat":
+    elif recipe in ("flat", "rotation"):
         H = np.full(g.shape2(), 20.0)
         az[g.interior()] = 1
     elif recipe == "islands":

@@ -111,6 +111,12 @@ int getm_timers_enable(getm_ctx *ctx, int on);
 int getm_timers_reset(getm_ctx *ctx);
 int getm_timers_read(getm_ctx *ctx, int slot, double *total_ms, int64_t *launches);
 const char *getm_timer_name(int slot);
+/* Process-wide choice of the horizontal split-sweep kernels (no counterpart in the reference: a
+ * tuning and testing switch). on != 0 (the default) runs the FP32 sweeps in the vectorised kernels
+ * wherever the rows and levels of the swept fields start on 16-byte boundaries; on == 0 uses the
+ * shared-memory tile sweeps everywhere (FP64 always does). Both give identical results. Returns
+ * the previous setting. */
+int getm_set_vector_sweeps(int on);
 /* Human-readable text of the last error on this context (never NULL). */
 const char *getm_ctx_last_error(const getm_ctx *ctx);
 const char *getm_version(void);
