@@ -11,8 +11,46 @@
 // and needs no atomics.
 #pragma once
 #include "kernels.cuh"
+#include "sweeps_vec.cuh"
 
 namespace gb {
+
+// ---------------------------------------------------------------------------------------------
+// Transposed cell and face operations of a horizontal split sweep, shared by the tile and the
+// vectorised adjoint sweeps so that both round identically.
+//  * adj_cell: the factors of cell (hio, Uhi, Ulo): kc = dt*splitfac*dyf*ard1/hin (the cotangent
+//    of the flux difference per unit cotangent of the new value) and pc = hio/hin (pass-through).
+//  * adj_face: the weights w[0..3] that face fa spreads its flux cotangent Fb over the cells
+//    fa-1, fa, fa+1, fa+2 (frozen limiter branch `code`, optional AH diffusion).
+template <class R>
+__device__ __forceinline__ void adj_cell(R dti, R dyf, R ard1, R kfac, R hio, R Uhi, R Ulo, R& kc, R& pc) {
+  const R dD = dti * (Uhi * dyf - Ulo * dyf) * ard1;
+  const R hin = hio - dD;
+  kc = kfac / hin;
+  pc = hio / hin;
+}
+template <class R, int S>
+__device__ __forceinline__ void adj_face(R Fb, R Uf, R DUf, bool mup, bool mdn, uint8_t code, R dti, R cdx, R dxf,
+                                         R AH, bool use_AH, R (&w)[4]) {
+  const bool pos = Uf > R(0);
+  R A = R(0), B = R(0);
+  if (S != UPSTREAM && (pos ? mup : mdn)) {
+    const R cfl = face_cfl<R>(pos, Uf, DUf, dti, cdx, dxf);
+    recon_coef<R, S>(code, cfl, A, B);
+  }
+  const R FU = Fb * Uf;
+  const R cu = FU * (R(1) + A - B), cuu = -FU * A, cd = FU * B;
+  if (pos) {
+    w[0] = cuu; w[1] = cu; w[2] = cd; w[3] = R(0);
+  } else {
+    w[0] = R(0); w[1] = cd; w[2] = cu; w[3] = cuu;
+  }
+  if (use_AH) {
+    const R ka = Fb * AH * DUf / dxf;
+    w[1] = w[1] + ka;
+    w[2] = w[2] - ka;
+  }
+}
 
 // ---------------------------------------------------------------------------------------------
 // Heights before sweeps 2..5 of u/2 v/2 w v/2 u/2 (the Di/hi updates of adv_split_u/v/w, in the
@@ -52,7 +90,9 @@ __global__ void k_adj_heights(Dev d, R dt, int sub, int has_w, const R* __restri
 // ---------------------------------------------------------------------------------------------
 // Adjoint of the u sweep over a row segment of TU cells, for up to NKB levels (the 2D masks are
 // staged once). Staged per level: U, DU at cells i0-3 .. i0+TU+1, cotangents and heights at cells
-// i0-2 .. i0+TU+1, branch codes of faces i0-2 .. i0+TU.
+// i0-2 .. i0+TU+1, branch codes of faces i0-2 .. i0+TU. Levels are double-buffered: the cp.async
+// copies (and the code bytes, through registers) of level k+1 are issued before level k is
+// computed.
 template <class R, int S>
 __global__ void __launch_bounds__(TU) k_adj_sweep_u(Dev d, R dt, R splitfac, R AH, int nk, bool copy0,
                                                     const R* __restrict__ gbar, R* __restrict__ fbar,
@@ -60,7 +100,9 @@ __global__ void __launch_bounds__(TU) k_adj_sweep_u(Dev d, R dt, R splitfac, R A
                                                     const R* __restrict__ DU, const uint8_t* __restrict__ mflux,
                                                     const uint8_t* __restrict__ mupd,
                                                     const uint8_t* __restrict__ code) {
-  __shared__ R sU[TU + 5], sDU[TU + 5];
+  __shared__ R sU[2][TU + 5], sDU[2][TU + 5];
+  __shared__ R sG[2][TU + 4], sD[2][TU + 4];
+  __shared__ uint8_t scd[2][TU + 3];
   __shared__ uint8_t sm[TU + 5], su[TU + 4];
   __shared__ R sg[TU + 4], skc[TU + 4], spc[TU + 4];
   __shared__ R sw[4][TU + 3];
@@ -84,32 +126,61 @@ __global__ void __launch_bounds__(TU) k_adj_sweep_u(Dev d, R dt, R splitfac, R A
     const int ii = ii0 - 2 + q;
     su[q] = (ii >= 0 && ii < ni && ii >= 1 + sub && ii <= ni - 2 - sub) ? mupd[crow + ii] : 0;
   }
+  __syncthreads();  // su is read by the staging below
   // level 0 (below the level pointers' origin) is not touched by the sweep: its cotangent passes
   if (copy0 && blockIdx.z == 0 && ii0 + t < ni) fbar[crow - d.sk + ii0 + t] = gbar[crow - d.sk + ii0 + t];
-  for (int k = k0; k < k1; ++k) {
+  auto stage = [&](int k, int b) {
     const long long row = crow + (long long)k * d.sk;
     for (int q = t; q < TU + 5; q += TU) {
       const int ii = ii0 - 3 + q;
-      const bool ok = ii >= 0 && ii < ni;
-      sU[q] = ok ? U[row + ii] : R(0);
-      sDU[q] = ok ? DU[row + ii] : R(0);
+      if (ii >= 0 && ii < ni) {
+        cp_async(&sU[b][q], U + row + ii);
+        cp_async(&sDU[b][q], DU + row + ii);
+      } else {
+        sU[b][q] = R(0);
+        sDU[b][q] = R(0);
+      }
+    }
+    for (int q = t; q < TU + 4; q += TU) {
+      const int ii = ii0 - 2 + q;
+      if (ii >= 0 && ii < ni) {
+        cp_async(&sG[b][q], gbar + row + ii);
+        if (su[q]) cp_async(&sD[b][q], Dio + row + ii);
+      } else {
+        sG[b][q] = R(0);
+      }
+    }
+    cp_async_commit();
+  };
+  // code bytes of the faces r = t and r = t + TU (t < 3) of a level, through registers
+  auto codes = [&](int k, uint8_t& c0, uint8_t& c1) {
+    const long long row = crow + (long long)k * d.sk;
+    const int fa0 = ii0 - 2 + t, fa1 = fa0 + TU;
+    c0 = (S != UPSTREAM && fa0 >= 0 && fa0 < ni) ? code[row + fa0] : 0;
+    c1 = (S != UPSTREAM && t < 3 && fa1 < ni) ? code[row + fa1] : 0;
+  };
+  uint8_t cn0 = 0, cn1 = 0;
+  if (k0 < k1) {
+    stage(k0, 0);
+    codes(k0, cn0, cn1);
+    scd[0][t] = cn0;
+    if (t < 3) scd[0][TU + t] = cn1;
+  }
+  for (int k = k0, b = 0; k < k1; ++k, b ^= 1) {
+    const long long row = crow + (long long)k * d.sk;
+    if (k + 1 < k1) {
+      stage(k + 1, b ^ 1);
+      codes(k + 1, cn0, cn1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
     __syncthreads();
     // cells q <-> ii = ii0-2+q; U of its east face = sU[q+1], of its west face = sU[q]
     for (int q = t; q < TU + 4; q += TU) {
-      const int ii = ii0 - 2 + q;
-      R g = R(0), kc = R(0), pc = R(1);
-      if (ii >= 0 && ii < ni) {
-        g = gbar[row + ii];
-        if (su[q]) {
-          const R hio = Dio[row + ii];
-          const R dD = dti * (sU[q + 1] * dyf - sU[q] * dyf) * ard1;
-          const R hin = hio - dD;
-          kc = kfac / hin;
-          pc = hio / hin;
-        }
-      }
-      sg[q] = g;
+      R kc = R(0), pc = R(1);
+      if (su[q]) adj_cell<R>(dti, dyf, ard1, kfac, sD[b][q], sU[b][q + 1], sU[b][q], kc, pc);
+      sg[q] = sG[b][q];
       skc[q] = kc;
       spc[q] = pc;
     }
@@ -117,43 +188,31 @@ __global__ void __launch_bounds__(TU) k_adj_sweep_u(Dev d, R dt, R splitfac, R A
     // faces r <-> fa = ii0-2+r (between cells fa and fa+1); U index r+1, cells r and r+1
     for (int r = t; r < TU + 3; r += TU) {
       const int fa = ii0 - 2 + r;
-      R wm1 = R(0), w0 = R(0), w1 = R(0), w2 = R(0);
+      R w[4] = {R(0), R(0), R(0), R(0)};
       if (fa >= sub && fa <= ni - 2 - sub && sm[r + 1]) {
         const R Fb = -sg[r] * skc[r] + sg[r + 1] * skc[r + 1];
-        const R Uf = sU[r + 1], DUf = sDU[r + 1];
-        const bool pos = Uf > R(0);
-        R A = R(0), B = R(0);
-        if (S != UPSTREAM && (pos ? sm[r] : sm[r + 2])) {
-          const R cfl = face_cfl<R>(pos, Uf, DUf, dti, cdx, dxf);
-          recon_coef<R, S>(code[row + fa], cfl, A, B);
-        }
-        const R FU = Fb * Uf;
-        const R cu = FU * (R(1) + A - B), cuu = -FU * A, cd = FU * B;
-        if (pos) {
-          wm1 = cuu; w0 = cu; w1 = cd;
-        } else {
-          w0 = cd; w1 = cu; w2 = cuu;
-        }
-        if (use_AH) {
-          const R ka = Fb * AH * DUf / dxf;
-          w0 = w0 + ka;
-          w1 = w1 - ka;
-        }
+        adj_face<R, S>(Fb, sU[b][r + 1], sDU[b][r + 1], sm[r] != 0, sm[r + 2] != 0, scd[b][r], dti, cdx, dxf, AH,
+                       use_AH, w);
       }
-      sw[0][r] = wm1;
-      sw[1][r] = w0;
-      sw[2][r] = w1;
-      sw[3][r] = w2;
+      sw[0][r] = w[0];
+      sw[1][r] = w[1];
+      sw[2][r] = w[2];
+      sw[3][r] = w[3];
     }
     __syncthreads();
     const int ii = ii0 + t;
     // cell ii: q = t+2; faces ii+1, ii, ii-1, ii-2 <-> r = t+3, t+2, t+1, t
     if (ii < ni) fbar[row + ii] = sg[t + 2] * spc[t + 2] + sw[0][t + 3] + sw[1][t + 2] + sw[2][t + 1] + sw[3][t];
+    if (k + 1 < k1) {  // the codes of level k+1 (buffer b^1 was last read before this level's barriers)
+      scd[b ^ 1][t] = cn0;
+      if (t < 3) scd[b ^ 1][TU + t] = cn1;
+    }
     __syncthreads();
   }
 }
 
-// Adjoint of the v sweep over a tile of TVX x TVY cells, for up to NKB levels.
+// Adjoint of the v sweep over a tile of TVX x TVY cells, for up to NKB levels, double-buffered
+// like the u sweep.
 template <class R, int S>
 __global__ void __launch_bounds__(TVX * TVY) k_adj_sweep_v(Dev d, R dt, R splitfac, R AH, int nk, bool copy0,
                                                            const R* __restrict__ gbar, R* __restrict__ fbar,
@@ -162,7 +221,9 @@ __global__ void __launch_bounds__(TVX * TVY) k_adj_sweep_v(Dev d, R dt, R splitf
                                                            const uint8_t* __restrict__ mflux,
                                                            const uint8_t* __restrict__ mupd,
                                                            const uint8_t* __restrict__ code) {
-  __shared__ R sV[TVY + 5][TVX], sDV[TVY + 5][TVX];
+  __shared__ R sV[2][TVY + 5][TVX], sDV[2][TVY + 5][TVX];
+  __shared__ R sG[2][TVY + 4][TVX], sD[2][TVY + 4][TVX];
+  __shared__ uint8_t scd[2][TVY + 3][TVX];
   __shared__ uint8_t sm[TVY + 5][TVX], su[TVY + 4][TVX];
   __shared__ R sg[TVY + 4][TVX], skc[TVY + 4][TVX], spc[TVY + 4][TVX];
   __shared__ R sw[4][TVY + 3][TVX];
@@ -194,72 +255,449 @@ __global__ void __launch_bounds__(TVX * TVY) k_adj_sweep_v(Dev d, R dt, R splitf
     const long long c0 = (long long)(jj0 + ty) * sj + ii - d.sk;
     fbar[c0] = gbar[c0];
   }
-  for (int k = k0; k < k1; ++k) {
+  auto stage = [&](int k, int b) {
     const long long lev = (long long)k * d.sk;
     for (int q = ty; q < TVY + 5; q += TVY) {
       const int jj = jj0 - 3 + q;
-      const bool ok = iok && jj >= 0 && jj < nj;
-      const long long c = lev + (long long)jj * sj + ii;
-      sV[q][tx] = ok ? V[c] : R(0);
-      sDV[q][tx] = ok ? DV[c] : R(0);
+      if (iok && jj >= 0 && jj < nj) {
+        const long long c = lev + (long long)jj * sj + ii;
+        cp_async(&sV[b][q][tx], V + c);
+        cp_async(&sDV[b][q][tx], DV + c);
+      } else {
+        sV[b][q][tx] = R(0);
+        sDV[b][q][tx] = R(0);
+      }
+    }
+    for (int q = ty; q < TVY + 4; q += TVY) {
+      const int jj = jj0 - 2 + q;
+      if (iok && jj >= 0 && jj < nj) {
+        const long long c = lev + (long long)jj * sj + ii;
+        cp_async(&sG[b][q][tx], gbar + c);
+        if (su[q][tx]) cp_async(&sD[b][q][tx], Dio + c);
+      } else {
+        sG[b][q][tx] = R(0);
+      }
+    }
+    cp_async_commit();
+  };
+  // code bytes of the face rows r = ty and r = ty + TVY (ty < 3) of a level, through registers
+  auto codes = [&](int k, uint8_t& c0, uint8_t& c1) {
+    const long long lev = (long long)k * d.sk;
+    const int fa0 = jj0 - 2 + ty, fa1 = fa0 + TVY;
+    c0 = (S != UPSTREAM && iok && fa0 >= 0 && fa0 < nj) ? code[lev + (long long)fa0 * sj + ii] : 0;
+    c1 = (S != UPSTREAM && iok && ty < 3 && fa1 < nj) ? code[lev + (long long)fa1 * sj + ii] : 0;
+  };
+  uint8_t cn0 = 0, cn1 = 0;
+  if (k0 < k1) {
+    stage(k0, 0);
+    codes(k0, cn0, cn1);
+    scd[0][ty][tx] = cn0;
+    if (ty < 3) scd[0][TVY + ty][tx] = cn1;
+  }
+  for (int k = k0, b = 0; k < k1; ++k, b ^= 1) {
+    const long long lev = (long long)k * d.sk;
+    if (k + 1 < k1) {
+      stage(k + 1, b ^ 1);
+      codes(k + 1, cn0, cn1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
     __syncthreads();
     for (int q = ty; q < TVY + 4; q += TVY) {
-      const int jj = jj0 - 2 + q;
-      R g = R(0), kc = R(0), pc = R(1);
-      if (iok && jj >= 0 && jj < nj) {
-        const long long c = lev + (long long)jj * sj + ii;
-        g = gbar[c];
-        if (su[q][tx]) {
-          const R hio = Dio[c];
-          const R dD = dti * (sV[q + 1][tx] * dyf - sV[q][tx] * dyf) * ard1;
-          const R hin = hio - dD;
-          kc = kfac / hin;
-          pc = hio / hin;
-        }
-      }
-      sg[q][tx] = g;
+      R kc = R(0), pc = R(1);
+      if (su[q][tx]) adj_cell<R>(dti, dyf, ard1, kfac, sD[b][q][tx], sV[b][q + 1][tx], sV[b][q][tx], kc, pc);
+      sg[q][tx] = sG[b][q][tx];
       skc[q][tx] = kc;
       spc[q][tx] = pc;
     }
     __syncthreads();
     for (int r = ty; r < TVY + 3; r += TVY) {
       const int fa = jj0 - 2 + r;
-      R wm1 = R(0), w0 = R(0), w1 = R(0), w2 = R(0);
+      R w[4] = {R(0), R(0), R(0), R(0)};
       if (iok && fa >= sub && fa <= nj - 2 - sub && sm[r + 1][tx]) {
         const R Fb = -sg[r][tx] * skc[r][tx] + sg[r + 1][tx] * skc[r + 1][tx];
-        const R Vf = sV[r + 1][tx], DVf = sDV[r + 1][tx];
-        const bool pos = Vf > R(0);
-        R A = R(0), B = R(0);
-        if (S != UPSTREAM && (pos ? sm[r][tx] : sm[r + 2][tx])) {
-          const R cfl = face_cfl<R>(pos, Vf, DVf, dti, cdx, dxf);
-          recon_coef<R, S>(code[lev + (long long)fa * sj + ii], cfl, A, B);
-        }
-        const R FV = Fb * Vf;
-        const R cu = FV * (R(1) + A - B), cuu = -FV * A, cd = FV * B;
-        if (pos) {
-          wm1 = cuu; w0 = cu; w1 = cd;
-        } else {
-          w0 = cd; w1 = cu; w2 = cuu;
-        }
-        if (use_AH) {
-          const R ka = Fb * AH * DVf / dxf;
-          w0 = w0 + ka;
-          w1 = w1 - ka;
-        }
+        adj_face<R, S>(Fb, sV[b][r + 1][tx], sDV[b][r + 1][tx], sm[r][tx] != 0, sm[r + 2][tx] != 0, scd[b][r][tx],
+                       dti, cdx, dxf, AH, use_AH, w);
       }
-      sw[0][r][tx] = wm1;
-      sw[1][r][tx] = w0;
-      sw[2][r][tx] = w1;
-      sw[3][r][tx] = w2;
+      sw[0][r][tx] = w[0];
+      sw[1][r][tx] = w[1];
+      sw[2][r][tx] = w[2];
+      sw[3][r][tx] = w[3];
     }
     __syncthreads();
     const int jj = jj0 + ty;
     if (iok && jj < nj)
       fbar[lev + (long long)jj * sj + ii] = sg[ty + 2][tx] * spc[ty + 2][tx] + sw[0][ty + 3][tx] +
                                             sw[1][ty + 2][tx] + sw[2][ty + 1][tx] + sw[3][ty][tx];
+    if (k + 1 < k1) {
+      scd[b ^ 1][ty][tx] = cn0;
+      if (ty < 3) scd[b ^ 1][TVY + ty][tx] = cn1;
+    }
     __syncthreads();
   }
+}
+
+// Vectorised adjoint of the u sweep (FP32, 16-byte aligned layouts): the lane layout of
+// k_sweep_u_vec -- a warp covers 32 float4 vectors of a row and lanes 1..30 own their cells. A
+// lane computes the factors of its cells and the weights of their left faces c0-1 .. c0+N-2; the
+// gather of a cell takes the weights of faces c+1, c, c-1, c-2, the outer ones by shuffles from
+// the neighbouring lanes. Levels are staged two ahead by cp.async like the forward sweep.
+template <class R, int S>
+__global__ void __launch_bounds__(32 * UWB) k_adj_sweep_u_vec(Dev d, R dt, R splitfac, R AH, int nk, bool copy0,
+                                                            const R* __restrict__ gbar, R* __restrict__ fbar,
+                                                            const R* __restrict__ Dio, const R* __restrict__ U,
+                                                            const R* __restrict__ DU,
+                                                            const uint8_t* __restrict__ mflux,
+                                                            const uint8_t* __restrict__ mupd,
+                                                            const uint8_t* __restrict__ code) {
+  static_assert(sizeof(R) == 4, "vectorised adjoint sweeps are FP32");
+  constexpr int N = 4;
+  constexpr int NA = 5;  // gbar, Dio, U, DU, codes
+  constexpr int sub = (S == UPSTREAM) ? 0 : 1;
+  constexpr unsigned FULL = 0xffffffffu;
+  __shared__ VecPack<R, N> sbuf[VST][NA][32 * UWB];
+  const int lane = threadIdx.x;
+  const int tid = threadIdx.y * 32 + lane;
+  const int ni = d.ni();
+  const int seg = blockIdx.x * UWB + threadIdx.y;
+  const int s0 = seg * UOWN * N;
+  if (s0 >= ni) return;  // whole warp (no barrier in this kernel)
+  const int c0 = s0 + (lane - 1) * N;
+  const bool act = c0 >= 0 && c0 < ni;
+  const int navail = ni - c0;
+  const bool full = act && navail >= N;
+  const int vbytes = act ? (full ? N : navail) * (int)sizeof(R) : 0;
+  const bool own = act && lane >= 1 && lane <= UOWN;
+  const long long crow = (long long)blockIdx.y * d.sj;
+  const int k0 = blockIdx.z * NKB;
+  const int k1 = min(k0 + NKB, nk);
+  const long long cc = act ? c0 : 0;
+  const R dti = splitfac * dt;
+  const R dxf = R(d.dx), dyf = R(d.dy), ard1 = R(d.ard1);
+  const R cdx = dti / dxf;
+  const bool use_AH = AH > R(0);
+  const R kfac = dt * splitfac * dyf * ard1;
+  // masks: flux masks of cells c0-2 .. c0+N-1, update masks of the lane's cells
+  uint32_t mfw = 0, muw = 0;
+  if (act) {
+    mfw = ld_mask_w<N>(mflux + crow + c0, full, navail);
+    muw = ld_mask_w<N>(mupd + crow + c0, full, navail);
+  }
+  const uint32_t mfl = __shfl_up_sync(FULL, mfw, 1);
+  bool mfx[N + 2], su[N];
+  mfx[0] = mbit(mfl, N - 2);
+  mfx[1] = mbit(mfl, N - 1);
+#pragma unroll
+  for (int m = 0; m < N; ++m) {
+    mfx[m + 2] = mbit(mfw, m);
+    const int c = c0 + m;
+    su[m] = act && m < navail && mbit(muw, m) && c >= 1 + sub && c <= ni - 2 - sub;
+  }
+  if (copy0 && blockIdx.z == 0 && own) {  // level 0 passes (not touched by the sweep)
+    R v[N];
+    ld_row<R, N>(gbar + crow - d.sk + c0, full, navail, v);
+    st_row<R, N>(fbar + crow - d.sk + c0, full, navail, v);
+  }
+  auto issue = [&](int k, int st) {
+    if (k < k1) {
+      const long long p = crow + (long long)k * d.sk + cc;
+      cp_async16(&sbuf[st][0][tid], gbar + p, vbytes);
+      cp_async16(&sbuf[st][1][tid], Dio + p, vbytes);
+      cp_async16(&sbuf[st][2][tid], U + p, vbytes);
+      cp_async16(&sbuf[st][3][tid], DU + p, vbytes);
+      if (S != UPSTREAM) {
+        const int cb = act ? (full ? N : navail) : 0;
+        if (cb == N) cp_async(reinterpret_cast<float*>(&sbuf[st][4][tid]), reinterpret_cast<const float*>(code + p));
+      }
+    }
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int q = 0; q < VST - 1; ++q) issue(k0 + q, q);
+  int st = 0;
+  for (int k = k0; k < k1; ++k) {
+    issue(k + VST - 1, st == 0 ? VST - 1 : st - 1);
+    cp_async_wait<VST - 1>();
+    const long long p = crow + (long long)k * d.sk + c0;
+    R g[N], hio[N], u[N], du[N];
+    lds_vec<R, N>(sbuf[st][0][tid], g);
+    lds_vec<R, N>(sbuf[st][1][tid], hio);
+    lds_vec<R, N>(sbuf[st][2][tid], u);
+    lds_vec<R, N>(sbuf[st][3][tid], du);
+    uint32_t cw = 0;
+    if (S != UPSTREAM) {
+      if (full) {
+        cw = *reinterpret_cast<const uint32_t*>(&sbuf[st][4][tid]);
+      } else if (act) {
+#pragma unroll
+        for (int m = 0; m < N; ++m)
+          if (m < navail) cw |= (uint32_t)code[p + m] << (8 * m);
+      }
+    }
+    st = st == VST - 1 ? 0 : st + 1;
+    const R uL = __shfl_up_sync(FULL, u[N - 1], 1);
+    // cell factors
+    R kc[N + 1], pc[N], gg[N + 1];  // index m+1 = cell c0+m; index 0 = cell c0-1 (left lane)
+#pragma unroll
+    for (int m = 0; m < N; ++m) {
+      R kcm = R(0), pcm = R(1);
+      if (su[m]) adj_cell<R>(dti, dyf, ard1, kfac, hio[m], u[m], m == 0 ? uL : u[m - 1], kcm, pcm);
+      kc[m + 1] = kcm;
+      pc[m] = pcm;
+      gg[m + 1] = g[m];
+    }
+    kc[0] = __shfl_up_sync(FULL, kc[N], 1);
+    gg[0] = __shfl_up_sync(FULL, gg[N], 1);
+    const uint32_t cl = __shfl_up_sync(FULL, cw, 1);
+    const R duL = __shfl_up_sync(FULL, du[N - 1], 1);
+    // weights of the left faces fa = c0+m-1 (cells fa, fa+1 = index m, m+1)
+    R w[N][4];
+#pragma unroll
+    for (int m = 0; m < N; ++m) {
+      const int fa = c0 + m - 1;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) w[m][q] = R(0);
+      if (act && fa >= sub && fa <= ni - 2 - sub && mfx[m + 1]) {
+        const R Fb = -gg[m] * kc[m] + gg[m + 1] * kc[m + 1];
+        const uint8_t cd = (uint8_t)((m == 0 ? (cl >> (8 * (N - 1))) : (cw >> (8 * (m - 1)))) & 0xffu);
+        adj_face<R, S>(Fb, m == 0 ? uL : u[m - 1], m == 0 ? duL : du[m - 1], mfx[m], mfx[m + 2], cd, dti, cdx, dxf,
+                       AH, use_AH, w[m]);
+      }
+    }
+    // neighbours' weights: wm1 of the next lane's faces 0 and 1, w0 of its face 0, w2 of the
+    // previous lane's last face
+    const R nm0 = __shfl_down_sync(FULL, w[0][0], 1), nm1 = __shfl_down_sync(FULL, w[1][0], 1);
+    const R n00 = __shfl_down_sync(FULL, w[0][1], 1);
+    const R p2 = __shfl_up_sync(FULL, w[N - 1][3], 1);
+    if (!own) continue;
+    R out[N];
+#pragma unroll
+    for (int m = 0; m < N; ++m) {
+      // faces c+1 (left face index m+2), c (m+1), c-1 (m), c-2 (m-1)
+      const R a = m + 2 < N ? w[m + 2][0] : (m + 2 == N ? nm0 : nm1);
+      const R b = m + 1 < N ? w[m + 1][1] : n00;
+      const R e = w[m][2];
+      const R f = m >= 1 ? w[m - 1][3] : p2;
+      out[m] = g[m] * pc[m] + a + b + e + f;
+    }
+    st_row<R, N>(fbar + p, full, navail, out);
+  }
+  cp_async_wait<0>();
+}
+
+// Vectorised adjoint of the v sweep (FP32, 16-byte aligned layouts): the lane layout of
+// k_sweep_v_vec -- a lane owns 4 cells along i and marches `rows` rows in j of one level. At row
+// step j it forms the factors of row j+2 and the weights of face j+1, and completes cell j from
+// the weights of faces j+1, j, j-1, j-2 kept in registers. Rows are staged two steps ahead by
+// cp.async.
+template <class R, int S>
+__global__ void __launch_bounds__(32 * VKW) k_adj_sweep_v_vec(Dev d, R dt, R splitfac, R AH, int nk, int rows,
+                                                            bool copy0, const R* __restrict__ gbar,
+                                                            R* __restrict__ fbar, const R* __restrict__ Dio,
+                                                            const R* __restrict__ V, const R* __restrict__ DV,
+                                                            const uint8_t* __restrict__ mflux,
+                                                            const uint8_t* __restrict__ mupd,
+                                                            const uint8_t* __restrict__ code) {
+  static_assert(sizeof(R) == 4, "vectorised adjoint sweeps are FP32");
+  constexpr int N = 4;
+  constexpr int NA = 5;  // gbar(j+2), Dio(j+2), V(j+2), DV(j+1), codes(j+1)
+  constexpr int sub = (S == UPSTREAM) ? 0 : 1;
+  __shared__ VecPack<R, N> sbuf[VST][NA][32 * VKW];
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  const int ni = d.ni(), nj = d.nj();
+  const int c0 = (blockIdx.x * 32 + threadIdx.x) * N;
+  const int k = blockIdx.z * VKW + threadIdx.y;
+  if (c0 >= ni || k >= nk) return;  // no barrier in this kernel
+  const int navail = ni - c0;
+  const bool full = navail >= N;
+  const int vbytes = (full ? N : navail) * (int)sizeof(R);
+  const int j0 = blockIdx.y * rows;
+  const int j1 = min(j0 + rows, nj);
+  const long long sj = d.sj;
+  const long long base = (long long)k * d.sk + c0;
+  const R dti = splitfac * dt;
+  const R dxf = R(d.dy), dyf = R(d.dx), ard1 = R(d.ard1);  // DYV, DXV
+  const R cdx = dti / dxf;
+  const bool use_AH = AH > R(0);
+  const R kfac = dt * splitfac * dyf * ard1;
+  if (copy0 && k == 0) {  // level 0 passes (not touched by the sweep)
+    for (int j = j0; j < j1; ++j) {
+      R v[N];
+      ld_row<R, N>(gbar + base - d.sk + (long long)j * sj, full, navail, v);
+      st_row<R, N>(fbar + base - d.sk + (long long)j * sj, full, navail, v);
+    }
+  }
+  auto rowv = [&](const R* a, int j, R (&v)[N]) {
+    if (j < 0 || j >= nj) {
+#pragma unroll
+      for (int m = 0; m < N; ++m) v[m] = R(0);
+    } else {
+      ld_row<R, N>(a + base + (long long)j * sj, full, navail, v);
+    }
+  };
+  auto mrow = [&](const uint8_t* a, int j) -> uint32_t {
+    return (j < 0 || j >= nj) ? 0u : ld_mask_w<N>(a + (long long)j * sj + c0, full, navail);
+  };
+  auto crow_of = [&](int j) -> uint32_t {  // code bytes of face row j
+    if (S == UPSTREAM || j < 0 || j >= nj) return 0u;
+    const uint8_t* p = code + base + (long long)j * sj;
+    if (full) return *reinterpret_cast<const uint32_t*>(p);
+    uint32_t x = 0;
+    for (int m = 0; m < navail; ++m) x |= (uint32_t)p[m] << (8 * m);
+    return x;
+  };
+  // factors of row r from its cotangent, heights and the transports of its faces
+  auto factors = [&](int r, const R (&g)[N], const R (&hio)[N], const R (&Vr)[N], const R (&Vrm1)[N],
+                     uint32_t mu, R (&kc)[N], R (&pc)[N]) {
+    const bool rin = r >= 1 + sub && r <= nj - 2 - sub;
+#pragma unroll
+    for (int m = 0; m < N; ++m) {
+      kc[m] = R(0);
+      pc[m] = R(1);
+      if (rin && mbit(mu, m)) adj_cell<R>(dti, dyf, ard1, kfac, hio[m], Vr[m], Vrm1[m], kc[m], pc[m]);
+    }
+    (void)g;
+  };
+  // weights of face f from the factors of rows f, f+1 and its transport, masks and branch codes
+  auto face = [&](int f, const R (&ga)[N], const R (&ka)[N], const R (&gb)[N], const R (&kb)[N], const R (&Vf)[N],
+                  const R (&DVf)[N], uint32_t mdn_m1, uint32_t m0, uint32_t mp1, uint32_t cw, R (&w)[4][N]) {
+    const bool fin = f >= sub && f <= nj - 2 - sub;
+#pragma unroll
+    for (int m = 0; m < N; ++m) {
+      R ww[4] = {R(0), R(0), R(0), R(0)};
+      if (fin && mbit(m0, m)) {
+        const R Fb = -ga[m] * ka[m] + gb[m] * kb[m];
+        adj_face<R, S>(Fb, Vf[m], DVf[m], mbit(mdn_m1, m), mbit(mp1, m), (uint8_t)((cw >> (8 * m)) & 0xffu), dti,
+                       cdx, dxf, AH, use_AH, ww);
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) w[q][m] = ww[q];
+    }
+  };
+  auto issue = [&](int j, int st) {
+    if (j < j1) {
+      const long long p = base + (long long)j * sj;
+      const bool r2 = j + 2 < nj;
+      cp_async16(&sbuf[st][0][tid], r2 ? gbar + p + 2 * sj : gbar + p, r2 ? vbytes : 0);
+      cp_async16(&sbuf[st][1][tid], r2 ? Dio + p + 2 * sj : Dio + p, r2 ? vbytes : 0);
+      cp_async16(&sbuf[st][2][tid], r2 ? V + p + 2 * sj : V + p, r2 ? vbytes : 0);
+      const bool r1 = j + 1 < nj;
+      cp_async16(&sbuf[st][3][tid], r1 ? DV + p + sj : DV + p, r1 ? vbytes : 0);
+      if (S != UPSTREAM && full && r1)
+        cp_async(reinterpret_cast<float*>(&sbuf[st][4][tid]), reinterpret_cast<const float*>(code + p + sj));
+    }
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int q = 0; q < VST - 1; ++q) issue(j0 + q, q);
+  // prologue: factors of rows j0-2 .. j0+1, weights of faces j0-2, j0-1, j0
+  R gA[N], kA[N], pA[N];  // row j0-2, then reused
+  R gB[N], kB[N], pB[N];  // row j0-1
+  R gC[N], kC[N], pC[N];  // row j0   (the window: rows j, j+1 after the prologue)
+  R gD[N], kD[N], pD[N];  // row j0+1
+  R Vprev[N];             // V of row j0+1 (the south face of row j0+2)
+  uint32_t mfw[4];        // flux masks of rows j0-3 .. j0 (face f uses rows f-1, f, f+1)
+  {
+    R Vm3[N], Vm2[N], Vm1[N], V0[N], hio[N];
+    rowv(V, j0 - 3, Vm3);
+    rowv(V, j0 - 2, Vm2);
+    rowv(V, j0 - 1, Vm1);
+    rowv(V, j0, V0);
+    rowv(V, j0 + 1, Vprev);
+    rowv(gbar, j0 - 2, gA);
+    rowv(Dio, j0 - 2, hio);
+    factors(j0 - 2, gA, hio, Vm2, Vm3, mrow(mupd, j0 - 2), kA, pA);
+    rowv(gbar, j0 - 1, gB);
+    rowv(Dio, j0 - 1, hio);
+    factors(j0 - 1, gB, hio, Vm1, Vm2, mrow(mupd, j0 - 1), kB, pB);
+    rowv(gbar, j0, gC);
+    rowv(Dio, j0, hio);
+    factors(j0, gC, hio, V0, Vm1, mrow(mupd, j0), kC, pC);
+    rowv(gbar, j0 + 1, gD);
+    rowv(Dio, j0 + 1, hio);
+    factors(j0 + 1, gD, hio, Vprev, V0, mrow(mupd, j0 + 1), kD, pD);
+    mfw[0] = mrow(mflux, j0 - 3);
+    mfw[1] = mrow(mflux, j0 - 2);
+    mfw[2] = mrow(mflux, j0 - 1);
+    mfw[3] = mrow(mflux, j0);
+    R DVr[N], w[4][N];
+    // face j0-2: rows j0-2 (A), j0-1 (B)
+    rowv(DV, j0 - 2, DVr);
+    face(j0 - 2, gA, kA, gB, kB, Vm2, DVr, mfw[0], mfw[1], mfw[2], crow_of(j0 - 2), w);
+    R s3a[N];
+#pragma unroll
+    for (int m = 0; m < N; ++m) s3a[m] = w[3][m];
+    // face j0-1: rows j0-1 (B), j0 (C)
+    rowv(DV, j0 - 1, DVr);
+    face(j0 - 1, gB, kB, gC, kC, Vm1, DVr, mfw[1], mfw[2], mfw[3], crow_of(j0 - 1), w);
+    R s2a[N], s3b[N];
+#pragma unroll
+    for (int m = 0; m < N; ++m) {
+      s2a[m] = w[2][m];
+      s3b[m] = w[3][m];
+    }
+    // face j0: rows j0 (C), j0+1 (D)
+    const uint32_t mf1 = mrow(mflux, j0 + 1);
+    rowv(DV, j0, DVr);
+    face(j0, gC, kC, gD, kD, V0, DVr, mfw[2], mfw[3], mf1, crow_of(j0), w);
+    R s1[N], s2b[N], s3c[N];
+#pragma unroll
+    for (int m = 0; m < N; ++m) {
+      s1[m] = w[1][m];
+      s2b[m] = w[2][m];
+      s3c[m] = w[3][m];
+    }
+    // masks for the loop: face j+1 uses flux rows j, j+1, j+2; the factors of row j+2 its update mask
+    uint32_t fm0 = mfw[3], fm1 = mf1;
+    uint32_t mfn = mrow(mflux, j0 + 2), mun = mrow(mupd, j0 + 2);
+    int st = 0;
+    for (int j = j0; j < j1; ++j) {
+      issue(j + VST - 1, st == 0 ? VST - 1 : st - 1);
+      const uint32_t fm2 = mfn, mu2 = mun;
+      if (j + 1 < j1) {
+        mfn = mrow(mflux, j + 3);
+        mun = mrow(mupd, j + 3);
+      }
+      cp_async_wait<VST - 1>();
+      R gE[N], hE[N], VE[N], DVj1[N];
+      lds_vec<R, N>(sbuf[st][0][tid], gE);
+      lds_vec<R, N>(sbuf[st][1][tid], hE);
+      lds_vec<R, N>(sbuf[st][2][tid], VE);
+      lds_vec<R, N>(sbuf[st][3][tid], DVj1);
+      uint32_t cw = 0;
+      if (S != UPSTREAM && j + 1 < nj) {
+        if (full) cw = *reinterpret_cast<const uint32_t*>(&sbuf[st][4][tid]);
+        else cw = crow_of(j + 1);
+      }
+      st = st == VST - 1 ? 0 : st + 1;
+      // factors of row j+2 (its south face is V(j+1) = Vprev)
+      R kE[N], pE[N];
+      factors(j + 2, gE, hE, VE, Vprev, mu2, kE, pE);
+      // face j+1: rows j+1 (D), j+2 (E)
+      face(j + 1, gD, kD, gE, kE, Vprev, DVj1, fm0, fm1, fm2, cw, w);
+      R out[N];
+#pragma unroll
+      for (int m = 0; m < N; ++m) out[m] = gC[m] * pC[m] + w[0][m] + s1[m] + s2a[m] + s3a[m];
+      st_row<R, N>(fbar + base + (long long)j * sj, full, navail, out);
+#pragma unroll
+      for (int m = 0; m < N; ++m) {
+        s1[m] = w[1][m];
+        s2a[m] = s2b[m];
+        s2b[m] = w[2][m];
+        s3a[m] = s3b[m];
+        s3b[m] = s3c[m];
+        s3c[m] = w[3][m];
+        gC[m] = gD[m]; kC[m] = kD[m]; pC[m] = pD[m];
+        gD[m] = gE[m]; kD[m] = kE[m]; pD[m] = pE[m];
+        Vprev[m] = VE[m];
+      }
+      fm0 = fm1;
+      fm1 = fm2;
+    }
+  }
+  cp_async_wait<0>();
+  (void)gA; (void)kA; (void)pA; (void)gB; (void)kB; (void)pB;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -468,6 +906,28 @@ int run_adj_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int 
   return dispatch_scheme(scheme, [&](auto sc) {
     constexpr int S = decltype(sc)::value;
     const int nz = (nk + NKB - 1) / NKB;
+    if constexpr (sizeof(R) == 4) {
+      if (DIR == 0 && vec_layout<R>(d, nk + (copy0 ? 1 : 0), {gbar, fbar, Dio, U, DU}, {mflux, mupd, code})) {
+        constexpr int N = 4;
+        const int nseg = (d.ni() + UOWN * N - 1) / (UOWN * N);
+        dim3 blk(32, UWB, 1);
+        dim3 grd((nseg + UWB - 1) / UWB, d.nj(), nz);
+        k_adj_sweep_u_vec<R, S><<<grd, blk, 0, s>>>(d, dt, splitfac, AH, nk, copy0, gbar, fbar, Dio, U, DU, mflux,
+                                                    mupd, code);
+        return (int)cudaGetLastError();
+      }
+      if (DIR == 1 && vec_layout<R>(d, nk + (copy0 ? 1 : 0), {gbar, fbar, Dio, U, DU}, {mflux, mupd, code})) {
+        constexpr int N = 4;
+        const long long nx = (d.ni() + 32 * N - 1) / (32 * N), nzv = (nk + VKW - 1) / VKW;
+        int rows = VJS;
+        while (rows > 8 && nx * ((d.nj() + rows - 1) / rows) * nzv * VKW < 148LL * 24) rows /= 2;
+        dim3 blk(32, VKW, 1);
+        dim3 grd((unsigned)nx, (d.nj() + rows - 1) / rows, (unsigned)nzv);
+        k_adj_sweep_v_vec<R, S><<<grd, blk, 0, s>>>(d, dt, splitfac, AH, nk, rows, copy0, gbar, fbar, Dio, U, DU,
+                                                    mflux, mupd, code);
+        return (int)cudaGetLastError();
+      }
+    }
     if (DIR == 0) {
       dim3 grd((d.ni() + TU - 1) / TU, d.nj(), nz);
       k_adj_sweep_u<R, S><<<grd, TU, 0, s>>>(d, dt, splitfac, AH, nk, copy0, gbar, fbar, Dio, U, DU, mflux, mupd,

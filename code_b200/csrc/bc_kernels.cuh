@@ -4,6 +4,7 @@
 #pragma once
 #include "bc_common.cuh"
 #include "common.cuh"
+#include "kernels.cuh"
 
 namespace gb {
 
@@ -136,13 +137,23 @@ __global__ void k_ip(Dev d, Bc3<R3> s, const R3* zzp) {
 // in both. The elimination carries ru(k+1), qu(k+1) in registers and stores ru(k), qu(k) in two
 // scratch 3D arrays (RUs, QUs) so that occupancy is not limited by shared memory; the back
 // substitution overwrites QUs with Res(k) and the last pass writes uu = Res + hn*Diff.
+// The eleven inputs of a level (ho, hn, uu, num at the column and its neighbour, the other
+// velocity at the four points of its average, the advection term, the pressure gradient) are
+// staged by cp.async into the thread's own shared-memory slots two levels ahead of the
+// elimination (a ring of UVM_SLOTS levels), and the back substitution and the last pass load
+// ahead through registers, so the column's loads are in flight while its recurrence runs.
+constexpr int UVM_SLOTS = 4;
+constexpr int UVM_IN = 11;
+constexpr int UVM_THREADS = 128;
 template <class R3, int DIR>
-__global__ void __launch_bounds__(128) k_uvmom3d(Dev d, Bc3<R3> s, R3* RUs, R3* QUs) {
+__global__ void __launch_bounds__(UVM_THREADS) k_uvmom3d(Dev d, Bc3<R3> s, R3* RUs, R3* QUs) {
   using T = R3;
+  __shared__ R3 sl[UVM_SLOTS][UVM_IN][UVM_THREADS];
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   const int kmax = d.kmax;
   const int i = blockIdx.x * blockDim.x + threadIdx.x + d.imin;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + d.jmin;
-  if (i > d.imax || j > d.jmax) return;
+  if (i > d.imax || j > d.jmax) return;  // no barrier in this kernel
   I2 mask{d, DIR == 0 ? s.au : s.av};
   if (!(mask(i, j) == 1 || mask(i, j) == 2)) return;
   V3<R3> uu{d, s.f3[DIR == 0 ? UU : VV]}, vv{d, s.f3[DIR == 0 ? VV : UU]}, ho{d, s.f3[DIR == 0 ? HUO : HVO]},
@@ -164,26 +175,55 @@ __global__ void __launch_bounds__(128) k_uvmom3d(Dev d, Bc3<R3> s, R3* RUs, R3* 
   const T dryij = T(dry(i, j)), corij = T(cor(i, j));
   const T ip_t = T(ip_fac), avm_t = T(avmmol), dt_t = T(dt), g_t = T(g);
   const T taus_top = T(dry(i, j) * 0.5 * (taus(i, j) + taus(i + di, j + dj)) * rho_0i);
-  auto HO = [&](int k) { return T(ho(i, j, k)); };
-  auto HN = [&](int k) { return T(hn(i, j, k)); };
-  auto UU_ = [&](int k) { return T(uu(i, j, k)); };
+  // the level's inputs into slot k % UVM_SLOTS (an empty group for k < 0 keeps the counting uniform)
+  auto issue = [&](int k) {
+    if (k >= 0) {
+      R3(*q)[UVM_THREADS] = sl[k & (UVM_SLOTS - 1)];
+      cp_async(&q[0][tid], &ho(i, j, k));
+      cp_async(&q[1][tid], &hn(i, j, k));
+      cp_async(&q[2][tid], &uu(i, j, k));
+      cp_async(&q[3][tid], &num(i, j, k));
+      cp_async(&q[4][tid], &num(i + di, j + dj, k));
+      if (DIR == 0) {
+        cp_async(&q[5][tid], &vv(i, j, k));
+        cp_async(&q[6][tid], &vv(i + 1, j, k));
+        cp_async(&q[7][tid], &vv(i, j - 1, k));
+        cp_async(&q[8][tid], &vv(i + 1, j - 1, k));
+      } else {
+        cp_async(&q[5][tid], &vv(i, j, k));
+        cp_async(&q[6][tid], &vv(i - 1, j, k));
+        cp_async(&q[7][tid], &vv(i, j + 1, k));
+        cp_async(&q[8][tid], &vv(i - 1, j + 1, k));
+      }
+      cp_async(&q[9][tid], &Ex(i, j, k));
+      cp_async(&q[10][tid], &idp(i, j, k));
+    }
+    cp_async_commit();
+  };
+  auto in = [&](int k, int q) -> T { return T(sl[k & (UVM_SLOTS - 1)][q][tid]); };
+  auto HO = [&](int k) { return in(k, 0); };
+  auto HN = [&](int k) { return in(k, 1); };
+  auto UU_ = [&](int k) { return in(k, 2); };
   auto exk = [&](int k) {
     T loc, e;
     if (DIR == 0) {
-      loc = T(0.25) * (T(vv(i, j, k)) + T(vv(i + 1, j, k)) + T(vv(i, j - 1, k)) + T(vv(i + 1, j - 1, k)));
+      loc = T(0.25) * (in(k, 5) + in(k, 6) + in(k, 7) + in(k, 8));
       e = corij * loc;
     } else {
-      loc = T(0.25) * (T(vv(i, j, k)) + T(vv(i - 1, j, k)) + T(vv(i, j + 1, k)) + T(vv(i - 1, j + 1, k)));
+      loc = T(0.25) * (in(k, 5) + in(k, 6) + in(k, 7) + in(k, 8));
       e = -corij * loc;
     }
-    T x = dryij * (e - T(Ex(i, j, k)) + ip_t * T(idp(i, j, k)));
+    T x = dryij * (e - in(k, 9) + ip_t * in(k, 10));
     if (k == kmax) {
       if constexpr (sizeof(T) == 8) x = x + dryij * 0.5 * (taus(i, j) + taus(i + di, j + dj)) * rho_0i;
       else x = x + taus_top;
     }
     return x;
   };
-  auto dif = [&](int k) { return T(0.5) * (T(num(i, j, k)) + T(num(i + di, j + dj, k))) + avm_t; };
+  auto dif = [&](int k) { return T(0.5) * (in(k, 3) + in(k, 4)) + avm_t; };
+  issue(kmax);
+  issue(kmax - 1);
+  issue(kmax - 2);
   const T c_o = T(2.0 * (1.0 - cnpar) * dt), c_n = T(2.0 * cnpar * dt);
   const double zp = fmax(sseo(i + di, j + dj), -H(i, j) + fmin(min_depth, D(i + di, j + dj)));
   const double zm = fmax(sseo(i, j), -H(i + di, j + dj) + fmin(min_depth, D(i, j)));
@@ -193,6 +233,7 @@ __global__ void __launch_bounds__(128) k_uvmom3d(Dev d, Bc3<R3> s, R3* RUs, R3* 
   else
     zx = (zp - zm + (airp(i, j + 1) - airp(i, j)) / gamma) / d.dy;
   const T zx_t = T(zx);
+  cp_async_wait<1>();  // levels kmax and kmax-1
   // column window: heights and velocity at k-1, k, k+1
   int k = kmax;
   T hok = HO(k), hnk = HN(k), hokm1 = HO(k - 1), hnkm1 = HN(k - 1);
@@ -211,6 +252,8 @@ __global__ void __launch_bounds__(128) k_uvmom3d(Dev d, Bc3<R3> s, R3* RUs, R3* 
     QU(i, j, k) = R3(qu);
   }
   for (k = kmax - 1; k >= 2; --k) {
+    issue(k - 2);          // into the slot of level k+2, last read in the iteration of level k+2
+    cp_async_wait<1>();    // level k-1
     const T ao_k = ao_km1, an_k = an_km1;
     hokp1 = hok; hnkp1 = hnk; ukp1 = uk;
     hok = hokm1; hnk = hnkm1; uk = ukm1;
@@ -241,23 +284,38 @@ __global__ void __launch_bounds__(128) k_uvmom3d(Dev d, Bc3<R3> s, R3* RUs, R3* 
                  dt_t * T(0.5) * (hok + hnk) * g_t * zx_t;
     v = qdiv(a4 - a3 * qu, a2 - a3 * ru);
   }
-  // back substitution (Res in QU) and its FP64 sum in ascending k
+  cp_async_wait<0>();
+  // back substitution (Res in QU) and its FP64 sum in ascending k; RU, QU two levels ahead
   double ResInt = 0.0;
   ResInt = ResInt + (double)v;
   QU(i, j, 1) = R3(v);
+  T q1 = T(0), r1 = T(0), q2 = T(0), r2 = T(0);
+  if (kmax >= 2) { q1 = T(QU(i, j, 2)); r1 = T(RU(i, j, 2)); }
+  if (kmax >= 3) { q2 = T(QU(i, j, 3)); r2 = T(RU(i, j, 3)); }
   for (k = 2; k <= kmax; ++k) {
-    v = T(QU(i, j, k)) - T(RU(i, j, k)) * v;
+    const T qc = q1, rc = r1;
+    q1 = q2; r1 = r2;
+    if (k + 2 <= kmax) { q2 = T(QU(i, j, k + 2)); r2 = T(RU(i, j, k + 2)); }
+    v = qc - rc * v;
     QU(i, j, k) = R3(v);
     ResInt = ResInt + (double)v;
   }
   const double Diff = (Uint(i, j) - ResInt) / (sso(i, j) + HX(i, j));
-  for (k = 1; k <= kmax; ++k) uu(i, j, k) = R3((double)QU(i, j, k) + (double)hn(i, j, k) * Diff);
+  // last pass, four independent levels at a time
+  for (k = 1; k + 3 <= kmax; k += 4) {
+    R3 q[4], h[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) { q[m] = QU(i, j, k + m); h[m] = hn(i, j, k + m); }
+#pragma unroll
+    for (int m = 0; m < 4; ++m) uu(i, j, k + m) = R3((double)q[m] + (double)h[m] * Diff);
+  }
+  for (; k <= kmax; ++k) uu(i, j, k) = R3((double)QU(i, j, k) + (double)hn(i, j, k) * Diff);
 }
 
 // sigma_coordinates.F90:85-113 (equidistant sigma): layer heights of all levels 0..kmax. A thread
-// covers LVC levels of one column (grid z = level chunk): the column's 2D inputs are read once per
-// chunk, and its stores (six per level) are independent.
-constexpr int LVC = 8;
+// covers up to LVC levels of one column (grid z = level chunk; one chunk for kmax < 64): the
+// column's 2D inputs are read once, and its stores (six per level) are independent.
+constexpr int LVC = 64;
 template <class R3>
 __global__ void k_sigma(Dev d, Bc3<R3> s) {
   GB_IJ_HALO
@@ -299,8 +357,27 @@ __global__ void k_ww(Dev d, Bc3<R3> s) {
   V3<R3> ww{d, s.f3[WW]}, hn{d, s.f3[HN]}, ho{d, s.f3[HO]}, uu{d, s.f3[UU]}, vv{d, s.f3[VV]};
   const R3 dtm1 = R3(1.0 / s.par[P_DT]);
   const R3 dx = R3(d.dx), dy = R3(d.dy), ard1 = R3(d.ard1);
+  // four levels' loads are issued before their four stores (the loads do not wait on the stores)
   R3 w = ww(i, j, 0);
-  for (int k = 1; k <= d.kmax - 1; ++k) {
+  int k = 1;
+  for (; k + 3 <= d.kmax - 1; k += 4) {
+    R3 a[4][6];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      a[m][0] = hn(i, j, k + m);
+      a[m][1] = ho(i, j, k + m);
+      a[m][2] = uu(i, j, k + m);
+      a[m][3] = uu(i - 1, j, k + m);
+      a[m][4] = vv(i, j, k + m);
+      a[m][5] = vv(i, j - 1, k + m);
+    }
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      w = w - (a[m][0] - a[m][1]) * dtm1 - (a[m][2] * dy - a[m][3] * dy + a[m][4] * dx - a[m][5] * dx) * ard1;
+      ww(i, j, k + m) = w;
+    }
+  }
+  for (; k <= d.kmax - 1; ++k) {
     w = w - (hn(i, j, k) - ho(i, j, k)) * dtm1 -
         (uu(i, j, k) * dy - uu(i - 1, j, k) * dy + vv(i, j, k) * dx - vv(i, j - 1, k) * dx) * ard1;
     ww(i, j, k) = w;
@@ -339,6 +416,80 @@ __global__ void k_uvadv3d_prep(Dev d, Bc3<R3> s, R3* fadvp, R3* uuadvp, R3* vvad
     huadv(i, j, k) = half * (hun(i, j, k) + hun(i, j + 1, k));
     hvadv(i, j, k) = half * (ho(i, j + 1, k) + hn(i, j + 1, k));
   }
+}
+
+// FP32 form of k_uvadv3d_prep for 16-byte aligned layouts: a thread forms 4 consecutive cells of a
+// row with float4 loads and stores (the i+1 neighbour of the last cell by one scalar load; the
+// j+1 neighbours are the next row's vector). Same expressions, same cells written.
+template <int DIR>
+__global__ void __launch_bounds__(128) k_uvadv3d_prep_vec(Dev d, Bc3<float> s, float* fadvp, float* uuadvp,
+                                                        float* vvadvp, float* wwadvp, float* huadvp, float* hvadvp) {
+  constexpr int N = 4;
+  const int ni = d.ni(), nj = d.nj();
+  const int c0 = (blockIdx.x * blockDim.x + threadIdx.x) * N;
+  const int jj = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (c0 >= ni || jj >= nj) return;
+  const long long p = (long long)k * d.sk + (long long)jj * d.sj + c0;
+  // cells written: DIR 0 -- every cell but the last of the row (k >= 1); DIR 1 -- rows but the last
+  int nw = min(N, ni - c0);
+  if (k == 0) {
+    if (DIR == 0) {
+      const float z[N] = {0.f, 0.f, 0.f, 0.f};
+      st_row<float, N>(wwadvp + p, nw == N, nw, z);
+    }
+    return;
+  }
+  if (DIR == 0) nw = min(nw, ni - 1 - c0);
+  if (DIR == 1 && jj > nj - 2) return;
+  if (nw <= 0) return;
+  const bool fullr = c0 + N <= ni;  // loads of the whole vector are in the row
+  auto ld = [&](int f, long long off, float (&v)[N]) { ld_row<float, N>(s.f3[f] + p + off, fullr, ni - c0, v); };
+  float uu[N], vv[N], ww[N], ho[N], hn[N], hun[N], hvn[N];
+  const float half = 0.5f;
+  float fa[N], ua[N], va[N], wa[N], ha[N], hb[N];
+  if (DIR == 0) {
+    ld(UU, 0, uu); ld(VV, 0, vv); ld(WW, 0, ww); ld(HO, 0, ho); ld(HN, 0, hn); ld(HUN, 0, hun); ld(HVN, 0, hvn);
+    // the i+1 neighbours of the last cell (only read when that cell is written)
+    const bool nb = c0 + N < ni;
+    const long long q = p + N;
+    const float uue = nb ? s.f3[UU][q] : 0.f, vve = nb ? s.f3[VV][q] : 0.f, wwe = nb ? s.f3[WW][q] : 0.f,
+                hoe = nb ? s.f3[HO][q] : 0.f, hne = nb ? s.f3[HN][q] : 0.f, hvne = nb ? s.f3[HVN][q] : 0.f;
+#pragma unroll
+    for (int m = 0; m < N; ++m) {
+      const float u1 = m + 1 < N ? uu[m + 1] : uue, v1 = m + 1 < N ? vv[m + 1] : vve, w1 = m + 1 < N ? ww[m + 1] : wwe;
+      const float o1 = m + 1 < N ? ho[m + 1] : hoe, n1 = m + 1 < N ? hn[m + 1] : hne,
+                  h1 = m + 1 < N ? hvn[m + 1] : hvne;
+      fa[m] = uu[m] / hun[m];
+      ua[m] = half * (uu[m] + u1);
+      va[m] = half * (vv[m] + v1);
+      wa[m] = half * (ww[m] + w1);
+      ha[m] = half * (o1 + n1);
+      hb[m] = half * (hvn[m] + h1);
+    }
+  } else {
+    float uu1[N], vv1[N], ww1[N], hun1[N], ho1[N], hn1[N];
+    const long long sj = d.sj;
+    ld(UU, 0, uu); ld(VV, 0, vv); ld(WW, 0, ww); ld(HUN, 0, hun); ld(HVN, 0, hvn);
+    ld(UU, sj, uu1); ld(VV, sj, vv1); ld(WW, sj, ww1); ld(HUN, sj, hun1); ld(HO, sj, ho1); ld(HN, sj, hn1);
+#pragma unroll
+    for (int m = 0; m < N; ++m) {
+      fa[m] = vv[m] / hvn[m];
+      ua[m] = half * (uu[m] + uu1[m]);
+      va[m] = half * (vv[m] + vv1[m]);
+      wa[m] = half * (ww[m] + ww1[m]);
+      ha[m] = half * (hun[m] + hun1[m]);
+      hb[m] = half * (ho1[m] + hn1[m]);
+    }
+    (void)ho; (void)hn;
+  }
+  const bool fullw = nw == N;
+  st_row<float, N>(fadvp + p, fullw, nw, fa);
+  st_row<float, N>(uuadvp + p, fullw, nw, ua);
+  st_row<float, N>(vvadvp + p, fullw, nw, va);
+  st_row<float, N>(wwadvp + p, fullw, nw, wa);
+  st_row<float, N>(huadvp + p, fullw, nw, ha);
+  st_row<float, N>(hvadvp + p, fullw, nw, hb);
 }
 
 // stresses_3d.F90:50-104 (bottom and surface stresses; FP64 from the bottom layer)
@@ -432,13 +583,29 @@ int run_bc3(int which, const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* cons
     case BC3_SIGMA: k_sigma<R3><<<plane_grid(d, blk, (d.kmax + LVC) / LVC), blk, 0, st>>>(d, s); break;
     case BC3_WW: k_ww<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s); break;
     case BC3_UVADV_PREP_U:
-      k_uvadv3d_prep<R3, 0><<<plane_grid(d, blk, d.kmax + 1), blk, 0, st>>>(d, s, scr[0], scr[1], scr[2], scr[3],
-                                                                            scr[4], scr[5]);
+    case BC3_UVADV_PREP_V: {
+      const bool u = which == BC3_UVADV_PREP_U;
+      if constexpr (sizeof(R3) == 4) {
+        bool ok = vector_sweeps_enabled() && d.sj % 4 == 0 && d.sk % 4 == 0;
+        for (int q = 0; q < 6 && ok; ++q) ok = reinterpret_cast<uintptr_t>(scr[q]) % 16 == 0;
+        for (int f : {UU, VV, WW, HO, HN, HUN, HVN})
+          ok = ok && reinterpret_cast<uintptr_t>(s.f3[f]) % 16 == 0;
+        if (ok) {
+          const dim3 bv(32, 4, 1);
+          const dim3 gv((d.ni() + 4 * 32 - 1) / (4 * 32), (d.nj() + 3) / 4, d.kmax + 1);
+          if (u) k_uvadv3d_prep_vec<0><<<gv, bv, 0, st>>>(d, s, scr[0], scr[1], scr[2], scr[3], scr[4], scr[5]);
+          else k_uvadv3d_prep_vec<1><<<gv, bv, 0, st>>>(d, s, scr[0], scr[1], scr[2], scr[3], scr[4], scr[5]);
+          break;
+        }
+      }
+      if (u)
+        k_uvadv3d_prep<R3, 0><<<plane_grid(d, blk, d.kmax + 1), blk, 0, st>>>(d, s, scr[0], scr[1], scr[2], scr[3],
+                                                                              scr[4], scr[5]);
+      else
+        k_uvadv3d_prep<R3, 1><<<plane_grid(d, blk, d.kmax + 1), blk, 0, st>>>(d, s, scr[0], scr[1], scr[2], scr[3],
+                                                                              scr[4], scr[5]);
       break;
-    case BC3_UVADV_PREP_V:
-      k_uvadv3d_prep<R3, 1><<<plane_grid(d, blk, d.kmax + 1), blk, 0, st>>>(d, s, scr[0], scr[1], scr[2], scr[3],
-                                                                            scr[4], scr[5]);
-      break;
+    }
     case BC3_STRESSES: k_stresses<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s); break;
     case BC3_EQSTATE: k_eqstate<R3><<<plane_grid(d, blk, d.kmax), blk, 0, st>>>(d, s); break;
     case BC3_SLOW_TERMS: k_slow_terms<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s); break;
