@@ -34,9 +34,17 @@ UNIT = "cell-steps/s"
 WORKLOAD = ("mode-split baroclinic step (20 x integrate_2d + integrate_3d: 2D momentum/sealevel, internal "
             "pressure, 3D momentum with implicit viscosity, P2_PDM advection of u, v, T, S, implicit diffusion), "
             "2048x2048x50 irregular domain, 30% land, depth 5-150 m")
-# algorithmic words per interior cell per launch of a stage (each field read/written once)
-STAGE_WORDS = {"adv_split_u": 6, "adv_split_v": 6, "adv_split_w": 5, "tracer_vdiff": 4, "uv_momentum_3d": 8,
+# algorithmic words per interior cell per launch of a stage (each field read/written once). The
+# horizontal sweeps of a macro step are momentum sweeps (read f, U, DU, Di, adv; write fi, Di, adv)
+# and paired tracer sweeps (read T, S, U, DU, Di; write T, S, Di): 8 words either way; the vertical
+# sweeps 7 (f, ww, hi, adv / T, S, ww, hi read; f, hi, adv / T, S, hi written).
+STAGE_WORDS = {"adv_split_u": 8, "adv_split_v": 8, "adv_split_w": 7, "tracer_vdiff": 4, "uv_momentum_3d": 8,
                "internal_pressure": 6}
+# DRAM bytes (read + write) per interior cell per launch of the FP32 stages, averaged over the
+# launches of one macro step in an ncu capture of the 1024 x 1024 x 24 case (the 2048 x 2048 x 50
+# workload is too large to capture under ncu; the sweeps' traffic grows with the cells processed).
+# Source: profiles/traffic_sweeps_mixed_1024x1024x24.md.
+TRAFFIC_PER_CELL_F32 = {}
 
 
 def parse():
@@ -456,7 +464,9 @@ def main():
             "stage_ms_per_step": {k: t[0] / args.steps for k, t in tim.items()},
             "stage_ms_per_step_fp64": ({k: t[0] / args.steps for k, t in tim64.items()} if tim64 else None),
             "roofline": {"bound": "hbm", "kernel": top_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": (TRAFFIC_PER_CELL_F32[top_name] * cells
+                                     if head == "mixed" and top_name in TRAFFIC_PER_CELL_F32 else None),
                          "alg_bytes_per_launch": alg_bytes,
                          "step_alg_bytes": step_bytes,
                          "step_frac": step_bytes / (res[head]["ms"] / args.steps / 1e3) / 1e9 / peak},

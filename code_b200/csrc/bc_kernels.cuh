@@ -77,7 +77,18 @@ __global__ void k_zz(Dev d, Bc3<R3> s, R3* zzp) {
   V2 H{d, s.f2[HH]};
   R3 z = R3(-H(i, j)) + hn(i, j, 1);
   zz(i, j, 1) = z;
-  for (int k = 2; k <= d.kmax; ++k) {
+  int k = 2;
+  for (; k + 3 <= d.kmax; k += 4) {  // four levels' loads before their stores
+    R3 h[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) h[m] = hn(i, j, k + m);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      z = z + h[m];
+      zz(i, j, k + m) = z;
+    }
+  }
+  for (; k <= d.kmax; ++k) {
     z = z + hn(i, j, k);
     zz(i, j, k) = z;
   }
@@ -95,38 +106,42 @@ __global__ void k_ip(Dev d, Bc3<R3> s, const R3* zzp) {
   I2 au{d, s.au}, av{d, s.av};
   const int kmax = d.kmax;
   const R3 half = R3(0.5);
-  if (au(i, j) >= 1) {
-    const R3 dxm1 = R3(1.0 / d.dx);
-    R3 grdl = (buoy(i + 1, j, kmax) - buoy(i, j, kmax)) * dxm1;
-    R3 buoyl = half * (buoy(i + 1, j, kmax) + buoy(i, j, kmax));
-    R3 prgr = grdl * half * hun(i, j, kmax);
-    idpdx(i, j, kmax) = hun(i, j, kmax) * prgr;
-    for (int k = kmax - 1; k >= 1; --k) {
+  // one column: downward integral with hx the layer heights at the face, (oi, oj) the neighbour
+  // across it; four levels' loads are issued before their stores
+  auto column = [&](V3<R3>& hx, V3<R3>& out, int oi, int oj, R3 dm1) {
+    R3 grdl = (buoy(i + oi, j + oj, kmax) - buoy(i, j, kmax)) * dm1;
+    R3 buoyl = half * (buoy(i + oi, j + oj, kmax) + buoy(i, j, kmax));
+    R3 hk1 = hx(i, j, kmax);
+    R3 prgr = grdl * half * hk1;
+    out(i, j, kmax) = hk1 * prgr;
+    auto level = [&](int k, R3 b1, R3 b0, R3 z1, R3 z0, R3 hk) {
       const R3 grdu = grdl;
-      grdl = (buoy(i + 1, j, k) - buoy(i, j, k)) * dxm1;
+      grdl = (b1 - b0) * dm1;
       const R3 buoyu = buoyl;
-      buoyl = half * (buoy(i + 1, j, k) + buoy(i, j, k));
-      const R3 dxz = (zz(i + 1, j, k) - zz(i, j, k)) * dxm1;
-      prgr = prgr + half * (grdu + grdl) * half * (hun(i, j, k) + hun(i, j, k + 1)) - dxz * (buoyu - buoyl);
-      idpdx(i, j, k) = hun(i, j, k) * prgr;
+      buoyl = half * (b1 + b0);
+      const R3 dz = (z1 - z0) * dm1;
+      prgr = prgr + half * (grdu + grdl) * half * (hk + hk1) - dz * (buoyu - buoyl);
+      out(i, j, k) = hk * prgr;
+      hk1 = hk;
+    };
+    int k = kmax - 1;
+    for (; k >= 4; k -= 4) {
+      R3 b1[4], b0[4], z1[4], z0[4], h[4];
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        b1[m] = buoy(i + oi, j + oj, k - m);
+        b0[m] = buoy(i, j, k - m);
+        z1[m] = zz(i + oi, j + oj, k - m);
+        z0[m] = zz(i, j, k - m);
+        h[m] = hx(i, j, k - m);
+      }
+#pragma unroll
+      for (int m = 0; m < 4; ++m) level(k - m, b1[m], b0[m], z1[m], z0[m], h[m]);
     }
-  }
-  if (av(i, j) >= 1) {
-    const R3 dym1 = R3(1.0 / d.dy);
-    R3 grdl = (buoy(i, j + 1, kmax) - buoy(i, j, kmax)) * dym1;
-    R3 buoyl = half * (buoy(i, j + 1, kmax) + buoy(i, j, kmax));
-    R3 prgr = grdl * half * hvn(i, j, kmax);
-    idpdy(i, j, kmax) = hvn(i, j, kmax) * prgr;
-    for (int k = kmax - 1; k >= 1; --k) {
-      const R3 grdu = grdl;
-      grdl = (buoy(i, j + 1, k) - buoy(i, j, k)) * dym1;
-      const R3 buoyu = buoyl;
-      buoyl = half * (buoy(i, j + 1, k) + buoy(i, j, k));
-      const R3 dyz = (zz(i, j + 1, k) - zz(i, j, k)) * dym1;
-      prgr = prgr + half * (grdu + grdl) * half * (hvn(i, j, k) + hvn(i, j, k + 1)) - dyz * (buoyu - buoyl);
-      idpdy(i, j, k) = hvn(i, j, k) * prgr;
-    }
-  }
+    for (; k >= 1; --k) level(k, buoy(i + oi, j + oj, k), buoy(i, j, k), zz(i + oi, j + oj, k), zz(i, j, k), hx(i, j, k));
+  };
+  if (au(i, j) >= 1) column(hun, idpdx, 1, 0, R3(1.0 / d.dx));
+  if (av(i, j) >= 1) column(hvn, idpdy, 0, 1, R3(1.0 / d.dy));
 }
 
 // uu_momentum_3d.F90:169-304 (DIR 0) / vv_momentum_3d.F90:174-315 (DIR 1), kumin = 1: explicit
@@ -343,6 +358,45 @@ __global__ void k_sigma(Dev d, Bc3<R3> s) {
     for (int k = k0; k < k1; ++k) {
       hvo(i, j, k) = a;
       hvn(i, j, k) = b;
+    }
+  }
+}
+
+// FP32 form of k_sigma for 16-byte aligned layouts: a thread covers 4 consecutive cells of a row
+// and stores float4 vectors (a quarter of the store instructions of the scalar form, whose
+// stores queue up behind one another).
+template <int N>
+__global__ void __launch_bounds__(128) k_sigma_vec(Dev d, Bc3<float> s) {
+  const int ni = d.ni(), nj = d.nj();
+  const int c0 = (blockIdx.x * blockDim.x + threadIdx.x) * N;
+  const int jj = blockIdx.y * blockDim.y + threadIdx.y;
+  if (c0 >= ni || jj >= nj) return;
+  const long long c = (long long)jj * d.sj + c0;
+  const int nall = min(N, ni - c0), nu = min(N, ni - 1 - c0);
+  const bool vrow = jj <= nj - 2;
+  const double kmaxm1 = 1.0 / (double)(float)d.kmax;
+  float a0[N], b0[N], a1[N], b1[N], a2[N], b2[N];
+#pragma unroll
+  for (int m = 0; m < N; ++m) {
+    const long long q = c + (m < nall ? m : 0);
+    a0[m] = (float)((s.f2[SSEO][q] + s.f2[HH][q]) * kmaxm1);
+    b0[m] = (float)((s.f2[SSEN][q] + s.f2[HH][q]) * kmaxm1);
+    a1[m] = (float)((s.f2[SSUO][q] + s.f2[HU][q]) * kmaxm1);
+    b1[m] = (float)((s.f2[SSUN][q] + s.f2[HU][q]) * kmaxm1);
+    a2[m] = (float)((s.f2[SSVO][q] + s.f2[HV][q]) * kmaxm1);
+    b2[m] = (float)((s.f2[SSVN][q] + s.f2[HV][q]) * kmaxm1);
+  }
+  for (int k = 0; k <= d.kmax; ++k) {
+    const long long p = c + (long long)k * d.sk;
+    st_row<float, N>(s.f3[HO] + p, nall == N, nall, a0);
+    st_row<float, N>(s.f3[HN] + p, nall == N, nall, b0);
+    if (nu > 0) {
+      st_row<float, N>(s.f3[HUO] + p, nu == N, nu, a1);
+      st_row<float, N>(s.f3[HUN] + p, nu == N, nu, b1);
+    }
+    if (vrow) {
+      st_row<float, N>(s.f3[HVO] + p, nall == N, nall, a2);
+      st_row<float, N>(s.f3[HVN] + p, nall == N, nall, b2);
     }
   }
 }
@@ -580,7 +634,19 @@ int run_bc3(int which, const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* cons
         k_uvmom3d<R3, 1><<<g2, b2, 0, st>>>(d, s, scr[0], scr[1]);
       break;
     }
-    case BC3_SIGMA: k_sigma<R3><<<plane_grid(d, blk, (d.kmax + LVC) / LVC), blk, 0, st>>>(d, s); break;
+    case BC3_SIGMA: {
+      if constexpr (sizeof(R3) == 4) {
+        bool ok = vector_sweeps_enabled() && d.sj % 4 == 0 && d.sk % 4 == 0;
+        for (int f : {HO, HN, HUO, HUN, HVO, HVN}) ok = ok && reinterpret_cast<uintptr_t>(s.f3[f]) % 16 == 0;
+        if (ok) {
+          const dim3 gv((d.ni() + 4 * 32 - 1) / (4 * 32), (d.nj() + 3) / 4, 1);
+          k_sigma_vec<4><<<gv, dim3(32, 4, 1), 0, st>>>(d, s);
+          break;
+        }
+      }
+      k_sigma<R3><<<plane_grid(d, blk, (d.kmax + LVC) / LVC), blk, 0, st>>>(d, s);
+      break;
+    }
     case BC3_WW: k_ww<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s); break;
     case BC3_UVADV_PREP_U:
     case BC3_UVADV_PREP_V: {
