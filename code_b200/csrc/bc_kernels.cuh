@@ -568,18 +568,50 @@ __global__ void k_stresses(Dev d, Bc3<R3> s) {
   }
 }
 
-// eqstate.F90:127-137 (linear) + :252-261 (buoyancy), levels 1..kmax over the haloed plane
+// eqstate.F90:127-137 (linear) + :252-261 (buoyancy) of one cell. FP64: the reference's expression;
+// FP32: explicitly rounded operations, so the scalar and the vectorised kernel agree bit for bit.
+template <class R3>
+__device__ __forceinline__ void eos_lin(const Bc3<R3>& s, R3 t, R3 sal, R3& r, R3& b) {
+  const R3 rho_0 = R3(s.par[P_RHO_0]), dtr0 = R3(s.par[P_DTR0]), dsr0 = R3(s.par[P_DSR0]), T0 = R3(s.par[P_T0]),
+           S0 = R3(s.par[P_S0]);
+  const R3 x = R3(-s.par[P_G] / s.par[P_RHO_0]);
+  if constexpr (sizeof(R3) == 8) {
+    r = rho_0 + dtr0 * (t - T0) + dsr0 * (sal - S0);
+    b = x * (r - rho_0);
+  } else {
+    r = __fmaf_rn(dsr0, __fsub_rn(sal, S0), __fmaf_rn(dtr0, __fsub_rn(t, T0), rho_0));
+    b = __fmul_rn(x, __fsub_rn(r, rho_0));
+  }
+}
+
+// levels 1..kmax over the haloed plane, one thread per cell
 template <class R3>
 __global__ void k_eqstate(Dev d, Bc3<R3> s) {
   GB_IJ_HALO
   const int k = blockIdx.z + 1;
   V3<R3> rho{d, s.f3[RHO]}, buoy{d, s.f3[BUOY]}, T{d, s.f3[TT]}, S{d, s.f3[SS]};
-  const R3 rho_0 = R3(s.par[P_RHO_0]), dtr0 = R3(s.par[P_DTR0]), dsr0 = R3(s.par[P_DSR0]), T0 = R3(s.par[P_T0]),
-           S0 = R3(s.par[P_S0]);
-  const R3 x = R3(-s.par[P_G] / s.par[P_RHO_0]);
-  const R3 r = rho_0 + dtr0 * (T(i, j, k) - T0) + dsr0 * (S(i, j, k) - S0);
+  R3 r, b;
+  eos_lin<R3>(s, T(i, j, k), S(i, j, k), r, b);
   rho(i, j, k) = r;
-  buoy(i, j, k) = x * (r - rho_0);
+  buoy(i, j, k) = b;
+}
+
+// FP32, 16-byte aligned layouts: 4 consecutive cells per thread with float4 accesses
+template <int N>
+__global__ void __launch_bounds__(128) k_eqstate_vec(Dev d, Bc3<float> s) {
+  const int ni = d.ni(), nj = d.nj();
+  const int c0 = (blockIdx.x * blockDim.x + threadIdx.x) * N;
+  const int jj = blockIdx.y * blockDim.y + threadIdx.y;
+  if (c0 >= ni || jj >= nj) return;
+  const long long p = (long long)(blockIdx.z + 1) * d.sk + (long long)jj * d.sj + c0;
+  const int na = min(N, ni - c0);
+  float t[N], sa[N], r[N], b[N];
+  ld_row<float, N>(s.f3[TT] + p, na == N, na, t);
+  ld_row<float, N>(s.f3[SS] + p, na == N, na, sa);
+#pragma unroll
+  for (int m = 0; m < N; ++m) eos_lin<float>(s, t[m], sa[m], r[m], b[m]);
+  st_row<float, N>(s.f3[RHO] + p, na == N, na, r);
+  st_row<float, N>(s.f3[BUOY] + p, na == N, na, b);
 }
 
 // slow_terms.F90:57-181 (kmax > 1, kumin = kvmin = 1): vertical sums in FP64
@@ -673,7 +705,19 @@ int run_bc3(int which, const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* cons
       break;
     }
     case BC3_STRESSES: k_stresses<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s); break;
-    case BC3_EQSTATE: k_eqstate<R3><<<plane_grid(d, blk, d.kmax), blk, 0, st>>>(d, s); break;
+    case BC3_EQSTATE: {
+      if constexpr (sizeof(R3) == 4) {
+        bool ok = vector_sweeps_enabled() && d.sj % 4 == 0 && d.sk % 4 == 0;
+        for (int f : {TT, SS, RHO, BUOY}) ok = ok && reinterpret_cast<uintptr_t>(s.f3[f]) % 16 == 0;
+        if (ok) {
+          const dim3 gv((d.ni() + 4 * 32 - 1) / (4 * 32), (d.nj() + 3) / 4, d.kmax);
+          k_eqstate_vec<4><<<gv, dim3(32, 4, 1), 0, st>>>(d, s);
+          break;
+        }
+      }
+      k_eqstate<R3><<<plane_grid(d, blk, d.kmax), blk, 0, st>>>(d, s);
+      break;
+    }
     case BC3_SLOW_TERMS: k_slow_terms<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s); break;
     default: return (int)cudaErrorInvalidValue;
   }

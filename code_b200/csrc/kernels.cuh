@@ -185,9 +185,44 @@ __device__ __forceinline__ R face_cfl(bool pos, R Uf, R DUf, R dti, R cdx, R dxf
 }
 
 // With REC the limiter branch is written to *code (0 when the face is not limited).
+// FP32 without branch recording: the same values computed without branches (every candidate is
+// evaluated and the result selected), so the lanes of a warp do not diverge on the masks, the
+// flow direction or the limiter's extremum test; the operations and their rounding are those of
+// the branching form below.
+template <int S>
+__device__ __forceinline__ float face_flux_f32(float Uf, float DUf, float fm1, float f0, float f1, float f2,
+                                               bool mm1, bool m0, bool mp1, float cdx, float AH, bool use_AH,
+                                               float dxf) {
+  const bool pos = Uf > 0.f;
+  float fu = pos ? f0 : f1;
+  if constexpr (S != UPSTREAM) {
+    const float fuu = pos ? fm1 : f2;
+    const float fd = pos ? f1 : f0;
+    const bool lim = pos ? mm1 : mp1;
+    const float cfl = __fdividef(fabsf(Uf) * cdx, DUf);
+    float val;
+    if constexpr (S == P2_PDM) {
+      const float df = fd - fu, du = fu - fuu;
+      const Pdm32 p = pdm32(cfl, fabsf(du), fabsf(df));
+      const float v = fu + copysignf(fminf(fminf(p.v1, p.v2), fabsf(df)), df);
+      val = (df * du > 0.f) ? v : fu;
+    } else {
+      val = recon_s<float, S>(cfl, fuu, fu, fd);
+    }
+    fu = lim ? val : fu;
+  }
+  float fl = Uf * fu;
+  if (use_AH) fl = fl - AH * DUf * (f1 - f0) / dxf;
+  return m0 ? fl : 0.f;
+}
+
 template <class R, int S, bool REC = false>
 __device__ __forceinline__ R face_flux_s(R Uf, R DUf, R fm1, R f0, R f1, R f2, bool mm1, bool m0, bool mp1,
                                          R dti, R cdx, R AH, bool use_AH, R dxf, uint8_t* code = nullptr) {
+  if constexpr (sizeof(R) == 4 && !REC) {
+    (void)dti; (void)code;
+    return face_flux_f32<S>(Uf, DUf, fm1, f0, f1, f2, mm1, m0, mp1, cdx, AH, use_AH, dxf);
+  }
   if (REC) *code = 0;
   if (!m0) return R(0);
   const bool pos = Uf > R(0);
@@ -823,17 +858,34 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, co
   // (ao+an)(k)*(S(k+1)-S(k)) - (ao+an)(k-1)*(S(k)-S(k-1)) [+ src]; the rounding then acts on the
   // small increment rather than on h*S (bias-free over hundreds of steps).
   constexpr bool incr = sizeof(R) == 4;
-  // The loads of level k-2 are issued one iteration ahead of their use (the elimination is a
-  // serial chain per column; this keeps two levels of loads in flight per thread).
+  // The inputs of a level (hn, nuh, the old tracer, src) are staged by cp.async into the thread's
+  // own shared-memory slots, a ring of four levels with three in flight ahead of the elimination
+  // (a serial chain per column), so the chain does not wait on their loads.
+  __shared__ R sl[4][4][128];
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  auto issue = [&](int lv) {
+    if (lv >= 1) {
+      R(*q)[128] = sl[lv & 3];
+      cp_async(&q[0][tid], hn + c + lv * sk);
+      cp_async(&q[1][tid], nuh + c + lv * sk);
+      cp_async(&q[2][tid], Sin + c + lv * sk);
+      if (src) cp_async(&q[3][tid], src + c + lv * sk);
+    }
+    cp_async_commit();
+  };
+  auto get = [&](int lv, int q) -> R { return sl[lv & 3][q][tid]; };
+  issue(kmax);
+  issue(kmax - 1);
+  issue(kmax - 2);
+  issue(kmax - 3);
+  cp_async_wait<2>();  // levels kmax and kmax-1
   // surface row k = kmax: au = a1, bu = a2, du = a4
   int k = kmax;
-  R hnk = L(hn, k), hnkm1 = L(hn, k - 1);
-  R nu = L(nuh, k - 1) + avmol;
-  R Sk = L(Sin, k), Skm1 = L(Sin, k - 1);
-  R srck = src ? L(src, k) : R(0);
-  // next window entries (level kmax-2 and the interface below it)
-  R hn_n = kmax >= 2 ? L(hn, kmax - 2) : R(0), nuh_n = kmax >= 2 ? L(nuh, kmax - 2) : R(0);
-  R S_n = kmax >= 2 ? L(Sin, kmax - 2) : R(0), src_n = (src && kmax >= 2) ? L(src, kmax - 1) : R(0);
+  R hnk = get(k, 0), hnkm1 = get(k - 1, 0);
+  R nu = get(k - 1, 1) + avmol;
+  R Sk = get(k, 2), Skm1 = get(k - 1, 2);
+  R srck = src ? get(k, 3) : R(0);
+  R src_n = src ? get(k - 1, 3) : R(0);  // the source of the next row
   R ao_km1 = co * nu / (hnk + hnkm1), an_km1 = cn * nu / (hnk + hnkm1);
   R ru, qu;
   {
@@ -848,20 +900,17 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, co
   }
   // inner rows k = kmax-1 .. 2
   for (k = kmax - 1; k >= 2; --k) {
+    issue(k - 3);        // into the slot of level k+1, whose values were read in the row above
+    cp_async_wait<2>();  // level k-1
     const R ao_k = ao_km1, an_k = an_km1;  // aux at interface k (computed as k-1 of row k+1)
     hnk = hnkm1;
-    hnkm1 = hn_n;
-    nu = nuh_n + avmol;
+    hnkm1 = get(k - 1, 0);
+    nu = get(k - 1, 1) + avmol;
     const R Skp1 = Sk;
     Sk = Skm1;
-    Skm1 = S_n;
+    Skm1 = get(k - 1, 2);
     const R srcv = src_n;
-    if (k >= 3) {
-      hn_n = L(hn, k - 2);
-      nuh_n = L(nuh, k - 2);
-      S_n = L(Sin, k - 2);
-    }
-    if (src) src_n = L(src, k - 1);
+    if (src) src_n = get(k - 1, 3);
     ao_km1 = co * nu / (hnk + hnkm1);
     an_km1 = cn * nu / (hnk + hnkm1);
     const R a3 = -an_k;
@@ -876,6 +925,7 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, co
     RUs[c + k * sk] = ru;
     QUs[c + k * sk] = qu;
   }
+  cp_async_wait<0>();
   // bottom row k = 1 (fi): only qu
   R v;
   {
@@ -886,19 +936,22 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, co
     const R a3 = -an_k;
     const R a2 = h1 + an_k;
     R a4 = incr ? (ao_k + an_k) * (Skp1 - S1) : Skp1 * ao_k + S1 * (h1 - ao_k);
-    if (src) a4 = a4 + L(src, 1);
+    if (src) a4 = a4 + src_n;  // src(1)
     v = (a4 - a3 * qu) / (a2 - a3 * ru);
     put(1, incr ? S1 + v : v);
   }
   // back substitution upwards, with the next level's coefficients loaded one step ahead
   R qn = kmax >= 2 ? QUs[c + 2 * sk] : R(0), rn = kmax >= 2 ? RUs[c + 2 * sk] : R(0);
   R sn = (incr && kmax >= 2) ? L(Sin, 2) : R(0);
+  R qn2 = kmax >= 3 ? QUs[c + 3 * sk] : R(0), rn2 = kmax >= 3 ? RUs[c + 3 * sk] : R(0);
+  R sn2 = (incr && kmax >= 3) ? L(Sin, 3) : R(0);
   for (k = 2; k <= kmax; ++k) {
     const R q = qn, r = rn, so = sn;
-    if (k < kmax) {
-      qn = QUs[c + (k + 1) * sk];
-      rn = RUs[c + (k + 1) * sk];
-      if (incr) sn = L(Sin, k + 1);
+    qn = qn2; rn = rn2; sn = sn2;
+    if (k + 2 <= kmax) {
+      qn2 = QUs[c + (k + 2) * sk];
+      rn2 = RUs[c + (k + 2) * sk];
+      if (incr) sn2 = L(Sin, k + 2);
     }
     v = q - r * v;
     put(k, incr ? so + v : v);
