@@ -31,14 +31,16 @@ struct Adv2dSmem {
 };
 
 // DIR 0: UEx on the U grid (fadv = U/DU, faces between U points); DIR 1: VEx on the V grid.
-template <class T, int S, int DIR>
-__global__ void __launch_bounds__(FT) k_uvadv2d_fused(Dev d, T dt, const double* __restrict__ U,
-                                                      const double* __restrict__ V, const double* __restrict__ DU,
-                                                      const double* __restrict__ DV,
+// TI: the storage type of U, V, DU, DV and Ex (FP64 state arrays, or the FP32 working copies of
+// the mixed-precision micro step)
+template <class T, int S, int DIR, class TI>
+__global__ void __launch_bounds__(FT) k_uvadv2d_fused(Dev d, T dt, const TI* __restrict__ U,
+                                                      const TI* __restrict__ V, const TI* __restrict__ DU,
+                                                      const TI* __restrict__ DV,
                                                       const uint8_t* __restrict__ mflux_u,
                                                       const uint8_t* __restrict__ mflux_v,
                                                       const uint8_t* __restrict__ mupd_u,
-                                                      const uint8_t* __restrict__ mupd_v, double* __restrict__ Ex) {
+                                                      const uint8_t* __restrict__ mupd_v, TI* __restrict__ Ex) {
   extern __shared__ unsigned char smem_raw[];
   Adv2dSmem<T>& sm = *reinterpret_cast<Adv2dSmem<T>*>(smem_raw);
   const int ni = d.ni(), nj = d.nj();
@@ -173,34 +175,52 @@ __global__ void __launch_bounds__(FT) k_uvadv2d_fused(Dev d, T dt, const double*
         const T advn = half * (sm.FL[r][q] * dyu - sm.FL[r][q - 1] * dyu) * ard1;
         a = a + advn;
       }
-      if (ii < ni && jj < nj) Ex[(long long)jj * sj + ii] = (double)a;
+      if (ii < ni && jj < nj) Ex[(long long)jj * sj + ii] = (TI)a;
     }
   }
 }
 
-template <class T, int S, int DIR>
-int launch_uvadv2d_fused(const Dev& d, cudaStream_t s, T dt, const double* U, const double* V, const double* DU,
-                         const double* DV, const uint8_t* mflux_u, const uint8_t* mflux_v, const uint8_t* mupd_u,
-                         const uint8_t* mupd_v, double* Ex) {
+template <class T, int S, int DIR, class TI>
+int launch_uvadv2d_fused(const Dev& d, cudaStream_t s, T dt, const TI* U, const TI* V, const TI* DU, const TI* DV,
+                         const uint8_t* mflux_u, const uint8_t* mflux_v, const uint8_t* mupd_u,
+                         const uint8_t* mupd_v, TI* Ex) {
   const size_t smem = sizeof(Adv2dSmem<T>);
   // opt-in above 48 KB of shared memory (a host-side setting of the current device's function)
-  const cudaError_t e = cudaFuncSetAttribute(k_uvadv2d_fused<T, S, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
+  const cudaError_t e = cudaFuncSetAttribute(k_uvadv2d_fused<T, S, DIR, TI>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return (int)e;
   dim3 grd((d.ni() + FX - 1) / FX, (d.nj() + FY - 1) / FY, 1);
-  k_uvadv2d_fused<T, S, DIR><<<grd, FT, smem, s>>>(d, dt, U, V, DU, DV, mflux_u, mflux_v, mupd_u, mupd_v, Ex);
+  k_uvadv2d_fused<T, S, DIR, TI><<<grd, FT, smem, s>>>(d, dt, U, V, DU, DV, mflux_u, mflux_v, mupd_u, mupd_v, Ex);
   return (int)cudaGetLastError();
+}
+
+template <class T, class TI>
+int run_uvadv2d_fused_t(const Dev& d, cudaStream_t s, int dir, T dt, int scheme, const TI* U, const TI* V,
+                        const TI* DU, const TI* DV, const uint8_t* mflux_u, const uint8_t* mflux_v,
+                        const uint8_t* mupd_u, const uint8_t* mupd_v, TI* Ex) {
+  return dispatch_scheme(scheme, [&](auto sc) {
+    constexpr int S = decltype(sc)::value;
+    return dir == 0 ? launch_uvadv2d_fused<T, S, 0, TI>(d, s, dt, U, V, DU, DV, mflux_u, mflux_v, mupd_u, mupd_v, Ex)
+                    : launch_uvadv2d_fused<T, S, 1, TI>(d, s, dt, U, V, DU, DV, mflux_u, mflux_v, mupd_u, mupd_v, Ex);
+  });
 }
 
 template <class T>
 int run_uvadv2d_fused(const Dev& d, cudaStream_t s, int dir, T dt, int scheme, const double* U, const double* V,
                       const double* DU, const double* DV, const uint8_t* mflux_u, const uint8_t* mflux_v,
                       const uint8_t* mupd_u, const uint8_t* mupd_v, double* Ex) {
-  return dispatch_scheme(scheme, [&](auto sc) {
-    constexpr int S = decltype(sc)::value;
-    return dir == 0 ? launch_uvadv2d_fused<T, S, 0>(d, s, dt, U, V, DU, DV, mflux_u, mflux_v, mupd_u, mupd_v, Ex)
-                    : launch_uvadv2d_fused<T, S, 1>(d, s, dt, U, V, DU, DV, mflux_u, mflux_v, mupd_u, mupd_v, Ex);
-  });
+  return run_uvadv2d_fused_t<T, double>(d, s, dir, dt, scheme, U, V, DU, DV, mflux_u, mflux_v, mupd_u, mupd_v, Ex);
 }
+
+// FP32 arithmetic on the FP32 working copies of the mixed-precision micro step (defined in the
+// FP32 translation unit only)
+#if defined(GB_REAL_IS_FLOAT)
+int run_uvadv2d_fused_f32(const Dev& d, cudaStream_t s, int dir, float dt, int scheme, const float* U,
+                          const float* V, const float* DU, const float* DV, const uint8_t* mflux_u,
+                          const uint8_t* mflux_v, const uint8_t* mupd_u, const uint8_t* mupd_v, float* Ex) {
+  return run_uvadv2d_fused_t<float, float>(d, s, dir, dt, scheme, U, V, DU, DV, mflux_u, mflux_v, mupd_u, mupd_v,
+                                           Ex);
+}
+#endif
 
 }  // namespace gb

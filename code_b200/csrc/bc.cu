@@ -16,6 +16,19 @@ struct W2 {
   double* p;
   __device__ double& operator()(int i, int j) const { return p[d.ix(i, j)]; }
 };
+// a 2D field of the micro step: the FP32 working copy (mixed step) or the FP64 state array
+template <class E>
+struct A2 {
+  const Dev& d;
+  E* p;
+  __device__ E& operator()(int i, int j) const { return p[d.ix(i, j)]; }
+};
+template <bool MIX, int Q>
+__device__ __forceinline__ auto f2a(const Dev& d, const Bc2& s, const Bc2W& w) {
+  if constexpr (MIX && is_work2(Q)) return A2<float>{d, w.w[Q]};
+  else return A2<double>{d, s.f2[Q]};
+}
+
 struct M2 {
   const Dev& d;
   const int32_t* p;
@@ -28,11 +41,18 @@ __device__ __forceinline__ bool interior(const Dev& d, int i, int j) {
 // bottom_friction.F90:48-150: ru/rv from the depth-averaged velocities (log-law drag). Arithmetic
 // type T: FP64 in the plain step (the reference's expressions and order), FP32 in the mixed step
 // (inputs and outputs stay FP64 arrays).
-template <class T>
-__global__ void k_bottom_friction(Dev d, Bc2 s, int runtype) {
+template <class T, bool MIX>
+__global__ void k_bottom_friction(Dev d, Bc2 s, Bc2W w, int runtype) {
   GB_IJ2
-  W2 U{d, s.f2[U_]}, V{d, s.f2[V_]}, DU_{d, s.f2[DU]}, DV_{d, s.f2[DV]}, ruu{d, s.f2[RUU]}, rvv{d, s.f2[RVV]},
-      ru{d, s.f2[RU]}, rv{d, s.f2[RV]}, zub{d, s.f2[ZUB]}, zvb{d, s.f2[ZVB]}, zub0{d, s.f2[ZUB0]}, zvb0{d, s.f2[ZVB0]};
+  auto U = f2a<MIX, U_>(d, s, w);
+  auto V = f2a<MIX, V_>(d, s, w);
+  auto DU_ = f2a<MIX, DU>(d, s, w);
+  auto DV_ = f2a<MIX, DV>(d, s, w);
+  auto ruu = f2a<MIX, RUU>(d, s, w);
+  auto rvv = f2a<MIX, RVV>(d, s, w);
+  auto ru = f2a<MIX, RU>(d, s, w);
+  auto rv = f2a<MIX, RV>(d, s, w);
+  W2 zub{d, s.f2[ZUB]}, zvb{d, s.f2[ZVB]}, zub0{d, s.f2[ZUB0]}, zvb0{d, s.f2[ZVB0]};
   M2 au{d, s.au}, av{d, s.av};
   const T kappa = T(s.par[P_KAPPA]), avmmol = T(s.par[P_AVMMOL]), min_depth = T(s.par[P_MIN_DEPTH]);
   const T q = T(0.25), h = T(0.5);
@@ -130,52 +150,64 @@ __global__ void k_finalise2d(Dev d, T dt, T* f, const T* Do, const T* adv, const
 
 // momentum.F90:157-174 (umomentum, DIR 0) / :319-336 (vmomentum, DIR 1): depth-integrated
 // transport update on U (V) points of the interior.
-template <int DIR>
-__global__ void k_momentum(Dev d, Bc2 s) {
+template <int DIR, bool MIX>
+__global__ void k_momentum(Dev d, Bc2 s, Bc2W w) {
   GB_IJ2
   if (!interior(d, i, j)) return;
   M2 mask{d, DIR == 0 ? s.au : s.av};
   if (!(mask(i, j) == 1 || mask(i, j) == 2)) return;
-  W2 X{d, s.f2[DIR == 0 ? U_ : V_]}, DX{d, s.f2[DIR == 0 ? DU : DV]}, z{d, s.f2[Z]}, H{d, s.f2[HH]}, D{d, s.f2[D_]},
-      airp{d, s.f2[AIRP]}, taus{d, s.f2[DIR == 0 ? TAUSX : TAUSY]}, Slr_{d, s.f2[DIR == 0 ? SLRU : SLRV]},
-      dry{d, s.f2[DIR == 0 ? DRY_U : DRY_V]}, fC{d, s.f2[DIR == 0 ? FV : FU]}, Ex{d, s.f2[DIR == 0 ? UEX : VEX]},
-      Slx{d, s.f2[DIR == 0 ? SLUX : SLVX]}, r{d, s.f2[DIR == 0 ? RU : RV]};
+  auto X = f2a<MIX, DIR == 0 ? U_ : V_>(d, s, w);
+  auto DX = f2a<MIX, DIR == 0 ? DU : DV>(d, s, w);
+  auto D = f2a<MIX, D_>(d, s, w);
+  auto airp = f2a<MIX, AIRP>(d, s, w);
+  auto taus = f2a<MIX, DIR == 0 ? TAUSX : TAUSY>(d, s, w);
+  auto Slr_ = f2a<MIX, DIR == 0 ? SLRU : SLRV>(d, s, w);
+  auto dry = f2a<MIX, DIR == 0 ? DRY_U : DRY_V>(d, s, w);
+  auto fC = f2a<MIX, DIR == 0 ? FV : FU>(d, s, w);
+  auto Ex = f2a<MIX, DIR == 0 ? UEX : VEX>(d, s, w);
+  auto Slx = f2a<MIX, DIR == 0 ? SLUX : SLVX>(d, s, w);
+  auto r = f2a<MIX, DIR == 0 ? RU : RV>(d, s, w);
+  W2 z{d, s.f2[Z]}, H{d, s.f2[HH]};
   const double g = s.par[P_G], rho_0 = s.par[P_RHO_0], dtm = s.par[P_DTM], min_depth = s.par[P_MIN_DEPTH];
   const double gamma = rho_0 * g;
   const double gammai = 1.0 / gamma;
   const int di = DIR == 0 ? 1 : 0, dj = DIR == 0 ? 0 : 1;
-  const double zp = fmax(z(i + di, j + dj), -H(i, j) + fmin(min_depth, D(i + di, j + dj)));
-  const double zm = fmax(z(i, j), -H(i + di, j + dj) + fmin(min_depth, D(i, j)));
-  const double zx = (zp - zm + (airp(i + di, j + dj) - airp(i, j)) * gammai) / (DIR == 0 ? d.dx : d.dy);
-  const double tau = 0.5 * (taus(i, j) + taus(i + di, j + dj));
-  const double Slr = X(i, j) > 0.0 ? fmax(Slr_(i, j), 0.0) : fmin(Slr_(i, j), 0.0);
+  const double zp = fmax(z(i + di, j + dj), -H(i, j) + fmin(min_depth, (double)D(i + di, j + dj)));
+  const double zm = fmax(z(i, j), -H(i + di, j + dj) + fmin(min_depth, (double)D(i, j)));
+  const double zx = (zp - zm + ((double)airp(i + di, j + dj) - (double)airp(i, j)) * gammai) / (DIR == 0 ? d.dx : d.dy);
+  const double tau = 0.5 * ((double)taus(i, j) + (double)taus(i + di, j + dj));
+  const double Slr = X(i, j) > 0.0 ? fmax((double)Slr_(i, j), 0.0) : fmin((double)Slr_(i, j), 0.0);
+  const double Xo = X(i, j), DXo = DX(i, j), dryo = dry(i, j), fCo = fC(i, j), Exo = Ex(i, j), Slxo = Slx(i, j),
+               ro = r(i, j);
   if (DIR == 0)
-    X(i, j) = (X(i, j) - dtm * (g * DX(i, j) * zx + dry(i, j) * (-tau / rho_0 - fC(i, j) + Ex(i, j) + Slx(i, j) + Slr))) /
-              (1.0 + dtm * r(i, j) / DX(i, j));
+    X(i, j) = (Xo - dtm * (g * DXo * zx + dryo * (-tau / rho_0 - fCo + Exo + Slxo + Slr))) / (1.0 + dtm * ro / DXo);
   else
-    X(i, j) = (X(i, j) - dtm * (g * DX(i, j) * zx + dry(i, j) * (-tau / rho_0 + fC(i, j) + Ex(i, j) + Slx(i, j) + Slr))) /
-              (1.0 + dtm * r(i, j) / DX(i, j));
+    X(i, j) = (Xo - dtm * (g * DXo * zx + dryo * (-tau / rho_0 + fCo + Exo + Slxo + Slr))) / (1.0 + dtm * ro / DXo);
 }
 
 // momentum.F90:193-216 / :356-379: Coriolis terms fU (after the U update) and fV (after V).
-template <int DIR>
-__global__ void k_coriolis(Dev d, Bc2 s) {
+template <int DIR, bool MIX>
+__global__ void k_coriolis(Dev d, Bc2 s, Bc2W w) {
   GB_IJ2
   if (!interior(d, i, j)) return;
   if (DIR == 0) {  // fU on V points from the new U
-    W2 U{d, s.f2[U_]}, fU{d, s.f2[FU]}, corv{d, s.f2[CORV]};
+    auto U = f2a<MIX, U_>(d, s, w);
+    auto fU = f2a<MIX, FU>(d, s, w);
+    W2 corv{d, s.f2[CORV]};
     M2 av{d, s.av};
     if (av(i, j) >= 1) {
-      const double Uloc = 0.25 * (U(i - 1, j) + U(i, j) + U(i - 1, j + 1) + U(i, j + 1));
+      const double Uloc = 0.25 * ((double)U(i - 1, j) + (double)U(i, j) + (double)U(i - 1, j + 1) + (double)U(i, j + 1));
       fU(i, j) = corv(i, j) * Uloc;
     } else {
       fU(i, j) = 0.0;
     }
   } else {  // fV on U points from the new V
-    W2 V{d, s.f2[V_]}, fV{d, s.f2[FV]}, coru{d, s.f2[CORU]};
+    auto V = f2a<MIX, V_>(d, s, w);
+    auto fV = f2a<MIX, FV>(d, s, w);
+    W2 coru{d, s.f2[CORU]};
     M2 au{d, s.au};
     if (au(i, j) >= 1) {
-      const double Vloc = 0.25 * (V(i, j - 1) + V(i + 1, j - 1) + V(i, j) + V(i + 1, j));
+      const double Vloc = 0.25 * ((double)V(i, j - 1) + (double)V(i + 1, j - 1) + (double)V(i, j) + (double)V(i + 1, j));
       fV(i, j) = coru(i, j) * Vloc;
     } else {
       fV(i, j) = 0.0;
@@ -184,10 +216,12 @@ __global__ void k_coriolis(Dev d, Bc2 s) {
 }
 
 // m2d.F90:471-472 (Uint, Vint accumulation, FP64) + sealevel.F90:89-112 (zo = z; z update).
-__global__ void k_accum_sealevel(Dev d, Bc2 s, int accumulate) {
+template <bool MIX>
+__global__ void k_accum_sealevel(Dev d, Bc2 s, Bc2W w, int accumulate) {
   GB_IJ2
-  W2 z{d, s.f2[Z]}, zo{d, s.f2[ZO]}, U{d, s.f2[U_]}, V{d, s.f2[V_]}, fwf{d, s.f2[FWF]}, Uint{d, s.f2[UINT]},
-      Vint{d, s.f2[VINT]};
+  auto U = f2a<MIX, U_>(d, s, w);
+  auto V = f2a<MIX, V_>(d, s, w);
+  W2 z{d, s.f2[Z]}, zo{d, s.f2[ZO]}, fwf{d, s.f2[FWF]}, Uint{d, s.f2[UINT]}, Vint{d, s.f2[VINT]};
   M2 az{d, s.az};
   const double dtm = s.par[P_DTM];
   if (accumulate) {
@@ -197,15 +231,21 @@ __global__ void k_accum_sealevel(Dev d, Bc2 s, int accumulate) {
   const double zold = z(i, j);
   zo(i, j) = zold;
   if (interior(d, i, j) && az(i, j) == 1)
-    z(i, j) = zold - dtm * ((U(i, j) * d.dy - U(i - 1, j) * d.dy) + (V(i, j) * d.dx - V(i, j - 1) * d.dx)) * d.ard1 +
+    z(i, j) = zold - dtm * (((double)U(i, j) * d.dy - (double)U(i - 1, j) * d.dy) +
+                            ((double)V(i, j) * d.dx - (double)V(i, j - 1) * d.dx)) * d.ard1 +
               dtm * fwf(i, j);
 }
 
 // depth_update.F90:55-110
-__global__ void k_depth_update(Dev d, Bc2 s) {
+template <bool MIX>
+__global__ void k_depth_update(Dev d, Bc2 s, Bc2W w) {
   GB_IJ2
-  W2 D{d, s.f2[D_]}, z{d, s.f2[Z]}, zo{d, s.f2[ZO]}, H{d, s.f2[HH]}, HU_{d, s.f2[HU]}, HV_{d, s.f2[HV]},
-      DU_{d, s.f2[DU]}, DV_{d, s.f2[DV]}, dry_z{d, s.f2[DRY_Z]}, dry_u{d, s.f2[DRY_U]}, dry_v{d, s.f2[DRY_V]};
+  auto D = f2a<MIX, D_>(d, s, w);
+  auto DU_ = f2a<MIX, DU>(d, s, w);
+  auto DV_ = f2a<MIX, DV>(d, s, w);
+  auto dry_u = f2a<MIX, DRY_U>(d, s, w);
+  auto dry_v = f2a<MIX, DRY_V>(d, s, w);
+  W2 z{d, s.f2[Z]}, zo{d, s.f2[ZO]}, H{d, s.f2[HH]}, HU_{d, s.f2[HU]}, HV_{d, s.f2[HV]}, dry_z{d, s.f2[DRY_Z]};
   M2 az{d, s.az}, au{d, s.au}, av{d, s.av};
   const double min_depth = s.par[P_MIN_DEPTH], crit_depth = s.par[P_CRIT_DEPTH];
   D(i, j) = z(i, j) + H(i, j);
@@ -618,30 +658,59 @@ int uv_advect_2d(getm_ctx* ctx, const getm_bc_state* st, const double* U, const 
   } while (0)
 
 // m2d.F90:412-490 integrate_2d (closed boundaries; no residual; Am <= 0, An_method = 0)
-int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop) {
+int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop, const Bc2W* wp = nullptr) {
   const Dev& d = ctx->dev;
   const Bc2 s = to_bc2(st);
   int* ip = st->ipar;
+  // wp != nullptr: the mixed-precision micro step on the FP32 working copies (no open boundaries)
+  const bool mix = wp != nullptr;
+  const Bc2W w = mix ? *wp : Bc2W{};
+  auto k2 = [&](auto kernel, auto... args) -> int {
+    TimerScope ts(ctx, GETM_TIM_BC2D);
+    kernel<<<grid2(d), kBlk2, 0, ctx->stream>>>(args...);
+    return (int)cudaGetLastError();
+  };
+  int rc = GETM_OK;
   if ((loop - 1) % ip[I_MM] == 0) {
-    if (st->prec3d == 8) GB_K2(k_bottom_friction<double>, d, s, ip[I_RUNTYPE]);
-    else GB_K2(k_bottom_friction<float>, d, s, ip[I_RUNTYPE]);
+    if (mix) rc = k2(k_bottom_friction<float, true>, d, s, w, ip[I_RUNTYPE]);
+    else if (st->prec3d == 8) rc = k2(k_bottom_friction<double, false>, d, s, w, ip[I_RUNTYPE]);
+    else rc = k2(k_bottom_friction<float, false>, d, s, w, ip[I_RUNTYPE]);
+    if (rc) return cuda_fail(ctx, rc, "bottom_friction");
   }
-  int rc = uv_advect_2d(ctx, st, st->f2[U_], st->f2[V_], st->f2[DU], st->f2[DV]);
-  if (rc) return rc;
+  if (mix) {
+    const int hor = ip[I_VEL2D_HOR];
+    if (hor == NOADV) {
+      GB_TRY(cudaMemsetAsync(w.w[UEX], 0, n2d(d) * sizeof(float), ctx->stream), "UEx=0");
+      GB_TRY(cudaMemsetAsync(w.w[VEX], 0, n2d(d) * sizeof(float), ctx->stream), "VEx=0");
+    } else {
+      for (int dir = 0; dir < 2; ++dir) {
+        getm_adv_grid g;
+        grid_for_tag(ctx, dir == 0 ? GETM_U_TAG : GETM_V_TAG, &g);
+        GB_TIMED(GETM_TIM_BC2D,
+                 run_uvadv2d_fused_f32(d, ctx->stream, dir, float(st->par[P_DTM]), hor, w.w[U_], w.w[V_], w.w[DU],
+                                       w.w[DV], g.mask_uflux, g.mask_vflux, g.mask_uupdate, g.mask_vupdate,
+                                       w.w[dir == 0 ? UEX : VEX]),
+                 "uv_advect");
+      }
+    }
+  } else {
+    rc = uv_advect_2d(ctx, st, st->f2[U_], st->f2[V_], st->f2[DU], st->f2[DV]);
+    if (rc) return rc;
+  }
   // umomentum / vmomentum: transport update, mirror_bdy_2d (momentum.F90:190,353), Coriolis term
   auto umom = [&]() -> int {
-    GB_K2(k_momentum<0>, d, s);
-    int r = mirror_bdy<double>(ctx, st->f2[U_], 0, 1);
-    if (r) return r;
-    GB_K2(k_coriolis<0>, d, s);
-    return GETM_OK;
+    int r = mix ? k2(k_momentum<0, true>, d, s, w) : k2(k_momentum<0, false>, d, s, w);
+    if (r) return cuda_fail(ctx, r, "umomentum");
+    if (!mix && (r = mirror_bdy<double>(ctx, st->f2[U_], 0, 1))) return r;
+    r = mix ? k2(k_coriolis<0, true>, d, s, w) : k2(k_coriolis<0, false>, d, s, w);
+    return r ? cuda_fail(ctx, r, "coriolis") : GETM_OK;
   };
   auto vmom = [&]() -> int {
-    GB_K2(k_momentum<1>, d, s);
-    int r = mirror_bdy<double>(ctx, st->f2[V_], 1, 1);
-    if (r) return r;
-    GB_K2(k_coriolis<1>, d, s);
-    return GETM_OK;
+    int r = mix ? k2(k_momentum<1, true>, d, s, w) : k2(k_momentum<1, false>, d, s, w);
+    if (r) return cuda_fail(ctx, r, "vmomentum");
+    if (!mix && (r = mirror_bdy<double>(ctx, st->f2[V_], 1, 1))) return r;
+    r = mix ? k2(k_coriolis<1, true>, d, s, w) : k2(k_coriolis<1, false>, d, s, w);
+    return r ? cuda_fail(ctx, r, "coriolis") : GETM_OK;
   };
   if (ip[I_UFIRST2D]) {
     if ((rc = umom()) || (rc = vmom())) return rc;
@@ -652,10 +721,49 @@ int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop) {
   }
   // update_2d_bdy sets the boundary elevations after the Uint accumulation and before sealevel
   // (m2d.F90:467-476); the accumulation does not touch z, so it runs inside the sealevel kernel
-  if ((rc = bdy_2d(ctx, s, loop))) return rc;
-  GB_K2(k_accum_sealevel, d, s, ip[I_RUNTYPE] > 1 ? 1 : 0);
-  GB_K2(k_depth_update, d, s);
+  if (!mix && (rc = bdy_2d(ctx, s, loop))) return rc;
+  rc = mix ? k2(k_accum_sealevel<true>, d, s, w, ip[I_RUNTYPE] > 1 ? 1 : 0)
+           : k2(k_accum_sealevel<false>, d, s, w, ip[I_RUNTYPE] > 1 ? 1 : 0);
+  if (rc) return cuda_fail(ctx, rc, "sealevel");
+  rc = mix ? k2(k_depth_update<true>, d, s, w) : k2(k_depth_update<false>, d, s, w);
+  if (rc) return cuda_fail(ctx, rc, "depth_update");
   return GETM_OK;
+}
+
+// Copies between the FP64 state and the FP32 working copies of the mixed-precision micro step:
+// to_w != 0 fills the copies of the fields in `mask` (bit q = field q) from the state, to_w == 0
+// writes them back.
+struct FieldList {
+  int n;
+  int q[NF2];
+};
+// The 2D fields are contiguous planes of n2 elements; each grid row (blockIdx.y) copies one field,
+// four elements per thread step (16-byte float4 / two double2 accesses when vec), grid-stride.
+__global__ void k_sync_w2(long long n2, Bc2 s, Bc2W w, FieldList fl, int to_w, int vec) {
+  const int q = fl.q[blockIdx.y];
+  double* a = s.f2[q];
+  float* b = w.w[q];
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long done = 0;
+  if (vec) {
+    const long long n4 = n2 / 4;
+    for (long long t = t0; t < n4; t += stride) {
+      if (to_w) {
+        const double2 x = reinterpret_cast<const double2*>(a)[2 * t], y = reinterpret_cast<const double2*>(a)[2 * t + 1];
+        reinterpret_cast<float4*>(b)[t] = make_float4((float)x.x, (float)x.y, (float)y.x, (float)y.y);
+      } else {
+        const float4 v = reinterpret_cast<const float4*>(b)[t];
+        reinterpret_cast<double2*>(a)[2 * t] = make_double2(v.x, v.y);
+        reinterpret_cast<double2*>(a)[2 * t + 1] = make_double2(v.z, v.w);
+      }
+    }
+    done = n4 * 4;
+  }
+  for (long long c = done + t0; c < n2; c += stride) {
+    if (to_w) b[c] = (float)a[c];
+    else a[c] = (double)b[c];
+  }
 }
 
 template <class R3>
@@ -942,13 +1050,64 @@ int getm_time_loop(getm_ctx* ctx, getm_bc_state* st, int n0, int count) {
   int rc = check_state(ctx, st);
   if (rc) return rc;
   if ((rc = ensure_bc_scratch(ctx, (size_t)st->prec3d))) return rc;
+  // The mixed-precision step (FP32 3D fields) runs its micro steps on FP32 working copies of the
+  // barotropic fields (is_work2) when the fused 2D momentum advection applies and there are no
+  // open boundaries; the elevation and Uint/Vint stay FP64 throughout.
+  const int* ip = st->ipar;
+  const bool mix = st->prec3d == 4 && !ctx->has_bdy &&
+                   (ip[I_VEL2D_HOR] == NOADV ||
+                    (ip[I_VEL2D_SPLIT] == GETM_HALFSPLIT && is_split_scheme(ip[I_VEL2D_HOR])));
+  Bc2W w{};
+  unsigned long long all = 0, written = 0, from3d = 0;
+  if (mix) {
+    const Dev& d = ctx->dev;
+    const long long n2 = n2d(d);
+    int nw = 0;
+    for (int q = 0; q < NF2; ++q) nw += is_work2(q) ? 1 : 0;
+    if (!ctx->w2) {
+      if (cudaMalloc(&ctx->w2, (size_t)nw * n2 * sizeof(float)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ctx, GETM_ERR_NOMEM, "mixed-precision 2D working copies: allocation failed");
+      }
+    }
+    int slot = 0;
+    for (int q = 0; q < NF2; ++q) {
+      w.w[q] = is_work2(q) ? ctx->w2 + (long long)(slot++) * n2 : nullptr;
+      if (is_work2(q)) all |= 1ull << q;
+    }
+    // written by the micro steps; written by the macro step and read by the micro steps
+    for (int q : {U_, V_, D_, DU, DV, DRY_U, DRY_V, FU, FV, RU, RV, RUU, RVV, UEX, VEX}) written |= 1ull << q;
+    for (int q : {SLUX, SLVX, SLRU, SLRV, RU, RV}) from3d |= 1ull << q;
+  }
+  auto sync = [&](unsigned long long mask, int to_w) -> int {
+    TimerScope ts(ctx, GETM_TIM_COPY);
+    FieldList fl{};
+    for (int q = 0; q < NF2; ++q)
+      if ((mask >> q) & 1ull) fl.q[fl.n++] = q;
+    if (fl.n == 0) return GETM_OK;
+    const long long n2 = n2d(ctx->dev);
+    bool vec = n2 % 4 == 0;
+    for (int m = 0; m < fl.n; ++m)
+      vec = vec && reinterpret_cast<uintptr_t>(st->f2[fl.q[m]]) % 16 == 0 &&
+            reinterpret_cast<uintptr_t>(w.w[fl.q[m]]) % 16 == 0;
+    k_sync_w2<<<dim3(592, fl.n, 1), 256, 0, ctx->stream>>>(n2, to_bc2(st), w, fl, to_w, vec ? 1 : 0);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? GETM_OK : cuda_fail(ctx, (int)e, "mixed-precision 2D copies");
+  };
+  if (mix && (rc = sync(all & ~((1ull << UEX) | (1ull << VEX)), 1))) return rc;
+  bool dirty = false;  // working copies newer than the state
   for (int n = n0; n < n0 + count; ++n) {
-    if ((rc = integrate_2d(ctx, st, n))) return rc;
+    if ((rc = integrate_2d(ctx, st, n, mix ? &w : nullptr))) return rc;
+    dirty = mix;
     if (n % st->ipar[I_M] == 0) {
+      if (mix && (rc = sync(written, 0))) return rc;
+      dirty = false;
       rc = st->prec3d == 8 ? integrate_3d<double>(ctx, st, n) : integrate_3d<float>(ctx, st, n);
       if (rc) return rc;
+      if (mix && (rc = sync(from3d, 1))) return rc;
     }
   }
+  if (dirty && (rc = sync(written, 0))) return rc;
   return GETM_OK;
 }
 

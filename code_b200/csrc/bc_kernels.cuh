@@ -568,8 +568,11 @@ __global__ void k_stresses(Dev d, Bc3<R3> s) {
   }
 }
 
-// eqstate.F90:127-137 (linear) + :252-261 (buoyancy) of one cell. FP64: the reference's expression;
-// FP32: explicitly rounded operations, so the scalar and the vectorised kernel agree bit for bit.
+// eqstate.F90:127-137 (linear) + :252-261 (buoyancy) of one cell. FP64: the reference's expression.
+// FP32: the buoyancy from the density anomaly dtr0*(T-T0) + dsr0*(S-S0) directly -- the same value
+// in exact arithmetic, without forming rho_0 + anomaly and subtracting rho_0 again (in FP32 that
+// cancellation keeps only ~1e-4 of the anomaly at rho ~ 1000 kg/m3); explicitly rounded operations,
+// so the scalar and the vectorised kernel agree bit for bit.
 template <class R3>
 __device__ __forceinline__ void eos_lin(const Bc3<R3>& s, R3 t, R3 sal, R3& r, R3& b) {
   const R3 rho_0 = R3(s.par[P_RHO_0]), dtr0 = R3(s.par[P_DTR0]), dsr0 = R3(s.par[P_DSR0]), T0 = R3(s.par[P_T0]),
@@ -579,8 +582,9 @@ __device__ __forceinline__ void eos_lin(const Bc3<R3>& s, R3 t, R3 sal, R3& r, R
     r = rho_0 + dtr0 * (t - T0) + dsr0 * (sal - S0);
     b = x * (r - rho_0);
   } else {
-    r = __fmaf_rn(dsr0, __fsub_rn(sal, S0), __fmaf_rn(dtr0, __fsub_rn(t, T0), rho_0));
-    b = __fmul_rn(x, __fsub_rn(r, rho_0));
+    const float anom = __fmaf_rn(dsr0, __fsub_rn(sal, S0), __fmul_rn(dtr0, __fsub_rn(t, T0)));
+    r = __fadd_rn(rho_0, anom);
+    b = __fmul_rn(x, anom);
   }
 }
 

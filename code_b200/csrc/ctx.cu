@@ -329,6 +329,7 @@ int getm_ctx_destroy(getm_ctx* ctx) {
   for (auto p : ctx->scr) cudaFree(p);
   cudaFree(ctx->bc_scr3);
   cudaFree(ctx->bc_scr2);
+  cudaFree(ctx->w2);
   cudaFree(ctx->adj_scr);
   cudaFree(ctx->adj_store);
   for (void* p : {(void*)ctx->bdy.pts, (void*)ctx->bdy.data, (void*)ctx->bdy.data_u, (void*)ctx->bdy.data_v,

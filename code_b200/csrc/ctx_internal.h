@@ -40,6 +40,9 @@ struct getm_ctx {
   void* bc_scr3 = nullptr;
   size_t bc_scr3_bytes = 0;
   double* bc_scr2 = nullptr;
+  // FP32 working copies of the 2D fields of the mixed-precision micro step (NF2 slots of n2d
+  // floats; only the is_work2 fields are used)
+  float* w2 = nullptr;
   // scratch of the tracer adjoint: ADJ_NSCR 3D arrays (adjoint.cu) and the checkpoints and tapes
   // of the checkpointed gradient
   void* adj_scr = nullptr;

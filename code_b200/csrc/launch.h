@@ -39,6 +39,9 @@ template <class T>
 int run_uvadv2d_fused(const Dev& d, cudaStream_t s, int dir, T dt, int scheme, const double* U, const double* V,
                       const double* DU, const double* DV, const uint8_t* mflux_u, const uint8_t* mflux_v,
                       const uint8_t* mupd_u, const uint8_t* mupd_v, double* Ex);
+int run_uvadv2d_fused_f32(const Dev& d, cudaStream_t s, int dir, float dt, int scheme, const float* U,
+                          const float* V, const float* DU, const float* DV, const uint8_t* mflux_u,
+                          const uint8_t* mflux_v, const uint8_t* mupd_u, const uint8_t* mupd_v, float* Ex);
 
 // Vertical sweep of two tracers in place (H_TAG, no sub-iterations), heights updated once.
 template <class R>

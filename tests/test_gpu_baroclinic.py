@@ -146,3 +146,41 @@ def test_mixed_precision_error_vs_fp64():
         assert errs[k] < 1e-5, errs
     for k in ("z", "U", "V", "uu", "vv"):
         assert errs[k] < 1e-3, errs
+
+
+def test_mixed_closed_basin_error_vs_fp64():
+    """The mixed variant on a closed basin -- its micro steps run on the FP32 working copies of the
+    barotropic fields (elevation and Uint/Vint FP64) -- against the FP64 oracle after 10 macro
+    steps: per-field error relative to the field's scale (stated bounds)."""
+    import torch
+
+    c = S.baroclinic_case(nx=48, ny=40, kmax=10, recipe="islands", land=0.3, M=10, dt3=60.0, seed=6)
+    ref = c.copy()
+    oracle.bc_steps(ref, 1, 100)
+    out, _ = run_gpu(c.copy(dtype3=np.float32), 1, 100, dtype3=torch.float32)
+    errs = {k: field_err(out.f2[k], ref.f2[k]) for k in ("z", "U", "V")}
+    errs.update({k: field_err(out.f3[k], ref.f3[k]) for k in ("uu", "vv", "T", "S")})
+    for k in ("T", "S"):
+        assert errs[k] < 1e-5, errs
+    for k in ("z", "U", "V", "uu", "vv"):
+        assert errs[k] < 1e-3, errs
+
+
+def test_mixed_time_loop_split_calls_match():
+    """The FP32 working copies are written back at the end of each getm_time_loop call and refilled
+    at the start of the next: four calls of 10 micro steps equal one call of 40, bit for bit."""
+    import torch
+
+    c = S.baroclinic_case(nx=40, ny=36, kmax=8, recipe="islands", land=0.3, M=5, dt3=60.0, seed=2)
+    c = c.copy(dtype3=np.float32)
+    a, _ = run_gpu(c, 1, 40, dtype3=torch.float32)
+    ctx, _ = make_ctx(c)
+    st = BcDevice(c, dtype3=torch.float32)
+    for n0 in (1, 11, 21, 31):
+        ctx.time_loop(st, n0, 10)
+    torch.cuda.synchronize()
+    b = st.to_host(c.copy())
+    for k in S.F2_NAMES:
+        assert np.array_equal(a.f2[k], b.f2[k], equal_nan=True), k
+    for k in S.F3_NAMES:
+        assert np.array_equal(a.f3[k], b.f3[k], equal_nan=True), k
