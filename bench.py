@@ -44,7 +44,7 @@ STAGE_WORDS = {"adv_split_u": 8, "adv_split_v": 8, "adv_split_w": 7, "tracer_vdi
 # launches of one macro step in an ncu capture of the 1024 x 1024 x 24 case (the 2048 x 2048 x 50
 # workload is too large to capture under ncu; the sweeps' traffic grows with the cells processed).
 # Source: profiles/traffic_sweeps_mixed_1024x1024x24.md.
-TRAFFIC_PER_CELL_F32 = {}
+TRAFFIC_PER_CELL_F32 = {"adv_split_u": 29.26, "adv_split_v": 29.63, "adv_split_w": 20.83, "tracer_vdiff": 20.38}
 
 
 def parse():
