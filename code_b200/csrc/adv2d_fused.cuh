@@ -17,7 +17,8 @@ namespace gb {
 
 constexpr int FX = 32, FY = 16;             // own tile
 constexpr int RW = FX + 8, RH = FY + 4;     // staged region: i in [-4, FX+3], j in [-2, FY+1]
-constexpr int FT = 256;                     // threads per block
+constexpr int FTY = 8;                      // thread rows: a block is RW x FTY threads, lane x <-> region column
+constexpr int FT = RW * FTY;                // threads per block
 
 template <class T>
 struct Adv2dSmem {
@@ -49,13 +50,15 @@ __global__ void __launch_bounds__(FT) k_uvadv2d_fused(Dev d, T dt, const TI* __r
   constexpr int sub = (S == UPSTREAM) ? 0 : 1;
   const T half = T(0.5), one = T(1), zero = T(0);
   const T dxu = T(d.dx), dyu = T(d.dy), ard1 = T(d.ard1);
-  // ---- stage: region cell (r, q) <-> array (jj0-2+r, ii0-4+q)
-  for (int e = threadIdx.x; e < RH * RW; e += FT) {
-    const int r = e / RW, q = e % RW;
-    const int jj = jj0 - 2 + r, ii = ii0 - 4 + q;
+  // ---- stage: region cell (r, q) <-> array (jj0-2+r, ii0-4+q); thread (q, ty) takes column q
+  const int q = threadIdx.x, ty = threadIdx.y;
+  const int ii = ii0 - 4 + q;
+  const bool iin = ii >= 0 && ii < ni;
+  for (int r = ty; r < RH; r += FTY) {
+    const int jj = jj0 - 2 + r;
     T f0 = zero, ua = zero, dua = zero, va = zero, dva = zero, dio = zero;
     uint8_t a = 0, b = 0, c2 = 0, e2 = 0;
-    if (ii >= 0 && ii < ni && jj >= 0 && jj < nj) {
+    if (iin && jj >= 0 && jj < nj) {
       const long long c = (long long)jj * sj + ii;
       a = mflux_u[c];
       b = mflux_v[c];
@@ -83,100 +86,102 @@ __global__ void __launch_bounds__(FT) k_uvadv2d_fused(Dev d, T dt, const TI* __r
     sm.mpu[r][q] = c2;
     sm.mpv[r][q] = e2;
   }
-  __syncthreads();
-  for (int e = threadIdx.x; e < FX * FY; e += FT) sm.A[e / FX][e % FX] = zero;
-  // region (r, q) -> own cell, for the flux-divergence sum
-  auto own = [&](int r, int q) { return r >= 2 && r < FY + 2 && q >= 4 && q < FX + 4; };
+  // own cells (r in [2, FY+2), q in [4, FX+4)): the flux-divergence sum
+  const bool qown = q >= 4 && q < FX + 4;
+  for (int r = ty; r < FY; r += FTY)
+    if (qown) sm.A[r][q - 4] = zero;
   __syncthreads();
 
   // ---- sweep 1: u/2 on rows r in [0, RH), cells q in [2, RW-2), faces q in [1, RW-3]
   {
     const T dti = half * dt, cdx = dti / dxu;
-    for (int e = threadIdx.x; e < RH * (RW - 3); e += FT) {
-      const int r = e / (RW - 3), q = 1 + e % (RW - 3);  // face between q and q+1
-      const int fa = ii0 - 4 + q;
-      T fl = zero;
-      if (fa >= sub && fa <= ni - 2 - sub)
-        fl = face_flux_s<T, S>(sm.Ua[r][q], sm.DUa[r][q], sm.F0[r][q - 1], sm.F0[r][q], sm.F0[r][q + 1],
-                               sm.F0[r][q + 2], sm.mfu[r][q - 1] != 0, sm.mfu[r][q] != 0, sm.mfu[r][q + 1] != 0,
-                               dti, cdx, zero, false, dxu);
-      sm.FL[r][q] = fl;
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < RH * (RW - 4); e += FT) {
-      const int r = e / (RW - 4), q = 2 + e % (RW - 4);
-      const int ii = ii0 - 4 + q;
-      const T fio = sm.F0[r][q];
-      T fnew = fio;
-      if (ii >= 1 + sub && ii <= ni - 2 - sub && sm.mpu[r][q]) {
-        const T Dio = sm.Di[r][q];
-        const T dD = dti * (sm.Ua[r][q] * dyu - sm.Ua[r][q - 1] * dyu) * ard1;
-        const T Dn = Dio - dD;
-        const T advn = half * (sm.FL[r][q] * dyu - sm.FL[r][q - 1] * dyu) * ard1;
-        sm.Di[r][q] = Dn;
-        fnew = fv_update<T>(Dio, dD, Dn, fio, dt, advn);
-        if (own(r, q)) sm.A[r - 2][q - 4] = sm.A[r - 2][q - 4] + advn;
+    const int fa = ii0 - 4 + q;  // face between q and q+1
+    const bool fok = q >= 1 && q <= RW - 3 && fa >= sub && fa <= ni - 2 - sub;
+    if (q >= 1 && q <= RW - 3)
+      for (int r = ty; r < RH; r += FTY) {
+        T fl = zero;
+        if (fok)
+          fl = face_flux_s<T, S>(sm.Ua[r][q], sm.DUa[r][q], sm.F0[r][q - 1], sm.F0[r][q], sm.F0[r][q + 1],
+                                 sm.F0[r][q + 2], sm.mfu[r][q - 1] != 0, sm.mfu[r][q] != 0, sm.mfu[r][q + 1] != 0,
+                                 dti, cdx, zero, false, dxu);
+        sm.FL[r][q] = fl;
       }
-      sm.F1[r][q] = fnew;
-    }
+    __syncthreads();
+    const bool cok = ii >= 1 + sub && ii <= ni - 2 - sub;
+    if (q >= 2 && q < RW - 2)
+      for (int r = ty; r < RH; r += FTY) {
+        const T fio = sm.F0[r][q];
+        T fnew = fio;
+        if (cok && sm.mpu[r][q]) {
+          const T Dio = sm.Di[r][q];
+          const T dD = dti * (sm.Ua[r][q] * dyu - sm.Ua[r][q - 1] * dyu) * ard1;
+          const T Dn = Dio - dD;
+          const T advn = half * (sm.FL[r][q] * dyu - sm.FL[r][q - 1] * dyu) * ard1;
+          sm.Di[r][q] = Dn;
+          fnew = fv_update<T>(Dio, dD, Dn, fio, dt, advn);
+          if (qown && r >= 2 && r < FY + 2) sm.A[r - 2][q - 4] = sm.A[r - 2][q - 4] + advn;
+        }
+        sm.F1[r][q] = fnew;
+      }
     __syncthreads();
   }
   // ---- sweep 2: v on columns q in [2, RW-2), cells r in [2, RH-2), faces r in [1, RH-3]
   {
     const T dti = one * dt, cdy = dti / dyu;
-    for (int e = threadIdx.x; e < (RH - 3) * (RW - 4); e += FT) {
-      const int r = 1 + e / (RW - 4), q = 2 + e % (RW - 4);  // face between r and r+1
-      const int fa = jj0 - 2 + r;
-      T fl = zero;
-      if (fa >= sub && fa <= nj - 2 - sub)
-        fl = face_flux_s<T, S>(sm.Va[r][q], sm.DVa[r][q], sm.F1[r - 1][q], sm.F1[r][q], sm.F1[r + 1][q],
-                               sm.F1[r + 2][q], sm.mfv[r - 1][q] != 0, sm.mfv[r][q] != 0, sm.mfv[r + 1][q] != 0,
-                               dti, cdy, zero, false, dyu);
-      sm.FL[r][q] = fl;
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < (RH - 4) * (RW - 4); e += FT) {
-      const int r = 2 + e / (RW - 4), q = 2 + e % (RW - 4);
-      const int jj = jj0 - 2 + r;
-      const T fio = sm.F1[r][q];
-      T fnew = fio;
-      if (jj >= 1 + sub && jj <= nj - 2 - sub && sm.mpv[r][q]) {
-        const T Dio = sm.Di[r][q];
-        const T dD = dti * (sm.Va[r][q] * dxu - sm.Va[r - 1][q] * dxu) * ard1;
-        const T Dn = Dio - dD;
-        const T advn = one * (sm.FL[r][q] * dxu - sm.FL[r - 1][q] * dxu) * ard1;
-        sm.Di[r][q] = Dn;
-        fnew = fv_update<T>(Dio, dD, Dn, fio, dt, advn);
-        if (own(r, q)) sm.A[r - 2][q - 4] = sm.A[r - 2][q - 4] + advn;
+    if (q >= 2 && q < RW - 2)
+      for (int r = 1 + ty; r <= RH - 3; r += FTY) {
+        const int fa = jj0 - 2 + r;  // face between r and r+1
+        T fl = zero;
+        if (fa >= sub && fa <= nj - 2 - sub)
+          fl = face_flux_s<T, S>(sm.Va[r][q], sm.DVa[r][q], sm.F1[r - 1][q], sm.F1[r][q], sm.F1[r + 1][q],
+                                 sm.F1[r + 2][q], sm.mfv[r - 1][q] != 0, sm.mfv[r][q] != 0, sm.mfv[r + 1][q] != 0,
+                                 dti, cdy, zero, false, dyu);
+        sm.FL[r][q] = fl;
       }
-      sm.F0[r][q] = fnew;  // the field after v (F0 is no longer needed)
-    }
+    __syncthreads();
+    if (q >= 2 && q < RW - 2)
+      for (int r = 2 + ty; r < RH - 2; r += FTY) {
+        const int jj = jj0 - 2 + r;
+        const T fio = sm.F1[r][q];
+        T fnew = fio;
+        if (jj >= 1 + sub && jj <= nj - 2 - sub && sm.mpv[r][q]) {
+          const T Dio = sm.Di[r][q];
+          const T dD = dti * (sm.Va[r][q] * dxu - sm.Va[r - 1][q] * dxu) * ard1;
+          const T Dn = Dio - dD;
+          const T advn = one * (sm.FL[r][q] * dxu - sm.FL[r - 1][q] * dxu) * ard1;
+          sm.Di[r][q] = Dn;
+          fnew = fv_update<T>(Dio, dD, Dn, fio, dt, advn);
+          if (qown) sm.A[r - 2][q - 4] = sm.A[r - 2][q - 4] + advn;
+        }
+        sm.F0[r][q] = fnew;  // the field after v (F0 is no longer needed)
+      }
     __syncthreads();
   }
   // ---- sweep 3: u/2 on the own rows r in [2, RH-2), own cells q in [4, RW-4), faces q in [3, RW-5]
   {
     const T dti = half * dt, cdx = dti / dxu;
-    for (int e = threadIdx.x; e < (RH - 4) * (RW - 7); e += FT) {
-      const int r = 2 + e / (RW - 7), q = 3 + e % (RW - 7);
-      const int fa = ii0 - 4 + q;
-      T fl = zero;
-      if (fa >= sub && fa <= ni - 2 - sub)
-        fl = face_flux_s<T, S>(sm.Ua[r][q], sm.DUa[r][q], sm.F0[r][q - 1], sm.F0[r][q], sm.F0[r][q + 1],
-                               sm.F0[r][q + 2], sm.mfu[r][q - 1] != 0, sm.mfu[r][q] != 0, sm.mfu[r][q + 1] != 0,
-                               dti, cdx, zero, false, dxu);
-      sm.FL[r][q] = fl;
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < FX * FY; e += FT) {
-      const int r = 2 + e / FX, q = 4 + e % FX;
-      const int ii = ii0 - 4 + q, jj = jj0 - 2 + r;
-      T a = sm.A[r - 2][q - 4];
-      if (ii >= 1 + sub && ii <= ni - 2 - sub && jj < nj && sm.mpu[r][q]) {
-        const T advn = half * (sm.FL[r][q] * dyu - sm.FL[r][q - 1] * dyu) * ard1;
-        a = a + advn;
+    const int fa = ii0 - 4 + q;
+    const bool fok = fa >= sub && fa <= ni - 2 - sub;
+    if (q >= 3 && q <= RW - 5)
+      for (int r = 2 + ty; r < RH - 2; r += FTY) {
+        T fl = zero;
+        if (fok)
+          fl = face_flux_s<T, S>(sm.Ua[r][q], sm.DUa[r][q], sm.F0[r][q - 1], sm.F0[r][q], sm.F0[r][q + 1],
+                                 sm.F0[r][q + 2], sm.mfu[r][q - 1] != 0, sm.mfu[r][q] != 0, sm.mfu[r][q + 1] != 0,
+                                 dti, cdx, zero, false, dxu);
+        sm.FL[r][q] = fl;
       }
-      if (ii < ni && jj < nj) Ex[(long long)jj * sj + ii] = (TI)a;
-    }
+    __syncthreads();
+    if (qown)
+      for (int r = 2 + ty; r < RH - 2; r += FTY) {
+        const int jj = jj0 - 2 + r;
+        T a = sm.A[r - 2][q - 4];
+        if (ii >= 1 + sub && ii <= ni - 2 - sub && jj < nj && sm.mpu[r][q]) {
+          const T advn = half * (sm.FL[r][q] * dyu - sm.FL[r][q - 1] * dyu) * ard1;
+          a = a + advn;
+        }
+        if (ii < ni && jj < nj) Ex[(long long)jj * sj + ii] = (TI)a;
+      }
   }
 }
 
@@ -190,7 +195,8 @@ int launch_uvadv2d_fused(const Dev& d, cudaStream_t s, T dt, const TI* U, const 
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return (int)e;
   dim3 grd((d.ni() + FX - 1) / FX, (d.nj() + FY - 1) / FY, 1);
-  k_uvadv2d_fused<T, S, DIR, TI><<<grd, FT, smem, s>>>(d, dt, U, V, DU, DV, mflux_u, mflux_v, mupd_u, mupd_v, Ex);
+  k_uvadv2d_fused<T, S, DIR, TI><<<grd, dim3(RW, FTY, 1), smem, s>>>(d, dt, U, V, DU, DV, mflux_u, mflux_v, mupd_u,
+                                                                      mupd_v, Ex);
   return (int)cudaGetLastError();
 }
 

@@ -157,13 +157,18 @@ __global__ void k_ip(Dev d, Bc3<R3> s, const R3* zzp) {
 // staged by cp.async into the thread's own shared-memory slots two levels ahead of the
 // elimination (a ring of UVM_SLOTS levels), and the back substitution and the last pass load
 // ahead through registers, so the column's loads are in flight while its recurrence runs.
+// SM: ru, qu (and the back substitution's Res) of the block's columns in dynamic shared memory
+// ([kmax+1][NT] each) instead of the scratch arrays -- FP32 with kmax < 64, where the columns fit
+// next to the staging ring at full occupancy of 64-thread blocks -- which removes their round
+// trips through DRAM.
 constexpr int UVM_SLOTS = 4;
 constexpr int UVM_IN = 11;
 constexpr int UVM_THREADS = 128;
-template <class R3, int DIR>
-__global__ void __launch_bounds__(UVM_THREADS) k_uvmom3d(Dev d, Bc3<R3> s, R3* RUs, R3* QUs) {
+template <class R3, int DIR, bool SM, int NT>
+__global__ void __launch_bounds__(NT) k_uvmom3d(Dev d, Bc3<R3> s, R3* RUs, R3* QUs) {
   using T = R3;
-  __shared__ R3 sl[UVM_SLOTS][UVM_IN][UVM_THREADS];
+  __shared__ R3 sl[UVM_SLOTS][UVM_IN][NT];
+  extern __shared__ unsigned char uvm_cols[];
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   const int kmax = d.kmax;
   const int i = blockIdx.x * blockDim.x + threadIdx.x + d.imin;
@@ -173,7 +178,17 @@ __global__ void __launch_bounds__(UVM_THREADS) k_uvmom3d(Dev d, Bc3<R3> s, R3* R
   if (!(mask(i, j) == 1 || mask(i, j) == 2)) return;
   V3<R3> uu{d, s.f3[DIR == 0 ? UU : VV]}, vv{d, s.f3[DIR == 0 ? VV : UU]}, ho{d, s.f3[DIR == 0 ? HUO : HVO]},
       hn{d, s.f3[DIR == 0 ? HUN : HVN]}, Ex{d, s.f3[DIR == 0 ? UUEX : VVEX]}, idp{d, s.f3[DIR == 0 ? IDPDX : IDPDY]},
-      num{d, s.f3[NUM]}, RU{d, RUs}, QU{d, QUs};
+      num{d, s.f3[NUM]}, RUg{d, RUs}, QUg{d, QUs};
+  R3* const sRU = reinterpret_cast<R3*>(uvm_cols);
+  R3* const sQU = sRU + (long long)(d.kmax + 1) * NT;
+  auto RU = [&](int, int, int k) -> R3& {
+    if constexpr (SM) return sRU[k * NT + tid];
+    else return RUg(i, j, k);
+  };
+  auto QU = [&](int, int, int k) -> R3& {
+    if constexpr (SM) return sQU[k * NT + tid];
+    else return QUg(i, j, k);
+  };
   V2 dry{d, s.f2[DIR == 0 ? DRY_U : DRY_V]}, cor{d, s.f2[DIR == 0 ? CORU : CORV]},
       taus{d, s.f2[DIR == 0 ? TAUSX : TAUSY]}, sseo{d, s.f2[SSEO]}, H{d, s.f2[HH]}, D{d, s.f2[D_]},
       airp{d, s.f2[AIRP]}, rr{d, s.f2[DIR == 0 ? RRU : RRV]}, Uint{d, s.f2[DIR == 0 ? UINT : VINT]},
@@ -193,7 +208,7 @@ __global__ void __launch_bounds__(UVM_THREADS) k_uvmom3d(Dev d, Bc3<R3> s, R3* R
   // the level's inputs into slot k % UVM_SLOTS (an empty group for k < 0 keeps the counting uniform)
   auto issue = [&](int k) {
     if (k >= 0) {
-      R3(*q)[UVM_THREADS] = sl[k & (UVM_SLOTS - 1)];
+      R3(*q)[NT] = sl[k & (UVM_SLOTS - 1)];
       cp_async(&q[0][tid], &ho(i, j, k));
       cp_async(&q[1][tid], &hn(i, j, k));
       cp_async(&q[2][tid], &uu(i, j, k));
@@ -662,12 +677,29 @@ int run_bc3(int which, const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* cons
     case BC3_IP: k_ip<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6]); break;
     case BC3_UUMOM:
     case BC3_VVMOM: {
-      const dim3 b2(32, 4, 1);
-      dim3 g2((d.imax - d.imin + 1 + 31) / 32, (d.jmax - d.jmin + 1 + 3) / 4, 1);
-      if (which == BC3_UUMOM)
-        k_uvmom3d<R3, 0><<<g2, b2, 0, st>>>(d, s, scr[0], scr[1]);
-      else
-        k_uvmom3d<R3, 1><<<g2, b2, 0, st>>>(d, s, scr[0], scr[1]);
+      const int nx = d.imax - d.imin + 1, ny = d.jmax - d.jmin + 1;
+      bool done = false;
+      if constexpr (sizeof(R3) == 4) {
+        if (d.kmax + 1 <= 64) {
+          constexpr int NT = 64;
+          const dim3 b2(32, 2, 1);
+          const dim3 g2((nx + 31) / 32, (ny + 1) / 2, 1);
+          const size_t dyn = 2 * (size_t)(d.kmax + 1) * NT * sizeof(R3);
+          if (which == BC3_UUMOM)
+            k_uvmom3d<R3, 0, true, NT><<<g2, b2, dyn, st>>>(d, s, scr[0], scr[1]);
+          else
+            k_uvmom3d<R3, 1, true, NT><<<g2, b2, dyn, st>>>(d, s, scr[0], scr[1]);
+          done = true;
+        }
+      }
+      if (!done) {
+        const dim3 b2(32, 4, 1);
+        const dim3 g2((nx + 31) / 32, (ny + 3) / 4, 1);
+        if (which == BC3_UUMOM)
+          k_uvmom3d<R3, 0, false, UVM_THREADS><<<g2, b2, 0, st>>>(d, s, scr[0], scr[1]);
+        else
+          k_uvmom3d<R3, 1, false, UVM_THREADS><<<g2, b2, 0, st>>>(d, s, scr[0], scr[1]);
+      }
       break;
     }
     case BC3_SIGMA: {

@@ -134,7 +134,10 @@ __global__ void __launch_bounds__(32 * VKW) k_sweep_v_vec(Dev d, SweepC<R> C, in
                                                         const uint8_t* __restrict__ mflux,
                                                         const uint8_t* __restrict__ mupd, uint8_t* code) {
   constexpr int N = 16 / sizeof(R);
-  constexpr int NA = 2 * NF + 4;  // f(j+2) and fi(j) per field, V, DV, Di, adv of row j
+  // slots: f(j+2) per field; for a single field also fi(j) and adv(j) (a tracer pair reads fi
+  // directly in the rare case that it is not f); V, DV, Di of row j
+  constexpr int XV = NF == 1 ? 2 : NF, XDV = XV + 1, XDI = XV + 2, XAD = XV + 3;
+  constexpr int NA = NF == 1 ? 6 : NF + 3;
   constexpr int sub = (S == UPSTREAM) ? 0 : 1;
   __shared__ VecPack<R, N> sbuf[VST][NA][32 * VKW];
   const int tid = threadIdx.y * 32 + threadIdx.x;
@@ -172,12 +175,12 @@ __global__ void __launch_bounds__(32 * VKW) k_sweep_v_vec(Dev d, SweepC<R> C, in
       for (int n = 0; n < NF; ++n) {
         const bool in = j + 2 < nj;
         cp_async16(&sbuf[st][n][tid], F.t[n].f + (in ? p + 2 * sj : p), in ? vbytes : 0);
-        if (!fis_f[n]) cp_async16(&sbuf[st][NF + n][tid], F.t[n].fi_src + p, vbytes);
+        if (NF == 1 && !fis_f[n]) cp_async16(&sbuf[st][1][tid], F.t[n].fi_src + p, vbytes);
       }
-      cp_async16(&sbuf[st][2 * NF][tid], V + p, vbytes);
-      cp_async16(&sbuf[st][2 * NF + 1][tid], DV + p, vbytes);
-      cp_async16(&sbuf[st][2 * NF + 2][tid], Di_src + p, vbytes);
-      if (NF == 1 && adv) cp_async16(&sbuf[st][2 * NF + 3][tid], adv + p, vbytes);
+      cp_async16(&sbuf[st][XV][tid], V + p, vbytes);
+      cp_async16(&sbuf[st][XDV][tid], DV + p, vbytes);
+      cp_async16(&sbuf[st][XDI][tid], Di_src + p, vbytes);
+      if (NF == 1 && adv) cp_async16(&sbuf[st][XAD][tid], adv + p, vbytes);
     }
     cp_async_commit();
   };
@@ -232,9 +235,9 @@ __global__ void __launch_bounds__(32 * VKW) k_sweep_v_vec(Dev d, SweepC<R> C, in
     }
     cp_async_wait<VST - 1>();
     R Vc[N], DVc[N], Dio[N];
-    lds_vec<R, N>(sbuf[st][2 * NF][tid], Vc);
-    lds_vec<R, N>(sbuf[st][2 * NF + 1][tid], DVc);
-    lds_vec<R, N>(sbuf[st][2 * NF + 2][tid], Dio);
+    lds_vec<R, N>(sbuf[st][XV][tid], Vc);
+    lds_vec<R, N>(sbuf[st][XDV][tid], DVc);
+    lds_vec<R, N>(sbuf[st][XDI][tid], Dio);
     R fio[NF][N];
 #pragma unroll
     for (int n = 0; n < NF; ++n) {
@@ -251,7 +254,8 @@ __global__ void __launch_bounds__(32 * VKW) k_sweep_v_vec(Dev d, SweepC<R> C, in
 #pragma unroll
         for (int m = 0; m < N; ++m) fio[n][m] = w[n][1][m];
       } else {
-        lds_vec<R, N>(sbuf[st][NF + n][tid], fio[n]);
+        if constexpr (NF == 1) lds_vec<R, N>(sbuf[st][1][tid], fio[n]);
+        else ld_row<R, N>(F.t[n].fi_src + base + (long long)j * sj, full, navail, fio[n]);
       }
     }
     const long long p = base + (long long)j * sj;
@@ -282,7 +286,7 @@ __global__ void __launch_bounds__(32 * VKW) k_sweep_v_vec(Dev d, SweepC<R> C, in
       Dn[m] = upd ? Dio[m] - dDv[m] : Dio[m];
     }
     R ad[N];
-    if (NF == 1 && adv) lds_vec<R, N>(sbuf[st][2 * NF + 3][tid], ad);
+    if (NF == 1 && adv) lds_vec<R, N>(sbuf[st][XAD][tid], ad);
 #pragma unroll
     for (int n = 0; n < NF; ++n) {
       R fo[N];
@@ -324,7 +328,9 @@ __global__ void __launch_bounds__(32 * UWB) k_sweep_u_vec(Dev d, SweepC<R> C, in
                                                         const uint8_t* __restrict__ mflux,
                                                         const uint8_t* __restrict__ mupd, uint8_t* code) {
   constexpr int N = 16 / sizeof(R);
-  constexpr int NA = 2 * NF + 4;  // f and fi per field, U, DU, Di, adv
+  // slots: f per field; for a single field also fi and adv; U, DU, Di
+  constexpr int XU = NF == 1 ? 2 : NF, XDU = XU + 1, XDI = XU + 2, XAD = XU + 3;
+  constexpr int NA = NF == 1 ? 6 : NF + 3;
   constexpr int sub = (S == UPSTREAM) ? 0 : 1;
   constexpr unsigned FULL = 0xffffffffu;
   __shared__ VecPack<R, N> sbuf[VST][NA][32 * UWB];
@@ -380,13 +386,13 @@ __global__ void __launch_bounds__(32 * UWB) k_sweep_u_vec(Dev d, SweepC<R> C, in
 #pragma unroll
       for (int n = 0; n < NF; ++n) {
         cp_async16(&sbuf[st][n][tid], F.t[n].f + p, vbytes);
-        if (own && !fis_f[n]) cp_async16(&sbuf[st][NF + n][tid], F.t[n].fi_src + p, vbytes);
+        if (NF == 1 && own && !fis_f[n]) cp_async16(&sbuf[st][1][tid], F.t[n].fi_src + p, vbytes);
       }
-      cp_async16(&sbuf[st][2 * NF][tid], U + p, vbytes);
-      cp_async16(&sbuf[st][2 * NF + 1][tid], DU + p, vbytes);
+      cp_async16(&sbuf[st][XU][tid], U + p, vbytes);
+      cp_async16(&sbuf[st][XDU][tid], DU + p, vbytes);
       if (own) {
-        cp_async16(&sbuf[st][2 * NF + 2][tid], Di_src + p, vbytes);
-        if (NF == 1 && adv && any) cp_async16(&sbuf[st][2 * NF + 3][tid], adv + p, vbytes);
+        cp_async16(&sbuf[st][XDI][tid], Di_src + p, vbytes);
+        if (NF == 1 && adv && any) cp_async16(&sbuf[st][XAD][tid], adv + p, vbytes);
       }
     }
     cp_async_commit();
@@ -412,8 +418,8 @@ __global__ void __launch_bounds__(32 * UWB) k_sweep_u_vec(Dev d, SweepC<R> C, in
     }
     {
       R u[N], du[N];
-      lds_vec<R, N>(sbuf[st][2 * NF][tid], u);
-      lds_vec<R, N>(sbuf[st][2 * NF + 1][tid], du);
+      lds_vec<R, N>(sbuf[st][XU][tid], u);
+      lds_vec<R, N>(sbuf[st][XDU][tid], du);
       Uv[0] = __shfl_up_sync(FULL, u[N - 1], 1);
       DUv[0] = __shfl_up_sync(FULL, du[N - 1], 1);
 #pragma unroll
@@ -453,14 +459,14 @@ __global__ void __launch_bounds__(32 * UWB) k_sweep_u_vec(Dev d, SweepC<R> C, in
       st_codes<N>(code + p, full, navail, cv);
     }
     R Dio[N], Dn[N], dDv[N];
-    lds_vec<R, N>(sbuf[stc][2 * NF + 2][tid], Dio);
+    lds_vec<R, N>(sbuf[stc][XDI][tid], Dio);
 #pragma unroll
     for (int q = 0; q < N; ++q) {
       dDv[q] = cell_dD<R>(C, Uv[q + 1], Uv[q]);
       Dn[q] = updm[q] ? Dio[q] - dDv[q] : Dio[q];
     }
     R ad[N];
-    if (NF == 1 && adv && any) lds_vec<R, N>(sbuf[stc][2 * NF + 3][tid], ad);
+    if (NF == 1 && adv && any) lds_vec<R, N>(sbuf[stc][XAD][tid], ad);
 #pragma unroll
     for (int n = 0; n < NF; ++n) {
       R fio[N], fo[N];
@@ -468,7 +474,8 @@ __global__ void __launch_bounds__(32 * UWB) k_sweep_u_vec(Dev d, SweepC<R> C, in
 #pragma unroll
         for (int q = 0; q < N; ++q) fio[q] = f[n][q + 2];
       } else {
-        lds_vec<R, N>(sbuf[stc][NF + n][tid], fio);
+        if constexpr (NF == 1) lds_vec<R, N>(sbuf[stc][1][tid], fio);
+        else ld_row<R, N>(F.t[n].fi_src + p, full, navail, fio);
       }
 #pragma unroll
       for (int q = 0; q < N; ++q) {
