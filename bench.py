@@ -65,6 +65,10 @@ def parse():
                     help="run the mixed-precision accuracy configuration (the 'rotation' recipe: flat 20 m, "
                          "dx = 500 m, closed, solid-body rotation and a temperature anomaly; --nx/--ny/--kmax) for "
                          "STEPS macro steps in FP64 and in the mixed variant and print the per-field errors")
+    ap.add_argument("--configs", action="store_true",
+                    help="time the smaller configurations: the 128x128x20 tracer rotation (200 steps) and the "
+                         "512x512x30 tidal shelf (100 macro steps), GPU FP64 / mixed and the CPU oracle on the "
+                         "host cores (a 5-macro-step sample for the shelf); one JSON line")
     ap.add_argument("--tile-sweeps", action="store_true",
                     help="use the shared-memory tile kernels for every horizontal sweep (comparison)")
     ap.add_argument("--tracer-adjoint", action="store_true",
@@ -255,6 +259,81 @@ def run_tracer_adjoint(args):
     print(json.dumps(out), flush=True)
 
 
+def run_configs(args):
+    """Device and host throughput of the tracer-rotation and tidal-shelf configurations."""
+    import numpy as np
+    import torch
+
+    import oracle
+    from code_b200 import cases
+    from code_b200 import state as S
+    from code_b200.getm import BcDevice, Context
+
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    out = {"cores": cores, "unit": UNIT}
+    # tracer rotation: 128 x 128 x 20, SUPERBEE HALFSPLIT, implicit diffusion, 200 steps
+    c = cases.tracer_rotation()
+    p = c.par
+    names = ("uu", "vv", "ww", "hun", "hvn", "ho", "hn", "nuh")
+    cells = c.grid.nx * c.grid.ny * c.grid.kmax
+    res = {}
+    for key, dt in (("gpu_fp64", torch.float64), ("gpu_fp32", torch.float32)):
+        ctx = Context(c.grid)
+        ctx.init_advection(*[torch.from_numpy(m).cuda() for m in c.masks()])
+        f = torch.from_numpy(c["f"]).cuda().to(dt)
+        t = [torch.from_numpy(c[n]).cuda().to(dt) for n in names]
+        for _ in range(3):
+            ctx.tracer_step(p["dt"], f.clone(), *t, p["split"], p["hscheme"], p["vscheme"], p["AH"], p["cnpar"],
+                            p["avmol"])
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(200):
+            ctx.tracer_step(p["dt"], f, *t, p["split"], p["hscheme"], p["vscheme"], p["AH"], p["cnpar"], p["avmol"])
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        res[key] = {"ms_per_step": ms / 200, "value": cells * 200 / (ms / 1e3)}
+        ctx.close()
+    o = oracle.Oracle(c.grid)
+    of = c["f"].copy()
+    t0 = time.perf_counter()
+    o.tracer_steps(c.masks(), 200, p["dt"], of, *[c[n] for n in names], p["split"], p["hscheme"], p["vscheme"],
+                   p["AH"], p["cnpar"], p["avmol"])
+    el = time.perf_counter() - t0
+    res["cpu_oracle_fp64"] = {"ms_per_step": el * 1e3 / 200, "value": cells * 200 / el}
+    out["tracer_rotation_128x128x20"] = res
+    # tidal shelf: 512 x 512 x 30, M = 20, M2 tide (1 m) on the western boundary
+    g = S.Grid(512, 512, 30, 1000.0, 1000.0)
+    b = S.OpenBoundaries(west=[(g.imin, g.jmin, g.jmax, S.CLAMPED)], ramp=40, amp=1.0, period=44712.0)
+    c2 = S.baroclinic_case(nx=512, ny=512, kmax=30, recipe="shelf", M=20, dt3=60.0, seed=3, bdy=b)
+    cells = 512 * 512 * 30
+    res = {}
+    for key, dt3 in (("gpu_fp64", torch.float64), ("gpu_mixed", torch.float32)):
+        cc = c2.copy(dtype3=np.float32 if dt3 == torch.float32 else None)
+        ctx = Context(cc.grid)
+        ctx.init_advection(*[torch.from_numpy(m).cuda() for m in cc.masks()])
+        ctx.set_open_boundaries(cc.bdy)
+        st = BcDevice(cc, dtype3=dt3)
+        ctx.time_loop(st, 1, 20 * 3)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ctx.time_loop(st, 61, 20 * 100)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        res[key] = {"ms_per_step": ms / 100, "value": cells * 100 / (ms / 1e3)}
+        ctx.close()
+        del st
+    cs = c2.copy()
+    t0 = time.perf_counter()
+    oracle.bc_steps(cs, 1, 20 * 5)
+    el = time.perf_counter() - t0
+    res["cpu_oracle_fp64"] = {"ms_per_step": el * 1e3 / 5, "value": cells * 5 / el, "sample": "5 macro steps"}
+    out["tidal_shelf_512x512x30"] = res
+    print(json.dumps(out), flush=True)
+
+
 def run_accuracy(args):
     """Mixed variant against the FP64 variant after args.accuracy macro steps: per field, the largest
     and the RMS difference relative to the largest magnitude of the FP64 field."""
@@ -310,6 +389,10 @@ def main():
     if args.accuracy > 0:
         if rank == 0:
             run_accuracy(args)
+        return
+    if args.configs:
+        if rank == 0:
+            run_configs(args)
         return
     import torch
     import torch.distributed as dist

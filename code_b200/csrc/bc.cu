@@ -105,6 +105,86 @@ __global__ void k_bottom_friction(Dev d, Bc2 s, Bc2W w, int runtype) {
   }
 }
 
+// FP32 form of k_bottom_friction on a 32x8 tile: the velocity quotients U/DU and V/DV of the tile
+// and its one-cell halo are formed once into shared memory (the 4-point averages of the U and V
+// points read them from there); the same operations as the per-thread form, so the same values.
+template <bool MIX>
+__global__ void __launch_bounds__(256) k_bottom_friction_f32t(Dev d, Bc2 s, Bc2W w, int runtype) {
+  __shared__ float suq[10][34], svq[10][34];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i0 = blockIdx.x * 32 + d.imin - HALO, j0 = blockIdx.y * 8 + d.jmin - HALO;
+  auto U = f2a<MIX, U_>(d, s, w);
+  auto V = f2a<MIX, V_>(d, s, w);
+  auto DU_ = f2a<MIX, DU>(d, s, w);
+  auto DV_ = f2a<MIX, DV>(d, s, w);
+  for (int e = ty * 32 + tx; e < 340; e += 256) {
+    const int r = e / 34, q = e % 34;
+    const int ii = i0 - 1 + q, jj = j0 - 1 + r;
+    float uq = 0.f, vq = 0.f;
+    if (ii >= d.imin - HALO && ii <= d.imax + HALO && jj >= d.jmin - HALO && jj <= d.jmax + HALO) {
+      uq = float(U(ii, jj)) / float(DU_(ii, jj));
+      vq = float(V(ii, jj)) / float(DV_(ii, jj));
+    }
+    suq[r][q] = uq;
+    svq[r][q] = vq;
+  }
+  __syncthreads();
+  const int i = i0 + tx, j = j0 + ty;
+  if (i > d.imax + HALO || j > d.jmax + HALO) return;
+  auto UQ = [&](int di, int dj) { return suq[ty + 1 + dj][tx + 1 + di]; };
+  auto VQ = [&](int di, int dj) { return svq[ty + 1 + dj][tx + 1 + di]; };
+  auto ruu = f2a<MIX, RUU>(d, s, w);
+  auto rvv = f2a<MIX, RVV>(d, s, w);
+  auto ru = f2a<MIX, RU>(d, s, w);
+  auto rv = f2a<MIX, RV>(d, s, w);
+  W2 zub{d, s.f2[ZUB]}, zvb{d, s.f2[ZVB]}, zub0{d, s.f2[ZUB0]}, zvb0{d, s.f2[ZVB0]};
+  M2 au{d, s.au}, av{d, s.av};
+  using T = float;
+  const T kappa = T(s.par[P_KAPPA]), avmmol = T(s.par[P_AVMMOL]), min_depth = T(s.par[P_MIN_DEPTH]);
+  const T q = T(0.25), h = T(0.5);
+  const bool in = interior(d, i, j);
+  if (i <= d.imax + HALO - 1 && au(i, j) > 0) {
+    const T vloc = in ? q * (VQ(0, 0) + VQ(1, 0) + VQ(0, -1) + VQ(1, -1)) : T(0);
+    const T uloc = UQ(0, 0);
+    const T HHl = fmax(min_depth, T(DU_(i, j)));
+    const T zb = T(zub(i, j));
+    T x = kappa / log((zb + h * HHl) / zb);
+    T r = x * x;
+    if (runtype == 1) {
+      const T fricvel = sqrt(r * (uloc * uloc + vloc * vloc));
+      const T zn = fmin(HHl, T(zub0(i, j)) + T(0.1) * avmmol / fmax(avmmol, fricvel));
+      zub(i, j) = zn;
+      r = (zn + h * HHl) / zn;
+      x = kappa / log(r);
+      r = x * x;
+    }
+    ruu(i, j) = r;
+    ru(i, j) = r * sqrt(uloc * uloc + vloc * vloc);
+  }
+  if (j <= d.jmax + HALO - 1 && av(i, j) > 0) {
+    T uloc;
+    if (in)
+      uloc = q * (UQ(0, 0) + UQ(-1, 0) + UQ(0, 1) + UQ(-1, 1));
+    else
+      uloc = (i <= d.imax + HALO - 1 && au(i, j) > 0) ? UQ(0, 0) : T(0);
+    const T vloc = VQ(0, 0);
+    const T HHl = fmax(min_depth, T(DV_(i, j)));
+    const T zb = T(zvb(i, j));
+    T x = kappa / log((zb + h * HHl) / zb);
+    T r = x * x;
+    if (runtype == 1) {
+      const T fricvel = sqrt(r * (uloc * uloc + vloc * vloc));
+      const T zn = fmin(HHl, T(zvb0(i, j)) + T(0.1) * avmmol / fmax(avmmol, fricvel));
+      zvb(i, j) = zn;
+      r = (zn + h * HHl) / zn;
+      x = kappa / log(r);
+      r = x * x;
+    }
+    rvv(i, j) = r;
+    rv(i, j) = r * sqrt(uloc * uloc + vloc * vloc);
+  }
+}
+
 // uv_advect.F90:94-110 (U grid) / :204-220 (V grid): quantities of the 2D momentum volumes, in
 // the working type T of the 2D advection (FP64 in the plain step, FP32 in the mixed step), plus
 // the control-volume depth Do (= DU or DV) in T.
@@ -672,9 +752,18 @@ int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop, const Bc2W* wp = nu
   };
   int rc = GETM_OK;
   if ((loop - 1) % ip[I_MM] == 0) {
-    if (mix) rc = k2(k_bottom_friction<float, true>, d, s, w, ip[I_RUNTYPE]);
-    else if (st->prec3d == 8) rc = k2(k_bottom_friction<double, false>, d, s, w, ip[I_RUNTYPE]);
-    else rc = k2(k_bottom_friction<float, false>, d, s, w, ip[I_RUNTYPE]);
+    const dim3 gt((d.ni() + 31) / 32, (d.nj() + 7) / 8, 1);
+    if (mix) {
+      TimerScope ts(ctx, GETM_TIM_BC2D);
+      k_bottom_friction_f32t<true><<<gt, dim3(32, 8, 1), 0, ctx->stream>>>(d, s, w, ip[I_RUNTYPE]);
+      rc = (int)cudaGetLastError();
+    } else if (st->prec3d == 8) {
+      rc = k2(k_bottom_friction<double, false>, d, s, w, ip[I_RUNTYPE]);
+    } else {
+      TimerScope ts(ctx, GETM_TIM_BC2D);
+      k_bottom_friction_f32t<false><<<gt, dim3(32, 8, 1), 0, ctx->stream>>>(d, s, w, ip[I_RUNTYPE]);
+      rc = (int)cudaGetLastError();
+    }
     if (rc) return cuda_fail(ctx, rc, "bottom_friction");
   }
   if (mix) {
@@ -787,7 +876,6 @@ int integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
   const Bc2 s2 = to_bc2(st);
   int* ip = st->ipar;
   const long long n3 = n3d(d);
-  const size_t b3 = (size_t)n3 * sizeof(R3);
   R3** f3 = (R3**)st->f3;
   int rc;
   // start_macro
@@ -798,11 +886,9 @@ int integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
     if ((rc = bc3<R3>(ctx, st, BC3_ZZ, GETM_TIM_BC3D))) return rc;
     if ((rc = bc3<R3>(ctx, st, BC3_IP, GETM_TIM_IP))) return rc;
   }
-  {
-    TimerScope ts(ctx, GETM_TIM_COPY);
-    GB_TRY(cudaMemcpyAsync(f3[HUO], f3[HUN], b3, cudaMemcpyDeviceToDevice, s), "huo=hun");
-    GB_TRY(cudaMemcpyAsync(f3[HVO], f3[HVN], b3, cudaMemcpyDeviceToDevice, s), "hvo=hvn");
-  }
+  // m3d.F90 sets huo = hun, hvo = hvn here for uu/vv_momentum_3d; sigma_coordinates below then
+  // recomputes huo/hvo from the same elevations, to the same values. The momentum kernels read
+  // hun/hvn as their old heights instead, so the two 3D copies are not made.
   // uu/vv_momentum_3d, each followed by its mirror_bdy_3d (uu_momentum_3d.F90:389, vv_momentum_3d.F90:400)
   auto uum = [&]() -> int {
     int r = bc3<R3>(ctx, st, BC3_UUMOM, GETM_TIM_MOM3D);

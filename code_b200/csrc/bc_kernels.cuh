@@ -145,6 +145,8 @@ __global__ void k_ip(Dev d, Bc3<R3> s, const R3* zzp) {
 }
 
 // uu_momentum_3d.F90:169-304 (DIR 0) / vv_momentum_3d.F90:174-315 (DIR 1), kumin = 1: explicit
+// (the old heights huo/hvo equal hun/hvn at this point of integrate_3d, m3d.F90, and are read from
+// hun/hvn);
 // terms, implicit vertical viscosity and the transport correction to the depth-integrated
 // transport Uint. One thread per column. The column arithmetic type T is FP64 for the FP64 step
 // (the reference's expressions in the reference's order) and FP32 for the mixed step (divisions by
@@ -176,7 +178,7 @@ __global__ void __launch_bounds__(NT) k_uvmom3d(Dev d, Bc3<R3> s, R3* RUs, R3* Q
   if (i > d.imax || j > d.jmax) return;  // no barrier in this kernel
   I2 mask{d, DIR == 0 ? s.au : s.av};
   if (!(mask(i, j) == 1 || mask(i, j) == 2)) return;
-  V3<R3> uu{d, s.f3[DIR == 0 ? UU : VV]}, vv{d, s.f3[DIR == 0 ? VV : UU]}, ho{d, s.f3[DIR == 0 ? HUO : HVO]},
+  V3<R3> uu{d, s.f3[DIR == 0 ? UU : VV]}, vv{d, s.f3[DIR == 0 ? VV : UU]}, ho{d, s.f3[DIR == 0 ? HUN : HVN]},
       hn{d, s.f3[DIR == 0 ? HUN : HVN]}, Ex{d, s.f3[DIR == 0 ? UUEX : VVEX]}, idp{d, s.f3[DIR == 0 ? IDPDX : IDPDY]},
       num{d, s.f3[NUM]}, RUg{d, RUs}, QUg{d, QUs};
   R3* const sRU = reinterpret_cast<R3*>(uvm_cols);
