@@ -42,8 +42,10 @@ STAGE_WORDS = {"adv_split_u": 8, "adv_split_v": 8, "adv_split_w": 7, "tracer_vdi
                "internal_pressure": 6}
 # DRAM bytes (read + write) per interior cell per launch of the FP32 stages, averaged over the
 # launches of one macro step in an ncu capture of the 1024 x 1024 x 24 case (the 2048 x 2048 x 50
-# workload is too large to capture under ncu; the sweeps' traffic grows with the cells processed).
-# Source: profiles/traffic_sweeps_mixed_1024x1024x24.md.
+# workload is too large to capture under ncu; the sweeps' traffic grows with the cells processed):
+# ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum on the 17 advection and diffusion
+# launches of the timed step of `bench.py --nx 1024 --ny 1024 --kmax 24 --steps 1 --warmup 1
+# --variants mixed --no-cpu-baseline --adj-steps 0`.
 TRAFFIC_PER_CELL_F32 = {"adv_split_u": 29.26, "adv_split_v": 29.63, "adv_split_w": 20.83, "tracer_vdiff": 20.38}
 
 

@@ -12,7 +12,7 @@
  * Calling convention: one host thread per context; every call is stream-ordered on the context's
  * stream and returns a status (0 = OK, < 0 = error, see GETM_ERR_*). No call exits the process:
  * where the reference calls stop / getm_error, the entry point returns an error code and the
- * Fortran-side wrapper turns it into getm_error (INTEGRATION.md shows that wrapper).
+ * Fortran-side wrapper turns it into getm_error.
  *
  * Suffixes: no suffix = FP64 (the reference's REALTYPE, cppdefs.h:130-131),
  *           _f32      = FP32 arithmetic for the same routine (the mixed-precision variant).
