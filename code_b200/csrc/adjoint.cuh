@@ -491,7 +491,7 @@ __global__ void __launch_bounds__(32 * UWB) k_adj_sweep_u_vec(Dev d, R dt, R spl
 // step j it forms the factors of row j+2 and the weights of face j+1, and completes cell j from
 // the weights of faces j+1, j, j-1, j-2 kept in registers. Rows are staged two steps ahead by
 // cp.async.
-template <class R, int S>
+template <class R, int S, int VN = 4>
 __global__ void __launch_bounds__(32 * VKW) k_adj_sweep_v_vec(Dev d, R dt, R splitfac, R AH, int nk, int rows,
                                                             bool copy0, const R* __restrict__ gbar,
                                                             R* __restrict__ fbar, const R* __restrict__ Dio,
@@ -500,8 +500,9 @@ __global__ void __launch_bounds__(32 * VKW) k_adj_sweep_v_vec(Dev d, R dt, R spl
                                                             const uint8_t* __restrict__ mupd,
                                                             const uint8_t* __restrict__ code) {
   static_assert(sizeof(R) == 4, "vectorised adjoint sweeps are FP32");
-  constexpr int N = 4;
-  constexpr int NA = 5;  // gbar(j+2), Dio(j+2), V(j+2), DV(j+1), codes(j+1)
+  constexpr int N = VN;  // cells per lane (4: float4; 2: float2, half the registers)
+  constexpr int VB = N * (int)sizeof(R);
+  constexpr int NA = 5;  // gbar(j+2), Dio(j+2), V(j+2), DV(j+1), codes(j+1) (the codes staged for N = 4)
   constexpr int sub = (S == UPSTREAM) ? 0 : 1;
   __shared__ VecPack<R, N> sbuf[VST][NA][32 * VKW];
   const int tid = threadIdx.y * 32 + threadIdx.x;
@@ -541,11 +542,7 @@ __global__ void __launch_bounds__(32 * VKW) k_adj_sweep_v_vec(Dev d, R dt, R spl
   };
   auto crow_of = [&](int j) -> uint32_t {  // code bytes of face row j
     if (S == UPSTREAM || j < 0 || j >= nj) return 0u;
-    const uint8_t* p = code + base + (long long)j * sj;
-    if (full) return *reinterpret_cast<const uint32_t*>(p);
-    uint32_t x = 0;
-    for (int m = 0; m < navail; ++m) x |= (uint32_t)p[m] << (8 * m);
-    return x;
+    return ld_mask_w<N>(code + base + (long long)j * sj, full, navail);  // N bytes, N-byte aligned
   };
   // factors of row r from its cotangent, heights and the transports of its faces
   auto factors = [&](int r, const R (&g)[N], const R (&hio)[N], const R (&Vr)[N], const R (&Vrm1)[N],
@@ -579,12 +576,12 @@ __global__ void __launch_bounds__(32 * VKW) k_adj_sweep_v_vec(Dev d, R dt, R spl
     if (j < j1) {
       const long long p = base + (long long)j * sj;
       const bool r2 = j + 2 < nj;
-      cp_async16(&sbuf[st][0][tid], r2 ? gbar + p + 2 * sj : gbar + p, r2 ? vbytes : 0);
-      cp_async16(&sbuf[st][1][tid], r2 ? Dio + p + 2 * sj : Dio + p, r2 ? vbytes : 0);
-      cp_async16(&sbuf[st][2][tid], r2 ? V + p + 2 * sj : V + p, r2 ? vbytes : 0);
+      cp_async_v<VB>(&sbuf[st][0][tid], r2 ? gbar + p + 2 * sj : gbar + p, r2 ? vbytes : 0);
+      cp_async_v<VB>(&sbuf[st][1][tid], r2 ? Dio + p + 2 * sj : Dio + p, r2 ? vbytes : 0);
+      cp_async_v<VB>(&sbuf[st][2][tid], r2 ? V + p + 2 * sj : V + p, r2 ? vbytes : 0);
       const bool r1 = j + 1 < nj;
-      cp_async16(&sbuf[st][3][tid], r1 ? DV + p + sj : DV + p, r1 ? vbytes : 0);
-      if (S != UPSTREAM && full && r1)
+      cp_async_v<VB>(&sbuf[st][3][tid], r1 ? DV + p + sj : DV + p, r1 ? vbytes : 0);
+      if (N == 4 && S != UPSTREAM && full && r1)
         cp_async(reinterpret_cast<float*>(&sbuf[st][4][tid]), reinterpret_cast<const float*>(code + p + sj));
     }
     cp_async_commit();
@@ -667,7 +664,7 @@ __global__ void __launch_bounds__(32 * VKW) k_adj_sweep_v_vec(Dev d, R dt, R spl
       lds_vec<R, N>(sbuf[st][3][tid], DVj1);
       uint32_t cw = 0;
       if (S != UPSTREAM && j + 1 < nj) {
-        if (full) cw = *reinterpret_cast<const uint32_t*>(&sbuf[st][4][tid]);
+        if (N == 4 && full) cw = *reinterpret_cast<const uint32_t*>(&sbuf[st][4][tid]);
         else cw = crow_of(j + 1);
       }
       st = st == VST - 1 ? 0 : st + 1;
@@ -917,13 +914,13 @@ int run_adj_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int 
         return (int)cudaGetLastError();
       }
       if (DIR == 1 && vec_layout<R>(d, nk + (copy0 ? 1 : 0), {gbar, fbar, Dio, U, DU}, {mflux, mupd, code})) {
-        constexpr int N = 4;
+        constexpr int N = 2;  // two cells per lane (the kernel's VN)
         const long long nx = (d.ni() + 32 * N - 1) / (32 * N), nzv = (nk + VKW - 1) / VKW;
         int rows = VJS;
         while (rows > 8 && nx * ((d.nj() + rows - 1) / rows) * nzv * VKW < 148LL * 24) rows /= 2;
         dim3 blk(32, VKW, 1);
         dim3 grd((unsigned)nx, (d.nj() + rows - 1) / rows, (unsigned)nzv);
-        k_adj_sweep_v_vec<R, S><<<grd, blk, 0, s>>>(d, dt, splitfac, AH, nk, rows, copy0, gbar, fbar, Dio, U, DU,
+        k_adj_sweep_v_vec<R, S, 2><<<grd, blk, 0, s>>>(d, dt, splitfac, AH, nk, rows, copy0, gbar, fbar, Dio, U, DU,
                                                     mflux, mupd, code);
         return (int)cudaGetLastError();
       }

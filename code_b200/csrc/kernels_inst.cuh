@@ -72,14 +72,15 @@ int run_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int sche
           return (int)cudaGetLastError();
         }
         if (vec) {
+          constexpr int VN = 16 / sizeof(R);  // float4 lanes (float2 lanes measured slower)
           // rows per thread: VJS, halved while the grid would give fewer than ~24 warps per SM
-          const long long nx = (d.ni() + 32 * N - 1) / (32 * N), nz = (nk + VKW - 1) / VKW;
+          const long long nx = (d.ni() + 32 * VN - 1) / (32 * VN), nz = (nk + VKW - 1) / VKW;
           int rows = VJS;
           while (rows > 8 && nx * ((d.nj() + rows - 1) / rows) * nz * VKW < 148LL * 24) rows /= 2;
           dim3 blk(32, VKW, 1);
           dim3 grd((unsigned)nx, (d.nj() + rows - 1) / rows, (unsigned)nz);
-          k_sweep_v_vec<R, S, REC, NF><<<grd, blk, 0, s>>>(d, C, nk, rows, set, Di_src, Di_dst, adv, U, DU, mflux,
-                                                           mupd, code);
+          k_sweep_v_vec<R, S, REC, NF, VN><<<grd, blk, 0, s>>>(d, C, nk, rows, set, Di_src, Di_dst, adv, U, DU,
+                                                               mflux, mupd, code);
           return (int)cudaGetLastError();
         }
       } else {
@@ -157,6 +158,15 @@ int run_vdiff(const Dev& d, cudaStream_t s, R dt, R cnpar, R avmol, R* S, const 
               const int32_t* az, const R* src, R* rus, R* qus, const R* Sin, R* S2) {
   if (d.kmax <= 1) return 0;
   const int nx = d.imax - d.imin + 1, ny = d.jmax - d.jmin + 1;
+  if constexpr (sizeof(R) == 4) {
+    if (d.kmax + 1 <= 64) {  // the elimination coefficients of 64 columns in shared memory
+      constexpr int NT = 64;
+      const size_t dyn = 2 * (size_t)(d.kmax + 1) * NT * sizeof(R);
+      k_vdiff<R, true, NT><<<dim3((nx + 31) / 32, (ny + 1) / 2, 1), dim3(32, 2, 1), dyn, s>>>(
+          d, dt, cnpar, avmol, Sin ? Sin : S, S, hn, nuh, az, src, rus, qus, S2);
+      return (int)cudaGetLastError();
+    }
+  }
   dim3 blk(32, 4, 1);
   dim3 grd((nx + 31) / 32, (ny + 3) / 4, 1);
   k_vdiff<R><<<grd, blk, 0, s>>>(d, dt, cnpar, avmol, Sin ? Sin : S, S, hn, nuh, az, src, rus, qus, S2);

@@ -113,6 +113,18 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int byt
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes) : "memory");
 }
 
+// The same for a vector of B = 8 or 16 bytes (8: cp.async.ca, the only form below 16 bytes).
+template <int B>
+__device__ __forceinline__ void cp_async_v(void* smem, const void* gmem, int bytes) {
+  if constexpr (B == 16) {
+    cp_async16(smem, gmem, bytes);
+  } else {
+    static_assert(B == 8, "cp_async_v: 8 or 16 bytes");
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes) : "memory");
+  }
+}
+
 // Each thread stages the inputs of its next steps in its own slots of a shared-memory ring
 // (slot [stage][array][thread]: a warp's 16-byte slots are contiguous) and reads back only what
 // it copied itself, so the pipeline needs no barrier; a slot is refilled one step after it was
@@ -127,13 +139,15 @@ __device__ __forceinline__ void lds_vec(const VecPack<R, N>& x, R (&v)[N]) {
   for (int m = 0; m < N; ++m) v[m] = x.v[m];
 }
 
-template <class R, int S, bool REC, int NF>
+// VN: cells per lane (16 bytes of R by default; 2 FP32 cells halve the registers of a lane)
+template <class R, int S, bool REC, int NF, int VN = 16 / sizeof(R)>
 __global__ void __launch_bounds__(32 * VKW) k_sweep_v_vec(Dev d, SweepC<R> C, int nk, int rows, TracerSet<R, NF> F,
                                                         const R* Di_src, R* Di_dst, R* adv,
                                                         const R* __restrict__ V, const R* __restrict__ DV,
                                                         const uint8_t* __restrict__ mflux,
                                                         const uint8_t* __restrict__ mupd, uint8_t* code) {
-  constexpr int N = 16 / sizeof(R);
+  constexpr int N = VN;
+  constexpr int VB = N * (int)sizeof(R);
   // slots: f(j+2) per field; for a single field also fi(j) and adv(j) (a tracer pair reads fi
   // directly in the rare case that it is not f); V, DV, Di of row j
   constexpr int XV = NF == 1 ? 2 : NF, XDV = XV + 1, XDI = XV + 2, XAD = XV + 3;
@@ -174,13 +188,13 @@ __global__ void __launch_bounds__(32 * VKW) k_sweep_v_vec(Dev d, SweepC<R> C, in
 #pragma unroll
       for (int n = 0; n < NF; ++n) {
         const bool in = j + 2 < nj;
-        cp_async16(&sbuf[st][n][tid], F.t[n].f + (in ? p + 2 * sj : p), in ? vbytes : 0);
-        if (NF == 1 && !fis_f[n]) cp_async16(&sbuf[st][1][tid], F.t[n].fi_src + p, vbytes);
+        cp_async_v<VB>(&sbuf[st][n][tid], F.t[n].f + (in ? p + 2 * sj : p), in ? vbytes : 0);
+        if (NF == 1 && !fis_f[n]) cp_async_v<VB>(&sbuf[st][1][tid], F.t[n].fi_src + p, vbytes);
       }
-      cp_async16(&sbuf[st][XV][tid], V + p, vbytes);
-      cp_async16(&sbuf[st][XDV][tid], DV + p, vbytes);
-      cp_async16(&sbuf[st][XDI][tid], Di_src + p, vbytes);
-      if (NF == 1 && adv) cp_async16(&sbuf[st][XAD][tid], adv + p, vbytes);
+      cp_async_v<VB>(&sbuf[st][XV][tid], V + p, vbytes);
+      cp_async_v<VB>(&sbuf[st][XDV][tid], DV + p, vbytes);
+      cp_async_v<VB>(&sbuf[st][XDI][tid], Di_src + p, vbytes);
+      if (NF == 1 && adv) cp_async_v<VB>(&sbuf[st][XAD][tid], adv + p, vbytes);
     }
     cp_async_commit();
   };
