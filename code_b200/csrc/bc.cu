@@ -230,10 +230,40 @@ __global__ void k_finalise2d(Dev d, T dt, T* f, const T* Do, const T* adv, const
 
 // momentum.F90:157-174 (umomentum, DIR 0) / :319-336 (vmomentum, DIR 1): depth-integrated
 // transport update on U (V) points of the interior.
-template <int DIR, bool MIX>
+// COR: the kernel first forms the Coriolis term that this update needs from the other velocity
+// (fV from V for the U update, fU from U for the V update; the expressions of k_coriolis) at
+// every interior point and stores it, then updates its own velocity with it -- one launch where
+// the momentum / Coriolis pair took two (the other velocity is not written by this kernel, so no
+// point reads a value another thread changes).
+template <int DIR, bool MIX, bool COR = false>
 __global__ void k_momentum(Dev d, Bc2 s, Bc2W w) {
   GB_IJ2
   if (!interior(d, i, j)) return;
+  if constexpr (COR) {
+    if (DIR == 0) {  // fV on U points from V
+      auto V = f2a<MIX, V_>(d, s, w);
+      auto fV = f2a<MIX, FV>(d, s, w);
+      W2 coru{d, s.f2[CORU]};
+      M2 au{d, s.au};
+      if (au(i, j) >= 1) {
+        const double Vloc = 0.25 * ((double)V(i, j - 1) + (double)V(i + 1, j - 1) + (double)V(i, j) + (double)V(i + 1, j));
+        fV(i, j) = coru(i, j) * Vloc;
+      } else {
+        fV(i, j) = 0.0;
+      }
+    } else {  // fU on V points from U
+      auto U = f2a<MIX, U_>(d, s, w);
+      auto fU = f2a<MIX, FU>(d, s, w);
+      W2 corv{d, s.f2[CORV]};
+      M2 av{d, s.av};
+      if (av(i, j) >= 1) {
+        const double Uloc = 0.25 * ((double)U(i - 1, j) + (double)U(i, j) + (double)U(i - 1, j + 1) + (double)U(i, j + 1));
+        fU(i, j) = corv(i, j) * Uloc;
+      } else {
+        fU(i, j) = 0.0;
+      }
+    }
+  }
   M2 mask{d, DIR == 0 ? s.au : s.av};
   if (!(mask(i, j) == 1 || mask(i, j) == 2)) return;
   auto X = f2a<MIX, DIR == 0 ? U_ : V_>(d, s, w);
@@ -786,19 +816,23 @@ int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop, const Bc2W* wp = nu
     rc = uv_advect_2d(ctx, st, st->f2[U_], st->f2[V_], st->f2[DU], st->f2[DV]);
     if (rc) return rc;
   }
-  // umomentum / vmomentum: transport update, mirror_bdy_2d (momentum.F90:190,353), Coriolis term
+  // umomentum / vmomentum: transport update, mirror_bdy_2d (momentum.F90:190,353), Coriolis term.
+  // The mixed micro step forms each Coriolis term inside the update that uses it (k_momentum
+  // with COR); the term of the last update of a call is formed by getm_time_loop at its end.
   auto umom = [&]() -> int {
-    int r = mix ? k2(k_momentum<0, true>, d, s, w) : k2(k_momentum<0, false>, d, s, w);
+    int r = mix ? k2(k_momentum<0, true, true>, d, s, w) : k2(k_momentum<0, false>, d, s, w);
     if (r) return cuda_fail(ctx, r, "umomentum");
-    if (!mix && (r = mirror_bdy<double>(ctx, st->f2[U_], 0, 1))) return r;
-    r = mix ? k2(k_coriolis<0, true>, d, s, w) : k2(k_coriolis<0, false>, d, s, w);
+    if (mix) return GETM_OK;
+    if ((r = mirror_bdy<double>(ctx, st->f2[U_], 0, 1))) return r;
+    r = k2(k_coriolis<0, false>, d, s, w);
     return r ? cuda_fail(ctx, r, "coriolis") : GETM_OK;
   };
   auto vmom = [&]() -> int {
-    int r = mix ? k2(k_momentum<1, true>, d, s, w) : k2(k_momentum<1, false>, d, s, w);
+    int r = mix ? k2(k_momentum<1, true, true>, d, s, w) : k2(k_momentum<1, false>, d, s, w);
     if (r) return cuda_fail(ctx, r, "vmomentum");
-    if (!mix && (r = mirror_bdy<double>(ctx, st->f2[V_], 1, 1))) return r;
-    r = mix ? k2(k_coriolis<1, true>, d, s, w) : k2(k_coriolis<1, false>, d, s, w);
+    if (mix) return GETM_OK;
+    if ((r = mirror_bdy<double>(ctx, st->f2[V_], 1, 1))) return r;
+    r = k2(k_coriolis<1, false>, d, s, w);
     return r ? cuda_fail(ctx, r, "coriolis") : GETM_OK;
   };
   if (ip[I_UFIRST2D]) {
@@ -1193,7 +1227,18 @@ int getm_time_loop(getm_ctx* ctx, getm_bc_state* st, int n0, int count) {
       if (mix && (rc = sync(from3d, 1))) return rc;
     }
   }
+  if (mix && count > 0) {
+    // the Coriolis term of the last velocity update (fV after a V update, fU after a U update):
+    // ufirst2d was toggled by the last micro step, so 0 means its order was u, v
+    TimerScope ts(ctx, GETM_TIM_BC2D);
+    const Bc2 s2 = to_bc2(st);
+    if (st->ipar[I_UFIRST2D] == 0) k_coriolis<1, true><<<grid2(ctx->dev), kBlk2, 0, ctx->stream>>>(ctx->dev, s2, w);
+    else k_coriolis<0, true><<<grid2(ctx->dev), kBlk2, 0, ctx->stream>>>(ctx->dev, s2, w);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(ctx, (int)e, "coriolis");
+  }
   if (dirty && (rc = sync(written, 0))) return rc;
+  if (mix && !dirty && count > 0 && (rc = sync((1ull << FU) | (1ull << FV), 0))) return rc;
   return GETM_OK;
 }
 

@@ -832,10 +832,8 @@ struct ThomasSmem {
 // interior column; the matrix rows are built top-down as the elimination proceeds, ru(k+1)/qu(k+1)
 // carried in registers and ru(k)/qu(k) stored in two scratch 3D arrays (full occupancy, no shared
 // memory) for the back substitution.
-// SM (FP32, kmax < 64): ru(k)/qu(k) of the block's NT columns in dynamic shared memory
-// ([kmax+1][NT] each) instead of the scratch arrays, which removes their round trips through DRAM.
-template <class R, bool SM = false, int NT = 128>
-__global__ void __launch_bounds__(NT) k_vdiff(Dev d, R dt, R cnpar, R avmol, const R* Sin, R* S,
+template <class R>
+__global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, const R* Sin, R* S,
                                                const R* __restrict__ hn, const R* __restrict__ nuh,
                                                const int32_t* __restrict__ az, const R* __restrict__ src, R* RUs,
                                                R* QUs, R* S2) {
@@ -863,14 +861,11 @@ __global__ void __launch_bounds__(NT) k_vdiff(Dev d, R dt, R cnpar, R avmol, con
   // The inputs of a level (hn, nuh, the old tracer, src) are staged by cp.async into the thread's
   // own shared-memory slots, a ring of four levels with three in flight ahead of the elimination
   // (a serial chain per column), so the chain does not wait on their loads.
-  __shared__ R sl[4][4][NT];
-  extern __shared__ unsigned char vd_cols[];
-  R* const sRU = reinterpret_cast<R*>(vd_cols);
-  R* const sQU = sRU + (long long)(d.kmax + 1) * NT;
+  __shared__ R sl[4][4][128];
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   auto issue = [&](int lv) {
     if (lv >= 1) {
-      R(*q)[NT] = sl[lv & 3];
+      R(*q)[128] = sl[lv & 3];
       cp_async(&q[0][tid], hn + c + lv * sk);
       cp_async(&q[1][tid], nuh + c + lv * sk);
       cp_async(&q[2][tid], Sin + c + lv * sk);
@@ -879,14 +874,6 @@ __global__ void __launch_bounds__(NT) k_vdiff(Dev d, R dt, R cnpar, R avmol, con
     cp_async_commit();
   };
   auto get = [&](int lv, int q) -> R { return sl[lv & 3][q][tid]; };
-  auto RUr = [&](int k) -> R& {
-    if constexpr (SM) return sRU[k * NT + tid];
-    else return RUs[c + k * sk];
-  };
-  auto QUr = [&](int k) -> R& {
-    if constexpr (SM) return sQU[k * NT + tid];
-    else return QUs[c + k * sk];
-  };
   issue(kmax);
   issue(kmax - 1);
   issue(kmax - 2);
@@ -908,8 +895,8 @@ __global__ void __launch_bounds__(NT) k_vdiff(Dev d, R dt, R cnpar, R avmol, con
     if (src) a4 = a4 + srck;
     ru = a1 / a2;
     qu = a4 / a2;
-    RUr(k) = ru;
-    QUr(k) = qu;
+    RUs[c + k * sk] = ru;
+    QUs[c + k * sk] = qu;
   }
   // inner rows k = kmax-1 .. 2
   for (k = kmax - 1; k >= 2; --k) {
@@ -935,8 +922,8 @@ __global__ void __launch_bounds__(NT) k_vdiff(Dev d, R dt, R cnpar, R avmol, con
     const R den = a2 - a3 * ru;
     ru = a1 / den;
     qu = (a4 - a3 * qu) / den;
-    RUr(k) = ru;
-    QUr(k) = qu;
+    RUs[c + k * sk] = ru;
+    QUs[c + k * sk] = qu;
   }
   cp_async_wait<0>();
   // bottom row k = 1 (fi): only qu
@@ -954,16 +941,16 @@ __global__ void __launch_bounds__(NT) k_vdiff(Dev d, R dt, R cnpar, R avmol, con
     put(1, incr ? S1 + v : v);
   }
   // back substitution upwards, with the next level's coefficients loaded one step ahead
-  R qn = kmax >= 2 ? QUr(2) : R(0), rn = kmax >= 2 ? RUr(2) : R(0);
+  R qn = kmax >= 2 ? QUs[c + 2 * sk] : R(0), rn = kmax >= 2 ? RUs[c + 2 * sk] : R(0);
   R sn = (incr && kmax >= 2) ? L(Sin, 2) : R(0);
-  R qn2 = kmax >= 3 ? QUr(3) : R(0), rn2 = kmax >= 3 ? RUr(3) : R(0);
+  R qn2 = kmax >= 3 ? QUs[c + 3 * sk] : R(0), rn2 = kmax >= 3 ? RUs[c + 3 * sk] : R(0);
   R sn2 = (incr && kmax >= 3) ? L(Sin, 3) : R(0);
   for (k = 2; k <= kmax; ++k) {
     const R q = qn, r = rn, so = sn;
     qn = qn2; rn = rn2; sn = sn2;
     if (k + 2 <= kmax) {
-      qn2 = QUr(k + 2);
-      rn2 = RUr(k + 2);
+      qn2 = QUs[c + (k + 2) * sk];
+      rn2 = RUs[c + (k + 2) * sk];
       if (incr) sn2 = L(Sin, k + 2);
     }
     v = q - r * v;

@@ -158,15 +158,6 @@ int run_vdiff(const Dev& d, cudaStream_t s, R dt, R cnpar, R avmol, R* S, const 
               const int32_t* az, const R* src, R* rus, R* qus, const R* Sin, R* S2) {
   if (d.kmax <= 1) return 0;
   const int nx = d.imax - d.imin + 1, ny = d.jmax - d.jmin + 1;
-  if constexpr (sizeof(R) == 4) {
-    if (d.kmax + 1 <= 64) {  // the elimination coefficients of 64 columns in shared memory
-      constexpr int NT = 64;
-      const size_t dyn = 2 * (size_t)(d.kmax + 1) * NT * sizeof(R);
-      k_vdiff<R, true, NT><<<dim3((nx + 31) / 32, (ny + 1) / 2, 1), dim3(32, 2, 1), dyn, s>>>(
-          d, dt, cnpar, avmol, Sin ? Sin : S, S, hn, nuh, az, src, rus, qus, S2);
-      return (int)cudaGetLastError();
-    }
-  }
   dim3 blk(32, 4, 1);
   dim3 grd((nx + 31) / 32, (ny + 3) / 4, 1);
   k_vdiff<R><<<grd, blk, 0, s>>>(d, dt, cnpar, avmol, Sin ? Sin : S, S, hn, nuh, az, src, rus, qus, S2);
