@@ -768,7 +768,7 @@ int uv_advect_2d(getm_ctx* ctx, const getm_bc_state* st, const double* U, const 
   } while (0)
 
 // m2d.F90:412-490 integrate_2d (closed boundaries; no residual; Am <= 0, An_method = 0)
-int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop, const Bc2W* wp = nullptr) {
+int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop, const Bc2W* wp = nullptr, bool first = false) {
   const Dev& d = ctx->dev;
   const Bc2 s = to_bc2(st);
   int* ip = st->ipar;
@@ -818,17 +818,22 @@ int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop, const Bc2W* wp = nu
   }
   // umomentum / vmomentum: transport update, mirror_bdy_2d (momentum.F90:190,353), Coriolis term.
   // The mixed micro step forms each Coriolis term inside the update that uses it (k_momentum
-  // with COR); the term of the last update of a call is formed by getm_time_loop at its end.
-  auto umom = [&]() -> int {
-    int r = mix ? k2(k_momentum<0, true, true>, d, s, w) : k2(k_momentum<0, false>, d, s, w);
+  // with COR): the stored term was formed from the other velocity as it is now, so recomputing
+  // it gives the same value. The first update of a getm_time_loop call (first) reads the stored
+  // term instead -- the state's fU/fV, which need not match the velocities (a start from rest of
+  // the Coriolis terms) -- and getm_time_loop forms the term of the last update at its end.
+  auto umom = [&](bool cor) -> int {
+    int r = !mix ? k2(k_momentum<0, false>, d, s, w)
+                 : cor ? k2(k_momentum<0, true, true>, d, s, w) : k2(k_momentum<0, true, false>, d, s, w);
     if (r) return cuda_fail(ctx, r, "umomentum");
     if (mix) return GETM_OK;
     if ((r = mirror_bdy<double>(ctx, st->f2[U_], 0, 1))) return r;
     r = k2(k_coriolis<0, false>, d, s, w);
     return r ? cuda_fail(ctx, r, "coriolis") : GETM_OK;
   };
-  auto vmom = [&]() -> int {
-    int r = mix ? k2(k_momentum<1, true, true>, d, s, w) : k2(k_momentum<1, false>, d, s, w);
+  auto vmom = [&](bool cor) -> int {
+    int r = !mix ? k2(k_momentum<1, false>, d, s, w)
+                 : cor ? k2(k_momentum<1, true, true>, d, s, w) : k2(k_momentum<1, true, false>, d, s, w);
     if (r) return cuda_fail(ctx, r, "vmomentum");
     if (mix) return GETM_OK;
     if ((r = mirror_bdy<double>(ctx, st->f2[V_], 1, 1))) return r;
@@ -836,10 +841,10 @@ int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop, const Bc2W* wp = nu
     return r ? cuda_fail(ctx, r, "coriolis") : GETM_OK;
   };
   if (ip[I_UFIRST2D]) {
-    if ((rc = umom()) || (rc = vmom())) return rc;
+    if ((rc = umom(!first)) || (rc = vmom(true))) return rc;
     ip[I_UFIRST2D] = 0;
   } else {
-    if ((rc = vmom()) || (rc = umom())) return rc;
+    if ((rc = vmom(!first)) || (rc = umom(true))) return rc;
     ip[I_UFIRST2D] = 1;
   }
   // update_2d_bdy sets the boundary elevations after the Uint accumulation and before sealevel
@@ -942,18 +947,19 @@ int integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
   if ((rc = bc3<R3>(ctx, st, BC3_SIGMA, GETM_TIM_BC3D))) return rc;
   if (d.kmax > 1) {
     if ((rc = bc3<R3>(ctx, st, BC3_WW, GETM_TIM_BC3D))) return rc;
-    // uv_advect_3d (uv_advect_3d.F90:62-460)
+    // uv_advect_3d (uv_advect_3d.F90:62-460); only the advection terms uuEx/vvEx are kept, so the
+    // last sweep writes no field
     const int split = ip[I_VEL3D_SPLIT], hor = ip[I_VEL3D_HOR], ver = ip[I_VEL3D_VER];
     if (hor != NOADV || ver != NOADV) {
       R3* w = (R3*)ctx->bc_scr3;
       R3 *fadv = w, *ua = w + n3, *va = w + 2 * n3, *wa = w + 3 * n3, *hua = w + 4 * n3, *hva = w + 5 * n3;
       if ((rc = bc3<R3>(ctx, st, BC3_UVADV_PREP_U, GETM_TIM_BC3D))) return rc;
       if ((rc = do_adv3d<R3>(ctx, R3(st->par[P_DT]), fadv, ua, va, wa, hua, hva, f3[HUN], f3[HUN], split, hor, ver,
-                             R3(0), GETM_U_TAG, nullptr, f3[UUEX], ip[I_ADV_VER_ITERS])))
+                             R3(0), GETM_U_TAG, nullptr, f3[UUEX], ip[I_ADV_VER_ITERS], false)))
         return rc;
       if ((rc = bc3<R3>(ctx, st, BC3_UVADV_PREP_V, GETM_TIM_BC3D))) return rc;
       if ((rc = do_adv3d<R3>(ctx, R3(st->par[P_DT]), fadv, ua, va, wa, hua, hva, f3[HVN], f3[HVN], split, hor, ver,
-                             R3(0), GETM_V_TAG, nullptr, f3[VVEX], ip[I_ADV_VER_ITERS])))
+                             R3(0), GETM_V_TAG, nullptr, f3[VVEX], ip[I_ADV_VER_ITERS], false)))
         return rc;
     }
     if ((rc = bc3<R3>(ctx, st, BC3_STRESSES, GETM_TIM_BC3D))) return rc;
@@ -1217,7 +1223,7 @@ int getm_time_loop(getm_ctx* ctx, getm_bc_state* st, int n0, int count) {
   if (mix && (rc = sync(all & ~((1ull << UEX) | (1ull << VEX)), 1))) return rc;
   bool dirty = false;  // working copies newer than the state
   for (int n = n0; n < n0 + count; ++n) {
-    if ((rc = integrate_2d(ctx, st, n, mix ? &w : nullptr))) return rc;
+    if ((rc = integrate_2d(ctx, st, n, mix ? &w : nullptr, n == n0))) return rc;
     dirty = mix;
     if (n % st->ipar[I_M] == 0) {
       if (mix && (rc = sync(written, 0))) return rc;

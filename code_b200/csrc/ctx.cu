@@ -56,7 +56,7 @@ using namespace gb;
 template <class R>
 int do_adv3d(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, const R* hu,
                     const R* hv, const R* ho, const R* hn, int split, int hs, int vs, R AH, int tag, R* hires,
-                    R* advres, int iters) {
+                    R* advres, int iters, bool field_out) {
   (void)hn;
   if (!ctx) return GETM_ERR_ARG;
   if (!ctx->adv_ready) return fail(ctx, GETM_ERR_STATE, "getm_init_advection has not been called");
@@ -158,8 +158,10 @@ int do_adv3d(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, c
       if (kmax > 1) GB_TIMED(GETM_TIM_ADV_W, run_sweep_w<R>(d, s, dt, one, vs, kshift, iters, f, f, f, H, A, ww, g.az, warn), "w");
       GB_TIMED(GETM_TIM_ADV_V, (run_sweep_h<R, 1>(d, s, nk, dt, half, hs, AH, L(f, 1), L(f, 1), L(S, 1), L(H, 1), L(H, 1), Al,
                                 L(vv, 1), L(hv, 1), g.mask_vflux, g.mask_vupdate)), "v2");
-      GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<R, 0>(d, s, nk, dt, half, hs, AH, L(S, 1), L(S, 1), L(f, 1), L(H, 1), L(H, 1), Al,
-                                L(uu, 1), L(hu, 1), g.mask_uflux, g.mask_uupdate)), "u2");
+      // the last sweep writes the field and heights only when the caller keeps them
+      GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<R, 0>(d, s, nk, dt, half, hs, AH, L(S, 1), L(S, 1),
+                                field_out ? L(f, 1) : nullptr, L(H, 1), (field_out || hires) ? L(H, 1) : nullptr,
+                                Al, L(uu, 1), L(hu, 1), g.mask_uflux, g.mask_uupdate)), "u2");
       break;
     case GETM_HVSPLIT:
       GB_TIMED(GETM_TIM_COPY, cudaMemcpyAsync(S, f, bytes3, cudaMemcpyDeviceToDevice, s), "copy f");
@@ -218,10 +220,10 @@ template int do_adv3d_pair<float>(getm_ctx*, float, float*, float*, const float*
 
 template int do_adv3d<double>(getm_ctx*, double, double*, const double*, const double*, const double*,
                                const double*, const double*, const double*, const double*, int, int, int, double,
-                               int, double*, double*, int);
+                               int, double*, double*, int, bool);
 template int do_adv3d<float>(getm_ctx*, float, float*, const float*, const float*, const float*, const float*,
                              const float*, const float*, const float*, int, int, int, float, int, float*, float*,
-                             int);
+                             int, bool);
 
 template <class R>
 static int sweep_h_api(getm_ctx* ctx, int dir, int nk, R dt, const R* f, R* fi, R* Di, R* adv, const R* U,

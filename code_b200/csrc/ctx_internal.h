@@ -160,7 +160,8 @@ static inline bool grid_for_tag(const getm_ctx* ctx, int tag, getm_adv_grid* g) 
 // do_advection_3d (advection_3d.F90:120-598) on device pointers; defined in ctx.cu.
 template <class R>
 int do_adv3d(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, const R* hu, const R* hv,
-             const R* ho, const R* hn, int split, int hs, int vs, R AH, int tag, R* hires, R* advres, int iters);
+             const R* ho, const R* hn, int split, int hs, int vs, R AH, int tag, R* hires, R* advres, int iters,
+             bool field_out = true);
 // Two tracers advected together with HALFSPLIT on the H grid (ctx.cu); the caller has checked that
 // hs is a split scheme, vs a split scheme or NOADV, and adv_ver_iterations = 1.
 template <class R>

@@ -430,20 +430,20 @@ __global__ void __launch_bounds__(TU, sizeof(R) == 4 ? 16 : 8) k_sweep_u_tile(De
       if (upd) {
         const R dD = cell_dD<R>(C, sU[b][t + 1], sU[b][t]);
         const R Dn = Dio - dD;
-        Di_dst[p] = Dn;
+        if (Di_dst) Di_dst[p] = Dn;
 #pragma unroll
         for (int n = 0; n < NF; ++n) {
           const R fio = F.t[n].fi_src == F.t[n].f ? sf[b][n][t + 2] : sfi[b][n][t];
           const R advn = cell_advn<R>(C, sfl[n][t + 1], sfl[n][t]);
-          F.t[n].fi_dst[p] = fv_update<R>(Dio, dD, Dn, fio, C.dt, advn);
+          if (F.t[n].fi_dst) F.t[n].fi_dst[p] = fv_update<R>(Dio, dD, Dn, fio, C.dt, advn);
           if (NF == 1 && adv) adv[p] = sA[b][t] + advn;
         }
       } else {
 #pragma unroll
         for (int n = 0; n < NF; ++n)
-          if (F.t[n].fi_dst != F.t[n].fi_src)
+          if (F.t[n].fi_dst && F.t[n].fi_dst != F.t[n].fi_src)
             F.t[n].fi_dst[p] = F.t[n].fi_src == F.t[n].f ? sf[b][n][t + 2] : sfi[b][n][t];
-        if (Di_dst != Di_src) Di_dst[p] = Dio;
+        if (Di_dst && Di_dst != Di_src) Di_dst[p] = Dio;
       }
     }
     __syncthreads();  // buffer b and sfl are restaged / rewritten for level k+2 / k+1
@@ -564,20 +564,20 @@ __global__ void __launch_bounds__(TVX * TVY, sizeof(R) == 4 ? (NF == 1 ? 8 : 6) 
       if (upd) {
         const R dD = cell_dD<R>(C, sV[b][ty + 1][tx], sV[b][ty][tx]);
         const R Dn = Dio - dD;
-        Di_dst[p] = Dn;
+        if (Di_dst) Di_dst[p] = Dn;
 #pragma unroll
         for (int n = 0; n < NF; ++n) {
           const R fio = F.t[n].fi_src == F.t[n].f ? sf[b][n][ty + 2][tx] : sfi[b][n][ty][tx];
           const R advn = cell_advn<R>(C, sfl[n][ty + 1][tx], sfl[n][ty][tx]);
-          F.t[n].fi_dst[p] = fv_update<R>(Dio, dD, Dn, fio, C.dt, advn);
+          if (F.t[n].fi_dst) F.t[n].fi_dst[p] = fv_update<R>(Dio, dD, Dn, fio, C.dt, advn);
           if (NF == 1 && adv) adv[p] = sA[b][ty][tx] + advn;
         }
       } else {
 #pragma unroll
         for (int n = 0; n < NF; ++n)
-          if (F.t[n].fi_dst != F.t[n].fi_src)
+          if (F.t[n].fi_dst && F.t[n].fi_dst != F.t[n].fi_src)
             F.t[n].fi_dst[p] = F.t[n].fi_src == F.t[n].f ? sf[b][n][ty + 2][tx] : sfi[b][n][ty][tx];
-        if (Di_dst != Di_src) Di_dst[p] = Dio;
+        if (Di_dst && Di_dst != Di_src) Di_dst[p] = Dio;
       }
     }
     __syncthreads();  // buffer b and sfl are restaged / rewritten for level k+2 / k+1

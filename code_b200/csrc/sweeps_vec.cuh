@@ -311,9 +311,9 @@ __global__ void __launch_bounds__(32 * VKW) k_sweep_v_vec(Dev d, SweepC<R> C, in
         fo[m] = upd ? fv_update<R>(Dio[m], dDv[m], Dn[m], fio[n][m], C.dt, advn) : fio[n][m];
         if (NF == 1 && adv && upd) ad[m] = ad[m] + advn;
       }
-      if (any || F.t[n].fi_dst != F.t[n].fi_src) st_row<R, N>(F.t[n].fi_dst + p, full, navail, fo);
+      if (F.t[n].fi_dst && (any || F.t[n].fi_dst != F.t[n].fi_src)) st_row<R, N>(F.t[n].fi_dst + p, full, navail, fo);
     }
-    if (any || Di_dst != Di_src) st_row<R, N>(Di_dst + p, full, navail, Dn);
+    if (Di_dst && (any || Di_dst != Di_src)) st_row<R, N>(Di_dst + p, full, navail, Dn);
     if (NF == 1 && adv && any) st_row<R, N>(adv + p, full, navail, ad);
 #pragma unroll
     for (int m = 0; m < N; ++m) Vp[m] = Vc[m];
@@ -497,9 +497,9 @@ __global__ void __launch_bounds__(32 * UWB) k_sweep_u_vec(Dev d, SweepC<R> C, in
         fo[q] = updm[q] ? fv_update<R>(Dio[q], dDv[q], Dn[q], fio[q], C.dt, advn) : fio[q];
         if (NF == 1 && adv && updm[q]) ad[q] = ad[q] + advn;
       }
-      if (any || F.t[n].fi_dst != F.t[n].fi_src) st_row<R, N>(F.t[n].fi_dst + p, full, navail, fo);
+      if (F.t[n].fi_dst && (any || F.t[n].fi_dst != F.t[n].fi_src)) st_row<R, N>(F.t[n].fi_dst + p, full, navail, fo);
     }
-    if (any || Di_dst != Di_src) st_row<R, N>(Di_dst + p, full, navail, Dn);
+    if (Di_dst && (any || Di_dst != Di_src)) st_row<R, N>(Di_dst + p, full, navail, Dn);
     if (NF == 1 && adv && any) st_row<R, N>(adv + p, full, navail, ad);
   }
   cp_async_wait<0>();
