@@ -20,6 +20,20 @@ constexpr int RW = FX + 8, RH = FY + 4;     // staged region: i in [-4, FX+3], j
 constexpr int FTY = 8;                      // thread rows: a block is RW x FTY threads, lane x <-> region column
 constexpr int FT = RW * FTY;                // threads per block
 
+// k*(a*s - b*s)*c as single rounded operations in this order: the volume and flux differences of
+// the cell updates. FP64: the plain operations (the FP64 build contracts nothing); FP32: explicit
+// intrinsics, so that the result does not depend on which products the compiler contracts.
+template <class T>
+__device__ __forceinline__ T diff_scaled(T k, T a, T b, T s, T c) {
+  if constexpr (sizeof(T) == 4) return __fmul_rn(__fmul_rn(k, __fsub_rn(__fmul_rn(a, s), __fmul_rn(b, s))), c);
+  else return k * (a * s - b * s) * c;
+}
+template <class T>
+__device__ __forceinline__ T add_r(T a, T b) {
+  if constexpr (sizeof(T) == 4) return __fadd_rn(a, b);
+  else return a + b;
+}
+
 template <class T>
 struct Adv2dSmem {
   T F0[RH][RW];   // advected quantity; reused for the field after the v sweep
@@ -114,12 +128,12 @@ __global__ void __launch_bounds__(FT) k_uvadv2d_fused(Dev d, T dt, const TI* __r
         T fnew = fio;
         if (cok && sm.mpu[r][q]) {
           const T Dio = sm.Di[r][q];
-          const T dD = dti * (sm.Ua[r][q] * dyu - sm.Ua[r][q - 1] * dyu) * ard1;
+          const T dD = diff_scaled<T>(dti, sm.Ua[r][q], sm.Ua[r][q - 1], dyu, ard1);
           const T Dn = Dio - dD;
-          const T advn = half * (sm.FL[r][q] * dyu - sm.FL[r][q - 1] * dyu) * ard1;
+          const T advn = diff_scaled<T>(half, sm.FL[r][q], sm.FL[r][q - 1], dyu, ard1);
           sm.Di[r][q] = Dn;
           fnew = fv_update<T>(Dio, dD, Dn, fio, dt, advn);
-          if (qown && r >= 2 && r < FY + 2) sm.A[r - 2][q - 4] = sm.A[r - 2][q - 4] + advn;
+          if (qown && r >= 2 && r < FY + 2) sm.A[r - 2][q - 4] = add_r<T>(sm.A[r - 2][q - 4], advn);
         }
         sm.F1[r][q] = fnew;
       }
@@ -146,12 +160,12 @@ __global__ void __launch_bounds__(FT) k_uvadv2d_fused(Dev d, T dt, const TI* __r
         T fnew = fio;
         if (jj >= 1 + sub && jj <= nj - 2 - sub && sm.mpv[r][q]) {
           const T Dio = sm.Di[r][q];
-          const T dD = dti * (sm.Va[r][q] * dxu - sm.Va[r - 1][q] * dxu) * ard1;
+          const T dD = diff_scaled<T>(dti, sm.Va[r][q], sm.Va[r - 1][q], dxu, ard1);
           const T Dn = Dio - dD;
-          const T advn = one * (sm.FL[r][q] * dxu - sm.FL[r - 1][q] * dxu) * ard1;
+          const T advn = diff_scaled<T>(one, sm.FL[r][q], sm.FL[r - 1][q], dxu, ard1);
           sm.Di[r][q] = Dn;
           fnew = fv_update<T>(Dio, dD, Dn, fio, dt, advn);
-          if (qown) sm.A[r - 2][q - 4] = sm.A[r - 2][q - 4] + advn;
+          if (qown) sm.A[r - 2][q - 4] = add_r<T>(sm.A[r - 2][q - 4], advn);
         }
         sm.F0[r][q] = fnew;  // the field after v (F0 is no longer needed)
       }
@@ -177,8 +191,8 @@ __global__ void __launch_bounds__(FT) k_uvadv2d_fused(Dev d, T dt, const TI* __r
         const int jj = jj0 - 2 + r;
         T a = sm.A[r - 2][q - 4];
         if (ii >= 1 + sub && ii <= ni - 2 - sub && jj < nj && sm.mpu[r][q]) {
-          const T advn = half * (sm.FL[r][q] * dyu - sm.FL[r][q - 1] * dyu) * ard1;
-          a = a + advn;
+          const T advn = diff_scaled<T>(half, sm.FL[r][q], sm.FL[r][q - 1], dyu, ard1);
+          a = add_r<T>(a, advn);
         }
         if (ii < ni && jj < nj) Ex[(long long)jj * sj + ii] = (TI)a;
       }
@@ -221,6 +235,7 @@ int run_uvadv2d_fused(const Dev& d, cudaStream_t s, int dir, T dt, int scheme, c
 // FP32 arithmetic on the FP32 working copies of the mixed-precision micro step (defined in the
 // FP32 translation unit only)
 #if defined(GB_REAL_IS_FLOAT)
+
 int run_uvadv2d_fused_f32(const Dev& d, cudaStream_t s, int dir, float dt, int scheme, const float* U,
                           const float* V, const float* DU, const float* DV, const uint8_t* mflux_u,
                           const uint8_t* mflux_v, const uint8_t* mupd_u, const uint8_t* mupd_v, float* Ex) {
