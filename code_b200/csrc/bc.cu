@@ -626,7 +626,7 @@ int bdy_2d(getm_ctx* ctx, const Bc2& s, int loop) {
 
 int ensure_bc_scratch(getm_ctx* ctx, size_t elem3) {
   const long long n3 = n3d(ctx->dev), n2 = n2d(ctx->dev);
-  const size_t b3 = (size_t)NB3 * n3 * elem3;
+  const size_t b3 = (size_t)(elem3 == 4 ? NB3F : NB3) * n3 * elem3;
   if (ctx->bc_scr3_bytes < b3) {
     if (ctx->bc_scr3) cudaFree(ctx->bc_scr3);
     ctx->bc_scr3 = nullptr;
@@ -899,8 +899,9 @@ int bc3(getm_ctx* ctx, const getm_bc_state* st, int which, int slot) {
   const Bc3<R3> s = to_bc3<R3>(st);
   const long long n3 = n3d(ctx->dev);
   R3* base = (R3*)ctx->bc_scr3;
-  R3* scr[NB3];
-  for (int q = 0; q < NB3; ++q) scr[q] = base + q * n3;
+  R3* scr[NB3F];
+  const int nb = sizeof(R3) == 4 ? NB3F : NB3;
+  for (int q = 0; q < NB3F; ++q) scr[q] = q < nb ? base + q * n3 : nullptr;
   GB_TIMED(slot, (run_bc3<R3>(which, ctx->dev, ctx->stream, s, scr)), "macro-step kernel");
   return GETM_OK;
 }
@@ -952,14 +953,18 @@ int integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
     const int split = ip[I_VEL3D_SPLIT], hor = ip[I_VEL3D_HOR], ver = ip[I_VEL3D_VER];
     if (hor != NOADV || ver != NOADV) {
       R3* w = (R3*)ctx->bc_scr3;
+      // FP32: both grids' quantities in one pass (U grid in scratch 0-5, V grid in 7-12); FP64: the
+      // U grid, its advection, then the V grid into the same six arrays
+      R3* wv = sizeof(R3) == 4 ? w + 7 * n3 : w;
       R3 *fadv = w, *ua = w + n3, *va = w + 2 * n3, *wa = w + 3 * n3, *hua = w + 4 * n3, *hva = w + 5 * n3;
-      if ((rc = bc3<R3>(ctx, st, BC3_UVADV_PREP_U, GETM_TIM_BC3D))) return rc;
+      R3 *fadvv = wv, *uav = wv + n3, *vav = wv + 2 * n3, *wav = wv + 3 * n3, *huav = wv + 4 * n3, *hvav = wv + 5 * n3;
+      if ((rc = bc3<R3>(ctx, st, sizeof(R3) == 4 ? BC3_UVADV_PREP_UV : BC3_UVADV_PREP_U, GETM_TIM_BC3D))) return rc;
       if ((rc = do_adv3d<R3>(ctx, R3(st->par[P_DT]), fadv, ua, va, wa, hua, hva, f3[HUN], f3[HUN], split, hor, ver,
                              R3(0), GETM_U_TAG, nullptr, f3[UUEX], ip[I_ADV_VER_ITERS], false)))
         return rc;
-      if ((rc = bc3<R3>(ctx, st, BC3_UVADV_PREP_V, GETM_TIM_BC3D))) return rc;
-      if ((rc = do_adv3d<R3>(ctx, R3(st->par[P_DT]), fadv, ua, va, wa, hua, hva, f3[HVN], f3[HVN], split, hor, ver,
-                             R3(0), GETM_V_TAG, nullptr, f3[VVEX], ip[I_ADV_VER_ITERS], false)))
+      if (sizeof(R3) == 8 && (rc = bc3<R3>(ctx, st, BC3_UVADV_PREP_V, GETM_TIM_BC3D))) return rc;
+      if ((rc = do_adv3d<R3>(ctx, R3(st->par[P_DT]), fadvv, uav, vav, wav, huav, hvav, f3[HVN], f3[HVN], split, hor,
+                             ver, R3(0), GETM_V_TAG, nullptr, f3[VVEX], ip[I_ADV_VER_ITERS], false)))
         return rc;
     }
     if ((rc = bc3<R3>(ctx, st, BC3_STRESSES, GETM_TIM_BC3D))) return rc;

@@ -563,6 +563,83 @@ __global__ void __launch_bounds__(128) k_uvadv3d_prep_vec(Dev d, Bc3<float> s, f
   st_row<float, N>(hvadvp + p, fullw, nw, hb);
 }
 
+// Both momentum grids' quantities in one pass (FP32, 16-byte aligned layouts): the inputs of a
+// vector of 4 cells are read once for the U and the V grid; the same expressions and cells as
+// k_uvadv3d_prep_vec<0> into u[0..5] and k_uvadv3d_prep_vec<1> into v[0..5] (fadv, uuadv, vvadv,
+// wwadv, huadv, hvadv), with wwadv(:,:,0) = 0 of the U grid.
+struct Prep6 {
+  float* a[6];
+};
+template <int N = 4>
+__global__ void __launch_bounds__(128) k_uvadv3d_prep_vec2(Dev d, Bc3<float> s, Prep6 u, Prep6 v) {
+  const int ni = d.ni(), nj = d.nj();
+  const int c0 = (blockIdx.x * blockDim.x + threadIdx.x) * N;
+  const int jj = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (c0 >= ni || jj >= nj) return;
+  const long long p = (long long)k * d.sk + (long long)jj * d.sj + c0;
+  const int nrow = min(N, ni - c0);
+  if (k == 0) {
+    const float z[N] = {0.f, 0.f, 0.f, 0.f};
+    st_row<float, N>(u.a[3] + p, nrow == N, nrow, z);
+    return;
+  }
+  const bool fullr = c0 + N <= ni;
+  auto ld = [&](int f, long long off, float (&x)[N]) { ld_row<float, N>(s.f3[f] + p + off, fullr, ni - c0, x); };
+  float uu[N], vv[N], ww[N], ho[N], hn[N], hun[N], hvn[N];
+  ld(UU, 0, uu); ld(VV, 0, vv); ld(WW, 0, ww); ld(HO, 0, ho); ld(HN, 0, hn); ld(HUN, 0, hun); ld(HVN, 0, hvn);
+  const float half = 0.5f;
+  const int nwu = min(nrow, ni - 1 - c0);  // U grid: every cell but the last of the row
+  if (nwu > 0) {
+    const bool nb = c0 + N < ni;
+    const long long q = p + N;
+    const float uue = nb ? s.f3[UU][q] : 0.f, vve = nb ? s.f3[VV][q] : 0.f, wwe = nb ? s.f3[WW][q] : 0.f,
+                hoe = nb ? s.f3[HO][q] : 0.f, hne = nb ? s.f3[HN][q] : 0.f, hvne = nb ? s.f3[HVN][q] : 0.f;
+    float fa[N], ua[N], va[N], wa[N], ha[N], hb[N];
+#pragma unroll
+    for (int m = 0; m < N; ++m) {
+      const float u1 = m + 1 < N ? uu[m + 1] : uue, v1 = m + 1 < N ? vv[m + 1] : vve, w1 = m + 1 < N ? ww[m + 1] : wwe;
+      const float o1 = m + 1 < N ? ho[m + 1] : hoe, n1 = m + 1 < N ? hn[m + 1] : hne,
+                  h1 = m + 1 < N ? hvn[m + 1] : hvne;
+      fa[m] = uu[m] / hun[m];
+      ua[m] = half * (uu[m] + u1);
+      va[m] = half * (vv[m] + v1);
+      wa[m] = half * (ww[m] + w1);
+      ha[m] = half * (o1 + n1);
+      hb[m] = half * (hvn[m] + h1);
+    }
+    const bool fw = nwu == N;
+    st_row<float, N>(u.a[0] + p, fw, nwu, fa);
+    st_row<float, N>(u.a[1] + p, fw, nwu, ua);
+    st_row<float, N>(u.a[2] + p, fw, nwu, va);
+    st_row<float, N>(u.a[3] + p, fw, nwu, wa);
+    st_row<float, N>(u.a[4] + p, fw, nwu, ha);
+    st_row<float, N>(u.a[5] + p, fw, nwu, hb);
+  }
+  if (jj <= nj - 2) {  // V grid: rows but the last
+    const long long sj = d.sj;
+    float uu1[N], vv1[N], ww1[N], hun1[N], ho1[N], hn1[N];
+    ld(UU, sj, uu1); ld(VV, sj, vv1); ld(WW, sj, ww1); ld(HUN, sj, hun1); ld(HO, sj, ho1); ld(HN, sj, hn1);
+    float fa[N], ua[N], va[N], wa[N], ha[N], hb[N];
+#pragma unroll
+    for (int m = 0; m < N; ++m) {
+      fa[m] = vv[m] / hvn[m];
+      ua[m] = half * (uu[m] + uu1[m]);
+      va[m] = half * (vv[m] + vv1[m]);
+      wa[m] = half * (ww[m] + ww1[m]);
+      ha[m] = half * (hun[m] + hun1[m]);
+      hb[m] = half * (ho1[m] + hn1[m]);
+    }
+    const bool fw = nrow == N;
+    st_row<float, N>(v.a[0] + p, fw, nrow, fa);
+    st_row<float, N>(v.a[1] + p, fw, nrow, ua);
+    st_row<float, N>(v.a[2] + p, fw, nrow, va);
+    st_row<float, N>(v.a[3] + p, fw, nrow, wa);
+    st_row<float, N>(v.a[4] + p, fw, nrow, ha);
+    st_row<float, N>(v.a[5] + p, fw, nrow, hb);
+  }
+}
+
 // stresses_3d.F90:50-104 (bottom and surface stresses; FP64 from the bottom layer)
 template <class R3>
 __global__ void k_stresses(Dev d, Bc3<R3> s) {
@@ -741,6 +818,28 @@ int run_bc3(int which, const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* cons
         k_uvadv3d_prep<R3, 1><<<plane_grid(d, blk, d.kmax + 1), blk, 0, st>>>(d, s, scr[0], scr[1], scr[2], scr[3],
                                                                               scr[4], scr[5]);
       break;
+    }
+    case BC3_UVADV_PREP_UV: {  // FP32 only: U grid into scr[0..5], V grid into scr[7..12]
+      if constexpr (sizeof(R3) == 4) {
+        bool ok = vector_sweeps_enabled() && d.sj % 4 == 0 && d.sk % 4 == 0;
+        for (int q : {0, 1, 2, 3, 4, 5, 7, 8, 9, 10, 11, 12}) ok = ok && reinterpret_cast<uintptr_t>(scr[q]) % 16 == 0;
+        for (int f : {UU, VV, WW, HO, HN, HUN, HVN})
+          ok = ok && reinterpret_cast<uintptr_t>(s.f3[f]) % 16 == 0;
+        if (ok) {
+          const dim3 bv(32, 4, 1);
+          const dim3 gv((d.ni() + 4 * 32 - 1) / (4 * 32), (d.nj() + 3) / 4, d.kmax + 1);
+          k_uvadv3d_prep_vec2<4><<<gv, bv, 0, st>>>(d, s, Prep6{{scr[0], scr[1], scr[2], scr[3], scr[4], scr[5]}},
+                                                    Prep6{{scr[7], scr[8], scr[9], scr[10], scr[11], scr[12]}});
+        } else {
+          k_uvadv3d_prep<R3, 0><<<plane_grid(d, blk, d.kmax + 1), blk, 0, st>>>(d, s, scr[0], scr[1], scr[2],
+                                                                                scr[3], scr[4], scr[5]);
+          k_uvadv3d_prep<R3, 1><<<plane_grid(d, blk, d.kmax + 1), blk, 0, st>>>(d, s, scr[7], scr[8], scr[9],
+                                                                                scr[10], scr[11], scr[12]);
+        }
+        break;
+      } else {
+        return (int)cudaErrorInvalidValue;
+      }
     }
     case BC3_STRESSES: k_stresses<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s); break;
     case BC3_EQSTATE: {

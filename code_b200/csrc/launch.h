@@ -99,10 +99,10 @@ int run_check_range(const Dev& d, cudaStream_t s, const R* f, const int32_t* az,
 int run_build_masks(const Dev& d, cudaStream_t s, const int32_t* az, const int32_t* au, const int32_t* av,
                     const int32_t* ax, uint8_t* planes);
 
-// 3D kernels of the macro step (bc_kernels.cuh); scr = the NB3 scratch arrays
+// 3D kernels of the macro step (bc_kernels.cuh); scr = the scratch arrays (NB3, FP32 NB3F)
 enum {
   BC3_BF3D = 0, BC3_ZZ, BC3_IP, BC3_UUMOM, BC3_VVMOM, BC3_SIGMA, BC3_WW, BC3_UVADV_PREP_U, BC3_UVADV_PREP_V,
-  BC3_STRESSES, BC3_EQSTATE, BC3_SLOW_TERMS
+  BC3_STRESSES, BC3_EQSTATE, BC3_SLOW_TERMS, BC3_UVADV_PREP_UV
 };
 template <class R3>
 struct Bc3;
