@@ -18,7 +18,7 @@ enum PD {
 enum PI {
   I_M, I_MM, I_RUNTYPE, I_VEL2D_SPLIT, I_VEL2D_HOR, I_VEL3D_SPLIT, I_VEL3D_HOR, I_VEL3D_VER, I_TEMP_SPLIT, I_TEMP_HOR,
   I_TEMP_VER, I_SALT_SPLIT, I_SALT_HOR, I_SALT_VER, I_ADV_VER_ITERS, I_UFIRST2D, I_UFIRST3D, I_CALC_TEMP,
-  I_CALC_SALT, NPI
+  I_CALC_SALT, I_IP_METHOD, NPI
 };
 
 // 2D part (all FP64) -- passed to kernels by value

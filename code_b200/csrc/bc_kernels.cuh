@@ -144,6 +144,168 @@ __global__ void k_ip(Dev d, Bc3<R3> s, const R3* zzp) {
   if (av(i, j) >= 1) column(hvn, idpdy, 0, 1, R3(1.0 / d.dy));
 }
 
+// ip_blumberg_mellor_lin.F90:87-97: heights of the pressure points (layer centres) of the
+// columns i = imin..imax+1, j = jmin..jmax+1 with az >= 1.
+template <class R3>
+__global__ void k_zz_lin(Dev d, Bc3<R3> s, R3* zzp) {
+  GB_IJ_HALO
+  if (i < d.imin || i > d.imax + 1 || j < d.jmin || j > d.jmax + 1) return;
+  I2 az{d, s.az};
+  if (az(i, j) < 1) return;
+  V3<R3> hn{d, s.f3[HN]}, zz{d, zzp};
+  V2 H{d, s.f2[HH]};
+  const R3 half = R3(0.5);
+  R3 hprev = hn(i, j, 1);
+  R3 z = R3(-H(i, j)) + half * hprev;
+  zz(i, j, 1) = z;
+  int k = 2;
+  for (; k + 3 <= d.kmax; k += 4) {  // four levels' loads before their stores
+    R3 h[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) h[m] = hn(i, j, k + m);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      z = z + half * (hprev + h[m]);
+      zz(i, j, k + m) = z;
+      hprev = h[m];
+    }
+  }
+  for (; k <= d.kmax; ++k) {
+    const R3 h = hn(i, j, k);
+    z = z + half * (hprev + h);
+    zz(i, j, k) = z;
+    hprev = h;
+  }
+}
+
+// ip_blumberg_mellor_lin.F90:99-158: downward integral per U and V column of the along-sigma
+// buoyancy gradient minus the slope of the pressure points times the mean vertical buoyancy
+// gradient of the two columns; lower bound kumin_pmz = kvmin_pmz = 1 (the only value the reference
+// assigns). The V integral starts from hun(kmax) as in the reference (ip_blumberg_mellor_lin.F90:
+// 143); its levels below use hvn. Expressions in the reference's order.
+template <class R3>
+__global__ void k_ip_lin(Dev d, Bc3<R3> s, const R3* zzp) {
+  GB_IJ_HALO
+  V3<R3> hun{d, s.f3[HUN]}, hvn{d, s.f3[HVN]}, buoy{d, s.f3[BUOY]}, idpdx{d, s.f3[IDPDX]}, idpdy{d, s.f3[IDPDY]},
+      zz{d, const_cast<R3*>(zzp)};
+  idpdx(i, j, 0) = R3(0);
+  idpdy(i, j, 0) = R3(0);
+  if (i < d.imin || i > d.imax || j < d.jmin || j > d.jmax) return;
+  I2 au{d, s.au}, av{d, s.av};
+  const int kmax = d.kmax;
+  const R3 half = R3(0.5);
+  auto column = [&](V3<R3>& hx, R3 h0, V3<R3>& out, int oi, int oj, R3 dm1) {
+    // the level k+1 values of both columns carried down in registers
+    R3 b1 = buoy(i + oi, j + oj, kmax), b0 = buoy(i, j, kmax);
+    R3 z1 = zz(i + oi, j + oj, kmax), z0 = zz(i, j, kmax), hk1 = hx(i, j, kmax);
+    R3 dzl = (z1 - z0) * dm1;
+    R3 drl = (b1 - b0) * dm1;
+    R3 prgr = drl * half * h0;
+    out(i, j, kmax) = hk1 * prgr;
+    for (int k = kmax - 1; k >= 1; --k) {
+      const R3 b1k = buoy(i + oi, j + oj, k), b0k = buoy(i, j, k);
+      const R3 z1k = zz(i + oi, j + oj, k), z0k = zz(i, j, k), hk = hx(i, j, k);
+      const R3 dzu = dzl;
+      dzl = (z1k - z0k) * dm1;
+      const R3 dru = drl;
+      drl = (b1k - b0k) * dm1;
+      const R3 dzr2 = (b1 - b1k) / (z1 - z1k);
+      const R3 dzr1 = (b0 - b0k) / (z0 - z0k);
+      const R3 aa = half * (drl + dru);
+      const R3 bb = half * (dzl + dzu);
+      const R3 cc = half * (dzr2 + dzr1);
+      prgr = prgr + (aa - bb * cc) * half * (hk1 + hk);
+      out(i, j, k) = hk * prgr;
+      b1 = b1k; b0 = b0k; z1 = z1k; z0 = z0k; hk1 = hk;
+    }
+  };
+  if (au(i, j) >= 1) column(hun, hun(i, j, kmax), idpdx, 1, 0, R3(1.0 / d.dx));
+  if (av(i, j) >= 1) column(hvn, hun(i, j, kmax), idpdy, 0, 1, R3(1.0 / d.dy));
+}
+
+// ip_song_wright.F90:99-150 (pressure-point heights from k_zz_lin): per U and V column the
+// gradient of the layer-mean buoyancy times the layer-mean height, less the change of the mean
+// buoyancy times the slope of the pressure points. The V column's first slope term is scaled by
+// 1/dx as in the reference (ip_song_wright.F90:128). Expressions in the reference's order.
+template <class R3>
+__global__ void k_ip_sw(Dev d, Bc3<R3> s, const R3* zzp) {
+  GB_IJ_HALO
+  V3<R3> hn{d, s.f3[HN]}, hun{d, s.f3[HUN]}, hvn{d, s.f3[HVN]}, buoy{d, s.f3[BUOY]}, idpdx{d, s.f3[IDPDX]},
+      idpdy{d, s.f3[IDPDY]}, zz{d, const_cast<R3*>(zzp)};
+  idpdx(i, j, 0) = R3(0);
+  idpdy(i, j, 0) = R3(0);
+  if (i < d.imin || i > d.imax || j < d.jmin || j > d.jmax) return;
+  I2 au{d, s.au}, av{d, s.av};
+  const int kmax = d.kmax;
+  const R3 half = R3(0.5), dxm1 = R3(1.0 / d.dx), dym1 = R3(1.0 / d.dy);
+  auto column = [&](V3<R3>& hx, V3<R3>& out, int oi, int oj, R3 dm1, R3 dm1top) {
+    const int i1 = i + oi, j1 = j + oj;
+    // level k+1 values of both columns carried down in registers
+    R3 b1 = buoy(i1, j1, kmax), b0 = buoy(i, j, kmax), h1 = hn(i1, j1, kmax), h0 = hn(i, j, kmax);
+    R3 grdl = half * hx(i, j, kmax) * (b1 - b0) * dm1;
+    R3 buoyl = half * (b1 + b0) * (zz(i1, j1, kmax) - zz(i, j, kmax)) * dm1top;
+    R3 prgr = grdl;
+    out(i, j, kmax) = hx(i, j, kmax) * prgr;
+    for (int k = kmax - 1; k >= 1; --k) {
+      const R3 b1k = buoy(i1, j1, k), b0k = buoy(i, j, k), h1k = hn(i1, j1, k), h0k = hn(i, j, k);
+      grdl = (half * (b1k + b1) * half * (h1k + h1) - half * (b0k + b0) * half * (h0k + h0)) * dm1;
+      const R3 buoyu = buoyl;
+      buoyl = half * (b1k + b0k) * (zz(i1, j1, k) - zz(i, j, k)) * dm1;
+      prgr = prgr + grdl - (buoyu - buoyl);
+      out(i, j, k) = hx(i, j, k) * prgr;
+      b1 = b1k; b0 = b0k; h1 = h1k; h0 = h0k;
+    }
+  };
+  if (au(i, j) >= 1) column(hun, idpdx, 1, 0, dxm1, dxm1);
+  if (av(i, j) >= 1) column(hvn, idpdy, 0, 1, dym1, dxm1);
+}
+
+// ip_chu_fan.F90:67-126 (interface heights from k_zz): the Blumberg-Mellor integral with a
+// correction hc from the squared height differences of the four corners of each interface cell;
+// the integral starts from the top gradient itself and the top level's term is hx*grad*hx/2, as in
+// the reference. Expressions in the reference's order.
+template <class R3>
+__global__ void k_ip_cf(Dev d, Bc3<R3> s, const R3* zzp) {
+  GB_IJ_HALO
+  V3<R3> hun{d, s.f3[HUN]}, hvn{d, s.f3[HVN]}, buoy{d, s.f3[BUOY]}, idpdx{d, s.f3[IDPDX]}, idpdy{d, s.f3[IDPDY]},
+      zz{d, const_cast<R3*>(zzp)};
+  idpdx(i, j, 0) = R3(0);
+  idpdy(i, j, 0) = R3(0);
+  if (i < d.imin || i > d.imax || j < d.jmin || j > d.jmax) return;
+  I2 au{d, s.au}, av{d, s.av};
+  const int kmax = d.kmax;
+  const R3 half = R3(0.5), sixth = R3(1.0 / 6);
+  auto column = [&](V3<R3>& hx, V3<R3>& out, int oi, int oj, R3 dm1) {
+    const int i1 = i + oi, j1 = j + oj;
+    R3 b1 = buoy(i1, j1, kmax), b0 = buoy(i, j, kmax), z1 = zz(i1, j1, kmax), z0 = zz(i, j, kmax);
+    R3 hk1 = hx(i, j, kmax);
+    R3 grdl = (b1 - b0) * dm1;
+    R3 buoyl = half * (b1 + b0);
+    R3 prgr = grdl;
+    out(i, j, kmax) = hk1 * prgr * half * hk1;
+    for (int k = kmax - 1; k >= 1; --k) {
+      const R3 b1k = buoy(i1, j1, k), b0k = buoy(i, j, k), z1k = zz(i1, j1, k), z0k = zz(i, j, k);
+      const R3 hk = hx(i, j, k);
+      const R3 grdu = grdl;
+      grdl = (b1k - b0k) * dm1;
+      const R3 buoyu = buoyl;
+      buoyl = half * (b1k + b0k);
+      const R3 dz = (z1k - z0k) * dm1;
+      const R3 a = z1k - z1, b = z0k - z0, c = z1 - z0, e = z1k - z0k;
+      R3 hc = a * a * (b1k - b1);
+      hc = hc - b * b * (b0k - b0);
+      hc = hc + c * c * (b1 - b0);
+      hc = hc - e * e * (b1k - b0k);
+      hc = hc * dm1 * sixth / (z0k + z1k - z0 - z1);
+      prgr = prgr + (grdu + grdl + hc) * half * (hk + hk1) - dz * (buoyu - buoyl);
+      out(i, j, k) = hk * prgr;
+      b1 = b1k; b0 = b0k; z1 = z1k; z0 = z0k; hk1 = hk;
+    }
+  };
+  if (au(i, j) >= 1) column(hun, idpdx, 1, 0, R3(1.0 / d.dx));
+  if (av(i, j) >= 1) column(hvn, idpdy, 0, 1, R3(1.0 / d.dy));
+}
+
 // uu_momentum_3d.F90:169-304 (DIR 0) / vv_momentum_3d.F90:174-315 (DIR 1), kumin = 1: explicit
 // (the old heights huo/hvo equal hun/hvn at this point of integrate_3d, m3d.F90, and are read from
 // hun/hvn);
@@ -754,6 +916,10 @@ int run_bc3(int which, const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* cons
     case BC3_BF3D: k_bf3d<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s); break;
     case BC3_ZZ: k_zz<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6]); break;
     case BC3_IP: k_ip<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6]); break;
+    case BC3_ZZ_LIN: k_zz_lin<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6]); break;
+    case BC3_IP_LIN: k_ip_lin<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6]); break;
+    case BC3_IP_SW: k_ip_sw<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6]); break;
+    case BC3_IP_CF: k_ip_cf<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6]); break;
     case BC3_UUMOM:
     case BC3_VVMOM: {
       const int nx = d.imax - d.imin + 1, ny = d.jmax - d.jmin + 1;

@@ -354,7 +354,7 @@ class BcState(C.Structure):
     """Mirror of getm_bc_state (include/getm_b200.h)."""
 
     _fields_ = [("f2", P * 54), ("f3", P * 19), ("az", P), ("au", P), ("av", P), ("ax", P), ("par", D * 18),
-                ("ipar", C.c_int32 * 19), ("prec3d", C.c_int32)]
+                ("ipar", C.c_int32 * 20), ("prec3d", C.c_int32)]
 
 
 class BcDevice:

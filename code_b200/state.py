@@ -24,7 +24,7 @@ PD_NAMES = ["dtm", "dt", "cnpar", "min_depth", "crit_depth", "g", "rho_0", "kapp
             "S0", "dtr0", "dsr0", "ip_fac", "temp_AH", "salt_AH"]
 PI_NAMES = ["M", "MM", "runtype", "vel2d_adv_split", "vel2d_adv_hor", "vel3d_adv_split", "vel3d_adv_hor",
             "vel3d_adv_ver", "temp_adv_split", "temp_adv_hor", "temp_adv_ver", "salt_adv_split", "salt_adv_hor",
-            "salt_adv_ver", "adv_ver_iterations", "ufirst2d", "ufirst3d", "calc_temp", "calc_salt"]
+            "salt_adv_ver", "adv_ver_iterations", "ufirst2d", "ufirst3d", "calc_temp", "calc_salt", "ip_method"]
 
 F32 = lambda x: float(np.float32(x))  # noqa: E731  -- a Fortran default-kind real literal widened to double
 
@@ -114,6 +114,7 @@ class BcCase:
         self.az = self.au = self.av = self.ax = None
         self.pd = {n: 0.0 for n in PD_NAMES}
         self.pi = {n: 0 for n in PI_NAMES}
+        self.pi["ip_method"] = 1  # internal_pressure.F90:80 (BLUMBERG_MELLOR)
         self.bdy = None  # OpenBoundaries, or None for a closed domain
 
     def copy(self, dtype3=None):

@@ -200,13 +200,16 @@ int getm_tracer_step_f32(getm_ctx *ctx, float dt, float *f, const float *uu, con
  *       ip_fac temp_AH salt_AH
  *  ipar: M MM runtype vel2d_adv_split vel2d_adv_hor vel3d_adv_split vel3d_adv_hor
  *       vel3d_adv_ver temp_adv_split temp_adv_hor temp_adv_ver salt_adv_split salt_adv_hor
- *       salt_adv_ver adv_ver_iterations ufirst2d ufirst3d calc_temp calc_salt
+ *       salt_adv_ver adv_ver_iterations ufirst2d ufirst3d calc_temp calc_salt ip_method
  * ufirst2d / ufirst3d are the SAVEd alternation switches of momentum.F90:33 (initially 0) and
- * m3d.F90:504 (initially 1); the calls update them in the host-side struct. */
+ * m3d.F90:504 (initially 1); the calls update them in the host-side struct. ip_method selects the
+ * internal pressure gradient (internal_pressure.F90:80, 149-168): 1 = BLUMBERG_MELLOR,
+ * 2 = BLUMBERG_MELLOR_LIN, 4 = SONG_WRIGHT, 5 = CHU_FAN; 3, 6 and 7 return
+ * GETM_ERR_UNSUPPORTED, other values GETM_ERR_ARG. */
 #define GETM_NF2 54
 #define GETM_NF3 19
 #define GETM_NPD 18
-#define GETM_NPI 19
+#define GETM_NPI 20
 typedef struct getm_bc_state {
   double *f2[GETM_NF2];
   void *f3[GETM_NF3];

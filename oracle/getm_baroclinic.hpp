@@ -35,7 +35,7 @@ enum PD {
 enum PI {
   I_M, I_MM, I_RUNTYPE, I_VEL2D_SPLIT, I_VEL2D_HOR, I_VEL3D_SPLIT, I_VEL3D_HOR, I_VEL3D_VER, I_TEMP_SPLIT, I_TEMP_HOR,
   I_TEMP_VER, I_SALT_SPLIT, I_SALT_HOR, I_SALT_VER, I_ADV_VER_ITERS, I_UFIRST2D, I_UFIRST3D, I_CALC_TEMP,
-  I_CALC_SALT, NPI
+  I_CALC_SALT, I_IP_METHOD, NPI
 };
 
 // Open boundaries (domain.F90:263-280, bdy_spec.F90:225-290): segments per side -- western
@@ -622,6 +622,197 @@ void ip_blumberg_mellor(const Dom& d, BcState<R3>& st) {
       }
 }
 
+// ip_blumberg_mellor_lin.F90:71-161: heights of the pressure points (layer centres), then per U
+// and V column a downward integral of the along-sigma buoyancy gradient corrected by the slope of
+// the pressure points times the mean vertical buoyancy gradient of the two columns. The lower
+// bound kumin_pmz / kvmin_pmz is 1: the only value the reference assigns (adaptive_coordinates.F90:
+// 237-238); with sigma coordinates it leaves the arrays unset. The V column starts its integral with
+// hun(kmax) (ip_blumberg_mellor_lin.F90:143), as the reference does; the levels below use hvn.
+template <class R3>
+void ip_blumberg_mellor_lin(const Dom& d, BcState<R3>& st) {
+  A3<R3> hn{d, st.f3[HN]}, hun{d, st.f3[HUN]}, hvn{d, st.f3[HVN]}, buoy{d, st.f3[BUOY]}, idpdx{d, st.f3[IDPDX]},
+      idpdy{d, st.f3[IDPDY]};
+  A2 H{d, st.f2[HH]};
+  M2 az{d, st.az}, au{d, st.au}, av{d, st.av};
+  const int kmax = d.kmax;
+  const R3 dxm1 = R3(1.0 / d.dx), dym1 = R3(1.0 / d.dy);
+  const R3 half = R3(0.5);
+  std::vector<R3> zz_(d.n3d(), R3(0));
+  A3<R3> zz{d, zz_.data()};
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO; ++i) {
+      idpdx(i, j, 0) = R3(0);
+      idpdy(i, j, 0) = R3(0);
+    }
+  for (int j = d.jmin; j <= d.jmax + 1; ++j)
+    for (int i = d.imin; i <= d.imax + 1; ++i)
+      if (az(i, j) >= 1) {
+        zz(i, j, 1) = R3(-H(i, j)) + half * hn(i, j, 1);
+        for (int k = 2; k <= kmax; ++k) zz(i, j, k) = zz(i, j, k - 1) + half * (hn(i, j, k - 1) + hn(i, j, k));
+      }
+  // one column; (oi, oj) = the neighbour across the face, hx = the face's layer heights, h0 = the
+  // height that starts the integral, dm1 = 1/dx or 1/dy
+  auto column = [&](int i, int j, int oi, int oj, A3<R3>& hx, R3 h0, A3<R3>& out, R3 dm1) {
+    R3 dzl = (zz(i + oi, j + oj, kmax) - zz(i, j, kmax)) * dm1;
+    R3 drl = (buoy(i + oi, j + oj, kmax) - buoy(i, j, kmax)) * dm1;
+    R3 prgr = drl * half * h0;
+    out(i, j, kmax) = hx(i, j, kmax) * prgr;
+    for (int k = kmax - 1; k >= 1; --k) {
+      const R3 dzu = dzl;
+      dzl = (zz(i + oi, j + oj, k) - zz(i, j, k)) * dm1;
+      const R3 dru = drl;
+      drl = (buoy(i + oi, j + oj, k) - buoy(i, j, k)) * dm1;
+      const R3 dzr2 = (buoy(i + oi, j + oj, k + 1) - buoy(i + oi, j + oj, k)) /
+                      (zz(i + oi, j + oj, k + 1) - zz(i + oi, j + oj, k));
+      const R3 dzr1 = (buoy(i, j, k + 1) - buoy(i, j, k)) / (zz(i, j, k + 1) - zz(i, j, k));
+      const R3 aa = half * (drl + dru);
+      const R3 bb = half * (dzl + dzu);
+      const R3 cc = half * (dzr2 + dzr1);
+      prgr = prgr + (aa - bb * cc) * half * (hx(i, j, k + 1) + hx(i, j, k));
+      out(i, j, k) = hx(i, j, k) * prgr;
+    }
+  };
+#pragma omp parallel for schedule(static)
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i)
+      if (au(i, j) >= 1) column(i, j, 1, 0, hun, hun(i, j, kmax), idpdx, dxm1);
+#pragma omp parallel for schedule(static)
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i)
+      if (av(i, j) >= 1) column(i, j, 0, 1, hvn, hun(i, j, kmax), idpdy, dym1);
+}
+
+// Heights of the layer interfaces (centres = false, ip_blumberg_mellor.F90:81-90, ip_chu_fan.F90)
+// or of the pressure points (centres = true, ip_blumberg_mellor_lin.F90:87-97, ip_song_wright.F90)
+// of the columns i = imin..imax+1, j = jmin..jmax+1 with az >= 1; zero elsewhere.
+template <class R3>
+std::vector<R3> ip_heights(const Dom& d, BcState<R3>& st, bool centres) {
+  A3<R3> hn{d, st.f3[HN]};
+  A2 H{d, st.f2[HH]};
+  M2 az{d, st.az};
+  const R3 half = R3(0.5);
+  std::vector<R3> zz_(d.n3d(), R3(0));
+  A3<R3> zz{d, zz_.data()};
+  for (int j = d.jmin; j <= d.jmax + 1; ++j)
+    for (int i = d.imin; i <= d.imax + 1; ++i)
+      if (az(i, j) >= 1) {
+        if (centres) {
+          zz(i, j, 1) = R3(-H(i, j)) + half * hn(i, j, 1);
+          for (int k = 2; k <= d.kmax; ++k) zz(i, j, k) = zz(i, j, k - 1) + half * (hn(i, j, k - 1) + hn(i, j, k));
+        } else {
+          zz(i, j, 1) = R3(-H(i, j)) + hn(i, j, 1);
+          for (int k = 2; k <= d.kmax; ++k) zz(i, j, k) = zz(i, j, k - 1) + hn(i, j, k);
+        }
+      }
+  return zz_;
+}
+
+// ip_song_wright.F90:86-150: pressure-point heights; per column the gradient of the layer-mean
+// buoyancy times the layer-mean height, less the change of the mean buoyancy times the slope of the
+// pressure points. The V column's first slope term is scaled by 1/dx (ip_song_wright.F90:128), as
+// in the reference.
+template <class R3>
+void ip_song_wright(const Dom& d, BcState<R3>& st) {
+  A3<R3> hn{d, st.f3[HN]}, hun{d, st.f3[HUN]}, hvn{d, st.f3[HVN]}, buoy{d, st.f3[BUOY]}, idpdx{d, st.f3[IDPDX]},
+      idpdy{d, st.f3[IDPDY]};
+  M2 au{d, st.au}, av{d, st.av};
+  const int kmax = d.kmax;
+  const R3 dxm1 = R3(1.0 / d.dx), dym1 = R3(1.0 / d.dy), half = R3(0.5);
+  std::vector<R3> zz_ = ip_heights(d, st, true);
+  A3<R3> zz{d, zz_.data()};
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO; ++i) {
+      idpdx(i, j, 0) = R3(0);
+      idpdy(i, j, 0) = R3(0);
+    }
+  auto column = [&](int i, int j, int oi, int oj, A3<R3>& hx, A3<R3>& out, R3 dm1, R3 dm1top) {
+    const int i1 = i + oi, j1 = j + oj;
+    R3 grdl = half * hx(i, j, kmax) * (buoy(i1, j1, kmax) - buoy(i, j, kmax)) * dm1;
+    R3 buoyl = half * (buoy(i1, j1, kmax) + buoy(i, j, kmax)) * (zz(i1, j1, kmax) - zz(i, j, kmax)) * dm1top;
+    R3 prgr = grdl;
+    out(i, j, kmax) = hx(i, j, kmax) * prgr;
+    for (int k = kmax - 1; k >= 1; --k) {
+      grdl = (half * (buoy(i1, j1, k) + buoy(i1, j1, k + 1)) * half * (hn(i1, j1, k) + hn(i1, j1, k + 1)) -
+              half * (buoy(i, j, k) + buoy(i, j, k + 1)) * half * (hn(i, j, k) + hn(i, j, k + 1))) *
+             dm1;
+      const R3 buoyu = buoyl;
+      buoyl = half * (buoy(i1, j1, k) + buoy(i, j, k)) * (zz(i1, j1, k) - zz(i, j, k)) * dm1;
+      prgr = prgr + grdl - (buoyu - buoyl);
+      out(i, j, k) = hx(i, j, k) * prgr;
+    }
+  };
+#pragma omp parallel for schedule(static)
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i)
+      if (au(i, j) >= 1) column(i, j, 1, 0, hun, idpdx, dxm1, dxm1);
+#pragma omp parallel for schedule(static)
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i)
+      if (av(i, j) >= 1) column(i, j, 0, 1, hvn, idpdy, dym1, dxm1);
+}
+
+// ip_chu_fan.F90:67-126: interface heights; the Blumberg-Mellor integral with a correction hc
+// from the squared height differences of the four corners of each interface cell. The integral
+// starts from the top gradient itself and the top level's term is hx*grad*hx/2, as in the reference.
+template <class R3>
+void ip_chu_fan(const Dom& d, BcState<R3>& st) {
+  A3<R3> hun{d, st.f3[HUN]}, hvn{d, st.f3[HVN]}, buoy{d, st.f3[BUOY]}, idpdx{d, st.f3[IDPDX]},
+      idpdy{d, st.f3[IDPDY]};
+  M2 au{d, st.au}, av{d, st.av};
+  const int kmax = d.kmax;
+  const R3 dxm1 = R3(1.0 / d.dx), dym1 = R3(1.0 / d.dy), half = R3(0.5), sixth = R3(1.0 / 6);
+  std::vector<R3> zz_ = ip_heights(d, st, false);
+  A3<R3> zz{d, zz_.data()};
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO; ++i) {
+      idpdx(i, j, 0) = R3(0);
+      idpdy(i, j, 0) = R3(0);
+    }
+  auto column = [&](int i, int j, int oi, int oj, A3<R3>& hx, A3<R3>& out, R3 dm1) {
+    const int i1 = i + oi, j1 = j + oj;
+    R3 grdl = (buoy(i1, j1, kmax) - buoy(i, j, kmax)) * dm1;
+    R3 buoyl = half * (buoy(i1, j1, kmax) + buoy(i, j, kmax));
+    R3 prgr = grdl;
+    out(i, j, kmax) = hx(i, j, kmax) * prgr * half * hx(i, j, kmax);
+    for (int k = kmax - 1; k >= 1; --k) {
+      const R3 grdu = grdl;
+      grdl = (buoy(i1, j1, k) - buoy(i, j, k)) * dm1;
+      const R3 buoyu = buoyl;
+      buoyl = half * (buoy(i1, j1, k) + buoy(i, j, k));
+      const R3 dz = (zz(i1, j1, k) - zz(i, j, k)) * dm1;
+      const R3 a = zz(i1, j1, k) - zz(i1, j1, k + 1), b = zz(i, j, k) - zz(i, j, k + 1);
+      const R3 c = zz(i1, j1, k + 1) - zz(i, j, k + 1), e = zz(i1, j1, k) - zz(i, j, k);
+      R3 hc = a * a * (buoy(i1, j1, k) - buoy(i1, j1, k + 1));
+      hc = hc - b * b * (buoy(i, j, k) - buoy(i, j, k + 1));
+      hc = hc + c * c * (buoy(i1, j1, k + 1) - buoy(i, j, k + 1));
+      hc = hc - e * e * (buoy(i1, j1, k) - buoy(i, j, k));
+      hc = hc * dm1 * sixth / (zz(i, j, k) + zz(i1, j1, k) - zz(i, j, k + 1) - zz(i1, j1, k + 1));
+      prgr = prgr + (grdu + grdl + hc) * half * (hx(i, j, k) + hx(i, j, k + 1)) - dz * (buoyu - buoyl);
+      out(i, j, k) = hx(i, j, k) * prgr;
+    }
+  };
+#pragma omp parallel for schedule(static)
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i)
+      if (au(i, j) >= 1) column(i, j, 1, 0, hun, idpdx, dxm1);
+#pragma omp parallel for schedule(static)
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i)
+      if (av(i, j) >= 1) column(i, j, 0, 1, hvn, idpdy, dym1);
+}
+
+// internal_pressure.F90:204-233: the configured method; nonzero for a method not provided here
+template <class R3>
+int do_internal_pressure(const Dom& d, BcState<R3>& st) {
+  switch (st.ipar[I_IP_METHOD]) {
+    case 1: ip_blumberg_mellor(d, st); return 0;
+    case 2: ip_blumberg_mellor_lin(d, st); return 0;
+    case 4: ip_song_wright(d, st); return 0;
+    case 5: ip_chu_fan(d, st); return 0;
+    default: return -1;
+  }
+}
+
 // uu_momentum_3d.F90:169-337 / vv_momentum_3d.F90:174-340 (kumin = kvmin = 1). dir 0 = uu.
 template <class R3>
 void uv_momentum_3d(const Dom& d, BcState<R3>& st, int dir) {
@@ -963,7 +1154,7 @@ int integrate_3d(const Dom& d, const AdvMasks& m, BcState<R3>& st, int n) {
   const long n2 = d.n2d();
   start_macro(d, f2, par, ip[I_M]);
   if (d.kmax > 1) bottom_friction_3d(d, st);
-  if (ip[I_RUNTYPE] == 4) ip_blumberg_mellor(d, st);
+  if (ip[I_RUNTYPE] == 4 && do_internal_pressure(d, st) != 0) return -1;
   for (long q = 0; q < n3; ++q) {
     st.f3[HUO][q] = st.f3[HUN][q];
     st.f3[HVO][q] = st.f3[HVN][q];

@@ -268,7 +268,9 @@ static int bc_call(const or_dom* o, or_bc* s, int which, int arg) {
     case BC_DEPTH_UPDATE: gor::depth_update(d, st.f2, st.az, st.au, st.av, st.par); break;
     case BC_START_MACRO: gor::start_macro(d, st.f2, st.par, st.ipar[gor::I_M]); break;
     case BC_BOTTOM_FRICTION_3D: gor::bottom_friction_3d(d, st); break;
-    case BC_IP: gor::ip_blumberg_mellor(d, st); break;
+    case BC_IP:
+      if (gor::do_internal_pressure(d, st) != 0) return -1;
+      break;
     case BC_UU_MOMENTUM_3D: gor::uv_momentum_3d(d, st, 0); break;
     case BC_VV_MOMENTUM_3D: gor::uv_momentum_3d(d, st, 1); break;
     case BC_SIGMA: gor::sigma_coordinates(d, st); break;

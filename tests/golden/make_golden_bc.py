@@ -3,10 +3,12 @@
 small closed basin, together with the inputs. The oracle and the CUDA path are compared with it
 bit for bit (tests/test_golden_bc_cpu.py) and the CUDA path within 1e-12 (tests/test_gpu_baroclinic.py).
 
-    python tests/golden/make_golden_bc.py [closed] [bdy]
+    python tests/golden/make_golden_bc.py [closed] [bdy] [ip2] [ip4] [ip5]
 
 Configuration: runtype 4 (prognostic T and S), sigma coordinates (equidistant), linear equation of
-state, Blumberg-Mellor internal pressure, P2_PDM / HALFSPLIT advection of momentum (2D and 3D) and
+state, Blumberg-Mellor internal pressure (reference_mode_split_ip2.npz: the linear Blumberg-Mellor
+variant, Song-Wright and Chu-Fan -- ip_method 2, 4, 5 -- in reference_mode_split_ip{2,4,5}.npz on an
+islands basin; see ip_case()), P2_PDM / HALFSPLIT advection of momentum (2D and 3D) and
 tracers, closed boundaries, num/nuh prescribed (the turbulence closure -- the un-vendored GOTM -- is
 replaced by a routine that leaves them unchanged; ss_nn, whose outputs only feed it, likewise),
 no wind, air pressure, freshwater or short-wave forcing. The second fixture,
@@ -35,7 +37,9 @@ FILES = [
     "src/2d/bottom_friction.F90", "src/2d/uv_advect.F90", "src/2d/uv_diffusion.F90", "src/2d/momentum.F90",
     "src/2d/sealevel.F90", "src/2d/depth_update.F90", "src/domain/mirror_bdy_2d.F90", "src/domain/mirror_bdy_3d.F90",
     "src/3d/start_macro.F90", "src/3d/stop_macro.F90", "src/3d/bottom_friction_3d.F90",
-    "src/3d/internal_pressure.F90", "src/3d/ip_blumberg_mellor.F90", "src/3d/uu_momentum_3d.F90",
+    "src/3d/internal_pressure.F90", "src/3d/ip_blumberg_mellor.F90", "src/3d/ip_blumberg_mellor_lin.F90",
+    "src/3d/ip_song_wright.F90", "src/3d/ip_chu_fan.F90",
+    "src/3d/uu_momentum_3d.F90",
     "src/3d/vv_momentum_3d.F90", "src/3d/coordinates.F90", "src/3d/sigma_coordinates.F90",
     "src/3d/ww_momentum_3d.F90", "src/3d/uv_advect_3d.F90", "src/3d/uv_diffusion_3d.F90", "src/3d/stresses_3d.F90",
     "src/3d/temperature.F90", "src/3d/salinity.F90", "src/3d/eqstate.F90", "src/3d/slow_bottom_friction.F90",
@@ -83,7 +87,10 @@ class RefBc:
                   do_numerical_analyses=False, nummix3d_s=None, nummix2d_s=None, phymix3d_s=None,
                   phymix2d_s=None, nummix3d_t=None, nummix2d_t=None, phymix3d_t=None, phymix2d_t=None,
                   numdis3d=None, numdis2d=None, light=None, tke=zero3(), eps=zero3())
-        for k in ("kmin", "kumin", "kvmin"):
+        # kumin_pmz / kvmin_pmz (ip_blumberg_mellor_lin.F90:114,145): 1, the only value the reference
+        # assigns them (adaptive_coordinates.F90:237-238)
+        v3.update(kumin_pmz=F2(np.ones(g.shape2())), kvmin_pmz=F2(np.ones(g.shape2())))
+        for k in ("kmin", "kumin", "kvmin", "kumin_pmz", "kvmin_pmz"):
             v3[k].a = v3[k].a.astype(np.int64)
         for v in (v2, v3):  # variables_2d/3d re-export the domain's index bounds (use domain)
             v.update(imin=g.imin, imax=g.imax, jmin=g.jmin, jmax=g.jmax, kmax=g.kmax)
@@ -146,7 +153,7 @@ class RefBc:
         eq.t0, eq.s0, eq.dtr0, eq.dsr0 = (np.float64(pd["T0"]), np.float64(pd["S0"]), np.float64(pd["dtr0"]),
                                           np.float64(pd["dsr0"]))
         ipm = P.modules["internal_pressure"]
-        ipm.ip_method = 1
+        ipm.ip_method = pi["ip_method"]
         ipm.zz = zero3()
         P.modules["advection"].init_advection()
         # sigma coordinates' first call sets the SAVEd equidistant switch and ga (coordinates.F90)
@@ -232,12 +239,24 @@ def bdy_case():
     return S.baroclinic_case(nx=12, ny=10, kmax=4, recipe="shelf", M=4, dt3=60.0, seed=3, bdy=b)
 
 
+def ip_case(method):
+    """12 x 10 x 5 islands basin (30% land) with another internal pressure method: 2
+    (BLUMBERG_MELLOR_LIN, ip_blumberg_mellor_lin.F90), 4 (SONG_WRIGHT, ip_song_wright.F90) or 5
+    (CHU_FAN, ip_chu_fan.F90). The stratified recipe on a varying bed, so that the height slopes
+    and the vertical buoyancy gradients both enter the gradient."""
+    c = S.baroclinic_case(nx=12, ny=10, kmax=5, recipe="islands", land=0.3, M=4, dt3=60.0, seed=7)
+    c.pi["ip_method"] = method
+    return c
+
+
 def write(c, name):
     out = {"meta": np.array([c.grid.nx, c.grid.ny, c.grid.kmax, c.grid.dx, c.grid.dy])}
-    for k, v in c.f2.items():
-        out["in_f2_" + k] = v
-    for k, v in c.f3.items():
-        out["in_f3_" + k] = v
+    r = RefBc(c)
+    # the inputs are the state the reference starts from: its first sigma_coordinates call (in
+    # RefBc) recomputes the layer heights from H and the elevations, which may differ from the
+    # case's in the last bit
+    for k, v in r.state().items():
+        out["in_" + k] = np.array(v, copy=True)  # state() views the arrays the run then updates
     for k, v in zip(("az", "au", "av", "ax"), c.masks()):
         out["in_" + k] = v
     out["in_pd"] = np.array([c.pd[n] for n in S.PD_NAMES])
@@ -249,7 +268,6 @@ def write(c, name):
         out["bdy_ramp"] = np.array(b.ramp)
         out["bdy_amp"], out["bdy_phase"], out["bdy_period"] = b.amp, b.phase, np.array(b.period)
         out["bdy_data_v"] = b.data_v
-    r = RefBc(c)
     # two macro steps (M = 4 micro steps each)
     r.time_loop(1, 8)
     for k, v in r.state().items():
@@ -260,12 +278,15 @@ def write(c, name):
 
 
 def main():
-    which = sys.argv[1:] or ["closed", "bdy"]
+    which = sys.argv[1:] or ["closed", "bdy", "ip2", "ip4", "ip5"]
     if "closed" in which:
         write(S.baroclinic_case(nx=12, ny=10, kmax=4, recipe="shelf", M=4, dt3=60.0, seed=3),
               "reference_mode_split.npz")
     if "bdy" in which:
         write(bdy_case(), "reference_mode_split_bdy.npz")
+    for m in (2, 4, 5):
+        if f"ip{m}" in which:
+            write(ip_case(m), f"reference_mode_split_ip{m}.npz")
 
 
 if __name__ == "__main__":

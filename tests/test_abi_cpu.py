@@ -55,3 +55,17 @@ def test_version_string():
     from code_b200 import getm
 
     assert b"sm_100a" in getm.lib().getm_version()
+
+
+def test_state_struct_matches_header():
+    """The Python mirror of getm_bc_state and the field / parameter name lists have the sizes that
+    include/getm_b200.h declares (GETM_NF2, GETM_NF3, GETM_NPD, GETM_NPI)."""
+    from code_b200 import state as S
+    from code_b200.getm import BcState
+
+    txt = open(os.path.join(ROOT, "include", "getm_b200.h")).read()
+    n = {k: int(v) for k, v in re.findall(r"#define GETM_(NF2|NF3|NPD|NPI) (\d+)", txt)}
+    assert n == {"NF2": len(S.F2_NAMES), "NF3": len(S.F3_NAMES), "NPD": len(S.PD_NAMES), "NPI": len(S.PI_NAMES)}
+    f = dict((name, t) for name, t in BcState._fields_)
+    assert (f["f2"]._length_, f["f3"]._length_, f["par"]._length_, f["ipar"]._length_) == (
+        n["NF2"], n["NF3"], n["NPD"], n["NPI"])

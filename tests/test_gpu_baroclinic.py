@@ -14,7 +14,7 @@ import oracle
 from code_b200 import state as S
 from code_b200.getm import BcDevice
 from helpers import make_ctx
-from test_golden_bc_cpu import GOLD, GOLD_BDY, load_case
+from test_golden_bc_cpu import GOLD, GOLD_BDY, GOLD_IP, load_case
 
 pytestmark = pytest.mark.gpu
 
@@ -50,7 +50,8 @@ def run_gpu(c, n0, count, dtype3=None):
     return out, ctx
 
 
-@pytest.mark.parametrize("path", [GOLD, GOLD_BDY], ids=["closed", "open boundaries"])
+@pytest.mark.parametrize("path", [GOLD, GOLD_BDY, GOLD_IP[2], GOLD_IP[4], GOLD_IP[5]],
+                         ids=["closed", "open boundaries", "ip_method 2", "ip_method 4", "ip_method 5"])
 def test_time_loop_vs_reference_fixture(path):
     gold = dict(np.load(path))
     c = load_case(gold)
@@ -242,3 +243,54 @@ def test_mixed_kernel_forms_agree(recipe, nx, ny):
         assert np.array_equal(out[True].f2[k], out[False].f2[k], equal_nan=True), k
     for k in S.F3_NAMES:
         assert np.array_equal(out[True].f3[k], out[False].f3[k], equal_nan=True), k
+
+
+@pytest.mark.parametrize("method", [2, 4, 5])
+@pytest.mark.parametrize("recipe", ["shelf", "islands"])
+def test_ip_method_vs_oracle(recipe, method):
+    """The other internal pressure methods -- linear Blumberg-Mellor (2), Song-Wright (4), Chu-Fan
+    (5) -- through getm_time_loop against the oracle, FP64, 1e-12 of each field's scale."""
+    c = S.baroclinic_case(nx=40, ny=28, kmax=10, recipe=recipe, M=5, dt3=60.0, seed=11, land=0.3)
+    c.pi["ip_method"] = method
+    ref = c.copy()
+    oracle.bc_steps(ref, 1, 15)
+    out, ctx = run_gpu(c, 1, 15)
+    bad, worst = compare(out, ref.f2, ref.f3, 1e-12)
+    assert not bad, bad
+    assert ctx.take_warnings() == 0
+
+
+@pytest.mark.parametrize("method", [2, 4, 5])
+def test_ip_method_mixed_error_vs_fp64(method):
+    """The mixed variant with internal pressure method 2, 4 or 5 against the FP64 oracle after 10
+    macro steps of the islands basin (the bounds of the Blumberg-Mellor case)."""
+    import torch
+
+    c = S.baroclinic_case(nx=48, ny=40, kmax=10, recipe="islands", land=0.3, M=10, dt3=60.0, seed=6)
+    c.pi["ip_method"] = method
+    ref = c.copy()
+    oracle.bc_steps(ref, 1, 100)
+    out, _ = run_gpu(c.copy(dtype3=np.float32), 1, 100, dtype3=torch.float32)
+    errs = {k: field_err(out.f2[k], ref.f2[k]) for k in ("z", "U", "V")}
+    errs.update({k: field_err(out.f3[k], ref.f3[k]) for k in ("uu", "vv", "T", "S")})
+    for k in ("T", "S"):
+        assert errs[k] < 1e-5, errs
+    for k in ("z", "U", "V", "uu", "vv"):
+        assert errs[k] < 1e-3, errs
+
+
+@pytest.mark.parametrize("method,code", [(3, "GETM_ERR_UNSUPPORTED"), (6, "GETM_ERR_UNSUPPORTED"),
+                                         (7, "GETM_ERR_UNSUPPORTED"), (0, "GETM_ERR_ARG"), (8, "GETM_ERR_ARG")])
+def test_ip_method_not_provided_is_refused(method, code):
+    """The methods not provided (z-interpolation 3, Shchepetkin-McWilliams 6, Stelling-van Kester
+    7) and invalid ids are refused with an error code before any work (the reference stops on an
+    invalid ip_method, internal_pressure.F90:166-167)."""
+    from code_b200 import getm as G
+
+    c = S.baroclinic_case(nx=16, ny=12, kmax=4, recipe="shelf", M=2, seed=1)
+    c.pi["ip_method"] = method
+    ctx, _ = make_ctx(c)
+    st = BcDevice(c)
+    with pytest.raises(G.GetmError) as e:
+        ctx.time_loop(st, 1, 2)
+    assert G.ERRORS[e.value.code] == code
