@@ -41,12 +41,11 @@ WORKLOAD = ("mode-split baroclinic step (20 x integrate_2d + integrate_3d: 2D mo
 STAGE_WORDS = {"adv_split_u": 8, "adv_split_v": 8, "adv_split_w": 7, "tracer_vdiff": 4, "uv_momentum_3d": 8,
                "internal_pressure": 6}
 # DRAM bytes (read + write) per interior cell per launch of the FP32 stages, averaged over the
-# launches of one macro step in an ncu capture of the 1024 x 1024 x 24 case (the 2048 x 2048 x 50
-# workload is too large to capture under ncu; the sweeps' traffic grows with the cells processed):
-# ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum on the 17 advection and diffusion
-# launches of the timed step of `bench.py --nx 1024 --ny 1024 --kmax 24 --steps 1 --warmup 1
-# --variants mixed --no-cpu-baseline --adj-steps 0`.
-TRAFFIC_PER_CELL_F32 = {"adv_split_u": 29.26, "adv_split_v": 29.63, "adv_split_w": 20.83, "tracer_vdiff": 20.38}
+# launches of the timed macro step of this workload (2048 x 2048 x 50): ncu --metrics
+# dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum (one pass) on the advection and
+# diffusion launches of `bench.py --steps 1 --warmup 1 --variants mixed --no-cpu-baseline
+# --adj-steps 0`. Source: profiles/traffic_sweeps_mixed_2048x2048x50.md.
+TRAFFIC_PER_CELL_F32 = {"adv_split_u": 28.01, "adv_split_v": 31.05, "adv_split_w": 20.94, "tracer_vdiff": 23.78}
 
 
 def parse():
