@@ -586,9 +586,10 @@ int check_state(getm_ctx* ctx, const getm_bc_state* st) {
   if (st->ipar[I_M] < 1 || st->ipar[I_MM] < 1) return fail(ctx, GETM_ERR_ARG, "M and MM must be >= 1");
   if (st->ipar[I_IP_METHOD] < 1 || st->ipar[I_IP_METHOD] > 7)
     return fail(ctx, GETM_ERR_ARG, "ip_method must be 1..7 (internal_pressure.F90:149-168)");
-  if (st->ipar[I_IP_METHOD] == 3 || st->ipar[I_IP_METHOD] > 5)
+  if (st->ipar[I_IP_METHOD] == 3 || st->ipar[I_IP_METHOD] == 7)
     return fail(ctx, GETM_ERR_UNSUPPORTED,
-                "ip_method: BLUMBERG_MELLOR (1), BLUMBERG_MELLOR_LIN (2), SONG_WRIGHT (4), CHU_FAN (5) are provided");
+                "ip_method: BLUMBERG_MELLOR (1), BLUMBERG_MELLOR_LIN (2), SONG_WRIGHT (4), CHU_FAN (5) and "
+                "SHCHEPETKIN_MCWILLIAMS (6) are provided");
   if ((size_t)2 * (ctx->dom.kmax + 1) * 64 * sizeof(double) > 200 * 1024)
     return fail(ctx, GETM_ERR_UNSUPPORTED, "kmax too large for the column solvers");
   return GETM_OK;
@@ -928,12 +929,17 @@ int integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
   GB_K2(k_start_macro_uv, d, s2, 1.0 / (double)(float)ip[I_M]);
   if (d.kmax > 1 && (rc = bc3<R3>(ctx, st, BC3_BF3D, GETM_TIM_BC3D))) return rc;
   if (ip[I_RUNTYPE] == 4) {
-    // internal_pressure.F90:215-229: the configured method (check_state admits 1, 2, 4, 5); heights
-    // of the layer interfaces (1, 5) or of the pressure points (2, 4), then the column integrals
+    // internal_pressure.F90:215-229: the configured method (check_state admits 1, 2, 4, 5, 6);
+    // heights of the layer interfaces (1, 5) or of the pressure points (2, 4; 6 over the whole
+    // haloed domain, with its column integrals), then the gradients
     const int ipm = ip[I_IP_METHOD];
     const bool centres = ipm == 2 || ipm == 4;
-    const int ipk = ipm == 1 ? BC3_IP : ipm == 2 ? BC3_IP_LIN : ipm == 4 ? BC3_IP_SW : BC3_IP_CF;
-    if ((rc = bc3<R3>(ctx, st, centres ? BC3_ZZ_LIN : BC3_ZZ, GETM_TIM_BC3D))) return rc;
+    const int ipk = ipm == 1   ? BC3_IP
+                    : ipm == 2 ? BC3_IP_LIN
+                    : ipm == 4 ? BC3_IP_SW
+                    : ipm == 5 ? BC3_IP_CF
+                               : BC3_IP_SM;
+    if ((rc = bc3<R3>(ctx, st, ipm == 6 ? BC3_SM_COLS : centres ? BC3_ZZ_LIN : BC3_ZZ, GETM_TIM_BC3D))) return rc;
     if ((rc = bc3<R3>(ctx, st, ipk, GETM_TIM_IP))) return rc;
   }
   // m3d.F90 sets huo = hun, hvo = hvn here for uu/vv_momentum_3d; sigma_coordinates below then

@@ -306,6 +306,113 @@ __global__ void k_ip_cf(Dev d, Bc3<R3> s, const R3* zzp) {
   if (av(i, j) >= 1) column(hvn, idpdy, 0, 1, R3(1.0 / d.dy));
 }
 
+// ip_shchepetkin_mcwilliams.F90 constants as the reference evaluates them: eps = 1.e-10 and
+// OneFifth = 0.2 are single-precision literals widened to double; 1./12. is a single-precision
+// quotient.
+template <class R3>
+struct SmConst {
+  static constexpr double eps = double(1.e-10f), fifth = double(0.2f), t = double(1.0f / 12.0f);
+};
+
+// ip_shchepetkin_mcwilliams.F90:61-145: pressure-point heights of every haloed column with az >= 1
+// (into zz), and for the columns i = imin..imax+1, j = jmin..jmax+1 the pressure integral P from
+// the harmonic means of the vertical buoyancy and height differences (marched down the column in
+// registers). Expressions in the reference's order.
+template <class R3>
+__global__ void k_sm_cols(Dev d, Bc3<R3> s, R3* zzp, R3* Pp) {
+  GB_IJ_HALO
+  I2 az{d, s.az};
+  if (az(i, j) < 1) return;
+  V3<R3> hn{d, s.f3[HN]}, buoy{d, s.f3[BUOY]}, zz{d, zzp}, P{d, Pp};
+  V2 H{d, s.f2[HH]};
+  const int kmax = d.kmax;
+  const R3 half = R3(0.5), two = R3(2.0), one = R3(1.0);
+  const R3 eps = R3(SmConst<R3>::eps), fifth = R3(SmConst<R3>::fifth), t = R3(SmConst<R3>::t);
+  R3 z = R3(-H(i, j)) + half * hn(i, j, 1);
+  zz(i, j, 1) = z;
+  for (int k = 2; k <= kmax; ++k) {
+    z = z + half * (hn(i, j, k - 1) + hn(i, j, k));
+    zz(i, j, k) = z;
+  }
+  if (i < d.imin || i > d.imax + 1 || j < d.jmin || j > d.jmax + 1) return;
+  // original differences o(k) = x(k+1) - x(k), k = 1..kmax-1, o(kmax) = o(kmax-1), o(0) = o(1);
+  // harmonic means h(k) of o(k), o(k-1) for k = 1..kmax
+  auto oR = [&](int k) {
+    const int kk = k < 1 ? 1 : (k > kmax - 1 ? kmax - 1 : k);
+    return buoy(i, j, kk + 1) - buoy(i, j, kk);
+  };
+  auto oZ = [&](int k) {
+    const int kk = k < 1 ? 1 : (k > kmax - 1 ? kmax - 1 : k);
+    return zz(i, j, kk + 1) - zz(i, j, kk);
+  };
+  auto hR = [&](int k) {
+    const R3 a = oR(k), b = oR(k - 1);
+    const R3 cff = two * a * b;
+    return cff > eps ? cff / (a + b) : R3(0);
+  };
+  auto hZ = [&](int k) {
+    const R3 a = oZ(k), b = oZ(k - 1);
+    return two * a * b / (a + b);
+  };
+  const R3 cff1 = one / (zz(i, j, kmax) - zz(i, j, kmax - 1));
+  const R3 cff2 = half * (buoy(i, j, kmax) - buoy(i, j, kmax - 1)) * half * hn(i, j, kmax) * cff1;
+  R3 p = (buoy(i, j, kmax) + cff2) * half * hn(i, j, kmax);
+  P(i, j, kmax) = p;
+  R3 dR1 = hR(kmax), dZ1 = hZ(kmax);  // level k+1
+  for (int k = kmax - 1; k >= 1; --k) {
+    const R3 dR0 = hR(k), dZ0 = hZ(k);
+    const R3 b1 = buoy(i, j, k + 1), b0 = buoy(i, j, k), z1 = zz(i, j, k + 1), z0 = zz(i, j, k);
+    p = p + half * ((b1 + b0) * (z1 - z0) -
+                    fifth * ((dR1 - dR0) * (z1 - z0 - t * (dZ1 + dZ0)) - (dZ1 - dZ0) * (b1 - b0 - t * (dR1 + dR0))));
+    P(i, j, k) = p;
+    dR1 = dR0;
+    dZ1 = dZ0;
+  }
+}
+
+// ip_shchepetkin_mcwilliams.F90:147-262: per U and V face of the interior and level, the pressure
+// difference of the two columns plus the flux term FC from the harmonic means of the horizontal
+// height and buoyancy differences (each thread forms the two means of its face from the columns
+// before, at and after the face), less the elevation-slope term. Expressions in the reference's
+// order.
+template <class R3>
+__global__ void k_ip_sm(Dev d, Bc3<R3> s, const R3* zzp, const R3* Pp) {
+  GB_IJ_HALO
+  V3<R3> hun{d, s.f3[HUN]}, hvn{d, s.f3[HVN]}, buoy{d, s.f3[BUOY]}, idpdx{d, s.f3[IDPDX]}, idpdy{d, s.f3[IDPDY]},
+      zz{d, const_cast<R3*>(zzp)}, P{d, const_cast<R3*>(Pp)};
+  V2 sseo{d, s.f2[SSEO]};
+  idpdx(i, j, 0) = R3(0);
+  idpdy(i, j, 0) = R3(0);
+  if (i < d.imin || i > d.imax || j < d.jmin || j > d.jmax) return;
+  I2 au{d, s.au}, av{d, s.av};
+  const int kmax = d.kmax;
+  const R3 half = R3(0.5), two = R3(2.0), one = R3(1.0);
+  const R3 eps = R3(SmConst<R3>::eps), fifth = R3(SmConst<R3>::fifth), t = R3(SmConst<R3>::t);
+  auto harm = [&](R3 a, R3 b) {
+    const R3 cff = two * a * b;
+    return cff > eps ? cff * (one / (a + b)) : R3(0);
+  };
+  auto column = [&](V3<R3>& hx, V3<R3>& out, int oi, int oj, R3 dm1) {
+    const int im = i - oi, jm = j - oj, i1 = i + oi, j1 = j + oj, i2 = i + 2 * oi, j2 = j + 2 * oj;
+    const R3 slope = R3(sseo(i1, j1) - sseo(i, j));
+    for (int k = kmax; k >= 1; --k) {
+      const R3 zm = zz(im, jm, k), z0 = zz(i, j, k), z1 = zz(i1, j1, k), z2 = zz(i2, j2, k);
+      const R3 bm = buoy(im, jm, k), b0 = buoy(i, j, k), b1 = buoy(i1, j1, k), b2 = buoy(i2, j2, k);
+      const R3 dZx0 = harm(z0 - zm, z1 - z0), dZx1 = harm(z1 - z0, z2 - z1);
+      const R3 dRx0 = harm(b0 - bm, b1 - b0), dRx1 = harm(b1 - b0, b2 - b1);
+      R3 AJ = P(i1, j1, k) - P(i, j, k);
+      const R3 FC = half * ((b1 + b0) * (z1 - z0) -
+                            fifth * ((dRx1 - dRx0) * (z1 - z0 - t * (dZx1 + dZx0)) -
+                                     (dZx1 - dZx0) * (b1 - b0 - t * (dRx1 + dRx0))));
+      AJ = AJ + FC;
+      const R3 hk = hx(i, j, k);
+      out(i, j, k) = AJ * dm1 * hk - hk * dm1 * slope * half * (buoy(i1, j1, kmax) + buoy(i, j, kmax));
+    }
+  };
+  if (au(i, j) >= 1) column(hun, idpdx, 1, 0, R3(1.0 / d.dx));
+  if (av(i, j) >= 1) column(hvn, idpdy, 0, 1, R3(1.0 / d.dy));
+}
+
 // uu_momentum_3d.F90:169-304 (DIR 0) / vv_momentum_3d.F90:174-315 (DIR 1), kumin = 1: explicit
 // (the old heights huo/hvo equal hun/hvn at this point of integrate_3d, m3d.F90, and are read from
 // hun/hvn);
@@ -920,6 +1027,8 @@ int run_bc3(int which, const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* cons
     case BC3_IP_LIN: k_ip_lin<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6]); break;
     case BC3_IP_SW: k_ip_sw<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6]); break;
     case BC3_IP_CF: k_ip_cf<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6]); break;
+    case BC3_SM_COLS: k_sm_cols<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6], scr[0]); break;
+    case BC3_IP_SM: k_ip_sm<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6], scr[0]); break;
     case BC3_UUMOM:
     case BC3_VVMOM: {
       const int nx = d.imax - d.imin + 1, ny = d.jmax - d.jmin + 1;

@@ -103,7 +103,7 @@ int run_build_masks(const Dev& d, cudaStream_t s, const int32_t* az, const int32
 enum {
   BC3_BF3D = 0, BC3_ZZ, BC3_IP, BC3_UUMOM, BC3_VVMOM, BC3_SIGMA, BC3_WW, BC3_UVADV_PREP_U, BC3_UVADV_PREP_V,
   BC3_STRESSES, BC3_EQSTATE, BC3_SLOW_TERMS, BC3_UVADV_PREP_UV, BC3_ZZ_LIN, BC3_IP_LIN,
-  BC3_IP_SW, BC3_IP_CF
+  BC3_IP_SW, BC3_IP_CF, BC3_SM_COLS, BC3_IP_SM
 };
 template <class R3>
 struct Bc3;

@@ -801,6 +801,91 @@ void ip_chu_fan(const Dom& d, BcState<R3>& st) {
       if (av(i, j) >= 1) column(i, j, 0, 1, hvn, idpdy, dym1);
 }
 
+// ip_shchepetkin_mcwilliams.F90:61-262: pressure-point heights over the whole haloed domain; per
+// column a pressure integral P with harmonic-mean vertical differences of buoyancy and height; per
+// level the along-level pressure difference from P plus a horizontal flux term FC with
+// harmonic-mean horizontal differences, less the elevation-slope term. Constants as the reference
+// evaluates them: eps = 1.e-10 and OneFifth = 0.2 are single-precision literals widened to double,
+// 1./12. a single-precision quotient (the factor t below).
+template <class R3>
+void ip_shchepetkin_mcwilliams(const Dom& d, BcState<R3>& st) {
+  A3<R3> hn{d, st.f3[HN]}, hun{d, st.f3[HUN]}, hvn{d, st.f3[HVN]}, buoy{d, st.f3[BUOY]}, idpdx{d, st.f3[IDPDX]},
+      idpdy{d, st.f3[IDPDY]};
+  A2 H{d, st.f2[HH]}, sseo{d, st.f2[SSEO]};
+  M2 az{d, st.az}, au{d, st.au}, av{d, st.av};
+  const int kmax = d.kmax;
+  const R3 dxm1 = R3(1.0 / d.dx), dym1 = R3(1.0 / d.dy), half = R3(0.5), two = R3(2.0), one = R3(1.0);
+  const R3 eps = R3(double(1.e-10f)), fifth = R3(double(0.2f)), t = R3(double(1.0f / 12.0f));
+  std::vector<R3> zz_(d.n3d(), R3(0)), P_(d.n3d(), R3(0));
+  A3<R3> zz{d, zz_.data()}, P{d, P_.data()};
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO; ++i)
+      if (az(i, j) >= 1) {
+        zz(i, j, 1) = R3(-H(i, j)) + half * hn(i, j, 1);
+        for (int k = 2; k <= kmax; ++k) zz(i, j, k) = zz(i, j, k - 1) + half * (hn(i, j, k - 1) + hn(i, j, k));
+      }
+  std::vector<R3> dR(kmax + 1), dZ(kmax + 1);
+  for (int j = d.jmin; j <= d.jmax + 1; ++j)
+    for (int i = d.imin; i <= d.imax + 1; ++i)
+      if (az(i, j) >= 1) {
+        for (int k = 1; k <= kmax - 1; ++k) {
+          dR[k] = buoy(i, j, k + 1) - buoy(i, j, k);
+          dZ[k] = zz(i, j, k + 1) - zz(i, j, k);
+        }
+        dR[kmax] = dR[kmax - 1];
+        dZ[kmax] = dZ[kmax - 1];
+        dR[0] = dR[1];
+        dZ[0] = dZ[1];
+        for (int k = kmax; k >= 1; --k) {
+          const R3 cff = two * dR[k] * dR[k - 1];
+          dR[k] = cff > eps ? cff / (dR[k] + dR[k - 1]) : R3(0);
+          dZ[k] = two * dZ[k] * dZ[k - 1] / (dZ[k] + dZ[k - 1]);
+        }
+        const R3 cff1 = one / (zz(i, j, kmax) - zz(i, j, kmax - 1));
+        const R3 cff2 = half * (buoy(i, j, kmax) - buoy(i, j, kmax - 1)) * half * hn(i, j, kmax) * cff1;
+        P(i, j, kmax) = (buoy(i, j, kmax) + cff2) * half * hn(i, j, kmax);
+        for (int k = kmax - 1; k >= 1; --k)
+          P(i, j, k) = P(i, j, k + 1) +
+                       half * ((buoy(i, j, k + 1) + buoy(i, j, k)) * (zz(i, j, k + 1) - zz(i, j, k)) -
+                               fifth * ((dR[k + 1] - dR[k]) * (zz(i, j, k + 1) - zz(i, j, k) - t * (dZ[k + 1] + dZ[k])) -
+                                        (dZ[k + 1] - dZ[k]) * (buoy(i, j, k + 1) - buoy(i, j, k) - t * (dR[k + 1] + dR[k]))));
+      }
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO; ++i) {
+      idpdx(i, j, 0) = R3(0);
+      idpdy(i, j, 0) = R3(0);
+    }
+  // harmonic mean of two neighbouring differences (ip_shchepetkin_mcwilliams.F90:172-186)
+  auto harm = [&](R3 a, R3 b) {
+    const R3 cff = two * a * b;
+    return cff > eps ? cff * (one / (a + b)) : R3(0);
+  };
+  // one face at level k: columns c0 (i, j) and c1 (i+oi, j+oj), the differences to the columns
+  // before c0 and after c1 along the direction
+  auto face = [&](int i, int j, int oi, int oj, int k, A3<R3>& hx, R3 dm1) {
+    const int im = i - oi, jm = j - oj, i1 = i + oi, j1 = j + oj, i2 = i + 2 * oi, j2 = j + 2 * oj;
+    const R3 z0 = zz(i, j, k) - zz(im, jm, k), z1 = zz(i1, j1, k) - zz(i, j, k), z2 = zz(i2, j2, k) - zz(i1, j1, k);
+    const R3 r0 = buoy(i, j, k) - buoy(im, jm, k), r1 = buoy(i1, j1, k) - buoy(i, j, k),
+             r2 = buoy(i2, j2, k) - buoy(i1, j1, k);
+    const R3 dZx0 = harm(z0, z1), dZx1 = harm(z1, z2), dRx0 = harm(r0, r1), dRx1 = harm(r1, r2);
+    R3 AJ = P(i1, j1, k) - P(i, j, k);
+    const R3 FC = half * ((buoy(i1, j1, k) + buoy(i, j, k)) * (zz(i1, j1, k) - zz(i, j, k)) -
+                          fifth * ((dRx1 - dRx0) * (zz(i1, j1, k) - zz(i, j, k) - t * (dZx1 + dZx0)) -
+                                   (dZx1 - dZx0) * (buoy(i1, j1, k) - buoy(i, j, k) - t * (dRx1 + dRx0))));
+    AJ = AJ + FC;
+    return AJ * dm1 * hx(i, j, k) -
+           hx(i, j, k) * dm1 * R3(sseo(i1, j1) - sseo(i, j)) * half * (buoy(i1, j1, kmax) + buoy(i, j, kmax));
+  };
+#pragma omp parallel for schedule(static)
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i) {
+      if (au(i, j) >= 1)
+        for (int k = kmax; k >= 1; --k) idpdx(i, j, k) = face(i, j, 1, 0, k, hun, dxm1);
+      if (av(i, j) >= 1)
+        for (int k = kmax; k >= 1; --k) idpdy(i, j, k) = face(i, j, 0, 1, k, hvn, dym1);
+    }
+}
+
 // internal_pressure.F90:204-233: the configured method; nonzero for a method not provided here
 template <class R3>
 int do_internal_pressure(const Dom& d, BcState<R3>& st) {
@@ -809,6 +894,7 @@ int do_internal_pressure(const Dom& d, BcState<R3>& st) {
     case 2: ip_blumberg_mellor_lin(d, st); return 0;
     case 4: ip_song_wright(d, st); return 0;
     case 5: ip_chu_fan(d, st); return 0;
+    case 6: ip_shchepetkin_mcwilliams(d, st); return 0;
     default: return -1;
   }
 }

@@ -465,6 +465,9 @@ class Scope:
         self.result = result
 
 
+_SINGLE_LIT = re.compile(r"np\.float64\(np\.float32\(([^()]*)\)\)")
+
+
 def _real_literal(txt: str) -> str:
     t = txt.lower()
     kind = None
@@ -531,6 +534,14 @@ class ExprParser:
                 break
             self.take()
             rhs = self.parse(p if right else p + 1)
+            # an operation between two default-kind real literals is evaluated in single precision,
+            # as Fortran does (e.g. 1.0/12.0), then widened like a literal
+            ml, mr = _SINGLE_LIT.fullmatch(left), _SINGLE_LIT.fullmatch(rhs)
+            if ml and mr and val in ("+", "-", "*", "/"):
+                a, b = np.float32(float(ml.group(1))), np.float32(float(mr.group(1)))
+                r = {"+": a + b, "-": a - b, "*": a * b, "/": a / b}[val]
+                left = f"np.float64(np.float32({float(r)!r}))"
+                continue
             left = f"{helper}({left}, {rhs})"
         return left
 

@@ -3,8 +3,8 @@
 reference's Fortran source): every 2D and 3D field of the state, bit for bit, after two macro
 steps of four micro steps -- a closed basin, (reference_mode_split_bdy.npz) a basin with open
 boundaries of all four 2D types (update_2d_bdy, mirror_bdy_2d/3d), and
-(reference_mode_split_ip{2,4,5}.npz) islands basins with the linear Blumberg-Mellor, Song-Wright
-and Chu-Fan internal pressure."""
+(reference_mode_split_ip{2,4,5,6}.npz) islands basins with the linear Blumberg-Mellor, Song-Wright,
+Chu-Fan and Shchepetkin-McWilliams internal pressure."""
 import os
 
 import numpy as np
@@ -17,7 +17,7 @@ from code_b200.grid import Grid
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_mode_split.npz")
 GOLD_BDY = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_mode_split_bdy.npz")
 GOLD_IP = {m: os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", f"reference_mode_split_ip{m}.npz")
-           for m in (2, 4, 5)}
+           for m in (2, 4, 5, 6)}
 GOLD_IP2 = GOLD_IP[2]
 
 
@@ -43,8 +43,7 @@ def load_case(gold, dtype3=np.float64):
     return c
 
 
-GOLDS = {"closed": GOLD, "open boundaries": GOLD_BDY, "ip_method 2": GOLD_IP[2], "ip_method 4": GOLD_IP[4],
-         "ip_method 5": GOLD_IP[5]}
+GOLDS = {"closed": GOLD, "open boundaries": GOLD_BDY, **{f"ip_method {m}": GOLD_IP[m] for m in (2, 4, 5, 6)}}
 
 
 @pytest.fixture(scope="module", params=list(GOLDS))
@@ -66,7 +65,7 @@ def test_time_loop_matches_reference(gold):
     assert not bad, bad
 
 
-@pytest.mark.parametrize("method", [2, 4, 5])
+@pytest.mark.parametrize("method", [2, 4, 5, 6])
 def test_ip_method_fixture_differs_from_method_1(method):
     """Each internal-pressure fixture pins a method of its own: the oracle with Blumberg-Mellor (1)
     on the same inputs gives other internal pressure gradients."""
