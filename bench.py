@@ -44,7 +44,7 @@ STAGE_WORDS = {"adv_split_u": 8, "adv_split_v": 8, "adv_split_w": 7, "tracer_vdi
 # launches of the timed macro step of this workload (2048 x 2048 x 50): ncu --metrics
 # dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum (one pass) on the advection and
 # diffusion launches of `bench.py --steps 1 --warmup 1 --variants mixed --no-cpu-baseline
-# --adj-steps 0`. Source: profiles/traffic_sweeps_mixed_2048x2048x50.md.
+# --adj-steps 0`.
 TRAFFIC_PER_CELL_F32 = {"adv_split_u": 28.01, "adv_split_v": 31.05, "adv_split_w": 20.94, "tracer_vdiff": 23.78}
 
 

@@ -322,8 +322,13 @@ template <class R3>
 __global__ void k_sm_cols(Dev d, Bc3<R3> s, R3* zzp, R3* Pp) {
   GB_IJ_HALO
   I2 az{d, s.az};
-  if (az(i, j) < 1) return;
   V3<R3> hn{d, s.f3[HN]}, buoy{d, s.f3[BUOY]}, zz{d, zzp}, P{d, Pp};
+  if (az(i, j) < 1) {
+    // land: zz stays zero, as the reference's array does (allocated zero, written on water only,
+    // internal_pressure.F90:135); the face terms of neighbouring water columns read it
+    for (int k = 1; k <= d.kmax; ++k) zz(i, j, k) = R3(0);
+    return;
+  }
   V2 H{d, s.f2[HH]};
   const int kmax = d.kmax;
   const R3 half = R3(0.5), two = R3(2.0), one = R3(1.0);

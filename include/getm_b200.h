@@ -343,7 +343,9 @@ int getm_check_3d_fields(getm_ctx *ctx, const double *f, const int32_t *az, doub
  * Device and stream: the caller makes the device that owns the arrays current and passes a
  * stream of that device (NULL = legacy default stream). The first call on each device looks up
  * the scratch address there (a one-time set-up, no allocation); make that first call before any
- * stream capture begins.
+ * stream capture begins. The address is kept per device together with the CUDA context it was
+ * found in: a call in another context of the device (e.g. after cudaDeviceReset ended the primary
+ * context) repeats that set-up.
  * Concurrency: all calls on one device share the one scratch array. Calls whose work overlaps in
  * time (on different streams, or from several host threads without ordering) race on it and give
  * wrong results; calls on one stream are ordered and safe. */

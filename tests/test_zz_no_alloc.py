@@ -59,6 +59,23 @@ def test_bad_arguments_are_rejected():
                                        None) == GETM_ERR_ARG
 
 
+def test_huge_strides_do_not_overflow_the_size_check():
+    """Strides so large that sk*(kmax+1) or sj*nj would overflow a 64-bit integer are refused
+    (GETM_ERR_TOO_LARGE for the 3D extent, GETM_ERR_ARG for inconsistent strides) before any device
+    work: the sizes are compared by division."""
+    g = Grid(8, 8, 50, 100.0, 100.0)
+    fake = C.c_void_p(256)
+    L = getm.lib()
+    dom = g.domain()
+    dom.sk = 1 << 62  # sk * 51 wraps around in int64
+    assert L.getm_tracer_vdiff_noalloc(C.byref(dom), None, 60.0, 0.9, 1e-9, fake, fake, fake, fake,
+                                       None) == GETM_ERR_TOO_LARGE
+    dom = g.domain()
+    dom.sj = 1 << 61  # sj * nj wraps around; sk smaller than sj
+    assert L.getm_tracer_vdiff_noalloc(C.byref(dom), None, 60.0, 0.9, 1e-9, fake, fake, fake, fake,
+                                       None) == GETM_ERR_ARG
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("with_src", [False, True])
 def test_noalloc_matches_context_entry_two_calls(with_src):
