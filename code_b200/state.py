@@ -17,21 +17,35 @@ from .grid import HALO, Grid
 F2_NAMES = ["z", "zo", "U", "V", "D", "DU", "DV", "UEx", "VEx", "fU", "fV", "ru", "rv", "ruu", "rvv", "Uint", "Vint",
             "Uinto", "Vinto", "SlUx", "SlVx", "Slru", "Slrv", "zub", "zvb", "zub0", "zvb0", "fwf", "H", "HU", "HV",
             "dry_z", "dry_u", "dry_v", "coru", "corv", "tausx", "tausy", "airp", "sseo", "ssen", "ssuo", "ssun",
-            "ssvo", "ssvn", "Dn", "Dun", "Dvn", "rru", "rrv", "taubx", "tauby", "taub", "taus"]
+            "ssvo", "ssvn", "Dn", "Dun", "Dvn", "rru", "rrv", "taubx", "tauby", "taub", "taus",
+            "swr", "shf", "A", "g1", "g2"]
 F3_NAMES = ["uu", "vv", "ww", "ho", "hn", "huo", "hun", "hvo", "hvn", "uuEx", "vvEx", "idpdx", "idpdy", "T", "S",
-            "rho", "buoy", "num", "nuh"]
+            "rho", "buoy", "num", "nuh", "rad", "tke", "eps"]
 PD_NAMES = ["dtm", "dt", "cnpar", "min_depth", "crit_depth", "g", "rho_0", "kappa", "avmmol", "avmolt", "avmols", "T0",
-            "S0", "dtr0", "dsr0", "ip_fac", "temp_AH", "salt_AH"]
+            "S0", "dtr0", "dsr0", "ip_fac", "temp_AH", "salt_AH", "avmback", "avhback", "cp", "swr_bot_refl_frac",
+            "swr_min_bot_frac"]
 PI_NAMES = ["M", "MM", "runtype", "vel2d_adv_split", "vel2d_adv_hor", "vel3d_adv_split", "vel3d_adv_hor",
             "vel3d_adv_ver", "temp_adv_split", "temp_adv_hor", "temp_adv_ver", "salt_adv_split", "salt_adv_hor",
-            "salt_adv_ver", "adv_ver_iterations", "ufirst2d", "ufirst3d", "calc_temp", "calc_salt", "ip_method"]
+            "salt_adv_ver", "adv_ver_iterations", "ufirst2d", "ufirst3d", "calc_temp", "calc_salt", "ip_method",
+            "viscosity", "eqstate_method", "sealevel_check", "radiation", "nan_warned"]
+# fields that only a switched-on option reads or writes (radiation: swr, shf, A, g1, g2, rad;
+# PARABOLIC_VISCOSITY: tke, eps, each optional): a device state may leave them out (NULL)
+OPTIONAL_F2 = ("swr", "shf", "A", "g1", "g2")
+OPTIONAL_F3 = ("rad", "tke", "eps")
+# values of the parameters added after the first fixtures were written (their defaults in the
+# reference: variables_3d.F90:120, parameters.F90:23, temperature.F90:50-51, m2d.F90:82,
+# eqstate.F90:27 -- where the configurations use the linear equation of state)
+PARAM_DEFAULTS_PD = dict(avmback=0.0, avhback=0.0, cp=3985.0, swr_bot_refl_frac=-1.0,
+                         swr_min_bot_frac=float(np.float32(0.01)))
+PARAM_DEFAULTS_PI = dict(ip_method=1, viscosity=0, eqstate_method=1, sealevel_check=0, radiation=0, nan_warned=0)
 
 F32 = lambda x: float(np.float32(x))  # noqa: E731  -- a Fortran default-kind real literal widened to double
 
 # parameters.F90:21-27 and eqstate.F90:27 literals are single precision in the reference
 DEFAULT_PD = dict(g=F32(9.81), rho_0=1025.0, kappa=F32(0.4), avmmol=F32(1.8e-6), avmolt=F32(1.4e-7),
                   avmols=F32(1.1e-9), T0=10.0, S0=33.75, dtr0=F32(-0.17), dsr0=F32(0.78), ip_fac=1.0, temp_AH=-1.0,
-                  salt_AH=-1.0, cnpar=F32(0.9), min_depth=0.5, crit_depth=2.0)
+                  salt_AH=-1.0, cnpar=F32(0.9), min_depth=0.5, crit_depth=2.0, avmback=0.0, avhback=0.0, cp=3985.0,
+                  swr_bot_refl_frac=-1.0, swr_min_bot_frac=F32(0.01))
 P2_PDM, HALFSPLIT = 6, 2
 
 
@@ -115,6 +129,7 @@ class BcCase:
         self.pd = {n: 0.0 for n in PD_NAMES}
         self.pi = {n: 0 for n in PI_NAMES}
         self.pi["ip_method"] = 1  # internal_pressure.F90:80 (BLUMBERG_MELLOR)
+        self.pi["eqstate_method"] = 1  # linear, as the configurations ask
         self.bdy = None  # OpenBoundaries, or None for a closed domain
 
     def copy(self, dtype3=None):

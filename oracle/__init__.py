@@ -89,13 +89,15 @@ def _declare(L):
         fn.argtypes = [P, P, C.c_int, C.c_int]
         fn.restype = C.c_int
     L.or_bc_sizes.argtypes = [P]
+    L.or_sealevel_nan_check.argtypes = [P, P, P, P]
+    L.or_sealevel_nan_check.restype = C.c_longlong
 
 
 # routine ids of or_bc_call (oracle_capi.cpp)
 BC_ROUTINES = ["bottom_friction", "uv_advect_2d", "umomentum", "vmomentum", "sealevel", "depth_update",
                "start_macro", "bottom_friction_3d", "internal_pressure", "uu_momentum_3d", "vv_momentum_3d",
                "sigma_coordinates", "ww_momentum_3d", "uv_advect_3d", "stresses_3d", "do_eqstate",
-               "slow_bottom_friction", "slow_terms", "integrate_2d", "integrate_3d"]
+               "slow_bottom_friction", "slow_terms", "integrate_2d", "integrate_3d", "gotm_parabolic", "sw_radiation"]
 
 
 def bc_sizes():
@@ -130,6 +132,16 @@ def bc_call(case, routine: str, arg: int = 0):
     read_back_ipar(case, s)
     if r != 0:
         raise ValueError(f"{routine} failed ({r})")
+
+
+def sealevel_nan_check(grid, z):
+    """sealevel_nan_check (sealevel.F90:172-314): (count, i, j) of the interior elevations that are
+    not below HUGE; (i, j) is the last such point in the reference's loop order (None if none)."""
+    dom = OrDom(grid.imin, grid.imax, grid.jmin, grid.jmax, grid.kmax, grid.ni, grid.ni * grid.nj, grid.dx, grid.dy,
+                grid.ard1)
+    i, j = C.c_int(0), C.c_int(0)
+    n = lib().or_sealevel_nan_check(C.addressof(dom), _p(np.ascontiguousarray(z, np.float64)), C.byref(i), C.byref(j))
+    return int(n), (int(i.value), int(j.value)) if n > 0 else None
 
 
 def _p(a):

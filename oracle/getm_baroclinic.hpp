@@ -8,13 +8,16 @@
 // variables_3d, domain) are passed as one table of pointers (BcState); 3D fields may be FP64 or
 // FP32 (template R3), 2D fields are always FP64.
 //
-// Scope: runtype 4 (prognostic T and S); no open boundaries (update_2d_bdy, mirror_bdy_2d/3d
-// are no-ops); vert_cord = 1 with equidistant sigma; eqstate_method = 1 (linear); ip_method = 1
-// (Blumberg-Mellor); num/nuh prescribed (gotm() leaves them unchanged); no numerical-mixing
-// analysis; no rivers; An_method = 0 and Am = 0 (no horizontal momentum diffusion).
+// Scope: runtype 4 (prognostic T and S); open boundaries of the four 2D types (update_2d_bdy,
+// mirror_bdy_2d/3d); vert_cord = 1 with equidistant sigma; eqstate_method 1 (linear), 2 (UNESCO80)
+// or 3 (Jackett et al. 2006); ip_method 1, 2, 4, 5, 6; num/nuh prescribed (CONSTANT_VISCOSITY) or
+// the PARABOLIC_VISCOSITY profile of gotm(); short-wave radiation and surface heat flux in
+// do_temperature; sealevel_nan_check; no numerical-mixing analysis; no rivers; An_method = 0 and
+// Am = 0 (no horizontal momentum diffusion).
 #pragma once
 #include <cmath>
 #include <cstdint>
+#include <limits>
 #include <vector>
 
 #include "getm_oracle.hpp"
@@ -25,18 +28,25 @@ namespace gor {
 enum F2 {
   Z, ZO, U_, V_, D_, DU, DV, UEX, VEX, FU, FV, RU, RV, RUU, RVV, UINT, VINT, UINTO, VINTO, SLUX, SLVX, SLRU, SLRV,
   ZUB, ZVB, ZUB0, ZVB0, FWF, HH, HU, HV, DRY_Z, DRY_U, DRY_V, CORU, CORV, TAUSX, TAUSY, AIRP, SSEO, SSEN, SSUO,
-  SSUN, SSVO, SSVN, DN, DUN, DVN, RRU, RRV, TAUBX, TAUBY, TAUB, TAUS, NF2
+  SSUN, SSVO, SSVN, DN, DUN, DVN, RRU, RRV, TAUBX, TAUBY, TAUB, TAUS, SWR, SHF, ATT_A, ATT_G1, ATT_G2, NF2
 };
-enum F3 { UU, VV, WW, HO, HN, HUO, HUN, HVO, HVN, UUEX, VVEX, IDPDX, IDPDY, TT, SS, RHO, BUOY, NUM, NUH, NF3 };
+enum F3 {
+  UU, VV, WW, HO, HN, HUO, HUN, HVO, HVN, UUEX, VVEX, IDPDX, IDPDY, TT, SS, RHO, BUOY, NUM, NUH, RAD, TKE, EPS, NF3
+};
 enum PD {
   P_DTM, P_DT, P_CNPAR, P_MIN_DEPTH, P_CRIT_DEPTH, P_G, P_RHO_0, P_KAPPA, P_AVMMOL, P_AVMOLT, P_AVMOLS, P_T0, P_S0,
-  P_DTR0, P_DSR0, P_IP_FAC, P_TEMP_AH, P_SALT_AH, NPD
+  P_DTR0, P_DSR0, P_IP_FAC, P_TEMP_AH, P_SALT_AH, P_AVMBACK, P_AVHBACK, P_CP, P_SWR_BOT_REFL_FRAC,
+  P_SWR_MIN_BOT_FRAC, NPD
 };
 enum PI {
   I_M, I_MM, I_RUNTYPE, I_VEL2D_SPLIT, I_VEL2D_HOR, I_VEL3D_SPLIT, I_VEL3D_HOR, I_VEL3D_VER, I_TEMP_SPLIT, I_TEMP_HOR,
   I_TEMP_VER, I_SALT_SPLIT, I_SALT_HOR, I_SALT_VER, I_ADV_VER_ITERS, I_UFIRST2D, I_UFIRST3D, I_CALC_TEMP,
-  I_CALC_SALT, I_IP_METHOD, NPI
+  I_CALC_SALT, I_IP_METHOD, I_VISCOSITY, I_EQSTATE_METHOD, I_SEALEVEL_CHECK, I_RADIATION, I_NAN_WARNED, NPI
 };
+// I_VISCOSITY: 0 = CONSTANT_VISCOSITY (num, nuh as given), 1 = PARABOLIC_VISCOSITY (gotm.F90:131-143)
+// I_EQSTATE_METHOD: 1 linear, 2 UNESCO80, 3 Jackett et al. 2006 (eqstate.F90:94-261)
+// I_RADIATION: 0 = no short-wave radiation or surface heat flux in do_temperature, 1 = both
+// I_NAN_WARNED: the SAVEd have_warned of sealevel_nan_check (sealevel.F90:178)
 
 // Open boundaries (domain.F90:263-280, bdy_spec.F90:225-290): segments per side -- western
 // (wi, wfj..wlj), northern (nj, nfi..nli), eastern (ei, efj..elj), southern (sj, sfi..sli) -- with
@@ -436,6 +446,24 @@ inline void depth_update(const Dom& d, double** f2, const int32_t* azp, const in
     }
 }
 
+// sealevel.F90:172-314 (sealevel_nan_check with sealevel_nandum): the number of interior
+// elevations z that are not below HUGE(z) -- NaN, +Inf or the largest double -- and the last such
+// point in the reference's loop order (j outer, i inner). The reference checks every point of the
+// interior, land included.
+inline long sealevel_nan_count(const Dom& d, const double* zp, int* inan, int* jnan) {
+  A2 z{d, const_cast<double*>(zp)};
+  const double ahuge = std::numeric_limits<double>::max();
+  long num_nan = 0;
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i)
+      if (!(ahuge > z(i, j))) {
+        ++num_nan;
+        if (inan) *inan = i;
+        if (jnan) *jnan = j;
+      }
+  return num_nan;
+}
+
 // m2d.F90:412-490 integrate_2d (closed boundaries, no residual, no uv_diffusion).
 template <class R3>
 int integrate_2d(const Dom& d, const AdvMasks& m, BcState<R3>& st, int loop) {
@@ -465,6 +493,15 @@ int integrate_2d(const Dom& d, const AdvMasks& m, BcState<R3>& st, int loop) {
   }
   if (st.bdy && st.bdy->nseg() > 0) update_2d_bdy(d, *st.bdy, f2, par, loop);  // m2d.F90:475
   sealevel(d, f2, st.az, par);
+  // sealevel.F90:115-117: the NaN sweep every |sealevel_check| micro steps until the first
+  // finding (have_warned); sealevel_check > 0 turns a finding into an error (getm_error)
+  const int chk = ip[I_SEALEVEL_CHECK];
+  if (chk != 0 && loop % std::abs(chk) == 0 && !ip[I_NAN_WARNED]) {
+    if (sealevel_nan_count(d, f2[Z], nullptr, nullptr) > 0) {
+      ip[I_NAN_WARNED] = 1;
+      if (chk > 0) return -3;
+    }
+  }
   depth_update(d, f2, st.az, st.au, st.av, par);
   return 0;
 }
@@ -1109,23 +1146,165 @@ void stresses_3d(const Dom& d, BcState<R3>& st) {
     }
 }
 
-// eqstate.F90:127-137 (linear) and :252-261 (buoyancy)
+// eqstate.F90:496-534 (rho_from_theta_unesco80): UNESCO 1980 density at zero pressure. The
+// coefficients are default-kind (single precision) literals in the reference, widened to double.
+inline double rho_unesco80(double T, double S) {
+  auto f = [](float c) { return (double)c; };
+  const double T1 = T, T2 = T1 * T1, T3 = T1 * T2, T4 = T2 * T2, T5 = T1 * T4;
+  const double S1 = S, S2 = S1 * S1, S3 = S1 * S2;
+  double x = f(999.842594f) + f(6.793952e-02f) * T1 - f(9.09529e-03f) * T2 + f(1.001685e-04f) * T3;
+  x = x - f(1.120083e-06f) * T4 + f(6.536332e-09f) * T5;
+  x = x + S1 * (f(0.824493f) - f(4.0899e-03f) * T1 + f(7.6438e-05f) * T2 - f(8.2467e-07f) * T3);
+  x = x + S1 * f(5.3875e-09f) * T4;
+  x = x + std::sqrt(S3) * (-f(5.72466e-03f) + f(1.0227e-04f) * T1 - f(1.6546e-06f) * T2);
+  x = x + f(4.8314e-04f) * S2;
+  return x;
+}
+
+// eqstate.F90:540-590 (rho_from_theta at p = 0): the rational function of Jackett et al. (2006)
+// for the density at zero pressure (double-precision coefficients).
+inline double rho_jackett06(double s, double th) {
+  const double th2 = th * th, sqrts = std::sqrt(s);
+  const double anum = 9.9984085444849347e+02 +
+                      th * (7.3471625860981584e+00 + th * (-5.3211231792841769e-02 + th * 3.6492439109814549e-04)) +
+                      s * (2.5880571023991390e+00 - th * 6.7168282786692355e-03 + s * 1.9203202055760151e-03);
+  const double aden =
+      1.0000000000000000e+00 +
+      th * (7.2815210113327091e-03 +
+            th * (-4.4787265461983921e-05 + th * (3.3851002965802430e-07 + th * 1.3651202389758572e-10))) +
+      s * (1.7632126669040377e-03 - th * (8.8066583251206474e-06 + th2 * 1.8832689434804897e-10) +
+           sqrts * (5.7463776745432097e-06 + th2 * 1.4716275472242334e-09));
+  return anum / aden;
+}
+
+// eqstate.F90:94-261 do_eqstate: density by the configured method -- 1 linear (:127-137, every
+// point), 2 UNESCO80 (:148-156) or 3 Jackett et al. 2006 without pressure (:184-204), both on water
+// columns (az > 0) only -- and the buoyancy -g/rho_0*(rho-rho_0) everywhere (:252-261). The
+// thermal and haline coefficients alpha, beta that methods 2 and 3 also form (:158-176, :206-224)
+// feed only the buoyancy frequency of the turbulence closure and are not formed here.
 template <class R3>
 void do_eqstate(const Dom& d, BcState<R3>& st) {
   A3<R3> rho{d, st.f3[RHO]}, buoy{d, st.f3[BUOY]}, T{d, st.f3[TT]}, S{d, st.f3[SS]};
+  M2 az{d, st.az};
   const double* par = st.par;
+  const int method = st.ipar[I_EQSTATE_METHOD];
   const R3 rho_0 = R3(par[P_RHO_0]), dtr0 = R3(par[P_DTR0]), dsr0 = R3(par[P_DSR0]), T0 = R3(par[P_T0]),
            S0 = R3(par[P_S0]);
 #pragma omp parallel for schedule(static)
   for (int k = 1; k <= d.kmax; ++k)
     for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
-      for (int i = d.imin - HALO; i <= d.imax + HALO; ++i)
-        rho(i, j, k) = rho_0 + dtr0 * (T(i, j, k) - T0) + dsr0 * (S(i, j, k) - S0);
+      for (int i = d.imin - HALO; i <= d.imax + HALO; ++i) {
+        if (method == 2) {
+          if (az(i, j) > 0) rho(i, j, k) = R3(rho_unesco80((double)T(i, j, k), (double)S(i, j, k)));
+        } else if (method == 3) {
+          if (az(i, j) > 0) rho(i, j, k) = R3(rho_jackett06((double)S(i, j, k), (double)T(i, j, k)));
+        } else {
+          rho(i, j, k) = rho_0 + dtr0 * (T(i, j, k) - T0) + dsr0 * (S(i, j, k) - S0);
+        }
+      }
   const R3 x = R3(-par[P_G] / par[P_RHO_0]);
 #pragma omp parallel for schedule(static)
   for (int k = 1; k <= d.kmax; ++k)
     for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
       for (int i = d.imin - HALO; i <= d.imax + HALO; ++i) buoy(i, j, k) = x * (rho(i, j, k) - rho_0);
+}
+
+// gotm.F90:96-163 with PARABOLIC_VISCOSITY (:131-143): per water column of the interior the
+// prescribed profiles of turbulent kinetic energy, length scale, dissipation and eddy viscosity
+// from the bottom stress taub and the bottom roughness, on the interfaces k = 1..kmax-1; num and nuh
+// get the background values avmback / avhback added on every level (at k = 0 and kmax onto the
+// values they held, which the reference copies through its 1D column arrays). tke and eps (may be
+// null) receive the profiles. Single-precision literals as in the reference.
+template <class R3>
+void gotm_parabolic(const Dom& d, BcState<R3>& st) {
+  A2 D{d, st.f2[D_]}, taub{d, st.f2[TAUB]}, zub{d, st.f2[ZUB]}, zvb{d, st.f2[ZVB]};
+  A3<R3> hn{d, st.f3[HN]}, num{d, st.f3[NUM]}, nuh{d, st.f3[NUH]}, tke{d, st.f3[TKE]}, eps{d, st.f3[EPS]};
+  M2 az{d, st.az};
+  const int kmax = d.kmax;
+  const double avmback = st.par[P_AVMBACK], avhback = st.par[P_AVHBACK];
+  auto f = [](float c) { return (double)c; };
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i) {
+      if (az(i, j) < 1) continue;
+      const double z0b = 0.5 * (std::max(zub(i - 1, j), zub(i, j)) + std::max(zvb(i, j - 1), zvb(i, j)));
+      double zz = 0.0;
+      for (int k = 1; k <= kmax - 1; ++k) {
+        zz = zz + (double)hn(i, j, k);
+        const double t = std::max(f(1.e-10f), f(3.333333f) * taub(i, j) * (1.0 - zz / D(i, j)));
+        const double L = f(0.4f) * (zz + z0b) * std::sqrt(1.0 - zz / D(i, j));
+        const double e = f(0.16431677f) * std::sqrt(t * t * t) / L;
+        const double nu = f(0.09f) * t * t / e;
+        if (st.f3[TKE]) tke(i, j, k) = R3(t);
+        if (st.f3[EPS]) eps(i, j, k) = R3(e);
+        num(i, j, k) = R3(nu + avmback);
+        nuh(i, j, k) = R3(nu + avhback);
+      }
+      for (int k : {0, kmax}) {
+        if (kmax < 1) break;
+        num(i, j, k) = R3((double)num(i, j, k) + avmback);
+        nuh(i, j, k) = R3((double)nuh(i, j, k) + avhback);
+      }
+    }
+}
+
+// temperature.F90:452-465: the short-wave radiation profile rad of the water columns (az >= 1) of
+// the interior: swr at the surface, below it the two-band exponential decay A*exp(-z/g1) +
+// (1-A)*exp(-z/g2) with the depth z under the surface.
+template <class R3>
+void sw_radiation(const Dom& d, BcState<R3>& st) {
+  A2 swr{d, st.f2[SWR]}, A{d, st.f2[ATT_A]}, g1{d, st.f2[ATT_G1]}, g2{d, st.f2[ATT_G2]};
+  A3<R3> hn{d, st.f3[HN]}, rad{d, st.f3[RAD]};
+  M2 az{d, st.az};
+  const int kmax = d.kmax;
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i) {
+      if (az(i, j) < 1) continue;
+      const double swr_loc = swr(i, j);
+      rad(i, j, kmax) = R3(swr_loc);
+      double zz = 0.0;
+      for (int k = kmax - 1; k >= 0; --k) {
+        zz = zz + (double)hn(i, j, k + 1);
+        rad(i, j, k) = R3(swr_loc * (A(i, j) * std::exp(-zz / g1(i, j)) + (1 - A(i, j)) * std::exp(-zz / g2(i, j))));
+      }
+    }
+}
+
+// temperature.F90:469-525: the source terms that do_temperature adds to the right-hand side of
+// its diffusion matrix, per layer k = 1..kmax of the water columns (az == 1) of the interior:
+// dry_z*dt*(rad1d(k) - rad1d(k-1)), plus shf*rho_0_cpi in the top layer. rad1d is rad less the
+// bottom-reflected part (when swr_bot_refl_frac > 0 and enough light reaches the bottom) scaled by
+// 1/(rho_0*cp); a cooling surface flux is dropped where the top layer is at the freezing point
+// (T <= -0.0575*S, "the most primitive sea ice model"). S is the salinity before do_salinity.
+template <class R3>
+void temperature_source(const Dom& d, BcState<R3>& st, R3* srcp) {
+  A2 shf{d, st.f2[SHF]}, A{d, st.f2[ATT_A]}, g1{d, st.f2[ATT_G1]}, g2{d, st.f2[ATT_G2]}, dry_z{d, st.f2[DRY_Z]};
+  A3<R3> hn{d, st.f3[HN]}, rad{d, st.f3[RAD]}, T{d, st.f3[TT]}, S{d, st.f3[SS]}, src{d, srcp};
+  M2 az{d, st.az};
+  const int kmax = d.kmax;
+  const double dt = st.par[P_DT];
+  const double rho_0_cpi = 1.0 / (st.par[P_RHO_0] * st.par[P_CP]);
+  const double refl = st.par[P_SWR_BOT_REFL_FRAC], minfrac = st.par[P_SWR_MIN_BOT_FRAC];
+  std::vector<double> rad1d(kmax + 1);
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i) {
+      if (az(i, j) != 1) continue;
+      double shf_loc = shf(i, j);
+      if ((double)T(i, j, kmax) <= -((double)0.0575f * (double)S(i, j, kmax))) shf_loc = std::max(0.0, shf_loc);
+      for (int k = 0; k <= kmax; ++k) rad1d[k] = (double)rad(i, j, k);
+      if (refl > 0.0 && rad1d[0] / rad1d[kmax] > minfrac) {
+        const double swr_refl = rad1d[0] * refl;
+        rad1d[0] = rad1d[0] - swr_refl;
+        double zz = 0.0;
+        for (int k = 1; k <= kmax; ++k) {
+          zz = zz + (double)hn(i, j, k);
+          rad1d[k] = (double)rad(i, j, k) -
+                     swr_refl * (A(i, j) * std::exp(-zz / g1(i, j)) + (1 - A(i, j)) * std::exp(-zz / g2(i, j)));
+        }
+      }
+      for (int k = 0; k <= kmax; ++k) rad1d[k] = rad1d[k] * rho_0_cpi;
+      for (int k = 1; k <= kmax - 1; ++k) src(i, j, k) = R3(dry_z(i, j) * dt * (rad1d[k] - rad1d[k - 1]));
+      src(i, j, kmax) = R3(dry_z(i, j) * dt * (rad1d[kmax] + shf_loc * rho_0_cpi - rad1d[kmax - 1]));
+    }
 }
 
 // slow_bottom_friction.F90:53-170
@@ -1259,6 +1438,7 @@ int integrate_3d(const Dom& d, const AdvMasks& m, BcState<R3>& st, int n) {
     ww_momentum_3d(d, st);
     if (uv_advect_3d(d, m, st) != 0) return -1;
     stresses_3d(d, st);
+    if (ip[I_VISCOSITY] == 1) gotm_parabolic(d, st);  // m3d.F90:570-575
   }
   if (ip[I_RUNTYPE] == 4) {
     const R3 dt = R3(par[P_DT]);
@@ -1268,7 +1448,14 @@ int integrate_3d(const Dom& d, const AdvMasks& m, BcState<R3>& st, int n) {
                               st.f3[HO], st.f3[HN], ip[I_TEMP_SPLIT], ip[I_TEMP_HOR], ip[I_TEMP_VER],
                               R3(par[P_TEMP_AH]), H_TAG, nullptr, nullptr, ip[I_ADV_VER_ITERS]) < 0)
         return -1;
-      tracer_vdiff<R3>(d, dt, R3(par[P_CNPAR]), R3(par[P_AVMOLT]), st.f3[TT], st.f3[HN], st.f3[NUH], st.az, nullptr);
+      std::vector<R3> src;
+      if (ip[I_RADIATION]) {  // temperature.F90:452-525
+        sw_radiation(d, st);
+        src.assign(n3, R3(0));
+        if (d.kmax > 1) temperature_source(d, st, src.data());
+      }
+      tracer_vdiff<R3>(d, dt, R3(par[P_CNPAR]), R3(par[P_AVMOLT]), st.f3[TT], st.f3[HN], st.f3[NUH], st.az,
+                       src.empty() ? nullptr : src.data());
     }
     if (ip[I_CALC_SALT]) {
       AdvGrid g = adv_grid(m, H_TAG, st.az, st.au, st.av);

@@ -243,7 +243,7 @@ enum {
   BC_BOTTOM_FRICTION = 0, BC_UV_ADVECT_2D, BC_UMOMENTUM, BC_VMOMENTUM, BC_SEALEVEL, BC_DEPTH_UPDATE,
   BC_START_MACRO, BC_BOTTOM_FRICTION_3D, BC_IP, BC_UU_MOMENTUM_3D, BC_VV_MOMENTUM_3D, BC_SIGMA, BC_WW,
   BC_UV_ADVECT_3D, BC_STRESSES_3D, BC_EQSTATE, BC_SLOW_BOTTOM_FRICTION, BC_SLOW_TERMS, BC_INTEGRATE_2D,
-  BC_INTEGRATE_3D
+  BC_INTEGRATE_3D, BC_GOTM_PARABOLIC, BC_SW_RADIATION
 };
 
 extern "C++" {
@@ -282,6 +282,8 @@ static int bc_call(const or_dom* o, or_bc* s, int which, int arg) {
     case BC_SLOW_TERMS: gor::slow_terms(d, st); break;
     case BC_INTEGRATE_2D: rc = gor::integrate_2d(d, m, st, arg); break;
     case BC_INTEGRATE_3D: rc = gor::integrate_3d(d, m, st, arg); break;
+    case BC_GOTM_PARABOLIC: gor::gotm_parabolic(d, st); break;
+    case BC_SW_RADIATION: gor::sw_radiation(d, st); break;
     default: return -2;
   }
   for (int q = 0; q < gor::NPI; ++q) s->ipar[q] = st.ipar[q];
@@ -290,6 +292,13 @@ static int bc_call(const or_dom* o, or_bc* s, int which, int arg) {
 }  // extern "C++"
 
 int or_bc_call_d(const or_dom* o, or_bc* s, int which, int arg) { return bc_call<double>(o, s, which, arg); }
+
+// sealevel_nan_check (sealevel.F90:172-314): count and last point (reference indices) of the
+// interior elevations that are not below HUGE
+long long or_sealevel_nan_check(const or_dom* o, const double* z, int* inan, int* jnan) {
+  gor::Dom d = mk(o);
+  return gor::sealevel_nan_count(d, z, inan, jnan);
+}
 int or_bc_call_f(const or_dom* o, or_bc* s, int which, int arg) { return bc_call<float>(o, s, which, arg); }
 
 }  // extern "C"

@@ -22,6 +22,7 @@ the GPU machine. OpenMP directives are comments to the translator, so loops run 
 """
 from __future__ import annotations
 
+import math
 import os
 import re
 import subprocess
@@ -170,10 +171,37 @@ def _num(x):
     return x
 
 
+def _powi(a, n):
+    """x**n for a real x and a constant integer n as gfortran compiles it: multiplications
+    (GCC expands __builtin_powi with a constant exponent into a chain of products: x*x for 2,
+    (x*x)*x for 3, (x*x)*(x*x) for 4, square-and-multiply beyond), never a call of pow()."""
+    if n < 0:
+        return np.float64(1.0) / _powi(a, -n)
+    if n == 0:
+        return np.float64(1.0)
+    if n == 1:
+        return a
+    if n == 2:
+        return a * a
+    if n == 3:
+        return (a * a) * a
+    half = _powi(a, n // 2)
+    return half * half if n % 2 == 0 else (half * half) * a
+
+
 def _pow(a, b):
     if isinstance(a, (int, np.integer)) and isinstance(b, (int, np.integer)) and b >= 0:
         return int(a) ** int(b)
     with np.errstate(all="ignore"):
+        if isinstance(b, (int, np.integer)) and not isinstance(b, bool):
+            if isinstance(a, np.ndarray):
+                return np.frompyfunc(lambda v: _powi(np.float64(v), int(b)), 1, 1)(a).astype(np.float64)
+            return _powi(np.float64(a), int(b))
+        if np.ndim(a) == 0 and np.ndim(b) == 0:
+            try:
+                return np.float64(math.pow(float(a), float(b)))  # the C library's pow, as gfortran calls it
+            except (ValueError, OverflowError):
+                pass
         return np.float64(a) ** b
 
 
@@ -311,8 +339,26 @@ def _sign(a, b):
     return abs(a) if b >= 0 else -abs(a)
 
 
+def _libm(fn, x):
+    """An elemental math function evaluated by the C library (math.exp / math.log call the
+    platform libm, as gfortran's compiled code does; numpy's own vectorised exp and log can differ
+    from it in the last bit)."""
+    x = _arr(x)
+    if np.ndim(x) == 0:
+        try:
+            return np.float64(fn(float(x)))
+        except (ValueError, OverflowError):
+            with np.errstate(all="ignore"):
+                return np.float64(np.exp(x) if fn is math.exp else np.log(x))
+    return np.frompyfunc(lambda v: _libm(fn, v), 1, 1)(x).astype(np.float64)
+
+
 def _exp(x):
-    return np.exp(_arr(x))
+    return _libm(math.exp, x)
+
+
+def _log(x):
+    return _libm(math.log, x)
 
 
 def _sqrt(x):
@@ -321,6 +367,12 @@ def _sqrt(x):
 
 def _present(x):
     return x is not None
+
+
+class _Out(dict):
+    """Final values of a subroutine's scalar dummy arguments, by position: the caller copies them
+    back into actual arguments that are variables or array elements (Fortran passes by reference;
+    the translated Python passes scalars by value)."""
 
 
 class Counter:
@@ -339,7 +391,7 @@ INTRINSICS = {
     "abs": "_abs", "min": "_fmin", "max": "_fmax", "ceiling": "_ceiling", "floor": "_floor", "maxval": "_maxval",
     "minval": "_minval", "sum": "_sum", "real": "_real", "dble": "_real", "int": "_int", "mod": "_mod",
     "sign": "_sign", "exp": "_exp", "sqrt": "_sqrt", "present": "_present", "tanh": "np.tanh", "sin": "np.sin",
-    "cos": "np.cos", "log": "np.log", "selected_real_kind": "_srk", "allocated": "_allocated", "float": "_real",
+    "cos": "np.cos", "log": "_log", "selected_real_kind": "_srk", "allocated": "_allocated", "float": "_real",
     "huge": "_huge",
 }
 
@@ -539,8 +591,12 @@ class ExprParser:
             ml, mr = _SINGLE_LIT.fullmatch(left), _SINGLE_LIT.fullmatch(rhs)
             if ml and mr and val in ("+", "-", "*", "/"):
                 a, b = np.float32(float(ml.group(1))), np.float32(float(mr.group(1)))
-                r = {"+": a + b, "-": a - b, "*": a * b, "/": a / b}[val]
-                left = f"np.float64(np.float32({float(r)!r}))"
+                with np.errstate(all="ignore"):
+                    r = {"+": a + b, "-": a - b, "*": a * b, "/": a / b}[val]
+                if np.isfinite(r):
+                    left = f"np.float64(np.float32({float(r)!r}))"
+                else:  # e.g. 0.0/0.0, the reference's way of making a NaN
+                    left = f"np.float64(np.float32(float({str(float(r))!r})))"
                 continue
             left = f"{helper}({left}, {rhs})"
         return left
@@ -799,7 +855,7 @@ def parse_units(text: str):
             elif not in_body and (low.startswith("implicit") or low.startswith("private") or low.startswith("public")):
                 pass
             elif not in_body and TYPE_RE.match(low) and not re.match(r"^(real|integer|logical)\s*\w*\s*function", low) \
-                    and ("::" in low or re.match(r"^(real|integer|logical)(\([^)]*\))?\s+[a-z]", low)):
+                    and ("::" in low or re.match(r"^(real|integer|logical)(\((?:[^()]|\([^()]*\))*\)\s*|\s+)[a-z]", low)):
                 for d in parse_decl(s):
                     u.decls[d.name] = d
             else:
@@ -861,7 +917,9 @@ def _parse_use(low: str):
     mod = m.group(1)
     only = None
     if m.group(3) is not None:
-        only = [x.strip() for x in m.group(3).split(",") if x.strip()]
+        # a renamed entity (local => remote) is listed under its local name: the module
+        # namespaces this translator is given for such modules hold the local names
+        only = [x.split("=>")[0].strip() for x in m.group(3).split(",") if x.strip()]
     return mod, only
 
 
@@ -915,10 +973,18 @@ class Gen:
             args.append(f"{pyname(a)}=None" if opt else pyname(a))
         # Python requires non-defaults first: all optionals in the reference come last
         self.lines.append(f"def {u.name}({', '.join(args)}):")
-        self.assigned_globals = sorted(self._assigned_names() & self.modvars)
+        assigned = self._assigned_names()
+        self.assigned_globals = sorted(assigned & self.modvars)
         if self.assigned_globals:
             self.emit(f"global {', '.join(pyname(n) for n in self.assigned_globals)}")
         self.emit("_result = None")
+        # a subroutine hands the final values of the scalar dummies it assigns back to its caller
+        outs = [(q, a) for q, a in enumerate(u.args)
+                if u.kind != "function" and a in assigned and not (u.decls.get(a) is not None and u.decls[a].is_array)]
+        self.ret = "_result"
+        if outs:
+            self.emit("_ret = lambda: _Out({" + ", ".join(f"{q}: {pyname(a)}" for q, a in outs) + "})")
+            self.ret = "_ret()"
         # parameters and locals (in declaration order, so that bounds can use earlier ones)
         for name, d in u.decls.items():
             if name == u.result and u.kind == "function":
@@ -958,7 +1024,7 @@ class Gen:
             self.ind += 1
         for s in u.body:
             self.stmt(s)
-        self.emit("return _result")
+        self.emit(f"return {self.ret}")
         if self.saved:
             self.ind -= 1
             self.emit("finally:")
@@ -1041,7 +1107,7 @@ class Gen:
             self.sel -= 1
             return
         if low == "return":
-            self.emit("return _result")
+            self.emit(f"return {self.ret}")
             return
         if low == "cycle":
             self.emit("continue")
@@ -1059,7 +1125,35 @@ class Gen:
         if m:
             name = m.group(1)
             args = tr_args(m.group(3), sc) if m.group(3) else ""
-            self.emit(f"{name}({args})")
+            # actual arguments that a scalar out-argument can be copied back into: plain local or
+            # module-assigned variables and array elements, by position (keyword arguments excluded)
+            back = []
+            if m.group(3):
+                for q, a in enumerate(_split_top(m.group(3), ",")):
+                    a = a.strip()
+                    if _top_assign(a) is not None:
+                        break
+                    d = self.u.decls.get(a)
+                    if d is not None and "parameter" in d.attrs:
+                        continue
+                    if re.match(r"^[a-z_]\w*$", a) and a not in self.u.args and (a not in self.modvars or
+                                                                                 a in self.assigned_globals):
+                        if d is None or not d.is_array:
+                            back.append((q, pyname(a)))
+                    elif re.match(r"^\w+\s*\(.*\)$", a) and a[:a.index("(")].strip() in self.scope.arrays:
+                        back.append((q, tr_expr(a, sc)))
+                    elif re.match(r"^[a-z_]\w*$", a) and a in self.u.args:
+                        if d is not None and not d.is_array:
+                            back.append((q, pyname(a)))
+            if back:
+                self.emit(f"_r = {name}({args})")
+                self.emit("if isinstance(_r, _Out):")
+                self.ind += 1
+                for q, tgt in back:
+                    self.emit(f"if {q} in _r: {tgt} = _r[{q}]")
+                self.ind -= 1
+            else:
+                self.emit(f"{name}({args})")
             return
         m = re.match(r"^allocate\s*\((.*)\)$", low)
         if m:

@@ -51,7 +51,8 @@ class RefBc:
     def __init__(self, c: S.BcCase):
         self.c = c
         g = self.g = c.grid
-        P = self.P = fs.Program()
+        # PARABOLIC_VISCOSITY is a compile-time option of the reference (gotm.F90:131, m3d.F90:571)
+        P = self.P = fs.Program(defines=("PARABOLIC_VISCOSITY",) if c.pi.get("viscosity", 0) == 1 else ())
         F2, F3 = self.F2, self.F3
         f2 = {k.lower(): F2(v) for k, v in c.f2.items()}
         f3 = {k.lower(): F3(v) for k, v in c.f3.items()}
@@ -59,7 +60,7 @@ class RefBc:
         zero2 = lambda: F2(np.zeros(g.shape2()))  # noqa: E731
         zero3 = lambda: F3(np.zeros(g.shape3()))  # noqa: E731
         pd, pi = c.pd, c.pi
-        P.add_module_namespace("parameters", g=pd["g"], rho_0=pd["rho_0"], cp=fs._real_literal and np.float64(np.float32(3985.)),
+        P.add_module_namespace("parameters", g=pd["g"], rho_0=pd["rho_0"], cp=np.float64(pd["cp"]),
                                kappa=pd["kappa"], avmmol=pd["avmmol"], avmolt=pd["avmolt"], avmols=pd["avmols"])
         P.add_module_namespace(
             "domain", imin=g.imin, imax=g.imax, jmin=g.jmin, jmax=g.jmax, kmax=g.kmax, ioff=0, joff=0, dx=g.dx,
@@ -83,10 +84,11 @@ class RefBc:
         ones2 = F2(np.ones(g.shape2()))
         v3.update(dt=np.float64(pd["dt"]), cnpar=np.float64(pd["cnpar"]), kmin=F2(np.ones(g.shape2())),
                   kumin=F2(np.ones(g.shape2())), kvmin=F2(np.ones(g.shape2())), ss=zero3(), nn=zero3(), zc=zero3(),
-                  rad=zero3(), a=ones2, g1=ones2, g2=ones2, alpha=zero3(), beta=zero3(), rk=None,
+                  rad=f3["rad"], a=f2["a"], g1=f2["g1"], g2=f2["g2"], alpha=zero3(), beta=zero3(), rk=None,
+                  avmback=np.float64(pd["avmback"]), avhback=np.float64(pd["avhback"]),
                   do_numerical_analyses=False, nummix3d_s=None, nummix2d_s=None, phymix3d_s=None,
                   phymix2d_s=None, nummix3d_t=None, nummix2d_t=None, phymix3d_t=None, phymix2d_t=None,
-                  numdis3d=None, numdis2d=None, light=None, tke=zero3(), eps=zero3())
+                  numdis3d=None, numdis2d=None, light=None, tke=f3["tke"], eps=f3["eps"])
         # kumin_pmz / kvmin_pmz (ip_blumberg_mellor_lin.F90:114,145): 1, the only value the reference
         # assigns them (adaptive_coordinates.F90:237-238)
         v3.update(kumin_pmz=F2(np.ones(g.shape2())), kvmin_pmz=F2(np.ones(g.shape2())))
@@ -96,8 +98,13 @@ class RefBc:
             v.update(imin=g.imin, imax=g.imax, jmin=g.jmin, jmax=g.jmax, kmax=g.kmax)
         P.add_module_namespace("variables_2d", **v2)
         P.add_module_namespace("variables_3d", **v3)
-        P.add_module_namespace("meteo", tausx=f2["tausx"], tausy=f2["tausy"], airp=f2["airp"], swr=zero2(),
-                               shf=zero2(), albedo=zero2())
+        P.add_module_namespace("meteo", tausx=f2["tausx"], tausy=f2["tausy"], airp=f2["airp"], swr=f2["swr"],
+                               shf=f2["shf"], albedo=zero2())
+        # GOTM's turbulence module (un-vendored): gotm.F90's 1D column arrays under the local names
+        # of its use-renames; PARABOLIC_VISCOSITY fills them itself and never calls do_turbulence
+        col = lambda: fs.FArr(np.zeros(g.kmax + 1), [0])  # noqa: E731
+        P.add_module_namespace("turbulence", tke1d=col(), eps1d=col(), l1d=col(), num1d=col(), nuh1d=col(),
+                               cde=np.float64(0.5477), do_turbulence=self._no_turbulence)
         P.add_module_namespace("halo_zones", h_tag=10, hu_tag=11, hv_tag=12, d_tag=20, du_tag=21, dv_tag=22,
                                z_tag=30, u_tag=31, v_tag=32, update_2d_halo=lambda *a, **k: None,
                                update_3d_halo=lambda *a, **k: None, wait_halo=lambda *a, **k: None)
@@ -105,7 +112,7 @@ class RefBc:
             "adv advh adv3d adv3dh salt temp mixanalysis bottfrict integr2d uvadv uvadvh uvdiff momentum momentumh "
             "sealevel sealevelh dpthupdate startmcr stopmcr bottfrict3d intpress uumomentum uumomentumh vvmomentum "
             "vvmomentumh coords wwmomentum wwmomentumh uvadv3d uvadv3dh uvdiff3d stresses3d stresses3dh tempH saltH "
-            "eqstate slowbfrict slowterms integr3d check3df temph salth".split())}
+            "eqstate slowbfrict slowterms integr3d check3df temph salth gotm gotmturb gotmh".split())}
         P.add_module_namespace("getm_timers", tic=lambda *a: None, toc=lambda *a: None, **timers)
         P.add_module_namespace("bdy_3d", do_bdy_3d=lambda *a, **k: None, init_bdy_3d=lambda *a, **k: None,
                                bdy3d_tmrlx=False, bdy3d_tmrlx_ucut=0.0, bdy3d_tmrlx_max=0.0, bdy3d_tmrlx_min=0.0)
@@ -113,8 +120,13 @@ class RefBc:
         P.add_module_namespace("time", julianday=0, secondsofday=0, month=1, yearday=1)
         for f in FILES:
             P.load(f)
-        # prescribed viscosity: the turbulence interface and its shear/stratification inputs are inert
-        P.procs["gotm"] = lambda *a, **k: None
+        # prescribed viscosity (CONSTANT_VISCOSITY): the turbulence interface is inert; with
+        # PARABOLIC_VISCOSITY gotm.F90 runs its own profile. The shear/stratification inputs of the
+        # closure (ss_nn) are never read by either
+        if c.pi.get("viscosity", 0) == 1:
+            P.load("src/3d/gotm.F90")
+        else:
+            P.procs["gotm"] = lambda *a, **k: None
         P.procs["ss_nn"] = lambda *a, **k: None
         P.procs["tke_eps_advect_3d"] = lambda *a, **k: None
         P.procs["do_residual"] = lambda *a, **k: None
@@ -125,7 +137,8 @@ class RefBc:
         m2.dtm = np.float64(pd["dtm"])
         m2.mm = pi["MM"]
         m2.vel2d_adv_split, m2.vel2d_adv_hor = pi["vel2d_adv_split"], pi["vel2d_adv_hor"]
-        m2.am, m2.an_method, m2.residual, m2.sealevel_check, m2.bdy2d_ramp = np.float64(-1.0), 0, -1, 0, -1
+        m2.am, m2.an_method, m2.residual, m2.sealevel_check, m2.bdy2d_ramp = (np.float64(-1.0), 0, -1,
+                                                                              int(pi.get("sealevel_check", 0)), -1)
         if c.bdy is not None:
             b, n = c.bdy, c.bdy.npoints()
             m2.bdy2d_ramp = b.ramp
@@ -144,12 +157,14 @@ class RefBc:
         tm.temp_adv_split, tm.temp_adv_hor, tm.temp_adv_ver = (pi["temp_adv_split"], pi["temp_adv_hor"],
                                                                pi["temp_adv_ver"])
         tm.temp_ah, tm.temp_check, tm.ncid = np.float64(pd["temp_AH"]), 0, -1
+        tm.swr_bot_refl_frac = np.float64(pd["swr_bot_refl_frac"])
+        tm.swr_min_bot_frac = np.float64(pd["swr_min_bot_frac"])
         sm = P.modules["salinity"]
         sm.salt_adv_split, sm.salt_adv_hor, sm.salt_adv_ver = (pi["salt_adv_split"], pi["salt_adv_hor"],
                                                                pi["salt_adv_ver"])
         sm.salt_ah, sm.salt_check = np.float64(pd["salt_AH"]), 0
         eq = P.modules["eqstate"]
-        eq.eqstate_method = 1
+        eq.eqstate_method = int(pi.get("eqstate_method", 1))
         eq.t0, eq.s0, eq.dtr0, eq.dsr0 = (np.float64(pd["T0"]), np.float64(pd["S0"]), np.float64(pd["dtr0"]),
                                           np.float64(pd["dsr0"]))
         ipm = P.modules["internal_pressure"]
@@ -180,6 +195,10 @@ class RefBc:
         out["bdy_index"] = fs.FArr(np.array(index, np.int64), [1])
         out["bdy_2d_type"] = fs.FArr(np.array(types, np.int64), [1])
         return out
+
+    @staticmethod
+    def _no_turbulence(*a, **k):
+        raise fs.FortranStop("do_turbulence: the GOTM closure is not part of this configuration")
 
     def _error(self, where, msg):
         raise fs.FortranStop(f"{where}: {msg}")
@@ -249,6 +268,37 @@ def ip_case(method):
     return c
 
 
+def phys_case(eqstate_method, parabolic, reflection, seed=8):
+    """12 x 10 x 5 islands basin (30% land) with the options of do_temperature, gotm and do_eqstate
+    that the configurations leave off: short-wave radiation (swr 50-350 W/m2 and Jerlov type I
+    attenuation A = 0.58, g1 = 0.35 m, g2 = 23 m, perturbed per column) and a surface heat flux of
+    either sign, with the top layer of a few columns below the freezing point (the sea-ice clamp of
+    the heat flux); optionally bottom reflection of the light (swr_bot_refl_frac = 0.2); the
+    nonlinear equation of state (2: UNESCO80, 3: Jackett et al. 2006); optionally the
+    PARABOLIC_VISCOSITY profile with background viscosity and diffusivity; the NaN sweep of the
+    elevations every second micro step (warnings only)."""
+    c = S.baroclinic_case(nx=12, ny=10, kmax=5, recipe="islands", land=0.3, M=4, dt3=60.0, seed=seed)
+    rng = np.random.default_rng(seed + 100)
+    g = c.grid
+    wet = c.az >= 1
+    c.pi.update(radiation=1, eqstate_method=eqstate_method, viscosity=1 if parabolic else 0, sealevel_check=-2)
+    c.f2["swr"][...] = np.where(wet, rng.uniform(50.0, 350.0, g.shape2()), 0.0)
+    c.f2["shf"][...] = np.where(wet, rng.uniform(-150.0, 100.0, g.shape2()), 0.0)
+    c.f2["A"][...] = S.F32(0.58) + 0.02 * rng.uniform(-1, 1, g.shape2())
+    c.f2["g1"][...] = S.F32(0.35) + 0.05 * rng.uniform(-1, 1, g.shape2())
+    c.f2["g2"][...] = S.F32(23.0) + 2.0 * rng.uniform(-1, 1, g.shape2())
+    T = c.f3["T"]
+    cold = wet & (rng.uniform(size=g.shape2()) < 0.25)
+    T[g.kmax][cold] = -2.5  # below -0.0575*S for S >= 30
+    if reflection:
+        c.pd["swr_bot_refl_frac"] = 0.2
+    if parabolic:
+        c.pd.update(avmback=1e-5, avhback=2e-6)
+        c.f2["taub"][...] = np.where(wet, rng.uniform(0.0, 2e-4, g.shape2()), 0.0)
+    S._eqstate(c)  # initial density and buoyancy of the modified temperature (linear)
+    return c
+
+
 def write(c, name):
     out = {"meta": np.array([c.grid.nx, c.grid.ny, c.grid.kmax, c.grid.dx, c.grid.dy])}
     r = RefBc(c)
@@ -261,6 +311,8 @@ def write(c, name):
         out["in_" + k] = v
     out["in_pd"] = np.array([c.pd[n] for n in S.PD_NAMES])
     out["in_pi"] = np.array([c.pi[n] for n in S.PI_NAMES])
+    out["names_pd"] = np.array(S.PD_NAMES)
+    out["names_pi"] = np.array(S.PI_NAMES)
     if c.bdy is not None:
         b = c.bdy
         out["bdy_counts"] = np.array([len(x) for x in b.sides])
@@ -277,8 +329,66 @@ def write(c, name):
     print(f"wrote {path} ({os.path.getsize(path) / 1024:.0f} KiB)")
 
 
+def nan_check_fixture():
+    """tests/golden/reference_sealevel_nan.npz: the reference's sealevel_nan_check
+    (sealevel.F90:172-314) on elevation fields holding NaN, +-Inf, HUGE, subnormal and ordinary
+    values, in the interior and in the halo, with land points among them. For each field: the number
+    of interior points that sealevel_nandum classifies as not below HUGE (recorded from the
+    reference's own per-point calls), the last such point in loop order, and whether sealevel(loop)
+    stops (getm_error) with sealevel_check = 1 and with sealevel_check = -1."""
+    c = S.baroclinic_case(nx=9, ny=7, kmax=3, recipe="islands", land=0.3, M=4, dt3=60.0, seed=5)
+    g = c.grid
+    rng = np.random.default_rng(21)
+    fields = []
+    z0 = c.f2["z"].copy()
+    fields.append(z0.copy())  # clean
+    z = z0.copy()
+    pts = [(g.jmin + 1, g.imin + 2, np.nan), (g.jmin + 3, g.imin, np.inf), (g.jmax, g.imax, np.finfo(np.float64).max),
+           (g.jmin, g.imax - 1, -np.inf), (g.jmin + 2, g.imin + 4, 5e-324), (g.jmin - 1, g.imin + 1, np.nan)]
+    for (j, i, v) in pts:
+        z[j - (g.jmin - 2), i - (g.imin - 2)] = v
+    fields.append(z)
+    z = z0.copy()
+    z[rng.uniform(size=z.shape) < 0.2] = np.nan  # random NaNs, halo included
+    fields.append(z)
+    out = {"meta": np.array([g.nx, g.ny, g.kmax, g.dx, g.dy]), "in_az": c.az}
+    for q, zf in enumerate(fields):
+        res = {}
+        for chk in (1, -1):
+            cc = c.copy()
+            cc.f2["z"][...] = zf
+            cc.pi["sealevel_check"] = chk
+            r = RefBc(cc)
+            calls = []
+            orig = r.P.procs["sealevel_nandum"]
+
+            def spy(a, b, idum, _orig=orig, _calls=calls):
+                ret = _orig(a, b, idum)
+                _calls.append(int(ret[2]) if ret else 2)
+                return ret
+
+            r.P.procs["sealevel_nandum"] = spy
+            r.P.modules["m2d"].dtm = np.float64(0.0)  # the sweep sees the field as given
+            stopped = False
+            try:
+                r.P.procs["sealevel"](1)
+            except fs.FortranStop:
+                stopped = True
+            res[chk] = (stopped, calls[2:])  # the first two calls are the compiler self-test
+        flags = np.array(res[1][1])
+        out[f"z{q}"] = zf
+        out[f"count{q}"] = np.array(int((flags == 2).sum()))
+        ii, jj = np.meshgrid(np.arange(g.imin, g.imax + 1), np.arange(g.jmin, g.jmax + 1))
+        hit = np.flatnonzero(flags == 2)
+        out[f"last{q}"] = np.array([ii.ravel()[hit[-1]], jj.ravel()[hit[-1]]] if hit.size else [0, 0])
+        out[f"stops{q}"] = np.array([res[1][0], res[-1][0]])
+    path = os.path.join(HERE, "reference_sealevel_nan.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path}")
+
+
 def main():
-    which = sys.argv[1:] or ["closed", "bdy", "ip2", "ip4", "ip5", "ip6"]
+    which = sys.argv[1:] or ["closed", "bdy", "ip2", "ip4", "ip5", "ip6", "phys3", "phys2", "nan"]
     if "closed" in which:
         write(S.baroclinic_case(nx=12, ny=10, kmax=4, recipe="shelf", M=4, dt3=60.0, seed=3),
               "reference_mode_split.npz")
@@ -287,6 +397,12 @@ def main():
     for m in (2, 4, 5, 6):
         if f"ip{m}" in which:
             write(ip_case(m), f"reference_mode_split_ip{m}.npz")
+    if "phys3" in which:  # Jackett 2006, PARABOLIC_VISCOSITY, radiation with bottom reflection
+        write(phys_case(3, parabolic=True, reflection=True), "reference_mode_split_phys3.npz")
+    if "nan" in which:
+        nan_check_fixture()
+    if "phys2" in which:  # UNESCO80, prescribed viscosity, radiation without reflection
+        write(phys_case(2, parabolic=False, reflection=False, seed=9), "reference_mode_split_phys2.npz")
 
 
 if __name__ == "__main__":

@@ -19,19 +19,28 @@ GOLD_BDY = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "r
 GOLD_IP = {m: os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", f"reference_mode_split_ip{m}.npz")
            for m in (2, 4, 5, 6)}
 GOLD_IP2 = GOLD_IP[2]
+GOLD_PHYS = {m: os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", f"reference_mode_split_phys{m}.npz")
+             for m in (2, 3)}
 
 
 def load_case(gold, dtype3=np.float64):
     nx, ny, kmax, dx, dy = gold["meta"]
     c = S.BcCase(Grid(int(nx), int(ny), int(kmax), dx, dy), dtype3)
+    # fields and parameters added to the state after a fixture was written keep the case's zeros /
+    # the reference's defaults (the options they belong to are off in such a fixture)
     for k in S.F2_NAMES:
-        c.f2[k] = gold["in_f2_" + k].copy()
+        if "in_f2_" + k in gold:
+            c.f2[k] = gold["in_f2_" + k].copy()
     for k in S.F3_NAMES:
-        c.f3[k] = gold["in_f3_" + k].astype(dtype3)
+        if "in_f3_" + k in gold:
+            c.f3[k] = gold["in_f3_" + k].astype(dtype3)
     c.az, c.au, c.av, c.ax = (gold["in_" + k].copy() for k in ("az", "au", "av", "ax"))
-    c.pd = dict(zip(S.PD_NAMES, (float(x) for x in gold["in_pd"])))
-    c.pi = dict(zip(S.PI_NAMES, (int(x) for x in gold["in_pi"])))
-    c.pi.setdefault("ip_method", 1)  # fixtures written before the parameter existed
+    names_pd = [str(x) for x in gold["names_pd"]] if "names_pd" in gold else S.PD_NAMES
+    names_pi = [str(x) for x in gold["names_pi"]] if "names_pi" in gold else S.PI_NAMES
+    c.pd = dict(S.PARAM_DEFAULTS_PD)
+    c.pd.update(zip(names_pd, (float(x) for x in gold["in_pd"])))
+    c.pi = dict(S.PARAM_DEFAULTS_PI)
+    c.pi.update(zip(names_pi, (int(x) for x in gold["in_pi"])))
     if "bdy_counts" in gold:
         sides, q = [], 0
         for n in gold["bdy_counts"]:
@@ -43,7 +52,16 @@ def load_case(gold, dtype3=np.float64):
     return c
 
 
-GOLDS = {"closed": GOLD, "open boundaries": GOLD_BDY, **{f"ip_method {m}": GOLD_IP[m] for m in (2, 4, 5, 6)}}
+def gold_names(gold, kind):
+    """The fields of the state table that a fixture holds outputs of (fixtures written before a
+    field was added to the table do not have it)."""
+    names = S.F2_NAMES if kind == "f2" else S.F3_NAMES
+    return [k for k in names if f"out_{kind}_{k}" in gold]
+
+
+GOLDS = {"closed": GOLD, "open boundaries": GOLD_BDY, **{f"ip_method {m}": GOLD_IP[m] for m in (2, 4, 5, 6)},
+         "radiation, UNESCO80": GOLD_PHYS[2], "radiation + bottom reflection, Jackett 2006, parabolic viscosity":
+         GOLD_PHYS[3]}
 
 
 @pytest.fixture(scope="module", params=list(GOLDS))
@@ -56,10 +74,10 @@ def test_time_loop_matches_reference(gold):
     c = load_case(gold)
     oracle.bc_steps(c, 1, 8)
     bad = []
-    for k in S.F2_NAMES:
+    for k in gold_names(gold, "f2"):
         if not np.array_equal(c.f2[k], gold["out_f2_" + k], equal_nan=True):
             bad.append((k, float(np.nanmax(np.abs(c.f2[k] - gold["out_f2_" + k])))))
-    for k in S.F3_NAMES:
+    for k in gold_names(gold, "f3"):
         if not np.array_equal(c.f3[k], gold["out_f3_" + k], equal_nan=True):
             bad.append((k, float(np.nanmax(np.abs(c.f3[k] - gold["out_f3_" + k])))))
     assert not bad, bad
@@ -76,3 +94,43 @@ def test_ip_method_fixture_differs_from_method_1(method):
     oracle.bc_steps(c, 1, 8)
     assert not np.array_equal(c.f3["idpdx"], gold["out_f3_idpdx"])
     assert not np.array_equal(c.f3["idpdy"], gold["out_f3_idpdy"])
+
+
+GOLD_NAN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_sealevel_nan.npz")
+
+
+def test_sealevel_nan_check_matches_reference():
+    """sealevel_nan_check (sealevel.F90:172-314) in the oracle against the reference's own per-point
+    classification (tests/golden/reference_sealevel_nan.npz): the number of interior elevations not
+    below HUGE (NaN, +Inf, HUGE; not -Inf, subnormals or halo points) and the last of them in loop
+    order."""
+    g = dict(np.load(GOLD_NAN))
+    nx, ny, kmax, dx, dy = g["meta"]
+    grid = Grid(int(nx), int(ny), int(kmax), dx, dy)
+    for q in range(3):
+        n, last = oracle.sealevel_nan_check(grid, g[f"z{q}"])
+        assert n == int(g[f"count{q}"]), q
+        if n:
+            assert last == tuple(int(x) for x in g[f"last{q}"]), q
+
+
+def test_sealevel_check_stops_like_reference():
+    """sealevel_check > 0 turns a NaN finding into an error, < 0 into a warning that also ends the
+    checks (have_warned), as the reference's sealevel does on the same fields."""
+    g = dict(np.load(GOLD_NAN))
+    nx, ny, kmax, dx, dy = g["meta"]
+    for q in range(3):
+        for col, chk in ((0, 1), (1, -1)):
+            c = S.baroclinic_case(nx=int(nx), ny=int(ny), kmax=int(kmax), recipe="islands", land=0.3, M=4, dt3=60.0,
+                                  seed=5)
+            c.f2["z"][...] = g[f"z{q}"]
+            c.pd["dtm"] = 0.0
+            c.pi["sealevel_check"] = chk
+            stops = bool(g[f"stops{q}"][col])
+            try:
+                oracle.bc_call(c, "integrate_2d", 1)
+                stopped = False
+            except ValueError:
+                stopped = True
+            assert stopped == stops, (q, chk)
+            assert c.pi["nan_warned"] == (1 if int(g[f"count{q}"]) > 0 else 0), (q, chk)
