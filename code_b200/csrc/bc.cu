@@ -533,6 +533,25 @@ __global__ void k_mirror(T* f, const long long* __restrict__ pairs, int n, int n
   for (int k = 0; k < nl; ++k) f[dst + k * sk] = f[src + k * sk];
 }
 
+// sealevel.F90:172-314 (sealevel_nan_check): counts the interior elevations that are not below
+// HUGE (NaN, +Inf, the largest double) into cnt[0] and keeps in cnt[1] one more than the largest
+// loop-order index (j outer, i inner) of such a point, i.e. the last one the reference reports.
+// With `latched`, cnt[2] != 0 (a finding of an earlier sweep: the reference's have_warned) skips the
+// sweep.
+__global__ void k_nan_sweep(Dev d, const double* __restrict__ z, unsigned long long* cnt, bool latched) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + d.imin;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + d.jmin;
+  if (i > d.imax || j > d.jmax) return;
+  if (latched && cnt[2] != 0) return;
+  const double v = z[d.ix(i, j)];
+  if (!(1.7976931348623157e308 > v)) {
+    atomicAdd(&cnt[0], 1ull);
+    const unsigned long long idx =
+        (unsigned long long)(j - d.jmin) * (unsigned long long)(d.imax - d.imin + 1) + (unsigned long long)(i - d.imin);
+    atomicMax(&cnt[1], idx + 1);
+  }
+}
+
 // stop_macro.F90:36-39
 __global__ void k_stop_macro(Dev d, Bc2 s) {
   GB_IJ2
@@ -541,6 +560,31 @@ __global__ void k_stop_macro(Dev d, Bc2 s) {
   Uint(i, j) = 0.0;
   Vinto(i, j) = Vint(i, j);
   Vint(i, j) = 0.0;
+}
+
+}  // namespace gb
+
+namespace gb {
+
+// after a sweep: a finding ends the sweeps (the reference's have_warned)
+__global__ void k_nan_latch(unsigned long long* cnt) {
+  if (cnt[0] != 0) cnt[2] = 1;
+}
+
+// one sweep into cnt[0..1] that neither reads nor sets a latch (getm_sealevel_nan_check)
+int run_nan_sweep_once(const Dev& d, cudaStream_t s, const double* z, unsigned long long* cnt) {
+  const dim3 blk(32, 4, 1);
+  const dim3 g((d.imax - d.imin + 1 + 31) / 32, (d.jmax - d.jmin + 1 + 3) / 4, 1);
+  k_nan_sweep<<<g, blk, 0, s>>>(d, z, cnt, false);
+  return (int)cudaGetLastError();
+}
+
+int run_nan_sweep(const Dev& d, cudaStream_t s, const double* z, unsigned long long* cnt) {
+  const dim3 blk(32, 4, 1);
+  const dim3 g((d.imax - d.imin + 1 + 31) / 32, (d.jmax - d.jmin + 1 + 3) / 4, 1);
+  k_nan_sweep<<<g, blk, 0, s>>>(d, z, cnt, true);
+  k_nan_latch<<<1, 1, 0, s>>>(cnt);
+  return (int)cudaGetLastError();
 }
 
 }  // namespace gb
@@ -576,10 +620,18 @@ int check_state(getm_ctx* ctx, const getm_bc_state* st) {
   if (!ctx || !st) return GETM_ERR_ARG;
   if (!ctx->adv_ready) return fail(ctx, GETM_ERR_STATE, "getm_init_advection has not been called");
   if (st->prec3d != 8 && st->prec3d != 4) return fail(ctx, GETM_ERR_ARG, "getm_bc_state.prec3d must be 8 or 4");
+  const int* ip = st->ipar;
   for (int q = 0; q < NF2; ++q)
-    if (!st->f2[q]) return fail(ctx, GETM_ERR_ARG, "getm_bc_state: null 2D field");
+    if (!st->f2[q] && !(optional_f2(q) && !ip[I_RADIATION]))
+      return fail(ctx, GETM_ERR_ARG, "getm_bc_state: null 2D field");
   for (int q = 0; q < NF3; ++q)
-    if (!st->f3[q]) return fail(ctx, GETM_ERR_ARG, "getm_bc_state: null 3D field");
+    if (!st->f3[q] && !(optional_f3(q) && (q != RAD || !ip[I_RADIATION])))
+      return fail(ctx, GETM_ERR_ARG, "getm_bc_state: null 3D field");
+  if (ip[I_VISCOSITY] != 0 && ip[I_VISCOSITY] != 1)
+    return fail(ctx, GETM_ERR_ARG, "viscosity must be 0 (CONSTANT_VISCOSITY) or 1 (PARABOLIC_VISCOSITY)");
+  if (ip[I_EQSTATE_METHOD] < 1 || ip[I_EQSTATE_METHOD] > 3)
+    return fail(ctx, GETM_ERR_ARG, "eqstate_method must be 1..3 (eqstate.F90:56-68)");
+  if (ip[I_RADIATION] != 0 && ip[I_RADIATION] != 1) return fail(ctx, GETM_ERR_ARG, "radiation must be 0 or 1");
   if (!st->az || !st->au || !st->av || !st->ax) return fail(ctx, GETM_ERR_ARG, "getm_bc_state: null mask");
   if (st->ipar[I_RUNTYPE] != 4 && st->ipar[I_RUNTYPE] != 2 && st->ipar[I_RUNTYPE] != 1 && st->ipar[I_RUNTYPE] != 3)
     return fail(ctx, GETM_ERR_ARG, "runtype must be 1..4");
@@ -773,6 +825,81 @@ int uv_advect_2d(getm_ctx* ctx, const getm_bc_state* st, const double* U, const 
     GB_TRY(cudaGetLastError(), #kernel);                           \
   } while (0)
 
+// sealevel.F90:115-117: the NaN sweep of the elevations every |sealevel_check| micro steps, until
+// a sweep finds one (have_warned). The sweeps count on the device without a host synchronisation;
+// nan_report reads the counters at the end of the call.
+int nan_sweep_due(getm_ctx* ctx, const getm_bc_state* st, int loop) {
+  const int chk = st->ipar[I_SEALEVEL_CHECK];
+  if (chk == 0 || st->ipar[I_NAN_WARNED] || loop % std::abs(chk) != 0) return GETM_OK;
+  TimerScope ts(ctx, GETM_TIM_BC2D);
+  ctx->nan_swept = true;
+  GB_TRY(run_nan_sweep(ctx->dev, ctx->stream, st->f2[Z], ctx->cnt + 3), "sealevel_nan_check");
+  return GETM_OK;
+}
+
+// End of a call that swept: a finding sets nan_warned and, for sealevel_check > 0, is the error
+// the reference stops with (getm_error 'NaN values encountered in elevations').
+int nan_report(getm_ctx* ctx, getm_bc_state* st) {
+  if (!ctx->nan_swept) return GETM_OK;
+  ctx->nan_swept = false;
+  unsigned long long h[2] = {0, 0};
+  GB_TRY(cudaMemcpyAsync(h, ctx->cnt + 3, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream), "read NaN sweep");
+  GB_TRY(cudaMemsetAsync(ctx->cnt + 3, 0, 3 * sizeof(unsigned long long), ctx->stream), "reset NaN sweep");
+  GB_TRY(cudaStreamSynchronize(ctx->stream), "NaN sweep");
+  if (h[0] == 0) return GETM_OK;
+  st->ipar[I_NAN_WARNED] = 1;
+  const Dev& d = ctx->dev;
+  const long long nx = d.imax - d.imin + 1, last = (long long)h[1] - 1;
+  char msg[160];
+  snprintf(msg, sizeof msg, "NaN values encountered in elevations: %llu values, the last at i = %lld, j = %lld",
+           h[0], d.imin + last % nx, d.jmin + last / nx);
+  ctx->err = msg;
+  return st->ipar[I_SEALEVEL_CHECK] > 0 ? GETM_ERR_CHECK : GETM_OK;
+}
+
+// bottom_friction.F90:8-250: ru, rv (and ruu, rvv; zub, zvb for runtype 1) from the transports;
+// FP64 arithmetic for the FP64 state, FP32 arithmetic in the mixed step (on the working copies when
+// wp is given)
+int bottom_friction_2d(getm_ctx* ctx, const getm_bc_state* st, int runtype, const Bc2W* wp) {
+  const Dev& d = ctx->dev;
+  const Bc2 s = to_bc2(st);
+  const Bc2W w = wp ? *wp : Bc2W{};
+  const dim3 gt((d.ni() + 31) / 32, (d.nj() + 7) / 8, 1);
+  TimerScope ts(ctx, GETM_TIM_BC2D);
+  if (wp) k_bottom_friction_f32t<true><<<gt, dim3(32, 8, 1), 0, ctx->stream>>>(d, s, w, runtype);
+  else if (st->prec3d == 8) k_bottom_friction<double, false><<<grid2(d), kBlk2, 0, ctx->stream>>>(d, s, w, runtype);
+  else k_bottom_friction_f32t<false><<<gt, dim3(32, 8, 1), 0, ctx->stream>>>(d, s, w, runtype);
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? GETM_OK : cuda_fail(ctx, (int)e, "bottom_friction");
+}
+
+// umomentum (DIR 0, momentum.F90:69-223) / vmomentum (DIR 1, :232-386): the transport update, the
+// mirror_bdy_2d copies of the open boundaries (:190, :353) and the Coriolis term for the other
+// velocity (:193-216, :356-379). Mixed micro step (wp): the update on the working copies, with
+// the term it needs formed in the same launch when `cor` (see integrate_2d).
+template <int DIR>
+int momentum_2d(getm_ctx* ctx, const getm_bc_state* st, const Bc2W* wp, bool cor) {
+  const Dev& d = ctx->dev;
+  const Bc2 s = to_bc2(st);
+  const Bc2W w = wp ? *wp : Bc2W{};
+  cudaStream_t cs = ctx->stream;
+  {
+    TimerScope ts(ctx, GETM_TIM_BC2D);
+    if (!wp) k_momentum<DIR, false><<<grid2(d), kBlk2, 0, cs>>>(d, s, w);
+    else if (cor) k_momentum<DIR, true, true><<<grid2(d), kBlk2, 0, cs>>>(d, s, w);
+    else k_momentum<DIR, true, false><<<grid2(d), kBlk2, 0, cs>>>(d, s, w);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(ctx, (int)e, DIR == 0 ? "umomentum" : "vmomentum");
+  }
+  if (wp) return GETM_OK;
+  int r;
+  if ((r = mirror_bdy<double>(ctx, st->f2[DIR == 0 ? U_ : V_], DIR, 1))) return r;
+  TimerScope ts(ctx, GETM_TIM_BC2D);
+  k_coriolis<DIR, false><<<grid2(d), kBlk2, 0, cs>>>(d, s, w);
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? GETM_OK : cuda_fail(ctx, (int)e, "coriolis");
+}
+
 // m2d.F90:412-490 integrate_2d (closed boundaries; no residual; Am <= 0, An_method = 0)
 int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop, const Bc2W* wp = nullptr, bool first = false) {
   const Dev& d = ctx->dev;
@@ -787,21 +914,7 @@ int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop, const Bc2W* wp = nu
     return (int)cudaGetLastError();
   };
   int rc = GETM_OK;
-  if ((loop - 1) % ip[I_MM] == 0) {
-    const dim3 gt((d.ni() + 31) / 32, (d.nj() + 7) / 8, 1);
-    if (mix) {
-      TimerScope ts(ctx, GETM_TIM_BC2D);
-      k_bottom_friction_f32t<true><<<gt, dim3(32, 8, 1), 0, ctx->stream>>>(d, s, w, ip[I_RUNTYPE]);
-      rc = (int)cudaGetLastError();
-    } else if (st->prec3d == 8) {
-      rc = k2(k_bottom_friction<double, false>, d, s, w, ip[I_RUNTYPE]);
-    } else {
-      TimerScope ts(ctx, GETM_TIM_BC2D);
-      k_bottom_friction_f32t<false><<<gt, dim3(32, 8, 1), 0, ctx->stream>>>(d, s, w, ip[I_RUNTYPE]);
-      rc = (int)cudaGetLastError();
-    }
-    if (rc) return cuda_fail(ctx, rc, "bottom_friction");
-  }
+  if ((loop - 1) % ip[I_MM] == 0 && (rc = bottom_friction_2d(ctx, st, ip[I_RUNTYPE], wp))) return rc;
   if (mix) {
     const int hor = ip[I_VEL2D_HOR];
     if (hor == NOADV) {
@@ -828,24 +941,8 @@ int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop, const Bc2W* wp = nu
   // it gives the same value. The first update of a getm_time_loop call (first) reads the stored
   // term instead -- the state's fU/fV, which need not match the velocities (a start from rest of
   // the Coriolis terms) -- and getm_time_loop forms the term of the last update at its end.
-  auto umom = [&](bool cor) -> int {
-    int r = !mix ? k2(k_momentum<0, false>, d, s, w)
-                 : cor ? k2(k_momentum<0, true, true>, d, s, w) : k2(k_momentum<0, true, false>, d, s, w);
-    if (r) return cuda_fail(ctx, r, "umomentum");
-    if (mix) return GETM_OK;
-    if ((r = mirror_bdy<double>(ctx, st->f2[U_], 0, 1))) return r;
-    r = k2(k_coriolis<0, false>, d, s, w);
-    return r ? cuda_fail(ctx, r, "coriolis") : GETM_OK;
-  };
-  auto vmom = [&](bool cor) -> int {
-    int r = !mix ? k2(k_momentum<1, false>, d, s, w)
-                 : cor ? k2(k_momentum<1, true, true>, d, s, w) : k2(k_momentum<1, true, false>, d, s, w);
-    if (r) return cuda_fail(ctx, r, "vmomentum");
-    if (mix) return GETM_OK;
-    if ((r = mirror_bdy<double>(ctx, st->f2[V_], 1, 1))) return r;
-    r = k2(k_coriolis<1, false>, d, s, w);
-    return r ? cuda_fail(ctx, r, "coriolis") : GETM_OK;
-  };
+  auto umom = [&](bool cor) -> int { return momentum_2d<0>(ctx, st, wp, cor); };
+  auto vmom = [&](bool cor) -> int { return momentum_2d<1>(ctx, st, wp, cor); };
   if (ip[I_UFIRST2D]) {
     if ((rc = umom(!first)) || (rc = vmom(true))) return rc;
     ip[I_UFIRST2D] = 0;
@@ -859,6 +956,7 @@ int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop, const Bc2W* wp = nu
   rc = mix ? k2(k_accum_sealevel<true>, d, s, w, ip[I_RUNTYPE] > 1 ? 1 : 0)
            : k2(k_accum_sealevel<false>, d, s, w, ip[I_RUNTYPE] > 1 ? 1 : 0);
   if (rc) return cuda_fail(ctx, rc, "sealevel");
+  if ((rc = nan_sweep_due(ctx, st, loop))) return rc;
   rc = mix ? k2(k_depth_update<true>, d, s, w) : k2(k_depth_update<false>, d, s, w);
   if (rc) return cuda_fail(ctx, rc, "depth_update");
   return GETM_OK;
@@ -912,6 +1010,23 @@ int bc3(getm_ctx* ctx, const getm_bc_state* st, int which, int slot) {
   return GETM_OK;
 }
 
+// do_internal_pressure (internal_pressure.F90:181-274) with the configured method (check_state
+// admits 1, 2, 4, 5, 6): heights of the layer interfaces (1, 5) or of the pressure points (2, 4; 6
+// over the whole haloed domain, with its column integrals), then the gradients idpdx, idpdy
+template <class R3>
+int internal_pressure(getm_ctx* ctx, const getm_bc_state* st) {
+  const int ipm = st->ipar[I_IP_METHOD];
+  const bool centres = ipm == 2 || ipm == 4;
+  const int ipk = ipm == 1   ? BC3_IP
+                  : ipm == 2 ? BC3_IP_LIN
+                  : ipm == 4 ? BC3_IP_SW
+                  : ipm == 5 ? BC3_IP_CF
+                             : BC3_IP_SM;
+  int rc;
+  if ((rc = bc3<R3>(ctx, st, ipm == 6 ? BC3_SM_COLS : centres ? BC3_ZZ_LIN : BC3_ZZ, GETM_TIM_BC3D))) return rc;
+  return bc3<R3>(ctx, st, ipk, GETM_TIM_IP);
+}
+
 // m3d.F90:422-636 integrate_3d for runtype 4 (closed boundaries, sigma coordinates, linear EOS,
 // Blumberg-Mellor internal pressure, prescribed viscosity)
 template <class R3>
@@ -928,20 +1043,7 @@ int integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
   GB_K2(k_start_macro_t, d, s2);
   GB_K2(k_start_macro_uv, d, s2, 1.0 / (double)(float)ip[I_M]);
   if (d.kmax > 1 && (rc = bc3<R3>(ctx, st, BC3_BF3D, GETM_TIM_BC3D))) return rc;
-  if (ip[I_RUNTYPE] == 4) {
-    // internal_pressure.F90:215-229: the configured method (check_state admits 1, 2, 4, 5, 6);
-    // heights of the layer interfaces (1, 5) or of the pressure points (2, 4; 6 over the whole
-    // haloed domain, with its column integrals), then the gradients
-    const int ipm = ip[I_IP_METHOD];
-    const bool centres = ipm == 2 || ipm == 4;
-    const int ipk = ipm == 1   ? BC3_IP
-                    : ipm == 2 ? BC3_IP_LIN
-                    : ipm == 4 ? BC3_IP_SW
-                    : ipm == 5 ? BC3_IP_CF
-                               : BC3_IP_SM;
-    if ((rc = bc3<R3>(ctx, st, ipm == 6 ? BC3_SM_COLS : centres ? BC3_ZZ_LIN : BC3_ZZ, GETM_TIM_BC3D))) return rc;
-    if ((rc = bc3<R3>(ctx, st, ipk, GETM_TIM_IP))) return rc;
-  }
+  if (ip[I_RUNTYPE] == 4 && (rc = internal_pressure<R3>(ctx, st))) return rc;
   // m3d.F90 sets huo = hun, hvo = hvn here for uu/vv_momentum_3d; sigma_coordinates below then
   // recomputes huo/hvo from the same elevations, to the same values. The momentum kernels read
   // hun/hvn as their old heights instead, so the two 3D copies are not made.
@@ -984,9 +1086,29 @@ int integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
         return rc;
     }
     if ((rc = bc3<R3>(ctx, st, BC3_STRESSES, GETM_TIM_BC3D))) return rc;
+    // m3d.F90:570-575: gotm() with PARABOLIC_VISCOSITY (CONSTANT_VISCOSITY leaves num, nuh)
+    if (ip[I_VISCOSITY] == 1 && (rc = bc3<R3>(ctx, st, BC3_GOTM_PARABOLIC, GETM_TIM_BC3D))) return rc;
   }
   if (ip[I_RUNTYPE] == 4) {
     const R3 dt = R3(st->par[P_DT]);
+    // do_temperature's short-wave radiation and surface heat flux (temperature.F90:452-525): the
+    // sources of the temperature diffusion in the tracer scratch, and (paired advection) the
+    // top-level salinity before it is advected, which the freezing-point test of the heat flux reads
+    const bool radn = ip[I_RADIATION] && ip[I_CALC_TEMP];
+    R3* tsrc = nullptr;
+    R3* s_top = nullptr;
+    if (radn) {
+      if ((rc = ensure_scratch(ctx, (size_t)n3 * sizeof(R3)))) return rc;
+      tsrc = (R3*)ctx->scr[2];
+      s_top = (R3*)(ctx->bc_scr2 + 7 * n2d(d));
+    }
+    auto temp_sources = [&](const R3* stop) -> int {
+      const Bc3<R3> s3 = to_bc3<R3>(st);
+      R3* sc[2] = {tsrc, const_cast<R3*>(stop)};
+      GB_TIMED(GETM_TIM_VDIFF, (run_bc3<R3>(BC3_SW_RADIATION, d, s, s3, sc)), "short-wave radiation");
+      if (d.kmax > 1) GB_TIMED(GETM_TIM_VDIFF, (run_bc3<R3>(BC3_TEMP_SOURCE, d, s, s3, sc)), "temperature sources");
+      return GETM_OK;
+    };
     // do_temperature and do_salinity advect with the same velocities and heights; with the same
     // schemes the two advections run as one paired sweep sequence (each field's arithmetic is
     // unchanged), followed by the two diffusion solves.
@@ -996,11 +1118,16 @@ int integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
                       (ip[I_TEMP_VER] == NOADV || is_split_scheme(ip[I_TEMP_VER])) &&
                       st->par[P_TEMP_AH] == st->par[P_SALT_AH] && ip[I_ADV_VER_ITERS] <= 1 && ctx->adv_ready;
     if (pair) {
+      if (radn)
+        GB_TRY(cudaMemcpyAsync(s_top, f3[SS] + (long long)d.kmax * d.sk, n2d(d) * sizeof(R3), cudaMemcpyDeviceToDevice,
+                               s),
+               "top-level salinity");
       if ((rc = do_adv3d_pair<R3>(ctx, dt, f3[TT], f3[SS], f3[UU], f3[VV], f3[WW], f3[HUN], f3[HVN], f3[HO],
                                   ip[I_TEMP_HOR], ip[I_TEMP_VER], R3(st->par[P_TEMP_AH]))))
         return rc;
+      if (radn && (rc = temp_sources(s_top))) return rc;
       GB_TIMED(GETM_TIM_VDIFF, run_vdiff<R3>(d, s, dt, R3(st->par[P_CNPAR]), R3(st->par[P_AVMOLT]), f3[TT], f3[HN],
-                                             f3[NUH], st->az, (const R3*)nullptr, (R3*)ctx->scr[0], (R3*)ctx->scr[1]),
+                                             f3[NUH], st->az, (const R3*)tsrc, (R3*)ctx->scr[0], (R3*)ctx->scr[1]),
                "vdiff T");
       GB_TIMED(GETM_TIM_VDIFF, run_vdiff<R3>(d, s, dt, R3(st->par[P_CNPAR]), R3(st->par[P_AVMOLS]), f3[SS], f3[HN],
                                              f3[NUH], st->az, (const R3*)nullptr, (R3*)ctx->scr[0], (R3*)ctx->scr[1]),
@@ -1011,8 +1138,9 @@ int integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
                              ip[I_TEMP_SPLIT], ip[I_TEMP_HOR], ip[I_TEMP_VER], R3(st->par[P_TEMP_AH]), GETM_H_TAG,
                              nullptr, nullptr, ip[I_ADV_VER_ITERS])))
         return rc;
+      if (radn && (rc = temp_sources(nullptr))) return rc;
       GB_TIMED(GETM_TIM_VDIFF, run_vdiff<R3>(d, s, dt, R3(st->par[P_CNPAR]), R3(st->par[P_AVMOLT]), f3[TT], f3[HN],
-                                             f3[NUH], st->az, (const R3*)nullptr, (R3*)ctx->scr[0], (R3*)ctx->scr[1]),
+                                             f3[NUH], st->az, (const R3*)tsrc, (R3*)ctx->scr[0], (R3*)ctx->scr[1]),
                "vdiff T");
     }
     if (!pair && ip[I_CALC_SALT]) {
@@ -1027,7 +1155,9 @@ int integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
     // m3d.F90:595,602
     if (ip[I_CALC_TEMP] && (rc = mirror_bdy<R3>(ctx, f3[TT], 2, d.kmax + 1))) return rc;
     if (ip[I_CALC_SALT] && (rc = mirror_bdy<R3>(ctx, f3[SS], 2, d.kmax + 1))) return rc;
-    if ((rc = bc3<R3>(ctx, st, BC3_EQSTATE, GETM_TIM_BC3D))) return rc;
+    const int eos = ip[I_EQSTATE_METHOD] == 2 ? BC3_EQSTATE_UNESCO : ip[I_EQSTATE_METHOD] == 3 ? BC3_EQSTATE_JACKETT
+                                                                                              : BC3_EQSTATE;
+    if ((rc = bc3<R3>(ctx, st, eos, GETM_TIM_BC3D))) return rc;
   }
   if (d.kmax > 1) {
     const long long n2 = n2d(d);
@@ -1183,7 +1313,119 @@ int getm_integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop) {
   int rc = check_state(ctx, st);
   if (rc) return rc;
   if ((rc = ensure_bc_scratch(ctx, (size_t)st->prec3d))) return rc;
-  return integrate_2d(ctx, st, loop);
+  rc = integrate_2d(ctx, st, loop);
+  const int rn = nan_report(ctx, st);
+  return rc ? rc : rn;
+}
+
+// ---- the substeps of integrate_2d / integrate_3d one by one (FP64 2D arithmetic of the state) ----
+#define GB_BC_ENTRY                                            \
+  int rc = check_state(ctx, st);                               \
+  if (rc) return rc;                                           \
+  if ((rc = ensure_bc_scratch(ctx, (size_t)st->prec3d))) return rc
+
+int getm_bottom_friction(getm_ctx* ctx, getm_bc_state* st, int runtype) {
+  GB_BC_ENTRY;
+  if (runtype < 1 || runtype > 4) return fail(ctx, GETM_ERR_ARG, "runtype must be 1..4");
+  return bottom_friction_2d(ctx, st, runtype, nullptr);
+}
+
+int getm_uv_advect(getm_ctx* ctx, getm_bc_state* st) {
+  GB_BC_ENTRY;
+  return uv_advect_2d(ctx, st, st->f2[U_], st->f2[V_], st->f2[DU], st->f2[DV]);
+}
+
+int getm_umomentum(getm_ctx* ctx, getm_bc_state* st) {
+  GB_BC_ENTRY;
+  return momentum_2d<0>(ctx, st, nullptr, false);
+}
+
+int getm_vmomentum(getm_ctx* ctx, getm_bc_state* st) {
+  GB_BC_ENTRY;
+  return momentum_2d<1>(ctx, st, nullptr, false);
+}
+
+int getm_momentum(getm_ctx* ctx, getm_bc_state* st, int n) {
+  (void)n;
+  GB_BC_ENTRY;
+  int* ip = st->ipar;
+  if (ip[I_UFIRST2D]) {
+    if ((rc = momentum_2d<0>(ctx, st, nullptr, false)) || (rc = momentum_2d<1>(ctx, st, nullptr, false))) return rc;
+    ip[I_UFIRST2D] = 0;
+  } else {
+    if ((rc = momentum_2d<1>(ctx, st, nullptr, false)) || (rc = momentum_2d<0>(ctx, st, nullptr, false))) return rc;
+    ip[I_UFIRST2D] = 1;
+  }
+  return GETM_OK;
+}
+
+int getm_update_2d_bdy(getm_ctx* ctx, getm_bc_state* st, int loop) {
+  GB_BC_ENTRY;
+  return bdy_2d(ctx, to_bc2(st), loop);
+}
+
+int getm_sealevel(getm_ctx* ctx, getm_bc_state* st, int loop) {
+  GB_BC_ENTRY;
+  const Dev& d = ctx->dev;
+  {
+    TimerScope ts(ctx, GETM_TIM_BC2D);
+    k_accum_sealevel<false><<<grid2(d), kBlk2, 0, ctx->stream>>>(d, to_bc2(st), Bc2W{}, 0);
+    GB_TRY(cudaGetLastError(), "sealevel");
+  }
+  if ((rc = nan_sweep_due(ctx, st, loop))) return rc;
+  return nan_report(ctx, st);
+}
+
+int getm_depth_update(getm_ctx* ctx, getm_bc_state* st) {
+  GB_BC_ENTRY;
+  const Dev& d = ctx->dev;
+  TimerScope ts(ctx, GETM_TIM_BC2D);
+  k_depth_update<false><<<grid2(d), kBlk2, 0, ctx->stream>>>(d, to_bc2(st), Bc2W{});
+  GB_TRY(cudaGetLastError(), "depth_update");
+  return GETM_OK;
+}
+
+int getm_internal_pressure(getm_ctx* ctx, getm_bc_state* st) {
+  GB_BC_ENTRY;
+  return st->prec3d == 8 ? internal_pressure<double>(ctx, st) : internal_pressure<float>(ctx, st);
+}
+
+int getm_do_eqstate(getm_ctx* ctx, getm_bc_state* st) {
+  GB_BC_ENTRY;
+  const int m = st->ipar[I_EQSTATE_METHOD];
+  const int which = m == 2 ? BC3_EQSTATE_UNESCO : m == 3 ? BC3_EQSTATE_JACKETT : BC3_EQSTATE;
+  return st->prec3d == 8 ? bc3<double>(ctx, st, which, GETM_TIM_BC3D) : bc3<float>(ctx, st, which, GETM_TIM_BC3D);
+}
+
+int getm_gotm(getm_ctx* ctx, getm_bc_state* st) {
+  GB_BC_ENTRY;
+  if (st->ipar[I_VISCOSITY] != 1) return GETM_OK;  // CONSTANT_VISCOSITY: num and nuh stay
+  return st->prec3d == 8 ? bc3<double>(ctx, st, BC3_GOTM_PARABOLIC, GETM_TIM_BC3D)
+                         : bc3<float>(ctx, st, BC3_GOTM_PARABOLIC, GETM_TIM_BC3D);
+}
+
+int getm_sw_radiation(getm_ctx* ctx, getm_bc_state* st) {
+  GB_BC_ENTRY;
+  if (!st->f3[RAD] || !st->f2[SWR] || !st->f2[ATT_A] || !st->f2[ATT_G1] || !st->f2[ATT_G2])
+    return fail(ctx, GETM_ERR_ARG, "sw_radiation: swr, A, g1, g2 and rad are needed");
+  return st->prec3d == 8 ? bc3<double>(ctx, st, BC3_SW_RADIATION, GETM_TIM_VDIFF)
+                         : bc3<float>(ctx, st, BC3_SW_RADIATION, GETM_TIM_VDIFF);
+}
+
+int getm_sealevel_nan_check(getm_ctx* ctx, const double* z, int64_t* num_nan, int32_t* inan, int32_t* jnan) {
+  if (!ctx || !z || !num_nan) return GETM_ERR_ARG;
+  const Dev& d = ctx->dev;
+  unsigned long long* c = ctx->cnt + 6;  // counters [6] findings, [7] last index + 1; latch unused
+  GB_TRY(cudaMemsetAsync(c, 0, 2 * sizeof(unsigned long long), ctx->stream), "reset");
+  GB_TRY(run_nan_sweep_once(d, ctx->stream, z, c), "sealevel_nan_check");
+  unsigned long long h[2] = {0, 0};
+  GB_TRY(cudaMemcpyAsync(h, c, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream), "read");
+  GB_TRY(cudaStreamSynchronize(ctx->stream), "sync");
+  *num_nan = (int64_t)h[0];
+  const long long nx = d.imax - d.imin + 1, last = (long long)h[1] - 1;
+  if (inan) *inan = h[0] ? (int32_t)(d.imin + last % nx) : 0;
+  if (jnan) *jnan = h[0] ? (int32_t)(d.jmin + last / nx) : 0;
+  return GETM_OK;
 }
 
 int getm_integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
@@ -1201,7 +1443,7 @@ int getm_time_loop(getm_ctx* ctx, getm_bc_state* st, int n0, int count) {
   // barotropic fields (is_work2) when the fused 2D momentum advection applies and there are no
   // open boundaries; the elevation and Uint/Vint stay FP64 throughout.
   const int* ip = st->ipar;
-  const bool mix = st->prec3d == 4 && !ctx->has_bdy &&
+  const bool mix = st->prec3d == 4 && !ctx->has_bdy && fp32_micro_steps_enabled() &&
                    (ip[I_VEL2D_HOR] == NOADV ||
                     (ip[I_VEL2D_SPLIT] == GETM_HALFSPLIT && is_split_scheme(ip[I_VEL2D_HOR])));
   Bc2W w{};
@@ -1266,7 +1508,7 @@ int getm_time_loop(getm_ctx* ctx, getm_bc_state* st, int n0, int count) {
   }
   if (dirty && (rc = sync(written, 0))) return rc;
   if (mix && !dirty && count > 0 && (rc = sync((1ull << FU) | (1ull << FV), 0))) return rc;
-  return GETM_OK;
+  return nan_report(ctx, st);
 }
 
 }  // extern "C"

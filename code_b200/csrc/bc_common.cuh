@@ -8,18 +8,24 @@ namespace gb {
 enum F2 {
   Z, ZO, U_, V_, D_, DU, DV, UEX, VEX, FU, FV, RU, RV, RUU, RVV, UINT, VINT, UINTO, VINTO, SLUX, SLVX, SLRU, SLRV,
   ZUB, ZVB, ZUB0, ZVB0, FWF, HH, HU, HV, DRY_Z, DRY_U, DRY_V, CORU, CORV, TAUSX, TAUSY, AIRP, SSEO, SSEN, SSUO,
-  SSUN, SSVO, SSVN, DN, DUN, DVN, RRU, RRV, TAUBX, TAUBY, TAUB, TAUS, NF2
+  SSUN, SSVO, SSVN, DN, DUN, DVN, RRU, RRV, TAUBX, TAUBY, TAUB, TAUS, SWR, SHF, ATT_A, ATT_G1, ATT_G2, NF2
 };
-enum F3 { UU, VV, WW, HO, HN, HUO, HUN, HVO, HVN, UUEX, VVEX, IDPDX, IDPDY, TT, SS, RHO, BUOY, NUM, NUH, NF3 };
+enum F3 {
+  UU, VV, WW, HO, HN, HUO, HUN, HVO, HVN, UUEX, VVEX, IDPDX, IDPDY, TT, SS, RHO, BUOY, NUM, NUH, RAD, TKE, EPS, NF3
+};
 enum PD {
   P_DTM, P_DT, P_CNPAR, P_MIN_DEPTH, P_CRIT_DEPTH, P_G, P_RHO_0, P_KAPPA, P_AVMMOL, P_AVMOLT, P_AVMOLS, P_T0, P_S0,
-  P_DTR0, P_DSR0, P_IP_FAC, P_TEMP_AH, P_SALT_AH, NPD
+  P_DTR0, P_DSR0, P_IP_FAC, P_TEMP_AH, P_SALT_AH, P_AVMBACK, P_AVHBACK, P_CP, P_SWR_BOT_REFL_FRAC,
+  P_SWR_MIN_BOT_FRAC, NPD
 };
 enum PI {
   I_M, I_MM, I_RUNTYPE, I_VEL2D_SPLIT, I_VEL2D_HOR, I_VEL3D_SPLIT, I_VEL3D_HOR, I_VEL3D_VER, I_TEMP_SPLIT, I_TEMP_HOR,
   I_TEMP_VER, I_SALT_SPLIT, I_SALT_HOR, I_SALT_VER, I_ADV_VER_ITERS, I_UFIRST2D, I_UFIRST3D, I_CALC_TEMP,
-  I_CALC_SALT, I_IP_METHOD, NPI
+  I_CALC_SALT, I_IP_METHOD, I_VISCOSITY, I_EQSTATE_METHOD, I_SEALEVEL_CHECK, I_RADIATION, I_NAN_WARNED, NPI
 };
+// fields a state may leave NULL: the radiation inputs and output when radiation = 0, tke and eps
+constexpr bool optional_f2(int q) { return q == SWR || q == SHF || q == ATT_A || q == ATT_G1 || q == ATT_G2; }
+constexpr bool optional_f3(int q) { return q == RAD || q == TKE || q == EPS; }
 
 // 2D part (all FP64) -- passed to kernels by value
 struct Bc2 {

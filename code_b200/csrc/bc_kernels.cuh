@@ -986,6 +986,168 @@ __global__ void __launch_bounds__(128) k_eqstate_vec(Dev d, Bc3<float> s) {
   st_row<float, N>(s.f3[BUOY] + p, na == N, na, b);
 }
 
+// eqstate.F90:496-534 (rho_from_theta_unesco80): UNESCO 1980 density at zero pressure; the
+// coefficients are the reference's default-kind (single precision) literals, widened to double.
+__device__ __forceinline__ double rho_unesco80(double T, double S) {
+  const double T1 = T, T2 = T1 * T1, T3 = T1 * T2, T4 = T2 * T2, T5 = T1 * T4;
+  const double S1 = S, S2 = S1 * S1, S3 = S1 * S2;
+  double x = (double)999.842594f + (double)6.793952e-02f * T1 - (double)9.09529e-03f * T2 +
+             (double)1.001685e-04f * T3;
+  x = x - (double)1.120083e-06f * T4 + (double)6.536332e-09f * T5;
+  x = x + S1 * ((double)0.824493f - (double)4.0899e-03f * T1 + (double)7.6438e-05f * T2 -
+                (double)8.2467e-07f * T3);
+  x = x + S1 * (double)5.3875e-09f * T4;
+  x = x + sqrt(S3) * (-(double)5.72466e-03f + (double)1.0227e-04f * T1 - (double)1.6546e-06f * T2);
+  x = x + (double)4.8314e-04f * S2;
+  return x;
+}
+
+// eqstate.F90:540-590 (rho_from_theta at p = 0): the rational function of Jackett et al. (2006).
+__device__ __forceinline__ double rho_jackett06(double s, double th) {
+  const double th2 = th * th, sqrts = sqrt(s);
+  const double anum = 9.9984085444849347e+02 +
+                      th * (7.3471625860981584e+00 + th * (-5.3211231792841769e-02 + th * 3.6492439109814549e-04)) +
+                      s * (2.5880571023991390e+00 - th * 6.7168282786692355e-03 + s * 1.9203202055760151e-03);
+  const double aden =
+      1.0000000000000000e+00 +
+      th * (7.2815210113327091e-03 +
+            th * (-4.4787265461983921e-05 + th * (3.3851002965802430e-07 + th * 1.3651202389758572e-10))) +
+      s * (1.7632126669040377e-03 - th * (8.8066583251206474e-06 + th2 * 1.8832689434804897e-10) +
+           sqrts * (5.7463776745432097e-06 + th2 * 1.4716275472242334e-09));
+  return anum / aden;
+}
+
+// eqstate.F90:144-261 with eqstate_method 2 (UNESCO80) or 3 (Jackett 2006): the density of the
+// water columns (az > 0; land keeps its density) and the buoyancy -g/rho_0*(rho-rho_0) of every
+// point of the haloed plane, levels 1..kmax. The density function is evaluated in FP64 for either
+// storage type: in the mixed step the buoyancy is then formed from the FP64 density before it is
+// rounded, which keeps the anomaly rho-rho_0 (a thousandth of rho) to FP32 precision. The thermal
+// and haline expansion coefficients alpha, beta that the reference also forms feed only the
+// turbulence closure's buoyancy frequency and are not formed.
+template <class R3, int METHOD>
+__global__ void k_eqstate_nl(Dev d, Bc3<R3> s) {
+  GB_IJ_HALO
+  const int k = blockIdx.z + 1;
+  V3<R3> rho{d, s.f3[RHO]}, buoy{d, s.f3[BUOY]}, T{d, s.f3[TT]}, S{d, s.f3[SS]};
+  I2 az{d, s.az};
+  const double rho_0 = s.par[P_RHO_0];
+  const double x = -s.par[P_G] / s.par[P_RHO_0];
+  double r;
+  if (az(i, j) > 0) {
+    r = METHOD == 2 ? rho_unesco80((double)T(i, j, k), (double)S(i, j, k))
+                    : rho_jackett06((double)S(i, j, k), (double)T(i, j, k));
+    rho(i, j, k) = R3(r);
+  } else {
+    r = (double)rho(i, j, k);
+  }
+  if constexpr (sizeof(R3) == 8) buoy(i, j, k) = R3(x) * (R3(r) - R3(rho_0));
+  else buoy(i, j, k) = R3(x * (r - rho_0));
+}
+
+// gotm.F90:96-163 with PARABOLIC_VISCOSITY (:131-143), after stresses_3d: per water column of the
+// interior the profiles of turbulent kinetic energy, length scale, dissipation and eddy viscosity
+// on the interfaces k = 1..kmax-1 from the bottom stress taub, the depth D and the bottom
+// roughness (z0b from zub, zvb of the four velocity points), then num = profile + avmback and
+// nuh = profile + avhback; at k = 0 and kmax the background is added to the stored values (the
+// reference passes them through its column arrays). tke and eps receive the profiles when given.
+// FP64 arithmetic with the reference's single-precision literals and expression order; one thread
+// per column.
+template <class R3>
+__global__ void k_gotm_parabolic(Dev d, Bc3<R3> s) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + d.imin;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + d.jmin;
+  if (i > d.imax || j > d.jmax) return;
+  I2 az{d, s.az};
+  if (az(i, j) < 1) return;
+  V2 D{d, s.f2[D_]}, taub{d, s.f2[TAUB]}, zub{d, s.f2[ZUB]}, zvb{d, s.f2[ZVB]};
+  V3<R3> hn{d, s.f3[HN]}, num{d, s.f3[NUM]}, nuh{d, s.f3[NUH]}, tke{d, s.f3[TKE]}, eps{d, s.f3[EPS]};
+  const int kmax = d.kmax;
+  const double avmback = s.par[P_AVMBACK], avhback = s.par[P_AVHBACK];
+  const double z0b = 0.5 * (fmax(zub(i - 1, j), zub(i, j)) + fmax(zvb(i, j - 1), zvb(i, j)));
+  const double Dl = D(i, j), tb = taub(i, j);
+  double zz = 0.0;
+  for (int k = 1; k <= kmax - 1; ++k) {
+    zz = zz + (double)hn(i, j, k);
+    const double t = fmax((double)1.e-10f, (double)3.333333f * tb * (1.0 - zz / Dl));
+    const double L = (double)0.4f * (zz + z0b) * sqrt(1.0 - zz / Dl);
+    const double e = (double)0.16431677f * sqrt(t * t * t) / L;
+    const double nu = (double)0.09f * t * t / e;
+    if (s.f3[TKE]) tke(i, j, k) = R3(t);
+    if (s.f3[EPS]) eps(i, j, k) = R3(e);
+    num(i, j, k) = R3(nu + avmback);
+    nuh(i, j, k) = R3(nu + avhback);
+  }
+  if (kmax >= 1) {
+    num(i, j, 0) = R3((double)num(i, j, 0) + avmback);
+    nuh(i, j, 0) = R3((double)nuh(i, j, 0) + avhback);
+    num(i, j, kmax) = R3((double)num(i, j, kmax) + avmback);
+    nuh(i, j, kmax) = R3((double)nuh(i, j, kmax) + avhback);
+  }
+}
+
+// temperature.F90:452-465: the short-wave radiation rad of the water columns (az >= 1) of the
+// interior, swr at the surface and below it swr*(A*exp(-z/g1) + (1-A)*exp(-z/g2)) with z the depth
+// of the interface under the surface; one thread per column, FP64 arithmetic.
+template <class R3>
+__global__ void k_sw_radiation(Dev d, Bc3<R3> s) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + d.imin;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + d.jmin;
+  if (i > d.imax || j > d.jmax) return;
+  I2 az{d, s.az};
+  if (az(i, j) < 1) return;
+  V2 swr{d, s.f2[SWR]}, A{d, s.f2[ATT_A]}, g1{d, s.f2[ATT_G1]}, g2{d, s.f2[ATT_G2]};
+  V3<R3> hn{d, s.f3[HN]}, rad{d, s.f3[RAD]};
+  const double swr_loc = swr(i, j), a = A(i, j), l1 = g1(i, j), l2 = g2(i, j);
+  rad(i, j, d.kmax) = R3(swr_loc);
+  double zz = 0.0;
+  for (int k = d.kmax - 1; k >= 0; --k) {
+    zz = zz + (double)hn(i, j, k + 1);
+    rad(i, j, k) = R3(swr_loc * (a * exp(-zz / l1) + (1 - a) * exp(-zz / l2)));
+  }
+}
+
+// temperature.F90:469-525: the sources that do_temperature adds to the right-hand side of its
+// diffusion matrix, per layer of the water columns (az == 1) of the interior: dry_z*dt*(rad1d(k) -
+// rad1d(k-1)), with shf*rho_0_cpi added in the top layer. rad1d = rad less the light reflected at
+// the bottom (swr_bot_refl_frac > 0 and rad(0)/rad(kmax) > swr_min_bot_frac) times 1/(rho_0*cp); a
+// cooling surface flux is dropped where the top layer is at the freezing point (T <= -0.0575*S).
+// S_top: the top-level salinity before do_salinity (NULL: read S itself). The column's rad1d is
+// formed level by level from the bottom up, so no column array is needed.
+template <class R3>
+__global__ void k_temp_source(Dev d, Bc3<R3> s, const R3* __restrict__ S_top, R3* __restrict__ srcp) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + d.imin;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + d.jmin;
+  if (i > d.imax || j > d.jmax) return;
+  I2 az{d, s.az};
+  if (az(i, j) != 1) return;
+  const int kmax = d.kmax;
+  V2 shf{d, s.f2[SHF]}, A{d, s.f2[ATT_A]}, g1{d, s.f2[ATT_G1]}, g2{d, s.f2[ATT_G2]}, dry_z{d, s.f2[DRY_Z]};
+  V3<R3> hn{d, s.f3[HN]}, rad{d, s.f3[RAD]}, T{d, s.f3[TT]}, S{d, s.f3[SS]}, src{d, srcp};
+  const double dt = s.par[P_DT];
+  const double rho_0_cpi = 1.0 / (s.par[P_RHO_0] * s.par[P_CP]);
+  const double refl = s.par[P_SWR_BOT_REFL_FRAC], minfrac = s.par[P_SWR_MIN_BOT_FRAC];
+  double shf_loc = shf(i, j);
+  const double stop = S_top ? (double)S_top[d.ix(i, j)] : (double)S(i, j, kmax);
+  if ((double)T(i, j, kmax) <= -((double)0.0575f * stop)) shf_loc = fmax(0.0, shf_loc);
+  const double rad0 = (double)rad(i, j, 0), radk = (double)rad(i, j, kmax);
+  const bool reflect = refl > 0.0 && rad0 / radk > minfrac;
+  const double swr_refl = reflect ? rad0 * refl : 0.0;
+  const double a = A(i, j), l1 = g1(i, j), l2 = g2(i, j), dz = dry_z(i, j);
+  // rad1d(k) before the scaling, k = 0..kmax
+  double zz = 0.0;
+  double below = reflect ? (rad0 - swr_refl) * rho_0_cpi : rad0 * rho_0_cpi;  // rad1d(k-1)
+  for (int k = 1; k <= kmax; ++k) {
+    double r = (double)rad(i, j, k);
+    if (reflect) {
+      zz = zz + (double)hn(i, j, k);
+      r = r - swr_refl * (a * exp(-zz / l1) + (1 - a) * exp(-zz / l2));
+    }
+    const double here = r * rho_0_cpi;
+    src(i, j, k) = k < kmax ? R3(dz * dt * (here - below)) : R3(dz * dt * (here + shf_loc * rho_0_cpi - below));
+    below = here;
+  }
+}
+
 // slow_terms.F90:57-181 (kmax > 1, kumin = kvmin = 1): vertical sums in FP64
 template <class R3>
 __global__ void k_slow_terms(Dev d, Bc3<R3> s) {
@@ -1122,6 +1284,23 @@ int run_bc3(int which, const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* cons
       }
     }
     case BC3_STRESSES: k_stresses<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s); break;
+    case BC3_EQSTATE_UNESCO: k_eqstate_nl<R3, 2><<<plane_grid(d, blk, d.kmax), blk, 0, st>>>(d, s); break;
+    case BC3_EQSTATE_JACKETT: k_eqstate_nl<R3, 3><<<plane_grid(d, blk, d.kmax), blk, 0, st>>>(d, s); break;
+    case BC3_GOTM_PARABOLIC: {
+      const dim3 g((d.imax - d.imin + 1 + 31) / 32, (d.jmax - d.jmin + 1 + 3) / 4, 1);
+      k_gotm_parabolic<R3><<<g, blk, 0, st>>>(d, s);
+      break;
+    }
+    case BC3_SW_RADIATION: {
+      const dim3 g((d.imax - d.imin + 1 + 31) / 32, (d.jmax - d.jmin + 1 + 3) / 4, 1);
+      k_sw_radiation<R3><<<g, blk, 0, st>>>(d, s);
+      break;
+    }
+    case BC3_TEMP_SOURCE: {  // scr[0] = the source array, scr[1] = the top-level salinity (may be null)
+      const dim3 g((d.imax - d.imin + 1 + 31) / 32, (d.jmax - d.jmin + 1 + 3) / 4, 1);
+      k_temp_source<R3><<<g, blk, 0, st>>>(d, s, scr[1], scr[0]);
+      break;
+    }
     case BC3_EQSTATE: {
       if constexpr (sizeof(R3) == 4) {
         bool ok = vector_sweeps_enabled() && d.sj % 4 == 0 && d.sk % 4 == 0;

@@ -15,6 +15,8 @@ namespace gb {
 
 std::atomic<int> g_vector_sweeps{1};
 bool vector_sweeps_enabled() { return g_vector_sweeps.load(std::memory_order_relaxed) != 0; }
+std::atomic<int> g_fp32_micro{1};
+bool fp32_micro_steps_enabled() { return g_fp32_micro.load(std::memory_order_relaxed) != 0; }
 
 
 
@@ -308,12 +310,12 @@ int getm_ctx_create(const getm_domain* dom, void* stream, getm_ctx** out) {
   if (cudaMalloc(&ctx->planes, (size_t)n * NPLANES) != cudaSuccess ||
       cudaMalloc(&ctx->zmask, (size_t)n * 3 * sizeof(int32_t)) != cudaSuccess ||
       cudaMalloc(&ctx->red, (2 * RED_BLOCKS + 2) * sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&ctx->cnt, 4 * sizeof(unsigned long long)) != cudaSuccess) {
+      cudaMalloc(&ctx->cnt, GB_NCOUNTERS * sizeof(unsigned long long)) != cudaSuccess) {
     cudaGetLastError();
     getm_ctx_destroy(ctx);
     return GETM_ERR_NOMEM;
   }
-  if (cudaMemsetAsync(ctx->cnt, 0, 4 * sizeof(unsigned long long), ctx->stream) != cudaSuccess) {
+  if (cudaMemsetAsync(ctx->cnt, 0, GB_NCOUNTERS * sizeof(unsigned long long), ctx->stream) != cudaSuccess) {
     getm_ctx_destroy(ctx);
     return GETM_ERR_CUDA;
   }
@@ -394,6 +396,10 @@ static void drain_timers(getm_ctx* ctx) {
 
 int getm_set_vector_sweeps(int on) {
   return gb::g_vector_sweeps.exchange(on != 0 ? 1 : 0);
+}
+
+int getm_set_fp32_micro_steps(int on) {
+  return gb::g_fp32_micro.exchange(on != 0 ? 1 : 0);
 }
 
 int getm_timers_enable(getm_ctx* ctx, int on) {

@@ -9,6 +9,8 @@
 #include "common.cuh"
 #include "launch.h"
 
+#define GB_NCOUNTERS 8
+
 namespace gb {
 enum MaskPlane { P_UPDATEH = 0, P_UFLUX, P_VFLUX, P_XFLUX, P_UUPDATEU, P_VUPDATEV, P_UFLUX_U, P_VFLUX_V, NPLANES };
 
@@ -27,7 +29,10 @@ struct getm_ctx {
   void* scr[3] = {nullptr, nullptr, nullptr};  // 3D scratch: tracer ping-pong, hi, adv
   size_t scr_bytes = 0;
   double* red = nullptr;                // reduction partials (2*RED_BLOCKS) + result (2)
-  unsigned long long* cnt = nullptr;    // [0] warnings, [1] range-check count
+  // device counters: [0] warnings, [1] range-check count, [2] slow bottom-friction log checks,
+  // [3..5] the elevation NaN sweep of the micro steps (findings, last index + 1, latch)
+  unsigned long long* cnt = nullptr;
+  bool nan_swept = false;  // a NaN sweep was launched since its counters were last read
   std::string err;
   // per-stage device timers (the counterpart of getm_timers' tic/toc, getm_timers.F90:275-357)
   bool timing = false;

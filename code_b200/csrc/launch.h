@@ -10,6 +10,9 @@ struct Dev;
 
 // Process-wide switch of the vectorised horizontal sweeps (getm_set_vector_sweeps; on by default).
 bool vector_sweeps_enabled();
+// Process-wide switch of the FP32 working copies of the mixed step's micro steps
+// (getm_set_fp32_micro_steps; on by default).
+bool fp32_micro_steps_enabled();
 
 constexpr int RED_BLOCKS = 1184;  // 8 x 148 SMs
 constexpr int RED_THREADS = 256;
@@ -103,8 +106,12 @@ int run_build_masks(const Dev& d, cudaStream_t s, const int32_t* az, const int32
 enum {
   BC3_BF3D = 0, BC3_ZZ, BC3_IP, BC3_UUMOM, BC3_VVMOM, BC3_SIGMA, BC3_WW, BC3_UVADV_PREP_U, BC3_UVADV_PREP_V,
   BC3_STRESSES, BC3_EQSTATE, BC3_SLOW_TERMS, BC3_UVADV_PREP_UV, BC3_ZZ_LIN, BC3_IP_LIN,
-  BC3_IP_SW, BC3_IP_CF, BC3_SM_COLS, BC3_IP_SM
+  BC3_IP_SW, BC3_IP_CF, BC3_SM_COLS, BC3_IP_SM, BC3_EQSTATE_UNESCO, BC3_EQSTATE_JACKETT, BC3_GOTM_PARABOLIC,
+  BC3_SW_RADIATION, BC3_TEMP_SOURCE
 };
+// sealevel_nan_check sweep of the interior elevations (bc.cu, k_nan_sweep): cnt[0] +=
+// findings, cnt[1] = max(cnt[1], last loop-order index + 1); skipped while cnt[2] != 0
+int run_nan_sweep(const Dev& d, cudaStream_t s, const double* z, unsigned long long* cnt);
 template <class R3>
 struct Bc3;
 template <class R3>

@@ -83,6 +83,7 @@ _PROTOS = {
     "getm_tracer_content_f32": [P, P, P, P, P],
     "getm_check_3d_fields": [P, P, P, D, D, P],
     "getm_set_vector_sweeps": [I],
+    "getm_set_fp32_micro_steps": [I],
     "getm_timers_enable": [P, I],
     "getm_timers_reset": [P],
     "getm_timers_read": [P, I, P, P],
@@ -90,6 +91,19 @@ _PROTOS = {
     "getm_integrate_2d": [P, P, I],
     "getm_integrate_3d": [P, P, I],
     "getm_time_loop": [P, P, I, I],
+    "getm_bottom_friction": [P, P, I],
+    "getm_uv_advect": [P, P],
+    "getm_momentum": [P, P, I],
+    "getm_umomentum": [P, P],
+    "getm_vmomentum": [P, P],
+    "getm_update_2d_bdy": [P, P, I],
+    "getm_sealevel": [P, P, I],
+    "getm_depth_update": [P, P],
+    "getm_internal_pressure": [P, P],
+    "getm_do_eqstate": [P, P],
+    "getm_gotm": [P, P],
+    "getm_sw_radiation": [P, P],
+    "getm_sealevel_nan_check": [P, P, P, P, P],
 }
 _RESTYPES = {"getm_ctx_last_error": C.c_char_p, "getm_version": C.c_char_p, "getm_timer_name": C.c_char_p}
 NTIMERS = 16
@@ -110,6 +124,12 @@ def lib():
                 fn.restype = _RESTYPES.get(name, C.c_int)
             _lib = L
     return _lib
+
+
+def set_fp32_micro_steps(on: bool) -> bool:
+    """Process-wide choice for the mixed step's micro steps: FP32 working copies of the 2D fields
+    (the default) or the FP64 state arrays; returns the previous setting."""
+    return bool(lib().getm_set_fp32_micro_steps(1 if on else 0))
 
 
 def set_vector_sweeps(on: bool) -> bool:
@@ -326,6 +346,61 @@ class Context:
         """Micro steps n0..n0+count-1 of time_loop (integration.F90:98-172)."""
         self._check(self.L.getm_time_loop(self.h, C.byref(st.c), n0, count))
 
+    # the substeps of integrate_2d / integrate_3d, one by one (reference routine names)
+    def bottom_friction(self, st: "BcDevice", runtype: int):
+        """bottom_friction (bottom_friction.F90:8-250)."""
+        self._check(self.L.getm_bottom_friction(self.h, C.byref(st.c), runtype))
+
+    def uv_advect(self, st: "BcDevice"):
+        """uv_advect(U, V, DU, DV) (uv_advect.F90:8-310): UEx, VEx."""
+        self._check(self.L.getm_uv_advect(self.h, C.byref(st.c)))
+
+    def momentum(self, st: "BcDevice", n: int):
+        """momentum (momentum.F90:8-60): umomentum and vmomentum in alternating order."""
+        self._check(self.L.getm_momentum(self.h, C.byref(st.c), n))
+
+    def umomentum(self, st: "BcDevice"):
+        """umomentum (momentum.F90:69-223)."""
+        self._check(self.L.getm_umomentum(self.h, C.byref(st.c)))
+
+    def vmomentum(self, st: "BcDevice"):
+        """vmomentum (momentum.F90:232-386)."""
+        self._check(self.L.getm_vmomentum(self.h, C.byref(st.c)))
+
+    def update_2d_bdy(self, st: "BcDevice", loop: int):
+        """update_2d_bdy (update_2d_bdy.F90:8-186) with the context's open boundaries."""
+        self._check(self.L.getm_update_2d_bdy(self.h, C.byref(st.c), loop))
+
+    def sealevel(self, st: "BcDevice", loop: int):
+        """sealevel (sealevel.F90:8-163), with its NaN sweep when sealevel_check asks for one."""
+        self._check(self.L.getm_sealevel(self.h, C.byref(st.c), loop))
+
+    def depth_update(self, st: "BcDevice"):
+        """depth_update (depth_update.F90:8-148)."""
+        self._check(self.L.getm_depth_update(self.h, C.byref(st.c)))
+
+    def internal_pressure(self, st: "BcDevice"):
+        """do_internal_pressure (internal_pressure.F90:181-274) with the state's ip_method."""
+        self._check(self.L.getm_internal_pressure(self.h, C.byref(st.c)))
+
+    def do_eqstate(self, st: "BcDevice"):
+        """do_eqstate (eqstate.F90:94-261) with the state's eqstate_method."""
+        self._check(self.L.getm_do_eqstate(self.h, C.byref(st.c)))
+
+    def gotm(self, st: "BcDevice"):
+        """gotm (gotm.F90:96-163) with PARABOLIC_VISCOSITY (viscosity = 1; no-op otherwise)."""
+        self._check(self.L.getm_gotm(self.h, C.byref(st.c)))
+
+    def sw_radiation(self, st: "BcDevice"):
+        """The short-wave radiation profile rad of do_temperature (temperature.F90:452-465)."""
+        self._check(self.L.getm_sw_radiation(self.h, C.byref(st.c)))
+
+    def sealevel_nan_check(self, z):
+        """sealevel_nan_check (sealevel.F90:172-314): (count, (i, j) of the last finding or None)."""
+        n, i, j = C.c_int64(), C.c_int32(), C.c_int32()
+        self._check(self.L.getm_sealevel_nan_check(self.h, _ptr(z), C.byref(n), C.byref(i), C.byref(j)))
+        return int(n.value), ((int(i.value), int(j.value)) if n.value else None)
+
     def check_3d_fields(self, f, az, minval, maxval) -> int:
         st = C.c_int64()
         self._check(self.L.getm_check_3d_fields(self.h, _ptr(f), _ptr(az), minval, maxval, C.byref(st)))
@@ -353,8 +428,8 @@ def _mask(m):
 class BcState(C.Structure):
     """Mirror of getm_bc_state (include/getm_b200.h)."""
 
-    _fields_ = [("f2", P * 54), ("f3", P * 19), ("az", P), ("au", P), ("av", P), ("ax", P), ("par", D * 18),
-                ("ipar", C.c_int32 * 20), ("prec3d", C.c_int32)]
+    _fields_ = [("f2", P * 59), ("f3", P * 22), ("az", P), ("au", P), ("av", P), ("ax", P), ("par", D * 23),
+                ("ipar", C.c_int32 * 25), ("prec3d", C.c_int32)]
 
 
 class BcDevice:
@@ -380,11 +455,16 @@ class BcDevice:
         f3dt = self.t["f3_uu"].dtype
         self.prec = 8 if f3dt == torch.float64 else 4
         c = BcState()
+        # optional fields (S.OPTIONAL_F2 / OPTIONAL_F3) that a state does not hold cross as NULL
         for q, n in enumerate(S.F2_NAMES):
-            c.f2[q] = _ptr(self.t["f2_" + n])
+            t2 = self.t.get("f2_" + n)
+            assert t2 is not None or n in S.OPTIONAL_F2, n
+            c.f2[q] = None if t2 is None else _ptr(t2)
         for q, n in enumerate(S.F3_NAMES):
-            assert self.t["f3_" + n].dtype == f3dt
-            c.f3[q] = _ptr(self.t["f3_" + n])
+            t3 = self.t.get("f3_" + n)
+            assert t3 is not None or n in S.OPTIONAL_F3, n
+            assert t3 is None or t3.dtype == f3dt
+            c.f3[q] = None if t3 is None else _ptr(t3)
         c.az, c.au, c.av, c.ax = (_ptr(self.t[n]) for n in ("az", "au", "av", "ax"))
         for q, n in enumerate(S.PD_NAMES):
             c.par[q] = float(pd[n])
@@ -406,9 +486,11 @@ class BcDevice:
         from . import state as S
 
         for n in S.F2_NAMES:
-            case.f2[n][...] = self.t["f2_" + n].cpu().numpy()
+            if "f2_" + n in self.t:
+                case.f2[n][...] = self.t["f2_" + n].cpu().numpy()
         for n in S.F3_NAMES:
-            case.f3[n][...] = self.t["f3_" + n].cpu().numpy().astype(case.dtype3)
+            if "f3_" + n in self.t:
+                case.f3[n][...] = self.t["f3_" + n].cpu().numpy().astype(case.dtype3)
         for q, n in enumerate(S.PI_NAMES):
             case.pi[n] = int(self.c.ipar[q])
         return case

@@ -117,6 +117,12 @@ const char *getm_timer_name(int slot);
  * shared-memory tile sweeps everywhere (FP64 always does). Both give identical results. Returns
  * the previous setting. */
 int getm_set_vector_sweeps(int on);
+/* Process-wide choice for the mixed-precision step (no counterpart in the reference: a testing and
+ * accuracy switch). on != 0 (the default) runs the barotropic micro steps of getm_time_loop on FP32
+ * working copies of the 2D fields whenever the step has no open boundaries (elevation, Uint/Vint
+ * and the static depths stay FP64); on == 0 keeps the micro steps on the FP64 state arrays, as the
+ * plain step does. Returns the previous setting. */
+int getm_set_fp32_micro_steps(int on);
 /* Human-readable text of the last error on this context (never NULL). */
 const char *getm_ctx_last_error(const getm_ctx *ctx);
 const char *getm_version(void);
@@ -194,22 +200,36 @@ int getm_tracer_step_f32(getm_ctx *ctx, float dt, float *f, const float *uu, con
  * transport accumulation Uint/Vint and all vertical sums stay FP64). The table order is:
  *  f2:  z zo U V D DU DV UEx VEx fU fV ru rv ruu rvv Uint Vint Uinto Vinto SlUx SlVx Slru Slrv
  *       zub zvb zub0 zvb0 fwf H HU HV dry_z dry_u dry_v coru corv tausx tausy airp sseo ssen
- *       ssuo ssun ssvo ssvn Dn Dun Dvn rru rrv taubx tauby taub taus
- *  f3:  uu vv ww ho hn huo hun hvo hvn uuEx vvEx idpdx idpdy T S rho buoy num nuh
+ *       ssuo ssun ssvo ssvn Dn Dun Dvn rru rrv taubx tauby taub taus swr shf A g1 g2
+ *  f3:  uu vv ww ho hn huo hun hvo hvn uuEx vvEx idpdx idpdy T S rho buoy num nuh rad tke eps
  *  par: dtm dt cnpar min_depth crit_depth g rho_0 kappa avmmol avmolt avmols T0 S0 dtr0 dsr0
- *       ip_fac temp_AH salt_AH
+ *       ip_fac temp_AH salt_AH avmback avhback cp swr_bot_refl_frac swr_min_bot_frac
  *  ipar: M MM runtype vel2d_adv_split vel2d_adv_hor vel3d_adv_split vel3d_adv_hor
  *       vel3d_adv_ver temp_adv_split temp_adv_hor temp_adv_ver salt_adv_split salt_adv_hor
  *       salt_adv_ver adv_ver_iterations ufirst2d ufirst3d calc_temp calc_salt ip_method
+ *       viscosity eqstate_method sealevel_check radiation nan_warned
  * ufirst2d / ufirst3d are the SAVEd alternation switches of momentum.F90:33 (initially 0) and
  * m3d.F90:504 (initially 1); the calls update them in the host-side struct. ip_method selects the
  * internal pressure gradient (internal_pressure.F90:80, 149-168): 1 = BLUMBERG_MELLOR,
  * 2 = BLUMBERG_MELLOR_LIN, 4 = SONG_WRIGHT, 5 = CHU_FAN, 6 = SHCHEPETKIN_MCWILLIAMS; 3 and 7
- * return GETM_ERR_UNSUPPORTED, other values GETM_ERR_ARG. */
-#define GETM_NF2 54
-#define GETM_NF3 19
-#define GETM_NPD 18
-#define GETM_NPI 20
+ * return GETM_ERR_UNSUPPORTED, other values GETM_ERR_ARG.
+ * viscosity: 0 = CONSTANT_VISCOSITY (num, nuh as given), 1 = PARABOLIC_VISCOSITY (gotm.F90:131-143:
+ * the profile from taub after stresses_3d, plus avmback / avhback; tke and eps receive the
+ * profiles when not NULL). eqstate_method (eqstate.F90:31): 1 linear, 2 UNESCO80, 3 Jackett et al.
+ * 2006 at zero pressure. radiation: 0 = do_temperature without sources (the reference with swr =
+ * shf = 0), 1 = the short-wave radiation profile into rad (temperature.F90:452-465, from swr and
+ * the attenuation A, g1, g2) and its absorption plus the surface heat flux shf as sources of the
+ * temperature diffusion (temperature.F90:469-525, cp the heat capacity of parameters.F90:23, bottom
+ * reflection when swr_bot_refl_frac > 0). sealevel_check (m2d.F90:82): every |sealevel_check|
+ * micro steps the elevations are swept for NaN (sealevel_nan_check, sealevel.F90:172-314) until the
+ * first finding, which sets nan_warned (the routine's SAVEd have_warned); sealevel_check > 0 makes a
+ * finding an error: the call that made it returns GETM_ERR_CHECK (getm_time_loop at its end, after
+ * finishing its steps; the reference stops at once). swr, shf, A, g1, g2 and rad may be NULL when
+ * radiation = 0, tke and eps may always be NULL. */
+#define GETM_NF2 59
+#define GETM_NF3 22
+#define GETM_NPD 23
+#define GETM_NPI 25
 typedef struct getm_bc_state {
   double *f2[GETM_NF2];
   void *f3[GETM_NF3];
@@ -224,15 +244,53 @@ typedef struct getm_bc_state {
  * depth_update. Closed boundaries (no update_2d_bdy), Am <= 0, An_method = 0, no residual. */
 int getm_integrate_2d(getm_ctx *ctx, getm_bc_state *st, int loop);
 /* integrate_3d (src/3d/m3d.F90:422-636): one baroclinic macro step for runtype 4 with sigma
- * coordinates, linear equation of state, Blumberg-Mellor internal pressure and prescribed
- * num/nuh: start_macro, bottom_friction_3d, internal pressure, uu/vv_momentum_3d, coordinates,
- * ww_momentum_3d, uv_advect_3d, stresses_3d, do_temperature / do_salinity (advection + implicit
- * vertical diffusion, no radiation / surface fluxes), do_eqstate, slow_bottom_friction,
- * uv_advect of Uint/Vint, slow_terms and stop_macro. */
+ * coordinates: start_macro, bottom_friction_3d, internal pressure (ip_method), uu/vv_momentum_3d,
+ * coordinates, ww_momentum_3d, uv_advect_3d, stresses_3d, gotm (PARABOLIC_VISCOSITY when
+ * viscosity = 1), do_temperature / do_salinity (advection + implicit vertical diffusion; with
+ * radiation = 1 the short-wave and surface heat-flux sources of temperature), do_eqstate
+ * (eqstate_method), slow_bottom_friction, uv_advect of Uint/Vint, slow_terms and stop_macro. */
 int getm_integrate_3d(getm_ctx *ctx, getm_bc_state *st, int n);
 /* The micro-step loop of time_loop (src/getm/integration.F90:98-172) for n = n0..n0+count-1:
  * integrate_2d every step, integrate_3d when mod(n, M) == 0. */
 int getm_time_loop(getm_ctx *ctx, getm_bc_state *st, int n0, int count);
+
+/* ---- the substeps of the mode-split step, one by one ------------------------------------
+ * Each is one reference subroutine on the state table (same validation as getm_integrate_2d; the
+ * 2D arithmetic of the 2D substeps is FP64, as in the plain step), for a host that keeps its own
+ * integrate_2d / integrate_3d and swaps single calls. */
+/* bottom_friction(runtype) (src/2d/bottom_friction.F90:8-250) */
+int getm_bottom_friction(getm_ctx *ctx, getm_bc_state *st, int runtype);
+/* uv_advect(U,V,DU,DV) (src/2d/uv_advect.F90:8-310): UEx, VEx */
+int getm_uv_advect(getm_ctx *ctx, getm_bc_state *st);
+/* momentum(n,tausx,tausy,airp) (src/2d/momentum.F90:8-60): umomentum and vmomentum in the order
+ * of the SAVEd switch ufirst2d, which the call toggles; tausx, tausy, airp are the state's */
+int getm_momentum(getm_ctx *ctx, getm_bc_state *st, int n);
+/* umomentum(tausx,airp) (src/2d/momentum.F90:69-223): U, its mirror_bdy_2d copies, fV */
+int getm_umomentum(getm_ctx *ctx, getm_bc_state *st);
+/* vmomentum(tausy,airp) (src/2d/momentum.F90:232-386): V, its mirror_bdy_2d copies, fU */
+int getm_vmomentum(getm_ctx *ctx, getm_bc_state *st);
+/* update_2d_bdy(loop,bdy2d_ramp) (src/2d/update_2d_bdy.F90:8-186) with the context's open
+ * boundaries (no-op without) */
+int getm_update_2d_bdy(getm_ctx *ctx, getm_bc_state *st, int loop);
+/* sealevel(loop) (src/2d/sealevel.F90:8-163): zo = z, the elevation update, and the NaN sweep of
+ * sealevel_check (GETM_ERR_CHECK for sealevel_check > 0 and a finding) */
+int getm_sealevel(getm_ctx *ctx, getm_bc_state *st, int loop);
+/* depth_update() (src/2d/depth_update.F90:8-148): D, DU, DV and the drying factors */
+int getm_depth_update(getm_ctx *ctx, getm_bc_state *st);
+/* do_internal_pressure() (src/3d/internal_pressure.F90:181-274): idpdx, idpdy by ip_method */
+int getm_internal_pressure(getm_ctx *ctx, getm_bc_state *st);
+/* do_eqstate() (src/3d/eqstate.F90:94-261): rho and buoy by eqstate_method */
+int getm_do_eqstate(getm_ctx *ctx, getm_bc_state *st);
+/* gotm() (src/3d/gotm.F90:96-163) with PARABOLIC_VISCOSITY when viscosity = 1 (no-op for 0) */
+int getm_gotm(getm_ctx *ctx, getm_bc_state *st);
+/* the short-wave radiation profile rad of do_temperature (src/3d/temperature.F90:452-465) */
+int getm_sw_radiation(getm_ctx *ctx, getm_bc_state *st);
+/* sealevel_nan_check() (src/2d/sealevel.F90:172-314) on a device elevation field z (E2DFIELD,
+ * FP64): the number of interior points that are not below HUGE (NaN, +Inf, HUGE; -Inf is not
+ * counted, nor are halo points) into the HOST *num_nan, and the last of them in the reference's
+ * loop order into *inan, *jnan (reference indices; may be NULL; 0 when none). Synchronises. */
+int getm_sealevel_nan_check(getm_ctx *ctx, const double *z, int64_t *num_nan, int32_t *inan,
+                            int32_t *jnan);
 
 /* ---- open boundaries ------------------------------------------------------------------ */
 /* The open-boundary description of bdy_spec.F90 (domain.F90:263-280 marks the points az = 2):
