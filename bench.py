@@ -48,6 +48,36 @@ STAGE_WORDS = {"adv_split_u": 8, "adv_split_v": 8, "adv_split_w": 7, "tracer_vdi
 TRAFFIC_PER_CELL_F32 = {"adv_split_u": 28.01, "adv_split_v": 31.05, "adv_split_w": 20.94, "tracer_vdiff": 23.78}
 
 
+ERR_FIELDS = ("f3_T", "f3_S", "f3_uu", "f3_vv", "f2_z", "f2_U", "f2_V")
+
+
+def field_errors(got: dict, ref: dict, az) -> dict:
+    """Per field, the largest and the RMS difference of `got` from `ref` over the wet interior cells
+    (az == 1; levels 1..kmax of 3D fields), relative to the largest magnitude of the reference field
+    and to its range (max - min) there."""
+    import torch
+
+    wet2 = az == 1
+    out = {}
+    for name, b in ref.items():
+        a = got[name].double()
+        b = b.double()
+        if b.dim() == 3:
+            m = wet2[None].expand_as(b).clone()
+            m[0] = False
+        else:
+            m = wet2
+        bb, d = b[m], (a - b).abs()[m]
+        scale = float(bb.abs().max())
+        rng = float(bb.max() - bb.min())
+        mx, rms = float(d.max()), float(d.pow(2).mean().sqrt())
+        out[name[3:]] = {"max": mx / max(scale, 1e-300), "rms": rms / max(scale, 1e-300),
+                         "max_range": mx / max(rng, 1e-300), "rms_range": rms / max(rng, 1e-300)}
+        del m, bb, d
+    torch.cuda.empty_cache()
+    return out
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -60,16 +90,25 @@ def parse():
     ap.add_argument("--M", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variants", default="fp64,mixed")
+    ap.add_argument("--err-steps", type=int, default=200,
+                    help="macro steps after which the mixed variant's error against the FP64 variant is stated "
+                         "(both variants run on to that step after the timing; the large domain's 200 steps)")
     ap.add_argument("--adj-steps", type=int, default=20, help="tracer steps of the adjoint measurement (0 = skip)")
     ap.add_argument("--adj-every", type=int, default=10, help="checkpoint interval of the adjoint")
     ap.add_argument("--accuracy", type=int, default=0, metavar="STEPS",
                     help="run the mixed-precision accuracy configuration (the 'rotation' recipe: flat 20 m, "
                          "dx = 500 m, closed, solid-body rotation and a temperature anomaly; --nx/--ny/--kmax) for "
                          "STEPS macro steps in FP64 and in the mixed variant and print the per-field errors")
+    ap.add_argument("--t-background", type=float, default=0.0,
+                    help="accuracy configuration: temperature the tracer blob sits on (0: the tracer-rotation "
+                         "configuration's tracer, a unit blob plus noise on zero)")
     ap.add_argument("--configs", action="store_true",
                     help="time the smaller configurations: the 128x128x20 tracer rotation (200 steps) and the "
                          "512x512x30 tidal shelf (100 macro steps), GPU FP64 / mixed and the CPU oracle on the "
                          "host cores (a 5-macro-step sample for the shelf); one JSON line")
+    ap.add_argument("--cpu-sizes", default="", metavar="N,N,...",
+                    help="time the CPU oracle (the reported CPU baseline) on the islands recipe at each NxN size "
+                         "(kmax and M of the workload) and print its rate per size; one JSON line")
     ap.add_argument("--tile-sweeps", action="store_true",
                     help="use the shared-memory tile kernels for every horizontal sweep (comparison)")
     ap.add_argument("--tracer-adjoint", action="store_true",
@@ -168,11 +207,22 @@ def oracle_sample(nx, ny, kmax, M):
     return S.baroclinic_case(nx=nx, ny=ny, kmax=kmax, recipe="islands", land=0.3, M=M, dt3=60.0, seed=6)
 
 
+def cpu_build():
+    """Select the oracle build tuned for this host's CPU (-march=native, built here with the
+    system g++), falling back to the portable build; returns the flags of the build in use."""
+    import oracle
+
+    oracle.use_native_build()
+    return oracle.BUILD_FLAGS[oracle.variant]
+
+
 def run_reference(args, world, rank):
     """CPU restatement (oracle) on a bounded sample of the workload, all host threads."""
     if rank != 0:
         return
     import oracle
+
+    flags = cpu_build()
 
     snx = min(args.nx, 256)
     sny = min(args.ny, 256)
@@ -196,7 +246,7 @@ def run_reference(args, world, rank):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "nx": args.nx, "ny": args.ny, "kmax": args.kmax, "M": M,
                    "sample": f"{snx}x{sny}x{args.kmax} islands domain per step"},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "build": flags,
                          "sample": f"oracle FP64 mode-split step on {snx}x{sny}x{args.kmax}, {args.steps} macro steps "
                                    f"after {args.warmup} warm-up"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -206,6 +256,7 @@ def run_reference(args, world, rank):
 def cpu_baseline_sample(args):
     import oracle
 
+    flags = cpu_build()
     snx, sny = min(args.nx, 256), min(args.ny, 256)
     c = oracle_sample(snx, sny, args.kmax, args.M)
     oracle.bc_steps(c, 1, args.M)
@@ -218,9 +269,35 @@ def cpu_baseline_sample(args):
         if el > 10.0 or steps >= 20:
             break
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return {"value": snx * sny * args.kmax * steps / el, "unit": UNIT, "cores": cores, "kind": "port",
+    return {"value": snx * sny * args.kmax * steps / el, "unit": UNIT, "cores": cores, "kind": "port", "build": flags,
             "sample": f"oracle FP64 mode-split step on {snx}x{sny}x{args.kmax} (islands), {steps} macro steps "
                       f"({el:.1f} s)"}
+
+
+def run_cpu_sizes(args):
+    """Per-cell rate of the CPU oracle (the timed baseline) against the sample size: the islands
+    recipe at each size of --cpu-sizes (kmax and M of the workload), one warm-up macro step, then
+    timed macro steps for at least 10 s (at least one)."""
+    import oracle
+
+    flags = cpu_build()
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    rows = []
+    for n in (int(x) for x in args.cpu_sizes.split(",")):
+        c = oracle_sample(n, n, args.kmax, args.M)
+        oracle.bc_steps(c, 1, args.M)
+        k, t0, el = 1 + args.M, time.perf_counter(), 0.0
+        steps = 0
+        while steps < 1 or el < 10.0:
+            oracle.bc_steps(c, k, args.M)
+            k += args.M
+            steps += 1
+            el = time.perf_counter() - t0
+        rows.append({"size": f"{n}x{n}x{args.kmax}", "cells": n * n * args.kmax, "macro_steps": steps,
+                     "s_per_step": el / steps, "value": n * n * args.kmax * steps / el})
+        del c
+    print(json.dumps({"cpu_oracle_rate_by_size": rows, "unit": UNIT, "cores": cores, "build": flags,
+                      "workload": f"islands recipe, kmax = {args.kmax}, M = {args.M}"}), flush=True)
 
 
 def run_tracer_adjoint(args):
@@ -345,7 +422,7 @@ def run_accuracy(args):
     from code_b200.getm import BcDevice, Context
 
     c = S.baroclinic_case(nx=args.nx, ny=args.ny, kmax=args.kmax, recipe="rotation", dx=500.0, M=args.M, dt3=60.0,
-                          seed=3)
+                          seed=3, t_background=args.t_background, t_noise=1e-3)
     res = {}
     t0 = time.time()
     for key, dt in (("fp64", torch.float64), ("mixed", torch.float32)):
@@ -354,23 +431,16 @@ def run_accuracy(args):
         st = BcDevice(c, dtype3=dt)
         ctx.time_loop(st, 1, args.M * args.accuracy)
         torch.cuda.synchronize()
-        res[key] = {n: st.t[n].double() for n in ("f2_z", "f2_U", "f2_V", "f3_uu", "f3_vv", "f3_T", "f3_S")}
+        res[key] = {n: st.t[n].clone() for n in ERR_FIELDS}
+        az = st.t["az"]
         ctx.close()
         del st
-    err = {}
-    for n in res["fp64"]:
-        a, b = res["fp64"][n], res["mixed"][n]
-        scale = float(a.abs().max())
-        d = (a - b).abs()
-        at = np.unravel_index(int(d.argmax()), tuple(d.shape))
-        dn = d.flatten().cpu().numpy()
-        err[n[3:]] = {"max": float(d.max()) / scale, "rms": float(d.pow(2).mean().sqrt()) / scale,
-                      "p99_9": float(np.percentile(dn, 99.9)) / scale, "argmax": [int(x) for x in at],
-                      "shape": list(d.shape)}
+    err = field_errors(res["mixed"], res["fp64"], az)
     print(json.dumps({"workload": f"mixed-precision accuracy: rotation recipe {args.nx}x{args.ny}x{args.kmax}, "
-                                  f"M = {args.M}, {args.accuracy} macro steps",
-                      "relative_to": "max |field| of the FP64 run", "errors": err,
-                      "wall_s": time.time() - t0}), flush=True)
+                                  f"M = {args.M}, {args.accuracy} macro steps, tracer: Gaussian blob of amplitude 1 "
+                                  f"plus uniform noise of 1e-3 on {args.t_background} C",
+                      "relative_to": "max: max |field| of the FP64 run; range: its max - min; wet interior cells",
+                      "errors": err, "wall_s": time.time() - t0}), flush=True)
 
 
 def main():
@@ -394,6 +464,10 @@ def main():
     if args.configs:
         if rank == 0:
             run_configs(args)
+        return
+    if args.cpu_sizes:
+        if rank == 0:
+            run_cpu_sizes(args)
         return
     import torch
     import torch.distributed as dist
@@ -454,14 +528,15 @@ def main():
     # stated error of the mixed variant against the FP64 run after the same number of steps
     err = None
     if "fp64" in variants and "mixed" in variants and variants["fp64"]["n"] == variants["mixed"]["n"]:
-        err = {"steps": (variants["fp64"]["n"] - 1) // M, "relative_to": "max |field| of the FP64 run"}
-        for name in ("f3_T", "f3_S", "f3_uu", "f3_vv", "f2_z", "f2_U", "f2_V"):
-            a = variants["fp64"]["st"].t[name]
-            b = variants["mixed"]["st"].t[name].double()
-            scale = float(a.abs().max())
-            d = (a - b).abs()
-            err[name[3:]] = {"max": float(d.max()) / max(scale, 1e-300),
-                             "rms": float(d.pow(2).mean().sqrt()) / max(scale, 1e-300)}
+        # both variants on to the stated number of macro steps (outside the timed region)
+        while (variants["fp64"]["n"] - 1) // M < args.err_steps:
+            macro_step("fp64")
+            macro_step("mixed")
+        torch.cuda.synchronize()
+        err = {"steps": (variants["fp64"]["n"] - 1) // M,
+               "relative_to": "max: max |field| of the FP64 run; range: its max - min; wet interior cells"}
+        err.update(field_errors({n: variants["mixed"]["st"].t[n] for n in ERR_FIELDS},
+                                {n: variants["fp64"]["st"].t[n] for n in ERR_FIELDS}, variants["fp64"]["st"].t["az"]))
     head = "mixed" if "mixed" in variants else "fp64"
     v = variants[head]
     # per-stage device timers over K more steps of the headline variant (dominant kernel roofline)

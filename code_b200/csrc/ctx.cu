@@ -7,6 +7,8 @@
 #include <vector>
 
 #include "common.cuh"
+#include <algorithm>
+
 #include "launch.h"
 
 #include "ctx_internal.h"
@@ -289,6 +291,58 @@ static int content_api(getm_ctx* ctx, const R* f, const R* h, const int32_t* az,
   return GETM_OK;
 }
 
+namespace gb {
+
+// Rows [r0, r0+nrows) (array rows, i.e. j - (jmin-2)) of nk consecutive levels of a field of elem
+// bytes, copied to or from a packed buffer laid out [level][row][i] (the ni elements of a row are
+// contiguous in both). 16-byte words where the whole block allows it, else elements.
+template <class W>
+__global__ void k_rows_copy(const Dev d, char* f, char* buf, int r0, int nrows, int nk, int words_per_row,
+                            long long row_stride_w, long long level_stride_w, int to_buf) {
+  const long long n = (long long)words_per_row * nrows * nk;
+  W* fw = reinterpret_cast<W*>(f);
+  W* bw = reinterpret_cast<W*>(buf);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const long long q = t % words_per_row, rk = t / words_per_row;
+    const long long r = rk % nrows, k = rk / nrows;
+    const long long fo = k * level_stride_w + (r0 + r) * row_stride_w + q;
+    if (to_buf) bw[t] = fw[fo];
+    else fw[fo] = bw[t];
+  }
+}
+
+}  // namespace gb
+
+static int rows_copy(getm_ctx* ctx, void* f, int elem_bytes, int nk, int j_first, int nrows, void* buf, int to_buf) {
+  using namespace gb;
+  if (!ctx || !f || !buf || (elem_bytes != 4 && elem_bytes != 8) || nk < 1 || nrows < 1) return GETM_ERR_ARG;
+  const Dev& d = ctx->dev;
+  const int r0 = j_first - (d.jmin - HALO);
+  if (r0 < 0 || r0 + nrows > d.nj() || nk > d.kmax + 1)
+    return fail(ctx, GETM_ERR_ARG, "halo rows: rows or levels outside the field");
+  const long long row_bytes = (long long)d.ni() * elem_bytes;
+  const long long sj_b = d.sj * elem_bytes, sk_b = d.sk * elem_bytes;
+  const bool w16 = row_bytes % 16 == 0 && sj_b % 16 == 0 && sk_b % 16 == 0 &&
+                   reinterpret_cast<uintptr_t>(f) % 16 == 0 && reinterpret_cast<uintptr_t>(buf) % 16 == 0;
+  const int wb = w16 ? 16 : elem_bytes;
+  const long long n = row_bytes / wb * nrows * nk;
+  const int blocks = (int)std::min<long long>((n + 255) / 256, 4 * 148);
+  TimerScope ts(ctx, GETM_TIM_COPY);
+  char* fc = static_cast<char*>(f);
+  char* bc = static_cast<char*>(buf);
+  if (wb == 16)
+    k_rows_copy<int4><<<blocks, 256, 0, ctx->stream>>>(d, fc, bc, r0, nrows, nk, (int)(row_bytes / 16), sj_b / 16,
+                                                       sk_b / 16, to_buf);
+  else if (wb == 8)
+    k_rows_copy<long long><<<blocks, 256, 0, ctx->stream>>>(d, fc, bc, r0, nrows, nk, (int)(row_bytes / 8), sj_b / 8,
+                                                            sk_b / 8, to_buf);
+  else
+    k_rows_copy<int><<<blocks, 256, 0, ctx->stream>>>(d, fc, bc, r0, nrows, nk, (int)(row_bytes / 4), sj_b / 4,
+                                                      sk_b / 4, to_buf);
+  GB_TRY(cudaGetLastError(), "halo rows");
+  return GETM_OK;
+}
+
 extern "C" {
 
 const char* getm_version(void) { return "getm-b200 0.1 (sm_100a)"; }
@@ -532,6 +586,14 @@ int getm_tracer_content(getm_ctx* ctx, const double* f, const double* h, const i
 
 int getm_tracer_content_f32(getm_ctx* ctx, const float* f, const float* h, const int32_t* az, double* out) {
   return content_api<float>(ctx, f, h, az, out);
+}
+
+int getm_halo_pack(getm_ctx* ctx, const void* f, int elem_bytes, int nk, int j_first, int nrows, void* buf) {
+  return rows_copy(ctx, const_cast<void*>(f), elem_bytes, nk, j_first, nrows, buf, 1);
+}
+
+int getm_halo_unpack(getm_ctx* ctx, void* f, int elem_bytes, int nk, int j_first, int nrows, const void* buf) {
+  return rows_copy(ctx, f, elem_bytes, nk, j_first, nrows, const_cast<void*>(buf), 0);
 }
 
 int getm_check_3d_fields(getm_ctx* ctx, const double* f, const int32_t* az, double minval, double maxval,

@@ -104,6 +104,8 @@ _PROTOS = {
     "getm_gotm": [P, P],
     "getm_sw_radiation": [P, P],
     "getm_sealevel_nan_check": [P, P, P, P, P],
+    "getm_halo_pack": [P, P, I, I, I, I, P],
+    "getm_halo_unpack": [P, P, I, I, I, I, P],
 }
 _RESTYPES = {"getm_ctx_last_error": C.c_char_p, "getm_version": C.c_char_p, "getm_timer_name": C.c_char_p}
 NTIMERS = 16
@@ -400,6 +402,17 @@ class Context:
         n, i, j = C.c_int64(), C.c_int32(), C.c_int32()
         self._check(self.L.getm_sealevel_nan_check(self.h, _ptr(z), C.byref(n), C.byref(i), C.byref(j)))
         return int(n.value), ((int(i.value), int(j.value)) if n.value else None)
+
+    # halo rows of a slab decomposition (update_3d_halo / update_2d_halo of the parallel build)
+    def halo_pack(self, f, j_first: int, nrows: int, buf):
+        """Rows j_first..j_first+nrows-1 of every level of f (3D, or 2D) into the packed buffer buf."""
+        nk = f.shape[0] if f.dim() == 3 else 1
+        self._check(self.L.getm_halo_pack(self.h, _ptr(f), f.element_size(), nk, j_first, nrows, _ptr(buf)))
+
+    def halo_unpack(self, f, j_first: int, nrows: int, buf):
+        """The packed buffer buf into rows j_first..j_first+nrows-1 of every level of f."""
+        nk = f.shape[0] if f.dim() == 3 else 1
+        self._check(self.L.getm_halo_unpack(self.h, _ptr(f), f.element_size(), nk, j_first, nrows, _ptr(buf)))
 
     def check_3d_fields(self, f, az, minval, maxval) -> int:
         st = C.c_int64()

@@ -157,12 +157,14 @@ def _eqstate(c: BcCase):
 
 
 def baroclinic_case(nx=32, ny=24, kmax=8, recipe="shelf", dx=1000.0, M=20, dt3=60.0, seed=2, dtype3=np.float64,
-                    land=0.0, hmin=5.0, hmax=150.0, nu_max=1e-2, latitude=54.0, bdy=None) -> BcCase:
+                    land=0.0, hmin=5.0, hmax=150.0, nu_max=1e-2, latitude=54.0, bdy=None, t_background=15.0,
+                    t_noise=0.0) -> BcCase:
     """Seeded initial state of the mode-split step, closed basin.
 
     recipe 'shelf': H = 10 + 190*0.5*(1+tanh((x-x0)/L)), L = 20 cells, x0 = nx/2.
     recipe 'flat':  H = 20 m.
-    recipe 'rotation': H = 20 m, solid-body rotation and a temperature anomaly (see _rotation_start).
+    recipe 'rotation': H = 20 m, solid-body rotation and a temperature anomaly (see _rotation_start)
+      of 1 C on t_background, plus seeded uniform noise of amplitude t_noise.
     recipe 'islands': H = hmin + (hmax-hmin)*(field-p)/(max-p) on wet cells of a Gaussian-smoothed
       noise field (sigma = 40 cells, scaled with the grid), land where field < its `land` quantile.
     Stratification: T from 20 C (surface) to 8 C (bottom) linear in depth plus N(0, 0.1) noise,
@@ -174,15 +176,16 @@ def baroclinic_case(nx=32, ny=24, kmax=8, recipe="shelf", dx=1000.0, M=20, dt3=6
     c, rng = _baroclinic_2d(nx, ny, kmax, recipe, dx, M, dt3, seed, dtype3, land, hmin, hmax, latitude, True, bdy)
     _baroclinic_3d_numpy(c, rng, nu_max)
     if recipe == "rotation":
-        _rotation_start(c)
+        _rotation_start(c, background=t_background, noise=t_noise, seed=seed)
     return c
 
 
-def _rotation_start(c: BcCase, umax=0.5, sigma_cells=8.0):
+def _rotation_start(c: BcCase, umax=0.5, sigma_cells=8.0, background=15.0, noise=0.0, seed=3):
     """recipe 'rotation' (flat 20 m): solid-body rotation of the whole water column (the discrete
     curl of psi = 0.5*omega*min(r,R)^2 at X points, R = nx/2 cells, omega = umax/R; depth-uniform
     velocity, so uu = u*hun, U = sum of uu) and a temperature anomaly of 1 C (Gaussian, sigma =
-    sigma_cells) on 15 C at (0.3 nx, 0.5 ny); S = 35."""
+    sigma_cells) on `background` C at (0.3 nx, 0.5 ny), plus uniform noise in [-noise, noise]
+    (numpy default_rng(seed + 1000)); S = 35."""
     g = c.grid
     f2, f3 = c.f2, c.f3
     dx = g.dx
@@ -211,7 +214,9 @@ def _rotation_start(c: BcCase, umax=0.5, sigma_cells=8.0):
     s = sigma_cells * dx
     blob = np.exp(-((xT[None, :] - 0.3 * g.nx * dx) ** 2 + (yT[:, None] - 0.5 * g.ny * dx) ** 2) / (2 * s * s))
     wet3 = (c.az >= 1)[None]
-    T = 15.0 + blob[None] + np.zeros(g.shape3())
+    T = background + blob[None] + np.zeros(g.shape3())
+    if noise > 0:
+        T = T + np.random.default_rng(seed + 1000).uniform(-noise, noise, g.shape3())
     S = np.full(g.shape3(), 35.0)
     T[0] = 0.0
     S[0] = 0.0

@@ -319,6 +319,20 @@ int getm_set_open_boundaries(getm_ctx *ctx, const getm_bdy *bdy);
  * npoints values each (data_u / data_v may be NULL); switches off harmonic data. */
 int getm_set_bdy_data(getm_ctx *ctx, const double *data, const double *data_u, const double *data_v);
 
+/* ---- halo rows of a slab decomposition ---------------------------------------------------- */
+/* The row exchange of the reference's parallel build (update_3d_halo / update_2d_halo,
+ * src/futils/halo_mpi.F90:376-558) for a domain cut into slabs of rows (a 1D decomposition in j):
+ * a rank sends its first and last two interior rows to its neighbours, which write them into their
+ * halo rows. getm_halo_pack copies the rows j_first .. j_first+nrows-1 (reference indices of the
+ * context's domain) of the levels 0 .. nk-1 of a field with elem_bytes-byte elements (4 or 8;
+ * nk = 1 for a 2D field) into the packed device buffer buf, laid out [level][row][i];
+ * getm_halo_unpack writes such a buffer back into those rows. The transfer between ranks is the
+ * caller's (NCCL send/recv, or a device copy between two slabs of one process). */
+int getm_halo_pack(getm_ctx *ctx, const void *f, int elem_bytes, int nk, int j_first, int nrows,
+                   void *buf);
+int getm_halo_unpack(getm_ctx *ctx, void *f, int elem_bytes, int nk, int j_first, int nrows,
+                     const void *buf);
+
 /* ---- adjoint of the tracer step ---------------------------------------------------------- */
 /* No counterpart in the reference. The tracer step of getm_tracer_step (HALFSPLIT advection,
  * split schemes, adv_ver_iterations = 1, then implicit vertical diffusion) is differentiated in

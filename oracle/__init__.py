@@ -19,7 +19,11 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_NATIVE_PATH = os.path.join(_HERE, "_build", "liboracle_native.so")
 _lib = None
+BUILD_FLAGS = {"portable": "g++ -O3 -march=x86-64-v2 -fopenmp -ffp-contract=off",
+               "native": "g++ -O3 -march=native -fopenmp -ffp-contract=off"}
+variant = "portable"  # which build lib() loads
 
 
 class OrDom(C.Structure):
@@ -37,12 +41,30 @@ def build(force: bool = False) -> str:
     return _LIB_PATH
 
 
+def use_native_build() -> bool:
+    """Build (with the machine's own g++) and select the -march=native oracle for timing on this
+    host's cores; returns False, keeping the portable build, if that build fails. Call before the
+    first oracle routine runs."""
+    global variant
+    if _lib is not None:
+        return variant == "native"
+    try:
+        # always rebuilt (-B): a library tuned for another machine's CPU must not be reused
+        subprocess.check_call(["make", "-s", "-B", "-C", _HERE, "native"], stdout=subprocess.DEVNULL,
+                              stderr=subprocess.DEVNULL)
+    except (OSError, subprocess.CalledProcessError):
+        return False
+    variant = "native"
+    return True
+
+
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(_LIB_PATH):
+        path = _NATIVE_PATH if variant == "native" else _LIB_PATH
+        if not os.path.exists(path):
             build()
-        _lib = C.CDLL(_LIB_PATH)
+        _lib = C.CDLL(path)
         _declare(_lib)
     return _lib
 

@@ -262,8 +262,8 @@ static int bc_call(const or_dom* o, or_bc* s, int which, int arg) {
                              st.f2[gor::DU], st.f2[gor::DV], st.ipar[gor::I_VEL2D_SPLIT], st.ipar[gor::I_VEL2D_HOR],
                              st.f2[gor::UEX], st.f2[gor::VEX]);
       break;
-    case BC_UMOMENTUM: gor::umomentum(d, st.f2, st.au, st.av, st.par); break;
-    case BC_VMOMENTUM: gor::vmomentum(d, st.f2, st.au, st.av, st.par); break;
+    case BC_UMOMENTUM: gor::umomentum(d, st.f2, st.au, st.av, st.par, st.bdy, st.az); break;
+    case BC_VMOMENTUM: gor::vmomentum(d, st.f2, st.au, st.av, st.par, st.bdy, st.az); break;
     case BC_SEALEVEL: gor::sealevel(d, st.f2, st.az, st.par); break;
     case BC_DEPTH_UPDATE: gor::depth_update(d, st.f2, st.az, st.au, st.av, st.par); break;
     case BC_START_MACRO: gor::start_macro(d, st.f2, st.par, st.ipar[gor::I_M]); break;

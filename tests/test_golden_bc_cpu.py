@@ -134,3 +134,26 @@ def test_sealevel_check_stops_like_reference():
                 stopped = True
             assert stopped == stops, (q, chk)
             assert c.pi["nan_warned"] == (1 if int(g[f"count{q}"]) > 0 else 0), (q, chk)
+
+
+def test_native_oracle_build_is_bit_exact():
+    """The -march=native build of the oracle (the one the benchmark times on the host cores) gives
+    the reference's bits on every mode-split fixture, like the portable build (no contraction, no
+    reassociation in either). Run in a child process, which selects that build."""
+    import subprocess
+    import sys
+
+    code = (
+        "import sys, numpy as np\n"
+        "sys.path[:0] = ['.', 'tests']\n"
+        "import oracle\n"
+        "assert oracle.use_native_build()\n"
+        "from test_golden_bc_cpu import GOLDS, gold_names, load_case\n"
+        "for name, path in GOLDS.items():\n"
+        "    g = dict(np.load(path)); c = load_case(g); oracle.bc_steps(c, 1, 8)\n"
+        "    for k in gold_names(g, 'f2'): assert np.array_equal(c.f2[k], g['out_f2_' + k], equal_nan=True), (name, k)\n"
+        "    for k in gold_names(g, 'f3'): assert np.array_equal(c.f3[k], g['out_f3_' + k], equal_nan=True), (name, k)\n"
+        "print('ok')\n")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and "ok" in r.stdout, r.stderr[-2000:]
