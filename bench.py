@@ -90,6 +90,8 @@ def parse():
     ap.add_argument("--M", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variants", default="fp64,mixed")
+    ap.add_argument("--plain-fp32-tracers", dest="compensated", action="store_false",
+                    help="mixed step with plain FP32 storage of T and S (no compensation arrays Tlo, Slo)")
     ap.add_argument("--err-steps", type=int, default=200,
                     help="macro steps after which the mixed variant's error against the FP64 variant is stated "
                          "(both variants run on to that step after the timing; the large domain's 200 steps)")
@@ -428,7 +430,7 @@ def run_accuracy(args):
     for key, dt in (("fp64", torch.float64), ("mixed", torch.float32)):
         ctx = Context(c.grid)
         ctx.init_advection(*[torch.from_numpy(m).cuda() for m in c.masks()])
-        st = BcDevice(c, dtype3=dt)
+        st = BcDevice(c, dtype3=dt, compensated=args.compensated)
         ctx.time_loop(st, 1, args.M * args.accuracy)
         torch.cuda.synchronize()
         res[key] = {n: st.t[n].clone() for n in ERR_FIELDS}
@@ -438,7 +440,8 @@ def run_accuracy(args):
     err = field_errors(res["mixed"], res["fp64"], az)
     print(json.dumps({"workload": f"mixed-precision accuracy: rotation recipe {args.nx}x{args.ny}x{args.kmax}, "
                                   f"M = {args.M}, {args.accuracy} macro steps, tracer: Gaussian blob of amplitude 1 "
-                                  f"plus uniform noise of 1e-3 on {args.t_background} C",
+                                  f"plus uniform noise of 1e-3 on {args.t_background} C; tracer storage "
+                                  f"{'FP32 with compensation' if args.compensated else 'FP32'}",
                       "relative_to": "max: max |field| of the FP64 run; range: its max - min; wet interior cells",
                       "errors": err, "wall_s": time.time() - t0}), flush=True)
 
@@ -498,7 +501,7 @@ def main():
         if key not in wanted:
             continue
         g, st = S.baroclinic_case_device(args.nx, args.ny, args.kmax, recipe="islands", land=0.3, M=M, dt3=60.0,
-                                         seed=6 + rank, dtype3=dt3)
+                                         seed=6 + rank, dtype3=dt3, compensated=args.compensated)
         ctx = Context(g, stream)
         ctx.init_advection(*st.masks())
         variants[key] = dict(g=g, st=st, ctx=ctx, n=1)
@@ -625,7 +628,9 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if head == "mixed" else "f64",
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "nx": args.nx, "ny": args.ny, "kmax": args.kmax, "M": M,
-                       "l2": "inputs larger than L2 (one FP32 3D field 0.86 GB)", "parallelism": f"replicas x{world}"},
+                       "l2": "inputs larger than L2 (one FP32 3D field 0.86 GB)", "parallelism": f"replicas x{world}",
+                       "tracer_storage": ("FP32 with compensation (T + Tlo, S + Slo)" if args.compensated
+                                          else "FP32")},
             "plain_fp64": ({"value": res["fp64"]["value"], "ms_per_step": res["fp64"]["ms"] / args.steps}
                            if "fp64" in res else None),
             "mixed_over_fp64": (res["mixed"]["value"] / res["fp64"]["value"]) if len(res) == 2 else None,

@@ -1,6 +1,8 @@
 // bc.cu -- the mode-split time step on the device: 2D (barotropic) kernels, the drivers of
 // integrate_2d / integrate_3d / the micro-step loop, and their C-ABI entry points.
 // Built with --fmad=false: the FP64 arithmetic rounds exactly as written (as in the reference).
+#include <algorithm>
+
 #include "bc_common.cuh"
 #include "ctx_internal.h"
 
@@ -549,6 +551,75 @@ __global__ void k_nan_sweep(Dev d, const double* __restrict__ z, unsigned long l
     const unsigned long long idx =
         (unsigned long long)(j - d.jmin) * (unsigned long long)(d.imax - d.imin + 1) + (unsigned long long)(i - d.imin);
     atomicMax(&cnt[1], idx + 1);
+  }
+}
+
+// Restart fields (hotstart): the interior (imin..imax, jmin..jmax; levels 0..nl-1) of a field of
+// type R to or from a packed FP64 buffer [level][j][i] -- the extent of a restart file without halos
+// (cppdefs.h:161-170, _2D_W_HOT_ / _3D_W_HOT_).
+template <class R>
+__global__ void k_interior_copy(Dev d, R* f, double* buf, int nl, int to_buf) {
+  const int nx = d.imax - d.imin + 1, ny = d.jmax - d.jmin + 1;
+  const long long n = (long long)nx * ny * nl;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int i = d.imin + (int)(t % nx);
+    const long long r = t / nx;
+    const int j = d.jmin + (int)(r % ny), k = (int)(r / ny);
+    const long long c = d.ix(i, j) + (long long)k * d.sk;
+    if (to_buf) buf[t] = (double)f[c];
+    else f[c] = (R)buf[t];
+  }
+}
+
+// postinit_2d (m2d.F90:358-390), first half: flag[0] = 1 if any U /= 0 where au == 0 or V /= 0 where
+// av == 0 (haloed plane)
+__global__ void k_hot_check(Dev d, Bc2 s, unsigned long long* flag) {
+  GB_IJ2
+  M2 au{d, s.au}, av{d, s.av};
+  W2 U{d, s.f2[U_]}, V{d, s.f2[V_]};
+  if ((au(i, j) == 0 && U(i, j) != 0.0) || (av(i, j) == 0 && V(i, j) != 0.0)) atomicOr(flag, 1ull);
+}
+
+// postinit_2d (m2d.F90:380-396): the reset of U, Uinto / V, Vinto on closed velocity points when the
+// check found any, and the elevations of land points set to -9999
+__global__ void k_hot_reset2d(Dev d, Bc2 s, const unsigned long long* flag) {
+  GB_IJ2
+  M2 az{d, s.az}, au{d, s.au}, av{d, s.av};
+  W2 U{d, s.f2[U_]}, V{d, s.f2[V_]}, Uinto{d, s.f2[UINTO]}, Vinto{d, s.f2[VINTO]}, z{d, s.f2[Z]}, zo{d, s.f2[ZO]};
+  if (*flag) {
+    if (au(i, j) == 0) {
+      U(i, j) = 0.0;
+      Uinto(i, j) = 0.0;
+    }
+    if (av(i, j) == 0) {
+      V(i, j) = 0.0;
+      Vinto(i, j) = 0.0;
+    }
+  }
+  if (az(i, j) == 0) {
+    z(i, j) = -9999.0;
+    zo(i, j) = -9999.0;
+  }
+}
+
+// postinit_3d (m3d.F90:376-405): uu = 0 on closed U points, vv = 0 on closed V points, and on land
+// tke = 0, num = nuh = 1e-15 (single-precision literal), T = S = -9999; every level
+template <class R3>
+__global__ void k_hot_reset3d(Dev d, Bc2 s, R3* uu, R3* vv, R3* tke, R3* num, R3* nuh, R3* T, R3* S) {
+  GB_IJ2
+  M2 az{d, s.az}, au{d, s.au}, av{d, s.av};
+  const long long c = d.ix(i, j);
+  for (int k = 0; k <= d.kmax; ++k) {
+    const long long q = c + (long long)k * d.sk;
+    if (au(i, j) == 0) uu[q] = R3(0);
+    if (av(i, j) == 0) vv[q] = R3(0);
+    if (az(i, j) == 0) {
+      if (tke) tke[q] = R3(0);
+      num[q] = R3((double)1.e-15f);
+      nuh[q] = R3((double)1.e-15f);
+      S[q] = R3(-9999.0);
+      T[q] = R3(-9999.0);
+    }
   }
 }
 
@@ -1123,33 +1194,37 @@ int integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
                                s),
                "top-level salinity");
       if ((rc = do_adv3d_pair<R3>(ctx, dt, f3[TT], f3[SS], f3[UU], f3[VV], f3[WW], f3[HUN], f3[HVN], f3[HO],
-                                  ip[I_TEMP_HOR], ip[I_TEMP_VER], R3(st->par[P_TEMP_AH]))))
+                                  ip[I_TEMP_HOR], ip[I_TEMP_VER], R3(st->par[P_TEMP_AH]), f3[TLO], f3[SLO])))
         return rc;
       if (radn && (rc = temp_sources(s_top))) return rc;
       GB_TIMED(GETM_TIM_VDIFF, run_vdiff<R3>(d, s, dt, R3(st->par[P_CNPAR]), R3(st->par[P_AVMOLT]), f3[TT], f3[HN],
-                                             f3[NUH], st->az, (const R3*)tsrc, (R3*)ctx->scr[0], (R3*)ctx->scr[1]),
+                                             f3[NUH], st->az, (const R3*)tsrc, (R3*)ctx->scr[0], (R3*)ctx->scr[1],
+                                             nullptr, nullptr, f3[TLO]),
                "vdiff T");
       GB_TIMED(GETM_TIM_VDIFF, run_vdiff<R3>(d, s, dt, R3(st->par[P_CNPAR]), R3(st->par[P_AVMOLS]), f3[SS], f3[HN],
-                                             f3[NUH], st->az, (const R3*)nullptr, (R3*)ctx->scr[0], (R3*)ctx->scr[1]),
+                                             f3[NUH], st->az, (const R3*)nullptr, (R3*)ctx->scr[0], (R3*)ctx->scr[1],
+                                             nullptr, nullptr, f3[SLO]),
                "vdiff S");
     }
     if (!pair && ip[I_CALC_TEMP]) {
       if ((rc = do_adv3d<R3>(ctx, dt, f3[TT], f3[UU], f3[VV], f3[WW], f3[HUN], f3[HVN], f3[HO], f3[HN],
                              ip[I_TEMP_SPLIT], ip[I_TEMP_HOR], ip[I_TEMP_VER], R3(st->par[P_TEMP_AH]), GETM_H_TAG,
-                             nullptr, nullptr, ip[I_ADV_VER_ITERS])))
+                             nullptr, nullptr, ip[I_ADV_VER_ITERS], true, f3[TLO])))
         return rc;
       if (radn && (rc = temp_sources(nullptr))) return rc;
       GB_TIMED(GETM_TIM_VDIFF, run_vdiff<R3>(d, s, dt, R3(st->par[P_CNPAR]), R3(st->par[P_AVMOLT]), f3[TT], f3[HN],
-                                             f3[NUH], st->az, (const R3*)tsrc, (R3*)ctx->scr[0], (R3*)ctx->scr[1]),
+                                             f3[NUH], st->az, (const R3*)tsrc, (R3*)ctx->scr[0], (R3*)ctx->scr[1],
+                                             nullptr, nullptr, f3[TLO]),
                "vdiff T");
     }
     if (!pair && ip[I_CALC_SALT]) {
       if ((rc = do_adv3d<R3>(ctx, dt, f3[SS], f3[UU], f3[VV], f3[WW], f3[HUN], f3[HVN], f3[HO], f3[HN],
                              ip[I_SALT_SPLIT], ip[I_SALT_HOR], ip[I_SALT_VER], R3(st->par[P_SALT_AH]), GETM_H_TAG,
-                             nullptr, nullptr, ip[I_ADV_VER_ITERS])))
+                             nullptr, nullptr, ip[I_ADV_VER_ITERS], true, f3[SLO])))
         return rc;
       GB_TIMED(GETM_TIM_VDIFF, run_vdiff<R3>(d, s, dt, R3(st->par[P_CNPAR]), R3(st->par[P_AVMOLS]), f3[SS], f3[HN],
-                                             f3[NUH], st->az, (const R3*)nullptr, (R3*)ctx->scr[0], (R3*)ctx->scr[1]),
+                                             f3[NUH], st->az, (const R3*)nullptr, (R3*)ctx->scr[0], (R3*)ctx->scr[1],
+                                             nullptr, nullptr, f3[SLO]),
                "vdiff S");
     }
     // m3d.F90:595,602
@@ -1410,6 +1485,129 @@ int getm_sw_radiation(getm_ctx* ctx, getm_bc_state* st) {
     return fail(ctx, GETM_ERR_ARG, "sw_radiation: swr, A, g1, g2 and rad are needed");
   return st->prec3d == 8 ? bc3<double>(ctx, st, BC3_SW_RADIATION, GETM_TIM_VDIFF)
                          : bc3<float>(ctx, st, BC3_SW_RADIATION, GETM_TIM_VDIFF);
+}
+
+// write_restart_ncdf.F90:86-204: the restart file's fields in its order, by runtype
+static void restart_lists(int runtype, int* f2, int* n2, int* f3, int* n3) {
+  static const int base2[] = {Z, ZO, U_, SLUX, SLRU, V_, SLVX, SLRV};
+  static const int more2[] = {SSEN, SSUN, SSVN, SSEO, SSUO, SSVO, UINTO, VINTO};
+  static const int base3[] = {UU, VV, WW, UUEX, VVEX, TKE, EPS, NUM, NUH, HN};
+  static const int ts3[] = {TT, SS};
+  int a = 0, b = 0;
+  for (int q : base2) f2[a++] = q;
+  if (runtype >= 2) {
+    for (int q : more2) f2[a++] = q;
+    for (int q : base3) f3[b++] = q;
+    if (runtype >= 3)
+      for (int q : ts3) f3[b++] = q;
+  }
+  *n2 = a;
+  *n3 = b;
+}
+
+int getm_restart_fields(int runtype, int32_t* f2_ids, int32_t* n2, int32_t* f3_ids, int32_t* n3) {
+  if (runtype < 1 || runtype > 4 || !n2 || !n3) return GETM_ERR_ARG;
+  int a[NF2], b[NF3], na, nb;
+  restart_lists(runtype, a, &na, b, &nb);
+  for (int q = 0; q < na; ++q)
+    if (f2_ids) f2_ids[q] = a[q];
+  for (int q = 0; q < nb; ++q)
+    if (f3_ids) f3_ids[q] = b[q];
+  *n2 = na;
+  *n3 = nb;
+  return GETM_OK;
+}
+
+// One restart field through the context's FP64 staging buffer (to_host: device -> host).
+static int restart_field(getm_ctx* ctx, void* f, int elem, int nl, double* host, int to_host) {
+  const Dev& d = ctx->dev;
+  const long long n = (long long)(d.imax - d.imin + 1) * (d.jmax - d.jmin + 1) * nl;
+  if (ctx->stage_bytes < (size_t)n * sizeof(double)) {
+    cudaFree(ctx->stage);
+    ctx->stage = nullptr;
+    ctx->stage_bytes = 0;
+    if (cudaMalloc(&ctx->stage, (size_t)n * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(ctx, GETM_ERR_NOMEM, "restart staging buffer: allocation failed");
+    }
+    ctx->stage_bytes = (size_t)n * sizeof(double);
+  }
+  const int blocks = (int)std::min<long long>((n + 255) / 256, 8 * 148);
+  if (!to_host) GB_TRY(cudaMemcpyAsync(ctx->stage, host, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream),
+                       "restart upload");
+  if (f) {
+    TimerScope ts(ctx, GETM_TIM_COPY);
+    if (elem == 8) k_interior_copy<double><<<blocks, 256, 0, ctx->stream>>>(d, (double*)f, ctx->stage, nl, to_host);
+    else k_interior_copy<float><<<blocks, 256, 0, ctx->stream>>>(d, (float*)f, ctx->stage, nl, to_host);
+    GB_TRY(cudaGetLastError(), "restart field");
+  } else if (to_host) {
+    GB_TRY(cudaMemsetAsync(ctx->stage, 0, n * sizeof(double), ctx->stream), "restart field");
+  }
+  if (to_host) {
+    GB_TRY(cudaMemcpyAsync(host, ctx->stage, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream),
+           "restart download");
+  }
+  // the staging buffer is reused by the next field
+  GB_TRY(cudaStreamSynchronize(ctx->stream), "restart field");
+  return GETM_OK;
+}
+
+int getm_restart_write(getm_ctx* ctx, const getm_bc_state* st, int runtype, double* const* host2,
+                       double* const* host3) {
+  int rc = check_state(ctx, st);
+  if (rc) return rc;
+  if (runtype < 1 || runtype > 4 || !host2 || (runtype >= 2 && !host3)) return GETM_ERR_ARG;
+  int a[NF2], b[NF3], na, nb;
+  restart_lists(runtype, a, &na, b, &nb);
+  for (int q = 0; q < na; ++q)
+    if ((rc = restart_field(ctx, st->f2[a[q]], 8, 1, host2[q], 1))) return rc;
+  for (int q = 0; q < nb; ++q)
+    if ((rc = restart_field(ctx, st->f3[b[q]], st->prec3d, ctx->dev.kmax + 1, host3[q], 1))) return rc;
+  return GETM_OK;
+}
+
+int getm_restart_read(getm_ctx* ctx, getm_bc_state* st, int runtype, const double* const* host2,
+                      const double* const* host3) {
+  int rc = check_state(ctx, st);
+  if (rc) return rc;
+  if (runtype < 1 || runtype > 4 || !host2 || (runtype >= 2 && !host3)) return GETM_ERR_ARG;
+  if ((rc = ensure_bc_scratch(ctx, (size_t)st->prec3d))) return rc;
+  int a[NF2], b[NF3], na, nb;
+  restart_lists(runtype, a, &na, b, &nb);
+  for (int q = 0; q < na; ++q)
+    if ((rc = restart_field(ctx, st->f2[a[q]], 8, 1, const_cast<double*>(host2[q]), 0))) return rc;
+  for (int q = 0; q < nb; ++q)
+    if (st->f3[b[q]] &&
+        (rc = restart_field(ctx, st->f3[b[q]], st->prec3d, ctx->dev.kmax + 1, const_cast<double*>(host3[q]), 0)))
+      return rc;
+  // postinit_2d / postinit_3d of a hotstart (initialise.F90:331-334)
+  const Dev& d = ctx->dev;
+  const Bc2 s2 = to_bc2(st);
+  unsigned long long* flag = ctx->cnt + 6;
+  GB_TRY(cudaMemsetAsync(flag, 0, sizeof(unsigned long long), ctx->stream), "hotstart");
+  {
+    TimerScope ts(ctx, GETM_TIM_BC2D);
+    k_hot_check<<<grid2(d), kBlk2, 0, ctx->stream>>>(d, s2, flag);
+    k_hot_reset2d<<<grid2(d), kBlk2, 0, ctx->stream>>>(d, s2, flag);
+    k_depth_update<false><<<grid2(d), kBlk2, 0, ctx->stream>>>(d, s2, Bc2W{});
+    GB_TRY(cudaGetLastError(), "postinit_2d");
+  }
+  if (runtype >= 2) {
+    TimerScope ts(ctx, GETM_TIM_BC3D);
+    void** f3 = st->f3;
+    if (st->prec3d == 8)
+      k_hot_reset3d<double><<<grid2(d), kBlk2, 0, ctx->stream>>>(d, s2, (double*)f3[UU], (double*)f3[VV],
+                                                               (double*)f3[TKE], (double*)f3[NUM], (double*)f3[NUH],
+                                                               (double*)f3[TT], (double*)f3[SS]);
+    else
+      k_hot_reset3d<float><<<grid2(d), kBlk2, 0, ctx->stream>>>(d, s2, (float*)f3[UU], (float*)f3[VV], (float*)f3[TKE],
+                                                              (float*)f3[NUM], (float*)f3[NUH], (float*)f3[TT],
+                                                              (float*)f3[SS]);
+    GB_TRY(cudaGetLastError(), "postinit_3d");
+    rc = st->prec3d == 8 ? bc3<double>(ctx, st, BC3_SIGMA, GETM_TIM_BC3D) : bc3<float>(ctx, st, BC3_SIGMA, GETM_TIM_BC3D);
+    if (rc) return rc;
+  }
+  return GETM_OK;
 }
 
 int getm_sealevel_nan_check(getm_ctx* ctx, const double* z, int64_t* num_nan, int32_t* inan, int32_t* jnan) {

@@ -11,7 +11,8 @@ enum F2 {
   SSUN, SSVO, SSVN, DN, DUN, DVN, RRU, RRV, TAUBX, TAUBY, TAUB, TAUS, SWR, SHF, ATT_A, ATT_G1, ATT_G2, NF2
 };
 enum F3 {
-  UU, VV, WW, HO, HN, HUO, HUN, HVO, HVN, UUEX, VVEX, IDPDX, IDPDY, TT, SS, RHO, BUOY, NUM, NUH, RAD, TKE, EPS, NF3
+  UU, VV, WW, HO, HN, HUO, HUN, HVO, HVN, UUEX, VVEX, IDPDX, IDPDY, TT, SS, RHO, BUOY, NUM, NUH, RAD, TKE, EPS,
+  TLO, SLO, NF3
 };
 enum PD {
   P_DTM, P_DT, P_CNPAR, P_MIN_DEPTH, P_CRIT_DEPTH, P_G, P_RHO_0, P_KAPPA, P_AVMMOL, P_AVMOLT, P_AVMOLS, P_T0, P_S0,
@@ -23,9 +24,10 @@ enum PI {
   I_TEMP_VER, I_SALT_SPLIT, I_SALT_HOR, I_SALT_VER, I_ADV_VER_ITERS, I_UFIRST2D, I_UFIRST3D, I_CALC_TEMP,
   I_CALC_SALT, I_IP_METHOD, I_VISCOSITY, I_EQSTATE_METHOD, I_SEALEVEL_CHECK, I_RADIATION, I_NAN_WARNED, NPI
 };
-// fields a state may leave NULL: the radiation inputs and output when radiation = 0, tke and eps
+// fields a state may leave NULL: the radiation inputs and output when radiation = 0, tke and eps,
+// and the compensated storage of T and S (Tlo, Slo)
 constexpr bool optional_f2(int q) { return q == SWR || q == SHF || q == ATT_A || q == ATT_G1 || q == ATT_G2; }
-constexpr bool optional_f3(int q) { return q == RAD || q == TKE || q == EPS; }
+constexpr bool optional_f3(int q) { return q == RAD || q == TKE || q == EPS || q == TLO || q == SLO; }
 
 // 2D part (all FP64) -- passed to kernels by value
 struct Bc2 {

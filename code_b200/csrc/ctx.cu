@@ -60,7 +60,7 @@ using namespace gb;
 template <class R>
 int do_adv3d(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, const R* hu,
                     const R* hv, const R* ho, const R* hn, int split, int hs, int vs, R AH, int tag, R* hires,
-                    R* advres, int iters, bool field_out) {
+                    R* advres, int iters, bool field_out, R* lo) {
   (void)hn;
   if (!ctx) return GETM_ERR_ARG;
   if (!ctx->adv_ready) return fail(ctx, GETM_ERR_STATE, "getm_init_advection has not been called");
@@ -137,6 +137,10 @@ int do_adv3d(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, c
     return GETM_OK;
   }
   R* Al = A ? L(A, 1) : nullptr;
+  // compensated storage of the tracer (FP32; the FULLSPLIT and HALFSPLIT sequences, whose updates
+  // are all increments)
+  R* lw = (lo && field_out) ? lo : nullptr;
+  R* ll = lw ? L(lw, 1) : nullptr;
   switch (split) {
     case GETM_NOSPLIT:
       GB_TIMED(GETM_TIM_COPY, cudaMemcpyAsync(S, f, bytes3, cudaMemcpyDeviceToDevice, s), "copy f");
@@ -149,23 +153,23 @@ int do_adv3d(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, c
       break;
     case GETM_FULLSPLIT:
       GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<R, 0>(d, s, nk, dt, one, hs, AH, L(f, 1), L(f, 1), L(S, 1), L(ho, 1), L(H, 1), Al,
-                                L(uu, 1), L(hu, 1), g.mask_uflux, g.mask_uupdate)), "u");
+                                L(uu, 1), L(hu, 1), g.mask_uflux, g.mask_uupdate, nullptr, nullptr, nullptr, nullptr, ll)), "u");
       GB_TIMED(GETM_TIM_ADV_V, (run_sweep_h<R, 1>(d, s, nk, dt, one, hs, AH, L(S, 1), L(S, 1), L(f, 1), L(H, 1), L(H, 1), Al,
-                                L(vv, 1), L(hv, 1), g.mask_vflux, g.mask_vupdate)), "v");
-      if (kmax > 1) GB_TIMED(GETM_TIM_ADV_W, run_sweep_w<R>(d, s, dt, one, vs, kshift, iters, f, f, f, H, A, ww, g.az, warn), "w");
+                                L(vv, 1), L(hv, 1), g.mask_vflux, g.mask_vupdate, nullptr, nullptr, nullptr, nullptr, ll)), "v");
+      if (kmax > 1) GB_TIMED(GETM_TIM_ADV_W, run_sweep_w<R>(d, s, dt, one, vs, kshift, iters, f, f, f, H, A, ww, g.az, warn, nullptr, lw), "w");
       break;
     case GETM_HALFSPLIT:
       GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<R, 0>(d, s, nk, dt, half, hs, AH, L(f, 1), L(f, 1), L(S, 1), L(ho, 1), L(H, 1), Al,
-                                L(uu, 1), L(hu, 1), g.mask_uflux, g.mask_uupdate)), "u1");
+                                L(uu, 1), L(hu, 1), g.mask_uflux, g.mask_uupdate, nullptr, nullptr, nullptr, nullptr, ll)), "u1");
       GB_TIMED(GETM_TIM_ADV_V, (run_sweep_h<R, 1>(d, s, nk, dt, half, hs, AH, L(S, 1), L(S, 1), L(f, 1), L(H, 1), L(H, 1), Al,
-                                L(vv, 1), L(hv, 1), g.mask_vflux, g.mask_vupdate)), "v1");
-      if (kmax > 1) GB_TIMED(GETM_TIM_ADV_W, run_sweep_w<R>(d, s, dt, one, vs, kshift, iters, f, f, f, H, A, ww, g.az, warn), "w");
+                                L(vv, 1), L(hv, 1), g.mask_vflux, g.mask_vupdate, nullptr, nullptr, nullptr, nullptr, ll)), "v1");
+      if (kmax > 1) GB_TIMED(GETM_TIM_ADV_W, run_sweep_w<R>(d, s, dt, one, vs, kshift, iters, f, f, f, H, A, ww, g.az, warn, nullptr, lw), "w");
       GB_TIMED(GETM_TIM_ADV_V, (run_sweep_h<R, 1>(d, s, nk, dt, half, hs, AH, L(f, 1), L(f, 1), L(S, 1), L(H, 1), L(H, 1), Al,
-                                L(vv, 1), L(hv, 1), g.mask_vflux, g.mask_vupdate)), "v2");
+                                L(vv, 1), L(hv, 1), g.mask_vflux, g.mask_vupdate, nullptr, nullptr, nullptr, nullptr, ll)), "v2");
       // the last sweep writes the field and heights only when the caller keeps them
       GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<R, 0>(d, s, nk, dt, half, hs, AH, L(S, 1), L(S, 1),
                                 field_out ? L(f, 1) : nullptr, L(H, 1), (field_out || hires) ? L(H, 1) : nullptr,
-                                Al, L(uu, 1), L(hu, 1), g.mask_uflux, g.mask_uupdate)), "u2");
+                                Al, L(uu, 1), L(hu, 1), g.mask_uflux, g.mask_uupdate, nullptr, nullptr, nullptr, nullptr, ll)), "u2");
       break;
     case GETM_HVSPLIT:
       GB_TIMED(GETM_TIM_COPY, cudaMemcpyAsync(S, f, bytes3, cudaMemcpyDeviceToDevice, s), "copy f");
@@ -186,7 +190,7 @@ int do_adv3d(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, c
 // same sweeps as do_adv3d's HALFSPLIT branch for each field, with the heights hi evolved once.
 template <class R>
 int do_adv3d_pair(getm_ctx* ctx, R dt, R* fa, R* fb, const R* uu, const R* vv, const R* ww, const R* hu,
-                  const R* hv, const R* ho, int hs, int vs, R AH) {
+                  const R* hv, const R* ho, int hs, int vs, R AH, R* lo_a, R* lo_b) {
   getm_adv_grid g;
   grid_for_tag(ctx, GETM_H_TAG, &g);
   const Dev& d = ctx->dev;
@@ -198,36 +202,38 @@ int do_adv3d_pair(getm_ctx* ctx, R dt, R* fa, R* fb, const R* uu, const R* vv, c
   R* Sa = (R*)ctx->scr[0];
   R* H = (R*)ctx->scr[1];
   R* Sb = (R*)ctx->scr[2];
-  auto L = [&](auto* p, int k) { return p + (long long)k * sk; };
+  auto L = [&](auto* p, int k) { return p ? p + (long long)k * sk : p; };
   const R half = R(0.5), one = R(1);
   const int nk = kmax;
+  R* la = L(lo_a, 1);
+  R* lb = L(lo_b, 1);
   GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<R, 0>(d, s, nk, dt, half, hs, AH, L(fa, 1), L(fa, 1), L(Sa, 1), L(ho, 1),
                             L(H, 1), nullptr, L(uu, 1), L(hu, 1), g.mask_uflux, g.mask_uupdate, nullptr, L(fb, 1),
-                            L(fb, 1), L(Sb, 1))), "u1");
+                            L(fb, 1), L(Sb, 1), la, lb)), "u1");
   GB_TIMED(GETM_TIM_ADV_V, (run_sweep_h<R, 1>(d, s, nk, dt, half, hs, AH, L(Sa, 1), L(Sa, 1), L(fa, 1), L(H, 1),
                             L(H, 1), nullptr, L(vv, 1), L(hv, 1), g.mask_vflux, g.mask_vupdate, nullptr, L(Sb, 1),
-                            L(Sb, 1), L(fb, 1))), "v1");
+                            L(Sb, 1), L(fb, 1), la, lb)), "v1");
   if (kmax > 1 && vs != NOADV)
-    GB_TIMED(GETM_TIM_ADV_W, run_sweep_w2<R>(d, s, dt, one, vs, fa, fb, H, ww, g.az), "w");
+    GB_TIMED(GETM_TIM_ADV_W, run_sweep_w2<R>(d, s, dt, one, vs, fa, fb, H, ww, g.az, lo_a, lo_b), "w");
   GB_TIMED(GETM_TIM_ADV_V, (run_sweep_h<R, 1>(d, s, nk, dt, half, hs, AH, L(fa, 1), L(fa, 1), L(Sa, 1), L(H, 1),
                             L(H, 1), nullptr, L(vv, 1), L(hv, 1), g.mask_vflux, g.mask_vupdate, nullptr, L(fb, 1),
-                            L(fb, 1), L(Sb, 1))), "v2");
+                            L(fb, 1), L(Sb, 1), la, lb)), "v2");
   GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<R, 0>(d, s, nk, dt, half, hs, AH, L(Sa, 1), L(Sa, 1), L(fa, 1), L(H, 1),
                             L(H, 1), nullptr, L(uu, 1), L(hu, 1), g.mask_uflux, g.mask_uupdate, nullptr, L(Sb, 1),
-                            L(Sb, 1), L(fb, 1))), "u2");
+                            L(Sb, 1), L(fb, 1), la, lb)), "u2");
   return GETM_OK;
 }
 template int do_adv3d_pair<double>(getm_ctx*, double, double*, double*, const double*, const double*, const double*,
-                                   const double*, const double*, const double*, int, int, double);
+                                   const double*, const double*, const double*, int, int, double, double*, double*);
 template int do_adv3d_pair<float>(getm_ctx*, float, float*, float*, const float*, const float*, const float*,
-                                  const float*, const float*, const float*, int, int, float);
+                                  const float*, const float*, const float*, int, int, float, float*, float*);
 
 template int do_adv3d<double>(getm_ctx*, double, double*, const double*, const double*, const double*,
                                const double*, const double*, const double*, const double*, int, int, int, double,
-                               int, double*, double*, int, bool);
+                               int, double*, double*, int, bool, double*);
 template int do_adv3d<float>(getm_ctx*, float, float*, const float*, const float*, const float*, const float*,
                              const float*, const float*, const float*, int, int, int, float, int, float*, float*,
-                             int, bool);
+                             int, bool, float*);
 
 template <class R>
 static int sweep_h_api(getm_ctx* ctx, int dir, int nk, R dt, const R* f, R* fi, R* Di, R* adv, const R* U,
@@ -384,6 +390,7 @@ int getm_ctx_destroy(getm_ctx* ctx) {
   cudaFree(ctx->zmask);
   cudaFree(ctx->red);
   cudaFree(ctx->cnt);
+  cudaFree(ctx->stage);
   for (auto p : ctx->scr) cudaFree(p);
   cudaFree(ctx->bc_scr3);
   cudaFree(ctx->bc_scr2);
@@ -511,8 +518,10 @@ int getm_adv_split_v(getm_ctx* ctx, int nk, double dt, const double* f, double* 
   return sweep_h_api<double>(ctx, 1, nk, dt, f, fi, Di, adv, V, DV, splitfac, scheme, AH, mask_flux, mask_update);
 }
 
-int getm_adv_split_w(getm_ctx* ctx, double dt, const double* f, double* fi, double* hi, double* adv,
-                     const double* ww, double splitfac, int scheme, int tag, const int32_t* az, int itersmax) {
+extern "C++" {
+template <class R>
+static int sweep_w_api(getm_ctx* ctx, R dt, const R* f, R* fi, R* hi, R* adv, const R* ww, R splitfac, int scheme,
+                       int tag, const int32_t* az, int itersmax) {
   if (!ctx || !f || !fi || !hi || !ww || !az) return fail(ctx, GETM_ERR_ARG, "adv_split_w: bad argument");
   if (scheme == NOADV) return GETM_OK;
   if (!is_split_scheme(scheme)) return fail(ctx, GETM_ERR_ARG, "adv_split_w: scheme is invalid");
@@ -520,9 +529,32 @@ int getm_adv_split_w(getm_ctx* ctx, double dt, const double* f, double* fi, doub
     return fail(ctx, GETM_ERR_UNSUPPORTED, "adv_split_w: itersmax > 1 needs kmax <= 128");
   const int kshift = (tag == GETM_W_TAG) ? 1 : 0;
   return cuda_fail(ctx,
-                   run_sweep_w<double>(ctx->dev, ctx->stream, dt, splitfac, scheme, kshift, itersmax < 1 ? 1 : itersmax,
-                                       f, fi, fi, hi, adv, ww, az, ctx->cnt),
+                   run_sweep_w<R>(ctx->dev, ctx->stream, dt, splitfac, scheme, kshift, itersmax < 1 ? 1 : itersmax, f,
+                                  fi, fi, hi, adv, ww, az, ctx->cnt),
                    "adv_split_w");
+}
+}  // extern "C++"
+
+int getm_adv_split_w(getm_ctx* ctx, double dt, const double* f, double* fi, double* hi, double* adv,
+                     const double* ww, double splitfac, int scheme, int tag, const int32_t* az, int itersmax) {
+  return sweep_w_api<double>(ctx, dt, f, fi, hi, adv, ww, splitfac, scheme, tag, az, itersmax);
+}
+
+int getm_adv_split_u_f32(getm_ctx* ctx, int nk, float dt, const float* f, float* fi, float* Di, float* adv,
+                         const float* U, const float* DU, float splitfac, int scheme, float AH,
+                         const uint8_t* mask_flux, const uint8_t* mask_update) {
+  return sweep_h_api<float>(ctx, 0, nk, dt, f, fi, Di, adv, U, DU, splitfac, scheme, AH, mask_flux, mask_update);
+}
+
+int getm_adv_split_v_f32(getm_ctx* ctx, int nk, float dt, const float* f, float* fi, float* Di, float* adv,
+                         const float* V, const float* DV, float splitfac, int scheme, float AH,
+                         const uint8_t* mask_flux, const uint8_t* mask_update) {
+  return sweep_h_api<float>(ctx, 1, nk, dt, f, fi, Di, adv, V, DV, splitfac, scheme, AH, mask_flux, mask_update);
+}
+
+int getm_adv_split_w_f32(getm_ctx* ctx, float dt, const float* f, float* fi, float* hi, float* adv, const float* ww,
+                         float splitfac, int scheme, int tag, const int32_t* az, int itersmax) {
+  return sweep_w_api<float>(ctx, dt, f, fi, hi, adv, ww, splitfac, scheme, tag, az, itersmax);
 }
 
 int getm_do_advection_3d(getm_ctx* ctx, double dt, double* f, const double* uu, const double* vv,

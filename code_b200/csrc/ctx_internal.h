@@ -33,6 +33,9 @@ struct getm_ctx {
   // [3..5] the elevation NaN sweep of the micro steps (findings, last index + 1, latch)
   unsigned long long* cnt = nullptr;
   bool nan_swept = false;  // a NaN sweep was launched since its counters were last read
+  // FP64 staging buffer of the restart-field transfers (getm_restart_read / _write)
+  double* stage = nullptr;
+  size_t stage_bytes = 0;
   std::string err;
   // per-stage device timers (the counterpart of getm_timers' tic/toc, getm_timers.F90:275-357)
   bool timing = false;
@@ -162,16 +165,17 @@ static inline bool grid_for_tag(const getm_ctx* ctx, int tag, getm_adv_grid* g) 
 }
 
 
-// do_advection_3d (advection_3d.F90:120-598) on device pointers; defined in ctx.cu.
+// do_advection_3d (advection_3d.F90:120-598) on device pointers; defined in ctx.cu. lo: the
+// tracer's compensated storage (FP32, FULLSPLIT / HALFSPLIT; null = none).
 template <class R>
 int do_adv3d(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, const R* hu, const R* hv,
              const R* ho, const R* hn, int split, int hs, int vs, R AH, int tag, R* hires, R* advres, int iters,
-             bool field_out = true);
+             bool field_out = true, R* lo = nullptr);
 // Two tracers advected together with HALFSPLIT on the H grid (ctx.cu); the caller has checked that
 // hs is a split scheme, vs a split scheme or NOADV, and adv_ver_iterations = 1.
 template <class R>
 int do_adv3d_pair(getm_ctx* ctx, R dt, R* fa, R* fb, const R* uu, const R* vv, const R* ww, const R* hu,
-                  const R* hv, const R* ho, int hs, int vs, R AH);
+                  const R* hv, const R* ho, int hs, int vs, R AH, R* lo_a = nullptr, R* lo_b = nullptr);
 
 // Tracer step: do_advection_3d(H_TAG) then the implicit vertical diffusion (ctx.cu).
 template <class R>

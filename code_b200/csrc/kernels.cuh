@@ -170,6 +170,32 @@ __device__ __forceinline__ R fv_update(R hio, R dh, R hin, R fio, R dt, R advn) 
   }
 }
 
+// Compensated storage of an FP32 tracer (the mixed step): the tracer is the unevaluated sum
+// hi + lo of two FP32 numbers. An update adds its increment and the carried lo to hi exactly
+// (Knuth's TwoSum): hi becomes the rounded sum and lo the rounding error, so increments smaller
+// than half an ulp of hi -- which a plain FP32 update drops, and which a tracer far from zero
+// (temperature near 15 C, salinity near 35) receives every sweep -- accumulate in lo until they
+// reach hi instead of being lost. |lo| stays below half an ulp of hi. The fluxes are formed from
+// hi alone, as in the plain update.
+__device__ __forceinline__ float add_comp(float hi, float inc, float& lo) {
+  const float b = __fadd_rn(inc, lo);
+  const float s = __fadd_rn(hi, b);
+  const float bb = __fsub_rn(s, hi);
+  lo = __fadd_rn(__fsub_rn(hi, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+  return s;
+}
+// fv_update with the compensated storage: lo is the cell's carried error (read and written)
+template <class R>
+__device__ __forceinline__ R fv_update_lo(R hio, R dh, R hin, R fio, R dt, R advn, R& lo) {
+  if constexpr (sizeof(R) == 8) {
+    (void)lo;
+    return fv_update<R>(hio, dh, hin, fio, dt, advn);
+  } else {
+    (void)hio;
+    return add_comp(fio, __fdividef(__fmaf_rn(fio, dh, -__fmul_rn(dt, advn)), hin), lo);
+  }
+}
+
 // Flux through face q (between cells q and q+1) from staged values: f at q-1..q+2, flux masks at
 // q-1..q+1. cdx = dti/dx (used by FP32 only).
 // Courant number of a horizontal face (adv_split_u.F90:229-246); cdx = dti/dx is used by FP32.
@@ -298,6 +324,7 @@ struct TracerIO {
   const R* f;
   const R* fi_src;
   R* fi_dst;
+  R* lo = nullptr;  // FP32 compensated storage: the carried error of the updated cells (may be null)
 };
 template <class R, int NF>
 struct TracerSet {
@@ -435,7 +462,15 @@ __global__ void __launch_bounds__(TU, sizeof(R) == 4 ? 16 : 8) k_sweep_u_tile(De
         for (int n = 0; n < NF; ++n) {
           const R fio = F.t[n].fi_src == F.t[n].f ? sf[b][n][t + 2] : sfi[b][n][t];
           const R advn = cell_advn<R>(C, sfl[n][t + 1], sfl[n][t]);
-          if (F.t[n].fi_dst) F.t[n].fi_dst[p] = fv_update<R>(Dio, dD, Dn, fio, C.dt, advn);
+          if (F.t[n].fi_dst) {
+            if (F.t[n].lo) {
+              R lo = F.t[n].lo[p];
+              F.t[n].fi_dst[p] = fv_update_lo<R>(Dio, dD, Dn, fio, C.dt, advn, lo);
+              F.t[n].lo[p] = lo;
+            } else {
+              F.t[n].fi_dst[p] = fv_update<R>(Dio, dD, Dn, fio, C.dt, advn);
+            }
+          }
           if (NF == 1 && adv) adv[p] = sA[b][t] + advn;
         }
       } else {
@@ -569,7 +604,15 @@ __global__ void __launch_bounds__(TVX * TVY, sizeof(R) == 4 ? (NF == 1 ? 8 : 6) 
         for (int n = 0; n < NF; ++n) {
           const R fio = F.t[n].fi_src == F.t[n].f ? sf[b][n][ty + 2][tx] : sfi[b][n][ty][tx];
           const R advn = cell_advn<R>(C, sfl[n][ty + 1][tx], sfl[n][ty][tx]);
-          if (F.t[n].fi_dst) F.t[n].fi_dst[p] = fv_update<R>(Dio, dD, Dn, fio, C.dt, advn);
+          if (F.t[n].fi_dst) {
+            if (F.t[n].lo) {
+              R lo = F.t[n].lo[p];
+              F.t[n].fi_dst[p] = fv_update_lo<R>(Dio, dD, Dn, fio, C.dt, advn, lo);
+              F.t[n].lo[p] = lo;
+            } else {
+              F.t[n].fi_dst[p] = fv_update<R>(Dio, dD, Dn, fio, C.dt, advn);
+            }
+          }
           if (NF == 1 && adv) adv[p] = sA[b][ty][tx] + advn;
         }
       } else {
@@ -617,7 +660,7 @@ template <class R, int S, bool REC>
 __global__ void __launch_bounds__(128) k_sweep_w(Dev d, R dt, R splitfac, int kshift,
                                                  const R* f, const R* fi_src, R* fi_dst, R* hi, R* adv,
                                                  const R* __restrict__ ww,
-                                                 const int32_t* __restrict__ az, uint8_t* code) {
+                                                 const int32_t* __restrict__ az, uint8_t* code, R* lo = nullptr) {
   const int ii = blockIdx.x * blockDim.x + threadIdx.x;
   const int jj = blockIdx.y * blockDim.y + threadIdx.y;
   // columns i = imin-2..imax+1, j = jmin-2..jmax+1 (adv_split_w.F90:160-162)
@@ -658,7 +701,13 @@ __global__ void __launch_bounds__(128) k_sweep_w(Dev d, R dt, R splitfac, int ks
     const R dh = dti * (wk - wkm1);
     const R hin = hio - dh;
     const R advn = splitfac * (wfl - wprev);
-    fi_dst[c + k * sk] = fv_update<R>(hio, dh, hin, fio, dt, advn);
+    if (lo) {
+      R l = lo[c + k * sk];
+      fi_dst[c + k * sk] = fv_update_lo<R>(hio, dh, hin, fio, dt, advn, l);
+      lo[c + k * sk] = l;
+    } else {
+      fi_dst[c + k * sk] = fv_update<R>(hio, dh, hin, fio, dt, advn);
+    }
     hi[c + k * sk] = hin;
     if (adv) adv[c + k * sk] = advo + advn;
     a = b; b = e; e = g; g = g2; g2 = gn;
@@ -672,7 +721,8 @@ __global__ void __launch_bounds__(128) k_sweep_w(Dev d, R dt, R splitfac, int ks
 // itersmax = 1): k_sweep_w's arithmetic for each field, the heights updated once.
 template <class R, int S>
 __global__ void __launch_bounds__(128) k_sweep_w2(Dev d, R dt, R splitfac, R* fa, R* fb, R* hi,
-                                                  const R* __restrict__ ww, const int32_t* __restrict__ az) {
+                                                  const R* __restrict__ ww, const int32_t* __restrict__ az,
+                                                  R* lo_a = nullptr, R* lo_b = nullptr) {
   const int ii = blockIdx.x * blockDim.x + threadIdx.x;
   const int jj = blockIdx.y * blockDim.y + threadIdx.y;
   if (ii >= d.ni() - 1 || jj >= d.nj() - 1) return;
@@ -702,8 +752,20 @@ __global__ void __launch_bounds__(128) k_sweep_w2(Dev d, R dt, R splitfac, R* fa
     const R hio = hA;
     const R dh = dti * (wk - wkm1);
     const R hin = hio - dh;
-    fa[c + k * sk] = fv_update<R>(hio, dh, hin, a1, dt, splitfac * (wfa - wpa));
-    fb[c + k * sk] = fv_update<R>(hio, dh, hin, b1, dt, splitfac * (wfb - wpb));
+    if (lo_a) {
+      R l = lo_a[c + k * sk];
+      fa[c + k * sk] = fv_update_lo<R>(hio, dh, hin, a1, dt, splitfac * (wfa - wpa), l);
+      lo_a[c + k * sk] = l;
+    } else {
+      fa[c + k * sk] = fv_update<R>(hio, dh, hin, a1, dt, splitfac * (wfa - wpa));
+    }
+    if (lo_b) {
+      R l = lo_b[c + k * sk];
+      fb[c + k * sk] = fv_update_lo<R>(hio, dh, hin, b1, dt, splitfac * (wfb - wpb), l);
+      lo_b[c + k * sk] = l;
+    } else {
+      fb[c + k * sk] = fv_update<R>(hio, dh, hin, b1, dt, splitfac * (wfb - wpb));
+    }
     hi[c + k * sk] = hin;
     a0 = a1; a1 = a2; a2 = a3; a3 = a4; a4 = an;
     b0 = b1; b1 = b2; b2 = b3; b3 = b4; b4 = bn;
@@ -725,7 +787,7 @@ __global__ void __launch_bounds__(64) k_sweep_w_iter(Dev d, R dt, R splitfac, in
                                                      R* fi_dst, R* hi, R* adv,
                                                      const R* __restrict__ ww,
                                                      const int32_t* __restrict__ az,
-                                                     unsigned long long* warn) {
+                                                     unsigned long long* warn, R* lo = nullptr) {
   const int ii = blockIdx.x * blockDim.x + threadIdx.x;
   const int jj = blockIdx.y * blockDim.y + threadIdx.y;
   if (ii >= d.ni() - 1 || jj >= d.nj() - 1) return;
@@ -735,7 +797,7 @@ __global__ void __launch_bounds__(64) k_sweep_w_iter(Dev d, R dt, R splitfac, in
   const long long sk = d.sk;
   const R dti = splitfac * dt;
   R fo[GB_KMAX_ITER + 1], fia[GB_KMAX_ITER + 1], hia[GB_KMAX_ITER + 1], ada[GB_KMAX_ITER + 1],
-      wfl[GB_KMAX_ITER + 1], cfl0[GB_KMAX_ITER + 1], cfls[GB_KMAX_ITER + 1];
+      wfl[GB_KMAX_ITER + 1], cfl0[GB_KMAX_ITER + 1], cfls[GB_KMAX_ITER + 1], loa[GB_KMAX_ITER + 1];
   for (int k = 0; k <= kmax; ++k) {
     fo[k] = f[c + k * sk];
     cfl0[k] = R(0);
@@ -754,6 +816,7 @@ __global__ void __launch_bounds__(64) k_sweep_w_iter(Dev d, R dt, R splitfac, in
         fia[k] = fi_src[c + k * sk];
         hia[k] = hi[c + k * sk];
         ada[k] = adv ? adv[c + k * sk] : R(0);
+        loa[k] = lo ? lo[c + k * sk] : R(0);
       }
       faux = fo;
       for (int k = 0; k <= kmax; ++k) cfls[k] = cfl0[k];
@@ -804,7 +867,8 @@ __global__ void __launch_bounds__(64) k_sweep_w_iter(Dev d, R dt, R splitfac, in
       const R dh = dtik * (ww[c + k * sk] - ww[c + (k - 1) * sk]);
       hia[k] = hio - dh;
       const R advn = splitfack * (wfl[k] - wfl[k - 1]);
-      fia[k] = fv_update<R>(hio, dh, hia[k], fia[k], dt, advn);
+      fia[k] = lo ? fv_update_lo<R>(hio, dh, hia[k], fia[k], dt, advn, loa[k])
+                  : fv_update<R>(hio, dh, hia[k], fia[k], dt, advn);
       ada[k] = ada[k] + advn;
     }
     faux = fia;
@@ -814,6 +878,7 @@ __global__ void __launch_bounds__(64) k_sweep_w_iter(Dev d, R dt, R splitfac, in
     fi_dst[c + k * sk] = fia[k];
     hi[c + k * sk] = hia[k];
     if (adv) adv[c + k * sk] = ada[k];
+    if (lo) lo[c + k * sk] = loa[k];
   }
 }
 
@@ -836,7 +901,7 @@ template <class R>
 __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, const R* Sin, R* S,
                                                const R* __restrict__ hn, const R* __restrict__ nuh,
                                                const int32_t* __restrict__ az, const R* __restrict__ src, R* RUs,
-                                               R* QUs, R* S2) {
+                                               R* QUs, R* S2, R* lo) {
   const int kmax = d.kmax;
   const int i = d.imin + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = d.jmin + blockIdx.y * blockDim.y + threadIdx.y;
@@ -850,6 +915,19 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, co
   auto put = [&](int k, R v) {
     S[c + k * sk] = v;
     if (S2) S2[c + k * sk] = v;
+  };
+  // the new value of level k from the old one and the increment: a plain FP32 sum, or the
+  // compensated sum of the carried error lo (the tracer's compensated storage)
+  auto new_level = [&](int k, R sold, R inc) -> R {
+    if constexpr (sizeof(R) == 4) {
+      if (lo) {
+        float l = lo[c + k * sk];
+        const float v = add_comp(sold, inc, l);
+        lo[c + k * sk] = l;
+        return v;
+      }
+    }
+    return sold + inc;
   };
   const R co = R(2) * (R(1) - cnpar) * dt;
   const R cn = R(2) * cnpar * dt;
@@ -938,7 +1016,7 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, co
     R a4 = incr ? (ao_k + an_k) * (Skp1 - S1) : Skp1 * ao_k + S1 * (h1 - ao_k);
     if (src) a4 = a4 + src_n;  // src(1)
     v = (a4 - a3 * qu) / (a2 - a3 * ru);
-    put(1, incr ? S1 + v : v);
+    put(1, incr ? new_level(1, S1, v) : v);
   }
   // back substitution upwards, with the next level's coefficients loaded one step ahead
   R qn = kmax >= 2 ? QUs[c + 2 * sk] : R(0), rn = kmax >= 2 ? RUs[c + 2 * sk] : R(0);
@@ -954,7 +1032,7 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, co
       if (incr) sn2 = L(Sin, k + 2);
     }
     v = q - r * v;
-    put(k, incr ? so + v : v);
+    put(k, incr ? new_level(k, so, v) : v);
   }
 }
 

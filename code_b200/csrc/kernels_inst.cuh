@@ -44,7 +44,7 @@ template <class R, int DIR>
 int run_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int scheme, R AH, const R* f,
                 const R* fi_src, R* fi_dst, const R* Di_src, R* Di_dst, R* adv, const R* U, const R* DU,
                 const uint8_t* mflux, const uint8_t* mupd, uint8_t* code, const R* f_b, const R* fi_src_b,
-                R* fi_dst_b) {
+                R* fi_dst_b, R* lo, R* lo_b) {
   if (nk <= 0) return 0;
   if (f_b && (code || adv)) return (int)cudaErrorInvalidValue;
   const SweepC<R> C = sweep_consts<R>(d, DIR, dt, splitfac, AH);
@@ -98,23 +98,26 @@ int run_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int sche
       }
       return (int)cudaGetLastError();
     };
+    // compensated storage (lo) only where the arithmetic is FP32
+    if (sizeof(R) == 8) lo = lo_b = nullptr;
     if (f_b) {
-      TracerSet<R, 2> set{{{f, fi_src, fi_dst}, {f_b, fi_src_b, fi_dst_b}}};
+      TracerSet<R, 2> set{{{f, fi_src, fi_dst, lo}, {f_b, fi_src_b, fi_dst_b, lo_b}}};
       return go(std::false_type(), set);
     }
-    TracerSet<R, 1> set{{{f, fi_src, fi_dst}}};
+    TracerSet<R, 1> set{{{f, fi_src, fi_dst, lo}}};
     return code ? go(std::true_type(), set) : go(std::false_type(), set);
   });
 }
 
 template <class R>
 int run_sweep_w2(const Dev& d, cudaStream_t s, R dt, R splitfac, int scheme, R* fa, R* fb, R* hi, const R* ww,
-                 const int32_t* az) {
+                 const int32_t* az, R* lo_a, R* lo_b) {
+  if (sizeof(R) == 8) lo_a = lo_b = nullptr;
   return dispatch_scheme(scheme, [&](auto sc) {
     constexpr int S = decltype(sc)::value;
     dim3 blk(64, 2, 1);
     dim3 grd((d.ni() - 1 + blk.x - 1) / blk.x, (d.nj() - 1 + blk.y - 1) / blk.y, 1);
-    k_sweep_w2<R, S><<<grd, blk, 0, s>>>(d, dt, splitfac, fa, fb, hi, ww, az);
+    k_sweep_w2<R, S><<<grd, blk, 0, s>>>(d, dt, splitfac, fa, fb, hi, ww, az, lo_a, lo_b);
     return (int)cudaGetLastError();
   });
 }
@@ -122,13 +125,14 @@ int run_sweep_w2(const Dev& d, cudaStream_t s, R dt, R splitfac, int scheme, R* 
 template <class R>
 int run_sweep_w(const Dev& d, cudaStream_t s, R dt, R splitfac, int scheme, int kshift, int itersmax,
                 const R* f, const R* fi_src, R* fi_dst, R* hi, R* adv, const R* ww, const int32_t* az,
-                unsigned long long* warn, uint8_t* code) {
+                unsigned long long* warn, uint8_t* code, R* lo) {
+  if (sizeof(R) == 8) lo = nullptr;
   if (itersmax > 1) {
     if (code) return (int)cudaErrorInvalidValue;
     dim3 blk(32, 2, 1);
     dim3 grd((d.ni() - 1 + blk.x - 1) / blk.x, (d.nj() - 1 + blk.y - 1) / blk.y, 1);
     k_sweep_w_iter<R><<<grd, blk, 0, s>>>(d, dt, splitfac, scheme, kshift, itersmax, f, fi_src, fi_dst, hi,
-                                          adv, ww, az, warn);
+                                          adv, ww, az, warn, lo);
     return (int)cudaGetLastError();
   }
   return dispatch_scheme(scheme, [&](auto sc) {
@@ -136,10 +140,11 @@ int run_sweep_w(const Dev& d, cudaStream_t s, R dt, R splitfac, int scheme, int 
     dim3 blk(64, 2, 1);
     dim3 grd((d.ni() - 1 + blk.x - 1) / blk.x, (d.nj() - 1 + blk.y - 1) / blk.y, 1);
     if (code)
-      k_sweep_w<R, S, true><<<grd, blk, 0, s>>>(d, dt, splitfac, kshift, f, fi_src, fi_dst, hi, adv, ww, az, code);
+      k_sweep_w<R, S, true><<<grd, blk, 0, s>>>(d, dt, splitfac, kshift, f, fi_src, fi_dst, hi, adv, ww, az, code,
+                                                lo);
     else
       k_sweep_w<R, S, false><<<grd, blk, 0, s>>>(d, dt, splitfac, kshift, f, fi_src, fi_dst, hi, adv, ww, az,
-                                                 nullptr);
+                                                 nullptr, lo);
     return (int)cudaGetLastError();
   });
 }
@@ -155,12 +160,13 @@ int run_finalise(const Dev& d, cudaStream_t s, R dt, R* f, const R* ho, const R*
 
 template <class R>
 int run_vdiff(const Dev& d, cudaStream_t s, R dt, R cnpar, R avmol, R* S, const R* hn, const R* nuh,
-              const int32_t* az, const R* src, R* rus, R* qus, const R* Sin, R* S2) {
+              const int32_t* az, const R* src, R* rus, R* qus, const R* Sin, R* S2, R* lo) {
   if (d.kmax <= 1) return 0;
+  if (sizeof(R) == 8) lo = nullptr;
   const int nx = d.imax - d.imin + 1, ny = d.jmax - d.jmin + 1;
   dim3 blk(32, 4, 1);
   dim3 grd((nx + 31) / 32, (ny + 3) / 4, 1);
-  k_vdiff<R><<<grd, blk, 0, s>>>(d, dt, cnpar, avmol, Sin ? Sin : S, S, hn, nuh, az, src, rus, qus, S2);
+  k_vdiff<R><<<grd, blk, 0, s>>>(d, dt, cnpar, avmol, Sin ? Sin : S, S, hn, nuh, az, src, rus, qus, S2, lo);
   return (int)cudaGetLastError();
 }
 
@@ -200,21 +206,21 @@ int run_check_range(const Dev& d, cudaStream_t s, const R* f, const int32_t* az,
 template int run_sweep_h<GB_REAL, 0>(const Dev&, cudaStream_t, int, GB_REAL, GB_REAL, int, GB_REAL,
                                      const GB_REAL*, const GB_REAL*, GB_REAL*, const GB_REAL*, GB_REAL*,
                                      GB_REAL*, const GB_REAL*, const GB_REAL*, const uint8_t*, const uint8_t*,
-                                     uint8_t*, const GB_REAL*, const GB_REAL*, GB_REAL*);
+                                     uint8_t*, const GB_REAL*, const GB_REAL*, GB_REAL*, GB_REAL*, GB_REAL*);
 template int run_sweep_h<GB_REAL, 1>(const Dev&, cudaStream_t, int, GB_REAL, GB_REAL, int, GB_REAL,
                                      const GB_REAL*, const GB_REAL*, GB_REAL*, const GB_REAL*, GB_REAL*,
                                      GB_REAL*, const GB_REAL*, const GB_REAL*, const uint8_t*, const uint8_t*,
-                                     uint8_t*, const GB_REAL*, const GB_REAL*, GB_REAL*);
+                                     uint8_t*, const GB_REAL*, const GB_REAL*, GB_REAL*, GB_REAL*, GB_REAL*);
 template int run_sweep_w2<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL, int, GB_REAL*, GB_REAL*, GB_REAL*,
-                                   const GB_REAL*, const int32_t*);
+                                   const GB_REAL*, const int32_t*, GB_REAL*, GB_REAL*);
 template int run_sweep_w<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL, int, int, int, const GB_REAL*,
                                   const GB_REAL*, GB_REAL*, GB_REAL*, GB_REAL*, const GB_REAL*, const int32_t*,
-                                  unsigned long long*, uint8_t*);
+                                  unsigned long long*, uint8_t*, GB_REAL*);
 template int run_finalise<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL*, const GB_REAL*, const GB_REAL*,
                                    const GB_REAL*, const uint8_t*);
 template int run_vdiff<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL, GB_REAL, GB_REAL*, const GB_REAL*,
                                 const GB_REAL*, const int32_t*, const GB_REAL*, GB_REAL*, GB_REAL*, const GB_REAL*,
-                                GB_REAL*);
+                                GB_REAL*, GB_REAL*);
 template int run_tridiag<GB_REAL>(cudaStream_t, int, int, int, int, const GB_REAL*, const GB_REAL*,
                                   const GB_REAL*, const GB_REAL*, GB_REAL*);
 template int run_content<GB_REAL>(const Dev&, cudaStream_t, const GB_REAL*, const GB_REAL*, const int32_t*,

@@ -17,6 +17,8 @@ bool fp32_micro_steps_enabled();
 constexpr int RED_BLOCKS = 1184;  // 8 x 148 SMs
 constexpr int RED_THREADS = 256;
 
+// lo (FP32 only; FP64 ignores it): compensated storage of a tracer, the carried rounding error of
+// every cell, read and written by the updates (fv_update_lo); null for plain FP32 storage.
 // Horizontal sweep over nk levels starting at the given level pointers. DIR 0 = u, 1 = v.
 // code != nullptr also writes the limiter branch of every face (one byte per face, stored at the
 // face's left / lower cell, same level pointer origin as f).
@@ -26,14 +28,14 @@ template <class R, int DIR>
 int run_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int scheme, R AH, const R* f,
                 const R* fi_src, R* fi_dst, const R* Di_src, R* Di_dst, R* adv, const R* U, const R* DU,
                 const uint8_t* mflux, const uint8_t* mupd, uint8_t* code = nullptr, const R* f_b = nullptr,
-                const R* fi_src_b = nullptr, R* fi_dst_b = nullptr);
+                const R* fi_src_b = nullptr, R* fi_dst_b = nullptr, R* lo = nullptr, R* lo_b = nullptr);
 
 // Vertical sweep on full 3D fields (level-0 pointers); code as above (face k stored at level k;
 // only without sub-iterations).
 template <class R>
 int run_sweep_w(const Dev& d, cudaStream_t s, R dt, R splitfac, int scheme, int kshift, int itersmax,
                 const R* f, const R* fi_src, R* fi_dst, R* hi, R* adv, const R* ww, const int32_t* az,
-                unsigned long long* warn, uint8_t* code = nullptr);
+                unsigned long long* warn, uint8_t* code = nullptr, R* lo = nullptr);
 
 // Depth-averaged momentum advection of one micro step with HALFSPLIT (adv2d_fused.cuh): UEx
 // (dir 0, U-grid masks) or VEx (dir 1, V-grid masks) from U, V, DU, DV in one launch, arithmetic
@@ -49,7 +51,7 @@ int run_uvadv2d_fused_f32(const Dev& d, cudaStream_t s, int dir, float dt, int s
 // Vertical sweep of two tracers in place (H_TAG, no sub-iterations), heights updated once.
 template <class R>
 int run_sweep_w2(const Dev& d, cudaStream_t s, R dt, R splitfac, int scheme, R* fa, R* fb, R* hi, const R* ww,
-                 const int32_t* az);
+                 const int32_t* az, R* lo_a = nullptr, R* lo_b = nullptr);
 
 // ---- adjoint of the tracer step (adjoint.cuh) ----
 // Layer heights before sweeps 2..5 of the HALFSPLIT sequence u/2 v/2 w v/2 u/2, from ho (levels
@@ -84,7 +86,8 @@ int run_finalise(const Dev& d, cudaStream_t s, R dt, R* f, const R* ho, const R*
 // (interior, az == 1) are written.
 template <class R>
 int run_vdiff(const Dev& d, cudaStream_t s, R dt, R cnpar, R avmol, R* S, const R* hn, const R* nuh,
-              const int32_t* az, const R* src, R* rus, R* qus, const R* Sin = nullptr, R* S2 = nullptr);
+              const int32_t* az, const R* src, R* rus, R* qus, const R* Sin = nullptr, R* S2 = nullptr,
+              R* lo = nullptr);
 
 template <class R>
 int run_tridiag(cudaStream_t s, int ncol, int kmax, int fi, int lt, const R* au, const R* bu, const R* cu,

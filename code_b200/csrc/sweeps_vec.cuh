@@ -303,15 +303,21 @@ __global__ void __launch_bounds__(32 * VKW) k_sweep_v_vec(Dev d, SweepC<R> C, in
     if (NF == 1 && adv) lds_vec<R, N>(sbuf[st][XAD][tid], ad);
 #pragma unroll
     for (int n = 0; n < NF; ++n) {
-      R fo[N];
+      R fo[N], lo[N];
+      const bool comp = F.t[n].lo && any;  // compensated storage: the cells' carried errors
+      if (comp) ld_row<R, N>(F.t[n].lo + p, full, navail, lo);
 #pragma unroll
       for (int m = 0; m < N; ++m) {
         const bool upd = jin && mbit(mu, m);
         const R advn = cell_advn<R>(C, fl_new[n][m], fl_old[n][m]);
-        fo[m] = upd ? fv_update<R>(Dio[m], dDv[m], Dn[m], fio[n][m], C.dt, advn) : fio[n][m];
+        if (comp)
+          fo[m] = upd ? fv_update_lo<R>(Dio[m], dDv[m], Dn[m], fio[n][m], C.dt, advn, lo[m]) : fio[n][m];
+        else
+          fo[m] = upd ? fv_update<R>(Dio[m], dDv[m], Dn[m], fio[n][m], C.dt, advn) : fio[n][m];
         if (NF == 1 && adv && upd) ad[m] = ad[m] + advn;
       }
       if (F.t[n].fi_dst && (any || F.t[n].fi_dst != F.t[n].fi_src)) st_row<R, N>(F.t[n].fi_dst + p, full, navail, fo);
+      if (comp) st_row<R, N>(F.t[n].lo + p, full, navail, lo);
     }
     if (Di_dst && (any || Di_dst != Di_src)) st_row<R, N>(Di_dst + p, full, navail, Dn);
     if (NF == 1 && adv && any) st_row<R, N>(adv + p, full, navail, ad);
@@ -491,13 +497,20 @@ __global__ void __launch_bounds__(32 * UWB) k_sweep_u_vec(Dev d, SweepC<R> C, in
         if constexpr (NF == 1) lds_vec<R, N>(sbuf[stc][1][tid], fio);
         else ld_row<R, N>(F.t[n].fi_src + p, full, navail, fio);
       }
+      R lo[N];
+      const bool comp = F.t[n].lo && any;  // compensated storage: the cells' carried errors
+      if (comp) ld_row<R, N>(F.t[n].lo + p, full, navail, lo);
 #pragma unroll
       for (int q = 0; q < N; ++q) {
         const R advn = cell_advn<R>(C, fl[n][q + 1], fl[n][q]);
-        fo[q] = updm[q] ? fv_update<R>(Dio[q], dDv[q], Dn[q], fio[q], C.dt, advn) : fio[q];
+        if (comp)
+          fo[q] = updm[q] ? fv_update_lo<R>(Dio[q], dDv[q], Dn[q], fio[q], C.dt, advn, lo[q]) : fio[q];
+        else
+          fo[q] = updm[q] ? fv_update<R>(Dio[q], dDv[q], Dn[q], fio[q], C.dt, advn) : fio[q];
         if (NF == 1 && adv && updm[q]) ad[q] = ad[q] + advn;
       }
       if (F.t[n].fi_dst && (any || F.t[n].fi_dst != F.t[n].fi_src)) st_row<R, N>(F.t[n].fi_dst + p, full, navail, fo);
+      if (comp) st_row<R, N>(F.t[n].lo + p, full, navail, lo);
     }
     if (Di_dst && (any || Di_dst != Di_src)) st_row<R, N>(Di_dst + p, full, navail, Dn);
     if (NF == 1 && adv && any) st_row<R, N>(adv + p, full, navail, ad);

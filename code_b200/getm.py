@@ -63,6 +63,9 @@ _PROTOS = {
     "getm_adv_split_u": [P, I, D, P, P, P, P, P, P, D, I, D, P, P],
     "getm_adv_split_v": [P, I, D, P, P, P, P, P, P, D, I, D, P, P],
     "getm_adv_split_w": [P, D, P, P, P, P, P, D, I, I, P, I],
+    "getm_adv_split_u_f32": [P, I, F, P, P, P, P, P, P, F, I, F, P, P],
+    "getm_adv_split_v_f32": [P, I, F, P, P, P, P, P, P, F, I, F, P, P],
+    "getm_adv_split_w_f32": [P, F, P, P, P, P, P, F, I, I, P, I],
     "getm_do_advection_3d": [P, D, P, P, P, P, P, P, P, P, I, I, I, D, I, P, P, I],
     "getm_do_advection_3d_f32": [P, F, P, P, P, P, P, P, P, P, I, I, I, F, I, P, P, I],
     "getm_tridiagonal_columns": [P, I, I, I, I, P, P, P, P, P],
@@ -105,6 +108,9 @@ _PROTOS = {
     "getm_sw_radiation": [P, P],
     "getm_sealevel_nan_check": [P, P, P, P, P],
     "getm_halo_pack": [P, P, I, I, I, I, P],
+    "getm_restart_fields": [I, P, P, P, P],
+    "getm_restart_write": [P, P, I, P, P],
+    "getm_restart_read": [P, P, I, P, P],
     "getm_halo_unpack": [P, P, I, I, I, I, P],
 }
 _RESTYPES = {"getm_ctx_last_error": C.c_char_p, "getm_version": C.c_char_p, "getm_timer_name": C.c_char_p}
@@ -126,6 +132,17 @@ def lib():
                 fn.restype = _RESTYPES.get(name, C.c_int)
             _lib = L
     return _lib
+
+
+def restart_fields(runtype: int):
+    """State-table indices (f2, f3) of the restart file's fields for a runtype, in the file's order."""
+    n2, n3 = C.c_int32(), C.c_int32()
+    a = (C.c_int32 * 64)()
+    b = (C.c_int32 * 64)()
+    rc = lib().getm_restart_fields(runtype, a, C.byref(n2), b, C.byref(n3))
+    if rc:
+        raise GetmError(rc, "restart_fields")
+    return list(a[:n2.value]), list(b[:n3.value])
 
 
 def set_fp32_micro_steps(on: bool) -> bool:
@@ -233,19 +250,22 @@ class Context:
     def adv_split_u(self, dt, f, fi, Di, adv, U, DU, splitfac, scheme, AH, mask_flux, mask_update, nk=None):
         _same_dtype(f, fi, Di, adv, U, DU)
         nk = nk if nk is not None else (f.shape[0] if f.dim() == 3 else 1)
-        self._check(self.L.getm_adv_split_u(self.h, nk, dt, _ptr(f), _ptr(fi), _ptr(Di), _ptr(adv), _ptr(U), _ptr(DU),
-                                            splitfac, scheme, AH, _mask(mask_flux), _mask(mask_update)))
+        fn = self.L.getm_adv_split_u if _is64(f) else self.L.getm_adv_split_u_f32
+        self._check(fn(self.h, nk, dt, _ptr(f), _ptr(fi), _ptr(Di), _ptr(adv), _ptr(U), _ptr(DU), splitfac, scheme, AH,
+                       _mask(mask_flux), _mask(mask_update)))
 
     def adv_split_v(self, dt, f, fi, Di, adv, V, DV, splitfac, scheme, AH, mask_flux, mask_update, nk=None):
         _same_dtype(f, fi, Di, adv, V, DV)
         nk = nk if nk is not None else (f.shape[0] if f.dim() == 3 else 1)
-        self._check(self.L.getm_adv_split_v(self.h, nk, dt, _ptr(f), _ptr(fi), _ptr(Di), _ptr(adv), _ptr(V), _ptr(DV),
-                                            splitfac, scheme, AH, _mask(mask_flux), _mask(mask_update)))
+        fn = self.L.getm_adv_split_v if _is64(f) else self.L.getm_adv_split_v_f32
+        self._check(fn(self.h, nk, dt, _ptr(f), _ptr(fi), _ptr(Di), _ptr(adv), _ptr(V), _ptr(DV), splitfac, scheme, AH,
+                       _mask(mask_flux), _mask(mask_update)))
 
     def adv_split_w(self, dt, f, fi, hi, adv, ww, splitfac, scheme, tag, az, itersmax=1):
         _same_dtype(f, fi, hi, adv, ww)
-        self._check(self.L.getm_adv_split_w(self.h, dt, _ptr(f), _ptr(fi), _ptr(hi), _ptr(adv), _ptr(ww), splitfac,
-                                            scheme, tag, _ptr(az), itersmax))
+        fn = self.L.getm_adv_split_w if _is64(f) else self.L.getm_adv_split_w_f32
+        self._check(fn(self.h, dt, _ptr(f), _ptr(fi), _ptr(hi), _ptr(adv), _ptr(ww), splitfac, scheme, tag, _ptr(az),
+                       itersmax))
 
     def do_advection_3d(self, dt, f, uu, vv, ww, hu, hv, ho, hn, split, hscheme, vscheme, AH, tag,
                         hires=None, advres=None, adv_ver_iterations=1):
@@ -258,6 +278,7 @@ class Context:
     def tridiagonal(self, kmax, fi, lt, au, bu, cu, du, value):
         """getm_tridiagonal (tridiagonal.F90:8-51) on the columns of [k][col] tensors."""
         ncol = au.shape[1]
+        _need64(au, bu, cu, du, value)
         self._check(self.L.getm_tridiagonal_columns(self.h, ncol, kmax, fi, lt, _ptr(au), _ptr(bu), _ptr(cu),
                                                     _ptr(du), _ptr(value)))
 
@@ -400,8 +421,40 @@ class Context:
     def sealevel_nan_check(self, z):
         """sealevel_nan_check (sealevel.F90:172-314): (count, (i, j) of the last finding or None)."""
         n, i, j = C.c_int64(), C.c_int32(), C.c_int32()
+        _need64(z)
         self._check(self.L.getm_sealevel_nan_check(self.h, _ptr(z), C.byref(n), C.byref(i), C.byref(j)))
         return int(n.value), ((int(i.value), int(j.value)) if n.value else None)
+
+    # hotstart: the restart file's fields (write_restart_ncdf.F90 / read_restart_ncdf.F90)
+    def restart_write(self, st: "BcDevice", runtype: int) -> dict:
+        """The restart fields' interiors as FP64 numpy arrays {name: (nk, ny, nx) or (ny, nx)}."""
+        import numpy as np
+
+        from . import state as S
+
+        i2, i3 = restart_fields(runtype)
+        g = self.grid
+        h2 = [np.zeros((g.ny, g.nx)) for _ in i2]
+        h3 = [np.zeros((g.kmax + 1, g.ny, g.nx)) for _ in i3]
+        p2 = (C.c_void_p * max(1, len(h2)))(*[a.ctypes.data for a in h2])
+        p3 = (C.c_void_p * max(1, len(h3)))(*[a.ctypes.data for a in h3])
+        self._check(self.L.getm_restart_write(self.h, C.byref(st.c), runtype, p2, p3 if h3 else None))
+        out = {S.F2_NAMES[q]: a for q, a in zip(i2, h2)}
+        out.update({S.F3_NAMES[q]: a for q, a in zip(i3, h3)})
+        return out
+
+    def restart_read(self, st: "BcDevice", runtype: int, fields: dict):
+        """Hotstart from restart-field interiors {name: FP64 array} (see restart_write)."""
+        import numpy as np
+
+        from . import state as S
+
+        i2, i3 = restart_fields(runtype)
+        h2 = [np.ascontiguousarray(fields[S.F2_NAMES[q]], np.float64) for q in i2]
+        h3 = [np.ascontiguousarray(fields[S.F3_NAMES[q]], np.float64) for q in i3]
+        p2 = (C.c_void_p * max(1, len(h2)))(*[a.ctypes.data for a in h2])
+        p3 = (C.c_void_p * max(1, len(h3)))(*[a.ctypes.data for a in h3])
+        self._check(self.L.getm_restart_read(self.h, C.byref(st.c), runtype, p2, p3 if h3 else None))
 
     # halo rows of a slab decomposition (update_3d_halo / update_2d_halo of the parallel build)
     def halo_pack(self, f, j_first: int, nrows: int, buf):
@@ -415,9 +468,19 @@ class Context:
         self._check(self.L.getm_halo_unpack(self.h, _ptr(f), f.element_size(), nk, j_first, nrows, _ptr(buf)))
 
     def check_3d_fields(self, f, az, minval, maxval) -> int:
+        _need64(f)
         st = C.c_int64()
         self._check(self.L.getm_check_3d_fields(self.h, _ptr(f), _ptr(az), minval, maxval, C.byref(st)))
         return st.value
+
+
+def _need64(*ts):
+    """The FP64-only entry points take FP64 tensors only (the library reads them as double)."""
+    import torch
+
+    for t in ts:
+        if t is not None and t.dtype != torch.float64:
+            raise TypeError(f"expected float64, got {t.dtype}")
 
 
 def _is64(t) -> bool:
@@ -441,14 +504,15 @@ def _mask(m):
 class BcState(C.Structure):
     """Mirror of getm_bc_state (include/getm_b200.h)."""
 
-    _fields_ = [("f2", P * 59), ("f3", P * 22), ("az", P), ("au", P), ("av", P), ("ax", P), ("par", D * 23),
+    _fields_ = [("f2", P * 59), ("f3", P * 24), ("az", P), ("au", P), ("av", P), ("ax", P), ("par", D * 23),
                 ("ipar", C.c_int32 * 25), ("prec3d", C.c_int32)]
 
 
 class BcDevice:
     """Device copy of a mode-split state (code_b200.state.BcCase) plus its C table."""
 
-    def __init__(self, case=None, dtype3=None, tensors=None, pd=None, pi=None):
+    def __init__(self, case=None, dtype3=None, tensors=None, pd=None, pi=None, compensated=True):
+        """compensated: with FP32 3D fields, keep the compensated storage of T and S (Tlo, Slo)."""
         import torch
 
         from . import state as S
@@ -459,6 +523,8 @@ class BcDevice:
             for n in S.F2_NAMES:
                 t["f2_" + n] = torch.from_numpy(case.f2[n]).cuda()
             for n in S.F3_NAMES:
+                if n in ("Tlo", "Slo") and (dt3 == torch.float64 or not compensated):
+                    continue
                 t["f3_" + n] = torch.from_numpy(case.f3[n]).to(dt3).cuda()
             for n, m in zip(("az", "au", "av", "ax"), case.masks()):
                 t[n] = torch.from_numpy(m).cuda()

@@ -20,7 +20,7 @@ F2_NAMES = ["z", "zo", "U", "V", "D", "DU", "DV", "UEx", "VEx", "fU", "fV", "ru"
             "ssvo", "ssvn", "Dn", "Dun", "Dvn", "rru", "rrv", "taubx", "tauby", "taub", "taus",
             "swr", "shf", "A", "g1", "g2"]
 F3_NAMES = ["uu", "vv", "ww", "ho", "hn", "huo", "hun", "hvo", "hvn", "uuEx", "vvEx", "idpdx", "idpdy", "T", "S",
-            "rho", "buoy", "num", "nuh", "rad", "tke", "eps"]
+            "rho", "buoy", "num", "nuh", "rad", "tke", "eps", "Tlo", "Slo"]
 PD_NAMES = ["dtm", "dt", "cnpar", "min_depth", "crit_depth", "g", "rho_0", "kappa", "avmmol", "avmolt", "avmols", "T0",
             "S0", "dtr0", "dsr0", "ip_fac", "temp_AH", "salt_AH", "avmback", "avhback", "cp", "swr_bot_refl_frac",
             "swr_min_bot_frac"]
@@ -29,9 +29,10 @@ PI_NAMES = ["M", "MM", "runtype", "vel2d_adv_split", "vel2d_adv_hor", "vel3d_adv
             "salt_adv_ver", "adv_ver_iterations", "ufirst2d", "ufirst3d", "calc_temp", "calc_salt", "ip_method",
             "viscosity", "eqstate_method", "sealevel_check", "radiation", "nan_warned"]
 # fields that only a switched-on option reads or writes (radiation: swr, shf, A, g1, g2, rad;
-# PARABOLIC_VISCOSITY: tke, eps, each optional): a device state may leave them out (NULL)
+# PARABOLIC_VISCOSITY: tke, eps, each optional; the mixed step's compensated storage of T and S:
+# Tlo, Slo): a device state may leave them out (NULL)
 OPTIONAL_F2 = ("swr", "shf", "A", "g1", "g2")
-OPTIONAL_F3 = ("rad", "tke", "eps")
+OPTIONAL_F3 = ("rad", "tke", "eps", "Tlo", "Slo")
 # values of the parameters added after the first fixtures were written (their defaults in the
 # reference: variables_3d.F90:120, parameters.F90:23, temperature.F90:50-51, m2d.F90:82,
 # eqstate.F90:27 -- where the configurations use the linear equation of state)
@@ -369,7 +370,8 @@ def _baroclinic_3d_numpy(c: BcCase, rng, nu_max):
 
 
 def baroclinic_case_device(nx=2048, ny=2048, kmax=50, recipe="islands", dx=1000.0, M=20, dt3=60.0, seed=6,
-                           dtype3=None, land=0.3, hmin=5.0, hmax=150.0, nu_max=1e-2, latitude=54.0, device="cuda"):
+                           dtype3=None, land=0.3, hmin=5.0, hmax=150.0, nu_max=1e-2, latitude=54.0, device="cuda",
+                           compensated=True):
     """:func:`baroclinic_case` with the 3D fields built on the device (for the 2048 x 2048 x 50
     domain, whose 19 FP64 3D fields would take ~33 GB of host memory). 2D fields and parameters
     are computed in numpy exactly as in baroclinic_case; the temperature noise comes from a seeded
@@ -421,6 +423,9 @@ def baroclinic_case_device(nx=2048, ny=2048, kmax=50, recipe="islands", dx=1000.
     t["f3_nuh"] = nuv.to(dtype3).contiguous()
     for n in ("uu", "vv", "ww", "uuEx", "vvEx", "idpdx", "idpdy"):
         t["f3_" + n] = torch.zeros(shp, dtype=dtype3, device=device)
+    if dtype3 == torch.float32 and compensated:  # the mixed step's compensated storage of T and S
+        t["f3_Tlo"] = torch.zeros(shp, dtype=dtype3, device=device)
+        t["f3_Slo"] = torch.zeros(shp, dtype=dtype3, device=device)
     return g, BcDevice(tensors=t, pd=dict(c.pd), pi=dict(c.pi))
 
 

@@ -151,6 +151,16 @@ int getm_adv_split_v(getm_ctx *ctx, int nk, double dt, const double *f, double *
 int getm_adv_split_w(getm_ctx *ctx, double dt, const double *f, double *fi, double *hi, double *adv,
                      const double *ww, double splitfac, int scheme, int tag, const int32_t *az,
                      int itersmax);
+/* The same three sweeps in FP32 (the arithmetic of the mixed-precision step). */
+int getm_adv_split_u_f32(getm_ctx *ctx, int nk, float dt, const float *f, float *fi, float *Di,
+                         float *adv, const float *U, const float *DU, float splitfac, int scheme,
+                         float AH, const uint8_t *mask_flux, const uint8_t *mask_update);
+int getm_adv_split_v_f32(getm_ctx *ctx, int nk, float dt, const float *f, float *fi, float *Di,
+                         float *adv, const float *V, const float *DV, float splitfac, int scheme,
+                         float AH, const uint8_t *mask_flux, const uint8_t *mask_update);
+int getm_adv_split_w_f32(getm_ctx *ctx, float dt, const float *f, float *fi, float *hi, float *adv,
+                         const float *ww, float splitfac, int scheme, int tag, const int32_t *az,
+                         int itersmax);
 
 /* do_advection_3d (src/3d/advection_3d.F90:120-598): NOSPLIT / FULLSPLIT / HALFSPLIT / HVSPLIT
  * with the split schemes UPSTREAM, P2, SUPERBEE, MUSCL, P2_PDM (the 2DH schemes are not
@@ -202,6 +212,7 @@ int getm_tracer_step_f32(getm_ctx *ctx, float dt, float *f, const float *uu, con
  *       zub zvb zub0 zvb0 fwf H HU HV dry_z dry_u dry_v coru corv tausx tausy airp sseo ssen
  *       ssuo ssun ssvo ssvn Dn Dun Dvn rru rrv taubx tauby taub taus swr shf A g1 g2
  *  f3:  uu vv ww ho hn huo hun hvo hvn uuEx vvEx idpdx idpdy T S rho buoy num nuh rad tke eps
+ *       Tlo Slo
  *  par: dtm dt cnpar min_depth crit_depth g rho_0 kappa avmmol avmolt avmols T0 S0 dtr0 dsr0
  *       ip_fac temp_AH salt_AH avmback avhback cp swr_bot_refl_frac swr_min_bot_frac
  *  ipar: M MM runtype vel2d_adv_split vel2d_adv_hor vel3d_adv_split vel3d_adv_hor
@@ -225,9 +236,16 @@ int getm_tracer_step_f32(getm_ctx *ctx, float dt, float *f, const float *uu, con
  * first finding, which sets nan_warned (the routine's SAVEd have_warned); sealevel_check > 0 makes a
  * finding an error: the call that made it returns GETM_ERR_CHECK (getm_time_loop at its end, after
  * finishing its steps; the reference stops at once). swr, shf, A, g1, g2 and rad may be NULL when
- * radiation = 0, tke and eps may always be NULL. */
+ * radiation = 0, tke and eps may always be NULL.
+ * Tlo, Slo (no counterpart in the reference; FP32 states only, may be NULL): compensated storage of
+ * the mixed step's temperature and salinity. T is then the unevaluated sum T + Tlo of two FP32
+ * numbers (likewise S): every advection sweep and diffusion solve adds its increment to T exactly and
+ * keeps the rounding error in Tlo (|Tlo| < half an ulp of T), so that the increments smaller than
+ * half an ulp of T -- which plain FP32 storage loses at every update, and which a tracer far from
+ * zero receives every sweep -- are kept. The fluxes and the equation of state read T alone. Start
+ * them at zero; NULL gives plain FP32 storage. The FP64 step ignores them. */
 #define GETM_NF2 59
-#define GETM_NF3 22
+#define GETM_NF3 24
 #define GETM_NPD 23
 #define GETM_NPI 25
 typedef struct getm_bc_state {
@@ -318,6 +336,30 @@ int getm_set_open_boundaries(getm_ctx *ctx, const getm_bdy *bdy);
 /* New boundary data for the following steps (get_2d_bdy's job in the reference): HOST arrays of
  * npoints values each (data_u / data_v may be NULL); switches off harmonic data. */
 int getm_set_bdy_data(getm_ctx *ctx, const double *data, const double *data_u, const double *data_v);
+
+/* ---- hotstart: the restart file's fields ------------------------------------------------- */
+/* The fields GETM writes to and reads from its restart file (write_restart_ncdf.F90:86-204,
+ * read_restart_ncdf.F90), in the file's order, as indices into getm_bc_state.f2 / .f3:
+ *   2D: z zo U SlUx Slru V SlVx Slrv; runtype >= 2 also ssen ssun ssvn sseo ssuo ssvo Uinto Vinto
+ *   3D (runtype >= 2): uu vv ww uuEx vvEx tke eps num nuh hn; runtype >= 3 also T S
+ * f2_ids / f3_ids (may be NULL) receive up to GETM_NF2 / GETM_NF3 indices; *n2, *n3 the counts. */
+int getm_restart_fields(int runtype, int32_t *f2_ids, int32_t *n2, int32_t *f3_ids, int32_t *n3);
+/* Device -> host for restart_file(WRITING) (output.F90:383): each restart field's extent in the file
+ * -- the interior imin..imax x jmin..jmax (x levels 0..kmax), no halos (cppdefs.h:161-170) -- into
+ * the HOST FP64 arrays host2[q] (nx*ny) and host3[q] (nx*ny*(kmax+1)), i fastest, in the order of
+ * getm_restart_fields; FP32 3D fields are widened, a NULL tke / eps is written as zeros.
+ * Synchronises. */
+int getm_restart_write(getm_ctx *ctx, const getm_bc_state *st, int runtype, double *const *host2,
+                       double *const *host3);
+/* Host -> device for a hotstart (restart_file(READING), then postinit_2d / postinit_3d of
+ * initialise.F90:331-334): the restart fields' interiors from host arrays laid out as above (FP32
+ * 3D fields narrowed; halo values are kept), then postinit_2d (m2d.F90:358-400: where any U or V is
+ * non-zero on a closed velocity point, U, Uinto / V, Vinto = 0 on all closed points; z = zo = -9999
+ * on land; depth_update) and, for runtype >= 2, postinit_3d (m3d.F90:376-409: uu = 0 where au = 0,
+ * vv = 0 where av = 0; on land tke = 0, num = nuh = 1e-15, T = S = -9999; the layer heights by
+ * coordinates(hotstart)). The SAVEd switches in ipar (ufirst2d, ufirst3d) are the caller's. */
+int getm_restart_read(getm_ctx *ctx, getm_bc_state *st, int runtype, const double *const *host2,
+                      const double *const *host3);
 
 /* ---- halo rows of a slab decomposition ---------------------------------------------------- */
 /* The row exchange of the reference's parallel build (update_3d_halo / update_2d_halo,

@@ -120,7 +120,7 @@ BC_ROUTINES = ["bottom_friction", "uv_advect_2d", "umomentum", "vmomentum", "sea
                "start_macro", "bottom_friction_3d", "internal_pressure", "uu_momentum_3d", "vv_momentum_3d",
                "sigma_coordinates", "ww_momentum_3d", "uv_advect_3d", "stresses_3d", "do_eqstate",
                "slow_bottom_friction", "slow_terms", "integrate_2d", "integrate_3d", "gotm_parabolic", "sw_radiation",
-               "update_2d_bdy"]
+               "update_2d_bdy", "hotstart_postinit"]
 
 
 def bc_sizes():

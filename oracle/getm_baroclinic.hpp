@@ -31,7 +31,8 @@ enum F2 {
   SSUN, SSVO, SSVN, DN, DUN, DVN, RRU, RRV, TAUBX, TAUBY, TAUB, TAUS, SWR, SHF, ATT_A, ATT_G1, ATT_G2, NF2
 };
 enum F3 {
-  UU, VV, WW, HO, HN, HUO, HUN, HVO, HVN, UUEX, VVEX, IDPDX, IDPDY, TT, SS, RHO, BUOY, NUM, NUH, RAD, TKE, EPS, NF3
+  UU, VV, WW, HO, HN, HUO, HUN, HVO, HVN, UUEX, VVEX, IDPDX, IDPDY, TT, SS, RHO, BUOY, NUM, NUH, RAD, TKE, EPS,
+  TLO, SLO, NF3  // TLO, SLO: the mixed step's compensated storage (not read by the FP64 restatement)
 };
 enum PD {
   P_DTM, P_DT, P_CNPAR, P_MIN_DEPTH, P_CRIT_DEPTH, P_G, P_RHO_0, P_KAPPA, P_AVMMOL, P_AVMOLT, P_AVMOLS, P_T0, P_S0,
@@ -1406,6 +1407,58 @@ void slow_terms(const Dom& d, BcState<R3>& st) {
       if (av(i, j) >= 1)
         Slrv(i, j) = -Vint(i, j) / (0.5 * (ssvo(i, j) + ssvn(i, j)) + HV_(i, j)) * rv(i, j) +
                      (double)vv(i, j, 1) / (0.5 * ((double)hvo(i, j, 1) + (double)hvn(i, j, 1))) * rrv(i, j);
+}
+
+// Hotstart (initialise.F90:295-334 with hotstart = .true.): after read_restart_ncdf has filled the
+// restart fields, postinit_2d (m2d.F90:358-400) and postinit_3d (m3d.F90:376-409) re-derive the rest.
+// postinit_2d: if any U /= 0 where au == 0 (or V /= 0 where av == 0), U, Uinto = 0 where au == 0
+// and V, Vinto = 0 where av == 0; z = zo = -9999 on land (az == 0); depth_update. postinit_3d
+// (runtype > 1): uu = 0 where au == 0, vv = 0 where av == 0; on land tke = 0, num = nuh = 1e-15
+// (a single-precision literal), T = S = -9999; coordinates(hotstart), i.e. sigma_coordinates.
+template <class R3>
+void hotstart_postinit(const Dom& d, BcState<R3>& st, int runtype) {
+  double** f2 = st.f2;
+  A2 U{d, f2[U_]}, V{d, f2[V_]}, Uinto{d, f2[UINTO]}, Vinto{d, f2[VINTO]}, z{d, f2[Z]}, zo{d, f2[ZO]};
+  M2 az{d, st.az}, au{d, st.au}, av{d, st.av};
+  bool change = false;
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO; ++i) {
+      if (au(i, j) == 0 && U(i, j) != 0.0) change = true;
+      if (av(i, j) == 0 && V(i, j) != 0.0) change = true;
+    }
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO; ++i) {
+      if (change && au(i, j) == 0) {
+        U(i, j) = 0.0;
+        Uinto(i, j) = 0.0;
+      }
+      if (change && av(i, j) == 0) {
+        V(i, j) = 0.0;
+        Vinto(i, j) = 0.0;
+      }
+      if (az(i, j) == 0) {
+        z(i, j) = -9999.0;
+        zo(i, j) = -9999.0;
+      }
+    }
+  depth_update(d, f2, st.az, st.au, st.av, st.par);
+  if (runtype <= 1) return;
+  A3<R3> uu{d, st.f3[UU]}, vv{d, st.f3[VV]}, tke{d, st.f3[TKE]}, num{d, st.f3[NUM]}, nuh{d, st.f3[NUH]},
+      T{d, st.f3[TT]}, S{d, st.f3[SS]};
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO; ++i)
+      for (int k = 0; k <= d.kmax; ++k) {
+        if (au(i, j) == 0) uu(i, j, k) = R3(0);
+        if (av(i, j) == 0) vv(i, j, k) = R3(0);
+        if (az(i, j) == 0) {
+          if (st.f3[TKE]) tke(i, j, k) = R3(0);
+          num(i, j, k) = R3((double)1.e-15f);
+          nuh(i, j, k) = R3((double)1.e-15f);
+          S(i, j, k) = R3(-9999.0);
+          T(i, j, k) = R3(-9999.0);
+        }
+      }
+  sigma_coordinates(d, st);
 }
 
 // m3d.F90:422-636 integrate_3d for runtype 4 (see header for the configuration covered)

@@ -243,7 +243,7 @@ enum {
   BC_BOTTOM_FRICTION = 0, BC_UV_ADVECT_2D, BC_UMOMENTUM, BC_VMOMENTUM, BC_SEALEVEL, BC_DEPTH_UPDATE,
   BC_START_MACRO, BC_BOTTOM_FRICTION_3D, BC_IP, BC_UU_MOMENTUM_3D, BC_VV_MOMENTUM_3D, BC_SIGMA, BC_WW,
   BC_UV_ADVECT_3D, BC_STRESSES_3D, BC_EQSTATE, BC_SLOW_BOTTOM_FRICTION, BC_SLOW_TERMS, BC_INTEGRATE_2D,
-  BC_INTEGRATE_3D, BC_GOTM_PARABOLIC, BC_SW_RADIATION, BC_UPDATE_2D_BDY
+  BC_INTEGRATE_3D, BC_GOTM_PARABOLIC, BC_SW_RADIATION, BC_UPDATE_2D_BDY, BC_HOTSTART_POSTINIT
 };
 
 extern "C++" {
@@ -284,6 +284,7 @@ static int bc_call(const or_dom* o, or_bc* s, int which, int arg) {
     case BC_INTEGRATE_3D: rc = gor::integrate_3d(d, m, st, arg); break;
     case BC_GOTM_PARABOLIC: gor::gotm_parabolic(d, st); break;
     case BC_SW_RADIATION: gor::sw_radiation(d, st); break;
+    case BC_HOTSTART_POSTINIT: gor::hotstart_postinit(d, st, arg); break;
     case BC_UPDATE_2D_BDY:
       if (st.bdy && st.bdy->nseg() > 0) gor::update_2d_bdy(d, *st.bdy, st.f2, st.par, arg);
       break;

@@ -2,7 +2,8 @@
 one process (their halo-row exchange is the library's pack / unpack kernels with a device copy in
 between -- no kernels that wait on one another), each stepped by the library's sweeps and diffusion
 solve, against the undivided domain's getm_tracer_step: every interior cell bit for bit, FP64 and
-FP32. The halo pack / unpack kernels are also checked against plain row slicing."""
+FP32. And the GPU slabs against the oracle's slabs (the checker of the decomposition on CPU) after
+every phase of two steps: whole slabs, halo rows and columns included, FP64 bit for bit. The halo pack / unpack kernels are also checked against plain row slicing."""
 import numpy as np
 import pytest
 
@@ -47,7 +48,9 @@ def test_slabs_match_single_domain(world, dtype):
     got[:, 2:-2, :] = np.nan
     for r, part in parts.items():
         part.slab.put(host(part.t["f"]), got)
-    assert np.array_equal(got, want)
+    # the interior cells (the halo columns of a closed domain are land, where the undivided step's
+    # scratch ping-pong and the slabs' in-place sweeps leave different bytes)
+    assert np.array_equal(got[:, 2:-2, 2:-2], want[:, 2:-2, 2:-2])
 
 
 def test_halo_pack_unpack_rows():
@@ -66,3 +69,38 @@ def test_halo_pack_unpack_rows():
         torch.cuda.synchronize()
         assert torch.equal(g[:, 1:3, :], f[:, 5:7, :])
         assert float(g[:, 3:, :].abs().max()) == 0.0 and float(g[:, 0, :].abs().max()) == 0.0
+
+
+def test_slab_phases_vs_oracle_slabs():
+    import torch
+
+    from test_slabs_cpu import OracleSlabPart
+
+    c = cases.random_case(nx=37, ny=31, kmax=7, seed=12, land=0.25, open_bdy=True)
+    dt, hs, vs, AH, cnpar, avmol = c.par["dt"], 6, 4, -1.0, float(np.float32(0.9)), 1.1e-9
+    gp, op = {}, {}
+    for sl in slabs.slabs_of(c.grid, 2):
+        cx = Context(sl.grid)
+        m = [dev(sl.take(a)) for a in c.masks()]
+        cx.init_advection(*m)
+        tt = {n: dev(sl.take(c[n])) for n in ("f",) + NAMES}
+        gp[sl.rank] = slabs.GpuSlabPart(sl, cx, tt["f"], tt["uu"], tt["vv"], tt["ww"], tt["hun"], tt["hvn"],
+                                        tt["ho"], tt["hn"], tt["nuh"], m[0])
+        op[sl.rank] = OracleSlabPart(sl, c)
+    gx, ox = slabs.RowExchange(gp), slabs.RowExchange(op)
+    phases = [lambda p: p.begin(), lambda p: p.sweep_u(dt, 0.5, hs, AH), lambda p: p.sweep_v(dt, 0.5, hs, AH),
+              lambda p: p.sweep_w(dt, vs, 10), None, lambda p: p.sweep_v(dt, 0.5, hs, AH),
+              lambda p: p.sweep_u(dt, 0.5, hs, AH), lambda p: p.vdiff(dt, cnpar, avmol), None]
+    for step in range(2):
+        for q, fn in enumerate(phases):
+            if fn is None:
+                gx.exchange("f")
+                ox.exchange("f")
+            else:
+                for r in gp:
+                    fn(gp[r])
+                    fn(op[r])
+            torch.cuda.synchronize()
+            for r in gp:
+                assert np.array_equal(host(gp[r].t["f"]), op[r].t["f"]), (step, q, r)
+                assert np.array_equal(host(gp[r].hi), op[r].hi), (step, q, r)
