@@ -369,6 +369,15 @@ def _present(x):
     return x is not None
 
 
+def _wassign(lhs, rhs, mask):
+    """An assignment inside a WHERE construct: the elements of lhs where mask holds."""
+    r = _arr(rhs)
+    if np.ndim(r) == 0:
+        lhs.a[mask] = r
+    else:
+        lhs.a[mask] = np.asarray(r)[mask]
+
+
 class _Out(dict):
     """Final values of a subroutine's scalar dummy arguments, by position: the caller copies them
     back into actual arguments that are variables or array elements (Fortran passes by reference;
@@ -528,7 +537,7 @@ def _real_literal(txt: str) -> str:
     if "d" in t:
         return repr(float(t.replace("d", "e"))).join(("np.float64(", ")"))
     if "." in t or "e" in t:
-        if kind == "8":
+        if kind in ("8", "rk"):  # rk = kind(_ONE_), the double kind (register_all_variables.F90:35)
             return f"np.float64({float(t)!r})"
         # default-kind real literal: single precision, widened where used in double context
         return f"np.float64(np.float32({float(t)!r}))"
@@ -1037,6 +1046,43 @@ class Gen:
     def stmt(self, s: str):
         low = s.lower().strip()
         sc = self.scope
+        # WHERE constructs (block and single-statement forms) with plain array assignments
+        if not hasattr(self, "wstack"):
+            self.wstack, self.nwhere = [], 0
+        m = re.match(r"^where\s*\((.*)$", low)
+        if m and not low.startswith("where_"):
+            rest = low[low.index("("):]
+            depth, q = 0, 0
+            for q, ch in enumerate(rest):
+                depth += ch == "("
+                depth -= ch == ")"
+                if depth == 0:
+                    break
+            cond, tail = rest[1:q], rest[q + 1:].strip()
+            self.nwhere += 1
+            w = f"_w{self.nwhere}"
+            self.emit(f"{w} = np.asarray(_arr({tr_expr(cond, sc)}), dtype=bool)")
+            self.wstack.append(w)
+            if tail:
+                self.stmt(tail)
+                self.wstack.pop()
+            return
+        if re.match(r"^else\s*where$", low):
+            w = self.wstack[-1]
+            self.emit(f"{w} = ~{w}")
+            return
+        if re.match(r"^end\s*where$", low):
+            self.wstack.pop()
+            return
+        if self.wstack:
+            k = _top_assign(low)
+            if k is None:
+                raise SyntaxError(f"unsupported statement in WHERE: {s}")
+            lhs = low[:k].strip()
+            if not re.match(r"^\w+$", lhs):
+                raise SyntaxError(f"unsupported WHERE assignment target: {s}")
+            self.emit(f"_wassign({pyname(lhs)}, {tr_expr(low[k + 1:].strip(), sc)}, {self.wstack[-1]})")
+            return
         m = re.match(r"^if\s*\((.*)\)\s*then$", low)
         if m and _balanced_prefix(low[2:].strip()):
             self.emit(f"if {tr_expr(m.group(1), sc)}:")

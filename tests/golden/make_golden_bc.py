@@ -387,8 +387,63 @@ def nan_check_fixture():
     print(f"wrote {path}")
 
 
+RESTART_2D = ["z", "zo", "U", "SlUx", "Slru", "V", "SlVx", "Slrv", "ssen", "ssun", "ssvn", "sseo", "ssuo", "ssvo",
+              "Uinto", "Vinto"]
+RESTART_3D = ["uu", "vv", "ww", "uuEx", "vvEx", "tke", "eps", "num", "nuh", "hn", "T", "S"]
+
+
+def hotstart_fixture():
+    """tests/golden/reference_hotstart.npz: the reference's hotstart re-initialisation. A state is run
+    8 micro steps by the reference; the interiors of its restart fields (write_restart_ncdf.F90:86-204,
+    runtype 4) are the 'file'. A fresh state of the same basin gets those interiors (the halos keep
+    the fresh state's values, as read_restart_ncdf leaves them), with a non-zero U and V placed on a
+    closed velocity point, then the reference's postinit_2d and postinit_3d (m2d.F90:325-403,
+    m3d.F90:302-412) run with hotstart = .true.: out_* is the state after them."""
+    c = S.baroclinic_case(nx=12, ny=10, kmax=5, recipe="islands", land=0.3, M=4, dt3=60.0, seed=7)
+    r = RefBc(c.copy())
+    r.time_loop(1, 8)
+    done = r.state()
+    g = c.grid
+    it = (slice(2, 2 + g.ny), slice(2, 2 + g.nx))
+    out = {"meta": np.array([g.nx, g.ny, g.kmax, g.dx, g.dy])}
+    fresh = c.copy()
+    file2 = {k: done["f2_" + k][it].copy() for k in RESTART_2D}
+    file3 = {k: done["f3_" + k][(slice(None),) + it].copy() for k in RESTART_3D}
+    # a closed U point and a closed V point of the interior with a non-zero value in the file
+    ju, iu = [int(x) for x in np.argwhere(c.au[it] == 0)[0]]
+    jv, iv = [int(x) for x in np.argwhere(c.av[it] == 0)[0]]
+    file2["U"][ju, iu] = 0.125
+    file2["V"][jv, iv] = -0.25
+    file2["Uinto"][ju, iu] = 3.0
+    for k, v in file2.items():
+        fresh.f2[k][it] = v
+        out["file_f2_" + k] = v
+    for k, v in file3.items():
+        fresh.f3[k][(slice(None),) + it] = v
+        out["file_f3_" + k] = v
+    pre = c.copy()  # the state before the file is read (the case's initial state)
+    for k in S.F2_NAMES:
+        out["in_f2_" + k] = pre.f2[k]
+    for k in S.F3_NAMES:
+        out["in_f3_" + k] = pre.f3[k]
+    for k, v in zip(("az", "au", "av", "ax"), c.masks()):
+        out["in_" + k] = v
+    out["in_pd"] = np.array([c.pd[n] for n in S.PD_NAMES])
+    out["in_pi"] = np.array([c.pi[n] for n in S.PI_NAMES])
+    out["names_pd"] = np.array(S.PD_NAMES)
+    out["names_pi"] = np.array(S.PI_NAMES)
+    rh = RefBc(fresh)
+    rh.P.modules["m2d"].postinit_2d(4, np.float64(c.pd["dtm"]), True)
+    rh.P.modules["m3d"].postinit_3d(4, np.float64(c.pd["dt"]), True)
+    for k, v in rh.state().items():
+        out["out_" + k] = v
+    path = os.path.join(HERE, "reference_hotstart.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path} ({os.path.getsize(path) / 1024:.0f} KiB)")
+
+
 def main():
-    which = sys.argv[1:] or ["closed", "bdy", "ip2", "ip4", "ip5", "ip6", "phys3", "phys2", "nan"]
+    which = sys.argv[1:] or ["closed", "bdy", "ip2", "ip4", "ip5", "ip6", "phys3", "phys2", "nan", "hotstart"]
     if "closed" in which:
         write(S.baroclinic_case(nx=12, ny=10, kmax=4, recipe="shelf", M=4, dt3=60.0, seed=3),
               "reference_mode_split.npz")
@@ -401,6 +456,8 @@ def main():
         write(phys_case(3, parabolic=True, reflection=True), "reference_mode_split_phys3.npz")
     if "nan" in which:
         nan_check_fixture()
+    if "hotstart" in which:
+        hotstart_fixture()
     if "phys2" in which:  # UNESCO80, prescribed viscosity, radiation without reflection
         write(phys_case(2, parabolic=False, reflection=False, seed=9), "reference_mode_split_phys2.npz")
 

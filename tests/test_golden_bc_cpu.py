@@ -157,3 +157,29 @@ def test_native_oracle_build_is_bit_exact():
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     r = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0 and "ok" in r.stdout, r.stderr[-2000:]
+
+
+GOLD_HOT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_hotstart.npz")
+
+
+def hotstart_case(gold):
+    """The fixture's state before the restart file is read, and the file's interiors {name: array}."""
+    c = load_case(gold)
+    files = {k[8:]: gold[k] for k in gold if k.startswith("file_f2_")}
+    files.update({k[8:]: gold[k] for k in gold if k.startswith("file_f3_")})
+    return c, files
+
+
+def test_hotstart_postinit_matches_reference():
+    """The oracle's hotstart re-initialisation (postinit_2d / postinit_3d with hotstart = .true.)
+    after the restart file's interiors are read, against the reference's own routines on the same
+    inputs (tests/golden/reference_hotstart.npz): every field bit for bit."""
+    g = dict(np.load(GOLD_HOT))
+    c, files = hotstart_case(g)
+    for k, v in files.items():
+        (c.f2 if k in c.f2 and v.ndim == 2 else c.f3)[k][..., 2:-2, 2:-2] = v
+    oracle.bc_call(c, "hotstart_postinit", 4)
+    for k in gold_names(g, "f2"):
+        assert np.array_equal(c.f2[k], g["out_f2_" + k], equal_nan=True), k
+    for k in gold_names(g, "f3"):
+        assert np.array_equal(c.f3[k], g["out_f3_" + k], equal_nan=True), k
