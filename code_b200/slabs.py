@@ -112,13 +112,14 @@ class RowExchange:
         sends, recvs, ops = [], [], []
         for r, p in self.parts.items():
             s = p.slab
-            for nb, (first, dst_first) in ((s.north, (s.ny - HALO + 1, 1 - HALO)),
-                                           (s.south, (1, s.ny + 1))):
-                # rows first..first+1 of this slab go into rows dst_first.. of the neighbour
+            for nb, first in ((s.north, s.ny - HALO + 1), (s.south, 1)):
+                # rows first..first+1 of this slab go into the neighbour's halo rows on this side:
+                # rows 1-HALO.. of the northern neighbour, rows ny+1.. (its own ny) of the southern one
                 if nb is None:
                     continue
                 buf = p.pack(name, first)
                 if nb in self.parts:
+                    dst_first = 1 - HALO if nb == s.north else self.parts[nb].slab.ny + 1
                     self.parts[nb].unpack(name, dst_first, buf)
                 else:
                     sends.append(buf)

@@ -136,6 +136,26 @@ def _rank(rank, world, port, out):
         dist.destroy_process_group()
 
 
+@pytest.mark.parametrize("world", [2, 3, 4])
+def test_slabs_in_one_process_match_single_domain(world):
+    """All slabs held by one process (their exchange is a copy between the parts, the form the GPU
+    test on one device uses), slabs of unequal row counts (21 rows into 11 + 10, 7 + 7 + 7 and
+    6 + 5 + 5 + 5): every interior cell bit for bit after several steps."""
+    from code_b200 import slabs
+
+    c = _case()
+    want = _single_domain(c)
+    parts = {sl.rank: OracleSlabPart(sl, c) for sl in slabs.slabs_of(c.grid, world)}
+    ex = slabs.RowExchange(parts)
+    for _ in range(STEPS):
+        slabs.tracer_step(parts, ex, c.par["dt"], SCHEMES[0], SCHEMES[1], AH, CNPAR, AVMOL)
+    got = want.copy()
+    got[:, 2:-2, :] = np.nan
+    for p in parts.values():
+        p.slab.put(p.t["f"], got)
+    assert np.array_equal(got[:, 2:-2, 2:-2], want[:, 2:-2, 2:-2])
+
+
 @pytest.mark.parametrize("world", [2, 3])
 def test_slab_tracer_steps_match_single_domain(world):
     import oracle
