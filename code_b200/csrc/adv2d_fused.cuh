@@ -15,7 +15,7 @@
 
 namespace gb {
 
-constexpr int FX = 32, FY = 16;             // own tile
+constexpr int FX = 56, FY = 16;             // own tile (region rows of two full warps)
 constexpr int RW = FX + 8, RH = FY + 4;     // staged region: i in [-4, FX+3], j in [-2, FY+1]
 constexpr int FTY = 8;                      // thread rows: a block is RW x FTY threads, lane x <-> region column
 constexpr int FT = RW * FTY;                // threads per block
@@ -42,8 +42,10 @@ struct Adv2dSmem {
   T Ua[RH][RW], DUa[RH][RW], Va[RH][RW], DVa[RH][RW];  // face transports / depths
   T FL[RH][RW];   // face fluxes of the current sweep
   T A[FY][FX];    // flux divergence of the own cells, summed over the sweeps (adv = 0 + u/2 + v + u/2)
+  T Q[RH][RW];    // bottom friction: the other component's velocity V/DV (DIR 0) or U/DU (DIR 1)
   uint8_t mfu[RH][RW], mfv[RH][RW], mpu[RH][RW], mpv[RH][RW];
 };
+
 
 // DIR 0: UEx on the U grid (fadv = U/DU, faces between U points); DIR 1: VEx on the V grid.
 // TI: the storage type of U, V, DU, DV and Ex (FP64 state arrays, or the FP32 working copies of
@@ -55,7 +57,8 @@ __global__ void __launch_bounds__(FT) k_uvadv2d_fused(Dev d, T dt, const TI* __r
                                                       const uint8_t* __restrict__ mflux_u,
                                                       const uint8_t* __restrict__ mflux_v,
                                                       const uint8_t* __restrict__ mupd_u,
-                                                      const uint8_t* __restrict__ mupd_v, TI* __restrict__ Ex) {
+                                                      const uint8_t* __restrict__ mupd_v, TI* __restrict__ Ex,
+                                                      Bf2Args bf) {
   extern __shared__ unsigned char smem_raw[];
   Adv2dSmem<T>& sm = *reinterpret_cast<Adv2dSmem<T>*>(smem_raw);
   const int ni = d.ni(), nj = d.nj();
@@ -70,10 +73,12 @@ __global__ void __launch_bounds__(FT) k_uvadv2d_fused(Dev d, T dt, const TI* __r
   const bool iin = ii >= 0 && ii < ni;
   for (int r = ty; r < RH; r += FTY) {
     const int jj = jj0 - 2 + r;
-    T f0 = zero, ua = zero, dua = zero, va = zero, dva = zero, dio = zero;
+    T f0 = zero, ua = zero, dua = zero, va = zero, dva = zero, dio = zero, oq = zero;
     uint8_t a = 0, b = 0, c2 = 0, e2 = 0;
     if (iin && jj >= 0 && jj < nj) {
       const long long c = (long long)jj * sj + ii;
+      if constexpr (sizeof(T) == 4 && sizeof(TI) == 4)
+        if (bf.r) oq = DIR == 0 ? float(V[c]) / float(DV[c]) : float(U[c]) / float(DU[c]);
       a = mflux_u[c];
       b = mflux_v[c];
       c2 = mupd_u[c];
@@ -90,6 +95,7 @@ __global__ void __launch_bounds__(FT) k_uvadv2d_fused(Dev d, T dt, const TI* __r
       }
     }
     sm.F0[r][q] = f0;
+    sm.Q[r][q] = oq;
     sm.Ua[r][q] = ua;
     sm.DUa[r][q] = dua;
     sm.Va[r][q] = va;
@@ -197,12 +203,63 @@ __global__ void __launch_bounds__(FT) k_uvadv2d_fused(Dev d, T dt, const TI* __r
         if (ii < ni && jj < nj) Ex[(long long)jj * sj + ii] = (TI)a;
       }
   }
+  if constexpr (sizeof(T) == 4 && sizeof(TI) == 4) {
+    if (bf.r && qown) {
+      // F0 rows 2.. of the region still hold the staged U/DU (DIR 0) or V/DV (DIR 1) only where the
+      // v sweep left them: the own quotient is re-formed from the arrays (a single division)
+      for (int r = 2 + ty; r < RH - 2; r += FTY) {
+        const int jj = jj0 - 2 + r;
+        if (ii >= ni || jj >= nj) continue;
+        const long long c = (long long)jj * sj + ii;
+        const int i = ii + d.imin - HALO, j = jj + d.jmin - HALO;
+        const bool in = i >= d.imin && i <= d.imax && j >= d.jmin && j <= d.jmax;
+        const float q4 = 0.25f, h = 0.5f, kappa = bf.kappa, avmmol = bf.avmmol, min_depth = bf.min_depth;
+        float uloc, vloc, HHl;
+        bool on;
+        if (DIR == 0) {
+          on = i <= d.imax + HALO - 1 && bf.mask[c] > 0;
+          if (!on) continue;
+          vloc = in ? __fmul_rn(q4, __fadd_rn(__fadd_rn(__fadd_rn(sm.Q[r][q], sm.Q[r][q + 1]), sm.Q[r - 1][q]),
+                                              sm.Q[r - 1][q + 1]))
+                    : 0.f;
+          uloc = float(U[c]) / float(DU[c]);
+          HHl = fmaxf(min_depth, float(DU[c]));
+        } else {
+          on = j <= d.jmax + HALO - 1 && bf.mask[c] > 0;
+          if (!on) continue;
+          if (in)
+            uloc = __fmul_rn(q4, __fadd_rn(__fadd_rn(__fadd_rn(sm.Q[r][q], sm.Q[r][q - 1]), sm.Q[r + 1][q]),
+                                           sm.Q[r + 1][q - 1]));
+          else
+            uloc = (i <= d.imax + HALO - 1 && bf.au[c] > 0) ? sm.Q[r][q] : 0.f;
+          vloc = float(V[c]) / float(DV[c]);
+          HHl = fmaxf(min_depth, float(DV[c]));
+        }
+        // explicitly rounded operations: this unit contracts multiply-adds, the separate kernel's
+        // does not
+        const float zb = float(bf.zb[c]);
+        const float sp = __fadd_rn(__fmul_rn(uloc, uloc), __fmul_rn(vloc, vloc));
+        float x = kappa / logf(__fadd_rn(zb, __fmul_rn(h, HHl)) / zb);
+        float rr = __fmul_rn(x, x);
+        if (bf.runtype == 1) {
+          const float fricvel = sqrtf(__fmul_rn(rr, sp));
+          const float zn = fminf(HHl, __fadd_rn(float(bf.zb0[c]), __fmul_rn(0.1f, avmmol) / fmaxf(avmmol, fricvel)));
+          bf.zb[c] = zn;
+          rr = __fadd_rn(zn, __fmul_rn(h, HHl)) / zn;
+          x = kappa / logf(rr);
+          rr = __fmul_rn(x, x);
+        }
+        bf.rr[c] = rr;
+        bf.r[c] = __fmul_rn(rr, sqrtf(sp));
+      }
+    }
+  }
 }
 
 template <class T, int S, int DIR, class TI>
 int launch_uvadv2d_fused(const Dev& d, cudaStream_t s, T dt, const TI* U, const TI* V, const TI* DU, const TI* DV,
                          const uint8_t* mflux_u, const uint8_t* mflux_v, const uint8_t* mupd_u,
-                         const uint8_t* mupd_v, TI* Ex) {
+                         const uint8_t* mupd_v, TI* Ex, const Bf2Args& bf) {
   const size_t smem = sizeof(Adv2dSmem<T>);
   // opt-in above 48 KB of shared memory (a host-side setting of the current device's function)
   const cudaError_t e = cudaFuncSetAttribute(k_uvadv2d_fused<T, S, DIR, TI>,
@@ -210,18 +267,19 @@ int launch_uvadv2d_fused(const Dev& d, cudaStream_t s, T dt, const TI* U, const 
   if (e != cudaSuccess) return (int)e;
   dim3 grd((d.ni() + FX - 1) / FX, (d.nj() + FY - 1) / FY, 1);
   k_uvadv2d_fused<T, S, DIR, TI><<<grd, dim3(RW, FTY, 1), smem, s>>>(d, dt, U, V, DU, DV, mflux_u, mflux_v, mupd_u,
-                                                                      mupd_v, Ex);
+                                                                      mupd_v, Ex, bf);
   return (int)cudaGetLastError();
 }
 
 template <class T, class TI>
 int run_uvadv2d_fused_t(const Dev& d, cudaStream_t s, int dir, T dt, int scheme, const TI* U, const TI* V,
                         const TI* DU, const TI* DV, const uint8_t* mflux_u, const uint8_t* mflux_v,
-                        const uint8_t* mupd_u, const uint8_t* mupd_v, TI* Ex) {
+                        const uint8_t* mupd_u, const uint8_t* mupd_v, TI* Ex, const Bf2Args& bf) {
   return dispatch_scheme(scheme, [&](auto sc) {
     constexpr int S = decltype(sc)::value;
-    return dir == 0 ? launch_uvadv2d_fused<T, S, 0, TI>(d, s, dt, U, V, DU, DV, mflux_u, mflux_v, mupd_u, mupd_v, Ex)
-                    : launch_uvadv2d_fused<T, S, 1, TI>(d, s, dt, U, V, DU, DV, mflux_u, mflux_v, mupd_u, mupd_v, Ex);
+    return dir == 0
+               ? launch_uvadv2d_fused<T, S, 0, TI>(d, s, dt, U, V, DU, DV, mflux_u, mflux_v, mupd_u, mupd_v, Ex, bf)
+               : launch_uvadv2d_fused<T, S, 1, TI>(d, s, dt, U, V, DU, DV, mflux_u, mflux_v, mupd_u, mupd_v, Ex, bf);
   });
 }
 
@@ -229,7 +287,8 @@ template <class T>
 int run_uvadv2d_fused(const Dev& d, cudaStream_t s, int dir, T dt, int scheme, const double* U, const double* V,
                       const double* DU, const double* DV, const uint8_t* mflux_u, const uint8_t* mflux_v,
                       const uint8_t* mupd_u, const uint8_t* mupd_v, double* Ex) {
-  return run_uvadv2d_fused_t<T, double>(d, s, dir, dt, scheme, U, V, DU, DV, mflux_u, mflux_v, mupd_u, mupd_v, Ex);
+  return run_uvadv2d_fused_t<T, double>(d, s, dir, dt, scheme, U, V, DU, DV, mflux_u, mflux_v, mupd_u, mupd_v, Ex,
+                                        Bf2Args{});
 }
 
 // FP32 arithmetic on the FP32 working copies of the mixed-precision micro step (defined in the
@@ -238,9 +297,10 @@ int run_uvadv2d_fused(const Dev& d, cudaStream_t s, int dir, T dt, int scheme, c
 
 int run_uvadv2d_fused_f32(const Dev& d, cudaStream_t s, int dir, float dt, int scheme, const float* U,
                           const float* V, const float* DU, const float* DV, const uint8_t* mflux_u,
-                          const uint8_t* mflux_v, const uint8_t* mupd_u, const uint8_t* mupd_v, float* Ex) {
+                          const uint8_t* mflux_v, const uint8_t* mupd_u, const uint8_t* mupd_v, float* Ex,
+                          const Bf2Args* bf) {
   return run_uvadv2d_fused_t<float, float>(d, s, dir, dt, scheme, U, V, DU, DV, mflux_u, mflux_v, mupd_u, mupd_v,
-                                           Ex);
+                                           Ex, bf ? *bf : Bf2Args{});
 }
 #endif
 

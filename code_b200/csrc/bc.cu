@@ -297,11 +297,77 @@ __global__ void k_momentum(Dev d, Bc2 s, Bc2W w) {
     X(i, j) = (Xo - dtm * (g * DXo * zx + dryo * (-tau / rho_0 + fCo + Exo + Slxo + Slr))) / (1.0 + dtm * ro / DXo);
 }
 
+// The mixed micro step's form of k_momentum: the same update with the elevation gradient's
+// difference zp - zm taken in FP64 (the elevations are FP64) and every other operation in FP32 on
+// the FP32 working copies (the Coriolis term with COR as well).
+template <int DIR, bool COR>
+__global__ void k_momentum_f32(Dev d, Bc2 s, Bc2W w) {
+  GB_IJ2
+  if (!interior(d, i, j)) return;
+  const long long c = d.ix(i, j);
+  const long long dn = DIR == 0 ? 1 : d.sj;  // the next T point along the component
+  if constexpr (COR) {
+    if (DIR == 0) {  // fV on U points from V
+      const float* V = w.w[V_];
+      if (s.au[c] >= 1) {
+        const float Vloc = 0.25f * (V[c - d.sj] + V[c + 1 - d.sj] + V[c] + V[c + 1]);
+        w.w[FV][c] = float(s.f2[CORU][c]) * Vloc;
+      } else {
+        w.w[FV][c] = 0.f;
+      }
+    } else {  // fU on V points from U
+      const float* U = w.w[U_];
+      if (s.av[c] >= 1) {
+        const float Uloc = 0.25f * (U[c - 1] + U[c] + U[c - 1 + d.sj] + U[c + d.sj]);
+        w.w[FU][c] = float(s.f2[CORV][c]) * Uloc;
+      } else {
+        w.w[FU][c] = 0.f;
+      }
+    }
+  }
+  const int32_t m = DIR == 0 ? s.au[c] : s.av[c];
+  if (!(m == 1 || m == 2)) return;
+  float* X = w.w[DIR == 0 ? U_ : V_];
+  const float* DX = w.w[DIR == 0 ? DU : DV];
+  const float* D = w.w[D_];
+  const float* airp = w.w[AIRP];
+  const float* taus = w.w[DIR == 0 ? TAUSX : TAUSY];
+  const double* z = s.f2[Z];
+  const double* H = s.f2[HH];
+  const float g = float(s.par[P_G]), rho_0 = float(s.par[P_RHO_0]), dtm = float(s.par[P_DTM]);
+  const double min_depth = s.par[P_MIN_DEPTH];
+  const float gammai = 1.f / (rho_0 * g);
+  const double zp = fmax(z[c + dn], -H[c] + fmin(min_depth, (double)D[c + dn]));
+  const double zm = fmax(z[c], -H[c + dn] + fmin(min_depth, (double)D[c]));
+  const float zx = (float(zp - zm) + (airp[c + dn] - airp[c]) * gammai) / float(DIR == 0 ? d.dx : d.dy);
+  const float tau = 0.5f * (taus[c] + taus[c + dn]);
+  const float Xo = X[c], sl = w.w[DIR == 0 ? SLRU : SLRV][c];
+  const float Slr = Xo > 0.f ? fmaxf(sl, 0.f) : fminf(sl, 0.f);
+  const float DXo = DX[c], dryo = w.w[DIR == 0 ? DRY_U : DRY_V][c], fCo = w.w[DIR == 0 ? FV : FU][c],
+              Exo = w.w[DIR == 0 ? UEX : VEX][c], Slxo = w.w[DIR == 0 ? SLUX : SLVX][c],
+              ro = w.w[DIR == 0 ? RU : RV][c];
+  const float fc = DIR == 0 ? -fCo : fCo;
+  X[c] = (Xo - dtm * (g * DXo * zx + dryo * (-tau / rho_0 + fc + Exo + Slxo + Slr))) / (1.f + dtm * ro / DXo);
+}
+
 // momentum.F90:193-216 / :356-379: Coriolis terms fU (after the U update) and fV (after V).
 template <int DIR, bool MIX>
 __global__ void k_coriolis(Dev d, Bc2 s, Bc2W w) {
   GB_IJ2
   if (!interior(d, i, j)) return;
+  if constexpr (MIX) {  // FP32 arithmetic on the working copies, as k_momentum_f32 forms the terms
+    const long long c = d.ix(i, j);
+    if (DIR == 0) {
+      const float* U = w.w[U_];
+      w.w[FU][c] = s.av[c] >= 1 ? float(s.f2[CORV][c]) * (0.25f * (U[c - 1] + U[c] + U[c - 1 + d.sj] + U[c + d.sj]))
+                                : 0.f;
+    } else {
+      const float* V = w.w[V_];
+      w.w[FV][c] = s.au[c] >= 1 ? float(s.f2[CORU][c]) * (0.25f * (V[c - d.sj] + V[c + 1 - d.sj] + V[c] + V[c + 1]))
+                                : 0.f;
+    }
+    return;
+  }
   if (DIR == 0) {  // fU on V points from the new U
     auto U = f2a<MIX, U_>(d, s, w);
     auto fU = f2a<MIX, FU>(d, s, w);
@@ -374,6 +440,69 @@ __global__ void k_depth_update(Dev d, Bc2 s, Bc2W w) {
   if (az(i, j) > 0) dry_z(i, j) = fmax(0.0, fmin(1.0, (D(i, j) - 0.5 * d1) * d2i));
   if (au(i, j) > 0) dry_u(i, j) = fmax(0.0, fmin(1.0, (DU_(i, j) - d1) * d2i));
   if (av(i, j) > 0) dry_v(i, j) = fmax(0.0, fmin(1.0, (DV_(i, j) - d1) * d2i));
+}
+
+// k_accum_sealevel and k_depth_update as one launch, for the micro-step loop without open
+// boundaries. The elevations ping-pong between the state's z and zo arrays: s.f2[Z] holds the
+// elevations before the step and is only read; the new ones go to s.f2[ZO], so the old array is
+// exactly the reference's zo = z of sealevel.F90:89 and the caller swaps the two pointers after
+// the launch. The depths of a U (V) point need the new elevation of the next T point, which the
+// thread forms itself from the same inputs with the same expression (no thread reads a value
+// that another writes). Same values as the two kernels, bit for bit.
+template <bool MIX>
+__global__ void k_sealevel_depth(Dev d, Bc2 s, Bc2W w, int accumulate) {
+  GB_IJ2
+  auto U = f2a<MIX, U_>(d, s, w);
+  auto V = f2a<MIX, V_>(d, s, w);
+  auto D = f2a<MIX, D_>(d, s, w);
+  auto DU_ = f2a<MIX, DU>(d, s, w);
+  auto DV_ = f2a<MIX, DV>(d, s, w);
+  auto dry_u = f2a<MIX, DRY_U>(d, s, w);
+  auto dry_v = f2a<MIX, DRY_V>(d, s, w);
+  W2 zold{d, s.f2[Z]}, znew{d, s.f2[ZO]}, fwf{d, s.f2[FWF]}, Uint{d, s.f2[UINT]}, Vint{d, s.f2[VINT]}, H{d, s.f2[HH]},
+      HU_{d, s.f2[HU]}, HV_{d, s.f2[HV]}, dry_z{d, s.f2[DRY_Z]};
+  M2 az{d, s.az}, au{d, s.au}, av{d, s.av};
+  const double dtm = s.par[P_DTM];
+  // sealevel.F90:94-108 at (ii, jj)
+  auto zn = [&](int ii, int jj) -> double {
+    const double zo_ = zold(ii, jj);
+    if (interior(d, ii, jj) && az(ii, jj) == 1)
+      return zo_ - dtm * (((double)U(ii, jj) * d.dy - (double)U(ii - 1, jj) * d.dy) +
+                          ((double)V(ii, jj) * d.dx - (double)V(ii, jj - 1) * d.dx)) * d.ard1 +
+             dtm * fwf(ii, jj);
+    return zo_;
+  };
+  if (accumulate) {
+    Uint(i, j) = Uint(i, j) + U(i, j);
+    Vint(i, j) = Vint(i, j) + V(i, j);
+  }
+  const double z0 = zn(i, j);
+  znew(i, j) = z0;
+  // depth_update.F90:55-110
+  const double min_depth = s.par[P_MIN_DEPTH], crit_depth = s.par[P_CRIT_DEPTH];
+  D(i, j) = z0 + H(i, j);
+  if (i <= d.imax + HALO - 1) {
+    const double x = fmax(0.25 * (zold(i, j) + zold(i + 1, j) + z0 + zn(i + 1, j)), -HU_(i, j) + min_depth);
+    DU_(i, j) = x + HU_(i, j);
+  }
+  if (j <= d.jmax + HALO - 1) {
+    const double x = fmax(0.25 * (zold(i, j) + zold(i, j + 1) + z0 + zn(i, j + 1)), -HV_(i, j) + min_depth);
+    DV_(i, j) = x + HV_(i, j);
+  }
+  const double d1 = 2 * min_depth;
+  const double d2i = 1.0 / (crit_depth - 2 * min_depth);
+  if (az(i, j) > 0) dry_z(i, j) = fmax(0.0, fmin(1.0, (D(i, j) - 0.5 * d1) * d2i));
+  if (au(i, j) > 0) dry_u(i, j) = fmax(0.0, fmin(1.0, (DU_(i, j) - d1) * d2i));
+  if (av(i, j) > 0) dry_v(i, j) = fmax(0.0, fmin(1.0, (DV_(i, j) - d1) * d2i));
+}
+
+// exchanges the contents of two 2D FP64 arrays (the elevation ping-pong's last state)
+__global__ void k_swap2(long long n2, double* a, double* b) {
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n2; c += (long long)gridDim.x * blockDim.x) {
+    const double x = a[c];
+    a[c] = b[c];
+    b[c] = x;
+  }
 }
 
 // start_macro.F90:54-86, first loop (T points) ...
@@ -957,8 +1086,8 @@ int momentum_2d(getm_ctx* ctx, const getm_bc_state* st, const Bc2W* wp, bool cor
   {
     TimerScope ts(ctx, GETM_TIM_BC2D);
     if (!wp) k_momentum<DIR, false><<<grid2(d), kBlk2, 0, cs>>>(d, s, w);
-    else if (cor) k_momentum<DIR, true, true><<<grid2(d), kBlk2, 0, cs>>>(d, s, w);
-    else k_momentum<DIR, true, false><<<grid2(d), kBlk2, 0, cs>>>(d, s, w);
+    else if (cor) k_momentum_f32<DIR, true><<<grid2(d), kBlk2, 0, cs>>>(d, s, w);
+    else k_momentum_f32<DIR, false><<<grid2(d), kBlk2, 0, cs>>>(d, s, w);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(ctx, (int)e, DIR == 0 ? "umomentum" : "vmomentum");
   }
@@ -972,7 +1101,10 @@ int momentum_2d(getm_ctx* ctx, const getm_bc_state* st, const Bc2W* wp, bool cor
 }
 
 // m2d.F90:412-490 integrate_2d (closed boundaries; no residual; Am <= 0, An_method = 0)
-int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop, const Bc2W* wp = nullptr, bool first = false) {
+// zswap (the micro-step loop without open boundaries): sealevel and depth_update as one launch that
+// writes the new elevations into st->f2[ZO]; the caller then swaps st->f2[Z] and st->f2[ZO].
+int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop, const Bc2W* wp = nullptr, bool first = false,
+                 bool zswap = false) {
   const Dev& d = ctx->dev;
   const Bc2 s = to_bc2(st);
   int* ip = st->ipar;
@@ -985,7 +1117,12 @@ int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop, const Bc2W* wp = nu
     return (int)cudaGetLastError();
   };
   int rc = GETM_OK;
-  if ((loop - 1) % ip[I_MM] == 0 && (rc = bottom_friction_2d(ctx, st, ip[I_RUNTYPE], wp))) return rc;
+  const bool bf_due = (loop - 1) % ip[I_MM] == 0;
+  // the mixed micro step forms the bottom friction inside its momentum-advection kernels (they
+  // stage the same velocities); the separate kernel otherwise (and with the fused micro-step
+  // kernels switched off, for the comparison of the two forms)
+  const bool bf_fused = mix && bf_due && ip[I_VEL2D_HOR] != NOADV && fused_micro_enabled();
+  if (bf_due && !bf_fused && (rc = bottom_friction_2d(ctx, st, ip[I_RUNTYPE], wp))) return rc;
   if (mix) {
     const int hor = ip[I_VEL2D_HOR];
     if (hor == NOADV) {
@@ -995,10 +1132,23 @@ int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop, const Bc2W* wp = nu
       for (int dir = 0; dir < 2; ++dir) {
         getm_adv_grid g;
         grid_for_tag(ctx, dir == 0 ? GETM_U_TAG : GETM_V_TAG, &g);
+        Bf2Args bf{};
+        if (bf_fused) {
+          bf.mask = dir == 0 ? st->au : st->av;
+          bf.au = st->au;
+          bf.zb = st->f2[dir == 0 ? ZUB : ZVB];
+          bf.zb0 = st->f2[dir == 0 ? ZUB0 : ZVB0];
+          bf.r = w.w[dir == 0 ? RU : RV];
+          bf.rr = w.w[dir == 0 ? RUU : RVV];
+          bf.kappa = float(st->par[P_KAPPA]);
+          bf.avmmol = float(st->par[P_AVMMOL]);
+          bf.min_depth = float(st->par[P_MIN_DEPTH]);
+          bf.runtype = ip[I_RUNTYPE];
+        }
         GB_TIMED(GETM_TIM_BC2D,
                  run_uvadv2d_fused_f32(d, ctx->stream, dir, float(st->par[P_DTM]), hor, w.w[U_], w.w[V_], w.w[DU],
                                        w.w[DV], g.mask_uflux, g.mask_vflux, g.mask_uupdate, g.mask_vupdate,
-                                       w.w[dir == 0 ? UEX : VEX]),
+                                       w.w[dir == 0 ? UEX : VEX], bf_fused ? &bf : nullptr),
                  "uv_advect");
       }
     }
@@ -1023,6 +1173,14 @@ int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop, const Bc2W* wp = nu
   }
   // update_2d_bdy sets the boundary elevations after the Uint accumulation and before sealevel
   // (m2d.F90:467-476); the accumulation does not touch z, so it runs inside the sealevel kernel
+  if (zswap) {
+    if (ctx->has_bdy) return fail(ctx, GETM_ERR_STATE, "integrate_2d: fused sealevel with open boundaries");
+    rc = mix ? k2(k_sealevel_depth<true>, d, s, w, ip[I_RUNTYPE] > 1 ? 1 : 0)
+             : k2(k_sealevel_depth<false>, d, s, w, ip[I_RUNTYPE] > 1 ? 1 : 0);
+    if (rc) return cuda_fail(ctx, rc, "sealevel + depth_update");
+    std::swap(st->f2[Z], st->f2[ZO]);
+    return nan_sweep_due(ctx, st, loop);
+  }
   if (!mix && (rc = bdy_2d(ctx, s, loop))) return rc;
   rc = mix ? k2(k_accum_sealevel<true>, d, s, w, ip[I_RUNTYPE] > 1 ? 1 : 0)
            : k2(k_accum_sealevel<false>, d, s, w, ip[I_RUNTYPE] > 1 ? 1 : 0);
@@ -1166,6 +1324,9 @@ int integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
     // sources of the temperature diffusion in the tracer scratch, and (paired advection) the
     // top-level salinity before it is advected, which the freezing-point test of the heat flux reads
     const bool radn = ip[I_RADIATION] && ip[I_CALC_TEMP];
+    // compensated storage of the tracers (FP16 scaled carried errors; null: plain storage)
+    __half* tlo = (__half*)st->f3[TLO];
+    __half* slo = (__half*)st->f3[SLO];
     R3* tsrc = nullptr;
     R3* s_top = nullptr;
     if (radn) {
@@ -1194,37 +1355,37 @@ int integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
                                s),
                "top-level salinity");
       if ((rc = do_adv3d_pair<R3>(ctx, dt, f3[TT], f3[SS], f3[UU], f3[VV], f3[WW], f3[HUN], f3[HVN], f3[HO],
-                                  ip[I_TEMP_HOR], ip[I_TEMP_VER], R3(st->par[P_TEMP_AH]), f3[TLO], f3[SLO])))
+                                  ip[I_TEMP_HOR], ip[I_TEMP_VER], R3(st->par[P_TEMP_AH]), tlo, slo)))
         return rc;
       if (radn && (rc = temp_sources(s_top))) return rc;
       GB_TIMED(GETM_TIM_VDIFF, run_vdiff<R3>(d, s, dt, R3(st->par[P_CNPAR]), R3(st->par[P_AVMOLT]), f3[TT], f3[HN],
                                              f3[NUH], st->az, (const R3*)tsrc, (R3*)ctx->scr[0], (R3*)ctx->scr[1],
-                                             nullptr, nullptr, f3[TLO]),
+                                             nullptr, nullptr, tlo),
                "vdiff T");
       GB_TIMED(GETM_TIM_VDIFF, run_vdiff<R3>(d, s, dt, R3(st->par[P_CNPAR]), R3(st->par[P_AVMOLS]), f3[SS], f3[HN],
                                              f3[NUH], st->az, (const R3*)nullptr, (R3*)ctx->scr[0], (R3*)ctx->scr[1],
-                                             nullptr, nullptr, f3[SLO]),
+                                             nullptr, nullptr, slo),
                "vdiff S");
     }
     if (!pair && ip[I_CALC_TEMP]) {
       if ((rc = do_adv3d<R3>(ctx, dt, f3[TT], f3[UU], f3[VV], f3[WW], f3[HUN], f3[HVN], f3[HO], f3[HN],
                              ip[I_TEMP_SPLIT], ip[I_TEMP_HOR], ip[I_TEMP_VER], R3(st->par[P_TEMP_AH]), GETM_H_TAG,
-                             nullptr, nullptr, ip[I_ADV_VER_ITERS], true, f3[TLO])))
+                             nullptr, nullptr, ip[I_ADV_VER_ITERS], true, tlo)))
         return rc;
       if (radn && (rc = temp_sources(nullptr))) return rc;
       GB_TIMED(GETM_TIM_VDIFF, run_vdiff<R3>(d, s, dt, R3(st->par[P_CNPAR]), R3(st->par[P_AVMOLT]), f3[TT], f3[HN],
                                              f3[NUH], st->az, (const R3*)tsrc, (R3*)ctx->scr[0], (R3*)ctx->scr[1],
-                                             nullptr, nullptr, f3[TLO]),
+                                             nullptr, nullptr, tlo),
                "vdiff T");
     }
     if (!pair && ip[I_CALC_SALT]) {
       if ((rc = do_adv3d<R3>(ctx, dt, f3[SS], f3[UU], f3[VV], f3[WW], f3[HUN], f3[HVN], f3[HO], f3[HN],
                              ip[I_SALT_SPLIT], ip[I_SALT_HOR], ip[I_SALT_VER], R3(st->par[P_SALT_AH]), GETM_H_TAG,
-                             nullptr, nullptr, ip[I_ADV_VER_ITERS], true, f3[SLO])))
+                             nullptr, nullptr, ip[I_ADV_VER_ITERS], true, slo)))
         return rc;
       GB_TIMED(GETM_TIM_VDIFF, run_vdiff<R3>(d, s, dt, R3(st->par[P_CNPAR]), R3(st->par[P_AVMOLS]), f3[SS], f3[HN],
                                              f3[NUH], st->az, (const R3*)nullptr, (R3*)ctx->scr[0], (R3*)ctx->scr[1],
-                                             nullptr, nullptr, f3[SLO]),
+                                             nullptr, nullptr, slo),
                "vdiff S");
     }
     // m3d.F90:595,602
@@ -1633,10 +1794,32 @@ int getm_integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
   return st->prec3d == 8 ? integrate_3d<double>(ctx, st, n) : integrate_3d<float>(ctx, st, n);
 }
 
-int getm_time_loop(getm_ctx* ctx, getm_bc_state* st, int n0, int count) {
-  int rc = check_state(ctx, st);
+static int time_loop(getm_ctx* ctx, getm_bc_state* st, int n0, int count, bool zswap);
+
+int getm_time_loop(getm_ctx* ctx, getm_bc_state* st_user, int n0, int count) {
+  int rc = check_state(ctx, st_user);
   if (rc) return rc;
-  if ((rc = ensure_bc_scratch(ctx, (size_t)st->prec3d))) return rc;
+  if ((rc = ensure_bc_scratch(ctx, (size_t)st_user->prec3d))) return rc;
+  // Without open boundaries the micro steps update the elevations by pointer ping-pong between z
+  // and zo (k_sealevel_depth) on a copy of the state table; after an odd number of swaps the two
+  // arrays' contents are exchanged at the end, so the caller's z and zo hold what the reference's
+  // would. The integer settings the steps update (ufirst2d/3d, nan_warned) are copied back.
+  const bool zswap = !ctx->has_bdy && fused_micro_enabled();
+  getm_bc_state loc = *st_user;
+  rc = time_loop(ctx, zswap ? &loc : st_user, n0, count, zswap);
+  if (zswap) {
+    std::copy(loc.ipar, loc.ipar + NPI, st_user->ipar);
+    if (loc.f2[Z] != st_user->f2[Z]) {
+      k_swap2<<<592, 256, 0, ctx->stream>>>(n2d(ctx->dev), st_user->f2[Z], st_user->f2[ZO]);
+      const cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess && rc == GETM_OK) rc = cuda_fail(ctx, (int)e, "elevation ping-pong");
+    }
+  }
+  return rc;
+}
+
+static int time_loop(getm_ctx* ctx, getm_bc_state* st, int n0, int count, bool zswap) {
+  int rc;
   // The mixed-precision step (FP32 3D fields) runs its micro steps on FP32 working copies of the
   // barotropic fields (is_work2) when the fused 2D momentum advection applies and there are no
   // open boundaries; the elevation and Uint/Vint stay FP64 throughout.
@@ -1684,7 +1867,7 @@ int getm_time_loop(getm_ctx* ctx, getm_bc_state* st, int n0, int count) {
   if (mix && (rc = sync(all & ~((1ull << UEX) | (1ull << VEX)), 1))) return rc;
   bool dirty = false;  // working copies newer than the state
   for (int n = n0; n < n0 + count; ++n) {
-    if ((rc = integrate_2d(ctx, st, n, mix ? &w : nullptr, n == n0))) return rc;
+    if ((rc = integrate_2d(ctx, st, n, mix ? &w : nullptr, n == n0, zswap))) return rc;
     dirty = mix;
     if (n % st->ipar[I_M] == 0) {
       if (mix && (rc = sync(written, 0))) return rc;

@@ -17,6 +17,9 @@ namespace gb {
 
 std::atomic<int> g_vector_sweeps{1};
 bool vector_sweeps_enabled() { return g_vector_sweeps.load(std::memory_order_relaxed) != 0; }
+
+std::atomic<int> g_fused_micro{1};
+bool fused_micro_enabled() { return g_fused_micro.load(std::memory_order_relaxed) != 0; }
 std::atomic<int> g_fp32_micro{1};
 bool fp32_micro_steps_enabled() { return g_fp32_micro.load(std::memory_order_relaxed) != 0; }
 
@@ -60,7 +63,7 @@ using namespace gb;
 template <class R>
 int do_adv3d(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, const R* hu,
                     const R* hv, const R* ho, const R* hn, int split, int hs, int vs, R AH, int tag, R* hires,
-                    R* advres, int iters, bool field_out, R* lo) {
+                    R* advres, int iters, bool field_out, __half* lo) {
   (void)hn;
   if (!ctx) return GETM_ERR_ARG;
   if (!ctx->adv_ready) return fail(ctx, GETM_ERR_STATE, "getm_init_advection has not been called");
@@ -139,8 +142,8 @@ int do_adv3d(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, c
   R* Al = A ? L(A, 1) : nullptr;
   // compensated storage of the tracer (FP32; the FULLSPLIT and HALFSPLIT sequences, whose updates
   // are all increments)
-  R* lw = (lo && field_out) ? lo : nullptr;
-  R* ll = lw ? L(lw, 1) : nullptr;
+  __half* lw = (lo && field_out) ? lo : nullptr;
+  __half* ll = lw ? L(lw, 1) : nullptr;
   switch (split) {
     case GETM_NOSPLIT:
       GB_TIMED(GETM_TIM_COPY, cudaMemcpyAsync(S, f, bytes3, cudaMemcpyDeviceToDevice, s), "copy f");
@@ -190,7 +193,7 @@ int do_adv3d(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, c
 // same sweeps as do_adv3d's HALFSPLIT branch for each field, with the heights hi evolved once.
 template <class R>
 int do_adv3d_pair(getm_ctx* ctx, R dt, R* fa, R* fb, const R* uu, const R* vv, const R* ww, const R* hu,
-                  const R* hv, const R* ho, int hs, int vs, R AH, R* lo_a, R* lo_b) {
+                  const R* hv, const R* ho, int hs, int vs, R AH, __half* lo_a, __half* lo_b) {
   getm_adv_grid g;
   grid_for_tag(ctx, GETM_H_TAG, &g);
   const Dev& d = ctx->dev;
@@ -205,8 +208,8 @@ int do_adv3d_pair(getm_ctx* ctx, R dt, R* fa, R* fb, const R* uu, const R* vv, c
   auto L = [&](auto* p, int k) { return p ? p + (long long)k * sk : p; };
   const R half = R(0.5), one = R(1);
   const int nk = kmax;
-  R* la = L(lo_a, 1);
-  R* lb = L(lo_b, 1);
+  __half* la = L(lo_a, 1);
+  __half* lb = L(lo_b, 1);
   GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<R, 0>(d, s, nk, dt, half, hs, AH, L(fa, 1), L(fa, 1), L(Sa, 1), L(ho, 1),
                             L(H, 1), nullptr, L(uu, 1), L(hu, 1), g.mask_uflux, g.mask_uupdate, nullptr, L(fb, 1),
                             L(fb, 1), L(Sb, 1), la, lb)), "u1");
@@ -224,16 +227,16 @@ int do_adv3d_pair(getm_ctx* ctx, R dt, R* fa, R* fb, const R* uu, const R* vv, c
   return GETM_OK;
 }
 template int do_adv3d_pair<double>(getm_ctx*, double, double*, double*, const double*, const double*, const double*,
-                                   const double*, const double*, const double*, int, int, double, double*, double*);
+                                   const double*, const double*, const double*, int, int, double, __half*, __half*);
 template int do_adv3d_pair<float>(getm_ctx*, float, float*, float*, const float*, const float*, const float*,
-                                  const float*, const float*, const float*, int, int, float, float*, float*);
+                                  const float*, const float*, const float*, int, int, float, __half*, __half*);
 
 template int do_adv3d<double>(getm_ctx*, double, double*, const double*, const double*, const double*,
                                const double*, const double*, const double*, const double*, int, int, int, double,
-                               int, double*, double*, int, bool, double*);
+                               int, double*, double*, int, bool, __half*);
 template int do_adv3d<float>(getm_ctx*, float, float*, const float*, const float*, const float*, const float*,
                              const float*, const float*, const float*, int, int, int, float, int, float*, float*,
-                             int, bool, float*);
+                             int, bool, __half*);
 
 template <class R>
 static int sweep_h_api(getm_ctx* ctx, int dir, int nk, R dt, const R* f, R* fi, R* Di, R* adv, const R* U,
@@ -461,6 +464,10 @@ int getm_set_vector_sweeps(int on) {
 
 int getm_set_fp32_micro_steps(int on) {
   return gb::g_fp32_micro.exchange(on != 0 ? 1 : 0);
+}
+
+int getm_set_fused_micro_step(int on) {
+  return gb::g_fused_micro.exchange(on != 0 ? 1 : 0);
 }
 
 int getm_timers_enable(getm_ctx* ctx, int on) {

@@ -170,12 +170,12 @@ static inline bool grid_for_tag(const getm_ctx* ctx, int tag, getm_adv_grid* g) 
 template <class R>
 int do_adv3d(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, const R* hu, const R* hv,
              const R* ho, const R* hn, int split, int hs, int vs, R AH, int tag, R* hires, R* advres, int iters,
-             bool field_out = true, R* lo = nullptr);
+             bool field_out = true, __half* lo = nullptr);
 // Two tracers advected together with HALFSPLIT on the H grid (ctx.cu); the caller has checked that
 // hs is a split scheme, vs a split scheme or NOADV, and adv_ver_iterations = 1.
 template <class R>
 int do_adv3d_pair(getm_ctx* ctx, R dt, R* fa, R* fb, const R* uu, const R* vv, const R* ww, const R* hu,
-                  const R* hv, const R* ho, int hs, int vs, R AH, R* lo_a = nullptr, R* lo_b = nullptr);
+                  const R* hv, const R* ho, int hs, int vs, R AH, __half* lo_a = nullptr, __half* lo_b = nullptr);
 
 // Tracer step: do_advection_3d(H_TAG) then the implicit vertical diffusion (ctx.cu).
 template <class R>

@@ -2,6 +2,7 @@
 // Instantiated for double in kernels_f64.cu (built without FMA contraction so that every
 // expression rounds exactly as the reference's) and for float in kernels_f32.cu.
 #pragma once
+#include <cuda_fp16.h>
 #include "common.cuh"
 #include "launch.h"
 
@@ -184,16 +185,36 @@ __device__ __forceinline__ float add_comp(float hi, float inc, float& lo) {
   lo = __fadd_rn(__fsub_rn(hi, __fsub_rn(s, bb)), __fsub_rn(b, bb));
   return s;
 }
-// fv_update with the compensated storage: lo is the cell's carried error (read and written)
+// The carried error is stored in FP16 as lo * 2^16 (an exact power-of-two scaling): |lo| <= half an
+// ulp of hi, so the stored value stays below 1 for |hi| < 2^24 and keeps lo to 11 bits wherever it
+// is a normal FP16 number (|lo| >= 2^-30, i.e. |hi| above about 2^-7; below, the tracer's own FP32
+// spacing is already that fine); the tracer then holds about 35 significant bits in 6 bytes.
+constexpr float LO_ENC = 65536.f, LO_DEC = 1.f / 65536.f;
+// hi + inc with the carried error given as its stored (scaled) value slo
+__device__ __forceinline__ float add_comp_scaled(float hi, float inc, float& slo) {
+  float lo = __fmul_rn(slo, LO_DEC);
+  const float s = add_comp(hi, inc, lo);
+  slo = __fmul_rn(lo, LO_ENC);
+  return s;
+}
+// fv_update with the compensated storage; slo: the cell's scaled carried error (read and written)
 template <class R>
-__device__ __forceinline__ R fv_update_lo(R hio, R dh, R hin, R fio, R dt, R advn, R& lo) {
+__device__ __forceinline__ R fv_update_lo(R hio, R dh, R hin, R fio, R dt, R advn, float& slo) {
   if constexpr (sizeof(R) == 8) {
-    (void)lo;
+    (void)slo;
     return fv_update<R>(hio, dh, hin, fio, dt, advn);
   } else {
     (void)hio;
-    return add_comp(fio, __fdividef(__fmaf_rn(fio, dh, -__fmul_rn(dt, advn)), hin), lo);
+    return add_comp_scaled(fio, __fdividef(__fmaf_rn(fio, dh, -__fmul_rn(dt, advn)), hin), slo);
   }
+}
+// the same on the FP16 array of the carried errors at element p
+template <class R>
+__device__ __forceinline__ R fv_update_lo(R hio, R dh, R hin, R fio, R dt, R advn, __half* lo, long long p) {
+  float slo = __half2float(lo[p]);
+  const R v = fv_update_lo<R>(hio, dh, hin, fio, dt, advn, slo);
+  lo[p] = __float2half_rn(slo);
+  return v;
 }
 
 // Flux through face q (between cells q and q+1) from staged values: f at q-1..q+2, flux masks at
@@ -324,7 +345,7 @@ struct TracerIO {
   const R* f;
   const R* fi_src;
   R* fi_dst;
-  R* lo = nullptr;  // FP32 compensated storage: the carried error of the updated cells (may be null)
+  __half* lo = nullptr;  // FP32 compensated storage: the cells' scaled carried errors (may be null)
 };
 template <class R, int NF>
 struct TracerSet {
@@ -464,9 +485,7 @@ __global__ void __launch_bounds__(TU, sizeof(R) == 4 ? 16 : 8) k_sweep_u_tile(De
           const R advn = cell_advn<R>(C, sfl[n][t + 1], sfl[n][t]);
           if (F.t[n].fi_dst) {
             if (F.t[n].lo) {
-              R lo = F.t[n].lo[p];
-              F.t[n].fi_dst[p] = fv_update_lo<R>(Dio, dD, Dn, fio, C.dt, advn, lo);
-              F.t[n].lo[p] = lo;
+              F.t[n].fi_dst[p] = fv_update_lo<R>(Dio, dD, Dn, fio, C.dt, advn, F.t[n].lo, p);
             } else {
               F.t[n].fi_dst[p] = fv_update<R>(Dio, dD, Dn, fio, C.dt, advn);
             }
@@ -606,9 +625,7 @@ __global__ void __launch_bounds__(TVX * TVY, sizeof(R) == 4 ? (NF == 1 ? 8 : 6) 
           const R advn = cell_advn<R>(C, sfl[n][ty + 1][tx], sfl[n][ty][tx]);
           if (F.t[n].fi_dst) {
             if (F.t[n].lo) {
-              R lo = F.t[n].lo[p];
-              F.t[n].fi_dst[p] = fv_update_lo<R>(Dio, dD, Dn, fio, C.dt, advn, lo);
-              F.t[n].lo[p] = lo;
+              F.t[n].fi_dst[p] = fv_update_lo<R>(Dio, dD, Dn, fio, C.dt, advn, F.t[n].lo, p);
             } else {
               F.t[n].fi_dst[p] = fv_update<R>(Dio, dD, Dn, fio, C.dt, advn);
             }
@@ -660,7 +677,7 @@ template <class R, int S, bool REC>
 __global__ void __launch_bounds__(128) k_sweep_w(Dev d, R dt, R splitfac, int kshift,
                                                  const R* f, const R* fi_src, R* fi_dst, R* hi, R* adv,
                                                  const R* __restrict__ ww,
-                                                 const int32_t* __restrict__ az, uint8_t* code, R* lo = nullptr) {
+                                                 const int32_t* __restrict__ az, uint8_t* code, __half* lo = nullptr) {
   const int ii = blockIdx.x * blockDim.x + threadIdx.x;
   const int jj = blockIdx.y * blockDim.y + threadIdx.y;
   // columns i = imin-2..imax+1, j = jmin-2..jmax+1 (adv_split_w.F90:160-162)
@@ -702,9 +719,7 @@ __global__ void __launch_bounds__(128) k_sweep_w(Dev d, R dt, R splitfac, int ks
     const R hin = hio - dh;
     const R advn = splitfac * (wfl - wprev);
     if (lo) {
-      R l = lo[c + k * sk];
-      fi_dst[c + k * sk] = fv_update_lo<R>(hio, dh, hin, fio, dt, advn, l);
-      lo[c + k * sk] = l;
+      fi_dst[c + k * sk] = fv_update_lo<R>(hio, dh, hin, fio, dt, advn, lo, c + k * sk);
     } else {
       fi_dst[c + k * sk] = fv_update<R>(hio, dh, hin, fio, dt, advn);
     }
@@ -722,7 +737,7 @@ __global__ void __launch_bounds__(128) k_sweep_w(Dev d, R dt, R splitfac, int ks
 template <class R, int S>
 __global__ void __launch_bounds__(128) k_sweep_w2(Dev d, R dt, R splitfac, R* fa, R* fb, R* hi,
                                                   const R* __restrict__ ww, const int32_t* __restrict__ az,
-                                                  R* lo_a = nullptr, R* lo_b = nullptr) {
+                                                  __half* lo_a = nullptr, __half* lo_b = nullptr) {
   const int ii = blockIdx.x * blockDim.x + threadIdx.x;
   const int jj = blockIdx.y * blockDim.y + threadIdx.y;
   if (ii >= d.ni() - 1 || jj >= d.nj() - 1) return;
@@ -753,16 +768,12 @@ __global__ void __launch_bounds__(128) k_sweep_w2(Dev d, R dt, R splitfac, R* fa
     const R dh = dti * (wk - wkm1);
     const R hin = hio - dh;
     if (lo_a) {
-      R l = lo_a[c + k * sk];
-      fa[c + k * sk] = fv_update_lo<R>(hio, dh, hin, a1, dt, splitfac * (wfa - wpa), l);
-      lo_a[c + k * sk] = l;
+      fa[c + k * sk] = fv_update_lo<R>(hio, dh, hin, a1, dt, splitfac * (wfa - wpa), lo_a, c + k * sk);
     } else {
       fa[c + k * sk] = fv_update<R>(hio, dh, hin, a1, dt, splitfac * (wfa - wpa));
     }
     if (lo_b) {
-      R l = lo_b[c + k * sk];
-      fb[c + k * sk] = fv_update_lo<R>(hio, dh, hin, b1, dt, splitfac * (wfb - wpb), l);
-      lo_b[c + k * sk] = l;
+      fb[c + k * sk] = fv_update_lo<R>(hio, dh, hin, b1, dt, splitfac * (wfb - wpb), lo_b, c + k * sk);
     } else {
       fb[c + k * sk] = fv_update<R>(hio, dh, hin, b1, dt, splitfac * (wfb - wpb));
     }
@@ -787,7 +798,7 @@ __global__ void __launch_bounds__(64) k_sweep_w_iter(Dev d, R dt, R splitfac, in
                                                      R* fi_dst, R* hi, R* adv,
                                                      const R* __restrict__ ww,
                                                      const int32_t* __restrict__ az,
-                                                     unsigned long long* warn, R* lo = nullptr) {
+                                                     unsigned long long* warn, __half* lo = nullptr) {
   const int ii = blockIdx.x * blockDim.x + threadIdx.x;
   const int jj = blockIdx.y * blockDim.y + threadIdx.y;
   if (ii >= d.ni() - 1 || jj >= d.nj() - 1) return;
@@ -797,7 +808,8 @@ __global__ void __launch_bounds__(64) k_sweep_w_iter(Dev d, R dt, R splitfac, in
   const long long sk = d.sk;
   const R dti = splitfac * dt;
   R fo[GB_KMAX_ITER + 1], fia[GB_KMAX_ITER + 1], hia[GB_KMAX_ITER + 1], ada[GB_KMAX_ITER + 1],
-      wfl[GB_KMAX_ITER + 1], cfl0[GB_KMAX_ITER + 1], cfls[GB_KMAX_ITER + 1], loa[GB_KMAX_ITER + 1];
+      wfl[GB_KMAX_ITER + 1], cfl0[GB_KMAX_ITER + 1], cfls[GB_KMAX_ITER + 1];
+  float loa[GB_KMAX_ITER + 1];  // the scaled carried errors of the column (compensated storage)
   for (int k = 0; k <= kmax; ++k) {
     fo[k] = f[c + k * sk];
     cfl0[k] = R(0);
@@ -816,7 +828,7 @@ __global__ void __launch_bounds__(64) k_sweep_w_iter(Dev d, R dt, R splitfac, in
         fia[k] = fi_src[c + k * sk];
         hia[k] = hi[c + k * sk];
         ada[k] = adv ? adv[c + k * sk] : R(0);
-        loa[k] = lo ? lo[c + k * sk] : R(0);
+        loa[k] = lo ? __half2float(lo[c + k * sk]) : 0.f;
       }
       faux = fo;
       for (int k = 0; k <= kmax; ++k) cfls[k] = cfl0[k];
@@ -878,7 +890,7 @@ __global__ void __launch_bounds__(64) k_sweep_w_iter(Dev d, R dt, R splitfac, in
     fi_dst[c + k * sk] = fia[k];
     hi[c + k * sk] = hia[k];
     if (adv) adv[c + k * sk] = ada[k];
-    if (lo) lo[c + k * sk] = loa[k];
+    if (lo) lo[c + k * sk] = __float2half_rn(loa[k]);
   }
 }
 
@@ -896,12 +908,13 @@ struct ThomasSmem {
 // Implicit vertical diffusion (salinity.F90:348-389; temperature form with src). One thread per
 // interior column; the matrix rows are built top-down as the elimination proceeds, ru(k+1)/qu(k+1)
 // carried in registers and ru(k)/qu(k) stored in two scratch 3D arrays (full occupancy, no shared
-// memory) for the back substitution.
+// memory for them: holding them in shared memory measured 1.6x slower at kmax = 50, from the lower
+// occupancy) for the back substitution.
 template <class R>
 __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, const R* Sin, R* S,
                                                const R* __restrict__ hn, const R* __restrict__ nuh,
                                                const int32_t* __restrict__ az, const R* __restrict__ src, R* RUs,
-                                               R* QUs, R* S2, R* lo) {
+                                               R* QUs, R* S2, __half* lo) {
   const int kmax = d.kmax;
   const int i = d.imin + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = d.jmin + blockIdx.y * blockDim.y + threadIdx.y;
@@ -921,9 +934,9 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, co
   auto new_level = [&](int k, R sold, R inc) -> R {
     if constexpr (sizeof(R) == 4) {
       if (lo) {
-        float l = lo[c + k * sk];
-        const float v = add_comp(sold, inc, l);
-        lo[c + k * sk] = l;
+        float slo = __half2float(lo[c + k * sk]);
+        const float v = add_comp_scaled(sold, inc, slo);
+        lo[c + k * sk] = __float2half_rn(slo);
         return v;
       }
     }
@@ -941,6 +954,12 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, co
   // (a serial chain per column), so the chain does not wait on their loads.
   __shared__ R sl[4][4][128];
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  auto set_rq = [&](int k, R r, R q) {
+    RUs[c + k * sk] = r;
+    QUs[c + k * sk] = q;
+  };
+  auto ru_of = [&](int k) -> R { return RUs[c + k * sk]; };
+  auto qu_of = [&](int k) -> R { return QUs[c + k * sk]; };
   auto issue = [&](int lv) {
     if (lv >= 1) {
       R(*q)[128] = sl[lv & 3];
@@ -973,8 +992,7 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, co
     if (src) a4 = a4 + srck;
     ru = a1 / a2;
     qu = a4 / a2;
-    RUs[c + k * sk] = ru;
-    QUs[c + k * sk] = qu;
+    set_rq(k, ru, qu);
   }
   // inner rows k = kmax-1 .. 2
   for (k = kmax - 1; k >= 2; --k) {
@@ -1000,8 +1018,7 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, co
     const R den = a2 - a3 * ru;
     ru = a1 / den;
     qu = (a4 - a3 * qu) / den;
-    RUs[c + k * sk] = ru;
-    QUs[c + k * sk] = qu;
+    set_rq(k, ru, qu);
   }
   cp_async_wait<0>();
   // bottom row k = 1 (fi): only qu
@@ -1019,16 +1036,16 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, co
     put(1, incr ? new_level(1, S1, v) : v);
   }
   // back substitution upwards, with the next level's coefficients loaded one step ahead
-  R qn = kmax >= 2 ? QUs[c + 2 * sk] : R(0), rn = kmax >= 2 ? RUs[c + 2 * sk] : R(0);
+  R qn = kmax >= 2 ? qu_of(2) : R(0), rn = kmax >= 2 ? ru_of(2) : R(0);
   R sn = (incr && kmax >= 2) ? L(Sin, 2) : R(0);
-  R qn2 = kmax >= 3 ? QUs[c + 3 * sk] : R(0), rn2 = kmax >= 3 ? RUs[c + 3 * sk] : R(0);
+  R qn2 = kmax >= 3 ? qu_of(3) : R(0), rn2 = kmax >= 3 ? ru_of(3) : R(0);
   R sn2 = (incr && kmax >= 3) ? L(Sin, 3) : R(0);
   for (k = 2; k <= kmax; ++k) {
     const R q = qn, r = rn, so = sn;
     qn = qn2; rn = rn2; sn = sn2;
     if (k + 2 <= kmax) {
-      qn2 = QUs[c + (k + 2) * sk];
-      rn2 = RUs[c + (k + 2) * sk];
+      qn2 = qu_of(k + 2);
+      rn2 = ru_of(k + 2);
       if (incr) sn2 = L(Sin, k + 2);
     }
     v = q - r * v;

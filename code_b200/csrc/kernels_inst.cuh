@@ -11,11 +11,11 @@
 namespace gb {
 
 // The vectorised sweeps of sweeps_vec.cuh apply when every row and level of the fields starts on
-// a 16-byte boundary; the tile kernels serve every other layout (and all layouts when the
-// vectorised sweeps are switched off, for comparison).
+// a 16-byte boundary (byte masks: N bytes, FP16 carried errors: 2N bytes); the tile kernels serve
+// every other layout (and all layouts when the vectorised sweeps are switched off, for comparison).
 template <class R>
 static bool vec_layout(const Dev& d, int nk, std::initializer_list<const void*> ptrs,
-                       std::initializer_list<const void*> bytes) {
+                       std::initializer_list<const void*> bytes, std::initializer_list<const void*> halves = {}) {
   constexpr long long N = 16 / sizeof(R);
   if (!vector_sweeps_enabled()) return false;
   if (d.sj % N != 0 || (nk > 1 && d.sk % N != 0)) return false;
@@ -23,6 +23,8 @@ static bool vec_layout(const Dev& d, int nk, std::initializer_list<const void*> 
     if (p && (reinterpret_cast<uintptr_t>(p) % 16) != 0) return false;
   for (const void* p : bytes)
     if (p && (reinterpret_cast<uintptr_t>(p) % N) != 0) return false;
+  for (const void* p : halves)
+    if (p && (reinterpret_cast<uintptr_t>(p) % (2 * N)) != 0) return false;
   return true;
 }
 
@@ -44,7 +46,7 @@ template <class R, int DIR>
 int run_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int scheme, R AH, const R* f,
                 const R* fi_src, R* fi_dst, const R* Di_src, R* Di_dst, R* adv, const R* U, const R* DU,
                 const uint8_t* mflux, const uint8_t* mupd, uint8_t* code, const R* f_b, const R* fi_src_b,
-                R* fi_dst_b, R* lo, R* lo_b) {
+                R* fi_dst_b, __half* lo, __half* lo_b) {
   if (nk <= 0) return 0;
   if (f_b && (code || adv)) return (int)cudaErrorInvalidValue;
   const SweepC<R> C = sweep_consts<R>(d, DIR, dt, splitfac, AH);
@@ -54,13 +56,13 @@ int run_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int sche
     auto go = [&](auto rec, auto set) {
       constexpr bool REC = decltype(rec)::value;
       constexpr int NF = sizeof(set.t) / sizeof(set.t[0]);
-      // FP64 sweeps measure faster in the tile kernels (division-bound faces), FP32 in the
-      // vectorised ones
-      const bool vec = sizeof(R) == 4 &&
+      // FP32: both directions vectorised; FP64: the v sweep (the FP64 u sweep measures faster in
+      // the tile kernel, division-bound faces)
+      const bool vec = (sizeof(R) == 4 || DIR == 1) &&
                        vec_layout<R>(d, nk,
                                      {set.t[0].f, set.t[0].fi_src, set.t[0].fi_dst, set.t[NF - 1].f,
                                       set.t[NF - 1].fi_src, set.t[NF - 1].fi_dst, Di_src, Di_dst, adv, U, DU},
-                                     {mflux, mupd, code});
+                                     {mflux, mupd, code}, {set.t[0].lo, set.t[NF - 1].lo});
       if constexpr (sizeof(R) == 4) {
         constexpr int N = 16 / sizeof(R);
         if (vec && DIR == 0) {
@@ -72,8 +74,28 @@ int run_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int sche
           return (int)cudaGetLastError();
         }
         if (vec) {
-          constexpr int VN = 16 / sizeof(R);  // float4 lanes (float2 lanes measured slower)
-          // rows per thread: VJS, halved while the grid would give fewer than ~24 warps per SM
+          auto vl = [&](auto vn) {
+            constexpr int VN = decltype(vn)::value;
+            // rows per thread: VJS, halved while the grid would give fewer than ~24 warps per SM
+            const long long nx = (d.ni() + 32 * VN - 1) / (32 * VN), nz = (nk + VKW - 1) / VKW;
+            int rows = VJS;
+            while (rows > 8 && nx * ((d.nj() + rows - 1) / rows) * nz * VKW < 148LL * 24) rows /= 2;
+            dim3 blk(32, VKW, 1);
+            dim3 grd((unsigned)nx, (d.nj() + rows - 1) / rows, (unsigned)nz);
+            k_sweep_v_vec<R, S, REC, NF, VN><<<grd, blk, 0, s>>>(d, C, nk, rows, set, Di_src, Di_dst, adv, U, DU,
+                                                                 mflux, mupd, code);
+            return (int)cudaGetLastError();
+          };
+          // float4 lanes for one field; float2 lanes for a tracer pair (72 registers against 116:
+          // measured 4% faster at 2048x2048x50 from the higher occupancy; one field measured slower)
+          if (NF == 2) return vl(std::integral_constant<int, 2>());
+          return vl(std::integral_constant<int, 4>());
+        }
+      } else {
+        // FP64: the j-marching v sweep on two-cell (16-byte) lanes (the 2048x2048x50 step's v
+        // sweeps measured 18.8 ms against 25.2 ms in the tile kernel)
+        constexpr int VN = 2;
+        if (vec && DIR == 1) {
           const long long nx = (d.ni() + 32 * VN - 1) / (32 * VN), nz = (nk + VKW - 1) / VKW;
           int rows = VJS;
           while (rows > 8 && nx * ((d.nj() + rows - 1) / rows) * nz * VKW < 148LL * 24) rows /= 2;
@@ -83,8 +105,6 @@ int run_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int sche
                                                                mflux, mupd, code);
           return (int)cudaGetLastError();
         }
-      } else {
-        (void)vec;
       }
       if (DIR == 0) {
         dim3 grd((d.ni() + OWU - 1) / OWU, d.nj(), nz);
@@ -111,7 +131,7 @@ int run_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int sche
 
 template <class R>
 int run_sweep_w2(const Dev& d, cudaStream_t s, R dt, R splitfac, int scheme, R* fa, R* fb, R* hi, const R* ww,
-                 const int32_t* az, R* lo_a, R* lo_b) {
+                 const int32_t* az, __half* lo_a, __half* lo_b) {
   if (sizeof(R) == 8) lo_a = lo_b = nullptr;
   return dispatch_scheme(scheme, [&](auto sc) {
     constexpr int S = decltype(sc)::value;
@@ -125,7 +145,7 @@ int run_sweep_w2(const Dev& d, cudaStream_t s, R dt, R splitfac, int scheme, R* 
 template <class R>
 int run_sweep_w(const Dev& d, cudaStream_t s, R dt, R splitfac, int scheme, int kshift, int itersmax,
                 const R* f, const R* fi_src, R* fi_dst, R* hi, R* adv, const R* ww, const int32_t* az,
-                unsigned long long* warn, uint8_t* code, R* lo) {
+                unsigned long long* warn, uint8_t* code, __half* lo) {
   if (sizeof(R) == 8) lo = nullptr;
   if (itersmax > 1) {
     if (code) return (int)cudaErrorInvalidValue;
@@ -160,7 +180,7 @@ int run_finalise(const Dev& d, cudaStream_t s, R dt, R* f, const R* ho, const R*
 
 template <class R>
 int run_vdiff(const Dev& d, cudaStream_t s, R dt, R cnpar, R avmol, R* S, const R* hn, const R* nuh,
-              const int32_t* az, const R* src, R* rus, R* qus, const R* Sin, R* S2, R* lo) {
+              const int32_t* az, const R* src, R* rus, R* qus, const R* Sin, R* S2, __half* lo) {
   if (d.kmax <= 1) return 0;
   if (sizeof(R) == 8) lo = nullptr;
   const int nx = d.imax - d.imin + 1, ny = d.jmax - d.jmin + 1;
@@ -206,21 +226,21 @@ int run_check_range(const Dev& d, cudaStream_t s, const R* f, const int32_t* az,
 template int run_sweep_h<GB_REAL, 0>(const Dev&, cudaStream_t, int, GB_REAL, GB_REAL, int, GB_REAL,
                                      const GB_REAL*, const GB_REAL*, GB_REAL*, const GB_REAL*, GB_REAL*,
                                      GB_REAL*, const GB_REAL*, const GB_REAL*, const uint8_t*, const uint8_t*,
-                                     uint8_t*, const GB_REAL*, const GB_REAL*, GB_REAL*, GB_REAL*, GB_REAL*);
+                                     uint8_t*, const GB_REAL*, const GB_REAL*, GB_REAL*, __half*, __half*);
 template int run_sweep_h<GB_REAL, 1>(const Dev&, cudaStream_t, int, GB_REAL, GB_REAL, int, GB_REAL,
                                      const GB_REAL*, const GB_REAL*, GB_REAL*, const GB_REAL*, GB_REAL*,
                                      GB_REAL*, const GB_REAL*, const GB_REAL*, const uint8_t*, const uint8_t*,
-                                     uint8_t*, const GB_REAL*, const GB_REAL*, GB_REAL*, GB_REAL*, GB_REAL*);
+                                     uint8_t*, const GB_REAL*, const GB_REAL*, GB_REAL*, __half*, __half*);
 template int run_sweep_w2<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL, int, GB_REAL*, GB_REAL*, GB_REAL*,
-                                   const GB_REAL*, const int32_t*, GB_REAL*, GB_REAL*);
+                                   const GB_REAL*, const int32_t*, __half*, __half*);
 template int run_sweep_w<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL, int, int, int, const GB_REAL*,
                                   const GB_REAL*, GB_REAL*, GB_REAL*, GB_REAL*, const GB_REAL*, const int32_t*,
-                                  unsigned long long*, uint8_t*, GB_REAL*);
+                                  unsigned long long*, uint8_t*, __half*);
 template int run_finalise<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL*, const GB_REAL*, const GB_REAL*,
                                    const GB_REAL*, const uint8_t*);
 template int run_vdiff<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL, GB_REAL, GB_REAL*, const GB_REAL*,
                                 const GB_REAL*, const int32_t*, const GB_REAL*, GB_REAL*, GB_REAL*, const GB_REAL*,
-                                GB_REAL*, GB_REAL*);
+                                GB_REAL*, __half*);
 template int run_tridiag<GB_REAL>(cudaStream_t, int, int, int, int, const GB_REAL*, const GB_REAL*,
                                   const GB_REAL*, const GB_REAL*, GB_REAL*);
 template int run_content<GB_REAL>(const Dev&, cudaStream_t, const GB_REAL*, const GB_REAL*, const int32_t*,

@@ -1,6 +1,7 @@
 // launch.h -- host-side launchers of the templated kernels (instantiated per precision in
 // kernels_f64.cu / kernels_f32.cu). Each returns a cudaError_t as int (0 = success).
 #pragma once
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -10,6 +11,7 @@ struct Dev;
 
 // Process-wide switch of the vectorised horizontal sweeps (getm_set_vector_sweeps; on by default).
 bool vector_sweeps_enabled();
+bool fused_micro_enabled();
 // Process-wide switch of the FP32 working copies of the mixed step's micro steps
 // (getm_set_fp32_micro_steps; on by default).
 bool fp32_micro_steps_enabled();
@@ -18,7 +20,8 @@ constexpr int RED_BLOCKS = 1184;  // 8 x 148 SMs
 constexpr int RED_THREADS = 256;
 
 // lo (FP32 only; FP64 ignores it): compensated storage of a tracer, the carried rounding error of
-// every cell, read and written by the updates (fv_update_lo); null for plain FP32 storage.
+// every cell in FP16, scaled to half an ulp of the cell's value, read and written by the updates
+// (fv_update_lo); null for plain FP32 storage.
 // Horizontal sweep over nk levels starting at the given level pointers. DIR 0 = u, 1 = v.
 // code != nullptr also writes the limiter branch of every face (one byte per face, stored at the
 // face's left / lower cell, same level pointer origin as f).
@@ -28,14 +31,15 @@ template <class R, int DIR>
 int run_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int scheme, R AH, const R* f,
                 const R* fi_src, R* fi_dst, const R* Di_src, R* Di_dst, R* adv, const R* U, const R* DU,
                 const uint8_t* mflux, const uint8_t* mupd, uint8_t* code = nullptr, const R* f_b = nullptr,
-                const R* fi_src_b = nullptr, R* fi_dst_b = nullptr, R* lo = nullptr, R* lo_b = nullptr);
+                const R* fi_src_b = nullptr, R* fi_dst_b = nullptr, __half* lo = nullptr,
+                __half* lo_b = nullptr);
 
 // Vertical sweep on full 3D fields (level-0 pointers); code as above (face k stored at level k;
 // only without sub-iterations).
 template <class R>
 int run_sweep_w(const Dev& d, cudaStream_t s, R dt, R splitfac, int scheme, int kshift, int itersmax,
                 const R* f, const R* fi_src, R* fi_dst, R* hi, R* adv, const R* ww, const int32_t* az,
-                unsigned long long* warn, uint8_t* code = nullptr, R* lo = nullptr);
+                unsigned long long* warn, uint8_t* code = nullptr, __half* lo = nullptr);
 
 // Depth-averaged momentum advection of one micro step with HALFSPLIT (adv2d_fused.cuh): UEx
 // (dir 0, U-grid masks) or VEx (dir 1, V-grid masks) from U, V, DU, DV in one launch, arithmetic
@@ -44,14 +48,30 @@ template <class T>
 int run_uvadv2d_fused(const Dev& d, cudaStream_t s, int dir, T dt, int scheme, const double* U, const double* V,
                       const double* DU, const double* DV, const uint8_t* mflux_u, const uint8_t* mflux_v,
                       const uint8_t* mupd_u, const uint8_t* mupd_v, double* Ex);
+// The bottom friction of the micro step (bottom_friction.F90:48-150), formed by the momentum
+// advection kernel of the same component from the velocities it stages anyway: DIR 0 the U points
+// (ru, ruu; zub for runtype 1), DIR 1 the V points (rv, rvv; zvb). FP32 arithmetic, the operations
+// of k_bottom_friction_f32t (bc.cu) in the same order, so the same values. r == nullptr: off.
+struct Bf2Args {
+  const int32_t* mask;  // au (DIR 0) / av (DIR 1)
+  const int32_t* au;    // DIR 1: the U points' mask for the velocity outside the interior
+  double* zb;           // zub / zvb
+  const double* zb0;    // zub0 / zvb0
+  float* r;             // ru / rv (FP32 working copies)
+  float* rr;            // ruu / rvv
+  float kappa, avmmol, min_depth;
+  int runtype;
+};
+// bf (may be null): also form the bottom friction of the micro step for this component's points
 int run_uvadv2d_fused_f32(const Dev& d, cudaStream_t s, int dir, float dt, int scheme, const float* U,
                           const float* V, const float* DU, const float* DV, const uint8_t* mflux_u,
-                          const uint8_t* mflux_v, const uint8_t* mupd_u, const uint8_t* mupd_v, float* Ex);
+                          const uint8_t* mflux_v, const uint8_t* mupd_u, const uint8_t* mupd_v, float* Ex,
+                          const Bf2Args* bf = nullptr);
 
 // Vertical sweep of two tracers in place (H_TAG, no sub-iterations), heights updated once.
 template <class R>
 int run_sweep_w2(const Dev& d, cudaStream_t s, R dt, R splitfac, int scheme, R* fa, R* fb, R* hi, const R* ww,
-                 const int32_t* az, R* lo_a = nullptr, R* lo_b = nullptr);
+                 const int32_t* az, __half* lo_a = nullptr, __half* lo_b = nullptr);
 
 // ---- adjoint of the tracer step (adjoint.cuh) ----
 // Layer heights before sweeps 2..5 of the HALFSPLIT sequence u/2 v/2 w v/2 u/2, from ho (levels
@@ -87,7 +107,7 @@ int run_finalise(const Dev& d, cudaStream_t s, R dt, R* f, const R* ho, const R*
 template <class R>
 int run_vdiff(const Dev& d, cudaStream_t s, R dt, R cnpar, R avmol, R* S, const R* hn, const R* nuh,
               const int32_t* az, const R* src, R* rus, R* qus, const R* Sin = nullptr, R* S2 = nullptr,
-              R* lo = nullptr);
+              __half* lo = nullptr);
 
 template <class R>
 int run_tridiag(cudaStream_t s, int ncol, int kmax, int fi, int lt, const R* au, const R* bu, const R* cu,

@@ -57,6 +57,32 @@ __device__ __forceinline__ void st_row(R* p, bool full, int navail, const R (&v)
       if (m < navail) p[m] = v[m];
   }
 }
+// the scaled carried errors of N cells (compensated storage, FP16) as floats, and back
+template <int N>
+__device__ __forceinline__ void ld_lo(const __half* p, bool full, int navail, float (&v)[N]) {
+  if (full && N == 4) {
+    const uint2 x = *reinterpret_cast<const uint2*>(p);
+    const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&x.x));
+    const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&x.y));
+    v[0] = a.x; v[1] = a.y; v[2 % N] = b.x; v[3 % N] = b.y;
+  } else {
+#pragma unroll
+    for (int m = 0; m < N; ++m) v[m] = m < navail ? __half2float(p[m]) : 0.f;
+  }
+}
+template <int N>
+__device__ __forceinline__ void st_lo(__half* p, bool full, int navail, const float (&v)[N]) {
+  if (full && N == 4) {
+    uint2 x;
+    *reinterpret_cast<__half2*>(&x.x) = __floats2half2_rn(v[0], v[1]);
+    *reinterpret_cast<__half2*>(&x.y) = __floats2half2_rn(v[2 % N], v[3 % N]);
+    *reinterpret_cast<uint2*>(p) = x;
+  } else {
+#pragma unroll
+    for (int m = 0; m < N; ++m)
+      if (m < navail) p[m] = __float2half_rn(v[m]);
+  }
+}
 template <int N>
 __device__ __forceinline__ void ld_mask(const uint8_t* p, bool full, int navail, uint8_t (&v)[N]) {
   if (full) {
@@ -77,6 +103,7 @@ __device__ __forceinline__ void ld_mask(const uint8_t* p, bool full, int navail,
 // the N mask bytes of a row from cell c0 packed into one word (byte m = cell c0+m)
 template <int N>
 __device__ __forceinline__ uint32_t ld_mask_w(const uint8_t* p, bool full, int navail) {
+  static_assert(N == 2 || N == 4, "mask words of 2 or 4 cells (aligned 16- or 32-bit loads)");
   if (full) {
     if constexpr (N == 4) return *reinterpret_cast<const uint32_t*>(p);
     else return *reinterpret_cast<const uint16_t*>(p);
@@ -91,6 +118,7 @@ __device__ __forceinline__ bool mbit(uint32_t w, int m) { return ((w >> (8 * m))
 
 template <int N>
 __device__ __forceinline__ void st_codes(uint8_t* p, bool full, int navail, const uint8_t (&v)[N]) {
+  static_assert(N == 2 || N == 4, "code words of 2 or 4 cells (aligned 16- or 32-bit stores)");
   if (full) {
     if constexpr (N == 4) {
       *reinterpret_cast<uint32_t*>(p) = (uint32_t)v[0] | ((uint32_t)v[1] << 8) | ((uint32_t)v[2] << 16) |
@@ -303,9 +331,10 @@ __global__ void __launch_bounds__(32 * VKW) k_sweep_v_vec(Dev d, SweepC<R> C, in
     if (NF == 1 && adv) lds_vec<R, N>(sbuf[st][XAD][tid], ad);
 #pragma unroll
     for (int n = 0; n < NF; ++n) {
-      R fo[N], lo[N];
+      R fo[N];
+      float lo[N];
       const bool comp = F.t[n].lo && any;  // compensated storage: the cells' carried errors
-      if (comp) ld_row<R, N>(F.t[n].lo + p, full, navail, lo);
+      if (comp) ld_lo<N>(F.t[n].lo + p, full, navail, lo);
 #pragma unroll
       for (int m = 0; m < N; ++m) {
         const bool upd = jin && mbit(mu, m);
@@ -317,7 +346,7 @@ __global__ void __launch_bounds__(32 * VKW) k_sweep_v_vec(Dev d, SweepC<R> C, in
         if (NF == 1 && adv && upd) ad[m] = ad[m] + advn;
       }
       if (F.t[n].fi_dst && (any || F.t[n].fi_dst != F.t[n].fi_src)) st_row<R, N>(F.t[n].fi_dst + p, full, navail, fo);
-      if (comp) st_row<R, N>(F.t[n].lo + p, full, navail, lo);
+      if (comp) st_lo<N>(F.t[n].lo + p, full, navail, lo);
     }
     if (Di_dst && (any || Di_dst != Di_src)) st_row<R, N>(Di_dst + p, full, navail, Dn);
     if (NF == 1 && adv && any) st_row<R, N>(adv + p, full, navail, ad);
@@ -497,9 +526,9 @@ __global__ void __launch_bounds__(32 * UWB) k_sweep_u_vec(Dev d, SweepC<R> C, in
         if constexpr (NF == 1) lds_vec<R, N>(sbuf[stc][1][tid], fio);
         else ld_row<R, N>(F.t[n].fi_src + p, full, navail, fio);
       }
-      R lo[N];
+      float lo[N];
       const bool comp = F.t[n].lo && any;  // compensated storage: the cells' carried errors
-      if (comp) ld_row<R, N>(F.t[n].lo + p, full, navail, lo);
+      if (comp) ld_lo<N>(F.t[n].lo + p, full, navail, lo);
 #pragma unroll
       for (int q = 0; q < N; ++q) {
         const R advn = cell_advn<R>(C, fl[n][q + 1], fl[n][q]);
@@ -510,7 +539,7 @@ __global__ void __launch_bounds__(32 * UWB) k_sweep_u_vec(Dev d, SweepC<R> C, in
         if (NF == 1 && adv && updm[q]) ad[q] = ad[q] + advn;
       }
       if (F.t[n].fi_dst && (any || F.t[n].fi_dst != F.t[n].fi_src)) st_row<R, N>(F.t[n].fi_dst + p, full, navail, fo);
-      if (comp) st_row<R, N>(F.t[n].lo + p, full, navail, lo);
+      if (comp) st_lo<N>(F.t[n].lo + p, full, navail, lo);
     }
     if (Di_dst && (any || Di_dst != Di_src)) st_row<R, N>(Di_dst + p, full, navail, Dn);
     if (NF == 1 && adv && any) st_row<R, N>(adv + p, full, navail, ad);

@@ -86,6 +86,7 @@ _PROTOS = {
     "getm_tracer_content_f32": [P, P, P, P, P],
     "getm_check_3d_fields": [P, P, P, D, D, P],
     "getm_set_vector_sweeps": [I],
+    "getm_set_fused_micro_step": [I],
     "getm_set_fp32_micro_steps": [I],
     "getm_timers_enable": [P, I],
     "getm_timers_reset": [P],
@@ -149,6 +150,13 @@ def set_fp32_micro_steps(on: bool) -> bool:
     """Process-wide choice for the mixed step's micro steps: FP32 working copies of the 2D fields
     (the default) or the FP64 state arrays; returns the previous setting."""
     return bool(lib().getm_set_fp32_micro_steps(1 if on else 0))
+
+
+def set_fused_micro_step(on: bool) -> bool:
+    """Process-wide choice of the micro-step launches (sealevel + depth_update as one launch with
+    the elevation ping-pong, bottom friction inside the mixed step's momentum advection; or the
+    separate launches); returns the previous setting."""
+    return bool(lib().getm_set_fused_micro_step(1 if on else 0))
 
 
 def set_vector_sweeps(on: bool) -> bool:
@@ -523,7 +531,10 @@ class BcDevice:
             for n in S.F2_NAMES:
                 t["f2_" + n] = torch.from_numpy(case.f2[n]).cuda()
             for n in S.F3_NAMES:
-                if n in ("Tlo", "Slo") and (dt3 == torch.float64 or not compensated):
+                if n in ("Tlo", "Slo"):
+                    # FP16, scaled carried errors, starting at zero
+                    if dt3 == torch.float32 and compensated:
+                        t["f3_" + n] = torch.zeros(case.f3[n].shape, dtype=torch.float16, device="cuda")
                     continue
                 t["f3_" + n] = torch.from_numpy(case.f3[n]).to(dt3).cuda()
             for n, m in zip(("az", "au", "av", "ax"), case.masks()):
@@ -542,7 +553,7 @@ class BcDevice:
         for q, n in enumerate(S.F3_NAMES):
             t3 = self.t.get("f3_" + n)
             assert t3 is not None or n in S.OPTIONAL_F3, n
-            assert t3 is None or t3.dtype == f3dt
+            assert t3 is None or t3.dtype == (torch.float16 if n in ("Tlo", "Slo") else f3dt)
             c.f3[q] = None if t3 is None else _ptr(t3)
         c.az, c.au, c.av, c.ax = (_ptr(self.t[n]) for n in ("az", "au", "av", "ax"))
         for q, n in enumerate(S.PD_NAMES):

@@ -424,8 +424,8 @@ def baroclinic_case_device(nx=2048, ny=2048, kmax=50, recipe="islands", dx=1000.
     for n in ("uu", "vv", "ww", "uuEx", "vvEx", "idpdx", "idpdy"):
         t["f3_" + n] = torch.zeros(shp, dtype=dtype3, device=device)
     if dtype3 == torch.float32 and compensated:  # the mixed step's compensated storage of T and S
-        t["f3_Tlo"] = torch.zeros(shp, dtype=dtype3, device=device)
-        t["f3_Slo"] = torch.zeros(shp, dtype=dtype3, device=device)
+        t["f3_Tlo"] = torch.zeros(shp, dtype=torch.float16, device=device)
+        t["f3_Slo"] = torch.zeros(shp, dtype=torch.float16, device=device)
     return g, BcDevice(tensors=t, pd=dict(c.pd), pi=dict(c.pi))
 
 

@@ -112,10 +112,10 @@ int getm_timers_reset(getm_ctx *ctx);
 int getm_timers_read(getm_ctx *ctx, int slot, double *total_ms, int64_t *launches);
 const char *getm_timer_name(int slot);
 /* Process-wide choice of the horizontal split-sweep kernels (no counterpart in the reference: a
- * tuning and testing switch). on != 0 (the default) runs the FP32 sweeps in the vectorised kernels
- * wherever the rows and levels of the swept fields start on 16-byte boundaries; on == 0 uses the
- * shared-memory tile sweeps everywhere (FP64 always does). Both give identical results. Returns
- * the previous setting. */
+ * tuning and testing switch). on != 0 (the default) runs the FP32 sweeps and the FP64 v sweeps in
+ * the vectorised kernels wherever the rows and levels of the swept fields start on 16-byte
+ * boundaries; on == 0 uses the shared-memory tile sweeps everywhere (the FP64 u sweep always
+ * does). Both give identical results. Returns the previous setting. */
 int getm_set_vector_sweeps(int on);
 /* Process-wide choice for the mixed-precision step (no counterpart in the reference: a testing and
  * accuracy switch). on != 0 (the default) runs the barotropic micro steps of getm_time_loop on FP32
@@ -123,6 +123,13 @@ int getm_set_vector_sweeps(int on);
  * and the static depths stay FP64); on == 0 keeps the micro steps on the FP64 state arrays, as the
  * plain step does. Returns the previous setting. */
 int getm_set_fp32_micro_steps(int on);
+/* Process-wide choice of the micro-step launches (no counterpart in the reference: a tuning and
+ * testing switch). on != 0 (the default): getm_time_loop without open boundaries runs sealevel and
+ * depth_update as one launch per micro step, the new elevations alternating between the z and zo
+ * arrays (at the end of the call z and zo hold what the separate launches leave), and the
+ * mixed-precision micro step forms its bottom friction inside the momentum-advection kernels;
+ * on == 0: the separate launches. Both give identical results. Returns the previous setting. */
+int getm_set_fused_micro_step(int on);
 /* Human-readable text of the last error on this context (never NULL). */
 const char *getm_ctx_last_error(const getm_ctx *ctx);
 const char *getm_version(void);
@@ -238,12 +245,14 @@ int getm_tracer_step_f32(getm_ctx *ctx, float dt, float *f, const float *uu, con
  * finishing its steps; the reference stops at once). swr, shf, A, g1, g2 and rad may be NULL when
  * radiation = 0, tke and eps may always be NULL.
  * Tlo, Slo (no counterpart in the reference; FP32 states only, may be NULL): compensated storage of
- * the mixed step's temperature and salinity. T is then the unevaluated sum T + Tlo of two FP32
- * numbers (likewise S): every advection sweep and diffusion solve adds its increment to T exactly and
- * keeps the rounding error in Tlo (|Tlo| < half an ulp of T), so that the increments smaller than
- * half an ulp of T -- which plain FP32 storage loses at every update, and which a tracer far from
- * zero receives every sweep -- are kept. The fluxes and the equation of state read T alone. Start
- * them at zero; NULL gives plain FP32 storage. The FP64 step ignores them. */
+ * the mixed step's temperature and salinity, as IEEE binary16 (2 bytes per element, the 3D layout of
+ * the other fields). T is then the unevaluated sum T + e of an FP32 number and its carried rounding
+ * error e (|e| <= half an ulp of T), stored as Tlo = e * 2^16 -- likewise S: every advection sweep
+ * and diffusion solve adds its increment to T exactly and keeps the rounding error in e, so that the
+ * increments smaller than half an ulp of T -- which plain FP32 storage loses at every update, and
+ * which a tracer far from zero receives every sweep -- are kept to about 11 more bits. Valid for
+ * |T| < 2^23. The fluxes and the equation of state read T alone. Start them at zero; NULL gives
+ * plain FP32 storage. The FP64 step ignores them. */
 #define GETM_NF2 59
 #define GETM_NF3 24
 #define GETM_NPD 23

@@ -220,6 +220,124 @@ def test_gradient_tracer_adjoint_configuration_fd():
     assert np.median(errs) <= 1e-5 and (errs > 1e-4).sum() <= 4 and errs.max() <= 1e-3, errs
 
 
+def _fd_sweep(c, nsteps, every, box, which, eps_list, ndirs=64):
+    """{eps: (relative differences, limiter-branch flips)} of the directional derivatives of the
+    checkpointed gradient against central differences of the GPU forward run, on the same ndirs
+    seeded directions for every eps; which = "f" (initial tracer) or "nuh" (relative perturbation
+    of the diffusivity). The two forward runs of a difference record their limiter branches
+    (getm_tracer_step_record, the same bits as getm_tracer_step); flips = the number of faces and
+    steps at which the + and - runs took different branches, i.e. at which the secant crosses a
+    kink of the piecewise-linear step."""
+    import torch
+
+    p = c.par
+    ctx, m = make_ctx(c)
+    t = _dev_fields(c)
+    w = cases.box_weights(c, box=box)
+    wt = dev(w)
+    _, fbar, nubar, _ = _gradient(ctx, c, t, nsteps, every, w)
+    rng = np.random.default_rng(11 if which == "f" else 12)
+    wet = torch.from_numpy((c["az"] >= 1)[None].astype(np.float64)).cuda()
+    tapes = [ctx.tape(torch.float64), ctx.tape(torch.float64)]
+    for tp in tapes:
+        tp[0].zero_()
+
+    def run(f0, nuh, tp, codes):
+        f = f0.clone()
+        for q in range(nsteps):
+            ctx.tracer_step_record(p["dt"], f, *[t[n] for n in NAMES], nuh, 2, p["hscheme"], p["vscheme"], p["AH"],
+                                   p["cnpar"], p["avmol"], tp)
+            codes[q].copy_(tp[0])
+        return f
+
+    codes = [[torch.empty_like(tapes[0][0]) for _ in range(nsteps)] for _ in range(2)]
+    f0 = dev(c["f"])
+    dirs = [torch.from_numpy(rng.normal(size=c["f"].shape)).cuda() * wet for _ in range(ndirs)]
+    out = {}
+    for eps in eps_list:
+        errs, flips = [], []
+        for d in dirs:
+            if which == "f":
+                fp = run(f0 + eps * d, t["nuh"], tapes[0], codes[0])
+                fm = run(f0 - eps * d, t["nuh"], tapes[1], codes[1])
+                ad = float(torch.sum(fbar * d))
+            else:
+                dn = d * t["nuh"]
+                fp = run(f0, t["nuh"] + eps * dn, tapes[0], codes[0])
+                fm = run(f0, t["nuh"] - eps * dn, tapes[1], codes[1])
+                ad = float(torch.sum(nubar * dn))
+            fd = float(torch.sum(wt * (fp - fm))) / (2 * eps)
+            errs.append(abs(ad - fd) / abs(fd))
+            flips.append(int(sum(int(torch.count_nonzero(a != b)) for a, b in zip(codes[0], codes[1]))))
+        out[eps] = (np.array(errs), np.array(flips))
+    return out
+
+
+def _report(which, res):
+    for eps, (e, fl) in res.items():
+        calm = e[fl == 0]
+        print(f"d{which} eps {eps:.0e}: median {np.median(e):.1e}, max {e.max():.1e}, "
+              f"{int((e <= 1e-4).sum())}/{len(e)} within 1e-4; {len(calm)} directions without branch flips"
+              + (f" (max {calm.max():.1e})" if len(calm) else "") + f"; flips per direction median {np.median(fl):.0f}")
+
+
+@pytest.mark.parametrize("which,eps_list", [("f", (1e-7, 1e-9, 1e-11)), ("nuh", (1e-2, 1e-4, 1e-6))])
+def test_tracer_adjoint_configuration_fd_sweep(which, eps_list):
+    """Both gradients of the tracer-adjoint configuration (256 x 256 x 30, SUPERBEE, 50 steps,
+    checkpoint every 10) against central differences on 64 seeded directions, for three step sizes
+    each: dJ/df0 (absolute steps on a tracer of range ~1) and dJ/dnuh (relative perturbations of
+    the diffusivity). Prints the median, the maximum, the share within 1e-4 and the limiter-branch
+    flips per direction. The step is piecewise linear in the tracer (SUPERBEE's branches) and the
+    gradient is that of the branches the forward run took, exactly (checked against the
+    tangent-linear model above); every secant here crosses kinks (no direction is flip-free, even
+    at 1e-11). In this configuration the flow is the same in every layer and the tracer's vertical
+    structure is its 1e-3 noise, so the diffusion only moves tracer within columns and J depends on
+    nuh only through the limiters (with a linear scheme dJ/dnuh is exactly zero: see the next
+    test): dJ/dnuh is the derivative of the branch pattern itself, which the secants measure to a
+    median of about 1e-3. Bounds at the best step size: dJ/df0 median 1e-5 and 56 of 64 within
+    1e-4; dJ/dnuh median 2e-3."""
+    c = cases.streamfunction_flow(nx=256, ny=256, kmax=30, dt=300.0, seed=4)
+    c.par.update(cnpar=1.0, avmol=0.0)
+    res = _fd_sweep(c, 50, 10, 32, which, eps_list)
+    _report(which, res)
+    best = max((e for e, _ in res.values()), key=lambda e: ((e <= 1e-4).sum(), -np.median(e)))
+    if which == "f":
+        assert np.median(best) <= 1e-5 and (best <= 1e-4).sum() >= 56, best
+    else:
+        assert np.median(best) <= 2e-3, best
+
+
+def test_tracer_adjoint_configuration_nuh_gradient_zero_for_linear_scheme():
+    """With the linear P2 scheme in the tracer-adjoint configuration (depth-uniform flow, ww = 0)
+    every layer is advected by the same linear map, so J (the box content summed over the layers)
+    is the advection of the column sums, which the vertical diffusion conserves: dJ/dnuh = 0. The
+    adjoint's nubar is zero to rounding (relative to the same configuration's dJ/df0)."""
+    import torch
+
+    c = cases.streamfunction_flow(nx=256, ny=256, kmax=30, dt=300.0, seed=4)
+    c.par.update(cnpar=1.0, avmol=0.0, hscheme=3, vscheme=3)
+    ctx, m = make_ctx(c)
+    t = _dev_fields(c)
+    w = cases.box_weights(c, box=32)
+    _, fbar, nubar, _ = _gradient(ctx, c, t, 50, 10, w)
+    scale = float(torch.abs(fbar).max()) * float(t["nuh"].max())
+    assert float(torch.abs(nubar * t["nuh"]).max()) <= 1e-9 * scale
+
+
+@pytest.mark.parametrize("which,eps", [("f", 1e-3), ("nuh", 1e-4)])
+def test_tracer_adjoint_sheared_linear_scheme_fd(which, eps):
+    """The tracer-adjoint configuration with the linear P2 scheme (no branches) and a vertically
+    sheared flow (the layers move at 0.5 .. 1.5 times the mean flow, so the vertical diffusion
+    changes J): both gradients against central differences on 64 seeded directions, each within
+    1e-4 (the step is linear in the tracer, so a large step size only reduces the rounding)."""
+    c = cases.streamfunction_flow(nx=256, ny=256, kmax=30, dt=300.0, seed=4, shear=1.0)
+    c.par.update(cnpar=1.0, avmol=0.0, hscheme=3, vscheme=3)
+    res = _fd_sweep(c, 50, 10, 32, which, (eps,))
+    _report(which, res)
+    e, _ = res[eps]
+    assert e.max() <= 1e-4, e
+
+
 @pytest.mark.parametrize("scheme,tol", [(3, 1e-4), (4, 1e-3)])
 def test_gradient_fp32_vs_fp64_tangent(scheme, tol):
     """FP32 checkpointed gradient against the FP64 tangent-linear oracle. With the linear P2 scheme

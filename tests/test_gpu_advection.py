@@ -233,11 +233,11 @@ def test_tracer_content_and_check(rc):
     assert ctx.check_3d_fields(tf, m[0], lo, hi) == want_n
 
 
-@pytest.mark.parametrize("dtype", ["f32"])
+@pytest.mark.parametrize("dtype", ["f32", "f64"])
 @pytest.mark.parametrize("hs", [G.UPSTREAM, G.SUPERBEE, G.P2_PDM])
 def test_vector_and_tile_sweeps_agree(dtype, hs):
-    """The vectorised FP32 sweeps and the tile sweeps give identical results (bit for bit), tracer
-    step with record tape included (FP64 always runs the tile sweeps)."""
+    """The vectorised sweeps (FP32: u and v; FP64: v on two-cell lanes) and the tile sweeps give
+    identical results (bit for bit), tracer step with record tape included."""
     import torch
 
     c = cases.random_case(nx=60, ny=45, kmax=7, seed=11)

@@ -245,6 +245,35 @@ def test_mixed_kernel_forms_agree(recipe, nx, ny):
         assert np.array_equal(out[True].f3[k], out[False].f3[k], equal_nan=True), k
 
 
+@pytest.mark.parametrize("count", [20, 23])
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_fused_micro_step_forms_agree(prec, count):
+    """getm_time_loop with the fused micro-step launches (the default: sealevel + depth_update in
+    one launch with the elevations alternating between z and zo; the mixed step's bottom friction
+    inside its momentum-advection kernels) and with the separate launches
+    (getm_set_fused_micro_step(0)) gives the same bits in every field, z and zo included -- after
+    an even and an odd number of micro steps."""
+    import torch
+
+    from code_b200 import getm as G
+
+    c = S.baroclinic_case(nx=77, ny=53, kmax=8, recipe="islands", land=0.3, M=5, dt3=60.0, seed=4)
+    if prec == "mixed":
+        c = c.copy(dtype3=np.float32)
+    out = {}
+    prev = G.set_fused_micro_step(True)
+    try:
+        for on in (True, False):
+            G.set_fused_micro_step(on)
+            out[on], _ = run_gpu(c, 1, count, dtype3=torch.float32 if prec == "mixed" else None)
+    finally:
+        G.set_fused_micro_step(prev)
+    for k in S.F2_NAMES:
+        assert np.array_equal(out[True].f2[k], out[False].f2[k], equal_nan=True), k
+    for k in S.F3_NAMES:
+        assert np.array_equal(out[True].f3[k], out[False].f3[k], equal_nan=True), k
+
+
 @pytest.mark.parametrize("method", [2, 4, 5, 6])
 @pytest.mark.parametrize("recipe", ["shelf", "islands"])
 def test_ip_method_vs_oracle(recipe, method):
