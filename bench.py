@@ -34,12 +34,37 @@ UNIT = "cell-steps/s"
 WORKLOAD = ("mode-split baroclinic step (20 x integrate_2d + integrate_3d: 2D momentum/sealevel, internal "
             "pressure, 3D momentum with implicit viscosity, P2_PDM advection of u, v, T, S, implicit diffusion), "
             "2048x2048x50 irregular domain, 30% land, depth 5-150 m")
-# algorithmic words per interior cell per launch of a stage (each field read/written once). The
-# horizontal sweeps of a macro step are momentum sweeps (read f, U, DU, Di, adv; write fi, Di, adv)
-# and paired tracer sweeps (read T, S, U, DU, Di; write T, S, Di): 8 words either way; the vertical
-# sweeps 7 (f, ww, hi, adv / T, S, ww, hi read; f, hi, adv / T, S, hi written).
-STAGE_WORDS = {"adv_split_u": 8, "adv_split_v": 8, "adv_split_w": 7, "tracer_vdiff": 4, "uv_momentum_3d": 8,
-               "internal_pressure": 6}
+# Algorithmic words (of the 3D fields' precision) per interior cell of each launch of a stage in one
+# macro step, each 3D field read or written once counted once; the 2D column heights that the sweeps
+# and the diffusion take in place of the 3D height arrays (equidistant sigma) are 1/kmax of a field
+# and not counted:
+#  * u sweeps: momentum U and V grids (u1: read f, U [+ adv in FP64, where the sum starts from a
+#    cleared array; the mixed step's vectorised first sweep starts it itself]; write fi, Di, adv.
+#    u2: read f, U, Di, adv; write adv), then the tracer pair (u1: read T, S, U; write T, S, Di.
+#    u2: read T, S, U, Di; write T, S, Di);
+#  * v sweeps: momentum v1, v2 on both grids (read f, V, Di, adv; write f, Di, adv), tracer pair v1,
+#    v2 (read T, S, V, Di; write T, S, Di);
+#  * w sweeps: momentum on both grids (read f, ww, hi, adv; write f, hi, adv), tracer pair (read T,
+#    S, ww, hi; write T, S, hi);
+#  * diffusion: one launch for T and S (read nuh, T, S; write T, S);
+# plus, with compensated tracer storage, the FP16 carried errors of T and S read and written by each
+# tracer launch (4 x 2 bytes = 2 words of 4 bytes).
+STAGE_LAUNCH_WORDS = {"adv_split_u": ([6, 5, 6, 5, 6, 7], [5, 5, 5, 5, 6, 7]),
+                      "adv_split_v": ([7, 7, 7, 7, 7, 7], [7, 7, 7, 7, 7, 7]),
+                      "adv_split_w": ([7, 7, 7], [7, 7, 7]),
+                      "tracer_vdiff": ([5], [5]),
+                      "uv_momentum_3d": ([8, 8], [8, 8]),
+                      "internal_pressure": ([6], [6])}
+LO_WORDS = {"adv_split_u": [0, 0, 0, 0, 2, 2], "adv_split_v": [0, 0, 0, 0, 2, 2], "adv_split_w": [0, 0, 2],
+            "tracer_vdiff": [2]}
+
+
+def stage_words(stage: str, mixed: bool, compensated: bool) -> float:
+    """Average algorithmic words per interior cell and launch of a stage of the macro step."""
+    w = list(STAGE_LAUNCH_WORDS[stage][1 if mixed else 0])
+    if mixed and compensated:
+        w = [a + b for a, b in zip(w, LO_WORDS.get(stage, [0] * len(w)))]
+    return sum(w) / len(w)
 # DRAM bytes (read + write) per interior cell per launch of the FP32 stages, averaged over the
 # launches of the timed macro step of this workload (2048 x 2048 x 50): ncu --metrics
 # dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum (one pass) on the advection and
@@ -558,10 +583,10 @@ def main():
             macro_step("fp64")
         torch.cuda.synchronize()
         tim64 = c64.timers(enable=False, reset=True)
-    timed = {k: t for k, t in tim.items() if k in STAGE_WORDS}
+    timed = {k: t for k, t in tim.items() if k in STAGE_LAUNCH_WORDS}
     top_name, (top_ms, top_n) = max(timed.items(), key=lambda kv: kv[1][0])
     wb = 4 if head == "mixed" else 8
-    alg_bytes = STAGE_WORDS[top_name] * cells * wb
+    alg_bytes = stage_words(top_name, head == "mixed", args.compensated) * cells * wb
     peak, peak_kind = load_peaks()
     achieved = alg_bytes / (top_ms / top_n / 1e3) / 1e9
     # whole-step algorithmic bytes (3D: read+write uu, vv, T, S; 2D: 17 FP64 words per column per micro step)

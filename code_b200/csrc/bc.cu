@@ -903,6 +903,12 @@ int ensure_bc_scratch(getm_ctx* ctx, size_t elem3) {
     }
     cudaMemsetAsync(ctx->bc_scr2, 0, (size_t)NB2 * n2 * sizeof(double), ctx->stream);
   }
+  if (!ctx->colh) {
+    if (cudaMalloc(&ctx->colh, (size_t)NCOLH * n2 * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(ctx, GETM_ERR_NOMEM, "mode-split column-height allocation failed");
+    }
+  }
   return GETM_OK;
 }
 
@@ -1228,13 +1234,14 @@ __global__ void k_sync_w2(long long n2, Bc2 s, Bc2W w, FieldList fl, int to_w, i
 }
 
 template <class R3>
-int bc3(getm_ctx* ctx, const getm_bc_state* st, int which, int slot) {
+int bc3(getm_ctx* ctx, const getm_bc_state* st, int which, int slot, unsigned skip = 0) {
   const Bc3<R3> s = to_bc3<R3>(st);
   const long long n3 = n3d(ctx->dev);
   R3* base = (R3*)ctx->bc_scr3;
   R3* scr[NB3F];
   const int nb = sizeof(R3) == 4 ? NB3F : NB3;
-  for (int q = 0; q < NB3F; ++q) scr[q] = q < nb ? base + q * n3 : nullptr;
+  // skip: scratch slots the kernel does not write (bit q = slot q)
+  for (int q = 0; q < NB3F; ++q) scr[q] = (q < nb && !((skip >> q) & 1u)) ? base + q * n3 : nullptr;
   GB_TIMED(slot, (run_bc3<R3>(which, ctx->dev, ctx->stream, s, scr)), "macro-step kernel");
   return GETM_OK;
 }
@@ -1293,6 +1300,13 @@ int integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
     ip[I_UFIRST3D] = 1;
   }
   if ((rc = bc3<R3>(ctx, st, BC3_SIGMA, GETM_TIM_BC3D))) return rc;
+  // the heights sigma_coordinates just set, as 2D planes of column values: the advection and
+  // diffusion launches below read them in place of the 3D height arrays (equidistant sigma: every
+  // level of a column has the same height)
+  R3* colh = (R3*)ctx->colh;
+  const long long n2 = n2d(d);
+  auto CH = [&](int q) { return colh + (long long)q * n2; };
+  GB_TIMED(GETM_TIM_BC3D, run_col_heights<R3>(d, s, to_bc3<R3>(st), colh), "column heights");
   if (d.kmax > 1) {
     if ((rc = bc3<R3>(ctx, st, BC3_WW, GETM_TIM_BC3D))) return rc;
     // uv_advect_3d (uv_advect_3d.F90:62-460); only the advection terms uuEx/vvEx are kept, so the
@@ -1301,17 +1315,32 @@ int integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
     if (hor != NOADV || ver != NOADV) {
       R3* w = (R3*)ctx->bc_scr3;
       // FP32: both grids' quantities in one pass (U grid in scratch 0-5, V grid in 7-12); FP64: the
-      // U grid, its advection, then the V grid into the same six arrays
+      // U grid, its advection, then the V grid into the same six arrays. With the split sweeps the
+      // face depths huadv, hvadv and the control-volume heights come from the column heights (h2d)
+      // and the set-up does not form them.
+      const bool cols = (split == GETM_HALFSPLIT || split == GETM_FULLSPLIT) && is_split_scheme(hor) &&
+                        is_split_scheme(ver);
+      const unsigned h2d = cols ? 7u : 0u;
+      const unsigned skip = cols ? ((1u << 4) | (1u << 5) | (1u << 11) | (1u << 12)) : 0u;
       R3* wv = sizeof(R3) == 4 ? w + 7 * n3 : w;
       R3 *fadv = w, *ua = w + n3, *va = w + 2 * n3, *wa = w + 3 * n3, *hua = w + 4 * n3, *hva = w + 5 * n3;
       R3 *fadvv = wv, *uav = wv + n3, *vav = wv + 2 * n3, *wav = wv + 3 * n3, *huav = wv + 4 * n3, *hvav = wv + 5 * n3;
-      if ((rc = bc3<R3>(ctx, st, sizeof(R3) == 4 ? BC3_UVADV_PREP_UV : BC3_UVADV_PREP_U, GETM_TIM_BC3D))) return rc;
-      if ((rc = do_adv3d<R3>(ctx, R3(st->par[P_DT]), fadv, ua, va, wa, hua, hva, f3[HUN], f3[HUN], split, hor, ver,
-                             R3(0), GETM_U_TAG, nullptr, f3[UUEX], ip[I_ADV_VER_ITERS], false)))
+      if (cols) {
+        hua = CH(COL_HUA_U);
+        hva = CH(COL_HVA_U);
+        huav = CH(COL_HUA_V);
+        hvav = CH(COL_HVA_V);
+      }
+      const R3* hou = cols ? CH(COL_HUN) : f3[HUN];
+      const R3* hov = cols ? CH(COL_HVN) : f3[HVN];
+      if ((rc = bc3<R3>(ctx, st, sizeof(R3) == 4 ? BC3_UVADV_PREP_UV : BC3_UVADV_PREP_U, GETM_TIM_BC3D, skip)))
         return rc;
-      if (sizeof(R3) == 8 && (rc = bc3<R3>(ctx, st, BC3_UVADV_PREP_V, GETM_TIM_BC3D))) return rc;
-      if ((rc = do_adv3d<R3>(ctx, R3(st->par[P_DT]), fadvv, uav, vav, wav, huav, hvav, f3[HVN], f3[HVN], split, hor,
-                             ver, R3(0), GETM_V_TAG, nullptr, f3[VVEX], ip[I_ADV_VER_ITERS], false)))
+      if ((rc = do_adv3d<R3>(ctx, R3(st->par[P_DT]), fadv, ua, va, wa, hua, hva, hou, hou, split, hor, ver, R3(0),
+                             GETM_U_TAG, nullptr, f3[UUEX], ip[I_ADV_VER_ITERS], false, nullptr, h2d)))
+        return rc;
+      if (sizeof(R3) == 8 && (rc = bc3<R3>(ctx, st, BC3_UVADV_PREP_V, GETM_TIM_BC3D, skip))) return rc;
+      if ((rc = do_adv3d<R3>(ctx, R3(st->par[P_DT]), fadvv, uav, vav, wav, huav, hvav, hov, hov, split, hor, ver,
+                             R3(0), GETM_V_TAG, nullptr, f3[VVEX], ip[I_ADV_VER_ITERS], false, nullptr, h2d)))
         return rc;
     }
     if ((rc = bc3<R3>(ctx, st, BC3_STRESSES, GETM_TIM_BC3D))) return rc;
@@ -1354,18 +1383,19 @@ int integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
         GB_TRY(cudaMemcpyAsync(s_top, f3[SS] + (long long)d.kmax * d.sk, n2d(d) * sizeof(R3), cudaMemcpyDeviceToDevice,
                                s),
                "top-level salinity");
-      if ((rc = do_adv3d_pair<R3>(ctx, dt, f3[TT], f3[SS], f3[UU], f3[VV], f3[WW], f3[HUN], f3[HVN], f3[HO],
-                                  ip[I_TEMP_HOR], ip[I_TEMP_VER], R3(st->par[P_TEMP_AH]), tlo, slo)))
+      if ((rc = do_adv3d_pair<R3>(ctx, dt, f3[TT], f3[SS], f3[UU], f3[VV], f3[WW], CH(COL_HUN), CH(COL_HVN),
+                                  CH(COL_HO), ip[I_TEMP_HOR], ip[I_TEMP_VER], R3(st->par[P_TEMP_AH]), tlo, slo,
+                                  7u)))
         return rc;
       if (radn && (rc = temp_sources(s_top))) return rc;
-      GB_TIMED(GETM_TIM_VDIFF, run_vdiff<R3>(d, s, dt, R3(st->par[P_CNPAR]), R3(st->par[P_AVMOLT]), f3[TT], f3[HN],
-                                             f3[NUH], st->az, (const R3*)tsrc, (R3*)ctx->scr[0], (R3*)ctx->scr[1],
-                                             nullptr, nullptr, tlo),
-               "vdiff T");
-      GB_TIMED(GETM_TIM_VDIFF, run_vdiff<R3>(d, s, dt, R3(st->par[P_CNPAR]), R3(st->par[P_AVMOLS]), f3[SS], f3[HN],
-                                             f3[NUH], st->az, (const R3*)nullptr, (R3*)ctx->scr[0], (R3*)ctx->scr[1],
-                                             nullptr, nullptr, slo),
-               "vdiff S");
+      // the two diffusion solves in one launch (shared hn, nuh); salinity's elimination
+      // coefficients in the macro-step scratch, free at this point of the step
+      R3* b3 = (R3*)ctx->bc_scr3;
+      GB_TIMED(GETM_TIM_VDIFF,
+               run_vdiff2<R3>(d, s, dt, R3(st->par[P_CNPAR]), CH(COL_HN), f3[NUH], st->az, f3[TT],
+                              R3(st->par[P_AVMOLT]), (const R3*)tsrc, (R3*)ctx->scr[0], (R3*)ctx->scr[1], tlo,
+                              f3[SS], R3(st->par[P_AVMOLS]), b3, b3 + n3, slo, true),
+               "vdiff T, S");
     }
     if (!pair && ip[I_CALC_TEMP]) {
       if ((rc = do_adv3d<R3>(ctx, dt, f3[TT], f3[UU], f3[VV], f3[WW], f3[HUN], f3[HVN], f3[HO], f3[HN],

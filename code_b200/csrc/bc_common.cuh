@@ -62,6 +62,8 @@ struct Bc3 {
 // number of 3D / 2D scratch arrays of the mode-split step
 constexpr int NB3 = 7;   // fadv, uuadv, vvadv, wwadv, huadv, hvadv, zz
 constexpr int NB3F = 13; // FP32: the same, then the V grid's six (both grids prepared in one pass)
+// planes of the column heights (k_col_heights)
+enum { COL_HO, COL_HN, COL_HUN, COL_HVN, COL_HUA_U, COL_HVA_U, COL_HUA_V, COL_HVA_V, NCOLH };
 constexpr int NB2 = 10;  // fadv, Uadv, Vadv, DUadv, DVadv, Di, adv, S, Ui, Vi
 
 }  // namespace gb

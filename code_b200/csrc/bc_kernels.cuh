@@ -693,37 +693,78 @@ __global__ void __launch_bounds__(128) k_sigma_vec(Dev d, Bc3<float> s) {
 }
 
 // ww_momentum_3d.F90:74-106 (kmin = 1): upward continuity integral per wet interior column.
+// The layer height that k_sigma / k_sigma_vec store at every level of a column (equidistant sigma
+// coordinates, sigma_coordinates.F90:85-113), formed with their expression from the column's
+// elevation e (sseo, ssen, ssuo, ssun, ssvo, ssvn) and depth hx (H, HU, HV): the kernels that run
+// after k_sigma in the same macro step take the heights from here instead of reading the 3D
+// arrays back (the same values where k_sigma wrote them).
+template <class R3>
+__device__ __forceinline__ R3 sig_h(const Bc3<R3>& s, int e, int hx, long long c, double kmaxm1) {
+  return R3((s.f2[e][c] + s.f2[hx][c]) * kmaxm1);
+}
+
+// The column heights of the macro step after k_sigma, as 2D planes of R3 (NCOLH of them, n2 apart):
+// COL_HO, COL_HN, COL_HUN, COL_HVN = the values k_sigma stored at every level of ho, hn, hun, hvn;
+// COL_HUA_U, COL_HVA_U, COL_HUA_V, COL_HVA_V = the face depths huadv, hvadv of the U and the V
+// momentum grids (uv_advect_3d.F90:76-98, :267-289), which are the same at every level. Cells where
+// k_sigma or uv_advect_3d form no value hold 0.
+template <class R3>
+__global__ void k_col_heights(Dev d, Bc3<R3> s, R3* out) {
+  GB_IJ_HALO
+  const int ni = d.ni(), nj = d.nj();
+  const long long n2 = (long long)ni * nj;
+  const int ii = i - (d.imin - HALO), jj = j - (d.jmin - HALO);
+  const long long c = d.ix(i, j);
+  const double kmaxm1 = 1.0 / (double)(float)d.kmax;
+  const R3 half = R3(0.5);
+  auto ho = [&](long long q) { return sig_h<R3>(s, SSEO, HH, q, kmaxm1); };
+  auto hn = [&](long long q) { return sig_h<R3>(s, SSEN, HH, q, kmaxm1); };
+  auto hun = [&](long long q) { return sig_h<R3>(s, SSUN, HU, q, kmaxm1); };
+  auto hvn = [&](long long q) { return sig_h<R3>(s, SSVN, HV, q, kmaxm1); };
+  const bool ulast = ii == ni - 1, vlast = jj == nj - 1;
+  out[COL_HO * n2 + c] = ho(c);
+  out[COL_HN * n2 + c] = hn(c);
+  out[COL_HUN * n2 + c] = ulast ? R3(0) : hun(c);
+  out[COL_HVN * n2 + c] = vlast ? R3(0) : hvn(c);
+  out[COL_HUA_U * n2 + c] = ulast ? R3(0) : half * (ho(c + 1) + hn(c + 1));
+  out[COL_HVA_U * n2 + c] = (ulast || vlast) ? R3(0) : half * (hvn(c) + hvn(c + 1));
+  out[COL_HUA_V * n2 + c] = (ulast || vlast) ? R3(0) : half * (hun(c) + hun(c + d.sj));
+  out[COL_HVA_V * n2 + c] = vlast ? R3(0) : half * (ho(c + d.sj) + hn(c + d.sj));
+}
+
+// ww_momentum_3d.F90:74-106 with the layer heights of the column from sig_h (read after k_sigma)
 template <class R3>
 __global__ void k_ww(Dev d, Bc3<R3> s) {
   GB_IJ_HALO
   if (i < d.imin || i > d.imax || j < d.jmin || j > d.jmax) return;
   I2 az{d, s.az};
   if (az(i, j) != 1) return;
-  V3<R3> ww{d, s.f3[WW]}, hn{d, s.f3[HN]}, ho{d, s.f3[HO]}, uu{d, s.f3[UU]}, vv{d, s.f3[VV]};
+  V3<R3> ww{d, s.f3[WW]}, uu{d, s.f3[UU]}, vv{d, s.f3[VV]};
   const R3 dtm1 = R3(1.0 / s.par[P_DT]);
   const R3 dx = R3(d.dx), dy = R3(d.dy), ard1 = R3(d.ard1);
+  const double kmaxm1 = 1.0 / (double)(float)d.kmax;
+  const long long c = d.ix(i, j);
+  const R3 hnc = sig_h<R3>(s, SSEN, HH, c, kmaxm1), hoc = sig_h<R3>(s, SSEO, HH, c, kmaxm1);
   // four levels' loads are issued before their four stores (the loads do not wait on the stores)
   R3 w = ww(i, j, 0);
   int k = 1;
   for (; k + 3 <= d.kmax - 1; k += 4) {
-    R3 a[4][6];
+    R3 a[4][4];
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
-      a[m][0] = hn(i, j, k + m);
-      a[m][1] = ho(i, j, k + m);
-      a[m][2] = uu(i, j, k + m);
-      a[m][3] = uu(i - 1, j, k + m);
-      a[m][4] = vv(i, j, k + m);
-      a[m][5] = vv(i, j - 1, k + m);
+      a[m][0] = uu(i, j, k + m);
+      a[m][1] = uu(i - 1, j, k + m);
+      a[m][2] = vv(i, j, k + m);
+      a[m][3] = vv(i, j - 1, k + m);
     }
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
-      w = w - (a[m][0] - a[m][1]) * dtm1 - (a[m][2] * dy - a[m][3] * dy + a[m][4] * dx - a[m][5] * dx) * ard1;
+      w = w - (hnc - hoc) * dtm1 - (a[m][0] * dy - a[m][1] * dy + a[m][2] * dx - a[m][3] * dx) * ard1;
       ww(i, j, k + m) = w;
     }
   }
   for (; k <= d.kmax - 1; ++k) {
-    w = w - (hn(i, j, k) - ho(i, j, k)) * dtm1 -
+    w = w - (hnc - hoc) * dtm1 -
         (uu(i, j, k) * dy - uu(i - 1, j, k) * dy + vv(i, j, k) * dx - vv(i, j - 1, k) * dx) * ard1;
     ww(i, j, k) = w;
   }
@@ -750,16 +791,16 @@ __global__ void k_uvadv3d_prep(Dev d, Bc3<R3> s, R3* fadvp, R3* uuadvp, R3* vvad
     uuadv(i, j, k) = half * (uu(i, j, k) + uu(i + 1, j, k));
     vvadv(i, j, k) = half * (vv(i, j, k) + vv(i + 1, j, k));
     wwadv(i, j, k) = half * (ww(i, j, k) + ww(i + 1, j, k));
-    huadv(i, j, k) = half * (ho(i + 1, j, k) + hn(i + 1, j, k));
-    hvadv(i, j, k) = half * (hvn(i, j, k) + hvn(i + 1, j, k));
+    if (huadvp) huadv(i, j, k) = half * (ho(i + 1, j, k) + hn(i + 1, j, k));
+    if (hvadvp) hvadv(i, j, k) = half * (hvn(i, j, k) + hvn(i + 1, j, k));
   } else {
     if (k == 0 || j > d.jmax + HALO - 1) return;
     fadv(i, j, k) = vv(i, j, k) / hvn(i, j, k);
     uuadv(i, j, k) = half * (uu(i, j, k) + uu(i, j + 1, k));
     vvadv(i, j, k) = half * (vv(i, j, k) + vv(i, j + 1, k));
     wwadv(i, j, k) = half * (ww(i, j, k) + ww(i, j + 1, k));
-    huadv(i, j, k) = half * (hun(i, j, k) + hun(i, j + 1, k));
-    hvadv(i, j, k) = half * (ho(i, j + 1, k) + hn(i, j + 1, k));
+    if (huadvp) huadv(i, j, k) = half * (hun(i, j, k) + hun(i, j + 1, k));
+    if (hvadvp) hvadv(i, j, k) = half * (ho(i, j + 1, k) + hn(i, j + 1, k));
   }
 }
 
@@ -833,8 +874,8 @@ __global__ void __launch_bounds__(128) k_uvadv3d_prep_vec(Dev d, Bc3<float> s, f
   st_row<float, N>(uuadvp + p, fullw, nw, ua);
   st_row<float, N>(vvadvp + p, fullw, nw, va);
   st_row<float, N>(wwadvp + p, fullw, nw, wa);
-  st_row<float, N>(huadvp + p, fullw, nw, ha);
-  st_row<float, N>(hvadvp + p, fullw, nw, hb);
+  if (huadvp) st_row<float, N>(huadvp + p, fullw, nw, ha);
+  if (hvadvp) st_row<float, N>(hvadvp + p, fullw, nw, hb);
 }
 
 // Both momentum grids' quantities in one pass (FP32, 16-byte aligned layouts): the inputs of a
@@ -849,68 +890,87 @@ __global__ void __launch_bounds__(128) k_uvadv3d_prep_vec2(Dev d, Bc3<float> s, 
   const int ni = d.ni(), nj = d.nj();
   const int c0 = (blockIdx.x * blockDim.x + threadIdx.x) * N;
   const int jj = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
   if (c0 >= ni || jj >= nj) return;
-  const long long p = (long long)k * d.sk + (long long)jj * d.sj + c0;
+  // levels k0..k1-1 of the thread's 4 cells (grid z = chunk of LVC levels)
+  const int k0 = max(1, (int)blockIdx.z * LVC), k1 = min((int)blockIdx.z * LVC + LVC, d.kmax + 1);
+  const long long c = (long long)jj * d.sj + c0;  // the 2D index of the first cell
   const int nrow = min(N, ni - c0);
-  if (k == 0) {
+  if (blockIdx.z == 0) {
     const float z[N] = {0.f, 0.f, 0.f, 0.f};
-    st_row<float, N>(u.a[3] + p, nrow == N, nrow, z);
-    return;
+    st_row<float, N>(u.a[3] + c, nrow == N, nrow, z);
   }
   const bool fullr = c0 + N <= ni;
-  auto ld = [&](int f, long long off, float (&x)[N]) { ld_row<float, N>(s.f3[f] + p + off, fullr, ni - c0, x); };
-  float uu[N], vv[N], ww[N], ho[N], hn[N], hun[N], hvn[N];
-  ld(UU, 0, uu); ld(VV, 0, vv); ld(WW, 0, ww); ld(HO, 0, ho); ld(HN, 0, hn); ld(HUN, 0, hun); ld(HVN, 0, hvn);
   const float half = 0.5f;
   const int nwu = min(nrow, ni - 1 - c0);  // U grid: every cell but the last of the row
-  if (nwu > 0) {
-    const bool nb = c0 + N < ni;
-    const long long q = p + N;
-    const float uue = nb ? s.f3[UU][q] : 0.f, vve = nb ? s.f3[VV][q] : 0.f, wwe = nb ? s.f3[WW][q] : 0.f,
-                hoe = nb ? s.f3[HO][q] : 0.f, hne = nb ? s.f3[HN][q] : 0.f, hvne = nb ? s.f3[HVN][q] : 0.f;
-    float fa[N], ua[N], va[N], wa[N], ha[N], hb[N];
+  const bool vrow = jj <= nj - 2;          // V grid: rows but the last
+  const bool nb = c0 + N < ni;
+  // the columns' layer heights (k_sigma's values): ho, hn, hvn at the cells and the i+1 neighbour
+  // (U grid), hun, hvn at the cells and ho, hn, hun of row j+1 (V grid)
+  const double kmaxm1 = 1.0 / (double)(float)d.kmax;
+  const long long sj = d.sj;
+  float ho[N + 1], hn[N + 1], hvn[N + 1], hun[N], ho1[N], hn1[N], hun1[N];
 #pragma unroll
-    for (int m = 0; m < N; ++m) {
-      const float u1 = m + 1 < N ? uu[m + 1] : uue, v1 = m + 1 < N ? vv[m + 1] : vve, w1 = m + 1 < N ? ww[m + 1] : wwe;
-      const float o1 = m + 1 < N ? ho[m + 1] : hoe, n1 = m + 1 < N ? hn[m + 1] : hne,
-                  h1 = m + 1 < N ? hvn[m + 1] : hvne;
-      fa[m] = uu[m] / hun[m];
-      ua[m] = half * (uu[m] + u1);
-      va[m] = half * (vv[m] + v1);
-      wa[m] = half * (ww[m] + w1);
-      ha[m] = half * (o1 + n1);
-      hb[m] = half * (hvn[m] + h1);
+  for (int m = 0; m <= N; ++m) {
+    const long long q = c + (m < nrow ? m : (m == N && nb ? N : 0));
+    ho[m] = sig_h<float>(s, SSEO, HH, q, kmaxm1);
+    hn[m] = sig_h<float>(s, SSEN, HH, q, kmaxm1);
+    hvn[m] = sig_h<float>(s, SSVN, HV, q, kmaxm1);
+    if (m < N) {
+      hun[m] = sig_h<float>(s, SSUN, HU, q, kmaxm1);
+      const long long q1 = vrow ? q + sj : q;
+      ho1[m] = sig_h<float>(s, SSEO, HH, q1, kmaxm1);
+      hn1[m] = sig_h<float>(s, SSEN, HH, q1, kmaxm1);
+      hun1[m] = sig_h<float>(s, SSUN, HU, q1, kmaxm1);
     }
-    const bool fw = nwu == N;
-    st_row<float, N>(u.a[0] + p, fw, nwu, fa);
-    st_row<float, N>(u.a[1] + p, fw, nwu, ua);
-    st_row<float, N>(u.a[2] + p, fw, nwu, va);
-    st_row<float, N>(u.a[3] + p, fw, nwu, wa);
-    st_row<float, N>(u.a[4] + p, fw, nwu, ha);
-    st_row<float, N>(u.a[5] + p, fw, nwu, hb);
   }
-  if (jj <= nj - 2) {  // V grid: rows but the last
-    const long long sj = d.sj;
-    float uu1[N], vv1[N], ww1[N], hun1[N], ho1[N], hn1[N];
-    ld(UU, sj, uu1); ld(VV, sj, vv1); ld(WW, sj, ww1); ld(HUN, sj, hun1); ld(HO, sj, ho1); ld(HN, sj, hn1);
-    float fa[N], ua[N], va[N], wa[N], ha[N], hb[N];
+  for (int k = k0; k < k1; ++k) {
+    const long long p = (long long)k * d.sk + c;
+    auto ld = [&](int f, long long off, float (&x)[N]) { ld_row<float, N>(s.f3[f] + p + off, fullr, ni - c0, x); };
+    float uu[N], vv[N], ww[N];
+    ld(UU, 0, uu); ld(VV, 0, vv); ld(WW, 0, ww);
+    if (nwu > 0) {
+      const long long q = p + N;
+      const float uue = nb ? s.f3[UU][q] : 0.f, vve = nb ? s.f3[VV][q] : 0.f, wwe = nb ? s.f3[WW][q] : 0.f;
+      float fa[N], ua[N], va[N], wa[N], ha[N], hb[N];
 #pragma unroll
-    for (int m = 0; m < N; ++m) {
-      fa[m] = vv[m] / hvn[m];
-      ua[m] = half * (uu[m] + uu1[m]);
-      va[m] = half * (vv[m] + vv1[m]);
-      wa[m] = half * (ww[m] + ww1[m]);
-      ha[m] = half * (hun[m] + hun1[m]);
-      hb[m] = half * (ho1[m] + hn1[m]);
+      for (int m = 0; m < N; ++m) {
+        const float u1 = m + 1 < N ? uu[m + 1] : uue, v1 = m + 1 < N ? vv[m + 1] : vve, w1 = m + 1 < N ? ww[m + 1] : wwe;
+        fa[m] = uu[m] / hun[m];
+        ua[m] = half * (uu[m] + u1);
+        va[m] = half * (vv[m] + v1);
+        wa[m] = half * (ww[m] + w1);
+        ha[m] = half * (ho[m + 1] + hn[m + 1]);
+        hb[m] = half * (hvn[m] + hvn[m + 1]);
+      }
+      const bool fw = nwu == N;
+      st_row<float, N>(u.a[0] + p, fw, nwu, fa);
+      st_row<float, N>(u.a[1] + p, fw, nwu, ua);
+      st_row<float, N>(u.a[2] + p, fw, nwu, va);
+      st_row<float, N>(u.a[3] + p, fw, nwu, wa);
+      if (u.a[4]) st_row<float, N>(u.a[4] + p, fw, nwu, ha);
+      if (u.a[5]) st_row<float, N>(u.a[5] + p, fw, nwu, hb);
     }
-    const bool fw = nrow == N;
-    st_row<float, N>(v.a[0] + p, fw, nrow, fa);
-    st_row<float, N>(v.a[1] + p, fw, nrow, ua);
-    st_row<float, N>(v.a[2] + p, fw, nrow, va);
-    st_row<float, N>(v.a[3] + p, fw, nrow, wa);
-    st_row<float, N>(v.a[4] + p, fw, nrow, ha);
-    st_row<float, N>(v.a[5] + p, fw, nrow, hb);
+    if (vrow) {
+      float uu1[N], vv1[N], ww1[N];
+      ld(UU, sj, uu1); ld(VV, sj, vv1); ld(WW, sj, ww1);
+      float fa[N], ua[N], va[N], wa[N], ha[N], hb[N];
+#pragma unroll
+      for (int m = 0; m < N; ++m) {
+        fa[m] = vv[m] / hvn[m];
+        ua[m] = half * (uu[m] + uu1[m]);
+        va[m] = half * (vv[m] + vv1[m]);
+        wa[m] = half * (ww[m] + ww1[m]);
+        ha[m] = half * (hun[m] + hun1[m]);
+        hb[m] = half * (ho1[m] + hn1[m]);
+      }
+      const bool fw = nrow == N;
+      st_row<float, N>(v.a[0] + p, fw, nrow, fa);
+      st_row<float, N>(v.a[1] + p, fw, nrow, ua);
+      st_row<float, N>(v.a[2] + p, fw, nrow, va);
+      st_row<float, N>(v.a[3] + p, fw, nrow, wa);
+      if (v.a[4]) st_row<float, N>(v.a[4] + p, fw, nrow, ha);
+      if (v.a[5]) st_row<float, N>(v.a[5] + p, fw, nrow, hb);
+    }
   }
 }
 
@@ -1184,6 +1244,13 @@ inline dim3 plane_grid(const Dev& d, dim3 blk, int nz = 1) {
 }
 
 template <class R3>
+int run_col_heights(const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* out) {
+  const dim3 blk(64, 4, 1);
+  k_col_heights<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, out);
+  return (int)cudaGetLastError();
+}
+
+template <class R3>
 int run_bc3(int which, const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* const* scr) {
   const dim3 blk(32, 4, 1);
   switch (which) {
@@ -1243,11 +1310,11 @@ int run_bc3(int which, const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* cons
       if constexpr (sizeof(R3) == 4) {
         bool ok = vector_sweeps_enabled() && d.sj % 4 == 0 && d.sk % 4 == 0;
         for (int q = 0; q < 6 && ok; ++q) ok = reinterpret_cast<uintptr_t>(scr[q]) % 16 == 0;
-        for (int f : {UU, VV, WW, HO, HN, HUN, HVN})
+        for (int f : {UU, VV, WW})
           ok = ok && reinterpret_cast<uintptr_t>(s.f3[f]) % 16 == 0;
         if (ok) {
           const dim3 bv(32, 4, 1);
-          const dim3 gv((d.ni() + 4 * 32 - 1) / (4 * 32), (d.nj() + 3) / 4, d.kmax + 1);
+          const dim3 gv((d.ni() + 4 * 32 - 1) / (4 * 32), (d.nj() + 3) / 4, (d.kmax + LVC) / LVC);
           if (u) k_uvadv3d_prep_vec<0><<<gv, bv, 0, st>>>(d, s, scr[0], scr[1], scr[2], scr[3], scr[4], scr[5]);
           else k_uvadv3d_prep_vec<1><<<gv, bv, 0, st>>>(d, s, scr[0], scr[1], scr[2], scr[3], scr[4], scr[5]);
           break;
@@ -1265,11 +1332,11 @@ int run_bc3(int which, const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* cons
       if constexpr (sizeof(R3) == 4) {
         bool ok = vector_sweeps_enabled() && d.sj % 4 == 0 && d.sk % 4 == 0;
         for (int q : {0, 1, 2, 3, 4, 5, 7, 8, 9, 10, 11, 12}) ok = ok && reinterpret_cast<uintptr_t>(scr[q]) % 16 == 0;
-        for (int f : {UU, VV, WW, HO, HN, HUN, HVN})
+        for (int f : {UU, VV, WW})
           ok = ok && reinterpret_cast<uintptr_t>(s.f3[f]) % 16 == 0;
         if (ok) {
           const dim3 bv(32, 4, 1);
-          const dim3 gv((d.ni() + 4 * 32 - 1) / (4 * 32), (d.nj() + 3) / 4, d.kmax + 1);
+          const dim3 gv((d.ni() + 4 * 32 - 1) / (4 * 32), (d.nj() + 3) / 4, (d.kmax + LVC) / LVC);
           k_uvadv3d_prep_vec2<4><<<gv, bv, 0, st>>>(d, s, Prep6{{scr[0], scr[1], scr[2], scr[3], scr[4], scr[5]}},
                                                     Prep6{{scr[7], scr[8], scr[9], scr[10], scr[11], scr[12]}});
         } else {

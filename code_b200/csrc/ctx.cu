@@ -63,7 +63,7 @@ using namespace gb;
 template <class R>
 int do_adv3d(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, const R* hu,
                     const R* hv, const R* ho, const R* hn, int split, int hs, int vs, R AH, int tag, R* hires,
-                    R* advres, int iters, bool field_out, __half* lo) {
+                    R* advres, int iters, bool field_out, __half* lo, unsigned h2d) {
   (void)hn;
   if (!ctx) return GETM_ERR_ARG;
   if (!ctx->adv_ready) return fail(ctx, GETM_ERR_STATE, "getm_init_advection has not been called");
@@ -93,7 +93,15 @@ int do_adv3d(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, c
   const bool needs_adv = (hs != NOADV && vs != NOADV && (split == GETM_NOSPLIT || split == GETM_HVSPLIT)) ||
                          (hs != NOADV && vs == NOADV && split == GETM_NOSPLIT);
   R* A = advres ? advres : (needs_adv ? (R*)ctx->scr[2] : nullptr);
-  if (A) GB_TRY(cudaMemsetAsync(A, 0, bytes3, s), "memset adv");
+  // p_adv = 0 (advection_3d.F90:296): FULLSPLIT and HALFSPLIT clear level 0 and let their first u
+  // sweep start the sum on levels 1..kmax; the other sequences clear the whole array
+  const bool split_first_u = hs != NOADV && vs != NOADV && kmax >= 1 &&
+                             (split == GETM_FULLSPLIT || split == GETM_HALFSPLIT);
+  // h2d (callers inside the step): bit 0 hu, bit 1 hv, bit 2 ho are 2D arrays of column values
+  // (the layer heights of equidistant sigma coordinates); only the FULLSPLIT and HALFSPLIT sweeps
+  // take them
+  if (h2d && (!split_first_u || hires)) return fail(ctx, GETM_ERR_STATE, "do_advection_3d: 2D heights need a split");
+  if (A) GB_TRY(cudaMemsetAsync(A, 0, split_first_u ? (size_t)sk * sizeof(R) : bytes3, s), "memset adv");
   auto L = [&](auto* p, int k) { return p + (long long)k * sk; };
   const R half = R(0.5), one = R(1);
   unsigned long long* warn = ctx->cnt;
@@ -144,6 +152,10 @@ int do_adv3d(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, c
   // are all increments)
   __half* lw = (lo && field_out) ? lo : nullptr;
   __half* ll = lw ? L(lw, 1) : nullptr;
+  const bool hu2 = h2d & 1u, hv2 = h2d & 2u, ho2 = h2d & 4u;
+  const R* HUl = hu2 ? hu : L(hu, 1);
+  const R* HVl = hv2 ? hv : L(hv, 1);
+  const R* HOl = ho2 ? ho : L(ho, 1);
   switch (split) {
     case GETM_NOSPLIT:
       GB_TIMED(GETM_TIM_COPY, cudaMemcpyAsync(S, f, bytes3, cudaMemcpyDeviceToDevice, s), "copy f");
@@ -155,24 +167,30 @@ int do_adv3d(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, c
       GB_TIMED(GETM_TIM_ADV_FINALISE, run_finalise<R>(d, s, dt, f, ho, A, H, g.mask_finalise), "finalise");
       break;
     case GETM_FULLSPLIT:
-      GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<R, 0>(d, s, nk, dt, one, hs, AH, L(f, 1), L(f, 1), L(S, 1), L(ho, 1), L(H, 1), Al,
-                                L(uu, 1), L(hu, 1), g.mask_uflux, g.mask_uupdate, nullptr, nullptr, nullptr, nullptr, ll)), "u");
+      GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<R, 0>(d, s, nk, dt, one, hs, AH, L(f, 1), L(f, 1), L(S, 1), HOl, L(H, 1), Al,
+                                L(uu, 1), HUl, g.mask_uflux, g.mask_uupdate, nullptr, nullptr, nullptr, nullptr, ll,
+                                nullptr, true, hu2, ho2)), "u");
       GB_TIMED(GETM_TIM_ADV_V, (run_sweep_h<R, 1>(d, s, nk, dt, one, hs, AH, L(S, 1), L(S, 1), L(f, 1), L(H, 1), L(H, 1), Al,
-                                L(vv, 1), L(hv, 1), g.mask_vflux, g.mask_vupdate, nullptr, nullptr, nullptr, nullptr, ll)), "v");
+                                L(vv, 1), HVl, g.mask_vflux, g.mask_vupdate, nullptr, nullptr, nullptr, nullptr, ll,
+                                nullptr, false, hv2)), "v");
       if (kmax > 1) GB_TIMED(GETM_TIM_ADV_W, run_sweep_w<R>(d, s, dt, one, vs, kshift, iters, f, f, f, H, A, ww, g.az, warn, nullptr, lw), "w");
       break;
     case GETM_HALFSPLIT:
-      GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<R, 0>(d, s, nk, dt, half, hs, AH, L(f, 1), L(f, 1), L(S, 1), L(ho, 1), L(H, 1), Al,
-                                L(uu, 1), L(hu, 1), g.mask_uflux, g.mask_uupdate, nullptr, nullptr, nullptr, nullptr, ll)), "u1");
+      GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<R, 0>(d, s, nk, dt, half, hs, AH, L(f, 1), L(f, 1), L(S, 1), HOl, L(H, 1), Al,
+                                L(uu, 1), HUl, g.mask_uflux, g.mask_uupdate, nullptr, nullptr, nullptr, nullptr, ll,
+                                nullptr, true, hu2, ho2)), "u1");
       GB_TIMED(GETM_TIM_ADV_V, (run_sweep_h<R, 1>(d, s, nk, dt, half, hs, AH, L(S, 1), L(S, 1), L(f, 1), L(H, 1), L(H, 1), Al,
-                                L(vv, 1), L(hv, 1), g.mask_vflux, g.mask_vupdate, nullptr, nullptr, nullptr, nullptr, ll)), "v1");
+                                L(vv, 1), HVl, g.mask_vflux, g.mask_vupdate, nullptr, nullptr, nullptr, nullptr, ll,
+                                nullptr, false, hv2)), "v1");
       if (kmax > 1) GB_TIMED(GETM_TIM_ADV_W, run_sweep_w<R>(d, s, dt, one, vs, kshift, iters, f, f, f, H, A, ww, g.az, warn, nullptr, lw), "w");
       GB_TIMED(GETM_TIM_ADV_V, (run_sweep_h<R, 1>(d, s, nk, dt, half, hs, AH, L(f, 1), L(f, 1), L(S, 1), L(H, 1), L(H, 1), Al,
-                                L(vv, 1), L(hv, 1), g.mask_vflux, g.mask_vupdate, nullptr, nullptr, nullptr, nullptr, ll)), "v2");
+                                L(vv, 1), HVl, g.mask_vflux, g.mask_vupdate, nullptr, nullptr, nullptr, nullptr, ll,
+                                nullptr, false, hv2)), "v2");
       // the last sweep writes the field and heights only when the caller keeps them
       GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<R, 0>(d, s, nk, dt, half, hs, AH, L(S, 1), L(S, 1),
                                 field_out ? L(f, 1) : nullptr, L(H, 1), (field_out || hires) ? L(H, 1) : nullptr,
-                                Al, L(uu, 1), L(hu, 1), g.mask_uflux, g.mask_uupdate, nullptr, nullptr, nullptr, nullptr, ll)), "u2");
+                                Al, L(uu, 1), HUl, g.mask_uflux, g.mask_uupdate, nullptr, nullptr, nullptr, nullptr, ll,
+                                nullptr, false, hu2)), "u2");
       break;
     case GETM_HVSPLIT:
       GB_TIMED(GETM_TIM_COPY, cudaMemcpyAsync(S, f, bytes3, cudaMemcpyDeviceToDevice, s), "copy f");
@@ -193,7 +211,7 @@ int do_adv3d(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, c
 // same sweeps as do_adv3d's HALFSPLIT branch for each field, with the heights hi evolved once.
 template <class R>
 int do_adv3d_pair(getm_ctx* ctx, R dt, R* fa, R* fb, const R* uu, const R* vv, const R* ww, const R* hu,
-                  const R* hv, const R* ho, int hs, int vs, R AH, __half* lo_a, __half* lo_b) {
+                  const R* hv, const R* ho, int hs, int vs, R AH, __half* lo_a, __half* lo_b, unsigned h2d) {
   getm_adv_grid g;
   grid_for_tag(ctx, GETM_H_TAG, &g);
   const Dev& d = ctx->dev;
@@ -210,33 +228,38 @@ int do_adv3d_pair(getm_ctx* ctx, R dt, R* fa, R* fb, const R* uu, const R* vv, c
   const int nk = kmax;
   __half* la = L(lo_a, 1);
   __half* lb = L(lo_b, 1);
-  GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<R, 0>(d, s, nk, dt, half, hs, AH, L(fa, 1), L(fa, 1), L(Sa, 1), L(ho, 1),
-                            L(H, 1), nullptr, L(uu, 1), L(hu, 1), g.mask_uflux, g.mask_uupdate, nullptr, L(fb, 1),
-                            L(fb, 1), L(Sb, 1), la, lb)), "u1");
+  // h2d as in do_adv3d: hu, hv, ho as 2D arrays of column values
+  const bool hu2 = h2d & 1u, hv2 = h2d & 2u, ho2 = h2d & 4u;
+  const R* HUl = hu2 ? hu : L(hu, 1);
+  const R* HVl = hv2 ? hv : L(hv, 1);
+  const R* HOl = ho2 ? ho : L(ho, 1);
+  GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<R, 0>(d, s, nk, dt, half, hs, AH, L(fa, 1), L(fa, 1), L(Sa, 1), HOl,
+                            L(H, 1), nullptr, L(uu, 1), HUl, g.mask_uflux, g.mask_uupdate, nullptr, L(fb, 1),
+                            L(fb, 1), L(Sb, 1), la, lb, false, hu2, ho2)), "u1");
   GB_TIMED(GETM_TIM_ADV_V, (run_sweep_h<R, 1>(d, s, nk, dt, half, hs, AH, L(Sa, 1), L(Sa, 1), L(fa, 1), L(H, 1),
-                            L(H, 1), nullptr, L(vv, 1), L(hv, 1), g.mask_vflux, g.mask_vupdate, nullptr, L(Sb, 1),
-                            L(Sb, 1), L(fb, 1), la, lb)), "v1");
+                            L(H, 1), nullptr, L(vv, 1), HVl, g.mask_vflux, g.mask_vupdate, nullptr, L(Sb, 1),
+                            L(Sb, 1), L(fb, 1), la, lb, false, hv2)), "v1");
   if (kmax > 1 && vs != NOADV)
     GB_TIMED(GETM_TIM_ADV_W, run_sweep_w2<R>(d, s, dt, one, vs, fa, fb, H, ww, g.az, lo_a, lo_b), "w");
   GB_TIMED(GETM_TIM_ADV_V, (run_sweep_h<R, 1>(d, s, nk, dt, half, hs, AH, L(fa, 1), L(fa, 1), L(Sa, 1), L(H, 1),
-                            L(H, 1), nullptr, L(vv, 1), L(hv, 1), g.mask_vflux, g.mask_vupdate, nullptr, L(fb, 1),
-                            L(fb, 1), L(Sb, 1), la, lb)), "v2");
+                            L(H, 1), nullptr, L(vv, 1), HVl, g.mask_vflux, g.mask_vupdate, nullptr, L(fb, 1),
+                            L(fb, 1), L(Sb, 1), la, lb, false, hv2)), "v2");
   GB_TIMED(GETM_TIM_ADV_U, (run_sweep_h<R, 0>(d, s, nk, dt, half, hs, AH, L(Sa, 1), L(Sa, 1), L(fa, 1), L(H, 1),
-                            L(H, 1), nullptr, L(uu, 1), L(hu, 1), g.mask_uflux, g.mask_uupdate, nullptr, L(Sb, 1),
-                            L(Sb, 1), L(fb, 1), la, lb)), "u2");
+                            L(H, 1), nullptr, L(uu, 1), HUl, g.mask_uflux, g.mask_uupdate, nullptr, L(Sb, 1),
+                            L(Sb, 1), L(fb, 1), la, lb, false, hu2)), "u2");
   return GETM_OK;
 }
 template int do_adv3d_pair<double>(getm_ctx*, double, double*, double*, const double*, const double*, const double*,
-                                   const double*, const double*, const double*, int, int, double, __half*, __half*);
+                                   const double*, const double*, const double*, int, int, double, __half*, __half*, unsigned);
 template int do_adv3d_pair<float>(getm_ctx*, float, float*, float*, const float*, const float*, const float*,
-                                  const float*, const float*, const float*, int, int, float, __half*, __half*);
+                                  const float*, const float*, const float*, int, int, float, __half*, __half*, unsigned);
 
 template int do_adv3d<double>(getm_ctx*, double, double*, const double*, const double*, const double*,
                                const double*, const double*, const double*, const double*, int, int, int, double,
-                               int, double*, double*, int, bool, __half*);
+                               int, double*, double*, int, bool, __half*, unsigned);
 template int do_adv3d<float>(getm_ctx*, float, float*, const float*, const float*, const float*, const float*,
                              const float*, const float*, const float*, int, int, int, float, int, float*, float*,
-                             int, bool, __half*);
+                             int, bool, __half*, unsigned);
 
 template <class R>
 static int sweep_h_api(getm_ctx* ctx, int dir, int nk, R dt, const R* f, R* fi, R* Di, R* adv, const R* U,
@@ -397,6 +420,7 @@ int getm_ctx_destroy(getm_ctx* ctx) {
   for (auto p : ctx->scr) cudaFree(p);
   cudaFree(ctx->bc_scr3);
   cudaFree(ctx->bc_scr2);
+  cudaFree(ctx->colh);
   cudaFree(ctx->w2);
   cudaFree(ctx->adj_scr);
   cudaFree(ctx->adj_store);

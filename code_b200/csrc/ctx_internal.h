@@ -48,6 +48,9 @@ struct getm_ctx {
   void* bc_scr3 = nullptr;
   size_t bc_scr3_bytes = 0;
   double* bc_scr2 = nullptr;
+  // the macro step's column heights (NCOLH 2D arrays of the 3D fields' type, run_col_heights),
+  // read by the advection and diffusion launches after sigma_coordinates in place of the 3D heights
+  void* colh = nullptr;
   // FP32 working copies of the 2D fields of the mixed-precision micro step (NF2 slots of n2d
   // floats; only the is_work2 fields are used)
   float* w2 = nullptr;
@@ -166,16 +169,18 @@ static inline bool grid_for_tag(const getm_ctx* ctx, int tag, getm_adv_grid* g) 
 
 
 // do_advection_3d (advection_3d.F90:120-598) on device pointers; defined in ctx.cu. lo: the
-// tracer's compensated storage (FP32, FULLSPLIT / HALFSPLIT; null = none).
+// tracer's compensated storage (FP32, FULLSPLIT / HALFSPLIT; null = none). h2d: bit 0 hu, bit 1 hv,
+// bit 2 ho are 2D arrays of values shared by every level of a column (FULLSPLIT / HALFSPLIT only).
 template <class R>
 int do_adv3d(getm_ctx* ctx, R dt, R* f, const R* uu, const R* vv, const R* ww, const R* hu, const R* hv,
              const R* ho, const R* hn, int split, int hs, int vs, R AH, int tag, R* hires, R* advres, int iters,
-             bool field_out = true, __half* lo = nullptr);
+             bool field_out = true, __half* lo = nullptr, unsigned h2d = 0);
 // Two tracers advected together with HALFSPLIT on the H grid (ctx.cu); the caller has checked that
 // hs is a split scheme, vs a split scheme or NOADV, and adv_ver_iterations = 1.
 template <class R>
 int do_adv3d_pair(getm_ctx* ctx, R dt, R* fa, R* fb, const R* uu, const R* vv, const R* ww, const R* hu,
-                  const R* hv, const R* ho, int hs, int vs, R AH, __half* lo_a = nullptr, __half* lo_b = nullptr);
+                  const R* hv, const R* ho, int hs, int vs, R AH, __half* lo_a = nullptr, __half* lo_b = nullptr,
+                  unsigned h2d = 0);
 
 // Tracer step: do_advection_3d(H_TAG) then the implicit vertical diffusion (ctx.cu).
 template <class R>

@@ -302,7 +302,12 @@ constexpr int NKB = 8;              // levels per block (the 2D masks are staged
 template <class R>
 struct SweepC {
   R dt, splitfac, AH, dti, dxf, dyf, ard1, cdx;
-  R cdy, cadv;  // FP32 cell update: dti*dyf*ard1 and splitfac*dyf*ard1
+  R cdy, cadv;   // FP32 cell update: dti*dyf*ard1 and splitfac*dyf*ard1
+  int adv_init;  // vectorised u sweep: start the flux-divergence sum adv instead of adding to it
+  // level strides of the face depths (DU / DV) and of the heights read (Di_src): the 3D level
+  // stride, or 0 for a 2D array of values that every level of a column shares (the layer heights
+  // of equidistant sigma coordinates)
+  long long skdu, skdi;
 };
 
 template <class R>
@@ -318,6 +323,8 @@ inline SweepC<R> sweep_consts(const Dev& d, int dir, R dt, R splitfac, R AH) {
   c.cdx = c.dti / c.dxf;
   c.cdy = c.dti * c.dyf * c.ard1;
   c.cadv = splitfac * c.dyf * c.ard1;
+  c.adv_init = 0;
+  c.skdu = c.skdi = d.sk;
   return c;
 }
 
@@ -407,7 +414,7 @@ __global__ void __launch_bounds__(TU, sizeof(R) == 4 ? 16 : 8) k_sweep_u_tile(De
   auto stage = [&](int k, int b) {
     const long long row = crow + (long long)k * d.sk;
     const R* Ur = U + row;
-    const R* DUr = DU + row;
+    const R* DUr = DU + crow + (long long)k * C.skdu;
     if (inner) {
 #pragma unroll
       for (int n = 0; n < NF; ++n) {
@@ -437,7 +444,7 @@ __global__ void __launch_bounds__(TU, sizeof(R) == 4 ? 16 : 8) k_sweep_u_tile(De
       }
     }
     if (own) {
-      cp_async(&sD[b][t], Di_src + row + ii);
+      cp_async(&sD[b][t], Di_src + crow + (long long)k * C.skdi + ii);
 #pragma unroll
       for (int n = 0; n < NF; ++n)
         if (F.t[n].fi_src != F.t[n].f) cp_async(&sfi[b][n][t], F.t[n].fi_src + row + ii);
@@ -550,7 +557,7 @@ __global__ void __launch_bounds__(TVX * TVY, sizeof(R) == 4 ? (NF == 1 ? 8 : 6) 
         if (ty < 4) cp_async(&sf[b][n][TVY + ty][tx], fc + (long long)(TVY + ty) * sj);
       }
       const R* Vc = V + b0 + sj;  // row jj0-1
-      const R* DVc = DV + b0 + sj;
+      const R* DVc = DV + (b0 - lev + (long long)k * C.skdu) + sj;
       cp_async(&sV[b][ty][tx], Vc + (long long)ty * sj);
       cp_async(&sDV[b][ty][tx], DVc + (long long)ty * sj);
       if (ty == 0) {
@@ -570,7 +577,7 @@ __global__ void __launch_bounds__(TVX * TVY, sizeof(R) == 4 ? (NF == 1 ? 8 : 6) 
         if (iok && j2 >= 0 && j2 < nj) {
           const long long c2 = lev + (long long)j2 * sj + ii;
           cp_async(&sV[b][q][tx], V + c2);
-          cp_async(&sDV[b][q][tx], DV + c2);
+          cp_async(&sDV[b][q][tx], DV + (c2 - lev + (long long)k * C.skdu));
         } else {
           sV[b][q][tx] = R(0);
           sDV[b][q][tx] = R(0);
@@ -578,7 +585,7 @@ __global__ void __launch_bounds__(TVX * TVY, sizeof(R) == 4 ? (NF == 1 ? 8 : 6) 
       }
     }
     if (own) {
-      cp_async(&sD[b][ty][tx], Di_src + lev + c);
+      cp_async(&sD[b][ty][tx], Di_src + (long long)k * C.skdi + c);
 #pragma unroll
       for (int n = 0; n < NF; ++n)
         if (F.t[n].fi_src != F.t[n].f) cp_async(&sfi[b][n][ty][tx], F.t[n].fi_src + lev + c);
@@ -905,16 +912,37 @@ struct ThomasSmem {
   __device__ R& QU(int k) { return qu[k * nt + threadIdx.x]; }
 };
 
-// Implicit vertical diffusion (salinity.F90:348-389; temperature form with src). One thread per
-// interior column; the matrix rows are built top-down as the elimination proceeds, ru(k+1)/qu(k+1)
-// carried in registers and ru(k)/qu(k) stored in two scratch 3D arrays (full occupancy, no shared
-// memory for them: holding them in shared memory measured 1.6x slower at kmax = 50, from the lower
-// occupancy) for the back substitution.
+// One tracer of the implicit vertical diffusion: the old values are read from Sin and the new ones
+// written to S (they may alias) and, when S2 is given, to S2 as well; src (may be null): the
+// temperature form's sources; RU, QU: two scratch 3D arrays; lo: the compensated storage (FP32).
 template <class R>
-__global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, const R* Sin, R* S,
-                                               const R* __restrict__ hn, const R* __restrict__ nuh,
-                                               const int32_t* __restrict__ az, const R* __restrict__ src, R* RUs,
-                                               R* QUs, R* S2, __half* lo) {
+struct VdField {
+  const R* Sin;
+  R* S;
+  const R* src;
+  R* RU;
+  R* QU;
+  R* S2;
+  __half* lo;
+  R avmol;
+};
+template <class R, int NF>
+struct VdSet {
+  VdField<R> t[NF];
+};
+
+// Implicit vertical diffusion (salinity.F90:348-389; temperature form with src) of NF = 1 or 2
+// tracers (do_temperature and do_salinity share hn and nuh). One thread per interior column; the
+// matrix rows are built top-down as the elimination proceeds, ru(k+1)/qu(k+1) carried in registers
+// and ru(k)/qu(k) stored in two scratch 3D arrays per tracer (full occupancy, no shared memory for
+// them: holding them in shared memory measured 1.6x slower at kmax = 50, from the lower occupancy)
+// for the back substitution. With two tracers the thread runs their two eliminations side by side
+// (independent chains) and loads hn and nuh once.
+// hsk: the level stride of hn (d.sk; 0 when hn is a 2D array of column heights)
+template <class R, int NF>
+__global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, VdSet<R, NF> F, const R* __restrict__ hn,
+                                               const R* __restrict__ nuh, const int32_t* __restrict__ az,
+                                               long long hsk) {
   const int kmax = d.kmax;
   const int i = d.imin + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = d.jmin + blockIdx.y * blockDim.y + threadIdx.y;
@@ -922,25 +950,22 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, co
   const long long c = d.ix(i, j);
   if (az[c] != 1 || kmax <= 1) return;
   const long long sk = d.sk;
-  auto L = [&](const R* a, int k) -> R { return a[c + k * sk]; };
-  // the old tracer is read from Sin and the new one written to S (they may alias) and, when S2 is
-  // given, also to S2
-  auto put = [&](int k, R v) {
-    S[c + k * sk] = v;
-    if (S2) S2[c + k * sk] = v;
-  };
   // the new value of level k from the old one and the increment: a plain FP32 sum, or the
   // compensated sum of the carried error lo (the tracer's compensated storage)
-  auto new_level = [&](int k, R sold, R inc) -> R {
+  auto new_level = [&](const VdField<R>& f, int k, R sold, R inc) -> R {
     if constexpr (sizeof(R) == 4) {
-      if (lo) {
-        float slo = __half2float(lo[c + k * sk]);
+      if (f.lo) {
+        float slo = __half2float(f.lo[c + k * sk]);
         const float v = add_comp_scaled(sold, inc, slo);
-        lo[c + k * sk] = __float2half_rn(slo);
+        f.lo[c + k * sk] = __float2half_rn(slo);
         return v;
       }
     }
     return sold + inc;
+  };
+  auto put = [&](const VdField<R>& f, int k, R v) {
+    f.S[c + k * sk] = v;
+    if (f.S2) f.S2[c + k * sk] = v;
   };
   const R co = R(2) * (R(1) - cnpar) * dt;
   const R cn = R(2) * cnpar * dt;
@@ -949,24 +974,22 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, co
   // (ao+an)(k)*(S(k+1)-S(k)) - (ao+an)(k-1)*(S(k)-S(k-1)) [+ src]; the rounding then acts on the
   // small increment rather than on h*S (bias-free over hundreds of steps).
   constexpr bool incr = sizeof(R) == 4;
-  // The inputs of a level (hn, nuh, the old tracer, src) are staged by cp.async into the thread's
-  // own shared-memory slots, a ring of four levels with three in flight ahead of the elimination
-  // (a serial chain per column), so the chain does not wait on their loads.
-  __shared__ R sl[4][4][128];
+  // The inputs of a level (hn, nuh, then per tracer the old value and src) are staged by cp.async
+  // into the thread's own shared-memory slots, a ring of four levels with three in flight ahead
+  // of the elimination (a serial chain per column), so the chain does not wait on their loads.
+  constexpr int NQ = 2 + 2 * NF;
+  __shared__ R sl[4][NQ][128];
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-  auto set_rq = [&](int k, R r, R q) {
-    RUs[c + k * sk] = r;
-    QUs[c + k * sk] = q;
-  };
-  auto ru_of = [&](int k) -> R { return RUs[c + k * sk]; };
-  auto qu_of = [&](int k) -> R { return QUs[c + k * sk]; };
   auto issue = [&](int lv) {
     if (lv >= 1) {
       R(*q)[128] = sl[lv & 3];
-      cp_async(&q[0][tid], hn + c + lv * sk);
+      cp_async(&q[0][tid], hn + c + lv * hsk);
       cp_async(&q[1][tid], nuh + c + lv * sk);
-      cp_async(&q[2][tid], Sin + c + lv * sk);
-      if (src) cp_async(&q[3][tid], src + c + lv * sk);
+#pragma unroll
+      for (int n = 0; n < NF; ++n) {
+        cp_async(&q[2 + 2 * n][tid], F.t[n].Sin + c + lv * sk);
+        if (F.t[n].src) cp_async(&q[3 + 2 * n][tid], F.t[n].src + c + lv * sk);
+      }
     }
     cp_async_commit();
   };
@@ -979,77 +1002,102 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, R avmol, co
   // surface row k = kmax: au = a1, bu = a2, du = a4
   int k = kmax;
   R hnk = get(k, 0), hnkm1 = get(k - 1, 0);
-  R nu = get(k - 1, 1) + avmol;
-  R Sk = get(k, 2), Skm1 = get(k - 1, 2);
-  R srck = src ? get(k, 3) : R(0);
-  R src_n = src ? get(k - 1, 3) : R(0);  // the source of the next row
-  R ao_km1 = co * nu / (hnk + hnkm1), an_km1 = cn * nu / (hnk + hnkm1);
-  R ru, qu;
-  {
-    const R a1 = -an_km1;
-    const R a2 = hnk + an_km1;
-    R a4 = incr ? -(ao_km1 + an_km1) * (Sk - Skm1) : Sk * (hnk - ao_km1) + Skm1 * ao_km1;
-    if (src) a4 = a4 + srck;
-    ru = a1 / a2;
-    qu = a4 / a2;
-    set_rq(k, ru, qu);
+  R nuk = get(k - 1, 1);
+  R Sk[NF], Skm1[NF], src_n[NF], ao_km1[NF], an_km1[NF], ru[NF], qu[NF];
+#pragma unroll
+  for (int n = 0; n < NF; ++n) {
+    const VdField<R>& f = F.t[n];
+    const R nu = nuk + f.avmol;
+    Sk[n] = get(k, 2 + 2 * n);
+    Skm1[n] = get(k - 1, 2 + 2 * n);
+    const R srck = f.src ? get(k, 3 + 2 * n) : R(0);
+    src_n[n] = f.src ? get(k - 1, 3 + 2 * n) : R(0);  // the source of the next row
+    ao_km1[n] = co * nu / (hnk + hnkm1);
+    an_km1[n] = cn * nu / (hnk + hnkm1);
+    const R a1 = -an_km1[n];
+    const R a2 = hnk + an_km1[n];
+    R a4 = incr ? -(ao_km1[n] + an_km1[n]) * (Sk[n] - Skm1[n]) : Sk[n] * (hnk - ao_km1[n]) + Skm1[n] * ao_km1[n];
+    if (f.src) a4 = a4 + srck;
+    ru[n] = a1 / a2;
+    qu[n] = a4 / a2;
+    f.RU[c + k * sk] = ru[n];
+    f.QU[c + k * sk] = qu[n];
   }
   // inner rows k = kmax-1 .. 2
   for (k = kmax - 1; k >= 2; --k) {
     issue(k - 3);        // into the slot of level k+1, whose values were read in the row above
     cp_async_wait<2>();  // level k-1
-    const R ao_k = ao_km1, an_k = an_km1;  // aux at interface k (computed as k-1 of row k+1)
     hnk = hnkm1;
     hnkm1 = get(k - 1, 0);
-    nu = get(k - 1, 1) + avmol;
-    const R Skp1 = Sk;
-    Sk = Skm1;
-    Skm1 = get(k - 1, 2);
-    const R srcv = src_n;
-    if (src) src_n = get(k - 1, 3);
-    ao_km1 = co * nu / (hnk + hnkm1);
-    an_km1 = cn * nu / (hnk + hnkm1);
-    const R a3 = -an_k;
-    const R a1 = -an_km1;
-    const R a2 = hnk + an_k + an_km1;
-    R a4 = incr ? (ao_k + an_k) * (Skp1 - Sk) - (ao_km1 + an_km1) * (Sk - Skm1)
-                : Skp1 * ao_k + Sk * (hnk - ao_k - ao_km1) + Skm1 * ao_km1;
-    if (src) a4 = a4 + srcv;
-    const R den = a2 - a3 * ru;
-    ru = a1 / den;
-    qu = (a4 - a3 * qu) / den;
-    set_rq(k, ru, qu);
+    nuk = get(k - 1, 1);
+#pragma unroll
+    for (int n = 0; n < NF; ++n) {
+      const VdField<R>& f = F.t[n];
+      const R ao_k = ao_km1[n], an_k = an_km1[n];  // aux at interface k (computed as k-1 of row k+1)
+      const R nu = nuk + f.avmol;
+      const R Skp1 = Sk[n];
+      Sk[n] = Skm1[n];
+      Skm1[n] = get(k - 1, 2 + 2 * n);
+      const R srcv = src_n[n];
+      if (f.src) src_n[n] = get(k - 1, 3 + 2 * n);
+      ao_km1[n] = co * nu / (hnk + hnkm1);
+      an_km1[n] = cn * nu / (hnk + hnkm1);
+      const R a3 = -an_k;
+      const R a1 = -an_km1[n];
+      const R a2 = hnk + an_k + an_km1[n];
+      R a4 = incr ? (ao_k + an_k) * (Skp1 - Sk[n]) - (ao_km1[n] + an_km1[n]) * (Sk[n] - Skm1[n])
+                  : Skp1 * ao_k + Sk[n] * (hnk - ao_k - ao_km1[n]) + Skm1[n] * ao_km1[n];
+      if (f.src) a4 = a4 + srcv;
+      const R den = a2 - a3 * ru[n];
+      ru[n] = a1 / den;
+      qu[n] = (a4 - a3 * qu[n]) / den;
+      f.RU[c + k * sk] = ru[n];
+      f.QU[c + k * sk] = qu[n];
+    }
   }
   cp_async_wait<0>();
   // bottom row k = 1 (fi): only qu
-  R v;
-  {
-    const R ao_k = ao_km1, an_k = an_km1;
-    const R Skp1 = Sk;  // S(2)
-    const R S1 = Skm1;  // S(1)
+  R v[NF];
+#pragma unroll
+  for (int n = 0; n < NF; ++n) {
+    const VdField<R>& f = F.t[n];
+    const R ao_k = ao_km1[n], an_k = an_km1[n];
+    const R Skp1 = Sk[n];  // S(2)
+    const R S1 = Skm1[n];  // S(1)
     const R h1 = hnkm1;
     const R a3 = -an_k;
     const R a2 = h1 + an_k;
     R a4 = incr ? (ao_k + an_k) * (Skp1 - S1) : Skp1 * ao_k + S1 * (h1 - ao_k);
-    if (src) a4 = a4 + src_n;  // src(1)
-    v = (a4 - a3 * qu) / (a2 - a3 * ru);
-    put(1, incr ? new_level(1, S1, v) : v);
+    if (f.src) a4 = a4 + src_n[n];  // src(1)
+    v[n] = (a4 - a3 * qu[n]) / (a2 - a3 * ru[n]);
+    put(f, 1, incr ? new_level(f, 1, S1, v[n]) : v[n]);
   }
   // back substitution upwards, with the next level's coefficients loaded one step ahead
-  R qn = kmax >= 2 ? qu_of(2) : R(0), rn = kmax >= 2 ? ru_of(2) : R(0);
-  R sn = (incr && kmax >= 2) ? L(Sin, 2) : R(0);
-  R qn2 = kmax >= 3 ? qu_of(3) : R(0), rn2 = kmax >= 3 ? ru_of(3) : R(0);
-  R sn2 = (incr && kmax >= 3) ? L(Sin, 3) : R(0);
+  R qn[NF], rn[NF], sn[NF], qn2[NF], rn2[NF], sn2[NF];
+#pragma unroll
+  for (int n = 0; n < NF; ++n) {
+    const VdField<R>& f = F.t[n];
+    qn[n] = kmax >= 2 ? f.QU[c + 2 * sk] : R(0);
+    rn[n] = kmax >= 2 ? f.RU[c + 2 * sk] : R(0);
+    sn[n] = (incr && kmax >= 2) ? f.Sin[c + 2 * sk] : R(0);
+    qn2[n] = kmax >= 3 ? f.QU[c + 3 * sk] : R(0);
+    rn2[n] = kmax >= 3 ? f.RU[c + 3 * sk] : R(0);
+    sn2[n] = (incr && kmax >= 3) ? f.Sin[c + 3 * sk] : R(0);
+  }
   for (k = 2; k <= kmax; ++k) {
-    const R q = qn, r = rn, so = sn;
-    qn = qn2; rn = rn2; sn = sn2;
-    if (k + 2 <= kmax) {
-      qn2 = qu_of(k + 2);
-      rn2 = ru_of(k + 2);
-      if (incr) sn2 = L(Sin, k + 2);
+#pragma unroll
+    for (int n = 0; n < NF; ++n) {
+      const VdField<R>& f = F.t[n];
+      const R q = qn[n], r = rn[n], so = sn[n];
+      qn[n] = qn2[n]; rn[n] = rn2[n]; sn[n] = sn2[n];
+      if (k + 2 <= kmax) {
+        qn2[n] = f.QU[c + (k + 2) * sk];
+        rn2[n] = f.RU[c + (k + 2) * sk];
+        if (incr) sn2[n] = f.Sin[c + (k + 2) * sk];
+      }
+      v[n] = q - r * v[n];
+      put(f, k, incr ? new_level(f, k, so, v[n]) : v[n]);
     }
-    v = q - r * v;
-    put(k, incr ? new_level(k, so, v) : v);
   }
 }
 

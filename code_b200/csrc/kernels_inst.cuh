@@ -46,10 +46,12 @@ template <class R, int DIR>
 int run_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int scheme, R AH, const R* f,
                 const R* fi_src, R* fi_dst, const R* Di_src, R* Di_dst, R* adv, const R* U, const R* DU,
                 const uint8_t* mflux, const uint8_t* mupd, uint8_t* code, const R* f_b, const R* fi_src_b,
-                R* fi_dst_b, __half* lo, __half* lo_b) {
+                R* fi_dst_b, __half* lo, __half* lo_b, bool adv_init, bool du2d, bool di2d) {
   if (nk <= 0) return 0;
   if (f_b && (code || adv)) return (int)cudaErrorInvalidValue;
-  const SweepC<R> C = sweep_consts<R>(d, DIR, dt, splitfac, AH);
+  SweepC<R> C = sweep_consts<R>(d, DIR, dt, splitfac, AH);
+  if (du2d) C.skdu = 0;
+  if (di2d) C.skdi = 0;
   const int nz = (nk + NKB - 1) / NKB;
   return dispatch_scheme(scheme, [&](auto sc) {
     constexpr int S = decltype(sc)::value;
@@ -63,13 +65,21 @@ int run_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int sche
                                      {set.t[0].f, set.t[0].fi_src, set.t[0].fi_dst, set.t[NF - 1].f,
                                       set.t[NF - 1].fi_src, set.t[NF - 1].fi_dst, Di_src, Di_dst, adv, U, DU},
                                      {mflux, mupd, code}, {set.t[0].lo, set.t[NF - 1].lo});
+      // adv_init: the vectorised u sweep starts the sum itself; every other kernel adds to a
+      // cleared one
+      if (adv_init && adv && !(sizeof(R) == 4 && vec && DIR == 0)) {
+        const cudaError_t e = cudaMemsetAsync(adv, 0, (size_t)nk * d.sk * sizeof(R), s);
+        if (e != cudaSuccess) return (int)e;
+      }
       if constexpr (sizeof(R) == 4) {
         constexpr int N = 16 / sizeof(R);
         if (vec && DIR == 0) {
           const int nseg = (d.ni() + UOWN * N - 1) / (UOWN * N);
           dim3 blk(32, UWB, 1);
           dim3 grd((nseg + UWB - 1) / UWB, d.nj(), nz);
-          k_sweep_u_vec<R, S, REC, NF><<<grd, blk, 0, s>>>(d, C, nk, set, Di_src, Di_dst, adv, U, DU, mflux,
+          SweepC<R> Cu = C;
+          Cu.adv_init = adv_init && adv ? 1 : 0;
+          k_sweep_u_vec<R, S, REC, NF><<<grd, blk, 0, s>>>(d, Cu, nk, set, Di_src, Di_dst, adv, U, DU, mflux,
                                                            mupd, code);
           return (int)cudaGetLastError();
         }
@@ -186,7 +196,23 @@ int run_vdiff(const Dev& d, cudaStream_t s, R dt, R cnpar, R avmol, R* S, const 
   const int nx = d.imax - d.imin + 1, ny = d.jmax - d.jmin + 1;
   dim3 blk(32, 4, 1);
   dim3 grd((nx + 31) / 32, (ny + 3) / 4, 1);
-  k_vdiff<R><<<grd, blk, 0, s>>>(d, dt, cnpar, avmol, Sin ? Sin : S, S, hn, nuh, az, src, rus, qus, S2, lo);
+  VdSet<R, 1> F{{{Sin ? Sin : S, S, src, rus, qus, S2, lo, avmol}}};
+  k_vdiff<R, 1><<<grd, blk, 0, s>>>(d, dt, cnpar, F, hn, nuh, az, d.sk);
+  return (int)cudaGetLastError();
+}
+
+template <class R>
+int run_vdiff2(const Dev& d, cudaStream_t s, R dt, R cnpar, const R* hn, const R* nuh, const int32_t* az,
+               R* Sa, R avmol_a, const R* src_a, R* rus_a, R* qus_a, __half* lo_a, R* Sb, R avmol_b, R* rus_b,
+               R* qus_b, __half* lo_b, bool hn2d) {
+  if (d.kmax <= 1) return 0;
+  if (sizeof(R) == 8) lo_a = lo_b = nullptr;
+  const int nx = d.imax - d.imin + 1, ny = d.jmax - d.jmin + 1;
+  dim3 blk(32, 4, 1);
+  dim3 grd((nx + 31) / 32, (ny + 3) / 4, 1);
+  VdSet<R, 2> F{{{Sa, Sa, src_a, rus_a, qus_a, nullptr, lo_a, avmol_a},
+                 {Sb, Sb, nullptr, rus_b, qus_b, nullptr, lo_b, avmol_b}}};
+  k_vdiff<R, 2><<<grd, blk, 0, s>>>(d, dt, cnpar, F, hn, nuh, az, hn2d ? 0LL : d.sk);
   return (int)cudaGetLastError();
 }
 
@@ -226,11 +252,13 @@ int run_check_range(const Dev& d, cudaStream_t s, const R* f, const int32_t* az,
 template int run_sweep_h<GB_REAL, 0>(const Dev&, cudaStream_t, int, GB_REAL, GB_REAL, int, GB_REAL,
                                      const GB_REAL*, const GB_REAL*, GB_REAL*, const GB_REAL*, GB_REAL*,
                                      GB_REAL*, const GB_REAL*, const GB_REAL*, const uint8_t*, const uint8_t*,
-                                     uint8_t*, const GB_REAL*, const GB_REAL*, GB_REAL*, __half*, __half*);
+                                     uint8_t*, const GB_REAL*, const GB_REAL*, GB_REAL*, __half*, __half*, bool, bool,
+                                     bool);
 template int run_sweep_h<GB_REAL, 1>(const Dev&, cudaStream_t, int, GB_REAL, GB_REAL, int, GB_REAL,
                                      const GB_REAL*, const GB_REAL*, GB_REAL*, const GB_REAL*, GB_REAL*,
                                      GB_REAL*, const GB_REAL*, const GB_REAL*, const uint8_t*, const uint8_t*,
-                                     uint8_t*, const GB_REAL*, const GB_REAL*, GB_REAL*, __half*, __half*);
+                                     uint8_t*, const GB_REAL*, const GB_REAL*, GB_REAL*, __half*, __half*, bool, bool,
+                                     bool);
 template int run_sweep_w2<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL, int, GB_REAL*, GB_REAL*, GB_REAL*,
                                    const GB_REAL*, const int32_t*, __half*, __half*);
 template int run_sweep_w<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL, int, int, int, const GB_REAL*,
@@ -241,6 +269,9 @@ template int run_finalise<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL*, 
 template int run_vdiff<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL, GB_REAL, GB_REAL*, const GB_REAL*,
                                 const GB_REAL*, const int32_t*, const GB_REAL*, GB_REAL*, GB_REAL*, const GB_REAL*,
                                 GB_REAL*, __half*);
+template int run_vdiff2<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL, const GB_REAL*, const GB_REAL*,
+                                 const int32_t*, GB_REAL*, GB_REAL, const GB_REAL*, GB_REAL*, GB_REAL*, __half*,
+                                 GB_REAL*, GB_REAL, GB_REAL*, GB_REAL*, __half*, bool);
 template int run_tridiag<GB_REAL>(cudaStream_t, int, int, int, int, const GB_REAL*, const GB_REAL*,
                                   const GB_REAL*, const GB_REAL*, GB_REAL*);
 template int run_content<GB_REAL>(const Dev&, cudaStream_t, const GB_REAL*, const GB_REAL*, const int32_t*,
@@ -281,4 +312,5 @@ template int run_adj_vdiff<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL, 
 #include "bc_kernels.cuh"
 namespace gb {
 template int run_bc3<GB_REAL>(int, const Dev&, cudaStream_t, const Bc3<GB_REAL>&, GB_REAL* const*);
+template int run_col_heights<GB_REAL>(const Dev&, cudaStream_t, const Bc3<GB_REAL>&, GB_REAL*);
 }  // namespace gb

@@ -27,12 +27,16 @@ constexpr int RED_THREADS = 256;
 // face's left / lower cell, same level pointer origin as f).
 // f_b != nullptr sweeps a second tracer (f_b, fi_src_b -> fi_dst_b) with the same transports,
 // heights and masks (then code and adv must be nullptr).
+// adv_init: adv (nk levels from the level pointer) is not cleared by the caller; the sweep starts
+// the sum, so that every cell of those levels ends as 0 + its flux divergence.
+// du2d / di2d: DU / Di_src are 2D arrays (the first cell of the plane, not a level pointer) whose
+// values hold at every level of the column.
 template <class R, int DIR>
 int run_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int scheme, R AH, const R* f,
                 const R* fi_src, R* fi_dst, const R* Di_src, R* Di_dst, R* adv, const R* U, const R* DU,
                 const uint8_t* mflux, const uint8_t* mupd, uint8_t* code = nullptr, const R* f_b = nullptr,
                 const R* fi_src_b = nullptr, R* fi_dst_b = nullptr, __half* lo = nullptr,
-                __half* lo_b = nullptr);
+                __half* lo_b = nullptr, bool adv_init = false, bool du2d = false, bool di2d = false);
 
 // Vertical sweep on full 3D fields (level-0 pointers); code as above (face k stored at level k;
 // only without sub-iterations).
@@ -109,6 +113,15 @@ int run_vdiff(const Dev& d, cudaStream_t s, R dt, R cnpar, R avmol, R* S, const 
               const int32_t* az, const R* src, R* rus, R* qus, const R* Sin = nullptr, R* S2 = nullptr,
               __half* lo = nullptr);
 
+// Two tracers (temperature a with its sources src_a, salinity b) diffused in one launch over the
+// same heights and diffusivity; each with its own molecular diffusivity, scratch pair and
+// compensated storage; each tracer's expressions are run_vdiff's. hn2d: hn is a 2D array of column
+// heights (every level of a column has that height).
+template <class R>
+int run_vdiff2(const Dev& d, cudaStream_t s, R dt, R cnpar, const R* hn, const R* nuh, const int32_t* az,
+               R* Sa, R avmol_a, const R* src_a, R* rus_a, R* qus_a, __half* lo_a, R* Sb, R avmol_b, R* rus_b,
+               R* qus_b, __half* lo_b, bool hn2d = false);
+
 template <class R>
 int run_tridiag(cudaStream_t s, int ncol, int kmax, int fi, int lt, const R* au, const R* bu, const R* cu,
                 const R* du, R* value);
@@ -139,5 +152,9 @@ template <class R3>
 struct Bc3;
 template <class R3>
 int run_bc3(int which, const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* const* scr);
+// the column heights of the macro step after sigma_coordinates (k_col_heights): NCOLH 2D planes
+// (COL_* in bc_common.cuh)
+template <class R3>
+int run_col_heights(const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* out);
 
 }  // namespace gb

@@ -194,18 +194,21 @@ __global__ void __launch_bounds__(32 * VKW) k_sweep_v_vec(Dev d, SweepC<R> C, in
   const int j1 = min(j0 + rows, nj);
   const long long sj = d.sj;
   const long long base = (long long)k * d.sk + c0;  // cell (c0, row 0) of level k
+  // the same cell of the face depths DV and of the heights Di_src (2D arrays: level stride 0)
+  const long long based = (long long)k * C.skdu + c0, basei = (long long)k * C.skdi + c0;
   const bool use_AH = C.AH > R(0);
   bool fis_f[NF];
 #pragma unroll
   for (int n = 0; n < NF; ++n) fis_f[n] = F.t[n].fi_src == F.t[n].f;
-  auto row_of = [&](const R* a, int j, R (&v)[N]) {
+  auto row_at = [&](const R* a, long long b, int j, R (&v)[N]) {
     if (j < 0 || j >= nj) {
 #pragma unroll
       for (int m = 0; m < N; ++m) v[m] = R(0);
     } else {
-      ld_row<R, N>(a + base + (long long)j * sj, full, navail, v);
+      ld_row<R, N>(a + b + (long long)j * sj, full, navail, v);
     }
   };
+  auto row_of = [&](const R* a, int j, R (&v)[N]) { row_at(a, base, j, v); };
   auto mrow_of = [&](const uint8_t* a, int j) -> uint32_t {
     return (j < 0 || j >= nj) ? 0u : ld_mask_w<N>(a + (long long)j * sj + c0, full, navail);
   };
@@ -220,8 +223,8 @@ __global__ void __launch_bounds__(32 * VKW) k_sweep_v_vec(Dev d, SweepC<R> C, in
         if (NF == 1 && !fis_f[n]) cp_async_v<VB>(&sbuf[st][1][tid], F.t[n].fi_src + p, vbytes);
       }
       cp_async_v<VB>(&sbuf[st][XV][tid], V + p, vbytes);
-      cp_async_v<VB>(&sbuf[st][XDV][tid], DV + p, vbytes);
-      cp_async_v<VB>(&sbuf[st][XDI][tid], Di_src + p, vbytes);
+      cp_async_v<VB>(&sbuf[st][XDV][tid], DV + (based + (long long)j * sj), vbytes);
+      cp_async_v<VB>(&sbuf[st][XDI][tid], Di_src + (basei + (long long)j * sj), vbytes);
       if (NF == 1 && adv) cp_async_v<VB>(&sbuf[st][XAD][tid], adv + p, vbytes);
     }
     cp_async_commit();
@@ -246,7 +249,7 @@ __global__ void __launch_bounds__(32 * VKW) k_sweep_v_vec(Dev d, SweepC<R> C, in
   {
     R DVp[N];
     row_of(V, j0 - 1, Vp);
-    row_of(DV, j0 - 1, DVp);
+    row_at(DV, based, j0 - 1, DVp);
     const int fa = j0 - 1;
     const bool valid = fa >= sub && fa <= nj - 2 - sub;
 #pragma unroll
@@ -395,6 +398,9 @@ __global__ void __launch_bounds__(32 * UWB) k_sweep_u_vec(Dev d, SweepC<R> C, in
   const bool full = act && navail >= N;
   const int vbytes = act ? (full ? N : navail) * (int)sizeof(R) : 0;
   const bool own = act && lane >= 1 && lane <= UOWN;
+  // adv_init: the sweep starts the flux-divergence sum, writing adv = 0 + its own term in every cell
+  // it owns (the caller does not clear adv first)
+  const bool ainit = C.adv_init != 0;
   const long long crow = (long long)blockIdx.y * d.sj;
   const int k0 = blockIdx.z * NKB;
   const int k1 = min(k0 + NKB, nk);
@@ -438,10 +444,10 @@ __global__ void __launch_bounds__(32 * UWB) k_sweep_u_vec(Dev d, SweepC<R> C, in
         if (NF == 1 && own && !fis_f[n]) cp_async16(&sbuf[st][1][tid], F.t[n].fi_src + p, vbytes);
       }
       cp_async16(&sbuf[st][XU][tid], U + p, vbytes);
-      cp_async16(&sbuf[st][XDU][tid], DU + p, vbytes);
+      cp_async16(&sbuf[st][XDU][tid], DU + (crow + (long long)k * C.skdu + cc), vbytes);
       if (own) {
-        cp_async16(&sbuf[st][XDI][tid], Di_src + p, vbytes);
-        if (NF == 1 && adv && any) cp_async16(&sbuf[st][XAD][tid], adv + p, vbytes);
+        cp_async16(&sbuf[st][XDI][tid], Di_src + (crow + (long long)k * C.skdi + cc), vbytes);
+        if (NF == 1 && adv && any && !ainit) cp_async16(&sbuf[st][XAD][tid], adv + p, vbytes);
       }
     }
     cp_async_commit();
@@ -515,7 +521,11 @@ __global__ void __launch_bounds__(32 * UWB) k_sweep_u_vec(Dev d, SweepC<R> C, in
       Dn[q] = updm[q] ? Dio[q] - dDv[q] : Dio[q];
     }
     R ad[N];
-    if (NF == 1 && adv && any) lds_vec<R, N>(sbuf[stc][XAD][tid], ad);
+    if (NF == 1 && adv && any && !ainit) lds_vec<R, N>(sbuf[stc][XAD][tid], ad);
+    if (NF == 1 && adv && ainit) {
+#pragma unroll
+      for (int q = 0; q < N; ++q) ad[q] = R(0);
+    }
 #pragma unroll
     for (int n = 0; n < NF; ++n) {
       R fio[N], fo[N];
@@ -542,7 +552,7 @@ __global__ void __launch_bounds__(32 * UWB) k_sweep_u_vec(Dev d, SweepC<R> C, in
       if (comp) st_lo<N>(F.t[n].lo + p, full, navail, lo);
     }
     if (Di_dst && (any || Di_dst != Di_src)) st_row<R, N>(Di_dst + p, full, navail, Dn);
-    if (NF == 1 && adv && any) st_row<R, N>(adv + p, full, navail, ad);
+    if (NF == 1 && adv && (any || ainit)) st_row<R, N>(adv + p, full, navail, ad);
   }
   cp_async_wait<0>();
 }
