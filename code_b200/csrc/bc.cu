@@ -36,6 +36,17 @@ struct M2 {
   const int32_t* p;
   __device__ int operator()(int i, int j) const { return p[d.ix(i, j)]; }
 };
+struct M8 {
+  const Dev& d;
+  const uint8_t* p;
+  __device__ int operator()(int i, int j) const { return p[d.ix(i, j)]; }
+};
+// mask q (0 az, 1 au, 2 av) of the micro step: the int32 state array, or its uint8 copy (mixed step)
+template <bool MIX>
+__device__ __forceinline__ auto m2a(const Dev& d, const Bc2& s, const Bc2W& w, int q) {
+  if constexpr (MIX) return M8{d, w.m8[q]};
+  else return M2{d, q == 0 ? s.az : q == 1 ? s.au : s.av};
+}
 __device__ __forceinline__ bool interior(const Dev& d, int i, int j) {
   return i >= d.imin && i <= d.imax && j >= d.jmin && j <= d.jmax;
 }
@@ -309,7 +320,7 @@ __global__ void k_momentum_f32(Dev d, Bc2 s, Bc2W w) {
   if constexpr (COR) {
     if (DIR == 0) {  // fV on U points from V
       const float* V = w.w[V_];
-      if (s.au[c] >= 1) {
+      if (w.m8[1][c] >= 1) {
         const float Vloc = 0.25f * (V[c - d.sj] + V[c + 1 - d.sj] + V[c] + V[c + 1]);
         w.w[FV][c] = float(s.f2[CORU][c]) * Vloc;
       } else {
@@ -317,7 +328,7 @@ __global__ void k_momentum_f32(Dev d, Bc2 s, Bc2W w) {
       }
     } else {  // fU on V points from U
       const float* U = w.w[U_];
-      if (s.av[c] >= 1) {
+      if (w.m8[2][c] >= 1) {
         const float Uloc = 0.25f * (U[c - 1] + U[c] + U[c - 1 + d.sj] + U[c + d.sj]);
         w.w[FU][c] = float(s.f2[CORV][c]) * Uloc;
       } else {
@@ -325,7 +336,7 @@ __global__ void k_momentum_f32(Dev d, Bc2 s, Bc2W w) {
       }
     }
   }
-  const int32_t m = DIR == 0 ? s.au[c] : s.av[c];
+  const int m = DIR == 0 ? w.m8[1][c] : w.m8[2][c];
   if (!(m == 1 || m == 2)) return;
   float* X = w.w[DIR == 0 ? U_ : V_];
   const float* DX = w.w[DIR == 0 ? DU : DV];
@@ -333,12 +344,12 @@ __global__ void k_momentum_f32(Dev d, Bc2 s, Bc2W w) {
   const float* airp = w.w[AIRP];
   const float* taus = w.w[DIR == 0 ? TAUSX : TAUSY];
   const double* z = s.f2[Z];
-  const double* H = s.f2[HH];
+  const float* H = w.w[HH];
   const float g = float(s.par[P_G]), rho_0 = float(s.par[P_RHO_0]), dtm = float(s.par[P_DTM]);
   const double min_depth = s.par[P_MIN_DEPTH];
   const float gammai = 1.f / (rho_0 * g);
-  const double zp = fmax(z[c + dn], -H[c] + fmin(min_depth, (double)D[c + dn]));
-  const double zm = fmax(z[c], -H[c + dn] + fmin(min_depth, (double)D[c]));
+  const double zp = fmax(z[c + dn], -(double)H[c] + fmin(min_depth, (double)D[c + dn]));
+  const double zm = fmax(z[c], -(double)H[c + dn] + fmin(min_depth, (double)D[c]));
   const float zx = (float(zp - zm) + (airp[c + dn] - airp[c]) * gammai) / float(DIR == 0 ? d.dx : d.dy);
   const float tau = 0.5f * (taus[c] + taus[c + dn]);
   const float Xo = X[c], sl = w.w[DIR == 0 ? SLRU : SLRV][c];
@@ -359,11 +370,11 @@ __global__ void k_coriolis(Dev d, Bc2 s, Bc2W w) {
     const long long c = d.ix(i, j);
     if (DIR == 0) {
       const float* U = w.w[U_];
-      w.w[FU][c] = s.av[c] >= 1 ? float(s.f2[CORV][c]) * (0.25f * (U[c - 1] + U[c] + U[c - 1 + d.sj] + U[c + d.sj]))
+      w.w[FU][c] = w.m8[2][c] >= 1 ? float(s.f2[CORV][c]) * (0.25f * (U[c - 1] + U[c] + U[c - 1 + d.sj] + U[c + d.sj]))
                                 : 0.f;
     } else {
       const float* V = w.w[V_];
-      w.w[FV][c] = s.au[c] >= 1 ? float(s.f2[CORU][c]) * (0.25f * (V[c - d.sj] + V[c + 1 - d.sj] + V[c] + V[c + 1]))
+      w.w[FV][c] = w.m8[1][c] >= 1 ? float(s.f2[CORU][c]) * (0.25f * (V[c - d.sj] + V[c + 1 - d.sj] + V[c] + V[c + 1]))
                                 : 0.f;
     }
     return;
@@ -399,8 +410,9 @@ __global__ void k_accum_sealevel(Dev d, Bc2 s, Bc2W w, int accumulate) {
   GB_IJ2
   auto U = f2a<MIX, U_>(d, s, w);
   auto V = f2a<MIX, V_>(d, s, w);
-  W2 z{d, s.f2[Z]}, zo{d, s.f2[ZO]}, fwf{d, s.f2[FWF]}, Uint{d, s.f2[UINT]}, Vint{d, s.f2[VINT]};
-  M2 az{d, s.az};
+  auto fwf = f2a<MIX, FWF>(d, s, w);
+  W2 z{d, s.f2[Z]}, zo{d, s.f2[ZO]}, Uint{d, s.f2[UINT]}, Vint{d, s.f2[VINT]};
+  auto az = m2a<MIX>(d, s, w, 0);
   const double dtm = s.par[P_DTM];
   if (accumulate) {
     Uint(i, j) = Uint(i, j) + U(i, j);
@@ -423,8 +435,13 @@ __global__ void k_depth_update(Dev d, Bc2 s, Bc2W w) {
   auto DV_ = f2a<MIX, DV>(d, s, w);
   auto dry_u = f2a<MIX, DRY_U>(d, s, w);
   auto dry_v = f2a<MIX, DRY_V>(d, s, w);
-  W2 z{d, s.f2[Z]}, zo{d, s.f2[ZO]}, H{d, s.f2[HH]}, HU_{d, s.f2[HU]}, HV_{d, s.f2[HV]}, dry_z{d, s.f2[DRY_Z]};
-  M2 az{d, s.az}, au{d, s.au}, av{d, s.av};
+  auto H = f2a<MIX, HH>(d, s, w);
+  auto HU_ = f2a<MIX, HU>(d, s, w);
+  auto HV_ = f2a<MIX, HV>(d, s, w);
+  W2 z{d, s.f2[Z]}, zo{d, s.f2[ZO]}, dry_z{d, s.f2[DRY_Z]};
+  auto az = m2a<MIX>(d, s, w, 0);
+  auto au = m2a<MIX>(d, s, w, 1);
+  auto av = m2a<MIX>(d, s, w, 2);
   const double min_depth = s.par[P_MIN_DEPTH], crit_depth = s.par[P_CRIT_DEPTH];
   D(i, j) = z(i, j) + H(i, j);
   if (i <= d.imax + HALO - 1) {
@@ -459,9 +476,14 @@ __global__ void k_sealevel_depth(Dev d, Bc2 s, Bc2W w, int accumulate) {
   auto DV_ = f2a<MIX, DV>(d, s, w);
   auto dry_u = f2a<MIX, DRY_U>(d, s, w);
   auto dry_v = f2a<MIX, DRY_V>(d, s, w);
-  W2 zold{d, s.f2[Z]}, znew{d, s.f2[ZO]}, fwf{d, s.f2[FWF]}, Uint{d, s.f2[UINT]}, Vint{d, s.f2[VINT]}, H{d, s.f2[HH]},
-      HU_{d, s.f2[HU]}, HV_{d, s.f2[HV]}, dry_z{d, s.f2[DRY_Z]};
-  M2 az{d, s.az}, au{d, s.au}, av{d, s.av};
+  auto fwf = f2a<MIX, FWF>(d, s, w);
+  auto H = f2a<MIX, HH>(d, s, w);
+  auto HU_ = f2a<MIX, HU>(d, s, w);
+  auto HV_ = f2a<MIX, HV>(d, s, w);
+  W2 zold{d, s.f2[Z]}, znew{d, s.f2[ZO]}, Uint{d, s.f2[UINT]}, Vint{d, s.f2[VINT]}, dry_z{d, s.f2[DRY_Z]};
+  auto az = m2a<MIX>(d, s, w, 0);
+  auto au = m2a<MIX>(d, s, w, 1);
+  auto av = m2a<MIX>(d, s, w, 2);
   const double dtm = s.par[P_DTM];
   // sealevel.F90:94-108 at (ii, jj)
   auto zn = [&](int ii, int jj) -> double {
@@ -1140,8 +1162,8 @@ int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop, const Bc2W* wp = nu
         grid_for_tag(ctx, dir == 0 ? GETM_U_TAG : GETM_V_TAG, &g);
         Bf2Args bf{};
         if (bf_fused) {
-          bf.mask = dir == 0 ? st->au : st->av;
-          bf.au = st->au;
+          bf.mask = w.m8[dir == 0 ? 1 : 2];
+          bf.au = w.m8[1];
           bf.zb = st->f2[dir == 0 ? ZUB : ZVB];
           bf.zb0 = st->f2[dir == 0 ? ZUB0 : ZVB0];
           bf.r = w.w[dir == 0 ? RU : RV];
@@ -1195,6 +1217,16 @@ int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop, const Bc2W* wp = nu
   rc = mix ? k2(k_depth_update<true>, d, s, w) : k2(k_depth_update<false>, d, s, w);
   if (rc) return cuda_fail(ctx, rc, "depth_update");
   return GETM_OK;
+}
+
+// uint8 copies of the masks az, au, av (values 0..3) for the mixed-precision micro step
+__global__ void k_mask8(long long n2, const int32_t* az, const int32_t* au, const int32_t* av, uint8_t* m8,
+                        long long pitch) {
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n2; c += (long long)gridDim.x * blockDim.x) {
+    m8[c] = (uint8_t)az[c];
+    m8[pitch + c] = (uint8_t)au[c];
+    m8[2 * pitch + c] = (uint8_t)av[c];
+  }
 }
 
 // Copies between the FP64 state and the FP32 working copies of the mixed-precision micro step:
@@ -1864,8 +1896,11 @@ static int time_loop(getm_ctx* ctx, getm_bc_state* st, int n0, int count, bool z
     const long long n2 = n2d(d);
     int nw = 0;
     for (int q = 0; q < NF2; ++q) nw += is_work2(q) ? 1 : 0;
+    // nw FP32 planes, then the uint8 copies of az, au, av (3 planes, 16-byte aligned)
+    const long long m8off = (long long)nw * n2 * (long long)sizeof(float);
+    const long long m8pitch = (n2 + 15) / 16 * 16;
     if (!ctx->w2) {
-      if (cudaMalloc(&ctx->w2, (size_t)nw * n2 * sizeof(float)) != cudaSuccess) {
+      if (cudaMalloc(&ctx->w2, (size_t)(m8off + 3 * m8pitch)) != cudaSuccess) {
         cudaGetLastError();
         return fail(ctx, GETM_ERR_NOMEM, "mixed-precision 2D working copies: allocation failed");
       }
@@ -1875,6 +1910,10 @@ static int time_loop(getm_ctx* ctx, getm_bc_state* st, int n0, int count, bool z
       w.w[q] = is_work2(q) ? ctx->w2 + (long long)(slot++) * n2 : nullptr;
       if (is_work2(q)) all |= 1ull << q;
     }
+    uint8_t* m8 = reinterpret_cast<uint8_t*>(ctx->w2) + m8off;
+    for (int q = 0; q < 3; ++q) w.m8[q] = m8 + q * m8pitch;
+    k_mask8<<<592, 256, 0, ctx->stream>>>(n2, st->az, st->au, st->av, m8, m8pitch);
+    GB_TRY(cudaGetLastError(), "uint8 masks");
     // written by the micro steps; written by the macro step and read by the micro steps
     for (int q : {U_, V_, D_, DU, DV, DRY_U, DRY_V, FU, FV, RU, RV, RUU, RVV, UEX, VEX}) written |= 1ull << q;
     for (int q : {SLUX, SLVX, SLRU, SLRV, RU, RV}) from3d |= 1ull << q;

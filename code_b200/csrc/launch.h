@@ -57,8 +57,8 @@ int run_uvadv2d_fused(const Dev& d, cudaStream_t s, int dir, T dt, int scheme, c
 // (ru, ruu; zub for runtype 1), DIR 1 the V points (rv, rvv; zvb). FP32 arithmetic, the operations
 // of k_bottom_friction_f32t (bc.cu) in the same order, so the same values. r == nullptr: off.
 struct Bf2Args {
-  const int32_t* mask;  // au (DIR 0) / av (DIR 1)
-  const int32_t* au;    // DIR 1: the U points' mask for the velocity outside the interior
+  const uint8_t* mask;  // au (DIR 0) / av (DIR 1), uint8 copies
+  const uint8_t* au;    // DIR 1: the U points' mask for the velocity outside the interior
   double* zb;           // zub / zvb
   const double* zb0;    // zub0 / zvb0
   float* r;             // ru / rv (FP32 working copies)

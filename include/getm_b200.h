@@ -119,9 +119,9 @@ const char *getm_timer_name(int slot);
 int getm_set_vector_sweeps(int on);
 /* Process-wide choice for the mixed-precision step (no counterpart in the reference: a testing and
  * accuracy switch). on != 0 (the default) runs the barotropic micro steps of getm_time_loop on FP32
- * working copies of the 2D fields whenever the step has no open boundaries (elevation, Uint/Vint
- * and the static depths stay FP64); on == 0 keeps the micro steps on the FP64 state arrays, as the
- * plain step does. Returns the previous setting. */
+ * working copies of the 2D fields whenever the step has no open boundaries (the elevation and
+ * Uint/Vint stay FP64); on == 0 keeps the micro steps on the FP64 state arrays, as the plain step
+ * does. Returns the previous setting. */
 int getm_set_fp32_micro_steps(int on);
 /* Process-wide choice of the micro-step launches (no counterpart in the reference: a tuning and
  * testing switch). on != 0 (the default): getm_time_loop without open boundaries runs sealevel and
