@@ -251,8 +251,10 @@ def run_reference(args, world, rank):
 
     flags = cpu_build()
 
-    snx = min(args.nx, 256)
-    sny = min(args.ny, 256)
+    # a 512x512 sample per step (the per-cell rate at 512x512 is within 3% of the rate the larger
+    # samples level off at, and a step takes ~1.6 s on 16 host cores)
+    snx = min(args.nx, 512)
+    sny = min(args.ny, 512)
     c = oracle_sample(snx, sny, args.kmax, args.M)
     M = args.M
     n = 1
@@ -284,7 +286,8 @@ def cpu_baseline_sample(args):
     import oracle
 
     flags = cpu_build()
-    snx, sny = min(args.nx, 256), min(args.ny, 256)
+    # the 1024x1024 sample: the oracle's per-cell rate has levelled off at that size
+    snx, sny = min(args.nx, 1024), min(args.ny, 1024)
     c = oracle_sample(snx, sny, args.kmax, args.M)
     oracle.bc_steps(c, 1, args.M)
     n, steps, t0 = 1 + args.M, 0, time.perf_counter()

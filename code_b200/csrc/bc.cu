@@ -1106,20 +1106,24 @@ int bottom_friction_2d(getm_ctx* ctx, const getm_bc_state* st, int runtype, cons
 // velocity (:193-216, :356-379). Mixed micro step (wp): the update on the working copies, with
 // the term it needs formed in the same launch when `cor` (see integrate_2d).
 template <int DIR>
-int momentum_2d(getm_ctx* ctx, const getm_bc_state* st, const Bc2W* wp, bool cor) {
+// fused (the FP64 micro-step loop without open boundaries; always for the mixed step): the update
+// forms the Coriolis term it needs itself when `cor`, and the term of the other velocity is left to
+// the next update (or to the end of the loop) instead of a k_coriolis launch after each update.
+int momentum_2d(getm_ctx* ctx, const getm_bc_state* st, const Bc2W* wp, bool cor, bool fused = false) {
   const Dev& d = ctx->dev;
   const Bc2 s = to_bc2(st);
   const Bc2W w = wp ? *wp : Bc2W{};
   cudaStream_t cs = ctx->stream;
   {
     TimerScope ts(ctx, GETM_TIM_BC2D);
-    if (!wp) k_momentum<DIR, false><<<grid2(d), kBlk2, 0, cs>>>(d, s, w);
+    if (!wp && fused && cor) k_momentum<DIR, false, true><<<grid2(d), kBlk2, 0, cs>>>(d, s, w);
+    else if (!wp) k_momentum<DIR, false><<<grid2(d), kBlk2, 0, cs>>>(d, s, w);
     else if (cor) k_momentum_f32<DIR, true><<<grid2(d), kBlk2, 0, cs>>>(d, s, w);
     else k_momentum_f32<DIR, false><<<grid2(d), kBlk2, 0, cs>>>(d, s, w);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(ctx, (int)e, DIR == 0 ? "umomentum" : "vmomentum");
   }
-  if (wp) return GETM_OK;
+  if (wp || fused) return GETM_OK;
   int r;
   if ((r = mirror_bdy<double>(ctx, st->f2[DIR == 0 ? U_ : V_], DIR, 1))) return r;
   TimerScope ts(ctx, GETM_TIM_BC2D);
@@ -1190,8 +1194,9 @@ int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop, const Bc2W* wp = nu
   // it gives the same value. The first update of a getm_time_loop call (first) reads the stored
   // term instead -- the state's fU/fV, which need not match the velocities (a start from rest of
   // the Coriolis terms) -- and getm_time_loop forms the term of the last update at its end.
-  auto umom = [&](bool cor) -> int { return momentum_2d<0>(ctx, st, wp, cor); };
-  auto vmom = [&](bool cor) -> int { return momentum_2d<1>(ctx, st, wp, cor); };
+  // the FP64 loop without open boundaries forms the Coriolis terms like the mixed step (zswap)
+  auto umom = [&](bool cor) -> int { return momentum_2d<0>(ctx, st, wp, cor, zswap); };
+  auto vmom = [&](bool cor) -> int { return momentum_2d<1>(ctx, st, wp, cor, zswap); };
   if (ip[I_UFIRST2D]) {
     if ((rc = umom(!first)) || (rc = vmom(true))) return rc;
     ip[I_UFIRST2D] = 0;
@@ -1266,7 +1271,7 @@ __global__ void k_sync_w2(long long n2, Bc2 s, Bc2W w, FieldList fl, int to_w, i
 }
 
 template <class R3>
-int bc3(getm_ctx* ctx, const getm_bc_state* st, int which, int slot, unsigned skip = 0) {
+int bc3(getm_ctx* ctx, const getm_bc_state* st, int which, int slot, unsigned skip = 0, const R3* colh = nullptr) {
   const Bc3<R3> s = to_bc3<R3>(st);
   const long long n3 = n3d(ctx->dev);
   R3* base = (R3*)ctx->bc_scr3;
@@ -1274,7 +1279,7 @@ int bc3(getm_ctx* ctx, const getm_bc_state* st, int which, int slot, unsigned sk
   const int nb = sizeof(R3) == 4 ? NB3F : NB3;
   // skip: scratch slots the kernel does not write (bit q = slot q)
   for (int q = 0; q < NB3F; ++q) scr[q] = (q < nb && !((skip >> q) & 1u)) ? base + q * n3 : nullptr;
-  GB_TIMED(slot, (run_bc3<R3>(which, ctx->dev, ctx->stream, s, scr)), "macro-step kernel");
+  GB_TIMED(slot, (run_bc3<R3>(which, ctx->dev, ctx->stream, s, scr, colh)), "macro-step kernel");
   return GETM_OK;
 }
 
@@ -1365,7 +1370,8 @@ int integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
       }
       const R3* hou = cols ? CH(COL_HUN) : f3[HUN];
       const R3* hov = cols ? CH(COL_HVN) : f3[HVN];
-      if ((rc = bc3<R3>(ctx, st, sizeof(R3) == 4 ? BC3_UVADV_PREP_UV : BC3_UVADV_PREP_U, GETM_TIM_BC3D, skip)))
+      if ((rc = bc3<R3>(ctx, st, sizeof(R3) == 4 ? BC3_UVADV_PREP_UV : BC3_UVADV_PREP_U, GETM_TIM_BC3D, skip,
+                        colh)))
         return rc;
       if ((rc = do_adv3d<R3>(ctx, R3(st->par[P_DT]), fadv, ua, va, wa, hua, hva, hou, hou, split, hor, ver, R3(0),
                              GETM_U_TAG, nullptr, f3[UUEX], ip[I_ADV_VER_ITERS], false, nullptr, h2d)))
@@ -1946,13 +1952,16 @@ static int time_loop(getm_ctx* ctx, getm_bc_state* st, int n0, int count, bool z
       if (mix && (rc = sync(from3d, 1))) return rc;
     }
   }
-  if (mix && count > 0) {
+  if ((mix || zswap) && count > 0) {
     // the Coriolis term of the last velocity update (fV after a V update, fU after a U update):
     // ufirst2d was toggled by the last micro step, so 0 means its order was u, v
     TimerScope ts(ctx, GETM_TIM_BC2D);
     const Bc2 s2 = to_bc2(st);
-    if (st->ipar[I_UFIRST2D] == 0) k_coriolis<1, true><<<grid2(ctx->dev), kBlk2, 0, ctx->stream>>>(ctx->dev, s2, w);
-    else k_coriolis<0, true><<<grid2(ctx->dev), kBlk2, 0, ctx->stream>>>(ctx->dev, s2, w);
+    const bool v_last = st->ipar[I_UFIRST2D] == 0;
+    if (mix && v_last) k_coriolis<1, true><<<grid2(ctx->dev), kBlk2, 0, ctx->stream>>>(ctx->dev, s2, w);
+    else if (mix) k_coriolis<0, true><<<grid2(ctx->dev), kBlk2, 0, ctx->stream>>>(ctx->dev, s2, w);
+    else if (v_last) k_coriolis<1, false><<<grid2(ctx->dev), kBlk2, 0, ctx->stream>>>(ctx->dev, s2, w);
+    else k_coriolis<0, false><<<grid2(ctx->dev), kBlk2, 0, ctx->stream>>>(ctx->dev, s2, w);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(ctx, (int)e, "coriolis");
   }

@@ -712,7 +712,7 @@ template <class R3>
 __global__ void k_col_heights(Dev d, Bc3<R3> s, R3* out) {
   GB_IJ_HALO
   const int ni = d.ni(), nj = d.nj();
-  const long long n2 = (long long)ni * nj;
+  const long long n2 = d.sj * (long long)nj;  // plane pitch (the 2D fields' size)
   const int ii = i - (d.imin - HALO), jj = j - (d.jmin - HALO);
   const long long c = d.ix(i, j);
   const double kmaxm1 = 1.0 / (double)(float)d.kmax;
@@ -886,91 +886,96 @@ struct Prep6 {
   float* a[6];
 };
 template <int N = 4>
-__global__ void __launch_bounds__(128) k_uvadv3d_prep_vec2(Dev d, Bc3<float> s, Prep6 u, Prep6 v) {
+__global__ void __launch_bounds__(128) k_uvadv3d_prep_vec2(Dev d, Bc3<float> s, Prep6 u, Prep6 v,
+                                                         const float* colh) {
   const int ni = d.ni(), nj = d.nj();
   const int c0 = (blockIdx.x * blockDim.x + threadIdx.x) * N;
   const int jj = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
   if (c0 >= ni || jj >= nj) return;
-  // levels k0..k1-1 of the thread's 4 cells (grid z = chunk of LVC levels)
-  const int k0 = max(1, (int)blockIdx.z * LVC), k1 = min((int)blockIdx.z * LVC + LVC, d.kmax + 1);
   const long long c = (long long)jj * d.sj + c0;  // the 2D index of the first cell
+  const long long p = (long long)k * d.sk + c;
   const int nrow = min(N, ni - c0);
-  if (blockIdx.z == 0) {
+  if (k == 0) {
     const float z[N] = {0.f, 0.f, 0.f, 0.f};
-    st_row<float, N>(u.a[3] + c, nrow == N, nrow, z);
+    st_row<float, N>(u.a[3] + p, nrow == N, nrow, z);
+    return;
   }
   const bool fullr = c0 + N <= ni;
+  auto ld = [&](int f, long long off, float (&x)[N]) { ld_row<float, N>(s.f3[f] + p + off, fullr, ni - c0, x); };
+  // heights: the 3D arrays, or (colh) the column planes of k_col_heights, the same values
+  const long long n2 = d.sj * (long long)nj;
+  auto ldh = [&](int f, int q, long long off, float (&x)[N]) {
+    if (colh) ld_row<float, N>(colh + q * n2 + c + off, fullr, ni - c0, x);
+    else ld_row<float, N>(s.f3[f] + p + off, fullr, ni - c0, x);
+  };
+  auto ldh1 = [&](int f, int q, long long off) -> float {
+    return colh ? colh[q * n2 + c + off] : s.f3[f][p + off];
+  };
+  float uu[N], vv[N], ww[N], hun[N], hvn[N];
+  ld(UU, 0, uu); ld(VV, 0, vv); ld(WW, 0, ww);
+  ldh(HUN, COL_HUN, 0, hun); ldh(HVN, COL_HVN, 0, hvn);
   const float half = 0.5f;
   const int nwu = min(nrow, ni - 1 - c0);  // U grid: every cell but the last of the row
-  const bool vrow = jj <= nj - 2;          // V grid: rows but the last
-  const bool nb = c0 + N < ni;
-  // the columns' layer heights (k_sigma's values): ho, hn, hvn at the cells and the i+1 neighbour
-  // (U grid), hun, hvn at the cells and ho, hn, hun of row j+1 (V grid)
-  const double kmaxm1 = 1.0 / (double)(float)d.kmax;
-  const long long sj = d.sj;
-  float ho[N + 1], hn[N + 1], hvn[N + 1], hun[N], ho1[N], hn1[N], hun1[N];
-#pragma unroll
-  for (int m = 0; m <= N; ++m) {
-    const long long q = c + (m < nrow ? m : (m == N && nb ? N : 0));
-    ho[m] = sig_h<float>(s, SSEO, HH, q, kmaxm1);
-    hn[m] = sig_h<float>(s, SSEN, HH, q, kmaxm1);
-    hvn[m] = sig_h<float>(s, SSVN, HV, q, kmaxm1);
-    if (m < N) {
-      hun[m] = sig_h<float>(s, SSUN, HU, q, kmaxm1);
-      const long long q1 = vrow ? q + sj : q;
-      ho1[m] = sig_h<float>(s, SSEO, HH, q1, kmaxm1);
-      hn1[m] = sig_h<float>(s, SSEN, HH, q1, kmaxm1);
-      hun1[m] = sig_h<float>(s, SSUN, HU, q1, kmaxm1);
+  if (nwu > 0) {
+    const bool nb = c0 + N < ni;
+    const long long q = p + N;
+    const float uue = nb ? s.f3[UU][q] : 0.f, vve = nb ? s.f3[VV][q] : 0.f, wwe = nb ? s.f3[WW][q] : 0.f;
+    float fa[N], ua[N], va[N], wa[N], ha[N], hb[N];
+    const bool hout = u.a[4] || u.a[5];
+    float ho[N], hn[N], hoe = 0.f, hne = 0.f, hvne = 0.f;
+    if (hout) {
+      ldh(HO, COL_HO, 0, ho); ldh(HN, COL_HN, 0, hn);
+      if (nb) { hoe = ldh1(HO, COL_HO, N); hne = ldh1(HN, COL_HN, N); hvne = ldh1(HVN, COL_HVN, N); }
     }
-  }
-  for (int k = k0; k < k1; ++k) {
-    const long long p = (long long)k * d.sk + c;
-    auto ld = [&](int f, long long off, float (&x)[N]) { ld_row<float, N>(s.f3[f] + p + off, fullr, ni - c0, x); };
-    float uu[N], vv[N], ww[N];
-    ld(UU, 0, uu); ld(VV, 0, vv); ld(WW, 0, ww);
-    if (nwu > 0) {
-      const long long q = p + N;
-      const float uue = nb ? s.f3[UU][q] : 0.f, vve = nb ? s.f3[VV][q] : 0.f, wwe = nb ? s.f3[WW][q] : 0.f;
-      float fa[N], ua[N], va[N], wa[N], ha[N], hb[N];
 #pragma unroll
-      for (int m = 0; m < N; ++m) {
-        const float u1 = m + 1 < N ? uu[m + 1] : uue, v1 = m + 1 < N ? vv[m + 1] : vve, w1 = m + 1 < N ? ww[m + 1] : wwe;
-        fa[m] = uu[m] / hun[m];
-        ua[m] = half * (uu[m] + u1);
-        va[m] = half * (vv[m] + v1);
-        wa[m] = half * (ww[m] + w1);
-        ha[m] = half * (ho[m + 1] + hn[m + 1]);
-        hb[m] = half * (hvn[m] + hvn[m + 1]);
+    for (int m = 0; m < N; ++m) {
+      const float u1 = m + 1 < N ? uu[m + 1] : uue, v1 = m + 1 < N ? vv[m + 1] : vve, w1 = m + 1 < N ? ww[m + 1] : wwe;
+      fa[m] = uu[m] / hun[m];
+      ua[m] = half * (uu[m] + u1);
+      va[m] = half * (vv[m] + v1);
+      wa[m] = half * (ww[m] + w1);
+      if (hout) {
+        const float o1 = m + 1 < N ? ho[m + 1] : hoe, n1 = m + 1 < N ? hn[m + 1] : hne,
+                    h1 = m + 1 < N ? hvn[m + 1] : hvne;
+        ha[m] = half * (o1 + n1);
+        hb[m] = half * (hvn[m] + h1);
       }
-      const bool fw = nwu == N;
-      st_row<float, N>(u.a[0] + p, fw, nwu, fa);
-      st_row<float, N>(u.a[1] + p, fw, nwu, ua);
-      st_row<float, N>(u.a[2] + p, fw, nwu, va);
-      st_row<float, N>(u.a[3] + p, fw, nwu, wa);
-      if (u.a[4]) st_row<float, N>(u.a[4] + p, fw, nwu, ha);
-      if (u.a[5]) st_row<float, N>(u.a[5] + p, fw, nwu, hb);
     }
-    if (vrow) {
-      float uu1[N], vv1[N], ww1[N];
-      ld(UU, sj, uu1); ld(VV, sj, vv1); ld(WW, sj, ww1);
-      float fa[N], ua[N], va[N], wa[N], ha[N], hb[N];
+    const bool fw = nwu == N;
+    st_row<float, N>(u.a[0] + p, fw, nwu, fa);
+    st_row<float, N>(u.a[1] + p, fw, nwu, ua);
+    st_row<float, N>(u.a[2] + p, fw, nwu, va);
+    st_row<float, N>(u.a[3] + p, fw, nwu, wa);
+    if (u.a[4]) st_row<float, N>(u.a[4] + p, fw, nwu, ha);
+    if (u.a[5]) st_row<float, N>(u.a[5] + p, fw, nwu, hb);
+  }
+  if (jj <= nj - 2) {  // V grid: rows but the last
+    const long long sj = d.sj;
+    float uu1[N], vv1[N], ww1[N];
+    ld(UU, sj, uu1); ld(VV, sj, vv1); ld(WW, sj, ww1);
+    float fa[N], ua[N], va[N], wa[N], ha[N], hb[N];
+    const bool hout = v.a[4] || v.a[5];
+    float hun1[N], ho1[N], hn1[N];
+    if (hout) { ldh(HUN, COL_HUN, sj, hun1); ldh(HO, COL_HO, sj, ho1); ldh(HN, COL_HN, sj, hn1); }
 #pragma unroll
-      for (int m = 0; m < N; ++m) {
-        fa[m] = vv[m] / hvn[m];
-        ua[m] = half * (uu[m] + uu1[m]);
-        va[m] = half * (vv[m] + vv1[m]);
-        wa[m] = half * (ww[m] + ww1[m]);
+    for (int m = 0; m < N; ++m) {
+      fa[m] = vv[m] / hvn[m];
+      ua[m] = half * (uu[m] + uu1[m]);
+      va[m] = half * (vv[m] + vv1[m]);
+      wa[m] = half * (ww[m] + ww1[m]);
+      if (hout) {
         ha[m] = half * (hun[m] + hun1[m]);
         hb[m] = half * (ho1[m] + hn1[m]);
       }
-      const bool fw = nrow == N;
-      st_row<float, N>(v.a[0] + p, fw, nrow, fa);
-      st_row<float, N>(v.a[1] + p, fw, nrow, ua);
-      st_row<float, N>(v.a[2] + p, fw, nrow, va);
-      st_row<float, N>(v.a[3] + p, fw, nrow, wa);
-      if (v.a[4]) st_row<float, N>(v.a[4] + p, fw, nrow, ha);
-      if (v.a[5]) st_row<float, N>(v.a[5] + p, fw, nrow, hb);
     }
+    const bool fw = nrow == N;
+    st_row<float, N>(v.a[0] + p, fw, nrow, fa);
+    st_row<float, N>(v.a[1] + p, fw, nrow, ua);
+    st_row<float, N>(v.a[2] + p, fw, nrow, va);
+    st_row<float, N>(v.a[3] + p, fw, nrow, wa);
+    if (v.a[4]) st_row<float, N>(v.a[4] + p, fw, nrow, ha);
+    if (v.a[5]) st_row<float, N>(v.a[5] + p, fw, nrow, hb);
   }
 }
 
@@ -1251,7 +1256,7 @@ int run_col_heights(const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* out) {
 }
 
 template <class R3>
-int run_bc3(int which, const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* const* scr) {
+int run_bc3(int which, const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* const* scr, const R3* colh) {
   const dim3 blk(32, 4, 1);
   switch (which) {
     case BC3_BF3D: k_bf3d<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s); break;
@@ -1309,12 +1314,12 @@ int run_bc3(int which, const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* cons
       const bool u = which == BC3_UVADV_PREP_U;
       if constexpr (sizeof(R3) == 4) {
         bool ok = vector_sweeps_enabled() && d.sj % 4 == 0 && d.sk % 4 == 0;
-        for (int q = 0; q < 6 && ok; ++q) ok = reinterpret_cast<uintptr_t>(scr[q]) % 16 == 0;
-        for (int f : {UU, VV, WW})
+        for (int q = 0; q < 6 && ok; ++q) ok = !scr[q] || reinterpret_cast<uintptr_t>(scr[q]) % 16 == 0;
+        for (int f : {UU, VV, WW, HO, HN, HUN, HVN})
           ok = ok && reinterpret_cast<uintptr_t>(s.f3[f]) % 16 == 0;
         if (ok) {
           const dim3 bv(32, 4, 1);
-          const dim3 gv((d.ni() + 4 * 32 - 1) / (4 * 32), (d.nj() + 3) / 4, (d.kmax + LVC) / LVC);
+          const dim3 gv((d.ni() + 4 * 32 - 1) / (4 * 32), (d.nj() + 3) / 4, d.kmax + 1);
           if (u) k_uvadv3d_prep_vec<0><<<gv, bv, 0, st>>>(d, s, scr[0], scr[1], scr[2], scr[3], scr[4], scr[5]);
           else k_uvadv3d_prep_vec<1><<<gv, bv, 0, st>>>(d, s, scr[0], scr[1], scr[2], scr[3], scr[4], scr[5]);
           break;
@@ -1332,13 +1337,15 @@ int run_bc3(int which, const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* cons
       if constexpr (sizeof(R3) == 4) {
         bool ok = vector_sweeps_enabled() && d.sj % 4 == 0 && d.sk % 4 == 0;
         for (int q : {0, 1, 2, 3, 4, 5, 7, 8, 9, 10, 11, 12}) ok = ok && reinterpret_cast<uintptr_t>(scr[q]) % 16 == 0;
-        for (int f : {UU, VV, WW})
+        for (int f : {UU, VV, WW, HO, HN, HUN, HVN})
           ok = ok && reinterpret_cast<uintptr_t>(s.f3[f]) % 16 == 0;
+        ok = ok && reinterpret_cast<uintptr_t>(colh) % 16 == 0;
         if (ok) {
           const dim3 bv(32, 4, 1);
-          const dim3 gv((d.ni() + 4 * 32 - 1) / (4 * 32), (d.nj() + 3) / 4, (d.kmax + LVC) / LVC);
+          const dim3 gv((d.ni() + 4 * 32 - 1) / (4 * 32), (d.nj() + 3) / 4, d.kmax + 1);
           k_uvadv3d_prep_vec2<4><<<gv, bv, 0, st>>>(d, s, Prep6{{scr[0], scr[1], scr[2], scr[3], scr[4], scr[5]}},
-                                                    Prep6{{scr[7], scr[8], scr[9], scr[10], scr[11], scr[12]}});
+                                                    Prep6{{scr[7], scr[8], scr[9], scr[10], scr[11], scr[12]}},
+                                                    colh);
         } else {
           k_uvadv3d_prep<R3, 0><<<plane_grid(d, blk, d.kmax + 1), blk, 0, st>>>(d, s, scr[0], scr[1], scr[2],
                                                                                 scr[3], scr[4], scr[5]);

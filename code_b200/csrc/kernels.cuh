@@ -704,15 +704,19 @@ __global__ void __launch_bounds__(128) k_sweep_w(Dev d, R dt, R splitfac, int ks
     wprev = wface_s<R, S, REC>(0, 1, kmax, dti, ww[c], R(0), F(0), F(1), F(2), H(0), H(1), &cd);
     if (REC) code[c] = cd;
   }
-  // window for face k = 1: f(0..4), hi(1..3), ww(0..2)
+  // window for face k = 1: f(0..4), hi(1..3), ww(0..2); the carried errors (compensated storage)
+  // of levels 1, 2
   R a = F(0), b = F(1), e = F(2), g = F(3), g2 = F(4);
   R hA = H(1), hB = H(2), hC = H(3);
   R wkm1 = W(0), wk = W(1), wk1 = W(2);
+  auto LO = [&](int k) -> float { return (lo && k <= kmax) ? __half2float(lo[c + k * sk]) : 0.f; };
+  float lk = LO(1), lk1 = LO(2);
   for (int k = 1; k <= kmax - kshift; ++k) {
     // loads two levels ahead, issued before this level's stores (f/hi may alias fi/hi)
     const R gn = F(k + 4);
     const R hn3 = H(k + 3);
     const R wn = W(k + 2);
+    const float ln = LO(k + 2);
     const R fio = fi_is_f ? b : fi_src[c + k * sk];
     const R advo = adv ? adv[c + k * sk] : R(0);
     R wfl = R(0);
@@ -726,7 +730,9 @@ __global__ void __launch_bounds__(128) k_sweep_w(Dev d, R dt, R splitfac, int ks
     const R hin = hio - dh;
     const R advn = splitfac * (wfl - wprev);
     if (lo) {
-      fi_dst[c + k * sk] = fv_update_lo<R>(hio, dh, hin, fio, dt, advn, lo, c + k * sk);
+      float slo = lk;
+      fi_dst[c + k * sk] = fv_update_lo<R>(hio, dh, hin, fio, dt, advn, slo);
+      lo[c + k * sk] = __float2half_rn(slo);
     } else {
       fi_dst[c + k * sk] = fv_update<R>(hio, dh, hin, fio, dt, advn);
     }
@@ -735,6 +741,7 @@ __global__ void __launch_bounds__(128) k_sweep_w(Dev d, R dt, R splitfac, int ks
     a = b; b = e; e = g; g = g2; g2 = gn;
     hA = hB; hB = hC; hC = hn3;
     wkm1 = wk; wk = wk1; wk1 = wn;
+    lk = lk1; lk1 = ln;
     wprev = wfl;
   }
 }
@@ -762,10 +769,14 @@ __global__ void __launch_bounds__(128) k_sweep_w2(Dev d, R dt, R splitfac, R* fa
   R hA = H(1), hB = H(2), hC = H(3);
   R wkm1 = W(0), wk = W(1), wk1 = W(2);
   R wpa = R(0), wpb = R(0);
+  // the carried errors (compensated storage) two levels ahead, like the window
+  auto LO = [&](const __half* l, int k) -> float { return (l && k <= kmax) ? __half2float(l[c + k * sk]) : 0.f; };
+  float la = LO(lo_a, 1), la1 = LO(lo_a, 2), lb = LO(lo_b, 1), lb1 = LO(lo_b, 2);
   for (int k = 1; k <= kmax; ++k) {
     const R an = FA(k + 4), bn = FB(k + 4);
     const R hn3 = H(k + 3);
     const R wn = W(k + 2);
+    const float lan = LO(lo_a, k + 2), lbn = LO(lo_b, k + 2);
     R wfa = R(0), wfb = R(0);
     if (k <= kmax - 1) {
       wfa = wface_s<R, S>(k, 0, kmax, dti, wk, a0, a1, a2, a3, hA, hB);
@@ -775,12 +786,16 @@ __global__ void __launch_bounds__(128) k_sweep_w2(Dev d, R dt, R splitfac, R* fa
     const R dh = dti * (wk - wkm1);
     const R hin = hio - dh;
     if (lo_a) {
-      fa[c + k * sk] = fv_update_lo<R>(hio, dh, hin, a1, dt, splitfac * (wfa - wpa), lo_a, c + k * sk);
+      float slo = la;
+      fa[c + k * sk] = fv_update_lo<R>(hio, dh, hin, a1, dt, splitfac * (wfa - wpa), slo);
+      lo_a[c + k * sk] = __float2half_rn(slo);
     } else {
       fa[c + k * sk] = fv_update<R>(hio, dh, hin, a1, dt, splitfac * (wfa - wpa));
     }
     if (lo_b) {
-      fb[c + k * sk] = fv_update_lo<R>(hio, dh, hin, b1, dt, splitfac * (wfb - wpb), lo_b, c + k * sk);
+      float slo = lb;
+      fb[c + k * sk] = fv_update_lo<R>(hio, dh, hin, b1, dt, splitfac * (wfb - wpb), slo);
+      lo_b[c + k * sk] = __float2half_rn(slo);
     } else {
       fb[c + k * sk] = fv_update<R>(hio, dh, hin, b1, dt, splitfac * (wfb - wpb));
     }
@@ -789,6 +804,8 @@ __global__ void __launch_bounds__(128) k_sweep_w2(Dev d, R dt, R splitfac, R* fa
     b0 = b1; b1 = b2; b2 = b3; b3 = b4; b4 = bn;
     hA = hB; hB = hC; hC = hn3;
     wkm1 = wk; wk = wk1; wk1 = wn;
+    la = la1; la1 = lan;
+    lb = lb1; lb1 = lbn;
     wpa = wfa;
     wpb = wfb;
   }
@@ -952,16 +969,21 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, VdSet<R, NF
   const long long sk = d.sk;
   // the new value of level k from the old one and the increment: a plain FP32 sum, or the
   // compensated sum of the carried error lo (the tracer's compensated storage)
-  auto new_level = [&](const VdField<R>& f, int k, R sold, R inc) -> R {
+  // (lin: the level's stored carried error, loaded ahead by the caller)
+  auto new_level = [&](const VdField<R>& f, int k, R sold, R inc, float lin) -> R {
     if constexpr (sizeof(R) == 4) {
       if (f.lo) {
-        float slo = __half2float(f.lo[c + k * sk]);
+        float slo = lin;
         const float v = add_comp_scaled(sold, inc, slo);
         f.lo[c + k * sk] = __float2half_rn(slo);
         return v;
       }
     }
     return sold + inc;
+  };
+  auto lo_at = [&](const VdField<R>& f, int k) -> float {
+    if constexpr (sizeof(R) == 4) return f.lo ? __half2float(f.lo[c + k * sk]) : 0.f;
+    else return 0.f;
   };
   auto put = [&](const VdField<R>& f, int k, R v) {
     f.S[c + k * sk] = v;
@@ -1070,33 +1092,38 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, VdSet<R, NF
     R a4 = incr ? (ao_k + an_k) * (Skp1 - S1) : Skp1 * ao_k + S1 * (h1 - ao_k);
     if (f.src) a4 = a4 + src_n[n];  // src(1)
     v[n] = (a4 - a3 * qu[n]) / (a2 - a3 * ru[n]);
-    put(f, 1, incr ? new_level(f, 1, S1, v[n]) : v[n]);
+    put(f, 1, incr ? new_level(f, 1, S1, v[n], lo_at(f, 1)) : v[n]);
   }
   // back substitution upwards, with the next level's coefficients loaded one step ahead
   R qn[NF], rn[NF], sn[NF], qn2[NF], rn2[NF], sn2[NF];
+  float ln[NF], ln2[NF];
 #pragma unroll
   for (int n = 0; n < NF; ++n) {
     const VdField<R>& f = F.t[n];
     qn[n] = kmax >= 2 ? f.QU[c + 2 * sk] : R(0);
     rn[n] = kmax >= 2 ? f.RU[c + 2 * sk] : R(0);
     sn[n] = (incr && kmax >= 2) ? f.Sin[c + 2 * sk] : R(0);
+    ln[n] = kmax >= 2 ? lo_at(f, 2) : 0.f;
     qn2[n] = kmax >= 3 ? f.QU[c + 3 * sk] : R(0);
     rn2[n] = kmax >= 3 ? f.RU[c + 3 * sk] : R(0);
     sn2[n] = (incr && kmax >= 3) ? f.Sin[c + 3 * sk] : R(0);
+    ln2[n] = kmax >= 3 ? lo_at(f, 3) : 0.f;
   }
   for (k = 2; k <= kmax; ++k) {
 #pragma unroll
     for (int n = 0; n < NF; ++n) {
       const VdField<R>& f = F.t[n];
       const R q = qn[n], r = rn[n], so = sn[n];
-      qn[n] = qn2[n]; rn[n] = rn2[n]; sn[n] = sn2[n];
+      const float lc = ln[n];
+      qn[n] = qn2[n]; rn[n] = rn2[n]; sn[n] = sn2[n]; ln[n] = ln2[n];
       if (k + 2 <= kmax) {
         qn2[n] = f.QU[c + (k + 2) * sk];
         rn2[n] = f.RU[c + (k + 2) * sk];
         if (incr) sn2[n] = f.Sin[c + (k + 2) * sk];
+        ln2[n] = lo_at(f, k + 2);
       }
       v[n] = q - r * v[n];
-      put(f, k, incr ? new_level(f, k, so, v[n]) : v[n]);
+      put(f, k, incr ? new_level(f, k, so, v[n], lc) : v[n]);
     }
   }
 }

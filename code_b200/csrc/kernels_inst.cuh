@@ -52,6 +52,7 @@ int run_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int sche
   SweepC<R> C = sweep_consts<R>(d, DIR, dt, splitfac, AH);
   if (du2d) C.skdu = 0;
   if (di2d) C.skdi = 0;
+  bool comp = false;  // set below: the sweep updates compensated storage
   const int nz = (nk + NKB - 1) / NKB;
   return dispatch_scheme(scheme, [&](auto sc) {
     constexpr int S = decltype(sc)::value;
@@ -79,8 +80,12 @@ int run_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int sche
           dim3 grd((nseg + UWB - 1) / UWB, d.nj(), nz);
           SweepC<R> Cu = C;
           Cu.adv_init = adv_init && adv ? 1 : 0;
-          k_sweep_u_vec<R, S, REC, NF><<<grd, blk, 0, s>>>(d, Cu, nk, set, Di_src, Di_dst, adv, U, DU, mflux,
-                                                           mupd, code);
+          if (comp)
+            k_sweep_u_vec<R, S, REC, NF, true><<<grd, blk, 0, s>>>(d, Cu, nk, set, Di_src, Di_dst, adv, U, DU,
+                                                                   mflux, mupd, code);
+          else
+            k_sweep_u_vec<R, S, REC, NF, false><<<grd, blk, 0, s>>>(d, Cu, nk, set, Di_src, Di_dst, adv, U, DU,
+                                                                    mflux, mupd, code);
           return (int)cudaGetLastError();
         }
         if (vec) {
@@ -92,8 +97,12 @@ int run_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int sche
             while (rows > 8 && nx * ((d.nj() + rows - 1) / rows) * nz * VKW < 148LL * 24) rows /= 2;
             dim3 blk(32, VKW, 1);
             dim3 grd((unsigned)nx, (d.nj() + rows - 1) / rows, (unsigned)nz);
-            k_sweep_v_vec<R, S, REC, NF, VN><<<grd, blk, 0, s>>>(d, C, nk, rows, set, Di_src, Di_dst, adv, U, DU,
-                                                                 mflux, mupd, code);
+            if (comp)
+              k_sweep_v_vec<R, S, REC, NF, VN, true><<<grd, blk, 0, s>>>(d, C, nk, rows, set, Di_src, Di_dst, adv,
+                                                                         U, DU, mflux, mupd, code);
+            else
+              k_sweep_v_vec<R, S, REC, NF, VN, false><<<grd, blk, 0, s>>>(d, C, nk, rows, set, Di_src, Di_dst, adv,
+                                                                          U, DU, mflux, mupd, code);
             return (int)cudaGetLastError();
           };
           // float4 lanes for one field; float2 lanes for a tracer pair (72 registers against 116:
@@ -130,6 +139,7 @@ int run_sweep_h(const Dev& d, cudaStream_t s, int nk, R dt, R splitfac, int sche
     };
     // compensated storage (lo) only where the arithmetic is FP32
     if (sizeof(R) == 8) lo = lo_b = nullptr;
+    comp = lo || lo_b;
     if (f_b) {
       TracerSet<R, 2> set{{{f, fi_src, fi_dst, lo}, {f_b, fi_src_b, fi_dst_b, lo_b}}};
       return go(std::false_type(), set);
@@ -311,6 +321,6 @@ template int run_adj_vdiff<GB_REAL>(const Dev&, cudaStream_t, GB_REAL, GB_REAL, 
 // ---- mode-split macro step (3D kernels) ----
 #include "bc_kernels.cuh"
 namespace gb {
-template int run_bc3<GB_REAL>(int, const Dev&, cudaStream_t, const Bc3<GB_REAL>&, GB_REAL* const*);
+template int run_bc3<GB_REAL>(int, const Dev&, cudaStream_t, const Bc3<GB_REAL>&, GB_REAL* const*, const GB_REAL*);
 template int run_col_heights<GB_REAL>(const Dev&, cudaStream_t, const Bc3<GB_REAL>&, GB_REAL*);
 }  // namespace gb

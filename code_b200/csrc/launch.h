@@ -150,8 +150,10 @@ enum {
 int run_nan_sweep(const Dev& d, cudaStream_t s, const double* z, unsigned long long* cnt);
 template <class R3>
 struct Bc3;
+// colh (may be null): the column-height planes of k_col_heights, which the FP32 momentum-advection
+// set-up (BC3_UVADV_PREP_UV) then reads in place of the 3D heights
 template <class R3>
-int run_bc3(int which, const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* const* scr);
+int run_bc3(int which, const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* const* scr, const R3* colh = nullptr);
 // the column heights of the macro step after sigma_coordinates (k_col_heights): NCOLH 2D planes
 // (COL_* in bc_common.cuh)
 template <class R3>

@@ -14,6 +14,7 @@
 // Each face flux and cell update evaluates the same expressions as the tile kernels of
 // kernels.cuh (face_flux_s, fv_update), so FP64 results are bit-identical to them.
 #pragma once
+#include <type_traits>
 #include "kernels.cuh"
 
 namespace gb {
@@ -57,26 +58,28 @@ __device__ __forceinline__ void st_row(R* p, bool full, int navail, const R (&v)
       if (m < navail) p[m] = v[m];
   }
 }
-// the scaled carried errors of N cells (compensated storage, FP16) as floats, and back
+// The carried errors of N cells (compensated storage, FP16) as one raw vector of N halves (8, 4
+// or 2 bytes), converted to and from floats.
 template <int N>
-__device__ __forceinline__ void ld_lo(const __half* p, bool full, int navail, float (&v)[N]) {
-  if (full && N == 4) {
-    const uint2 x = *reinterpret_cast<const uint2*>(p);
-    const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&x.x));
-    const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&x.y));
-    v[0] = a.x; v[1] = a.y; v[2 % N] = b.x; v[3 % N] = b.y;
-  } else {
+using LoVec = std::conditional_t<N == 4, uint2, std::conditional_t<N == 2, uint32_t, uint16_t>>;
+template <int N>
+__device__ __forceinline__ void lo_unpack(const LoVec<N>& x, float (&v)[N]) {
+  const __half* h = reinterpret_cast<const __half*>(&x);
 #pragma unroll
-    for (int m = 0; m < N; ++m) v[m] = m < navail ? __half2float(p[m]) : 0.f;
-  }
+  for (int m = 0; m < N; ++m) v[m] = __half2float(h[m]);
+}
+template <int N>
+__device__ __forceinline__ LoVec<N> lo_pack(const float (&v)[N]) {
+  LoVec<N> x;
+  __half* h = reinterpret_cast<__half*>(&x);
+#pragma unroll
+  for (int m = 0; m < N; ++m) h[m] = __float2half_rn(v[m]);
+  return x;
 }
 template <int N>
 __device__ __forceinline__ void st_lo(__half* p, bool full, int navail, const float (&v)[N]) {
-  if (full && N == 4) {
-    uint2 x;
-    *reinterpret_cast<__half2*>(&x.x) = __floats2half2_rn(v[0], v[1]);
-    *reinterpret_cast<__half2*>(&x.y) = __floats2half2_rn(v[2 % N], v[3 % N]);
-    *reinterpret_cast<uint2*>(p) = x;
+  if (full) {
+    *reinterpret_cast<LoVec<N>*>(p) = lo_pack<N>(v);
   } else {
 #pragma unroll
     for (int m = 0; m < N; ++m)
@@ -153,6 +156,18 @@ __device__ __forceinline__ void cp_async_v(void* smem, const void* gmem, int byt
   }
 }
 
+// The same for the raw carried-error vector of N cells (8 or 4 bytes; cp.async.ca), reading
+// `bytes` of it and zero-filling the rest.
+template <int N>
+__device__ __forceinline__ void cp_async_lo(void* smem, const void* gmem, int bytes) {
+  static_assert(N == 4 || N == 2, "carried errors of 4 or 2 cells");
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  if constexpr (N == 4)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes) : "memory");
+}
+
 // Each thread stages the inputs of its next steps in its own slots of a shared-memory ring
 // (slot [stage][array][thread]: a warp's 16-byte slots are contiguous) and reads back only what
 // it copied itself, so the pipeline needs no barrier; a slot is refilled one step after it was
@@ -168,7 +183,9 @@ __device__ __forceinline__ void lds_vec(const VecPack<R, N>& x, R (&v)[N]) {
 }
 
 // VN: cells per lane (16 bytes of R by default; 2 FP32 cells halve the registers of a lane)
-template <class R, int S, bool REC, int NF, int VN = 16 / sizeof(R)>
+// LO: the tracers carry compensated storage (F.t[n].lo; FP32 only), which the kernel then stages
+// and updates; without it the kernel holds none of that code
+template <class R, int S, bool REC, int NF, int VN = 16 / sizeof(R), bool LO = false>
 __global__ void __launch_bounds__(32 * VKW) k_sweep_v_vec(Dev d, SweepC<R> C, int nk, int rows, TracerSet<R, NF> F,
                                                         const R* Di_src, R* Di_dst, R* adv,
                                                         const R* __restrict__ V, const R* __restrict__ DV,
@@ -182,6 +199,8 @@ __global__ void __launch_bounds__(32 * VKW) k_sweep_v_vec(Dev d, SweepC<R> C, in
   constexpr int NA = NF == 1 ? 6 : NF + 3;
   constexpr int sub = (S == UPSTREAM) ? 0 : 1;
   __shared__ VecPack<R, N> sbuf[VST][NA][32 * VKW];
+  // the carried errors of the tracers (compensated storage), staged with the other inputs
+  __shared__ LoVec<N> slo[LO ? VST : 1][NF][32 * VKW];
   const int tid = threadIdx.y * 32 + threadIdx.x;
   const int ni = d.ni(), nj = d.nj();
   const int c0 = (blockIdx.x * 32 + threadIdx.x) * N;
@@ -226,6 +245,11 @@ __global__ void __launch_bounds__(32 * VKW) k_sweep_v_vec(Dev d, SweepC<R> C, in
       cp_async_v<VB>(&sbuf[st][XDV][tid], DV + (based + (long long)j * sj), vbytes);
       cp_async_v<VB>(&sbuf[st][XDI][tid], Di_src + (basei + (long long)j * sj), vbytes);
       if (NF == 1 && adv) cp_async_v<VB>(&sbuf[st][XAD][tid], adv + p, vbytes);
+      if constexpr (LO && (N == 2 || N == 4)) {
+#pragma unroll
+        for (int n = 0; n < NF; ++n)
+          if (F.t[n].lo) cp_async_lo<N>(&slo[st][n][tid], F.t[n].lo + p, vbytes / (int)sizeof(R) * 2);
+      }
     }
     cp_async_commit();
   };
@@ -336,8 +360,10 @@ __global__ void __launch_bounds__(32 * VKW) k_sweep_v_vec(Dev d, SweepC<R> C, in
     for (int n = 0; n < NF; ++n) {
       R fo[N];
       float lo[N];
-      const bool comp = F.t[n].lo && any;  // compensated storage: the cells' carried errors
-      if (comp) ld_lo<N>(F.t[n].lo + p, full, navail, lo);
+      const bool comp = LO && F.t[n].lo && any;  // compensated storage: the cells' carried errors
+      if constexpr (LO && (N == 2 || N == 4)) {
+        if (comp) lo_unpack<N>(slo[st][n][tid], lo);
+      }
 #pragma unroll
       for (int m = 0; m < N; ++m) {
         const bool upd = jin && mbit(mu, m);
@@ -373,7 +399,7 @@ __global__ void __launch_bounds__(32 * VKW) k_sweep_v_vec(Dev d, SweepC<R> C, in
 constexpr int UOWN = 30;
 constexpr int UWB = 4;  // warps (segments) per block
 
-template <class R, int S, bool REC, int NF>
+template <class R, int S, bool REC, int NF, bool LO = false>
 __global__ void __launch_bounds__(32 * UWB) k_sweep_u_vec(Dev d, SweepC<R> C, int nk, TracerSet<R, NF> F,
                                                         const R* Di_src, R* Di_dst, R* adv,
                                                         const R* __restrict__ U, const R* __restrict__ DU,
@@ -386,6 +412,8 @@ __global__ void __launch_bounds__(32 * UWB) k_sweep_u_vec(Dev d, SweepC<R> C, in
   constexpr int sub = (S == UPSTREAM) ? 0 : 1;
   constexpr unsigned FULL = 0xffffffffu;
   __shared__ VecPack<R, N> sbuf[VST][NA][32 * UWB];
+  // the carried errors of the tracers (compensated storage), staged with the other inputs
+  __shared__ LoVec<N> slo[LO ? VST : 1][NF][32 * UWB];
   const int lane = threadIdx.x;
   const int tid = threadIdx.y * 32 + lane;
   const int ni = d.ni();
@@ -448,6 +476,11 @@ __global__ void __launch_bounds__(32 * UWB) k_sweep_u_vec(Dev d, SweepC<R> C, in
       if (own) {
         cp_async16(&sbuf[st][XDI][tid], Di_src + (crow + (long long)k * C.skdi + cc), vbytes);
         if (NF == 1 && adv && any && !ainit) cp_async16(&sbuf[st][XAD][tid], adv + p, vbytes);
+        if constexpr (LO && (N == 2 || N == 4)) {
+#pragma unroll
+          for (int n = 0; n < NF; ++n)
+            if (F.t[n].lo && any) cp_async_lo<N>(&slo[st][n][tid], F.t[n].lo + p, vbytes / (int)sizeof(R) * 2);
+        }
       }
     }
     cp_async_commit();
@@ -537,8 +570,10 @@ __global__ void __launch_bounds__(32 * UWB) k_sweep_u_vec(Dev d, SweepC<R> C, in
         else ld_row<R, N>(F.t[n].fi_src + p, full, navail, fio);
       }
       float lo[N];
-      const bool comp = F.t[n].lo && any;  // compensated storage: the cells' carried errors
-      if (comp) ld_lo<N>(F.t[n].lo + p, full, navail, lo);
+      const bool comp = LO && F.t[n].lo && any;  // compensated storage: the cells' carried errors
+      if constexpr (LO && (N == 2 || N == 4)) {
+        if (comp) lo_unpack<N>(slo[stc][n][tid], lo);
+      }
 #pragma unroll
       for (int q = 0; q < N; ++q) {
         const R advn = cell_advn<R>(C, fl[n][q + 1], fl[n][q]);

@@ -126,8 +126,9 @@ int getm_set_fp32_micro_steps(int on);
 /* Process-wide choice of the micro-step launches (no counterpart in the reference: a tuning and
  * testing switch). on != 0 (the default): getm_time_loop without open boundaries runs sealevel and
  * depth_update as one launch per micro step, the new elevations alternating between the z and zo
- * arrays (at the end of the call z and zo hold what the separate launches leave), and the
- * mixed-precision micro step forms its bottom friction inside the momentum-advection kernels;
+ * arrays (at the end of the call z and zo hold what the separate launches leave), forms each
+ * Coriolis term inside the velocity update that reads it (the call's last term at its end), and
+ * the mixed-precision micro step forms its bottom friction inside the momentum-advection kernels;
  * on == 0: the separate launches. Both give identical results. Returns the previous setting. */
 int getm_set_fused_micro_step(int on);
 /* Human-readable text of the last error on this context (never NULL). */
