@@ -310,35 +310,23 @@ __global__ void k_momentum(Dev d, Bc2 s, Bc2W w) {
 
 // The mixed micro step's form of k_momentum: the same update with the elevation gradient's
 // difference zp - zm taken in FP64 (the elevations are FP64) and every other operation in FP32 on
-// the FP32 working copies (the Coriolis term with COR as well).
-template <int DIR, bool COR>
-__global__ void k_momentum_f32(Dev d, Bc2 s, Bc2W w) {
-  GB_IJ2
-  if (!interior(d, i, j)) return;
-  const long long c = d.ix(i, j);
-  const long long dn = DIR == 0 ? 1 : d.sj;  // the next T point along the component
-  if constexpr (COR) {
-    if (DIR == 0) {  // fV on U points from V
-      const float* V = w.w[V_];
-      if (w.m8[1][c] >= 1) {
-        const float Vloc = 0.25f * (V[c - d.sj] + V[c + 1 - d.sj] + V[c] + V[c + 1]);
-        w.w[FV][c] = float(s.f2[CORU][c]) * Vloc;
-      } else {
-        w.w[FV][c] = 0.f;
-      }
-    } else {  // fU on V points from U
-      const float* U = w.w[U_];
-      if (w.m8[2][c] >= 1) {
-        const float Uloc = 0.25f * (U[c - 1] + U[c] + U[c - 1 + d.sj] + U[c + d.sj]);
-        w.w[FU][c] = float(s.f2[CORV][c]) * Uloc;
-      } else {
-        w.w[FU][c] = 0.f;
-      }
-    }
-  }
+// the FP32 working copies (the Coriolis term with COR as well). Split into the Coriolis term and
+// the update of one point, which k_micro_tail shares.
+//
+// The Coriolis term of the DIR update at c (DIR 0: fV on U points from V at c-sj, c+1-sj, c, c+1;
+// DIR 1: fU on V points from U at c-1, c, c-1+sj, c+sj), given those four values in that order.
+template <int DIR>
+__device__ __forceinline__ float cor_term_f32(const Bc2& s, const Bc2W& w, long long c, float a, float b, float e,
+                                              float f) {
   const int m = DIR == 0 ? w.m8[1][c] : w.m8[2][c];
-  if (!(m == 1 || m == 2)) return;
-  float* X = w.w[DIR == 0 ? U_ : V_];
+  return m >= 1 ? float(s.f2[DIR == 0 ? CORU : CORV][c]) * (0.25f * (a + b + e + f)) : 0.f;
+}
+// The new velocity of the DIR update at an interior point c whose mask is 1 or 2, from its old value
+// Xo and the Coriolis term fCo.
+template <int DIR>
+__device__ __forceinline__ float momentum_new_f32(const Dev& d, const Bc2& s, const Bc2W& w, long long c, float Xo,
+                                                  float fCo) {
+  const long long dn = DIR == 0 ? 1 : d.sj;  // the next T point along the component
   const float* DX = w.w[DIR == 0 ? DU : DV];
   const float* D = w.w[D_];
   const float* airp = w.w[AIRP];
@@ -352,13 +340,32 @@ __global__ void k_momentum_f32(Dev d, Bc2 s, Bc2W w) {
   const double zm = fmax(z[c], -(double)H[c + dn] + fmin(min_depth, (double)D[c]));
   const float zx = (float(zp - zm) + (airp[c + dn] - airp[c]) * gammai) / float(DIR == 0 ? d.dx : d.dy);
   const float tau = 0.5f * (taus[c] + taus[c + dn]);
-  const float Xo = X[c], sl = w.w[DIR == 0 ? SLRU : SLRV][c];
+  const float sl = w.w[DIR == 0 ? SLRU : SLRV][c];
   const float Slr = Xo > 0.f ? fmaxf(sl, 0.f) : fminf(sl, 0.f);
-  const float DXo = DX[c], dryo = w.w[DIR == 0 ? DRY_U : DRY_V][c], fCo = w.w[DIR == 0 ? FV : FU][c],
-              Exo = w.w[DIR == 0 ? UEX : VEX][c], Slxo = w.w[DIR == 0 ? SLUX : SLVX][c],
-              ro = w.w[DIR == 0 ? RU : RV][c];
+  const float DXo = DX[c], dryo = w.w[DIR == 0 ? DRY_U : DRY_V][c], Exo = w.w[DIR == 0 ? UEX : VEX][c],
+              Slxo = w.w[DIR == 0 ? SLUX : SLVX][c], ro = w.w[DIR == 0 ? RU : RV][c];
   const float fc = DIR == 0 ? -fCo : fCo;
-  X[c] = (Xo - dtm * (g * DXo * zx + dryo * (-tau / rho_0 + fc + Exo + Slxo + Slr))) / (1.f + dtm * ro / DXo);
+  return (Xo - dtm * (g * DXo * zx + dryo * (-tau / rho_0 + fc + Exo + Slxo + Slr))) / (1.f + dtm * ro / DXo);
+}
+
+template <int DIR, bool COR>
+__global__ void k_momentum_f32(Dev d, Bc2 s, Bc2W w) {
+  GB_IJ2
+  if (!interior(d, i, j)) return;
+  const long long c = d.ix(i, j);
+  if constexpr (COR) {
+    if (DIR == 0) {  // fV on U points from V
+      const float* V = w.w[V_];
+      w.w[FV][c] = cor_term_f32<0>(s, w, c, V[c - d.sj], V[c + 1 - d.sj], V[c], V[c + 1]);
+    } else {  // fU on V points from U
+      const float* U = w.w[U_];
+      w.w[FU][c] = cor_term_f32<1>(s, w, c, U[c - 1], U[c], U[c - 1 + d.sj], U[c + d.sj]);
+    }
+  }
+  const int m = DIR == 0 ? w.m8[1][c] : w.m8[2][c];
+  if (!(m == 1 || m == 2)) return;
+  float* X = w.w[DIR == 0 ? U_ : V_];
+  X[c] = momentum_new_f32<DIR>(d, s, w, c, X[c], w.w[DIR == 0 ? FV : FU][c]);
 }
 
 // momentum.F90:193-216 / :356-379: Coriolis terms fU (after the U update) and fV (after V).
