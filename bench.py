@@ -66,11 +66,11 @@ def stage_words(stage: str, mixed: bool, compensated: bool) -> float:
         w = [a + b for a, b in zip(w, LO_WORDS.get(stage, [0] * len(w)))]
     return sum(w) / len(w)
 # DRAM bytes (read + write) per interior cell per launch of the FP32 stages, averaged over the
-# launches of the timed macro step of this workload (2048 x 2048 x 50): ncu --metrics
-# dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum (one pass) on the advection and
-# diffusion launches of `bench.py --steps 1 --warmup 1 --variants mixed --no-cpu-baseline
-# --adj-steps 0`.
-TRAFFIC_PER_CELL_F32 = {"adv_split_u": 28.01, "adv_split_v": 31.05, "adv_split_w": 20.94, "tracer_vdiff": 23.78}
+# stage's launches in one macro step: ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum (one
+# kernel, up to three launches) on the 1024 x 1024 x 32 case of this workload, scaled per cell
+# (v sweeps: four momentum launches at 25.6 and two tracer-pair launches at 34.6; w sweeps: two at
+# 21.2 and the pair at 28.2; diffusion: one launch for T and S at 46.5).
+TRAFFIC_PER_CELL_F32 = {"adv_split_v": 28.6, "adv_split_w": 23.5, "tracer_vdiff": 46.5}
 
 
 ERR_FIELDS = ("f3_T", "f3_S", "f3_uu", "f3_vv", "f2_z", "f2_U", "f2_V")
