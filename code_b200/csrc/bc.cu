@@ -525,149 +525,6 @@ __global__ void k_sealevel_depth(Dev d, Bc2 s, Bc2W w, int accumulate) {
   if (av(i, j) > 0) dry_v(i, j) = fmax(0.0, fmin(1.0, (DV_(i, j) - d1) * d2i));
 }
 
-// The mixed micro step after its momentum advection, in one launch (getm_time_loop without open
-// boundaries): both velocity updates (umomentum/vmomentum in the micro step's order, each forming
-// the Coriolis term it reads), sealevel and depth_update. The velocities, depths and drying
-// factors the launch writes go to a second set of working arrays (o) and the elevations to zo,
-// while every input is read from the current ones, so no block reads a value another block writes;
-// the caller swaps the sets (and z, zo) after the launch. A block owns an MTX x MTY tile and forms
-// the first-updated velocity F on the tile widened by the points that the second update's Coriolis
-// average and sealevel read, the second one G on the points sealevel reads, the new elevations on
-// the tile plus its next row and column (depth_update reads them), each from the same expressions
-// as k_momentum_f32 and k_sealevel_depth<true>, so the values are theirs bit for bit.
-struct MicroOut {
-  float *U, *V, *D, *DU, *DV, *dry_u, *dry_v;
-};
-constexpr int MTX = 32, MTY = 16;
-template <bool UFIRST, bool COR1>
-__global__ void __launch_bounds__(MTX * MTY) k_micro_tail(Dev d, Bc2 s, Bc2W w, MicroOut o, int accumulate) {
-  // velocities on the region origin (ii0-1, jj0-1); elevations on the origin (ii0, jj0)
-  __shared__ float sF[MTY + 3][MTX + 3], sG[MTY + 3][MTX + 3];
-  __shared__ double sZ[MTY + 1][MTX + 1];
-  constexpr int FD = UFIRST ? 0 : 1, GD = 1 - FD;  // 0: U, 1: V
-  constexpr int NT = MTX * MTY;
-  const int ni = d.ni(), nj = d.nj();
-  const int ii0 = blockIdx.x * MTX, jj0 = blockIdx.y * MTY;
-  const int tid = threadIdx.y * MTX + threadIdx.x;
-  const long long sj = d.sj;
-  auto own = [&](int x, int y) { return x >= ii0 && x < ii0 + MTX && y >= jj0 && y < jj0 + MTY && x < ni && y < nj; };
-  auto cix = [&](int x, int y) { return (long long)y * sj + x; };
-  auto iof = [&](int x) { return x + d.imin - HALO; };
-  auto jof = [&](int y) { return y + d.jmin - HALO; };
-  float* oF = FD == 0 ? o.U : o.V;
-  float* oG = GD == 0 ? o.U : o.V;
-  // ---- the first update on its region
-  {
-    const int x0 = ii0 - 1, x1 = UFIRST ? ii0 + MTX + 1 : ii0 + MTX + 2;
-    const int y0 = jj0 - 1, y1 = UFIRST ? jj0 + MTY + 2 : jj0 + MTY + 1;
-    const int W = x1 - x0, n = W * (y1 - y0);
-    const float* Fo = w.w[FD == 0 ? U_ : V_];
-    const float* Go = w.w[GD == 0 ? U_ : V_];
-    for (int q = tid; q < n; q += NT) {
-      const int x = x0 + q % W, y = y0 + q / W;
-      if (x < 0 || x >= ni || y < 0 || y >= nj) continue;
-      const long long c = cix(x, y);
-      float v = Fo[c];
-      if (interior(d, iof(x), jof(y))) {
-        float fC;
-        if (COR1) {
-          fC = FD == 0 ? cor_term_f32<0>(s, w, c, Go[c - sj], Go[c + 1 - sj], Go[c], Go[c + 1])
-                       : cor_term_f32<1>(s, w, c, Go[c - 1], Go[c], Go[c - 1 + sj], Go[c + sj]);
-          if (own(x, y)) w.w[FD == 0 ? FV : FU][c] = fC;
-        } else {
-          fC = w.w[FD == 0 ? FV : FU][c];
-        }
-        const int m = FD == 0 ? w.m8[1][c] : w.m8[2][c];
-        if (m == 1 || m == 2) v = momentum_new_f32<FD>(d, s, w, c, v, fC);
-      }
-      sF[y - y0][x - x0] = v;
-      if (own(x, y)) oF[c] = v;
-    }
-  }
-  __syncthreads();
-  // ---- the second update (its Coriolis term from the first one's new values)
-  {
-    const int x0 = UFIRST ? ii0 : ii0 - 1, x1 = ii0 + MTX + 1;
-    const int y0 = UFIRST ? jj0 - 1 : jj0, y1 = jj0 + MTY + 1;
-    const int W = x1 - x0, n = W * (y1 - y0);
-    const float* Go = w.w[GD == 0 ? U_ : V_];
-    // the first velocity's new value at (x, y) (region origin ii0-1, jj0-1)
-    auto F = [&](int x, int y) { return sF[y - (jj0 - 1)][x - (ii0 - 1)]; };
-    for (int q = tid; q < n; q += NT) {
-      const int x = x0 + q % W, y = y0 + q / W;
-      if (x < 0 || x >= ni || y < 0 || y >= nj) continue;
-      const long long c = cix(x, y);
-      float v = Go[c];
-      if (interior(d, iof(x), jof(y))) {
-        const float fC = GD == 0 ? cor_term_f32<0>(s, w, c, F(x, y - 1), F(x + 1, y - 1), F(x, y), F(x + 1, y))
-                                 : cor_term_f32<1>(s, w, c, F(x - 1, y), F(x, y), F(x - 1, y + 1), F(x, y + 1));
-        if (own(x, y)) w.w[GD == 0 ? FV : FU][c] = fC;
-        const int m = GD == 0 ? w.m8[1][c] : w.m8[2][c];
-        if (m == 1 || m == 2) v = momentum_new_f32<GD>(d, s, w, c, v, fC);
-      }
-      sG[y - (jj0 - 1)][x - (ii0 - 1)] = v;
-      if (own(x, y)) oG[c] = v;
-    }
-  }
-  __syncthreads();
-  auto Un = [&](int x, int y) { return UFIRST ? sF[y - (jj0 - 1)][x - (ii0 - 1)] : sG[y - (jj0 - 1)][x - (ii0 - 1)]; };
-  auto Vn = [&](int x, int y) { return UFIRST ? sG[y - (jj0 - 1)][x - (ii0 - 1)] : sF[y - (jj0 - 1)][x - (ii0 - 1)]; };
-  const double* zold = s.f2[Z];
-  const double dtm = s.par[P_DTM];
-  // ---- sealevel.F90:89-112 on the tile and its next row and column
-  {
-    const int W = MTX + 1, n = W * (MTY + 1);
-    for (int q = tid; q < n; q += NT) {
-      const int x = ii0 + q % W, y = jj0 + q / W;
-      if (x >= ni || y >= nj) continue;
-      const long long c = cix(x, y);
-      double z = zold[c];
-      if (interior(d, iof(x), jof(y)) && w.m8[0][c] == 1)
-        z = z - dtm * (((double)Un(x, y) * d.dy - (double)Un(x - 1, y) * d.dy) +
-                       ((double)Vn(x, y) * d.dx - (double)Vn(x, y - 1) * d.dx)) * d.ard1 +
-            dtm * w.w[FWF][c];
-      sZ[y - jj0][x - ii0] = z;
-    }
-  }
-  __syncthreads();
-  // ---- the own points: Uint/Vint, the new elevation, depth_update.F90:55-110
-  for (int q = tid; q < NT; q += NT) {
-    const int x = ii0 + q % MTX, y = jj0 + q / MTX;
-    if (x >= ni || y >= nj) continue;
-    const long long c = cix(x, y);
-    double* Uint = s.f2[UINT];
-    double* Vint = s.f2[VINT];
-    if (accumulate) {
-      Uint[c] = Uint[c] + Un(x, y);
-      Vint[c] = Vint[c] + Vn(x, y);
-    }
-    const double z0 = sZ[y - jj0][x - ii0];
-    s.f2[ZO][c] = z0;
-    const double min_depth = s.par[P_MIN_DEPTH], crit_depth = s.par[P_CRIT_DEPTH];
-    const float* H = w.w[HH];
-    const float* HU_ = w.w[HU];
-    const float* HV_ = w.w[HV];
-    const float Dn = float(z0 + H[c]);
-    o.D[c] = Dn;
-    float DUn = w.w[DU][c], DVn = w.w[DV][c];
-    if (iof(x) <= d.imax + HALO - 1) {
-      const double xx = fmax(0.25 * (zold[c] + zold[c + 1] + z0 + sZ[y - jj0][x + 1 - ii0]), -HU_[c] + min_depth);
-      DUn = float(xx + HU_[c]);
-    }
-    if (jof(y) <= d.jmax + HALO - 1) {
-      const double xx = fmax(0.25 * (zold[c] + zold[c + sj] + z0 + sZ[y + 1 - jj0][x - ii0]), -HV_[c] + min_depth);
-      DVn = float(xx + HV_[c]);
-    }
-    o.DU[c] = DUn;
-    o.DV[c] = DVn;
-    const double d1 = 2 * min_depth;
-    const double d2i = 1.0 / (crit_depth - 2 * min_depth);
-    if (w.m8[0][c] > 0) s.f2[DRY_Z][c] = fmax(0.0, fmin(1.0, ((double)Dn - 0.5 * d1) * d2i));
-    o.dry_u[c] = w.m8[1][c] > 0 ? float(fmax(0.0, fmin(1.0, ((double)DUn - d1) * d2i))) : w.w[DRY_U][c];
-    o.dry_v[c] = w.m8[2][c] > 0 ? float(fmax(0.0, fmin(1.0, ((double)DVn - d1) * d2i))) : w.w[DRY_V][c];
-  }
-}
-
 // exchanges the contents of two 2D FP64 arrays (the elevation ping-pong's last state)
 __global__ void k_swap2(long long n2, double* a, double* b) {
   for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n2; c += (long long)gridDim.x * blockDim.x) {
@@ -1285,10 +1142,8 @@ int momentum_2d(getm_ctx* ctx, const getm_bc_state* st, const Bc2W* wp, bool cor
 // m2d.F90:412-490 integrate_2d (closed boundaries; no residual; Am <= 0, An_method = 0)
 // zswap (the micro-step loop without open boundaries): sealevel and depth_update as one launch that
 // writes the new elevations into st->f2[ZO]; the caller then swaps st->f2[Z] and st->f2[ZO].
-// tail (with zswap, mixed step): the velocity updates, sealevel and depth_update as one launch
-// (k_micro_tail) writing into the second set of working arrays `tail`; the caller swaps the sets.
 int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop, const Bc2W* wp = nullptr, bool first = false,
-                 bool zswap = false, const MicroOut* tail = nullptr) {
+                 bool zswap = false) {
   const Dev& d = ctx->dev;
   const Bc2 s = to_bc2(st);
   int* ip = st->ipar;
@@ -1346,21 +1201,6 @@ int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop, const Bc2W* wp = nu
   // it gives the same value. The first update of a getm_time_loop call (first) reads the stored
   // term instead -- the state's fU/fV, which need not match the velocities (a start from rest of
   // the Coriolis terms) -- and getm_time_loop forms the term of the last update at its end.
-  if (tail && zswap && mix) {
-    TimerScope ts(ctx, GETM_TIM_BC2D);
-    const dim3 grd((d.ni() + MTX - 1) / MTX, (d.nj() + MTY - 1) / MTY, 1), blk(MTX, MTY, 1);
-    const int acc = ip[I_RUNTYPE] > 1 ? 1 : 0;
-    const bool u1 = ip[I_UFIRST2D] != 0;
-    if (u1 && !first) k_micro_tail<true, true><<<grd, blk, 0, ctx->stream>>>(d, s, w, *tail, acc);
-    else if (u1) k_micro_tail<true, false><<<grd, blk, 0, ctx->stream>>>(d, s, w, *tail, acc);
-    else if (!first) k_micro_tail<false, true><<<grd, blk, 0, ctx->stream>>>(d, s, w, *tail, acc);
-    else k_micro_tail<false, false><<<grd, blk, 0, ctx->stream>>>(d, s, w, *tail, acc);
-    const cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_fail(ctx, (int)e, "micro-step tail");
-    ip[I_UFIRST2D] = u1 ? 0 : 1;
-    std::swap(st->f2[Z], st->f2[ZO]);
-    return nan_sweep_due(ctx, st, loop);
-  }
   // the FP64 loop without open boundaries forms the Coriolis terms like the mixed step (zswap)
   auto umom = [&](bool cor) -> int { return momentum_2d<0>(ctx, st, wp, cor, zswap); };
   auto vmom = [&](bool cor) -> int { return momentum_2d<1>(ctx, st, wp, cor, zswap); };
@@ -2063,17 +1903,14 @@ static int time_loop(getm_ctx* ctx, getm_bc_state* st, int n0, int count, bool z
                    (ip[I_VEL2D_HOR] == NOADV ||
                     (ip[I_VEL2D_SPLIT] == GETM_HALFSPLIT && is_split_scheme(ip[I_VEL2D_HOR])));
   Bc2W w{};
-  MicroOut tail{};
   unsigned long long all = 0, written = 0, from3d = 0;
   if (mix) {
     const Dev& d = ctx->dev;
     const long long n2 = n2d(d);
     int nw = 0;
     for (int q = 0; q < NF2; ++q) nw += is_work2(q) ? 1 : 0;
-    // nw FP32 planes, the second set of the fields the micro-step tail writes (NTAIL planes), then
-    // the uint8 copies of az, au, av (3 planes, 16-byte aligned)
-    constexpr int NTAIL = 7;
-    const long long m8off = (long long)(nw + NTAIL) * n2 * (long long)sizeof(float);
+    // nw FP32 planes, then the uint8 copies of az, au, av (3 planes, 16-byte aligned)
+    const long long m8off = (long long)nw * n2 * (long long)sizeof(float);
     const long long m8pitch = (n2 + 15) / 16 * 16;
     if (!ctx->w2) {
       if (cudaMalloc(&ctx->w2, (size_t)(m8off + 3 * m8pitch)) != cudaSuccess) {
@@ -2085,10 +1922,6 @@ static int time_loop(getm_ctx* ctx, getm_bc_state* st, int n0, int count, bool z
     for (int q = 0; q < NF2; ++q) {
       w.w[q] = is_work2(q) ? ctx->w2 + (long long)(slot++) * n2 : nullptr;
       if (is_work2(q)) all |= 1ull << q;
-    }
-    {
-      float* t = ctx->w2 + (long long)nw * n2;
-      tail = MicroOut{t, t + n2, t + 2 * n2, t + 3 * n2, t + 4 * n2, t + 5 * n2, t + 6 * n2};
     }
     uint8_t* m8 = reinterpret_cast<uint8_t*>(ctx->w2) + m8off;
     for (int q = 0; q < 3; ++q) w.m8[q] = m8 + q * m8pitch;
@@ -2116,18 +1949,7 @@ static int time_loop(getm_ctx* ctx, getm_bc_state* st, int n0, int count, bool z
   if (mix && (rc = sync(all & ~((1ull << UEX) | (1ull << VEX)), 1))) return rc;
   bool dirty = false;  // working copies newer than the state
   for (int n = n0; n < n0 + count; ++n) {
-    const bool use_tail = mix && zswap;
-    if ((rc = integrate_2d(ctx, st, n, mix ? &w : nullptr, n == n0, zswap, use_tail ? &tail : nullptr))) return rc;
-    if (use_tail) {
-      // the tail wrote the new velocities, depths and drying factors into the second set
-      std::swap(w.w[U_], tail.U);
-      std::swap(w.w[V_], tail.V);
-      std::swap(w.w[D_], tail.D);
-      std::swap(w.w[DU], tail.DU);
-      std::swap(w.w[DV], tail.DV);
-      std::swap(w.w[DRY_U], tail.dry_u);
-      std::swap(w.w[DRY_V], tail.dry_v);
-    }
+    if ((rc = integrate_2d(ctx, st, n, mix ? &w : nullptr, n == n0, zswap))) return rc;
     dirty = mix;
     if (n % st->ipar[I_M] == 0) {
       if (mix && (rc = sync(written, 0))) return rc;
