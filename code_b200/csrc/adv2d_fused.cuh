@@ -51,14 +51,12 @@ struct Adv2dSmem {
 // TI: the storage type of U, V, DU, DV and Ex (FP64 state arrays, or the FP32 working copies of
 // the mixed-precision micro step)
 template <class T, int S, int DIR, class TI>
-__global__ void __launch_bounds__(FT) k_uvadv2d_fused(Dev d, T dt, const TI* __restrict__ U,
-                                                      const TI* __restrict__ V, const TI* __restrict__ DU,
-                                                      const TI* __restrict__ DV,
-                                                      const uint8_t* __restrict__ mflux_u,
-                                                      const uint8_t* __restrict__ mflux_v,
-                                                      const uint8_t* __restrict__ mupd_u,
-                                                      const uint8_t* __restrict__ mupd_v, TI* __restrict__ Ex,
-                                                      Bf2Args bf) {
+__device__ __forceinline__ void uvadv2d_tile(const Dev& d, T dt, const TI* __restrict__ U, const TI* __restrict__ V,
+                                             const TI* __restrict__ DU, const TI* __restrict__ DV,
+                                             const uint8_t* __restrict__ mflux_u,
+                                             const uint8_t* __restrict__ mflux_v,
+                                             const uint8_t* __restrict__ mupd_u, const uint8_t* __restrict__ mupd_v,
+                                             TI* __restrict__ Ex, const Bf2Args& bf) {
   extern __shared__ unsigned char smem_raw[];
   Adv2dSmem<T>& sm = *reinterpret_cast<Adv2dSmem<T>*>(smem_raw);
   const int ni = d.ni(), nj = d.nj();
@@ -78,7 +76,7 @@ __global__ void __launch_bounds__(FT) k_uvadv2d_fused(Dev d, T dt, const TI* __r
     if (iin && jj >= 0 && jj < nj) {
       const long long c = (long long)jj * sj + ii;
       if constexpr (sizeof(T) == 4 && sizeof(TI) == 4)
-        if (bf.r) oq = DIR == 0 ? float(V[c]) / float(DV[c]) : float(U[c]) / float(DU[c]);
+        if (bf.r) oq = DIR == 0 ? __fdividef(float(V[c]), float(DV[c])) : __fdividef(float(U[c]), float(DU[c]));
       a = mflux_u[c];
       b = mflux_v[c];
       c2 = mupd_u[c];
@@ -87,7 +85,11 @@ __global__ void __launch_bounds__(FT) k_uvadv2d_fused(Dev d, T dt, const TI* __r
       const long long cn = DIR == 0 ? c + 1 : c + sj;  // the next U (V) point
       const bool ok = DIR == 0 ? (ii <= ni - 2) : (jj <= nj - 2);
       if (ok) {
-        f0 = T(DIR == 0 ? U[c] / DU[c] : V[c] / DV[c]);
+        // FP32 working copies: the approximate division (2 ulp); FP64 arrays: the reference's quotient
+        if constexpr (sizeof(T) == 4 && sizeof(TI) == 4)
+          f0 = DIR == 0 ? __fdividef(U[c], DU[c]) : __fdividef(V[c], DV[c]);
+        else
+          f0 = T(DIR == 0 ? U[c] / DU[c] : V[c] / DV[c]);
         ua = T(0.5 * (U[c] + U[cn]));
         va = T(0.5 * (V[c] + V[cn]));
         dua = T(0.5 * (DU[c] + DU[cn]));
@@ -213,7 +215,7 @@ __global__ void __launch_bounds__(FT) k_uvadv2d_fused(Dev d, T dt, const TI* __r
         const long long c = (long long)jj * sj + ii;
         const int i = ii + d.imin - HALO, j = jj + d.jmin - HALO;
         const bool in = i >= d.imin && i <= d.imax && j >= d.jmin && j <= d.jmax;
-        const float q4 = 0.25f, h = 0.5f, kappa = bf.kappa, avmmol = bf.avmmol, min_depth = bf.min_depth;
+        const float q4 = 0.25f;
         float uloc, vloc, HHl;
         bool on;
         if (DIR == 0) {
@@ -222,8 +224,8 @@ __global__ void __launch_bounds__(FT) k_uvadv2d_fused(Dev d, T dt, const TI* __r
           vloc = in ? __fmul_rn(q4, __fadd_rn(__fadd_rn(__fadd_rn(sm.Q[r][q], sm.Q[r][q + 1]), sm.Q[r - 1][q]),
                                               sm.Q[r - 1][q + 1]))
                     : 0.f;
-          uloc = float(U[c]) / float(DU[c]);
-          HHl = fmaxf(min_depth, float(DU[c]));
+          uloc = __fdividef(float(U[c]), float(DU[c]));
+          HHl = fmaxf(bf.min_depth, float(DU[c]));
         } else {
           on = j <= d.jmax + HALO - 1 && bf.mask[c] > 0;
           if (!on) continue;
@@ -232,28 +234,44 @@ __global__ void __launch_bounds__(FT) k_uvadv2d_fused(Dev d, T dt, const TI* __r
                                            sm.Q[r + 1][q - 1]));
           else
             uloc = (i <= d.imax + HALO - 1 && bf.au[c] > 0) ? sm.Q[r][q] : 0.f;
-          vloc = float(V[c]) / float(DV[c]);
-          HHl = fmaxf(min_depth, float(DV[c]));
+          vloc = __fdividef(float(V[c]), float(DV[c]));
+          HHl = fmaxf(bf.min_depth, float(DV[c]));
         }
-        // explicitly rounded operations: this unit contracts multiply-adds, the separate kernel's
-        // does not
-        const float zb = float(bf.zb[c]);
-        const float sp = __fadd_rn(__fmul_rn(uloc, uloc), __fmul_rn(vloc, vloc));
-        float x = kappa / logf(__fadd_rn(zb, __fmul_rn(h, HHl)) / zb);
-        float rr = __fmul_rn(x, x);
-        if (bf.runtype == 1) {
-          const float fricvel = sqrtf(__fmul_rn(rr, sp));
-          const float zn = fminf(HHl, __fadd_rn(float(bf.zb0[c]), __fmul_rn(0.1f, avmmol) / fmaxf(avmmol, fricvel)));
-          bf.zb[c] = zn;
-          rr = __fadd_rn(zn, __fmul_rn(h, HHl)) / zn;
-          x = kappa / logf(rr);
-          rr = __fmul_rn(x, x);
-        }
-        bf.rr[c] = rr;
-        bf.r[c] = __fmul_rn(rr, sqrtf(sp));
+        const BfLaw b = bf_law_f32(bf.zb[c], bf.zb0[c], HHl, uloc, vloc, bf.kappa, bf.avmmol, bf.runtype);
+        if (bf.runtype == 1) bf.zb[c] = b.zn;
+        bf.rr[c] = b.rr;
+        bf.r[c] = b.r;
       }
     }
   }
+}
+
+template <class T, int S, int DIR, class TI>
+__global__ void __launch_bounds__(FT) k_uvadv2d_fused(Dev d, T dt, const TI* __restrict__ U,
+                                                      const TI* __restrict__ V, const TI* __restrict__ DU,
+                                                      const TI* __restrict__ DV,
+                                                      const uint8_t* __restrict__ mflux_u,
+                                                      const uint8_t* __restrict__ mflux_v,
+                                                      const uint8_t* __restrict__ mupd_u,
+                                                      const uint8_t* __restrict__ mupd_v, TI* __restrict__ Ex,
+                                                      Bf2Args bf) {
+  uvadv2d_tile<T, S, DIR, TI>(d, dt, U, V, DU, DV, mflux_u, mflux_v, mupd_u, mupd_v, Ex, bf);
+}
+
+// Both components in one launch (blockIdx.z = 0: UEx on the U grid, 1: VEx on the V grid): the
+// same tiles as two k_uvadv2d_fused launches, one grid, one tail.
+struct Adv2dMasks {
+  const uint8_t *mflux_u, *mflux_v, *mupd_u, *mupd_v;
+};
+template <class T, int S, class TI>
+__global__ void __launch_bounds__(FT) k_uvadv2d_both(Dev d, T dt, const TI* __restrict__ U, const TI* __restrict__ V,
+                                                     const TI* __restrict__ DU, const TI* __restrict__ DV,
+                                                     Adv2dMasks mu, Adv2dMasks mv, TI* __restrict__ UEx,
+                                                     TI* __restrict__ VEx, Bf2Args bfu, Bf2Args bfv) {
+  if (blockIdx.z == 0)
+    uvadv2d_tile<T, S, 0, TI>(d, dt, U, V, DU, DV, mu.mflux_u, mu.mflux_v, mu.mupd_u, mu.mupd_v, UEx, bfu);
+  else
+    uvadv2d_tile<T, S, 1, TI>(d, dt, U, V, DU, DV, mv.mflux_u, mv.mflux_v, mv.mupd_u, mv.mupd_v, VEx, bfv);
 }
 
 template <class T, int S, int DIR, class TI>
@@ -301,6 +319,23 @@ int run_uvadv2d_fused_f32(const Dev& d, cudaStream_t s, int dir, float dt, int s
                           const Bf2Args* bf) {
   return run_uvadv2d_fused_t<float, float>(d, s, dir, dt, scheme, U, V, DU, DV, mflux_u, mflux_v, mupd_u, mupd_v,
                                            Ex, bf ? *bf : Bf2Args{});
+}
+
+int run_uvadv2d_both_f32(const Dev& d, cudaStream_t s, float dt, int scheme, const float* U, const float* V,
+                         const float* DU, const float* DV, const uint8_t* const* mu, const uint8_t* const* mv,
+                         float* UEx, float* VEx, const Bf2Args* bfu, const Bf2Args* bfv) {
+  return dispatch_scheme(scheme, [&](auto sc) {
+    constexpr int S = decltype(sc)::value;
+    const size_t smem = sizeof(Adv2dSmem<float>);
+    const cudaError_t e = cudaFuncSetAttribute(k_uvadv2d_both<float, S, float>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return (int)e;
+    dim3 grd((d.ni() + FX - 1) / FX, (d.nj() + FY - 1) / FY, 2);
+    k_uvadv2d_both<float, S, float><<<grd, dim3(RW, FTY, 1), smem, s>>>(
+        d, dt, U, V, DU, DV, Adv2dMasks{mu[0], mu[1], mu[2], mu[3]}, Adv2dMasks{mv[0], mv[1], mv[2], mv[3]}, UEx,
+        VEx, bfu ? *bfu : Bf2Args{}, bfv ? *bfv : Bf2Args{});
+    return (int)cudaGetLastError();
+  });
 }
 #endif
 

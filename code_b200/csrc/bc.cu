@@ -120,7 +120,8 @@ __global__ void k_bottom_friction(Dev d, Bc2 s, Bc2W w, int runtype) {
 
 // FP32 form of k_bottom_friction on a 32x8 tile: the velocity quotients U/DU and V/DV of the tile
 // and its one-cell halo are formed once into shared memory (the 4-point averages of the U and V
-// points read them from there); the same operations as the per-thread form, so the same values.
+// points read them from there); the drag itself is bf_law_f32, as in the fused momentum advection.
+// MIX: the roughness arrays are the FP32 working copies.
 template <bool MIX>
 __global__ void __launch_bounds__(256) k_bottom_friction_f32t(Dev d, Bc2 s, Bc2W w, int runtype) {
   __shared__ float suq[10][34], svq[10][34];
@@ -135,8 +136,8 @@ __global__ void __launch_bounds__(256) k_bottom_friction_f32t(Dev d, Bc2 s, Bc2W
     const int ii = i0 - 1 + q, jj = j0 - 1 + r;
     float uq = 0.f, vq = 0.f;
     if (ii >= d.imin - HALO && ii <= d.imax + HALO && jj >= d.jmin - HALO && jj <= d.jmax + HALO) {
-      uq = float(U(ii, jj)) / float(DU_(ii, jj));
-      vq = float(V(ii, jj)) / float(DV_(ii, jj));
+      uq = __fdividef(float(U(ii, jj)), float(DU_(ii, jj)));
+      vq = __fdividef(float(V(ii, jj)), float(DV_(ii, jj)));
     }
     suq[r][q] = uq;
     svq[r][q] = vq;
@@ -150,51 +151,33 @@ __global__ void __launch_bounds__(256) k_bottom_friction_f32t(Dev d, Bc2 s, Bc2W
   auto rvv = f2a<MIX, RVV>(d, s, w);
   auto ru = f2a<MIX, RU>(d, s, w);
   auto rv = f2a<MIX, RV>(d, s, w);
-  W2 zub{d, s.f2[ZUB]}, zvb{d, s.f2[ZVB]}, zub0{d, s.f2[ZUB0]}, zvb0{d, s.f2[ZVB0]};
+  auto zub = f2a<MIX, ZUB>(d, s, w);
+  auto zvb = f2a<MIX, ZVB>(d, s, w);
+  auto zub0 = f2a<MIX, ZUB0>(d, s, w);
+  auto zvb0 = f2a<MIX, ZVB0>(d, s, w);
   M2 au{d, s.au}, av{d, s.av};
-  using T = float;
-  const T kappa = T(s.par[P_KAPPA]), avmmol = T(s.par[P_AVMMOL]), min_depth = T(s.par[P_MIN_DEPTH]);
-  const T q = T(0.25), h = T(0.5);
+  const float kappa = float(s.par[P_KAPPA]), avmmol = float(s.par[P_AVMMOL]), min_depth = float(s.par[P_MIN_DEPTH]);
+  const float q = 0.25f;
   const bool in = interior(d, i, j);
   if (i <= d.imax + HALO - 1 && au(i, j) > 0) {
-    const T vloc = in ? q * (VQ(0, 0) + VQ(1, 0) + VQ(0, -1) + VQ(1, -1)) : T(0);
-    const T uloc = UQ(0, 0);
-    const T HHl = fmax(min_depth, T(DU_(i, j)));
-    const T zb = T(zub(i, j));
-    T x = kappa / log((zb + h * HHl) / zb);
-    T r = x * x;
-    if (runtype == 1) {
-      const T fricvel = sqrt(r * (uloc * uloc + vloc * vloc));
-      const T zn = fmin(HHl, T(zub0(i, j)) + T(0.1) * avmmol / fmax(avmmol, fricvel));
-      zub(i, j) = zn;
-      r = (zn + h * HHl) / zn;
-      x = kappa / log(r);
-      r = x * x;
-    }
-    ruu(i, j) = r;
-    ru(i, j) = r * sqrt(uloc * uloc + vloc * vloc);
+    const float vloc = in ? __fmul_rn(q, __fadd_rn(__fadd_rn(__fadd_rn(VQ(0, 0), VQ(1, 0)), VQ(0, -1)), VQ(1, -1))) : 0.f;
+    const float HHl = fmaxf(min_depth, float(DU_(i, j)));
+    const BfLaw b = bf_law_f32(float(zub(i, j)), float(zub0(i, j)), HHl, UQ(0, 0), vloc, kappa, avmmol, runtype);
+    if (runtype == 1) zub(i, j) = b.zn;
+    ruu(i, j) = b.rr;
+    ru(i, j) = b.r;
   }
   if (j <= d.jmax + HALO - 1 && av(i, j) > 0) {
-    T uloc;
+    float uloc;
     if (in)
-      uloc = q * (UQ(0, 0) + UQ(-1, 0) + UQ(0, 1) + UQ(-1, 1));
+      uloc = __fmul_rn(q, __fadd_rn(__fadd_rn(__fadd_rn(UQ(0, 0), UQ(-1, 0)), UQ(0, 1)), UQ(-1, 1)));
     else
-      uloc = (i <= d.imax + HALO - 1 && au(i, j) > 0) ? UQ(0, 0) : T(0);
-    const T vloc = VQ(0, 0);
-    const T HHl = fmax(min_depth, T(DV_(i, j)));
-    const T zb = T(zvb(i, j));
-    T x = kappa / log((zb + h * HHl) / zb);
-    T r = x * x;
-    if (runtype == 1) {
-      const T fricvel = sqrt(r * (uloc * uloc + vloc * vloc));
-      const T zn = fmin(HHl, T(zvb0(i, j)) + T(0.1) * avmmol / fmax(avmmol, fricvel));
-      zvb(i, j) = zn;
-      r = (zn + h * HHl) / zn;
-      x = kappa / log(r);
-      r = x * x;
-    }
-    rvv(i, j) = r;
-    rv(i, j) = r * sqrt(uloc * uloc + vloc * vloc);
+      uloc = (i <= d.imax + HALO - 1 && au(i, j) > 0) ? UQ(0, 0) : 0.f;
+    const float HHl = fmaxf(min_depth, float(DV_(i, j)));
+    const BfLaw b = bf_law_f32(float(zvb(i, j)), float(zvb0(i, j)), HHl, uloc, VQ(0, 0), kappa, avmmol, runtype);
+    if (runtype == 1) zvb(i, j) = b.zn;
+    rvv(i, j) = b.rr;
+    rv(i, j) = b.r;
   }
 }
 
@@ -472,9 +455,12 @@ __global__ void k_depth_update(Dev d, Bc2 s, Bc2W w) {
 // exactly the reference's zo = z of sealevel.F90:89 and the caller swaps the two pointers after
 // the launch. The depths of a U (V) point need the new elevation of the next T point, which the
 // thread forms itself from the same inputs with the same expression (no thread reads a value
-// that another writes). Same values as the two kernels, bit for bit.
+// that another writes). Same values as the two kernels, bit for bit. flags: bit 0 accumulates
+// Uint/Vint; bit 1 writes the drying factor dry_z, which no micro-step kernel reads: the caller asks
+// for it on the micro steps whose state a macro step or the host reads next.
 template <bool MIX>
-__global__ void k_sealevel_depth(Dev d, Bc2 s, Bc2W w, int accumulate) {
+__global__ void k_sealevel_depth(Dev d, Bc2 s, Bc2W w, int flags) {
+  const int accumulate = flags & 1;
   GB_IJ2
   auto U = f2a<MIX, U_>(d, s, w);
   auto V = f2a<MIX, V_>(d, s, w);
@@ -520,7 +506,7 @@ __global__ void k_sealevel_depth(Dev d, Bc2 s, Bc2W w, int accumulate) {
   }
   const double d1 = 2 * min_depth;
   const double d2i = 1.0 / (crit_depth - 2 * min_depth);
-  if (az(i, j) > 0) dry_z(i, j) = fmax(0.0, fmin(1.0, (D(i, j) - 0.5 * d1) * d2i));
+  if ((flags & 2) && az(i, j) > 0) dry_z(i, j) = fmax(0.0, fmin(1.0, (D(i, j) - 0.5 * d1) * d2i));
   if (au(i, j) > 0) dry_u(i, j) = fmax(0.0, fmin(1.0, (DU_(i, j) - d1) * d2i));
   if (av(i, j) > 0) dry_v(i, j) = fmax(0.0, fmin(1.0, (DV_(i, j) - d1) * d2i));
 }
@@ -1141,9 +1127,11 @@ int momentum_2d(getm_ctx* ctx, const getm_bc_state* st, const Bc2W* wp, bool cor
 
 // m2d.F90:412-490 integrate_2d (closed boundaries; no residual; Am <= 0, An_method = 0)
 // zswap (the micro-step loop without open boundaries): sealevel and depth_update as one launch that
-// writes the new elevations into st->f2[ZO]; the caller then swaps st->f2[Z] and st->f2[ZO].
+// writes the new elevations into st->f2[ZO]; the caller then swaps st->f2[Z] and st->f2[ZO]. With
+// zswap, dryz = false leaves dry_z as it is (a micro step that neither a macro step nor the
+// caller follows).
 int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop, const Bc2W* wp = nullptr, bool first = false,
-                 bool zswap = false) {
+                 bool zswap = false, bool dryz = true) {
   const Dev& d = ctx->dev;
   const Bc2 s = to_bc2(st);
   int* ip = st->ipar;
@@ -1168,28 +1156,34 @@ int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop, const Bc2W* wp = nu
       GB_TRY(cudaMemsetAsync(w.w[UEX], 0, n2d(d) * sizeof(float), ctx->stream), "UEx=0");
       GB_TRY(cudaMemsetAsync(w.w[VEX], 0, n2d(d) * sizeof(float), ctx->stream), "VEx=0");
     } else {
+      // both components in one launch: UEx and VEx each read U, V, DU, DV only
+      const uint8_t* masks[2][4];
+      Bf2Args bf[2]{};
       for (int dir = 0; dir < 2; ++dir) {
         getm_adv_grid g;
         grid_for_tag(ctx, dir == 0 ? GETM_U_TAG : GETM_V_TAG, &g);
-        Bf2Args bf{};
+        masks[dir][0] = g.mask_uflux;
+        masks[dir][1] = g.mask_vflux;
+        masks[dir][2] = g.mask_uupdate;
+        masks[dir][3] = g.mask_vupdate;
         if (bf_fused) {
-          bf.mask = w.m8[dir == 0 ? 1 : 2];
-          bf.au = w.m8[1];
-          bf.zb = st->f2[dir == 0 ? ZUB : ZVB];
-          bf.zb0 = st->f2[dir == 0 ? ZUB0 : ZVB0];
-          bf.r = w.w[dir == 0 ? RU : RV];
-          bf.rr = w.w[dir == 0 ? RUU : RVV];
-          bf.kappa = float(st->par[P_KAPPA]);
-          bf.avmmol = float(st->par[P_AVMMOL]);
-          bf.min_depth = float(st->par[P_MIN_DEPTH]);
-          bf.runtype = ip[I_RUNTYPE];
+          bf[dir].mask = w.m8[dir == 0 ? 1 : 2];
+          bf[dir].au = w.m8[1];
+          bf[dir].zb = w.w[dir == 0 ? ZUB : ZVB];
+          bf[dir].zb0 = w.w[dir == 0 ? ZUB0 : ZVB0];
+          bf[dir].r = w.w[dir == 0 ? RU : RV];
+          bf[dir].rr = w.w[dir == 0 ? RUU : RVV];
+          bf[dir].kappa = float(st->par[P_KAPPA]);
+          bf[dir].avmmol = float(st->par[P_AVMMOL]);
+          bf[dir].min_depth = float(st->par[P_MIN_DEPTH]);
+          bf[dir].runtype = ip[I_RUNTYPE];
         }
-        GB_TIMED(GETM_TIM_BC2D,
-                 run_uvadv2d_fused_f32(d, ctx->stream, dir, float(st->par[P_DTM]), hor, w.w[U_], w.w[V_], w.w[DU],
-                                       w.w[DV], g.mask_uflux, g.mask_vflux, g.mask_uupdate, g.mask_vupdate,
-                                       w.w[dir == 0 ? UEX : VEX], bf_fused ? &bf : nullptr),
-                 "uv_advect");
       }
+      GB_TIMED(GETM_TIM_BC2D,
+               run_uvadv2d_both_f32(d, ctx->stream, float(st->par[P_DTM]), hor, w.w[U_], w.w[V_], w.w[DU], w.w[DV],
+                                    masks[0], masks[1], w.w[UEX], w.w[VEX], bf_fused ? &bf[0] : nullptr,
+                                    bf_fused ? &bf[1] : nullptr),
+               "uv_advect");
     }
   } else {
     rc = uv_advect_2d(ctx, st, st->f2[U_], st->f2[V_], st->f2[DU], st->f2[DV]);
@@ -1215,8 +1209,8 @@ int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop, const Bc2W* wp = nu
   // (m2d.F90:467-476); the accumulation does not touch z, so it runs inside the sealevel kernel
   if (zswap) {
     if (ctx->has_bdy) return fail(ctx, GETM_ERR_STATE, "integrate_2d: fused sealevel with open boundaries");
-    rc = mix ? k2(k_sealevel_depth<true>, d, s, w, ip[I_RUNTYPE] > 1 ? 1 : 0)
-             : k2(k_sealevel_depth<false>, d, s, w, ip[I_RUNTYPE] > 1 ? 1 : 0);
+    const int flags = (ip[I_RUNTYPE] > 1 ? 1 : 0) | (dryz ? 2 : 0);
+    rc = mix ? k2(k_sealevel_depth<true>, d, s, w, flags) : k2(k_sealevel_depth<false>, d, s, w, flags);
     if (rc) return cuda_fail(ctx, rc, "sealevel + depth_update");
     std::swap(st->f2[Z], st->f2[ZO]);
     return nan_sweep_due(ctx, st, loop);
@@ -1929,6 +1923,7 @@ static int time_loop(getm_ctx* ctx, getm_bc_state* st, int n0, int count, bool z
     GB_TRY(cudaGetLastError(), "uint8 masks");
     // written by the micro steps; written by the macro step and read by the micro steps
     for (int q : {U_, V_, D_, DU, DV, DRY_U, DRY_V, FU, FV, RU, RV, RUU, RVV, UEX, VEX}) written |= 1ull << q;
+    if (st->ipar[I_RUNTYPE] == 1) written |= (1ull << ZUB) | (1ull << ZVB);  // renewed by the bottom friction
     for (int q : {SLUX, SLVX, SLRU, SLRV, RU, RV}) from3d |= 1ull << q;
   }
   auto sync = [&](unsigned long long mask, int to_w) -> int {
@@ -1949,7 +1944,8 @@ static int time_loop(getm_ctx* ctx, getm_bc_state* st, int n0, int count, bool z
   if (mix && (rc = sync(all & ~((1ull << UEX) | (1ull << VEX)), 1))) return rc;
   bool dirty = false;  // working copies newer than the state
   for (int n = n0; n < n0 + count; ++n) {
-    if ((rc = integrate_2d(ctx, st, n, mix ? &w : nullptr, n == n0, zswap))) return rc;
+    const bool dryz = n % st->ipar[I_M] == 0 || n == n0 + count - 1;
+    if ((rc = integrate_2d(ctx, st, n, mix ? &w : nullptr, n == n0, zswap, dryz))) return rc;
     dirty = mix;
     if (n % st->ipar[I_M] == 0) {
       if (mix && (rc = sync(written, 0))) return rc;

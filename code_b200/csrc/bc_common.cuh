@@ -38,15 +38,17 @@ struct Bc2 {
 
 // The mixed-precision micro step keeps FP32 working copies of the 2D fields that the barotropic
 // kernels read and write every micro step (transports, depths, the momentum terms and the
-// forcing; the static depths H, HU, HV and the freshwater flux as read-only copies); the
-// elevation, the accumulated transports Uint/Vint, the bottom roughness and the Coriolis factors
-// stay FP64. The FP64 state is the authoritative copy between calls: the copies are filled at the
-// start of getm_time_loop and written back before each macro step and at the end.
+// forcing; the static depths H, HU, HV, the freshwater flux and the bottom roughness zub0/zvb0 as
+// read-only copies; the roughness zub/zvb, which the FP32 bottom friction reads as FP32 and renews
+// with FP32 values, written back only when it renews them); the elevation, the accumulated
+// transports Uint/Vint and the Coriolis factors stay FP64. The FP64 state is the authoritative
+// copy between calls: the copies are filled at the start of getm_time_loop and written back
+// before each macro step and at the end.
 constexpr bool is_work2(int q) {
   return q == U_ || q == V_ || q == D_ || q == DU || q == DV || q == DRY_U || q == DRY_V || q == FU || q == FV ||
          q == RU || q == RV || q == RUU || q == RVV || q == UEX || q == VEX || q == SLUX || q == SLVX ||
          q == SLRU || q == SLRV || q == TAUSX || q == TAUSY || q == AIRP || q == HH || q == HU || q == HV ||
-         q == FWF;
+         q == FWF || q == ZUB || q == ZVB || q == ZUB0 || q == ZVB0;
 }
 struct Bc2W {
   float* w[NF2];         // FP32 working copy of field q (used where is_work2(q))

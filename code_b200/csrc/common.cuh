@@ -80,4 +80,33 @@ __device__ __forceinline__ R recon(int scheme, R cfl, R fuu, R fu, R fd) {
   return fu;
 }
 
+// FP32 log-law bottom drag of one velocity point (bottom_friction.F90:86-103 / :121-138), shared by
+// every FP32 form of the bottom friction so that they give the same bits: from the roughness zb,
+// the point's depth HH and the velocity components, the drag coefficient rr and r = rr*|u|; with
+// runtype 1 the roughness is first renewed from the friction velocity (zn, which the caller
+// stores). Every operation is explicitly rounded (no dependence on multiply-add contraction); the
+// divisions outside the logarithm's argument are the approximate ones (2 ulp).
+struct BfLaw {
+  float zn, rr, r;
+};
+__device__ __forceinline__ BfLaw bf_law_f32(float zb, float zb0, float HH, float uloc, float vloc, float kappa,
+                                            float avmmol, int runtype) {
+  const float h = 0.5f;
+  const float sp = __fadd_rn(__fmul_rn(uloc, uloc), __fmul_rn(vloc, vloc));
+  float x = __fdividef(kappa, logf(__fdiv_rn(__fadd_rn(zb, __fmul_rn(h, HH)), zb)));
+  float rr = __fmul_rn(x, x);
+  BfLaw o;
+  o.zn = zb;
+  if (runtype == 1) {
+    const float fricvel = __fsqrt_rn(__fmul_rn(rr, sp));
+    const float zn = fminf(HH, __fadd_rn(zb0, __fdividef(__fmul_rn(0.1f, avmmol), fmaxf(avmmol, fricvel))));
+    o.zn = zn;
+    x = __fdividef(kappa, logf(__fdiv_rn(__fadd_rn(zn, __fmul_rn(h, HH)), zn)));
+    rr = __fmul_rn(x, x);
+  }
+  o.rr = rr;
+  o.r = __fmul_rn(rr, __fsqrt_rn(sp));
+  return o;
+}
+
 }  // namespace gb

@@ -59,13 +59,18 @@ int run_uvadv2d_fused(const Dev& d, cudaStream_t s, int dir, T dt, int scheme, c
 struct Bf2Args {
   const uint8_t* mask;  // au (DIR 0) / av (DIR 1), uint8 copies
   const uint8_t* au;    // DIR 1: the U points' mask for the velocity outside the interior
-  double* zb;           // zub / zvb
-  const double* zb0;    // zub0 / zvb0
+  float* zb;            // zub / zvb (FP32 working copies)
+  const float* zb0;     // zub0 / zvb0
   float* r;             // ru / rv (FP32 working copies)
   float* rr;            // ruu / rvv
   float kappa, avmmol, min_depth;
   int runtype;
 };
+// both components in one launch (mu / mv: the U and the V grid's flux-u, flux-v, update-u,
+// update-v masks; bfu / bfv: their bottom friction, may be null)
+int run_uvadv2d_both_f32(const Dev& d, cudaStream_t s, float dt, int scheme, const float* U, const float* V,
+                         const float* DU, const float* DV, const uint8_t* const* mu, const uint8_t* const* mv,
+                         float* UEx, float* VEx, const Bf2Args* bfu, const Bf2Args* bfv);
 // bf (may be null): also form the bottom friction of the micro step for this component's points
 int run_uvadv2d_fused_f32(const Dev& d, cudaStream_t s, int dir, float dt, int scheme, const float* U,
                           const float* V, const float* DU, const float* DV, const uint8_t* mflux_u,
