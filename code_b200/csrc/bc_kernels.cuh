@@ -428,17 +428,20 @@ __global__ void k_ip_sm(Dev d, Bc3<R3> s, const R3* zzp, const R3* Pp) {
 // in both. The elimination carries ru(k+1), qu(k+1) in registers and stores ru(k), qu(k) in two
 // scratch 3D arrays (RUs, QUs) so that occupancy is not limited by shared memory; the back
 // substitution overwrites QUs with Res(k) and the last pass writes uu = Res + hn*Diff.
-// The eleven inputs of a level (ho, hn, uu, num at the column and its neighbour, the other
-// velocity at the four points of its average, the advection term, the pressure gradient) are
-// staged by cp.async into the thread's own shared-memory slots two levels ahead of the
-// elimination (a ring of UVM_SLOTS levels), and the back substitution and the last pass load
-// ahead through registers, so the column's loads are in flight while its recurrence runs.
+// The layer heights (hun / hvn, which the reference passes as both the old and the new heights
+// here) are level-constant in sigma coordinates with equidistant layers, the only vertical grid
+// this kernel supports: the column's height is read once (at kmax) for every level. The nine
+// inputs of a level (uu, num at the column and its neighbour, the other velocity at the four
+// points of its average, the advection term, the pressure gradient) are staged by cp.async into
+// the thread's own shared-memory slots two levels ahead of the elimination (a ring of UVM_SLOTS
+// levels), and the back substitution and the last pass load ahead through registers, so the
+// column's loads are in flight while its recurrence runs.
 // SM: ru, qu (and the back substitution's Res) of the block's columns in dynamic shared memory
 // ([kmax+1][NT] each) instead of the scratch arrays -- FP32 with kmax < 64, where the columns fit
 // next to the staging ring at full occupancy of 64-thread blocks -- which removes their round
 // trips through DRAM.
 constexpr int UVM_SLOTS = 4;
-constexpr int UVM_IN = 11;
+constexpr int UVM_IN = 9;
 constexpr int UVM_THREADS = 128;
 template <class R3, int DIR, bool SM, int NT>
 __global__ void __launch_bounds__(NT) k_uvmom3d(Dev d, Bc3<R3> s, R3* RUs, R3* QUs) {
@@ -452,9 +455,9 @@ __global__ void __launch_bounds__(NT) k_uvmom3d(Dev d, Bc3<R3> s, R3* RUs, R3* Q
   if (i > d.imax || j > d.jmax) return;  // no barrier in this kernel
   I2 mask{d, DIR == 0 ? s.au : s.av};
   if (!(mask(i, j) == 1 || mask(i, j) == 2)) return;
-  V3<R3> uu{d, s.f3[DIR == 0 ? UU : VV]}, vv{d, s.f3[DIR == 0 ? VV : UU]}, ho{d, s.f3[DIR == 0 ? HUN : HVN]},
-      hn{d, s.f3[DIR == 0 ? HUN : HVN]}, Ex{d, s.f3[DIR == 0 ? UUEX : VVEX]}, idp{d, s.f3[DIR == 0 ? IDPDX : IDPDY]},
-      num{d, s.f3[NUM]}, RUg{d, RUs}, QUg{d, QUs};
+  V3<R3> uu{d, s.f3[DIR == 0 ? UU : VV]}, vv{d, s.f3[DIR == 0 ? VV : UU]}, hn{d, s.f3[DIR == 0 ? HUN : HVN]},
+      Ex{d, s.f3[DIR == 0 ? UUEX : VVEX]}, idp{d, s.f3[DIR == 0 ? IDPDX : IDPDY]}, num{d, s.f3[NUM]}, RUg{d, RUs},
+      QUg{d, QUs};
   R3* const sRU = reinterpret_cast<R3*>(uvm_cols);
   R3* const sQU = sRU + (long long)(d.kmax + 1) * NT;
   auto RU = [&](int, int, int k) -> R3& {
@@ -485,48 +488,47 @@ __global__ void __launch_bounds__(NT) k_uvmom3d(Dev d, Bc3<R3> s, R3* RUs, R3* Q
   auto issue = [&](int k) {
     if (k >= 0) {
       R3(*q)[NT] = sl[k & (UVM_SLOTS - 1)];
-      cp_async(&q[0][tid], &ho(i, j, k));
-      cp_async(&q[1][tid], &hn(i, j, k));
-      cp_async(&q[2][tid], &uu(i, j, k));
-      cp_async(&q[3][tid], &num(i, j, k));
-      cp_async(&q[4][tid], &num(i + di, j + dj, k));
+      cp_async(&q[0][tid], &uu(i, j, k));
+      cp_async(&q[1][tid], &num(i, j, k));
+      cp_async(&q[2][tid], &num(i + di, j + dj, k));
       if (DIR == 0) {
-        cp_async(&q[5][tid], &vv(i, j, k));
-        cp_async(&q[6][tid], &vv(i + 1, j, k));
-        cp_async(&q[7][tid], &vv(i, j - 1, k));
-        cp_async(&q[8][tid], &vv(i + 1, j - 1, k));
+        cp_async(&q[3][tid], &vv(i, j, k));
+        cp_async(&q[4][tid], &vv(i + 1, j, k));
+        cp_async(&q[5][tid], &vv(i, j - 1, k));
+        cp_async(&q[6][tid], &vv(i + 1, j - 1, k));
       } else {
-        cp_async(&q[5][tid], &vv(i, j, k));
-        cp_async(&q[6][tid], &vv(i - 1, j, k));
-        cp_async(&q[7][tid], &vv(i, j + 1, k));
-        cp_async(&q[8][tid], &vv(i - 1, j + 1, k));
+        cp_async(&q[3][tid], &vv(i, j, k));
+        cp_async(&q[4][tid], &vv(i - 1, j, k));
+        cp_async(&q[5][tid], &vv(i, j + 1, k));
+        cp_async(&q[6][tid], &vv(i - 1, j + 1, k));
       }
-      cp_async(&q[9][tid], &Ex(i, j, k));
-      cp_async(&q[10][tid], &idp(i, j, k));
+      cp_async(&q[7][tid], &Ex(i, j, k));
+      cp_async(&q[8][tid], &idp(i, j, k));
     }
     cp_async_commit();
   };
   auto in = [&](int k, int q) -> T { return T(sl[k & (UVM_SLOTS - 1)][q][tid]); };
-  auto HO = [&](int k) { return in(k, 0); };
-  auto HN = [&](int k) { return in(k, 1); };
-  auto UU_ = [&](int k) { return in(k, 2); };
+  const T hcol = T(hn(i, j, kmax));
+  auto HO = [&](int) { return hcol; };
+  auto HN = [&](int) { return hcol; };
+  auto UU_ = [&](int k) { return in(k, 0); };
   auto exk = [&](int k) {
     T loc, e;
     if (DIR == 0) {
-      loc = T(0.25) * (in(k, 5) + in(k, 6) + in(k, 7) + in(k, 8));
+      loc = T(0.25) * (in(k, 3) + in(k, 4) + in(k, 5) + in(k, 6));
       e = corij * loc;
     } else {
-      loc = T(0.25) * (in(k, 5) + in(k, 6) + in(k, 7) + in(k, 8));
+      loc = T(0.25) * (in(k, 3) + in(k, 4) + in(k, 5) + in(k, 6));
       e = -corij * loc;
     }
-    T x = dryij * (e - in(k, 9) + ip_t * in(k, 10));
+    T x = dryij * (e - in(k, 7) + ip_t * in(k, 8));
     if (k == kmax) {
       if constexpr (sizeof(T) == 8) x = x + dryij * 0.5 * (taus(i, j) + taus(i + di, j + dj)) * rho_0i;
       else x = x + taus_top;
     }
     return x;
   };
-  auto dif = [&](int k) { return T(0.5) * (in(k, 3) + in(k, 4)) + avm_t; };
+  auto dif = [&](int k) { return T(0.5) * (in(k, 1) + in(k, 2)) + avm_t; };
   issue(kmax);
   issue(kmax - 1);
   issue(kmax - 2);
@@ -609,13 +611,13 @@ __global__ void __launch_bounds__(NT) k_uvmom3d(Dev d, Bc3<R3> s, R3* RUs, R3* Q
   const double Diff = (Uint(i, j) - ResInt) / (sso(i, j) + HX(i, j));
   // last pass, four independent levels at a time
   for (k = 1; k + 3 <= kmax; k += 4) {
-    R3 q[4], h[4];
+    R3 q[4];
 #pragma unroll
-    for (int m = 0; m < 4; ++m) { q[m] = QU(i, j, k + m); h[m] = hn(i, j, k + m); }
+    for (int m = 0; m < 4; ++m) q[m] = QU(i, j, k + m);
 #pragma unroll
-    for (int m = 0; m < 4; ++m) uu(i, j, k + m) = R3((double)q[m] + (double)h[m] * Diff);
+    for (int m = 0; m < 4; ++m) uu(i, j, k + m) = R3((double)q[m] + (double)hcol * Diff);
   }
-  for (; k <= kmax; ++k) uu(i, j, k) = R3((double)QU(i, j, k) + (double)hn(i, j, k) * Diff);
+  for (; k <= kmax; ++k) uu(i, j, k) = R3((double)QU(i, j, k) + (double)hcol * Diff);
 }
 
 // sigma_coordinates.F90:85-113 (equidistant sigma): layer heights of all levels 0..kmax. A thread

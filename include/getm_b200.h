@@ -276,7 +276,10 @@ int getm_integrate_2d(getm_ctx *ctx, getm_bc_state *st, int loop);
  * coordinates, ww_momentum_3d, uv_advect_3d, stresses_3d, gotm (PARABOLIC_VISCOSITY when
  * viscosity = 1), do_temperature / do_salinity (advection + implicit vertical diffusion; with
  * radiation = 1 the short-wave and surface heat-flux sources of temperature), do_eqstate
- * (eqstate_method), slow_bottom_friction, uv_advect of Uint/Vint, slow_terms and stop_macro. */
+ * (eqstate_method), slow_bottom_friction, uv_advect of Uint/Vint, slow_terms and stop_macro.
+ * The vertical grid is sigma coordinates with equidistant layers: every level of a column has the
+ * same layer height (ho, hn, huo, hun, hvo, hvn), as sigma_coordinates and the initialisation
+ * produce them; the step reads a column's height once where it needs it for all levels. */
 int getm_integrate_3d(getm_ctx *ctx, getm_bc_state *st, int n);
 /* The micro-step loop of time_loop (src/getm/integration.F90:98-172) for n = n0..n0+count-1:
  * integrate_2d every step, integrate_3d when mod(n, M) == 0. */
