@@ -75,21 +75,12 @@ __global__ void k_zz(Dev d, Bc3<R3> s, R3* zzp) {
   if (az(i, j) < 1) return;
   V3<R3> hn{d, s.f3[HN]}, zz{d, zzp};
   V2 H{d, s.f2[HH]};
-  R3 z = R3(-H(i, j)) + hn(i, j, 1);
+  // equidistant sigma layers: the column's height, the same at every level
+  const R3 h = hn(i, j, d.kmax);
+  R3 z = R3(-H(i, j)) + h;
   zz(i, j, 1) = z;
-  int k = 2;
-  for (; k + 3 <= d.kmax; k += 4) {  // four levels' loads before their stores
-    R3 h[4];
-#pragma unroll
-    for (int m = 0; m < 4; ++m) h[m] = hn(i, j, k + m);
-#pragma unroll
-    for (int m = 0; m < 4; ++m) {
-      z = z + h[m];
-      zz(i, j, k + m) = z;
-    }
-  }
-  for (; k <= d.kmax; ++k) {
-    z = z + hn(i, j, k);
+  for (int k = 2; k <= d.kmax; ++k) {
+    z = z + h;
     zz(i, j, k) = z;
   }
 }
@@ -106,12 +97,14 @@ __global__ void k_ip(Dev d, Bc3<R3> s, const R3* zzp) {
   I2 au{d, s.au}, av{d, s.av};
   const int kmax = d.kmax;
   const R3 half = R3(0.5);
-  // one column: downward integral with hx the layer heights at the face, (oi, oj) the neighbour
-  // across it; four levels' loads are issued before their stores
+  // one column: downward integral with hx the layer heights at the face (level-constant with
+  // equidistant sigma layers: the column's height is read once), (oi, oj) the neighbour across
+  // it; four levels' loads are issued before their stores
   auto column = [&](V3<R3>& hx, V3<R3>& out, int oi, int oj, R3 dm1) {
     R3 grdl = (buoy(i + oi, j + oj, kmax) - buoy(i, j, kmax)) * dm1;
     R3 buoyl = half * (buoy(i + oi, j + oj, kmax) + buoy(i, j, kmax));
-    R3 hk1 = hx(i, j, kmax);
+    const R3 hc = hx(i, j, kmax);
+    R3 hk1 = hc;
     R3 prgr = grdl * half * hk1;
     out(i, j, kmax) = hk1 * prgr;
     auto level = [&](int k, R3 b1, R3 b0, R3 z1, R3 z0, R3 hk) {
@@ -126,19 +119,18 @@ __global__ void k_ip(Dev d, Bc3<R3> s, const R3* zzp) {
     };
     int k = kmax - 1;
     for (; k >= 4; k -= 4) {
-      R3 b1[4], b0[4], z1[4], z0[4], h[4];
+      R3 b1[4], b0[4], z1[4], z0[4];
 #pragma unroll
       for (int m = 0; m < 4; ++m) {
         b1[m] = buoy(i + oi, j + oj, k - m);
         b0[m] = buoy(i, j, k - m);
         z1[m] = zz(i + oi, j + oj, k - m);
         z0[m] = zz(i, j, k - m);
-        h[m] = hx(i, j, k - m);
       }
 #pragma unroll
-      for (int m = 0; m < 4; ++m) level(k - m, b1[m], b0[m], z1[m], z0[m], h[m]);
+      for (int m = 0; m < 4; ++m) level(k - m, b1[m], b0[m], z1[m], z0[m], hc);
     }
-    for (; k >= 1; --k) level(k, buoy(i + oi, j + oj, k), buoy(i, j, k), zz(i + oi, j + oj, k), zz(i, j, k), hx(i, j, k));
+    for (; k >= 1; --k) level(k, buoy(i + oi, j + oj, k), buoy(i, j, k), zz(i + oi, j + oj, k), zz(i, j, k), hc);
   };
   if (au(i, j) >= 1) column(hun, idpdx, 1, 0, R3(1.0 / d.dx));
   if (av(i, j) >= 1) column(hvn, idpdy, 0, 1, R3(1.0 / d.dy));
