@@ -9,7 +9,10 @@
 // x for two u/2 sweeps, 2 in y for the v sweep) in shared memory, runs u/2 on the tile+halo, v on
 // the tile widened in x, u/2 on the tile, and writes UEx once. Every flux and update is the
 // expression of the split-sweep kernels (face_flux_s, fv_update) in the same order, so FP64
-// results equal the three-sweep sequence bit for bit.
+// results equal the three-sweep sequence bit for bit. The u sweeps pass face fluxes between
+// neighbouring cells by warp shuffles (the two warps of a region row overlap by one column), the v
+// sweep through shared memory; each thread's own cells keep their depth and flux-divergence sum
+// in registers across the three sweeps.
 #pragma once
 #include "kernels.cuh"
 
@@ -38,10 +41,9 @@ template <class T>
 struct Adv2dSmem {
   T F0[RH][RW];   // advected quantity; reused for the field after the v sweep
   T F1[RH][RW];   // after the first u/2 sweep
-  T Di[RH][RW];   // control-volume depth, updated in place by each sweep
+  T Di[RH][RW];   // staged control-volume depth (the sweeps carry their rows' updated depths in registers)
   T Ua[RH][RW], DUa[RH][RW], Va[RH][RW], DVa[RH][RW];  // face transports / depths
-  T FL[RH][RW];   // face fluxes of the current sweep
-  T A[FY][FX];    // flux divergence of the own cells, summed over the sweeps (adv = 0 + u/2 + v + u/2)
+  T FL[RH][RW];   // face fluxes of the v sweep
   T Q[RH][RW];    // bottom friction: the other component's velocity V/DV (DIR 0) or U/DU (DIR 1)
   uint8_t mfu[RH][RW], mfv[RH][RW], mpu[RH][RW], mpv[RH][RW];
 };
@@ -108,112 +110,121 @@ __device__ __forceinline__ void uvadv2d_tile(const Dev& d, T dt, const TI* __res
     sm.mpu[r][q] = c2;
     sm.mpv[r][q] = e2;
   }
-  // own cells (r in [2, FY+2), q in [4, FX+4)): the flux-divergence sum
-  const bool qown = q >= 4 && q < FX + 4;
-  for (int r = ty; r < FY; r += FTY)
-    if (qown) sm.A[r][q - 4] = zero;
   __syncthreads();
-
+  // ---- the sweeps. A thread takes region column qc of the rows below; the two warps of a row
+  // overlap by one column (warp 0: qc = 0..31, warp 1: qc = 31..62; warp 1's copy of column 31,
+  // `dup`, updates and stores nothing), so that the left face flux of every cell a u sweep updates
+  // is the flux of the lane before it (a warp shuffle, no shared-memory round trip or barrier).
+  // The own rows of a thread, r = 2 + ty + 8m (m = 0, 1), are the same in all three sweeps: their
+  // depths and flux-divergence sums stay in registers.
+  const int qc = q - (q >> 5);
+  const bool dup = q == 32;
+  const int iic = ii0 - 4 + qc;
+  const bool qown = qc >= 4 && qc < FX + 4 && !dup;  // own cells q in [4, FX+4)
+  T di[2], acc[2] = {zero, zero};
   // ---- sweep 1: u/2 on rows r in [0, RH), cells q in [2, RW-2), faces q in [1, RW-3]
   {
     const T dti = half * dt, cdx = dti / dxu;
-    const int fa = ii0 - 4 + q;  // face between q and q+1
-    const bool fok = q >= 1 && q <= RW - 3 && fa >= sub && fa <= ni - 2 - sub;
-    if (q >= 1 && q <= RW - 3)
-      for (int r = ty; r < RH; r += FTY) {
-        T fl = zero;
-        if (fok)
-          fl = face_flux_s<T, S>(sm.Ua[r][q], sm.DUa[r][q], sm.F0[r][q - 1], sm.F0[r][q], sm.F0[r][q + 1],
-                                 sm.F0[r][q + 2], sm.mfu[r][q - 1] != 0, sm.mfu[r][q] != 0, sm.mfu[r][q + 1] != 0,
-                                 dti, cdx, zero, false, dxu);
-        sm.FL[r][q] = fl;
-      }
-    __syncthreads();
-    const bool cok = ii >= 1 + sub && ii <= ni - 2 - sub;
-    if (q >= 2 && q < RW - 2)
-      for (int r = ty; r < RH; r += FTY) {
-        const T fio = sm.F0[r][q];
+    const bool fok = qc >= 1 && qc <= RW - 3 && iic >= sub && iic <= ni - 2 - sub;  // face between qc, qc+1
+    const bool cok = iic >= 1 + sub && iic <= ni - 2 - sub;
+    const bool upd = qc >= 2 && qc < RW - 2 && !dup;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      // the own rows, then the halo rows 0, 1, RH-2, RH-1 (thread rows 0..3)
+      const int r = m < 2 ? 2 + ty + 8 * m : (ty < 2 ? ty : RH - 4 + ty);
+      if (m == 2 && ty >= 4) continue;
+      T fl = zero;
+      if (fok)
+        fl = face_flux_s<T, S>(sm.Ua[r][qc], sm.DUa[r][qc], sm.F0[r][qc - 1], sm.F0[r][qc], sm.F0[r][qc + 1],
+                               sm.F0[r][qc + 2], sm.mfu[r][qc - 1] != 0, sm.mfu[r][qc] != 0,
+                               sm.mfu[r][qc + 1] != 0, dti, cdx, zero, false, dxu);
+      const T flm = __shfl_up_sync(0xffffffffu, fl, 1);  // the face between qc-1 and qc
+      if (upd) {
+        const T fio = sm.F0[r][qc];
         T fnew = fio;
-        if (cok && sm.mpu[r][q]) {
-          const T Dio = sm.Di[r][q];
-          const T dD = diff_scaled<T>(dti, sm.Ua[r][q], sm.Ua[r][q - 1], dyu, ard1);
+        T Dio = sm.Di[r][qc];
+        if (cok && sm.mpu[r][qc]) {
+          const T dD = diff_scaled<T>(dti, sm.Ua[r][qc], sm.Ua[r][qc - 1], dyu, ard1);
           const T Dn = Dio - dD;
-          const T advn = diff_scaled<T>(half, sm.FL[r][q], sm.FL[r][q - 1], dyu, ard1);
-          sm.Di[r][q] = Dn;
+          const T advn = diff_scaled<T>(half, fl, flm, dyu, ard1);
           fnew = fv_update<T>(Dio, dD, Dn, fio, dt, advn);
-          if (qown && r >= 2 && r < FY + 2) sm.A[r - 2][q - 4] = add_r<T>(sm.A[r - 2][q - 4], advn);
+          Dio = Dn;
+          if (m < 2 && qown) acc[m] = add_r<T>(acc[m], advn);
         }
-        sm.F1[r][q] = fnew;
+        if (m < 2) di[m] = Dio;
+        sm.F1[r][qc] = fnew;
       }
+    }
     __syncthreads();
   }
   // ---- sweep 2: v on columns q in [2, RW-2), cells r in [2, RH-2), faces r in [1, RH-3]
   {
     const T dti = one * dt, cdy = dti / dyu;
-    if (q >= 2 && q < RW - 2)
+    const bool col = qc >= 2 && qc < RW - 2 && !dup;
+    if (col)
       for (int r = 1 + ty; r <= RH - 3; r += FTY) {
         const int fa = jj0 - 2 + r;  // face between r and r+1
         T fl = zero;
         if (fa >= sub && fa <= nj - 2 - sub)
-          fl = face_flux_s<T, S>(sm.Va[r][q], sm.DVa[r][q], sm.F1[r - 1][q], sm.F1[r][q], sm.F1[r + 1][q],
-                                 sm.F1[r + 2][q], sm.mfv[r - 1][q] != 0, sm.mfv[r][q] != 0, sm.mfv[r + 1][q] != 0,
-                                 dti, cdy, zero, false, dyu);
-        sm.FL[r][q] = fl;
+          fl = face_flux_s<T, S>(sm.Va[r][qc], sm.DVa[r][qc], sm.F1[r - 1][qc], sm.F1[r][qc], sm.F1[r + 1][qc],
+                                 sm.F1[r + 2][qc], sm.mfv[r - 1][qc] != 0, sm.mfv[r][qc] != 0,
+                                 sm.mfv[r + 1][qc] != 0, dti, cdy, zero, false, dyu);
+        sm.FL[r][qc] = fl;
       }
     __syncthreads();
-    if (q >= 2 && q < RW - 2)
-      for (int r = 2 + ty; r < RH - 2; r += FTY) {
+    if (col) {
+#pragma unroll
+      for (int m = 0; m < 2; ++m) {
+        const int r = 2 + ty + 8 * m;
         const int jj = jj0 - 2 + r;
-        const T fio = sm.F1[r][q];
+        const T fio = sm.F1[r][qc];
         T fnew = fio;
-        if (jj >= 1 + sub && jj <= nj - 2 - sub && sm.mpv[r][q]) {
-          const T Dio = sm.Di[r][q];
-          const T dD = diff_scaled<T>(dti, sm.Va[r][q], sm.Va[r - 1][q], dxu, ard1);
+        if (jj >= 1 + sub && jj <= nj - 2 - sub && sm.mpv[r][qc]) {
+          const T Dio = di[m];
+          const T dD = diff_scaled<T>(dti, sm.Va[r][qc], sm.Va[r - 1][qc], dxu, ard1);
           const T Dn = Dio - dD;
-          const T advn = diff_scaled<T>(one, sm.FL[r][q], sm.FL[r - 1][q], dxu, ard1);
-          sm.Di[r][q] = Dn;
+          const T advn = diff_scaled<T>(one, sm.FL[r][qc], sm.FL[r - 1][qc], dxu, ard1);
           fnew = fv_update<T>(Dio, dD, Dn, fio, dt, advn);
-          if (qown) sm.A[r - 2][q - 4] = add_r<T>(sm.A[r - 2][q - 4], advn);
+          if (qown) acc[m] = add_r<T>(acc[m], advn);
         }
-        sm.F0[r][q] = fnew;  // the field after v (F0 is no longer needed)
+        sm.F0[r][qc] = fnew;  // the field after v (F0 is no longer needed)
       }
+    }
     __syncthreads();
   }
-  // ---- sweep 3: u/2 on the own rows r in [2, RH-2), own cells q in [4, RW-4), faces q in [3, RW-5]
+  // ---- sweep 3: u/2 on the own rows, own cells q in [4, RW-4), faces q in [3, RW-5]
   {
     const T dti = half * dt, cdx = dti / dxu;
-    const int fa = ii0 - 4 + q;
-    const bool fok = fa >= sub && fa <= ni - 2 - sub;
-    if (q >= 3 && q <= RW - 5)
-      for (int r = 2 + ty; r < RH - 2; r += FTY) {
-        T fl = zero;
-        if (fok)
-          fl = face_flux_s<T, S>(sm.Ua[r][q], sm.DUa[r][q], sm.F0[r][q - 1], sm.F0[r][q], sm.F0[r][q + 1],
-                                 sm.F0[r][q + 2], sm.mfu[r][q - 1] != 0, sm.mfu[r][q] != 0, sm.mfu[r][q + 1] != 0,
-                                 dti, cdx, zero, false, dxu);
-        sm.FL[r][q] = fl;
-      }
-    __syncthreads();
-    if (qown)
-      for (int r = 2 + ty; r < RH - 2; r += FTY) {
+    const bool fok = qc >= 3 && qc <= RW - 5 && iic >= sub && iic <= ni - 2 - sub;
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+      const int r = 2 + ty + 8 * m;
+      T fl = zero;
+      if (fok)
+        fl = face_flux_s<T, S>(sm.Ua[r][qc], sm.DUa[r][qc], sm.F0[r][qc - 1], sm.F0[r][qc], sm.F0[r][qc + 1],
+                               sm.F0[r][qc + 2], sm.mfu[r][qc - 1] != 0, sm.mfu[r][qc] != 0,
+                               sm.mfu[r][qc + 1] != 0, dti, cdx, zero, false, dxu);
+      const T flm = __shfl_up_sync(0xffffffffu, fl, 1);
+      if (qown) {
         const int jj = jj0 - 2 + r;
-        T a = sm.A[r - 2][q - 4];
-        if (ii >= 1 + sub && ii <= ni - 2 - sub && jj < nj && sm.mpu[r][q]) {
-          const T advn = diff_scaled<T>(half, sm.FL[r][q], sm.FL[r][q - 1], dyu, ard1);
+        T a = acc[m];
+        if (iic >= 1 + sub && iic <= ni - 2 - sub && jj < nj && sm.mpu[r][qc]) {
+          const T advn = diff_scaled<T>(half, fl, flm, dyu, ard1);
           a = add_r<T>(a, advn);
         }
-        if (ii < ni && jj < nj) Ex[(long long)jj * sj + ii] = (TI)a;
+        if (iic < ni && jj < nj) Ex[(long long)jj * sj + iic] = (TI)a;
       }
+    }
   }
   if constexpr (sizeof(T) == 4 && sizeof(TI) == 4) {
     if (bf.r && qown) {
-      // F0 rows 2.. of the region still hold the staged U/DU (DIR 0) or V/DV (DIR 1) only where the
-      // v sweep left them: the own quotient is re-formed from the arrays (a single division)
-      for (int r = 2 + ty; r < RH - 2; r += FTY) {
+#pragma unroll
+      for (int m = 0; m < 2; ++m) {
+        const int r = 2 + ty + 8 * m;
         const int jj = jj0 - 2 + r;
-        if (ii >= ni || jj >= nj) continue;
-        const long long c = (long long)jj * sj + ii;
-        const int i = ii + d.imin - HALO, j = jj + d.jmin - HALO;
+        if (iic >= ni || jj >= nj) continue;
+        const long long c = (long long)jj * sj + iic;
+        const int i = iic + d.imin - HALO, j = jj + d.jmin - HALO;
         const bool in = i >= d.imin && i <= d.imax && j >= d.jmin && j <= d.jmax;
         const float q4 = 0.25f;
         float uloc, vloc, HHl;
@@ -221,8 +232,8 @@ __device__ __forceinline__ void uvadv2d_tile(const Dev& d, T dt, const TI* __res
         if (DIR == 0) {
           on = i <= d.imax + HALO - 1 && bf.mask[c] > 0;
           if (!on) continue;
-          vloc = in ? __fmul_rn(q4, __fadd_rn(__fadd_rn(__fadd_rn(sm.Q[r][q], sm.Q[r][q + 1]), sm.Q[r - 1][q]),
-                                              sm.Q[r - 1][q + 1]))
+          vloc = in ? __fmul_rn(q4, __fadd_rn(__fadd_rn(__fadd_rn(sm.Q[r][qc], sm.Q[r][qc + 1]), sm.Q[r - 1][qc]),
+                                              sm.Q[r - 1][qc + 1]))
                     : 0.f;
           uloc = __fdividef(float(U[c]), float(DU[c]));
           HHl = fmaxf(bf.min_depth, float(DU[c]));
@@ -230,10 +241,10 @@ __device__ __forceinline__ void uvadv2d_tile(const Dev& d, T dt, const TI* __res
           on = j <= d.jmax + HALO - 1 && bf.mask[c] > 0;
           if (!on) continue;
           if (in)
-            uloc = __fmul_rn(q4, __fadd_rn(__fadd_rn(__fadd_rn(sm.Q[r][q], sm.Q[r][q - 1]), sm.Q[r + 1][q]),
-                                           sm.Q[r + 1][q - 1]));
+            uloc = __fmul_rn(q4, __fadd_rn(__fadd_rn(__fadd_rn(sm.Q[r][qc], sm.Q[r][qc - 1]), sm.Q[r + 1][qc]),
+                                           sm.Q[r + 1][qc - 1]));
           else
-            uloc = (i <= d.imax + HALO - 1 && bf.au[c] > 0) ? sm.Q[r][q] : 0.f;
+            uloc = (i <= d.imax + HALO - 1 && bf.au[c] > 0) ? sm.Q[r][qc] : 0.f;
           vloc = __fdividef(float(V[c]), float(DV[c]));
           HHl = fmaxf(bf.min_depth, float(DV[c]));
         }
