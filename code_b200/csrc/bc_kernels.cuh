@@ -671,7 +671,10 @@ __global__ void __launch_bounds__(128) k_sigma_vec(Dev d, Bc3<float> s) {
     a2[m] = (float)((s.f2[SSVO][q] + s.f2[HV][q]) * kmaxm1);
     b2[m] = (float)((s.f2[SSVN][q] + s.f2[HV][q]) * kmaxm1);
   }
-  for (int k = 0; k <= d.kmax; ++k) {
+  // levels in gridDim.z chunks: more threads, each with fewer stores queued behind one another
+  const int kc = (d.kmax + 1 + gridDim.z - 1) / gridDim.z;
+  const int ka = blockIdx.z * kc, kb = min(d.kmax + 1, ka + kc);
+  for (int k = ka; k < kb; ++k) {
     const long long p = c + (long long)k * d.sk;
     st_row<float, N>(s.f3[HO] + p, nall == N, nall, a0);
     st_row<float, N>(s.f3[HN] + p, nall == N, nall, b0);
@@ -1294,7 +1297,7 @@ int run_bc3(int which, const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* cons
         bool ok = vector_sweeps_enabled() && d.sj % 4 == 0 && d.sk % 4 == 0;
         for (int f : {HO, HN, HUO, HUN, HVO, HVN}) ok = ok && reinterpret_cast<uintptr_t>(s.f3[f]) % 16 == 0;
         if (ok) {
-          const dim3 gv((d.ni() + 4 * 32 - 1) / (4 * 32), (d.nj() + 3) / 4, 1);
+          const dim3 gv((d.ni() + 4 * 32 - 1) / (4 * 32), (d.nj() + 3) / 4, 4);
           k_sigma_vec<4><<<gv, dim3(32, 4, 1), 0, st>>>(d, s);
           break;
         }
