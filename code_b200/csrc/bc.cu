@@ -1944,10 +1944,12 @@ static int time_loop(getm_ctx* ctx, getm_bc_state* st, int n0, int count, bool z
   if (mix && (rc = sync(all & ~((1ull << UEX) | (1ull << VEX)), 1))) return rc;
   bool dirty = false;  // working copies newer than the state
   for (int n = n0; n < n0 + count; ++n) {
-    const bool dryz = n % st->ipar[I_M] == 0 || n == n0 + count - 1;
+    // do_3d (integration.F90:106): a macro step after every M-th micro step, for runtype >= 2
+    const bool do_3d = st->ipar[I_RUNTYPE] >= 2 && n % st->ipar[I_M] == 0;
+    const bool dryz = do_3d || n == n0 + count - 1;
     if ((rc = integrate_2d(ctx, st, n, mix ? &w : nullptr, n == n0, zswap, dryz))) return rc;
     dirty = mix;
-    if (n % st->ipar[I_M] == 0) {
+    if (do_3d) {
       if (mix && (rc = sync(written, 0))) return rc;
       dirty = false;
       rc = st->prec3d == 8 ? integrate_3d<double>(ctx, st, n) : integrate_3d<float>(ctx, st, n);

@@ -425,9 +425,9 @@ __global__ void k_ip_sm(Dev d, Bc3<R3> s, const R3* zzp, const R3* Pp) {
 // this kernel supports: the column's height is read once (at kmax) for every level. The nine
 // inputs of a level (uu, num at the column and its neighbour, the other velocity at the four
 // points of its average, the advection term, the pressure gradient) are staged by cp.async into
-// the thread's own shared-memory slots two levels ahead of the elimination (a ring of UVM_SLOTS
-// levels), and the back substitution and the last pass load ahead through registers, so the
-// column's loads are in flight while its recurrence runs.
+// the thread's own shared-memory slots ahead of the elimination (a ring of SL levels, SL - 2 of
+// them in flight), and the back substitution and the last pass load ahead through registers, so
+// the column's loads are in flight while its recurrence runs.
 // SM: ru, qu (and the back substitution's Res) of the block's columns in dynamic shared memory
 // ([kmax+1][NT] each) instead of the scratch arrays -- FP32 with kmax < 64, where the columns fit
 // next to the staging ring at full occupancy of 64-thread blocks -- which removes their round
@@ -435,10 +435,11 @@ __global__ void k_ip_sm(Dev d, Bc3<R3> s, const R3* zzp, const R3* Pp) {
 constexpr int UVM_SLOTS = 4;
 constexpr int UVM_IN = 9;
 constexpr int UVM_THREADS = 128;
-template <class R3, int DIR, bool SM, int NT>
+template <class R3, int DIR, bool SM, int NT, int SL = UVM_SLOTS>
 __global__ void __launch_bounds__(NT) k_uvmom3d(Dev d, Bc3<R3> s, R3* RUs, R3* QUs) {
   using T = R3;
-  __shared__ R3 sl[UVM_SLOTS][UVM_IN][NT];
+  static_assert(SL == 4 || SL == 8, "a ring of 4 or 8 levels");
+  __shared__ R3 sl[SL][UVM_IN][NT];
   extern __shared__ unsigned char uvm_cols[];
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   const int kmax = d.kmax;
@@ -479,7 +480,7 @@ __global__ void __launch_bounds__(NT) k_uvmom3d(Dev d, Bc3<R3> s, R3* RUs, R3* Q
   // the level's inputs into slot k % UVM_SLOTS (an empty group for k < 0 keeps the counting uniform)
   auto issue = [&](int k) {
     if (k >= 0) {
-      R3(*q)[NT] = sl[k & (UVM_SLOTS - 1)];
+      R3(*q)[NT] = sl[k & (SL - 1)];
       cp_async(&q[0][tid], &uu(i, j, k));
       cp_async(&q[1][tid], &num(i, j, k));
       cp_async(&q[2][tid], &num(i + di, j + dj, k));
@@ -499,7 +500,7 @@ __global__ void __launch_bounds__(NT) k_uvmom3d(Dev d, Bc3<R3> s, R3* RUs, R3* Q
     }
     cp_async_commit();
   };
-  auto in = [&](int k, int q) -> T { return T(sl[k & (UVM_SLOTS - 1)][q][tid]); };
+  auto in = [&](int k, int q) -> T { return T(sl[k & (SL - 1)][q][tid]); };
   const T hcol = T(hn(i, j, kmax));
   auto HO = [&](int) { return hcol; };
   auto HN = [&](int) { return hcol; };
@@ -521,9 +522,8 @@ __global__ void __launch_bounds__(NT) k_uvmom3d(Dev d, Bc3<R3> s, R3* RUs, R3* Q
     return x;
   };
   auto dif = [&](int k) { return T(0.5) * (in(k, 1) + in(k, 2)) + avm_t; };
-  issue(kmax);
-  issue(kmax - 1);
-  issue(kmax - 2);
+#pragma unroll
+  for (int m = 0; m <= SL - 2; ++m) issue(kmax - m);
   const T c_o = T(2.0 * (1.0 - cnpar) * dt), c_n = T(2.0 * cnpar * dt);
   const double zp = fmax(sseo(i + di, j + dj), -H(i, j) + fmin(min_depth, D(i + di, j + dj)));
   const double zm = fmax(sseo(i, j), -H(i + di, j + dj) + fmin(min_depth, D(i, j)));
@@ -533,7 +533,7 @@ __global__ void __launch_bounds__(NT) k_uvmom3d(Dev d, Bc3<R3> s, R3* RUs, R3* Q
   else
     zx = (zp - zm + (airp(i, j + 1) - airp(i, j)) / gamma) / d.dy;
   const T zx_t = T(zx);
-  cp_async_wait<1>();  // levels kmax and kmax-1
+  cp_async_wait<SL - 3>();  // levels kmax and kmax-1
   // column window: heights and velocity at k-1, k, k+1
   int k = kmax;
   T hok = HO(k), hnk = HN(k), hokm1 = HO(k - 1), hnkm1 = HN(k - 1);
@@ -552,8 +552,8 @@ __global__ void __launch_bounds__(NT) k_uvmom3d(Dev d, Bc3<R3> s, R3* RUs, R3* Q
     QU(i, j, k) = R3(qu);
   }
   for (k = kmax - 1; k >= 2; --k) {
-    issue(k - 2);          // into the slot of level k+2, last read in the iteration of level k+2
-    cp_async_wait<1>();    // level k-1
+    issue(k - (SL - 2));      // into the slot of level k+2, last read in the iteration of level k+2
+    cp_async_wait<SL - 3>();  // level k-1
     const T ao_k = ao_km1, an_k = an_km1;
     hokp1 = hok; hnkp1 = hnk; ukp1 = uk;
     hok = hokm1; hnk = hnkm1; uk = ukm1;
@@ -1275,10 +1275,13 @@ int run_bc3(int which, const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* cons
           const dim3 b2(32, 2, 1);
           const dim3 g2((nx + 31) / 32, (ny + 1) / 2, 1);
           const size_t dyn = 2 * (size_t)(d.kmax + 1) * NT * sizeof(R3);
-          if (which == BC3_UUMOM)
-            k_uvmom3d<R3, 0, true, NT><<<g2, b2, dyn, st>>>(d, s, scr[0], scr[1]);
-          else
-            k_uvmom3d<R3, 1, true, NT><<<g2, b2, dyn, st>>>(d, s, scr[0], scr[1]);
+          // a ring of eight levels (six in flight ahead of the elimination): with the coefficients
+          // in shared memory a block of 64 columns holds few warps, so each column keeps more of
+          // its loads in flight; above 48 KB of shared memory per block the launch opts in
+          auto kern = which == BC3_UUMOM ? k_uvmom3d<R3, 0, true, NT, 8> : k_uvmom3d<R3, 1, true, NT, 8>;
+          const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+          if (e != cudaSuccess) return (int)e;
+          kern<<<g2, b2, dyn, st>>>(d, s, scr[0], scr[1]);
           done = true;
         }
       }

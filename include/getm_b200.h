@@ -282,7 +282,8 @@ int getm_integrate_2d(getm_ctx *ctx, getm_bc_state *st, int loop);
  * produce them; the step reads a column's height once where it needs it for all levels. */
 int getm_integrate_3d(getm_ctx *ctx, getm_bc_state *st, int n);
 /* The micro-step loop of time_loop (src/getm/integration.F90:98-172) for n = n0..n0+count-1:
- * integrate_2d every step, integrate_3d when mod(n, M) == 0. */
+ * integrate_2d every step, integrate_3d when runtype >= 2 and mod(n, M) == 0 (do_3d,
+ * integration.F90:106). */
 int getm_time_loop(getm_ctx *ctx, getm_bc_state *st, int n0, int count);
 
 /* ---- the substeps of the mode-split step, one by one ------------------------------------

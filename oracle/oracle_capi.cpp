@@ -216,7 +216,8 @@ static gor::BcState<R3> to_state(or_bc* s, gor::Bdy* bdy) {
 }  // extern "C++"
 
 // time_loop (integration.F90:98-172): micro steps n = n0 .. n0+count-1, integrate_2d every step and
-// integrate_3d when mod(n, M) == 0. The SAVEd momentum toggles are carried in ipar.
+// integrate_3d when do_3d = (runtype >= 2 and mod(n, M) == 0) (integration.F90:106). The SAVEd
+// momentum toggles are carried in ipar.
 extern "C++" {
 template <class R3>
 static long long bc_steps(const or_dom* o, or_bc* s, int n0, int count) {
@@ -227,7 +228,7 @@ static long long bc_steps(const or_dom* o, or_bc* s, int n0, int count) {
   gor::BcState<R3> st = to_state<R3>(s, &bdy);
   for (int n = n0; n < n0 + count; ++n) {
     if (gor::integrate_2d(d, m, st, n) != 0) return -1;
-    if (n % st.ipar[gor::I_M] == 0)
+    if (st.ipar[gor::I_RUNTYPE] >= 2 && n % st.ipar[gor::I_M] == 0)
       if (gor::integrate_3d(d, m, st, n) != 0) return -1;
   }
   for (int q = 0; q < gor::NPI; ++q) s->ipar[q] = st.ipar[q];

@@ -73,6 +73,56 @@ def test_time_loop_vs_oracle(recipe, nx, ny, kmax):
     assert ctx.take_warnings() == 0
 
 
+def test_barotropic_runtype_vs_oracle():
+    """runtype 1 (barotropic only): the time loop runs no macro step (do_3d, integration.F90:106),
+    the bottom friction renews the roughness zub/zvb every MM micro steps and Uint/Vint are not
+    accumulated; FP64 against the oracle, and the 3D fields left as they were."""
+    c = S.baroclinic_case(nx=48, ny=40, kmax=8, recipe="islands", M=5, dt3=60.0, seed=11, land=0.3)
+    c.pi["runtype"] = 1
+    ref = c.copy()
+    oracle.bc_steps(ref, 1, 17)
+    out, ctx = run_gpu(c, 1, 17)
+    bad, worst = compare(out, ref.f2, ref.f3, 1e-12)
+    assert not bad, bad
+    for k in S.F3_NAMES:
+        assert np.array_equal(out.f3[k], c.f3[k], equal_nan=True), k
+    assert not np.array_equal(out.f2["zub"], c.f2["zub"])  # renewed
+    assert ctx.take_warnings() == 0
+
+
+@pytest.mark.parametrize("runtype", [1, 4])
+def test_mixed_roughness_working_copies(runtype):
+    """The mixed micro steps keep the bottom roughness as FP32 working copies: with runtype 1 the
+    FP32 bottom friction renews it and the new values come back to the state (the fused and the
+    separate launches give the same bits, within 1e-5 of the FP64 run); with runtype 4 it is only
+    read, and the state's FP64 roughness stays bit for bit what it was."""
+    import torch
+
+    from code_b200 import getm as G
+
+    c = S.baroclinic_case(nx=77, ny=53, kmax=8, recipe="islands", land=0.3, M=5, dt3=60.0, seed=4)
+    c.pi["runtype"] = runtype
+    ref = c.copy()
+    oracle.bc_steps(ref, 1, 23)
+    c32 = c.copy(dtype3=np.float32)
+    out = {}
+    prev = G.set_fused_micro_step(True)
+    try:
+        for on in (True, False):
+            G.set_fused_micro_step(on)
+            out[on], _ = run_gpu(c32, 1, 23, dtype3=torch.float32)
+    finally:
+        G.set_fused_micro_step(prev)
+    for k in S.F2_NAMES:
+        assert np.array_equal(out[True].f2[k], out[False].f2[k], equal_nan=True), k
+    for k in ("zub", "zvb"):
+        if runtype == 1:
+            assert field_err(out[True].f2[k], ref.f2[k]) <= 1e-5, k
+            assert not np.array_equal(out[True].f2[k], c.f2[k]), k
+        else:
+            assert np.array_equal(out[True].f2[k], c.f2[k]), k
+
+
 def tidal_shelf(nx=40, ny=28, kmax=10, M=5, period=900.0, seed=11):
     """The shelf configuration with its western side open and clamped to a tide (1 m amplitude;
     the period is shortened from M2 so that the test sees a full cycle), ramped over 40 micro
