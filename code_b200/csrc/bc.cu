@@ -294,7 +294,8 @@ __global__ void k_momentum(Dev d, Bc2 s, Bc2W w) {
 // The mixed micro step's form of k_momentum: the same update with the elevation gradient's
 // difference zp - zm taken in FP64 (the elevations are FP64) and every other operation in FP32 on
 // the FP32 working copies (the Coriolis term with COR as well). Split into the Coriolis term and
-// the update of one point, which k_micro_tail shares.
+// the update of one point (momentum_core_f32 from the point's inputs), which the one- and
+// two-point kernels share.
 //
 // The Coriolis term of the DIR update at c (DIR 0: fV on U points from V at c-sj, c+1-sj, c, c+1;
 // DIR 1: fU on V points from U at c-1, c, c-1+sj, c+sj), given those four values in that order.
@@ -304,31 +305,42 @@ __device__ __forceinline__ float cor_term_f32(const Bc2& s, const Bc2W& w, long 
   const int m = DIR == 0 ? w.m8[1][c] : w.m8[2][c];
   return m >= 1 ? float(s.f2[DIR == 0 ? CORU : CORV][c]) * (0.25f * (a + b + e + f)) : 0.f;
 }
+// The new velocity of the DIR update at one point from its inputs: old value Xo, Coriolis term fCo,
+// elevation, depth H, total depth D, air pressure and surface stress at the point (c) and at the
+// next T point along the component (n), then the point's slow term, face depth, drying factor,
+// advection term, slow advection term and drag coefficient.
+template <int DIR>
+__device__ __forceinline__ float momentum_core_f32(const Dev& d, const Bc2& s, float Xo, float fCo, double zc, double zn,
+                                                   float Hc, float Hn, float Dc, float Dn, float ac, float an,
+                                                   float tc, float tn, float sl, float DXo, float dryo, float Exo,
+                                                   float Slxo, float ro) {
+  const float g = float(s.par[P_G]), rho_0 = float(s.par[P_RHO_0]), dtm = float(s.par[P_DTM]);
+  const double min_depth = s.par[P_MIN_DEPTH];
+  const float gammai = 1.f / (rho_0 * g);
+  const double zp = fmax(zn, -(double)Hc + fmin(min_depth, (double)Dn));
+  const double zm = fmax(zc, -(double)Hn + fmin(min_depth, (double)Dc));
+  const float zx = (float(zp - zm) + (an - ac) * gammai) / float(DIR == 0 ? d.dx : d.dy);
+  const float tau = 0.5f * (tc + tn);
+  const float Slr = Xo > 0.f ? fmaxf(sl, 0.f) : fminf(sl, 0.f);
+  const float fc = DIR == 0 ? -fCo : fCo;
+  return (Xo - dtm * (g * DXo * zx + dryo * (-tau / rho_0 + fc + Exo + Slxo + Slr))) / (1.f + dtm * ro / DXo);
+}
 // The new velocity of the DIR update at an interior point c whose mask is 1 or 2, from its old value
 // Xo and the Coriolis term fCo.
 template <int DIR>
 __device__ __forceinline__ float momentum_new_f32(const Dev& d, const Bc2& s, const Bc2W& w, long long c, float Xo,
                                                   float fCo) {
   const long long dn = DIR == 0 ? 1 : d.sj;  // the next T point along the component
-  const float* DX = w.w[DIR == 0 ? DU : DV];
   const float* D = w.w[D_];
   const float* airp = w.w[AIRP];
   const float* taus = w.w[DIR == 0 ? TAUSX : TAUSY];
   const double* z = s.f2[Z];
   const float* H = w.w[HH];
-  const float g = float(s.par[P_G]), rho_0 = float(s.par[P_RHO_0]), dtm = float(s.par[P_DTM]);
-  const double min_depth = s.par[P_MIN_DEPTH];
-  const float gammai = 1.f / (rho_0 * g);
-  const double zp = fmax(z[c + dn], -(double)H[c] + fmin(min_depth, (double)D[c + dn]));
-  const double zm = fmax(z[c], -(double)H[c + dn] + fmin(min_depth, (double)D[c]));
-  const float zx = (float(zp - zm) + (airp[c + dn] - airp[c]) * gammai) / float(DIR == 0 ? d.dx : d.dy);
-  const float tau = 0.5f * (taus[c] + taus[c + dn]);
-  const float sl = w.w[DIR == 0 ? SLRU : SLRV][c];
-  const float Slr = Xo > 0.f ? fmaxf(sl, 0.f) : fminf(sl, 0.f);
-  const float DXo = DX[c], dryo = w.w[DIR == 0 ? DRY_U : DRY_V][c], Exo = w.w[DIR == 0 ? UEX : VEX][c],
-              Slxo = w.w[DIR == 0 ? SLUX : SLVX][c], ro = w.w[DIR == 0 ? RU : RV][c];
-  const float fc = DIR == 0 ? -fCo : fCo;
-  return (Xo - dtm * (g * DXo * zx + dryo * (-tau / rho_0 + fc + Exo + Slxo + Slr))) / (1.f + dtm * ro / DXo);
+  return momentum_core_f32<DIR>(d, s, Xo, fCo, z[c], z[c + dn], H[c], H[c + dn], D[c], D[c + dn], airp[c],
+                                airp[c + dn], taus[c], taus[c + dn], w.w[DIR == 0 ? SLRU : SLRV][c],
+                                w.w[DIR == 0 ? DU : DV][c], w.w[DIR == 0 ? DRY_U : DRY_V][c],
+                                w.w[DIR == 0 ? UEX : VEX][c], w.w[DIR == 0 ? SLUX : SLVX][c],
+                                w.w[DIR == 0 ? RU : RV][c]);
 }
 
 template <int DIR, bool COR>
@@ -349,6 +361,99 @@ __global__ void k_momentum_f32(Dev d, Bc2 s, Bc2W w) {
   if (!(m == 1 || m == 2)) return;
   float* X = w.w[DIR == 0 ? U_ : V_];
   X[c] = momentum_new_f32<DIR>(d, s, w, c, X[c], w.w[DIR == 0 ? FV : FU][c]);
+}
+
+// k_momentum_f32 on two neighbouring points per thread (region columns 2t and 2t+1 of a row, for
+// layouts with an even row pitch): the inputs are loaded as pairs (float2, double2, uchar2), the
+// values at the next T point along the component are the pair's second element and one more load
+// (DIR 0) or a second pair (DIR 1). The same expressions per point, so the same values.
+__device__ __forceinline__ float2 ld_f2(const float* p) { return *reinterpret_cast<const float2*>(p); }
+__device__ __forceinline__ double2 ld_d2(const double* p) { return *reinterpret_cast<const double2*>(p); }
+template <int DIR, bool COR>
+__global__ void k_momentum_f32v(Dev d, Bc2 s, Bc2W w) {
+  const int ii = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int jj = blockIdx.y * blockDim.y + threadIdx.y;
+  if (ii >= d.ni() || jj >= d.nj()) return;
+  const int i0 = ii + d.imin - HALO, j = jj + d.jmin - HALO;
+  const bool in0 = interior(d, i0, j), in1 = interior(d, i0 + 1, j);
+  if (!in0 && !in1) return;
+  const long long c = (long long)jj * d.sj + ii;
+  const long long sj = d.sj;
+  const uchar2 mk = *reinterpret_cast<const uchar2*>(w.m8[DIR == 0 ? 1 : 2] + c);
+  float* fCp = w.w[DIR == 0 ? FV : FU];
+  float fC0, fC1;
+  if constexpr (COR) {
+    const double2 cor = ld_d2(s.f2[DIR == 0 ? CORU : CORV] + c);
+    if (DIR == 0) {  // fV on U points from V at c-sj, c+1-sj, c, c+1
+      const float* V = w.w[V_];
+      const float2 vs = ld_f2(V + c - sj), vc = ld_f2(V + c);
+      const float vs2 = V[c + 2 - sj], vc2 = V[c + 2];
+      fC0 = mk.x >= 1 ? float(cor.x) * (0.25f * (vs.x + vs.y + vc.x + vc.y)) : 0.f;
+      fC1 = mk.y >= 1 ? float(cor.y) * (0.25f * (vs.y + vs2 + vc.y + vc2)) : 0.f;
+    } else {  // fU on V points from U at c-1, c, c-1+sj, c+sj
+      const float* U = w.w[U_];
+      const float2 uc = ld_f2(U + c), up = ld_f2(U + c + sj);
+      const float um = U[c - 1], upm = U[c - 1 + sj];
+      fC0 = mk.x >= 1 ? float(cor.x) * (0.25f * (um + uc.x + upm + up.x)) : 0.f;
+      fC1 = mk.y >= 1 ? float(cor.y) * (0.25f * (uc.x + uc.y + up.x + up.y)) : 0.f;
+    }
+  } else {
+    const float2 f = ld_f2(fCp + c);
+    fC0 = f.x;
+    fC1 = f.y;
+  }
+  const bool u0 = in0 && (mk.x == 1 || mk.x == 2), u1 = in1 && (mk.y == 1 || mk.y == 2);
+  float* X = w.w[DIR == 0 ? U_ : V_];
+  float r0 = 0.f, r1 = 0.f;
+  if (u0 || u1) {
+    const float* D = w.w[D_];
+    const float* airp = w.w[AIRP];
+    const float* taus = w.w[DIR == 0 ? TAUSX : TAUSY];
+    const float* H = w.w[HH];
+    const double* z = s.f2[Z];
+    const float2 Xo = ld_f2(X + c), Hc = ld_f2(H + c), Dc = ld_f2(D + c), ac = ld_f2(airp + c), tc = ld_f2(taus + c);
+    const double2 zc = ld_d2(z + c);
+    double zn0, zn1;
+    float Hn0, Hn1, Dn0, Dn1, an0, an1, tn0, tn1;
+    if (DIR == 0) {
+      zn0 = zc.y;
+      zn1 = z[c + 2];
+      Hn0 = Hc.y;
+      Hn1 = H[c + 2];
+      Dn0 = Dc.y;
+      Dn1 = D[c + 2];
+      an0 = ac.y;
+      an1 = airp[c + 2];
+      tn0 = tc.y;
+      tn1 = taus[c + 2];
+    } else {
+      const double2 zn = ld_d2(z + c + sj);
+      const float2 Hn = ld_f2(H + c + sj), Dn = ld_f2(D + c + sj), an = ld_f2(airp + c + sj), tn = ld_f2(taus + c + sj);
+      zn0 = zn.x;
+      zn1 = zn.y;
+      Hn0 = Hn.x;
+      Hn1 = Hn.y;
+      Dn0 = Dn.x;
+      Dn1 = Dn.y;
+      an0 = an.x;
+      an1 = an.y;
+      tn0 = tn.x;
+      tn1 = tn.y;
+    }
+    const float2 sl = ld_f2(w.w[DIR == 0 ? SLRU : SLRV] + c), DX = ld_f2(w.w[DIR == 0 ? DU : DV] + c),
+                 dry = ld_f2(w.w[DIR == 0 ? DRY_U : DRY_V] + c), Ex = ld_f2(w.w[DIR == 0 ? UEX : VEX] + c),
+                 Slx = ld_f2(w.w[DIR == 0 ? SLUX : SLVX] + c), ro = ld_f2(w.w[DIR == 0 ? RU : RV] + c);
+    r0 = momentum_core_f32<DIR>(d, s, Xo.x, fC0, zc.x, zn0, Hc.x, Hn0, Dc.x, Dn0, ac.x, an0, tc.x, tn0, sl.x, DX.x,
+                                dry.x, Ex.x, Slx.x, ro.x);
+    r1 = momentum_core_f32<DIR>(d, s, Xo.y, fC1, zc.y, zn1, Hc.y, Hn1, Dc.y, Dn1, ac.y, an1, tc.y, tn1, sl.y, DX.y,
+                                dry.y, Ex.y, Slx.y, ro.y);
+  }
+  if constexpr (COR) {
+    if (in0) fCp[c] = fC0;
+    if (in1) fCp[c + 1] = fC1;
+  }
+  if (u0) X[c] = r0;
+  if (u1) X[c + 1] = r1;
 }
 
 // momentum.F90:193-216 / :356-379: Coriolis terms fU (after the U update) and fV (after V).
@@ -1094,6 +1199,19 @@ int bottom_friction_2d(getm_ctx* ctx, const getm_bc_state* st, int runtype, cons
   return e == cudaSuccess ? GETM_OK : cuda_fail(ctx, (int)e, "bottom_friction");
 }
 
+// the two-point velocity update applies: an even row pitch and plane size, the whole row pair in the
+// plane (an even number of columns), and pair-aligned FP64 and FP32 arrays
+bool pairs_ok(const Dev& d, const Bc2& s, const Bc2W& w) {
+  if (!vector_sweeps_enabled() || d.sj % 2 != 0 || d.ni() % 2 != 0) return false;
+  for (int q : {Z, CORU, CORV})
+    if (reinterpret_cast<uintptr_t>(s.f2[q]) % 16 != 0) return false;
+  for (int q : {U_, V_, D_, DU, DV, FU, FV, HH, AIRP, TAUSX, TAUSY, SLRU, SLRV, DRY_U, DRY_V, UEX, VEX, SLUX, SLVX, RU, RV})
+    if (reinterpret_cast<uintptr_t>(w.w[q]) % 8 != 0) return false;
+  for (int q = 1; q < 3; ++q)
+    if (reinterpret_cast<uintptr_t>(w.m8[q]) % 2 != 0) return false;
+  return true;
+}
+
 // umomentum (DIR 0, momentum.F90:69-223) / vmomentum (DIR 1, :232-386): the transport update, the
 // mirror_bdy_2d copies of the open boundaries (:190, :353) and the Coriolis term for the other
 // velocity (:193-216, :356-379). Mixed micro step (wp): the update on the working copies, with
@@ -1111,7 +1229,11 @@ int momentum_2d(getm_ctx* ctx, const getm_bc_state* st, const Bc2W* wp, bool cor
     TimerScope ts(ctx, GETM_TIM_BC2D);
     if (!wp && fused && cor) k_momentum<DIR, false, true><<<grid2(d), kBlk2, 0, cs>>>(d, s, w);
     else if (!wp) k_momentum<DIR, false><<<grid2(d), kBlk2, 0, cs>>>(d, s, w);
-    else if (cor) k_momentum_f32<DIR, true><<<grid2(d), kBlk2, 0, cs>>>(d, s, w);
+    else if (pairs_ok(d, s, w)) {
+      const dim3 gp((d.ni() / 2 + 31) / 32, (d.nj() + 3) / 4, 1);
+      if (cor) k_momentum_f32v<DIR, true><<<gp, kBlk2, 0, cs>>>(d, s, w);
+      else k_momentum_f32v<DIR, false><<<gp, kBlk2, 0, cs>>>(d, s, w);
+    } else if (cor) k_momentum_f32<DIR, true><<<grid2(d), kBlk2, 0, cs>>>(d, s, w);
     else k_momentum_f32<DIR, false><<<grid2(d), kBlk2, 0, cs>>>(d, s, w);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(ctx, (int)e, DIR == 0 ? "umomentum" : "vmomentum");
