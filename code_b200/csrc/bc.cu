@@ -616,6 +616,118 @@ __global__ void k_sealevel_depth(Dev d, Bc2 s, Bc2W w, int flags) {
   if (av(i, j) > 0) dry_v(i, j) = fmax(0.0, fmin(1.0, (DV_(i, j) - d1) * d2i));
 }
 
+// k_sealevel_depth<true> on two neighbouring points per thread (region columns 2t and 2t+1 of a row,
+// even row pitch): paired loads of the FP32 working copies, the FP64 elevations and the masks; the
+// new elevations of the pair, of the next point along the row and of the pair in the next row are
+// formed once each (the one-point form forms three per point). The same expressions, so the same
+// values; every load stays inside the haloed plane (the conditions are those of the one-point form).
+__global__ void k_sealevel_depth_p(Dev d, Bc2 s, Bc2W w, int flags) {
+  const int ii = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int jj = blockIdx.y * blockDim.y + threadIdx.y;
+  if (ii >= d.ni() || jj >= d.nj()) return;
+  const int i = ii + d.imin - HALO, j = jj + d.jmin - HALO;  // the pair's points: i, i+1
+  const long long c = (long long)jj * d.sj + ii, sj = d.sj;
+  const float *U = w.w[U_], *V = w.w[V_], *fwf = w.w[FWF], *H = w.w[HH], *HUa = w.w[HU], *HVa = w.w[HV];
+  float *D = w.w[D_], *DUa = w.w[DU], *DVa = w.w[DV], *dry_u = w.w[DRY_U], *dry_v = w.w[DRY_V];
+  const double* zold = s.f2[Z];
+  const uint8_t *az = w.m8[0], *au = w.m8[1], *av = w.m8[2];
+  const double dtm = s.par[P_DTM];
+  // sealevel.F90:94-108 from a point's inputs
+  auto zn_of = [&](bool upd, double zo_, float u0, float um, float v0, float vm, float f) -> double {
+    return upd ? zo_ - dtm * (((double)u0 * d.dy - (double)um * d.dy) + ((double)v0 * d.dx - (double)vm * d.dx)) *
+                           d.ard1 +
+                     dtm * f
+               : zo_;
+  };
+  const bool lastcol = i + 1 > d.imax + HALO - 1;  // the pair's second point has no DU (i+1 = imax+2)
+  const bool dvrow = j <= d.jmax + HALO - 1;
+  // row j: the pair and the point after it
+  const bool in0 = interior(d, i, j), in1 = interior(d, i + 1, j), in2 = interior(d, i + 2, j);
+  const double2 zo = ld_d2(zold + c);
+  const uchar2 a01 = *reinterpret_cast<const uchar2*>(az + c);
+  double z0, z1, z2 = 0.0, zo2 = 0.0;
+  {
+    float2 u = make_float2(0.f, 0.f), v = u, vs = u, f = u;
+    float um = 0.f;
+    if (in0 || in1 || in2) {  // (the point after the pair reads U at i+1)
+      u = ld_f2(U + c);
+      v = ld_f2(V + c);
+      vs = ld_f2(V + c - sj);
+      f = ld_f2(fwf + c);
+    }
+    if (in0) um = U[c - 1];
+    z0 = zn_of(in0 && a01.x == 1, zo.x, u.x, um, v.x, vs.x, f.x);
+    z1 = zn_of(in1 && a01.y == 1, zo.y, u.y, u.x, v.y, vs.y, f.y);
+    if (!lastcol) {
+      zo2 = zold[c + 2];
+      if (in2 && az[c + 2] == 1) z2 = zn_of(true, zo2, U[c + 2], u.y, V[c + 2], V[c + 2 - sj], fwf[c + 2]);
+      else z2 = zo2;
+    }
+  }
+  // row j+1: the pair
+  double2 zoN = make_double2(0.0, 0.0);
+  double zN0 = 0.0, zN1 = 0.0;
+  if (dvrow) {
+    const bool n0 = interior(d, i, j + 1), n1 = interior(d, i + 1, j + 1);
+    zoN = ld_d2(zold + c + sj);
+    const uchar2 aN = *reinterpret_cast<const uchar2*>(az + c + sj);
+    float2 u = make_float2(0.f, 0.f), v = u, vs = u, f = u;
+    float um = 0.f;
+    if (n0 || n1) {
+      u = ld_f2(U + c + sj);
+      v = ld_f2(V + c + sj);
+      vs = ld_f2(V + c);
+      f = ld_f2(fwf + c + sj);
+    }
+    if (n0) um = U[c - 1 + sj];
+    zN0 = zn_of(n0 && aN.x == 1, zoN.x, u.x, um, v.x, vs.x, f.x);
+    zN1 = zn_of(n1 && aN.y == 1, zoN.y, u.y, u.x, v.y, vs.y, f.y);
+  }
+  if (flags & 1) {
+    double2 ui = ld_d2(s.f2[UINT] + c), vi = ld_d2(s.f2[VINT] + c);
+    const float2 u = ld_f2(U + c), v = ld_f2(V + c);
+    ui.x = ui.x + u.x;
+    ui.y = ui.y + u.y;
+    vi.x = vi.x + v.x;
+    vi.y = vi.y + v.y;
+    *reinterpret_cast<double2*>(s.f2[UINT] + c) = ui;
+    *reinterpret_cast<double2*>(s.f2[VINT] + c) = vi;
+  }
+  *reinterpret_cast<double2*>(s.f2[ZO] + c) = make_double2(z0, z1);
+  // depth_update.F90:55-110
+  const double min_depth = s.par[P_MIN_DEPTH], crit_depth = s.par[P_CRIT_DEPTH];
+  const float2 Hc = ld_f2(H + c), HUc = ld_f2(HUa + c), HVc = ld_f2(HVa + c);
+  const float2 Dn = make_float2(float(z0 + Hc.x), float(z1 + Hc.y));
+  *reinterpret_cast<float2*>(D + c) = Dn;
+  float2 DUn, DVn;
+  DUn.x = float(fmax(0.25 * (zo.x + zo.y + z0 + z1), -HUc.x + min_depth) + HUc.x);
+  if (!lastcol) {
+    DUn.y = float(fmax(0.25 * (zo.y + zo2 + z1 + z2), -HUc.y + min_depth) + HUc.y);
+    *reinterpret_cast<float2*>(DUa + c) = DUn;
+  } else {
+    DUa[c] = DUn.x;
+    DUn.y = DUa[c + 1];  // not updated at imax+2, as in the one-point form
+  }
+  if (dvrow) {
+    DVn.x = float(fmax(0.25 * (zo.x + zoN.x + z0 + zN0), -HVc.x + min_depth) + HVc.x);
+    DVn.y = float(fmax(0.25 * (zo.y + zoN.y + z1 + zN1), -HVc.y + min_depth) + HVc.y);
+    *reinterpret_cast<float2*>(DVa + c) = DVn;
+  } else {
+    DVn = ld_f2(DVa + c);
+  }
+  const double d1 = 2 * min_depth;
+  const double d2i = 1.0 / (crit_depth - 2 * min_depth);
+  if (flags & 2) {
+    if (a01.x > 0) s.f2[DRY_Z][c] = fmax(0.0, fmin(1.0, ((double)Dn.x - 0.5 * d1) * d2i));
+    if (a01.y > 0) s.f2[DRY_Z][c + 1] = fmax(0.0, fmin(1.0, ((double)Dn.y - 0.5 * d1) * d2i));
+  }
+  const uchar2 mu = *reinterpret_cast<const uchar2*>(au + c), mv = *reinterpret_cast<const uchar2*>(av + c);
+  if (mu.x > 0) dry_u[c] = float(fmax(0.0, fmin(1.0, ((double)DUn.x - d1) * d2i)));
+  if (mu.y > 0) dry_u[c + 1] = float(fmax(0.0, fmin(1.0, ((double)DUn.y - d1) * d2i)));
+  if (mv.x > 0) dry_v[c] = float(fmax(0.0, fmin(1.0, ((double)DVn.x - d1) * d2i)));
+  if (mv.y > 0) dry_v[c + 1] = float(fmax(0.0, fmin(1.0, ((double)DVn.y - d1) * d2i)));
+}
+
 // exchanges the contents of two 2D FP64 arrays (the elevation ping-pong's last state)
 __global__ void k_swap2(long long n2, double* a, double* b) {
   for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n2; c += (long long)gridDim.x * blockDim.x) {
@@ -1199,15 +1311,16 @@ int bottom_friction_2d(getm_ctx* ctx, const getm_bc_state* st, int runtype, cons
   return e == cudaSuccess ? GETM_OK : cuda_fail(ctx, (int)e, "bottom_friction");
 }
 
-// the two-point velocity update applies: an even row pitch and plane size, the whole row pair in the
-// plane (an even number of columns), and pair-aligned FP64 and FP32 arrays
+// the two-point kernels (velocity update, sealevel + depth_update) apply: an even row pitch and an
+// even number of columns (a pair never straddles the plane's edge), pair-aligned FP64 and FP32 arrays
 bool pairs_ok(const Dev& d, const Bc2& s, const Bc2W& w) {
   if (!vector_sweeps_enabled() || d.sj % 2 != 0 || d.ni() % 2 != 0) return false;
-  for (int q : {Z, CORU, CORV})
+  for (int q : {Z, ZO, CORU, CORV, UINT, VINT})
     if (reinterpret_cast<uintptr_t>(s.f2[q]) % 16 != 0) return false;
-  for (int q : {U_, V_, D_, DU, DV, FU, FV, HH, AIRP, TAUSX, TAUSY, SLRU, SLRV, DRY_U, DRY_V, UEX, VEX, SLUX, SLVX, RU, RV})
+  for (int q : {U_, V_, D_, DU, DV, FU, FV, HH, HU, HV, FWF, AIRP, TAUSX, TAUSY, SLRU, SLRV, DRY_U, DRY_V, UEX, VEX,
+                SLUX, SLVX, RU, RV})
     if (reinterpret_cast<uintptr_t>(w.w[q]) % 8 != 0) return false;
-  for (int q = 1; q < 3; ++q)
+  for (int q = 0; q < 3; ++q)
     if (reinterpret_cast<uintptr_t>(w.m8[q]) % 2 != 0) return false;
   return true;
 }
@@ -1332,7 +1445,13 @@ int integrate_2d(getm_ctx* ctx, getm_bc_state* st, int loop, const Bc2W* wp = nu
   if (zswap) {
     if (ctx->has_bdy) return fail(ctx, GETM_ERR_STATE, "integrate_2d: fused sealevel with open boundaries");
     const int flags = (ip[I_RUNTYPE] > 1 ? 1 : 0) | (dryz ? 2 : 0);
-    rc = mix ? k2(k_sealevel_depth<true>, d, s, w, flags) : k2(k_sealevel_depth<false>, d, s, w, flags);
+    if (mix && pairs_ok(d, s, w)) {
+      TimerScope ts(ctx, GETM_TIM_BC2D);
+      k_sealevel_depth_p<<<dim3((d.ni() / 2 + 31) / 32, (d.nj() + 3) / 4, 1), kBlk2, 0, ctx->stream>>>(d, s, w, flags);
+      rc = (int)cudaGetLastError();
+    } else {
+      rc = mix ? k2(k_sealevel_depth<true>, d, s, w, flags) : k2(k_sealevel_depth<false>, d, s, w, flags);
+    }
     if (rc) return cuda_fail(ctx, rc, "sealevel + depth_update");
     std::swap(st->f2[Z], st->f2[ZO]);
     return nan_sweep_due(ctx, st, loop);
