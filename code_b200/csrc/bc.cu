@@ -1668,13 +1668,14 @@ int integrate_3d(getm_ctx* ctx, getm_bc_state* st, int n) {
                                   7u)))
         return rc;
       if (radn && (rc = temp_sources(s_top))) return rc;
-      // the two diffusion solves in one launch (shared hn, nuh); salinity's elimination
-      // coefficients in the macro-step scratch, free at this point of the step
+      // the two diffusion solves in one launch (shared hn, nuh); the elimination coefficients of
+      // both tracers, as interleaved (ru, qu) pairs, in the macro-step scratch (its first four
+      // slots, free at this point of the step)
       R3* b3 = (R3*)ctx->bc_scr3;
       GB_TIMED(GETM_TIM_VDIFF,
                run_vdiff2<R3>(d, s, dt, R3(st->par[P_CNPAR]), CH(COL_HN), f3[NUH], st->az, f3[TT],
-                              R3(st->par[P_AVMOLT]), (const R3*)tsrc, (R3*)ctx->scr[0], (R3*)ctx->scr[1], tlo,
-                              f3[SS], R3(st->par[P_AVMOLS]), b3, b3 + n3, slo, true),
+                              R3(st->par[P_AVMOLT]), (const R3*)tsrc, b3 + 2 * n3, nullptr, tlo, f3[SS],
+                              R3(st->par[P_AVMOLS]), b3, nullptr, slo, true),
                "vdiff T, S");
     }
     if (!pair && ip[I_CALC_TEMP]) {

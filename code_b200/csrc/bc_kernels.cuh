@@ -477,7 +477,7 @@ __global__ void __launch_bounds__(NT) k_uvmom3d(Dev d, Bc3<R3> s, R3* RUs, R3* Q
   const T dryij = T(dry(i, j)), corij = T(cor(i, j));
   const T ip_t = T(ip_fac), avm_t = T(avmmol), dt_t = T(dt), g_t = T(g);
   const T taus_top = T(dry(i, j) * 0.5 * (taus(i, j) + taus(i + di, j + dj)) * rho_0i);
-  // the level's inputs into slot k % UVM_SLOTS (an empty group for k < 0 keeps the counting uniform)
+  // the level's inputs into slot k % SL (an empty group for k < 0 keeps the counting uniform)
   auto issue = [&](int k) {
     if (k >= 0) {
       R3(*q)[NT] = sl[k & (SL - 1)];

@@ -2,6 +2,7 @@
 // Instantiated for double in kernels_f64.cu (built without FMA contraction so that every
 // expression rounds exactly as the reference's) and for float in kernels_f32.cu.
 #pragma once
+#include <type_traits>
 #include <cuda_fp16.h>
 #include "common.cuh"
 #include "launch.h"
@@ -956,7 +957,7 @@ struct VdSet {
 // for the back substitution. With two tracers the thread runs their two eliminations side by side
 // (independent chains) and loads hn and nuh once.
 // hsk: the level stride of hn (d.sk; 0 when hn is a 2D array of column heights)
-template <class R, int NF>
+template <class R, int NF, bool IL = false>
 __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, VdSet<R, NF> F, const R* __restrict__ hn,
                                                const R* __restrict__ nuh, const int32_t* __restrict__ az,
                                                long long hsk) {
@@ -967,6 +968,30 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, VdSet<R, NF
   const long long c = d.ix(i, j);
   if (az[c] != 1 || kmax <= 1) return;
   const long long sk = d.sk;
+  // the elimination coefficients ru(k), qu(k) of a tracer: two scratch arrays, or (IL) one array of
+  // (ru, qu) pairs at RU (twice the elements), one 8- or 16-byte access per level
+  using R2 = std::conditional_t<sizeof(R) == 4, float2, double2>;
+  auto put_rq = [&](const VdField<R>& f, int k, R r, R q) {
+    if constexpr (IL) {
+      R2 v;
+      v.x = r;
+      v.y = q;
+      reinterpret_cast<R2*>(f.RU)[c + k * sk] = v;
+    } else {
+      f.RU[c + k * sk] = r;
+      f.QU[c + k * sk] = q;
+    }
+  };
+  auto get_rq = [&](const VdField<R>& f, int k, R& r, R& q) {
+    if constexpr (IL) {
+      const R2 v = reinterpret_cast<const R2*>(f.RU)[c + k * sk];
+      r = v.x;
+      q = v.y;
+    } else {
+      r = f.RU[c + k * sk];
+      q = f.QU[c + k * sk];
+    }
+  };
   // the new value of level k from the old one and the increment: a plain FP32 sum, or the
   // compensated sum of the carried error lo (the tracer's compensated storage)
   // (lin: the level's stored carried error, loaded ahead by the caller)
@@ -1042,8 +1067,7 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, VdSet<R, NF
     if (f.src) a4 = a4 + srck;
     ru[n] = a1 / a2;
     qu[n] = a4 / a2;
-    f.RU[c + k * sk] = ru[n];
-    f.QU[c + k * sk] = qu[n];
+    put_rq(f, k, ru[n], qu[n]);
   }
   // inner rows k = kmax-1 .. 2
   for (k = kmax - 1; k >= 2; --k) {
@@ -1073,8 +1097,7 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, VdSet<R, NF
       const R den = a2 - a3 * ru[n];
       ru[n] = a1 / den;
       qu[n] = (a4 - a3 * qu[n]) / den;
-      f.RU[c + k * sk] = ru[n];
-      f.QU[c + k * sk] = qu[n];
+      put_rq(f, k, ru[n], qu[n]);
     }
   }
   cp_async_wait<0>();
@@ -1100,12 +1123,12 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, VdSet<R, NF
 #pragma unroll
   for (int n = 0; n < NF; ++n) {
     const VdField<R>& f = F.t[n];
-    qn[n] = kmax >= 2 ? f.QU[c + 2 * sk] : R(0);
-    rn[n] = kmax >= 2 ? f.RU[c + 2 * sk] : R(0);
+    qn[n] = rn[n] = R(0);
+    if (kmax >= 2) get_rq(f, 2, rn[n], qn[n]);
     sn[n] = (incr && kmax >= 2) ? f.Sin[c + 2 * sk] : R(0);
     ln[n] = kmax >= 2 ? lo_at(f, 2) : 0.f;
-    qn2[n] = kmax >= 3 ? f.QU[c + 3 * sk] : R(0);
-    rn2[n] = kmax >= 3 ? f.RU[c + 3 * sk] : R(0);
+    qn2[n] = rn2[n] = R(0);
+    if (kmax >= 3) get_rq(f, 3, rn2[n], qn2[n]);
     sn2[n] = (incr && kmax >= 3) ? f.Sin[c + 3 * sk] : R(0);
     ln2[n] = kmax >= 3 ? lo_at(f, 3) : 0.f;
   }
@@ -1117,8 +1140,7 @@ __global__ void __launch_bounds__(128) k_vdiff(Dev d, R dt, R cnpar, VdSet<R, NF
       const float lc = ln[n];
       qn[n] = qn2[n]; rn[n] = rn2[n]; sn[n] = sn2[n]; ln[n] = ln2[n];
       if (k + 2 <= kmax) {
-        qn2[n] = f.QU[c + (k + 2) * sk];
-        rn2[n] = f.RU[c + (k + 2) * sk];
+        get_rq(f, k + 2, rn2[n], qn2[n]);
         if (incr) sn2[n] = f.Sin[c + (k + 2) * sk];
         ln2[n] = lo_at(f, k + 2);
       }

@@ -222,7 +222,12 @@ int run_vdiff2(const Dev& d, cudaStream_t s, R dt, R cnpar, const R* hn, const R
   dim3 grd((nx + 31) / 32, (ny + 3) / 4, 1);
   VdSet<R, 2> F{{{Sa, Sa, src_a, rus_a, qus_a, nullptr, lo_a, avmol_a},
                  {Sb, Sb, nullptr, rus_b, qus_b, nullptr, lo_b, avmol_b}}};
-  k_vdiff<R, 2><<<grd, blk, 0, s>>>(d, dt, cnpar, F, hn, nuh, az, hn2d ? 0LL : d.sk);
+  // qus_a == qus_b == nullptr: each tracer's (ru, qu) pairs interleaved in its rus array (two
+  // elements per cell): one access per level instead of two
+  if (!qus_a && !qus_b)
+    k_vdiff<R, 2, true><<<grd, blk, 0, s>>>(d, dt, cnpar, F, hn, nuh, az, hn2d ? 0LL : d.sk);
+  else
+    k_vdiff<R, 2><<<grd, blk, 0, s>>>(d, dt, cnpar, F, hn, nuh, az, hn2d ? 0LL : d.sk);
   return (int)cudaGetLastError();
 }
 

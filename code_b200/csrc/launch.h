@@ -121,7 +121,9 @@ int run_vdiff(const Dev& d, cudaStream_t s, R dt, R cnpar, R avmol, R* S, const 
 // Two tracers (temperature a with its sources src_a, salinity b) diffused in one launch over the
 // same heights and diffusivity; each with its own molecular diffusivity, scratch pair and
 // compensated storage; each tracer's expressions are run_vdiff's. hn2d: hn is a 2D array of column
-// heights (every level of a column has that height).
+// heights (every level of a column has that height). qus_a == qus_b == nullptr: each tracer's
+// elimination coefficients go to its rus array as interleaved (ru, qu) pairs (2 * sk * (kmax+1)
+// elements).
 template <class R>
 int run_vdiff2(const Dev& d, cudaStream_t s, R dt, R cnpar, const R* hn, const R* nuh, const int32_t* az,
                R* Sa, R avmol_a, const R* src_a, R* rus_a, R* qus_a, __half* lo_a, R* Sb, R avmol_b, R* rus_b,
