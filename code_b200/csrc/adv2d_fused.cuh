@@ -270,12 +270,14 @@ __global__ void __launch_bounds__(FT) k_uvadv2d_fused(Dev d, T dt, const TI* __r
 }
 
 // Both components in one launch (blockIdx.z = 0: UEx on the U grid, 1: VEx on the V grid): the
-// same tiles as two k_uvadv2d_fused launches, one grid, one tail.
+// same tiles as two k_uvadv2d_fused launches, one grid, one tail. Four blocks per SM (32 registers,
+// no spills; the shared memory holds four): the issue-bound sweeps then have 64 warps to choose
+// from instead of 48.
 struct Adv2dMasks {
   const uint8_t *mflux_u, *mflux_v, *mupd_u, *mupd_v;
 };
 template <class T, int S, class TI>
-__global__ void __launch_bounds__(FT) k_uvadv2d_both(Dev d, T dt, const TI* __restrict__ U, const TI* __restrict__ V,
+__global__ void __launch_bounds__(FT, 4) k_uvadv2d_both(Dev d, T dt, const TI* __restrict__ U, const TI* __restrict__ V,
                                                      const TI* __restrict__ DU, const TI* __restrict__ DV,
                                                      Adv2dMasks mu, Adv2dMasks mv, TI* __restrict__ UEx,
                                                      TI* __restrict__ VEx, Bf2Args bfu, Bf2Args bfv) {

@@ -97,43 +97,61 @@ __global__ void k_ip(Dev d, Bc3<R3> s, const R3* zzp) {
   I2 au{d, s.au}, av{d, s.av};
   const int kmax = d.kmax;
   const R3 half = R3(0.5);
-  // one column: downward integral with hx the layer heights at the face (level-constant with
-  // equidistant sigma layers: the column's height is read once), (oi, oj) the neighbour across
-  // it; four levels' loads are issued before their stores
-  auto column = [&](V3<R3>& hx, V3<R3>& out, int oi, int oj, R3 dm1) {
-    R3 grdl = (buoy(i + oi, j + oj, kmax) - buoy(i, j, kmax)) * dm1;
-    R3 buoyl = half * (buoy(i + oi, j + oj, kmax) + buoy(i, j, kmax));
-    const R3 hc = hx(i, j, kmax);
-    R3 hk1 = hc;
-    R3 prgr = grdl * half * hk1;
-    out(i, j, kmax) = hk1 * prgr;
-    auto level = [&](int k, R3 b1, R3 b0, R3 z1, R3 z0, R3 hk) {
-      const R3 grdu = grdl;
-      grdl = (b1 - b0) * dm1;
-      const R3 buoyu = buoyl;
-      buoyl = half * (b1 + b0);
-      const R3 dz = (z1 - z0) * dm1;
-      prgr = prgr + half * (grdu + grdl) * half * (hk + hk1) - dz * (buoyu - buoyl);
-      out(i, j, k) = hk * prgr;
-      hk1 = hk;
-    };
-    int k = kmax - 1;
-    for (; k >= 4; k -= 4) {
-      R3 b1[4], b0[4], z1[4], z0[4];
-#pragma unroll
-      for (int m = 0; m < 4; ++m) {
-        b1[m] = buoy(i + oi, j + oj, k - m);
-        b0[m] = buoy(i, j, k - m);
-        z1[m] = zz(i + oi, j + oj, k - m);
-        z0[m] = zz(i, j, k - m);
-      }
-#pragma unroll
-      for (int m = 0; m < 4; ++m) level(k - m, b1[m], b0[m], z1[m], z0[m], hc);
-    }
-    for (; k >= 1; --k) level(k, buoy(i + oi, j + oj, k), buoy(i, j, k), zz(i + oi, j + oj, k), zz(i, j, k), hc);
+  // the point's U and V columns side by side: each a downward integral with its face's layer
+  // height (level-constant with equidistant sigma layers: read once) and its neighbour across the
+  // face ((i+1, j) and (i, j+1)); the loads of B levels of both columns are issued before their
+  // stores, the point's own buoyancy and interface heights loaded once for both
+  const bool uc = au(i, j) >= 1, vc = av(i, j) >= 1;
+  if (!uc && !vc) return;
+  struct Col {
+    R3 grdl, buoyl, hc, hk1, prgr, dm1;
   };
-  if (au(i, j) >= 1) column(hun, idpdx, 1, 0, R3(1.0 / d.dx));
-  if (av(i, j) >= 1) column(hvn, idpdy, 0, 1, R3(1.0 / d.dy));
+  auto start = [&](Col& c, V3<R3>& hx, V3<R3>& out, int oi, int oj, R3 dm1) {
+    c.dm1 = dm1;
+    c.grdl = (buoy(i + oi, j + oj, kmax) - buoy(i, j, kmax)) * dm1;
+    c.buoyl = half * (buoy(i + oi, j + oj, kmax) + buoy(i, j, kmax));
+    c.hc = hx(i, j, kmax);
+    c.hk1 = c.hc;
+    c.prgr = c.grdl * half * c.hk1;
+    out(i, j, kmax) = c.hk1 * c.prgr;
+  };
+  auto level = [&](Col& c, V3<R3>& out, int k, R3 b1, R3 b0, R3 z1, R3 z0) {
+    const R3 grdu = c.grdl;
+    c.grdl = (b1 - b0) * c.dm1;
+    const R3 buoyu = c.buoyl;
+    c.buoyl = half * (b1 + b0);
+    const R3 dz = (z1 - z0) * c.dm1;
+    c.prgr = c.prgr + half * (grdu + c.grdl) * half * (c.hc + c.hk1) - dz * (buoyu - c.buoyl);
+    out(i, j, k) = c.hc * c.prgr;
+    c.hk1 = c.hc;
+  };
+  Col cu{}, cv{};
+  if (uc) start(cu, hun, idpdx, 1, 0, R3(1.0 / d.dx));
+  if (vc) start(cv, hvn, idpdy, 0, 1, R3(1.0 / d.dy));
+  constexpr int B = sizeof(R3) == 4 ? 8 : 4;
+  int k = kmax - 1;
+  for (; k >= B; k -= B) {
+    R3 b0[B], z0[B], bu[B], zu[B], bv[B], zv[B];
+#pragma unroll
+    for (int m = 0; m < B; ++m) {
+      b0[m] = buoy(i, j, k - m);
+      z0[m] = zz(i, j, k - m);
+      bu[m] = uc ? buoy(i + 1, j, k - m) : R3(0);
+      zu[m] = uc ? zz(i + 1, j, k - m) : R3(0);
+      bv[m] = vc ? buoy(i, j + 1, k - m) : R3(0);
+      zv[m] = vc ? zz(i, j + 1, k - m) : R3(0);
+    }
+#pragma unroll
+    for (int m = 0; m < B; ++m) {
+      if (uc) level(cu, idpdx, k - m, bu[m], b0[m], zu[m], z0[m]);
+      if (vc) level(cv, idpdy, k - m, bv[m], b0[m], zv[m], z0[m]);
+    }
+  }
+  for (; k >= 1; --k) {
+    const R3 b0 = buoy(i, j, k), z0 = zz(i, j, k);
+    if (uc) level(cu, idpdx, k, buoy(i + 1, j, k), b0, zz(i + 1, j, k), z0);
+    if (vc) level(cv, idpdy, k, buoy(i, j + 1, k), b0, zz(i, j + 1, k), z0);
+  }
 }
 
 // ip_blumberg_mellor_lin.F90:87-97: heights of the pressure points (layer centres) of the
