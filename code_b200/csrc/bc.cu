@@ -1538,7 +1538,11 @@ int internal_pressure(getm_ctx* ctx, const getm_bc_state* st) {
                   : ipm == 5 ? BC3_IP_CF
                              : BC3_IP_SM;
   int rc;
-  if ((rc = bc3<R3>(ctx, st, ipm == 6 ? BC3_SM_COLS : centres ? BC3_ZZ_LIN : BC3_ZZ, GETM_TIM_BC3D))) return rc;
+  // the FP32 Blumberg-Mellor integral forms its interface heights itself (k_ip with ZS)
+  const bool zz_inside = sizeof(R3) == 4 && ipm == 1;
+  if (!zz_inside &&
+      (rc = bc3<R3>(ctx, st, ipm == 6 ? BC3_SM_COLS : centres ? BC3_ZZ_LIN : BC3_ZZ, GETM_TIM_BC3D)))
+    return rc;
   return bc3<R3>(ctx, st, ipk, GETM_TIM_IP);
 }
 

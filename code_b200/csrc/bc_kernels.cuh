@@ -86,11 +86,44 @@ __global__ void k_zz(Dev d, Bc3<R3> s, R3* zzp) {
 }
 
 // ip_blumberg_mellor.F90:94-148: downward integral of the buoyancy gradient per U and V column.
-template <class R3>
+// ZS (blocks of 32 x 4 points): the interface heights of the block's columns and of the next column
+// and row (the neighbours across the faces) are formed into dynamic shared memory with k_zz's
+// expressions, (kmax+1) x 5 x 33 values, instead of read from the zz array that k_zz writes.
+constexpr int IPZ_W = 33, IPZ_H = 5;
+template <class R3, bool ZS = false>
 __global__ void k_ip(Dev d, Bc3<R3> s, const R3* zzp) {
+  extern __shared__ unsigned char ip_smem[];
+  R3* const zsm = reinterpret_cast<R3*>(ip_smem);
+  auto zsh = [&](int k, int r, int q) -> R3& { return zsm[(k * IPZ_H + r) * IPZ_W + q]; };
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  if constexpr (ZS) {
+    const int i0 = blockIdx.x * 32 + d.imin - HALO, j0 = blockIdx.y * 4 + d.jmin - HALO;
+    V3<R3> hn{d, s.f3[HN]};
+    V2 H{d, s.f2[HH]};
+    I2 az{d, s.az};
+    for (int p = ty * 32 + tx; p < IPZ_W * IPZ_H; p += 128) {
+      const int r = p / IPZ_W, q = p - r * IPZ_W;
+      const int ii = i0 + q, jj = j0 + r;
+      // k_zz at (ii, jj); dry columns and those outside the plane are never read
+      if (ii > d.imax + HALO || jj > d.jmax + HALO || az(ii, jj) < 1) continue;
+      const R3 h = hn(ii, jj, d.kmax);
+      R3 z = R3(-H(ii, jj)) + h;
+      zsh(1, r, q) = z;
+      for (int k = 2; k <= d.kmax; ++k) {
+        z = z + h;
+        zsh(k, r, q) = z;
+      }
+    }
+    __syncthreads();
+  }
   GB_IJ_HALO
   V3<R3> hun{d, s.f3[HUN]}, hvn{d, s.f3[HVN]}, buoy{d, s.f3[BUOY]}, idpdx{d, s.f3[IDPDX]}, idpdy{d, s.f3[IDPDY]},
-      zz{d, const_cast<R3*>(zzp)};
+      zzg{d, const_cast<R3*>(zzp)};
+  // the interface height at level k of the point (di = dj = 0) or of its neighbour (1, 0) / (0, 1)
+  auto zz = [&](int ii, int jj, int k) -> R3 {
+    if constexpr (ZS) return zsh(k, ty + (jj - j), tx + (ii - i));
+    else return zzg(ii, jj, k);
+  };
   idpdx(i, j, 0) = R3(0);
   idpdy(i, j, 0) = R3(0);
   if (i < d.imin || i > d.imax || j < d.jmin || j > d.jmax) return;
@@ -1276,7 +1309,16 @@ int run_bc3(int which, const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* cons
   switch (which) {
     case BC3_BF3D: k_bf3d<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s); break;
     case BC3_ZZ: k_zz<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6]); break;
-    case BC3_IP: k_ip<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6]); break;
+    case BC3_IP:
+      if constexpr (sizeof(R3) == 4) {  // the interface heights formed in shared memory (no k_zz)
+        const size_t dyn = (size_t)(d.kmax + 1) * IPZ_H * IPZ_W * sizeof(R3);
+        const cudaError_t e = cudaFuncSetAttribute(k_ip<R3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+        if (e != cudaSuccess) return (int)e;
+        k_ip<R3, true><<<plane_grid(d, blk), blk, dyn, st>>>(d, s, nullptr);
+      } else {
+        k_ip<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6]);
+      }
+      break;
     case BC3_ZZ_LIN: k_zz_lin<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6]); break;
     case BC3_IP_LIN: k_ip_lin<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6]); break;
     case BC3_IP_SW: k_ip_sw<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6]); break;
