@@ -2200,7 +2200,9 @@ static int time_loop(getm_ctx* ctx, getm_bc_state* st, int n0, int count, bool z
       dirty = false;
       rc = st->prec3d == 8 ? integrate_3d<double>(ctx, st, n) : integrate_3d<float>(ctx, st, n);
       if (rc) return rc;
-      if (mix && (rc = sync(from3d, 1))) return rc;
+      // the macro step's 2D results into the working copies, unless the call ends here (the next
+      // call fills every working copy from the state anyway)
+      if (mix && n + 1 < n0 + count && (rc = sync(from3d, 1))) return rc;
     }
   }
   if ((mix || zswap) && count > 0) {
