@@ -266,6 +266,208 @@ __global__ void k_ip_lin(Dev d, Bc3<R3> s, const R3* zzp) {
   if (av(i, j) >= 1) column(hvn, hun(i, j, kmax), idpdy, 0, 1, R3(1.0 / d.dy));
 }
 
+// ip_z_interpol.F90:61-168 (pressure-point heights from k_zz_lin). Per U (V) column, downward from
+// kmax-1, the neighbour buoyancies at the face's own pressure-point height zx(k), found by a search
+// from the top for the first neighbour level at or below zx(k) and interpolated with the level
+// above. Where a search ends at level 1 or finds nothing the reference keeps buoyplus / buoyminus
+// of the previous level -- at a column's first levels, of the previous column in its loop order (j
+// outer, i inner, every U column before the V columns); both start at 0. The device form numbers
+// the columns in that order (position p: U columns 0 .. nx*ny-1, then the V columns) and runs in
+// three steps with the same results as the sequential loops:
+//   1. k_zi_cols<1>: every column runs with carried values of 0, writes its gradients and records
+//      whether it read a carried value before setting its own (need), and the last value it set
+//      with key p (key -1: it set none);
+//   2. k_zi_scan_blocks + k_zi_scan_aggs: an inclusive max-scan of the keys gives, for every
+//      position, the nearest preceding column that set the value;
+//   3. k_zi_cols<3>: the columns that read a carried value run again with it.
+template <class R3>
+struct ZiScr {
+  R3* last_p;  // per position: the last buoyplus / buoyminus the column set
+  R3* last_m;
+  int* key_p;  // p where the column set the value, else -1; scanned in place (per block of 1024)
+  int* key_m;
+  int* need;   // bit 0: read buoyplus before setting it; bit 1: buoyminus
+  int* agg_p;  // per block of 1024 positions: the block's largest key, then scanned
+  int* agg_m;
+  long long np;
+};
+constexpr int ZI_SCAN = 1024;
+
+template <class R3>
+struct ZiOut {
+  R3 bp, bm;
+  bool set_p, set_m, read_p, read_m;
+};
+
+// One column of ip_z_interpol with the carried values bp, bm coming in. zx(k) is formed upward in
+// the output column first and read back level by level as the downward loop overwrites it. A
+// level's search starts where the level above stopped whenever zx did not rise from that level (the
+// levels above it failed the test there, so they fail it again): the same index as a search from the
+// top, in fewer steps.
+template <class R3>
+__device__ ZiOut<R3> zi_column(const Dev& d, const Bc3<R3>& s, const R3* zzp, int i, int j, bool vg, R3 bp, R3 bm) {
+  V3<R3> hn{d, s.f3[HN]}, buoy{d, s.f3[BUOY]}, zz{d, const_cast<R3*>(zzp)};
+  V3<R3> hx{d, s.f3[vg ? HVN : HUN]}, out{d, s.f3[vg ? IDPDY : IDPDX]};
+  V2 H{d, s.f2[HH]}, Hx{d, s.f2[vg ? HV : HU]};
+  const int oi = vg ? 0 : 1, oj = vg ? 1 : 0;
+  const int kmax = d.kmax;
+  const R3 half = R3(0.5);
+  const R3 dm1 = vg ? R3(1.0 / d.dy) : R3(1.0 / d.dx);
+  ZiOut<R3> o{bp, bm, false, false, false, false};
+  R3 z = R3(-Hx(i, j)) + half * hx(i, j, 1);
+  out(i, j, 1) = z;
+  for (int k = 2; k <= kmax; ++k) {
+    z = z + half * (hx(i, j, k - 1) + hx(i, j, k));
+    out(i, j, k) = z;
+  }
+  const R3 zbed = R3(-H(i + oi, j + oj)), zbed0 = R3(-H(i, j));
+  R3 grdl = half * hx(i, j, kmax) * (buoy(i + oi, j + oj, kmax) - buoy(i, j, kmax)) * dm1;
+  R3 prgr = grdl;
+  out(i, j, kmax) = hx(i, j, kmax) * prgr;
+  int kp = kmax, km = kmax;
+  R3 zxa = R3(0);
+  for (int k = kmax - 1; k >= 1; --k) {
+    const R3 zx = out(i, j, k);
+    if (!(k < kmax - 1 && zx <= zxa)) kp = km = kmax;
+    zxa = zx;
+    const R3 grdu = grdl;
+    for (; kp >= 1; --kp)
+      if (zz(i + oi, j + oj, kp) <= zx) break;
+    for (; km >= 1; --km)
+      if (zz(i, j, km) <= zx) break;
+    if (kp == kmax) {
+      o.bp = buoy(i + oi, j + oj, kp);
+      o.set_p = true;
+    }
+    if (kp < kmax && kp > 1) {
+      o.bp = ((zx - zz(i + oi, j + oj, kp)) * buoy(i + oi, j + oj, kp + 1) +
+              (zz(i + oi, j + oj, kp + 1) - zx) * buoy(i + oi, j + oj, kp)) /
+             (half * (hn(i + oi, j + oj, kp + 1) + hn(i + oi, j + oj, kp)));
+      o.set_p = true;
+    }
+    if (km == kmax) {
+      o.bm = buoy(i, j, km);
+      o.set_m = true;
+    }
+    if (km < kmax && km > 1) {
+      o.bm = ((zx - zz(i, j, km)) * buoy(i, j, km + 1) + (zz(i, j, km + 1) - zx) * buoy(i, j, km)) /
+             (half * (hn(i, j, km + 1) + hn(i, j, km)));
+      o.set_m = true;
+    }
+    if (zx > zbed && zx > zbed0) {  // zx(k) > max(-H(i+oi,j+oj), -H(i,j))
+      o.read_p = o.read_p || !o.set_p;
+      o.read_m = o.read_m || !o.set_m;
+      grdl = half * hx(i, j, k) * (o.bp - o.bm) * dm1;
+    } else {
+      grdl = R3(0);
+    }
+    prgr = prgr + grdu + grdl;
+    out(i, j, k) = hx(i, j, k) * prgr;
+  }
+  return o;
+}
+
+// the largest key at or before this thread's in its block (blockDim.x = ZI_SCAN)
+static __device__ __forceinline__ int zi_block_max_scan(int v, int* sh) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int u = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v = max(v, u);
+  }
+  if (lane == 31) sh[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    int t = sh[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t = max(t, u);
+    }
+    sh[lane] = t;
+  }
+  __syncthreads();
+  const int r = w > 0 ? max(v, sh[w - 1]) : v;
+  __syncthreads();  // sh is reused by the caller's next scan
+  return r;
+}
+
+template <class R3, int PASS>
+__global__ void __launch_bounds__(128) k_zi_cols(Dev d, Bc3<R3> s, const R3* zzp, ZiScr<R3> z) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= z.np) return;
+  const int nx = d.imax - d.imin + 1;
+  const long long nn = z.np / 2;
+  const bool vg = p >= nn;
+  const long long q = vg ? p - nn : p;
+  const int i = d.imin + (int)(q % nx), j = d.jmin + (int)(q / nx);
+  I2 mask{d, vg ? s.av : s.au};
+  if (mask(i, j) < 1) {
+    if (PASS == 1) {
+      z.key_p[p] = -1;
+      z.key_m[p] = -1;
+      z.need[p] = 0;
+    }
+    return;
+  }
+  if (PASS == 1) {
+    const ZiOut<R3> o = zi_column<R3>(d, s, zzp, i, j, vg, R3(0), R3(0));
+    z.last_p[p] = o.bp;
+    z.last_m[p] = o.bm;
+    z.key_p[p] = o.set_p ? (int)p : -1;
+    z.key_m[p] = o.set_m ? (int)p : -1;
+    z.need[p] = (o.read_p ? 1 : 0) | (o.read_m ? 2 : 0);
+  } else {
+    const int need = z.need[p];
+    if (!need) return;
+    // the nearest preceding position that set the value: the scanned key of p-1 within its block,
+    // and the scanned aggregate of the blocks before it
+    auto prev = [&](const int* key, const int* agg) {
+      if (p == 0) return -1;
+      const long long b = (p - 1) / ZI_SCAN;
+      const int in_block = key[p - 1];
+      return b > 0 ? max(in_block, agg[b - 1]) : in_block;
+    };
+    const int pp = (need & 1) ? prev(z.key_p, z.agg_p) : -1;
+    const int pm = (need & 2) ? prev(z.key_m, z.agg_m) : -1;
+    const R3 bp = pp >= 0 ? z.last_p[pp] : R3(0);
+    const R3 bm = pm >= 0 ? z.last_m[pm] : R3(0);
+    zi_column<R3>(d, s, zzp, i, j, vg, bp, bm);
+  }
+}
+
+// in-place inclusive max-scan of both key arrays per block of ZI_SCAN positions; block maxima to agg
+static __global__ void __launch_bounds__(ZI_SCAN) k_zi_scan_blocks(int* key_p, int* key_m, int* agg_p, int* agg_m,
+                                                            long long np) {
+  __shared__ int sh[32];
+  const long long p = (long long)blockIdx.x * ZI_SCAN + threadIdx.x;
+  int* keys[2] = {key_p, key_m};
+  int* aggs[2] = {agg_p, agg_m};
+  for (int a = 0; a < 2; ++a) {
+    const int v = zi_block_max_scan(p < np ? keys[a][p] : -1, sh);
+    if (p < np) keys[a][p] = v;
+    if (threadIdx.x == ZI_SCAN - 1) aggs[a][blockIdx.x] = v;
+  }
+}
+
+// in-place inclusive max-scan of the nb block maxima (one block, chunks of ZI_SCAN)
+static __global__ void __launch_bounds__(ZI_SCAN) k_zi_scan_aggs(int* agg_p, int* agg_m, int nb) {
+  __shared__ int sh[32];
+  int* aggs[2] = {agg_p, agg_m};
+  for (int a = 0; a < 2; ++a) {
+    int carry = -1;
+    for (int c0 = 0; c0 < nb; c0 += ZI_SCAN) {
+      const int t = c0 + threadIdx.x;
+      const int v = max(zi_block_max_scan(t < nb ? aggs[a][t] : -1, sh), carry);
+      if (t < nb) aggs[a][t] = v;
+      if (threadIdx.x == ZI_SCAN - 1) sh[0] = v;
+      __syncthreads();
+      carry = sh[0];
+      __syncthreads();
+    }
+  }
+}
+
 // ip_song_wright.F90:99-150 (pressure-point heights from k_zz_lin): per U and V column the
 // gradient of the layer-mean buoyancy times the layer-mean height, less the change of the mean
 // buoyancy times the slope of the pressure points. The V column's first slope term is scaled by
@@ -1323,6 +1525,17 @@ int run_bc3(int which, const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* cons
     case BC3_IP_LIN: k_ip_lin<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6]); break;
     case BC3_IP_SW: k_ip_sw<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6]); break;
     case BC3_IP_CF: k_ip_cf<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6]); break;
+    case BC3_IP_ZI: {  // zz (from k_zz_lin) in scr[6]; the carried-value records in scr[0..5]
+      const long long np = 2LL * (d.imax - d.imin + 1) * (d.jmax - d.jmin + 1);
+      const int nb = (int)((np + ZI_SCAN - 1) / ZI_SCAN);
+      ZiScr<R3> z{scr[0], scr[4], (int*)scr[1], (int*)scr[5], (int*)scr[2], (int*)scr[3], (int*)scr[3] + nb, np};
+      const int g = (int)((np + 127) / 128);
+      k_zi_cols<R3, 1><<<g, 128, 0, st>>>(d, s, scr[6], z);
+      k_zi_scan_blocks<<<nb, ZI_SCAN, 0, st>>>(z.key_p, z.key_m, z.agg_p, z.agg_m, np);
+      k_zi_scan_aggs<<<1, ZI_SCAN, 0, st>>>(z.agg_p, z.agg_m, nb);
+      k_zi_cols<R3, 3><<<g, 128, 0, st>>>(d, s, scr[6], z);
+      break;
+    }
     case BC3_SM_COLS: k_sm_cols<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6], scr[0]); break;
     case BC3_IP_SM: k_ip_sm<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6], scr[0]); break;
     case BC3_UUMOM:

@@ -10,7 +10,7 @@
 //
 // Scope: runtype 4 (prognostic T and S); open boundaries of the four 2D types (update_2d_bdy,
 // mirror_bdy_2d/3d); vert_cord = 1 with equidistant sigma; eqstate_method 1 (linear), 2 (UNESCO80)
-// or 3 (Jackett et al. 2006); ip_method 1, 2, 4, 5, 6; num/nuh prescribed (CONSTANT_VISCOSITY) or
+// or 3 (Jackett et al. 2006); ip_method 1 to 6; num/nuh prescribed (CONSTANT_VISCOSITY) or
 // the PARABOLIC_VISCOSITY profile of gotm(); short-wave radiation and surface heat flux in
 // do_temperature; sealevel_nan_check; no numerical-mixing analysis; no rivers; An_method = 0 and
 // Am = 0 (no horizontal momentum diffusion).
@@ -745,6 +745,72 @@ std::vector<R3> ip_heights(const Dom& d, BcState<R3>& st, bool centres) {
   return zz_;
 }
 
+// ip_z_interpol.F90:61-168: pressure-point heights; per U (then V) column, downward from kmax-1,
+// the neighbour buoyancies at the face's own pressure-point height zx(k), each found by a search
+// from the top for the first neighbour level at or below zx(k) and interpolated between it and the
+// level above. Where the search ends at level 1 or finds none, the reference keeps the value of
+// the previous level -- or, at a column's first level, of the previous column in loop order (j
+// outer, i inner, all U columns before all V columns) -- and 0 before any assignment (the
+// reference's locals are unset there; executed from source they start at 0). That carried state
+// makes the routine sequential in the loop order; it is restated here exactly so.
+template <class R3>
+void ip_z_interpol(const Dom& d, BcState<R3>& st) {
+  A3<R3> hn{d, st.f3[HN]}, hun{d, st.f3[HUN]}, hvn{d, st.f3[HVN]}, buoy{d, st.f3[BUOY]}, idpdx{d, st.f3[IDPDX]},
+      idpdy{d, st.f3[IDPDY]};
+  A2 H{d, st.f2[HH]}, HU_{d, st.f2[HU]}, HV_{d, st.f2[HV]};
+  M2 au{d, st.au}, av{d, st.av};
+  const int kmax = d.kmax;
+  const R3 dxm1 = R3(1.0 / d.dx), dym1 = R3(1.0 / d.dy), half = R3(0.5);
+  std::vector<R3> zz_ = ip_heights(d, st, true);
+  A3<R3> zz{d, zz_.data()};
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO; ++i) {
+      idpdx(i, j, 0) = R3(0);
+      idpdy(i, j, 0) = R3(0);
+    }
+  std::vector<R3> zx(kmax + 1);
+  R3 buoyplus = R3(0), buoyminus = R3(0);
+  // di, dj: the neighbour's offset; hx: hun or hvn; Hx: HU or HV; out: idpdx or idpdy
+  auto column = [&](int i, int j, int di, int dj, A3<R3>& hx, A2& Hx, A3<R3>& out, R3 dm1) {
+    zx[1] = R3(-Hx(i, j)) + half * hx(i, j, 1);
+    for (int k = 2; k <= kmax; ++k) zx[k] = zx[k - 1] + half * (hx(i, j, k - 1) + hx(i, j, k));
+    R3 grdl = half * hx(i, j, kmax) * (buoy(i + di, j + dj, kmax) - buoy(i, j, kmax)) * dm1;
+    R3 prgr = grdl;
+    out(i, j, kmax) = hx(i, j, kmax) * prgr;
+    for (int k = kmax - 1; k >= 1; --k) {
+      const R3 grdu = grdl;
+      int kplus = kmax;
+      for (; kplus >= 1; --kplus)
+        if (zz(i + di, j + dj, kplus) <= zx[k]) break;
+      int kminus = kmax;
+      for (; kminus >= 1; --kminus)
+        if (zz(i, j, kminus) <= zx[k]) break;
+      if (kplus == kmax) buoyplus = buoy(i + di, j + dj, kplus);
+      if (kplus < kmax && kplus > 1)
+        buoyplus = ((zx[k] - zz(i + di, j + dj, kplus)) * buoy(i + di, j + dj, kplus + 1) +
+                    (zz(i + di, j + dj, kplus + 1) - zx[k]) * buoy(i + di, j + dj, kplus)) /
+                   (half * (hn(i + di, j + dj, kplus + 1) + hn(i + di, j + dj, kplus)));
+      if (kminus == kmax) buoyminus = buoy(i, j, kminus);
+      if (kminus < kmax && kminus > 1)
+        buoyminus = ((zx[k] - zz(i, j, kminus)) * buoy(i, j, kminus + 1) +
+                     (zz(i, j, kminus + 1) - zx[k]) * buoy(i, j, kminus)) /
+                    (half * (hn(i, j, kminus + 1) + hn(i, j, kminus)));
+      if (zx[k] > std::max(R3(-H(i + di, j + dj)), R3(-H(i, j))))
+        grdl = half * hx(i, j, k) * (buoyplus - buoyminus) * dm1;
+      else
+        grdl = R3(0);
+      prgr = prgr + grdu + grdl;
+      out(i, j, k) = hx(i, j, k) * prgr;
+    }
+  };
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i)
+      if (au(i, j) >= 1) column(i, j, 1, 0, hun, HU_, idpdx, dxm1);
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i)
+      if (av(i, j) >= 1) column(i, j, 0, 1, hvn, HV_, idpdy, dym1);
+}
+
 // ip_song_wright.F90:86-150: pressure-point heights; per column the gradient of the layer-mean
 // buoyancy times the layer-mean height, less the change of the mean buoyancy times the slope of the
 // pressure points. The V column's first slope term is scaled by 1/dx (ip_song_wright.F90:128), as
@@ -930,6 +996,7 @@ int do_internal_pressure(const Dom& d, BcState<R3>& st) {
   switch (st.ipar[I_IP_METHOD]) {
     case 1: ip_blumberg_mellor(d, st); return 0;
     case 2: ip_blumberg_mellor_lin(d, st); return 0;
+    case 3: ip_z_interpol(d, st); return 0;
     case 4: ip_song_wright(d, st); return 0;
     case 5: ip_chu_fan(d, st); return 0;
     case 6: ip_shchepetkin_mcwilliams(d, st); return 0;

@@ -112,7 +112,7 @@ def test_update_2d_bdy_vs_oracle():
         assert np.array_equal(got.f2[k], want.f2[k], equal_nan=True), k
 
 
-@pytest.mark.parametrize("method", [1, 2, 4, 5, 6])
+@pytest.mark.parametrize("method", [1, 2, 3, 4, 5, 6])
 @pytest.mark.parametrize("prec", [8, 4], ids=["fp64", "fp32"])
 def test_internal_pressure_vs_oracle(method, prec):
     """getm_internal_pressure = do_internal_pressure with the state's ip_method: FP64 bit for bit;
@@ -303,3 +303,55 @@ def test_time_loop_nan_sweep(chk):
     torch.cuda.synchronize()
     assert raised == (chk > 0)
     assert st.ipar()["nan_warned"] == 1
+
+
+def _z_interpol_first_level_carries(c):
+    """U columns whose first level (kmax-1) in ip_z_interpol.F90:83-125 finds no neighbour or own
+    level to interpolate from (the search ends at level 1 or finds none) while below the surface
+    test, so that it reads the buoyancy carried from the previous column in the loop order."""
+    g = c.grid
+    K = g.kmax
+
+    def heights(Hb, h):
+        z = np.empty_like(h)
+        z[1] = -Hb + 0.5 * h[1]
+        for k in range(2, K + 1):
+            z[k] = z[k - 1] + 0.5 * (h[k - 1] + h[k])
+        return z
+
+    H = c.f2["H"]
+    zz, zx = heights(H, c.f3["hn"]), heights(c.f2["HU"], c.f3["hun"])
+    n = 0
+    for j in range(2, 2 + g.ny):
+        for i in range(2, 2 + g.nx):
+            if c.au[j, i] < 1:
+                continue
+            x = zx[K - 1, j, i]
+            kp = max([k for k in range(1, K + 1) if zz[k, j, i + 1] <= x], default=0)
+            km = max([k for k in range(1, K + 1) if zz[k, j, i] <= x], default=0)
+            n += (kp <= 1 or km <= 1) and x > max(-H[j, i + 1], -H[j, i])
+    return n
+
+
+def test_internal_pressure_z_interpol_carried_values():
+    """ip_method 3 (Z_INTERPOL) on a steep islands bed (2-600 m, 5 levels): dozens of U columns
+    start their downward loop without a level to interpolate from and read the buoyancies carried
+    from the previous column of the reference's sequential loops (the device form finds them by a
+    scan over the columns in loop order). FP64 bit for bit against the oracle, twice in a row on
+    one context (the scan's scratch starts from the previous call's contents)."""
+    import torch
+
+    c = S.baroclinic_case(nx=40, ny=28, kmax=5, recipe="islands", M=5, dt3=60.0, seed=11, land=0.3, hmin=2.0,
+                          hmax=600.0)
+    c.pi["ip_method"] = 3
+    assert _z_interpol_first_level_carries(c) >= 10
+    want = c.copy()
+    oracle.bc_call(want, "internal_pressure")
+    ctx, _ = make_ctx(c)
+    st = BcDevice(c, dtype3=torch.float64)
+    for _ in range(2):
+        ctx.internal_pressure(st)
+        torch.cuda.synchronize()
+        got = st.to_host(c.copy())
+        for k in ("idpdx", "idpdy"):
+            assert np.array_equal(got.f3[k], want.f3[k]), k
