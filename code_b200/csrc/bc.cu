@@ -1070,10 +1070,8 @@ int check_state(getm_ctx* ctx, const getm_bc_state* st) {
   if (st->ipar[I_M] < 1 || st->ipar[I_MM] < 1) return fail(ctx, GETM_ERR_ARG, "M and MM must be >= 1");
   if (st->ipar[I_IP_METHOD] < 1 || st->ipar[I_IP_METHOD] > 7)
     return fail(ctx, GETM_ERR_ARG, "ip_method must be 1..7 (internal_pressure.F90:149-168)");
-  if (st->ipar[I_IP_METHOD] == 7)
-    return fail(ctx, GETM_ERR_UNSUPPORTED,
-                "ip_method: BLUMBERG_MELLOR (1), BLUMBERG_MELLOR_LIN (2), Z_INTERPOL (3), SONG_WRIGHT (4), "
-                "CHU_FAN (5) and SHCHEPETKIN_MCWILLIAMS (6) are provided");
+  if (st->ipar[I_IP_METHOD] == 7 && ctx->dom.kmax > 64)  // the work arrays of k_svk_cols (SVK_KMAX)
+    return fail(ctx, GETM_ERR_UNSUPPORTED, "ip_method 7 (STELLING_VANKESTER): at most 64 levels");
   if ((size_t)2 * (ctx->dom.kmax + 1) * 64 * sizeof(double) > 200 * 1024)
     return fail(ctx, GETM_ERR_UNSUPPORTED, "kmax too large for the column solvers");
   return GETM_OK;
@@ -1526,15 +1524,16 @@ int bc3(getm_ctx* ctx, const getm_bc_state* st, int which, int slot, unsigned sk
 }
 
 // do_internal_pressure (internal_pressure.F90:181-274) with the configured method (check_state
-// admits 1 to 6): heights of the layer interfaces (1, 5) or of the pressure points (2, 3, 4; 6
+// admits 1 to 7): heights of the layer interfaces (1, 5) or of the pressure points (2, 3, 4, 7; 6
 // over the whole haloed domain, with its column integrals), then the gradients idpdx, idpdy
 template <class R3>
 int internal_pressure(getm_ctx* ctx, const getm_bc_state* st) {
   const int ipm = st->ipar[I_IP_METHOD];
-  const bool centres = ipm == 2 || ipm == 3 || ipm == 4;
+  const bool centres = ipm == 2 || ipm == 3 || ipm == 4 || ipm == 7;
   const int ipk = ipm == 1   ? BC3_IP
                   : ipm == 2 ? BC3_IP_LIN
                   : ipm == 3 ? BC3_IP_ZI
+                  : ipm == 7 ? BC3_IP_SVK
                   : ipm == 4 ? BC3_IP_SW
                   : ipm == 5 ? BC3_IP_CF
                              : BC3_IP_SM;

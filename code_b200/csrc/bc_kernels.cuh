@@ -468,6 +468,164 @@ static __global__ void __launch_bounds__(ZI_SCAN) k_zi_scan_aggs(int* agg_p, int
   }
 }
 
+// ip_stelling_vankester.F90:56-398 (pressure-point heights from k_zz_lin, interface heights zi
+// from k_svk_zi). Per U (V) column the interface heights of both columns and the face's surface are
+// sorted into zl (the reference's exchange sort, in the thread's local memory); each interval adds
+// its height times the limited buoyancy difference db; level k takes the integral down to zx(k).
+// The reference's work arrays lvel and dzfrac keep the previous column's values wherever the
+// interval loop does not reach a level (kcount > 0 at its end), and db is not reset per V column.
+// Every column whose loop reaches all levels sets them all before reading them, so the parallel
+// pass (one thread per column) gives the sequential result; a column that does not reach them
+// raises a flag, and then one thread redoes every column in the reference's loop order with the
+// carried arrays (k_svk_serial). Levels up to SVK_KMAX.
+constexpr int SVK_KMAX = 64;
+constexpr int SVK_L = 2 * SVK_KMAX + 1;
+
+template <class R3>
+struct SvkWork {
+  R3 zx[SVK_KMAX + 1], zl[SVK_L + 1], dzl[SVK_L + 1], dzfrac[SVK_KMAX + 1];
+  int lvel[SVK_KMAX + 2], m[SVK_L + 1], n[SVK_L + 1];
+};
+
+template <class R3>
+__global__ void k_svk_zi(Dev d, Bc3<R3> s, R3* zip) {
+  GB_IJ_HALO
+  if (i < d.imin || i > d.imax + 1 || j < d.jmin || j > d.jmax + 1) return;
+  I2 az{d, s.az};
+  if (az(i, j) < 1) return;
+  V3<R3> hn{d, s.f3[HN]}, zi{d, zip};
+  V2 H{d, s.f2[HH]};
+  R3 z = R3(-H(i, j));
+  zi(i, j, 1) = z;
+  for (int k = 2; k <= d.kmax; ++k) {
+    z = z + hn(i, j, k - 1);
+    zi(i, j, k) = z;
+  }
+}
+
+// one column; returns the levels the interval loop left unset (kcount). par: the parallel pass,
+// which then writes nothing (the serial pass redoes the column with the carried arrays). Where the
+// reference would read lvel below 1 (a level no column has reached yet; outside its work arrays)
+// the interval loop stops at 1.
+template <class R3>
+__device__ int svk_column(const Dev& d, const Bc3<R3>& s, const R3* zzp, const R3* zip, int i, int j, bool vg,
+                          SvkWork<R3>& w, R3& db, bool par) {
+  V3<R3> buoy{d, s.f3[BUOY]}, zz{d, const_cast<R3*>(zzp)}, zi{d, const_cast<R3*>(zip)};
+  V3<R3> hx{d, s.f3[vg ? HVN : HUN]}, out{d, s.f3[vg ? IDPDY : IDPDX]};
+  V2 Hx{d, s.f2[vg ? HV : HU]}, ssx{d, s.f2[vg ? SSVN : SSUN]};
+  const int di = vg ? 0 : 1, dj = vg ? 1 : 0, i1 = i + di, j1 = j + dj;
+  const int kmax = d.kmax, lnum = 2 * kmax + 1;
+  const R3 half = R3(0.5);
+  const R3 dm1 = vg ? R3(1.0 / d.dy) : R3(1.0 / d.dx);
+  w.zx[1] = R3(-Hx(i, j)) + half * hx(i, j, 1);
+  w.zl[1] = zi(i, j, 1);
+  w.zl[2] = zi(i1, j1, 1);
+  for (int k = 2; k <= kmax; ++k) {
+    w.zx[k] = w.zx[k - 1] + half * (hx(i, j, k - 1) + hx(i, j, k));
+    w.zl[2 * k - 1] = zi(i, j, k);
+    w.zl[2 * k] = zi(i1, j1, k);
+  }
+  w.zl[lnum] = R3(ssx(i, j));
+  for (bool changed = true; changed;) {  // ends: every pass that swaps removes an inversion
+    changed = false;
+    for (int l = 1; l <= lnum - 1; ++l)
+      if (w.zl[l] > w.zl[l + 1]) {
+        const R3 t = w.zl[l + 1];
+        w.zl[l + 1] = w.zl[l];
+        w.zl[l] = t;
+        changed = true;
+      }
+  }
+  w.m[lnum] = kmax;
+  w.n[lnum] = kmax;
+  int kcount = kmax;
+  w.lvel[kmax + 1] = lnum;
+  for (int l = lnum - 1; l >= 1; --l) {
+    w.dzl[l] = w.zl[l + 1] - w.zl[l];
+    w.m[l] = w.m[l + 1];
+    w.n[l] = w.n[l + 1];
+    if (w.zl[l + 1] <= zi(i, j, w.m[l])) w.m[l] = max(1, w.m[l] - 1);
+    if (w.zl[l + 1] <= zi(i1, j1, w.n[l])) w.n[l] = max(1, w.n[l] - 1);
+    if (kcount > 0 && w.zx[kcount] > w.zl[l]) {
+      w.lvel[kcount] = l;
+      w.dzfrac[kcount] = w.zx[kcount] - w.zl[l];
+      --kcount;
+    }
+  }
+  if (par && kcount > 0) return kcount;
+  R3 prgr = R3(0);
+  if (!vg) db = R3(0);
+  for (int k = kmax; k >= 1; --k) {
+    for (int l = w.lvel[k + 1] - 1; l >= max(w.lvel[k], 1); --l) {
+      const int ml = w.m[l], nl = w.n[l];
+      const R3 zn = zz(i1, j1, nl), zm = zz(i, j, ml);
+      R3 bminus, bplus;
+      if (zn >= zz(i, j, kmax)) bminus = buoy(i, j, kmax);
+      else if (zn <= zz(i, j, 1)) bminus = buoy(i, j, 1);
+      else {
+        const int kl = zn >= zm ? ml : ml - 1, ku = zn >= zm ? ml + 1 : ml;
+        const R3 dzz = zz(i, j, ku) - zz(i, j, kl);
+        bminus = (zn - zz(i, j, kl)) / dzz * buoy(i, j, ku) + (zz(i, j, ku) - zn) / dzz * buoy(i, j, kl);
+      }
+      if (zm >= zz(i1, j1, kmax)) bplus = buoy(i1, j1, kmax);
+      else if (zm <= zz(i1, j1, 1)) bplus = buoy(i1, j1, 1);
+      else {
+        const int kl = zm >= zn ? nl : nl - 1, ku = zm >= zn ? nl + 1 : nl;
+        const R3 dzz = zz(i1, j1, ku) - zz(i1, j1, kl);
+        bplus = (zm - zz(i1, j1, kl)) / dzz * buoy(i1, j1, ku) + (zz(i1, j1, ku) - zm) / dzz * buoy(i1, j1, kl);
+      }
+      const R3 dcm = buoy(i1, j1, nl) - bminus;
+      const R3 dcn = bplus - buoy(i, j, ml);
+      const R3 mn = dcm < dcn ? dcm : dcn, mx = dcn < dcm ? dcm : dcn;
+      if (dcn * dcm < R3(0)) db = R3(0);
+      else if (!vg) db = dcn >= R3(0) ? mn : mx;
+      else {
+        if (dcn >= R3(0)) db = mn;
+        if (dcn <= R3(0)) db = mx;
+      }
+      prgr = prgr + w.dzl[l] * db * dm1;
+    }
+    out(i, j, k) = hx(i, j, k) * (prgr - w.dzfrac[k] * db * dm1);
+  }
+  return kcount;
+}
+
+// the parallel pass: positions in loop order (U columns, then V); flag: some column left levels
+template <class R3>
+__global__ void __launch_bounds__(128) k_svk_cols(Dev d, Bc3<R3> s, const R3* zzp, const R3* zip, int* flag,
+                                                  long long np) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= np) return;
+  const int nx = d.imax - d.imin + 1;
+  const long long nn = np / 2;
+  const bool vg = p >= nn;
+  const long long q = vg ? p - nn : p;
+  const int i = d.imin + (int)(q % nx), j = d.jmin + (int)(q / nx);
+  I2 mask{d, vg ? s.av : s.au};
+  if (mask(i, j) < 1) return;
+  SvkWork<R3> w;
+  R3 db = R3(0);
+  if (svk_column<R3>(d, s, zzp, zip, i, j, vg, w, db, true) > 0) atomicOr(flag, 1);
+}
+
+// the reference's loops in their order with the carried work arrays; only when flagged
+template <class R3>
+__global__ void k_svk_serial(Dev d, Bc3<R3> s, const R3* zzp, const R3* zip, const int* flag) {
+  if (*flag == 0) return;
+  SvkWork<R3> w;
+  for (int k = 0; k <= SVK_KMAX; ++k) {
+    w.dzfrac[k] = R3(0);
+    w.lvel[k] = 0;
+  }
+  w.lvel[SVK_KMAX + 1] = 0;
+  R3 db = R3(0);
+  I2 au{d, s.au}, av{d, s.av};
+  for (int g = 0; g < 2; ++g)
+    for (int j = d.jmin; j <= d.jmax; ++j)
+      for (int i = d.imin; i <= d.imax; ++i)
+        if ((g ? av(i, j) : au(i, j)) >= 1) svk_column<R3>(d, s, zzp, zip, i, j, g == 1, w, db, false);
+}
+
 // ip_song_wright.F90:99-150 (pressure-point heights from k_zz_lin): per U and V column the
 // gradient of the layer-mean buoyancy times the layer-mean height, less the change of the mean
 // buoyancy times the slope of the pressure points. The V column's first slope term is scaled by
@@ -1525,6 +1683,15 @@ int run_bc3(int which, const Dev& d, cudaStream_t st, const Bc3<R3>& s, R3* cons
     case BC3_IP_LIN: k_ip_lin<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6]); break;
     case BC3_IP_SW: k_ip_sw<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6]); break;
     case BC3_IP_CF: k_ip_cf<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[6]); break;
+    case BC3_IP_SVK: {  // zz (from k_zz_lin) in scr[6]; zi in scr[5]; the flag in scr[0]
+      const long long np = 2LL * (d.imax - d.imin + 1) * (d.jmax - d.jmin + 1);
+      int* flag = (int*)scr[0];
+      cudaMemsetAsync(flag, 0, sizeof(int), st);
+      k_svk_zi<R3><<<plane_grid(d, blk), blk, 0, st>>>(d, s, scr[5]);
+      k_svk_cols<R3><<<(int)((np + 127) / 128), 128, 0, st>>>(d, s, scr[6], scr[5], flag, np);
+      k_svk_serial<R3><<<1, 1, 0, st>>>(d, s, scr[6], scr[5], flag);
+      break;
+    }
     case BC3_IP_ZI: {  // zz (from k_zz_lin) in scr[6]; the carried-value records in scr[0..5]
       const long long np = 2LL * (d.imax - d.imin + 1) * (d.jmax - d.jmin + 1);
       const int nb = (int)((np + ZI_SCAN - 1) / ZI_SCAN);

@@ -150,7 +150,7 @@ enum {
   BC3_BF3D = 0, BC3_ZZ, BC3_IP, BC3_UUMOM, BC3_VVMOM, BC3_SIGMA, BC3_WW, BC3_UVADV_PREP_U, BC3_UVADV_PREP_V,
   BC3_STRESSES, BC3_EQSTATE, BC3_SLOW_TERMS, BC3_UVADV_PREP_UV, BC3_ZZ_LIN, BC3_IP_LIN,
   BC3_IP_SW, BC3_IP_CF, BC3_SM_COLS, BC3_IP_SM, BC3_EQSTATE_UNESCO, BC3_EQSTATE_JACKETT, BC3_GOTM_PARABOLIC,
-  BC3_SW_RADIATION, BC3_TEMP_SOURCE, BC3_IP_ZI
+  BC3_SW_RADIATION, BC3_TEMP_SOURCE, BC3_IP_ZI, BC3_IP_SVK
 };
 // sealevel_nan_check sweep of the interior elevations (bc.cu, k_nan_sweep): cnt[0] +=
 // findings, cnt[1] = max(cnt[1], last loop-order index + 1); skipped while cnt[2] != 0

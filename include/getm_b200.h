@@ -230,8 +230,8 @@ int getm_tracer_step_f32(getm_ctx *ctx, float dt, float *f, const float *uu, con
  * ufirst2d / ufirst3d are the SAVEd alternation switches of momentum.F90:33 (initially 0) and
  * m3d.F90:504 (initially 1); the calls update them in the host-side struct. ip_method selects the
  * internal pressure gradient (internal_pressure.F90:80, 149-168): 1 = BLUMBERG_MELLOR,
- * 2 = BLUMBERG_MELLOR_LIN, 3 = Z_INTERPOL, 4 = SONG_WRIGHT, 5 = CHU_FAN, 6 = SHCHEPETKIN_MCWILLIAMS;
- * 7 returns GETM_ERR_UNSUPPORTED, other values GETM_ERR_ARG.
+ * 2 = BLUMBERG_MELLOR_LIN, 3 = Z_INTERPOL, 4 = SONG_WRIGHT, 5 = CHU_FAN, 6 = SHCHEPETKIN_MCWILLIAMS,
+ * 7 = STELLING_VANKESTER (kmax <= 64, else GETM_ERR_UNSUPPORTED); other values GETM_ERR_ARG.
  * viscosity: 0 = CONSTANT_VISCOSITY (num, nuh as given), 1 = PARABOLIC_VISCOSITY (gotm.F90:131-143:
  * the profile from taub after stresses_3d, plus avmback / avhback; tke and eps receive the
  * profiles when not NULL). eqstate_method (eqstate.F90:31): 1 linear, 2 UNESCO80, 3 Jackett et al.

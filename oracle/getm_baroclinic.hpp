@@ -10,7 +10,7 @@
 //
 // Scope: runtype 4 (prognostic T and S); open boundaries of the four 2D types (update_2d_bdy,
 // mirror_bdy_2d/3d); vert_cord = 1 with equidistant sigma; eqstate_method 1 (linear), 2 (UNESCO80)
-// or 3 (Jackett et al. 2006); ip_method 1 to 6; num/nuh prescribed (CONSTANT_VISCOSITY) or
+// or 3 (Jackett et al. 2006); ip_method 1 to 7; num/nuh prescribed (CONSTANT_VISCOSITY) or
 // the PARABOLIC_VISCOSITY profile of gotm(); short-wave radiation and surface heat flux in
 // do_temperature; sealevel_nan_check; no numerical-mixing analysis; no rivers; An_method = 0 and
 // Am = 0 (no horizontal momentum diffusion).
@@ -811,6 +811,115 @@ void ip_z_interpol(const Dom& d, BcState<R3>& st) {
       if (av(i, j) >= 1) column(i, j, 0, 1, hvn, HV_, idpdy, dym1);
 }
 
+// ip_stelling_vankester.F90:56-398: per U (then V) column the interface heights of both columns
+// and the face's surface are merged into one sorted list zl (the reference's exchange sort); each
+// interval of zl contributes its height times a limited buoyancy difference (the smaller of the two
+// one-sided differences of the interpolated neighbour buoyancies, 0 where they differ in sign),
+// and each level k takes the integral down to its pressure point zx(k). The work arrays lvel and
+// dzfrac keep their values from the previous column wherever the interval loop does not reach a
+// level; db is reset per U column but not per V column (the reference's V loop has no reset), and
+// its V form takes max(dcn, dcm) when dcn = 0 where the U form takes min. Work arrays and db start
+// at 0 (executed from source, the reference's locals do).
+template <class R3>
+void ip_stelling_vankester(const Dom& d, BcState<R3>& st) {
+  A3<R3> hn{d, st.f3[HN]}, hun{d, st.f3[HUN]}, hvn{d, st.f3[HVN]}, buoy{d, st.f3[BUOY]}, idpdx{d, st.f3[IDPDX]},
+      idpdy{d, st.f3[IDPDY]};
+  A2 H{d, st.f2[HH]}, HU_{d, st.f2[HU]}, HV_{d, st.f2[HV]}, ssun{d, st.f2[SSUN]}, ssvn{d, st.f2[SSVN]};
+  M2 az{d, st.az}, au{d, st.au}, av{d, st.av};
+  const int kmax = d.kmax, lnum = 2 * kmax + 1;
+  const R3 dxm1 = R3(1.0 / d.dx), dym1 = R3(1.0 / d.dy), half = R3(0.5);
+  std::vector<R3> zz_ = ip_heights(d, st, true), zi_(d.n3d(), R3(0));
+  A3<R3> zz{d, zz_.data()}, zi{d, zi_.data()};
+  for (int j = d.jmin; j <= d.jmax + 1; ++j)
+    for (int i = d.imin; i <= d.imax + 1; ++i)
+      if (az(i, j) >= 1) {
+        zi(i, j, 1) = R3(-H(i, j));
+        for (int k = 2; k <= kmax; ++k) zi(i, j, k) = zi(i, j, k - 1) + hn(i, j, k - 1);
+      }
+  for (int j = d.jmin - HALO; j <= d.jmax + HALO; ++j)
+    for (int i = d.imin - HALO; i <= d.imax + HALO; ++i) {
+      idpdx(i, j, 0) = R3(0);
+      idpdy(i, j, 0) = R3(0);
+    }
+  std::vector<R3> zx(kmax + 1), zl(lnum + 1), dzl(lnum + 1), dzfrac(kmax + 1, R3(0));
+  std::vector<int> lvel(kmax + 2, 0), m(lnum + 1), n(lnum + 1);
+  R3 db = R3(0);
+  auto column = [&](int i, int j, int di, int dj, A3<R3>& hx, A2& Hx, A2& ssx, A3<R3>& out, R3 dm1, bool vform) {
+    const int i1 = i + di, j1 = j + dj;
+    zx[1] = R3(-Hx(i, j)) + half * hx(i, j, 1);
+    zl[1] = zi(i, j, 1);
+    zl[2] = zi(i1, j1, 1);
+    for (int k = 2; k <= kmax; ++k) {
+      zx[k] = zx[k - 1] + half * (hx(i, j, k - 1) + hx(i, j, k));
+      zl[2 * k - 1] = zi(i, j, k);
+      zl[2 * k] = zi(i1, j1, k);
+    }
+    zl[lnum] = R3(ssx(i, j));
+    for (bool changed = true; changed;) {
+      changed = false;
+      for (int l = 1; l <= lnum - 1; ++l)
+        if (zl[l] > zl[l + 1]) {
+          std::swap(zl[l], zl[l + 1]);
+          changed = true;
+        }
+    }
+    m[lnum] = kmax;
+    n[lnum] = kmax;
+    int kcount = kmax;
+    lvel[kmax + 1] = lnum;
+    for (int l = lnum - 1; l >= 1; --l) {
+      dzl[l] = zl[l + 1] - zl[l];
+      m[l] = m[l + 1];
+      n[l] = n[l + 1];
+      if (zl[l + 1] <= zi(i, j, m[l])) m[l] = std::max(1, m[l] - 1);
+      if (zl[l + 1] <= zi(i1, j1, n[l])) n[l] = std::max(1, n[l] - 1);
+      if (kcount > 0 && zx[kcount] > zl[l]) {
+        lvel[kcount] = l;
+        dzfrac[kcount] = zx[kcount] - zl[l];
+        --kcount;
+      }
+    }
+    R3 prgr = R3(0);
+    if (!vform) db = R3(0);
+    for (int k = kmax; k >= 1; --k) {
+      for (int l = lvel[k + 1] - 1; l >= lvel[k]; --l) {
+        const R3 zn = zz(i1, j1, n[l]), zm = zz(i, j, m[l]);
+        R3 buoyminus, buoyplus;
+        if (zn >= zz(i, j, kmax)) buoyminus = buoy(i, j, kmax);
+        else if (zn <= zz(i, j, 1)) buoyminus = buoy(i, j, 1);
+        else {
+          const int klower = zn >= zm ? m[l] : m[l] - 1, kupper = zn >= zm ? m[l] + 1 : m[l];
+          const R3 dzz = zz(i, j, kupper) - zz(i, j, klower);
+          buoyminus = (zn - zz(i, j, klower)) / dzz * buoy(i, j, kupper) + (zz(i, j, kupper) - zn) / dzz * buoy(i, j, klower);
+        }
+        if (zm >= zz(i1, j1, kmax)) buoyplus = buoy(i1, j1, kmax);
+        else if (zm <= zz(i1, j1, 1)) buoyplus = buoy(i1, j1, 1);
+        else {
+          const int klower = zm >= zn ? n[l] : n[l] - 1, kupper = zm >= zn ? n[l] + 1 : n[l];
+          const R3 dzz = zz(i1, j1, kupper) - zz(i1, j1, klower);
+          buoyplus = (zm - zz(i1, j1, klower)) / dzz * buoy(i1, j1, kupper) + (zz(i1, j1, kupper) - zm) / dzz * buoy(i1, j1, klower);
+        }
+        const R3 dcm = buoy(i1, j1, n[l]) - buoyminus;
+        const R3 dcn = buoyplus - buoy(i, j, m[l]);
+        if (dcn * dcm < R3(0)) db = R3(0);
+        else if (!vform) db = dcn >= R3(0) ? std::min(dcn, dcm) : std::max(dcn, dcm);
+        else {
+          if (dcn >= R3(0)) db = std::min(dcn, dcm);
+          if (dcn <= R3(0)) db = std::max(dcn, dcm);
+        }
+        prgr = prgr + dzl[l] * db * dm1;
+      }
+      out(i, j, k) = hx(i, j, k) * (prgr - dzfrac[k] * db * dm1);
+    }
+  };
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i)
+      if (au(i, j) >= 1) column(i, j, 1, 0, hun, HU_, ssun, idpdx, dxm1, false);
+  for (int j = d.jmin; j <= d.jmax; ++j)
+    for (int i = d.imin; i <= d.imax; ++i)
+      if (av(i, j) >= 1) column(i, j, 0, 1, hvn, HV_, ssvn, idpdy, dym1, true);
+}
+
 // ip_song_wright.F90:86-150: pressure-point heights; per column the gradient of the layer-mean
 // buoyancy times the layer-mean height, less the change of the mean buoyancy times the slope of the
 // pressure points. The V column's first slope term is scaled by 1/dx (ip_song_wright.F90:128), as
@@ -1000,6 +1109,7 @@ int do_internal_pressure(const Dom& d, BcState<R3>& st) {
     case 4: ip_song_wright(d, st); return 0;
     case 5: ip_chu_fan(d, st); return 0;
     case 6: ip_shchepetkin_mcwilliams(d, st); return 0;
+    case 7: ip_stelling_vankester(d, st); return 0;
     default: return -1;
   }
 }

@@ -1110,6 +1110,10 @@ class Gen:
             self.stmt(rest)
             self.ind -= 1
             return
+        if low == "do":  # a DO without control, left by EXIT
+            self.emit("while True:")
+            self.ind += 1
+            return
         m = re.match(r"^do\s+while\s*\((.*)\)$", low)
         if m:
             self.emit(f"while {tr_expr(m.group(1), sc)}:")

@@ -39,7 +39,7 @@ FILES = [
     "src/3d/start_macro.F90", "src/3d/stop_macro.F90", "src/3d/bottom_friction_3d.F90",
     "src/3d/internal_pressure.F90", "src/3d/ip_blumberg_mellor.F90", "src/3d/ip_blumberg_mellor_lin.F90",
     "src/3d/ip_z_interpol.F90", "src/3d/ip_song_wright.F90", "src/3d/ip_chu_fan.F90",
-    "src/3d/ip_shchepetkin_mcwilliams.F90",
+    "src/3d/ip_shchepetkin_mcwilliams.F90", "src/3d/ip_stelling_vankester.F90",
     "src/3d/uu_momentum_3d.F90",
     "src/3d/vv_momentum_3d.F90", "src/3d/coordinates.F90", "src/3d/sigma_coordinates.F90",
     "src/3d/ww_momentum_3d.F90", "src/3d/uv_advect_3d.F90", "src/3d/uv_diffusion_3d.F90", "src/3d/stresses_3d.F90",
@@ -261,7 +261,8 @@ def bdy_case():
 
 def ip_case(method):
     """12 x 10 x 5 islands basin (30% land) with another internal pressure method: 2
-    (BLUMBERG_MELLOR_LIN, ip_blumberg_mellor_lin.F90), 3 (Z_INTERPOL, ip_z_interpol.F90), 4 (SONG_WRIGHT, ip_song_wright.F90) or 5
+    (BLUMBERG_MELLOR_LIN, ip_blumberg_mellor_lin.F90), 3 (Z_INTERPOL, ip_z_interpol.F90), 7 (STELLING_VANKESTER,
+    ip_stelling_vankester.F90), 4 (SONG_WRIGHT, ip_song_wright.F90) or 5
     (CHU_FAN, ip_chu_fan.F90). The stratified recipe on a varying bed, so that the height slopes
     and the vertical buoyancy gradients both enter the gradient."""
     c = S.baroclinic_case(nx=12, ny=10, kmax=5, recipe="islands", land=0.3, M=4, dt3=60.0, seed=7)
@@ -444,13 +445,13 @@ def hotstart_fixture():
 
 
 def main():
-    which = sys.argv[1:] or ["closed", "bdy", "ip2", "ip3", "ip4", "ip5", "ip6", "phys3", "phys2", "nan", "hotstart"]
+    which = sys.argv[1:] or ["closed", "bdy", "ip2", "ip3", "ip4", "ip5", "ip6", "ip7", "phys3", "phys2", "nan", "hotstart"]
     if "closed" in which:
         write(S.baroclinic_case(nx=12, ny=10, kmax=4, recipe="shelf", M=4, dt3=60.0, seed=3),
               "reference_mode_split.npz")
     if "bdy" in which:
         write(bdy_case(), "reference_mode_split_bdy.npz")
-    for m in (2, 3, 4, 5, 6):
+    for m in (2, 3, 4, 5, 6, 7):
         if f"ip{m}" in which:
             write(ip_case(m), f"reference_mode_split_ip{m}.npz")
     if "phys3" in which:  # Jackett 2006, PARABOLIC_VISCOSITY, radiation with bottom reflection

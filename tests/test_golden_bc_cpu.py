@@ -3,7 +3,7 @@
 reference's Fortran source): every 2D and 3D field of the state, bit for bit, after two macro
 steps of four micro steps -- a closed basin, (reference_mode_split_bdy.npz) a basin with open
 boundaries of all four 2D types (update_2d_bdy, mirror_bdy_2d/3d), and
-(reference_mode_split_ip{2,3,4,5,6}.npz) islands basins with the linear Blumberg-Mellor, z-interpolation, Song-Wright,
+(reference_mode_split_ip{2,...,7}.npz) islands basins with the linear Blumberg-Mellor, z-interpolation, Stelling-van Kester, Song-Wright,
 Chu-Fan and Shchepetkin-McWilliams internal pressure."""
 import os
 
@@ -17,7 +17,7 @@ from code_b200.grid import Grid
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_mode_split.npz")
 GOLD_BDY = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_mode_split_bdy.npz")
 GOLD_IP = {m: os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", f"reference_mode_split_ip{m}.npz")
-           for m in (2, 3, 4, 5, 6)}
+           for m in (2, 3, 4, 5, 6, 7)}
 GOLD_IP2 = GOLD_IP[2]
 GOLD_PHYS = {m: os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", f"reference_mode_split_phys{m}.npz")
              for m in (2, 3)}
@@ -59,7 +59,7 @@ def gold_names(gold, kind):
     return [k for k in names if f"out_{kind}_{k}" in gold]
 
 
-GOLDS = {"closed": GOLD, "open boundaries": GOLD_BDY, **{f"ip_method {m}": GOLD_IP[m] for m in (2, 3, 4, 5, 6)},
+GOLDS = {"closed": GOLD, "open boundaries": GOLD_BDY, **{f"ip_method {m}": GOLD_IP[m] for m in (2, 3, 4, 5, 6, 7)},
          "radiation, UNESCO80": GOLD_PHYS[2], "radiation + bottom reflection, Jackett 2006, parabolic viscosity":
          GOLD_PHYS[3]}
 
@@ -83,7 +83,7 @@ def test_time_loop_matches_reference(gold):
     assert not bad, bad
 
 
-@pytest.mark.parametrize("method", [2, 3, 4, 5, 6])
+@pytest.mark.parametrize("method", [2, 3, 4, 5, 6, 7])
 def test_ip_method_fixture_differs_from_method_1(method):
     """Each internal-pressure fixture pins a method of its own: the oracle with Blumberg-Mellor (1)
     on the same inputs gives other internal pressure gradients."""

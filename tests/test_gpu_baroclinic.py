@@ -50,9 +50,8 @@ def run_gpu(c, n0, count, dtype3=None):
     return out, ctx
 
 
-@pytest.mark.parametrize("path", [GOLD, GOLD_BDY, GOLD_IP[2], GOLD_IP[3], GOLD_IP[4], GOLD_IP[5], GOLD_IP[6]],
-                         ids=["closed", "open boundaries", "ip_method 2", "ip_method 3", "ip_method 4", "ip_method 5",
-                              "ip_method 6"])
+@pytest.mark.parametrize("path", [GOLD, GOLD_BDY] + [GOLD_IP[m] for m in (2, 3, 4, 5, 6, 7)],
+                         ids=["closed", "open boundaries"] + [f"ip_method {m}" for m in (2, 3, 4, 5, 6, 7)])
 def test_time_loop_vs_reference_fixture(path):
     gold = dict(np.load(path))
     c = load_case(gold)
@@ -326,11 +325,11 @@ def test_fused_micro_step_forms_agree(prec, count):
         assert np.array_equal(out[True].f3[k], out[False].f3[k], equal_nan=True), k
 
 
-@pytest.mark.parametrize("method", [2, 3, 4, 5, 6])
+@pytest.mark.parametrize("method", [2, 3, 4, 5, 6, 7])
 @pytest.mark.parametrize("recipe", ["shelf", "islands"])
 def test_ip_method_vs_oracle(recipe, method):
     """The other internal pressure methods -- linear Blumberg-Mellor (2), z-interpolation (3),
-    Song-Wright (4), Chu-Fan
+    Stelling-van Kester (7), Song-Wright (4), Chu-Fan
     (5), Shchepetkin-McWilliams (6) -- through getm_time_loop against the oracle, FP64, 1e-12 of
     each field's scale."""
     c = S.baroclinic_case(nx=40, ny=28, kmax=10, recipe=recipe, M=5, dt3=60.0, seed=11, land=0.3)
@@ -343,7 +342,7 @@ def test_ip_method_vs_oracle(recipe, method):
     assert ctx.take_warnings() == 0
 
 
-@pytest.mark.parametrize("method", [2, 3, 4, 5, 6])
+@pytest.mark.parametrize("method", [2, 3, 4, 5, 6, 7])
 def test_ip_method_mixed_error_vs_fp64(method):
     """The mixed variant with internal pressure method 2, 4, 5 or 6 against the FP64 oracle after 10
     macro steps of the islands basin (the bounds of the Blumberg-Mellor case)."""
@@ -362,9 +361,9 @@ def test_ip_method_mixed_error_vs_fp64(method):
         assert errs[k] < 1e-3, errs
 
 
-@pytest.mark.parametrize("method,code", [(7, "GETM_ERR_UNSUPPORTED"), (0, "GETM_ERR_ARG"), (8, "GETM_ERR_ARG")])
+@pytest.mark.parametrize("method,code", [(0, "GETM_ERR_ARG"), (8, "GETM_ERR_ARG")])
 def test_ip_method_not_provided_is_refused(method, code):
-    """The method not provided (Stelling-van Kester 7) and invalid ids are
+    """Invalid ids are
     refused with an error code before any work (the reference stops on an invalid ip_method,
     internal_pressure.F90:166-167)."""
     from code_b200 import getm as G

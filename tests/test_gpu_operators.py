@@ -112,7 +112,7 @@ def test_update_2d_bdy_vs_oracle():
         assert np.array_equal(got.f2[k], want.f2[k], equal_nan=True), k
 
 
-@pytest.mark.parametrize("method", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("method", [1, 2, 3, 4, 5, 6, 7])
 @pytest.mark.parametrize("prec", [8, 4], ids=["fp64", "fp32"])
 def test_internal_pressure_vs_oracle(method, prec):
     """getm_internal_pressure = do_internal_pressure with the state's ip_method: FP64 bit for bit;
@@ -345,6 +345,26 @@ def test_internal_pressure_z_interpol_carried_values():
                           hmax=600.0)
     c.pi["ip_method"] = 3
     assert _z_interpol_first_level_carries(c) >= 10
+    want = c.copy()
+    oracle.bc_call(want, "internal_pressure")
+    ctx, _ = make_ctx(c)
+    st = BcDevice(c, dtype3=torch.float64)
+    for _ in range(2):
+        ctx.internal_pressure(st)
+        torch.cuda.synchronize()
+        got = st.to_host(c.copy())
+        for k in ("idpdx", "idpdy"):
+            assert np.array_equal(got.f3[k], want.f3[k]), k
+
+
+def test_internal_pressure_stelling_vankester_steep_bed():
+    """ip_method 7 (STELLING_VANKESTER) on the steep islands bed (2-600 m, 5 levels): FP64 bit for
+    bit against the oracle's sequential loops, twice in a row on one context."""
+    import torch
+
+    c = S.baroclinic_case(nx=40, ny=28, kmax=5, recipe="islands", M=5, dt3=60.0, seed=11, land=0.3, hmin=2.0,
+                          hmax=600.0)
+    c.pi["ip_method"] = 7
     want = c.copy()
     oracle.bc_call(want, "internal_pressure")
     ctx, _ = make_ctx(c)
