@@ -3,7 +3,7 @@
 small closed basin, together with the inputs. The oracle and the CUDA path are compared with it
 bit for bit (tests/test_golden_bc_cpu.py) and the CUDA path within 1e-12 (tests/test_gpu_baroclinic.py).
 
-    python tests/golden/make_golden_bc.py [closed] [bdy] [ip2] [ip4] [ip5]
+    python tests/golden/make_golden_bc.py [closed] [bdy] [ip2] ... [ip7] [phys3] [phys2] [nan] [hotstart]
 
 Configuration: runtype 4 (prognostic T and S), sigma coordinates (equidistant), linear equation of
 state, Blumberg-Mellor internal pressure (reference_mode_split_ip2.npz: the linear Blumberg-Mellor
